@@ -1,0 +1,211 @@
+/*
+ * mochii_gpu.h -- C ABI of the B200 photon-packet transport and
+ * ionisation/thermal-balance library (libmochii_gpu.so).
+ *
+ * The library replaces the four module entry points MoCHII's driver loop
+ * calls once per iteration (main.f90:128-185, :225):
+ *
+ *   ionizing_field_and_rates(label, with_peel)   ionizing_field_mod.f90:72
+ *   gas_equilibrium_update(max_dx, dx_vol)       ion_balance_mod.f90:352
+ *   gas_thermal_update(max_dx, max_dte, dx_vol, dte_vol)   thermal_mod.f90:124
+ *   gas_opacity_fill()                           gas_opacity_mod.f90:299
+ *
+ * and the parameter-file interface read_input (setup.f90:11-35, namelist
+ * "&parameters par%key = value /").  All signatures use plain C types,
+ * pointers and sizes; no CUDA or torch types cross the boundary.  Every
+ * call returns an int status (MOCHII_OK = 0).  Nothing aborts, traps or
+ * waits without a bound: device guards raise flags that are read after the
+ * stream synchronises and come back as status codes.
+ *
+ * Threading: one host thread per context; calls on one context are not
+ * reentrant.  Each context owns one CUDA stream on the device that was
+ * current when mochii_init ran.
+ */
+#ifndef MOCHII_GPU_H
+#define MOCHII_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes (reference: MPI_ABORT / error stop sites) ---------- */
+enum {
+    MOCHII_OK = 0,
+    MOCHII_ERR_BAD_PARAM = 1,     /* read_input validation, setup.f90:76-626      */
+    MOCHII_ERR_TABLE = 2,         /* unreadable / inconsistent data table          */
+    MOCHII_ERR_CUDA = 3,          /* CUDA runtime error                            */
+    MOCHII_ERR_TIMEOUT = 4,       /* a bounded device loop hit its cap             */
+    MOCHII_ERR_NONFINITE = 5,     /* NaN/Inf in a tally or state field             */
+    MOCHII_ERR_CLOSURE = 6,       /* energy closure > 5e-13, ion_score_mod.f90:386 */
+    MOCHII_ERR_NOT_CONVERGED = 7, /* require_convergence, main.f90:197-207         */
+    MOCHII_ERR_UNSUPPORTED = 8,   /* configuration outside the built path          */
+    MOCHII_ERR_NO_DEVICE = 9      /* no CUDA device visible                        */
+};
+
+#define MOCHII_MAX_SRC 16   /* define.f90:74 MAX_SRC */
+#define MOCHII_STRLEN 256
+
+/* Device arithmetic for the transport pass. */
+enum { MOCHII_PREC_FP64 = 0, MOCHII_PREC_FP32 = 1 };
+
+/*
+ * Parameters: the subset of type(params_type) (define.f90:189-861) that the
+ * transport + balance path reads, with the reference's names and defaults
+ * (mochii_params_default).  Strings are NUL-terminated.
+ */
+typedef struct mochii_params {
+    /* launch (define.f90:196-215) */
+    int64_t nphotons;                /* par%no_photons                        */
+    int launch_sobol;                /* par%launch_sequence == 'sobol'        */
+    int qmc_seed;                    /* par%qmc_seed                          */
+    double source_cdf_tol;           /* par%source_cdf_tol                    */
+    double luminosity;               /* par%luminosity [erg/s]                */
+    double tstar;                    /* par%tstar [K]                         */
+    int random_seed;                 /* par%iseed (counter RNG key)           */
+    /* band (define.f90 ion block) */
+    int nnu_ion;
+    double eion_min, eion_max;
+    int add_fuv;
+    double efuv_min;
+    int nnu_fuv;
+    int ion_align_edges;
+    /* geometry */
+    int grid_car;                    /* par%grid_type == 'car'                */
+    int car_walk_dda;                /* par%car_walk == 'dda'                 */
+    int nx, ny, nz;
+    double xmax, ymax, zmax;
+    double rmax, rmin, nH_const;
+    double distance2cm;              /* from par%distance_unit                */
+    char distance_unit[16];
+    char amr_file[MOCHII_STRLEN];
+    /* sources */
+    int source_point;                /* par%source_geometry == 'point'        */
+    double xs_point, ys_point, zs_point;
+    int nsource;
+    double src_tstar[MOCHII_MAX_SRC], src_lum[MOCHII_MAX_SRC];
+    double src_x[MOCHII_MAX_SRC], src_y[MOCHII_MAX_SRC], src_z[MOCHII_MAX_SRC];
+    /* gas state and iteration */
+    double xHI_init, xHeI_init, xHeII_init;
+    double He_abund;
+    int gas_niter;
+    double gas_tol, te_fixed, ion_relax;
+    int caseA;                       /* par%case_ab == 'A'                    */
+    int recomb_hui_gnedin;           /* par%recomb_model == 'hui_gnedin'      */
+    int ci_dere_hybrid;              /* par%ci_model == 'dere_hybrid'         */
+    int conv_vol;                    /* par%conv_crit == 'vol'                */
+    int solve_te;
+    double te_min, te_max, gas_tol_te;
+    int require_convergence;
+    /* metals (define.f90 abund_* and metal switches) */
+    int use_metals;
+    double abund_C, abund_N, abund_O, abund_Ne, abund_S, abund_Ar,
+           abund_Mg, abund_Fe, abund_Si, abund_Cl, abund_Ca;
+    int ion_metal_abs, metal_ne, metal_heat, metal_freefree;
+    int charge_exchange_two_way;     /* par%charge_exchange == 'two_way'      */
+    int cooling_local_ne;            /* par%cooling_model == 'local_ne'       */
+    int gaunt_vh14;
+    /* diffuse field, secondary ionisation, dust, FUV */
+    int diffuse_field, diffuse_milne, use_sec_ion;
+    int ion_add_dust, ion_dust_scatter;
+    int dust_law;                    /* 0 global_dgr, 1 none, 2 other         */
+    double DGR, cext_dust;
+    int grain_pe;
+    char ion_dust_kext[MOCHII_STRLEN];
+    char data_dir[MOCHII_STRLEN];
+    char atomic_dir[MOCHII_STRLEN];
+    /* device arithmetic (not a reference key: 'fp64' or 'fp32') */
+    int precision;
+} mochii_params;
+
+/* Per-pass statistics (ion_score_report_energy_closure, ion_score_mod.f90:364-387). */
+typedef struct mochii_pass_stats {
+    double energy_emitted, energy_absorbed, energy_escaped, closure;
+    int64_t direct_segments, scattered_segments;
+    int64_t packets;
+    double kernel_ms;                /* device time of the transport kernel   */
+    double pass_ms;                  /* device time of the whole pass         */
+    int64_t walk_kills;              /* MAX_WALK_STEPS guard hits             */
+} mochii_pass_stats;
+
+/* Convergence measures (gas_thermal_update / gas_equilibrium_update outputs). */
+typedef struct mochii_metrics {
+    double max_dx, max_dte, dx_vol, dte_vol;
+    int64_t cells_solved;
+    int64_t fixed_point_cap_hits;    /* cells whose n_e loop used all 200 passes */
+    double kernel_ms;
+} mochii_metrics;
+
+typedef struct mochii_ctx mochii_ctx;
+
+/* ---- parameters: read_input, setup.f90:11-35 ----------------------------- */
+/* Fill *p with the define.f90 defaults. */
+int mochii_params_default(mochii_params* p);
+/* sizeof(mochii_params), for FFI bindings that mirror the struct. */
+size_t mochii_params_size(void);
+/* Set one key (the name after "par%", case-insensitive, optional "(i)"
+ * index) from its namelist text value.  Unknown keys are an error. */
+int mochii_params_set(mochii_params* p, const char* key, const char* value);
+/* Parse a namelist text "&parameters par%key = value ... /" into *p,
+ * starting from its current contents.  errbuf receives a message. */
+int mochii_params_parse_namelist(mochii_params* p, const char* text, char* errbuf, size_t errlen);
+/* Read a namelist file (read_input, setup.f90:33-35). */
+int mochii_params_read_namelist(mochii_params* p, const char* path, char* errbuf, size_t errlen);
+
+/* ---- context: grid_create_amr + ion_setup + gas_state_setup ---------------- */
+/* Builds the grid (grid_mod_amr.f90:27-350), the band and source samplers
+ * (ion_band_mod.f90:122-258), the leaf state (gas_state_mod.f90:41-90) and
+ * uploads everything to device memory on the current device. */
+int mochii_init(const mochii_params* p, mochii_ctx** out);
+void mochii_destroy(mochii_ctx* ctx);
+const char* mochii_strerror(int status);
+/* Message of the last failed call on ctx (or of the last failed
+ * mochii_init on this thread when ctx is NULL). */
+const char* mochii_last_error(const mochii_ctx* ctx);
+
+/* ---- the replaced entry points ------------------------------------------------- */
+/* ionizing_field_and_rates (ionizing_field_mod.f90:72-170): one transport
+ * pass of every stellar packet through the current opacity, the energy
+ * ledger, and the rate normalisation (gas_rates_compute).  with_peel must
+ * be 0 (observer imaging is outside this library). */
+int mochii_transport_pass(mochii_ctx* ctx, int with_peel, mochii_pass_stats* stats);
+/* gas_equilibrium_update (solve_te = 0) or gas_thermal_update (solve_te = 1). */
+int mochii_balance_update(mochii_ctx* ctx, int solve_te, mochii_metrics* m);
+/* gas_opacity_fill: refresh the per-leaf absorber columns the transport reads. */
+int mochii_opacity_fill(mochii_ctx* ctx);
+
+/* ---- state exchange (host buffers; sizes in elements) ---------------------- */
+int64_t mochii_nleaf(const mochii_ctx* ctx);
+int mochii_nnu_band(const mochii_ctx* ctx);
+/* Field names: "nH" "x_HI" "x_HeI" "x_HeII" "n_e" "T_e" "gamma_HI"
+ * "gamma_HeI" "gamma_HeII" "heat_HI" "heat_HeI" "heat_HeII" (nleaf each),
+ * "jt_ion" (nleaf*nnu_band, leaf-major), "eedge" (nnu_band+1),
+ * "leaf_half" (nleaf). */
+int mochii_get_field(mochii_ctx* ctx, const char* name, double* out, int64_t n);
+/* Upload a state field ("x_HI" "x_HeI" "x_HeII" "n_e" "T_e" "nH"). */
+int mochii_set_field(mochii_ctx* ctx, const char* name, const double* in, int64_t n);
+/* Launch-set size of later passes (par%nphotons). */
+int mochii_set_nphotons(mochii_ctx* ctx, int64_t nphotons);
+double mochii_ion_Ltot(const mochii_ctx* ctx);
+
+/* ---- test hooks (bit-exact fixtures) -------------------------------------------- */
+/* Owen-scrambled Sobol uniforms computed on the device
+ * (qmc_uniforms_stream, qmc_mod.f90:157-168): out[i*nd + d] for the 0-based
+ * indices idx0 .. idx0+n-1, stream 1 (stellar) or 2 (diffuse), nd <= 12. */
+int mochii_sobol_uniforms(int seed, int stream, int64_t idx0, int64_t n, int nd, double* out);
+/* Geometry-only cell walk of nray rays (x,y,z,kx,ky,kz each, code units)
+ * on ctx's grid (raytrace_ion_to_edge_car, raytrace_amr.f90:534-592, with
+ * no optical-depth cut): leaves[r*max_steps + s] (0-based leaf index) and
+ * nsteps[r]. */
+int mochii_walk_leaves(mochii_ctx* ctx, int64_t nray, const double* rays, int max_steps,
+                       int32_t* leaves, int32_t* nsteps);
+/* Launch records of packets ip0..ip0+n-1: x,y,z,kx,ky,kz,E,inu (8 doubles
+ * each), as gen_ion_photon_qmc (ion_band_mod.f90:1880-1935) makes them. */
+int mochii_launch_records(mochii_ctx* ctx, int64_t ip0, int64_t n, double* out8);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* MOCHII_GPU_H */

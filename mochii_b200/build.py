@@ -1,0 +1,68 @@
+"""Build libmochii_gpu.so in-tree with nvcc for sm_100a.
+
+    python -m mochii_b200.build        (or mochii_b200.build.build())
+
+The device code is compiled with -fmad=false: the FP64 cell-walk geometry
+and the source-energy inversion must round exactly as the FP64 source
+expressions do (no fused multiply-add contraction), which is what makes
+leaf sequences and sampled energies bit-identical to the CPU restatement.
+"""
+import os
+import shutil
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(HERE)
+CSRC = os.path.join(HERE, "csrc")
+INCLUDE = os.path.join(ROOT, "include")
+LIB = os.path.join(HERE, "libmochii_gpu.so")
+
+SOURCES = ["api.cu", "transport.cu", "balance.cu", "band.cpp", "params.cpp"]
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+
+
+def nvcc_path():
+    for cand in (os.environ.get("NVCC"), "/usr/local/cuda/bin/nvcc", shutil.which("nvcc")):
+        if cand and os.path.exists(cand):
+            return cand
+    raise RuntimeError("nvcc not found")
+
+
+def needs_rebuild():
+    if not os.path.exists(LIB):
+        return True
+    t = os.path.getmtime(LIB)
+    deps = [os.path.join(CSRC, f) for f in os.listdir(CSRC)] + [os.path.join(INCLUDE, "mochii_gpu.h"), __file__]
+    return any(os.path.getmtime(d) > t for d in deps)
+
+
+def build(force=False, verbose=False):
+    if not force and not needs_rebuild():
+        return LIB
+    nvcc = nvcc_path()
+    hostcxx = "/usr/bin/g++" if os.path.exists("/usr/bin/g++") else "g++"
+    objdir = os.path.join(HERE, "_build")
+    os.makedirs(objdir, exist_ok=True)
+    common = ["-O3", "-std=c++17", "-lineinfo", "-fmad=false", "-Xcompiler", "-fPIC",
+              "-ccbin", hostcxx, "-I", INCLUDE, "-I", CSRC] + ARCH
+    objs = []
+    for src in SOURCES:
+        obj = os.path.join(objdir, src + ".o")
+        cmd = [nvcc, "-c", os.path.join(CSRC, src), "-o", obj] + common
+        if src.endswith(".cpp"):
+            cmd = [nvcc, "-x", "cu", "-c", os.path.join(CSRC, src), "-o", obj] + common
+        if verbose:
+            print(" ".join(cmd))
+        subprocess.run(cmd, check=True)
+        objs.append(obj)
+    tmp = LIB + ".tmp"
+    cmd = [nvcc, "-shared", "-o", tmp] + objs + ARCH + ["-ccbin", hostcxx, "-lcudart"]
+    subprocess.run(cmd, check=True)
+    os.replace(tmp, LIB)
+    return LIB
+
+
+if __name__ == "__main__":
+    build(force="--force" in sys.argv, verbose=True)
+    print(LIB)

@@ -1,0 +1,112 @@
+"""Synthetic benchmark nebulae as namelist texts (the reference's own input
+format), with fixed seeds.  No public dataset exists for this path; these
+configurations are the workloads.
+
+  stromgren64   pure-H Stromgren sphere: uniform 64^3 Cartesian grid whose
+                box side is twice the analytic Stromgren radius, n_H = 100,
+                40 kK blackbody with Q(H) = 1e49 s^-1 over 13.598-100 eV (the
+                luminosity is Q(H) times the mean photon energy of that Planck
+                band, 18.633 eV), case
+                B, T_e fixed at 1e4 K, Owen-scrambled Sobol launch (seed
+                12345), 1e6 packets, 10 iterations, FP64 arithmetic.
+  hhe128        the H+He part of the 128^3 H II region (n_H = 100, He/H 0.1,
+                45 kK, Q(H) = 5e49 s^-1, case A), 1e7 packets per pass, FP32
+                segments with compensated FP32 tallies.
+"""
+import math
+
+PC2CM = 3.0856776e18
+KB_CGS = 1.380649e-16
+EV2ERG = 1.602176634e-12
+
+
+def _alphaB_HII_1e4():
+    """Case-B H recombination at 1e4 K as recomb_mod evaluates it by default
+    (Badnell total minus the Milne ground-level fit), recomb_mod.f90:51,63,188."""
+    T = 1.0e4
+    tt = math.sqrt(T / 2.965)
+    aA = 8.318e-11 / (tt * (1.0 + tt) ** (1.0 - 0.7472) * (1.0 + math.sqrt(T / 7.001e5)) ** (1.0 + 0.7472))
+    te = T * (KB_CGS / EV2ERG)
+    a1 = (1.87007e-2 * 1.0e-10 * te ** (-1.29077 + 2.17465e-3 * math.log(te))
+          * (1.0 + 8.44399e-2 * te ** (-5.93940e-4)) / (1.0 + 1.29189e1 * te ** (-8.05060e-1)))
+    return aA - a1
+
+
+def mean_photon_energy_ev(T, emin=13.598, emax=100.0, n=200001):
+    """<E> = int B_E dE / int B_E/E dE of a blackbody over [emin, emax] eV, so
+    that luminosity = Q(H) <E> ev2erg gives the band photon rate Q(H)."""
+    h = (emax - emin) / (n - 1)
+    num = den = 0.0
+    for i in range(n):
+        e = emin + i * h
+        w = 0.5 if i in (0, n - 1) else 1.0
+        b = e ** 3 / math.expm1(e / (8.617333262145e-5 * T))
+        num += w * b
+        den += w * b / e
+    return num / den
+
+
+def stromgren_radius_pc(Q=1.0e49, nH=100.0):
+    """Sharp-edge R_S = (3 Q / (4 pi n_H^2 alpha_B))^(1/3) [pc]."""
+    return (3.0 * Q / (4.0 * math.pi * nH * nH * _alphaB_HII_1e4())) ** (1.0 / 3.0) / PC2CM
+
+
+def stromgren64(nphotons=1_000_000, niter=10, n=64, precision="fp64", seed=12345):
+    rs = stromgren_radius_pc()
+    return f"""&parameters
+ par%no_photons = {float(nphotons):.6e}
+ par%launch_sequence = 'sobol'
+ par%qmc_seed = {seed}
+ par%grid_type = 'car'
+ par%car_walk = 'dda'
+ par%nx = {n}
+ par%ny = {n}
+ par%nz = {n}
+ par%xmax = {rs:.10f}
+ par%ymax = {rs:.10f}
+ par%zmax = {rs:.10f}
+ par%distance_unit = 'pc'
+ par%nH_const = 100.0
+ par%He_abund = 0.0
+ par%xHI_init = 1.0
+ par%tstar = 4.0e4
+ par%luminosity = {1.0e49 * mean_photon_energy_ev(4.0e4) * EV2ERG:.6e}
+ par%eion_min = 13.598
+ par%eion_max = 100.0
+ par%case_ab = 'B'
+ par%te_fixed = 1.0e4
+ par%ion_relax = 1.0
+ par%gas_niter = {niter}
+ par%gas_tol = 1.0e-3
+ par%precision = '{precision}'
+/
+"""
+
+
+def hhe128(nphotons=10_000_000, niter=20, n=128, precision="fp32", seed=12345, rs_factor=1.0):
+    """H+He H II region on a uniform grid, case A, fixed T_e (the He/H and
+    source of the 128^3 H II-region workload; metals, diffuse packets and the
+    thermal solve are separate rows)."""
+    rs = stromgren_radius_pc(Q=5.0e49) * rs_factor
+    return f"""&parameters
+ par%no_photons = {float(nphotons):.6e}
+ par%launch_sequence = 'sobol'
+ par%qmc_seed = {seed}
+ par%grid_type = 'car'
+ par%nx = {n}
+ par%ny = {n}
+ par%nz = {n}
+ par%xmax = {rs:.10f}
+ par%ymax = {rs:.10f}
+ par%zmax = {rs:.10f}
+ par%distance_unit = 'pc'
+ par%nH_const = 100.0
+ par%He_abund = 0.1
+ par%tstar = 4.5e4
+ par%luminosity = {5.0e49 * mean_photon_energy_ev(4.5e4) * EV2ERG:.6e}
+ par%case_ab = 'A'
+ par%te_fixed = 1.0e4
+ par%gas_niter = {niter}
+ par%precision = '{precision}'
+/
+"""

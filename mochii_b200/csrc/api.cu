@@ -1,0 +1,490 @@
+// C-ABI layer: context life cycle, the replaced module entry points and the
+// state-exchange / test hooks declared in include/mochii_gpu.h.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "band.h"
+#include "ctx.h"
+#include "mochii_gpu.h"
+#include "physics.cuh"
+#include "qmc.cuh"
+#include "transport.h"
+
+using namespace mochii;
+
+namespace {
+
+thread_local std::string g_init_error;
+
+int fail(mochii_ctx* c, int code, const std::string& msg) {
+    if (c) c->last_error = msg; else g_init_error = msg;
+    return code;
+}
+
+#define CK(c, call)                                                                              \
+    do {                                                                                         \
+        cudaError_t e_ = (call);                                                                 \
+        if (e_ != cudaSuccess)                                                                   \
+            return fail((c), MOCHII_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+template <typename T>
+cudaError_t dalloc(T** p, size_t n) {
+    return cudaMalloc(reinterpret_cast<void**>(p), n * sizeof(T) + 16);
+}
+
+void release(mochii_ctx* c) {
+    if (!c) return;
+    void* ptrs[] = {c->nH, c->xHI, c->xHeI, c->xHeII, c->ne, c->Te, c->col, c->tally, c->jt, c->rates,
+                    c->tab.tab_e, c->tab.tab_f, c->tab.tab_c, c->tab.tab_off, c->tab.comp, c->tab.eedge,
+                    c->tab.qmc, c->tw.ledger, c->tw.counters, c->bw.partial, c->bw.counters};
+    for (void* p : ptrs)
+        if (p) cudaFree(p);
+    for (cudaEvent_t e : {c->ev0, c->ev1, c->evA, c->evB})
+        if (e) cudaEventDestroy(e);
+    if (c->stream) cudaStreamDestroy(c->stream);
+}
+
+// Checks read_input applies (setup.f90:76-626) plus the extent of this build.
+int validate(const mochii_params& p, std::string* why, int* code) {
+    *code = MOCHII_ERR_BAD_PARAM;
+    if (p.nphotons < 1) return *why = "par%no_photons must be >= 1", 1;
+    if (p.eion_max <= p.eion_min || p.eion_min <= 0.0) return *why = "need 0 < par%eion_min < par%eion_max", 1;
+    if (p.grid_car) {
+        if (p.xmax <= 0.0 || p.nx < 1 || p.ny < 1 || p.nz < 1) return *why = "car grid needs par%xmax > 0 and nx,ny,nz >= 1", 1;
+        const double dcx = 2.0 * p.xmax / p.nx, dcy = 2.0 * p.ymax / p.ny, dcz = 2.0 * p.zmax / p.nz;
+        if (std::fabs(dcy - dcx) > 1.0e-9 * dcx || std::fabs(dcz - dcx) > 1.0e-9 * dcx)
+            return *why = "car grid needs cubic cells: 2*xmax/nx = 2*ymax/ny = 2*zmax/nz", 1;   // grid_mod_amr.f90:91-96
+    }
+    if (p.ion_relax <= 0.0 || p.ion_relax > 1.0) return *why = "par%ion_relax must lie in (0, 1]", 1;
+    if (p.te_fixed <= 0.0) return *why = "par%te_fixed must be positive", 1;
+    if (p.He_abund < 0.0) return *why = "par%He_abund must be >= 0", 1;
+    *code = MOCHII_ERR_UNSUPPORTED;
+    if (!p.grid_car) return *why = "grid_type='amr' (octree leaf list) is not built in this library version", 1;
+    if (!p.car_walk_dda) return *why = "car_walk='amr' is not built; use the DDA walk (car_walk='dda')", 1;
+    if (!p.source_point) return *why = "only internal point sources are built", 1;
+    if (!p.launch_sobol) return *why = "launch_sequence='random' is not built; use 'sobol'", 1;
+    if (p.use_metals) return *why = "use_metals is not built in this library version", 1;
+    if (p.diffuse_field) return *why = "diffuse_field is not built in this library version", 1;
+    if (p.ion_add_dust) return *why = "ion_add_dust is not built in this library version", 1;
+    if (p.use_sec_ion) return *why = "use_sec_ion is not built in this library version", 1;
+    if (p.add_fuv) return *why = "add_fuv is not built in this library version", 1;
+    if (p.grain_pe) return *why = "grain_pe is not built in this library version", 1;
+    return 0;
+}
+
+}  // namespace
+
+extern "C" const char* mochii_strerror(int s) {
+    switch (s) {
+        case MOCHII_OK: return "ok";
+        case MOCHII_ERR_BAD_PARAM: return "bad parameter";
+        case MOCHII_ERR_TABLE: return "data table error";
+        case MOCHII_ERR_CUDA: return "CUDA runtime error";
+        case MOCHII_ERR_TIMEOUT: return "device loop hit its iteration cap";
+        case MOCHII_ERR_NONFINITE: return "non-finite value";
+        case MOCHII_ERR_CLOSURE: return "energy closure exceeds 5e-13";
+        case MOCHII_ERR_NOT_CONVERGED: return "iteration did not converge";
+        case MOCHII_ERR_UNSUPPORTED: return "configuration outside the built path";
+        case MOCHII_ERR_NO_DEVICE: return "no CUDA device";
+    }
+    return "unknown status";
+}
+
+extern "C" const char* mochii_last_error(const mochii_ctx* c) {
+    return c ? c->last_error.c_str() : g_init_error.c_str();
+}
+
+extern "C" int mochii_init(const mochii_params* pin, mochii_ctx** out) {
+    if (!pin || !out) return fail(nullptr, MOCHII_ERR_BAD_PARAM, "null argument");
+    *out = nullptr;
+    std::string why;
+    int code;
+    if (validate(*pin, &why, &code)) return fail(nullptr, code, why);
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev < 1) {
+        cudaGetLastError();
+        return fail(nullptr, MOCHII_ERR_NO_DEVICE, "no CUDA device is visible");
+    }
+    auto* c = new mochii_ctx();
+    c->par = *pin;
+    mochii_params& p = c->par;
+    if (!band_build(p, c->band, &why)) {
+        delete c;
+        return fail(nullptr, MOCHII_ERR_BAD_PARAM, why);
+    }
+    cudaGetDevice(&c->device);
+    // namelist car grid, grid_mod_amr.f90:64-133 and amr_build_car (octree_mod.f90:648-674)
+    Grid& g = c->grid;
+    g.nx = p.nx; g.ny = p.ny; g.nz = p.nz;
+    g.nleaf = (long long)p.nx * p.ny * p.nz;
+    g.xmin = -p.xmax; g.xmax = p.xmax;
+    g.ymin = -p.ymax; g.ymax = p.ymax;
+    g.zmin = -p.zmax; g.zmax = p.zmax;
+    g.dcell = (g.xmax - g.xmin) / (double)g.nx;
+    c->fp32 = p.precision == MOCHII_PREC_FP32;
+    c->nabs = p.He_abund > 0.0 ? 4 : 1;
+    c->ntally = p.He_abund > 0.0 ? 6 : 2;
+    c->nnu = c->band.nnu_band;
+    const long long n = g.nleaf;
+    auto bail = [&](int rc) {
+        std::string m = c->last_error;
+        release(c);
+        delete c;
+        return fail(nullptr, rc, m);
+    };
+#define CKI(call)                                                                         \
+    do {                                                                                  \
+        cudaError_t e_ = (call);                                                          \
+        if (e_ != cudaSuccess) {                                                          \
+            c->last_error = std::string(#call) + ": " + cudaGetErrorString(e_);           \
+            return bail(MOCHII_ERR_CUDA);                                                 \
+        }                                                                                 \
+    } while (0)
+    CKI(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+    CKI(cudaEventCreate(&c->ev0));
+    CKI(cudaEventCreate(&c->ev1));
+    CKI(cudaEventCreate(&c->evA));
+    CKI(cudaEventCreate(&c->evB));
+    // leaf state (gas_state_setup, gas_state_mod.f90:58-77) on the host
+    std::vector<double> nH(n, 1.0), xHI(n, p.xHI_init), xHeI(n, p.xHeI_init), xHeII(n, p.xHeII_init), ne(n),
+        Te(n, p.te_fixed);
+    {
+        const double dcx = 2.0 * p.xmax / p.nx, dcy = 2.0 * p.ymax / p.ny, dcz = 2.0 * p.zmax / p.nz;
+        long long il = 0;
+        for (int iz = 0; iz < p.nz; ++iz)
+            for (int iy = 0; iy < p.ny; ++iy)
+                for (int ix = 0; ix < p.nx; ++ix, ++il) {
+                    if (p.nH_const >= 0.0) nH[il] = p.nH_const;   // grid_mod_amr.f90:137-147
+                    if (p.rmax > 0.0 || p.rmin > 0.0) {
+                        const double xl = -p.xmax + ((double)ix + 0.5) * dcx;
+                        const double yl = -p.ymax + ((double)iy + 0.5) * dcy;
+                        const double zl = -p.zmax + ((double)iz + 0.5) * dcz;
+                        const double rho = std::sqrt(xl * xl + yl * yl + zl * zl);
+                        if (p.rmax > 0.0 && rho > p.rmax) nH[il] = 0.0;
+                        if (p.rmin > 0.0 && rho < p.rmin) nH[il] = 0.0;
+                    }
+                }
+        for (long long i = 0; i < n; ++i)
+            ne[i] = nH[i] * ((1.0 - xHI[i]) + p.He_abund * (xHeII[i] + 2.0 * std::max(0.0, 1.0 - xHeI[i] - xHeII[i])));
+    }
+    CKI(dalloc(&c->nH, n));
+    CKI(dalloc(&c->xHI, n));
+    CKI(dalloc(&c->xHeI, n));
+    CKI(dalloc(&c->xHeII, n));
+    CKI(dalloc(&c->ne, n));
+    CKI(dalloc(&c->Te, n));
+    CKI(cudaMemcpy(c->nH, nH.data(), n * 8, cudaMemcpyHostToDevice));
+    CKI(cudaMemcpy(c->xHI, xHI.data(), n * 8, cudaMemcpyHostToDevice));
+    CKI(cudaMemcpy(c->xHeI, xHeI.data(), n * 8, cudaMemcpyHostToDevice));
+    CKI(cudaMemcpy(c->xHeII, xHeII.data(), n * 8, cudaMemcpyHostToDevice));
+    CKI(cudaMemcpy(c->ne, ne.data(), n * 8, cudaMemcpyHostToDevice));
+    CKI(cudaMemcpy(c->Te, Te.data(), n * 8, cudaMemcpyHostToDevice));
+    const size_t rsz = c->fp32 ? 4 : 8;
+    const size_t tsz = c->fp32 ? 8 : 8;   // float2 pair or double
+    CKI(cudaMalloc(&c->col, (size_t)n * c->nabs * rsz + 64));
+    CKI(cudaMalloc(&c->tally, (size_t)n * c->ntally * tsz + 64));
+    CKI(cudaMalloc(&c->jt, (size_t)n * c->nnu * tsz + 64));
+    CKI(dalloc(&c->rates, 6 * (size_t)n));
+    CKI(cudaMemset(c->rates, 0, 6 * (size_t)n * 8));
+    // sampler tables, component table, bin edges, QMC tables
+    std::vector<double> te, tf, tc, comp;
+    std::vector<int> off{0};
+    for (int k = 0; k < c->band.ncomp; ++k) {
+        const EnergyTable& t = c->band.tables[k];
+        te.insert(te.end(), t.energy.begin(), t.energy.end());
+        tf.insert(tf.end(), t.density.begin(), t.density.end());
+        tc.insert(tc.end(), t.cdf.begin(), t.cdf.end());
+        off.push_back((int)te.size());
+        comp.push_back(c->band.comp_cdf[k]);
+        comp.push_back(c->band.comp_x[k]);
+        comp.push_back(c->band.comp_y[k]);
+        comp.push_back(c->band.comp_z[k]);
+    }
+    CKI(dalloc(&c->tab.tab_e, te.size()));
+    CKI(dalloc(&c->tab.tab_f, tf.size()));
+    CKI(dalloc(&c->tab.tab_c, tc.size()));
+    CKI(dalloc(&c->tab.tab_off, off.size()));
+    CKI(dalloc(&c->tab.comp, comp.size()));
+    CKI(dalloc(&c->tab.eedge, c->band.eedge.size()));
+    CKI(dalloc(&c->tab.qmc, 1));
+    CKI(cudaMemcpy(c->tab.tab_e, te.data(), te.size() * 8, cudaMemcpyHostToDevice));
+    CKI(cudaMemcpy(c->tab.tab_f, tf.data(), tf.size() * 8, cudaMemcpyHostToDevice));
+    CKI(cudaMemcpy(c->tab.tab_c, tc.data(), tc.size() * 8, cudaMemcpyHostToDevice));
+    CKI(cudaMemcpy(c->tab.tab_off, off.data(), off.size() * sizeof(int), cudaMemcpyHostToDevice));
+    CKI(cudaMemcpy(c->tab.comp, comp.data(), comp.size() * 8, cudaMemcpyHostToDevice));
+    CKI(cudaMemcpy(c->tab.eedge, c->band.eedge.data(), c->band.eedge.size() * 8, cudaMemcpyHostToDevice));
+    QmcTables qt;
+    qmc_build_tables(p.qmc_seed, qt);
+    CKI(cudaMemcpy(c->tab.qmc, &qt, sizeof(qt), cudaMemcpyHostToDevice));
+    // work areas
+    c->tw.ledger_blocks = transport_blocks(c);
+    CKI(dalloc(&c->tw.ledger, 3 * (size_t)c->tw.ledger_blocks));
+    CKI(dalloc(&c->tw.counters, 4));
+    c->bw.blocks = balance_blocks(c);
+    CKI(dalloc(&c->bw.partial, 6 * (size_t)c->bw.blocks));
+    CKI(dalloc(&c->bw.counters, 4));
+    CKI(launch_columns(c));
+    CKI(cudaStreamSynchronize(c->stream));
+    c->columns_fresh = true;
+#undef CKI
+    *out = c;
+    return MOCHII_OK;
+}
+
+extern "C" void mochii_destroy(mochii_ctx* c) {
+    if (!c) return;
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    release(c);
+    delete c;
+}
+
+extern "C" int64_t mochii_nleaf(const mochii_ctx* c) { return c ? c->grid.nleaf : 0; }
+extern "C" int mochii_nnu_band(const mochii_ctx* c) { return c ? c->nnu : 0; }
+extern "C" double mochii_ion_Ltot(const mochii_ctx* c) { return c ? c->band.ion_Ltot : 0.0; }
+
+extern "C" int mochii_set_nphotons(mochii_ctx* c, int64_t np) {
+    if (!c || np < 1) return MOCHII_ERR_BAD_PARAM;
+    c->par.nphotons = np;
+    const int nb = transport_blocks(c);
+    if (nb > c->tw.ledger_blocks) {
+        cudaFree(c->tw.ledger);
+        c->tw.ledger = nullptr;
+        CK(c, dalloc(&c->tw.ledger, 3 * (size_t)nb));
+    }
+    c->tw.ledger_blocks = nb;
+    return MOCHII_OK;
+}
+
+// ionizing_field_and_rates, ionizing_field_mod.f90:72-170.
+extern "C" int mochii_transport_pass(mochii_ctx* c, int with_peel, mochii_pass_stats* st) {
+    if (!c) return MOCHII_ERR_BAD_PARAM;
+    if (with_peel) return fail(c, MOCHII_ERR_UNSUPPORTED, "observer peel-off is not built (with_peel must be 0)");
+    const long long n = c->grid.nleaf;
+    const size_t tsz = 8;
+    if (!c->columns_fresh) {
+        CK(c, launch_columns(c));
+        c->columns_fresh = true;
+    }
+    CK(c, cudaEventRecord(c->evA, c->stream));
+    // jt_ion(:,:) = 0 and ion_score_reset (ionizing_field_mod.f90:90-91)
+    CK(c, cudaMemsetAsync(c->tally, 0, (size_t)n * c->ntally * tsz, c->stream));
+    CK(c, cudaMemsetAsync(c->jt, 0, (size_t)n * c->nnu * tsz, c->stream));
+    CK(c, cudaMemsetAsync(c->tw.counters, 0, 4 * sizeof(unsigned long long), c->stream));
+    CK(c, cudaEventRecord(c->ev0, c->stream));
+    CK(c, launch_transport(c));
+    CK(c, cudaEventRecord(c->ev1, c->stream));
+    CK(c, launch_rates(c));
+    CK(c, cudaEventRecord(c->evB, c->stream));
+    std::vector<double> led(3 * (size_t)c->tw.ledger_blocks);
+    unsigned long long cnt[4];
+    CK(c, cudaMemcpyAsync(led.data(), c->tw.ledger, led.size() * 8, cudaMemcpyDeviceToHost, c->stream));
+    CK(c, cudaMemcpyAsync(cnt, c->tw.counters, sizeof(cnt), cudaMemcpyDeviceToHost, c->stream));
+    CK(c, cudaStreamSynchronize(c->stream));
+    float ms = 0.0f, pms = 0.0f;
+    cudaEventElapsedTime(&ms, c->ev0, c->ev1);
+    cudaEventElapsedTime(&pms, c->evA, c->evB);
+    long double e[3] = {0, 0, 0};
+    for (int b = 0; b < c->tw.ledger_blocks; ++b)
+        for (int k = 0; k < 3; ++k) e[k] += (long double)led[3 * (size_t)b + k];
+    mochii_pass_stats s;
+    std::memset(&s, 0, sizeof(s));
+    s.energy_emitted = (double)e[0];
+    s.energy_absorbed = (double)e[1];
+    s.energy_escaped = (double)e[2];
+    s.closure = std::fabs(s.energy_absorbed + s.energy_escaped - s.energy_emitted) /
+                std::max(s.energy_emitted, kTinest);
+    s.direct_segments = (int64_t)cnt[0];
+    s.walk_kills = (int64_t)cnt[1];
+    s.packets = c->par.nphotons;
+    s.kernel_ms = ms;
+    s.pass_ms = pms;
+    if (st) *st = s;
+    if (!std::isfinite(s.energy_emitted) || !std::isfinite(s.energy_absorbed))
+        return fail(c, MOCHII_ERR_NONFINITE, "non-finite energy ledger");
+    if (s.closure > 5.0e-13)   // ion_score_mod.f90:386
+        return fail(c, MOCHII_ERR_CLOSURE, "energy closure exceeds 5e-13");
+    return MOCHII_OK;
+}
+
+// gas_equilibrium_update (ion_balance_mod.f90:352) / gas_thermal_update
+// (thermal_mod.f90:124).
+extern "C" int mochii_balance_update(mochii_ctx* c, int solve_te, mochii_metrics* m) {
+    if (!c) return MOCHII_ERR_BAD_PARAM;
+    if (solve_te) return fail(c, MOCHII_ERR_UNSUPPORTED, "the thermal solve is not built in this library version");
+    CK(c, cudaMemsetAsync(c->bw.counters, 0, 4 * sizeof(unsigned long long), c->stream));
+    CK(c, cudaEventRecord(c->ev0, c->stream));
+    CK(c, launch_balance(c));
+    CK(c, cudaEventRecord(c->ev1, c->stream));
+    c->columns_fresh = true;   // the balance kernel refreshes the columns it changes
+    std::vector<double> part(3 * (size_t)c->bw.blocks);
+    unsigned long long cnt[4];
+    CK(c, cudaMemcpyAsync(part.data(), c->bw.partial, part.size() * 8, cudaMemcpyDeviceToHost, c->stream));
+    CK(c, cudaMemcpyAsync(cnt, c->bw.counters, sizeof(cnt), cudaMemcpyDeviceToHost, c->stream));
+    CK(c, cudaStreamSynchronize(c->stream));
+    float ms = 0.0f;
+    cudaEventElapsedTime(&ms, c->ev0, c->ev1);
+    double mdx = 0.0, sdx = 0.0, sx = 0.0;
+    for (int b = 0; b < c->bw.blocks; ++b) {
+        mdx = std::max(mdx, part[3 * (size_t)b]);
+        sdx += part[3 * (size_t)b + 1];
+        sx += part[3 * (size_t)b + 2];
+    }
+    mochii_metrics r;
+    std::memset(&r, 0, sizeof(r));
+    r.max_dx = mdx;
+    r.dx_vol = sdx / std::max(sx, kTinest);
+    r.cells_solved = (int64_t)cnt[0];
+    r.fixed_point_cap_hits = (int64_t)cnt[1];
+    r.kernel_ms = ms;
+    if (m) *m = r;
+    if (!std::isfinite(mdx) || !std::isfinite(sdx)) return fail(c, MOCHII_ERR_NONFINITE, "non-finite state after the solve");
+    return MOCHII_OK;
+}
+
+// gas_opacity_fill (gas_opacity_mod.f90:299-332).  The balance kernel
+// already rewrites the columns of every leaf it solves, so this launches
+// only when the state changed through mochii_set_field since.
+extern "C" int mochii_opacity_fill(mochii_ctx* c) {
+    if (!c) return MOCHII_ERR_BAD_PARAM;
+    if (c->columns_fresh) return MOCHII_OK;
+    CK(c, launch_columns(c));
+    CK(c, cudaStreamSynchronize(c->stream));
+    c->columns_fresh = true;
+    return MOCHII_OK;
+}
+
+namespace {
+double* field_ptr(mochii_ctx* c, const std::string& n, long long* count) {
+    const long long nl = c->grid.nleaf;
+    *count = nl;
+    if (n == "nH") return c->nH;
+    if (n == "x_HI") return c->xHI;
+    if (n == "x_HeI") return c->xHeI;
+    if (n == "x_HeII") return c->xHeII;
+    if (n == "n_e") return c->ne;
+    if (n == "T_e") return c->Te;
+    static const char* rn[6] = {"gamma_HI", "gamma_HeI", "gamma_HeII", "heat_HI", "heat_HeI", "heat_HeII"};
+    for (int k = 0; k < 6; ++k)
+        if (n == rn[k]) return c->rates + (size_t)k * nl;
+    return nullptr;
+}
+}  // namespace
+
+extern "C" int mochii_get_field(mochii_ctx* c, const char* name, double* out, int64_t n) {
+    if (!c || !name || !out) return MOCHII_ERR_BAD_PARAM;
+    const std::string nm(name);
+    if (nm == "eedge") {
+        if (n != (int64_t)c->band.eedge.size()) return fail(c, MOCHII_ERR_BAD_PARAM, "eedge size mismatch");
+        std::memcpy(out, c->band.eedge.data(), n * 8);
+        return MOCHII_OK;
+    }
+    if (nm == "leaf_half") {
+        if (n != c->grid.nleaf) return fail(c, MOCHII_ERR_BAD_PARAM, "leaf_half size mismatch");
+        for (int64_t i = 0; i < n; ++i) out[i] = 0.5 * c->grid.dcell;
+        return MOCHII_OK;
+    }
+    if (nm == "jt_ion") {
+        const long long cnt = c->grid.nleaf * (long long)c->nnu;
+        if (n != cnt) return fail(c, MOCHII_ERR_BAD_PARAM, "jt_ion size mismatch (nleaf*nnu_band)");
+        double* d = nullptr;
+        CK(c, cudaMallocAsync(&d, cnt * 8, c->stream));
+        CK(c, launch_jt_export(c, d));
+        CK(c, cudaMemcpyAsync(out, d, cnt * 8, cudaMemcpyDeviceToHost, c->stream));
+        CK(c, cudaFreeAsync(d, c->stream));
+        CK(c, cudaStreamSynchronize(c->stream));
+        return MOCHII_OK;
+    }
+    long long cnt = 0;
+    double* p = field_ptr(c, nm, &cnt);
+    if (!p) return fail(c, MOCHII_ERR_BAD_PARAM, "unknown field " + nm);
+    if (n != cnt) return fail(c, MOCHII_ERR_BAD_PARAM, "size mismatch for " + nm);
+    CK(c, cudaMemcpyAsync(out, p, cnt * 8, cudaMemcpyDeviceToHost, c->stream));
+    CK(c, cudaStreamSynchronize(c->stream));
+    return MOCHII_OK;
+}
+
+extern "C" int mochii_set_field(mochii_ctx* c, const char* name, const double* in, int64_t n) {
+    if (!c || !name || !in) return MOCHII_ERR_BAD_PARAM;
+    const std::string nm(name);
+    if (nm != "nH" && nm != "x_HI" && nm != "x_HeI" && nm != "x_HeII" && nm != "n_e" && nm != "T_e")
+        return fail(c, MOCHII_ERR_BAD_PARAM, "field is not settable: " + nm);
+    long long cnt = 0;
+    double* p = field_ptr(c, nm, &cnt);
+    if (n != cnt) return fail(c, MOCHII_ERR_BAD_PARAM, "size mismatch for " + nm);
+    CK(c, cudaMemcpyAsync(p, in, cnt * 8, cudaMemcpyHostToDevice, c->stream));
+    CK(c, cudaStreamSynchronize(c->stream));
+    c->columns_fresh = false;
+    return MOCHII_OK;
+}
+
+extern "C" int mochii_sobol_uniforms(int seed, int stream, int64_t idx0, int64_t n, int nd, double* out) {
+    if (!out || nd < 1 || nd > kQmcMaxDim || (stream != 1 && stream != 2) || n < 0 || idx0 < 0)
+        return fail(nullptr, MOCHII_ERR_BAD_PARAM, "mochii_sobol_uniforms: bad argument");
+    if (n == 0) return MOCHII_OK;
+    QmcTables qt;
+    qmc_build_tables(seed, qt);
+    QmcTables* dq = nullptr;
+    double* d = nullptr;
+    cudaStream_t s = nullptr;
+    auto cleanup = [&]() {
+        if (dq) cudaFree(dq);
+        if (d) cudaFree(d);
+        if (s) cudaStreamDestroy(s);
+    };
+#define CKS(call)                                                                                        \
+    do {                                                                                                 \
+        cudaError_t e_ = (call);                                                                         \
+        if (e_ != cudaSuccess) {                                                                         \
+            cleanup();                                                                                   \
+            return fail(nullptr, MOCHII_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_));   \
+        }                                                                                                \
+    } while (0)
+    CKS(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+    CKS(cudaMalloc(&dq, sizeof(QmcTables)));
+    CKS(cudaMalloc(&d, (size_t)n * nd * 8));
+    CKS(cudaMemcpyAsync(dq, &qt, sizeof(qt), cudaMemcpyHostToDevice, s));
+    CKS(launch_sobol(dq, stream - 1, idx0, n, nd, d, s));
+    CKS(cudaMemcpyAsync(out, d, (size_t)n * nd * 8, cudaMemcpyDeviceToHost, s));
+    CKS(cudaStreamSynchronize(s));
+#undef CKS
+    cleanup();
+    return MOCHII_OK;
+}
+
+extern "C" int mochii_walk_leaves(mochii_ctx* c, int64_t nray, const double* rays, int max_steps, int32_t* leaves,
+                                  int32_t* nsteps) {
+    if (!c || !rays || !leaves || !nsteps || nray < 0 || max_steps < 1) return MOCHII_ERR_BAD_PARAM;
+    if (nray == 0) return MOCHII_OK;
+    double* dr = nullptr;
+    int *dl = nullptr, *dn = nullptr;
+    CK(c, cudaMallocAsync(&dr, nray * 6 * 8, c->stream));
+    CK(c, cudaMallocAsync(&dl, (size_t)nray * max_steps * 4, c->stream));
+    CK(c, cudaMallocAsync(&dn, nray * 4, c->stream));
+    CK(c, cudaMemcpyAsync(dr, rays, nray * 6 * 8, cudaMemcpyHostToDevice, c->stream));
+    CK(c, launch_walk(c, dr, nray, max_steps, dl, dn));
+    CK(c, cudaMemcpyAsync(leaves, dl, (size_t)nray * max_steps * 4, cudaMemcpyDeviceToHost, c->stream));
+    CK(c, cudaMemcpyAsync(nsteps, dn, nray * 4, cudaMemcpyDeviceToHost, c->stream));
+    CK(c, cudaFreeAsync(dr, c->stream));
+    CK(c, cudaFreeAsync(dl, c->stream));
+    CK(c, cudaFreeAsync(dn, c->stream));
+    CK(c, cudaStreamSynchronize(c->stream));
+    return MOCHII_OK;
+}
+
+extern "C" int mochii_launch_records(mochii_ctx* c, int64_t ip0, int64_t n, double* out8) {
+    if (!c || !out8 || n < 0 || ip0 < 0) return MOCHII_ERR_BAD_PARAM;
+    if (n == 0) return MOCHII_OK;
+    double* d = nullptr;
+    CK(c, cudaMallocAsync(&d, n * 8 * 8, c->stream));
+    CK(c, launch_records(c, ip0, n, d));
+    CK(c, cudaMemcpyAsync(out8, d, n * 8 * 8, cudaMemcpyDeviceToHost, c->stream));
+    CK(c, cudaFreeAsync(d, c->stream));
+    CK(c, cudaStreamSynchronize(c->stream));
+    return MOCHII_OK;
+}

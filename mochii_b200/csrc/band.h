@@ -1,0 +1,39 @@
+// Host-side set-up of the ionising band: diagnostic bin edges and the
+// continuous source-energy samplers (ion_band_mod.f90:122-495 and
+// energy_sampler_mod.f90).  Set-up time only; the tables are uploaded to
+// device memory and inverted there per packet.
+#pragma once
+#include <string>
+#include <vector>
+
+#include "mochii_gpu.h"
+
+namespace mochii {
+
+// Piecewise-linear spectral density with its analytic CDF
+// (energy_sampler_type, energy_sampler_mod.f90:20-25).
+struct EnergyTable {
+    std::vector<double> energy, density, cdf;
+    double total = 0.0;
+};
+
+bool table_from_points(EnergyTable& t, const std::vector<double>& e, const std::vector<double>& f,
+                       std::string* err);
+bool planck_table(EnergyTable& t, double T, double emin, double emax, double rtol,
+                  const std::vector<double>& knots, std::string* err);
+double table_sample(const EnergyTable& t, double u);   // sample_energy_cdf
+double table_cdf(const EnergyTable& t, double e);      // energy_cdf_value
+
+struct BandSetup {
+    int nnu_band = 0, nfuv_band = 0;
+    std::vector<double> eedge;          // nnu_band + 1 ascending edges [eV]
+    int ncomp = 1, multi = 0, qmc_ndim = 3;
+    std::vector<double> comp_cdf;       // component-selection CDF (multi only)
+    std::vector<double> comp_x, comp_y, comp_z;
+    std::vector<EnergyTable> tables;    // one per component
+    double ion_Ltot = 0.0;
+};
+
+bool band_build(const mochii_params& p, BandSetup& b, std::string* err);
+
+}  // namespace mochii

@@ -1,0 +1,75 @@
+// Library context: everything one nebula needs on one device.  No global
+// state, so several contexts (nebulae) can coexist in a process.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <string>
+#include <vector>
+
+#include "band.h"
+#include "mochii_gpu.h"
+#include "qmc.cuh"
+
+namespace mochii {
+
+// Device-resident layout (structure of arrays over leaves, raster order for
+// the Cartesian grid, leaf index = ix + nx*(iy + ny*iz)):
+//   state   FP64: nH, xHI, xHeI, xHeII, ne, Te                 (6 x nleaf)
+//   columns per-leaf absorber columns n_i * distance2cm * 1e-18 [1/(1e-18 cm^2)
+//           per code length], nabs = 1 (H I) or 4 (H I, He I, He II, pad);
+//           FP64 or FP32 by the transport precision
+//   tally   per-leaf rate sums, ntally = 2 (Gamma_HI, H_HI) or 6 (+He I, He II);
+//           FP64 or (hi, lo) FP32 pairs
+//   jt      per-leaf diagnostic spectrum, nnu_band bins per leaf, same type
+//   rates   FP64 Gamma/heat, 6 x nleaf (gamma_HI..heat_HeII)
+struct DeviceTables {
+    double* tab_e = nullptr;   // concatenated sampler knots of all components
+    double* tab_f = nullptr;
+    double* tab_c = nullptr;
+    int* tab_off = nullptr;    // ncomp + 1 offsets
+    double* comp = nullptr;    // per component: cdf, x, y, z
+    double* eedge = nullptr;   // nnu_band + 1
+    QmcTables* qmc = nullptr;
+};
+
+struct Grid {
+    int nx = 0, ny = 0, nz = 0;
+    long long nleaf = 0;
+    double xmin = 0, xmax = 0, ymin = 0, ymax = 0, zmin = 0, zmax = 0, dcell = 0;
+};
+
+struct TransportWork {
+    double* ledger = nullptr;              // per block: emitted, absorbed, escaped
+    unsigned long long* counters = nullptr;  // segments, walk kills
+    int ledger_blocks = 0;
+};
+
+struct BalanceWork {
+    double* partial = nullptr;   // per block: max_dx, max_dte, sum_dxv, sum_xv, sum_dtv, sum_tv
+    unsigned long long* counters = nullptr;
+    int blocks = 0;
+};
+
+}  // namespace mochii
+
+struct mochii_ctx {
+    mochii_params par;
+    mochii::BandSetup band;
+    mochii::Grid grid;
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr, evA = nullptr, evB = nullptr;
+    bool columns_fresh = false;   // absorber columns match the state
+    bool fp32 = false;
+    int nabs = 1, ntally = 2, nnu = 0;
+    // device memory
+    double *nH = nullptr, *xHI = nullptr, *xHeI = nullptr, *xHeII = nullptr, *ne = nullptr, *Te = nullptr;
+    void* col = nullptr;
+    void* tally = nullptr;
+    void* jt = nullptr;
+    double* rates = nullptr;
+    mochii::DeviceTables tab;
+    mochii::TransportWork tw;
+    mochii::BalanceWork bw;
+    std::string last_error;
+};

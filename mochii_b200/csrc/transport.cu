@@ -1,0 +1,483 @@
+// Ionising-band transport pass on the device.
+//
+// One thread carries one packet at a time (grid-stride over packet
+// indices, so the launch set is the global Sobol sequence whatever the
+// grid shape): Owen-scrambled Sobol launch (qmc_mod.f90), source-energy
+// CDF inversion (energy_sampler_mod.f90:187-238), isotropic point emission
+// (ion_band_mod.f90:2232-2247), the packet's cross sections at its exact
+// energy (ion_packet_mod.f90:21-53), then the analytic zero-variance edge
+// walk through the Cartesian grid by the Amanatides-Woo stepping of
+// raytrace_amr.f90:495-592, scoring every segment's expected path
+// luminosity into the per-leaf rate tallies (ion_score_mod.f90:137-231) and
+// the packet's energy into the emitted/absorbed/escaped ledger
+// (ion_score_mod.f90:233-252).
+//
+// Geometry (positions, tMax/tDelta, face choice) is FP64 and compiled
+// without FMA contraction, so leaf sequences equal the reference's FP64
+// walk bit for bit.  Opacity, attenuation and tallies run in the
+// precision of R: FP64, or FP32 with compensated (hi, lo) tally pairs that
+// are summed in FP64 by the rate kernel.
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "ctx.h"
+#include "physics.cuh"
+#include "qmc.cuh"
+#include "transport.h"
+
+namespace mochii {
+
+namespace {
+
+constexpr int kThreads = 256;
+
+struct PassArgs {
+    const QmcTables* qmc;
+    const double* tab_e;
+    const double* tab_f;
+    const double* tab_c;
+    const int* tab_off;
+    const double* comp;   // ncomp x (cdf, x, y, z)
+    const double* eedge;
+    const void* col;
+    void* tally;
+    void* jt;
+    double* ledger;
+    unsigned long long* counters;
+    long long np;
+    double Lpacket;
+    double org[3];
+    double dcell;
+    int n[3];
+    int ncomp, multi, ndim, nnu;
+};
+
+// sample_energy_cdf, energy_sampler_mod.f90:187-238.  The bracket search and
+// the exact inverse of the linear density follow the same FP64 operation
+// sequence as the host restatement, so energies are bit-identical to it.
+__device__ double sample_energy(const double* __restrict__ e, const double* __restrict__ f,
+                                const double* __restrict__ c, int n, double u) {
+    const double q = fmin(fmax(u, 0.0), 1.0);
+    if (q <= 0.0) return e[0];
+    if (q >= 1.0) return e[n - 1];
+    int lo = 0, hi = n - 1;
+    while (hi - lo > 1) {
+        const int mid = (lo + hi + 2) / 2 - 1;
+        if (__ldg(c + mid) <= q) lo = mid; else hi = mid;
+    }
+    const double clo = __ldg(c + lo), chi = __ldg(c + hi);
+    const double area = chi - clo;
+    const double elo = __ldg(e + lo), ehi = __ldg(e + hi);
+    if (area <= 0.0) return ehi;
+    const double dx = ehi - elo;
+    const double y0 = __ldg(f + lo), y1 = __ldg(f + hi);
+    const double a = (q - clo) / area * (0.5 * (y0 + y1) * dx);
+    const double slope = (y1 - y0) / dx;
+    const double sc = fmax(fmax(fabs(y0), fabs(y1)), kTinest);
+    double off;
+    if (fabs(slope * dx) <= 64.0 * 2.220446049250313e-16 * sc)
+        off = y0 > 0.0 ? a / y0 : 0.0;
+    else
+        off = 2.0 * a / (y0 + sqrt(fmax(0.0, y0 * y0 + 2.0 * slope * a)));
+    return elo + fmin(fmax(off, 0.0), dx);
+}
+
+// ion_bin_of with include_fuv (ion_band_mod.f90:624-646), 0-based bin.
+__device__ int bin_of(const double* __restrict__ edge, int nnu, double eph) {
+    int lo = 1, hi = nnu;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) / 2;
+        if (__ldg(edge + mid - 1) <= eph) lo = mid; else hi = mid - 1;
+    }
+    return min(max(lo, 1), nnu) - 1;
+}
+
+// Compensated FP32 accumulation: the atomic returns the old value, the
+// rounding error of old + v is recovered exactly (Knuth TwoSum, valid for a
+// round-to-nearest add) and accumulated in the low word.
+__device__ __forceinline__ void tally_add(float2* p, float v) {
+    const float old = atomicAdd(&p->x, v);
+    const float s = old + v;
+    const float bp = s - old;
+    const float err = (old - (s - bp)) + (v - bp);
+    if (err != 0.0f) atomicAdd(&p->y, err);
+}
+__device__ __forceinline__ void tally_add(double* p, double v) { atomicAdd(p, v); }
+
+__device__ __forceinline__ float attenuation(float x) { return expf(-x); }
+__device__ __forceinline__ double attenuation(double x) { return exp(-x); }
+
+template <typename R> struct Acc;
+template <> struct Acc<double> { typedef double T; };
+template <> struct Acc<float> { typedef float2 T; };
+
+template <typename R, int NABS>
+__device__ __forceinline__ R opacity(const void* col, long long il, R s0, R s1, R s2) {
+    if constexpr (NABS == 1) {
+        const R c = __ldg(static_cast<const R*>(col) + il);
+        return c * s0;
+    } else if constexpr (sizeof(R) == 4) {
+        const float4 c = __ldg(static_cast<const float4*>(col) + il);
+        return c.x * s0 + (c.y * s1 + c.z * s2);
+    } else {
+        const double2* p = static_cast<const double2*>(col) + 2 * il;
+        const double2 c01 = __ldg(p);
+        const double c2 = __ldg(reinterpret_cast<const double*>(p + 1));
+        return c01.x * s0 + (c01.y * s1 + c2 * s2);
+    }
+}
+
+// Block reduction of a double in fixed order (deterministic).
+__device__ double block_sum(double v, double* sh) {
+    const int t = threadIdx.x;
+    sh[t] = v;
+    __syncthreads();
+    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+        if (t < s) sh[t] = sh[t] + sh[t + s];
+        __syncthreads();
+    }
+    const double r = sh[0];
+    __syncthreads();
+    return r;
+}
+
+template <typename R, int NABS>
+__global__ void __launch_bounds__(kThreads) k_transport(const PassArgs a) {
+    typedef typename Acc<R>::T T;
+    constexpr int NT = NABS == 1 ? 2 : 6;
+    __shared__ QmcTables sq;
+    __shared__ double sh[kThreads];
+    {
+        const uint32_t* src = reinterpret_cast<const uint32_t*>(a.qmc);
+        uint32_t* dst = reinterpret_cast<uint32_t*>(&sq);
+        for (int i = threadIdx.x; i < (int)(sizeof(QmcTables) / 4); i += blockDim.x) dst[i] = src[i];
+    }
+    __syncthreads();
+
+    double emitted = 0.0, absorbed = 0.0, escaped = 0.0;
+    unsigned long long nseg = 0, kills = 0;
+    T* tal = static_cast<T*>(a.tally);
+    T* jt = static_cast<T*>(a.jt);
+    const long long stride = (long long)gridDim.x * blockDim.x;
+
+    for (long long ip = (long long)blockIdx.x * blockDim.x + threadIdx.x; ip < a.np; ip += stride) {
+        // ---- launch: gen_ion_photon_qmc (ion_band_mod.f90:1880-1935) ----
+        double u[7];
+        for (int d = 0; d < a.ndim; ++d) u[d] = qmc_uniform(sq, (uint64_t)ip, d, 0);
+        int ic = 0;
+        double umu, uphi, ue;
+        if (!a.multi) {
+            ue = u[0]; umu = u[1]; uphi = u[2];
+        } else {
+            ic = a.ncomp - 1;
+            for (int i = 0; i < a.ncomp; ++i)
+                if (u[0] <= a.comp[4 * i]) { ic = i; break; }
+            ue = u[1]; umu = u[2]; uphi = u[3];
+        }
+        const int t0 = a.tab_off[ic], t1 = a.tab_off[ic + 1];
+        const double E = sample_energy(a.tab_e + t0, a.tab_f + t0, a.tab_c + t0, t1 - t0, ue);
+        const double pos[3] = {a.comp[4 * ic + 1], a.comp[4 * ic + 2], a.comp[4 * ic + 3]};
+        const double cost = 2.0 * umu - 1.0;
+        const double sint = sqrt(1.0 - cost * cost);
+        const double phi = kTwoPi * uphi;
+        double sphi, cphi;
+        sincos(phi, &sphi, &cphi);
+        const double kk[3] = {sint * cphi, sint * sphi, cost};
+        const int inu = bin_of(a.eedge, a.nnu, E);
+        // ---- packet cross sections (build_ion_packet_physics), 1e-18 cm^2 units
+        const double sHI = sigma_HI(E), sHeI = sigma_HeI(E), sHeII = sigma_HeII(E);
+        const R s0 = (R)(sHI * 1.0e18), s1 = (R)(sHeI * 1.0e18), s2 = (R)(sHeII * 1.0e18);
+        // rate coefficients per unit path (ion_score_mod.f90:213-221), scaled:
+        // Gamma_i: sigma_i/E [1e-18 cm^2/eV]; H_i: sigma_i (1 - E_th,i/E)
+        R cf[6];
+        cf[0] = (R)(sHI * 1.0e18 / E);
+        cf[1] = (R)(sHI * 1.0e18 * fmax(1.0 - kEthHI / E, 0.0));
+        cf[2] = (R)(sHeI * 1.0e18 / E);
+        cf[3] = (R)(sHeI * 1.0e18 * fmax(1.0 - kEthHeI / E, 0.0));
+        cf[4] = (R)(sHeII * 1.0e18 / E);
+        cf[5] = (R)(sHeII * 1.0e18 * fmax(1.0 - kEthHeII / E, 0.0));
+
+        // ---- dda_init (raytrace_amr.f90:495-532) ----
+        const double d = a.dcell;
+        int idx[3], stp[3];
+        double tmax[3], tdel[3];
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            idx[k] = min(max((int)((pos[k] - a.org[k]) / d), 0), a.n[k] - 1);
+            if (kk[k] > 0.0) {
+                stp[k] = 1; tmax[k] = (a.org[k] + (double)(idx[k] + 1) * d - pos[k]) / kk[k]; tdel[k] = d / kk[k];
+            } else if (kk[k] < 0.0) {
+                stp[k] = -1; tmax[k] = (a.org[k] + (double)idx[k] * d - pos[k]) / kk[k]; tdel[k] = -d / kk[k];
+            } else {
+                stp[k] = 0; tmax[k] = kHugest; tdel[k] = kHugest;
+            }
+        }
+        // ---- raytrace_ion_to_edge_car (raytrace_amr.f90:534-592) ----
+        R expo = (R)1.0;
+        double tau = 0.0, t_cur = 0.0;
+        int nstep = 0;
+        for (;;) {
+            if (++nstep > kMaxWalkSteps) { ++kills; break; }
+            const long long il = (long long)idx[0] + (long long)a.n[0] * ((long long)idx[1] + (long long)a.n[1] * idx[2]);
+            int ax = 0;
+            if (tmax[1] < tmax[ax]) ax = 1;
+            if (tmax[2] < tmax[ax]) ax = 2;
+            const double seg = tmax[ax] - t_cur;
+            const R kap = opacity<R, NABS>(a.col, il, s0, s1, s2);
+            const R ks = kap * (R)seg;
+            R w;
+            if (ks > (R)0) {
+                const R eo = expo * attenuation(ks);
+                w = (expo - eo) / kap;
+                expo = eo;
+            } else {
+                w = expo * (R)seg;
+            }
+            if (w != (R)0) {   // score_ion_path returns on a zero path (ion_score_mod.f90:148)
+                ++nseg;
+                T* tl = tal + il * NT;
+#pragma unroll
+                for (int k = 0; k < NT; ++k) tally_add(tl + k, w * cf[k]);
+                tally_add(jt + il * a.nnu + inu, w);
+            }
+            tau = tau + (double)ks;
+            if (tau >= kTauHuge) break;
+            t_cur = tmax[ax];
+            tmax[ax] = tmax[ax] + tdel[ax];
+            idx[ax] += stp[ax];
+            if (idx[ax] < 0 || idx[ax] >= a.n[ax]) break;
+        }
+        // ---- ion_score_energy_packet (ion_score_mod.f90:233-252) ----
+        const double lum = a.Lpacket;
+        const double tr = exp(-fmax(tau, 0.0));
+        emitted += lum;
+        absorbed += lum * (1.0 - tr);
+        escaped += lum * tr;
+    }
+    const double e0 = block_sum(emitted, sh);
+    const double e1 = block_sum(absorbed, sh);
+    const double e2 = block_sum(escaped, sh);
+    if (threadIdx.x == 0) {
+        a.ledger[3 * blockIdx.x + 0] = e0;
+        a.ledger[3 * blockIdx.x + 1] = e1;
+        a.ledger[3 * blockIdx.x + 2] = e2;
+    }
+    // counters: warp-reduce then one atomic per warp
+    for (int o = 16; o > 0; o >>= 1) {
+        nseg += __shfl_down_sync(0xffffffffu, nseg, o);
+        kills += __shfl_down_sync(0xffffffffu, kills, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        if (nseg) atomicAdd(a.counters + 0, nseg);
+        if (kills) atomicAdd(a.counters + 1, kills);
+    }
+}
+
+// gas_rates_compute + ion_score_apply_hhe (gas_rates_mod.f90:82-153,
+// ion_score_mod.f90:298-317): Gamma = sum * Lpacket * 1e-18 / ev2erg * fac,
+// H = sum * Lpacket * 1e-18 * fac, fac = 1/((2h)^3 distance2cm^2).  The
+// FP32 pair is reduced in FP64 here.
+template <typename T>
+__device__ __forceinline__ double tval(const T& v);
+template <> __device__ __forceinline__ double tval<double>(const double& v) { return v; }
+template <> __device__ __forceinline__ double tval<float2>(const float2& v) { return (double)v.x + (double)v.y; }
+
+template <typename T, int NT>
+__global__ void k_rates(const T* __restrict__ tal, double* __restrict__ rates, long long nleaf, double cg, double ch) {
+    for (long long il = (long long)blockIdx.x * blockDim.x + threadIdx.x; il < nleaf;
+         il += (long long)gridDim.x * blockDim.x) {
+        const T* t = tal + il * NT;
+        rates[0 * nleaf + il] = tval<T>(t[0]) * cg;
+        rates[3 * nleaf + il] = tval<T>(t[1]) * ch;
+        if (NT == 6) {
+            rates[1 * nleaf + il] = tval<T>(t[2]) * cg;
+            rates[4 * nleaf + il] = tval<T>(t[3]) * ch;
+            rates[2 * nleaf + il] = tval<T>(t[4]) * cg;
+            rates[5 * nleaf + il] = tval<T>(t[5]) * ch;
+        } else {
+            rates[1 * nleaf + il] = 0.0;
+            rates[4 * nleaf + il] = 0.0;
+            rates[2 * nleaf + il] = 0.0;
+            rates[5 * nleaf + il] = 0.0;
+        }
+    }
+}
+
+template <typename T>
+__global__ void k_jt(const T* __restrict__ jt, double* __restrict__ out, long long n, double scale) {
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        out[i] = tval<T>(jt[i]) * scale;
+}
+
+// Sobol uniforms for the test hook.
+__global__ void k_sobol(const QmcTables* t, int stream, long long idx0, long long n, int nd, double* out) {
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        for (int d = 0; d < nd; ++d) out[i * nd + d] = qmc_uniform(*t, (uint64_t)(idx0 + i), d, stream);
+}
+
+// Geometry-only DDA (no optical-depth cut) for the leaf-sequence hook.
+__global__ void k_walk(const double* rays, long long nray, int max_steps, int* leaves, int* nsteps, double ox,
+                       double oy, double oz, double d, int nx, int ny, int nz) {
+    const long long r = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= nray) return;
+    const double pos[3] = {rays[6 * r], rays[6 * r + 1], rays[6 * r + 2]};
+    const double kk[3] = {rays[6 * r + 3], rays[6 * r + 4], rays[6 * r + 5]};
+    const double org[3] = {ox, oy, oz};
+    const int n[3] = {nx, ny, nz};
+    int idx[3], stp[3];
+    double tmax[3], tdel[3];
+    for (int k = 0; k < 3; ++k) {
+        idx[k] = min(max((int)((pos[k] - org[k]) / d), 0), n[k] - 1);
+        if (kk[k] > 0.0) {
+            stp[k] = 1; tmax[k] = (org[k] + (double)(idx[k] + 1) * d - pos[k]) / kk[k]; tdel[k] = d / kk[k];
+        } else if (kk[k] < 0.0) {
+            stp[k] = -1; tmax[k] = (org[k] + (double)idx[k] * d - pos[k]) / kk[k]; tdel[k] = -d / kk[k];
+        } else {
+            stp[k] = 0; tmax[k] = kHugest; tdel[k] = kHugest;
+        }
+    }
+    int ns = 0;
+    while (ns < max_steps) {
+        leaves[r * max_steps + ns++] = idx[0] + n[0] * (idx[1] + n[1] * idx[2]);
+        int ax = 0;
+        if (tmax[1] < tmax[ax]) ax = 1;
+        if (tmax[2] < tmax[ax]) ax = 2;
+        tmax[ax] = tmax[ax] + tdel[ax];
+        idx[ax] += stp[ax];
+        if (idx[ax] < 0 || idx[ax] >= n[ax]) break;
+    }
+    nsteps[r] = ns;
+}
+
+// Launch records (x, y, z, kx, ky, kz, E, inu) for the launch hook.
+__global__ void k_launch_records(const PassArgs a, long long ip0, long long n, double* out) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const long long ip = ip0 + i;
+    double u[7];
+    for (int d = 0; d < a.ndim; ++d) u[d] = qmc_uniform(*a.qmc, (uint64_t)ip, d, 0);
+    int ic = 0;
+    double umu, uphi, ue;
+    if (!a.multi) {
+        ue = u[0]; umu = u[1]; uphi = u[2];
+    } else {
+        ic = a.ncomp - 1;
+        for (int k = 0; k < a.ncomp; ++k)
+            if (u[0] <= a.comp[4 * k]) { ic = k; break; }
+        ue = u[1]; umu = u[2]; uphi = u[3];
+    }
+    const int t0 = a.tab_off[ic], t1 = a.tab_off[ic + 1];
+    const double E = sample_energy(a.tab_e + t0, a.tab_f + t0, a.tab_c + t0, t1 - t0, ue);
+    const double cost = 2.0 * umu - 1.0;
+    const double sint = sqrt(1.0 - cost * cost);
+    double sphi, cphi;
+    sincos(kTwoPi * uphi, &sphi, &cphi);
+    double* o = out + 8 * i;
+    o[0] = a.comp[4 * ic + 1]; o[1] = a.comp[4 * ic + 2]; o[2] = a.comp[4 * ic + 3];
+    o[3] = sint * cphi; o[4] = sint * sphi; o[5] = cost;
+    o[6] = E;
+    o[7] = (double)bin_of(a.eedge, a.nnu, E);
+}
+
+PassArgs make_args(mochii_ctx* c) {
+    PassArgs a;
+    a.qmc = c->tab.qmc;
+    a.tab_e = c->tab.tab_e;
+    a.tab_f = c->tab.tab_f;
+    a.tab_c = c->tab.tab_c;
+    a.tab_off = c->tab.tab_off;
+    a.comp = c->tab.comp;
+    a.eedge = c->tab.eedge;
+    a.col = c->col;
+    a.tally = c->tally;
+    a.jt = c->jt;
+    a.ledger = c->tw.ledger;
+    a.counters = c->tw.counters;
+    a.np = c->par.nphotons;
+    a.Lpacket = c->band.ion_Ltot / (double)c->par.nphotons;
+    a.org[0] = c->grid.xmin; a.org[1] = c->grid.ymin; a.org[2] = c->grid.zmin;
+    a.dcell = c->grid.dcell;
+    a.n[0] = c->grid.nx; a.n[1] = c->grid.ny; a.n[2] = c->grid.nz;
+    a.ncomp = c->band.ncomp;
+    a.multi = c->band.multi;
+    a.ndim = c->band.qmc_ndim;
+    a.nnu = c->nnu;
+    return a;
+}
+
+int grid_blocks(long long work, int threads, int cap) {
+    long long b = (work + threads - 1) / threads;
+    if (b < 1) b = 1;
+    if (b > cap) b = cap;
+    return (int)b;
+}
+
+}  // namespace
+
+int transport_blocks(const mochii_ctx* c) {
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device);
+    return grid_blocks(c->par.nphotons, kThreads, sms * 8);
+}
+
+cudaError_t launch_transport(mochii_ctx* c) {
+    const PassArgs a = make_args(c);
+    const int blocks = c->tw.ledger_blocks;
+    if (c->fp32) {
+        if (c->nabs == 1) k_transport<float, 1><<<blocks, kThreads, 0, c->stream>>>(a);
+        else k_transport<float, 4><<<blocks, kThreads, 0, c->stream>>>(a);
+    } else {
+        if (c->nabs == 1) k_transport<double, 1><<<blocks, kThreads, 0, c->stream>>>(a);
+        else k_transport<double, 4><<<blocks, kThreads, 0, c->stream>>>(a);
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_rates(mochii_ctx* c) {
+    const double h = 0.5 * c->grid.dcell;
+    const double w = 2.0 * h;
+    const double fac = 1.0 / ((w * w * w) * (c->par.distance2cm * c->par.distance2cm));
+    const double Lp = c->band.ion_Ltot / (double)c->par.nphotons;
+    const double cg = Lp * 1.0e-18 / kEv2erg * fac;
+    const double ch = Lp * 1.0e-18 * fac;
+    const long long n = c->grid.nleaf;
+    const int blocks = grid_blocks(n, 256, 148 * 16);
+    if (c->fp32) {
+        if (c->ntally == 2) k_rates<float2, 2><<<blocks, 256, 0, c->stream>>>((const float2*)c->tally, c->rates, n, cg, ch);
+        else k_rates<float2, 6><<<blocks, 256, 0, c->stream>>>((const float2*)c->tally, c->rates, n, cg, ch);
+    } else {
+        if (c->ntally == 2) k_rates<double, 2><<<blocks, 256, 0, c->stream>>>((const double*)c->tally, c->rates, n, cg, ch);
+        else k_rates<double, 6><<<blocks, 256, 0, c->stream>>>((const double*)c->tally, c->rates, n, cg, ch);
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_jt_export(mochii_ctx* c, double* dst) {
+    const long long n = c->grid.nleaf * (long long)c->nnu;
+    const double Lp = c->band.ion_Ltot / (double)c->par.nphotons;
+    const int blocks = grid_blocks(n, 256, 148 * 16);
+    if (c->fp32) k_jt<float2><<<blocks, 256, 0, c->stream>>>((const float2*)c->jt, dst, n, Lp);
+    else k_jt<double><<<blocks, 256, 0, c->stream>>>((const double*)c->jt, dst, n, Lp);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_sobol(const QmcTables* t, int stream01, long long idx0, long long n, int nd, double* out,
+                         cudaStream_t s) {
+    k_sobol<<<grid_blocks(n, 256, 148 * 16), 256, 0, s>>>(t, stream01, idx0, n, nd, out);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_walk(mochii_ctx* c, const double* rays, long long nray, int max_steps, int* leaves, int* nsteps) {
+    k_walk<<<grid_blocks(nray, 128, 1 << 20), 128, 0, c->stream>>>(rays, nray, max_steps, leaves, nsteps,
+                                                                     c->grid.xmin, c->grid.ymin, c->grid.zmin,
+                                                                     c->grid.dcell, c->grid.nx, c->grid.ny, c->grid.nz);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_records(mochii_ctx* c, long long ip0, long long n, double* out) {
+    const PassArgs a = make_args(c);
+    k_launch_records<<<grid_blocks(n, 128, 1 << 20), 128, 0, c->stream>>>(a, ip0, n, out);
+    return cudaGetLastError();
+}
+
+}  // namespace mochii

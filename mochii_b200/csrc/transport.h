@@ -1,0 +1,22 @@
+// Kernel launchers shared between the C-ABI layer and the kernel files.
+#pragma once
+#include <cuda_runtime.h>
+
+#include "ctx.h"
+
+namespace mochii {
+
+int transport_blocks(const mochii_ctx* c);
+cudaError_t launch_transport(mochii_ctx* c);
+cudaError_t launch_rates(mochii_ctx* c);
+cudaError_t launch_jt_export(mochii_ctx* c, double* dst);
+cudaError_t launch_sobol(const QmcTables* t, int stream01, long long idx0, long long n, int nd, double* out,
+                         cudaStream_t s);
+cudaError_t launch_walk(mochii_ctx* c, const double* rays, long long nray, int max_steps, int* leaves, int* nsteps);
+cudaError_t launch_records(mochii_ctx* c, long long ip0, long long n, double* out);
+
+int balance_blocks(const mochii_ctx* c);
+cudaError_t launch_columns(mochii_ctx* c);
+cudaError_t launch_balance(mochii_ctx* c);
+
+}  // namespace mochii

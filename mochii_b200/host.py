@@ -1,0 +1,203 @@
+"""Host side of the transport + balance path, mirroring MoCHII's interface.
+
+    par = read_input("hii.in")                     # setup.f90:11-35
+    neb = Nebula(par)                              # grid_create_amr + ion_setup + gas_state_setup
+    neb.ionizing_field_and_rates()                 # ionizing_field_mod.f90:72
+    max_dx, dx_vol = neb.gas_equilibrium_update()  # ion_balance_mod.f90:352
+    neb.gas_opacity_fill()                         # gas_opacity_mod.f90:299
+    result = run(par)                              # the driver loop, main.f90:128-225
+
+Every call goes through libmochii_gpu.so; errors come back as MochiiError
+carrying the library's status code (the reference aborts instead).
+"""
+import ctypes as C
+
+import numpy as np
+
+from . import _lib
+from ._lib import Metrics, MochiiError, Params, PassStats
+
+STATE_FIELDS = ("nH", "x_HI", "x_HeI", "x_HeII", "n_e", "T_e")
+RATE_FIELDS = ("gamma_HI", "gamma_HeI", "gamma_HeII", "heat_HI", "heat_HeI", "heat_HeII")
+
+
+def _check(lib, status, ctx=None):
+    if status != _lib.OK:
+        msg = lib.mochii_last_error(ctx)
+        raise MochiiError(status, (msg or b"").decode() or lib.mochii_strerror(status).decode())
+
+
+def default_params():
+    lib = _lib.load()
+    p = Params()
+    _check(lib, lib.mochii_params_default(C.byref(p)))
+    return p
+
+
+def parse_namelist(text, base=None):
+    """Parse '&parameters par%key = value ... /' text over base (or defaults)."""
+    lib = _lib.load()
+    p = base if base is not None else default_params()
+    err = C.create_string_buffer(512)
+    rc = lib.mochii_params_parse_namelist(C.byref(p), text.encode(), err, 512)
+    if rc != _lib.OK:
+        raise MochiiError(rc, err.value.decode())
+    return p
+
+
+def read_input(path):
+    """read_input (setup.f90:11-35): the namelist file named on the command line."""
+    lib = _lib.load()
+    p = default_params()
+    err = C.create_string_buffer(512)
+    rc = lib.mochii_params_read_namelist(C.byref(p), str(path).encode(), err, 512)
+    if rc != _lib.OK:
+        raise MochiiError(rc, err.value.decode())
+    return p
+
+
+def set_param(p, key, value):
+    lib = _lib.load()
+    if isinstance(value, bool):
+        value = ".true." if value else ".false."
+    rc = lib.mochii_params_set(C.byref(p), key.encode(), str(value).encode())
+    if rc != _lib.OK:
+        raise MochiiError(rc, f"par%{key} = {value!r}")
+    return p
+
+
+def sobol_uniforms(seed, stream, idx0, n, nd):
+    """Device Owen-scrambled Sobol uniforms (qmc_uniforms_stream), shape (n, nd)."""
+    lib = _lib.load()
+    out = np.zeros((n, nd), dtype=np.float64)
+    rc = lib.mochii_sobol_uniforms(int(seed), int(stream), int(idx0), int(n), int(nd), out.ctypes.data)
+    _check(lib, rc)
+    return out
+
+
+class Nebula:
+    """One nebula on the current CUDA device (a mochii_ctx)."""
+
+    def __init__(self, par):
+        self.lib = _lib.load()
+        self.par = par
+        h = C.c_void_p()
+        _check(self.lib, self.lib.mochii_init(C.byref(par), C.byref(h)))
+        self.ctx = h
+        self.nleaf = int(self.lib.mochii_nleaf(h))
+        self.nnu_band = int(self.lib.mochii_nnu_band(h))
+        self.last_pass = None
+        self.last_metrics = None
+
+    def close(self):
+        if self.ctx:
+            self.lib.mochii_destroy(self.ctx)
+            self.ctx = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _ok(self, rc):
+        _check(self.lib, rc, self.ctx)
+
+    # ---- the replaced module entry points ------------------------------
+    def ionizing_field_and_rates(self, with_peel=False):
+        st = PassStats()
+        self._ok(self.lib.mochii_transport_pass(self.ctx, int(bool(with_peel)), C.byref(st)))
+        self.last_pass = st
+        return st
+
+    def gas_equilibrium_update(self):
+        m = Metrics()
+        self._ok(self.lib.mochii_balance_update(self.ctx, 0, C.byref(m)))
+        self.last_metrics = m
+        return m.max_dx, m.dx_vol
+
+    def gas_thermal_update(self):
+        m = Metrics()
+        self._ok(self.lib.mochii_balance_update(self.ctx, 1, C.byref(m)))
+        self.last_metrics = m
+        return m.max_dx, m.max_dte, m.dx_vol, m.dte_vol
+
+    def gas_opacity_fill(self):
+        self._ok(self.lib.mochii_opacity_fill(self.ctx))
+
+    # ---- state exchange ---------------------------------------------------
+    def get(self, name):
+        n = {"jt_ion": self.nleaf * self.nnu_band, "eedge": self.nnu_band + 1}.get(name, self.nleaf)
+        out = np.zeros(n, dtype=np.float64)
+        self._ok(self.lib.mochii_get_field(self.ctx, name.encode(), out.ctypes.data, n))
+        if name == "jt_ion":
+            out = out.reshape(self.nleaf, self.nnu_band)
+        return out
+
+    def set(self, name, values):
+        a = np.ascontiguousarray(values, dtype=np.float64)
+        self._ok(self.lib.mochii_set_field(self.ctx, name.encode(), a.ctypes.data, a.size))
+
+    def set_nphotons(self, n):
+        self._ok(self.lib.mochii_set_nphotons(self.ctx, int(n)))
+
+    @property
+    def ion_Ltot(self):
+        return float(self.lib.mochii_ion_Ltot(self.ctx))
+
+    def walk_leaves(self, rays, max_steps):
+        rays = np.ascontiguousarray(rays, dtype=np.float64).reshape(-1, 6)
+        nray = rays.shape[0]
+        leaves = np.full((nray, max_steps), -1, dtype=np.int32)
+        nsteps = np.zeros(nray, dtype=np.int32)
+        self._ok(self.lib.mochii_walk_leaves(self.ctx, nray, rays.ctypes.data, int(max_steps),
+                                             leaves.ctypes.data, nsteps.ctypes.data))
+        return leaves, nsteps
+
+    def launch_records(self, ip0, n):
+        out = np.zeros((n, 8), dtype=np.float64)
+        self._ok(self.lib.mochii_launch_records(self.ctx, int(ip0), int(n), out.ctypes.data))
+        return out
+
+
+def run(par, log=None, final_pass=True):
+    """The iteration of main.f90:120-225: transport -> rates -> balance ->
+    opacity feedback until converged or par%gas_niter, then one final
+    consistency pass.  Returns (nebula, history)."""
+    neb = Nebula(par)
+    niter = max(par.gas_niter, 1)
+    history = []
+    converged = False
+    for it in range(1, niter + 1):
+        st = neb.ionizing_field_and_rates()
+        rec = {"iter": it, "closure": st.closure, "segments": st.direct_segments, "transport_ms": st.kernel_ms}
+        if par.gas_niter < 1:
+            history.append(rec)
+            break
+        if par.solve_te:
+            max_dx, max_dte, dx_vol, dte_vol = neb.gas_thermal_update()
+            converged = (dx_vol < par.gas_tol and dte_vol < par.gas_tol_te) if par.conv_vol else \
+                (max_dx < par.gas_tol and max_dte < par.gas_tol_te)
+            rec.update(max_dx=max_dx, max_dte=max_dte, dx_vol=dx_vol, dte_vol=dte_vol)
+        else:
+            max_dx, dx_vol = neb.gas_equilibrium_update()
+            converged = dx_vol < par.gas_tol if par.conv_vol else max_dx < par.gas_tol
+            rec.update(max_dx=max_dx, dx_vol=dx_vol)
+        rec["balance_ms"] = neb.last_metrics.kernel_ms
+        neb.gas_opacity_fill()
+        history.append(rec)
+        if log:
+            log(rec)
+        if converged:
+            break
+    if par.gas_niter >= 1 and not converged and par.require_convergence:
+        raise MochiiError(7, f"gas iteration did not converge in {niter} iterations")
+    if final_pass and par.gas_niter >= 1:
+        neb.ionizing_field_and_rates()   # final consistency pass, main.f90:225
+    return neb, history

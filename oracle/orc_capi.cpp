@@ -1,0 +1,239 @@
+// Oracle C entry points for ctypes (test infrastructure only).
+#include <cstring>
+#include <string>
+
+#include "orc_core.h"
+
+using namespace orc;
+
+namespace {
+thread_local std::string g_err;
+void copy_err(char* buf, int n) {
+    if (buf && n > 0) {
+        std::strncpy(buf, g_err.c_str(), (size_t)n - 1);
+        buf[n - 1] = 0;
+    }
+}
+}  // namespace
+
+extern "C" {
+
+const char* orc_last_error() { return g_err.c_str(); }
+
+// Scrambled uniforms u[i*nd + d] for 0-based indices idx0..idx0+n-1
+// (qmc_uniforms_stream, qmc_mod.f90:157-168).
+int orc_qmc_uniforms(int seed, int stream, long long idx0, long long n, int nd, double* out) {
+    if (nd < 1 || nd > 12 || (stream != 1 && stream != 2)) return 1;
+    Qmc q;
+    q.setup(seed);
+    for (long long i = 0; i < n; ++i)
+        for (int d = 1; d <= nd; ++d) out[i * nd + d - 1] = q.uniform(idx0 + i, d, stream);
+    return 0;
+}
+
+// Unscrambled codes (qmc_uniforms_raw, qmc_mod.f90:174-184).
+int orc_qmc_raw_codes(long long idx0, long long n, int nd, unsigned* out) {
+    if (nd < 1 || nd > 12) return 1;
+    Qmc q;
+    q.setup(0);
+    for (long long i = 0; i < n; ++i)
+        for (int d = 1; d <= nd; ++d) out[i * nd + d - 1] = q.sobol_code(idx0 + i, d);
+    return 0;
+}
+
+void orc_qmc_keys(int seed, unsigned* out24) {
+    Qmc q;
+    q.setup(seed);
+    for (int s = 0; s < 2; ++s)
+        for (int d = 0; d < 12; ++d) out24[s * 12 + d] = q.key[s][d];
+}
+
+// ---- samplers ------------------------------------------------------------
+void* orc_sampler_planck(double T, double emin, double emax, double rtol, const double* thr, int nthr) {
+    auto* s = new Sampler();
+    std::vector<double> t(thr, thr + nthr);
+    if (!build_planck_sampler(*s, T, emin, emax, rtol, t, &g_err)) {
+        delete s;
+        return nullptr;
+    }
+    return s;
+}
+void* orc_sampler_tab(const double* e, const double* f, int n) {
+    auto* s = new Sampler();
+    if (!build_tabulated_sampler(*s, std::vector<double>(e, e + n), std::vector<double>(f, f + n), &g_err)) {
+        delete s;
+        return nullptr;
+    }
+    return s;
+}
+void* orc_sampler_tab_band(const double* e, const double* f, int n, double emin, double emax) {
+    auto* s = new Sampler();
+    if (!build_tabulated_band_sampler(*s, std::vector<double>(e, e + n), std::vector<double>(f, f + n), emin, emax,
+                                      &g_err)) {
+        delete s;
+        return nullptr;
+    }
+    return s;
+}
+int orc_sampler_size(void* h) { return (int)static_cast<Sampler*>(h)->energy.size(); }
+double orc_sampler_total(void* h) { return static_cast<Sampler*>(h)->total_integral; }
+void orc_sampler_get(void* h, double* e, double* f, double* c) {
+    auto* s = static_cast<Sampler*>(h);
+    for (size_t i = 0; i < s->energy.size(); ++i) {
+        e[i] = s->energy[i];
+        f[i] = s->density[i];
+        c[i] = s->cdf[i];
+    }
+}
+void orc_sampler_sample(void* h, const double* u, long long n, double* out) {
+    auto* s = static_cast<Sampler*>(h);
+    for (long long i = 0; i < n; ++i) out[i] = sample_energy_cdf(*s, u[i]);
+}
+void orc_sampler_cdf(void* h, const double* e, long long n, double* out) {
+    auto* s = static_cast<Sampler*>(h);
+    for (long long i = 0; i < n; ++i) out[i] = energy_cdf_value(*s, e[i]);
+}
+void orc_sampler_free(void* h) { delete static_cast<Sampler*>(h); }
+
+// ---- scalar physics --------------------------------------------------------
+// name in {alphaA_HII, alphaB_HII, alpha1_HII, ... , ci_HI, ci_HeI, ci_HeII,
+// sigma_HI, sigma_HeI, sigma_HeII}; model 0 = badnell_milne, 1 = hui_gnedin.
+int orc_eval(const char* name, int recomb_model, const double* x, long long n, double* out) {
+    RateModel m;
+    m.recomb = recomb_model;
+    std::string s(name);
+    for (long long i = 0; i < n; ++i) {
+        const double T = x[i];
+        double v;
+        if (s == "alphaA_HII") v = alphaA_HII(m, T);
+        else if (s == "alphaB_HII") v = alphaB_HII(m, T);
+        else if (s == "alpha1_HII") v = alpha1_HII(T);
+        else if (s == "alphaA_HeII") v = alphaA_HeII(m, T);
+        else if (s == "alphaB_HeII") v = alphaB_HeII(m, T);
+        else if (s == "alpha1_HeII") v = alpha1_HeII(T);
+        else if (s == "alphaA_HeIII") v = alphaA_HeIII(m, T);
+        else if (s == "alphaB_HeIII") v = alphaB_HeIII(m, T);
+        else if (s == "alpha1_HeIII") v = alpha1_HeIII(T);
+        else if (s == "ci_HI") v = ci_HI(m, T);
+        else if (s == "ci_HeI") v = ci_HeI(m, T);
+        else if (s == "ci_HeII") v = ci_HeII(m, T);
+        else if (s == "sigma_HI") v = sigma_HI(T);
+        else if (s == "sigma_HeI") v = sigma_HeI(T);
+        else if (s == "sigma_HeII") v = sigma_HeII(T);
+        else return 1;
+        out[i] = v;
+    }
+    return 0;
+}
+
+// Bin edges for a namelist (ion_setup band part).
+int orc_band_edges(const char* nl, double* out, int cap) {
+    Par p;
+    if (!parse_namelist(nl, p, &g_err)) return -1;
+    Band b;
+    if (!band_setup(p, b, &g_err)) return -1;
+    if ((int)b.eedge.size() > cap) return -1;
+    for (size_t i = 0; i < b.eedge.size(); ++i) out[i] = b.eedge[i];
+    return (int)b.eedge.size();
+}
+
+// ---- simulation ------------------------------------------------------------
+void* orc_sim_new(const char* namelist, int nthreads, char* errbuf, int errlen) {
+    auto* s = new Sim();
+    s->nthreads = nthreads;
+    if (!s->setup(namelist, &g_err)) {
+        copy_err(errbuf, errlen);
+        delete s;
+        return nullptr;
+    }
+    return s;
+}
+void orc_sim_free(void* h) { delete static_cast<Sim*>(h); }
+int orc_sim_nleaf(void* h) { return static_cast<Sim*>(h)->grid.nleaf; }
+int orc_sim_nnu(void* h) { return static_cast<Sim*>(h)->band.nnu_band; }
+double orc_sim_ion_Ltot(void* h) { return static_cast<Sim*>(h)->band.ion_Ltot; }
+void orc_sim_set_nphotons(void* h, long long n) { static_cast<Sim*>(h)->par.nphotons = n; }
+int orc_sim_transport_pass(void* h) {
+    static_cast<Sim*>(h)->transport_pass();
+    return 0;
+}
+int orc_sim_equilibrium_update(void* h, double* metrics2) {
+    static_cast<Sim*>(h)->gas_equilibrium_update(&metrics2[0], &metrics2[1]);
+    return 0;
+}
+// energy ledger (emitted, absorbed, escaped) and segment counts
+void orc_sim_energy(void* h, double* e3, long long* segs2) {
+    auto* s = static_cast<Sim*>(h);
+    e3[0] = (double)s->tally.emitted;
+    e3[1] = (double)s->tally.absorbed;
+    e3[2] = (double)s->tally.escaped;
+    segs2[0] = s->tally.direct_segments;
+    segs2[1] = s->tally.scattered_segments;
+}
+// field names: nH x_HI x_HeI x_HeII n_e T_e gamma_HI gamma_HeI gamma_HeII
+// heat_HI heat_HeI heat_HeII jt_ion (nleaf*nnu, leaf-major) hhe (nleaf*6)
+long long orc_sim_get(void* h, const char* name, double* out, long long cap) {
+    auto* s = static_cast<Sim*>(h);
+    std::string n(name);
+    const std::vector<double>* v = nullptr;
+    if (n == "nH") v = &s->st.nH;
+    else if (n == "x_HI") v = &s->st.xHI;
+    else if (n == "x_HeI") v = &s->st.xHeI;
+    else if (n == "x_HeII") v = &s->st.xHeII;
+    else if (n == "n_e") v = &s->st.ne;
+    else if (n == "T_e") v = &s->st.Te;
+    else if (n == "gamma_HI") v = &s->gamma_HI;
+    else if (n == "gamma_HeI") v = &s->gamma_HeI;
+    else if (n == "gamma_HeII") v = &s->gamma_HeII;
+    else if (n == "heat_HI") v = &s->heat_HI;
+    else if (n == "heat_HeI") v = &s->heat_HeI;
+    else if (n == "heat_HeII") v = &s->heat_HeII;
+    else if (n == "jt_ion") v = &s->tally.jt;
+    else if (n == "hhe") v = &s->tally.hhe;
+    else if (n == "eedge") v = &s->band.eedge;
+    if (!v) return -1;
+    if ((long long)v->size() > cap) return -(long long)v->size();
+    std::memcpy(out, v->data(), v->size() * sizeof(double));
+    return (long long)v->size();
+}
+long long orc_sim_set(void* h, const char* name, const double* in, long long n) {
+    auto* s = static_cast<Sim*>(h);
+    std::string nm(name);
+    std::vector<double>* v = nullptr;
+    if (nm == "x_HI") v = &s->st.xHI;
+    else if (nm == "x_HeI") v = &s->st.xHeI;
+    else if (nm == "x_HeII") v = &s->st.xHeII;
+    else if (nm == "n_e") v = &s->st.ne;
+    else if (nm == "T_e") v = &s->st.Te;
+    else if (nm == "nH") v = &s->st.nH;
+    if (!v || (long long)v->size() != n) return -1;
+    std::memcpy(v->data(), in, (size_t)n * sizeof(double));
+    return n;
+}
+// Launch record of packet ip: x,y,z,kx,ky,kz,E,inu
+void orc_sim_photon(void* h, long long ip, double* out8) {
+    auto* s = static_cast<Sim*>(h);
+    Photon ph;
+    s->gen_photon_qmc(ip, ph);
+    out8[0] = ph.x; out8[1] = ph.y; out8[2] = ph.z;
+    out8[3] = ph.kx; out8[4] = ph.ky; out8[5] = ph.kz;
+    out8[6] = ph.E; out8[7] = ph.inu;
+}
+// Geometry-only leaf sequences for nray rays (x,y,z,kx,ky,kz each).
+int orc_sim_walk_leaves(void* h, long long nray, const double* rays, int max_steps, int* leaves, int* nsteps) {
+    auto* s = static_cast<Sim*>(h);
+    for (long long r = 0; r < nray; ++r) {
+        const double* q = rays + 6 * r;
+        nsteps[r] = s->walk_leaves_car(q[0], q[1], q[2], q[3], q[4], q[5], max_steps, leaves + r * max_steps);
+    }
+    return 0;
+}
+// Single-cell solve (ion_balance_mod.f90:53-150), H/He path.
+void orc_solve_ion_cell(int recomb_model, double yHe, double gH, double gHe1, double gHe2, double nH, double T,
+                        int caseA, double* x3, double* ne) {
+    RateModel m;
+    m.recomb = recomb_model;
+    solve_ion_cell(m, yHe, gH, gHe1, gHe2, nH, T, caseA != 0, x3[0], x3[1], x3[2], *ne);
+}
+
+}  // extern "C"

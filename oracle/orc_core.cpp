@@ -1,0 +1,1254 @@
+// Oracle (test infrastructure only): FP64 CPU restatement of the MoCHII
+// transport + balance path.  See orc_core.h for the contract.
+#include "orc_core.h"
+
+#include <algorithm>
+#include <cctype>
+#include <cstdio>
+#include <cstring>
+#include <sstream>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+namespace orc {
+
+// =========================================================================
+// qmc_mod.f90
+// =========================================================================
+// lowbias32 avalanche hash, qmc_mod.f90:250-260 (all arithmetic mod 2^32).
+uint32_t hash32(uint32_t x) {
+    x ^= x >> 16;
+    x *= 0x7FEB352Du;
+    x ^= x >> 15;
+    x *= 0x846CA68Bu;
+    x ^= x >> 16;
+    return x;
+}
+
+// 32-bit reversal by swaps, qmc_mod.f90:233-247.
+uint32_t reverse32(uint32_t n) {
+    n = (n << 16) | (n >> 16);
+    n = ((n & 0x00FF00FFu) << 8) | ((n & 0xFF00FF00u) >> 8);
+    n = ((n & 0x0F0F0F0Fu) << 4) | ((n & 0xF0F0F0F0u) >> 4);
+    n = ((n & 0x33333333u) << 2) | ((n & 0xCCCCCCCCu) >> 2);
+    n = ((n & 0x55555555u) << 1) | ((n & 0xAAAAAAAAu) >> 1);
+    return n;
+}
+
+// Laine-Karras nested permutation, qmc_mod.f90:221-230.  The Fortran
+// multiplies two values below 2^32 in int64 and masks the low 32 bits,
+// which equals the uint32 product.
+uint32_t laine_karras(uint32_t x, uint32_t seed) {
+    x = x + seed;
+    x ^= x * 0x6C50B47Cu;
+    x ^= x * 0xB82F1E52u;
+    x ^= x * 0xC7AFE638u;
+    x ^= x * 0x8D22F6E6u;
+    return x;
+}
+
+uint32_t owen_scramble(uint32_t x, uint32_t seed) {  // qmc_mod.f90:212-219
+    return reverse32(laine_karras(reverse32(x), seed));
+}
+
+// qmc_mod.f90:73-139.  Dimension 1 is van der Corput; dimensions 2..12 use
+// the Joe-Kuo new-joe-kuo-6 degree / polynomial / initial integers of
+// qmc_mod.f90:80-97 with the direction-number recurrence of :104-123.
+void Qmc::setup(int seed) {
+    static const int sdeg[13] = {0, 0, 1, 2, 3, 3, 4, 4, 5, 5, 5, 5, 5};
+    static const int apoly[13] = {0, 0, 0, 1, 1, 2, 1, 4, 2, 4, 7, 11, 13};
+    static const int minit[13][5] = {
+        {0}, {0}, {1}, {1, 3}, {1, 3, 1}, {1, 1, 1}, {1, 1, 3, 3}, {1, 3, 5, 13},
+        {1, 1, 5, 5, 17}, {1, 1, 5, 5, 5}, {1, 1, 7, 11, 19}, {1, 1, 5, 1, 1},
+        {1, 1, 1, 3, 11}};
+    for (int k = 1; k <= 32; ++k) V[0][k - 1] = 1u << (32 - k);
+    for (int d = 2; d <= 12; ++d) {
+        const int s = sdeg[d], a = apoly[d];
+        for (int k = 1; k <= s; ++k)
+            V[d - 1][k - 1] = (uint32_t)((uint64_t)minit[d][k - 1] << (32 - k));
+        for (int k = s + 1; k <= 32; ++k) {
+            uint32_t v = V[d - 1][k - s - 1] ^ (V[d - 1][k - s - 1] >> s);
+            for (int j = 1; j <= s - 1; ++j)
+                if ((a >> (s - 1 - j)) & 1) v ^= V[d - 1][k - j - 1];
+            V[d - 1][k - 1] = v;
+        }
+    }
+    // Owen keys, qmc_mod.f90:130-136: hash32((seed + d*0x9E3779B9 [+0x85EBCA6B]) mod 2^32)
+    for (int d = 1; d <= 12; ++d) {
+        const uint32_t base = (uint32_t)(int64_t)seed + (uint32_t)d * 0x9E3779B9u;
+        key[0][d - 1] = hash32(base);
+        key[1][d - 1] = hash32(base + 0x85EBCA6Bu);
+    }
+}
+
+// sobol_code, qmc_mod.f90:192-206: XOR of V_d(k) over the set bits k of
+// idx; bits above 32 carry no direction number.
+uint32_t Qmc::sobol_code(int64_t idx, int d) const {
+    uint32_t code = 0;
+    uint64_t ii = (uint64_t)idx;
+    int k = 1;
+    while (ii != 0 && k <= 32) {
+        if (ii & 1u) code ^= V[d - 1][k - 1];
+        ii >>= 1;
+        ++k;
+    }
+    return code;
+}
+
+uint32_t Qmc::scrambled(int64_t idx, int d, int stream) const {
+    return owen_scramble(sobol_code(idx, d), key[stream - 1][d - 1]);
+}
+
+// u = (code + 0.5) 2^-32, qmc_mod.f90:166.
+double Qmc::uniform(int64_t idx, int d, int stream) const {
+    return ((double)scrambled(idx, d, stream) + 0.5) * (1.0 / 4294967296.0);
+}
+
+// =========================================================================
+// energy_sampler_mod.f90
+// =========================================================================
+static void set_err(std::string* err, const char* msg) {
+    if (err) *err = msg;
+}
+
+// build_tabulated_sampler, energy_sampler_mod.f90:34-64.
+bool build_tabulated_sampler(Sampler& s, const std::vector<double>& e,
+                             const std::vector<double>& f, std::string* err) {
+    const size_t n = e.size();
+    if (n < 2 || f.size() != n) {
+        set_err(err, "energy sampler: table needs at least two matching columns");
+        return false;
+    }
+    for (double v : f)
+        if (v < 0.0) {
+            set_err(err, "energy sampler: negative spectral density");
+            return false;
+        }
+    for (size_t i = 0; i + 1 < n; ++i)
+        if (e[i + 1] <= e[i]) {
+            set_err(err, "energy sampler: energies must be strictly ascending");
+            return false;
+        }
+    s.energy = e;
+    s.density = f;
+    s.cdf.assign(n, 0.0);
+    for (size_t i = 0; i + 1 < n; ++i) {
+        const double area = 0.5 * (f[i] + f[i + 1]) * (e[i + 1] - e[i]);
+        s.cdf[i + 1] = s.cdf[i] + area;
+    }
+    const double total = s.cdf[n - 1];
+    if (total <= 0.0) {
+        set_err(err, "energy sampler: zero integrated luminosity");
+        return false;
+    }
+    s.total_integral = total;
+    for (size_t i = 0; i < n; ++i) s.cdf[i] = s.cdf[i] / total;
+    s.cdf[n - 1] = 1.0;
+    return true;
+}
+
+// linear_table_value, energy_sampler_mod.f90:336-359.
+static double linear_table_value(const std::vector<double>& e,
+                                 const std::vector<double>& f, double v) {
+    const int n = (int)e.size();
+    if (v <= e[0]) return f[0];
+    if (v >= e[n - 1]) return f[n - 1];
+    int lo = 1, hi = n;  // 1-based
+    while (hi - lo > 1) {
+        const int mid = (lo + hi) / 2;
+        if (e[mid - 1] <= v) lo = mid; else hi = mid;
+    }
+    const double fr = (v - e[lo - 1]) / (e[hi - 1] - e[lo - 1]);
+    return f[lo - 1] + fr * (f[hi - 1] - f[lo - 1]);
+}
+
+// build_tabulated_band_sampler, energy_sampler_mod.f90:66-104.
+bool build_tabulated_band_sampler(Sampler& s, const std::vector<double>& e,
+                                  const std::vector<double>& f, double emin,
+                                  double emax, std::string* err) {
+    const size_t n = e.size();
+    if (n < 2 || f.size() != n) {
+        set_err(err, "energy sampler: table needs at least two matching columns");
+        return false;
+    }
+    if (emax <= emin) {
+        set_err(err, "energy sampler: invalid requested band");
+        return false;
+    }
+    const double lo = std::max(emin, e[0]);
+    const double hi = std::min(emax, e[n - 1]);
+    if (hi <= lo) {
+        set_err(err, "energy sampler: table does not overlap requested band");
+        return false;
+    }
+    std::vector<double> ce, cf;
+    ce.push_back(lo);
+    cf.push_back(linear_table_value(e, f, lo));
+    for (size_t i = 0; i < n; ++i)
+        if (e[i] > lo && e[i] < hi) {
+            ce.push_back(e[i]);
+            cf.push_back(f[i]);
+        }
+    ce.push_back(hi);
+    cf.push_back(linear_table_value(e, f, hi));
+    return build_tabulated_sampler(s, ce, cf, err);
+}
+
+// planck_energy_shape, energy_sampler_mod.f90:277-290 (energy**3 as e*e*e).
+double planck_energy_shape(double energy, double T) {
+    const double x = energy / (KB_EV * T);
+    const double e3 = energy * energy * energy;
+    if (x <= 0.0) return 0.0;
+    if (x < 1.0e-3) return e3 / (x * (1.0 + 0.5 * x + x * x / 6.0));
+    if (x < 700.0) return e3 / (std::exp(x) - 1.0);
+    return e3 * std::exp(-x);
+}
+
+// rough_planck_integral, energy_sampler_mod.f90:321-334.
+static double rough_planck_integral(double T, double emin, double emax) {
+    const int n = 256;
+    double total = 0.0;
+    for (int i = 1; i <= n; ++i) {
+        const double e0 = emin + (emax - emin) * (double)(i - 1) / (double)n;
+        const double e1 = emin + (emax - emin) * (double)i / (double)n;
+        total = total + 0.5 * (planck_energy_shape(e0, T) + planck_energy_shape(e1, T)) * (e1 - e0);
+    }
+    return total;
+}
+
+// refine_planck_interval, energy_sampler_mod.f90:159-185 (depth-first, left
+// half first, so the knots come out in ascending order).
+static bool refine_planck_interval(double T, double e0, double e1, double f0,
+                                   double f1, double tol, double scale,
+                                   double span, int depth,
+                                   std::vector<double>& we,
+                                   std::vector<double>& wf) {
+    const double em = 0.5 * (e0 + e1);
+    const double fm = planck_energy_shape(em, T);
+    const double coarse = 0.5 * (f0 + f1) * (e1 - e0);
+    const double fine = 0.25 * (f0 + 2.0 * fm + f1) * (e1 - e0);
+    const double err = std::fabs(fine - coarse) / 3.0;
+    const double allowance = tol * (std::fabs(fine) + scale * (e1 - e0) / span);
+    if (err <= allowance || depth >= 50) {
+        if ((int)we.size() + 1 > MAX_PLANCK_KNOTS) return false;
+        we.push_back(e1);
+        wf.push_back(f1);
+        return true;
+    }
+    if (!refine_planck_interval(T, e0, em, f0, fm, tol, scale, span, depth + 1, we, wf)) return false;
+    return refine_planck_interval(T, em, e1, fm, f1, tol, scale, span, depth + 1, we, wf);
+}
+
+// build_planck_sampler, energy_sampler_mod.f90:106-157 (+ sort_unique :361-391).
+bool build_planck_sampler(Sampler& s, double T, double emin, double emax,
+                          double rtol, const std::vector<double>& thr,
+                          std::string* err) {
+    if (T <= 0.0 || emin < 0.0 || emax <= emin) {
+        set_err(err, "energy sampler: invalid Planck temperature or energy band");
+        return false;
+    }
+    const double tol = rtol;
+    if (tol <= 0.0) {
+        set_err(err, "energy sampler: Planck rtol must be positive");
+        return false;
+    }
+    std::vector<double> mand;
+    mand.push_back(emin);
+    for (double t : thr)
+        if (t > emin && t < emax) mand.push_back(t);
+    mand.push_back(emax);
+    // sort_unique: insertion sort then drop repeats.
+    for (size_t i = 1; i < mand.size(); ++i) {
+        const double hold = mand[i];
+        size_t j = i;
+        while (j >= 1 && mand[j - 1] > hold) {
+            mand[j] = mand[j - 1];
+            --j;
+        }
+        mand[j] = hold;
+    }
+    std::vector<double> uniq;
+    uniq.push_back(mand[0]);
+    for (size_t i = 1; i < mand.size(); ++i)
+        if (mand[i] > uniq.back()) uniq.push_back(mand[i]);
+
+    const double scale = rough_planck_integral(T, emin, emax);
+    if (scale <= 0.0) {
+        set_err(err, "energy sampler: zero Planck band luminosity");
+        return false;
+    }
+    const double span = emax - emin;
+    std::vector<double> we, wf;
+    we.push_back(uniq[0]);
+    wf.push_back(planck_energy_shape(uniq[0], T));
+    for (size_t i = 0; i + 1 < uniq.size(); ++i) {
+        if (!refine_planck_interval(T, uniq[i], uniq[i + 1],
+                                    planck_energy_shape(uniq[i], T),
+                                    planck_energy_shape(uniq[i + 1], T), tol,
+                                    scale, span, 0, we, wf)) {
+            set_err(err, "energy sampler: Planck knot limit");
+            return false;
+        }
+    }
+    return build_tabulated_sampler(s, we, wf, err);
+}
+
+// sample_energy_cdf, energy_sampler_mod.f90:187-238.
+double sample_energy_cdf(const Sampler& s, double u) {
+    const int n = (int)s.cdf.size();
+    const double target = std::min(std::max(u, 0.0), 1.0);
+    if (target <= 0.0) return s.energy[0];
+    if (target >= 1.0) return s.energy[n - 1];
+    int lo = 1, hi = n;
+    while (hi - lo > 1) {
+        const int mid = (lo + hi) / 2;
+        if (s.cdf[mid - 1] <= target) lo = mid; else hi = mid;
+    }
+    const double interval_area = s.cdf[hi - 1] - s.cdf[lo - 1];
+    if (interval_area <= 0.0) return s.energy[hi - 1];
+    const double dx = s.energy[hi - 1] - s.energy[lo - 1];
+    const double y0 = s.density[lo - 1];
+    const double y1 = s.density[hi - 1];
+    const double local_area = (target - s.cdf[lo - 1]) / interval_area * (0.5 * (y0 + y1) * dx);
+    const double slope = (y1 - y0) / dx;
+    const double slope_scale = std::max(std::max(std::fabs(y0), std::fabs(y1)), TINEST);
+    double offset;
+    if (std::fabs(slope * dx) <= 64.0 * 2.220446049250313e-16 * slope_scale) {
+        offset = (y0 > 0.0) ? local_area / y0 : 0.0;
+    } else {
+        const double disc = std::sqrt(std::max(0.0, y0 * y0 + 2.0 * slope * local_area));
+        offset = 2.0 * local_area / (y0 + disc);
+    }
+    return s.energy[lo - 1] + std::min(std::max(offset, 0.0), dx);
+}
+
+// energy_cdf_value, energy_sampler_mod.f90:240-275.
+double energy_cdf_value(const Sampler& s, double energy) {
+    const int n = (int)s.energy.size();
+    if (energy <= s.energy[0]) return 0.0;
+    if (energy >= s.energy[n - 1]) return 1.0;
+    int lo = 1, hi = n;
+    while (hi - lo > 1) {
+        const int mid = (lo + hi) / 2;
+        if (s.energy[mid - 1] <= energy) lo = mid; else hi = mid;
+    }
+    const double dx = s.energy[hi - 1] - s.energy[lo - 1];
+    const double offset = energy - s.energy[lo - 1];
+    const double y0 = s.density[lo - 1];
+    const double slope = (s.density[hi - 1] - y0) / dx;
+    const double interval_total = 0.5 * (y0 + s.density[hi - 1]) * dx;
+    const double partial = y0 * offset + 0.5 * slope * offset * offset;
+    if (interval_total > 0.0)
+        return s.cdf[lo - 1] + (s.cdf[hi - 1] - s.cdf[lo - 1]) * partial / interval_total;
+    return s.cdf[lo - 1];
+}
+
+// =========================================================================
+// photo_xsec.f90
+// =========================================================================
+// sigma_vfky96, photo_xsec.f90:46-59 (VFKY96 Eq. 1; sigma_0 in Mb).
+double sigma_vfky96(double E, double Eth, double E0, double s0, double ya,
+                    double P, double yw, double y0, double y1) {
+    if (E < Eth) return 0.0;
+    const double x = E / E0 - y0;
+    const double z = std::sqrt(x * x + y1 * y1);
+    const double Q = 5.5 - 0.5 * P;
+    const double xm1 = x - 1.0;
+    const double Fy = (xm1 * xm1 + yw * yw) * std::pow(z, -Q) * std::pow(1.0 + std::sqrt(z / ya), -P);
+    return s0 * Fy * 1.0e-18;
+}
+
+// sigma_vy95, photo_xsec.f90:69-82.
+double sigma_vy95(double E, double Eth, double E0, double s0, double ya,
+                  double P, double yw, double l) {
+    if (E < Eth) return 0.0;
+    const double y = E / E0;
+    const double Q = 5.5 + l - 0.5 * P;
+    const double ym1 = y - 1.0;
+    const double Fy = (ym1 * ym1 + yw * yw) * std::pow(y, -Q) * std::pow(1.0 + std::sqrt(y / ya), -P);
+    return s0 * Fy * 1.0e-18;
+}
+
+// sigma_hydrogenic, photo_xsec.f90:92-107 ((E_th/E)**4 by squaring).
+double sigma_hydrogenic(double E, double Eth, double Z) {
+    const double s0 = 6.30e-18 / (Z * Z);
+    if (E < Eth) return 0.0;
+    if (E > Eth) {
+        const double eps = std::sqrt(E / Eth - 1.0);
+        const double r = Eth / E;
+        const double r2 = r * r;
+        return s0 * (r2 * r2) * std::exp(4.0 - 4.0 * std::atan(eps) / eps) /
+               (1.0 - std::exp(-2.0 * PI / eps));
+    }
+    return s0;
+}
+
+double sigma_HI(double E) { return sigma_hydrogenic(E, ETH_HI, 1.0); }       // :110-113
+double sigma_HeI(double E) {                                                 // :116-120
+    return sigma_vfky96(E, ETH_HEI, 1.361e1, 9.492e2, 1.469, 3.188, 2.039, 4.434e-1, 2.136);
+}
+double sigma_HeII(double E) { return sigma_hydrogenic(E, ETH_HEII, 2.0); }   // :123-126
+
+// =========================================================================
+// recomb_mod.f90
+// =========================================================================
+static double rr_badnell(double T, double A, double B, double T0, double T1,
+                         double Cc, double T2) {  // recomb_mod.f90:124-130
+    const double bp = B + Cc * std::exp(-T2 / T);
+    const double tt = std::sqrt(T / T0);
+    return A / (tt * std::pow(1.0 + tt, 1.0 - bp) * std::pow(1.0 + std::sqrt(T / T1), 1.0 + bp));
+}
+static double dr_HeII_badnell(double T) {  // recomb_mod.f90:132-137
+    return std::pow(T, -1.5) * (1.417e-3 * std::exp(-4.633e5 / T) +
+                                2.235e-4 * std::exp(-5.532e5 / T) -
+                                2.185e-5 * std::exp(-8.887e5 / T));
+}
+static double rr_mao(double T, double a0, double b0, double c0, double a1,
+                     double b1, double a2, double b2) {  // recomb_mod.f90:145-151
+    const double te = T * (KBOLTZ_CGS / EV2ERG);
+    return a0 * 1.0e-10 * std::pow(te, -b0 - c0 * std::log(te)) *
+           (1.0 + a2 * std::pow(te, -b2)) / (1.0 + a1 * std::pow(te, -b1));
+}
+double alpha1_HII(double T) {  // recomb_mod.f90:188-192
+    return rr_mao(T, 1.87007e-2, 1.29077, -2.17465e-3, 1.29189e1, 8.05060e-1, 8.44399e-2, 5.93940e-4);
+}
+double alpha1_HeIII(double T) {  // :194-198
+    return rr_mao(T, 2.61525e-1, 1.39527, -3.22079e-4, 6.40708e1, 8.97582e-1, 5.01551e-1, 1.21533e-3);
+}
+double alpha1_HeII(double T) {  // :200-204
+    return rr_mao(T, 3.26862e-3, 6.97361e-1, 3.14907e-4, 5.76341e1, 1.18534, 2.58417e1, 9.90134e-1);
+}
+// Hui & Gnedin fits, recomb_mod.f90:209-251.
+static double hg_aA_HII(double T) {
+    const double lam = 2.0 * 157807.0 / T;
+    return 1.269e-13 * std::pow(lam, 1.503) / std::pow(1.0 + std::pow(lam / 0.522, 0.470), 1.923);
+}
+static double hg_aB_HII(double T) {
+    const double lam = 2.0 * 157807.0 / T;
+    return 2.753e-14 * std::pow(lam, 1.500) / std::pow(1.0 + std::pow(lam / 2.740, 0.407), 2.242);
+}
+static double hg_aA_HeII(double T) { return 3.000e-14 * std::pow(2.0 * 285335.0 / T, 0.654); }
+static double hg_aB_HeII(double T) { return 1.260e-14 * std::pow(2.0 * 285335.0 / T, 0.750); }
+static double hg_aA_HeIII(double T) {
+    const double lam = 2.0 * 631515.0 / T;
+    return 2.0 * 1.269e-13 * std::pow(lam, 1.503) / std::pow(1.0 + std::pow(lam / 0.522, 0.470), 1.923);
+}
+static double hg_aB_HeIII(double T) {
+    const double lam = 2.0 * 631515.0 / T;
+    return 2.0 * 2.753e-14 * std::pow(lam, 1.500) / std::pow(1.0 + std::pow(lam / 2.740, 0.407), 2.242);
+}
+// Public dispatch, recomb_mod.f90:47-118.
+double alphaA_HII(const RateModel& m, double T) {
+    return m.recomb == RECOMB_HUI_GNEDIN ? hg_aA_HII(T)
+                                         : rr_badnell(T, 8.318e-11, 0.7472, 2.965, 7.001e5, 0.0, 0.0);
+}
+double alphaB_HII(const RateModel& m, double T) {
+    return m.recomb == RECOMB_HUI_GNEDIN ? hg_aB_HII(T) : alphaA_HII(m, T) - alpha1_HII(T);
+}
+double alphaA_HeII(const RateModel& m, double T) {
+    return m.recomb == RECOMB_HUI_GNEDIN
+               ? hg_aA_HeII(T)
+               : rr_badnell(T, 5.235e-11, 0.6988, 7.301, 4.475e6, 0.0829, 1.682e5) + dr_HeII_badnell(T);
+}
+double alphaB_HeII(const RateModel& m, double T) {
+    return m.recomb == RECOMB_HUI_GNEDIN ? hg_aB_HeII(T) : alphaA_HeII(m, T) - alpha1_HeII(T);
+}
+double alphaA_HeIII(const RateModel& m, double T) {
+    return m.recomb == RECOMB_HUI_GNEDIN ? hg_aA_HeIII(T)
+                                         : rr_badnell(T, 1.818e-10, 0.7492, 1.017e1, 2.786e6, 0.0, 0.0);
+}
+double alphaB_HeIII(const RateModel& m, double T) {
+    return m.recomb == RECOMB_HUI_GNEDIN ? hg_aB_HeIII(T) : alphaA_HeIII(m, T) - alpha1_HeIII(T);
+}
+// Voronov (1997), recomb_mod.f90:256-261.
+double voronov(double T, double dE, double P, double A, double X, double K) {
+    const double U = dE * EV2ERG / (KBOLTZ_CGS * T);
+    return A * (1.0 + P * std::sqrt(U)) * std::pow(U, K) * std::exp(-U) / (X + U);
+}
+// Dere hybrid ratio table, recomb_mod.f90:288-311.
+double ci_dere_ratio(const RateModel& m, int Z, int stage) {
+    if (m.ci != CI_DERE_HYBRID) return 1.0;
+    double tab[4] = {1, 1, 1, 1};
+    int n = 0;
+    switch (Z) {
+        case 1: tab[0] = 0.9063; n = 1; break;
+        case 2: tab[0] = 1.0389; tab[1] = 1.0686; n = 2; break;
+        case 6: tab[0] = 1.0499; tab[1] = 0.913; tab[2] = 1.0377; n = 3; break;
+        case 7: tab[0] = 1.0421; tab[1] = 1.1966; n = 2; break;
+        case 8: tab[0] = 1.041; tab[1] = 1.1181; n = 2; break;
+        case 10: tab[0] = 0.8089; tab[1] = 1.1395; n = 2; break;
+        case 12: tab[0] = 0.3793; tab[1] = 0.9857; n = 2; break;
+        case 14: tab[0] = 0.7328; tab[1] = 0.8798; tab[2] = 0.4492; tab[3] = 0.8221; n = 4; break;
+        case 16: tab[0] = 1.3572; tab[1] = 0.8925; tab[2] = 0.8119; n = 3; break;
+        case 17: tab[0] = 0.5412; tab[1] = 0.8428; tab[2] = 0.9237; tab[3] = 0.819; n = 4; break;
+        case 18: tab[0] = 0.9242; tab[1] = 0.8644; tab[2] = 0.9752; n = 3; break;
+        case 20: tab[0] = 0.7652; tab[1] = 1.1668; tab[2] = 1.0422; tab[3] = 0.8705; n = 4; break;
+        case 26: tab[0] = 0.9904; tab[1] = 1.0568; tab[2] = 1.824; n = 3; break;
+    }
+    if (stage >= 1 && stage <= n) return tab[stage - 1];
+    return 1.0;
+}
+double ci_HI(const RateModel& m, double T) {  // recomb_mod.f90:263-267
+    return voronov(T, 13.6, 0.0, 2.91e-8, 0.232, 0.39) * ci_dere_ratio(m, 1, 1);
+}
+double ci_HeI(const RateModel& m, double T) {  // :269-273
+    return voronov(T, 24.6, 0.0, 1.75e-8, 0.180, 0.35) * ci_dere_ratio(m, 2, 1);
+}
+double ci_HeII(const RateModel& m, double T) {  // :275-279
+    return voronov(T, 54.4, 1.0, 2.05e-9, 0.265, 0.25) * ci_dere_ratio(m, 2, 2);
+}
+
+// =========================================================================
+// namelist (setup.f90:23-35) and parameter defaults (define.f90:189-861)
+// =========================================================================
+Par::Par() {
+    for (int i = 0; i < MAX_SRC; ++i) {
+        src_tstar[i] = -999.0;
+        src_lum[i] = -999.0;
+        src_x[i] = src_y[i] = src_z[i] = 0.0;
+    }
+}
+
+static std::string lower(std::string s) {
+    for (auto& c : s) c = (char)std::tolower((unsigned char)c);
+    return s;
+}
+static std::string trim(const std::string& s) {
+    size_t a = s.find_first_not_of(" \t\r\n");
+    if (a == std::string::npos) return "";
+    size_t b = s.find_last_not_of(" \t\r\n");
+    return s.substr(a, b - a + 1);
+}
+static bool to_bool(const std::string& v) {
+    std::string s = lower(trim(v));
+    return s == ".true." || s == "t" || s == "true" || s == ".t.";
+}
+static double to_dbl(const std::string& v) {
+    std::string s = trim(v);
+    for (auto& c : s)
+        if (c == 'd' || c == 'D') c = 'e';
+    return std::strtod(s.c_str(), nullptr);
+}
+static std::string to_str(const std::string& v) {
+    std::string s = trim(v);
+    if (s.size() >= 2 && (s[0] == '\'' || s[0] == '"')) s = s.substr(1, s.size() - 2);
+    return trim(s);
+}
+
+bool parse_namelist(const std::string& text, Par& p, std::string* err) {
+    // Strip '!' comments outside quotes, then split on commas/newlines into
+    // "par%key[(i)] = value[, value...]" assignments.
+    std::string clean;
+    bool inq = false;
+    char q = 0;
+    for (size_t i = 0; i < text.size(); ++i) {
+        char c = text[i];
+        if (inq) {
+            if (c == q) inq = false;
+            clean += c;
+            continue;
+        }
+        if (c == '\'' || c == '"') {
+            inq = true;
+            q = c;
+            clean += c;
+            continue;
+        }
+        if (c == '!') {
+            while (i < text.size() && text[i] != '\n') ++i;
+            clean += '\n';
+            continue;
+        }
+        clean += c;
+    }
+    // tokenise assignments: find "par%"
+    std::map<std::string, std::vector<std::string>> kv;
+    size_t pos = 0;
+    std::string lc = lower(clean);
+    while ((pos = lc.find("par%", pos)) != std::string::npos) {
+        size_t eq = lc.find('=', pos);
+        if (eq == std::string::npos) break;
+        std::string key = trim(lc.substr(pos + 4, eq - pos - 4));
+        size_t next = lc.find("par%", eq);
+        size_t endslash = std::string::npos;
+        // value ends at next par% or a terminating '/' outside quotes
+        std::string raw = clean.substr(eq + 1, (next == std::string::npos ? clean.size() : next) - eq - 1);
+        {
+            bool iq = false;
+            char qq = 0;
+            for (size_t k = 0; k < raw.size(); ++k) {
+                char c = raw[k];
+                if (iq) {
+                    if (c == qq) iq = false;
+                    continue;
+                }
+                if (c == '\'' || c == '"') {
+                    iq = true;
+                    qq = c;
+                    continue;
+                }
+                if (c == '/') {
+                    endslash = k;
+                    break;
+                }
+            }
+        }
+        if (endslash != std::string::npos) raw = raw.substr(0, endslash);
+        std::vector<std::string> vals;
+        {
+            std::string cur;
+            bool iq = false;
+            char qq = 0;
+            for (char c : raw) {
+                if (iq) {
+                    cur += c;
+                    if (c == qq) iq = false;
+                    continue;
+                }
+                if (c == '\'' || c == '"') {
+                    iq = true;
+                    qq = c;
+                    cur += c;
+                    continue;
+                }
+                if (c == ',' || c == '\n') {
+                    if (!trim(cur).empty()) vals.push_back(trim(cur));
+                    cur.clear();
+                    continue;
+                }
+                cur += c;
+            }
+            if (!trim(cur).empty()) vals.push_back(trim(cur));
+        }
+        int index = 1;
+        size_t lp = key.find('(');
+        if (lp != std::string::npos) {
+            index = std::atoi(key.substr(lp + 1).c_str());
+            key = trim(key.substr(0, lp));
+        }
+        auto& slot = kv[key];
+        if ((int)slot.size() < index - 1 + (int)vals.size()) slot.resize(index - 1 + vals.size());
+        for (size_t k = 0; k < vals.size(); ++k) slot[index - 1 + k] = vals[k];
+        pos = eq;
+    }
+    for (auto& it : kv) {
+        const std::string& k = it.first;
+        const auto& v = it.second;
+        if (v.empty()) continue;
+        const std::string& s = v[0];
+#define D(name) else if (k == #name) p.name = to_dbl(s)
+#define I(name) else if (k == #name) p.name = (int)std::llround(to_dbl(s))
+#define B(name) else if (k == #name) p.name = to_bool(s)
+#define S(name) else if (k == #name) p.name = to_str(s)
+        if (k == "no_photons") p.nphotons = (int64_t)to_dbl(s);
+        else if (k == "nphotons") p.nphotons = (int64_t)to_dbl(s);
+        S(launch_sequence); I(qmc_seed); D(source_cdf_tol); D(luminosity); D(tstar);
+        I(nnu_ion); D(eion_min); D(eion_max); B(add_fuv); D(efuv_min); I(nnu_fuv);
+        B(ion_align_edges); S(grid_type); S(car_walk); S(amr_file);
+        I(nx); I(ny); I(nz); D(xmax); D(ymax); D(zmax); D(rmax); D(rmin); D(nH_const);
+        S(distance_unit); S(source_geometry); D(xs_point); D(ys_point); D(zs_point);
+        I(nsource); D(xHI_init); D(xHeI_init); D(xHeII_init); D(He_abund);
+        I(gas_niter); D(gas_tol); D(te_fixed); D(ion_relax); S(case_ab); S(ci_model);
+        S(recomb_model); S(cooling_model); S(charge_exchange); S(conv_crit);
+        B(solve_te); D(te_min); D(te_max); D(gas_tol_te); B(use_metals);
+        B(diffuse_field); B(use_sec_ion); B(ion_add_dust); B(ion_dust_scatter);
+        S(dust_density_law); D(cext_dust); S(data_dir); S(atomic_dir); S(ion_dust_kext);
+        else if (k == "dgr") p.DGR = to_dbl(s);
+        else if (k == "he_abund") p.He_abund = to_dbl(s);
+        else if (k == "nh_const") p.nH_const = to_dbl(s);
+        else if (k == "xhi_init") p.xHI_init = to_dbl(s);
+        else if (k == "xhei_init") p.xHeI_init = to_dbl(s);
+        else if (k == "xheii_init") p.xHeII_init = to_dbl(s);
+        else if (k == "src_tstar" || k == "src_lum" || k == "src_x" || k == "src_y" || k == "src_z") {
+            double* arr = k == "src_tstar" ? p.src_tstar : k == "src_lum" ? p.src_lum
+                        : k == "src_x" ? p.src_x : k == "src_y" ? p.src_y : p.src_z;
+            for (size_t j = 0; j < v.size() && j < (size_t)MAX_SRC; ++j)
+                if (!v[j].empty()) arr[j] = to_dbl(v[j]);
+        } else {
+            // keys outside the hot path are accepted and ignored by the oracle
+        }
+#undef D
+#undef I
+#undef B
+#undef S
+    }
+    // Derived values, setup.f90:72 (nphotons) and :586-595 (distance unit).
+    std::string du = lower(p.distance_unit);
+    if (du == "kpc") p.distance2cm = KPC2CM;
+    else if (du == "pc") p.distance2cm = PC2CM;
+    else if (du == "au") p.distance2cm = AU2CM;
+    else if (du == "cm") p.distance2cm = 1.0;
+    if (p.diffuse_field && p.case_ab != "A") p.case_ab = "A";  // setup.f90:580-583
+    if (p.grid_type == "uniform") p.grid_type = "car";
+    (void)err;
+    return true;
+}
+
+// =========================================================================
+// ion_band_mod.f90
+// =========================================================================
+// build_aligned_edges, ion_band_mod.f90:1053-1214.
+bool build_aligned_edges(std::vector<double>& eedge, int nfuv, int nnu,
+                         double lo, double hi, const std::vector<double>& meth,
+                         std::string* err) {
+    const int nion = nnu - nfuv;
+    const double MERGE_TOL = 0.01;
+    std::vector<double> cand;
+    std::vector<int> cpri;
+    auto add = [&](double E, int pri) {
+        if (E > lo && E < hi) {
+            cand.push_back(E);
+            cpri.push_back(pri);
+        }
+    };
+    add(ETH_HI, 1);
+    add(ETH_HEI, 1);
+    add(ETH_HEII, 1);
+    for (double m : meth)
+        if (m > 0.0) add(m, 0);
+    const int ncand = (int)cand.size();
+    for (int i = 1; i < ncand; ++i) {
+        double tmp = cand[i];
+        int itmp = cpri[i];
+        int j = i - 1;
+        while (j >= 0 && cand[j] > tmp) {
+            cand[j + 1] = cand[j];
+            cpri[j + 1] = cpri[j];
+            --j;
+        }
+        cand[j + 1] = tmp;
+        cpri[j + 1] = itmp;
+    }
+    std::vector<double> thr;
+    std::vector<int> tpri;
+    for (int i = 0; i < ncand; ++i) {
+        bool dup = false;
+        if (!thr.empty() && std::fabs(std::log(cand[i] / thr.back())) < MERGE_TOL) dup = true;
+        if (dup) {
+            if (cpri[i] > tpri.back()) {
+                thr.back() = cand[i];
+                tpri.back() = cpri[i];
+            }
+        } else {
+            thr.push_back(cand[i]);
+            tpri.push_back(cpri[i]);
+        }
+    }
+    while ((int)thr.size() + 1 > nion) {
+        int best = -1;
+        double frac = 1.0e30;
+        const int nthr = (int)thr.size();
+        for (int i = 0; i < nthr; ++i) {
+            if (tpri[i] != 0) continue;
+            double tmp = (i == 0) ? std::log(thr[i] / lo) : std::log(thr[i] / thr[i - 1]);
+            if (i == nthr - 1) tmp = std::min(tmp, std::log(hi / thr[i]));
+            else tmp = std::min(tmp, std::log(thr[i + 1] / thr[i]));
+            if (tmp < frac) {
+                frac = tmp;
+                best = i;
+            }
+        }
+        if (best < 0) break;
+        thr.erase(thr.begin() + best);
+        tpri.erase(tpri.begin() + best);
+    }
+    const int nthr = (int)thr.size();
+    std::vector<double> points;
+    points.push_back(lo);
+    for (double t : thr) points.push_back(t);
+    points.push_back(hi);
+    const int nseg = nthr + 1;
+    if (nion < nseg) {
+        set_err(err, "ion_align_edges: nnu_ion cannot fit the H/He thresholds");
+        return false;
+    }
+    std::vector<double> w(nseg);
+    double wsum = 0.0;
+    for (int j = 0; j < nseg; ++j) {
+        w[j] = std::log(points[j + 1]) - std::log(points[j]);
+        wsum = wsum + w[j];
+    }
+    std::vector<int> nb(nseg);
+    int ntot = 0;
+    for (int j = 0; j < nseg; ++j) {
+        nb[j] = std::max(1, (int)((double)nion * w[j] / wsum));
+        ntot += nb[j];
+    }
+    int r = nion - ntot;
+    while (r > 0) {
+        int best = 0;
+        double frac = -1.0;
+        for (int j = 0; j < nseg; ++j) {
+            double tmp = (double)nion * w[j] / wsum - (double)nb[j];
+            if (tmp > frac) {
+                frac = tmp;
+                best = j;
+            }
+        }
+        nb[best] += 1;
+        r -= 1;
+    }
+    while (r < 0) {
+        int best = -1;
+        double frac = -1.0e30;
+        for (int j = 0; j < nseg; ++j) {
+            if (nb[j] <= 1) continue;
+            double tmp = (double)nb[j] - (double)nion * w[j] / wsum;
+            if (tmp > frac) {
+                frac = tmp;
+                best = j;
+            }
+        }
+        if (best < 0) break;
+        nb[best] -= 1;
+        r += 1;
+    }
+    int off = nfuv;  // 0-based index of points(1)
+    eedge[off] = points[0];
+    int ipt = off;
+    for (int j = 0; j < nseg; ++j)
+        for (int ib = 1; ib <= nb[j]; ++ib) {
+            ++ipt;
+            eedge[ipt] = std::exp(std::log(points[j]) +
+                                  (std::log(points[j + 1]) - std::log(points[j])) * (double)ib / (double)nb[j]);
+        }
+    return true;
+}
+
+// ion_bin_of, ion_band_mod.f90:624-646 (returns a 0-based bin).
+int ion_bin_of(const Band& b, double eph, bool include_fuv) {
+    int lo = 1, hi = b.nnu_band;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) / 2;
+        if (b.eedge[mid - 1] <= eph) lo = mid; else hi = mid - 1;
+    }
+    int r = include_fuv ? std::min(std::max(lo, 1), b.nnu_band)
+                        : std::min(std::max(lo, b.nfuv_band + 1), b.nnu_band);
+    return r - 1;
+}
+
+// ion_setup (ion_band_mod.f90:122-258) restricted to internal point
+// sources with Planck spectra (the hot-path configurations), plus
+// setup_continuous_source_sampler / build_point_source_sampler
+// (:275-353, :437-495) and ion_qmc_ndim (:654-663).
+bool band_setup(const Par& p, Band& b, std::string* err) {
+    int nfuv = 0;
+    if (p.add_fuv) {
+        if (p.efuv_min >= p.eion_min) {
+            set_err(err, "add_fuv requires efuv_min < eion_min");
+            return false;
+        }
+        nfuv = p.nnu_fuv;
+    }
+    const int nnu = p.nnu_ion + nfuv;
+    b.nnu_band = nnu;
+    b.nfuv_band = nfuv;
+    b.eedge.assign(nnu + 1, 0.0);
+    const double lo = std::log(p.eion_min), hi = std::log(p.eion_max);
+    for (int i = 1; i <= nfuv; ++i)
+        b.eedge[i - 1] = std::exp(std::log(p.efuv_min) + (lo - std::log(p.efuv_min)) * (double)(i - 1) / (double)nfuv);
+    std::vector<double> meth;  // metal thresholds: none on the H/He path
+    if (p.ion_align_edges) {
+        if (!build_aligned_edges(b.eedge, nfuv, nnu, p.eion_min, p.eion_max, meth, err)) return false;
+    } else {
+        for (int i = nfuv + 1; i <= nnu + 1; ++i)
+            b.eedge[i - 1] = std::exp(lo + (hi - lo) * (double)(i - 1 - nfuv) / (double)(nnu - nfuv));
+    }
+    if (p.source_geometry != "point") {
+        set_err(err, "oracle: only point sources are restated");
+        return false;
+    }
+    b.ncomp = p.nsource;
+    b.multi_src = b.ncomp >= 2;
+    b.qmc_ndim = b.multi_src ? 7 : 3;
+    const double elo = p.add_fuv ? p.efuv_min : p.eion_min;
+    std::vector<double> knots = {ETH_HI, ETH_HEI, ETH_HEII};
+    if (p.add_fuv) knots.push_back(p.eion_min);
+    b.samplers.resize(b.ncomp);
+    std::vector<double> band_L(b.ncomp);
+    for (int ic = 0; ic < b.ncomp; ++ic) {
+        const double tst = b.multi_src ? p.src_tstar[ic] : p.tstar;
+        const double scale = b.multi_src ? p.src_lum[ic] : p.luminosity;
+        if (tst <= 0.0) {
+            set_err(err, "oracle: point source needs a Planck temperature");
+            return false;
+        }
+        if (!build_planck_sampler(b.samplers[ic], tst, elo, p.eion_max, p.source_cdf_tol, knots, err)) return false;
+        // source_band_luminosity, ion_band_mod.f90:379-399
+        const double f_ion = 1.0 - energy_cdf_value(b.samplers[ic], p.eion_min);
+        if (f_ion <= 0.0) {
+            set_err(err, "source has no ionizing-band luminosity");
+            return false;
+        }
+        band_L[ic] = scale / f_ion;
+    }
+    b.ion_Ltot = 0.0;
+    for (double L : band_L) b.ion_Ltot += L;
+    if (b.multi_src) {
+        b.comp_kind.resize(b.ncomp);
+        b.src_cdf.resize(b.ncomp);
+        for (int ic = 0; ic < b.ncomp; ++ic) b.comp_kind[ic] = ic + 1;
+        b.src_cdf[0] = band_L[0];
+        for (int ic = 1; ic < b.ncomp; ++ic) b.src_cdf[ic] = b.src_cdf[ic - 1] + band_L[ic];
+        const double last = b.src_cdf[b.ncomp - 1];
+        for (auto& c : b.src_cdf) c = c / last;
+    }
+    return true;
+}
+
+// =========================================================================
+// Tallies
+// =========================================================================
+void Tally::reset(int nleaf, int nnu) {
+    hhe.assign((size_t)6 * nleaf, 0.0);
+    jt.assign((size_t)nnu * nleaf, 0.0);
+    emitted = absorbed = escaped = 0;
+    direct_segments = scattered_segments = 0;
+}
+void Tally::add(const Tally& o) {
+    for (size_t i = 0; i < hhe.size(); ++i) hhe[i] += o.hhe[i];
+    for (size_t i = 0; i < jt.size(); ++i) jt[i] += o.jt[i];
+    emitted += o.emitted;
+    absorbed += o.absorbed;
+    escaped += o.escaped;
+    direct_segments += o.direct_segments;
+    scattered_segments += o.scattered_segments;
+}
+
+// =========================================================================
+// Simulation: setup (setup.f90, grid_mod_amr.f90:64-147,163-200,
+// gas_state_mod.f90:41-90, ion_band_mod.f90:122-258)
+// =========================================================================
+bool Sim::setup(const std::string& nl, std::string* err) {
+    if (!parse_namelist(nl, par, err)) return false;
+    rm.recomb = par.recomb_model == "hui_gnedin" ? RECOMB_HUI_GNEDIN : RECOMB_BADNELL_MILNE;
+    rm.ci = par.ci_model == "dere_hybrid" ? CI_DERE_HYBRID : CI_VORONOV;
+    qmc.setup(par.qmc_seed);
+    if (par.grid_type != "car") {
+        set_err(err, "oracle: only the namelist car grid is restated");
+        return false;
+    }
+    if (par.use_metals || par.diffuse_field || par.ion_add_dust || par.solve_te || par.use_sec_ion || par.add_fuv) {
+        set_err(err, "oracle: metals/diffuse/dust/thermal/sec_ion/fuv not restated yet");
+        return false;
+    }
+    // namelist car grid, grid_mod_amr.f90:64-133,193-198 and octree_mod.f90:648-674
+    grid.car = true;
+    grid.nx = par.nx;
+    grid.ny = par.ny;
+    grid.nz = par.nz;
+    grid.nleaf = par.nx * par.ny * par.nz;
+    grid.xmin = -par.xmax; grid.xmax = par.xmax;
+    grid.ymin = -par.ymax; grid.ymax = par.ymax;
+    grid.zmin = -par.zmax; grid.zmax = par.zmax;
+    grid.dcell = (grid.xmax - grid.xmin) / (double)grid.nx;
+    const int nleaf = grid.nleaf;
+    const double dcx = 2.0 * par.xmax / (double)par.nx;
+    const double dcy = 2.0 * par.ymax / (double)par.ny;
+    const double dcz = 2.0 * par.zmax / (double)par.nz;
+    st.nH.assign(nleaf, 1.0);
+    int il = 0;
+    for (int iz = 0; iz < par.nz; ++iz)
+        for (int iy = 0; iy < par.ny; ++iy)
+            for (int ix = 0; ix < par.nx; ++ix, ++il) {
+                const double xl = -par.xmax + ((double)ix + 0.5) * dcx;
+                const double yl = -par.ymax + ((double)iy + 0.5) * dcy;
+                const double zl = -par.zmax + ((double)iz + 0.5) * dcz;
+                if (par.nH_const >= 0.0) st.nH[il] = par.nH_const;
+                if (par.rmax > 0.0 || par.rmin > 0.0) {
+                    const double rho = std::sqrt(xl * xl + yl * yl + zl * zl);
+                    if (par.rmax > 0.0 && rho > par.rmax) st.nH[il] = 0.0;
+                    if (par.rmin > 0.0 && rho < par.rmin) st.nH[il] = 0.0;
+                }
+            }
+    // gas_state_setup, gas_state_mod.f90:58-77
+    st.xHI.assign(nleaf, par.xHI_init);
+    st.xHeI.assign(nleaf, par.xHeI_init);
+    st.xHeII.assign(nleaf, par.xHeII_init);
+    st.ne.resize(nleaf);
+    st.Te.assign(nleaf, par.te_fixed);
+    for (int i = 0; i < nleaf; ++i)
+        st.ne[i] = st.nH[i] * ((1.0 - st.xHI[i]) +
+                               par.He_abund * (st.xHeII[i] + 2.0 * std::max(0.0, 1.0 - st.xHeI[i] - st.xHeII[i])));
+    if (!band_setup(par, band, err)) return false;
+    if (par.launch_sequence != "sobol") {
+        set_err(err, "oracle: only the sobol launch sequence is restated");
+        return false;
+    }
+    tally.reset(nleaf, band.nnu_band);
+    gamma_HI.assign(nleaf, 0.0); gamma_HeI.assign(nleaf, 0.0); gamma_HeII.assign(nleaf, 0.0);
+    heat_HI.assign(nleaf, 0.0); heat_HeI.assign(nleaf, 0.0); heat_HeII.assign(nleaf, 0.0);
+    return true;
+}
+
+// gen_ion_photon_qmc, ion_band_mod.f90:1880-1935, with emit_point_qmc
+// (:2232-2247) and build_ion_packet_physics (ion_packet_mod.f90:21-53).
+void Sim::gen_photon_qmc(int64_t ip, Photon& ph) const {
+    double u[12];
+    for (int d = 1; d <= band.qmc_ndim; ++d) u[d - 1] = qmc.uniform(ip, d, 1);
+    double e;
+    double umu, uphi, xs, ys, zs;
+    int ic = 0;
+    if (!band.multi_src) {
+        xs = par.xs_point; ys = par.ys_point; zs = par.zs_point;
+        umu = u[1]; uphi = u[2];
+        e = sample_energy_cdf(band.samplers[0], u[0]);
+    } else {
+        ic = band.ncomp - 1;
+        for (int i = 0; i < band.ncomp; ++i)
+            if (u[0] <= band.src_cdf[i]) { ic = i; break; }
+        const int ik = band.comp_kind[ic];
+        xs = par.src_x[ik - 1]; ys = par.src_y[ik - 1]; zs = par.src_z[ik - 1];
+        umu = u[2]; uphi = u[3];
+        e = sample_energy_cdf(band.samplers[ic], u[1]);
+    }
+    ph.x = xs; ph.y = ys; ph.z = zs;
+    const double cost = 2.0 * umu - 1.0;
+    const double sint = std::sqrt(1.0 - cost * cost);
+    const double phi = TWOPI * uphi;
+    ph.kx = sint * std::cos(phi);
+    ph.ky = sint * std::sin(phi);
+    ph.kz = cost;
+    ph.inu = ion_bin_of(band, e, true);
+    ph.wgt = 1.0;
+    ph.Lpacket = band.ion_Ltot / (double)par.nphotons;
+    ph.E = e;
+    ph.sHI = sigma_HI(e);
+    ph.sHeI = sigma_HeI(e);
+    ph.sHeII = sigma_HeII(e);
+}
+
+// score_ion_path, ion_score_mod.f90:137-231 (H/He part).
+static inline void score(const Sim& s, const Photon& ph, int il, double path_lum, Tally& t) {
+    if (path_lum == 0.0) return;
+    t.jt[(size_t)s.band.nnu_band * il + ph.inu] += path_lum;
+    t.direct_segments += 1;
+    const double energy = ph.E;
+    double c[6];
+    c[0] = ph.sHI / (energy * EV2ERG);
+    c[1] = ph.sHeI / (energy * EV2ERG);
+    c[2] = ph.sHeII / (energy * EV2ERG);
+    c[3] = ph.sHI * std::max(1.0 - ETH_HI / energy, 0.0);
+    c[4] = ph.sHeI * std::max(1.0 - ETH_HEI / energy, 0.0);
+    c[5] = ph.sHeII * std::max(1.0 - ETH_HEII / energy, 0.0);
+    double* h = &t.hhe[(size_t)6 * il];
+    for (int k = 0; k < 6; ++k) h[k] = h[k] + path_lum * c[k];
+}
+
+// ion_packet_opacity, ion_packet_mod.f90:55-87 (gas part).
+static inline double opacity(const Sim& s, const Photon& ph, int il) {
+    return s.st.nH[il] *
+           (s.st.xHI[il] * ph.sHI + s.par.He_abund * (s.st.xHeI[il] * ph.sHeI + s.st.xHeII[il] * ph.sHeII)) *
+           s.par.distance2cm;
+}
+
+// dda_init (raytrace_amr.f90:495-532) + raytrace_ion_to_edge_car (:534-592).
+void Sim::walk_edge_car(const Photon& ph, Tally& t, double* tau_edge) const {
+    const double d = grid.dcell;
+    const double pos[3] = {ph.x, ph.y, ph.z};
+    const double kk[3] = {ph.kx, ph.ky, ph.kz};
+    const double org[3] = {grid.xmin, grid.ymin, grid.zmin};
+    const int n[3] = {grid.nx, grid.ny, grid.nz};
+    int idx[3];
+    for (int a = 0; a < 3; ++a) idx[a] = std::min(std::max((int)((pos[a] - org[a]) / d), 0), n[a] - 1);
+    int stp[3];
+    double tmax[3], tdel[3];
+    for (int a = 0; a < 3; ++a) {
+        if (kk[a] > 0.0) {
+            stp[a] = 1;
+            tmax[a] = (org[a] + (double)(idx[a] + 1) * d - pos[a]) / kk[a];
+            tdel[a] = d / kk[a];
+        } else if (kk[a] < 0.0) {
+            stp[a] = -1;
+            tmax[a] = (org[a] + (double)idx[a] * d - pos[a]) / kk[a];
+            tdel[a] = -d / kk[a];
+        } else {
+            stp[a] = 0;
+            tmax[a] = HUGEST;
+            tdel[a] = HUGEST;
+        }
+    }
+    const double wl = ph.wgt * ph.Lpacket;
+    double expo = 1.0, tau = 0.0, t_cur = 0.0;
+    int nstep = 0;
+    for (;;) {
+        if (++nstep > MAX_WALK_STEPS) break;
+        const int il = idx[0] + n[0] * (idx[1] + n[1] * idx[2]);
+        int a = 0;
+        if (tmax[1] < tmax[a]) a = 1;
+        if (tmax[2] < tmax[a]) a = 2;
+        const double seg = tmax[a] - t_cur;
+        const double kap = opacity(*this, ph, il);
+        if (kap * seg > 0.0) {
+            const double expo_out = expo * std::exp(-kap * seg);
+            score(*this, ph, il, wl * (expo - expo_out) / kap, t);
+            expo = expo_out;
+        } else {
+            score(*this, ph, il, wl * expo * seg, t);
+        }
+        tau = tau + kap * seg;
+        if (tau >= TAU_HUGE) break;
+        t_cur = tmax[a];
+        tmax[a] = tmax[a] + tdel[a];
+        idx[a] += stp[a];
+        if (idx[a] < 0 || idx[a] >= n[a]) break;
+    }
+    *tau_edge = tau;
+}
+
+// Geometry-only DDA (no tau cut): the leaf sequence of one ray, 0-based.
+int Sim::walk_leaves_car(double x, double y, double z, double kx, double ky,
+                         double kz, int max_steps, int32_t* out) const {
+    const double d = grid.dcell;
+    const double pos[3] = {x, y, z};
+    const double kk[3] = {kx, ky, kz};
+    const double org[3] = {grid.xmin, grid.ymin, grid.zmin};
+    const int n[3] = {grid.nx, grid.ny, grid.nz};
+    int idx[3], stp[3];
+    double tmax[3], tdel[3];
+    for (int a = 0; a < 3; ++a) idx[a] = std::min(std::max((int)((pos[a] - org[a]) / d), 0), n[a] - 1);
+    for (int a = 0; a < 3; ++a) {
+        if (kk[a] > 0.0) {
+            stp[a] = 1; tmax[a] = (org[a] + (double)(idx[a] + 1) * d - pos[a]) / kk[a]; tdel[a] = d / kk[a];
+        } else if (kk[a] < 0.0) {
+            stp[a] = -1; tmax[a] = (org[a] + (double)idx[a] * d - pos[a]) / kk[a]; tdel[a] = -d / kk[a];
+        } else {
+            stp[a] = 0; tmax[a] = HUGEST; tdel[a] = HUGEST;
+        }
+    }
+    int ns = 0;
+    while (ns < max_steps) {
+        out[ns++] = idx[0] + n[0] * (idx[1] + n[1] * idx[2]);
+        int a = 0;
+        if (tmax[1] < tmax[a]) a = 1;
+        if (tmax[2] < tmax[a]) a = 2;
+        tmax[a] = tmax[a] + tdel[a];
+        idx[a] += stp[a];
+        if (idx[a] < 0 || idx[a] >= n[a]) break;
+    }
+    return ns;
+}
+
+// ionizing_field_and_rates, ionizing_field_mod.f90:72-170 (stellar loop,
+// static cyclic packet split over threads as photon_schedule_mod's static
+// schedule splits packet indices over ranks; ion_score_reduce sums them).
+void Sim::transport_pass() {
+    const int nleaf = grid.nleaf;
+    const int nnu = band.nnu_band;
+    const int nt = std::max(1, nthreads);
+    std::vector<Tally> loc(nt);
+    for (auto& t : loc) t.reset(nleaf, nnu);
+    const int64_t np = par.nphotons;
+#pragma omp parallel num_threads(nt)
+    {
+        int tid = 0;
+#ifdef _OPENMP
+        tid = omp_get_thread_num();
+#endif
+        Tally& t = loc[tid];
+        Photon ph;
+        for (int64_t ip = 1 + tid; ip <= np; ip += nt) {
+            gen_photon_qmc(ip - 1, ph);
+            double tau_edge = 0.0;
+            walk_edge_car(ph, t, &tau_edge);
+            // ion_score_energy_packet, ion_score_mod.f90:233-252 (x87 extended)
+            const double lum = ph.Lpacket * ph.wgt;
+            const double tr = std::exp(-std::max(tau_edge, 0.0));
+            t.emitted += (long double)lum;
+            t.absorbed += (long double)(lum * (1.0 - tr));
+            t.escaped += (long double)(lum * tr);
+        }
+    }
+    tally.reset(nleaf, nnu);
+    for (auto& t : loc) tally.add(t);
+    gas_rates_compute();
+}
+
+// gas_rates_compute + ion_score_apply_hhe, gas_rates_mod.f90:82-153 and
+// ion_score_mod.f90:298-317.
+void Sim::gas_rates_compute() {
+    const int nleaf = grid.nleaf;
+    const double h = 0.5 * grid.dcell;
+    const double w = 2.0 * h;
+    const double fac = 1.0 / ((w * w * w) * (par.distance2cm * par.distance2cm));
+    for (int il = 0; il < nleaf; ++il) {
+        const double* t = &tally.hhe[(size_t)6 * il];
+        gamma_HI[il] = t[0] * fac;
+        gamma_HeI[il] = t[1] * fac;
+        gamma_HeII[il] = t[2] * fac;
+        heat_HI[il] = t[3] * fac;
+        heat_HeI[il] = t[4] * fac;
+        heat_HeII[il] = t[5] * fac;
+    }
+}
+
+// solve_ion_cell, ion_balance_mod.f90:53-150 (H/He path: no metal sums, so
+// r_cx_in = r_cx_out = 0 and the closed-form substitution branch is used).
+void solve_ion_cell(const RateModel& rm, double yHe, double gH, double gHe1,
+                    double gHe2, double nH, double T, bool caseA, double& xHI,
+                    double& xHeI, double& xHeII, double& ne) {
+    double aH, aHe2, aHe3;
+    if (caseA) {
+        aH = alphaA_HII(rm, T); aHe2 = alphaA_HeII(rm, T); aHe3 = alphaA_HeIII(rm, T);
+    } else {
+        aH = alphaB_HII(rm, T); aHe2 = alphaB_HeII(rm, T); aHe3 = alphaB_HeIII(rm, T);
+    }
+    const double cH = ci_HI(rm, T), cHe1 = ci_HeI(rm, T), cHe2 = ci_HeII(rm, T);
+    double xHeIII = std::max(0.0, 1.0 - xHeI - xHeII);
+    ne = nH * ((1.0 - xHI) + yHe * (xHeII + 2.0 * xHeIII));
+    ne = std::max(ne, 1.0e-12 * nH);
+    const double r_cx_in = 0.0, r_cx_out = 0.0;
+    for (int it = 1; it <= 200; ++it) {
+        const double ne_old = ne;
+        const double denH = gH + (cH + aH) * ne + r_cx_in + r_cx_out;
+        xHI = (denH > 0.0) ? (aH * ne + r_cx_in) / denH : 1.0;
+        const double r1 = std::min((gHe1 + cHe1 * ne) / (aHe2 * ne), 1.0e150);
+        const double r2 = std::min((gHe2 + cHe2 * ne) / (aHe3 * ne), 1.0e150);
+        xHeI = 1.0 / (1.0 + r1 + r1 * r2);
+        xHeII = xHeI * r1;
+        xHeIII = xHeII * r2;
+        ne = nH * ((1.0 - xHI) + yHe * (xHeII + 2.0 * xHeIII));
+        ne = std::max(0.5 * (ne + ne_old), 1.0e-12 * nH);
+        if (std::fabs(ne - ne_old) <= 1.0e-10 * ne) break;
+    }
+}
+
+// gas_equilibrium_update, ion_balance_mod.f90:352-434.
+void Sim::gas_equilibrium_update(double* max_dx, double* dx_vol) {
+    const double T = par.te_fixed, yHe = par.He_abund, w = par.ion_relax;
+    const bool caseA = par.case_ab == "A";
+    const int nleaf = grid.nleaf;
+    std::vector<double> xHI_new(nleaf), xHeI_new(nleaf), xHeII_new(nleaf), ne_new(nleaf);
+#pragma omp parallel for num_threads(std::max(1, nthreads)) schedule(static)
+    for (int il = 0; il < nleaf; ++il) {
+        const double nH = st.nH[il];
+        if (nH <= 0.0) {
+            xHI_new[il] = st.xHI[il]; xHeI_new[il] = st.xHeI[il];
+            xHeII_new[il] = st.xHeII[il]; ne_new[il] = 0.0;
+            continue;
+        }
+        double xHI = st.xHI[il], xHeI = st.xHeI[il], xHeII = st.xHeII[il], ne;
+        solve_ion_cell(rm, yHe, gamma_HI[il], gamma_HeI[il], gamma_HeII[il], nH, T, caseA, xHI, xHeI, xHeII, ne);
+        xHI_new[il] = (1.0 - w) * st.xHI[il] + w * xHI;
+        xHeI_new[il] = (1.0 - w) * st.xHeI[il] + w * xHeI;
+        xHeII_new[il] = (1.0 - w) * st.xHeII[il] + w * xHeII;
+        const double xHeIII = std::max(0.0, 1.0 - xHeI_new[il] - xHeII_new[il]);
+        ne_new[il] = nH * ((1.0 - xHI_new[il]) + yHe * (xHeII_new[il] + 2.0 * xHeIII));
+    }
+    const double hw = grid.dcell;
+    const double vol = hw * hw * hw;
+    double mdx = 0.0, sdx = 0.0, sx = 0.0;
+    for (int il = 0; il < nleaf; ++il) {
+        if (st.nH[il] <= 0.0) continue;
+        const double d = std::fabs(xHI_new[il] - st.xHI[il]);
+        mdx = std::max(mdx, d);
+        sdx = sdx + vol * d;
+        sx = sx + vol * (1.0 - xHI_new[il]);
+    }
+    *max_dx = mdx;
+    *dx_vol = sdx / std::max(sx, TINEST);
+    st.xHI = xHI_new; st.xHeI = xHeI_new; st.xHeII = xHeII_new; st.ne = ne_new;
+}
+
+}  // namespace orc

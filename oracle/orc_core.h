@@ -1,0 +1,223 @@
+// Oracle for the MoCHII photon-packet transport + ionisation/thermal balance
+// path.  TEST INFRASTRUCTURE ONLY: a plain FP64 CPU restatement of the
+// reference Fortran, used by tests/, __graft_entry__.smoke() and the
+// cpu_baseline leg of bench.py as the checker.  Nothing in the product
+// (mochii_b200/) includes, links or calls this code.
+//
+// Every routine names the reference file:line it restates (paths relative
+// to the seoncafe/MoCHII source tree).  Built with -O2 -fno-fast-math
+// -ffp-contract=off so that the FP64 rounding sequence follows the
+// source expressions term by term.
+#pragma once
+#include <cmath>
+#include <cstdint>
+#include <string>
+#include <vector>
+#include <map>
+
+namespace orc {
+
+// ---- constants: define.f90:29-67, energy_sampler_mod.f90:16-18 ----------
+constexpr double PI = 3.141592653589793238462643383279502884197;
+constexpr double TWOPI = 6.283185307179586476925286766559005768394;
+constexpr double PC2CM = 3.0856776e18;
+constexpr double KPC2CM = PC2CM * 1e3;
+constexpr double AU2CM = 1.4960e13;
+constexpr double H_PLANCK_CGS = 6.62607015e-27;
+constexpr double CLIGHT_CGS = 2.99792458e10;
+constexpr double EV2ERG = 1.602176634e-12;
+constexpr double KBOLTZ_CGS = 1.380649e-16;
+constexpr double ETH_HI = 13.598;
+constexpr double ETH_HEI = 24.587;
+constexpr double ETH_HEII = 54.416;
+constexpr double KB_EV = 8.617333262145e-5;
+constexpr double TAU_HUGE = 745.2;             // raytrace_amr.f90:33
+constexpr int MAX_WALK_STEPS = 20000000;       // raytrace_amr.f90:43
+constexpr int MAX_PLANCK_KNOTS = 200000;       // energy_sampler_mod.f90:16
+constexpr int MAX_SRC = 16;                    // define.f90:74
+constexpr double HUGEST = 1.7976931348623157e308;
+constexpr double TINEST = 2.2250738585072014e-308;
+
+// ---- qmc_mod.f90 ---------------------------------------------------------
+struct Qmc {
+    uint32_t V[12][32];     // Vdir(k,d), qmc_mod.f90:60
+    uint32_t key[2][12];    // dkey(d,stream), qmc_mod.f90:61
+    void setup(int seed);   // qmc_mod.f90:73-139
+    uint32_t sobol_code(int64_t idx, int d) const;            // :192-206
+    uint32_t scrambled(int64_t idx, int d, int stream) const;  // :164-166
+    double uniform(int64_t idx, int d, int stream) const;      // :157-168
+};
+uint32_t hash32(uint32_t x);                     // qmc_mod.f90:250-260
+uint32_t reverse32(uint32_t x);                  // :233-247
+uint32_t laine_karras(uint32_t x, uint32_t s);   // :221-230
+uint32_t owen_scramble(uint32_t x, uint32_t s);  // :212-219
+
+// ---- energy_sampler_mod.f90 ---------------------------------------------
+struct Sampler {
+    std::vector<double> energy, density, cdf;
+    double total_integral = 0.0;
+};
+bool build_tabulated_sampler(Sampler& s, const std::vector<double>& e,
+                             const std::vector<double>& f, std::string* err);
+bool build_tabulated_band_sampler(Sampler& s, const std::vector<double>& e,
+                                  const std::vector<double>& f, double emin,
+                                  double emax, std::string* err);
+bool build_planck_sampler(Sampler& s, double T, double emin, double emax,
+                          double rtol, const std::vector<double>& thr,
+                          std::string* err);
+double sample_energy_cdf(const Sampler& s, double u);
+double energy_cdf_value(const Sampler& s, double e);
+double planck_energy_shape(double e, double T);
+
+// ---- photo_xsec.f90 -------------------------------------------------------
+double sigma_hydrogenic(double E, double Eth, double Z);
+double sigma_vfky96(double E, double Eth, double E0, double s0, double ya,
+                    double P, double yw, double y0, double y1);
+double sigma_vy95(double E, double Eth, double E0, double s0, double ya,
+                  double P, double yw, double l);
+double sigma_HI(double E);
+double sigma_HeI(double E);
+double sigma_HeII(double E);
+
+// ---- recomb_mod.f90 -------------------------------------------------------
+enum { RECOMB_BADNELL_MILNE = 0, RECOMB_HUI_GNEDIN = 1 };
+enum { CI_VORONOV = 0, CI_DERE_HYBRID = 1 };
+struct RateModel { int recomb = RECOMB_BADNELL_MILNE; int ci = CI_VORONOV; };
+double alphaA_HII(const RateModel&, double T);
+double alphaB_HII(const RateModel&, double T);
+double alphaA_HeII(const RateModel&, double T);
+double alphaB_HeII(const RateModel&, double T);
+double alphaA_HeIII(const RateModel&, double T);
+double alphaB_HeIII(const RateModel&, double T);
+double alpha1_HII(double T);
+double alpha1_HeII(double T);
+double alpha1_HeIII(double T);
+double ci_HI(const RateModel&, double T);
+double ci_HeI(const RateModel&, double T);
+double ci_HeII(const RateModel&, double T);
+double ci_dere_ratio(const RateModel&, int Z, int stage);
+double voronov(double T, double dE, double P, double A, double X, double K);
+
+// ---- namelist + parameters (define.f90:189-861, setup.f90:11-626) -------
+struct Par {
+    // launch
+    int64_t nphotons = 100000;
+    std::string launch_sequence = "random";
+    int qmc_seed = 12345;
+    double source_cdf_tol = 1.0e-8;
+    double luminosity = -999.0;
+    double tstar = -999.0;
+    // band
+    int nnu_ion = 16;
+    double eion_min = 13.598, eion_max = 100.0;
+    bool add_fuv = false;
+    double efuv_min = 6.0;
+    int nnu_fuv = 8;
+    bool ion_align_edges = true;
+    // geometry
+    std::string grid_type = "car";
+    std::string car_walk = "dda";
+    std::string amr_file;
+    int nx = 1, ny = 1, nz = 11;
+    double xmax = 1.0, ymax = 1.0, zmax = 1.0;
+    double rmax = -999.0, rmin = 0.0, nH_const = -1.0;
+    std::string distance_unit = "kpc";
+    double distance2cm = KPC2CM;
+    std::string source_geometry = "point";
+    double xs_point = 0.0, ys_point = 0.0, zs_point = 0.0;
+    int nsource = 1;
+    double src_tstar[MAX_SRC], src_lum[MAX_SRC];
+    double src_x[MAX_SRC], src_y[MAX_SRC], src_z[MAX_SRC];
+    // gas
+    double xHI_init = 1.0, xHeI_init = 1.0, xHeII_init = 0.0;
+    double He_abund = 0.1;
+    int gas_niter = 0;
+    double gas_tol = 1.0e-3, te_fixed = 1.0e4, ion_relax = 1.0;
+    std::string case_ab = "B";
+    std::string ci_model = "voronov";
+    std::string recomb_model = "badnell_milne";
+    std::string cooling_model = "local_ne";
+    std::string charge_exchange = "two_way";
+    std::string conv_crit = "cell";
+    bool solve_te = false;
+    double te_min = 1.0e3, te_max = 5.0e4, gas_tol_te = 1.0e-3;
+    bool use_metals = false, diffuse_field = false, use_sec_ion = false;
+    bool ion_add_dust = false, ion_dust_scatter = false;
+    std::string dust_density_law = "global_dgr";
+    double DGR = 1.0e-2, cext_dust = 1.6059e-21;
+    std::string data_dir, atomic_dir, ion_dust_kext;
+    Par();
+};
+// Parse a Fortran "&parameters par%key = value /" namelist text.
+bool parse_namelist(const std::string& text, Par& p, std::string* err);
+
+// ---- band (ion_band_mod.f90) ----------------------------------------------
+struct Band {
+    int nnu_band = 0, nfuv_band = 0;
+    std::vector<double> eedge;       // ion_eedge, size nnu_band+1
+    int ncomp = 1;
+    bool multi_src = false;
+    std::vector<int> comp_kind;      // multi only
+    std::vector<double> src_cdf;     // multi only
+    std::vector<Sampler> samplers;   // source_energy_sampler
+    double ion_Ltot = 0.0;
+    int qmc_ndim = 3;
+};
+bool build_aligned_edges(std::vector<double>& eedge, int nfuv, int nnu,
+                         double lo, double hi, const std::vector<double>& meth,
+                         std::string* err);
+int ion_bin_of(const Band& b, double e, bool include_fuv);
+bool band_setup(const Par& p, Band& b, std::string* err);
+
+// ---- car grid + state ----------------------------------------------------
+struct Grid {
+    bool car = true;
+    int nx = 0, ny = 0, nz = 0, nleaf = 0;
+    double xmin, xmax, ymin, ymax, zmin, zmax, dcell;
+};
+struct State {
+    std::vector<double> nH, xHI, xHeI, xHeII, ne, Te, rhokap;
+};
+
+// ---- tallies ----------------------------------------------------------------
+struct Tally {
+    std::vector<double> hhe;         // (6, nleaf), leaf-major: hhe[6*il + k]
+    std::vector<double> jt;          // (nnu_band, nleaf): jt[nnu*il + inu]
+    long double emitted = 0, absorbed = 0, escaped = 0;
+    int64_t direct_segments = 0, scattered_segments = 0;
+    void reset(int nleaf, int nnu);
+    void add(const Tally& o);
+};
+
+struct Photon {
+    double x, y, z, kx, ky, kz;
+    double E, wgt, Lpacket;
+    int inu;
+    double sHI, sHeI, sHeII;
+};
+
+struct Sim {
+    Par par;
+    RateModel rm;
+    Qmc qmc;
+    Band band;
+    Grid grid;
+    State st;
+    Tally tally;
+    std::vector<double> gamma_HI, gamma_HeI, gamma_HeII, heat_HI, heat_HeI, heat_HeII;
+    int nthreads = 1;
+    bool setup(const std::string& namelist, std::string* err);
+    void transport_pass();           // ionizing_field_mod.f90:72-170
+    void gas_rates_compute();        // gas_rates_mod.f90:82-153
+    void gas_equilibrium_update(double* max_dx, double* dx_vol);  // ion_balance_mod.f90:352
+    void gen_photon_qmc(int64_t ip, Photon& ph) const;          // ion_band_mod.f90:1880
+    void walk_edge_car(const Photon& ph, Tally& t, double* tau_edge) const;  // raytrace_amr.f90:534
+    int walk_leaves_car(double x, double y, double z, double kx, double ky,
+                        double kz, int max_steps, int32_t* out) const;
+};
+
+void solve_ion_cell(const RateModel& rm, double He_abund, double gH,
+                    double gHe1, double gHe2, double nH, double T, bool caseA,
+                    double& xHI, double& xHeI, double& xHeII, double& ne);
+
+}  // namespace orc

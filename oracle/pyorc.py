@@ -1,0 +1,224 @@
+"""ctypes wrapper of the oracle library (TEST INFRASTRUCTURE ONLY).
+
+Imported by tests/, __graft_entry__.smoke() and bench.py's cpu_baseline leg
+as the checker; the product package never imports it.
+"""
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB = os.path.join(HERE, "liborc.so")
+_lib = None
+
+
+def build(force=False):
+    srcs = [os.path.join(HERE, f) for f in ("orc_core.cpp", "orc_capi.cpp", "orc_core.h", "Makefile")]
+    if force or not os.path.exists(LIB) or any(os.path.getmtime(s) > os.path.getmtime(LIB) for s in srcs):
+        subprocess.run(["make", "-s", "-C", HERE], check=True)
+    return LIB
+
+
+def load():
+    global _lib
+    if _lib is not None:
+        return _lib
+    build()
+    lib = C.CDLL(LIB)
+    V, D, I, LL = C.c_void_p, C.c_double, C.c_int, C.c_longlong
+    sig = {
+        "orc_qmc_uniforms": (I, [I, I, LL, LL, I, V]),
+        "orc_qmc_raw_codes": (I, [LL, LL, I, V]),
+        "orc_qmc_keys": (None, [I, V]),
+        "orc_sampler_planck": (V, [D, D, D, D, V, I]),
+        "orc_sampler_tab": (V, [V, V, I]),
+        "orc_sampler_tab_band": (V, [V, V, I, D, D]),
+        "orc_sampler_size": (I, [V]),
+        "orc_sampler_total": (D, [V]),
+        "orc_sampler_get": (None, [V, V, V, V]),
+        "orc_sampler_sample": (None, [V, V, LL, V]),
+        "orc_sampler_cdf": (None, [V, V, LL, V]),
+        "orc_sampler_free": (None, [V]),
+        "orc_eval": (I, [C.c_char_p, I, V, LL, V]),
+        "orc_band_edges": (I, [C.c_char_p, V, I]),
+        "orc_sim_new": (V, [C.c_char_p, I, C.c_char_p, I]),
+        "orc_sim_free": (None, [V]),
+        "orc_sim_nleaf": (I, [V]),
+        "orc_sim_nnu": (I, [V]),
+        "orc_sim_ion_Ltot": (D, [V]),
+        "orc_sim_set_nphotons": (None, [V, LL]),
+        "orc_sim_transport_pass": (I, [V]),
+        "orc_sim_equilibrium_update": (I, [V, V]),
+        "orc_sim_energy": (None, [V, V, V]),
+        "orc_sim_get": (LL, [V, C.c_char_p, V, LL]),
+        "orc_sim_set": (LL, [V, C.c_char_p, V, LL]),
+        "orc_sim_photon": (None, [V, LL, V]),
+        "orc_sim_walk_leaves": (I, [V, LL, V, I, V, V]),
+        "orc_solve_ion_cell": (None, [I, D, D, D, D, D, D, I, V, V]),
+        "orc_last_error": (C.c_char_p, []),
+    }
+    for name, (res, args) in sig.items():
+        f = getattr(lib, name)
+        f.restype = res
+        f.argtypes = args
+    _lib = lib
+    return lib
+
+
+def qmc_uniforms(seed, stream, idx0, n, nd):
+    lib = load()
+    out = np.zeros((n, nd))
+    assert lib.orc_qmc_uniforms(seed, stream, idx0, n, nd, out.ctypes.data) == 0
+    return out
+
+
+def qmc_raw_codes(idx0, n, nd):
+    lib = load()
+    out = np.zeros((n, nd), dtype=np.uint32)
+    assert lib.orc_qmc_raw_codes(idx0, n, nd, out.ctypes.data) == 0
+    return out
+
+
+class Sampler:
+    def __init__(self, handle):
+        if not handle:
+            raise RuntimeError(load().orc_last_error().decode())
+        self.h = handle
+
+    @classmethod
+    def planck(cls, T, emin, emax, rtol, thresholds):
+        thr = np.ascontiguousarray(thresholds, dtype=float)
+        return cls(load().orc_sampler_planck(T, emin, emax, rtol, thr.ctypes.data, thr.size))
+
+    @classmethod
+    def tabulated(cls, e, f):
+        e = np.ascontiguousarray(e, dtype=float)
+        f = np.ascontiguousarray(f, dtype=float)
+        return cls(load().orc_sampler_tab(e.ctypes.data, f.ctypes.data, e.size))
+
+    @classmethod
+    def tabulated_band(cls, e, f, emin, emax):
+        e = np.ascontiguousarray(e, dtype=float)
+        f = np.ascontiguousarray(f, dtype=float)
+        return cls(load().orc_sampler_tab_band(e.ctypes.data, f.ctypes.data, e.size, emin, emax))
+
+    @property
+    def total(self):
+        return load().orc_sampler_total(self.h)
+
+    def tables(self):
+        n = load().orc_sampler_size(self.h)
+        e, f, c = np.zeros(n), np.zeros(n), np.zeros(n)
+        load().orc_sampler_get(self.h, e.ctypes.data, f.ctypes.data, c.ctypes.data)
+        return e, f, c
+
+    def sample(self, u):
+        u = np.ascontiguousarray(u, dtype=float)
+        out = np.zeros_like(u)
+        load().orc_sampler_sample(self.h, u.ctypes.data, u.size, out.ctypes.data)
+        return out
+
+    def cdf(self, e):
+        e = np.ascontiguousarray(e, dtype=float)
+        out = np.zeros_like(e)
+        load().orc_sampler_cdf(self.h, e.ctypes.data, e.size, out.ctypes.data)
+        return out
+
+    def __del__(self):
+        try:
+            load().orc_sampler_free(self.h)
+        except Exception:
+            pass
+
+
+def evaluate(name, x, model=0):
+    x = np.ascontiguousarray(x, dtype=float)
+    out = np.zeros_like(x)
+    assert load().orc_eval(name.encode(), model, x.ctypes.data, x.size, out.ctypes.data) == 0, name
+    return out
+
+
+def band_edges(namelist):
+    out = np.zeros(512)
+    n = load().orc_band_edges(namelist.encode(), out.ctypes.data, 512)
+    assert n > 0, load().orc_last_error()
+    return out[:n]
+
+
+def solve_ion_cell(gH, gHe1, gHe2, nH, T, caseA, x3, yHe=0.1, model=0):
+    x = np.array(x3, dtype=float)
+    ne = C.c_double()
+    load().orc_solve_ion_cell(model, yHe, gH, gHe1, gHe2, nH, T, int(caseA), x.ctypes.data, C.byref(ne))
+    return x, ne.value
+
+
+class Sim:
+    """The oracle's nebula: the same namelist text the product reads."""
+
+    def __init__(self, namelist, nthreads=None):
+        lib = load()
+        if nthreads is None:
+            nthreads = os.cpu_count() or 1
+        err = C.create_string_buffer(512)
+        self.h = lib.orc_sim_new(namelist.encode(), int(nthreads), err, 512)
+        if not self.h:
+            raise RuntimeError("oracle setup failed: " + err.value.decode())
+        self.nleaf = lib.orc_sim_nleaf(self.h)
+        self.nnu = lib.orc_sim_nnu(self.h)
+        self.nthreads = nthreads
+
+    def transport_pass(self):
+        load().orc_sim_transport_pass(self.h)
+
+    def equilibrium_update(self):
+        m = np.zeros(2)
+        load().orc_sim_equilibrium_update(self.h, m.ctypes.data)
+        return m[0], m[1]
+
+    def set_nphotons(self, n):
+        load().orc_sim_set_nphotons(self.h, int(n))
+
+    @property
+    def ion_Ltot(self):
+        return load().orc_sim_ion_Ltot(self.h)
+
+    def energy(self):
+        e = np.zeros(3)
+        s = np.zeros(2, dtype=np.int64)
+        load().orc_sim_energy(self.h, e.ctypes.data, s.ctypes.data)
+        return e, s
+
+    def get(self, name):
+        cap = self.nleaf * max(self.nnu, 6) + 1024
+        out = np.zeros(cap)
+        n = load().orc_sim_get(self.h, name.encode(), out.ctypes.data, cap)
+        assert n >= 0, name
+        out = out[:n]
+        if name == "jt_ion":
+            out = out.reshape(self.nleaf, self.nnu)
+        return out
+
+    def set(self, name, values):
+        a = np.ascontiguousarray(values, dtype=float)
+        assert load().orc_sim_set(self.h, name.encode(), a.ctypes.data, a.size) == a.size
+
+    def photon(self, ip):
+        out = np.zeros(8)
+        load().orc_sim_photon(self.h, int(ip), out.ctypes.data)
+        return out
+
+    def walk_leaves(self, rays, max_steps):
+        rays = np.ascontiguousarray(rays, dtype=float).reshape(-1, 6)
+        nray = rays.shape[0]
+        leaves = np.full((nray, max_steps), -1, dtype=np.int32)
+        nsteps = np.zeros(nray, dtype=np.int32)
+        load().orc_sim_walk_leaves(self.h, nray, rays.ctypes.data, max_steps, leaves.ctypes.data, nsteps.ctypes.data)
+        return leaves, nsteps
+
+    def __del__(self):
+        try:
+            load().orc_sim_free(self.h)
+        except Exception:
+            pass
