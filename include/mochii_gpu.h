@@ -197,8 +197,8 @@ double mochii_ion_Ltot(const mochii_ctx* ctx);
 int mochii_sobol_uniforms(int seed, int stream, int64_t idx0, int64_t n, int nd, double* out);
 /* Geometry-only cell walk of nray rays (x,y,z,kx,ky,kz each, code units)
  * on ctx's grid (raytrace_ion_to_edge_car, raytrace_amr.f90:534-592, with
- * no optical-depth cut): leaves[r*max_steps + s] (0-based leaf index) and
- * nsteps[r]. */
+ * no optical-depth cut): leaves[r*max_steps + s] (0-based leaf index, -1
+ * past the last step) and nsteps[r]. */
 int mochii_walk_leaves(mochii_ctx* ctx, int64_t nray, const double* rays, int max_steps,
                        int32_t* leaves, int32_t* nsteps);
 /* Launch records of packets ip0..ip0+n-1: x,y,z,kx,ky,kz,E,inu (8 doubles

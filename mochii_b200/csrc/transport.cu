@@ -347,6 +347,7 @@ __global__ void k_walk(const double* rays, long long nray, int max_steps, int* l
         if (idx[ax] < 0 || idx[ax] >= n[ax]) break;
     }
     nsteps[r] = ns;
+    for (int s = ns; s < max_steps; ++s) leaves[r * max_steps + s] = -1;
 }
 
 // Launch records (x, y, z, kx, ky, kz, E, inu) for the launch hook.
