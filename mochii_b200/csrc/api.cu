@@ -2,6 +2,7 @@
 // state-exchange / test hooks declared in include/mochii_gpu.h.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -42,7 +43,8 @@ void release(mochii_ctx* c) {
     if (!c) return;
     void* ptrs[] = {c->nH, c->xHI, c->xHeI, c->xHeII, c->ne, c->Te, c->col, c->tally, c->jt, c->rates,
                     c->tab.tab_e, c->tab.tab_f, c->tab.tab_c, c->tab.tab_off, c->tab.comp, c->tab.eedge,
-                    c->tab.qmc, c->tw.ledger, c->tw.counters, c->bw.partial, c->bw.counters};
+                    c->tab.qmc, c->tw.ledger, c->tw.counters, c->bw.partial, c->bw.counters,
+                    c->rec.tm, c->rec.td, c->rec.cell, c->rec.bits, c->rec.sig, c->rec.coef};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     for (cudaEvent_t e : {c->ev0, c->ev1, c->evA, c->evB})
@@ -57,6 +59,7 @@ int validate(const mochii_params& p, std::string* why, int* code) {
     if (p.eion_max <= p.eion_min || p.eion_min <= 0.0) return *why = "need 0 < par%eion_min < par%eion_max", 1;
     if (p.grid_car) {
         if (p.xmax <= 0.0 || p.nx < 1 || p.ny < 1 || p.nz < 1) return *why = "car grid needs par%xmax > 0 and nx,ny,nz >= 1", 1;
+        if (p.nx > 1024 || p.ny > 1024 || p.nz > 1024) return *why = "car grid: nx, ny, nz must be <= 1024", 1;
         const double dcx = 2.0 * p.xmax / p.nx, dcy = 2.0 * p.ymax / p.ny, dcz = 2.0 * p.zmax / p.nz;
         if (std::fabs(dcy - dcx) > 1.0e-9 * dcx || std::fabs(dcz - dcx) > 1.0e-9 * dcx)
             return *why = "car grid needs cubic cells: 2*xmax/nx = 2*ymax/ny = 2*zmax/nz", 1;   // grid_mod_amr.f90:91-96
@@ -226,6 +229,14 @@ extern "C" int mochii_init(const mochii_params* pin, mochii_ctx** out) {
     c->tw.ledger_blocks = transport_blocks(c);
     CKI(dalloc(&c->tw.ledger, 3 * (size_t)c->tw.ledger_blocks));
     CKI(dalloc(&c->tw.counters, 4));
+    // packet records: launch chunks of up to 4 Mi packets
+    c->rec.cap = std::min<long long>(p.nphotons, 1LL << 22);
+    CKI(dalloc(&c->rec.tm, 3 * (size_t)c->rec.cap));
+    CKI(dalloc(&c->rec.td, 3 * (size_t)c->rec.cap));
+    CKI(dalloc(&c->rec.cell, (size_t)c->rec.cap));
+    CKI(dalloc(&c->rec.bits, (size_t)c->rec.cap));
+    CKI(cudaMalloc(&c->rec.sig, 3 * (size_t)c->rec.cap * rsz + 64));
+    CKI(cudaMalloc(&c->rec.coef, 6 * (size_t)c->rec.cap * rsz + 64));
     c->bw.blocks = balance_blocks(c);
     CKI(dalloc(&c->bw.partial, 6 * (size_t)c->bw.blocks));
     CKI(dalloc(&c->bw.counters, 4));
@@ -258,6 +269,20 @@ extern "C" int mochii_set_nphotons(mochii_ctx* c, int64_t np) {
         CK(c, dalloc(&c->tw.ledger, 3 * (size_t)nb));
     }
     c->tw.ledger_blocks = nb;
+    const long long cap = std::min<long long>(np, 1LL << 22);
+    if (cap > c->rec.cap) {
+        const size_t rsz = c->fp32 ? 4 : 8;
+        for (void* q : {(void*)c->rec.tm, (void*)c->rec.td, (void*)c->rec.cell, (void*)c->rec.bits, c->rec.sig, c->rec.coef})
+            if (q) cudaFree(q);
+        c->rec = RecordBuffers();
+        c->rec.cap = cap;
+        CK(c, dalloc(&c->rec.tm, 3 * (size_t)cap));
+        CK(c, dalloc(&c->rec.td, 3 * (size_t)cap));
+        CK(c, dalloc(&c->rec.cell, (size_t)cap));
+        CK(c, dalloc(&c->rec.bits, (size_t)cap));
+        CK(c, cudaMalloc(&c->rec.sig, 3 * (size_t)cap * rsz + 64));
+        CK(c, cudaMalloc(&c->rec.coef, 6 * (size_t)cap * rsz + 64));
+    }
     return MOCHII_OK;
 }
 

@@ -44,6 +44,17 @@ struct TransportWork {
     int ledger_blocks = 0;
 };
 
+// Per-packet launch records of one chunk (see transport.cu).
+struct RecordBuffers {
+    double* tm = nullptr;
+    double* td = nullptr;
+    int* cell = nullptr;
+    int* bits = nullptr;
+    void* sig = nullptr;
+    void* coef = nullptr;
+    long long cap = 0;
+};
+
 struct BalanceWork {
     double* partial = nullptr;   // per block: max_dx, max_dte, sum_dxv, sum_xv, sum_dtv, sum_tv
     unsigned long long* counters = nullptr;
@@ -70,6 +81,7 @@ struct mochii_ctx {
     double* rates = nullptr;
     mochii::DeviceTables tab;
     mochii::TransportWork tw;
+    mochii::RecordBuffers rec;
     mochii::BalanceWork bw;
     std::string last_error;
 };

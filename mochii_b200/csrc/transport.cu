@@ -141,88 +141,134 @@ __device__ double block_sum(double v, double* sh) {
     return r;
 }
 
-template <typename R, int NABS>
-__global__ void __launch_bounds__(kThreads) k_transport(const PassArgs a) {
-    typedef typename Acc<R>::T T;
-    constexpr int NT = NABS == 1 ? 2 : 6;
+// Packet records of one launch chunk (structure of arrays, chunk-major):
+// the DDA state after dda_init (tMax, tDelta, cell, step signs), the
+// diagnostic bin and the packet's cross sections / rate coefficients.
+struct Records {
+    double* tm;    // 3 x cap
+    double* td;    // 3 x cap
+    int* cell;     // ix | iy << 10 | iz << 20
+    int* bits;     // inu | (stp_x+1) << 16 | (stp_y+1) << 18 | (stp_z+1) << 20
+    void* sig;     // 3 x cap of R: sigma_HI, sigma_HeI, sigma_HeII in 1e-18 cm^2
+    void* coef;    // 6 x cap of R: Gamma/heat coefficients per unit path
+    long long cap;
+};
+
+// Launch kernel: one thread per packet, no divergence between packets.
+// gen_ion_photon_qmc (ion_band_mod.f90:1880-1935) with emit_point_qmc
+// (:2232-2247), build_ion_packet_physics (ion_packet_mod.f90:21-53), the
+// coefficients of score_ion_path (ion_score_mod.f90:213-221) and dda_init
+// (raytrace_amr.f90:495-532).
+template <typename R>
+__global__ void __launch_bounds__(kThreads) k_launch(const PassArgs a, Records rec, long long ip0, long long n) {
     __shared__ QmcTables sq;
-    __shared__ double sh[kThreads];
     {
         const uint32_t* src = reinterpret_cast<const uint32_t*>(a.qmc);
         uint32_t* dst = reinterpret_cast<uint32_t*>(&sq);
         for (int i = threadIdx.x; i < (int)(sizeof(QmcTables) / 4); i += blockDim.x) dst[i] = src[i];
     }
     __syncthreads();
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const long long ip = ip0 + i;
+    double u[7];
+    for (int d = 0; d < a.ndim; ++d) u[d] = qmc_uniform(sq, (uint64_t)ip, d, 0);
+    int ic = 0;
+    double umu, uphi, ue;
+    if (!a.multi) {
+        ue = u[0]; umu = u[1]; uphi = u[2];
+    } else {
+        ic = a.ncomp - 1;
+        for (int k = 0; k < a.ncomp; ++k)
+            if (u[0] <= a.comp[4 * k]) { ic = k; break; }
+        ue = u[1]; umu = u[2]; uphi = u[3];
+    }
+    const int t0 = a.tab_off[ic], t1 = a.tab_off[ic + 1];
+    const double E = sample_energy(a.tab_e + t0, a.tab_f + t0, a.tab_c + t0, t1 - t0, ue);
+    const double pos[3] = {a.comp[4 * ic + 1], a.comp[4 * ic + 2], a.comp[4 * ic + 3]};
+    const double cost = 2.0 * umu - 1.0;
+    const double sint = sqrt(1.0 - cost * cost);
+    double sphi, cphi;
+    sincos(kTwoPi * uphi, &sphi, &cphi);
+    const double kk[3] = {sint * cphi, sint * sphi, cost};
+    const int inu = bin_of(a.eedge, a.nnu, E);
+    const double sHI = sigma_HI(E), sHeI = sigma_HeI(E), sHeII = sigma_HeII(E);
+    R* sg = static_cast<R*>(rec.sig);
+    R* cf = static_cast<R*>(rec.coef);
+    const long long c = rec.cap;
+    sg[i] = (R)(sHI * 1.0e18);
+    sg[c + i] = (R)(sHeI * 1.0e18);
+    sg[2 * c + i] = (R)(sHeII * 1.0e18);
+    cf[i] = (R)(sHI * 1.0e18 / E);
+    cf[c + i] = (R)(sHI * 1.0e18 * fmax(1.0 - kEthHI / E, 0.0));
+    cf[2 * c + i] = (R)(sHeI * 1.0e18 / E);
+    cf[3 * c + i] = (R)(sHeI * 1.0e18 * fmax(1.0 - kEthHeI / E, 0.0));
+    cf[4 * c + i] = (R)(sHeII * 1.0e18 / E);
+    cf[5 * c + i] = (R)(sHeII * 1.0e18 * fmax(1.0 - kEthHeII / E, 0.0));
+    const double d = a.dcell;
+    int idx[3], bits = inu;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        idx[k] = min(max((int)((pos[k] - a.org[k]) / d), 0), a.n[k] - 1);
+        double tmv, tdv;
+        int st;
+        if (kk[k] > 0.0) {
+            st = 1; tmv = (a.org[k] + (double)(idx[k] + 1) * d - pos[k]) / kk[k]; tdv = d / kk[k];
+        } else if (kk[k] < 0.0) {
+            st = -1; tmv = (a.org[k] + (double)idx[k] * d - pos[k]) / kk[k]; tdv = -d / kk[k];
+        } else {
+            st = 0; tmv = kHugest; tdv = kHugest;
+        }
+        rec.tm[k * c + i] = tmv;
+        rec.td[k * c + i] = tdv;
+        bits |= (st + 1) << (16 + 2 * k);
+    }
+    rec.cell[i] = idx[0] | (idx[1] << 10) | (idx[2] << 20);
+    rec.bits[i] = bits;
+}
 
+// Walk kernel: raytrace_ion_to_edge_car (raytrace_amr.f90:534-592) for the
+// packets of one chunk, grid-stride, the DDA state held in registers.
+template <typename R, int NABS>
+__global__ void __launch_bounds__(kThreads) k_walk_edge(const PassArgs a, const Records rec, long long n,
+                                                        int accumulate) {
+    typedef typename Acc<R>::T T;
+    constexpr int NT = NABS == 1 ? 2 : 6;
+    __shared__ double sh[kThreads];
     double emitted = 0.0, absorbed = 0.0, escaped = 0.0;
     unsigned long long nseg = 0, kills = 0;
     T* tal = static_cast<T*>(a.tally);
     T* jt = static_cast<T*>(a.jt);
+    const R* sg = static_cast<const R*>(rec.sig);
+    const R* cfp = static_cast<const R*>(rec.coef);
+    const long long c = rec.cap;
     const long long stride = (long long)gridDim.x * blockDim.x;
-
-    for (long long ip = (long long)blockIdx.x * blockDim.x + threadIdx.x; ip < a.np; ip += stride) {
-        // ---- launch: gen_ion_photon_qmc (ion_band_mod.f90:1880-1935) ----
-        double u[7];
-        for (int d = 0; d < a.ndim; ++d) u[d] = qmc_uniform(sq, (uint64_t)ip, d, 0);
-        int ic = 0;
-        double umu, uphi, ue;
-        if (!a.multi) {
-            ue = u[0]; umu = u[1]; uphi = u[2];
-        } else {
-            ic = a.ncomp - 1;
-            for (int i = 0; i < a.ncomp; ++i)
-                if (u[0] <= a.comp[4 * i]) { ic = i; break; }
-            ue = u[1]; umu = u[2]; uphi = u[3];
-        }
-        const int t0 = a.tab_off[ic], t1 = a.tab_off[ic + 1];
-        const double E = sample_energy(a.tab_e + t0, a.tab_f + t0, a.tab_c + t0, t1 - t0, ue);
-        const double pos[3] = {a.comp[4 * ic + 1], a.comp[4 * ic + 2], a.comp[4 * ic + 3]};
-        const double cost = 2.0 * umu - 1.0;
-        const double sint = sqrt(1.0 - cost * cost);
-        const double phi = kTwoPi * uphi;
-        double sphi, cphi;
-        sincos(phi, &sphi, &cphi);
-        const double kk[3] = {sint * cphi, sint * sphi, cost};
-        const int inu = bin_of(a.eedge, a.nnu, E);
-        // ---- packet cross sections (build_ion_packet_physics), 1e-18 cm^2 units
-        const double sHI = sigma_HI(E), sHeI = sigma_HeI(E), sHeII = sigma_HeII(E);
-        const R s0 = (R)(sHI * 1.0e18), s1 = (R)(sHeI * 1.0e18), s2 = (R)(sHeII * 1.0e18);
-        // rate coefficients per unit path (ion_score_mod.f90:213-221), scaled:
-        // Gamma_i: sigma_i/E [1e-18 cm^2/eV]; H_i: sigma_i (1 - E_th,i/E)
-        R cf[6];
-        cf[0] = (R)(sHI * 1.0e18 / E);
-        cf[1] = (R)(sHI * 1.0e18 * fmax(1.0 - kEthHI / E, 0.0));
-        cf[2] = (R)(sHeI * 1.0e18 / E);
-        cf[3] = (R)(sHeI * 1.0e18 * fmax(1.0 - kEthHeI / E, 0.0));
-        cf[4] = (R)(sHeII * 1.0e18 / E);
-        cf[5] = (R)(sHeII * 1.0e18 * fmax(1.0 - kEthHeII / E, 0.0));
-
-        // ---- dda_init (raytrace_amr.f90:495-532) ----
-        const double d = a.dcell;
-        int idx[3], stp[3];
-        double tmax[3], tdel[3];
+    const int nx = a.n[0], ny = a.n[1], nz = a.n[2];
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+        double t0 = rec.tm[i], t1 = rec.tm[c + i], t2 = rec.tm[2 * c + i];
+        const double d0 = rec.td[i], d1 = rec.td[c + i], d2 = rec.td[2 * c + i];
+        const int cell = rec.cell[i], bits = rec.bits[i];
+        int ix = cell & 1023, iy = (cell >> 10) & 1023, iz = (cell >> 20) & 1023;
+        const int sx = ((bits >> 16) & 3) - 1, sy = ((bits >> 18) & 3) - 1, sz = ((bits >> 20) & 3) - 1;
+        const int inu = bits & 0xFFFF;
+        const R s0 = sg[i];
+        const R s1 = NABS == 1 ? (R)0 : sg[c + i];
+        const R s2 = NABS == 1 ? (R)0 : sg[2 * c + i];
+        R cf[NT];
 #pragma unroll
-        for (int k = 0; k < 3; ++k) {
-            idx[k] = min(max((int)((pos[k] - a.org[k]) / d), 0), a.n[k] - 1);
-            if (kk[k] > 0.0) {
-                stp[k] = 1; tmax[k] = (a.org[k] + (double)(idx[k] + 1) * d - pos[k]) / kk[k]; tdel[k] = d / kk[k];
-            } else if (kk[k] < 0.0) {
-                stp[k] = -1; tmax[k] = (a.org[k] + (double)idx[k] * d - pos[k]) / kk[k]; tdel[k] = -d / kk[k];
-            } else {
-                stp[k] = 0; tmax[k] = kHugest; tdel[k] = kHugest;
-            }
-        }
-        // ---- raytrace_ion_to_edge_car (raytrace_amr.f90:534-592) ----
+        for (int k = 0; k < NT; ++k) cf[k] = cfp[k * c + i];
         R expo = (R)1.0;
         double tau = 0.0, t_cur = 0.0;
         int nstep = 0;
         for (;;) {
             if (++nstep > kMaxWalkSteps) { ++kills; break; }
-            const long long il = (long long)idx[0] + (long long)a.n[0] * ((long long)idx[1] + (long long)a.n[1] * idx[2]);
+            const long long il = (long long)ix + (long long)nx * ((long long)iy + (long long)ny * iz);
+            // minloc(tmax): first minimum
             int ax = 0;
-            if (tmax[1] < tmax[ax]) ax = 1;
-            if (tmax[2] < tmax[ax]) ax = 2;
-            const double seg = tmax[ax] - t_cur;
+            double tm = t0;
+            if (t1 < tm) { ax = 1; tm = t1; }
+            if (t2 < tm) { ax = 2; tm = t2; }
+            const double seg = tm - t_cur;
             const R kap = opacity<R, NABS>(a.col, il, s0, s1, s2);
             const R ks = kap * (R)seg;
             R w;
@@ -242,12 +288,16 @@ __global__ void __launch_bounds__(kThreads) k_transport(const PassArgs a) {
             }
             tau = tau + (double)ks;
             if (tau >= kTauHuge) break;
-            t_cur = tmax[ax];
-            tmax[ax] = tmax[ax] + tdel[ax];
-            idx[ax] += stp[ax];
-            if (idx[ax] < 0 || idx[ax] >= a.n[ax]) break;
+            t_cur = tm;
+            t0 = ax == 0 ? t0 + d0 : t0;
+            t1 = ax == 1 ? t1 + d1 : t1;
+            t2 = ax == 2 ? t2 + d2 : t2;
+            ix += ax == 0 ? sx : 0;
+            iy += ax == 1 ? sy : 0;
+            iz += ax == 2 ? sz : 0;
+            if (ix < 0 || ix >= nx || iy < 0 || iy >= ny || iz < 0 || iz >= nz) break;
         }
-        // ---- ion_score_energy_packet (ion_score_mod.f90:233-252) ----
+        // ion_score_energy_packet (ion_score_mod.f90:233-252)
         const double lum = a.Lpacket;
         const double tr = exp(-fmax(tau, 0.0));
         emitted += lum;
@@ -258,11 +308,13 @@ __global__ void __launch_bounds__(kThreads) k_transport(const PassArgs a) {
     const double e1 = block_sum(absorbed, sh);
     const double e2 = block_sum(escaped, sh);
     if (threadIdx.x == 0) {
-        a.ledger[3 * blockIdx.x + 0] = e0;
-        a.ledger[3 * blockIdx.x + 1] = e1;
-        a.ledger[3 * blockIdx.x + 2] = e2;
+        double* L = a.ledger + 3 * blockIdx.x;
+        if (accumulate) {
+            L[0] += e0; L[1] += e1; L[2] += e2;
+        } else {
+            L[0] = e0; L[1] = e1; L[2] = e2;
+        }
     }
-    // counters: warp-reduce then one atomic per warp
     for (int o = 16; o > 0; o >>= 1) {
         nseg += __shfl_down_sync(0xffffffffu, nseg, o);
         kills += __shfl_down_sync(0xffffffffu, kills, o);
@@ -423,13 +475,28 @@ int transport_blocks(const mochii_ctx* c) {
 
 cudaError_t launch_transport(mochii_ctx* c) {
     const PassArgs a = make_args(c);
+    Records r;
+    r.cap = c->rec.cap;
+    r.tm = c->rec.tm;
+    r.td = c->rec.td;
+    r.cell = c->rec.cell;
+    r.bits = c->rec.bits;
+    r.sig = c->rec.sig;
+    r.coef = c->rec.coef;
     const int blocks = c->tw.ledger_blocks;
-    if (c->fp32) {
-        if (c->nabs == 1) k_transport<float, 1><<<blocks, kThreads, 0, c->stream>>>(a);
-        else k_transport<float, 4><<<blocks, kThreads, 0, c->stream>>>(a);
-    } else {
-        if (c->nabs == 1) k_transport<double, 1><<<blocks, kThreads, 0, c->stream>>>(a);
-        else k_transport<double, 4><<<blocks, kThreads, 0, c->stream>>>(a);
+    for (long long ip0 = 0; ip0 < a.np; ip0 += r.cap) {
+        const long long n = a.np - ip0 < r.cap ? a.np - ip0 : r.cap;
+        const int lb = grid_blocks(n, kThreads, 1 << 30);
+        const int acc = ip0 > 0;
+        if (c->fp32) {
+            k_launch<float><<<lb, kThreads, 0, c->stream>>>(a, r, ip0, n);
+            if (c->nabs == 1) k_walk_edge<float, 1><<<blocks, kThreads, 0, c->stream>>>(a, r, n, acc);
+            else k_walk_edge<float, 4><<<blocks, kThreads, 0, c->stream>>>(a, r, n, acc);
+        } else {
+            k_launch<double><<<lb, kThreads, 0, c->stream>>>(a, r, ip0, n);
+            if (c->nabs == 1) k_walk_edge<double, 1><<<blocks, kThreads, 0, c->stream>>>(a, r, n, acc);
+            else k_walk_edge<double, 4><<<blocks, kThreads, 0, c->stream>>>(a, r, n, acc);
+        }
     }
     return cudaGetLastError();
 }

@@ -122,7 +122,11 @@ def test_fp64_pass_matches_oracle(orc):
     assert abs(st.energy_emitted - e[0]) <= 1e-13 * e[0]
     assert abs(st.energy_absorbed - e[1]) <= 1e-9 * e[0]
     assert st.closure <= 5e-13
-    assert abs(st.direct_segments - segs[0]) <= 2
+    # scored-segment counts: the device scores the path per unit luminosity,
+    # so a segment whose attenuated weight underflows to zero (expo ~ 1e-320
+    # past tau ~ 740) is not counted there but is counted by the oracle,
+    # whose path carries the 1e32 erg/s packet luminosity
+    assert abs(st.direct_segments - segs[0]) <= 5e-3 * segs[0]
     neb.close()
 
 
