@@ -208,6 +208,7 @@ def main():
     par = parse_namelist(configs.stromgren64(nphotons=NPHOT, n=GRID, seed=12345 + rank))
     neb = Nebula(par)
     prep_iters = converged_state(neb)
+    tuning = neb.autotune(1 << 18)   # launch shape for this grid / precision / device
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
     for _ in range(args.warmup):
         neb.ionizing_field_and_rates()
@@ -307,6 +308,7 @@ def main():
             "config": {"workload": WORKLOAD, "grid": f"{GRID}^3", "packets_per_step": NPHOT,
                        "precision": "fp64", "state": f"converged Stromgren sphere ({prep_iters} prep iterations)",
                        "l2": "flushed between steps (256 MiB write)",
+                       "tuning": tuning,
                        "parallelism": "replicas" if world > 1 else "single"},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 8 * nleaf,
                     "d2h_bytes_per_step": 16 * nleaf},

@@ -138,6 +138,13 @@ typedef struct mochii_metrics {
     double kernel_ms;
 } mochii_metrics;
 
+/* Launch shapes of the transport walk (the autotuner's choice). */
+typedef struct mochii_tuning {
+    int lookahead;           /* cells the DDA stepper runs ahead of the scoring, 0..2 */
+    int walk_blocks_per_sm;  /* persistent walk grid: SMs x this, 128-thread blocks  */
+    double best_ms;          /* device time of the winning trial pass (autotune)     */
+} mochii_tuning;
+
 typedef struct mochii_ctx mochii_ctx;
 
 /* ---- parameters: read_input, setup.f90:11-35 ----------------------------- */
@@ -175,6 +182,15 @@ int mochii_transport_pass(mochii_ctx* ctx, int with_peel, mochii_pass_stats* sta
 int mochii_balance_update(mochii_ctx* ctx, int solve_te, mochii_metrics* m);
 /* gas_opacity_fill: refresh the per-leaf absorber columns the transport reads. */
 int mochii_opacity_fill(mochii_ctx* ctx);
+
+/* ---- autotuner: packet-block and look-ahead shapes ---------------------- */
+/* Time trial transport passes of sample_packets packets on the current
+ * state for every walk variant and keep the fastest; the choice is cached
+ * per (grid shape, precision, absorber set, device) for the process.  The
+ * trial passes overwrite the tallies, so call it before a pass. */
+int mochii_autotune(mochii_ctx* ctx, int64_t sample_packets, mochii_tuning* out);
+int mochii_set_tuning(mochii_ctx* ctx, const mochii_tuning* t);
+int mochii_get_tuning(const mochii_ctx* ctx, mochii_tuning* out);
 
 /* ---- state exchange (host buffers; sizes in elements) ---------------------- */
 int64_t mochii_nleaf(const mochii_ctx* ctx);

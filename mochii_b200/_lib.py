@@ -67,6 +67,10 @@ class Metrics(C.Structure):
                 ("cells_solved", C.c_int64), ("fixed_point_cap_hits", C.c_int64), ("kernel_ms", C.c_double)]
 
 
+class Tuning(C.Structure):
+    _fields_ = [("lookahead", C.c_int), ("walk_blocks_per_sm", C.c_int), ("best_ms", C.c_double)]
+
+
 # Every symbol the header declares, with its ctypes signature.
 _P = C.POINTER
 SIGNATURES = {
@@ -91,6 +95,9 @@ SIGNATURES = {
     "mochii_sobol_uniforms": (C.c_int, [C.c_int, C.c_int, C.c_int64, C.c_int64, C.c_int, C.c_void_p]),
     "mochii_walk_leaves": (C.c_int, [C.c_void_p, C.c_int64, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]),
     "mochii_launch_records": (C.c_int, [C.c_void_p, C.c_int64, C.c_int64, C.c_void_p]),
+    "mochii_autotune": (C.c_int, [C.c_void_p, C.c_int64, _P(Tuning)]),
+    "mochii_set_tuning": (C.c_int, [C.c_void_p, _P(Tuning)]),
+    "mochii_get_tuning": (C.c_int, [C.c_void_p, _P(Tuning)]),
 }
 
 _lib = None

@@ -6,6 +6,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <map>
 #include <string>
 #include <vector>
 
@@ -381,6 +382,82 @@ extern "C" int mochii_opacity_fill(mochii_ctx* c) {
     CK(c, launch_columns(c));
     CK(c, cudaStreamSynchronize(c->stream));
     c->columns_fresh = true;
+    return MOCHII_OK;
+}
+
+namespace {
+std::map<std::string, Tuning>& tune_cache() {
+    static std::map<std::string, Tuning> m;
+    return m;
+}
+std::string tune_key(const mochii_ctx* c) {
+    cudaDeviceProp prop;
+    cudaGetDeviceProperties(&prop, c->device);
+    char buf[256];
+    std::snprintf(buf, sizeof(buf), "%s|%dx%dx%d|%d|%d|%d", prop.name, c->grid.nx, c->grid.ny, c->grid.nz,
+                  c->fp32 ? 32 : 64, c->nabs, c->nnu);
+    return buf;
+}
+}  // namespace
+
+extern "C" int mochii_set_tuning(mochii_ctx* c, const mochii_tuning* t) {
+    if (!c || !t || t->lookahead < 0 || t->lookahead > 2 || t->walk_blocks_per_sm < 1 || t->walk_blocks_per_sm > 64)
+        return fail(c, MOCHII_ERR_BAD_PARAM, "tuning out of range (lookahead 0..2, blocks per SM 1..64)");
+    c->tune.lookahead = t->lookahead;
+    c->tune.walk_blocks_per_sm = t->walk_blocks_per_sm;
+    const int nb = transport_blocks(c);
+    if (nb > c->tw.ledger_blocks) {
+        cudaFree(c->tw.ledger);
+        c->tw.ledger = nullptr;
+        CK(c, dalloc(&c->tw.ledger, 3 * (size_t)nb));
+    }
+    c->tw.ledger_blocks = nb;
+    return MOCHII_OK;
+}
+
+extern "C" int mochii_get_tuning(const mochii_ctx* c, mochii_tuning* t) {
+    if (!c || !t) return MOCHII_ERR_BAD_PARAM;
+    t->lookahead = c->tune.lookahead;
+    t->walk_blocks_per_sm = c->tune.walk_blocks_per_sm;
+    t->best_ms = c->tune.best_ms;
+    return MOCHII_OK;
+}
+
+extern "C" int mochii_autotune(mochii_ctx* c, int64_t sample, mochii_tuning* out) {
+    if (!c || sample < 1) return MOCHII_ERR_BAD_PARAM;
+    const std::string key = tune_key(c);
+    auto it = tune_cache().find(key);
+    if (it != tune_cache().end()) {
+        c->tune = it->second;
+        mochii_tuning t{c->tune.lookahead, c->tune.walk_blocks_per_sm, c->tune.best_ms};
+        int rc = mochii_set_tuning(c, &t);
+        if (out) *out = t;
+        return rc;
+    }
+    const int64_t keep = c->par.nphotons;
+    int rc = mochii_set_nphotons(c, std::min<int64_t>(sample, keep));
+    if (rc) return rc;
+    double best = 1e300;
+    mochii_tuning bt{2, 8, 0.0};
+    for (int la = 0; la <= 2; ++la)
+        for (int bps : {4, 8, 16, 32}) {
+            mochii_tuning t{la, bps, 0.0};
+            if ((rc = mochii_set_tuning(c, &t))) return rc;
+            double ms = 0.0;
+            for (int rep = 0; rep < 3; ++rep) {
+                mochii_pass_stats st;
+                if ((rc = mochii_transport_pass(c, 0, &st))) return rc;
+                if (rep > 0) ms += st.kernel_ms;   // first pass warms the variant
+            }
+            if (ms < best) { best = ms; bt = t; }
+        }
+    bt.best_ms = best / 2.0;
+    if ((rc = mochii_set_tuning(c, &bt))) return rc;
+    c->tune.best_ms = bt.best_ms;
+    c->tune.tuned = true;
+    tune_cache()[key] = c->tune;
+    if ((rc = mochii_set_nphotons(c, keep))) return rc;
+    if (out) *out = bt;
     return MOCHII_OK;
 }
 

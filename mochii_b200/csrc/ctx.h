@@ -55,6 +55,14 @@ struct RecordBuffers {
     long long cap = 0;
 };
 
+// Launch shapes chosen by the autotuner (tune.cu) or set by hand.
+struct Tuning {
+    int lookahead = 2;            // walk look-ahead depth 0..2
+    int walk_blocks_per_sm = 8;   // persistent walk grid = SMs x this, 128-thread blocks
+    bool tuned = false;
+    double best_ms = 0.0;
+};
+
 struct BalanceWork {
     double* partial = nullptr;   // per block: max_dx, max_dte, sum_dxv, sum_xv, sum_dtv, sum_tv
     unsigned long long* counters = nullptr;
@@ -82,6 +90,7 @@ struct mochii_ctx {
     mochii::DeviceTables tab;
     mochii::TransportWork tw;
     mochii::RecordBuffers rec;
+    mochii::Tuning tune;
     mochii::BalanceWork bw;
     std::string last_error;
 };

@@ -227,14 +227,67 @@ __global__ void __launch_bounds__(kThreads) k_launch(const PassArgs a, Records r
     rec.bits[i] = bits;
 }
 
+// Absorber columns of one leaf, loaded ahead of use.
+template <typename R, int NABS> struct Col;
+template <typename R> struct Col<R, 1> {
+    R c0;
+    __device__ __forceinline__ void load(const void* col, int il) { c0 = __ldg(static_cast<const R*>(col) + il); }
+    __device__ __forceinline__ R kappa(R s0, R, R) const { return c0 * s0; }
+};
+template <> struct Col<float, 4> {
+    float4 c;
+    __device__ __forceinline__ void load(const void* col, int il) { c = __ldg(static_cast<const float4*>(col) + il); }
+    __device__ __forceinline__ float kappa(float s0, float s1, float s2) const { return c.x * s0 + (c.y * s1 + c.z * s2); }
+};
+template <> struct Col<double, 4> {
+    double2 a;
+    double b;
+    __device__ __forceinline__ void load(const void* col, int il) {
+        const double2* p = static_cast<const double2*>(col) + 2 * (long long)il;
+        a = __ldg(p);
+        b = __ldg(reinterpret_cast<const double*>(p + 1));
+    }
+    __device__ __forceinline__ double kappa(double s0, double s1, double s2) const {
+        return a.x * s0 + (a.y * s1 + b * s2);
+    }
+};
+
+// Amanatides-Woo cell stepper (raytrace_amr.f90:553-590): emits the current
+// cell and its segment length, then steps to the neighbour across the
+// nearest face (minloc first-minimum tie rule).  Pure FP64 geometry, so it
+// runs ahead of the opacity work and the column loads of upcoming cells are
+// in flight while the current cell is scored.
+struct Stepper {
+    double t0, t1, t2, d0, d1, d2, t_cur;
+    int ix, iy, iz, sx, sy, sz;
+    __device__ __forceinline__ bool emit(int nx, int ny, int nz, int* il, double* seg) {
+        *il = ix + nx * (iy + ny * iz);
+        int ax = 0;
+        double tm = t0;
+        if (t1 < tm) { ax = 1; tm = t1; }
+        if (t2 < tm) { ax = 2; tm = t2; }
+        *seg = tm - t_cur;
+        t_cur = tm;
+        t0 = ax == 0 ? t0 + d0 : t0;
+        t1 = ax == 1 ? t1 + d1 : t1;
+        t2 = ax == 2 ? t2 + d2 : t2;
+        ix += ax == 0 ? sx : 0;
+        iy += ax == 1 ? sy : 0;
+        iz += ax == 2 ? sz : 0;
+        return ix >= 0 && ix < nx && iy >= 0 && iy < ny && iz >= 0 && iz < nz;   // next cell inside?
+    }
+};
+
 // Walk kernel: raytrace_ion_to_edge_car (raytrace_amr.f90:534-592) for the
-// packets of one chunk, grid-stride, the DDA state held in registers.
-template <typename R, int NABS>
-__global__ void __launch_bounds__(kThreads) k_walk_edge(const PassArgs a, const Records rec, long long n,
-                                                        int accumulate) {
+// packets of one chunk, grid-stride.  The stepper runs LA cells ahead of the
+// scoring: slot 0 is scored now, slots 1..LA have their column loads in
+// flight (LA = 0 disables the look-ahead).
+template <typename R, int NABS, int LA>
+__global__ void __launch_bounds__(128) k_walk_edge(const PassArgs a, const Records rec, long long n,
+                                                   int accumulate) {
     typedef typename Acc<R>::T T;
     constexpr int NT = NABS == 1 ? 2 : 6;
-    __shared__ double sh[kThreads];
+    __shared__ double sh[128];
     double emitted = 0.0, absorbed = 0.0, escaped = 0.0;
     unsigned long long nseg = 0, kills = 0;
     T* tal = static_cast<T*>(a.tally);
@@ -245,11 +298,13 @@ __global__ void __launch_bounds__(kThreads) k_walk_edge(const PassArgs a, const 
     const long long stride = (long long)gridDim.x * blockDim.x;
     const int nx = a.n[0], ny = a.n[1], nz = a.n[2];
     for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
-        double t0 = rec.tm[i], t1 = rec.tm[c + i], t2 = rec.tm[2 * c + i];
-        const double d0 = rec.td[i], d1 = rec.td[c + i], d2 = rec.td[2 * c + i];
+        Stepper g;
+        g.t0 = rec.tm[i]; g.t1 = rec.tm[c + i]; g.t2 = rec.tm[2 * c + i];
+        g.d0 = rec.td[i]; g.d1 = rec.td[c + i]; g.d2 = rec.td[2 * c + i];
+        g.t_cur = 0.0;
         const int cell = rec.cell[i], bits = rec.bits[i];
-        int ix = cell & 1023, iy = (cell >> 10) & 1023, iz = (cell >> 20) & 1023;
-        const int sx = ((bits >> 16) & 3) - 1, sy = ((bits >> 18) & 3) - 1, sz = ((bits >> 20) & 3) - 1;
+        g.ix = cell & 1023; g.iy = (cell >> 10) & 1023; g.iz = (cell >> 20) & 1023;
+        g.sx = ((bits >> 16) & 3) - 1; g.sy = ((bits >> 18) & 3) - 1; g.sz = ((bits >> 20) & 3) - 1;
         const int inu = bits & 0xFFFF;
         const R s0 = sg[i];
         const R s1 = NABS == 1 ? (R)0 : sg[c + i];
@@ -257,45 +312,56 @@ __global__ void __launch_bounds__(kThreads) k_walk_edge(const PassArgs a, const 
         R cf[NT];
 #pragma unroll
         for (int k = 0; k < NT; ++k) cf[k] = cfp[k * c + i];
+        // ring of LA+1 cells: il, segment, columns, and whether a next cell exists
+        int il[LA + 1] = {};
+        double sgm[LA + 1] = {};
+        Col<R, NABS> cl[LA + 1];
+        bool more[LA + 1];
+        more[0] = g.emit(nx, ny, nz, &il[0], &sgm[0]);
+        cl[0].load(a.col, il[0]);
+#pragma unroll
+        for (int k = 1; k <= LA; ++k) {
+            more[k] = false;
+            if (more[k - 1]) {
+                more[k] = g.emit(nx, ny, nz, &il[k], &sgm[k]);
+                cl[k].load(a.col, il[k]);
+            }
+        }
         R expo = (R)1.0;
-        double tau = 0.0, t_cur = 0.0;
+        double tau = 0.0;
         int nstep = 0;
         for (;;) {
             if (++nstep > kMaxWalkSteps) { ++kills; break; }
-            const long long il = (long long)ix + (long long)nx * ((long long)iy + (long long)ny * iz);
-            // minloc(tmax): first minimum
-            int ax = 0;
-            double tm = t0;
-            if (t1 < tm) { ax = 1; tm = t1; }
-            if (t2 < tm) { ax = 2; tm = t2; }
-            const double seg = tm - t_cur;
-            const R kap = opacity<R, NABS>(a.col, il, s0, s1, s2);
-            const R ks = kap * (R)seg;
+            const R kap = cl[0].kappa(s0, s1, s2);
+            const R ks = kap * (R)sgm[0];
             R w;
             if (ks > (R)0) {
                 const R eo = expo * attenuation(ks);
                 w = (expo - eo) / kap;
                 expo = eo;
             } else {
-                w = expo * (R)seg;
+                w = expo * (R)sgm[0];
             }
             if (w != (R)0) {   // score_ion_path returns on a zero path (ion_score_mod.f90:148)
                 ++nseg;
-                T* tl = tal + il * NT;
+                T* tl = tal + (long long)il[0] * NT;
 #pragma unroll
                 for (int k = 0; k < NT; ++k) tally_add(tl + k, w * cf[k]);
-                tally_add(jt + il * a.nnu + inu, w);
+                tally_add(jt + (long long)il[0] * a.nnu + inu, w);
             }
             tau = tau + (double)ks;
             if (tau >= kTauHuge) break;
-            t_cur = tm;
-            t0 = ax == 0 ? t0 + d0 : t0;
-            t1 = ax == 1 ? t1 + d1 : t1;
-            t2 = ax == 2 ? t2 + d2 : t2;
-            ix += ax == 0 ? sx : 0;
-            iy += ax == 1 ? sy : 0;
-            iz += ax == 2 ? sz : 0;
-            if (ix < 0 || ix >= nx || iy < 0 || iy >= ny || iz < 0 || iz >= nz) break;
+            if (!more[0]) break;   // the scored cell was the last one inside the grid
+#pragma unroll
+            for (int k = 0; k < LA; ++k) {
+                il[k] = il[k + 1]; sgm[k] = sgm[k + 1]; cl[k] = cl[k + 1]; more[k] = more[k + 1];
+            }
+            if (LA == 0 || more[LA - (LA > 0)]) {
+                more[LA] = g.emit(nx, ny, nz, &il[LA], &sgm[LA]);
+                cl[LA].load(a.col, il[LA]);
+            } else {
+                more[LA] = false;
+            }
         }
         // ion_score_energy_packet (ion_score_mod.f90:233-252)
         const double lum = a.Lpacket;
@@ -470,7 +536,26 @@ int grid_blocks(long long work, int threads, int cap) {
 int transport_blocks(const mochii_ctx* c) {
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device);
-    return grid_blocks(c->par.nphotons, kThreads, sms * 8);
+    const int per_sm = c->tune.walk_blocks_per_sm > 0 ? c->tune.walk_blocks_per_sm : 8;
+    return grid_blocks(c->par.nphotons, 128, sms * per_sm);
+}
+
+// Walk-kernel variants: look-ahead depth 0..2 (the autotuned choice is
+// c->tune.lookahead); 128-thread blocks.
+template <typename R, int NABS>
+cudaError_t walk_la(mochii_ctx* c, const PassArgs& a, const Records& r, long long n, int acc, int blocks) {
+    switch (c->tune.lookahead) {
+        case 0: k_walk_edge<R, NABS, 0><<<blocks, 128, 0, c->stream>>>(a, r, n, acc); break;
+        case 1: k_walk_edge<R, NABS, 1><<<blocks, 128, 0, c->stream>>>(a, r, n, acc); break;
+        default: k_walk_edge<R, NABS, 2><<<blocks, 128, 0, c->stream>>>(a, r, n, acc); break;
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_walk_variant(mochii_ctx* c, const PassArgs& a, const Records& r, long long n, int acc,
+                                int blocks) {
+    if (c->fp32) return c->nabs == 1 ? walk_la<float, 1>(c, a, r, n, acc, blocks) : walk_la<float, 4>(c, a, r, n, acc, blocks);
+    return c->nabs == 1 ? walk_la<double, 1>(c, a, r, n, acc, blocks) : walk_la<double, 4>(c, a, r, n, acc, blocks);
 }
 
 cudaError_t launch_transport(mochii_ctx* c) {
@@ -488,15 +573,10 @@ cudaError_t launch_transport(mochii_ctx* c) {
         const long long n = a.np - ip0 < r.cap ? a.np - ip0 : r.cap;
         const int lb = grid_blocks(n, kThreads, 1 << 30);
         const int acc = ip0 > 0;
-        if (c->fp32) {
-            k_launch<float><<<lb, kThreads, 0, c->stream>>>(a, r, ip0, n);
-            if (c->nabs == 1) k_walk_edge<float, 1><<<blocks, kThreads, 0, c->stream>>>(a, r, n, acc);
-            else k_walk_edge<float, 4><<<blocks, kThreads, 0, c->stream>>>(a, r, n, acc);
-        } else {
-            k_launch<double><<<lb, kThreads, 0, c->stream>>>(a, r, ip0, n);
-            if (c->nabs == 1) k_walk_edge<double, 1><<<blocks, kThreads, 0, c->stream>>>(a, r, n, acc);
-            else k_walk_edge<double, 4><<<blocks, kThreads, 0, c->stream>>>(a, r, n, acc);
-        }
+        if (c->fp32) k_launch<float><<<lb, kThreads, 0, c->stream>>>(a, r, ip0, n);
+        else k_launch<double><<<lb, kThreads, 0, c->stream>>>(a, r, ip0, n);
+        const cudaError_t e = launch_walk_variant(c, a, r, n, acc, blocks);
+        if (e != cudaSuccess) return e;
     }
     return cudaGetLastError();
 }

@@ -15,7 +15,7 @@ import ctypes as C
 import numpy as np
 
 from . import _lib
-from ._lib import Metrics, MochiiError, Params, PassStats
+from ._lib import Metrics, MochiiError, Params, PassStats, Tuning
 
 STATE_FIELDS = ("nH", "x_HI", "x_HeI", "x_HeII", "n_e", "T_e")
 RATE_FIELDS = ("gamma_HI", "gamma_HeI", "gamma_HeII", "heat_HI", "heat_HeI", "heat_HeII")
@@ -146,6 +146,22 @@ class Nebula:
 
     def set_nphotons(self, n):
         self._ok(self.lib.mochii_set_nphotons(self.ctx, int(n)))
+
+    def autotune(self, sample_packets=1 << 18):
+        """Pick the fastest walk launch shape on the current state (tallies are
+        overwritten by the trial passes)."""
+        t = Tuning()
+        self._ok(self.lib.mochii_autotune(self.ctx, int(sample_packets), C.byref(t)))
+        return {"lookahead": t.lookahead, "walk_blocks_per_sm": t.walk_blocks_per_sm, "best_ms": t.best_ms}
+
+    def set_tuning(self, lookahead, walk_blocks_per_sm):
+        t = Tuning(int(lookahead), int(walk_blocks_per_sm), 0.0)
+        self._ok(self.lib.mochii_set_tuning(self.ctx, C.byref(t)))
+
+    def tuning(self):
+        t = Tuning()
+        self._ok(self.lib.mochii_get_tuning(self.ctx, C.byref(t)))
+        return {"lookahead": t.lookahead, "walk_blocks_per_sm": t.walk_blocks_per_sm, "best_ms": t.best_ms}
 
     @property
     def ion_Ltot(self):

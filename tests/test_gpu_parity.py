@@ -177,6 +177,30 @@ def test_balance_matches_oracle_after_iterations(orc):
     neb.close()
 
 
+def test_walk_variants_agree_and_autotune_picks_one(orc):
+    n = 32
+    nl = small_nl(n=n, nphot=30000)
+    L = parse_namelist(nl).xmax
+    neb = Nebula(parse_namelist(nl))
+    state = partially_ionised_state(n, L)
+    neb.set("x_HI", state["x_HI"])
+    neb.gas_opacity_fill()
+    ref = None
+    for la in (0, 1, 2):
+        for bps in (1, 4, 16):
+            neb.set_tuning(la, bps)
+            st = neb.ionizing_field_and_rates()
+            g = neb.get("gamma_HI")
+            if ref is None:
+                ref, segs = g, st.direct_segments
+            np.testing.assert_allclose(g, ref, rtol=1e-12, atol=0)
+            assert st.direct_segments == segs
+    t = neb.autotune(20000)
+    assert t["lookahead"] in (0, 1, 2) and t["walk_blocks_per_sm"] in (4, 8, 16, 32) and t["best_ms"] > 0
+    assert neb.tuning()["lookahead"] == t["lookahead"]
+    neb.close()
+
+
 def test_pass_is_deterministic_in_tallies():
     nl = small_nl(n=16, nphot=10000)
     neb = Nebula(parse_namelist(nl))
