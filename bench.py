@@ -184,6 +184,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="mochii_b200")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32"],
+                    help="transport arithmetic (the workload is defined in fp64)")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
@@ -205,7 +207,7 @@ def main():
     if dist is not None:
         dist.barrier()
 
-    par = parse_namelist(configs.stromgren64(nphotons=NPHOT, n=GRID, seed=12345 + rank))
+    par = parse_namelist(configs.stromgren64(nphotons=NPHOT, n=GRID, seed=12345 + rank, precision=args.precision))
     neb = Nebula(par)
     prep_iters = converged_state(neb)
     tuning = neb.autotune(1 << 18)   # launch shape for this grid / precision / device
@@ -304,9 +306,9 @@ def main():
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "grid": f"{GRID}^3", "packets_per_step": NPHOT,
-                       "precision": "fp64", "state": f"converged Stromgren sphere ({prep_iters} prep iterations)",
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f32+f64",
+            "data": "synthetic", "config": {"workload": WORKLOAD, "grid": f"{GRID}^3", "packets_per_step": NPHOT,
+                       "precision": args.precision, "state": f"converged Stromgren sphere ({prep_iters} prep iterations)",
                        "l2": "flushed between steps (256 MiB write)",
                        "tuning": tuning,
                        "parallelism": "replicas" if world > 1 else "single"},
