@@ -18,7 +18,7 @@ CSRC = os.path.join(HERE, "csrc")
 INCLUDE = os.path.join(ROOT, "include")
 LIB = os.path.join(HERE, "libmochii_gpu.so")
 
-SOURCES = ["api.cu", "transport.cu", "balance.cu", "band.cpp", "params.cpp"]
+SOURCES = ["api.cu", "transport.cu", "balance.cu", "band.cpp", "params.cpp", "thermal_setup.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 
@@ -57,7 +57,7 @@ def build(force=False, verbose=False):
         subprocess.run(cmd, check=True)
         objs.append(obj)
     tmp = LIB + ".tmp"
-    cmd = [nvcc, "-shared", "-o", tmp] + objs + ARCH + ["-ccbin", hostcxx, "-lcudart"]
+    cmd = [nvcc, "-shared", "-o", tmp] + objs + ARCH + ["-ccbin", hostcxx, "-lcudart", "-ldl"]
     subprocess.run(cmd, check=True)
     os.replace(tmp, LIB)
     return LIB

@@ -14,6 +14,9 @@ configurations are the workloads.
                 segments with compensated FP32 tallies.
 """
 import math
+import os
+
+ATOMIC_DIR = os.path.join(os.path.dirname(os.path.abspath(__file__)), "data", "atomic")
 
 PC2CM = 3.0856776e18
 KB_CGS = 1.380649e-16
@@ -78,6 +81,39 @@ def stromgren64(nphotons=1_000_000, niter=10, n=64, precision="fp64", seed=12345
  par%ion_relax = 1.0
  par%gas_niter = {niter}
  par%gas_tol = 1.0e-3
+ par%precision = '{precision}'
+/
+"""
+
+
+def hii_thermal(nphotons=10_000_000, niter=20, n=128, precision="fp32", seed=12345, rs_factor=1.0):
+    """H+He H II region with the thermal balance (the 128^3, n_H = 100,
+    He/H 0.1, 45 kK, Q(H) = 5e49 s^-1, case A workload with T_e solved in
+    [3e3, 3e4] K; the metals and the diffuse packets are separate rows)."""
+    rs = stromgren_radius_pc(Q=5.0e49) * rs_factor
+    return f"""&parameters
+ par%no_photons = {float(nphotons):.6e}
+ par%launch_sequence = 'sobol'
+ par%qmc_seed = {seed}
+ par%grid_type = 'car'
+ par%nx = {n}
+ par%ny = {n}
+ par%nz = {n}
+ par%xmax = {rs:.10f}
+ par%ymax = {rs:.10f}
+ par%zmax = {rs:.10f}
+ par%distance_unit = 'pc'
+ par%nH_const = 100.0
+ par%He_abund = 0.1
+ par%tstar = 4.5e4
+ par%luminosity = {5.0e49 * mean_photon_energy_ev(4.5e4) * EV2ERG:.6e}
+ par%case_ab = 'A'
+ par%solve_te = .true.
+ par%te_min = 3.0e3
+ par%te_max = 3.0e4
+ par%te_fixed = 1.0e4
+ par%gas_niter = {niter}
+ par%atomic_dir = '{ATOMIC_DIR}'
  par%precision = '{precision}'
 /
 """

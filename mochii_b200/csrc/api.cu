@@ -15,6 +15,7 @@
 #include "mochii_gpu.h"
 #include "physics.cuh"
 #include "qmc.cuh"
+#include "thermal.h"
 #include "transport.h"
 
 using namespace mochii;
@@ -45,7 +46,8 @@ void release(mochii_ctx* c) {
     void* ptrs[] = {c->nH, c->xHI, c->xHeI, c->xHeII, c->ne, c->Te, c->col, c->tally, c->jt, c->rates,
                     c->tab.tab_e, c->tab.tab_f, c->tab.tab_c, c->tab.tab_off, c->tab.comp, c->tab.eedge,
                     c->tab.qmc, c->tw.ledger, c->tw.counters, c->bw.partial, c->bw.counters,
-                    c->rec.tm, c->rec.td, c->rec.cell, c->rec.bits, c->rec.sig, c->rec.coef};
+                    c->rec.tm, c->rec.td, c->rec.cell, c->rec.bits, c->rec.sig, c->rec.coef,
+                    c->th.gff, c->th.lamref, c->th.Ssup, c->th.tinv};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     for (cudaEvent_t e : {c->ev0, c->ev1, c->evA, c->evB})
@@ -67,6 +69,7 @@ int validate(const mochii_params& p, std::string* why, int* code) {
     }
     if (p.ion_relax <= 0.0 || p.ion_relax > 1.0) return *why = "par%ion_relax must lie in (0, 1]", 1;
     if (p.te_fixed <= 0.0) return *why = "par%te_fixed must be positive", 1;
+    if (p.solve_te && !(p.te_min > 0.0 && p.te_max > p.te_min)) return *why = "need 0 < par%te_min < par%te_max", 1;
     if (p.He_abund < 0.0) return *why = "par%He_abund must be >= 0", 1;
     *code = MOCHII_ERR_UNSUPPORTED;
     if (!p.grid_car) return *why = "grid_type='amr' (octree leaf list) is not built in this library version", 1;
@@ -239,6 +242,29 @@ extern "C" int mochii_init(const mochii_params* pin, mochii_ctx** out) {
     CKI(cudaMalloc(&c->rec.sig, 3 * (size_t)c->rec.cap * rsz + 64));
     CKI(cudaMalloc(&c->rec.coef, 6 * (size_t)c->rec.cap * rsz + 64));
     c->bw.blocks = balance_blocks(c);
+    if (p.solve_te) {
+        ThermalHost th;
+        if (!thermal_tables_build(p, th, &why)) {
+            c->last_error = why;
+            return bail(MOCHII_ERR_TABLE);
+        }
+        std::vector<double> tinv(kNlNT);
+        for (int i = 0; i < kNlNT; ++i) tinv[i] = 1.0 / std::pow(10.0, 2.0 + 0.01 * (double)i);
+        CKI(dalloc(&c->th.gff, (size_t)kGffNT * kGffNZ));
+        CKI(cudaMemcpy(c->th.gff, th.gff, sizeof(th.gff), cudaMemcpyHostToDevice));
+        CKI(dalloc(&c->th.tinv, (size_t)kNlNT));
+        CKI(cudaMemcpy(c->th.tinv, tinv.data(), kNlNT * 8, cudaMemcpyHostToDevice));
+        c->th.hi_nterm = th.hi_nterm;
+        for (int i = 0; i < th.hi_nterm; ++i) { c->th.hi_A[i] = th.hi_A[i]; c->th.hi_T[i] = th.hi_T[i]; }
+        c->th.use_hi_table = th.use_hi_table ? 1 : 0;
+        if (th.use_hi_table) {
+            CKI(dalloc(&c->th.lamref, (size_t)kNlNT));
+            CKI(dalloc(&c->th.Ssup, (size_t)kNlNT * kNlNNE));
+            CKI(cudaMemcpy(c->th.lamref, th.hi_lamref.data(), kNlNT * 8, cudaMemcpyHostToDevice));
+            CKI(cudaMemcpy(c->th.Ssup, th.hi_Ssup.data(), (size_t)kNlNT * kNlNNE * 8, cudaMemcpyHostToDevice));
+        }
+        c->thermal_ready = true;
+    }
     CKI(dalloc(&c->bw.partial, 6 * (size_t)c->bw.blocks));
     CKI(dalloc(&c->bw.counters, 4));
     CKI(launch_columns(c));
@@ -342,34 +368,49 @@ extern "C" int mochii_transport_pass(mochii_ctx* c, int with_peel, mochii_pass_s
 // (thermal_mod.f90:124).
 extern "C" int mochii_balance_update(mochii_ctx* c, int solve_te, mochii_metrics* m) {
     if (!c) return MOCHII_ERR_BAD_PARAM;
-    if (solve_te) return fail(c, MOCHII_ERR_UNSUPPORTED, "the thermal solve is not built in this library version");
+    if (solve_te && !c->thermal_ready)
+        return fail(c, MOCHII_ERR_BAD_PARAM, "the thermal solve needs par%solve_te = .true. at mochii_init (tables)");
     CK(c, cudaMemsetAsync(c->bw.counters, 0, 4 * sizeof(unsigned long long), c->stream));
     CK(c, cudaEventRecord(c->ev0, c->stream));
-    CK(c, launch_balance(c));
+    if (solve_te) CK(c, launch_thermal(c));
+    else CK(c, launch_balance(c));
     CK(c, cudaEventRecord(c->ev1, c->stream));
-    c->columns_fresh = true;   // the balance kernel refreshes the columns it changes
-    std::vector<double> part(3 * (size_t)c->bw.blocks);
+    c->columns_fresh = true;   // both kernels refresh the columns they change
+    const int np = solve_te ? 6 : 3;
+    std::vector<double> part((size_t)np * c->bw.blocks);
     unsigned long long cnt[4];
     CK(c, cudaMemcpyAsync(part.data(), c->bw.partial, part.size() * 8, cudaMemcpyDeviceToHost, c->stream));
     CK(c, cudaMemcpyAsync(cnt, c->bw.counters, sizeof(cnt), cudaMemcpyDeviceToHost, c->stream));
     CK(c, cudaStreamSynchronize(c->stream));
     float ms = 0.0f;
     cudaEventElapsedTime(&ms, c->ev0, c->ev1);
-    double mdx = 0.0, sdx = 0.0, sx = 0.0;
-    for (int b = 0; b < c->bw.blocks; ++b) {
-        mdx = std::max(mdx, part[3 * (size_t)b]);
-        sdx += part[3 * (size_t)b + 1];
-        sx += part[3 * (size_t)b + 2];
-    }
     mochii_metrics r;
     std::memset(&r, 0, sizeof(r));
-    r.max_dx = mdx;
-    r.dx_vol = sdx / std::max(sx, kTinest);
+    if (solve_te) {
+        double s[4] = {0, 0, 0, 0};
+        for (int b = 0; b < c->bw.blocks; ++b) {
+            const double* q = &part[6 * (size_t)b];
+            r.max_dx = std::max(r.max_dx, q[0]);
+            r.max_dte = std::max(r.max_dte, q[1]);
+            for (int k = 0; k < 4; ++k) s[k] += q[2 + k];
+        }
+        r.dx_vol = s[0] / std::max(s[1], kTinest);    // thermal_mod.f90:223-224
+        r.dte_vol = s[2] / std::max(s[3], kTinest);
+    } else {
+        double sdx = 0.0, sx = 0.0;
+        for (int b = 0; b < c->bw.blocks; ++b) {
+            r.max_dx = std::max(r.max_dx, part[3 * (size_t)b]);
+            sdx += part[3 * (size_t)b + 1];
+            sx += part[3 * (size_t)b + 2];
+        }
+        r.dx_vol = sdx / std::max(sx, kTinest);
+    }
     r.cells_solved = (int64_t)cnt[0];
     r.fixed_point_cap_hits = (int64_t)cnt[1];
     r.kernel_ms = ms;
     if (m) *m = r;
-    if (!std::isfinite(mdx) || !std::isfinite(sdx)) return fail(c, MOCHII_ERR_NONFINITE, "non-finite state after the solve");
+    if (!std::isfinite(r.max_dx) || !std::isfinite(r.dx_vol) || !std::isfinite(r.max_dte))
+        return fail(c, MOCHII_ERR_NONFINITE, "non-finite state after the solve");
     return MOCHII_OK;
 }
 

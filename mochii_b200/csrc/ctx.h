@@ -9,6 +9,7 @@
 #include "band.h"
 #include "mochii_gpu.h"
 #include "qmc.cuh"
+#include "thermal.h"
 
 namespace mochii {
 
@@ -91,6 +92,8 @@ struct mochii_ctx {
     mochii::TransportWork tw;
     mochii::RecordBuffers rec;
     mochii::Tuning tune;
+    mochii::ThermalDev th;          // thermal tables (solve_te)
+    bool thermal_ready = false;
     mochii::BalanceWork bw;
     std::string last_error;
 };

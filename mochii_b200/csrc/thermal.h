@@ -1,0 +1,50 @@
+// Thermal-balance tables (host build, device layout) and the per-cell
+// cooling evaluation shared by the thermal kernel.
+#pragma once
+#include <string>
+#include <vector>
+
+#include "mochii_gpu.h"
+
+namespace mochii {
+
+constexpr int kGffNT = 41, kGffNZ = 4;      // cooling_mod.f90:61 (log T = 2..6, Z = 1..4)
+constexpr int kNlNT = 401, kNlNNE = 161;    // nlevel_cooling_mod.f90:58 (log T 2..6 by 0.01, log n_e -6..10 by 0.1)
+constexpr int kMaxFitTerms = 8;
+constexpr int kMaxLev = 40;
+
+struct NlevelAtomData {
+    struct Rad { int l, u; double A; };
+    struct Ups { int l, u, type, logf; double C, dE, st_lo, st_hi; std::vector<double> c; };
+    std::vector<double> g, e_cm1;
+    std::vector<Rad> rad;
+    std::vector<Ups> ups;
+    bool load(const std::string& path);
+    static double upsilon(const Ups& u, double T);
+    void cooling_column(double T, const double* ne, int nne, double* out) const;
+};
+
+struct ThermalHost {
+    double gff_logT[kGffNT];
+    double gff[kGffNT * kGffNZ];
+    int hi_nterm = 0;
+    double hi_A[kMaxFitTerms], hi_T[kMaxFitTerms];
+    bool use_hi_table = false;
+    std::vector<double> hi_lamref, hi_Ssup;
+};
+
+// Device copy of the tables (one allocation per array).
+struct ThermalDev {
+    double* gff = nullptr;      // kGffNT x kGffNZ
+    double* lamref = nullptr;   // kNlNT
+    double* Ssup = nullptr;     // kNlNT x kNlNNE
+    double* tinv = nullptr;     // kNlNT: 1 / 10^logT_i
+    double hi_A[kMaxFitTerms], hi_T[kMaxFitTerms];
+    int hi_nterm = 0, use_hi_table = 0;
+};
+
+std::string data_root();
+std::string atomic_dir(const mochii_params& p);
+bool thermal_tables_build(const mochii_params& p, ThermalHost& t, std::string* err);
+
+}  // namespace mochii

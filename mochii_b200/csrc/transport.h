@@ -18,5 +18,6 @@ cudaError_t launch_records(mochii_ctx* c, long long ip0, long long n, double* ou
 int balance_blocks(const mochii_ctx* c);
 cudaError_t launch_columns(mochii_ctx* c);
 cudaError_t launch_balance(mochii_ctx* c);
+cudaError_t launch_thermal(mochii_ctx* c);
 
 }  // namespace mochii

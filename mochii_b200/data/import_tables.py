@@ -1,0 +1,29 @@
+#!/usr/bin/env python3
+"""Copy the physical data tables this path reads from a MoCHII checkout
+(default /root/reference, or argv[1]) into mochii_b200/data/.
+
+  atomic/cooling_<el>_<stage>.txt   collisional line-cooling fits (cooling_mod)
+  atomic/nlevel_<el>_<stage>.txt    n-level atom data (nlevel_mod)
+  atomic/element_<el>.txt           trace-element registry (species_mod)
+  kext_albedo_WD_MW_3.1_60_D03.all_2003   MW R_V = 3.1 grain extinction (gas_opacity_mod)
+
+These are data (CHIANTI / Verner / Weingartner & Draine fits with provenance
+headers), not code; the library loads them at set-up.
+"""
+import glob
+import os
+import shutil
+import sys
+
+SRC = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+DST = os.path.dirname(os.path.abspath(__file__))
+
+os.makedirs(os.path.join(DST, "atomic"), exist_ok=True)
+for pat in ("cooling_*.txt", "nlevel_*.txt", "element_*.txt"):
+    for f in sorted(glob.glob(os.path.join(SRC, "data", "atomic", pat))):
+        if f.endswith("cooling_fit_parameters.txt"):
+            continue
+        shutil.copyfile(f, os.path.join(DST, "atomic", os.path.basename(f)))
+shutil.copyfile(os.path.join(SRC, "data", "kext_albedo_WD_MW_3.1_60_D03.all_2003"),
+                os.path.join(DST, "kext_albedo_WD_MW_3.1_60_D03.all_2003"))
+print("copied", len(os.listdir(os.path.join(DST, "atomic"))), "atomic tables")

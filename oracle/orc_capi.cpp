@@ -3,6 +3,7 @@
 #include <string>
 
 #include "orc_core.h"
+#include "orc_thermal.h"
 
 using namespace orc;
 
@@ -160,6 +161,30 @@ int orc_sim_transport_pass(void* h) {
 int orc_sim_equilibrium_update(void* h, double* metrics2) {
     static_cast<Sim*>(h)->gas_equilibrium_update(&metrics2[0], &metrics2[1]);
     return 0;
+}
+int orc_sim_thermal_update(void* h, double* metrics4) {
+    auto* s = static_cast<Sim*>(h);
+    if (!s->th) return 1;
+    s->gas_thermal_update(metrics4);
+    return 0;
+}
+// Thermal building blocks for the tests.
+void orc_gff_table(double* logT41, double* z164) {
+    GffTable t;
+    t.build();
+    for (int i = 0; i < 41; ++i) {
+        logT41[i] = t.logT[i];
+        for (int k = 0; k < 4; ++k) z164[i * 4 + k] = t.z[i][k];
+    }
+}
+double orc_cooling_total(void* h, double T, double nH, double ne, double xHI, double xHeI, double xHeII) {
+    auto* s = static_cast<Sim*>(h);
+    return cooling_total(*s->th, s->rm, s->par.case_ab == "A", s->par.He_abund, T, nH, ne, xHI, xHeI, xHeII);
+}
+double orc_nlevel_cooling_at(const char* path, double T, double ne) {
+    NlevelAtom a;
+    if (!a.load(path)) return -1.0;
+    return nlevel_cooling_at(a, T, ne);
 }
 // energy ledger (emitted, absorbed, escaped) and segment counts
 void orc_sim_energy(void* h, double* e3, long long* segs2) {

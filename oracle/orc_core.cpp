@@ -1,6 +1,7 @@
 // Oracle (test infrastructure only): FP64 CPU restatement of the MoCHII
 // transport + balance path.  See orc_core.h for the contract.
 #include "orc_core.h"
+#include "orc_thermal.h"
 
 #include <algorithm>
 #include <cctype>
@@ -929,9 +930,13 @@ bool Sim::setup(const std::string& nl, std::string* err) {
         set_err(err, "oracle: only the namelist car grid is restated");
         return false;
     }
-    if (par.use_metals || par.diffuse_field || par.ion_add_dust || par.solve_te || par.use_sec_ion || par.add_fuv) {
-        set_err(err, "oracle: metals/diffuse/dust/thermal/sec_ion/fuv not restated yet");
+    if (par.use_metals || par.diffuse_field || par.ion_add_dust || par.use_sec_ion || par.add_fuv) {
+        set_err(err, "oracle: metals/diffuse/dust/sec_ion/fuv not restated yet");
         return false;
+    }
+    if (par.solve_te) {
+        th = new Thermal();
+        if (!th->setup(par, err)) return false;
     }
     // namelist car grid, grid_mod_amr.f90:64-133,193-198 and octree_mod.f90:648-674
     grid.car = true;
@@ -1212,6 +1217,74 @@ void solve_ion_cell(const RateModel& rm, double yHe, double gH, double gHe1,
         ne = std::max(0.5 * (ne + ne_old), 1.0e-12 * nH);
         if (std::fabs(ne - ne_old) <= 1.0e-10 * ne) break;
     }
+}
+
+Sim::~Sim() { delete th; }
+
+// net_rate, thermal_mod.f90:38-115 (H/He; no metals, no grain PE, no
+// secondary ionisation so sec_dgamma = 0 and sec_heat = heat).
+double Sim::net_rate(int il, double T, bool caseA, double& xHI, double& xHeI, double& xHeII, double& ne) const {
+    const double nH = st.nH[il];
+    solve_ion_cell(rm, par.He_abund, gamma_HI[il], gamma_HeI[il], gamma_HeII[il], nH, T, caseA, xHI, xHeI, xHeII, ne);
+    const double heat = nH * (xHI * heat_HI[il] + par.He_abund * (xHeI * heat_HeI[il] + xHeII * heat_HeII[il]));
+    return heat - cooling_total(*th, rm, caseA, par.He_abund, T, nH, ne, xHI, xHeI, xHeII);
+}
+
+// gas_thermal_update, thermal_mod.f90:124-249.
+void Sim::gas_thermal_update(double m[4]) {
+    const bool caseA = par.case_ab == "A";
+    const double w = par.ion_relax;
+    const int nleaf = grid.nleaf;
+    std::vector<double> xHI_new(nleaf), xHeI_new(nleaf), xHeII_new(nleaf), ne_new(nleaf), te_new(nleaf);
+#pragma omp parallel for num_threads(std::max(1, nthreads)) schedule(dynamic, 64)
+    for (int il = 0; il < nleaf; ++il) {
+        const double nH = st.nH[il];
+        if (nH <= 0.0) {
+            xHI_new[il] = st.xHI[il]; xHeI_new[il] = st.xHeI[il]; xHeII_new[il] = st.xHeII[il];
+            ne_new[il] = 0.0; te_new[il] = st.Te[il];
+            continue;
+        }
+        double xHI = st.xHI[il], xHeI = st.xHeI[il], xHeII = st.xHeII[il], ne = 0.0;
+        double tlo = par.te_min, thi = par.te_max, te;
+        const double net_lo = net_rate(il, tlo, caseA, xHI, xHeI, xHeII, ne);
+        const double net_hi = net_rate(il, thi, caseA, xHI, xHeI, xHeII, ne);
+        if (net_lo <= 0.0) {
+            te = tlo;
+        } else if (net_hi >= 0.0) {
+            te = thi;
+        } else {
+            for (int it = 1; it <= 60; ++it) {
+                const double tmid = std::sqrt(tlo * thi);
+                const double net_mid = net_rate(il, tmid, caseA, xHI, xHeI, xHeII, ne);
+                if (net_mid > 0.0) tlo = tmid; else thi = tmid;
+                if (thi / tlo - 1.0 < 1.0e-5) break;
+            }
+            te = std::sqrt(tlo * thi);
+        }
+        net_rate(il, te, caseA, xHI, xHeI, xHeII, ne);
+        xHI_new[il] = (1.0 - w) * st.xHI[il] + w * xHI;
+        xHeI_new[il] = (1.0 - w) * st.xHeI[il] + w * xHeI;
+        xHeII_new[il] = (1.0 - w) * st.xHeII[il] + w * xHeII;
+        const double xHeIII = std::max(0.0, 1.0 - xHeI_new[il] - xHeII_new[il]);
+        ne_new[il] = nH * ((1.0 - xHI_new[il]) + par.He_abund * (xHeII_new[il] + 2.0 * xHeIII));
+        te_new[il] = te;
+    }
+    const double hw = grid.dcell;
+    const double vol = hw * hw * hw;
+    double mx = 0.0, mt = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0, s4 = 0.0;
+    for (int il = 0; il < nleaf; ++il) {
+        if (st.nH[il] <= 0.0) continue;
+        mx = std::max(mx, std::fabs(xHI_new[il] - st.xHI[il]));
+        mt = std::max(mt, std::fabs(te_new[il] - st.Te[il]) / st.Te[il]);
+        s1 = s1 + vol * std::fabs(xHI_new[il] - st.xHI[il]);
+        s2 = s2 + vol * (1.0 - xHI_new[il]);
+        s3 = s3 + vol * ne_new[il] * std::fabs(te_new[il] - st.Te[il]);
+        s4 = s4 + vol * ne_new[il] * te_new[il];
+    }
+    m[0] = mx; m[1] = mt;
+    m[2] = s1 / std::max(s2, TINEST);
+    m[3] = s3 / std::max(s4, TINEST);
+    st.xHI = xHI_new; st.xHeI = xHeI_new; st.xHeII = xHeII_new; st.ne = ne_new; st.Te = te_new;
 }
 
 // gas_equilibrium_update, ion_balance_mod.f90:352-434.

@@ -196,8 +196,11 @@ struct Photon {
     double sHI, sHeI, sHeII;
 };
 
+struct Thermal;
+
 struct Sim {
     Par par;
+    Thermal* th = nullptr;           // thermal tables (solve_te)
     RateModel rm;
     Qmc qmc;
     Band band;
@@ -210,6 +213,10 @@ struct Sim {
     void transport_pass();           // ionizing_field_mod.f90:72-170
     void gas_rates_compute();        // gas_rates_mod.f90:82-153
     void gas_equilibrium_update(double* max_dx, double* dx_vol);  // ion_balance_mod.f90:352
+    void gas_thermal_update(double m[4]);                         // thermal_mod.f90:124-249
+    double net_rate(int il, double T, bool caseA, double& xHI, double& xHeI, double& xHeII,
+                    double& ne) const;                             // thermal_mod.f90:38-115
+    ~Sim();
     void gen_photon_qmc(int64_t ip, Photon& ph) const;          // ion_band_mod.f90:1880
     void walk_edge_car(const Photon& ph, Tally& t, double* tau_edge) const;  // raytrace_amr.f90:534
     int walk_leaves_car(double x, double y, double z, double kx, double ky,

@@ -15,7 +15,8 @@ _lib = None
 
 
 def build(force=False):
-    srcs = [os.path.join(HERE, f) for f in ("orc_core.cpp", "orc_capi.cpp", "orc_core.h", "Makefile")]
+    srcs = [os.path.join(HERE, f) for f in ("orc_core.cpp", "orc_thermal.cpp", "orc_capi.cpp", "orc_core.h",
+                                          "orc_thermal.h", "Makefile")]
     if force or not os.path.exists(LIB) or any(os.path.getmtime(s) > os.path.getmtime(LIB) for s in srcs):
         subprocess.run(["make", "-s", "-C", HERE], check=True)
     return LIB
@@ -58,6 +59,10 @@ def load():
         "orc_sim_walk_leaves": (I, [V, LL, V, I, V, V]),
         "orc_solve_ion_cell": (None, [I, D, D, D, D, D, D, I, V, V]),
         "orc_last_error": (C.c_char_p, []),
+        "orc_sim_thermal_update": (I, [V, V]),
+        "orc_gff_table": (None, [V, V]),
+        "orc_cooling_total": (D, [V, D, D, D, D, D, D]),
+        "orc_nlevel_cooling_at": (D, [C.c_char_p, D, D]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)
@@ -140,6 +145,13 @@ def evaluate(name, x, model=0):
     return out
 
 
+def gff_table():
+    logT = np.zeros(41)
+    z = np.zeros((41, 4))
+    load().orc_gff_table(logT.ctypes.data, z.ctypes.data)
+    return logT, z
+
+
 def band_edges(namelist):
     out = np.zeros(512)
     n = load().orc_band_edges(namelist.encode(), out.ctypes.data, 512)
@@ -179,6 +191,14 @@ class Sim:
 
     def set_nphotons(self, n):
         load().orc_sim_set_nphotons(self.h, int(n))
+
+    def thermal_update(self):
+        m = np.zeros(4)
+        assert load().orc_sim_thermal_update(self.h, m.ctypes.data) == 0
+        return tuple(m)
+
+    def cooling_total(self, T, nH, ne, xHI, xHeI, xHeII):
+        return load().orc_cooling_total(self.h, T, nH, ne, xHI, xHeI, xHeII)
 
     @property
     def ion_Ltot(self):

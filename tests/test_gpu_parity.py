@@ -239,3 +239,26 @@ def test_stromgren_gate():
     assert abs(v2 / vs - 1) < 0.02, (v2 / vs, r_eff / rs)
     assert 0.995 < r_eff / rs < 1.03, r_eff / rs
     neb.close()
+
+
+def test_thermal_balance_matches_oracle(orc):
+    """gas_thermal_update: bisection on log T with the ionisation re-solved
+    at every trial T; T_e within 20 K and x_HII within 1e-3 of the FP64
+    oracle after each iteration, on the same tallies."""
+    nl = configs.hii_thermal(nphotons=60000, niter=4, n=24, precision="fp64", rs_factor=1.2)
+    neb = Nebula(parse_namelist(nl))
+    sim = orc.Sim(nl)
+    for _ in range(4):
+        neb.ionizing_field_and_rates()
+        sim.transport_pass()
+        mg = neb.gas_thermal_update()
+        mo = sim.thermal_update()
+        neb.gas_opacity_fill()
+        assert abs(mg[0] - mo[0]) < 1e-3 and abs(mg[1] - mo[1]) < 1e-3
+        tg, to = neb.get("T_e"), sim.get("T_e")
+        assert np.max(np.abs(tg - to)) < 20.0, np.max(np.abs(tg - to))
+        assert np.max(np.abs(neb.get("x_HI") - sim.get("x_HI"))) < 1e-3
+    t = neb.get("T_e")
+    assert t.min() >= 3.0e3 and t.max() <= 3.0e4
+    assert np.median(t[neb.get("x_HI") < 0.1]) > 5.0e3   # photo-heated gas
+    neb.close()

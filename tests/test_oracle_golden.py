@@ -142,3 +142,29 @@ def test_aligned_band_edges(orc):
         seg = e[(e >= lo) & (e <= hi)]
         d = np.diff(np.log(seg))
         assert np.allclose(d, d[0], rtol=1e-12)
+
+
+def test_gaunt_table_matches_reference_nodes(orc, golden_rates):
+    # cooling_mod's gbar_ff nodes (gaunt_ff_mean over the Hummer 1988
+    # expansion, evaluated in single precision), dumped from the reference
+    # build into tools/python/mochii_rates.py.  The expansion runs in REAL*4,
+    # so two builds agree to single-precision rounding of the Chebyshev
+    # recurrence, ~1e-5 relative.
+    logT, z = orc.gff_table()
+    assert np.array_equal(logT, golden_rates["gff_logT"])
+    np.testing.assert_allclose(z, golden_rates["gff_z"], rtol=3e-5, atol=0)
+
+
+def test_hi_nlevel_cooling_low_density_limit_equals_fit(orc):
+    # the n-level H I cooling at n_e -> 0 is the ground-level excitation power
+    # the cooling_h_1 fit represents (fit error 0.52%, cooling_h_1.txt header)
+    import os
+    from conftest import ROOT
+    d = os.path.join(ROOT, "mochii_b200", "data", "atomic")
+    rows = [l.split() for l in open(os.path.join(d, "cooling_h_1.txt")) if l.strip() and not l.startswith("#")]
+    A = np.array([[float(x) for x in r] for r in rows[1:]])
+    lib = orc.load()
+    for T in (5e3, 1e4, 2e4, 5e4):
+        lam = lib.orc_nlevel_cooling_at(os.path.join(d, "nlevel_h_1.txt").encode(), T, 1e-6)
+        fit = np.sum(A[:, 0] * np.exp(-A[:, 1] / T)) / np.sqrt(T)
+        assert abs(lam / fit - 1) < 6e-3, T
