@@ -221,6 +221,18 @@ int mochii_walk_leaves(mochii_ctx* ctx, int64_t nray, const double* rays, int ma
  * each), as gen_ion_photon_qmc (ion_band_mod.f90:1880-1935) makes them. */
 int mochii_launch_records(mochii_ctx* ctx, int64_t ip0, int64_t n, double* out8);
 
+/* Same records as mochii_launch_records, for callers that cannot allocate
+ * device memory at call time (their device memory belongs to another
+ * allocator such as a PyTorch caching allocator or a host pool, or an MPS
+ * limit makes cudaMalloc fail).  No counterpart in the reference: it is a
+ * staging variant of this library's own hook.  Allocates nothing: the
+ * records are staged in a static device array of the library (4 MiB, held
+ * by every GPU that loads the library until exit).  n <= 65536 records per
+ * call, larger n is refused with MOCHII_ERR_BAD_PARAM.  The first call on a
+ * device looks up that array's device address (make it before any stream
+ * capture).  Calls share the array: calls that overlap on the GPU race. */
+int mochii_launch_records_noalloc(mochii_ctx* ctx, int64_t ip0, int64_t n, double* out8);
+
 #ifdef __cplusplus
 }
 #endif

@@ -96,6 +96,7 @@ SIGNATURES = {
     "mochii_walk_leaves": (C.c_int, [C.c_void_p, C.c_int64, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]),
     "mochii_launch_records": (C.c_int, [C.c_void_p, C.c_int64, C.c_int64, C.c_void_p]),
     "mochii_autotune": (C.c_int, [C.c_void_p, C.c_int64, _P(Tuning)]),
+    "mochii_launch_records_noalloc": (C.c_int, [C.c_void_p, C.c_int64, C.c_int64, C.c_void_p]),
     "mochii_set_tuning": (C.c_int, [C.c_void_p, _P(Tuning)]),
     "mochii_get_tuning": (C.c_int, [C.c_void_p, _P(Tuning)]),
 }

@@ -631,3 +631,15 @@ extern "C" int mochii_launch_records(mochii_ctx* c, int64_t ip0, int64_t n, doub
     CK(c, cudaStreamSynchronize(c->stream));
     return MOCHII_OK;
 }
+
+// Launch records staged in the library's static device array (see
+// transport.cu): no device allocation; n <= 65536 per call.
+extern "C" int mochii_launch_records_noalloc(mochii_ctx* c, int64_t ip0, int64_t n, double* out8) {
+    if (!c || !out8 || n < 0 || ip0 < 0) return fail(c, MOCHII_ERR_BAD_PARAM, "mochii_launch_records_noalloc: bad argument");
+    if (n > noalloc_max_records())
+        return fail(c, MOCHII_ERR_BAD_PARAM,
+                    "mochii_launch_records_noalloc: n exceeds the 65536 records of the static staging array");
+    if (n == 0) return MOCHII_OK;
+    CK(c, launch_records_noalloc(c, ip0, n, out8));
+    return MOCHII_OK;
+}

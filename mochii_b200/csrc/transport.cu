@@ -20,6 +20,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <mutex>
+
 #include "ctx.h"
 #include "physics.cuh"
 #include "qmc.cuh"
@@ -626,6 +628,73 @@ cudaError_t launch_records(mochii_ctx* c, long long ip0, long long n, double* ou
     const PassArgs a = make_args(c);
     k_launch_records<<<grid_blocks(n, 128, 1 << 20), 128, 0, c->stream>>>(a, ip0, n, out);
     return cudaGetLastError();
+}
+
+}  // namespace mochii
+
+// ===========================================================================
+// Launch records without allocation.
+//
+// mochii_launch_records stages the device-side records in a buffer it takes
+// from cudaMallocAsync.  Some callers of this library cannot allocate device
+// memory at call time: a host program whose device memory is handed out by
+// another allocator (a PyTorch caching allocator, a Fortran host's memory
+// pool, an MPS client under a memory limit) can see cudaMalloc fail although
+// the job has room, and a time-critical loop may not accept an allocation.
+// mochii_launch_records_noalloc stages the records in the file-scope device
+// array below instead and calls no allocating routine.
+//
+// The array lives in every GPU that loads the library until the process
+// exits (kNoallocMaxRecords x 8 doubles = 4 MiB).  Host code cannot use the
+// array's name as a device address: each device's address is obtained once,
+// with that device current, by cudaGetSymbolAddress on the first call made on
+// that device (so make that first call before any stream capture).  Every
+// call shares the array and it keeps the previous call's contents; the kernel
+// writes every slot it reads back, so nothing has to start at zero.  Calls
+// whose work overlaps on the GPU (several streams, several host threads)
+// race on the array.
+// ===========================================================================
+namespace mochii {
+namespace {
+constexpr long long kNoallocMaxRecords = 65536;
+static __device__ __align__(256) double g_noalloc_records[kNoallocMaxRecords * 8];
+
+constexpr int kNoallocMaxDevices = 64;
+std::mutex g_noalloc_mutex;
+double* g_noalloc_ptr[kNoallocMaxDevices] = {};
+
+// Device address of g_noalloc_records on the current device (set-up on the
+// first call per device).
+cudaError_t noalloc_scratch(double** out) {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev < 0 || dev >= kNoallocMaxDevices) return cudaErrorInvalidDevice;
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    if (!g_noalloc_ptr[dev]) {
+        void* p = nullptr;
+        e = cudaGetSymbolAddress(&p, g_noalloc_records);
+        if (e != cudaSuccess) return e;
+        g_noalloc_ptr[dev] = static_cast<double*>(p);
+    }
+    *out = g_noalloc_ptr[dev];
+    return cudaSuccess;
+}
+}  // namespace
+
+long long noalloc_max_records() { return kNoallocMaxRecords; }
+
+cudaError_t launch_records_noalloc(mochii_ctx* c, long long ip0, long long n, double* host_out) {
+    double* scratch = nullptr;
+    cudaError_t e = noalloc_scratch(&scratch);
+    if (e != cudaSuccess) return e;
+    const PassArgs a = make_args(c);
+    k_launch_records<<<grid_blocks(n, 128, 1 << 20), 128, 0, c->stream>>>(a, ip0, n, scratch);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    e = cudaMemcpyAsync(host_out, scratch, (size_t)n * 8 * sizeof(double), cudaMemcpyDeviceToHost, c->stream);
+    if (e != cudaSuccess) return e;
+    return cudaStreamSynchronize(c->stream);
 }
 
 }  // namespace mochii

@@ -14,6 +14,8 @@ cudaError_t launch_sobol(const QmcTables* t, int stream01, long long idx0, long 
                          cudaStream_t s);
 cudaError_t launch_walk(mochii_ctx* c, const double* rays, long long nray, int max_steps, int* leaves, int* nsteps);
 cudaError_t launch_records(mochii_ctx* c, long long ip0, long long n, double* out);
+long long noalloc_max_records();
+cudaError_t launch_records_noalloc(mochii_ctx* c, long long ip0, long long n, double* host_out);
 
 int balance_blocks(const mochii_ctx* c);
 cudaError_t launch_columns(mochii_ctx* c);
