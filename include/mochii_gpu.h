@@ -108,7 +108,8 @@ typedef struct mochii_params {
     int cooling_local_ne;            /* par%cooling_model == 'local_ne'       */
     int gaunt_vh14;
     /* diffuse field, secondary ionisation, dust, FUV */
-    int diffuse_field, diffuse_milne, use_sec_ion;
+    int diffuse_field, use_sec_ion;
+    int diffuse_model;               /* par%diffuse_energy_model: 0 milne, 1 exponential, 2 threshold */
     int ion_add_dust, ion_dust_scatter;
     int dust_law;                    /* 0 global_dgr, 1 none, 2 other         */
     double DGR, cext_dust;
@@ -128,6 +129,8 @@ typedef struct mochii_pass_stats {
     double kernel_ms;                /* device time of the transport kernel   */
     double pass_ms;                  /* device time of the whole pass         */
     int64_t walk_kills;              /* MAX_WALK_STEPS guard hits             */
+    int64_t diffuse_packets;         /* diffuse_nphot of this pass            */
+    double diffuse_lum;              /* diffuse_lum [erg/s]                   */
 } mochii_pass_stats;
 
 /* Convergence measures (gas_thermal_update / gas_equilibrium_update outputs). */
@@ -220,6 +223,13 @@ int mochii_walk_leaves(mochii_ctx* ctx, int64_t nray, const double* rays, int ma
 /* Launch records of packets ip0..ip0+n-1: x,y,z,kx,ky,kz,E,inu (8 doubles
  * each), as gen_ion_photon_qmc (ion_band_mod.f90:1880-1935) makes them. */
 int mochii_launch_records(mochii_ctx* ctx, int64_t ip0, int64_t n, double* out8);
+
+/* Diffuse field of the current state (diffuse_build, diffuse_mod.f90:60-121)
+ * and the launch of diffuse packets ip0..ip0+n-1 (gen_diffuse_photon_qmc,
+ * diffuse_mod.f90:221-296): out8 per packet = start cell (ix, iy, iz), the
+ * DDA tMax (x, y, z), sigma_HI [1e-18 cm^2] and the diagnostic bin; *lum =
+ * diffuse_lum [erg/s], *nphot = diffuse_nphot. */
+int mochii_diffuse_records(mochii_ctx* ctx, int64_t ip0, int64_t n, double* out8, double* lum, int64_t* nphot);
 
 /* Same records as mochii_launch_records, for callers that cannot allocate
  * device memory at call time (their device memory belongs to another

@@ -47,7 +47,7 @@ class Params(C.Structure):
         ("abund_Si", C.c_double), ("abund_Cl", C.c_double), ("abund_Ca", C.c_double),
         ("ion_metal_abs", C.c_int), ("metal_ne", C.c_int), ("metal_heat", C.c_int), ("metal_freefree", C.c_int),
         ("charge_exchange_two_way", C.c_int), ("cooling_local_ne", C.c_int), ("gaunt_vh14", C.c_int),
-        ("diffuse_field", C.c_int), ("diffuse_milne", C.c_int), ("use_sec_ion", C.c_int),
+        ("diffuse_field", C.c_int), ("use_sec_ion", C.c_int), ("diffuse_model", C.c_int),
         ("ion_add_dust", C.c_int), ("ion_dust_scatter", C.c_int), ("dust_law", C.c_int),
         ("DGR", C.c_double), ("cext_dust", C.c_double), ("grain_pe", C.c_int),
         ("ion_dust_kext", C.c_char * STRLEN), ("data_dir", C.c_char * STRLEN), ("atomic_dir", C.c_char * STRLEN),
@@ -59,7 +59,7 @@ class PassStats(C.Structure):
     _fields_ = [("energy_emitted", C.c_double), ("energy_absorbed", C.c_double), ("energy_escaped", C.c_double),
                 ("closure", C.c_double), ("direct_segments", C.c_int64), ("scattered_segments", C.c_int64),
                 ("packets", C.c_int64), ("kernel_ms", C.c_double), ("pass_ms", C.c_double),
-                ("walk_kills", C.c_int64)]
+                ("walk_kills", C.c_int64), ("diffuse_packets", C.c_int64), ("diffuse_lum", C.c_double)]
 
 
 class Metrics(C.Structure):
@@ -97,6 +97,7 @@ SIGNATURES = {
     "mochii_launch_records": (C.c_int, [C.c_void_p, C.c_int64, C.c_int64, C.c_void_p]),
     "mochii_autotune": (C.c_int, [C.c_void_p, C.c_int64, _P(Tuning)]),
     "mochii_launch_records_noalloc": (C.c_int, [C.c_void_p, C.c_int64, C.c_int64, C.c_void_p]),
+    "mochii_diffuse_records": (C.c_int, [C.c_void_p, C.c_int64, C.c_int64, C.c_void_p, _P(C.c_double), _P(C.c_int64)]),
     "mochii_set_tuning": (C.c_int, [C.c_void_p, _P(Tuning)]),
     "mochii_get_tuning": (C.c_int, [C.c_void_p, _P(Tuning)]),
 }

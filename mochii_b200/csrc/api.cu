@@ -47,7 +47,8 @@ void release(mochii_ctx* c) {
                     c->tab.tab_e, c->tab.tab_f, c->tab.tab_c, c->tab.tab_off, c->tab.comp, c->tab.eedge,
                     c->tab.qmc, c->tw.ledger, c->tw.counters, c->bw.partial, c->bw.counters,
                     c->rec.tm, c->rec.td, c->rec.cell, c->rec.bits, c->rec.sig, c->rec.coef,
-                    c->th.gff, c->th.lamref, c->th.Ssup, c->th.tinv};
+                    c->th.gff, c->th.lamref, c->th.Ssup, c->th.tinv,
+                    c->dif.ch, c->dif.tot, c->dif.scan_tmp, c->dif.tables};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     for (cudaEvent_t e : {c->ev0, c->ev1, c->evA, c->evB})
@@ -77,7 +78,6 @@ int validate(const mochii_params& p, std::string* why, int* code) {
     if (!p.source_point) return *why = "only internal point sources are built", 1;
     if (!p.launch_sobol) return *why = "launch_sequence='random' is not built; use 'sobol'", 1;
     if (p.use_metals) return *why = "use_metals is not built in this library version", 1;
-    if (p.diffuse_field) return *why = "diffuse_field is not built in this library version", 1;
     if (p.ion_add_dust) return *why = "ion_add_dust is not built in this library version", 1;
     if (p.use_sec_ion) return *why = "use_sec_ion is not built in this library version", 1;
     if (p.add_fuv) return *why = "add_fuv is not built in this library version", 1;
@@ -121,6 +121,7 @@ extern "C" int mochii_init(const mochii_params* pin, mochii_ctx** out) {
     auto* c = new mochii_ctx();
     c->par = *pin;
     mochii_params& p = c->par;
+    if (p.diffuse_field) p.caseA = 1;   // setup.f90:580-583: the diffuse field forces case A
     if (!band_build(p, c->band, &why)) {
         delete c;
         return fail(nullptr, MOCHII_ERR_BAD_PARAM, why);
@@ -242,6 +243,30 @@ extern "C" int mochii_init(const mochii_params* pin, mochii_ctx** out) {
     CKI(cudaMalloc(&c->rec.sig, 3 * (size_t)c->rec.cap * rsz + 64));
     CKI(cudaMalloc(&c->rec.coef, 6 * (size_t)c->rec.cap * rsz + 64));
     c->bw.blocks = balance_blocks(c);
+    if (p.diffuse_field) {
+        MilneHost mh;
+        milne_tables_build(p.eion_max, mh);
+        const size_t nt = mh.xg.size() + mh.cdf.size() + mh.xbar.size() + mh.frac.size();
+        CKI(dalloc(&c->dif.tables, nt));
+        double* q = c->dif.tables;
+        CKI(cudaMemcpy(q, mh.xg.data(), mh.xg.size() * 8, cudaMemcpyHostToDevice));
+        c->dif.m.xg = q;
+        q += mh.xg.size();
+        CKI(cudaMemcpy(q, mh.cdf.data(), mh.cdf.size() * 8, cudaMemcpyHostToDevice));
+        c->dif.m.cdf = q;
+        q += mh.cdf.size();
+        CKI(cudaMemcpy(q, mh.xbar.data(), mh.xbar.size() * 8, cudaMemcpyHostToDevice));
+        c->dif.m.xbar = q;
+        q += mh.xbar.size();
+        CKI(cudaMemcpy(q, mh.frac.data(), mh.frac.size() * 8, cudaMemcpyHostToDevice));
+        c->dif.m.frac = q;
+        c->dif.m.lgT0 = mh.lgT[0];
+        c->dif.m.dlgT = mh.lgT[1] - mh.lgT[0];
+        CKI(dalloc(&c->dif.ch, 4 * (size_t)n));
+        CKI(dalloc(&c->dif.tot, (size_t)n));
+        c->dif.scan_bytes = diffuse_scan_bytes(n);
+        CKI(cudaMalloc(&c->dif.scan_tmp, c->dif.scan_bytes + 16));
+    }
     if (p.solve_te) {
         ThermalHost th;
         if (!thermal_tables_build(p, th, &why)) {
@@ -330,6 +355,14 @@ extern "C" int mochii_transport_pass(mochii_ctx* c, int with_peel, mochii_pass_s
     CK(c, cudaMemsetAsync(c->tw.counters, 0, 4 * sizeof(unsigned long long), c->stream));
     CK(c, cudaEventRecord(c->ev0, c->stream));
     CK(c, launch_transport(c));
+    double dlum = 0.0;
+    long long nd = 0;
+    if (c->par.diffuse_field) {   // ionizing_field_mod.f90:139-161
+        CK(c, diffuse_build(c, &dlum));
+        const double lpacket = c->band.ion_Ltot / (double)c->par.nphotons;
+        nd = dlum > 0.0 ? std::llround(dlum / lpacket) : 0;
+        if (nd > 0) CK(c, launch_transport_diffuse(c, dlum, nd));
+    }
     CK(c, cudaEventRecord(c->ev1, c->stream));
     CK(c, launch_rates(c));
     CK(c, cudaEventRecord(c->evB, c->stream));
@@ -353,9 +386,11 @@ extern "C" int mochii_transport_pass(mochii_ctx* c, int with_peel, mochii_pass_s
                 std::max(s.energy_emitted, kTinest);
     s.direct_segments = (int64_t)cnt[0];
     s.walk_kills = (int64_t)cnt[1];
-    s.packets = c->par.nphotons;
     s.kernel_ms = ms;
     s.pass_ms = pms;
+    s.diffuse_packets = nd;
+    s.diffuse_lum = dlum;
+    s.packets = c->par.nphotons + nd;
     if (st) *st = s;
     if (!std::isfinite(s.energy_emitted) || !std::isfinite(s.energy_absorbed))
         return fail(c, MOCHII_ERR_NONFINITE, "non-finite energy ledger");
@@ -641,5 +676,22 @@ extern "C" int mochii_launch_records_noalloc(mochii_ctx* c, int64_t ip0, int64_t
                     "mochii_launch_records_noalloc: n exceeds the 65536 records of the static staging array");
     if (n == 0) return MOCHII_OK;
     CK(c, launch_records_noalloc(c, ip0, n, out8));
+    return MOCHII_OK;
+}
+
+// Diffuse launch records (x, y, z, kx, ky, kz, E, inu) of packets ip0..ip0+n-1
+// from the current state: diffuse_build + gen_diffuse_photon_qmc.
+extern "C" int mochii_diffuse_records(mochii_ctx* c, int64_t ip0, int64_t n, double* out8, double* lum,
+                                      int64_t* nphot) {
+    if (!c || n < 0 || ip0 < 0) return MOCHII_ERR_BAD_PARAM;
+    if (!c->par.diffuse_field) return fail(c, MOCHII_ERR_BAD_PARAM, "par%diffuse_field is off");
+    double total = 0.0;
+    CK(c, diffuse_build(c, &total));
+    if (lum) *lum = total;
+    if (nphot) *nphot = total > 0.0 ? std::llround(total / (c->band.ion_Ltot / (double)c->par.nphotons)) : 0;
+    if (n == 0 || total <= 0.0) return MOCHII_OK;
+    if (n > c->rec.cap) return fail(c, MOCHII_ERR_BAD_PARAM, "n exceeds the record buffer");
+    CK(c, launch_diffuse_chunk(c, total, ip0, n));
+    CK(c, launch_records_from_buffer(c, n, out8));
     return MOCHII_OK;
 }

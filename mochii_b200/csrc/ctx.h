@@ -7,6 +7,7 @@
 #include <vector>
 
 #include "band.h"
+#include "diffuse.h"
 #include "mochii_gpu.h"
 #include "qmc.cuh"
 #include "thermal.h"
@@ -93,6 +94,7 @@ struct mochii_ctx {
     mochii::RecordBuffers rec;
     mochii::Tuning tune;
     mochii::ThermalDev th;          // thermal tables (solve_te)
+    mochii::DiffuseBuffers dif;     // diffuse field (diffuse_field)
     bool thermal_ready = false;
     mochii::BalanceWork bw;
     std::string last_error;

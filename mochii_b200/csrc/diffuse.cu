@@ -1,0 +1,320 @@
+// Diffuse ground-recombination packets on the device (diffuse_mod.f90 with
+// the Milne ground-continuum spectra of milne_recomb_spectrum_mod.f90).
+//
+// Per pass: k_diffuse_lum evaluates, per leaf, the luminosity of the three
+// ground channels (H II -> H I 1s, He II -> He I 1^1S, He III -> He II 1s):
+// L = n_e n_ion (alpha_A - alpha_B)(T) <E>_Milne(T) V  (diffuse_mod.f90:78-90);
+// a device prefix sum over leaves turns the leaf totals into the emission
+// CDF; the packet count is nint(L_diffuse / L_packet) (:116).  k_launch_diffuse
+// then draws leaf (binary search of the CDF), position in the leaf, isotropic
+// direction, channel and Milne energy from the 9-dimensional diffuse Sobol
+// stream (diffuse_mod.f90:221-296) and writes the same packet records as the
+// stellar launch, so the walk kernel is shared.
+#include <cub/cub.cuh>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+
+#include "ctx.h"
+#include "diffuse.h"
+#include "physics.cuh"
+#include "qmc.cuh"
+#include "records.cuh"
+#include "transport.h"
+
+namespace mochii {
+
+// ---- host: Milne tables (milne_recomb_spectrum_mod.f90:99-228) -------------
+// Quadratically clustered x = (E - E_th)/kT nodes on [0, 60] (512), log T
+// nodes 1e2-1e6 K (192); per (T, channel) the energy-luminosity CDF of the
+// photon PDF E^2 sigma(E) exp(-x) by Simpson panels truncated at eion_max,
+// the mean x under the number PDF and the in-band photon fraction.
+void milne_tables_build(double eion_max, MilneHost& m) {
+    const double XMAX = 60.0;
+    const double eth[3] = {kEthHI, kEthHeI, kEthHeII};
+    m.xg.resize(kMilneNX);
+    m.lgT.resize(kMilneNT);
+    for (int ix = 0; ix < kMilneNX; ++ix) {
+        const double t = (double)ix / (double)(kMilneNX - 1);
+        m.xg[ix] = XMAX * t * t;
+    }
+    for (int it = 0; it < kMilneNT; ++it)
+        m.lgT[it] = std::log10(1.0e2) + (std::log10(1.0e6) - std::log10(1.0e2)) * (double)it / (double)(kMilneNT - 1);
+    m.cdf.assign((size_t)3 * kMilneNT * kMilneNX, 0.0);
+    m.xbar.assign((size_t)3 * kMilneNT, 0.0);
+    m.frac.assign((size_t)3 * kMilneNT, 0.0);
+    for (int ich = 0; ich < 3; ++ich) {
+        for (int it = 0; it < kMilneNT; ++it) {
+            double* c = &m.cdf[((size_t)ich * kMilneNT + it) * kMilneNX];
+            const double kT = kKboltz * std::pow(10.0, m.lgT[it]) / kEv2erg;
+            auto shape = [&](double x) {
+                const double E = eth[ich] + x * kT;
+                const double s = ich == 0 ? sigma_HI(E) : ich == 1 ? sigma_HeI(E) : sigma_HeII(E);
+                return E * E * s * std::exp(-x);
+            };
+            const double x_hi = std::min(XMAX, (eion_max - eth[ich]) / kT);
+            if (x_hi <= 0.0) {
+                std::fill(c, c + kMilneNX, 1.0);
+                continue;
+            }
+            double sn = 0.0, se = 0.0, sxn = 0.0;
+            c[0] = 0.0;
+            for (int ix = 1; ix < kMilneNX; ++ix) {
+                const double xa = m.xg[ix - 1], xb = std::min(m.xg[ix], x_hi);
+                if (xb > xa) {
+                    const double xm = 0.5 * (xa + xb);
+                    const double fa = shape(xa), fm = shape(xm), fb = shape(xb);
+                    sn = sn + (xb - xa) / 6.0 * (fa + 4.0 * fm + fb);
+                    se = se + (xb - xa) / 6.0 *
+                                  (fa * (eth[ich] + xa * kT) + 4.0 * fm * (eth[ich] + xm * kT) + fb * (eth[ich] + xb * kT));
+                    sxn = sxn + (xb - xa) / 6.0 * (fa * xa + 4.0 * fm * xm + fb * xb);
+                }
+                c[ix] = se;
+            }
+            double tail = sn;
+            for (double xa = x_hi; xa < XMAX;) {
+                const double xb = std::min(xa + 0.25, XMAX), xm = 0.5 * (xa + xb);
+                tail = tail + (xb - xa) / 6.0 * (shape(xa) + 4.0 * shape(xm) + shape(xb));
+                xa = xb;
+            }
+            if (se > 0.0) {
+                for (int ix = 0; ix < kMilneNX; ++ix) c[ix] = c[ix] / se;
+            } else {
+                std::fill(c, c + kMilneNX, 1.0);
+            }
+            c[kMilneNX - 1] = 1.0;
+            m.xbar[(size_t)ich * kMilneNT + it] = sxn / std::max(sn, kTinest);
+            m.frac[(size_t)ich * kMilneNT + it] = sn / std::max(tail, kTinest);
+        }
+    }
+}
+
+namespace {
+
+constexpr int kThreads = 256;
+
+struct DiffArgs {
+    const double* nH;
+    const double* xHI;
+    const double* xHeI;
+    const double* xHeII;
+    const double* ne;
+    const double* Te;
+    double* ch;        // 4 x nleaf (channel luminosities, leaf-major)
+    double* tot;       // nleaf leaf totals, then their inclusive prefix sum
+    MilneDev m;
+    long long nleaf;
+    double yHe, vol, eion_max;
+    RateSel rs;
+    int energy_model;  // 0 milne, 1 exponential, 2 threshold
+};
+
+// milne_tbracket (:286-297): it is 1-based as in the reference.
+__device__ __forceinline__ void tbracket(const MilneDev& m, double T, int& it, double& w) {
+    double s = (log10(fmax(T, kTinest)) - m.lgT0) / m.dlgT;
+    s = fmin(fmax(s, 0.0), (double)(kMilneNT - 1));
+    it = min((int)s + 1, kMilneNT - 1);
+    w = s - (double)(it - 1);
+}
+
+// milne_energy_per_recomb (:302-312).
+__device__ double energy_per_recomb(const MilneDev& m, int ich, double T, double eth) {
+    int it;
+    double w;
+    tbracket(m, T, it, w);
+    const double xb = (1.0 - w) * m.xbar[ich * kMilneNT + it - 1] + w * m.xbar[ich * kMilneNT + it];
+    const double fk = (1.0 - w) * m.frac[ich * kMilneNT + it - 1] + w * m.frac[ich * kMilneNT + it];
+    return fk * (eth + xb * (kKboltz * T / kEv2erg));
+}
+
+// milne_sample_energy (:320-350): binary search of the log-T-interpolated CDF,
+// then linear inversion inside the bracket.
+__device__ double milne_sample(const MilneDev& m, int ich, double T, double u, double eth, double eion_max) {
+    int it;
+    double w;
+    tbracket(m, T, it, w);
+    const double kT = kKboltz * T / kEv2erg;
+    const double uu = fmin(fmax(u, 0.0), 1.0);
+    const double* c0 = m.cdf + ((size_t)ich * kMilneNT + it - 1) * kMilneNX;
+    const double* c1 = c0 + kMilneNX;
+    int lo = 1, hi = kMilneNX;
+    double ca = (1.0 - w) * c0[0] + w * c1[0];
+    double cb = (1.0 - w) * c0[kMilneNX - 1] + w * c1[kMilneNX - 1];
+    while (hi - lo > 1) {
+        const int mid = (lo + hi) / 2;
+        const double cm = (1.0 - w) * c0[mid - 1] + w * c1[mid - 1];
+        if (uu > cm) { lo = mid; ca = cm; } else { hi = mid; cb = cm; }
+    }
+    const double x = cb > ca ? m.xg[lo - 1] + (m.xg[hi - 1] - m.xg[lo - 1]) * (uu - ca) / (cb - ca) : m.xg[lo - 1];
+    return fmin(eth + x * kT, eion_max * (1.0 - 1.0e-12));
+}
+
+__global__ void k_diffuse_lum(const DiffArgs a) {
+    for (long long il = (long long)blockIdx.x * blockDim.x + threadIdx.x; il < a.nleaf;
+         il += (long long)gridDim.x * blockDim.x) {
+        double c0 = 0.0, c1 = 0.0, c2 = 0.0;
+        const double nH = a.nH[il];
+        if (nH > 0.0) {
+            const double T = a.Te[il], ne = a.ne[il];
+            const double kT = kKboltz * T / kEv2erg;
+            const double xHeIII = fmax(0.0, 1.0 - a.xHeI[il] - a.xHeII[il]);
+            const double nHII = nH * (1.0 - a.xHI[il]);
+            const double nHeII = nH * a.yHe * a.xHeII[il];
+            const double nHeIII = nH * a.yHe * xHeIII;
+            double e0, e1, e2;
+            if (a.energy_model == 0) {
+                e0 = energy_per_recomb(a.m, 0, T, kEthHI);
+                e1 = energy_per_recomb(a.m, 1, T, kEthHeI);
+                e2 = energy_per_recomb(a.m, 2, T, kEthHeII);
+            } else if (a.energy_model == 1) {
+                e0 = kEthHI + kT; e1 = kEthHeI + kT; e2 = kEthHeII + kT;
+            } else {
+                e0 = kEthHI; e1 = kEthHeI; e2 = kEthHeII;
+            }
+            c0 = ne * nHII * (alphaA_HII(a.rs, T) - alphaB_HII(a.rs, T)) * e0 * kEv2erg * a.vol;
+            c1 = ne * nHeII * (alphaA_HeII(a.rs, T) - alphaB_HeII(a.rs, T)) * e1 * kEv2erg * a.vol;
+            c2 = ne * nHeIII * (alphaA_HeIII(a.rs, T) - alphaB_HeIII(a.rs, T)) * e2 * kEv2erg * a.vol;
+        }
+        a.ch[4 * il + 0] = c0;
+        a.ch[4 * il + 1] = c1;
+        a.ch[4 * il + 2] = c2;
+        a.ch[4 * il + 3] = 0.0;
+        a.tot[il] = ((c0 + c1) + c2) + 0.0;
+    }
+}
+
+struct DiffLaunchArgs {
+    const QmcTables* qmc;
+    const double* cum;     // inclusive prefix sum of the leaf totals
+    const double* ch;
+    const double* Te;
+    const double* eedge;
+    MilneDev m;
+    double total, org[3], dcell, eion_max;
+    int n[3], nnu, nfuv, energy_model;
+    long long nleaf;
+};
+
+// gen_diffuse_photon_qmc (diffuse_mod.f90:221-296) and dda_init.
+template <typename R>
+__global__ void __launch_bounds__(kThreads) k_launch_diffuse(const DiffLaunchArgs a, PacketRecords rec, long long ip0,
+                                                             long long n) {
+    __shared__ QmcTables sq;
+    {
+        const uint32_t* src = reinterpret_cast<const uint32_t*>(a.qmc);
+        uint32_t* dst = reinterpret_cast<uint32_t*>(&sq);
+        for (int i = threadIdx.x; i < (int)(sizeof(QmcTables) / 4); i += blockDim.x) dst[i] = src[i];
+    }
+    __syncthreads();
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const uint64_t ip = (uint64_t)(ip0 + i);
+    double u[8];
+#pragma unroll
+    for (int d = 0; d < 8; ++d) u[d] = qmc_uniform(sq, ip, d, 1);
+    // first leaf whose normalised CDF reaches u1
+    long long lo = 1, hi = a.nleaf;
+    while (lo < hi) {
+        const long long mid = (lo + hi) / 2;
+        if (a.cum[mid - 1] / a.total < u[0]) lo = mid + 1; else hi = mid;
+    }
+    const long long il = lo - 1;
+    const int ix = (int)(il % a.n[0]), iy = (int)((il / a.n[0]) % a.n[1]), iz = (int)(il / ((long long)a.n[0] * a.n[1]));
+    const double half = 0.5 * a.dcell;
+    const double pos[3] = {(a.org[0] + ((double)ix + 0.5) * a.dcell) + (2.0 * u[1] - 1.0) * half,
+                           (a.org[1] + ((double)iy + 0.5) * a.dcell) + (2.0 * u[2] - 1.0) * half,
+                           (a.org[2] + ((double)iz + 0.5) * a.dcell) + (2.0 * u[3] - 1.0) * half};
+    const double cost = 2.0 * u[4] - 1.0;
+    const double sint = sqrt(1.0 - cost * cost);
+    double sphi, cphi;
+    sincos(kTwoPi * u[5], &sphi, &cphi);
+    const double kk[3] = {sint * cphi, sint * sphi, cost};
+    const double w0 = a.ch[4 * il], w1 = a.ch[4 * il + 1], w2 = a.ch[4 * il + 2], w3 = a.ch[4 * il + 3];
+    const double uu = u[6] * (((w0 + w1) + w2) + w3);
+    int ch;
+    double eph;
+    if (uu <= w0) { ch = 0; eph = kEthHI; }
+    else if (uu <= w0 + w1) { ch = 1; eph = kEthHeI; }
+    else if (uu <= w0 + w1 + w2) { ch = 2; eph = kEthHeII; }
+    else { ch = 3; eph = kEthHI; }
+    if (ch <= 2) {
+        const double T = a.Te[il];
+        if (a.energy_model == 0) eph = milne_sample(a.m, ch, T, u[7], eph, a.eion_max);
+        else if (a.energy_model == 1) eph = eph + (kKboltz * T / kEv2erg) * (-log(fmax(u[7], kTinest)));
+        eph = fmin(eph, a.eion_max * 0.999);
+    }
+    // ion_bin_of without the FUV bins (ion_band_mod.f90:624-646)
+    int blo = 1, bhi = a.nnu;
+    while (blo < bhi) {
+        const int mid = (blo + bhi + 1) / 2;
+        if (a.eedge[mid - 1] <= eph) blo = mid; else bhi = mid - 1;
+    }
+    const int inu = min(max(blo, a.nfuv + 1), a.nnu) - 1;
+    write_record<R>(rec, i, pos, kk, eph, inu, a.org, a.dcell, a.n);
+}
+
+int nblk(long long work, int threads, int cap) {
+    long long b = (work + threads - 1) / threads;
+    return (int)(b < 1 ? 1 : b > cap ? cap : b);
+}
+
+}  // namespace
+
+// Per-leaf diffuse luminosities and their prefix sum; returns the total
+// diffuse luminosity (one 8-byte device-to-host read).
+cudaError_t diffuse_build(mochii_ctx* c, double* total) {
+    DiffArgs a;
+    a.nH = c->nH; a.xHI = c->xHI; a.xHeI = c->xHeI; a.xHeII = c->xHeII; a.ne = c->ne; a.Te = c->Te;
+    a.ch = c->dif.ch;
+    a.tot = c->dif.tot;
+    a.m = c->dif.m;
+    a.nleaf = c->grid.nleaf;
+    a.yHe = c->par.He_abund;
+    const double w = c->grid.dcell * c->par.distance2cm;
+    a.vol = w * w * w;
+    a.eion_max = c->par.eion_max;
+    a.rs.hui_gnedin = c->par.recomb_hui_gnedin;
+    a.rs.dere_hybrid = c->par.ci_dere_hybrid;
+    a.energy_model = c->par.diffuse_model;
+    k_diffuse_lum<<<nblk(a.nleaf, kThreads, 148 * 16), kThreads, 0, c->stream>>>(a);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    size_t tmp = c->dif.scan_bytes;
+    e = cub::DeviceScan::InclusiveSum(c->dif.scan_tmp, tmp, c->dif.tot, c->dif.tot, (int)a.nleaf, c->stream);
+    if (e != cudaSuccess) return e;
+    e = cudaMemcpyAsync(total, c->dif.tot + (a.nleaf - 1), sizeof(double), cudaMemcpyDeviceToHost, c->stream);
+    if (e != cudaSuccess) return e;
+    return cudaStreamSynchronize(c->stream);
+}
+
+size_t diffuse_scan_bytes(long long nleaf) {
+    size_t bytes = 0;
+    cub::DeviceScan::InclusiveSum(nullptr, bytes, (double*)nullptr, (double*)nullptr, (int)nleaf);
+    return bytes;
+}
+
+cudaError_t launch_diffuse_chunk(mochii_ctx* c, double total, long long ip0, long long n) {
+    DiffLaunchArgs a;
+    a.qmc = c->tab.qmc;
+    a.cum = c->dif.tot;
+    a.ch = c->dif.ch;
+    a.Te = c->Te;
+    a.eedge = c->tab.eedge;
+    a.m = c->dif.m;
+    a.total = total;
+    a.org[0] = c->grid.xmin; a.org[1] = c->grid.ymin; a.org[2] = c->grid.zmin;
+    a.dcell = c->grid.dcell;
+    a.eion_max = c->par.eion_max;
+    a.n[0] = c->grid.nx; a.n[1] = c->grid.ny; a.n[2] = c->grid.nz;
+    a.nnu = c->nnu;
+    a.nfuv = c->band.nfuv_band;
+    a.energy_model = c->par.diffuse_model;
+    a.nleaf = c->grid.nleaf;
+    const PacketRecords r = packet_records(c);
+    if (c->fp32) k_launch_diffuse<float><<<nblk(n, kThreads, 1 << 30), kThreads, 0, c->stream>>>(a, r, ip0, n);
+    else k_launch_diffuse<double><<<nblk(n, kThreads, 1 << 30), kThreads, 0, c->stream>>>(a, r, ip0, n);
+    return cudaGetLastError();
+}
+
+}  // namespace mochii

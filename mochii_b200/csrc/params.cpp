@@ -27,7 +27,7 @@ namespace {
 const char* const kOtherKeys[] = {
     "albedo", "allsky", "allsky_nside", "allsky_x", "allsky_y", "allsky_z", "alpha", "amr_type",
     "base_name", "beta", "centering", "cone_opening", "density_file", "density_powerlaw_index",
-    "density_rscale", "density_zprofile", "density_zscale", "diffuse_energy_model", "distance",
+    "density_rscale", "density_zprofile", "density_zscale", "distance",
     "dust_emis_bands", "dust_emis_transport", "dust_emission_method", "dust_fast_table", "dust_model",
     "dust_niter", "dust_no_photons", "dust_nu", "dust_sed", "dust_single_teq", "dust_tol", "dxim", "dyim",
     "emis_output", "exetime", "ext_geometry", "ext_intensity", "ext_scale", "ext_spectrum", "ext_tstar",
@@ -129,7 +129,7 @@ extern "C" int mochii_params_default(mochii_params* p) {
     p->ion_metal_abs = 1; p->metal_ne = 1; p->metal_heat = 1; p->metal_freefree = 1;
     p->charge_exchange_two_way = 1;
     p->cooling_local_ne = 1;
-    p->diffuse_milne = 1;
+    p->diffuse_model = 0;
     p->dust_law = 0;
     p->DGR = 1.0e-2; p->cext_dust = 1.6059e-21;
     p->precision = MOCHII_PREC_FP64;
@@ -255,6 +255,14 @@ int set_key(mochii_params* p, std::string key, const std::vector<std::string>& v
     if (key == "dust_density_law") {
         const std::string s = lower(unquote(v));
         p->dust_law = s == "global_dgr" ? 0 : s == "none" ? 1 : 2;
+        return 0;
+    }
+    if (key == "diffuse_energy_model") {   // setup.f90:186-193
+        const std::string s = lower(unquote(v));
+        if (s == "milne") p->diffuse_model = 0;
+        else if (s == "exponential") p->diffuse_model = 1;
+        else if (s == "threshold") p->diffuse_model = 2;
+        else return bad("must be 'milne', 'exponential' or 'threshold'");
         return 0;
     }
     if (key == "ion_dust_kext") { copy_str(p->ion_dust_kext, sizeof(p->ion_dust_kext), unquote(v)); return 0; }

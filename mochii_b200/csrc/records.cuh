@@ -1,0 +1,65 @@
+// Packet records: the hand-off between the launch kernels (stellar and
+// diffuse) and the walk kernel.  Structure of arrays over the packets of one
+// chunk: the DDA state after dda_init (tMax, tDelta, start cell, step
+// signs), the diagnostic bin, and the packet's cross sections and
+// rate coefficients at its exact energy.
+#pragma once
+#include <cuda_runtime.h>
+
+#include "physics.cuh"
+
+namespace mochii {
+
+struct PacketRecords {
+    double* tm;    // 3 x cap
+    double* td;    // 3 x cap
+    int* cell;     // ix | iy << 10 | iz << 20
+    int* bits;     // inu | (stp_x+1) << 16 | (stp_y+1) << 18 | (stp_z+1) << 20
+    void* sig;     // 3 x cap of R: sigma_HI, sigma_HeI, sigma_HeII in 1e-18 cm^2
+    void* coef;    // 6 x cap of R: Gamma/heat coefficients per unit path
+    long long cap;
+};
+
+// Record of one packet: build_ion_packet_physics (ion_packet_mod.f90:21-53),
+// the per-path coefficients of score_ion_path (ion_score_mod.f90:213-221),
+// scaled by 1e18 so FP32 stays in range (sigma in 1e-18 cm^2, E in eV), and
+// dda_init (raytrace_amr.f90:495-532) in FP64.
+template <typename R>
+__device__ __forceinline__ void write_record(const PacketRecords& rec, long long i, const double pos[3],
+                                             const double kk[3], double E, int inu, const double org[3],
+                                             double d, const int n[3]) {
+    const double sHI = sigma_HI(E), sHeI = sigma_HeI(E), sHeII = sigma_HeII(E);
+    R* sg = static_cast<R*>(rec.sig);
+    R* cf = static_cast<R*>(rec.coef);
+    const long long c = rec.cap;
+    sg[i] = (R)(sHI * 1.0e18);
+    sg[c + i] = (R)(sHeI * 1.0e18);
+    sg[2 * c + i] = (R)(sHeII * 1.0e18);
+    cf[i] = (R)(sHI * 1.0e18 / E);
+    cf[c + i] = (R)(sHI * 1.0e18 * fmax(1.0 - kEthHI / E, 0.0));
+    cf[2 * c + i] = (R)(sHeI * 1.0e18 / E);
+    cf[3 * c + i] = (R)(sHeI * 1.0e18 * fmax(1.0 - kEthHeI / E, 0.0));
+    cf[4 * c + i] = (R)(sHeII * 1.0e18 / E);
+    cf[5 * c + i] = (R)(sHeII * 1.0e18 * fmax(1.0 - kEthHeII / E, 0.0));
+    int idx[3], bits = inu;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        idx[k] = min(max((int)((pos[k] - org[k]) / d), 0), n[k] - 1);
+        double tmv, tdv;
+        int st;
+        if (kk[k] > 0.0) {
+            st = 1; tmv = (org[k] + (double)(idx[k] + 1) * d - pos[k]) / kk[k]; tdv = d / kk[k];
+        } else if (kk[k] < 0.0) {
+            st = -1; tmv = (org[k] + (double)idx[k] * d - pos[k]) / kk[k]; tdv = -d / kk[k];
+        } else {
+            st = 0; tmv = kHugest; tdv = kHugest;
+        }
+        rec.tm[k * c + i] = tmv;
+        rec.td[k * c + i] = tdv;
+        bits |= (st + 1) << (16 + 2 * k);
+    }
+    rec.cell[i] = idx[0] | (idx[1] << 10) | (idx[2] << 20);
+    rec.bits[i] = bits;
+}
+
+}  // namespace mochii

@@ -25,6 +25,7 @@
 #include "ctx.h"
 #include "physics.cuh"
 #include "qmc.cuh"
+#include "records.cuh"
 #include "transport.h"
 
 namespace mochii {
@@ -143,26 +144,13 @@ __device__ double block_sum(double v, double* sh) {
     return r;
 }
 
-// Packet records of one launch chunk (structure of arrays, chunk-major):
-// the DDA state after dda_init (tMax, tDelta, cell, step signs), the
-// diagnostic bin and the packet's cross sections / rate coefficients.
-struct Records {
-    double* tm;    // 3 x cap
-    double* td;    // 3 x cap
-    int* cell;     // ix | iy << 10 | iz << 20
-    int* bits;     // inu | (stp_x+1) << 16 | (stp_y+1) << 18 | (stp_z+1) << 20
-    void* sig;     // 3 x cap of R: sigma_HI, sigma_HeI, sigma_HeII in 1e-18 cm^2
-    void* coef;    // 6 x cap of R: Gamma/heat coefficients per unit path
-    long long cap;
-};
-
 // Launch kernel: one thread per packet, no divergence between packets.
 // gen_ion_photon_qmc (ion_band_mod.f90:1880-1935) with emit_point_qmc
 // (:2232-2247), build_ion_packet_physics (ion_packet_mod.f90:21-53), the
 // coefficients of score_ion_path (ion_score_mod.f90:213-221) and dda_init
 // (raytrace_amr.f90:495-532).
 template <typename R>
-__global__ void __launch_bounds__(kThreads) k_launch(const PassArgs a, Records rec, long long ip0, long long n) {
+__global__ void __launch_bounds__(kThreads) k_launch(const PassArgs a, PacketRecords rec, long long ip0, long long n) {
     __shared__ QmcTables sq;
     {
         const uint32_t* src = reinterpret_cast<const uint32_t*>(a.qmc);
@@ -194,39 +182,7 @@ __global__ void __launch_bounds__(kThreads) k_launch(const PassArgs a, Records r
     sincos(kTwoPi * uphi, &sphi, &cphi);
     const double kk[3] = {sint * cphi, sint * sphi, cost};
     const int inu = bin_of(a.eedge, a.nnu, E);
-    const double sHI = sigma_HI(E), sHeI = sigma_HeI(E), sHeII = sigma_HeII(E);
-    R* sg = static_cast<R*>(rec.sig);
-    R* cf = static_cast<R*>(rec.coef);
-    const long long c = rec.cap;
-    sg[i] = (R)(sHI * 1.0e18);
-    sg[c + i] = (R)(sHeI * 1.0e18);
-    sg[2 * c + i] = (R)(sHeII * 1.0e18);
-    cf[i] = (R)(sHI * 1.0e18 / E);
-    cf[c + i] = (R)(sHI * 1.0e18 * fmax(1.0 - kEthHI / E, 0.0));
-    cf[2 * c + i] = (R)(sHeI * 1.0e18 / E);
-    cf[3 * c + i] = (R)(sHeI * 1.0e18 * fmax(1.0 - kEthHeI / E, 0.0));
-    cf[4 * c + i] = (R)(sHeII * 1.0e18 / E);
-    cf[5 * c + i] = (R)(sHeII * 1.0e18 * fmax(1.0 - kEthHeII / E, 0.0));
-    const double d = a.dcell;
-    int idx[3], bits = inu;
-#pragma unroll
-    for (int k = 0; k < 3; ++k) {
-        idx[k] = min(max((int)((pos[k] - a.org[k]) / d), 0), a.n[k] - 1);
-        double tmv, tdv;
-        int st;
-        if (kk[k] > 0.0) {
-            st = 1; tmv = (a.org[k] + (double)(idx[k] + 1) * d - pos[k]) / kk[k]; tdv = d / kk[k];
-        } else if (kk[k] < 0.0) {
-            st = -1; tmv = (a.org[k] + (double)idx[k] * d - pos[k]) / kk[k]; tdv = -d / kk[k];
-        } else {
-            st = 0; tmv = kHugest; tdv = kHugest;
-        }
-        rec.tm[k * c + i] = tmv;
-        rec.td[k * c + i] = tdv;
-        bits |= (st + 1) << (16 + 2 * k);
-    }
-    rec.cell[i] = idx[0] | (idx[1] << 10) | (idx[2] << 20);
-    rec.bits[i] = bits;
+    write_record<R>(rec, i, pos, kk, E, inu, a.org, a.dcell, a.n);
 }
 
 // Absorber columns of one leaf, loaded ahead of use.
@@ -285,7 +241,7 @@ struct Stepper {
 // scoring: slot 0 is scored now, slots 1..LA have their column loads in
 // flight (LA = 0 disables the look-ahead).
 template <typename R, int NABS, int LA>
-__global__ void __launch_bounds__(128) k_walk_edge(const PassArgs a, const Records rec, long long n,
+__global__ void __launch_bounds__(128) k_walk_edge(const PassArgs a, const PacketRecords rec, long long n,
                                                    int accumulate) {
     typedef typename Acc<R>::T T;
     constexpr int NT = NABS == 1 ? 2 : 6;
@@ -545,7 +501,7 @@ int transport_blocks(const mochii_ctx* c) {
 // Walk-kernel variants: look-ahead depth 0..2 (the autotuned choice is
 // c->tune.lookahead); 128-thread blocks.
 template <typename R, int NABS>
-cudaError_t walk_la(mochii_ctx* c, const PassArgs& a, const Records& r, long long n, int acc, int blocks) {
+cudaError_t walk_la(mochii_ctx* c, const PassArgs& a, const PacketRecords& r, long long n, int acc, int blocks) {
     switch (c->tune.lookahead) {
         case 0: k_walk_edge<R, NABS, 0><<<blocks, 128, 0, c->stream>>>(a, r, n, acc); break;
         case 1: k_walk_edge<R, NABS, 1><<<blocks, 128, 0, c->stream>>>(a, r, n, acc); break;
@@ -554,15 +510,14 @@ cudaError_t walk_la(mochii_ctx* c, const PassArgs& a, const Records& r, long lon
     return cudaGetLastError();
 }
 
-cudaError_t launch_walk_variant(mochii_ctx* c, const PassArgs& a, const Records& r, long long n, int acc,
+cudaError_t launch_walk_variant(mochii_ctx* c, const PassArgs& a, const PacketRecords& r, long long n, int acc,
                                 int blocks) {
     if (c->fp32) return c->nabs == 1 ? walk_la<float, 1>(c, a, r, n, acc, blocks) : walk_la<float, 4>(c, a, r, n, acc, blocks);
     return c->nabs == 1 ? walk_la<double, 1>(c, a, r, n, acc, blocks) : walk_la<double, 4>(c, a, r, n, acc, blocks);
 }
 
-cudaError_t launch_transport(mochii_ctx* c) {
-    const PassArgs a = make_args(c);
-    Records r;
+PacketRecords packet_records(mochii_ctx* c) {
+    PacketRecords r;
     r.cap = c->rec.cap;
     r.tm = c->rec.tm;
     r.td = c->rec.td;
@@ -570,6 +525,14 @@ cudaError_t launch_transport(mochii_ctx* c) {
     r.bits = c->rec.bits;
     r.sig = c->rec.sig;
     r.coef = c->rec.coef;
+    return r;
+}
+
+// The stellar packets of ionizing_field_and_rates (ionizing_field_mod.f90:
+// 113-137), in chunks of the record buffer: launch, then walk.
+cudaError_t launch_transport(mochii_ctx* c) {
+    const PassArgs a = make_args(c);
+    const PacketRecords r = packet_records(c);
     const int blocks = c->tw.ledger_blocks;
     for (long long ip0 = 0; ip0 < a.np; ip0 += r.cap) {
         const long long n = a.np - ip0 < r.cap ? a.np - ip0 : r.cap;
@@ -578,6 +541,22 @@ cudaError_t launch_transport(mochii_ctx* c) {
         if (c->fp32) k_launch<float><<<lb, kThreads, 0, c->stream>>>(a, r, ip0, n);
         else k_launch<double><<<lb, kThreads, 0, c->stream>>>(a, r, ip0, n);
         const cudaError_t e = launch_walk_variant(c, a, r, n, acc, blocks);
+        if (e != cudaSuccess) return e;
+    }
+    return cudaGetLastError();
+}
+
+// The diffuse packets (ionizing_field_mod.f90:139-161): their launch records
+// come from launch_diffuse_chunk, the walk is the stellar one.
+cudaError_t launch_transport_diffuse(mochii_ctx* c, double total, long long nd) {
+    const PassArgs a = make_args(c);
+    const PacketRecords r = packet_records(c);
+    const int blocks = c->tw.ledger_blocks;
+    for (long long ip0 = 0; ip0 < nd; ip0 += r.cap) {
+        const long long n = nd - ip0 < r.cap ? nd - ip0 : r.cap;
+        cudaError_t e = launch_diffuse_chunk(c, total, ip0, n);
+        if (e != cudaSuccess) return e;
+        e = launch_walk_variant(c, a, r, n, 1, blocks);
         if (e != cudaSuccess) return e;
     }
     return cudaGetLastError();
@@ -683,6 +662,40 @@ cudaError_t noalloc_scratch(double** out) {
 }  // namespace
 
 long long noalloc_max_records() { return kNoallocMaxRecords; }
+
+}  // namespace mochii
+
+namespace mochii {
+namespace {
+// Dump of packet records for the test hooks: start cell, tMax, the H I
+// cross section and the bin, as (ix, iy, iz, tMax_x, tMax_y, tMax_z,
+// sigma_HI*1e18, inu).
+template <typename R>
+__global__ void k_records_dump(const PacketRecords r, long long n, double* out) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int cell = r.cell[i];
+    double* o = out + 8 * i;
+    o[0] = cell & 1023; o[1] = (cell >> 10) & 1023; o[2] = (cell >> 20) & 1023;
+    o[3] = r.tm[i]; o[4] = r.tm[r.cap + i]; o[5] = r.tm[2 * r.cap + i];
+    o[6] = (double)static_cast<const R*>(r.sig)[i];
+    o[7] = (double)(r.bits[i] & 0xFFFF);
+}
+}  // namespace
+
+cudaError_t launch_records_from_buffer(mochii_ctx* c, long long n, double* host_out) {
+    double* d = nullptr;
+    cudaError_t e = cudaMallocAsync(&d, (size_t)n * 64, c->stream);
+    if (e != cudaSuccess) return e;
+    const PacketRecords r = packet_records(c);
+    if (c->fp32) k_records_dump<float><<<grid_blocks(n, 128, 1 << 30), 128, 0, c->stream>>>(r, n, d);
+    else k_records_dump<double><<<grid_blocks(n, 128, 1 << 30), 128, 0, c->stream>>>(r, n, d);
+    e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaMemcpyAsync(host_out, d, (size_t)n * 64, cudaMemcpyDeviceToHost, c->stream);
+    cudaFreeAsync(d, c->stream);
+    if (e != cudaSuccess) return e;
+    return cudaStreamSynchronize(c->stream);
+}
 
 cudaError_t launch_records_noalloc(mochii_ctx* c, long long ip0, long long n, double* host_out) {
     double* scratch = nullptr;

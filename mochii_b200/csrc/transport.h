@@ -3,11 +3,17 @@
 #include <cuda_runtime.h>
 
 #include "ctx.h"
+#include "records.cuh"
 
 namespace mochii {
 
 int transport_blocks(const mochii_ctx* c);
 cudaError_t launch_transport(mochii_ctx* c);
+PacketRecords packet_records(mochii_ctx* c);
+cudaError_t launch_transport_diffuse(mochii_ctx* c, double total, long long nd);
+cudaError_t diffuse_build(mochii_ctx* c, double* total);
+size_t diffuse_scan_bytes(long long nleaf);
+cudaError_t launch_diffuse_chunk(mochii_ctx* c, double total, long long ip0, long long n);
 cudaError_t launch_rates(mochii_ctx* c);
 cudaError_t launch_jt_export(mochii_ctx* c, double* dst);
 cudaError_t launch_sobol(const QmcTables* t, int stream01, long long idx0, long long n, int nd, double* out,
@@ -15,6 +21,7 @@ cudaError_t launch_sobol(const QmcTables* t, int stream01, long long idx0, long 
 cudaError_t launch_walk(mochii_ctx* c, const double* rays, long long nray, int max_steps, int* leaves, int* nsteps);
 cudaError_t launch_records(mochii_ctx* c, long long ip0, long long n, double* out);
 long long noalloc_max_records();
+cudaError_t launch_records_from_buffer(mochii_ctx* c, long long n, double* host_out);
 cudaError_t launch_records_noalloc(mochii_ctx* c, long long ip0, long long n, double* host_out);
 
 int balance_blocks(const mochii_ctx* c);

@@ -176,6 +176,16 @@ class Nebula:
                                              leaves.ctypes.data, nsteps.ctypes.data))
         return leaves, nsteps
 
+    def diffuse_records(self, ip0, n):
+        """Diffuse field of the current state and the launch records of
+        diffuse packets ip0..ip0+n-1: (ix, iy, iz, tMax_x, tMax_y, tMax_z,
+        sigma_HI*1e18, inu) each; returns (records, diffuse_lum, diffuse_nphot)."""
+        out = np.zeros((n, 8), dtype=np.float64)
+        lum, nph = C.c_double(), C.c_int64()
+        self._ok(self.lib.mochii_diffuse_records(self.ctx, int(ip0), int(n), out.ctypes.data, C.byref(lum),
+                                                  C.byref(nph)))
+        return out, lum.value, nph.value
+
     def launch_records(self, ip0, n):
         out = np.zeros((n, 8), dtype=np.float64)
         self._ok(self.lib.mochii_launch_records(self.ctx, int(ip0), int(n), out.ctypes.data))

@@ -235,6 +235,25 @@ long long orc_sim_set(void* h, const char* name, const double* in, long long n) 
     std::memcpy(v->data(), in, (size_t)n * sizeof(double));
     return n;
 }
+// Diffuse field: build from the current state, then launch records.
+double orc_sim_diffuse_build(void* h, long long* nphot) {
+    auto* s = static_cast<Sim*>(h);
+    s->diffuse_build(s->band.ion_Ltot / (double)s->par.nphotons);
+    *nphot = s->diffuse_nphot;
+    return s->diffuse_lum;
+}
+void orc_sim_diffuse_photon(void* h, long long ip, double* out8) {
+    auto* s = static_cast<Sim*>(h);
+    Photon ph;
+    s->gen_diffuse_qmc(ip, ph);
+    out8[0] = ph.x; out8[1] = ph.y; out8[2] = ph.z;
+    out8[3] = ph.kx; out8[4] = ph.ky; out8[5] = ph.kz;
+    out8[6] = ph.E; out8[7] = ph.inu;
+}
+double orc_milne_sample(void* h, int ich, double T, double u) {
+    auto* s = static_cast<Sim*>(h);
+    return s->milne.sample(ich, T, u, s->par.eion_max);
+}
 // Launch record of packet ip: x,y,z,kx,ky,kz,E,inu
 void orc_sim_photon(void* h, long long ip, double* out8) {
     auto* s = static_cast<Sim*>(h);

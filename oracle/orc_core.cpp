@@ -655,6 +655,7 @@ bool parse_namelist(const std::string& text, Par& p, std::string* err) {
         B(solve_te); D(te_min); D(te_max); D(gas_tol_te); B(use_metals);
         B(diffuse_field); B(use_sec_ion); B(ion_add_dust); B(ion_dust_scatter);
         S(dust_density_law); D(cext_dust); S(data_dir); S(atomic_dir); S(ion_dust_kext);
+        S(diffuse_energy_model);
         else if (k == "dgr") p.DGR = to_dbl(s);
         else if (k == "he_abund") p.He_abund = to_dbl(s);
         else if (k == "nh_const") p.nH_const = to_dbl(s);
@@ -930,8 +931,8 @@ bool Sim::setup(const std::string& nl, std::string* err) {
         set_err(err, "oracle: only the namelist car grid is restated");
         return false;
     }
-    if (par.use_metals || par.diffuse_field || par.ion_add_dust || par.use_sec_ion || par.add_fuv) {
-        set_err(err, "oracle: metals/diffuse/dust/sec_ion/fuv not restated yet");
+    if (par.use_metals || par.ion_add_dust || par.use_sec_ion || par.add_fuv) {
+        set_err(err, "oracle: metals/dust/sec_ion/fuv not restated yet");
         return false;
     }
     if (par.solve_te) {
@@ -977,6 +978,7 @@ bool Sim::setup(const std::string& nl, std::string* err) {
         st.ne[i] = st.nH[i] * ((1.0 - st.xHI[i]) +
                                par.He_abund * (st.xHeII[i] + 2.0 * std::max(0.0, 1.0 - st.xHeI[i] - st.xHeII[i])));
     if (!band_setup(par, band, err)) return false;
+    if (par.diffuse_field) milne.setup(par.eion_max);   // main.f90:102
     if (par.launch_sequence != "sobol") {
         set_err(err, "oracle: only the sobol launch sequence is restated");
         return false;
@@ -1165,9 +1167,236 @@ void Sim::transport_pass() {
             t.escaped += (long double)(lum * tr);
         }
     }
+    // diffuse ground-recombination packets from the current state,
+    // ionizing_field_mod.f90:139-161 (stream 2, 9 launch dimensions)
+    if (par.diffuse_field) {
+        diffuse_build(band.ion_Ltot / (double)par.nphotons);
+        const int64_t nd = diffuse_nphot;
+#pragma omp parallel num_threads(nt)
+        {
+            int tid = 0;
+#ifdef _OPENMP
+            tid = omp_get_thread_num();
+#endif
+            Tally& t = loc[tid];
+            Photon ph;
+            for (int64_t ip = 1 + tid; ip <= nd; ip += nt) {
+                gen_diffuse_qmc(ip - 1, ph);
+                double tau_edge = 0.0;
+                walk_edge_car(ph, t, &tau_edge);
+                const double lum = ph.Lpacket * ph.wgt;
+                const double tr = std::exp(-std::max(tau_edge, 0.0));
+                t.emitted += (long double)lum;
+                t.absorbed += (long double)(lum * (1.0 - tr));
+                t.escaped += (long double)(lum * tr);
+            }
+        }
+    }
     tally.reset(nleaf, nnu);
     for (auto& t : loc) tally.add(t);
     gas_rates_compute();
+}
+
+// ---- milne_recomb_spectrum_mod.f90 -------------------------------------------
+static double milne_sigma(int ich, double E) {
+    return ich == 0 ? sigma_HI(E) : ich == 1 ? sigma_HeI(E) : sigma_HeII(E);
+}
+
+void Milne::setup(double eion_max) {   // :99-228 (the table part)
+    eth[0] = ETH_HI; eth[1] = ETH_HEI; eth[2] = ETH_HEII;
+    const double XMAX = 60.0, TLO = 1.0e2, THI = 1.0e6;
+    for (int ix = 1; ix <= NX; ++ix) {
+        const double t = (double)(ix - 1) / (double)(NX - 1);
+        xg[ix - 1] = XMAX * t * t;
+    }
+    for (int it = 1; it <= NT; ++it)
+        lgT[it - 1] = std::log10(TLO) + (std::log10(THI) - std::log10(TLO)) * (double)(it - 1) / (double)(NT - 1);
+    cdf.assign((size_t)NX * NT * NCH, 0.0);
+    xbar.assign((size_t)NT * NCH, 0.0);
+    frac.assign((size_t)NT * NCH, 0.0);
+    for (int ich = 0; ich < NCH; ++ich) {
+        for (int it = 0; it < NT; ++it) {
+            double* c = &cdf[((size_t)ich * NT + it) * NX];
+            const double T_K = std::pow(10.0, lgT[it]);
+            const double kT = KBOLTZ_CGS * T_K / EV2ERG;
+            auto shape = [&](double x) {
+                const double E = eth[ich] + x * kT;
+                return E * E * milne_sigma(ich, E) * std::exp(-x);
+            };
+            const double x_hi = std::min(XMAX, (eion_max - eth[ich]) / kT);
+            if (x_hi <= 0.0) {
+                for (int ix = 0; ix < NX; ++ix) c[ix] = 1.0;
+                xbar[(size_t)ich * NT + it] = 0.0;
+                frac[(size_t)ich * NT + it] = 0.0;
+                continue;
+            }
+            double sum_n = 0.0, sum_e = 0.0, sum_xn = 0.0;
+            c[0] = 0.0;
+            for (int ix = 1; ix <= NX - 1; ++ix) {
+                const double xa = xg[ix - 1];
+                const double xb = std::min(xg[ix], x_hi);
+                if (xb > xa) {
+                    const double xm = 0.5 * (xa + xb);
+                    const double fa = shape(xa), fm = shape(xm), fb = shape(xb);
+                    const double seg_n = (xb - xa) / 6.0 * (fa + 4.0 * fm + fb);
+                    const double seg_e = (xb - xa) / 6.0 *
+                                         (fa * (eth[ich] + xa * kT) + 4.0 * fm * (eth[ich] + xm * kT) + fb * (eth[ich] + xb * kT));
+                    sum_n = sum_n + seg_n;
+                    sum_e = sum_e + seg_e;
+                    sum_xn = sum_xn + (xb - xa) / 6.0 * (fa * xa + 4.0 * fm * xm + fb * xb);
+                }
+                c[ix] = sum_e;
+            }
+            double tail_n = sum_n;
+            if (x_hi < XMAX) {
+                double xa = x_hi;
+                while (xa < XMAX) {
+                    const double xb = std::min(xa + 0.25, XMAX);
+                    const double xm = 0.5 * (xa + xb);
+                    tail_n = tail_n + (xb - xa) / 6.0 * (shape(xa) + 4.0 * shape(xm) + shape(xb));
+                    xa = xb;
+                }
+            }
+            if (sum_e > 0.0) {
+                for (int ix = 0; ix < NX; ++ix) c[ix] = c[ix] / sum_e;
+            } else {
+                for (int ix = 0; ix < NX; ++ix) c[ix] = 1.0;
+            }
+            c[NX - 1] = 1.0;
+            xbar[(size_t)ich * NT + it] = sum_xn / std::max(sum_n, TINEST);
+            frac[(size_t)ich * NT + it] = sum_n / std::max(tail_n, TINEST);
+        }
+    }
+}
+
+void Milne::tbracket(double T, int& it, double& w) const {   // it 1-based
+    double s = (std::log10(std::max(T, TINEST)) - lgT[0]) / (lgT[1] - lgT[0]);
+    s = std::min(std::max(s, 0.0), (double)(NT - 1));
+    it = std::min((int)s + 1, NT - 1);
+    w = s - (double)(it - 1);
+}
+
+double Milne::energy_per_recomb(int ich, double T) const {
+    int it;
+    double w;
+    tbracket(T, it, w);
+    const double xb = (1.0 - w) * xbar[(size_t)ich * NT + it - 1] + w * xbar[(size_t)ich * NT + it];
+    const double fk = (1.0 - w) * frac[(size_t)ich * NT + it - 1] + w * frac[(size_t)ich * NT + it];
+    const double kT = KBOLTZ_CGS * T / EV2ERG;
+    return fk * (eth[ich] + xb * kT);
+}
+
+double Milne::sample(int ich, double T, double u, double eion_max) const {
+    int it;
+    double w;
+    tbracket(T, it, w);
+    const double kT = KBOLTZ_CGS * T / EV2ERG;
+    const double uu = std::min(std::max(u, 0.0), 1.0);
+    const double* c0 = &cdf[((size_t)ich * NT + it - 1) * NX];
+    const double* c1 = &cdf[((size_t)ich * NT + it) * NX];
+    int lo = 1, hi = NX;
+    double ca = (1.0 - w) * c0[lo - 1] + w * c1[lo - 1];
+    double cb = (1.0 - w) * c0[hi - 1] + w * c1[hi - 1];
+    while (hi - lo > 1) {
+        const int mid = (lo + hi) / 2;
+        const double cm = (1.0 - w) * c0[mid - 1] + w * c1[mid - 1];
+        if (uu > cm) { lo = mid; ca = cm; } else { hi = mid; cb = cm; }
+    }
+    double x;
+    if (cb > ca) x = xg[lo - 1] + (xg[hi - 1] - xg[lo - 1]) * (uu - ca) / (cb - ca);
+    else x = xg[lo - 1];
+    double E = eth[ich] + x * kT;
+    return std::min(E, eion_max * (1.0 - 1.0e-12));
+}
+
+// ---- diffuse_mod.f90 ---------------------------------------------------------
+// diffuse_build, diffuse_mod.f90:60-121 (milne energy model; no He I
+// excited channel).
+void Sim::diffuse_build(double lpacket) {
+    const int nleaf = grid.nleaf;
+    dif_ch.assign((size_t)4 * nleaf, 0.0);
+    dif_cdf.assign(nleaf, 0.0);
+    const double w = grid.dcell * par.distance2cm;
+    const double vol = w * w * w;
+    for (int il = 0; il < nleaf; ++il) {
+        const double nH = st.nH[il];
+        if (nH <= 0.0) continue;
+        const double T = st.Te[il], ne = st.ne[il];
+        const double kT = KBOLTZ_CGS * T / EV2ERG;
+        const double xHeIII = std::max(0.0, 1.0 - st.xHeI[il] - st.xHeII[il]);
+        const double nHII = nH * (1.0 - st.xHI[il]);
+        const double nHeII = nH * par.He_abund * st.xHeII[il];
+        const double nHeIII = nH * par.He_abund * xHeIII;
+        auto mean_e = [&](int ich, double eth) {
+            if (par.diffuse_energy_model == "milne") return milne.energy_per_recomb(ich, T);
+            if (par.diffuse_energy_model == "exponential") return eth + kT;
+            return eth;
+        };
+        double a1 = alphaA_HII(rm, T) - alphaB_HII(rm, T);
+        dif_ch[4 * (size_t)il + 0] = ne * nHII * a1 * mean_e(0, ETH_HI) * EV2ERG * vol;
+        a1 = alphaA_HeII(rm, T) - alphaB_HeII(rm, T);
+        dif_ch[4 * (size_t)il + 1] = ne * nHeII * a1 * mean_e(1, ETH_HEI) * EV2ERG * vol;
+        a1 = alphaA_HeIII(rm, T) - alphaB_HeIII(rm, T);
+        dif_ch[4 * (size_t)il + 2] = ne * nHeIII * a1 * mean_e(2, ETH_HEII) * EV2ERG * vol;
+    }
+    diffuse_lum = 0.0;
+    for (int il = 0; il < nleaf; ++il) {
+        const double* c = &dif_ch[4 * (size_t)il];
+        diffuse_lum = diffuse_lum + (((c[0] + c[1]) + c[2]) + c[3]);
+        dif_cdf[il] = diffuse_lum;
+    }
+    if (diffuse_lum > 0.0) {
+        for (auto& v : dif_cdf) v = v / diffuse_lum;
+        diffuse_nphot = (int64_t)std::llround(diffuse_lum / lpacket);
+    } else {
+        diffuse_nphot = 0;
+    }
+}
+
+// gen_diffuse_photon_qmc, diffuse_mod.f90:221-296 (ground channels).
+void Sim::gen_diffuse_qmc(int64_t ip, Photon& ph) const {
+    double u[9];
+    for (int d = 1; d <= 9; ++d) u[d - 1] = qmc.uniform(ip, d, 2);
+    const int nleaf = grid.nleaf;
+    int lo = 1, hi = nleaf;
+    while (lo < hi) {
+        const int mid = (lo + hi) / 2;
+        if (dif_cdf[mid - 1] < u[0]) lo = mid + 1; else hi = mid;
+    }
+    const int il = lo - 1;
+    const int ix = il % grid.nx, iy = (il / grid.nx) % grid.ny, iz = il / (grid.nx * grid.ny);
+    const double half = 0.5 * grid.dcell;
+    ph.x = (grid.xmin + ((double)ix + 0.5) * grid.dcell) + (2.0 * u[1] - 1.0) * half;
+    ph.y = (grid.ymin + ((double)iy + 0.5) * grid.dcell) + (2.0 * u[2] - 1.0) * half;
+    ph.z = (grid.zmin + ((double)iz + 0.5) * grid.dcell) + (2.0 * u[3] - 1.0) * half;
+    const double cost = 2.0 * u[4] - 1.0;
+    const double sint = std::sqrt(1.0 - cost * cost);
+    const double phi = TWOPI * u[5];
+    ph.kx = sint * std::cos(phi);
+    ph.ky = sint * std::sin(phi);
+    ph.kz = cost;
+    const double* w = &dif_ch[4 * (size_t)il];
+    const double uu = u[6] * (((w[0] + w[1]) + w[2]) + w[3]);
+    int ch;
+    double eph;
+    if (uu <= w[0]) { ch = 0; eph = ETH_HI; }
+    else if (uu <= w[0] + w[1]) { ch = 1; eph = ETH_HEI; }
+    else if (uu <= w[0] + w[1] + w[2]) { ch = 2; eph = ETH_HEII; }
+    else { ch = 3; eph = ETH_HI; }
+    if (ch <= 2) {
+        const double T = st.Te[il];
+        const double kT = KBOLTZ_CGS * T / EV2ERG;
+        if (par.diffuse_energy_model == "milne") eph = milne.sample(ch, T, u[7], par.eion_max);
+        else if (par.diffuse_energy_model == "exponential") eph = eph + kT * (-std::log(std::max(u[7], TINEST)));
+        eph = std::min(eph, par.eion_max * 0.999);
+    }
+    ph.inu = ion_bin_of(band, eph, false);
+    ph.wgt = 1.0;
+    ph.Lpacket = band.ion_Ltot / (double)par.nphotons;
+    ph.E = eph;
+    ph.sHI = sigma_HI(eph);
+    ph.sHeI = sigma_HeI(eph);
+    ph.sHeII = sigma_HeII(eph);
 }
 
 // gas_rates_compute + ion_score_apply_hhe, gas_rates_mod.f90:82-153 and

@@ -142,6 +142,7 @@ struct Par {
     bool solve_te = false;
     double te_min = 1.0e3, te_max = 5.0e4, gas_tol_te = 1.0e-3;
     bool use_metals = false, diffuse_field = false, use_sec_ion = false;
+    std::string diffuse_energy_model = "milne";
     bool ion_add_dust = false, ion_dust_scatter = false;
     std::string dust_density_law = "global_dgr";
     double DGR = 1.0e-2, cext_dust = 1.6059e-21;
@@ -198,6 +199,18 @@ struct Photon {
 
 struct Thermal;
 
+// milne_recomb_spectrum_mod.f90: ground-continuum recombination spectra.
+struct Milne {
+    static constexpr int NT = 192, NX = 512, NCH = 3;
+    double lgT[NT], xg[NX], eth[NCH];
+    std::vector<double> cdf;           // (NX, NT, NCH): cdf[(ich*NT + it)*NX + ix]
+    std::vector<double> xbar, frac;    // (NT, NCH): [ich*NT + it]
+    void setup(double eion_max);       // :99-228
+    void tbracket(double T, int& it, double& w) const;              // :286-297
+    double energy_per_recomb(int ich, double T) const;              // :302-312
+    double sample(int ich, double T, double u, double eion_max) const;  // :320-350
+};
+
 struct Sim {
     Par par;
     Thermal* th = nullptr;           // thermal tables (solve_te)
@@ -209,6 +222,13 @@ struct Sim {
     Tally tally;
     std::vector<double> gamma_HI, gamma_HeI, gamma_HeII, heat_HI, heat_HeI, heat_HeII;
     int nthreads = 1;
+    // diffuse field (diffuse_mod.f90)
+    Milne milne;
+    std::vector<double> dif_ch, dif_cdf;   // (4, nleaf), (nleaf)
+    double diffuse_lum = 0.0;
+    int64_t diffuse_nphot = 0;
+    void diffuse_build(double lpacket);                          // diffuse_mod.f90:60-121
+    void gen_diffuse_qmc(int64_t ip, Photon& ph) const;          // diffuse_mod.f90:221-296
     bool setup(const std::string& namelist, std::string* err);
     void transport_pass();           // ionizing_field_mod.f90:72-170
     void gas_rates_compute();        // gas_rates_mod.f90:82-153

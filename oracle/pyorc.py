@@ -63,6 +63,9 @@ def load():
         "orc_gff_table": (None, [V, V]),
         "orc_cooling_total": (D, [V, D, D, D, D, D, D]),
         "orc_nlevel_cooling_at": (D, [C.c_char_p, D, D]),
+        "orc_sim_diffuse_build": (D, [V, V]),
+        "orc_sim_diffuse_photon": (None, [V, LL, V]),
+        "orc_milne_sample": (D, [V, I, D, D]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)
@@ -223,6 +226,16 @@ class Sim:
     def set(self, name, values):
         a = np.ascontiguousarray(values, dtype=float)
         assert load().orc_sim_set(self.h, name.encode(), a.ctypes.data, a.size) == a.size
+
+    def diffuse_build(self):
+        n = C.c_longlong()
+        lum = load().orc_sim_diffuse_build(self.h, C.byref(n))
+        return lum, n.value
+
+    def diffuse_photon(self, ip):
+        out = np.zeros(8)
+        load().orc_sim_diffuse_photon(self.h, int(ip), out.ctypes.data)
+        return out
 
     def photon(self, ip):
         out = np.zeros(8)

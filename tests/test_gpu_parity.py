@@ -262,3 +262,55 @@ def test_thermal_balance_matches_oracle(orc):
     assert t.min() >= 3.0e3 and t.max() <= 3.0e4
     assert np.median(t[neb.get("x_HI") < 0.1]) > 5.0e3   # photo-heated gas
     neb.close()
+
+
+def diffuse_pair(orc, n=24, nphot=60000, iters=3):
+    nl = configs.hii_thermal(nphotons=nphot, niter=iters, n=n, precision="fp64", rs_factor=1.2)
+    nl = nl.replace("/\n", " par%diffuse_field = .true.\n/\n")
+    sim = orc.Sim(nl)
+    for _ in range(iters):
+        sim.transport_pass()
+        sim.thermal_update()
+    neb = Nebula(parse_namelist(nl))
+    for f in ("x_HI", "x_HeI", "x_HeII", "n_e", "T_e"):
+        neb.set(f, sim.get(f))
+    neb.gas_opacity_fill()
+    return nl, sim, neb
+
+
+def test_diffuse_field_matches_oracle(orc):
+    """diffuse_build (per-leaf ground-recombination luminosities, Milne mean
+    energies) and the diffuse launch on the same state as the oracle.  The leaf
+    CDF is a device prefix sum whose rounding differs from the sequential sum,
+    so a packet may land in the neighbouring leaf when u1 sits within rounding
+    of a CDF step; everything else is bit-exact."""
+    nl, sim, neb = diffuse_pair(orc)
+    lum_o, n_o = sim.diffuse_build()
+    nrec = min(n_o, 4000)
+    rec, lum_g, n_g = neb.diffuse_records(0, nrec)
+    assert abs(lum_g / lum_o - 1) < 1e-12 and n_g == n_o and n_o > 100
+    L, d, nx = neb.par.xmax, 2 * neb.par.xmax / 24, 24
+    ref = np.array([sim.diffuse_photon(i) for i in range(nrec)])
+    cell_o = np.clip(((ref[:, :3] + L) / d).astype(int), 0, nx - 1)
+    same = np.all(rec[:, :3] == cell_o, axis=1)
+    assert same.mean() > 0.999
+    sig_o = np.array([orc.evaluate("sigma_HI", [e])[0] for e in ref[:, 6]]) * 1e18
+    np.testing.assert_allclose(rec[same, 6], sig_o[same], rtol=1e-14)   # Milne energies bit-exact
+    assert np.array_equal(rec[same, 7], ref[same, 7])
+    neb.close()
+
+
+def test_pass_with_diffuse_matches_oracle(orc):
+    nl, sim, neb = diffuse_pair(orc)
+    st = neb.ionizing_field_and_rates()
+    sim.transport_pass()
+    assert st.diffuse_packets > 100 and st.closure <= 5e-13
+    e, _ = sim.energy()
+    assert abs(st.energy_emitted / e[0] - 1) < 1e-12
+    for f in ("gamma_HI", "gamma_HeI", "heat_HI"):
+        g, o = neb.get(f), sim.get(f)
+        big = o > 1e-3 * o.max()
+        # a few diffuse packets start in a neighbouring leaf (prefix-sum rounding)
+        assert np.median(np.abs(g[big] / o[big] - 1)) < 1e-9
+        assert abs(g.sum() / o.sum() - 1) < 2e-3, f
+    neb.close()
