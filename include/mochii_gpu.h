@@ -119,6 +119,8 @@ typedef struct mochii_params {
     char atomic_dir[MOCHII_STRLEN];
     /* device arithmetic (not a reference key: 'fp64' or 'fp32') */
     int precision;
+    /* par%fe_levels_full: Fe n-level atoms from the '_full' files */
+    int fe_levels_full;
 } mochii_params;
 
 /* Per-pass statistics (ion_score_report_energy_closure, ion_score_mod.f90:364-387). */
@@ -197,11 +199,18 @@ int mochii_get_tuning(const mochii_ctx* ctx, mochii_tuning* out);
 
 /* ---- state exchange (host buffers; sizes in elements) ---------------------- */
 int64_t mochii_nleaf(const mochii_ctx* ctx);
+/* Metal registry shape: transitions and stages over all active elements
+ * (species_mod.f90 n_elements / elem_nstage); both 0 without metals. */
+int mochii_metal_shape(const mochii_ctx* ctx, int* ntransitions, int* nstages);
 int mochii_nnu_band(const mochii_ctx* ctx);
 /* Field names: "nH" "x_HI" "x_HeI" "x_HeII" "n_e" "T_e" "gamma_HI"
  * "gamma_HeI" "gamma_HeII" "heat_HI" "heat_HeI" "heat_HeII" (nleaf each),
  * "jt_ion" (nleaf*nnu_band, leaf-major), "eedge" (nnu_band+1),
- * "leaf_half" (nleaf). */
+ * "leaf_half" (nleaf); with par%use_metals also "gamma_metal" and
+ * "heat_metal" (nleaf*ntransitions: Gamma_<el>_stages / Heat_<el>_stages
+ * of species_write) and "x_metal" (nleaf*nstages: x_<el>_stages), each
+ * leaf-major with elements in registry order (c n o ne s ar mg fe si cl ca,
+ * those with a positive abundance) and stages ascending. */
 int mochii_get_field(mochii_ctx* ctx, const char* name, double* out, int64_t n);
 /* Upload a state field ("x_HI" "x_HeI" "x_HeII" "n_e" "T_e" "nH"). */
 int mochii_set_field(mochii_ctx* ctx, const char* name, const double* in, int64_t n);

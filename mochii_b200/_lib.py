@@ -52,6 +52,7 @@ class Params(C.Structure):
         ("DGR", C.c_double), ("cext_dust", C.c_double), ("grain_pe", C.c_int),
         ("ion_dust_kext", C.c_char * STRLEN), ("data_dir", C.c_char * STRLEN), ("atomic_dir", C.c_char * STRLEN),
         ("precision", C.c_int),
+        ("fe_levels_full", C.c_int),
     ]
 
 
@@ -87,6 +88,7 @@ SIGNATURES = {
     "mochii_balance_update": (C.c_int, [C.c_void_p, C.c_int, _P(Metrics)]),
     "mochii_opacity_fill": (C.c_int, [C.c_void_p]),
     "mochii_nleaf": (C.c_int64, [C.c_void_p]),
+    "mochii_metal_shape": (C.c_int, [C.c_void_p, _P(C.c_int), _P(C.c_int)]),
     "mochii_nnu_band": (C.c_int, [C.c_void_p]),
     "mochii_get_field": (C.c_int, [C.c_void_p, C.c_char_p, C.c_void_p, C.c_int64]),
     "mochii_set_field": (C.c_int, [C.c_void_p, C.c_char_p, C.c_void_p, C.c_int64]),

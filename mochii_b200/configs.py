@@ -119,6 +119,50 @@ def hii_thermal(nphotons=10_000_000, niter=20, n=128, precision="fp32", seed=123
 """
 
 
+# Trace metals by number of the 128^3 H II-region workload.
+METALS = dict(C=2.7e-4, N=6.8e-5, O=4.9e-4, Ne=8.5e-5, S=1.3e-5, Ar=2.5e-6, Mg=4.0e-5, Si=3.2e-5, Fe=3.2e-5,
+              Cl=3.0e-7, Ca=2.0e-6)
+
+
+def hii_metals(nphotons=10_000_000, niter=20, n=128, precision="fp32", seed=12345, rs_factor=1.0,
+               diffuse=True, solve_te=True):
+    """H+He+metals H II region with the thermal balance: 128^3 uniform grid,
+    n_H = 100, He/H 0.1, eleven trace metals, a 45 kK blackbody with Q(H) =
+    5e49 s^-1, case A with explicit diffuse Milne recombination packets, no
+    dust; T_e solved in [3e3, 3e4] K."""
+    rs = stromgren_radius_pc(Q=5.0e49) * rs_factor
+    ab = "\n".join(f" par%abund_{k} = {v:.6e}" for k, v in METALS.items())
+    return f"""&parameters
+ par%no_photons = {float(nphotons):.6e}
+ par%launch_sequence = 'sobol'
+ par%qmc_seed = {seed}
+ par%grid_type = 'car'
+ par%nx = {n}
+ par%ny = {n}
+ par%nz = {n}
+ par%xmax = {rs:.10f}
+ par%ymax = {rs:.10f}
+ par%zmax = {rs:.10f}
+ par%distance_unit = 'pc'
+ par%nH_const = 100.0
+ par%He_abund = 0.1
+ par%tstar = 4.5e4
+ par%luminosity = {5.0e49 * mean_photon_energy_ev(4.5e4) * EV2ERG:.6e}
+ par%case_ab = 'A'
+ par%diffuse_field = {'.true.' if diffuse else '.false.'}
+ par%solve_te = {'.true.' if solve_te else '.false.'}
+ par%te_min = 3.0e3
+ par%te_max = 3.0e4
+ par%te_fixed = 1.0e4
+ par%gas_niter = {niter}
+ par%use_metals = .true.
+{ab}
+ par%atomic_dir = '{ATOMIC_DIR}'
+ par%precision = '{precision}'
+/
+"""
+
+
 def hhe128(nphotons=10_000_000, niter=20, n=128, precision="fp32", seed=12345, rs_factor=1.0):
     """H+He H II region on a uniform grid, case A, fixed T_e (the He/H and
     source of the 128^3 H II-region workload; metals, diffuse packets and the

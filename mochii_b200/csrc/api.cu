@@ -15,6 +15,7 @@
 #include "mochii_gpu.h"
 #include "physics.cuh"
 #include "qmc.cuh"
+#include "species.h"
 #include "thermal.h"
 #include "transport.h"
 
@@ -41,6 +42,31 @@ cudaError_t dalloc(T** p, size_t n) {
     return cudaMalloc(reinterpret_cast<void**>(p), n * sizeof(T) + 16);
 }
 
+void free_records(mochii_ctx* c) {
+    for (void* q : {(void*)c->rec.tm, (void*)c->rec.td, (void*)c->rec.cell, (void*)c->rec.bits, c->rec.sig, c->rec.coef,
+                    (void*)c->rec.E, c->rec.msig})
+        if (q) cudaFree(q);
+    c->rec = RecordBuffers();
+}
+
+// Launch records of one chunk of up to cap packets (transport.cu).
+cudaError_t alloc_records(mochii_ctx* c, long long cap) {
+    const size_t rsz = c->fp32 ? 4 : 8;
+    c->rec.cap = cap;
+    cudaError_t e;
+    if ((e = dalloc(&c->rec.tm, 3 * (size_t)cap)) != cudaSuccess) return e;
+    if ((e = dalloc(&c->rec.td, 3 * (size_t)cap)) != cudaSuccess) return e;
+    if ((e = dalloc(&c->rec.cell, (size_t)cap)) != cudaSuccess) return e;
+    if ((e = dalloc(&c->rec.bits, (size_t)cap)) != cudaSuccess) return e;
+    if ((e = cudaMalloc(&c->rec.sig, 3 * (size_t)cap * rsz + 64)) != cudaSuccess) return e;
+    if ((e = cudaMalloc(&c->rec.coef, 6 * (size_t)cap * rsz + 64)) != cudaSuccess) return e;
+    if (c->metal.ntr > 0) {
+        if ((e = dalloc(&c->rec.E, (size_t)cap)) != cudaSuccess) return e;
+        if ((e = cudaMalloc(&c->rec.msig, (size_t)c->metal.ntrp * cap * rsz + 64)) != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+}
+
 void release(mochii_ctx* c) {
     if (!c) return;
     void* ptrs[] = {c->nH, c->xHI, c->xHeI, c->xHeII, c->ne, c->Te, c->col, c->tally, c->jt, c->rates,
@@ -48,7 +74,9 @@ void release(mochii_ctx* c) {
                     c->tab.qmc, c->tw.ledger, c->tw.counters, c->bw.partial, c->bw.counters,
                     c->rec.tm, c->rec.td, c->rec.cell, c->rec.bits, c->rec.sig, c->rec.coef,
                     c->th.gff, c->th.lamref, c->th.Ssup, c->th.tinv,
-                    c->dif.ch, c->dif.tot, c->dif.scan_tmp, c->dif.tables};
+                    c->dif.ch, c->dif.tot, c->dif.scan_tmp, c->dif.tables,
+                    (void*)c->metal.el, c->metal.egam, c->metal.eheat, c->metal.opac, c->metal.raw,
+                    (void*)c->rec.E, c->rec.msig};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     for (cudaEvent_t e : {c->ev0, c->ev1, c->evA, c->evB})
@@ -77,7 +105,6 @@ int validate(const mochii_params& p, std::string* why, int* code) {
     if (!p.car_walk_dda) return *why = "car_walk='amr' is not built; use the DDA walk (car_walk='dda')", 1;
     if (!p.source_point) return *why = "only internal point sources are built", 1;
     if (!p.launch_sobol) return *why = "launch_sequence='random' is not built; use 'sobol'", 1;
-    if (p.use_metals) return *why = "use_metals is not built in this library version", 1;
     if (p.ion_add_dust) return *why = "ion_add_dust is not built in this library version", 1;
     if (p.use_sec_ion) return *why = "use_sec_ion is not built in this library version", 1;
     if (p.add_fuv) return *why = "add_fuv is not built in this library version", 1;
@@ -122,7 +149,13 @@ extern "C" int mochii_init(const mochii_params* pin, mochii_ctx** out) {
     c->par = *pin;
     mochii_params& p = c->par;
     if (p.diffuse_field) p.caseA = 1;   // setup.f90:580-583: the diffuse field forces case A
-    if (!band_build(p, c->band, &why)) {
+    // species before the band (main.f90:64-83): the metal thresholds pin
+    // band edges and sampler knots
+    if (p.use_metals && !species_build(p, c->species, &why)) {
+        delete c;
+        return fail(nullptr, MOCHII_ERR_TABLE, why);
+    }
+    if (!band_build(p, c->band, &why, c->species.thresholds())) {
         delete c;
         return fail(nullptr, MOCHII_ERR_BAD_PARAM, why);
     }
@@ -200,6 +233,45 @@ extern "C" int mochii_init(const mochii_params* pin, mochii_ctx** out) {
     CKI(cudaMalloc(&c->jt, (size_t)n * c->nnu * tsz + 64));
     CKI(dalloc(&c->rates, 6 * (size_t)n));
     CKI(cudaMemset(c->rates, 0, 6 * (size_t)n * 8));
+    if (!c->species.tr.empty()) {
+        // registry tables in one blob: el | tr | st | photo | form | eth | lamref | Ssup
+        const SpeciesHost& sp = c->species;
+        MetalDev& m = c->metal;
+        m.nel = (int)sp.el.size();
+        m.ntr = (int)sp.tr.size();
+        m.nst = (int)sp.st.size();
+        m.ntrp = (m.ntr + 3) / 4 * 4;
+        auto al = [](size_t b) { return (b + 255) / 256 * 256; };
+        const size_t b_el = al(sp.el.size() * sizeof(MetalEl)), b_tr = al(sp.tr.size() * sizeof(MetalTr)),
+                     b_st = al(sp.st.size() * sizeof(MetalStage)), b_ph = al(sp.photo.size() * 8),
+                     b_fo = al(sp.form.size() * 4), b_et = al(sp.eth_flat.size() * 8), b_lr = al(sp.lamref.size() * 8),
+                     b_ss = al(sp.Ssup.size() * 8);
+        char* blob = nullptr;
+        CKI(cudaMalloc(&blob, b_el + b_tr + b_st + b_ph + b_fo + b_et + b_lr + b_ss));
+        char* q = blob;
+        auto put = [&](const void* src, size_t bytes, size_t span) {
+            char* dst = q;
+            if (bytes) cudaMemcpy(dst, src, bytes, cudaMemcpyHostToDevice);
+            q += span;
+            return dst;
+        };
+        m.el = reinterpret_cast<const MetalEl*>(put(sp.el.data(), sp.el.size() * sizeof(MetalEl), b_el));
+        m.tr = reinterpret_cast<const MetalTr*>(put(sp.tr.data(), sp.tr.size() * sizeof(MetalTr), b_tr));
+        m.st = reinterpret_cast<const MetalStage*>(put(sp.st.data(), sp.st.size() * sizeof(MetalStage), b_st));
+        m.photo = reinterpret_cast<const double*>(put(sp.photo.data(), sp.photo.size() * 8, b_ph));
+        m.form = reinterpret_cast<const int*>(put(sp.form.data(), sp.form.size() * 4, b_fo));
+        m.eth = reinterpret_cast<const double*>(put(sp.eth_flat.data(), sp.eth_flat.size() * 8, b_et));
+        m.lamref = reinterpret_cast<const double*>(put(sp.lamref.data(), sp.lamref.size() * 8, b_lr));
+        m.Ssup = reinterpret_cast<const double*>(put(sp.Ssup.data(), sp.Ssup.size() * 8, b_ss));
+        CKI(cudaGetLastError());
+        CKI(dalloc(&m.egam, (size_t)n * m.ntr));
+        CKI(dalloc(&m.eheat, (size_t)n * m.ntr));
+        CKI(cudaMemset(m.egam, 0, (size_t)n * m.ntr * 8));
+        CKI(cudaMemset(m.eheat, 0, (size_t)n * m.ntr * 8));
+        CKI(cudaMalloc(&m.opac, (size_t)n * m.ntrp * rsz + 64));
+        CKI(cudaMemset(m.opac, 0, (size_t)n * m.ntrp * rsz));
+        CKI(cudaMalloc(&m.raw, (size_t)n * m.ntrp * 2 * tsz + 64));
+    }
     // sampler tables, component table, bin edges, QMC tables
     std::vector<double> te, tf, tc, comp;
     std::vector<int> off{0};
@@ -235,13 +307,7 @@ extern "C" int mochii_init(const mochii_params* pin, mochii_ctx** out) {
     CKI(dalloc(&c->tw.ledger, 3 * (size_t)c->tw.ledger_blocks));
     CKI(dalloc(&c->tw.counters, 4));
     // packet records: launch chunks of up to 4 Mi packets
-    c->rec.cap = std::min<long long>(p.nphotons, 1LL << 22);
-    CKI(dalloc(&c->rec.tm, 3 * (size_t)c->rec.cap));
-    CKI(dalloc(&c->rec.td, 3 * (size_t)c->rec.cap));
-    CKI(dalloc(&c->rec.cell, (size_t)c->rec.cap));
-    CKI(dalloc(&c->rec.bits, (size_t)c->rec.cap));
-    CKI(cudaMalloc(&c->rec.sig, 3 * (size_t)c->rec.cap * rsz + 64));
-    CKI(cudaMalloc(&c->rec.coef, 6 * (size_t)c->rec.cap * rsz + 64));
+    CKI(alloc_records(c, std::min<long long>(p.nphotons, 1LL << 22)));
     c->bw.blocks = balance_blocks(c);
     if (p.diffuse_field) {
         MilneHost mh;
@@ -308,6 +374,12 @@ extern "C" void mochii_destroy(mochii_ctx* c) {
 }
 
 extern "C" int64_t mochii_nleaf(const mochii_ctx* c) { return c ? c->grid.nleaf : 0; }
+extern "C" int mochii_metal_shape(const mochii_ctx* c, int* ntransitions, int* nstages) {
+    if (!c) return MOCHII_ERR_BAD_PARAM;
+    if (ntransitions) *ntransitions = c->metal.ntr;
+    if (nstages) *nstages = c->metal.nst;
+    return MOCHII_OK;
+}
 extern "C" int mochii_nnu_band(const mochii_ctx* c) { return c ? c->nnu : 0; }
 extern "C" double mochii_ion_Ltot(const mochii_ctx* c) { return c ? c->band.ion_Ltot : 0.0; }
 
@@ -323,17 +395,9 @@ extern "C" int mochii_set_nphotons(mochii_ctx* c, int64_t np) {
     c->tw.ledger_blocks = nb;
     const long long cap = std::min<long long>(np, 1LL << 22);
     if (cap > c->rec.cap) {
-        const size_t rsz = c->fp32 ? 4 : 8;
-        for (void* q : {(void*)c->rec.tm, (void*)c->rec.td, (void*)c->rec.cell, (void*)c->rec.bits, c->rec.sig, c->rec.coef})
-            if (q) cudaFree(q);
-        c->rec = RecordBuffers();
-        c->rec.cap = cap;
-        CK(c, dalloc(&c->rec.tm, 3 * (size_t)cap));
-        CK(c, dalloc(&c->rec.td, 3 * (size_t)cap));
-        CK(c, dalloc(&c->rec.cell, (size_t)cap));
-        CK(c, dalloc(&c->rec.bits, (size_t)cap));
-        CK(c, cudaMalloc(&c->rec.sig, 3 * (size_t)cap * rsz + 64));
-        CK(c, cudaMalloc(&c->rec.coef, 6 * (size_t)cap * rsz + 64));
+        CK(c, cudaStreamSynchronize(c->stream));
+        free_records(c);
+        CK(c, alloc_records(c, cap));
     }
     return MOCHII_OK;
 }
@@ -352,6 +416,8 @@ extern "C" int mochii_transport_pass(mochii_ctx* c, int with_peel, mochii_pass_s
     // jt_ion(:,:) = 0 and ion_score_reset (ionizing_field_mod.f90:90-91)
     CK(c, cudaMemsetAsync(c->tally, 0, (size_t)n * c->ntally * tsz, c->stream));
     CK(c, cudaMemsetAsync(c->jt, 0, (size_t)n * c->nnu * tsz, c->stream));
+    if (c->metal.ntr > 0)   // species_rate_path_reset (species_mod.f90:321-326)
+        CK(c, cudaMemsetAsync(c->metal.raw, 0, (size_t)n * c->metal.ntrp * 2 * tsz, c->stream));
     CK(c, cudaMemsetAsync(c->tw.counters, 0, 4 * sizeof(unsigned long long), c->stream));
     CK(c, cudaEventRecord(c->ev0, c->stream));
     CK(c, launch_transport(c));
@@ -469,9 +535,9 @@ std::map<std::string, Tuning>& tune_cache() {
 std::string tune_key(const mochii_ctx* c) {
     cudaDeviceProp prop;
     cudaGetDeviceProperties(&prop, c->device);
-    char buf[256];
-    std::snprintf(buf, sizeof(buf), "%s|%dx%dx%d|%d|%d|%d", prop.name, c->grid.nx, c->grid.ny, c->grid.nz,
-                  c->fp32 ? 32 : 64, c->nabs, c->nnu);
+    char buf[512];
+    std::snprintf(buf, sizeof(buf), "%s|%dx%dx%d|%d|%d|%d|%d", prop.name, c->grid.nx, c->grid.ny, c->grid.nz,
+                  c->fp32 ? 32 : 64, c->nabs, c->nnu, c->metal.ntr);
     return buf;
 }
 }  // namespace
@@ -565,6 +631,26 @@ extern "C" int mochii_get_field(mochii_ctx* c, const char* name, double* out, in
     if (nm == "leaf_half") {
         if (n != c->grid.nleaf) return fail(c, MOCHII_ERR_BAD_PARAM, "leaf_half size mismatch");
         for (int64_t i = 0; i < n; ++i) out[i] = 0.5 * c->grid.dcell;
+        return MOCHII_OK;
+    }
+    if (nm == "gamma_metal" || nm == "heat_metal" || nm == "x_metal") {
+        // leaf-major blocks in registry order: transitions (Gamma, heating) or
+        // stages (fractions of the written state, species_write)
+        if (c->metal.ntr == 0) return fail(c, MOCHII_ERR_BAD_PARAM, nm + ": par%use_metals is off");
+        const long long per = nm == "x_metal" ? c->metal.nst : c->metal.ntr;
+        const long long cnt = c->grid.nleaf * per;
+        if (n != cnt) return fail(c, MOCHII_ERR_BAD_PARAM, nm + " size mismatch (nleaf*" + std::to_string(per) + ")");
+        if (nm == "x_metal") {
+            double* d = nullptr;
+            CK(c, cudaMallocAsync(&d, cnt * 8, c->stream));
+            CK(c, launch_metal_fractions(c, d));
+            CK(c, cudaMemcpyAsync(out, d, cnt * 8, cudaMemcpyDeviceToHost, c->stream));
+            CK(c, cudaFreeAsync(d, c->stream));
+        } else {
+            CK(c, cudaMemcpyAsync(out, nm == "gamma_metal" ? c->metal.egam : c->metal.eheat, cnt * 8,
+                                  cudaMemcpyDeviceToHost, c->stream));
+        }
+        CK(c, cudaStreamSynchronize(c->stream));
         return MOCHII_OK;
     }
     if (nm == "jt_ion") {

@@ -11,6 +11,7 @@
 #include <cuda_runtime.h>
 
 #include "ctx.h"
+#include "metals.cuh"
 #include "physics.cuh"
 #include "thermal.h"
 #include "transport.h"
@@ -43,6 +44,8 @@ struct BalArgs {
     RateSel rs;
     Coef k;   // coefficients at the fixed temperature (equilibrium update)
     int caseA, nabs, fp32;
+    MetalDev m;                       // trace metals; m.ntr == 0 without
+    int metal_ne, two_way, metal_heat, metal_ff;
 };
 
 // Absorber columns n_i * distance2cm * 1e-18 for one leaf.
@@ -64,12 +67,28 @@ __device__ __forceinline__ void write_columns(void* col, long long il, int nabs,
     }
 }
 
+// The metal opacity weights of one leaf at its written state (T_e, n_e, x_HI).
+__device__ __noinline__ void metal_fill_at(const MetalDev& m, MetalCache& mc, long long il, double T, double nH,
+                                           double ne, double xHI, double scale, int fp32) {
+    metal_prepare(m, il, T, mc);
+    if (fp32) metal_opacity_fill<float>(m, mc, il, nH, ne, xHI, scale);
+    else metal_opacity_fill<double>(m, mc, il, nH, ne, xHI, scale);
+}
+
+// gas_opacity_fill (gas_opacity_mod.f90:299-306): absorber columns and, with
+// metals, the stage-fraction opacity weights (species_stage_cache_refresh).
 __global__ void k_columns(const double* __restrict__ nH, const double* __restrict__ xHI,
-                          const double* __restrict__ xHeI, const double* __restrict__ xHeII, void* col,
-                          long long nleaf, int nabs, int fp32, double yHe, double scale) {
+                          const double* __restrict__ xHeI, const double* __restrict__ xHeII,
+                          const double* __restrict__ ne, const double* __restrict__ Te, void* col,
+                          long long nleaf, int nabs, int fp32, double yHe, double scale, const MetalDev m) {
     for (long long il = (long long)blockIdx.x * blockDim.x + threadIdx.x; il < nleaf;
-         il += (long long)gridDim.x * blockDim.x)
+         il += (long long)gridDim.x * blockDim.x) {
         write_columns(col, il, nabs, fp32, nH[il], yHe, xHI[il], xHeI[il], xHeII[il], scale);
+        if (m.ntr > 0) {
+            MetalCache mc;
+            metal_fill_at(m, mc, il, Te[il], nH[il], ne[il], xHI[il], scale, fp32);
+        }
+    }
 }
 
 __host__ __device__ Coef coef_at(const RateSel& rs, int caseA, double T) {
@@ -112,6 +131,46 @@ __device__ int solve_cell(const Coef& k, double yHe, double gH, double gHe1, dou
     return it;
 }
 
+// solve_ion_cell with the metal cascade (ion_balance_mod.f90:53-150): metal
+// electrons join the n_e closure (metal_ne), and with the two-way charge
+// exchange x_HI is the root of hydrogen's balance at each n_e
+// (hydrogen_neutral_fraction); the cache mc is prepared at T.
+__device__ __noinline__ int solve_cell_metal(const Coef& k, double yHe, double gH, double gHe1, double gHe2, double nH,
+                                             double& xHI, double& xHeI, double& xHeII, double& ne, const MetalDev& m,
+                                             const MetalCache& mc, int with_ne, int with_cx) {
+    double xHeIII = fmax(0.0, 1.0 - xHeI - xHeII);
+    ne = nH * ((1.0 - xHI) + yHe * (xHeII + 2.0 * xHeIII));
+    ne = fmax(ne, 1.0e-12 * nH);
+    double nem = 0.0, rin = 0.0, rout = 0.0;
+    int it = 1;
+    for (; it <= 200; ++it) {
+        const double ne_old = ne;
+        if (with_ne || with_cx) {
+            metal_sums(m, mc, nH, ne_old, nH * xHI, nH * (1.0 - xHI), nem, rin, rout);
+            if (!with_cx) {
+                rin = 0.0;
+                rout = 0.0;
+            }
+        }
+        if (with_cx) {
+            xHI = hydrogen_neutral_fraction(m, mc, nH, ne, k.aH * ne, gH + (k.cH + k.aH) * ne);
+        } else {
+            const double denH = gH + (k.cH + k.aH) * ne + rin + rout;
+            xHI = denH > 0.0 ? (k.aH * ne + rin) / denH : 1.0;
+        }
+        const double r1 = fmin((gHe1 + k.cHe1 * ne) / (k.aHe2 * ne), 1.0e150);
+        const double r2 = fmin((gHe2 + k.cHe2 * ne) / (k.aHe3 * ne), 1.0e150);
+        xHeI = 1.0 / (1.0 + r1 + r1 * r2);
+        xHeII = xHeI * r1;
+        xHeIII = xHeII * r2;
+        ne = nH * ((1.0 - xHI) + yHe * (xHeII + 2.0 * xHeIII));
+        if (with_ne) ne = ne + nem;
+        ne = fmax(0.5 * (ne + ne_old), 1.0e-12 * nH);
+        if (fabs(ne - ne_old) <= 1.0e-10 * ne) break;
+    }
+    return it;
+}
+
 __global__ void __launch_bounds__(kBThreads) k_balance(const BalArgs a) {
     __shared__ double sh[3][kBThreads];
     double mdx = 0.0, sdx = 0.0, sx = 0.0;
@@ -126,8 +185,16 @@ __global__ void __launch_bounds__(kBThreads) k_balance(const BalArgs a) {
             continue;
         }
         double xHI = x0, xHeI = h10, xHeII = h20, ne;
-        const int it = solve_cell(a.k, a.yHe, a.rates[il], a.rates[a.nleaf + il], a.rates[2 * a.nleaf + il], nH, xHI,
-                                  xHeI, xHeII, ne);
+        MetalCache mc;
+        int it;
+        if (a.m.ntr > 0) {
+            metal_prepare(a.m, il, a.T, mc);
+            it = solve_cell_metal(a.k, a.yHe, a.rates[il], a.rates[a.nleaf + il], a.rates[2 * a.nleaf + il], nH, xHI,
+                                  xHeI, xHeII, ne, a.m, mc, a.metal_ne, a.two_way);
+        } else {
+            it = solve_cell(a.k, a.yHe, a.rates[il], a.rates[a.nleaf + il], a.rates[2 * a.nleaf + il], nH, xHI, xHeI,
+                            xHeII, ne);
+        }
         ++solved;
         if (it > 200) ++caps;
         const double w = a.relax;
@@ -138,7 +205,17 @@ __global__ void __launch_bounds__(kBThreads) k_balance(const BalArgs a) {
         a.xHI[il] = xn;
         a.xHeI[il] = h1n;
         a.xHeII[il] = h2n;
-        a.ne[il] = nH * ((1.0 - xn) + a.yHe * (h2n + 2.0 * h3n));
+        double nen = nH * ((1.0 - xn) + a.yHe * (h2n + 2.0 * h3n));
+        if (a.m.ntr > 0) {
+            // metal electrons of the written state (ion_balance_mod.f90:401-410),
+            // then the stage cache at the written T_e (gas_opacity_fill)
+            if (a.metal_ne) nen = charge_neutrality_ne(a.m, mc, nH, nen, xn, ne);
+            const double Tw = a.Te[il];
+            if (Tw != a.T) metal_prepare(a.m, il, Tw, mc);
+            if (a.fp32) metal_opacity_fill<float>(a.m, mc, il, nH, nen, xn, a.colscale);
+            else metal_opacity_fill<double>(a.m, mc, il, nH, nen, xn, a.colscale);
+        }
+        a.ne[il] = nen;
         write_columns(a.col, il, a.nabs, a.fp32, nH, a.yHe, xn, h1n, h2n, a.colscale);
         const double dx = fabs(xn - x0);
         mdx = fmax(mdx, dx);
@@ -196,35 +273,36 @@ __device__ double gbar_ff(const double* __restrict__ gff, double T, int Z) {
 // Lambda = lam_fit [f_cov S + 1 - f_cov], S = Lambda_SE(T, ne)/Lambda_SE(T, floor),
 // f_cov = min(1, Lambda_SE(T, floor)/lam_fit); ln(Lambda) linear in 1/T
 // inside a log-T cell and log-linear in log n_e (nlevel_cooling_mod.f90:163-271).
-__device__ double nl_col(const ThermalDev& t, int it, int j, double w1, double wt) {
-    const double Li = t.lamref[it - 1] * t.Ssup[(it - 1) * kNlNNE + (j - 1)];
-    const double Lip = t.lamref[it] * t.Ssup[it * kNlNNE + (j - 1)];
+__device__ double nl_col(const double* lamref, const double* Ssup, int it, int j, double w1, double wt) {
+    const double Li = lamref[it - 1] * Ssup[(it - 1) * kNlNNE + (j - 1)];
+    const double Lip = lamref[it] * Ssup[it * kNlNNE + (j - 1)];
     if (Li > 0.0 && Lip > 0.0) return exp(log(Li) + w1 * (log(Lip) - log(Li)));
     return Li * (1.0 - wt) + Lip * wt;
 }
 
-__device__ double nl_apply(const ThermalDev& t, double lam_fit, double T, double ne) {
+__device__ __noinline__ double nl_apply(const double* lamref, const double* Ssup, const double* tinv, double lam_fit,
+                                        double T, double ne) {
     const double lt = fmin(fmax(log10(T), 2.0), 2.0 + 0.01 * (double)(kNlNT - 1));
     const int it = min((int)((lt - 2.0) / 0.01) + 1, kNlNT - 1);
     const double gi = 2.0 + 0.01 * (double)(it - 1), gi1 = 2.0 + 0.01 * (double)it;
-    const double w1 = (1.0 / pow(10.0, lt) - t.tinv[it - 1]) / (t.tinv[it] - t.tinv[it - 1]);
+    const double w1 = (1.0 / pow(10.0, lt) - tinv[it - 1]) / (tinv[it] - tinv[it - 1]);
     const double wt = fmin(fmax((lt - gi) / (gi1 - gi), 0.0), 1.0);
-    const double lamref = nl_col(t, it, 1, w1, wt);
+    const double lref = nl_col(lamref, Ssup, it, 1, w1, wt);
     const double lne = log10(ne);
     double lam;
     if (lne <= -6.0) {
-        lam = lamref;
+        lam = lref;
     } else if (lne >= -6.0 + 0.1 * (double)(kNlNNE - 1)) {
-        lam = nl_col(t, it, kNlNNE, w1, wt);
+        lam = nl_col(lamref, Ssup, it, kNlNNE, w1, wt);
     } else {
         const int je = min((int)((lne + 6.0) / 0.1) + 1, kNlNNE - 1);
         const double gj = -6.0 + 0.1 * (double)(je - 1), gj1 = -6.0 + 0.1 * (double)je;
         const double wn = (lne - gj) / (gj1 - gj);
-        const double L0 = nl_col(t, it, je, w1, wt), L1 = nl_col(t, it, je + 1, w1, wt);
+        const double L0 = nl_col(lamref, Ssup, it, je, w1, wt), L1 = nl_col(lamref, Ssup, it, je + 1, w1, wt);
         lam = (L0 > 0.0 && L1 > 0.0) ? exp(log(L0) + wn * (log(L1) - log(L0))) : L0 * (1.0 - wn) + L1 * wn;
     }
-    const double S = lam / fmax(lamref, kTinest);
-    const double fcov = fmin(1.0, lamref / fmax(lam_fit, kTinest));
+    const double S = lam / fmax(lref, kTinest);
+    const double fcov = fmin(1.0, lref / fmax(lam_fit, kTinest));
     return lam_fit * (fcov * S + (1.0 - fcov));
 }
 
@@ -251,19 +329,86 @@ __device__ __noinline__ double cooling_total(const ThermalDev& t, const RateSel&
     double fit = 0.0;
     for (int i = 0; i < t.hi_nterm; ++i) fit = fit + t.hi_A[i] * exp(-t.hi_T[i] / T);
     fit = fit / sqrt(T);
-    const double lam = t.use_hi_table ? nl_apply(t, fit, T, ne) : fit;
+    const double lam = t.use_hi_table ? nl_apply(t.lamref, t.Ssup, t.tinv, fit, T, ne) : fit;
     return cool + ne * nHI * lam;
 }
 
-// net_rate (thermal_mod.f90:38-115), H/He path.
+// The metal terms of net_rate (thermal_mod.f90:53-71): metal_cooling
+// (species_mod.f90:825-846), metal_cooling_H (:704-731), metal_freefree
+// (:852-871) and metal_heating (:739-752).  One evaluation of each element's
+// stage chain (from the cache at T) serves all four sums.
+__device__ __noinline__ MetalThermalTerms metal_thermal(const ThermalDev& td, const MetalDev& m, const MetalCache& c,
+                                                        long long il, double T, double nH, double ne, double nHI,
+                                                        double nHII) {
+    const double A_CII = 2.321e-6, A_OI = 8.865e-5;
+    MetalThermalTerms o = {0.0, 0.0, 0.0, 0.0};
+    double g[4];
+    for (int z = 1; z <= 4; ++z) g[z - 1] = gbar_ff(td.gff, T, z);
+    const double rsT = 1.0 / sqrt(T);
+    double ff = 0.0;
+    double r[kMaxSt], frac[kMaxSt];
+    for (int ie = 0; ie < m.nel; ++ie) {
+        const MetalEl e = m.el[ie];
+        frac[0] = metal_chain(c, e.tr0, e.nstage, ne, nHI, nHII, r);
+        for (int i = 2; i <= e.nstage; ++i) frac[i - 1] = frac[i - 2] * r[i - 2];
+        const double nel = e.abund * nH;
+        for (int i = 1; i <= e.nstage; ++i) {
+            const MetalStage& st = m.st[e.st0 + i - 1];
+            if (!st.has_cool) continue;
+            double fit = 0.0;
+            for (int q = 0; q < st.nterm; ++q) fit = fit + st.A[q] * exp(-st.Ti[q] / T);
+            fit = fit * rsT;
+            const double lam = st.table >= 0 ? nl_apply(m.lamref + (size_t)st.table * kNlNT,
+                                                        m.Ssup + (size_t)st.table * kNlNT * kNlNNE, td.tinv, fit, T, ne)
+                                             : fit;
+            o.cool = o.cool + ne * nel * frac[i - 1] * lam;
+        }
+        if (e.kind == 1 && e.nstage >= 2) {   // [C II] 158 um, H impact
+            const double nion = e.abund * nH * frac[1];
+            const double qul = 7.6e-10 * pow(T / 100.0, 0.14);
+            const double qlu = 2.0 * qul * exp(-91.25 / T);
+            o.cool_H = o.cool_H + nion * nHI * qlu * (91.25 * kKboltz) / (1.0 + nHI * (qul + qlu) / A_CII);
+        } else if (e.kind == 2) {             // [O I] 63 um
+            const double nion = e.abund * nH * frac[0];
+            const double qul = 9.2e-11 * pow(T / 100.0, 0.67);
+            const double qlu = 0.6 * qul * exp(-227.7 / T);
+            o.cool_H = o.cool_H + nion * nHI * qlu * (227.7 * kKboltz) / (1.0 + nHI * (qul + qlu) / A_OI);
+        }
+        for (int j = 2; j <= e.nstage; ++j) {
+            const int zion = j - 1;
+            ff = ff + e.abund * frac[j - 1] * (double)(zion * zion) * g[min(zion, 4) - 1];
+        }
+        for (int i = 1; i <= e.nstage - 1; ++i)
+            o.heat = o.heat + e.abund * nH * frac[i - 1] * m.eheat[il * m.ntr + e.tr0 + i - 1];
+    }
+    o.freefree = 1.42554e-27 * sqrt(T) * ne * nH * ff;
+    return o;
+}
+
+// net_rate (thermal_mod.f90:38-115).  With metals the (leaf, T) cache mc is
+// prepared here at T and left for the caller.
 __device__ double net_rate(const ThArgs& a, long long il, double T, double nH, double& xHI, double& xHeI,
-                           double& xHeII, double& ne, int* passes) {
+                           double& xHeII, double& ne, int* passes, MetalCache& mc) {
     const BalArgs& b = a.b;
     const long long n = b.nleaf;
     const Coef k = coef_at_call(b.rs, b.caseA, T);
-    *passes += solve_cell(k, b.yHe, b.rates[il], b.rates[n + il], b.rates[2 * n + il], nH, xHI, xHeI, xHeII, ne);
+    if (b.m.ntr > 0) {
+        metal_prepare(b.m, il, T, mc);
+        *passes += solve_cell_metal(k, b.yHe, b.rates[il], b.rates[n + il], b.rates[2 * n + il], nH, xHI, xHeI, xHeII,
+                                    ne, b.m, mc, b.metal_ne, b.two_way);
+    } else {
+        *passes += solve_cell(k, b.yHe, b.rates[il], b.rates[n + il], b.rates[2 * n + il], nH, xHI, xHeI, xHeII, ne);
+    }
     const double heat = nH * (xHI * b.rates[3 * n + il] + b.yHe * (xHeI * b.rates[4 * n + il] + xHeII * b.rates[5 * n + il]));
-    return heat - cooling_total(a.td, b.rs, b.caseA, b.yHe, T, nH, ne, xHI, xHeI, xHeII);
+    double net = heat - cooling_total(a.td, b.rs, b.caseA, b.yHe, T, nH, ne, xHI, xHeI, xHeII);
+    if (b.m.ntr > 0) {
+        const MetalThermalTerms mt = metal_thermal(a.td, b.m, mc, il, T, nH, ne, nH * xHI, nH * (1.0 - xHI));
+        net = net - mt.cool;
+        net = net - mt.cool_H;
+        if (b.metal_ff) net = net - mt.freefree;
+        if (b.metal_heat) net = net + mt.heat;
+    }
+    return net;
 }
 
 // gas_thermal_update (thermal_mod.f90:124-249): bisection on log T in
@@ -286,8 +431,9 @@ __global__ void __launch_bounds__(kBThreads) k_thermal(const ThArgs a) {
         double xHI = x0, xHeI = h10, xHeII = h20, ne = 0.0;
         int passes = 0;
         double tlo = a.te_min, thi = a.te_max, te;
-        const double net_lo = net_rate(a, il, tlo, nH, xHI, xHeI, xHeII, ne, &passes);
-        const double net_hi = net_rate(a, il, thi, nH, xHI, xHeI, xHeII, ne, &passes);
+        MetalCache mc;
+        const double net_lo = net_rate(a, il, tlo, nH, xHI, xHeI, xHeII, ne, &passes, mc);
+        const double net_hi = net_rate(a, il, thi, nH, xHI, xHeI, xHeII, ne, &passes, mc);
         if (net_lo <= 0.0) {
             te = tlo;
         } else if (net_hi >= 0.0) {
@@ -295,14 +441,14 @@ __global__ void __launch_bounds__(kBThreads) k_thermal(const ThArgs a) {
         } else {
             for (int it = 1; it <= 60; ++it) {
                 const double tmid = sqrt(tlo * thi);
-                const double nm = net_rate(a, il, tmid, nH, xHI, xHeI, xHeII, ne, &passes);
+                const double nm = net_rate(a, il, tmid, nH, xHI, xHeI, xHeII, ne, &passes, mc);
                 if (nm > 0.0) tlo = tmid; else thi = tmid;
                 if (thi / tlo - 1.0 < 1.0e-5) break;
             }
             te = sqrt(tlo * thi);
         }
         int last = 0;
-        net_rate(a, il, te, nH, xHI, xHeI, xHeII, ne, &last);
+        net_rate(a, il, te, nH, xHI, xHeI, xHeII, ne, &last, mc);
         ++solved;
         if (last > 200) ++caps;
         const double w = b.relax;
@@ -310,7 +456,14 @@ __global__ void __launch_bounds__(kBThreads) k_thermal(const ThArgs a) {
         const double h1n = (1.0 - w) * h10 + w * xHeI;
         const double h2n = (1.0 - w) * h20 + w * xHeII;
         const double h3n = fmax(0.0, 1.0 - h1n - h2n);
-        const double nen = nH * ((1.0 - xn) + b.yHe * (h2n + 2.0 * h3n));
+        double nen = nH * ((1.0 - xn) + b.yHe * (h2n + 2.0 * h3n));
+        if (b.m.ntr > 0) {
+            // written state at te (thermal_mod.f90:191-203); mc is at te from
+            // the final net_rate, which is also the stage cache's temperature
+            if (b.metal_ne) nen = charge_neutrality_ne(b.m, mc, nH, nen, xn, ne);
+            if (b.fp32) metal_opacity_fill<float>(b.m, mc, il, nH, nen, xn, b.colscale);
+            else metal_opacity_fill<double>(b.m, mc, il, nH, nen, xn, b.colscale);
+        }
         b.xHI[il] = xn;
         b.xHeI[il] = h1n;
         b.xHeII[il] = h2n;
@@ -348,6 +501,37 @@ __global__ void __launch_bounds__(kBThreads) k_thermal(const ThArgs a) {
     }
 }
 
+// Stage fractions of the written state (species_write, species_mod.f90:873-904):
+// leaf-major, registry order; an empty leaf is all neutral.
+__global__ void k_metal_fractions(const MetalDev m, const double* __restrict__ nH, const double* __restrict__ xHI,
+                                  const double* __restrict__ ne, const double* __restrict__ Te, long long nleaf,
+                                  double* out) {
+    for (long long il = (long long)blockIdx.x * blockDim.x + threadIdx.x; il < nleaf;
+         il += (long long)gridDim.x * blockDim.x) {
+        double* o = out + il * m.nst;
+        if (nH[il] <= 0.0) {
+            for (int ie = 0; ie < m.nel; ++ie) {
+                const MetalEl e = m.el[ie];
+                for (int i = 0; i < e.nstage; ++i) o[e.st0 + i] = i == 0 ? 1.0 : 0.0;
+            }
+            continue;
+        }
+        MetalCache mc;
+        metal_prepare(m, il, Te[il], mc);
+        const double nHI = nH[il] * xHI[il], nHII = nH[il] * (1.0 - xHI[il]);
+        double r[kMaxSt];
+        for (int ie = 0; ie < m.nel; ++ie) {
+            const MetalEl e = m.el[ie];
+            double fr = metal_chain(mc, e.tr0, e.nstage, ne[il], nHI, nHII, r);
+            o[e.st0] = fr;
+            for (int i = 2; i <= e.nstage; ++i) {
+                fr = fr * r[i - 2];
+                o[e.st0 + i - 1] = fr;
+            }
+        }
+    }
+}
+
 int nblocks(long long work, int threads, int cap) {
     long long b = (work + threads - 1) / threads;
     return (int)(b < 1 ? 1 : b > cap ? cap : b);
@@ -363,8 +547,14 @@ int balance_blocks(const mochii_ctx* c) {
 
 cudaError_t launch_columns(mochii_ctx* c) {
     k_columns<<<nblocks(c->grid.nleaf, 256, 148 * 16), 256, 0, c->stream>>>(
-        c->nH, c->xHI, c->xHeI, c->xHeII, c->col, c->grid.nleaf, c->nabs, c->fp32 ? 1 : 0, c->par.He_abund,
-        c->par.distance2cm * 1.0e-18);
+        c->nH, c->xHI, c->xHeI, c->xHeII, c->ne, c->Te, c->col, c->grid.nleaf, c->nabs, c->fp32 ? 1 : 0,
+        c->par.He_abund, c->par.distance2cm * 1.0e-18, c->metal);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_metal_fractions(mochii_ctx* c, double* out) {
+    k_metal_fractions<<<nblocks(c->grid.nleaf, 128, 148 * 16), 128, 0, c->stream>>>(c->metal, c->nH, c->xHI, c->ne,
+                                                                                   c->Te, c->grid.nleaf, out);
     return cudaGetLastError();
 }
 
@@ -393,6 +583,11 @@ static BalArgs bal_args(mochii_ctx* c) {
     a.nabs = c->nabs;
     a.fp32 = c->fp32 ? 1 : 0;
     a.k = coef_at(a.rs, a.caseA, a.T);   // fixed T: evaluated once on the host
+    a.m = c->metal;
+    a.metal_ne = c->par.metal_ne;
+    a.two_way = c->par.charge_exchange_two_way;
+    a.metal_heat = c->par.metal_heat;
+    a.metal_ff = c->par.metal_freefree;
     return a;
 }
 

@@ -229,7 +229,7 @@ bool aligned_edges(std::vector<double>& edge, int nfuv, int nnu, double lo, doub
 // ion_setup + setup_continuous_source_sampler + build_point_source_sampler
 // (ion_band_mod.f90:122-258, :275-353, :437-495) for internal point sources
 // with Planck spectra, and ion_qmc_ndim (:654-663).
-bool band_build(const mochii_params& p, BandSetup& b, std::string* err) {
+bool band_build(const mochii_params& p, BandSetup& b, std::string* err, const std::vector<double>& metal_eth) {
     const int nfuv = p.add_fuv ? p.nnu_fuv : 0;
     if (p.add_fuv && p.efuv_min >= p.eion_min) return fail(err, "add_fuv requires par%efuv_min < par%eion_min");
     if (p.nnu_ion < 1) return fail(err, "par%nnu_ion must be >= 1");
@@ -241,7 +241,7 @@ bool band_build(const mochii_params& p, BandSetup& b, std::string* err) {
     for (int i = 0; i < nfuv; ++i)
         b.eedge[i] = std::exp(std::log(p.efuv_min) + (lo - std::log(p.efuv_min)) * (double)i / (double)nfuv);
     if (p.ion_align_edges) {
-        if (!aligned_edges(b.eedge, nfuv, nnu, p.eion_min, p.eion_max, {}, err)) return false;
+        if (!aligned_edges(b.eedge, nfuv, nnu, p.eion_min, p.eion_max, metal_eth, err)) return false;
     } else {
         for (int i = nfuv; i <= nnu; ++i)
             b.eedge[i] = std::exp(lo + (hi - lo) * (double)(i - nfuv) / (double)(nnu - nfuv));
@@ -252,7 +252,10 @@ bool band_build(const mochii_params& p, BandSetup& b, std::string* err) {
     b.multi = b.ncomp >= 2;
     b.qmc_ndim = b.multi ? 7 : 3;
     const double elo = p.add_fuv ? p.efuv_min : p.eion_min;
+    // photoionization_threshold_knots (ion_band_mod.f90:408-419): H, He, the
+    // metal thresholds in registry order, then eion_min with the FUV band
     std::vector<double> knots{kEthHI, kEthHeI, kEthHeII};
+    knots.insert(knots.end(), metal_eth.begin(), metal_eth.end());
     if (p.add_fuv) knots.push_back(p.eion_min);
     b.tables.assign(b.ncomp, EnergyTable());
     b.comp_x.assign(b.ncomp, 0.0);

@@ -34,6 +34,8 @@ struct BandSetup {
     double ion_Ltot = 0.0;
 };
 
-bool band_build(const mochii_params& p, BandSetup& b, std::string* err);
+// metal_eth: the active metal thresholds in registry order (main.f90:65-82),
+// which pin band edges and sampler knots as the H/He thresholds do.
+bool band_build(const mochii_params& p, BandSetup& b, std::string* err, const std::vector<double>& metal_eth = {});
 
 }  // namespace mochii

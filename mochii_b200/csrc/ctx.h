@@ -10,6 +10,7 @@
 #include "diffuse.h"
 #include "mochii_gpu.h"
 #include "qmc.cuh"
+#include "species.h"
 #include "thermal.h"
 
 namespace mochii {
@@ -54,6 +55,8 @@ struct RecordBuffers {
     int* bits = nullptr;
     void* sig = nullptr;
     void* coef = nullptr;
+    double* E = nullptr;      // metals: packet energy
+    void* msig = nullptr;     // metals: ntrp x cap cross sections
     long long cap = 0;
 };
 
@@ -95,6 +98,8 @@ struct mochii_ctx {
     mochii::Tuning tune;
     mochii::ThermalDev th;          // thermal tables (solve_te)
     mochii::DiffuseBuffers dif;     // diffuse field (diffuse_field)
+    mochii::MetalDev metal;         // trace metals (use_metals); metal.ntr == 0 without
+    mochii::SpeciesHost species;
     bool thermal_ready = false;
     mochii::BalanceWork bw;
     std::string last_error;

@@ -18,6 +18,7 @@
 
 #include "ctx.h"
 #include "diffuse.h"
+#include "metals.cuh"
 #include "physics.cuh"
 #include "qmc.cuh"
 #include "records.cuh"
@@ -191,6 +192,7 @@ struct DiffLaunchArgs {
     const double* Te;
     const double* eedge;
     MilneDev m;
+    MetalDev metal;
     double total, org[3], dcell, eion_max;
     int n[3], nnu, nfuv, energy_model;
     long long nleaf;
@@ -252,6 +254,7 @@ __global__ void __launch_bounds__(kThreads) k_launch_diffuse(const DiffLaunchArg
     }
     const int inu = min(max(blo, a.nfuv + 1), a.nnu) - 1;
     write_record<R>(rec, i, pos, kk, eph, inu, a.org, a.dcell, a.n);
+    if (a.metal.ntr > 0) write_metal_record<R>(rec, a.metal, i, eph);
 }
 
 int nblk(long long work, int threads, int cap) {
@@ -304,6 +307,7 @@ cudaError_t launch_diffuse_chunk(mochii_ctx* c, double total, long long ip0, lon
     a.m = c->dif.m;
     a.total = total;
     a.org[0] = c->grid.xmin; a.org[1] = c->grid.ymin; a.org[2] = c->grid.zmin;
+    a.metal = c->metal;
     a.dcell = c->grid.dcell;
     a.eion_max = c->par.eion_max;
     a.n[0] = c->grid.nx; a.n[1] = c->grid.ny; a.n[2] = c->grid.nz;

@@ -1,0 +1,232 @@
+// Device side of the trace-metal registry (species_mod.f90): packet cross
+// sections, rate coefficients, the per-(leaf, T) rate cache, the cascade
+// sums that feed hydrogen's balance and the n_e closure, the charge-exchange
+// hydrogen root (ion_balance_mod.f90:177-208), the n_e closure of the written
+// state (:235-253), the stage fractions behind the packet opacity, and the
+// metal cooling / heating terms of the thermal balance (thermal_mod.f90:53-71).
+// All FP64; element order j, threshold order k (species.h).
+#pragma once
+#include "physics.cuh"
+#include "records.cuh"
+#include "species.h"
+
+namespace mochii {
+
+// sigma_vy95, photo_xsec.f90:69-82 (Verner & Yakovlev 1995 outer shell).
+MHD double sigma_vy95(double E, double Eth, double E0, double s0, double ya, double P, double yw, double l) {
+    if (E < Eth) return 0.0;
+    const double y = E / E0;
+    const double Q = 5.5 + l - 0.5 * P;
+    const double ym1 = y - 1.0;
+    return s0 * ((ym1 * ym1 + yw * yw) * pow(y, -Q) * pow(1.0 + sqrt(y / ya), -P)) * 1.0e-18;
+}
+
+// species_sigma (species_mod.f90:763-778), threshold order k.
+__device__ __forceinline__ double metal_sigma(const MetalDev& m, int k, double E) {
+    const double* c = m.photo + 8 * k;
+    if (m.form[k] == 2) return sigma_vy95(E, c[0], c[1], c[2], c[3], c[4], c[5], c[6]);
+    return sigma_vfky96(E, c[0], c[1], c[2], c[3], c[4], c[5], c[6], c[7]);
+}
+
+// Number of active transitions (E >= E_th) of a packet: the prefix that
+// species_packet_cross_sections (species_mod.f90:263-275) fills.
+__device__ __forceinline__ int metal_nactive(const MetalDev& m, double E) {
+    int n = 0;
+    while (n < m.ntr && !(E < __ldg(m.eth + n))) ++n;
+    return n;
+}
+
+// Metal part of a packet record: E and sigma_k * 1e18 for the active prefix.
+template <typename R>
+__device__ __forceinline__ void write_metal_record(const PacketRecords& rec, const MetalDev& m, long long i, double E) {
+    rec.E[i] = E;
+    R* ms = static_cast<R*>(rec.msig);
+    const int nm = metal_nactive(m, E);
+    for (int k = 0; k < nm; ++k) ms[k * rec.cap + i] = (R)(metal_sigma(m, k, E) * 1.0e18);
+}
+
+// alpha_rec (species_mod.f90:428-447): Badnell RR (or the RR2 power law) plus
+// Badnell DR and the Shull & Van Steenberg DR2 term.
+static __device__ __noinline__ double metal_alpha_rec(const MetalTr& r, double T) {
+    double a;
+    if (r.has_rr2) {
+        a = r.rr2[0] * pow(T / 1.0e4, -r.rr2[1]);
+    } else {
+        const double s0 = sqrt(T / r.rr[2]), s1 = sqrt(T / r.rr[3]);
+        const double b = r.rr[1] + r.rr[4] * exp(-r.rr[5] / T);
+        a = r.rr[0] / (s0 * pow(1.0 + s0, 1.0 - b) * pow(1.0 + s1, 1.0 + b));
+    }
+    if (r.ndr > 0 || r.has_dr2) {
+        const double t15 = pow(T, -1.5);
+        for (int k = 0; k < r.ndr; ++k) a = a + t15 * r.dr_c[k] * exp(-r.dr_e[k] / T);
+        if (r.has_dr2) a = a + r.dr2[0] * t15 * exp(-r.dr2[2] / T) * (1.0 + r.dr2[1] * exp(-r.dr2[3] / T));
+    }
+    return a;
+}
+
+// cx_rate (species_mod.f90:452-487): the seven charge-exchange fit forms.
+static __device__ __noinline__ double metal_cx_rate(int form, const double* c, double T) {
+    double t4 = T / 1.0e4, k, lnT;
+    switch (form) {
+        case 1:
+            k = c[0] * pow(T / 300.0, c[1]);
+            if (c[2] != 0.0) k = k * exp(-c[2] / t4);
+            return k;
+        case 2: return c[0] * pow(t4, c[1]) + c[2] * pow(t4, c[3]);
+        case 3: return (c[0] * pow(t4, c[1]) + c[2] * pow(t4, c[3])) * exp(-c[4] / T);
+        case 4:
+            lnT = log(T);
+            return exp(c[0] + lnT * (c[1] + lnT * (c[2] + lnT * (c[3] + lnT * c[4]))));
+        case 5:
+            lnT = log(T);
+            return exp(c[0] + lnT * (c[1] + lnT * (c[2] + lnT * (c[3] + lnT * c[4]))) - c[5] / t4);
+        case 6:
+            t4 = fmin(fmax(t4, 0.5), 5.0);
+            k = c[0] * pow(t4, c[1]) * (1.0 + c[2] * exp(c[3] * t4));
+            return fmax(k, 0.0);
+        case 7:
+            t4 = fmin(fmax(t4, 0.5), 5.0);
+            k = c[0] * pow(t4, c[1]) * (1.0 + c[2] * exp(c[3] * t4)) * exp(-c[4] / t4);
+            return fmax(k, 0.0);
+        default: return 0.0;
+    }
+}
+
+// The (leaf, T) rate cache of species_ne_prepare (species_mod.f90:517-536).
+struct MetalCache {
+    double gam[kMaxTr], ci[kMaxTr], rec[kMaxTr], cxi[kMaxTr], cxr[kMaxTr];
+};
+
+static __device__ __noinline__ void metal_prepare(const MetalDev& m, long long il, double T, MetalCache& c) {
+    for (int j = 0; j < m.ntr; ++j) {
+        const MetalTr& r = m.tr[j];
+        c.gam[j] = m.egam[il * m.ntr + j];
+        c.ci[j] = voronov(T, r.ci[0], r.ci[1], r.ci[2], r.ci[3], r.ci[4]) * r.cidr;
+        c.rec[j] = metal_alpha_rec(r, T);
+        c.cxi[j] = r.cxi_form > 0 ? metal_cx_rate(r.cxi_form, r.cxi, T) : 0.0;
+        c.cxr[j] = r.cxr_form > 0 ? metal_cx_rate(r.cxr_form, r.cxr, T) : 0.0;
+    }
+}
+
+// Ratio chain n_{i+1}/n_i of one element from the cache; returns the stage-1
+// fraction 1/s and leaves the ratios in r (species_mod.f90:591-603, 794-812).
+__device__ __forceinline__ double metal_chain(const MetalCache& c, int tr0, int ns, double ne, double nHI, double nHII,
+                                              double* r) {
+    for (int it = 1; it <= ns - 1; ++it) {
+        const int j = tr0 + it - 1;
+        double rion = c.gam[j] + ne * c.ci[j];
+        if (c.cxi[j] > 0.0) rion = rion + nHII * c.cxi[j];
+        double rrec = ne * c.rec[j];
+        if (c.cxr[j] > 0.0) rrec = rrec + nHI * c.cxr[j];
+        r[it - 1] = rion / fmax(rrec, kTinest);
+    }
+    double s = 1.0, prod = 1.0;
+    for (int i = 1; i <= ns - 1; ++i) {
+        prod = prod * r[i - 1];
+        s = s + prod;
+    }
+    return 1.0 / s;
+}
+
+// species_metal_sums (species_mod.f90:566-614): metal electrons and the two
+// charge-exchange rates hydrogen sees, from one walk of each chain.
+static __device__ __noinline__ void metal_sums(const MetalDev& m, const MetalCache& c, double nH, double ne, double nHI,
+                                        double nHII, double& nem, double& rin, double& rout) {
+    nem = 0.0;
+    rin = 0.0;
+    rout = 0.0;
+    double r[kMaxSt];
+    for (int ie = 0; ie < m.nel; ++ie) {
+        const MetalEl e = m.el[ie];
+        const int ns = e.nstage;
+        double fr = metal_chain(c, e.tr0, ns, ne, nHI, nHII, r);
+        const double nX = e.abund * nH;
+        if (ns > 1) rin = rin + c.cxi[e.tr0] * nX * fr;
+        for (int i = 2; i <= ns; ++i) {
+            fr = fr * r[i - 2];
+            nem = nem + e.abund * nH * fr * (double)(i - 1);
+            rout = rout + c.cxr[e.tr0 + i - 2] * nX * fr;
+            if (i < ns) rin = rin + c.cxi[e.tr0 + i - 1] * nX * fr;
+        }
+    }
+}
+
+// hydrogen_neutral_fraction (ion_balance_mod.f90:177-208): Illinois false
+// position for x_HI on [0, 1] with the charge-exchange terms re-evaluated at
+// every trial x.
+static __device__ __noinline__ double hydrogen_neutral_fraction(const MetalDev& m, const MetalCache& c, double nH, double ne,
+                                                         double A, double B) {
+    double nem, rin, rout;
+    double xa = 0.0;
+    metal_sums(m, c, nH, ne, 0.0, nH, nem, rin, rout);
+    double Ra = -(A + rin);
+    double xb = 1.0;
+    metal_sums(m, c, nH, ne, nH, 0.0, nem, rin, rout);
+    double Rb = B + rout;
+    const double scale = A + B + fabs(Ra) + fabs(Rb);
+    double x = xb;
+    for (int k = 1; k <= 80; ++k) {
+        if (Rb == Ra) break;
+        x = xb - Rb * (xb - xa) / (Rb - Ra);
+        x = fmin(fmax(x, fmin(xa, xb)), fmax(xa, xb));
+        metal_sums(m, c, nH, ne, nH * x, nH * (1.0 - x), nem, rin, rout);
+        const double Rx = x * (B + rin + rout) - (A + rin);
+        if (fabs(Rx) <= 1.0e-15 * scale) break;
+        if (fabs(xb - xa) <= 1.0e-15) break;
+        if (Rx * Rb < 0.0) {
+            xa = xb;
+            Ra = Rb;
+        } else {
+            Ra = 0.5 * Ra;
+        }
+        xb = x;
+        Rb = Rx;
+    }
+    return x;
+}
+
+// charge_neutrality_ne (ion_balance_mod.f90:235-253) with a cache already
+// prepared at the written temperature.
+static __device__ __noinline__ double charge_neutrality_ne(const MetalDev& m, const MetalCache& c, double nH, double ne_HHe,
+                                                    double xHI, double ne_seed) {
+    const double nHI = nH * xHI, nHII = nH * (1.0 - xHI);
+    double ne = fmax(ne_seed, 1.0e-12 * nH);
+    for (int it = 1; it <= 200; ++it) {
+        const double ne_old = ne;
+        double nem, rin, rout;
+        metal_sums(m, c, nH, ne_old, nHI, nHII, nem, rin, rout);
+        ne = ne_HHe + nem;
+        ne = fmax(0.5 * (ne + ne_old), 1.0e-12 * nH);
+        if (fabs(ne - ne_old) <= 1.0e-10 * ne) break;
+    }
+    return ne;
+}
+
+// species_stage_cache_refresh (species_mod.f90:247-261) for one leaf, stored
+// as the opacity weight n_H A_el f_it * colscale of each transition in
+// threshold order (the factor species_cached_opacity applies per packet).
+template <typename R>
+static __device__ __noinline__ void metal_opacity_fill(const MetalDev& m, const MetalCache& c, long long il, double nH,
+                                                double ne, double xHI, double colscale) {
+    R* o = static_cast<R*>(m.opac) + il * m.ntrp;
+    double r[kMaxSt];
+    const double nHI = nH * xHI, nHII = nH * (1.0 - xHI);
+    for (int ie = 0; ie < m.nel; ++ie) {
+        const MetalEl e = m.el[ie];
+        double fr = metal_chain(c, e.tr0, e.nstage, ne, nHI, nHII, r);
+        for (int it = 1; it <= e.nstage - 1; ++it) {
+            if (it > 1) fr = fr * r[it - 2];
+            const MetalTr& t = m.tr[e.tr0 + it - 1];
+            o[t.flat] = (R)(nH * (e.abund * fr) * colscale);
+        }
+    }
+}
+
+// The four metal terms of net_rate (thermal_mod.f90:53-71): line cooling
+// (fits with the n-level suppression), H-impact [C II] 158 um / [O I] 63 um,
+// net-charge free-free and photoheating, at one (T, n_e, x_HI).
+struct MetalThermalTerms {
+    double cool, cool_H, freefree, heat;
+};
+
+}  // namespace mochii

@@ -17,6 +17,8 @@ struct PacketRecords {
     int* bits;     // inu | (stp_x+1) << 16 | (stp_y+1) << 18 | (stp_z+1) << 20
     void* sig;     // 3 x cap of R: sigma_HI, sigma_HeI, sigma_HeII in 1e-18 cm^2
     void* coef;    // 6 x cap of R: Gamma/heat coefficients per unit path
+    double* E;     // metals only: packet energy [eV]
+    void* msig;    // metals only: ntrp x cap of R, active-prefix sigma_k in 1e-18 cm^2
     long long cap;
 };
 

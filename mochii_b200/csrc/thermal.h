@@ -46,5 +46,7 @@ struct ThermalDev {
 std::string data_root();
 std::string atomic_dir(const mochii_params& p);
 bool thermal_tables_build(const mochii_params& p, ThermalHost& t, std::string* err);
+// Collisional line-cooling fit file (cooling_mod.f90:98-122): Lambda = sum A_i exp(-T_i/T) / sqrt(T).
+bool cooling_fit_read(const std::string& path, std::vector<double>& A, std::vector<double>& Ti);
 
 }  // namespace mochii

@@ -4,6 +4,7 @@
 // (cooling_mod.f90:73-75, 98-134) and its (T, n_e) n-level suppression
 // table (nlevel_cooling_mod.f90 over the nlevel_mod.f90 solver).
 #include "thermal.h"
+#include "species.h"
 
 #include <dlfcn.h>
 
@@ -100,7 +101,9 @@ double gff_mean(double T, double Z) {
     return s / (std::exp(-1.0e-4) - std::exp(-20.0));
 }
 
-bool read_fit(const std::string& path, std::vector<double>& A, std::vector<double>& Ti) {
+}  // namespace
+
+bool cooling_fit_read(const std::string& path, std::vector<double>& A, std::vector<double>& Ti) {
     std::ifstream f(path);
     if (!f) return false;
     std::string line;
@@ -118,8 +121,6 @@ bool read_fit(const std::string& path, std::vector<double>& A, std::vector<doubl
         if (!(f >> A[i] >> Ti[i])) return false;
     return true;
 }
-
-}  // namespace
 
 std::string data_root() {
     Dl_info info;
@@ -276,30 +277,31 @@ bool thermal_tables_build(const mochii_params& p, ThermalHost& t, std::string* e
     }
     const std::string dir = atomic_dir(p);
     std::vector<double> A, Ti;
-    if (!read_fit(dir + "/cooling_h_1.txt", A, Ti)) {
+    if (!cooling_fit_read(dir + "/cooling_h_1.txt", A, Ti)) {
         if (err) *err = "cannot read " + dir + "/cooling_h_1.txt";
         return false;
     }
     t.hi_nterm = (int)A.size();
     for (int i = 0; i < t.hi_nterm; ++i) { t.hi_A[i] = A[i]; t.hi_T[i] = Ti[i]; }
     t.use_hi_table = p.cooling_local_ne;
-    if (t.use_hi_table) {
-        NlevelAtomData atom;
-        if (!atom.load(dir + "/nlevel_h_1.txt")) {
-            t.use_hi_table = false;   // nlevel_cooling_add returns 0: the fit is used unchanged
-        } else {
-            std::vector<double> ne(kNlNNE), lam((size_t)kNlNT * kNlNNE);
-            for (int j = 0; j < kNlNNE; ++j) ne[j] = std::pow(10.0, -6.0 + 0.1 * (double)j);
-            for (int i = 0; i < kNlNT; ++i)
-                atom.cooling_column(std::pow(10.0, 2.0 + 0.01 * (double)i), ne.data(), kNlNNE, &lam[(size_t)i * kNlNNE]);
-            t.hi_lamref.resize(kNlNT);
-            t.hi_Ssup.resize((size_t)kNlNT * kNlNNE);
-            for (int i = 0; i < kNlNT; ++i) {
-                const double ref = lam[(size_t)i * kNlNNE];
-                t.hi_lamref[i] = ref;
-                for (int j = 0; j < kNlNNE; ++j) t.hi_Ssup[(size_t)i * kNlNNE + j] = lam[(size_t)i * kNlNNE + j] / std::max(ref, kTinest);
-            }
-        }
+    // nlevel_cooling_add returns 0 without the atom file: the fit is used unchanged
+    if (t.use_hi_table) t.use_hi_table = nlevel_table_build(dir + "/nlevel_h_1.txt", t.hi_lamref, t.hi_Ssup);
+    return true;
+}
+
+bool nlevel_table_build(const std::string& path, std::vector<double>& lamref, std::vector<double>& Ssup) {
+    NlevelAtomData atom;
+    if (!atom.load(path)) return false;
+    std::vector<double> ne(kNlNNE), lam((size_t)kNlNT * kNlNNE);
+    for (int j = 0; j < kNlNNE; ++j) ne[j] = std::pow(10.0, -6.0 + 0.1 * (double)j);
+    for (int i = 0; i < kNlNT; ++i)
+        atom.cooling_column(std::pow(10.0, 2.0 + 0.01 * (double)i), ne.data(), kNlNNE, &lam[(size_t)i * kNlNNE]);
+    lamref.resize(kNlNT);
+    Ssup.resize((size_t)kNlNT * kNlNNE);
+    for (int i = 0; i < kNlNT; ++i) {
+        const double ref = lam[(size_t)i * kNlNNE];
+        lamref[i] = ref;
+        for (int j = 0; j < kNlNNE; ++j) Ssup[(size_t)i * kNlNNE + j] = lam[(size_t)i * kNlNNE + j] / std::max(ref, kTinest);
     }
     return true;
 }

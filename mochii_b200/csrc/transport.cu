@@ -23,6 +23,7 @@
 #include <mutex>
 
 #include "ctx.h"
+#include "metals.cuh"
 #include "physics.cuh"
 #include "qmc.cuh"
 #include "records.cuh"
@@ -53,6 +54,8 @@ struct PassArgs {
     double dcell;
     int n[3];
     int ncomp, multi, ndim, nnu;
+    MetalDev m;          // trace metals; m.ntr == 0 without
+    int metal_abs;       // par%ion_metal_abs
 };
 
 // sample_energy_cdf, energy_sampler_mod.f90:187-238.  The bracket search and
@@ -183,6 +186,7 @@ __global__ void __launch_bounds__(kThreads) k_launch(const PassArgs a, PacketRec
     const double kk[3] = {sint * cphi, sint * sphi, cost};
     const int inu = bin_of(a.eedge, a.nnu, E);
     write_record<R>(rec, i, pos, kk, E, inu, a.org, a.dcell, a.n);
+    if (a.m.ntr > 0) write_metal_record<R>(rec, a.m, i, E);
 }
 
 // Absorber columns of one leaf, loaded ahead of use.
@@ -240,12 +244,23 @@ struct Stepper {
 // packets of one chunk, grid-stride.  The stepper runs LA cells ahead of the
 // scoring: slot 0 is scored now, slots 1..LA have their column loads in
 // flight (LA = 0 disables the look-ahead).
-template <typename R, int NABS, int LA>
+//
+// METAL adds the trace-metal terms: the packet's active-prefix cross
+// sections sigma_k and heating coefficients sigma_k (1 - E_th,k/E) sit in
+// dynamic shared memory ([k][thread], 2 x ntrp x 128 of R); per segment the
+// leaf's opacity weights add sum_k w_k sigma_k to the absorption
+// (species_cached_opacity, species_mod.f90:291-303) and two tallies per
+// active transition are scored (species_rate_path_score, :329-343).
+template <typename R, int NABS, int LA, bool METAL>
 __global__ void __launch_bounds__(128) k_walk_edge(const PassArgs a, const PacketRecords rec, long long n,
                                                    int accumulate) {
     typedef typename Acc<R>::T T;
     constexpr int NT = NABS == 1 ? 2 : 6;
     __shared__ double sh[128];
+    extern __shared__ __align__(16) unsigned char dsm[];
+    R* const msg = reinterpret_cast<R*>(dsm);                 // sigma_k        [k][thread]
+    R* const mhc = msg + (METAL ? a.m.ntrp * blockDim.x : 0);  // sigma_k h_k    [k][thread]
+    const int tb = blockDim.x, tx = threadIdx.x;
     double emitted = 0.0, absorbed = 0.0, escaped = 0.0;
     unsigned long long nseg = 0, kills = 0;
     T* tal = static_cast<T*>(a.tally);
@@ -270,6 +285,19 @@ __global__ void __launch_bounds__(128) k_walk_edge(const PassArgs a, const Packe
         R cf[NT];
 #pragma unroll
         for (int k = 0; k < NT; ++k) cf[k] = cfp[k * c + i];
+        int nm = 0;
+        R invE = (R)0;
+        if constexpr (METAL) {
+            const double E = rec.E[i];
+            nm = metal_nactive(a.m, E);
+            invE = (R)(1.0 / E);
+            const R* ms = static_cast<const R*>(rec.msig);
+            for (int k = 0; k < nm; ++k) {
+                const R sk = ms[k * c + i];
+                msg[k * tb + tx] = sk;
+                mhc[k * tb + tx] = (R)((double)sk * fmax(1.0 - __ldg(a.m.eth + k) / E, 0.0));
+            }
+        }
         // ring of LA+1 cells: il, segment, columns, and whether a next cell exists
         int il[LA + 1] = {};
         double sgm[LA + 1] = {};
@@ -290,7 +318,15 @@ __global__ void __launch_bounds__(128) k_walk_edge(const PassArgs a, const Packe
         int nstep = 0;
         for (;;) {
             if (++nstep > kMaxWalkSteps) { ++kills; break; }
-            const R kap = cl[0].kappa(s0, s1, s2);
+            R kap = cl[0].kappa(s0, s1, s2);
+            if constexpr (METAL) {
+                if (a.metal_abs && nm > 0) {
+                    const R* op = static_cast<const R*>(a.m.opac) + (long long)il[0] * a.m.ntrp;
+                    R km = (R)0;
+                    for (int k = 0; k < nm; ++k) km = km + __ldg(op + k) * msg[k * tb + tx];
+                    kap = kap + km;
+                }
+            }
             const R ks = kap * (R)sgm[0];
             R w;
             if (ks > (R)0) {
@@ -306,6 +342,14 @@ __global__ void __launch_bounds__(128) k_walk_edge(const PassArgs a, const Packe
 #pragma unroll
                 for (int k = 0; k < NT; ++k) tally_add(tl + k, w * cf[k]);
                 tally_add(jt + (long long)il[0] * a.nnu + inu, w);
+                if constexpr (METAL) {
+                    T* rw = static_cast<T*>(a.m.raw) + (long long)il[0] * a.m.ntrp * 2;
+                    const R wi = w * invE;
+                    for (int k = 0; k < nm; ++k) {
+                        tally_add(rw + 2 * k, wi * msg[k * tb + tx]);
+                        tally_add(rw + 2 * k + 1, w * mhc[k * tb + tx]);
+                    }
+                }
             }
             tau = tau + (double)ks;
             if (tau >= kTauHuge) break;
@@ -383,6 +427,22 @@ template <typename T>
 __global__ void k_jt(const T* __restrict__ jt, double* __restrict__ out, long long n, double scale) {
     for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
         out[i] = tval<T>(jt[i]) * scale;
+}
+
+// species_gamma_compute (species_mod.f90:493-512): per-leaf metal Gamma and
+// photoheating from the path tallies, into element order.
+template <typename T>
+__global__ void k_metal_rates(const MetalDev m, long long nleaf, double cg, double ch) {
+    const T* raw = static_cast<const T*>(m.raw);
+    for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < nleaf * m.ntr;
+         q += (long long)gridDim.x * blockDim.x) {
+        const long long il = q / m.ntr;
+        const int j = (int)(q - il * m.ntr);
+        const int k = m.tr[j].flat;
+        const T* r = raw + (il * m.ntrp + k) * 2;
+        m.egam[q] = tval<T>(r[0]) * cg;
+        m.eheat[q] = tval<T>(r[1]) * ch;
+    }
 }
 
 // Sobol uniforms for the test hook.
@@ -479,6 +539,8 @@ PassArgs make_args(mochii_ctx* c) {
     a.multi = c->band.multi;
     a.ndim = c->band.qmc_ndim;
     a.nnu = c->nnu;
+    a.m = c->metal;
+    a.metal_abs = c->par.ion_metal_abs;
     return a;
 }
 
@@ -491,29 +553,64 @@ int grid_blocks(long long work, int threads, int cap) {
 
 }  // namespace
 
+// Dynamic shared memory of the metal walk: sigma_k and sigma_k h_k per thread.
+size_t metal_smem(const mochii_ctx* c) {
+    return c->metal.ntr > 0 ? 2 * (size_t)c->metal.ntrp * 128 * (c->fp32 ? 4 : 8) : 0;
+}
+
+template <typename R, int NABS, int LA, bool METAL>
+int walk_occupancy(size_t smem) {
+    auto k = k_walk_edge<R, NABS, LA, METAL>;
+    if (smem > 48 * 1024) cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    int nb = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k, 128, smem) != cudaSuccess) {
+        cudaGetLastError();
+        return 1;
+    }
+    return nb > 0 ? nb : 1;
+}
+
 int transport_blocks(const mochii_ctx* c) {
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device);
-    const int per_sm = c->tune.walk_blocks_per_sm > 0 ? c->tune.walk_blocks_per_sm : 8;
+    int per_sm = c->tune.walk_blocks_per_sm > 0 ? c->tune.walk_blocks_per_sm : 8;
+    if (c->metal.ntr > 0) {   // resident blocks only: each holds its packets' sigma_k in shared memory
+        const size_t smem = metal_smem(c);
+        const int occ = c->fp32 ? (c->nabs == 1 ? walk_occupancy<float, 1, 2, true>(smem) : walk_occupancy<float, 4, 2, true>(smem))
+                                : (c->nabs == 1 ? walk_occupancy<double, 1, 2, true>(smem) : walk_occupancy<double, 4, 2, true>(smem));
+        per_sm = per_sm < occ ? per_sm : occ;
+    }
     return grid_blocks(c->par.nphotons, 128, sms * per_sm);
 }
 
 // Walk-kernel variants: look-ahead depth 0..2 (the autotuned choice is
 // c->tune.lookahead); 128-thread blocks.
-template <typename R, int NABS>
+template <typename R, int NABS, bool METAL>
 cudaError_t walk_la(mochii_ctx* c, const PassArgs& a, const PacketRecords& r, long long n, int acc, int blocks) {
+    const size_t smem = METAL ? metal_smem(c) : 0;
+    if (METAL && smem > 48 * 1024) {
+        cudaFuncSetAttribute(k_walk_edge<R, NABS, 0, METAL>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        cudaFuncSetAttribute(k_walk_edge<R, NABS, 1, METAL>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        cudaFuncSetAttribute(k_walk_edge<R, NABS, 2, METAL>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    }
     switch (c->tune.lookahead) {
-        case 0: k_walk_edge<R, NABS, 0><<<blocks, 128, 0, c->stream>>>(a, r, n, acc); break;
-        case 1: k_walk_edge<R, NABS, 1><<<blocks, 128, 0, c->stream>>>(a, r, n, acc); break;
-        default: k_walk_edge<R, NABS, 2><<<blocks, 128, 0, c->stream>>>(a, r, n, acc); break;
+        case 0: k_walk_edge<R, NABS, 0, METAL><<<blocks, 128, smem, c->stream>>>(a, r, n, acc); break;
+        case 1: k_walk_edge<R, NABS, 1, METAL><<<blocks, 128, smem, c->stream>>>(a, r, n, acc); break;
+        default: k_walk_edge<R, NABS, 2, METAL><<<blocks, 128, smem, c->stream>>>(a, r, n, acc); break;
     }
     return cudaGetLastError();
 }
 
+template <typename R>
+cudaError_t walk_prec(mochii_ctx* c, const PassArgs& a, const PacketRecords& r, long long n, int acc, int blocks) {
+    if (c->metal.ntr > 0)
+        return c->nabs == 1 ? walk_la<R, 1, true>(c, a, r, n, acc, blocks) : walk_la<R, 4, true>(c, a, r, n, acc, blocks);
+    return c->nabs == 1 ? walk_la<R, 1, false>(c, a, r, n, acc, blocks) : walk_la<R, 4, false>(c, a, r, n, acc, blocks);
+}
+
 cudaError_t launch_walk_variant(mochii_ctx* c, const PassArgs& a, const PacketRecords& r, long long n, int acc,
                                 int blocks) {
-    if (c->fp32) return c->nabs == 1 ? walk_la<float, 1>(c, a, r, n, acc, blocks) : walk_la<float, 4>(c, a, r, n, acc, blocks);
-    return c->nabs == 1 ? walk_la<double, 1>(c, a, r, n, acc, blocks) : walk_la<double, 4>(c, a, r, n, acc, blocks);
+    return c->fp32 ? walk_prec<float>(c, a, r, n, acc, blocks) : walk_prec<double>(c, a, r, n, acc, blocks);
 }
 
 PacketRecords packet_records(mochii_ctx* c) {
@@ -525,6 +622,8 @@ PacketRecords packet_records(mochii_ctx* c) {
     r.bits = c->rec.bits;
     r.sig = c->rec.sig;
     r.coef = c->rec.coef;
+    r.E = c->rec.E;
+    r.msig = c->rec.msig;
     return r;
 }
 
@@ -577,6 +676,11 @@ cudaError_t launch_rates(mochii_ctx* c) {
     } else {
         if (c->ntally == 2) k_rates<double, 2><<<blocks, 256, 0, c->stream>>>((const double*)c->tally, c->rates, n, cg, ch);
         else k_rates<double, 6><<<blocks, 256, 0, c->stream>>>((const double*)c->tally, c->rates, n, cg, ch);
+    }
+    if (c->metal.ntr > 0) {
+        const int mb = grid_blocks(n * c->metal.ntr, 256, 148 * 16);
+        if (c->fp32) k_metal_rates<float2><<<mb, 256, 0, c->stream>>>(c->metal, n, cg, ch);
+        else k_metal_rates<double><<<mb, 256, 0, c->stream>>>(c->metal, n, cg, ch);
     }
     return cudaGetLastError();
 }

@@ -26,6 +26,7 @@ cudaError_t launch_records_noalloc(mochii_ctx* c, long long ip0, long long n, do
 
 int balance_blocks(const mochii_ctx* c);
 cudaError_t launch_columns(mochii_ctx* c);
+cudaError_t launch_metal_fractions(mochii_ctx* c, double* out);   // nleaf x nstages, registry order
 cudaError_t launch_balance(mochii_ctx* c);
 cudaError_t launch_thermal(mochii_ctx* c);
 

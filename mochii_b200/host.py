@@ -132,12 +132,25 @@ class Nebula:
         self._ok(self.lib.mochii_opacity_fill(self.ctx))
 
     # ---- state exchange ---------------------------------------------------
+    def metal_shape(self):
+        """(transitions, stages) of the active metal registry; (0, 0) without metals."""
+        a, b = C.c_int(), C.c_int()
+        self._ok(self.lib.mochii_metal_shape(self.ctx, C.byref(a), C.byref(b)))
+        return a.value, b.value
+
     def get(self, name):
-        n = {"jt_ion": self.nleaf * self.nnu_band, "eedge": self.nnu_band + 1}.get(name, self.nleaf)
+        ntr, nst = self.metal_shape() if name in ("gamma_metal", "heat_metal", "x_metal") else (0, 0)
+        n = {"jt_ion": self.nleaf * self.nnu_band, "eedge": self.nnu_band + 1,
+             "gamma_metal": self.nleaf * ntr, "heat_metal": self.nleaf * ntr,
+             "x_metal": self.nleaf * nst}.get(name, self.nleaf)
         out = np.zeros(n, dtype=np.float64)
         self._ok(self.lib.mochii_get_field(self.ctx, name.encode(), out.ctypes.data, n))
         if name == "jt_ion":
             out = out.reshape(self.nleaf, self.nnu_band)
+        elif name in ("gamma_metal", "heat_metal"):
+            out = out.reshape(self.nleaf, ntr)
+        elif name == "x_metal":
+            out = out.reshape(self.nleaf, nst)
         return out
 
     def set(self, name, values):

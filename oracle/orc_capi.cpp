@@ -4,6 +4,7 @@
 
 #include "orc_core.h"
 #include "orc_thermal.h"
+#include "orc_species.h"
 
 using namespace orc;
 
@@ -158,15 +159,79 @@ int orc_sim_transport_pass(void* h) {
     static_cast<Sim*>(h)->transport_pass();
     return 0;
 }
+// Each update is followed by gas_opacity_fill, as in the iteration loop of
+// main.f90:130-171.
 int orc_sim_equilibrium_update(void* h, double* metrics2) {
-    static_cast<Sim*>(h)->gas_equilibrium_update(&metrics2[0], &metrics2[1]);
+    auto* s = static_cast<Sim*>(h);
+    s->gas_equilibrium_update(&metrics2[0], &metrics2[1]);
+    s->opacity_fill();
     return 0;
 }
 int orc_sim_thermal_update(void* h, double* metrics4) {
     auto* s = static_cast<Sim*>(h);
     if (!s->th) return 1;
     s->gas_thermal_update(metrics4);
+    s->opacity_fill();
     return 0;
+}
+// Metal registry probes for the charge-exchange gates (leaf 0 of the sim,
+// whose Gammas are zero before a transport pass).
+int orc_sim_metal_nel(void* h) {
+    auto* s = static_cast<Sim*>(h);
+    return s->metals() ? (int)s->sp->el.size() : 0;
+}
+int orc_sim_metal_el(void* h, int ie, char* name3, int* Z, int* nstage) {
+    auto* s = static_cast<Sim*>(h);
+    if (!s->metals() || ie < 0 || ie >= (int)s->sp->el.size()) return -1;
+    const Element& e = s->sp->el[ie];
+    std::strncpy(name3, e.name.c_str(), 2);
+    name3[2] = 0;
+    *Z = e.Z;
+    *nstage = e.nstage;
+    return 0;
+}
+double orc_sim_metal_eth(void* h, int ie, int it) { return static_cast<Sim*>(h)->sp->el[ie].eth[it - 1]; }
+void orc_sim_metal_cx(void* h, int ie, int it, double T, double* out2) {
+    const Element& e = static_cast<Sim*>(h)->sp->el[ie];
+    out2[0] = e.cxi_form[it - 1] > 0 ? cx_rate(e.cxi_form[it - 1], e.cxi[it - 1], T) : 0.0;
+    out2[1] = e.cxr_form[it - 1] > 0 ? cx_rate(e.cxr_form[it - 1], e.cxr[it - 1], T) : 0.0;
+}
+void orc_sim_metal_sums(void* h, double T, double nH, double ne, double nHI, double nHII, double* out3) {
+    auto* s = static_cast<Sim*>(h);
+    MetalCache c;
+    s->sp->prepare(0, T, s->rm, c);
+    s->sp->metal_sums(c, nH, ne, nHI, nHII, out3[0], out3[1], out3[2]);
+}
+void orc_sim_metal_fractions(void* h, int ie, double T, double ne, double nHI, double nHII, double* out) {
+    auto* s = static_cast<Sim*>(h);
+    s->sp->fractions(ie, 0, T, ne, nHI, nHII, s->rm, out);
+}
+// solve_ion_cell on leaf 0 with the sim's metal switches; st4 = x_HI, x_HeI,
+// x_HeII in, n_e out.
+void orc_sim_solve_cell(void* h, double gH, double gHe1, double gHe2, double nH, double T, int caseA, double* st4) {
+    auto* s = static_cast<Sim*>(h);
+    solve_ion_cell(s->rm, s->par.He_abund, gH, gHe1, gHe2, nH, T, caseA != 0, st4[0], st4[1], st4[2], st4[3],
+                   s->metals() ? s->sp : nullptr, 0, s->par.metal_ne, s->par.charge_exchange == "two_way");
+}
+// Metal terms of net_rate on leaf il: cool, cool_H, freefree, heat.
+int orc_sim_metal_thermal(void* h, int il, double T, double nH, double ne, double xHI, double* out4) {
+    auto* s = static_cast<Sim*>(h);
+    if (!s->metals() || !s->th) return -1;
+    const MetalThermal m = s->sp->thermal(il, T, nH, ne, nH * xHI, nH * (1.0 - xHI), s->rm, s->th->gff);
+    out4[0] = m.cool; out4[1] = m.cool_H; out4[2] = m.freefree; out4[3] = m.heat;
+    return 0;
+}
+// Metal registry shape: transitions and stages in element order.
+int orc_sim_metal_ntr(void* h) {
+    auto* s = static_cast<Sim*>(h);
+    return s->metals() ? s->sp->ntr : 0;
+}
+int orc_sim_metal_nstage(void* h) {
+    auto* s = static_cast<Sim*>(h);
+    if (!s->metals()) return 0;
+    int n = 0;
+    for (const Element& e : s->sp->el) n += e.nstage;
+    return n;
 }
 // Thermal building blocks for the tests.
 void orc_gff_table(double* logT41, double* z164) {
@@ -216,6 +281,38 @@ long long orc_sim_get(void* h, const char* name, double* out, long long cap) {
     else if (n == "jt_ion") v = &s->tally.jt;
     else if (n == "hhe") v = &s->tally.hhe;
     else if (n == "eedge") v = &s->band.eedge;
+    else if (s->metals() && (n == "gamma_metal" || n == "heat_metal" || n == "x_metal" || n == "metal_raw")) {
+        // leaf-major blocks in element order: (it, il) -> out[il*ntr + j]
+        const Species& sp = *s->sp;
+        const int nl = sp.nleaf;
+        std::vector<double> tmp;
+        if (n == "metal_raw") {
+            tmp = s->tally.metal;
+        } else if (n == "x_metal") {
+            int ns = 0;
+            for (const Element& e : sp.el) ns += e.nstage;
+            tmp.assign((size_t)ns * nl, 0.0);
+            int j0 = 0;
+            for (size_t ie = 0; ie < sp.el.size(); ++ie) {
+                for (int i = 0; i < sp.el[ie].nstage; ++i)
+                    for (int il = 0; il < nl; ++il) tmp[(size_t)il * ns + j0 + i] = sp.stage_frac[ie][(size_t)i * nl + il];
+                j0 += sp.el[ie].nstage;
+            }
+        } else {
+            const auto& src = n == "gamma_metal" ? sp.egam : sp.eheat;
+            tmp.assign((size_t)sp.ntr * nl, 0.0);
+            int j0 = 0;
+            for (size_t ie = 0; ie < sp.el.size(); ++ie) {
+                const int nt = sp.el[ie].nstage - 1;
+                for (int i = 0; i < nt; ++i)
+                    for (int il = 0; il < nl; ++il) tmp[(size_t)il * sp.ntr + j0 + i] = src[ie][(size_t)i * nl + il];
+                j0 += nt;
+            }
+        }
+        if ((long long)tmp.size() > cap) return -(long long)tmp.size();
+        std::memcpy(out, tmp.data(), tmp.size() * sizeof(double));
+        return (long long)tmp.size();
+    }
     if (!v) return -1;
     if ((long long)v->size() > cap) return -(long long)v->size();
     std::memcpy(out, v->data(), v->size() * sizeof(double));
@@ -233,6 +330,7 @@ long long orc_sim_set(void* h, const char* name, const double* in, long long n) 
     else if (nm == "nH") v = &s->st.nH;
     if (!v || (long long)v->size() != n) return -1;
     std::memcpy(v->data(), in, (size_t)n * sizeof(double));
+    s->opacity_fill();   // the stage cache follows the state it is read from
     return n;
 }
 // Diffuse field: build from the current state, then launch records.

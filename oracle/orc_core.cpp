@@ -2,6 +2,7 @@
 // transport + balance path.  See orc_core.h for the contract.
 #include "orc_core.h"
 #include "orc_thermal.h"
+#include "orc_species.h"
 
 #include <algorithm>
 #include <cctype>
@@ -656,6 +657,18 @@ bool parse_namelist(const std::string& text, Par& p, std::string* err) {
         B(diffuse_field); B(use_sec_ion); B(ion_add_dust); B(ion_dust_scatter);
         S(dust_density_law); D(cext_dust); S(data_dir); S(atomic_dir); S(ion_dust_kext);
         S(diffuse_energy_model);
+        B(ion_metal_abs); B(metal_ne); B(metal_heat); B(metal_freefree); B(fe_levels_full);
+        else if (k == "abund_c") p.abund_C = to_dbl(s);
+        else if (k == "abund_n") p.abund_N = to_dbl(s);
+        else if (k == "abund_o") p.abund_O = to_dbl(s);
+        else if (k == "abund_ne") p.abund_Ne = to_dbl(s);
+        else if (k == "abund_s") p.abund_S = to_dbl(s);
+        else if (k == "abund_ar") p.abund_Ar = to_dbl(s);
+        else if (k == "abund_mg") p.abund_Mg = to_dbl(s);
+        else if (k == "abund_fe") p.abund_Fe = to_dbl(s);
+        else if (k == "abund_si") p.abund_Si = to_dbl(s);
+        else if (k == "abund_cl") p.abund_Cl = to_dbl(s);
+        else if (k == "abund_ca") p.abund_Ca = to_dbl(s);
         else if (k == "dgr") p.DGR = to_dbl(s);
         else if (k == "he_abund") p.He_abund = to_dbl(s);
         else if (k == "nh_const") p.nH_const = to_dbl(s);
@@ -834,7 +847,7 @@ int ion_bin_of(const Band& b, double eph, bool include_fuv) {
 // sources with Planck spectra (the hot-path configurations), plus
 // setup_continuous_source_sampler / build_point_source_sampler
 // (:275-353, :437-495) and ion_qmc_ndim (:654-663).
-bool band_setup(const Par& p, Band& b, std::string* err) {
+bool band_setup(const Par& p, Band& b, std::string* err, const std::vector<double>& metal_eth) {
     int nfuv = 0;
     if (p.add_fuv) {
         if (p.efuv_min >= p.eion_min) {
@@ -850,7 +863,7 @@ bool band_setup(const Par& p, Band& b, std::string* err) {
     const double lo = std::log(p.eion_min), hi = std::log(p.eion_max);
     for (int i = 1; i <= nfuv; ++i)
         b.eedge[i - 1] = std::exp(std::log(p.efuv_min) + (lo - std::log(p.efuv_min)) * (double)(i - 1) / (double)nfuv);
-    std::vector<double> meth;  // metal thresholds: none on the H/He path
+    const std::vector<double>& meth = metal_eth;   // ion_band_mod.f90:166-175
     if (p.ion_align_edges) {
         if (!build_aligned_edges(b.eedge, nfuv, nnu, p.eion_min, p.eion_max, meth, err)) return false;
     } else {
@@ -865,7 +878,9 @@ bool band_setup(const Par& p, Band& b, std::string* err) {
     b.multi_src = b.ncomp >= 2;
     b.qmc_ndim = b.multi_src ? 7 : 3;
     const double elo = p.add_fuv ? p.efuv_min : p.eion_min;
+    // photoionization_threshold_knots, ion_band_mod.f90:408-419
     std::vector<double> knots = {ETH_HI, ETH_HEI, ETH_HEII};
+    for (double e : meth) knots.push_back(e);
     if (p.add_fuv) knots.push_back(p.eion_min);
     b.samplers.resize(b.ncomp);
     std::vector<double> band_L(b.ncomp);
@@ -902,15 +917,17 @@ bool band_setup(const Par& p, Band& b, std::string* err) {
 // =========================================================================
 // Tallies
 // =========================================================================
-void Tally::reset(int nleaf, int nnu) {
+void Tally::reset(int nleaf, int nnu, int ntr) {
     hhe.assign((size_t)6 * nleaf, 0.0);
     jt.assign((size_t)nnu * nleaf, 0.0);
+    metal.assign((size_t)2 * ntr * nleaf, 0.0);
     emitted = absorbed = escaped = 0;
     direct_segments = scattered_segments = 0;
 }
 void Tally::add(const Tally& o) {
     for (size_t i = 0; i < hhe.size(); ++i) hhe[i] += o.hhe[i];
     for (size_t i = 0; i < jt.size(); ++i) jt[i] += o.jt[i];
+    for (size_t i = 0; i < metal.size(); ++i) metal[i] += o.metal[i];
     emitted += o.emitted;
     absorbed += o.absorbed;
     escaped += o.escaped;
@@ -931,8 +948,8 @@ bool Sim::setup(const std::string& nl, std::string* err) {
         set_err(err, "oracle: only the namelist car grid is restated");
         return false;
     }
-    if (par.use_metals || par.ion_add_dust || par.use_sec_ion || par.add_fuv) {
-        set_err(err, "oracle: metals/dust/sec_ion/fuv not restated yet");
+    if (par.ion_add_dust || par.use_sec_ion || par.add_fuv) {
+        set_err(err, "oracle: dust/sec_ion/fuv not restated yet");
         return false;
     }
     if (par.solve_te) {
@@ -977,16 +994,36 @@ bool Sim::setup(const std::string& nl, std::string* err) {
     for (int i = 0; i < nleaf; ++i)
         st.ne[i] = st.nH[i] * ((1.0 - st.xHI[i]) +
                                par.He_abund * (st.xHeII[i] + 2.0 * std::max(0.0, 1.0 - st.xHeI[i] - st.xHeII[i])));
-    if (!band_setup(par, band, err)) return false;
+    // species before the band: the metal thresholds pin band edges and
+    // sampler knots (main.f90:64-83)
+    std::vector<double> meth;
+    if (par.use_metals) {
+        sp = new Species();
+        if (!sp->setup(par, nleaf, err)) return false;
+        meth = sp->thresholds();
+    }
+    if (!band_setup(par, band, err, meth)) return false;
     if (par.diffuse_field) milne.setup(par.eion_max);   // main.f90:102
     if (par.launch_sequence != "sobol") {
         set_err(err, "oracle: only the sobol launch sequence is restated");
         return false;
     }
-    tally.reset(nleaf, band.nnu_band);
+    tally.reset(nleaf, band.nnu_band, metals() ? sp->ntr : 0);
     gamma_HI.assign(nleaf, 0.0); gamma_HeI.assign(nleaf, 0.0); gamma_HeII.assign(nleaf, 0.0);
     heat_HI.assign(nleaf, 0.0); heat_HeI.assign(nleaf, 0.0); heat_HeII.assign(nleaf, 0.0);
+    opacity_fill();   // gas_opacity_setup -> gas_opacity_fill (gas_opacity_mod.f90:240-290)
     return true;
+}
+
+bool Sim::metals() const { return par.use_metals && sp != nullptr && !sp->el.empty(); }
+
+void Sim::opacity_fill() {
+    if (metals()) sp->stage_cache_refresh(st, rm);
+}
+
+void Sim::metal_sigma(Photon& ph) const {
+    ph.nm = 0;
+    if (metals()) ph.nm = sp->packet_sigma(ph.E, ph.sm);
 }
 
 // gen_ion_photon_qmc, ion_band_mod.f90:1880-1935, with emit_point_qmc
@@ -1024,6 +1061,7 @@ void Sim::gen_photon_qmc(int64_t ip, Photon& ph) const {
     ph.sHI = sigma_HI(e);
     ph.sHeI = sigma_HeI(e);
     ph.sHeII = sigma_HeII(e);
+    metal_sigma(ph);
 }
 
 // score_ion_path, ion_score_mod.f90:137-231 (H/He part).
@@ -1041,12 +1079,16 @@ static inline void score(const Sim& s, const Photon& ph, int il, double path_lum
     c[5] = ph.sHeII * std::max(1.0 - ETH_HEII / energy, 0.0);
     double* h = &t.hhe[(size_t)6 * il];
     for (int k = 0; k < 6; ++k) h[k] = h[k] + path_lum * c[k];
+    if (ph.nm > 0) s.sp->score(energy, ph.sm, ph.nm, il, path_lum, t.metal.data());
 }
 
 // ion_packet_opacity, ion_packet_mod.f90:55-87 (gas part).
 static inline double opacity(const Sim& s, const Photon& ph, int il) {
+    double metal = 0.0;
+    if (ph.nm > 0 && s.par.ion_metal_abs) metal = s.sp->cached_opacity(ph.sm, ph.nm, il);
     return s.st.nH[il] *
-           (s.st.xHI[il] * ph.sHI + s.par.He_abund * (s.st.xHeI[il] * ph.sHeI + s.st.xHeII[il] * ph.sHeII)) *
+           (s.st.xHI[il] * ph.sHI + s.par.He_abund * (s.st.xHeI[il] * ph.sHeI + s.st.xHeII[il] * ph.sHeII) +
+            metal) *
            s.par.distance2cm;
 }
 
@@ -1145,7 +1187,8 @@ void Sim::transport_pass() {
     const int nnu = band.nnu_band;
     const int nt = std::max(1, nthreads);
     std::vector<Tally> loc(nt);
-    for (auto& t : loc) t.reset(nleaf, nnu);
+    const int ntr = metals() ? sp->ntr : 0;
+    for (auto& t : loc) t.reset(nleaf, nnu, ntr);
     const int64_t np = par.nphotons;
 #pragma omp parallel num_threads(nt)
     {
@@ -1192,9 +1235,13 @@ void Sim::transport_pass() {
             }
         }
     }
-    tally.reset(nleaf, nnu);
+    tally.reset(nleaf, nnu, ntr);
     for (auto& t : loc) tally.add(t);
     gas_rates_compute();
+    if (metals()) {   // species_gamma_compute, species_mod.f90:493-512
+        const double w = grid.dcell;
+        sp->gamma_compute(tally.metal, 1.0 / ((w * w * w) * (par.distance2cm * par.distance2cm)));
+    }
 }
 
 // ---- milne_recomb_spectrum_mod.f90 -------------------------------------------
@@ -1397,6 +1444,7 @@ void Sim::gen_diffuse_qmc(int64_t ip, Photon& ph) const {
     ph.sHI = sigma_HI(eph);
     ph.sHeI = sigma_HeI(eph);
     ph.sHeII = sigma_HeII(eph);
+    metal_sigma(ph);
 }
 
 // gas_rates_compute + ion_score_apply_hhe, gas_rates_mod.f90:82-153 and
@@ -1417,11 +1465,17 @@ void Sim::gas_rates_compute() {
     }
 }
 
-// solve_ion_cell, ion_balance_mod.f90:53-150 (H/He path: no metal sums, so
-// r_cx_in = r_cx_out = 0 and the closed-form substitution branch is used).
+// solve_ion_cell, ion_balance_mod.f90:53-150.  Without metals r_cx_in =
+// r_cx_out = 0 and the closed-form substitution branch is used; with the
+// two-way charge exchange x_HI comes from hydrogen_neutral_fraction.
 void solve_ion_cell(const RateModel& rm, double yHe, double gH, double gHe1,
                     double gHe2, double nH, double T, bool caseA, double& xHI,
-                    double& xHeI, double& xHeII, double& ne) {
+                    double& xHeI, double& xHeII, double& ne, const Species* sp, int il,
+                    bool metal_ne, bool two_way) {
+    const bool with_ne = sp != nullptr && metal_ne;
+    const bool with_cx = sp != nullptr && two_way;
+    MetalCache mc;
+    if (with_ne || with_cx) sp->prepare(il, T, rm, mc);
     double aH, aHe2, aHe3;
     if (caseA) {
         aH = alphaA_HII(rm, T); aHe2 = alphaA_HeII(rm, T); aHe3 = alphaA_HeIII(rm, T);
@@ -1432,31 +1486,56 @@ void solve_ion_cell(const RateModel& rm, double yHe, double gH, double gHe1,
     double xHeIII = std::max(0.0, 1.0 - xHeI - xHeII);
     ne = nH * ((1.0 - xHI) + yHe * (xHeII + 2.0 * xHeIII));
     ne = std::max(ne, 1.0e-12 * nH);
-    const double r_cx_in = 0.0, r_cx_out = 0.0;
+    double nem = 0.0, r_cx_in = 0.0, r_cx_out = 0.0;
     for (int it = 1; it <= 200; ++it) {
         const double ne_old = ne;
-        const double denH = gH + (cH + aH) * ne + r_cx_in + r_cx_out;
-        xHI = (denH > 0.0) ? (aH * ne + r_cx_in) / denH : 1.0;
+        if (with_ne || with_cx) {
+            sp->metal_sums(mc, nH, ne_old, nH * xHI, nH * (1.0 - xHI), nem, r_cx_in, r_cx_out);
+            if (!with_cx) {
+                r_cx_in = 0.0;
+                r_cx_out = 0.0;
+            }
+        }
+        if (with_cx) {
+            xHI = hydrogen_neutral_fraction(*sp, mc, nH, ne, aH * ne, gH + (cH + aH) * ne);
+        } else {
+            const double denH = gH + (cH + aH) * ne + r_cx_in + r_cx_out;
+            xHI = (denH > 0.0) ? (aH * ne + r_cx_in) / denH : 1.0;
+        }
         const double r1 = std::min((gHe1 + cHe1 * ne) / (aHe2 * ne), 1.0e150);
         const double r2 = std::min((gHe2 + cHe2 * ne) / (aHe3 * ne), 1.0e150);
         xHeI = 1.0 / (1.0 + r1 + r1 * r2);
         xHeII = xHeI * r1;
         xHeIII = xHeII * r2;
         ne = nH * ((1.0 - xHI) + yHe * (xHeII + 2.0 * xHeIII));
+        if (with_ne) ne = ne + nem;
         ne = std::max(0.5 * (ne + ne_old), 1.0e-12 * nH);
         if (std::fabs(ne - ne_old) <= 1.0e-10 * ne) break;
     }
 }
 
-Sim::~Sim() { delete th; }
+Sim::~Sim() {
+    delete th;
+    delete sp;
+}
 
 // net_rate, thermal_mod.f90:38-115 (H/He; no metals, no grain PE, no
 // secondary ionisation so sec_dgamma = 0 and sec_heat = heat).
 double Sim::net_rate(int il, double T, bool caseA, double& xHI, double& xHeI, double& xHeII, double& ne) const {
     const double nH = st.nH[il];
-    solve_ion_cell(rm, par.He_abund, gamma_HI[il], gamma_HeI[il], gamma_HeII[il], nH, T, caseA, xHI, xHeI, xHeII, ne);
+    const bool m = metals();
+    solve_ion_cell(rm, par.He_abund, gamma_HI[il], gamma_HeI[il], gamma_HeII[il], nH, T, caseA, xHI, xHeI, xHeII, ne,
+                   m ? sp : nullptr, il, par.metal_ne, par.charge_exchange == "two_way");
     const double heat = nH * (xHI * heat_HI[il] + par.He_abund * (xHeI * heat_HeI[il] + xHeII * heat_HeII[il]));
-    return heat - cooling_total(*th, rm, caseA, par.He_abund, T, nH, ne, xHI, xHeI, xHeII);
+    double net = heat - cooling_total(*th, rm, caseA, par.He_abund, T, nH, ne, xHI, xHeI, xHeII);
+    if (par.use_metals && m) {   // thermal_mod.f90:53-71
+        const MetalThermal mt = sp->thermal(il, T, nH, ne, nH * xHI, nH * (1.0 - xHI), rm, th->gff);
+        net = net - mt.cool;
+        net = net - mt.cool_H;
+        if (par.metal_freefree) net = net - mt.freefree;
+        if (par.metal_heat) net = net + mt.heat;
+    }
+    return net;
 }
 
 // gas_thermal_update, thermal_mod.f90:124-249.
@@ -1496,6 +1575,8 @@ void Sim::gas_thermal_update(double m[4]) {
         xHeII_new[il] = (1.0 - w) * st.xHeII[il] + w * xHeII;
         const double xHeIII = std::max(0.0, 1.0 - xHeI_new[il] - xHeII_new[il]);
         ne_new[il] = nH * ((1.0 - xHI_new[il]) + par.He_abund * (xHeII_new[il] + 2.0 * xHeIII));
+        if (par.metal_ne && metals())   // thermal_mod.f90:198-203
+            ne_new[il] = charge_neutrality_ne(*sp, rm, il, te, nH, ne_new[il], xHI_new[il], ne);
         te_new[il] = te;
     }
     const double hw = grid.dcell;
@@ -1531,12 +1612,15 @@ void Sim::gas_equilibrium_update(double* max_dx, double* dx_vol) {
             continue;
         }
         double xHI = st.xHI[il], xHeI = st.xHeI[il], xHeII = st.xHeII[il], ne;
-        solve_ion_cell(rm, yHe, gamma_HI[il], gamma_HeI[il], gamma_HeII[il], nH, T, caseA, xHI, xHeI, xHeII, ne);
+        solve_ion_cell(rm, yHe, gamma_HI[il], gamma_HeI[il], gamma_HeII[il], nH, T, caseA, xHI, xHeI, xHeII, ne,
+                       metals() ? sp : nullptr, il, par.metal_ne, par.charge_exchange == "two_way");
         xHI_new[il] = (1.0 - w) * st.xHI[il] + w * xHI;
         xHeI_new[il] = (1.0 - w) * st.xHeI[il] + w * xHeI;
         xHeII_new[il] = (1.0 - w) * st.xHeII[il] + w * xHeII;
         const double xHeIII = std::max(0.0, 1.0 - xHeI_new[il] - xHeII_new[il]);
         ne_new[il] = nH * ((1.0 - xHI_new[il]) + yHe * (xHeII_new[il] + 2.0 * xHeIII));
+        if (par.metal_ne && metals())   // ion_balance_mod.f90:401-410
+            ne_new[il] = charge_neutrality_ne(*sp, rm, il, T, nH, ne_new[il], xHI_new[il], ne);
     }
     const double hw = grid.dcell;
     const double vol = hw * hw * hw;

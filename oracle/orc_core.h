@@ -147,6 +147,11 @@ struct Par {
     std::string dust_density_law = "global_dgr";
     double DGR = 1.0e-2, cext_dust = 1.6059e-21;
     std::string data_dir, atomic_dir, ion_dust_kext;
+    // metals (define.f90:578-580, 593, 622-623, 652, 843-857)
+    double abund_C = 2.2e-4, abund_N = 4.0e-5, abund_O = 3.3e-4, abund_Ne = 5.0e-5, abund_S = 9.0e-6;
+    double abund_Ar = 0.0, abund_Mg = 0.0, abund_Fe = 0.0, abund_Si = 0.0, abund_Cl = 0.0, abund_Ca = 0.0;
+    bool ion_metal_abs = true, metal_ne = true, metal_heat = true, metal_freefree = true;
+    bool fe_levels_full = false;
     Par();
 };
 // Parse a Fortran "&parameters par%key = value /" namelist text.
@@ -168,7 +173,7 @@ bool build_aligned_edges(std::vector<double>& eedge, int nfuv, int nnu,
                          double lo, double hi, const std::vector<double>& meth,
                          std::string* err);
 int ion_bin_of(const Band& b, double e, bool include_fuv);
-bool band_setup(const Par& p, Band& b, std::string* err);
+bool band_setup(const Par& p, Band& b, std::string* err, const std::vector<double>& meth = {});
 
 // ---- car grid + state ----------------------------------------------------
 struct Grid {
@@ -184,9 +189,10 @@ struct State {
 struct Tally {
     std::vector<double> hhe;         // (6, nleaf), leaf-major: hhe[6*il + k]
     std::vector<double> jt;          // (nnu_band, nleaf): jt[nnu*il + inu]
+    std::vector<double> metal;       // metal path estimators [(il*ntr + k)*2 + m]
     long double emitted = 0, absorbed = 0, escaped = 0;
     int64_t direct_segments = 0, scattered_segments = 0;
-    void reset(int nleaf, int nnu);
+    void reset(int nleaf, int nnu, int ntr = 0);
     void add(const Tally& o);
 };
 
@@ -195,9 +201,12 @@ struct Photon {
     double E, wgt, Lpacket;
     int inu;
     double sHI, sHeI, sHeII;
+    int nm = 0;                      // active metal transitions (E >= E_th)
+    double sm[64];                   // their cross sections, threshold order
 };
 
 struct Thermal;
+struct Species;
 
 // milne_recomb_spectrum_mod.f90: ground-continuum recombination spectra.
 struct Milne {
@@ -214,6 +223,7 @@ struct Milne {
 struct Sim {
     Par par;
     Thermal* th = nullptr;           // thermal tables (solve_te)
+    Species* sp = nullptr;           // metal registry (use_metals)
     RateModel rm;
     Qmc qmc;
     Band band;
@@ -236,6 +246,9 @@ struct Sim {
     void gas_thermal_update(double m[4]);                         // thermal_mod.f90:124-249
     double net_rate(int il, double T, bool caseA, double& xHI, double& xHeI, double& xHeII,
                     double& ne) const;                             // thermal_mod.f90:38-115
+    void opacity_fill();             // gas_opacity_fill, gas_opacity_mod.f90:299-306
+    bool metals() const;             // use_metals with at least one element
+    void metal_sigma(Photon& ph) const;   // species_packet_cross_sections
     ~Sim();
     void gen_photon_qmc(int64_t ip, Photon& ph) const;          // ion_band_mod.f90:1880
     void walk_edge_car(const Photon& ph, Tally& t, double* tau_edge) const;  // raytrace_amr.f90:534
@@ -243,8 +256,12 @@ struct Sim {
                         double kz, int max_steps, int32_t* out) const;
 };
 
+// With sp != nullptr the metal electrons (metal_ne) and the two-way charge
+// exchange (two_way) of leaf il join the closure.
 void solve_ion_cell(const RateModel& rm, double He_abund, double gH,
                     double gHe1, double gHe2, double nH, double T, bool caseA,
-                    double& xHI, double& xHeI, double& xHeII, double& ne);
+                    double& xHI, double& xHeI, double& xHeII, double& ne,
+                    const Species* sp = nullptr, int il = -1, bool metal_ne = false,
+                    bool two_way = false);
 
 }  // namespace orc

@@ -60,6 +60,16 @@ def load():
         "orc_solve_ion_cell": (None, [I, D, D, D, D, D, D, I, V, V]),
         "orc_last_error": (C.c_char_p, []),
         "orc_sim_thermal_update": (I, [V, V]),
+        "orc_sim_metal_ntr": (I, [V]),
+        "orc_sim_metal_nel": (I, [V]),
+        "orc_sim_metal_el": (I, [V, I, C.c_char_p, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
+        "orc_sim_metal_eth": (D, [V, I, I]),
+        "orc_sim_metal_cx": (None, [V, I, I, D, V]),
+        "orc_sim_metal_sums": (None, [V, D, D, D, D, D, V]),
+        "orc_sim_metal_fractions": (None, [V, I, D, D, D, D, V]),
+        "orc_sim_solve_cell": (None, [V, D, D, D, D, D, I, V]),
+        "orc_sim_metal_thermal": (I, [V, I, D, D, D, D, V]),
+        "orc_sim_metal_nstage": (I, [V]),
         "orc_gff_table": (None, [V, V]),
         "orc_cooling_total": (D, [V, D, D, D, D, D, D]),
         "orc_nlevel_cooling_at": (D, [C.c_char_p, D, D]),
@@ -213,14 +223,75 @@ class Sim:
         load().orc_sim_energy(self.h, e.ctypes.data, s.ctypes.data)
         return e, s
 
+    # ---- metal registry probes (leaf 0) -----------------------------------
+    def metal_elements(self):
+        """[(name, Z, nstage)] in registry order."""
+        lib = load()
+        out = []
+        for ie in range(lib.orc_sim_metal_nel(self.h)):
+            nm = C.create_string_buffer(3)
+            z, ns = C.c_int(), C.c_int()
+            lib.orc_sim_metal_el(self.h, ie, nm, C.byref(z), C.byref(ns))
+            out.append((nm.value.decode(), z.value, ns.value))
+        return out
+
+    def metal_eth(self, ie, it):
+        return load().orc_sim_metal_eth(self.h, ie, it)
+
+    def metal_cx(self, ie, it, T):
+        o = np.zeros(2)
+        load().orc_sim_metal_cx(self.h, ie, it, float(T), o.ctypes.data)
+        return o[0], o[1]
+
+    def metal_sums(self, T, nH, ne, nHI, nHII):
+        o = np.zeros(3)
+        load().orc_sim_metal_sums(self.h, float(T), float(nH), float(ne), float(nHI), float(nHII), o.ctypes.data)
+        return tuple(o)
+
+    def metal_fractions(self, ie, T, ne, nHI, nHII):
+        o = np.zeros(8)
+        load().orc_sim_metal_fractions(self.h, ie, float(T), float(ne), float(nHI), float(nHII), o.ctypes.data)
+        return o[: self.metal_elements()[ie][2]]
+
+    def solve_cell(self, gH, gHe1, gHe2, nH, T, caseA, xHI, xHeI, xHeII):
+        st = np.array([xHI, xHeI, xHeII, 0.0])
+        load().orc_sim_solve_cell(self.h, float(gH), float(gHe1), float(gHe2), float(nH), float(T), int(caseA),
+                                  st.ctypes.data)
+        return tuple(st)
+
+    def metal_thermal(self, il, T, nH, ne, xHI):
+        o = np.zeros(4)
+        assert load().orc_sim_metal_thermal(self.h, int(il), float(T), float(nH), float(ne), float(xHI),
+                                            o.ctypes.data) == 0
+        return tuple(o)
+
+    @property
+    def metal_ntr(self):
+        return load().orc_sim_metal_ntr(self.h)
+
+    @property
+    def metal_nstage(self):
+        return load().orc_sim_metal_nstage(self.h)
+
     def get(self, name):
+        lib = load()
         cap = self.nleaf * max(self.nnu, 6) + 1024
         out = np.zeros(cap)
-        n = load().orc_sim_get(self.h, name.encode(), out.ctypes.data, cap)
+        n = lib.orc_sim_get(self.h, name.encode(), out.ctypes.data, cap)
+        if n < -1:   # larger field: the negative return is its size
+            cap = -n
+            out = np.zeros(cap)
+            n = lib.orc_sim_get(self.h, name.encode(), out.ctypes.data, cap)
         assert n >= 0, name
         out = out[:n]
         if name == "jt_ion":
             out = out.reshape(self.nleaf, self.nnu)
+        elif name in ("gamma_metal", "heat_metal"):
+            out = out.reshape(self.nleaf, self.metal_ntr)
+        elif name == "x_metal":
+            out = out.reshape(self.nleaf, self.metal_nstage)
+        elif name == "metal_raw":
+            out = out.reshape(self.nleaf, self.metal_ntr, 2)
         return out
 
     def set(self, name, values):
