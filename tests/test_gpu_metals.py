@@ -154,9 +154,10 @@ def test_metal_pass_with_diffuse_and_thermal_runs_clean():
     FP32 transport) on a small grid: closure, finite state, bounded T_e."""
     nl = configs.hii_metals(nphotons=100000, niter=3, n=24, precision="fp32", rs_factor=1.2)
     neb = Nebula(parse_namelist(nl))
-    for _ in range(3):
+    for it in range(3):
         st = neb.ionizing_field_and_rates()
-        assert st.closure <= 5e-13 and st.diffuse_packets > 0
+        assert st.closure <= 5e-13
+        assert it == 0 or st.diffuse_packets > 0   # the neutral start has no recombinations
         neb.gas_thermal_update()
     t, x = neb.get("T_e"), neb.get("x_HI")
     assert np.isfinite(t).all() and np.isfinite(x).all()
