@@ -121,6 +121,11 @@ typedef struct mochii_params {
     int precision;
     /* par%fe_levels_full: Fe n-level atoms from the '_full' files */
     int fe_levels_full;
+    /* metal path tallies (not a reference key, 'moments' or 'exact'):
+     * 1 = per-leaf Chebyshev energy moments in threshold-aligned bins,
+     * contracted with the cross sections after the pass; 0 = one pair of
+     * tallies per active transition per segment (species_rate_path_score) */
+    int metal_moments;
 } mochii_params;
 
 /* Per-pass statistics (ion_score_report_energy_closure, ion_score_mod.f90:364-387). */
@@ -141,6 +146,9 @@ typedef struct mochii_metrics {
     int64_t cells_solved;
     int64_t fixed_point_cap_hits;    /* cells whose n_e loop used all 200 passes */
     double kernel_ms;
+    int64_t fixed_point_passes;      /* n_e fixed-point passes over all cells and trial T */
+    int64_t metal_sum_calls;         /* metal cascade sums (species_metal_sums) evaluated */
+    int64_t rate_evaluations;        /* net_rate evaluations (thermal) or cell solves      */
 } mochii_metrics;
 
 /* Launch shapes of the transport walk (the autotuner's choice). */

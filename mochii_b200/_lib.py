@@ -52,7 +52,7 @@ class Params(C.Structure):
         ("DGR", C.c_double), ("cext_dust", C.c_double), ("grain_pe", C.c_int),
         ("ion_dust_kext", C.c_char * STRLEN), ("data_dir", C.c_char * STRLEN), ("atomic_dir", C.c_char * STRLEN),
         ("precision", C.c_int),
-        ("fe_levels_full", C.c_int),
+        ("fe_levels_full", C.c_int), ("metal_moments", C.c_int),
     ]
 
 
@@ -65,7 +65,8 @@ class PassStats(C.Structure):
 
 class Metrics(C.Structure):
     _fields_ = [("max_dx", C.c_double), ("max_dte", C.c_double), ("dx_vol", C.c_double), ("dte_vol", C.c_double),
-                ("cells_solved", C.c_int64), ("fixed_point_cap_hits", C.c_int64), ("kernel_ms", C.c_double)]
+                ("cells_solved", C.c_int64), ("fixed_point_cap_hits", C.c_int64), ("kernel_ms", C.c_double),
+                ("fixed_point_passes", C.c_int64), ("metal_sum_calls", C.c_int64), ("rate_evaluations", C.c_int64)]
 
 
 class Tuning(C.Structure):

@@ -7,6 +7,7 @@ and the source-energy inversion must round exactly as the FP64 source
 expressions do (no fused multiply-add contraction), which is what makes
 leaf sequences and sampled energies bit-identical to the CPU restatement.
 """
+import concurrent.futures
 import os
 import shutil
 import subprocess
@@ -46,7 +47,7 @@ def build(force=False, verbose=False):
     os.makedirs(objdir, exist_ok=True)
     common = ["-O3", "-std=c++17", "-lineinfo", "-fmad=false", "-Xcompiler", "-fPIC",
               "-ccbin", hostcxx, "-I", INCLUDE, "-I", CSRC] + ARCH
-    objs = []
+    objs, cmds = [], []
     for src in SOURCES:
         obj = os.path.join(objdir, src + ".o")
         cmd = [nvcc, "-c", os.path.join(CSRC, src), "-o", obj] + common
@@ -54,8 +55,16 @@ def build(force=False, verbose=False):
             cmd = [nvcc, "-x", "cu", "-c", os.path.join(CSRC, src), "-o", obj] + common
         if verbose:
             print(" ".join(cmd))
-        subprocess.run(cmd, check=True)
+        cmds.append(cmd)
         objs.append(obj)
+    # the translation units are independent: compile them concurrently
+    with concurrent.futures.ThreadPoolExecutor(max_workers=min(len(cmds), os.cpu_count() or 1)) as ex:
+        for r in ex.map(lambda c: subprocess.run(c, capture_output=True, text=True), cmds):
+            if r.returncode != 0:
+                sys.stderr.write(r.stdout + r.stderr)
+                raise subprocess.CalledProcessError(r.returncode, r.args)
+            if verbose and r.stderr:
+                sys.stderr.write(r.stderr)
     tmp = LIB + ".tmp"
     cmd = [nvcc, "-shared", "-o", tmp] + objs + ARCH + ["-ccbin", hostcxx, "-lcudart", "-ldl"]
     subprocess.run(cmd, check=True)

@@ -129,7 +129,8 @@ def hii_metals(nphotons=10_000_000, niter=20, n=128, precision="fp32", seed=1234
     """H+He+metals H II region with the thermal balance: 128^3 uniform grid,
     n_H = 100, He/H 0.1, eleven trace metals, a 45 kK blackbody with Q(H) =
     5e49 s^-1, case A with explicit diffuse Milne recombination packets, no
-    dust; T_e solved in [3e3, 3e4] K."""
+    dust; T_e solved in [3e3, 3e4] K, from an ionized start (x_HI = 1e-3,
+    He half singly ionized) as the reference's H II-region inputs use."""
     rs = stromgren_radius_pc(Q=5.0e49) * rs_factor
     ab = "\n".join(f" par%abund_{k} = {v:.6e}" for k, v in METALS.items())
     return f"""&parameters
@@ -149,6 +150,9 @@ def hii_metals(nphotons=10_000_000, niter=20, n=128, precision="fp32", seed=1234
  par%tstar = 4.5e4
  par%luminosity = {5.0e49 * mean_photon_energy_ev(4.5e4) * EV2ERG:.6e}
  par%case_ab = 'A'
+ par%xHI_init = 1.0e-3
+ par%xHeI_init = 0.5
+ par%xHeII_init = 0.5
  par%diffuse_field = {'.true.' if diffuse else '.false.'}
  par%solve_te = {'.true.' if solve_te else '.false.'}
  par%te_min = 3.0e3

@@ -76,6 +76,7 @@ void release(mochii_ctx* c) {
                     c->th.gff, c->th.lamref, c->th.Ssup, c->th.tinv,
                     c->dif.ch, c->dif.tot, c->dif.scan_tmp, c->dif.tables,
                     (void*)c->metal.el, c->metal.egam, c->metal.eheat, c->metal.opac, c->metal.raw,
+                    (void*)c->metal.medge, c->metal.mom,
                     (void*)c->rec.E, c->rec.msig};
     for (void* p : ptrs)
         if (p) cudaFree(p);
@@ -270,7 +271,24 @@ extern "C" int mochii_init(const mochii_params* pin, mochii_ctx** out) {
         CKI(cudaMemset(m.eheat, 0, (size_t)n * m.ntr * 8));
         CKI(cudaMalloc(&m.opac, (size_t)n * m.ntrp * rsz + 64));
         CKI(cudaMemset(m.opac, 0, (size_t)n * m.ntrp * rsz));
-        CKI(cudaMalloc(&m.raw, (size_t)n * m.ntrp * 2 * tsz + 64));
+        if (p.metal_moments) {
+            species_moment_tables(c->species, p.add_fuv ? p.efuv_min : p.eion_min, p.eion_max);
+            const SpeciesHost& s2 = c->species;
+            m.nmb = (int)s2.medge.size() - 1;
+            // one allocation: medge | mcoef | mb0
+            const size_t b1 = al(s2.medge.size() * 8), b2 = al(s2.mcoef.size() * 8), b3 = al(s2.mb0.size() * 4);
+            char* mq = nullptr;
+            CKI(cudaMalloc(&mq, b1 + b2 + b3));
+            CKI(cudaMemcpy(mq, s2.medge.data(), s2.medge.size() * 8, cudaMemcpyHostToDevice));
+            CKI(cudaMemcpy(mq + b1, s2.mcoef.data(), s2.mcoef.size() * 8, cudaMemcpyHostToDevice));
+            CKI(cudaMemcpy(mq + b1 + b2, s2.mb0.data(), s2.mb0.size() * 4, cudaMemcpyHostToDevice));
+            m.medge = reinterpret_cast<const double*>(mq);
+            m.mcoef = reinterpret_cast<const double*>(mq + b1);
+            m.mb0 = reinterpret_cast<const int*>(mq + b1 + b2);
+            CKI(cudaMalloc(&m.mom, (size_t)n * m.nmb * kMomDeg * tsz + 64));
+        } else {
+            CKI(cudaMalloc(&m.raw, (size_t)n * m.ntrp * 2 * tsz + 64));
+        }
     }
     // sampler tables, component table, bin edges, QMC tables
     std::vector<double> te, tf, tc, comp;
@@ -357,7 +375,7 @@ extern "C" int mochii_init(const mochii_params* pin, mochii_ctx** out) {
         c->thermal_ready = true;
     }
     CKI(dalloc(&c->bw.partial, 6 * (size_t)c->bw.blocks));
-    CKI(dalloc(&c->bw.counters, 4));
+    CKI(dalloc(&c->bw.counters, 8));
     CKI(launch_columns(c));
     CKI(cudaStreamSynchronize(c->stream));
     c->columns_fresh = true;
@@ -416,7 +434,9 @@ extern "C" int mochii_transport_pass(mochii_ctx* c, int with_peel, mochii_pass_s
     // jt_ion(:,:) = 0 and ion_score_reset (ionizing_field_mod.f90:90-91)
     CK(c, cudaMemsetAsync(c->tally, 0, (size_t)n * c->ntally * tsz, c->stream));
     CK(c, cudaMemsetAsync(c->jt, 0, (size_t)n * c->nnu * tsz, c->stream));
-    if (c->metal.ntr > 0)   // species_rate_path_reset (species_mod.f90:321-326)
+    if (c->metal.ntr > 0 && c->metal.nmb > 0)   // species_rate_path_reset (species_mod.f90:321-326)
+        CK(c, cudaMemsetAsync(c->metal.mom, 0, (size_t)n * c->metal.nmb * kMomDeg * tsz, c->stream));
+    else if (c->metal.ntr > 0)
         CK(c, cudaMemsetAsync(c->metal.raw, 0, (size_t)n * c->metal.ntrp * 2 * tsz, c->stream));
     CK(c, cudaMemsetAsync(c->tw.counters, 0, 4 * sizeof(unsigned long long), c->stream));
     CK(c, cudaEventRecord(c->ev0, c->stream));
@@ -471,7 +491,7 @@ extern "C" int mochii_balance_update(mochii_ctx* c, int solve_te, mochii_metrics
     if (!c) return MOCHII_ERR_BAD_PARAM;
     if (solve_te && !c->thermal_ready)
         return fail(c, MOCHII_ERR_BAD_PARAM, "the thermal solve needs par%solve_te = .true. at mochii_init (tables)");
-    CK(c, cudaMemsetAsync(c->bw.counters, 0, 4 * sizeof(unsigned long long), c->stream));
+    CK(c, cudaMemsetAsync(c->bw.counters, 0, 8 * sizeof(unsigned long long), c->stream));
     CK(c, cudaEventRecord(c->ev0, c->stream));
     if (solve_te) CK(c, launch_thermal(c));
     else CK(c, launch_balance(c));
@@ -479,7 +499,7 @@ extern "C" int mochii_balance_update(mochii_ctx* c, int solve_te, mochii_metrics
     c->columns_fresh = true;   // both kernels refresh the columns they change
     const int np = solve_te ? 6 : 3;
     std::vector<double> part((size_t)np * c->bw.blocks);
-    unsigned long long cnt[4];
+    unsigned long long cnt[8];
     CK(c, cudaMemcpyAsync(part.data(), c->bw.partial, part.size() * 8, cudaMemcpyDeviceToHost, c->stream));
     CK(c, cudaMemcpyAsync(cnt, c->bw.counters, sizeof(cnt), cudaMemcpyDeviceToHost, c->stream));
     CK(c, cudaStreamSynchronize(c->stream));
@@ -508,6 +528,9 @@ extern "C" int mochii_balance_update(mochii_ctx* c, int solve_te, mochii_metrics
     }
     r.cells_solved = (int64_t)cnt[0];
     r.fixed_point_cap_hits = (int64_t)cnt[1];
+    r.fixed_point_passes = (int64_t)cnt[2];
+    r.metal_sum_calls = (int64_t)cnt[3];
+    r.rate_evaluations = (int64_t)cnt[4];
     r.kernel_ms = ms;
     if (m) *m = r;
     if (!std::isfinite(r.max_dx) || !std::isfinite(r.dx_vol) || !std::isfinite(r.max_dte))

@@ -137,7 +137,7 @@ __device__ int solve_cell(const Coef& k, double yHe, double gH, double gHe1, dou
 // (hydrogen_neutral_fraction); the cache mc is prepared at T.
 __device__ __noinline__ int solve_cell_metal(const Coef& k, double yHe, double gH, double gHe1, double gHe2, double nH,
                                              double& xHI, double& xHeI, double& xHeII, double& ne, const MetalDev& m,
-                                             const MetalCache& mc, int with_ne, int with_cx) {
+                                             const MetalCache& mc, int with_ne, int with_cx, int* nsum) {
     double xHeIII = fmax(0.0, 1.0 - xHeI - xHeII);
     ne = nH * ((1.0 - xHI) + yHe * (xHeII + 2.0 * xHeIII));
     ne = fmax(ne, 1.0e-12 * nH);
@@ -147,13 +147,14 @@ __device__ __noinline__ int solve_cell_metal(const Coef& k, double yHe, double g
         const double ne_old = ne;
         if (with_ne || with_cx) {
             metal_sums(m, mc, nH, ne_old, nH * xHI, nH * (1.0 - xHI), nem, rin, rout);
+            ++*nsum;
             if (!with_cx) {
                 rin = 0.0;
                 rout = 0.0;
             }
         }
         if (with_cx) {
-            xHI = hydrogen_neutral_fraction(m, mc, nH, ne, k.aH * ne, gH + (k.cH + k.aH) * ne);
+            xHI = hydrogen_neutral_fraction(m, mc, nH, ne, k.aH * ne, gH + (k.cH + k.aH) * ne, nsum);
         } else {
             const double denH = gH + (k.cH + k.aH) * ne + rin + rout;
             xHI = denH > 0.0 ? (k.aH * ne + rin) / denH : 1.0;
@@ -174,7 +175,7 @@ __device__ __noinline__ int solve_cell_metal(const Coef& k, double yHe, double g
 __global__ void __launch_bounds__(kBThreads) k_balance(const BalArgs a) {
     __shared__ double sh[3][kBThreads];
     double mdx = 0.0, sdx = 0.0, sx = 0.0;
-    unsigned long long solved = 0, caps = 0;
+    unsigned long long solved = 0, caps = 0, passes = 0, sums = 0;
     for (long long il = (long long)blockIdx.x * blockDim.x + threadIdx.x; il < a.nleaf;
          il += (long long)gridDim.x * blockDim.x) {
         const double nH = a.nH[il];
@@ -186,17 +187,19 @@ __global__ void __launch_bounds__(kBThreads) k_balance(const BalArgs a) {
         }
         double xHI = x0, xHeI = h10, xHeII = h20, ne;
         MetalCache mc;
-        int it;
+        int it, nsum = 0;
         if (a.m.ntr > 0) {
             metal_prepare(a.m, il, a.T, mc);
             it = solve_cell_metal(a.k, a.yHe, a.rates[il], a.rates[a.nleaf + il], a.rates[2 * a.nleaf + il], nH, xHI,
-                                  xHeI, xHeII, ne, a.m, mc, a.metal_ne, a.two_way);
+                                  xHeI, xHeII, ne, a.m, mc, a.metal_ne, a.two_way, &nsum);
         } else {
             it = solve_cell(a.k, a.yHe, a.rates[il], a.rates[a.nleaf + il], a.rates[2 * a.nleaf + il], nH, xHI, xHeI,
                             xHeII, ne);
         }
         ++solved;
         if (it > 200) ++caps;
+        passes += (unsigned long long)min(it, 200);
+        sums += (unsigned long long)nsum;
         const double w = a.relax;
         const double xn = (1.0 - w) * x0 + w * xHI;
         const double h1n = (1.0 - w) * h10 + w * xHeI;
@@ -243,10 +246,15 @@ __global__ void __launch_bounds__(kBThreads) k_balance(const BalArgs a) {
     for (int o = 16; o > 0; o >>= 1) {
         solved += __shfl_down_sync(0xffffffffu, solved, o);
         caps += __shfl_down_sync(0xffffffffu, caps, o);
+        passes += __shfl_down_sync(0xffffffffu, passes, o);
+        sums += __shfl_down_sync(0xffffffffu, sums, o);
     }
     if ((t & 31) == 0) {
         if (solved) atomicAdd(a.counters + 0, solved);
         if (caps) atomicAdd(a.counters + 1, caps);
+        if (passes) atomicAdd(a.counters + 2, passes);
+        if (sums) atomicAdd(a.counters + 3, sums);
+        if (solved) atomicAdd(a.counters + 4, solved);
     }
 }
 
@@ -388,14 +396,14 @@ __device__ __noinline__ MetalThermalTerms metal_thermal(const ThermalDev& td, co
 // net_rate (thermal_mod.f90:38-115).  With metals the (leaf, T) cache mc is
 // prepared here at T and left for the caller.
 __device__ double net_rate(const ThArgs& a, long long il, double T, double nH, double& xHI, double& xHeI,
-                           double& xHeII, double& ne, int* passes, MetalCache& mc) {
+                           double& xHeII, double& ne, int* passes, MetalCache& mc, int* nsum) {
     const BalArgs& b = a.b;
     const long long n = b.nleaf;
     const Coef k = coef_at_call(b.rs, b.caseA, T);
     if (b.m.ntr > 0) {
         metal_prepare(b.m, il, T, mc);
         *passes += solve_cell_metal(k, b.yHe, b.rates[il], b.rates[n + il], b.rates[2 * n + il], nH, xHI, xHeI, xHeII,
-                                    ne, b.m, mc, b.metal_ne, b.two_way);
+                                    ne, b.m, mc, b.metal_ne, b.two_way, nsum);
     } else {
         *passes += solve_cell(k, b.yHe, b.rates[il], b.rates[n + il], b.rates[2 * n + il], nH, xHI, xHeI, xHeII, ne);
     }
@@ -418,7 +426,7 @@ __global__ void __launch_bounds__(kBThreads) k_thermal(const ThArgs a) {
     __shared__ double sh[6][kBThreads];
     const BalArgs& b = a.b;
     double mdx = 0.0, mdt = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0, s4 = 0.0;
-    unsigned long long solved = 0, caps = 0;
+    unsigned long long solved = 0, caps = 0, tpass = 0, tsums = 0, nevals = 0;
     for (long long il = (long long)blockIdx.x * blockDim.x + threadIdx.x; il < b.nleaf;
          il += (long long)gridDim.x * blockDim.x) {
         const double nH = b.nH[il];
@@ -429,11 +437,11 @@ __global__ void __launch_bounds__(kBThreads) k_thermal(const ThArgs a) {
             continue;
         }
         double xHI = x0, xHeI = h10, xHeII = h20, ne = 0.0;
-        int passes = 0;
+        int passes = 0, nsum = 0, nev = 2;
         double tlo = a.te_min, thi = a.te_max, te;
         MetalCache mc;
-        const double net_lo = net_rate(a, il, tlo, nH, xHI, xHeI, xHeII, ne, &passes, mc);
-        const double net_hi = net_rate(a, il, thi, nH, xHI, xHeI, xHeII, ne, &passes, mc);
+        const double net_lo = net_rate(a, il, tlo, nH, xHI, xHeI, xHeII, ne, &passes, mc, &nsum);
+        const double net_hi = net_rate(a, il, thi, nH, xHI, xHeI, xHeII, ne, &passes, mc, &nsum);
         if (net_lo <= 0.0) {
             te = tlo;
         } else if (net_hi >= 0.0) {
@@ -441,16 +449,20 @@ __global__ void __launch_bounds__(kBThreads) k_thermal(const ThArgs a) {
         } else {
             for (int it = 1; it <= 60; ++it) {
                 const double tmid = sqrt(tlo * thi);
-                const double nm = net_rate(a, il, tmid, nH, xHI, xHeI, xHeII, ne, &passes, mc);
+                const double nm = net_rate(a, il, tmid, nH, xHI, xHeI, xHeII, ne, &passes, mc, &nsum);
+                ++nev;
                 if (nm > 0.0) tlo = tmid; else thi = tmid;
                 if (thi / tlo - 1.0 < 1.0e-5) break;
             }
             te = sqrt(tlo * thi);
         }
         int last = 0;
-        net_rate(a, il, te, nH, xHI, xHeI, xHeII, ne, &last, mc);
+        net_rate(a, il, te, nH, xHI, xHeI, xHeII, ne, &last, mc, &nsum);
         ++solved;
         if (last > 200) ++caps;
+        tpass += (unsigned long long)(passes + last);
+        tsums += (unsigned long long)nsum;
+        nevals += (unsigned long long)(nev + 1);
         const double w = b.relax;
         const double xn = (1.0 - w) * x0 + w * xHI;
         const double h1n = (1.0 - w) * h10 + w * xHeI;
@@ -494,10 +506,16 @@ __global__ void __launch_bounds__(kBThreads) k_thermal(const ThArgs a) {
     for (int o = 16; o > 0; o >>= 1) {
         solved += __shfl_down_sync(0xffffffffu, solved, o);
         caps += __shfl_down_sync(0xffffffffu, caps, o);
+        tpass += __shfl_down_sync(0xffffffffu, tpass, o);
+        tsums += __shfl_down_sync(0xffffffffu, tsums, o);
+        nevals += __shfl_down_sync(0xffffffffu, nevals, o);
     }
     if ((t & 31) == 0) {
         if (solved) atomicAdd(b.counters + 0, solved);
         if (caps) atomicAdd(b.counters + 1, caps);
+        if (tpass) atomicAdd(b.counters + 2, tpass);
+        if (tsums) atomicAdd(b.counters + 3, tsums);
+        if (nevals) atomicAdd(b.counters + 4, nevals);
     }
 }
 

@@ -155,8 +155,9 @@ static __device__ __noinline__ void metal_sums(const MetalDev& m, const MetalCac
 // position for x_HI on [0, 1] with the charge-exchange terms re-evaluated at
 // every trial x.
 static __device__ __noinline__ double hydrogen_neutral_fraction(const MetalDev& m, const MetalCache& c, double nH, double ne,
-                                                         double A, double B) {
+                                                         double A, double B, int* nsum) {
     double nem, rin, rout;
+    *nsum += 2;
     double xa = 0.0;
     metal_sums(m, c, nH, ne, 0.0, nH, nem, rin, rout);
     double Ra = -(A + rin);
@@ -170,6 +171,7 @@ static __device__ __noinline__ double hydrogen_neutral_fraction(const MetalDev& 
         x = xb - Rb * (xb - xa) / (Rb - Ra);
         x = fmin(fmax(x, fmin(xa, xb)), fmax(xa, xb));
         metal_sums(m, c, nH, ne, nH * x, nH * (1.0 - x), nem, rin, rout);
+        ++*nsum;
         const double Rx = x * (B + rin + rout) - (A + rin);
         if (fabs(Rx) <= 1.0e-15 * scale) break;
         if (fabs(xb - xa) <= 1.0e-15) break;

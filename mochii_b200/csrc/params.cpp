@@ -133,6 +133,7 @@ extern "C" int mochii_params_default(mochii_params* p) {
     p->dust_law = 0;
     p->DGR = 1.0e-2; p->cext_dust = 1.6059e-21;
     p->precision = MOCHII_PREC_FP64;
+    p->metal_moments = 1;
     return MOCHII_OK;
 }
 
@@ -269,6 +270,12 @@ int set_key(mochii_params* p, std::string key, const std::vector<std::string>& v
     if (key == "ion_dust_kext") { copy_str(p->ion_dust_kext, sizeof(p->ion_dust_kext), unquote(v)); return 0; }
     if (key == "data_dir") { copy_str(p->data_dir, sizeof(p->data_dir), unquote(v)); return 0; }
     if (key == "atomic_dir") { copy_str(p->atomic_dir, sizeof(p->atomic_dir), unquote(v)); return 0; }
+    if (key == "metal_tally") {
+        const std::string s = lower(unquote(v));
+        if (s != "moments" && s != "exact") return bad("must be 'moments' or 'exact'");
+        p->metal_moments = s == "moments";
+        return 0;
+    }
     if (key == "precision") {
         const std::string s = lower(unquote(v));
         if (s != "fp64" && s != "fp32") return bad("must be 'fp64' or 'fp32'");

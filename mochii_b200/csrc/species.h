@@ -46,7 +46,22 @@ struct SpeciesHost {
     std::vector<double> lamref, Ssup; // n-level tables: ntab x kNlNT, ntab x kNlNT x kNlNNE
     int ntab = 0;
     std::vector<double> thresholds() const;   // element order (main.f90:65-82)
+    // energy-moment tally (metal_tally = 'moments'): bin edges and the
+    // Chebyshev coefficients of sigma_k/E and sigma_k (1 - E_th,k/E) per bin
+    std::vector<double> medge, mcoef;
+    std::vector<int> mb0;             // threshold order: first bin where the transition is active
 };
+
+constexpr int kMomDeg = 6;            // Chebyshev moments per bin (degree 5)
+constexpr double kMomTol = 2.0e-7;    // interpolation error bound per bin, relative to the bin's peak
+
+// Moment bins over [emin, emax]: the H/He and metal thresholds inside are
+// edges, each sub-range is split log-uniformly with ln(hi/lo) <= 0.04 per
+// bin, and in every bin both rate integrands of every active transition are
+// interpolated at the kMomDeg Chebyshev nodes (1e-18 cm^2 units).  A bin
+// whose interpolant misses any integrand by more than kMomTol of that
+// integrand's peak over the bin (checked at 33 points) is halved in ln E.
+void species_moment_tables(SpeciesHost& s, double emin, double emax);
 
 // Device copy: registry tables plus the per-leaf metal arrays.
 struct MetalDev {
@@ -63,6 +78,11 @@ struct MetalDev {
     double* eheat = nullptr;           // nleaf x ntr, element order [erg/s]
     void* opac = nullptr;              // nleaf x ntrp (R), threshold order: n_H A_el f_it d2cm 1e-18
     void* raw = nullptr;               // nleaf x ntrp x 2 tallies (FP64 or FP32 pairs), threshold order
+    int nmb = 0;                       // moment bins (0: exact tallies)
+    const double* medge = nullptr;     // nmb + 1
+    const double* mcoef = nullptr;     // (nmb*kMomDeg) x ntrp x 2
+    const int* mb0 = nullptr;          // ntr, threshold order
+    void* mom = nullptr;               // nleaf x nmb x kMomDeg tallies
 };
 
 bool species_build(const mochii_params& p, SpeciesHost& s, std::string* err);

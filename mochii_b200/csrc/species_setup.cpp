@@ -5,7 +5,10 @@
 // (nlevel_cooling_add, nlevel_cooling_mod.f90:104-163).
 #include "species.h"
 
+#include "metals.cuh"
+
 #include <algorithm>
+#include <cmath>
 #include <fstream>
 #include <sstream>
 #include <thread>
@@ -237,6 +240,102 @@ bool species_build(const mochii_params& p, SpeciesHost& s, std::string* err) {
         std::copy(ss[t].begin(), ss[t].end(), s.Ssup.begin() + (size_t)t * kNlNT * kNlNNE);
     }
     return true;
+}
+
+void species_moment_tables(SpeciesHost& s, double emin, double emax) {
+    const int ntr = (int)s.tr.size();
+    const int ntrp = (ntr + 3) / 4 * 4;
+    const double pi = 3.141592653589793;
+    auto integrand = [&](int k, int q, double E) {
+        const double* c = &s.photo[8 * k];
+        const double sk = (s.form[k] == 2 ? sigma_vy95(E, c[0], c[1], c[2], c[3], c[4], c[5], c[6])
+                                          : sigma_vfky96(E, c[0], c[1], c[2], c[3], c[4], c[5], c[6], c[7])) * 1.0e18;
+        return q == 0 ? sk / E : sk * std::max(1.0 - s.eth_flat[k] / E, 0.0);
+    };
+    double node[kMomDeg];
+    for (int j = 0; j < kMomDeg; ++j) node[j] = std::cos(pi * (j + 0.5) / kMomDeg);
+    // Chebyshev interpolation coefficients of integrand (k, q) on [lo, hi]
+    auto coefs = [&](int k, int q, double lo, double hi, double* a) {
+        const double mid = 0.5 * (lo + hi), half = 0.5 * (hi - lo);
+        double f[kMomDeg];
+        for (int j = 0; j < kMomDeg; ++j) f[j] = integrand(k, q, mid + half * node[j]);
+        for (int m = 0; m < kMomDeg; ++m) {
+            double v = 0.0;
+            for (int j = 0; j < kMomDeg; ++j) v += f[j] * std::cos(m * std::acos(node[j]));
+            a[m] = v * (m == 0 ? 1.0 : 2.0) / kMomDeg;
+        }
+    };
+    auto bin_error = [&](double lo, double hi) {
+        double worst = 0.0;
+        const double mid = 0.5 * (lo + hi), half = 0.5 * (hi - lo);
+        for (int k = 0; k < ntr; ++k) {
+            if (s.eth_flat[k] > lo) continue;
+            for (int q = 0; q < 2; ++q) {
+                double a[kMomDeg], peak = 0.0, err = 0.0;
+                coefs(k, q, lo, hi, a);
+                for (int i = 0; i <= 32; ++i) {
+                    const double t = -1.0 + 2.0 * i / 32.0;
+                    const double ex = integrand(k, q, mid + half * t);
+                    double tm1 = 1.0, tm = t, ap = a[0] + a[1] * t;
+                    for (int m = 2; m < kMomDeg; ++m) {
+                        const double tn = 2.0 * t * tm - tm1;
+                        ap += a[m] * tn;
+                        tm1 = tm;
+                        tm = tn;
+                    }
+                    peak = std::max(peak, std::fabs(ex));
+                    err = std::max(err, std::fabs(ap - ex));
+                }
+                if (peak > 0.0) worst = std::max(worst, err / peak);
+            }
+        }
+        return worst;
+    };
+    std::vector<double> bp{emin, emax};
+    for (double e : {13.598, 24.587, 54.416}) if (e > emin && e < emax) bp.push_back(e);
+    for (double e : s.eth_flat) if (e > emin && e < emax) bp.push_back(e);
+    std::sort(bp.begin(), bp.end());
+    bp.erase(std::unique(bp.begin(), bp.end()), bp.end());
+    std::vector<std::pair<double, double>> todo;
+    const double dl = 0.04;
+    for (size_t i = 0; i + 1 < bp.size(); ++i) {
+        const double lo = bp[i], hi = bp[i + 1];
+        const int n = std::max(1, (int)std::ceil(std::log(hi / lo) / dl - 1e-9));
+        for (int j = 0; j < n; ++j)
+            todo.push_back({j == 0 ? lo : lo * std::exp(std::log(hi / lo) * (double)j / n),
+                            j == n - 1 ? hi : lo * std::exp(std::log(hi / lo) * (double)(j + 1) / n)});
+    }
+    s.medge.clear();
+    for (auto& seg : todo) {   // depth-first halving in ln E, in ascending order
+        std::vector<std::pair<std::pair<double, double>, int>> st{{seg, 0}};
+        while (!st.empty()) {
+            const auto cur = st.back();
+            st.pop_back();
+            const double lo = cur.first.first, hi = cur.first.second;
+            if (cur.second < 16 && bin_error(lo, hi) > kMomTol) {
+                const double m = std::sqrt(lo * hi);
+                st.push_back({{m, hi}, cur.second + 1});
+                st.push_back({{lo, m}, cur.second + 1});
+            } else {
+                s.medge.push_back(lo);
+            }
+        }
+    }
+    s.medge.push_back(bp.back());
+    const int nmb = (int)s.medge.size() - 1;
+    s.mcoef.assign((size_t)nmb * kMomDeg * ntrp * 2, 0.0);
+    s.mb0.assign(ntr, nmb);
+    for (int k = 0; k < ntr; ++k)
+        for (int b = 0; b < nmb; ++b) {
+            const double lo = s.medge[b], hi = s.medge[b + 1];
+            if (s.eth_flat[k] > lo) continue;   // thresholds are edges: inactive over the whole bin
+            s.mb0[k] = std::min(s.mb0[k], b);
+            for (int q = 0; q < 2; ++q) {
+                double a[kMomDeg];
+                coefs(k, q, lo, hi, a);
+                for (int m = 0; m < kMomDeg; ++m) s.mcoef[(((size_t)b * kMomDeg + m) * ntrp + k) * 2 + q] = a[m];
+            }
+        }
 }
 
 }  // namespace mochii

@@ -245,21 +245,25 @@ struct Stepper {
 // scoring: slot 0 is scored now, slots 1..LA have their column loads in
 // flight (LA = 0 disables the look-ahead).
 //
-// METAL adds the trace-metal terms: the packet's active-prefix cross
-// sections sigma_k and heating coefficients sigma_k (1 - E_th,k/E) sit in
-// dynamic shared memory ([k][thread], 2 x ntrp x 128 of R); per segment the
-// leaf's opacity weights add sum_k w_k sigma_k to the absorption
-// (species_cached_opacity, species_mod.f90:291-303) and two tallies per
-// active transition are scored (species_rate_path_score, :329-343).
-template <typename R, int NABS, int LA, bool METAL>
+// MET adds the trace-metal terms.  The packet's active-prefix cross
+// sections sigma_k sit in dynamic shared memory ([k][thread], ntrp x 128 of
+// R); per segment the leaf's opacity weights add sum_k w_k sigma_k to the
+// absorption (species_cached_opacity, species_mod.f90:291-303).  The path
+// estimators of species_rate_path_score (:329-343) are either scored
+// directly, two tallies per active transition (MET = 1, with the heating
+// coefficients sigma_k (1 - E_th,k/E) in a second shared array), or as the
+// kMomDeg Chebyshev moments of the packet energy in its moment bin (MET = 2),
+// which the rate kernel contracts with the tabulated integrands.
+template <typename R, int NABS, int LA, int MET>
 __global__ void __launch_bounds__(128) k_walk_edge(const PassArgs a, const PacketRecords rec, long long n,
                                                    int accumulate) {
     typedef typename Acc<R>::T T;
     constexpr int NT = NABS == 1 ? 2 : 6;
+    constexpr bool METAL = MET > 0;
     __shared__ double sh[128];
     extern __shared__ __align__(16) unsigned char dsm[];
-    R* const msg = reinterpret_cast<R*>(dsm);                 // sigma_k        [k][thread]
-    R* const mhc = msg + (METAL ? a.m.ntrp * blockDim.x : 0);  // sigma_k h_k    [k][thread]
+    R* const msg = reinterpret_cast<R*>(dsm);                      // sigma_k      [k][thread]
+    R* const mhc = msg + (MET == 1 ? a.m.ntrp * blockDim.x : 0);    // sigma_k h_k  [k][thread]
     const int tb = blockDim.x, tx = threadIdx.x;
     double emitted = 0.0, absorbed = 0.0, escaped = 0.0;
     unsigned long long nseg = 0, kills = 0;
@@ -285,8 +289,8 @@ __global__ void __launch_bounds__(128) k_walk_edge(const PassArgs a, const Packe
         R cf[NT];
 #pragma unroll
         for (int k = 0; k < NT; ++k) cf[k] = cfp[k * c + i];
-        int nm = 0;
-        R invE = (R)0;
+        int nm = 0, mb = 0;
+        R invE = (R)0, phi[kMomDeg];
         if constexpr (METAL) {
             const double E = rec.E[i];
             nm = metal_nactive(a.m, E);
@@ -295,7 +299,27 @@ __global__ void __launch_bounds__(128) k_walk_edge(const PassArgs a, const Packe
             for (int k = 0; k < nm; ++k) {
                 const R sk = ms[k * c + i];
                 msg[k * tb + tx] = sk;
-                mhc[k * tb + tx] = (R)((double)sk * fmax(1.0 - __ldg(a.m.eth + k) / E, 0.0));
+                if constexpr (MET == 1) mhc[k * tb + tx] = (R)((double)sk * fmax(1.0 - __ldg(a.m.eth + k) / E, 0.0));
+            }
+            if constexpr (MET == 2) {   // moment bin and the Chebyshev values T_0..T_5 of E in it
+                int lo = 0, hi = a.m.nmb - 1;
+                while (lo < hi) {
+                    const int mid = (lo + hi + 1) >> 1;
+                    if (__ldg(a.m.medge + mid) <= E) lo = mid; else hi = mid - 1;
+                }
+                mb = lo;
+                const double e0 = __ldg(a.m.medge + mb), e1 = __ldg(a.m.medge + mb + 1);
+                const double t = fmin(fmax((2.0 * E - (e0 + e1)) / (e1 - e0), -1.0), 1.0);
+                double tm1 = 1.0, tm = t;
+                phi[0] = (R)1;
+                phi[1] = (R)t;
+#pragma unroll
+                for (int q = 2; q < kMomDeg; ++q) {
+                    const double tn = 2.0 * t * tm - tm1;
+                    phi[q] = (R)tn;
+                    tm1 = tm;
+                    tm = tn;
+                }
             }
         }
         // ring of LA+1 cells: il, segment, columns, and whether a next cell exists
@@ -342,13 +366,17 @@ __global__ void __launch_bounds__(128) k_walk_edge(const PassArgs a, const Packe
 #pragma unroll
                 for (int k = 0; k < NT; ++k) tally_add(tl + k, w * cf[k]);
                 tally_add(jt + (long long)il[0] * a.nnu + inu, w);
-                if constexpr (METAL) {
+                if constexpr (MET == 1) {
                     T* rw = static_cast<T*>(a.m.raw) + (long long)il[0] * a.m.ntrp * 2;
                     const R wi = w * invE;
                     for (int k = 0; k < nm; ++k) {
                         tally_add(rw + 2 * k, wi * msg[k * tb + tx]);
                         tally_add(rw + 2 * k + 1, w * mhc[k * tb + tx]);
                     }
+                } else if constexpr (MET == 2) {
+                    T* mt = static_cast<T*>(a.m.mom) + ((long long)il[0] * a.m.nmb + mb) * kMomDeg;
+#pragma unroll
+                    for (int q = 0; q < kMomDeg; ++q) tally_add(mt + q, w * phi[q]);
                 }
             }
             tau = tau + (double)ks;
@@ -442,6 +470,36 @@ __global__ void k_metal_rates(const MetalDev m, long long nleaf, double cg, doub
         const T* r = raw + (il * m.ntrp + k) * 2;
         m.egam[q] = tval<T>(r[0]) * cg;
         m.eheat[q] = tval<T>(r[1]) * ch;
+    }
+}
+
+// The same from the energy moments: raw_{k,q}(leaf) = sum over the moment
+// bins b where transition k is active and the Chebyshev orders m of
+// mom(leaf, b, m) * coef(b, m, k, q).  One warp per leaf: the leaf's moments
+// are read once and broadcast, lanes run over the transitions.
+template <typename T>
+__global__ void k_metal_rates_mom(const MetalDev m, long long nleaf, double cg, double ch) {
+    const T* mom = static_cast<const T*>(m.mom);
+    const int lane = threadIdx.x & 31;
+    const long long warps = (long long)gridDim.x * (blockDim.x >> 5);
+    for (long long il = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); il < nleaf; il += warps) {
+        const T* ml = mom + il * m.nmb * kMomDeg;
+        for (int j = lane; j < m.ntr; j += 32) {
+            const int k = m.tr[j].flat;
+            double s0 = 0.0, s1 = 0.0;
+            for (int b = m.mb0[k]; b < m.nmb; ++b) {
+#pragma unroll
+                for (int q = 0; q < kMomDeg; ++q) {
+                    const double v = tval<T>(ml[b * kMomDeg + q]);
+                    const double2 cf = __ldg(reinterpret_cast<const double2*>(m.mcoef) +
+                                             ((long long)(b * kMomDeg + q) * m.ntrp + k));
+                    s0 = s0 + v * cf.x;
+                    s1 = s1 + v * cf.y;
+                }
+            }
+            m.egam[il * m.ntr + j] = s0 * cg;
+            m.eheat[il * m.ntr + j] = s1 * ch;
+        }
     }
 }
 
@@ -553,14 +611,16 @@ int grid_blocks(long long work, int threads, int cap) {
 
 }  // namespace
 
-// Dynamic shared memory of the metal walk: sigma_k and sigma_k h_k per thread.
+// Dynamic shared memory of the metal walk: sigma_k (and sigma_k h_k for the
+// exact tallies) per thread.
 size_t metal_smem(const mochii_ctx* c) {
-    return c->metal.ntr > 0 ? 2 * (size_t)c->metal.ntrp * 128 * (c->fp32 ? 4 : 8) : 0;
+    if (c->metal.ntr == 0) return 0;
+    return (c->metal.nmb > 0 ? 1 : 2) * (size_t)c->metal.ntrp * 128 * (c->fp32 ? 4 : 8);
 }
 
-template <typename R, int NABS, int LA, bool METAL>
+template <typename R, int NABS, int LA, int MET>
 int walk_occupancy(size_t smem) {
-    auto k = k_walk_edge<R, NABS, LA, METAL>;
+    auto k = k_walk_edge<R, NABS, LA, MET>;
     if (smem > 48 * 1024) cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     int nb = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k, 128, smem) != cudaSuccess) {
@@ -576,8 +636,8 @@ int transport_blocks(const mochii_ctx* c) {
     int per_sm = c->tune.walk_blocks_per_sm > 0 ? c->tune.walk_blocks_per_sm : 8;
     if (c->metal.ntr > 0) {   // resident blocks only: each holds its packets' sigma_k in shared memory
         const size_t smem = metal_smem(c);
-        const int occ = c->fp32 ? (c->nabs == 1 ? walk_occupancy<float, 1, 2, true>(smem) : walk_occupancy<float, 4, 2, true>(smem))
-                                : (c->nabs == 1 ? walk_occupancy<double, 1, 2, true>(smem) : walk_occupancy<double, 4, 2, true>(smem));
+        const int occ = c->fp32 ? (c->nabs == 1 ? walk_occupancy<float, 1, 2, 1>(smem) : walk_occupancy<float, 4, 2, 1>(smem))
+                                : (c->nabs == 1 ? walk_occupancy<double, 1, 2, 1>(smem) : walk_occupancy<double, 4, 2, 1>(smem));
         per_sm = per_sm < occ ? per_sm : occ;
     }
     return grid_blocks(c->par.nphotons, 128, sms * per_sm);
@@ -585,27 +645,31 @@ int transport_blocks(const mochii_ctx* c) {
 
 // Walk-kernel variants: look-ahead depth 0..2 (the autotuned choice is
 // c->tune.lookahead); 128-thread blocks.
-template <typename R, int NABS, bool METAL>
+template <typename R, int NABS, int MET>
 cudaError_t walk_la(mochii_ctx* c, const PassArgs& a, const PacketRecords& r, long long n, int acc, int blocks) {
-    const size_t smem = METAL ? metal_smem(c) : 0;
-    if (METAL && smem > 48 * 1024) {
-        cudaFuncSetAttribute(k_walk_edge<R, NABS, 0, METAL>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        cudaFuncSetAttribute(k_walk_edge<R, NABS, 1, METAL>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        cudaFuncSetAttribute(k_walk_edge<R, NABS, 2, METAL>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    const size_t smem = MET ? metal_smem(c) : 0;
+    if (MET && smem > 48 * 1024) {
+        cudaFuncSetAttribute(k_walk_edge<R, NABS, 0, MET>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        cudaFuncSetAttribute(k_walk_edge<R, NABS, 1, MET>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        cudaFuncSetAttribute(k_walk_edge<R, NABS, 2, MET>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     }
     switch (c->tune.lookahead) {
-        case 0: k_walk_edge<R, NABS, 0, METAL><<<blocks, 128, smem, c->stream>>>(a, r, n, acc); break;
-        case 1: k_walk_edge<R, NABS, 1, METAL><<<blocks, 128, smem, c->stream>>>(a, r, n, acc); break;
-        default: k_walk_edge<R, NABS, 2, METAL><<<blocks, 128, smem, c->stream>>>(a, r, n, acc); break;
+        case 0: k_walk_edge<R, NABS, 0, MET><<<blocks, 128, smem, c->stream>>>(a, r, n, acc); break;
+        case 1: k_walk_edge<R, NABS, 1, MET><<<blocks, 128, smem, c->stream>>>(a, r, n, acc); break;
+        default: k_walk_edge<R, NABS, 2, MET><<<blocks, 128, smem, c->stream>>>(a, r, n, acc); break;
     }
     return cudaGetLastError();
 }
 
+template <typename R, int MET>
+cudaError_t walk_abs(mochii_ctx* c, const PassArgs& a, const PacketRecords& r, long long n, int acc, int blocks) {
+    return c->nabs == 1 ? walk_la<R, 1, MET>(c, a, r, n, acc, blocks) : walk_la<R, 4, MET>(c, a, r, n, acc, blocks);
+}
+
 template <typename R>
 cudaError_t walk_prec(mochii_ctx* c, const PassArgs& a, const PacketRecords& r, long long n, int acc, int blocks) {
-    if (c->metal.ntr > 0)
-        return c->nabs == 1 ? walk_la<R, 1, true>(c, a, r, n, acc, blocks) : walk_la<R, 4, true>(c, a, r, n, acc, blocks);
-    return c->nabs == 1 ? walk_la<R, 1, false>(c, a, r, n, acc, blocks) : walk_la<R, 4, false>(c, a, r, n, acc, blocks);
+    if (c->metal.ntr == 0) return walk_abs<R, 0>(c, a, r, n, acc, blocks);
+    return c->metal.nmb > 0 ? walk_abs<R, 2>(c, a, r, n, acc, blocks) : walk_abs<R, 1>(c, a, r, n, acc, blocks);
 }
 
 cudaError_t launch_walk_variant(mochii_ctx* c, const PassArgs& a, const PacketRecords& r, long long n, int acc,
@@ -677,7 +741,11 @@ cudaError_t launch_rates(mochii_ctx* c) {
         if (c->ntally == 2) k_rates<double, 2><<<blocks, 256, 0, c->stream>>>((const double*)c->tally, c->rates, n, cg, ch);
         else k_rates<double, 6><<<blocks, 256, 0, c->stream>>>((const double*)c->tally, c->rates, n, cg, ch);
     }
-    if (c->metal.ntr > 0) {
+    if (c->metal.ntr > 0 && c->metal.nmb > 0) {
+        const int mb = grid_blocks(n * 32, 256, 148 * 32);
+        if (c->fp32) k_metal_rates_mom<float2><<<mb, 256, 0, c->stream>>>(c->metal, n, cg, ch);
+        else k_metal_rates_mom<double><<<mb, 256, 0, c->stream>>>(c->metal, n, cg, ch);
+    } else if (c->metal.ntr > 0) {
         const int mb = grid_blocks(n * c->metal.ntr, 256, 148 * 16);
         if (c->fp32) k_metal_rates<float2><<<mb, 256, 0, c->stream>>>(c->metal, n, cg, ch);
         else k_metal_rates<double><<<mb, 256, 0, c->stream>>>(c->metal, n, cg, ch);

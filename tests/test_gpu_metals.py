@@ -2,8 +2,11 @@
 against the CPU oracle, through the C ABI.
 
 Bars: the band edges with the metal thresholds equal the oracle's; in FP64
-the metal Gamma and photoheating per (leaf, transition) equal the oracle's
-to 1e-9 relative (atomic ordering and last-ulp differences of pow/exp);
+with the per-transition tallies the metal Gamma and photoheating per (leaf,
+transition) equal the oracle's to 1e-9 relative (atomic ordering and
+last-ulp differences of pow/exp); the energy-moment tallies (degree-5
+Chebyshev interpolation per threshold-aligned bin, 2e-7 of the bin's peak)
+within 2e-6 of the per-transition ones on the same packets;
 the H/He rates with the metal opacity in the packet absorption to 1e-9;
 after the balance (fixed T_e, metal electrons, two-way charge exchange) the
 x_HII within 1e-3 and the metal stage fractions within 1e-6 absolute of the
@@ -19,9 +22,10 @@ from mochii_b200 import Nebula, configs, parse_namelist
 pytestmark = pytest.mark.gpu
 
 
-def metal_nl(n=16, nphot=40000, precision="fp64", solve_te=False, diffuse=False, rs_factor=1.3):
-    return configs.hii_metals(nphotons=nphot, niter=3, n=n, precision=precision, rs_factor=rs_factor,
-                              diffuse=diffuse, solve_te=solve_te)
+def metal_nl(n=16, nphot=40000, precision="fp64", solve_te=False, diffuse=False, rs_factor=1.3, tally="exact"):
+    nl = configs.hii_metals(nphotons=nphot, niter=3, n=n, precision=precision, rs_factor=rs_factor,
+                            diffuse=diffuse, solve_te=solve_te)
+    return nl.replace("/\n", f" par%metal_tally = '{tally}'\n/\n")
 
 
 def partial_state(n, L):
@@ -133,9 +137,27 @@ def test_metal_thermal_matches_oracle(orc):
     neb.close()
 
 
-def test_fp32_metal_pass_within_tolerance(orc):
+def test_moment_tallies_match_exact_tallies():
     n = 16
-    nl = metal_nl(n=n, precision="fp32")
+    L = parse_namelist(metal_nl(n=n)).xmax
+    out = {}
+    for tally in ("exact", "moments"):
+        neb = Nebula(parse_namelist(metal_nl(n=n, tally=tally)))
+        for k, v in partial_state(n, L).items():
+            neb.set(k, v)
+        neb.gas_opacity_fill()
+        neb.ionizing_field_and_rates()
+        out[tally] = (neb.get("gamma_metal"), neb.get("heat_metal"), neb.get("gamma_HI"))
+        neb.close()
+    for i in range(3):
+        ok, worst = close_rel(out["moments"][i], out["exact"][i], 2e-6)
+        assert ok, (i, worst)
+
+
+@pytest.mark.parametrize("tally", ["exact", "moments"])
+def test_fp32_metal_pass_within_tolerance(orc, tally):
+    n = 16
+    nl = metal_nl(n=n, precision="fp32", tally=tally)
     L = parse_namelist(nl).xmax
     neb, sim = pair(orc, nl, partial_state(n, L))
     st = neb.ionizing_field_and_rates()
