@@ -221,6 +221,16 @@ int orc_sim_metal_thermal(void* h, int il, double T, double nH, double ne, doubl
     out4[0] = m.cool; out4[1] = m.cool_H; out4[2] = m.freefree; out4[3] = m.heat;
     return 0;
 }
+// net_rate on leaf il at T from the leaf's current state: out = net, x_HI,
+// x_HeI, x_HeII, n_e after the cell solve at T.
+int orc_sim_net_rate(void* h, int il, double T, double* out5) {
+    auto* s = static_cast<Sim*>(h);
+    if (!s->th) return -1;
+    double xHI = s->st.xHI[il], xHeI = s->st.xHeI[il], xHeII = s->st.xHeII[il], ne = 0.0;
+    out5[0] = s->net_rate(il, T, s->par.case_ab == "A", xHI, xHeI, xHeII, ne);
+    out5[1] = xHI; out5[2] = xHeI; out5[3] = xHeII; out5[4] = ne;
+    return 0;
+}
 // Metal registry shape: transitions and stages in element order.
 int orc_sim_metal_ntr(void* h) {
     auto* s = static_cast<Sim*>(h);

