@@ -1,31 +1,43 @@
 #!/usr/bin/env python3
 """Benchmark: packets/s of one iteration of the transport + balance path.
 
-A step is one iteration of the reference driver loop (main.f90:128-185) on
-the Stromgren workload (stromgren64: 64^3 Cartesian grid, n_H = 100, 40 kK
-point source, Q(H) = 1e49 s^-1, 1e6 Owen-scrambled Sobol packets, case B,
-T_e = 1e4 K, FP64): the transport pass (launch, DDA walk, rate tallies,
-energy ledger, rate normalisation) followed by the per-leaf balance and the
-absorber-column refresh.  Before timing, the nebula is iterated (untimed,
-as input preparation) to a converged ionisation structure so every timed
-step walks the converged Stromgren sphere, as the bulk of a real run does.
+A step is one iteration of the reference driver loop (main.f90:128-185):
+the transport pass (Sobol launch, DDA walk, rate tallies, diffuse Milne
+packets, energy ledger, rate normalisation) followed by the per-leaf balance
+(thermal balance where the workload solves T_e) and the opacity refresh.
 
-  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+Workloads (--workload):
+  hii_metals128  (default) the H+He+metals H II region with the thermal
+                 balance: 128^3 grid, n_H = 100, He/H 0.1, eleven metals,
+                 45 kK blackbody with Q(H) = 5e49 s^-1, case A with explicit
+                 diffuse Milne packets, 1e7 stellar packets per pass, FP32
+                 segments with compensated FP32 tallies (metal rates from
+                 the energy-moment tallies).  Untimed preparation iterations
+                 bring the ionized start to a developed H II region first.
+  stromgren64    the pure-H Stromgren sphere: 64^3, 40 kK, Q(H) = 1e49,
+                 1e6 packets, case B, T_e = 1e4 K, FP64; prepared to the
+                 converged sphere.
 
-value     packets / device time of the K steps (CUDA events on the
-          library's stream), L2 flushed between steps (a 256 MiB write).
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--workload W] [--impl reference]
+
+value     packets transported (stellar + diffuse) / device time of the K
+          steps (CUDA events on the library's stream), L2 flushed between
+          steps (a 256 MiB write).
 e2e       the same metric through the C ABI with host buffers: each step
-          uploads the leaf ionisation state from pinned host memory and
-          reads back the new state and Gamma_HI, copies inside the timing.
-roofline  the transport kernel: algorithmic bytes (56 B per scored
-          segment: one FP64 absorber column read and three FP64 tally
-          read-modify-writes) per launch / its event-timed duration.
+          uploads the leaf state (x_HI, T_e) from pinned host memory and
+          reads back x_HI, T_e and Gamma_HI, copies inside the timing.
+roofline  the transport kernels: algorithmic bytes per scored segment
+          B_seg = 4 F_state + 16 F_tally (state words read, compensated
+          tally pairs read and written; FP64 words count 8 B) over their
+          event-timed duration; the metal state words are counted per
+          segment in the kernel (one per active transition).
 N > 1     one process per GPU, each an independent nebula (replicas: the
           packets of one nebula are not split across GPUs), value = sum.
 --impl reference
           the CPU restatement of the reference's path (the oracle port) on
-          every host thread, on a bounded packet sample of the same
-          workload per step.
+          every host thread: a bounded packet sample of the same workload
+          and the thermal solve on a sample of its leaves, scaled to the
+          step's packet and leaf counts.
 """
 import argparse
 import json
@@ -35,19 +47,60 @@ import subprocess
 import sys
 import time
 
+import numpy as np
+
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "packets/s on 1 B200 (transport + balance iteration)"
 UNIT = "packets/s"
-WORKLOAD = "stromgren64"
-NPHOT = 1_000_000
-GRID = 64
-BYTES_PER_SEGMENT = 56
-# DRAM bytes per scored segment of the transport kernel, from the ncu
-# capture summarised in profiles/transport_stromgren64.md (None until
-# captured).
-DRAM_BYTES_PER_SEGMENT = None
+
+
+# DRAM bytes per scored segment of the transport kernels, from the ncu
+# captures summarised in profiles/ (absent until captured).
+DRAM_BYTES_PER_SEGMENT = {}
+
+
+class Workload:
+    """A benchmark configuration: its namelist and how a step is run."""
+
+    def __init__(self, name):
+        from mochii_b200 import configs
+        self.name = name
+        if name == "hii_metals128":
+            self.grid, self.nphot, self.thermal, self.prep = 128, 10_000_000, True, 8
+            self.default_precision = "fp32"
+            self.make = lambda nphot, prec, seed: configs.hii_metals(nphotons=nphot, niter=20, n=128,
+                                                                      precision=prec, seed=seed)
+        elif name == "stromgren64":
+            self.grid, self.nphot, self.thermal, self.prep = 64, 1_000_000, False, 60
+            self.default_precision = "fp64"
+            self.make = lambda nphot, prec, seed: configs.stromgren64(nphotons=nphot, n=64, precision=prec, seed=seed)
+        else:
+            raise SystemExit(f"unknown workload {name}")
+
+    def balance(self, neb):
+        return neb.gas_thermal_update() if self.thermal else neb.gas_equilibrium_update()
+
+
+def bytes_per_segment(wl, precision):
+    """B_seg = 4 F_state + 16 F_tally without the per-segment metal words
+    (added from the kernel's count), state words 8 B in FP64."""
+    w = 8 if precision == "fp64" else 4
+    if wl.name == "stromgren64":
+        return w * 2 + 16 * 3          # n_H, x_HI; Gamma_HI, H_HI, jt_ion
+    return w * 4 + 16 * (7 + 6)        # n_H, x_HI, x_HeI, x_HeII; 6 H/He + jt_ion + 6 metal moments
+
+
+def prepare(neb, wl):
+    it = 0
+    for it in range(1, wl.prep + 1):
+        neb.ionizing_field_and_rates()
+        m = wl.balance(neb)
+        neb.gas_opacity_fill()
+        if not wl.thermal and m[0] < 1e-3:
+            break
+    return it
 
 
 def dist_env():
@@ -116,62 +169,90 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def oracle_baseline(nphot_sample, nthreads):
-    """The oracle port (FP64 CPU restatement, OpenMP) on a bounded sample:
-    one converged-state transport pass + balance of nphot_sample packets."""
-    from mochii_b200 import configs
+def cpu_threads(wl):
+    """Host threads for the CPU port: all cores, capped so the per-thread
+    tally copies (the reference's per-rank tallies) use at most half the
+    host memory."""
+    n = os.cpu_count() or 1
+    try:
+        mem = os.sysconf("SC_PAGE_SIZE") * os.sysconf("SC_PHYS_PAGES")
+    except (ValueError, OSError):
+        mem = 64 << 30
+    per = wl.grid ** 3 * 8 * (6 + 16 + (2 * 32 if wl.name == "hii_metals128" else 0))
+    return max(1, min(n, int(0.5 * mem // max(per, 1))))
+
+
+def cpu_reference(wl, state, nthreads, budget_s=20.0):
+    """The oracle port (FP64 CPU restatement, OpenMP) on a bounded sample of
+    one step: transport passes of `sample` packets on the given state and the
+    thermal (or ionisation) solve on every stride-th leaf, each scaled to the
+    step's packet / leaf count.  Returns (packets/s, description)."""
     from oracle import pyorc
-    nl = configs.stromgren64(nphotons=nphot_sample, n=GRID)
-    sim = pyorc.Sim(nl, nthreads=nthreads)
-    return sim
+    sample = int(os.environ.get("MOCHII_CPU_SAMPLE", "200000" if wl.grid <= 64 else "100000"))
+    sim = pyorc.Sim(wl.make(sample, "fp64", 12345), nthreads=nthreads)
+    for k, v in state.items():
+        sim.set(k, v)
+    # per-packet cost from passes of sample and 2 x sample packets (the
+    # per-pass tally reset and reduction is a fixed cost of a pass)
+    t_of = {}
+    for n in (sample, 2 * sample):
+        sim.set_nphotons(n)
+        t0 = time.perf_counter()
+        reps = 0
+        while True:
+            sim.transport_pass()
+            reps += 1
+            if time.perf_counter() - t0 > 0.25 * budget_s or reps >= 5:
+                break
+        t_of[n] = (time.perf_counter() - t0) / reps
+    t_pp = max(t_of[2 * sample] - t_of[sample], 1e-3 * t_of[sample]) / sample
+    t_fixed = max(t_of[sample] - sample * t_pp, 0.0)
+    t_pass = t_fixed + t_pp * wl.nphot
+    nleaf = wl.grid ** 3
+    if wl.thermal:
+        stride = int(os.environ.get("MOCHII_CPU_CELL_STRIDE", "256"))
+        t1 = time.perf_counter()
+        solved = sim.thermal_sample(stride)
+        t_cells = time.perf_counter() - t1
+        ngas = int(np.count_nonzero(state.get("nH", np.ones(nleaf)) > 0)) if "nH" in state else nleaf
+        t_bal = t_cells / max(solved, 1) * ngas
+        what = f"thermal solve of {solved} leaves (every {stride}th)"
+    else:
+        t1 = time.perf_counter()
+        sim.equilibrium_update()
+        t_bal = time.perf_counter() - t1
+        what = "ionisation solve of every leaf"
+    t_step = t_pass + t_bal
+    value = wl.nphot / t_step
+    desc = (f"transport passes of {sample} and {2 * sample} stellar packets (per-packet time scaled to "
+            f"{wl.nphot}, plus the per-pass fixed cost) + {what}, scaled to all leaves; stellar packets "
+            f"only; {nthreads} threads")
+    return value, desc, t_step
 
 
-def converged_state(neb, max_iter=60, tol=1e-3):
-    it = 0
-    for it in range(1, max_iter + 1):
-        neb.ionizing_field_and_rates()
-        dx, _ = neb.gas_equilibrium_update()
-        neb.gas_opacity_fill()
-        if dx < tol:
-            break
-    return it
-
-
-def run_reference(args):
+def run_reference(args, wl):
     rank, world, _ = dist_env()
     if rank != 0:
         return 0
-    import numpy as np
-    from oracle import pyorc
-    from mochii_b200 import configs
-    nthreads = os.cpu_count() or 1
-    sample = int(os.environ.get("MOCHII_REF_SAMPLE", "200000"))
-    nl = configs.stromgren64(nphotons=sample, n=GRID)
-    sim = pyorc.Sim(nl, nthreads=nthreads)
-    # the same converged structure as the GPU arm: a converged x_HI taken
-    # from a cheap oracle iteration at this sample size
-    for _ in range(40):
-        sim.transport_pass()
-        dx, _ = sim.equilibrium_update()
-        if dx < 2e-3:
-            break
-    for _ in range(args.warmup):
-        sim.transport_pass()
-        sim.equilibrium_update()
-    t0 = time.perf_counter()
-    for _ in range(args.steps):
-        sim.transport_pass()
-        sim.equilibrium_update()
-    dt = time.perf_counter() - t0
-    value = sample * args.steps / dt
+    nthreads = cpu_threads(wl)
+    # the workload's initial state (the GPU arm's preparation iterations would
+    # take the CPU port hours at this grid size)
+    state = {}
+    times = []
+    for k in range(args.warmup + args.steps):
+        _, desc, t_step = cpu_reference(wl, state, nthreads, budget_s=10.0)
+        if k >= args.warmup:
+            times.append(t_step)
+    dt = sum(times)
+    value = wl.nphot * args.steps / dt
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt / args.steps * 1e3,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic",
-            "config": {"workload": WORKLOAD, "grid": f"{GRID}^3", "packets_per_step": sample,
-                       "note": "bounded packet sample of the 1e6-packet step"},
-            "cpu_baseline": {"value": value, "unit": UNIT, "cores": nthreads, "kind": "port",
-                             "sample": f"{sample} packets per step, converged Stromgren state"},
+            "config": {"workload": wl.name, "grid": f"{wl.grid}^3", "packets_per_step": wl.nphot,
+                       "state": "the workload's initial state",
+                       "note": "each step a bounded sample of the workload's step, scaled"},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": nthreads, "kind": "port", "sample": desc},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
     return 0
@@ -183,43 +264,44 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="mochii_b200")
+    ap.add_argument("--workload", default="hii_metals128", choices=["hii_metals128", "stromgren64"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32"],
-                    help="transport arithmetic (the workload is defined in fp64)")
+    ap.add_argument("--precision", default=None, choices=["fp64", "fp32"],
+                    help="transport arithmetic (default: the workload's)")
     args = ap.parse_args()
+    wl = Workload(args.workload)
+    prec = args.precision or wl.default_precision
     if args.impl == "reference":
-        return run_reference(args)
+        return run_reference(args, wl)
 
     rank, world, local = dist_env()
-    import numpy as np
     import torch
     torch.cuda.set_device(local)
     dist = None
     if world > 1:
         import datetime
         import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
                                 device_id=torch.device("cuda", local))
-    from mochii_b200 import Nebula, configs, parse_namelist
+    from mochii_b200 import Nebula, parse_namelist
     from mochii_b200.build import build
     if rank == 0 or not os.path.exists(os.path.join(ROOT, "mochii_b200", "libmochii_gpu.so")):
         build()
     if dist is not None:
         dist.barrier()
 
-    par = parse_namelist(configs.stromgren64(nphotons=NPHOT, n=GRID, seed=12345 + rank, precision=args.precision))
+    par = parse_namelist(wl.make(wl.nphot, prec, 12345 + rank))
     neb = Nebula(par)
-    prep_iters = converged_state(neb)
-    tuning = neb.autotune(1 << 18)   # launch shape for this grid / precision / device
+    prep_iters = prepare(neb, wl)
+    tuning = neb.autotune(1 << 20)   # launch shape for this grid / precision / device
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
     for _ in range(args.warmup):
         neb.ionizing_field_and_rates()
-        neb.gas_equilibrium_update()
+        wl.balance(neb)
         neb.gas_opacity_fill()
 
     # ---- device-timed steps ---------------------------------------------
-    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
-    pass_ms, kern_ms, bal_ms, segs = [], [], [], []
+    pass_ms, kern_ms, bal_ms, segs, nact, npk = [], [], [], [], [], []
     if dist is not None:
         dist.barrier()
     torch.cuda.synchronize()
@@ -229,42 +311,54 @@ def main():
             flush.zero_()
             torch.cuda.synchronize()
             st = neb.ionizing_field_and_rates()
-            neb.gas_equilibrium_update()
+            wl.balance(neb)
             neb.gas_opacity_fill()
             pass_ms.append(st.pass_ms)
             kern_ms.append(st.kernel_ms)
             bal_ms.append(neb.last_metrics.kernel_ms)
             segs.append(st.direct_segments)
+            nact.append(st.metal_active)
+            npk.append(st.packets)
         torch.cuda.synchronize()
         t_wall = time.perf_counter() - t_wall
     # Each API call synchronises its own stream and reports the device time
     # (CUDA events on the library's stream) of its work: the pass (tally
-    # reset, transport, rate normalisation) and the balance (solve + column
+    # reset, transport, rate normalisation) and the balance (solve + opacity
     # refresh); a step is their sum.
-    step_ms = [a + b for a, b in zip(pass_ms, bal_ms)]
+    step_ms = [x + y for x, y in zip(pass_ms, bal_ms)]
     total_ms = sum(step_ms)
+    packets = sum(npk)
     if dist is not None:
         t = torch.tensor([total_ms], device="cuda", dtype=torch.float64)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         total_ms = float(t.item())
-    value = NPHOT * args.steps * world / (total_ms * 1e-3)
+        p = torch.tensor([float(packets)], device="cuda", dtype=torch.float64)
+        dist.all_reduce(p, op=dist.ReduceOp.SUM)
+        packets = int(p.item())
+    value = packets / (total_ms * 1e-3)
 
     # ---- end-to-end through the C ABI with host buffers --------------------
     nleaf = neb.nleaf
     x_host = torch.from_numpy(neb.get("x_HI")).pin_memory()
+    t_host = torch.from_numpy(neb.get("T_e")).pin_memory()
     x_out = torch.empty(nleaf, dtype=torch.float64).pin_memory()
+    t_out = torch.empty(nleaf, dtype=torch.float64).pin_memory()
     g_out = torch.empty(nleaf, dtype=torch.float64).pin_memory()
     lib, ctx = neb.lib, neb.ctx
     if dist is not None:
         dist.barrier()
     torch.cuda.synchronize()
+    e_packets = 0
     e0 = time.perf_counter()
     for k in range(args.steps):
         rc = lib.mochii_set_field(ctx, b"x_HI", x_host.data_ptr(), nleaf)
+        rc |= lib.mochii_set_field(ctx, b"T_e", t_host.data_ptr(), nleaf)
         rc |= lib.mochii_opacity_fill(ctx)
-        neb.ionizing_field_and_rates()
-        neb.gas_equilibrium_update()
+        st = neb.ionizing_field_and_rates()
+        e_packets += st.packets
+        wl.balance(neb)
         rc |= lib.mochii_get_field(ctx, b"x_HI", x_out.data_ptr(), nleaf)
+        rc |= lib.mochii_get_field(ctx, b"T_e", t_out.data_ptr(), nleaf)
         rc |= lib.mochii_get_field(ctx, b"gamma_HI", g_out.data_ptr(), nleaf)
         assert rc == 0
     torch.cuda.synchronize()
@@ -273,55 +367,52 @@ def main():
         t = torch.tensor([e2e_s], device="cuda", dtype=torch.float64)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e_s = float(t.item())
-    e2e_value = NPHOT * args.steps * world / e2e_s
+        p = torch.tensor([float(e_packets)], device="cuda", dtype=torch.float64)
+        dist.all_reduce(p, op=dist.ReduceOp.SUM)
+        e_packets = int(p.item())
+    e2e_value = e_packets / e2e_s
 
-    # ---- roofline of the transport kernel -------------------------------------
+    # ---- roofline of the transport kernels -----------------------------------
     peak, peak_kind = peaks()
+    wbytes = 8 if prec == "fp64" else 4
+    bseg = bytes_per_segment(wl, prec)
+    alg_bytes = float(np.mean([bseg * s_ + wbytes * a_ for s_, a_ in zip(segs, nact)]))
     mean_seg = float(np.mean(segs))
     mean_ms = float(np.mean(kern_ms))
-    achieved = BYTES_PER_SEGMENT * mean_seg / (mean_ms * 1e-3) / 1e9
-    traffic = DRAM_BYTES_PER_SEGMENT * mean_seg if DRAM_BYTES_PER_SEGMENT else None
+    achieved = alg_bytes / (mean_ms * 1e-3) / 1e9
+    traffic = None
+    if DRAM_BYTES_PER_SEGMENT.get(wl.name):
+        traffic = DRAM_BYTES_PER_SEGMENT[wl.name] * mean_seg
 
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
-        from oracle import pyorc
-        nthreads = os.cpu_count() or 1
-        sample = int(os.environ.get("MOCHII_CPU_SAMPLE", "200000"))
-        sim = pyorc.Sim(configs.stromgren64(nphotons=sample, n=GRID), nthreads=nthreads)
-        sim.set("x_HI", x_host.numpy())
-        t0 = time.perf_counter()
-        reps = 0
-        while True:
-            sim.transport_pass()
-            sim.equilibrium_update()
-            sim.set("x_HI", x_host.numpy())
-            reps += 1
-            if time.perf_counter() - t0 > 10.0 or reps >= 20:
-                break
-        dt = time.perf_counter() - t0
-        cpu = {"value": sample * reps / dt, "unit": UNIT, "cores": nthreads, "kind": "port",
-               "sample": f"{reps} iterations of {sample} packets on the same converged state"}
+        nthreads = cpu_threads(wl)
+        state = {f: neb.get(f) for f in ("x_HI", "x_HeI", "x_HeII", "n_e", "T_e")}
+        v, desc, _ = cpu_reference(wl, state, nthreads)
+        cpu = {"value": v, "unit": UNIT, "cores": nthreads, "kind": "port", "sample": desc}
 
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f32+f64",
-            "data": "synthetic", "config": {"workload": WORKLOAD, "grid": f"{GRID}^3", "packets_per_step": NPHOT,
-                       "precision": args.precision, "state": f"converged Stromgren sphere ({prep_iters} prep iterations)",
-                       "l2": "flushed between steps (256 MiB write)",
-                       "tuning": tuning,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64" if prec == "fp64" else "f32+f64",
+            "data": "synthetic",
+            "config": {"workload": wl.name, "grid": f"{wl.grid}^3", "stellar_packets_per_step": wl.nphot,
+                       "packets_per_step": packets / args.steps / world,
+                       "precision": prec, "balance": "thermal" if wl.thermal else "ionisation, fixed T_e",
+                       "state": f"{prep_iters} untimed preparation iterations from the configured start",
+                       "l2": "flushed between steps (256 MiB write)", "tuning": tuning,
                        "parallelism": "replicas" if world > 1 else "single"},
-            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 8 * nleaf,
-                    "d2h_bytes_per_step": 16 * nleaf},
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 16 * nleaf,
+                    "d2h_bytes_per_step": 24 * nleaf},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "peak_kind": peak_kind,
-                         "traffic": traffic, "kernel": "k_transport",
-                         "bytes_per_segment": BYTES_PER_SEGMENT, "segments_per_launch": mean_seg,
+                         "traffic": traffic, "kernel": "k_launch + k_walk_edge (transport pass)",
+                         "bytes_per_segment": alg_bytes / mean_seg, "segments_per_launch": mean_seg,
                          "kernel_ms": mean_ms},
             "cpu_baseline": cpu,
             "clocks": clk.summary(),
-            "gpu_launches": 3 * args.steps,
+            "gpu_launches": int(sum(launches_per_step(wl, n_ - wl.nphot) for n_ in npk)),
             "breakdown_ms": {"transport": float(np.mean(pass_ms)), "balance": float(np.mean(bal_ms))},
             "wall_s": t_wall,
         }
@@ -331,6 +422,18 @@ def main():
         dist.barrier()
         dist.destroy_process_group()
     return 0
+
+
+def launches_per_step(wl, diffuse_packets):
+    """Kernels of this library per step: a launch and a walk per chunk of up
+    to 4 Mi stellar packets, the H/He rates (+ the metal rates), the balance;
+    with the diffuse field the leaf luminosities and a launch and a walk per
+    diffuse chunk (the prefix sum is a library scan, not counted)."""
+    cap = 1 << 22
+    n = 2 * -(-wl.nphot // cap) + 1 + 1
+    if wl.name == "hii_metals128":
+        n += 1 + 1 + 2 * -(-diffuse_packets // cap)
+    return n
 
 
 if __name__ == "__main__":

@@ -138,6 +138,7 @@ typedef struct mochii_pass_stats {
     int64_t walk_kills;              /* MAX_WALK_STEPS guard hits             */
     int64_t diffuse_packets;         /* diffuse_nphot of this pass            */
     double diffuse_lum;              /* diffuse_lum [erg/s]                   */
+    int64_t metal_active;            /* sum over scored segments of the packet's active metal transitions */
 } mochii_pass_stats;
 
 /* Convergence measures (gas_thermal_update / gas_equilibrium_update outputs). */

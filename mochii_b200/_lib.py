@@ -60,7 +60,8 @@ class PassStats(C.Structure):
     _fields_ = [("energy_emitted", C.c_double), ("energy_absorbed", C.c_double), ("energy_escaped", C.c_double),
                 ("closure", C.c_double), ("direct_segments", C.c_int64), ("scattered_segments", C.c_int64),
                 ("packets", C.c_int64), ("kernel_ms", C.c_double), ("pass_ms", C.c_double),
-                ("walk_kills", C.c_int64), ("diffuse_packets", C.c_int64), ("diffuse_lum", C.c_double)]
+                ("walk_kills", C.c_int64), ("diffuse_packets", C.c_int64), ("diffuse_lum", C.c_double),
+                ("metal_active", C.c_int64)]
 
 
 class Metrics(C.Structure):

@@ -472,6 +472,7 @@ extern "C" int mochii_transport_pass(mochii_ctx* c, int with_peel, mochii_pass_s
                 std::max(s.energy_emitted, kTinest);
     s.direct_segments = (int64_t)cnt[0];
     s.walk_kills = (int64_t)cnt[1];
+    s.metal_active = (int64_t)cnt[2];
     s.kernel_ms = ms;
     s.pass_ms = pms;
     s.diffuse_packets = nd;

@@ -266,7 +266,7 @@ __global__ void __launch_bounds__(128) k_walk_edge(const PassArgs a, const Packe
     R* const mhc = msg + (MET == 1 ? a.m.ntrp * blockDim.x : 0);    // sigma_k h_k  [k][thread]
     const int tb = blockDim.x, tx = threadIdx.x;
     double emitted = 0.0, absorbed = 0.0, escaped = 0.0;
-    unsigned long long nseg = 0, kills = 0;
+    unsigned long long nseg = 0, kills = 0, nact = 0;
     T* tal = static_cast<T*>(a.tally);
     T* jt = static_cast<T*>(a.jt);
     const R* sg = static_cast<const R*>(rec.sig);
@@ -362,6 +362,7 @@ __global__ void __launch_bounds__(128) k_walk_edge(const PassArgs a, const Packe
             }
             if (w != (R)0) {   // score_ion_path returns on a zero path (ion_score_mod.f90:148)
                 ++nseg;
+                nact += nm;
                 T* tl = tal + (long long)il[0] * NT;
 #pragma unroll
                 for (int k = 0; k < NT; ++k) tally_add(tl + k, w * cf[k]);
@@ -414,10 +415,12 @@ __global__ void __launch_bounds__(128) k_walk_edge(const PassArgs a, const Packe
     for (int o = 16; o > 0; o >>= 1) {
         nseg += __shfl_down_sync(0xffffffffu, nseg, o);
         kills += __shfl_down_sync(0xffffffffu, kills, o);
+        if (METAL) nact += __shfl_down_sync(0xffffffffu, nact, o);
     }
     if ((threadIdx.x & 31) == 0) {
         if (nseg) atomicAdd(a.counters + 0, nseg);
         if (kills) atomicAdd(a.counters + 1, kills);
+        if (METAL && nact) atomicAdd(a.counters + 2, nact);
     }
 }
 

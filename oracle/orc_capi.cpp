@@ -1,4 +1,5 @@
 // Oracle C entry points for ctypes (test infrastructure only).
+#include <algorithm>
 #include <cstring>
 #include <string>
 
@@ -230,6 +231,21 @@ int orc_sim_net_rate(void* h, int il, double T, double* out5) {
     out5[0] = s->net_rate(il, T, s->par.case_ab == "A", xHI, xHeI, xHeII, ne);
     out5[1] = xHI; out5[2] = xHeI; out5[3] = xHeII; out5[4] = ne;
     return 0;
+}
+// The thermal bisection on every stride-th leaf with nH > 0, state left
+// unchanged (the CPU-baseline sample); returns the leaves solved.
+long long orc_sim_thermal_sample(void* h, long long stride) {
+    auto* s = static_cast<Sim*>(h);
+    if (!s->th || stride < 1) return -1;
+    long long solved = 0;
+#pragma omp parallel for num_threads(std::max(1, s->nthreads)) schedule(dynamic, 16) reduction(+ : solved)
+    for (long long il = 0; il < s->grid.nleaf; il += stride) {
+        if (s->st.nH[il] <= 0.0) continue;
+        double x, h1, h2, ne;
+        s->thermal_cell((int)il, x, h1, h2, ne);
+        ++solved;
+    }
+    return solved;
 }
 // Metal registry shape: transitions and stages in element order.
 int orc_sim_metal_ntr(void* h) {

@@ -1538,9 +1538,33 @@ double Sim::net_rate(int il, double T, bool caseA, double& xHI, double& xHeI, do
     return net;
 }
 
+// The per-leaf bisection of gas_thermal_update (thermal_mod.f90:160-188):
+// T_e and the ionisation state solved at it, from the leaf's current state.
+double Sim::thermal_cell(int il, double& xHI, double& xHeI, double& xHeII, double& ne) const {
+    const bool caseA = par.case_ab == "A";
+    xHI = st.xHI[il]; xHeI = st.xHeI[il]; xHeII = st.xHeII[il]; ne = 0.0;
+    double tlo = par.te_min, thi = par.te_max, te;
+    const double net_lo = net_rate(il, tlo, caseA, xHI, xHeI, xHeII, ne);
+    const double net_hi = net_rate(il, thi, caseA, xHI, xHeI, xHeII, ne);
+    if (net_lo <= 0.0) {
+        te = tlo;
+    } else if (net_hi >= 0.0) {
+        te = thi;
+    } else {
+        for (int it = 1; it <= 60; ++it) {
+            const double tmid = std::sqrt(tlo * thi);
+            const double net_mid = net_rate(il, tmid, caseA, xHI, xHeI, xHeII, ne);
+            if (net_mid > 0.0) tlo = tmid; else thi = tmid;
+            if (thi / tlo - 1.0 < 1.0e-5) break;
+        }
+        te = std::sqrt(tlo * thi);
+    }
+    net_rate(il, te, caseA, xHI, xHeI, xHeII, ne);
+    return te;
+}
+
 // gas_thermal_update, thermal_mod.f90:124-249.
 void Sim::gas_thermal_update(double m[4]) {
-    const bool caseA = par.case_ab == "A";
     const double w = par.ion_relax;
     const int nleaf = grid.nleaf;
     std::vector<double> xHI_new(nleaf), xHeI_new(nleaf), xHeII_new(nleaf), ne_new(nleaf), te_new(nleaf);
@@ -1552,24 +1576,8 @@ void Sim::gas_thermal_update(double m[4]) {
             ne_new[il] = 0.0; te_new[il] = st.Te[il];
             continue;
         }
-        double xHI = st.xHI[il], xHeI = st.xHeI[il], xHeII = st.xHeII[il], ne = 0.0;
-        double tlo = par.te_min, thi = par.te_max, te;
-        const double net_lo = net_rate(il, tlo, caseA, xHI, xHeI, xHeII, ne);
-        const double net_hi = net_rate(il, thi, caseA, xHI, xHeI, xHeII, ne);
-        if (net_lo <= 0.0) {
-            te = tlo;
-        } else if (net_hi >= 0.0) {
-            te = thi;
-        } else {
-            for (int it = 1; it <= 60; ++it) {
-                const double tmid = std::sqrt(tlo * thi);
-                const double net_mid = net_rate(il, tmid, caseA, xHI, xHeI, xHeII, ne);
-                if (net_mid > 0.0) tlo = tmid; else thi = tmid;
-                if (thi / tlo - 1.0 < 1.0e-5) break;
-            }
-            te = std::sqrt(tlo * thi);
-        }
-        net_rate(il, te, caseA, xHI, xHeI, xHeII, ne);
+        double xHI, xHeI, xHeII, ne;
+        const double te = thermal_cell(il, xHI, xHeI, xHeII, ne);
         xHI_new[il] = (1.0 - w) * st.xHI[il] + w * xHI;
         xHeI_new[il] = (1.0 - w) * st.xHeI[il] + w * xHeI;
         xHeII_new[il] = (1.0 - w) * st.xHeII[il] + w * xHeII;

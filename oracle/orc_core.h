@@ -246,6 +246,7 @@ struct Sim {
     void gas_thermal_update(double m[4]);                         // thermal_mod.f90:124-249
     double net_rate(int il, double T, bool caseA, double& xHI, double& xHeI, double& xHeII,
                     double& ne) const;                             // thermal_mod.f90:38-115
+    double thermal_cell(int il, double& xHI, double& xHeI, double& xHeII, double& ne) const;
     void opacity_fill();             // gas_opacity_fill, gas_opacity_mod.f90:299-306
     bool metals() const;             // use_metals with at least one element
     void metal_sigma(Photon& ph) const;   // species_packet_cross_sections

@@ -70,6 +70,7 @@ def load():
         "orc_sim_solve_cell": (None, [V, D, D, D, D, D, I, V]),
         "orc_sim_metal_thermal": (I, [V, I, D, D, D, D, V]),
         "orc_sim_net_rate": (I, [V, I, D, V]),
+        "orc_sim_thermal_sample": (LL, [V, LL]),
         "orc_sim_metal_nstage": (I, [V]),
         "orc_gff_table": (None, [V, V]),
         "orc_cooling_total": (D, [V, D, D, D, D, D, D]),
@@ -259,6 +260,10 @@ class Sim:
         load().orc_sim_solve_cell(self.h, float(gH), float(gHe1), float(gHe2), float(nH), float(T), int(caseA),
                                   st.ctypes.data)
         return tuple(st)
+
+    def thermal_sample(self, stride):
+        """The thermal bisection on every stride-th gas leaf, state unchanged."""
+        return load().orc_sim_thermal_sample(self.h, int(stride))
 
     def net_rate(self, il, T):
         """thermal_mod.f90 net_rate on leaf il at T: (net, x_HI, x_HeI, x_HeII, n_e)."""
