@@ -268,6 +268,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--precision", default=None, choices=["fp64", "fp32"],
                     help="transport arithmetic (default: the workload's)")
+    ap.add_argument("--solver", default="bracketed", choices=["bisection", "bracketed"],
+                    help="cell solver: the reference's bisection or the bracketed roots")
     args = ap.parse_args()
     wl = Workload(args.workload)
     prec = args.precision or wl.default_precision
@@ -290,7 +292,8 @@ def main():
     if dist is not None:
         dist.barrier()
 
-    par = parse_namelist(wl.make(wl.nphot, prec, 12345 + rank))
+    par = parse_namelist(wl.make(wl.nphot, prec, 12345 + rank).replace(
+        "/\n", f" par%thermal_solver = '{args.solver}'\n/\n"))
     neb = Nebula(par)
     prep_iters = prepare(neb, wl)
     tuning = neb.autotune(1 << 20)   # launch shape for this grid / precision / device
@@ -400,6 +403,7 @@ def main():
             "config": {"workload": wl.name, "grid": f"{wl.grid}^3", "stellar_packets_per_step": wl.nphot,
                        "packets_per_step": packets / args.steps / world,
                        "precision": prec, "balance": "thermal" if wl.thermal else "ionisation, fixed T_e",
+                       "solver": args.solver,
                        "state": f"{prep_iters} untimed preparation iterations from the configured start",
                        "l2": "flushed between steps (256 MiB write)", "tuning": tuning,
                        "parallelism": "replicas" if world > 1 else "single"},

@@ -126,6 +126,12 @@ typedef struct mochii_params {
      * contracted with the cross sections after the pass; 0 = one pair of
      * tallies per active transition per segment (species_rate_path_score) */
     int metal_moments;
+    /* cell solver (not a reference key, 'bisection' or 'bracketed'):
+     * 0 = the reference's damped n_e fixed point and bisection on log T over
+     * [te_min, te_max]; 1 = the same roots found by bracketed Illinois
+     * iterations, n_e from the cell's current state and T_e from a warm start
+     * (the cell's current T_e, or a supplied prediction) */
+    int solver_bracketed;
 } mochii_params;
 
 /* Per-pass statistics (ion_score_report_energy_closure, ion_score_mod.f90:364-387). */
@@ -212,7 +218,10 @@ int64_t mochii_nleaf(const mochii_ctx* ctx);
  * (species_mod.f90 n_elements / elem_nstage); both 0 without metals. */
 int mochii_metal_shape(const mochii_ctx* ctx, int* ntransitions, int* nstages);
 int mochii_nnu_band(const mochii_ctx* ctx);
-/* Field names: "nH" "x_HI" "x_HeI" "x_HeII" "n_e" "T_e" "gamma_HI"
+/* mochii_set_field also takes "T_warm" (nleaf): a warm-start T_e per leaf
+ * for the next bracketed thermal solve (par thermal_solver = 'bracketed'),
+ * used once; without it the solve starts from the current T_e.
+ * Field names: "nH" "x_HI" "x_HeI" "x_HeII" "n_e" "T_e" "gamma_HI"
  * "gamma_HeI" "gamma_HeII" "heat_HI" "heat_HeI" "heat_HeII" (nleaf each),
  * "jt_ion" (nleaf*nnu_band, leaf-major), "eedge" (nnu_band+1),
  * "leaf_half" (nleaf); with par%use_metals also "gamma_metal" and

@@ -52,7 +52,7 @@ class Params(C.Structure):
         ("DGR", C.c_double), ("cext_dust", C.c_double), ("grain_pe", C.c_int),
         ("ion_dust_kext", C.c_char * STRLEN), ("data_dir", C.c_char * STRLEN), ("atomic_dir", C.c_char * STRLEN),
         ("precision", C.c_int),
-        ("fe_levels_full", C.c_int), ("metal_moments", C.c_int),
+        ("fe_levels_full", C.c_int), ("metal_moments", C.c_int), ("solver_bracketed", C.c_int),
     ]
 
 

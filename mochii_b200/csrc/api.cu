@@ -76,7 +76,7 @@ void release(mochii_ctx* c) {
                     c->th.gff, c->th.lamref, c->th.Ssup, c->th.tinv,
                     c->dif.ch, c->dif.tot, c->dif.scan_tmp, c->dif.tables,
                     (void*)c->metal.el, c->metal.egam, c->metal.eheat, c->metal.opac, c->metal.raw,
-                    (void*)c->metal.medge, c->metal.mom,
+                    (void*)c->metal.medge, c->metal.mom, c->twarm,
                     (void*)c->rec.E, c->rec.msig};
     for (void* p : ptrs)
         if (p) cudaFree(p);
@@ -496,6 +496,7 @@ extern "C" int mochii_balance_update(mochii_ctx* c, int solve_te, mochii_metrics
     CK(c, cudaEventRecord(c->ev0, c->stream));
     if (solve_te) CK(c, launch_thermal(c));
     else CK(c, launch_balance(c));
+    c->twarm_set = false;
     CK(c, cudaEventRecord(c->ev1, c->stream));
     c->columns_fresh = true;   // both kernels refresh the columns they change
     const int np = solve_te ? 6 : 3;
@@ -700,6 +701,14 @@ extern "C" int mochii_get_field(mochii_ctx* c, const char* name, double* out, in
 extern "C" int mochii_set_field(mochii_ctx* c, const char* name, const double* in, int64_t n) {
     if (!c || !name || !in) return MOCHII_ERR_BAD_PARAM;
     const std::string nm(name);
+    if (nm == "T_warm") {   // warm start of the next bracketed thermal solve
+        if (n != c->grid.nleaf) return fail(c, MOCHII_ERR_BAD_PARAM, "size mismatch for T_warm");
+        if (!c->twarm) CK(c, dalloc(&c->twarm, (size_t)n));
+        CK(c, cudaMemcpyAsync(c->twarm, in, n * 8, cudaMemcpyHostToDevice, c->stream));
+        CK(c, cudaStreamSynchronize(c->stream));
+        c->twarm_set = true;
+        return MOCHII_OK;
+    }
     if (nm != "nH" && nm != "x_HI" && nm != "x_HeI" && nm != "x_HeII" && nm != "n_e" && nm != "T_e")
         return fail(c, MOCHII_ERR_BAD_PARAM, "field is not settable: " + nm);
     long long cnt = 0;

@@ -46,6 +46,8 @@ struct BalArgs {
     int caseA, nabs, fp32;
     MetalDev m;                       // trace metals; m.ntr == 0 without
     int metal_ne, two_way, metal_heat, metal_ff;
+    int fast;                         // bracketed Illinois solves (solver_bracketed)
+    double nemax;                     // largest n_e per n_H: 1 + 2 y_He + metal electrons
 };
 
 // Absorber columns n_i * distance2cm * 1e-18 for one leaf.
@@ -172,6 +174,100 @@ __device__ __noinline__ int solve_cell_metal(const Coef& k, double yHe, double g
     return it;
 }
 
+// ---- bracketed solves (solver_bracketed) -----------------------------------
+// The reference's damped iteration converges to the n_e at which the
+// electrons the cell releases equal n_e, F(n_e) = n_e, with x_HI the root of
+// hydrogen's balance at that n_e and the metal cascade evaluated there.  The
+// bracketed solve finds the same root of h(n_e) = F(n_e) - n_e directly:
+// geometric bracketing from the cell's current n_e, then Illinois iterations
+// in ln n_e, to |h| <= 2e-10 n_e (the reference stops its damped steps
+// h/2 at 1e-10 n_e).
+struct CellState {
+    double x, h1, h2;
+};
+
+__device__ __noinline__ double cell_electrons(const Coef& k, double yHe, double gH, double gHe1, double gHe2, double nH,
+                                              double ne, const MetalDev& m, const MetalCache& mc, int with_ne,
+                                              int with_cx, int* nsum, CellState& o) {
+    const bool metals = m.ntr > 0;
+    if (metals && with_cx) {
+        o.x = hydrogen_neutral_fraction(m, mc, nH, ne, k.aH * ne, gH + (k.cH + k.aH) * ne, nsum);
+    } else {
+        const double denH = gH + (k.cH + k.aH) * ne;
+        o.x = denH > 0.0 ? (k.aH * ne) / denH : 1.0;
+    }
+    const double r1 = fmin((gHe1 + k.cHe1 * ne) / (k.aHe2 * ne), 1.0e150);
+    const double r2 = fmin((gHe2 + k.cHe2 * ne) / (k.aHe3 * ne), 1.0e150);
+    o.h1 = 1.0 / (1.0 + r1 + r1 * r2);
+    o.h2 = o.h1 * r1;
+    const double h3 = o.h2 * r2;
+    double nen = nH * ((1.0 - o.x) + yHe * (o.h2 + 2.0 * h3));
+    if (metals && with_ne) {
+        double nem, rin, rout;
+        metal_sums(m, mc, nH, ne, nH * o.x, nH * (1.0 - o.x), nem, rin, rout);
+        ++*nsum;
+        nen = nen + nem;
+    }
+    return nen;
+}
+
+// Returns the number of F evaluations.
+__device__ __noinline__ int solve_cell_fast(const Coef& k, double yHe, double gH, double gHe1, double gHe2, double nH,
+                                            double& xHI, double& xHeI, double& xHeII, double& ne, const MetalDev& m,
+                                            const MetalCache& mc, int with_ne, int with_cx, int* nsum, double nemax) {
+    const double floor = 1.0e-12 * nH, top = nemax * nH;
+    const double xHeIII = fmax(0.0, 1.0 - xHeI - xHeII);
+    double a = ne > floor ? ne : fmax(nH * ((1.0 - xHI) + yHe * (xHeII + 2.0 * xHeIII)), floor);
+    a = fmin(a, top);
+    int nev = 0;
+    CellState ea, eb, ec;
+    double fa = cell_electrons(k, yHe, gH, gHe1, gHe2, nH, a, m, mc, with_ne, with_cx, nsum, ea) - a;
+    ++nev;
+    double b = a, fb = fa;
+    eb = ea;
+    bool done = fabs(fa) <= 2.0e-10 * a;
+    if (!done) {   // geometric bracketing toward the root
+        double fac = 1.25;
+        while (nev < 60) {
+            const double c = fa > 0.0 ? fmin(a * fac, top) : fmax(a / fac, floor);
+            const double fc = cell_electrons(k, yHe, gH, gHe1, gHe2, nH, c, m, mc, with_ne, with_cx, nsum, ec) - c;
+            ++nev;
+            b = c; fb = fc; eb = ec;
+            if (fc == 0.0 || (fc > 0.0) != (fa > 0.0)) break;
+            if (c >= top || c <= floor) {   // the damped iteration would sit on its clamp
+                done = true;
+                break;
+            }
+            a = c; fa = fc; ea = ec;
+            fac = fac * fac;
+        }
+        if (fb == 0.0) done = true;
+    }
+    if (!done) {   // Illinois in ln n_e on the bracket [a, b]
+        double la = log(a), lb = log(b);
+        for (int it = 0; it < 80 && nev < 140; ++it) {
+            const double lc = (la * fb - lb * fa) / (fb - fa);
+            const double c = exp(lc);
+            const double fc = cell_electrons(k, yHe, gH, gHe1, gHe2, nH, c, m, mc, with_ne, with_cx, nsum, ec) - c;
+            ++nev;
+            const double lprev = lb;
+            if ((fc > 0.0) != (fb > 0.0)) {
+                la = lb;
+                fa = fb;
+            } else {
+                fa = 0.5 * fa;
+            }
+            lb = lc; fb = fc; b = c; eb = ec;
+            if (fabs(fc) <= 2.0e-10 * c || fabs(lc - lprev) <= 1.0e-14 || fabs(lb - la) <= 1.0e-14) break;
+        }
+    }
+    ne = b;
+    xHI = eb.x;
+    xHeI = eb.h1;
+    xHeII = eb.h2;
+    return nev;
+}
+
 __global__ void __launch_bounds__(kBThreads) k_balance(const BalArgs a) {
     __shared__ double sh[3][kBThreads];
     double mdx = 0.0, sdx = 0.0, sx = 0.0;
@@ -188,7 +284,12 @@ __global__ void __launch_bounds__(kBThreads) k_balance(const BalArgs a) {
         double xHI = x0, xHeI = h10, xHeII = h20, ne;
         MetalCache mc;
         int it, nsum = 0;
-        if (a.m.ntr > 0) {
+        if (a.fast) {
+            if (a.m.ntr > 0) metal_prepare(a.m, il, a.T, mc);
+            ne = a.ne[il];
+            it = solve_cell_fast(a.k, a.yHe, a.rates[il], a.rates[a.nleaf + il], a.rates[2 * a.nleaf + il], nH, xHI,
+                                 xHeI, xHeII, ne, a.m, mc, a.metal_ne, a.two_way, &nsum, a.nemax);
+        } else if (a.m.ntr > 0) {
             metal_prepare(a.m, il, a.T, mc);
             it = solve_cell_metal(a.k, a.yHe, a.rates[il], a.rates[a.nleaf + il], a.rates[2 * a.nleaf + il], nH, xHI,
                                   xHeI, xHeII, ne, a.m, mc, a.metal_ne, a.two_way, &nsum);
@@ -263,6 +364,7 @@ struct ThArgs {
     BalArgs b;
     ThermalDev td;
     double te_min, te_max;
+    const double* Twarm;   // bracketed solve: warm-start T_e per leaf (nullptr: the current T_e)
 };
 
 // gbar_ff (cooling_mod.f90:223-234): linear in log10 T on the 41-node table.
@@ -400,7 +502,11 @@ __device__ double net_rate(const ThArgs& a, long long il, double T, double nH, d
     const BalArgs& b = a.b;
     const long long n = b.nleaf;
     const Coef k = coef_at_call(b.rs, b.caseA, T);
-    if (b.m.ntr > 0) {
+    if (b.fast) {
+        if (b.m.ntr > 0) metal_prepare(b.m, il, T, mc);
+        *passes += solve_cell_fast(k, b.yHe, b.rates[il], b.rates[n + il], b.rates[2 * n + il], nH, xHI, xHeI, xHeII,
+                                   ne, b.m, mc, b.metal_ne, b.two_way, nsum, b.nemax);
+    } else if (b.m.ntr > 0) {
         metal_prepare(b.m, il, T, mc);
         *passes += solve_cell_metal(k, b.yHe, b.rates[il], b.rates[n + il], b.rates[2 * n + il], nH, xHI, xHeI, xHeII,
                                     ne, b.m, mc, b.metal_ne, b.two_way, nsum);
@@ -417,6 +523,53 @@ __device__ double net_rate(const ThArgs& a, long long il, double T, double nH, d
         if (b.metal_heat) net = net + mt.heat;
     }
     return net;
+}
+
+// The bracketed T_e solve (solver_bracketed): the root of net(T) that the
+// reference's bisection on [te_min, te_max] converges to, found from a warm
+// start T_w.  net(T_w) gives the direction; geometric steps in ln T (x1.1,
+// squared each step) bracket the sign change, or reach te_min with net <= 0
+// (the reference's "cooling wins at te_min") or te_max with net >= 0; then
+// Illinois iterations in ln T until the bracket or the step is below 1e-5 in
+// ln T.  The cell state left behind is the one solved at the returned T_e.
+__device__ double thermal_bracketed(const ThArgs& a, long long il, double nH, double& xHI, double& xHeI, double& xHeII,
+                                    double& ne, int* passes, MetalCache& mc, int* nsum, int* nev, double Tw) {
+    const double lo_lim = a.te_min, hi_lim = a.te_max;
+    double ta = fmin(fmax(Tw, lo_lim), hi_lim);
+    double fa = net_rate(a, il, ta, nH, xHI, xHeI, xHeII, ne, passes, mc, nsum);
+    ++*nev;
+    if (fa == 0.0) return ta;
+    double tb = ta, fb = fa, fac = 1.1;
+    for (int s = 0; s < 40; ++s) {
+        tb = fa > 0.0 ? fmin(ta * fac, hi_lim) : fmax(ta / fac, lo_lim);
+        fb = net_rate(a, il, tb, nH, xHI, xHeI, xHeII, ne, passes, mc, nsum);
+        ++*nev;
+        if (fb == 0.0) return tb;
+        if ((fb > 0.0) != (fa > 0.0)) break;
+        if (tb >= hi_lim || tb <= lo_lim) return tb;   // heating wins at te_max / cooling at te_min
+        ta = tb;
+        fa = fb;
+        fac = fac * fac;
+    }
+    double la = log(ta), lb = log(tb), t = tb;
+    for (int it = 0; it < 60; ++it) {
+        const double lc = (la * fb - lb * fa) / (fb - fa);
+        t = exp(lc);
+        const double fc = net_rate(a, il, t, nH, xHI, xHeI, xHeII, ne, passes, mc, nsum);
+        ++*nev;
+        if (fc == 0.0) break;
+        const double step = fabs(lc - lb);
+        if ((fc > 0.0) != (fb > 0.0)) {
+            la = lb;
+            fa = fb;
+        } else {
+            fa = 0.5 * fa;
+        }
+        lb = lc;
+        fb = fc;
+        if (fabs(lb - la) < 1.0e-5 || step < 1.0e-7) break;
+    }
+    return t;
 }
 
 // gas_thermal_update (thermal_mod.f90:124-249): bisection on log T in
@@ -437,32 +590,39 @@ __global__ void __launch_bounds__(kBThreads) k_thermal(const ThArgs a) {
             continue;
         }
         double xHI = x0, xHeI = h10, xHeII = h20, ne = 0.0;
-        int passes = 0, nsum = 0, nev = 2;
-        double tlo = a.te_min, thi = a.te_max, te;
+        int passes = 0, nsum = 0, nev = 0, last = 0;
+        double te;
         MetalCache mc;
-        const double net_lo = net_rate(a, il, tlo, nH, xHI, xHeI, xHeII, ne, &passes, mc, &nsum);
-        const double net_hi = net_rate(a, il, thi, nH, xHI, xHeI, xHeII, ne, &passes, mc, &nsum);
-        if (net_lo <= 0.0) {
-            te = tlo;
-        } else if (net_hi >= 0.0) {
-            te = thi;
+        if (b.fast) {
+            ne = b.ne[il];
+            te = thermal_bracketed(a, il, nH, xHI, xHeI, xHeII, ne, &passes, mc, &nsum, &nev,
+                                   a.Twarm ? a.Twarm[il] : T0);
         } else {
-            for (int it = 1; it <= 60; ++it) {
-                const double tmid = sqrt(tlo * thi);
-                const double nm = net_rate(a, il, tmid, nH, xHI, xHeI, xHeII, ne, &passes, mc, &nsum);
-                ++nev;
-                if (nm > 0.0) tlo = tmid; else thi = tmid;
-                if (thi / tlo - 1.0 < 1.0e-5) break;
+            double tlo = a.te_min, thi = a.te_max;
+            nev = 3;
+            const double net_lo = net_rate(a, il, tlo, nH, xHI, xHeI, xHeII, ne, &passes, mc, &nsum);
+            const double net_hi = net_rate(a, il, thi, nH, xHI, xHeI, xHeII, ne, &passes, mc, &nsum);
+            if (net_lo <= 0.0) {
+                te = tlo;
+            } else if (net_hi >= 0.0) {
+                te = thi;
+            } else {
+                for (int it = 1; it <= 60; ++it) {
+                    const double tmid = sqrt(tlo * thi);
+                    const double nm = net_rate(a, il, tmid, nH, xHI, xHeI, xHeII, ne, &passes, mc, &nsum);
+                    ++nev;
+                    if (nm > 0.0) tlo = tmid; else thi = tmid;
+                    if (thi / tlo - 1.0 < 1.0e-5) break;
+                }
+                te = sqrt(tlo * thi);
             }
-            te = sqrt(tlo * thi);
+            net_rate(a, il, te, nH, xHI, xHeI, xHeII, ne, &last, mc, &nsum);
+            if (last > 200) ++caps;
         }
-        int last = 0;
-        net_rate(a, il, te, nH, xHI, xHeI, xHeII, ne, &last, mc, &nsum);
         ++solved;
-        if (last > 200) ++caps;
         tpass += (unsigned long long)(passes + last);
         tsums += (unsigned long long)nsum;
-        nevals += (unsigned long long)(nev + 1);
+        nevals += (unsigned long long)nev;
         const double w = b.relax;
         const double xn = (1.0 - w) * x0 + w * xHI;
         const double h1n = (1.0 - w) * h10 + w * xHeI;
@@ -606,6 +766,9 @@ static BalArgs bal_args(mochii_ctx* c) {
     a.two_way = c->par.charge_exchange_two_way;
     a.metal_heat = c->par.metal_heat;
     a.metal_ff = c->par.metal_freefree;
+    a.fast = c->par.solver_bracketed;
+    a.nemax = 1.0 + 2.0 * c->par.He_abund;
+    for (const MetalEl& e : c->species.el) a.nemax += e.abund * (double)(e.nstage - 1);
     return a;
 }
 
@@ -621,6 +784,7 @@ cudaError_t launch_thermal(mochii_ctx* c) {
     a.td = c->th;
     a.te_min = c->par.te_min;
     a.te_max = c->par.te_max;
+    a.Twarm = c->twarm_set ? c->twarm : nullptr;
     k_thermal<<<c->bw.blocks, kBThreads, 0, c->stream>>>(a);
     return cudaGetLastError();
 }

@@ -99,6 +99,8 @@ struct mochii_ctx {
     mochii::ThermalDev th;          // thermal tables (solve_te)
     mochii::DiffuseBuffers dif;     // diffuse field (diffuse_field)
     mochii::MetalDev metal;         // trace metals (use_metals); metal.ntr == 0 without
+    double* twarm = nullptr;        // bracketed thermal solve: warm-start T_e per leaf ("T_warm")
+    bool twarm_set = false;         // consumed by the next thermal update
     mochii::SpeciesHost species;
     bool thermal_ready = false;
     mochii::BalanceWork bw;

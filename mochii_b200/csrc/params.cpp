@@ -270,6 +270,12 @@ int set_key(mochii_params* p, std::string key, const std::vector<std::string>& v
     if (key == "ion_dust_kext") { copy_str(p->ion_dust_kext, sizeof(p->ion_dust_kext), unquote(v)); return 0; }
     if (key == "data_dir") { copy_str(p->data_dir, sizeof(p->data_dir), unquote(v)); return 0; }
     if (key == "atomic_dir") { copy_str(p->atomic_dir, sizeof(p->atomic_dir), unquote(v)); return 0; }
+    if (key == "thermal_solver") {
+        const std::string s = lower(unquote(v));
+        if (s != "bisection" && s != "bracketed") return bad("must be 'bisection' or 'bracketed'");
+        p->solver_bracketed = s == "bracketed";
+        return 0;
+    }
     if (key == "metal_tally") {
         const std::string s = lower(unquote(v));
         if (s != "moments" && s != "exact") return bad("must be 'moments' or 'exact'");

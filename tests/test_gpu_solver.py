@@ -1,0 +1,100 @@
+"""The bracketed cell solver (thermal_solver = 'bracketed') against the
+reference's algorithm in the CPU oracle (damped n_e fixed point, bisection on
+log T over [te_min, te_max]), through the C ABI.
+
+Both find the same roots: n_e where the electrons the cell releases equal
+n_e, and T_e where net heating vanishes.  Bars as for the reference solve:
+T_e within 20 K and x_HII within 1e-3 of the FP64 oracle on the same
+tallies, n_e within 1e-6 relative at fixed T_e; and the bracketed solve
+uses fewer net-rate evaluations than the bisection on the same state.
+"""
+import numpy as np
+import pytest
+
+from mochii_b200 import Nebula, configs, parse_namelist
+
+pytestmark = pytest.mark.gpu
+
+
+def with_solver(nl, solver):
+    return nl.replace("/\n", f" par%thermal_solver = '{solver}'\n/\n")
+
+
+def partial_state(n, L):
+    d = 2 * L / n
+    c = (np.arange(n) + 0.5) * d - L
+    z, y, x = np.meshgrid(c, c, c, indexing="ij")
+    r = np.sqrt(x * x + y * y + z * z).ravel()
+    xHI = np.clip(1e-4 + (r / (0.7 * L)) ** 6, 1e-4, 1.0)
+    xHeI = np.clip(1.5 * xHI, 0.0, 1.0)
+    return {"x_HI": xHI, "x_HeI": xHeI, "x_HeII": 1.0 - xHeI}
+
+
+def run_pair(orc, nl, n, iters, thermal=True):
+    neb = Nebula(parse_namelist(with_solver(nl, "bracketed")))
+    sim = orc.Sim(nl)
+    L = parse_namelist(nl).xmax
+    st = partial_state(n, L)
+    for k, v in st.items():
+        neb.set(k, v)
+        sim.set(k, v)
+    ne = neb.get("nH") * ((1 - st["x_HI"]) + 0.1 * st["x_HeII"])
+    neb.set("n_e", ne)
+    sim.set("n_e", ne)
+    neb.gas_opacity_fill()
+    out = []
+    for _ in range(iters):
+        neb.ionizing_field_and_rates()
+        sim.transport_pass()
+        if thermal:
+            neb.gas_thermal_update()
+            sim.thermal_update()
+        else:
+            neb.gas_equilibrium_update()
+            sim.equilibrium_update()
+        out.append(neb.last_metrics.rate_evaluations)
+        yield neb, sim
+
+
+@pytest.mark.parametrize("metals", [False, True])
+def test_bracketed_thermal_matches_oracle_bisection(orc, metals):
+    if metals:
+        n = 12
+        nl = configs.hii_metals(nphotons=40000, niter=3, n=n, precision="fp64", rs_factor=1.3, diffuse=False)
+    else:
+        n = 24
+        nl = configs.hii_thermal(nphotons=60000, niter=3, n=n, precision="fp64", rs_factor=1.2)
+    for neb, sim in run_pair(orc, nl, n, 3):
+        tg, to = neb.get("T_e"), sim.get("T_e")
+        assert np.max(np.abs(tg - to)) < 20.0, np.max(np.abs(tg - to))
+        assert np.max(np.abs(neb.get("x_HI") - sim.get("x_HI"))) < 1e-3
+    neb.close()
+
+
+def test_bracketed_equilibrium_matches_oracle(orc):
+    n = 16
+    nl = configs.hii_metals(nphotons=60000, niter=3, n=n, precision="fp64", rs_factor=1.3, diffuse=False,
+                            solve_te=False)
+    for neb, sim in run_pair(orc, nl, n, 3, thermal=False):
+        assert np.max(np.abs(neb.get("x_HI") - sim.get("x_HI"))) < 1e-3
+        np.testing.assert_allclose(neb.get("n_e"), sim.get("n_e"), rtol=1e-6)
+    neb.close()
+
+
+def test_bracketed_solve_needs_fewer_evaluations():
+    """Same tallies and state, the two solvers: evaluations of net(T) and
+    the metal cascade sums, and the T_e they reach."""
+    n = 24
+    nl = configs.hii_metals(nphotons=100000, niter=3, n=n, precision="fp64", rs_factor=1.2, diffuse=False)
+    res = {}
+    for solver in ("bisection", "bracketed"):
+        neb = Nebula(parse_namelist(with_solver(nl, solver)))
+        for _ in range(2):
+            neb.ionizing_field_and_rates()
+            neb.gas_thermal_update()
+        m = neb.last_metrics
+        res[solver] = (m.rate_evaluations, m.metal_sum_calls, neb.get("T_e"))
+        neb.close()
+    assert res["bracketed"][0] < 0.6 * res["bisection"][0], (res["bracketed"][0], res["bisection"][0])
+    assert res["bracketed"][1] < 0.6 * res["bisection"][1]
+    assert np.max(np.abs(res["bracketed"][2] - res["bisection"][2])) < 20.0
