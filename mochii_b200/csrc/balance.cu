@@ -179,9 +179,9 @@ __device__ __noinline__ int solve_cell_metal(const Coef& k, double yHe, double g
 // electrons the cell releases equal n_e, F(n_e) = n_e, with x_HI the root of
 // hydrogen's balance at that n_e and the metal cascade evaluated there.  The
 // bracketed solve finds the same root of h(n_e) = F(n_e) - n_e directly:
-// geometric bracketing from the cell's current n_e, then Illinois iterations
-// in ln n_e, to |h| <= 2e-10 n_e (the reference stops its damped steps
-// h/2 at 1e-10 n_e).
+// geometric bracketing from the cell's current n_e, then safeguarded false
+// position in ln n_e, to |h| <= 2e-10 n_e (the reference stops its damped
+// steps h/2 at 1e-10 n_e).
 struct CellState {
     double x, h1, h2;
 };
@@ -243,22 +243,28 @@ __device__ __noinline__ int solve_cell_fast(const Coef& k, double yHe, double gH
         }
         if (fb == 0.0) done = true;
     }
-    if (!done) {   // Illinois in ln n_e on the bracket [a, b]
+    if (!done) {   // safeguarded false position in ln n_e on the bracket [a, b]
         double la = log(a), lb = log(b);
-        for (int it = 0; it < 80 && nev < 140; ++it) {
-            const double lc = (la * fb - lb * fa) / (fb - fa);
+        bool bisect = false;
+        for (int it = 0; it < 100 && nev < 160; ++it) {
+            const double width = fabs(lb - la);
+            if (width <= 1.0e-13) break;
+            double lc = (la * fb - lb * fa) / (fb - fa);
+            if (bisect || !(fabs(lc - la) > 0.05 * width && fabs(lc - lb) > 0.05 * width)) lc = 0.5 * (la + lb);
             const double c = exp(lc);
             const double fc = cell_electrons(k, yHe, gH, gHe1, gHe2, nH, c, m, mc, with_ne, with_cx, nsum, ec) - c;
             ++nev;
-            const double lprev = lb;
-            if ((fc > 0.0) != (fb > 0.0)) {
-                la = lb;
-                fa = fb;
+            b = c;          // the returned point is the last one evaluated
+            eb = ec;
+            if (fabs(fc) <= 2.0e-10 * c) break;
+            if ((fc > 0.0) == (fa > 0.0)) {
+                la = lc;
+                fa = fc;
             } else {
-                fa = 0.5 * fa;
+                lb = lc;
+                fb = fc;
             }
-            lb = lc; fb = fc; b = c; eb = ec;
-            if (fabs(fc) <= 2.0e-10 * c || fabs(lc - lprev) <= 1.0e-14 || fabs(lb - la) <= 1.0e-14) break;
+            bisect = fabs(lb - la) > 0.5 * width;
         }
     }
     ne = b;
@@ -530,8 +536,9 @@ __device__ double net_rate(const ThArgs& a, long long il, double T, double nH, d
 // start T_w.  net(T_w) gives the direction; geometric steps in ln T (x1.1,
 // squared each step) bracket the sign change, or reach te_min with net <= 0
 // (the reference's "cooling wins at te_min") or te_max with net >= 0; then
-// Illinois iterations in ln T until the bracket or the step is below 1e-5 in
-// ln T.  The cell state left behind is the one solved at the returned T_e.
+// safeguarded false position in ln T until the bracket is below 1e-5 in ln T
+// (the reference's bisection stops at thi/tlo - 1 < 1e-5).  The cell state
+// left behind is the one solved at the returned T_e.
 __device__ double thermal_bracketed(const ThArgs& a, long long il, double nH, double& xHI, double& xHeI, double& xHeII,
                                     double& ne, int* passes, MetalCache& mc, int* nsum, int* nev, double Tw) {
     const double lo_lim = a.te_min, hi_lim = a.te_max;
@@ -551,23 +558,28 @@ __device__ double thermal_bracketed(const ThArgs& a, long long il, double nH, do
         fa = fb;
         fac = fac * fac;
     }
+    // safeguarded false position: net(T) spans many decades across the
+    // bracket, so a point within 5% of an end, or a bracket that did not
+    // halve, is replaced by the midpoint
     double la = log(ta), lb = log(tb), t = tb;
-    for (int it = 0; it < 60; ++it) {
-        const double lc = (la * fb - lb * fa) / (fb - fa);
+    bool bisect = false;
+    for (int it = 0; it < 80; ++it) {
+        const double width = fabs(lb - la);
+        if (width < 1.0e-5) break;
+        double lc = (la * fb - lb * fa) / (fb - fa);
+        if (bisect || !(fabs(lc - la) > 0.05 * width && fabs(lc - lb) > 0.05 * width)) lc = 0.5 * (la + lb);
         t = exp(lc);
         const double fc = net_rate(a, il, t, nH, xHI, xHeI, xHeII, ne, passes, mc, nsum);
         ++*nev;
         if (fc == 0.0) break;
-        const double step = fabs(lc - lb);
-        if ((fc > 0.0) != (fb > 0.0)) {
-            la = lb;
-            fa = fb;
+        if ((fc > 0.0) == (fa > 0.0)) {
+            la = lc;
+            fa = fc;
         } else {
-            fa = 0.5 * fa;
+            lb = lc;
+            fb = fc;
         }
-        lb = lc;
-        fb = fc;
-        if (fabs(lb - la) < 1.0e-5 || step < 1.0e-7) break;
+        bisect = fabs(lb - la) > 0.5 * width;
     }
     return t;
 }
