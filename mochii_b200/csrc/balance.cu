@@ -546,6 +546,7 @@ __device__ double thermal_bracketed(const ThArgs& a, long long il, double nH, do
     double fa = net_rate(a, il, ta, nH, xHI, xHeI, xHeII, ne, passes, mc, nsum);
     ++*nev;
     if (fa == 0.0) return ta;
+    if ((ta <= lo_lim && fa < 0.0) || (ta >= hi_lim && fa > 0.0)) return ta;   // pinned at a limit
     double tb = ta, fb = fa, fac = 1.1;
     for (int s = 0; s < 40; ++s) {
         tb = fa > 0.0 ? fmin(ta * fac, hi_lim) : fmax(ta / fac, lo_lim);
