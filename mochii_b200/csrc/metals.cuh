@@ -135,53 +135,18 @@ static __device__ __noinline__ void metal_sums(const MetalDev& m, const MetalCac
     nem = 0.0;
     rin = 0.0;
     rout = 0.0;
+    double r[kMaxSt];
     for (int ie = 0; ie < m.nel; ++ie) {
         const MetalEl e = m.el[ie];
-        const int ns = e.nstage, j0 = e.tr0;
-        // Stage weights w_i = prod_{j<i} R_ion,j prod_{j>=i} R_rec,j, so that
-        // f_i = w_i / sum w: the ratio chain of the reference with a single
-        // division per element (R_rec clamped at tinest as there; with a rate
-        // below 1e-60 the products of up to five rates could underflow, and
-        // the ratio chain is used instead).
-        double rion[kMaxSt], rrec[kMaxSt], w[kMaxSt];
-        bool tiny = false;
-        for (int it = 0; it < ns - 1; ++it) {
-            const int j = j0 + it;
-            double a = c.gam[j] + ne * c.ci[j];
-            if (c.cxi[j] > 0.0) a = a + nHII * c.cxi[j];
-            double b = ne * c.rec[j];
-            if (c.cxr[j] > 0.0) b = b + nHI * c.cxr[j];
-            b = fmax(b, kTinest);
-            tiny = tiny || b < 1.0e-60;
-            rion[it] = a;
-            rrec[it] = b;
-        }
-        double fr[kMaxSt];
-        if (!tiny) {
-            double suf = 1.0;
-            for (int i = ns - 1; i >= 0; --i) {   // w_i carries prod_{j>=i} R_rec,j
-                w[i] = suf;
-                if (i > 0) suf = suf * rrec[i - 1];
-            }
-            double pre = 1.0, sum = 0.0;
-            for (int i = 0; i < ns; ++i) {
-                w[i] = w[i] * pre;
-                sum = sum + w[i];
-                if (i < ns - 1) pre = pre * rion[i];
-            }
-            const double inv = 1.0 / sum;
-            for (int i = 0; i < ns; ++i) fr[i] = w[i] * inv;
-        } else {
-            double r[kMaxSt];
-            fr[0] = metal_chain(c, j0, ns, ne, nHI, nHII, r);
-            for (int i = 1; i < ns; ++i) fr[i] = fr[i - 1] * r[i - 1];
-        }
+        const int ns = e.nstage;
+        double fr = metal_chain(c, e.tr0, ns, ne, nHI, nHII, r);
         const double nX = e.abund * nH;
-        if (ns > 1) rin = rin + c.cxi[j0] * nX * fr[0];
+        if (ns > 1) rin = rin + c.cxi[e.tr0] * nX * fr;
         for (int i = 2; i <= ns; ++i) {
-            nem = nem + e.abund * nH * fr[i - 1] * (double)(i - 1);
-            rout = rout + c.cxr[j0 + i - 2] * nX * fr[i - 1];
-            if (i < ns) rin = rin + c.cxi[j0 + i - 1] * nX * fr[i - 1];
+            fr = fr * r[i - 2];
+            nem = nem + e.abund * nH * fr * (double)(i - 1);
+            rout = rout + c.cxr[e.tr0 + i - 2] * nX * fr;
+            if (i < ns) rin = rin + c.cxi[e.tr0 + i - 1] * nX * fr;
         }
     }
 }
