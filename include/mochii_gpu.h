@@ -270,6 +270,36 @@ int mochii_diffuse_records(mochii_ctx* ctx, int64_t ip0, int64_t n, double* out8
  * capture).  Calls share the array: calls that overlap on the GPU race. */
 int mochii_launch_records_noalloc(mochii_ctx* ctx, int64_t ip0, int64_t n, double* out8);
 
+/* ---- learned warm start of the thermal balance (no reference counterpart:
+ * the warm start is this library's addition) -------------------------------
+ * A 4-layer MLP, 16 -> 128 -> 128 -> 128 -> 4 with GELU, BF16 tensor-core
+ * GEMMs with FP32 accumulation and FP32 master weights, trained with Adam on
+ * (features, solved state) pairs of the cell solver.  Features per leaf
+ * (16 floats, 12 used): log Gamma_HI/HeI/HeII, log heating HI/HeI/HeII,
+ * log n_H, dust-absorbed power, previous x_HII, x_HeII, x_HeIII, log T_e,
+ * each scaled to order one (mochii_mlp_features).  Targets per leaf (4
+ * floats): x_HII, x_HeII, x_HeIII, 4 (log10 T_e - 4). */
+typedef struct mochii_mlp mochii_mlp;
+int mochii_mlp_create(uint64_t seed, mochii_mlp** out);
+void mochii_mlp_destroy(mochii_mlp* m);
+const char* mochii_mlp_last_error(const mochii_mlp* m);
+int64_t mochii_mlp_num_params(void);
+/* parameters in layer order: W (out x in, row-major) then b of each layer */
+int mochii_mlp_get_params(mochii_mlp* m, float* out);
+int mochii_mlp_set_params(mochii_mlp* m, const float* in);
+/* loss gradient over one batch of n rows, parameter layout; no update */
+int mochii_mlp_gradients(mochii_mlp* m, const float* X, const float* Y, int64_t n, float* grads, float* loss);
+/* epochs of shuffled mini-batches with Adam; losses[epochs] = mean batch loss */
+int mochii_mlp_train(mochii_mlp* m, const float* X, const float* Y, int64_t n, int epochs, int batch, float lr,
+                     uint64_t seed, float* losses);
+/* out4 per row: x_HII, x_HeII, x_HeIII, T_e [K] */
+int mochii_mlp_predict(mochii_mlp* m, const float* X, int64_t n, double* out4);
+/* features of every leaf from the nebula's current rates and state (nleaf x 16) */
+int mochii_mlp_features(mochii_ctx* ctx, float* out);
+/* predicted T_e of every leaf as the warm start of the next bracketed
+ * thermal solve (par thermal_solver = 'bracketed'), computed on the device */
+int mochii_mlp_warm_start(mochii_ctx* ctx, mochii_mlp* m);
+
 #ifdef __cplusplus
 }
 #endif

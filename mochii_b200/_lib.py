@@ -89,6 +89,18 @@ SIGNATURES = {
     "mochii_transport_pass": (C.c_int, [C.c_void_p, C.c_int, _P(PassStats)]),
     "mochii_balance_update": (C.c_int, [C.c_void_p, C.c_int, _P(Metrics)]),
     "mochii_opacity_fill": (C.c_int, [C.c_void_p]),
+    "mochii_mlp_create": (C.c_int, [C.c_uint64, _P(C.c_void_p)]),
+    "mochii_mlp_destroy": (None, [C.c_void_p]),
+    "mochii_mlp_last_error": (C.c_char_p, [C.c_void_p]),
+    "mochii_mlp_num_params": (C.c_int64, []),
+    "mochii_mlp_get_params": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "mochii_mlp_set_params": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "mochii_mlp_gradients": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p, _P(C.c_float)]),
+    "mochii_mlp_train": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64, C.c_int, C.c_int, C.c_float,
+                                   C.c_uint64, C.c_void_p]),
+    "mochii_mlp_predict": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p]),
+    "mochii_mlp_features": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "mochii_mlp_warm_start": (C.c_int, [C.c_void_p, C.c_void_p]),
     "mochii_nleaf": (C.c_int64, [C.c_void_p]),
     "mochii_metal_shape": (C.c_int, [C.c_void_p, _P(C.c_int), _P(C.c_int)]),
     "mochii_nnu_band": (C.c_int, [C.c_void_p]),

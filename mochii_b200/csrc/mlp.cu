@@ -1,0 +1,589 @@
+// Learned warm start of the per-leaf thermal balance: a 4-layer MLP
+// (16 -> 128 -> 128 -> 128 -> 4, GELU) that maps a leaf's rates, density and
+// previous state to its solved state (x_HII, x_HeII, x_HeIII, log T_e).
+// Trained on (features, solved state) pairs that the cell solver itself
+// produces; its T_e prediction seeds the bracketed thermal solve, which still
+// solves every leaf to the same tolerance.
+//
+// The GEMMs run on the tensor cores with BF16 operands (FP32 master weights
+// rounded to BF16 as tiles are staged; activations and gradients likewise)
+// and FP32 accumulation: mma.sync m16n8k16 BF16 tiles, 64x64x32 block tiles.
+// Forward, backward (weight and activation gradients), the GELU derivative,
+// bias gradients and the Adam step are kernels of this file.
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <random>
+#include <string>
+#include <vector>
+
+#include "ctx.h"
+#include "mochii_gpu.h"
+#include "transport.h"
+
+namespace mochii {
+namespace {
+
+constexpr int kIn = 16, kHid = 128, kOut = 4, kLayers = 4;
+constexpr int kDim[kLayers + 1] = {kIn, kHid, kHid, kHid, kOut};
+
+// ---- BF16 tensor-core GEMM ---------------------------------------------------
+// C[m, n] = sum_k A(m, k) B(k, n) with A(m, k) = A[m*am + k*ak] and
+// B(k, n) = B[k*bk + n*bn], both FP32 in memory, rounded to BF16 in shared
+// memory; FP32 accumulation.  Epilogue: EPI_STORE C = acc; EPI_BIAS C = acc +
+// bias[n]; EPI_BIAS_GELU Z = acc + bias[n] (kept), C = GELU(Z).
+enum { EPI_STORE = 0, EPI_BIAS = 1, EPI_BIAS_GELU = 2 };
+constexpr int BM = 64, BN = 64, BK = 32, PAD = 8;
+
+__device__ __forceinline__ uint32_t pack2(__nv_bfloat16 lo, __nv_bfloat16 hi) {
+    return (uint32_t)__bfloat16_as_ushort(lo) | ((uint32_t)__bfloat16_as_ushort(hi) << 16);
+}
+
+__device__ __forceinline__ float gelu(float z) { return 0.5f * z * (1.0f + erff(z * 0.70710678118654752f)); }
+__device__ __forceinline__ float gelu_grad(float z) {
+    return 0.5f * (1.0f + erff(z * 0.70710678118654752f)) + z * 0.39894228040143268f * expf(-0.5f * z * z);
+}
+
+template <int EPI>
+__global__ void __launch_bounds__(128) k_gemm(int M, int N, int K, const float* __restrict__ A, long long am,
+                                              long long ak, const float* __restrict__ B, long long bk, long long bn,
+                                              float* __restrict__ C, long long ldc, const float* __restrict__ bias,
+                                              float* __restrict__ Z) {
+    __shared__ __nv_bfloat16 As[BM][BK + PAD];
+    __shared__ __nv_bfloat16 Bs[BN][BK + PAD];   // [n][k]
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int wm = (warp >> 1) * 32, wn = (warp & 1) * 32;
+    const int g = lane >> 2, t = lane & 3;
+    const int m0 = blockIdx.y * BM, n0 = blockIdx.x * BN;
+    float acc[2][4][4];
+#pragma unroll
+    for (int i = 0; i < 2; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+#pragma unroll
+            for (int q = 0; q < 4; ++q) acc[i][j][q] = 0.0f;
+    for (int k0 = 0; k0 < K; k0 += BK) {
+        for (int e = tid; e < BM * BK; e += 128) {
+            const int r = e / BK, c = e % BK;
+            const int m = m0 + r, k = k0 + c;
+            As[r][c] = __float2bfloat16_rn(m < M && k < K ? A[(long long)m * am + (long long)k * ak] : 0.0f);
+        }
+        for (int e = tid; e < BN * BK; e += 128) {
+            const int r = e / BK, c = e % BK;
+            const int n = n0 + r, k = k0 + c;
+            Bs[r][c] = __float2bfloat16_rn(n < N && k < K ? B[(long long)k * bk + (long long)n * bn] : 0.0f);
+        }
+        __syncthreads();
+#pragma unroll
+        for (int kk = 0; kk < BK; kk += 16) {
+            uint32_t a[2][4], b[4][2];
+#pragma unroll
+            for (int i = 0; i < 2; ++i) {
+                const int r = wm + i * 16 + g, c = kk + t * 2;
+                a[i][0] = pack2(As[r][c], As[r][c + 1]);
+                a[i][1] = pack2(As[r + 8][c], As[r + 8][c + 1]);
+                a[i][2] = pack2(As[r][c + 8], As[r][c + 9]);
+                a[i][3] = pack2(As[r + 8][c + 8], As[r + 8][c + 9]);
+            }
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const int n = wn + j * 8 + g, c = kk + t * 2;
+                b[j][0] = pack2(Bs[n][c], Bs[n][c + 1]);
+                b[j][1] = pack2(Bs[n][c + 8], Bs[n][c + 9]);
+            }
+#pragma unroll
+            for (int i = 0; i < 2; ++i)
+#pragma unroll
+                for (int j = 0; j < 4; ++j)
+                    asm volatile(
+                        "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, "
+                        "{%8,%9}, {%0,%1,%2,%3};\n"
+                        : "+f"(acc[i][j][0]), "+f"(acc[i][j][1]), "+f"(acc[i][j][2]), "+f"(acc[i][j][3])
+                        : "r"(a[i][0]), "r"(a[i][1]), "r"(a[i][2]), "r"(a[i][3]), "r"(b[j][0]), "r"(b[j][1]));
+        }
+        __syncthreads();
+    }
+#pragma unroll
+    for (int i = 0; i < 2; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const int m = m0 + wm + i * 16 + g + (q >= 2 ? 8 : 0);
+                const int n = n0 + wn + j * 8 + t * 2 + (q & 1);
+                if (m >= M || n >= N) continue;
+                float v = acc[i][j][q];
+                if (EPI != EPI_STORE) v = v + bias[n];
+                if (EPI == EPI_BIAS_GELU) {
+                    Z[(long long)m * ldc + n] = v;
+                    v = gelu(v);
+                }
+                C[(long long)m * ldc + n] = v;
+            }
+}
+
+template <int EPI>
+void gemm(cudaStream_t s, int M, int N, int K, const float* A, long long am, long long ak, const float* B, long long bk,
+          long long bn, float* C, long long ldc, const float* bias = nullptr, float* Z = nullptr) {
+    dim3 grid((N + BN - 1) / BN, (M + BM - 1) / BM);
+    k_gemm<EPI><<<grid, 128, 0, s>>>(M, N, K, A, am, ak, B, bk, bn, C, ldc, bias, Z);
+}
+
+// ---- elementwise kernels ------------------------------------------------------
+// Output head: o0 -> x_HII = sigmoid; (0, o1, o2) -> He stage fractions by
+// softmax; o3 -> 4 (log10 T_e - 4).  Prediction p = (x_HII, x_HeII, x_HeIII, 4 (log T - 4)).
+__device__ __forceinline__ void head(const float* o, float* p, float* he) {
+    p[0] = 1.0f / (1.0f + expf(-o[0]));
+    const float mx = fmaxf(0.0f, fmaxf(o[1], o[2]));
+    const float e0 = expf(-mx), e1 = expf(o[1] - mx), e2 = expf(o[2] - mx);
+    const float inv = 1.0f / (e0 + e1 + e2);
+    he[0] = e0 * inv;
+    p[1] = e1 * inv;
+    p[2] = e2 * inv;
+    p[3] = o[3];
+}
+
+// Loss (mean over the batch of the mean squared error of p against y) and
+// its gradient with respect to the raw outputs, scaled by 1/B.
+__global__ void k_loss(int B, const float* __restrict__ out, const float* __restrict__ y, float* __restrict__ dout,
+                       float* __restrict__ loss) {
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    float l = 0.0f;
+    if (b < B) {
+        const float* o = out + (long long)b * kOut;
+        float p[4], he0;
+        head(o, p, &he0);
+        float dp[4];
+        for (int j = 0; j < 4; ++j) {
+            const float e = p[j] - y[(long long)b * kOut + j];
+            l += e * e * 0.25f;
+            dp[j] = 0.5f * e / (float)B;
+        }
+        float* d = dout + (long long)b * kOut;
+        d[0] = dp[0] * p[0] * (1.0f - p[0]);
+        // softmax over (0, o1, o2): dp/dz_k = p_j (delta_jk - p_k), j, k in {1, 2}
+        d[1] = dp[1] * p[1] * (1.0f - p[1]) - dp[2] * p[2] * p[1];
+        d[2] = dp[2] * p[2] * (1.0f - p[2]) - dp[1] * p[1] * p[2];
+        d[3] = dp[3];
+    }
+    for (int o = 16; o > 0; o >>= 1) l += __shfl_down_sync(0xffffffffu, l, o);
+    if ((threadIdx.x & 31) == 0 && l != 0.0f) atomicAdd(loss, l);
+}
+
+__global__ void k_gelu_back(long long n, const float* __restrict__ Z, float* __restrict__ dH) {
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        dH[i] = dH[i] * gelu_grad(Z[i]);
+}
+
+// Bias gradient: column sums of dZ [B x N].
+__global__ void k_colsum(int B, int N, const float* __restrict__ dZ, float* __restrict__ db) {
+    const int n = blockIdx.x;
+    float s = 0.0f;
+    for (int b = threadIdx.x; b < B; b += blockDim.x) s += dZ[(long long)b * N + n];
+    __shared__ float sh[256];
+    sh[threadIdx.x] = s;
+    __syncthreads();
+    for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+        if (threadIdx.x < o) sh[threadIdx.x] += sh[threadIdx.x + o];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) db[n] = sh[0];
+}
+
+__global__ void k_adam(long long n, float* __restrict__ w, const float* __restrict__ g, float* __restrict__ m,
+                       float* __restrict__ v, float lr, float b1, float b2, float c1, float c2, float eps) {
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const float gi = g[i];
+        const float mi = b1 * m[i] + (1.0f - b1) * gi;
+        const float vi = b2 * v[i] + (1.0f - b2) * gi * gi;
+        m[i] = mi;
+        v[i] = vi;
+        w[i] -= lr * (mi / c1) / (sqrtf(vi / c2) + eps);
+    }
+}
+
+__global__ void k_gather(int B, int width, const int* __restrict__ idx, const float* __restrict__ src,
+                         float* __restrict__ dst) {
+    const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= (long long)B * width) return;
+    const int b = (int)(e / width), c = (int)(e % width);
+    dst[e] = src[(long long)idx[b] * width + c];
+}
+
+// Features of one leaf (12 used, 16 wide): log Gamma_HI/HeI/HeII, log
+// photoheating HI/HeI/HeII, log n_H, the dust-absorbed power (0 without
+// dust), and the previous x_HII, x_HeII, x_HeIII and log T_e, each scaled to
+// order unity.
+__global__ void k_features(long long n, long long stride, const double* __restrict__ rates, const double* __restrict__ nH,
+                           const double* __restrict__ xHI, const double* __restrict__ xHeI,
+                           const double* __restrict__ xHeII, const double* __restrict__ Te, float* __restrict__ X) {
+    for (long long il = (long long)blockIdx.x * blockDim.x + threadIdx.x; il < n;
+         il += (long long)gridDim.x * blockDim.x) {
+        float* f = X + il * kIn;
+        for (int k = 0; k < 3; ++k) f[k] = (float)((log10(fmax(rates[k * stride + il], 1e-30)) + 10.0) / 5.0);
+        for (int k = 0; k < 3; ++k)
+            f[3 + k] = (float)((log10(fmax(rates[(3 + k) * stride + il], 1e-40)) + 21.0) / 5.0);
+        f[6] = (float)(log10(fmax(nH[il], 1e-10)) / 3.0);
+        f[7] = 0.0f;
+        const double h3 = fmax(0.0, 1.0 - xHeI[il] - xHeII[il]);
+        f[8] = (float)(1.0 - xHI[il]);
+        f[9] = (float)xHeII[il];
+        f[10] = (float)h3;
+        f[11] = (float)(4.0 * (log10(fmax(Te[il], 1.0)) - 4.0));
+        for (int k = 12; k < kIn; ++k) f[k] = 0.0f;
+    }
+}
+
+// Predictions (x_HII, x_HeII, x_HeIII, T_e) from the raw outputs; the T_e
+// column also goes to the warm-start array when given.
+__global__ void k_predict(long long n, const float* __restrict__ out, double* __restrict__ pred,
+                          double* __restrict__ twarm, double te_min, double te_max) {
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        float p[4], he0;
+        head(out + i * kOut, p, &he0);
+        const double T = pow(10.0, 4.0 + (double)p[3] / 4.0);
+        if (pred) {
+            pred[i * 4 + 0] = p[0];
+            pred[i * 4 + 1] = p[1];
+            pred[i * 4 + 2] = p[2];
+            pred[i * 4 + 3] = T;
+        }
+        if (twarm) twarm[i] = fmin(fmax(T, te_min), te_max);
+    }
+}
+
+int nb(long long n, int t) { return (int)std::min<long long>((n + t - 1) / t, 148LL * 32); }
+
+}  // namespace
+}  // namespace mochii
+
+using namespace mochii;
+
+struct mochii_mlp {
+    cudaStream_t stream = nullptr;
+    float* W[kLayers] = {};   // [out x in] row-major, FP32 masters
+    float* b[kLayers] = {};
+    float *gW[kLayers] = {}, *gb[kLayers] = {};
+    float *mW[kLayers] = {}, *vW[kLayers] = {}, *mb[kLayers] = {}, *vb[kLayers] = {};
+    // activations of the current batch: H[0] = input, H[l] = GELU(Z[l]) for l = 1..3, out
+    float* H[kLayers] = {};
+    float* Z[kLayers] = {};
+    float *out = nullptr, *dout = nullptr, *dA = nullptr, *dB2 = nullptr, *loss = nullptr;
+    int* idx = nullptr;
+    float *X = nullptr, *Y = nullptr;   // resident training set
+    long long cap = 0, nset = 0, setcap = 0;
+    long long step = 0;
+    std::string err;
+};
+
+namespace {
+
+int mlp_fail(mochii_mlp* m, int code, const std::string& msg) {
+    if (m) m->err = msg;
+    return code;
+}
+
+#define MK(call)                                                                                   \
+    do {                                                                                           \
+        cudaError_t e_ = (call);                                                                   \
+        if (e_ != cudaSuccess) return mlp_fail(m, MOCHII_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+int ensure_batch(mochii_mlp* m, long long B) {
+    if (B <= m->cap) return MOCHII_OK;
+    for (int l = 0; l < kLayers; ++l) {
+        cudaFree(m->H[l]);
+        cudaFree(m->Z[l]);
+        m->H[l] = m->Z[l] = nullptr;
+    }
+    cudaFree(m->out); cudaFree(m->dout); cudaFree(m->dA); cudaFree(m->dB2); cudaFree(m->idx);
+    m->out = m->dout = m->dA = m->dB2 = nullptr;
+    m->idx = nullptr;
+    for (int l = 0; l < kLayers; ++l) {
+        MK(cudaMalloc(&m->H[l], (size_t)B * kDim[l] * 4));
+        MK(cudaMalloc(&m->Z[l], (size_t)B * kHid * 4));
+    }
+    MK(cudaMalloc(&m->out, (size_t)B * kOut * 4));
+    MK(cudaMalloc(&m->dout, (size_t)B * kOut * 4));
+    MK(cudaMalloc(&m->dA, (size_t)B * kHid * 4));
+    MK(cudaMalloc(&m->dB2, (size_t)B * kHid * 4));
+    MK(cudaMalloc(&m->idx, (size_t)B * 4));
+    m->cap = B;
+    return MOCHII_OK;
+}
+
+// Forward of B rows already in H[0]: Z/H of the hidden layers and the raw outputs.
+void forward(mochii_mlp* m, long long B) {
+    cudaStream_t s = m->stream;
+    for (int l = 0; l < kLayers - 1; ++l)
+        gemm<EPI_BIAS_GELU>(s, (int)B, kDim[l + 1], kDim[l], m->H[l], kDim[l], 1, m->W[l], 1, kDim[l], m->H[l + 1],
+                            kDim[l + 1], m->b[l], m->Z[l + 1]);
+    gemm<EPI_BIAS>(s, (int)B, kOut, kHid, m->H[kLayers - 1], kHid, 1, m->W[kLayers - 1], 1, kHid, m->out, kOut,
+                   m->b[kLayers - 1]);
+}
+
+// Backward from dout: gW, gb of every layer.
+void backward(mochii_mlp* m, long long B) {
+    cudaStream_t s = m->stream;
+    const float* dZ = m->dout;   // gradient with respect to this layer's pre-activation
+    for (int l = kLayers - 1; l >= 0; --l) {
+        const int no = kDim[l + 1], ni = kDim[l];
+        // gW[o, i] = sum_b dZ[b, o] H_l[b, i]
+        gemm<EPI_STORE>(s, no, ni, (int)B, dZ, 1, no, m->H[l], ni, 1, m->gW[l], ni);
+        k_colsum<<<no, 256, 0, s>>>((int)B, no, dZ, m->gb[l]);
+        if (l == 0) break;
+        // dH_l[b, i] = sum_o dZ[b, o] W[o, i], then through the GELU of layer l
+        float* dH = (dZ == m->dA) ? m->dB2 : m->dA;
+        gemm<EPI_STORE>(s, (int)B, ni, no, dZ, no, 1, m->W[l], ni, 1, dH, ni);
+        k_gelu_back<<<nb((long long)B * ni, 256), 256, 0, s>>>((long long)B * ni, m->Z[l], dH);
+        dZ = dH;
+    }
+}
+
+void adam(mochii_mlp* m, float lr) {
+    ++m->step;
+    const float b1 = 0.9f, b2 = 0.999f;
+    const float c1 = 1.0f - std::pow(b1, (float)m->step), c2 = 1.0f - std::pow(b2, (float)m->step);
+    for (int l = 0; l < kLayers; ++l) {
+        const long long nw = (long long)kDim[l + 1] * kDim[l];
+        k_adam<<<nb(nw, 256), 256, 0, m->stream>>>(nw, m->W[l], m->gW[l], m->mW[l], m->vW[l], lr, b1, b2, c1, c2, 1e-8f);
+        k_adam<<<nb(kDim[l + 1], 256), 256, 0, m->stream>>>(kDim[l + 1], m->b[l], m->gb[l], m->mb[l], m->vb[l], lr, b1,
+                                                             b2, c1, c2, 1e-8f);
+    }
+}
+
+}  // namespace
+
+extern "C" int mochii_mlp_create(uint64_t seed, mochii_mlp** out) {
+    if (!out) return MOCHII_ERR_BAD_PARAM;
+    *out = nullptr;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev < 1) {
+        cudaGetLastError();
+        return MOCHII_ERR_NO_DEVICE;
+    }
+    auto* m = new mochii_mlp();
+    std::mt19937_64 rng(seed);
+    auto bail = [&](int rc) {
+        mochii_mlp_destroy(m);
+        return rc;
+    };
+    if (cudaStreamCreateWithFlags(&m->stream, cudaStreamNonBlocking) != cudaSuccess) return bail(MOCHII_ERR_CUDA);
+    for (int l = 0; l < kLayers; ++l) {
+        const int no = kDim[l + 1], ni = kDim[l];
+        std::vector<float> w((size_t)no * ni), z((size_t)no * ni, 0.0f), zb(no, 0.0f);
+        // He-uniform for the GELU layers, Glorot-uniform for the head
+        const double lim = l < kLayers - 1 ? std::sqrt(6.0 / ni) : std::sqrt(6.0 / (ni + no));
+        std::uniform_real_distribution<double> u(-lim, lim);
+        for (auto& x : w) x = (float)u(rng);
+        float** bufs[] = {&m->W[l], &m->gW[l], &m->mW[l], &m->vW[l]};
+        for (float** p : bufs)
+            if (cudaMalloc(p, w.size() * 4) != cudaSuccess) return bail(MOCHII_ERR_CUDA);
+        float** bb[] = {&m->b[l], &m->gb[l], &m->mb[l], &m->vb[l]};
+        for (float** p : bb)
+            if (cudaMalloc(p, (size_t)no * 4) != cudaSuccess) return bail(MOCHII_ERR_CUDA);
+        cudaMemcpy(m->W[l], w.data(), w.size() * 4, cudaMemcpyHostToDevice);
+        cudaMemcpy(m->mW[l], z.data(), z.size() * 4, cudaMemcpyHostToDevice);
+        cudaMemcpy(m->vW[l], z.data(), z.size() * 4, cudaMemcpyHostToDevice);
+        cudaMemcpy(m->b[l], zb.data(), no * 4, cudaMemcpyHostToDevice);
+        cudaMemcpy(m->mb[l], zb.data(), no * 4, cudaMemcpyHostToDevice);
+        cudaMemcpy(m->vb[l], zb.data(), no * 4, cudaMemcpyHostToDevice);
+    }
+    if (cudaMalloc(&m->loss, 16) != cudaSuccess) return bail(MOCHII_ERR_CUDA);
+    if (cudaDeviceSynchronize() != cudaSuccess) return bail(MOCHII_ERR_CUDA);
+    *out = m;
+    return MOCHII_OK;
+}
+
+extern "C" void mochii_mlp_destroy(mochii_mlp* m) {
+    if (!m) return;
+    if (m->stream) cudaStreamSynchronize(m->stream);
+    for (int l = 0; l < kLayers; ++l) {
+        float* ps[] = {m->W[l], m->b[l], m->gW[l], m->gb[l], m->mW[l], m->vW[l], m->mb[l], m->vb[l], m->H[l], m->Z[l]};
+        for (float* p : ps)
+            if (p) cudaFree(p);
+    }
+    for (void* p : {(void*)m->out, (void*)m->dout, (void*)m->dA, (void*)m->dB2, (void*)m->loss, (void*)m->idx,
+                    (void*)m->X, (void*)m->Y})
+        if (p) cudaFree(p);
+    if (m->stream) cudaStreamDestroy(m->stream);
+    delete m;
+}
+
+extern "C" const char* mochii_mlp_last_error(const mochii_mlp* m) { return m ? m->err.c_str() : ""; }
+
+extern "C" int64_t mochii_mlp_num_params(void) {
+    int64_t n = 0;
+    for (int l = 0; l < kLayers; ++l) n += (int64_t)kDim[l + 1] * kDim[l] + kDim[l + 1];
+    return n;
+}
+
+// Parameters in layer order, W[l] (out x in, row-major) then b[l].
+extern "C" int mochii_mlp_get_params(mochii_mlp* m, float* out) {
+    if (!m || !out) return MOCHII_ERR_BAD_PARAM;
+    for (int l = 0; l < kLayers; ++l) {
+        const size_t nw = (size_t)kDim[l + 1] * kDim[l];
+        MK(cudaMemcpy(out, m->W[l], nw * 4, cudaMemcpyDeviceToHost));
+        out += nw;
+        MK(cudaMemcpy(out, m->b[l], kDim[l + 1] * 4, cudaMemcpyDeviceToHost));
+        out += kDim[l + 1];
+    }
+    return MOCHII_OK;
+}
+
+extern "C" int mochii_mlp_set_params(mochii_mlp* m, const float* in) {
+    if (!m || !in) return MOCHII_ERR_BAD_PARAM;
+    for (int l = 0; l < kLayers; ++l) {
+        const size_t nw = (size_t)kDim[l + 1] * kDim[l];
+        MK(cudaMemcpy(m->W[l], in, nw * 4, cudaMemcpyHostToDevice));
+        in += nw;
+        MK(cudaMemcpy(m->b[l], in, kDim[l + 1] * 4, cudaMemcpyHostToDevice));
+        in += kDim[l + 1];
+    }
+    return MOCHII_OK;
+}
+
+// Gradients of the loss over one batch of n rows (no update): same layout as
+// the parameters; *loss = the batch loss.
+extern "C" int mochii_mlp_gradients(mochii_mlp* m, const float* X, const float* Y, int64_t n, float* grads,
+                                    float* loss) {
+    if (!m || !X || !Y || !grads || n < 1 || n > (1 << 22)) return MOCHII_ERR_BAD_PARAM;
+    int rc = ensure_batch(m, n);
+    if (rc) return rc;
+    float* dy = nullptr;
+    MK(cudaMallocAsync(&dy, (size_t)n * kOut * 4, m->stream));
+    MK(cudaMemcpyAsync(m->H[0], X, (size_t)n * kIn * 4, cudaMemcpyHostToDevice, m->stream));
+    MK(cudaMemcpyAsync(dy, Y, (size_t)n * kOut * 4, cudaMemcpyHostToDevice, m->stream));
+    MK(cudaMemsetAsync(m->loss, 0, 4, m->stream));
+    forward(m, n);
+    k_loss<<<(int)((n + 255) / 256), 256, 0, m->stream>>>((int)n, m->out, dy, m->dout, m->loss);
+    backward(m, n);
+    MK(cudaGetLastError());
+    for (int l = 0; l < kLayers; ++l) {
+        const size_t nw = (size_t)kDim[l + 1] * kDim[l];
+        MK(cudaMemcpyAsync(grads, m->gW[l], nw * 4, cudaMemcpyDeviceToHost, m->stream));
+        grads += nw;
+        MK(cudaMemcpyAsync(grads, m->gb[l], kDim[l + 1] * 4, cudaMemcpyDeviceToHost, m->stream));
+        grads += kDim[l + 1];
+    }
+    float lh = 0.0f;
+    MK(cudaMemcpyAsync(&lh, m->loss, 4, cudaMemcpyDeviceToHost, m->stream));
+    MK(cudaFreeAsync(dy, m->stream));
+    MK(cudaStreamSynchronize(m->stream));
+    if (loss) *loss = lh / (float)n;
+    return MOCHII_OK;
+}
+
+// Train on n (features, target) rows: epochs of shuffled mini-batches with
+// Adam.  The set is uploaded once and stays on the device; losses[e] = the
+// mean batch loss of epoch e.
+extern "C" int mochii_mlp_train(mochii_mlp* m, const float* X, const float* Y, int64_t n, int epochs, int batch,
+                                float lr, uint64_t seed, float* losses) {
+    if (!m || !X || !Y || n < 1 || epochs < 1 || batch < 16 || batch > (1 << 20)) return MOCHII_ERR_BAD_PARAM;
+    int rc = ensure_batch(m, batch);
+    if (rc) return rc;
+    if (n > m->setcap) {
+        cudaFree(m->X);
+        cudaFree(m->Y);
+        m->X = m->Y = nullptr;
+        MK(cudaMalloc(&m->X, (size_t)n * kIn * 4));
+        MK(cudaMalloc(&m->Y, (size_t)n * kOut * 4));
+        m->setcap = n;
+    }
+    MK(cudaMemcpyAsync(m->X, X, (size_t)n * kIn * 4, cudaMemcpyHostToDevice, m->stream));
+    MK(cudaMemcpyAsync(m->Y, Y, (size_t)n * kOut * 4, cudaMemcpyHostToDevice, m->stream));
+    std::mt19937_64 rng(seed);
+    std::vector<int> perm(n);
+    for (int64_t i = 0; i < n; ++i) perm[i] = (int)i;
+    float* ybatch = nullptr;
+    MK(cudaMallocAsync(&ybatch, (size_t)batch * kOut * 4, m->stream));
+    int* dperm = nullptr;
+    MK(cudaMallocAsync(&dperm, (size_t)n * 4, m->stream));
+    for (int e = 0; e < epochs; ++e) {
+        std::shuffle(perm.begin(), perm.end(), rng);
+        MK(cudaMemcpyAsync(dperm, perm.data(), (size_t)n * 4, cudaMemcpyHostToDevice, m->stream));
+        MK(cudaMemsetAsync(m->loss, 0, 4, m->stream));
+        long long nbatch = 0;
+        for (int64_t b0 = 0; b0 + batch <= n; b0 += batch, ++nbatch) {
+            const int* ib = dperm + b0;
+            k_gather<<<(batch * kIn + 255) / 256, 256, 0, m->stream>>>(batch, kIn, ib, m->X, m->H[0]);
+            k_gather<<<(batch * kOut + 255) / 256, 256, 0, m->stream>>>(batch, kOut, ib, m->Y, ybatch);
+            forward(m, batch);
+            k_loss<<<(batch + 255) / 256, 256, 0, m->stream>>>(batch, m->out, ybatch, m->dout, m->loss);
+            backward(m, batch);
+            adam(m, lr);
+        }
+        float lh = 0.0f;
+        MK(cudaMemcpyAsync(&lh, m->loss, 4, cudaMemcpyDeviceToHost, m->stream));
+        MK(cudaStreamSynchronize(m->stream));
+        MK(cudaGetLastError());
+        if (losses) losses[e] = nbatch ? lh / (float)(nbatch * batch) : 0.0f;
+    }
+    MK(cudaFreeAsync(ybatch, m->stream));
+    MK(cudaFreeAsync(dperm, m->stream));
+    MK(cudaStreamSynchronize(m->stream));
+    return MOCHII_OK;
+}
+
+// Predictions for n rows of features: (x_HII, x_HeII, x_HeIII, T_e) per row.
+extern "C" int mochii_mlp_predict(mochii_mlp* m, const float* X, int64_t n, double* out4) {
+    if (!m || !X || !out4 || n < 1) return MOCHII_ERR_BAD_PARAM;
+    const long long chunk = 1 << 20;
+    int rc = ensure_batch(m, std::min<long long>(n, chunk));
+    if (rc) return rc;
+    double* d = nullptr;
+    MK(cudaMallocAsync(&d, (size_t)std::min<long long>(n, chunk) * 32, m->stream));
+    for (long long i0 = 0; i0 < n; i0 += chunk) {
+        const long long c = std::min<long long>(chunk, n - i0);
+        MK(cudaMemcpyAsync(m->H[0], X + i0 * kIn, (size_t)c * kIn * 4, cudaMemcpyHostToDevice, m->stream));
+        forward(m, c);
+        k_predict<<<nb(c, 256), 256, 0, m->stream>>>(c, m->out, d, nullptr, 0.0, 0.0);
+        MK(cudaMemcpyAsync(out4 + i0 * 4, d, (size_t)c * 32, cudaMemcpyDeviceToHost, m->stream));
+    }
+    MK(cudaFreeAsync(d, m->stream));
+    MK(cudaStreamSynchronize(m->stream));
+    MK(cudaGetLastError());
+    return MOCHII_OK;
+}
+
+// Features of every leaf of a nebula (nleaf x 16 floats), for training sets.
+extern "C" int mochii_mlp_features(mochii_ctx* c, float* out) {
+    if (!c || !out) return MOCHII_ERR_BAD_PARAM;
+    const long long n = c->grid.nleaf;
+    float* d = nullptr;
+    if (cudaMallocAsync(&d, (size_t)n * kIn * 4, c->stream) != cudaSuccess) return MOCHII_ERR_CUDA;
+    k_features<<<nb(n, 256), 256, 0, c->stream>>>(n, n, c->rates, c->nH, c->xHI, c->xHeI, c->xHeII, c->Te, d);
+    cudaMemcpyAsync(out, d, (size_t)n * kIn * 4, cudaMemcpyDeviceToHost, c->stream);
+    cudaFreeAsync(d, c->stream);
+    return cudaStreamSynchronize(c->stream) == cudaSuccess && cudaGetLastError() == cudaSuccess ? MOCHII_OK
+                                                                                                : MOCHII_ERR_CUDA;
+}
+
+// The warm start of the next thermal update: features of every leaf from the
+// nebula's current rates and state, inference, and the predicted T_e (clamped
+// to [te_min, te_max]) as the bracketed solve's starting point.  All on the
+// device; the MLP's stream is ordered after the nebula's work.
+extern "C" int mochii_mlp_warm_start(mochii_ctx* c, mochii_mlp* m) {
+    if (!c || !m) return MOCHII_ERR_BAD_PARAM;
+    const long long n = c->grid.nleaf, chunk = 1 << 20;
+    int rc = ensure_batch(m, std::min<long long>(n, chunk));
+    if (rc) return rc;
+    if (!c->twarm && cudaMalloc(&c->twarm, (size_t)n * 8 + 16) != cudaSuccess) return MOCHII_ERR_CUDA;
+    if (cudaStreamSynchronize(c->stream) != cudaSuccess) return MOCHII_ERR_CUDA;
+    for (long long i0 = 0; i0 < n; i0 += chunk) {
+        const long long k = std::min<long long>(chunk, n - i0);
+        // features of leaves i0..i0+k-1 straight into the input buffer
+        k_features<<<nb(k, 256), 256, 0, m->stream>>>(k, n, c->rates + i0, c->nH + i0, c->xHI + i0, c->xHeI + i0,
+                                                      c->xHeII + i0, c->Te + i0, m->H[0]);
+        forward(m, k);
+        k_predict<<<nb(k, 256), 256, 0, m->stream>>>(k, m->out, nullptr, c->twarm + i0, c->par.te_min, c->par.te_max);
+    }
+    MK(cudaStreamSynchronize(m->stream));
+    MK(cudaGetLastError());
+    c->twarm_set = true;
+    return MOCHII_OK;
+}
