@@ -266,6 +266,7 @@ def main():
     ap.add_argument("--impl", default="mochii_b200")
     ap.add_argument("--workload", default="hii_metals128", choices=["hii_metals128", "stromgren64"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-converge", action="store_true", help="skip the time-to-converged comparison")
     ap.add_argument("--precision", default=None, choices=["fp64", "fp32"],
                     help="transport arithmetic (default: the workload's)")
     ap.add_argument("--solver", default="bracketed", choices=["bisection", "bracketed"],
@@ -394,6 +395,10 @@ def main():
         v, desc, _ = cpu_reference(wl, state, nthreads)
         cpu = {"value": v, "unit": UNIT, "cores": nthreads, "kind": "port", "sample": desc}
 
+    conv = None
+    if rank == 0 and not args.no_converge and wl.name == "hii_metals128":
+        conv = time_to_converged()
+
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -415,6 +420,7 @@ def main():
                          "bytes_per_segment": alg_bytes / mean_seg, "segments_per_launch": mean_seg,
                          "kernel_ms": mean_ms},
             "cpu_baseline": cpu,
+            "time_to_converged": conv,
             "clocks": clk.summary(),
             "gpu_launches": int(sum(launches_per_step(wl, n_ - wl.nphot) for n_ in npk)),
             "breakdown_ms": {"transport": float(np.mean(pass_ms)), "balance": float(np.mean(bal_ms))},
@@ -426,6 +432,67 @@ def main():
         dist.barrier()
         dist.destroy_process_group()
     return 0
+
+
+def time_to_converged(n=64, nphot=1_000_000, iters=20, train_iters=10, seed_train=777, seed=12345):
+    """Time to a converged nebula of the metals H II-region class (n^3, the
+    128^3 workload's physics): `iters` transport + thermal iterations from the
+    ionized start with the reference's solver (damped n_e fixed point,
+    bisection on T_e) against the bracketed solver warm-started by the MLP.
+    The MLP is trained first on the plain solver's (features, solved state)
+    pairs of another nebula of the class (launch seed seed_train).  Device
+    time from the library's CUDA events; the accuracy is the largest |dx_HII|
+    and |dT_e| between the two final states."""
+    from mochii_b200 import Nebula, configs, parse_namelist
+    from mochii_b200.mlp import WarmStartMLP
+
+    def neb_of(solver, sd):
+        nl = configs.hii_metals(nphotons=nphot, niter=iters, n=n, precision="fp32", seed=sd)
+        return Nebula(parse_namelist(nl.replace("/\n", f" par%thermal_solver = '{solver}'\n/\n")))
+
+    t0 = time.perf_counter()
+    X, Y = [], []
+    neb = neb_of("bisection", seed_train)
+    for _ in range(train_iters):
+        neb.ionizing_field_and_rates()
+        X.append(WarmStartMLP.features(neb))
+        neb.gas_thermal_update()
+        Y.append(WarmStartMLP.targets(neb))
+    neb.close()
+    X, Y = np.concatenate(X), np.concatenate(Y)
+    t_data = time.perf_counter() - t0
+    mlp = WarmStartMLP(seed=1)
+    t0 = time.perf_counter()
+    losses = mlp.train(X, Y, epochs=20, batch=4096, lr=2e-3, seed=2)
+    t_train = time.perf_counter() - t0
+    res = {}
+    for mode in ("plain", "bracketed", "mlp"):
+        neb = neb_of("bisection" if mode == "plain" else "bracketed", seed)
+        ms, evals = 0.0, 0
+        for _ in range(iters):
+            st = neb.ionizing_field_and_rates()
+            ms += st.pass_ms
+            if mode == "mlp":
+                e0 = time.perf_counter()
+                mlp.warm_start(neb)          # synchronous: device inference + features
+                ms += (time.perf_counter() - e0) * 1e3
+            neb.gas_thermal_update()
+            ms += neb.last_metrics.kernel_ms
+            evals += neb.last_metrics.rate_evaluations
+        res[mode] = (ms / 1e3, evals, neb.get("x_HI"), neb.get("T_e"))
+        neb.close()
+    mlp.close()
+    dx = lambda a, b: float(np.max(np.abs(res[a][2] - res[b][2])))
+    dT = lambda a, b: float(np.max(np.abs(res[a][3] - res[b][3])))
+    return {"config": f"hii_metals {n}^3, {nphot:.0e} packets, {iters} iterations, FP32 transport",
+            "plain_s": res["plain"][0], "bracketed_s": res["bracketed"][0], "mlp_s": res["mlp"][0],
+            "speedup_mlp_vs_plain": res["plain"][0] / res["mlp"][0],
+            "speedup_bracketed_vs_plain": res["plain"][0] / res["bracketed"][0],
+            "net_rate_evaluations": {k: v[1] for k, v in res.items()},
+            "max_dx_HII_vs_plain": {"bracketed": dx("bracketed", "plain"), "mlp": dx("mlp", "plain")},
+            "max_dT_e_vs_plain_K": {"bracketed": dT("bracketed", "plain"), "mlp": dT("mlp", "plain")},
+            "training": {"pairs": int(len(X)), "data_s": t_data, "train_s": t_train, "epochs": 20,
+                         "loss_first": float(losses[0]), "loss_last": float(losses[-1])}}
 
 
 def launches_per_step(wl, diffuse_packets):
