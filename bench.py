@@ -457,7 +457,7 @@ def time_to_converged(n=64, nphot=1_000_000, iters=20, train_iters=10, seed_trai
         neb.ionizing_field_and_rates()
         X.append(WarmStartMLP.features(neb))
         neb.gas_thermal_update()
-        Y.append(WarmStartMLP.targets(neb))
+        Y.append(WarmStartMLP.targets(neb, X[-1]))
     neb.close()
     X, Y = np.concatenate(X), np.concatenate(Y)
     t_data = time.perf_counter() - t0
@@ -482,15 +482,23 @@ def time_to_converged(n=64, nphot=1_000_000, iters=20, train_iters=10, seed_trai
         res[mode] = (ms / 1e3, evals, neb.get("x_HI"), neb.get("T_e"))
         neb.close()
     mlp.close()
-    dx = lambda a, b: float(np.max(np.abs(res[a][2] - res[b][2])))
-    dT = lambda a, b: float(np.max(np.abs(res[a][3] - res[b][3])))
+    def stats(a, b, k):
+        d = np.abs(res[a][k] - res[b][k])
+        return {"p50": float(np.percentile(d, 50)), "p99": float(np.percentile(d, 99)), "max": float(d.max())}
+
+    def glob(a):
+        x, T = res[a][2], res[a][3]
+        return {"ionized_fraction": float(np.mean(1 - x)), "mean_T_e_ionized": float(np.mean(T[x < 0.5]))}
     return {"config": f"hii_metals {n}^3, {nphot:.0e} packets, {iters} iterations, FP32 transport",
             "plain_s": res["plain"][0], "bracketed_s": res["bracketed"][0], "mlp_s": res["mlp"][0],
             "speedup_mlp_vs_plain": res["plain"][0] / res["mlp"][0],
             "speedup_bracketed_vs_plain": res["plain"][0] / res["bracketed"][0],
             "net_rate_evaluations": {k: v[1] for k, v in res.items()},
-            "max_dx_HII_vs_plain": {"bracketed": dx("bracketed", "plain"), "mlp": dx("mlp", "plain")},
-            "max_dT_e_vs_plain_K": {"bracketed": dT("bracketed", "plain"), "mlp": dT("mlp", "plain")},
+            "dx_HII_vs_plain": {"bracketed": stats("bracketed", "plain", 2), "mlp": stats("mlp", "plain", 2)},
+            "dT_e_vs_plain_K": {"bracketed": stats("bracketed", "plain", 3), "mlp": stats("mlp", "plain", 3)},
+            "global": {k: glob(k) for k in res},
+            "note": "final states after the same iterations; the solvers agree per iteration (tests), the coupled "
+                    "iteration then carries Monte Carlo differences at the ionization front",
             "training": {"pairs": int(len(X)), "data_s": t_data, "train_s": t_train, "epochs": 20,
                          "loss_first": float(losses[0]), "loss_last": float(losses[-1])}}
 

@@ -278,7 +278,8 @@ int mochii_launch_records_noalloc(mochii_ctx* ctx, int64_t ip0, int64_t n, doubl
  * (16 floats, 12 used): log Gamma_HI/HeI/HeII, log heating HI/HeI/HeII,
  * log n_H, dust-absorbed power, previous x_HII, x_HeII, x_HeIII, log T_e,
  * each scaled to order one (mochii_mlp_features).  Targets per leaf (4
- * floats): x_HII, x_HeII, x_HeIII, 4 (log10 T_e - 4). */
+ * floats): x_HII, x_HeII, x_HeIII and the change of T_e over the iteration,
+ * 4 (log10 T_e - log10 T_e,prev), with T_e,prev = 10^(4 + feature_11/4). */
 typedef struct mochii_mlp mochii_mlp;
 int mochii_mlp_create(uint64_t seed, mochii_mlp** out);
 void mochii_mlp_destroy(mochii_mlp* m);

@@ -135,7 +135,8 @@ void gemm(cudaStream_t s, int M, int N, int K, const float* A, long long am, lon
 
 // ---- elementwise kernels ------------------------------------------------------
 // Output head: o0 -> x_HII = sigmoid; (0, o1, o2) -> He stage fractions by
-// softmax; o3 -> 4 (log10 T_e - 4).  Prediction p = (x_HII, x_HeII, x_HeIII, 4 (log T - 4)).
+// softmax; o3 -> the change of T_e over the iteration, 4 (log10 T_e -
+// log10 T_e,prev).  Prediction p = (x_HII, x_HeII, x_HeIII, 4 dlog T).
 __device__ __forceinline__ void head(const float* o, float* p, float* he) {
     p[0] = 1.0f / (1.0f + expf(-o[0]));
     const float mx = fmaxf(0.0f, fmaxf(o[1], o[2]));
@@ -238,14 +239,15 @@ __global__ void k_features(long long n, long long stride, const double* __restri
     }
 }
 
-// Predictions (x_HII, x_HeII, x_HeIII, T_e) from the raw outputs; the T_e
-// column also goes to the warm-start array when given.
-__global__ void k_predict(long long n, const float* __restrict__ out, double* __restrict__ pred,
-                          double* __restrict__ twarm, double te_min, double te_max) {
+// Predictions (x_HII, x_HeII, x_HeIII, T_e) from the raw outputs and the
+// features (the previous T_e is feature 11); the T_e column also goes to the
+// warm-start array when given.
+__global__ void k_predict(long long n, const float* __restrict__ out, const float* __restrict__ X,
+                          double* __restrict__ pred, double* __restrict__ twarm, double te_min, double te_max) {
     for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
         float p[4], he0;
         head(out + i * kOut, p, &he0);
-        const double T = pow(10.0, 4.0 + (double)p[3] / 4.0);
+        const double T = pow(10.0, 4.0 + ((double)X[i * kIn + 11] + (double)p[3]) / 4.0);
         if (pred) {
             pred[i * 4 + 0] = p[0];
             pred[i * 4 + 1] = p[1];
@@ -541,7 +543,7 @@ extern "C" int mochii_mlp_predict(mochii_mlp* m, const float* X, int64_t n, doub
         const long long c = std::min<long long>(chunk, n - i0);
         MK(cudaMemcpyAsync(m->H[0], X + i0 * kIn, (size_t)c * kIn * 4, cudaMemcpyHostToDevice, m->stream));
         forward(m, c);
-        k_predict<<<nb(c, 256), 256, 0, m->stream>>>(c, m->out, d, nullptr, 0.0, 0.0);
+        k_predict<<<nb(c, 256), 256, 0, m->stream>>>(c, m->out, m->H[0], d, nullptr, 0.0, 0.0);
         MK(cudaMemcpyAsync(out4 + i0 * 4, d, (size_t)c * 32, cudaMemcpyDeviceToHost, m->stream));
     }
     MK(cudaFreeAsync(d, m->stream));
@@ -580,7 +582,8 @@ extern "C" int mochii_mlp_warm_start(mochii_ctx* c, mochii_mlp* m) {
         k_features<<<nb(k, 256), 256, 0, m->stream>>>(k, n, c->rates + i0, c->nH + i0, c->xHI + i0, c->xHeI + i0,
                                                       c->xHeII + i0, c->Te + i0, m->H[0]);
         forward(m, k);
-        k_predict<<<nb(k, 256), 256, 0, m->stream>>>(k, m->out, nullptr, c->twarm + i0, c->par.te_min, c->par.te_max);
+        k_predict<<<nb(k, 256), 256, 0, m->stream>>>(k, m->out, m->H[0], nullptr, c->twarm + i0, c->par.te_min,
+                                                     c->par.te_max);
     }
     MK(cudaStreamSynchronize(m->stream));
     MK(cudaGetLastError());

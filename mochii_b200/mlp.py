@@ -13,7 +13,7 @@ solver evaluations, never accuracy.
         neb.ionizing_field_and_rates()
         X.append(WarmStartMLP.features(neb))
         neb.gas_thermal_update()
-        Y.append(WarmStartMLP.targets(neb))
+        Y.append(WarmStartMLP.targets(neb, X[-1]))
     mlp.train(np.concatenate(X), np.concatenate(Y), epochs=20)
     neb.ionizing_field_and_rates()
     mlp.warm_start(neb)                            # predicted T_e -> the solver
@@ -106,8 +106,11 @@ class WarmStartMLP:
         return X
 
     @staticmethod
-    def targets(neb):
-        """The solved state as training targets: x_HII, x_HeII, x_HeIII, 4 (log10 T_e - 4)."""
+    def targets(neb, X):
+        """The solved state as training targets for the features X taken
+        before the solve: x_HII, x_HeII, x_HeIII and 4 (log10 T_e - log10
+        T_e,prev), the previous T_e being the one feature 11 encodes."""
         xHI, h1, h2, T = neb.get("x_HI"), neb.get("x_HeI"), neb.get("x_HeII"), neb.get("T_e")
-        return np.stack([1.0 - xHI, h2, np.maximum(0.0, 1.0 - h1 - h2), 4.0 * (np.log10(T) - 4.0)],
+        lprev = 4.0 + X[:, 11].astype(np.float64) / 4.0
+        return np.stack([1.0 - xHI, h2, np.maximum(0.0, 1.0 - h1 - h2), 4.0 * (np.log10(T) - lprev)],
                         axis=1).astype(np.float32)

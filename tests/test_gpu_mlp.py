@@ -57,7 +57,7 @@ def test_predictions_match_oracle():
     _, _, out = mlp_ref.forward(mlp.params().astype(np.float64), X.astype(np.float64))
     po = mlp_ref.head(out)
     np.testing.assert_allclose(pred[:, :3], po[:, :3], atol=1e-2)
-    np.testing.assert_allclose(np.log10(pred[:, 3]), 4.0 + po[:, 3] / 4.0, atol=1e-2)
+    np.testing.assert_allclose(np.log10(pred[:, 3]), 4.0 + (X[:, 11] + po[:, 3]) / 4.0, atol=1e-2)
     mlp.close()
 
 
@@ -89,7 +89,7 @@ def test_warm_start_gain():
         neb.ionizing_field_and_rates()
         X.append(WarmStartMLP.features(neb))
         neb.gas_thermal_update()
-        Y.append(WarmStartMLP.targets(neb))
+        Y.append(WarmStartMLP.targets(neb, X[-1]))
     neb.close()
     X, Y = np.concatenate(X), np.concatenate(Y)
     mlp = WarmStartMLP(seed=1)
