@@ -533,7 +533,7 @@ __device__ double net_rate(const ThArgs& a, long long il, double T, double nH, d
 
 // The bracketed T_e solve (solver_bracketed): the root of net(T) that the
 // reference's bisection on [te_min, te_max] converges to, found from a warm
-// start T_w.  net(T_w) gives the direction; geometric steps in ln T (x1.02,
+// start T_w.  net(T_w) gives the direction; geometric steps in ln T (x1.05,
 // squared each step) bracket the sign change, or reach te_min with net <= 0
 // (the reference's "cooling wins at te_min") or te_max with net >= 0; then
 // safeguarded false position in ln T until the bracket is below 1e-5 in ln T
@@ -547,7 +547,7 @@ __device__ double thermal_bracketed(const ThArgs& a, long long il, double nH, do
     ++*nev;
     if (fa == 0.0) return ta;
     if ((ta <= lo_lim && fa < 0.0) || (ta >= hi_lim && fa > 0.0)) return ta;   // pinned at a limit
-    double tb = ta, fb = fa, fac = 1.02;
+    double tb = ta, fb = fa, fac = 1.05;
     for (int s = 0; s < 40; ++s) {
         tb = fa > 0.0 ? fmin(ta * fac, hi_lim) : fmax(ta / fac, lo_lim);
         fb = net_rate(a, il, tb, nH, xHI, xHeI, xHeII, ne, passes, mc, nsum);
