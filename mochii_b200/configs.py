@@ -194,3 +194,22 @@ def hhe128(nphotons=10_000_000, niter=20, n=128, precision="fp32", seed=12345, r
  par%precision = '{precision}'
 /
 """
+
+
+def on_octree(namelist, amr_file, density_from_file=True):
+    """The same nebula on an octree read from a generic text leaf list
+    (grid_type = 'amr'): the box side comes from the file, and with
+    density_from_file the leaves keep the file's n_H (the namelist's
+    par%nH_const line is dropped)."""
+    out = []
+    for line in namelist.splitlines():
+        key = line.strip().split("=")[0].strip()
+        if key in ("par%grid_type", "par%car_walk", "par%nx", "par%ny", "par%nz", "par%xmax", "par%ymax", "par%zmax"):
+            continue
+        if density_from_file and key == "par%nH_const":
+            continue
+        if line.strip() == "/":
+            out.append(" par%grid_type = 'amr'")
+            out.append(f" par%amr_file = '{amr_file}'")
+        out.append(line)
+    return "\n".join(out) + "\n"

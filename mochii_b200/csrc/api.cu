@@ -77,7 +77,7 @@ void release(mochii_ctx* c) {
                     c->dif.ch, c->dif.tot, c->dif.scan_tmp, c->dif.tables,
                     (void*)c->metal.el, c->metal.egam, c->metal.eheat, c->metal.opac, c->metal.raw,
                     (void*)c->metal.medge, c->metal.mom, c->twarm,
-                    (void*)c->rec.E, c->rec.msig};
+                    (void*)c->rec.E, c->rec.msig, c->oct_blob};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     for (cudaEvent_t e : {c->ev0, c->ev1, c->evA, c->evB})
@@ -101,9 +101,9 @@ int validate(const mochii_params& p, std::string* why, int* code) {
     if (p.te_fixed <= 0.0) return *why = "par%te_fixed must be positive", 1;
     if (p.solve_te && !(p.te_min > 0.0 && p.te_max > p.te_min)) return *why = "need 0 < par%te_min < par%te_max", 1;
     if (p.He_abund < 0.0) return *why = "par%He_abund must be >= 0", 1;
+    if (!p.grid_car && !p.amr_file[0]) return *why = "grid_type='amr' needs par%amr_file (a text leaf list)", 1;
     *code = MOCHII_ERR_UNSUPPORTED;
-    if (!p.grid_car) return *why = "grid_type='amr' (octree leaf list) is not built in this library version", 1;
-    if (!p.car_walk_dda) return *why = "car_walk='amr' is not built; use the DDA walk (car_walk='dda')", 1;
+    if (p.grid_car && !p.car_walk_dda) return *why = "car_walk='amr' is not built; use the DDA walk (car_walk='dda')", 1;
     if (!p.source_point) return *why = "only internal point sources are built", 1;
     if (!p.launch_sobol) return *why = "launch_sequence='random' is not built; use 'sobol'", 1;
     if (p.ion_add_dust) return *why = "ion_add_dust is not built in this library version", 1;
@@ -161,14 +161,37 @@ extern "C" int mochii_init(const mochii_params* pin, mochii_ctx** out) {
         return fail(nullptr, MOCHII_ERR_BAD_PARAM, why);
     }
     cudaGetDevice(&c->device);
-    // namelist car grid, grid_mod_amr.f90:64-133 and amr_build_car (octree_mod.f90:648-674)
     Grid& g = c->grid;
-    g.nx = p.nx; g.ny = p.ny; g.nz = p.nz;
-    g.nleaf = (long long)p.nx * p.ny * p.nz;
-    g.xmin = -p.xmax; g.xmax = p.xmax;
-    g.ymin = -p.ymax; g.ymax = p.ymax;
-    g.zmin = -p.zmax; g.zmax = p.zmax;
-    g.dcell = (g.xmax - g.xmin) / (double)g.nx;
+    // octree from a text leaf list (grid_mod_amr.f90:50-62, read_generic_amr.f90:60-81,
+    // octree_mod.f90:342-479): leaf centres, levels and n_H from the file
+    std::vector<double> lx, ly, lz, lnH;
+    OctHost oh;
+    if (!p.grid_car) {
+        std::vector<int> lev;
+        double boxlen = 0.0;
+        if (!leaf_list_read(p.amr_file, lx, ly, lz, lev, lnH, &boxlen, &why) ||
+            !octree_build(lx, ly, lz, lev, 0.5 * boxlen, oh, &why)) {
+            delete c;
+            return fail(nullptr, MOCHII_ERR_BAD_PARAM, why);
+        }
+        const double half = 0.5 * boxlen;
+        p.xmax = p.ymax = p.zmax = half;
+        g.nx = g.ny = g.nz = 0;
+        g.nleaf = oh.nleaf;
+        g.xmin = g.ymin = g.zmin = -half;
+        g.xmax = g.ymax = g.zmax = half;
+        g.dcell = 0.0;
+        c->lhalf.resize(oh.nleaf);
+        for (int l = 0; l < oh.nleaf; ++l) c->lhalf[l] = oh.lgeo[4 * (size_t)l + 3];
+    } else {
+        // namelist car grid, grid_mod_amr.f90:64-133 and amr_build_car (octree_mod.f90:648-674)
+        g.nx = p.nx; g.ny = p.ny; g.nz = p.nz;
+        g.nleaf = (long long)p.nx * p.ny * p.nz;
+        g.xmin = -p.xmax; g.xmax = p.xmax;
+        g.ymin = -p.ymax; g.ymax = p.ymax;
+        g.zmin = -p.zmax; g.zmax = p.zmax;
+        g.dcell = (g.xmax - g.xmin) / (double)g.nx;
+    }
     c->fp32 = p.precision == MOCHII_PREC_FP32;
     c->nabs = p.He_abund > 0.0 ? 4 : 1;
     c->ntally = p.He_abund > 0.0 ? 6 : 2;
@@ -196,7 +219,38 @@ extern "C" int mochii_init(const mochii_params* pin, mochii_ctx** out) {
     // leaf state (gas_state_setup, gas_state_mod.f90:58-77) on the host
     std::vector<double> nH(n, 1.0), xHI(n, p.xHI_init), xHeI(n, p.xHeI_init), xHeII(n, p.xHeII_init), ne(n),
         Te(n, p.te_fixed);
-    {
+    if (!p.grid_car) {   // the file's n_H, then the namelist density model on the file's leaf centres
+        for (long long il = 0; il < n; ++il) {
+            nH[il] = lnH[il];
+            if (p.nH_const >= 0.0) nH[il] = p.nH_const;   // grid_mod_amr.f90:137-147
+            if (p.rmax > 0.0 || p.rmin > 0.0) {
+                const double rho = std::sqrt(lx[il] * lx[il] + ly[il] * ly[il] + lz[il] * lz[il]);
+                if (p.rmax > 0.0 && rho > p.rmax) nH[il] = 0.0;
+                if (p.rmin > 0.0 && rho < p.rmin) nH[il] = 0.0;
+            }
+        }
+        for (long long i = 0; i < n; ++i)
+            ne[i] = nH[i] * ((1.0 - xHI[i]) + p.He_abund * (xHeII[i] + 2.0 * std::max(0.0, 1.0 - xHeI[i] - xHeII[i])));
+        // the octree tables in one allocation: cell geo | children | leaf of cell | leaf geo | leaf faces
+        const size_t nc = oh.ncells, nl = oh.nleaf;
+        auto al = [](size_t b) { return (b + 255) & ~(size_t)255; };
+        const size_t b_geo = al(nc * 32), b_ch = al(nc * 32), b_il = al(nc * 4), b_lg = al(nl * 32), b_ln = al(nl * 32);
+        CKI(cudaMalloc(&c->oct_blob, b_geo + b_ch + b_il + b_lg + b_ln));
+        char* base = static_cast<char*>(c->oct_blob);
+        CKI(cudaMemcpy(base, oh.geo.data(), nc * 32, cudaMemcpyHostToDevice));
+        CKI(cudaMemcpy(base + b_geo, oh.children.data(), nc * 32, cudaMemcpyHostToDevice));
+        CKI(cudaMemcpy(base + b_geo + b_ch, oh.ileaf.data(), nc * 4, cudaMemcpyHostToDevice));
+        CKI(cudaMemcpy(base + b_geo + b_ch + b_il, oh.lgeo.data(), nl * 32, cudaMemcpyHostToDevice));
+        CKI(cudaMemcpy(base + b_geo + b_ch + b_il + b_lg, oh.lnext.data(), nl * 32, cudaMemcpyHostToDevice));
+        c->oct.ncells = oh.ncells;
+        c->oct.nshared = oh.nshared;
+        c->oct.half = oh.half;
+        c->oct.geo = reinterpret_cast<const double4*>(base);
+        c->oct.children = reinterpret_cast<const int*>(base + b_geo);
+        c->oct.ileaf = reinterpret_cast<const int*>(base + b_geo + b_ch);
+        c->oct.lgeo = reinterpret_cast<const double4*>(base + b_geo + b_ch + b_il);
+        c->oct.lnext = reinterpret_cast<const int*>(base + b_geo + b_ch + b_il + b_lg);
+    } else {
         const double dcx = 2.0 * p.xmax / p.nx, dcy = 2.0 * p.ymax / p.ny, dcz = 2.0 * p.zmax / p.nz;
         long long il = 0;
         for (int iz = 0; iz < p.nz; ++iz)
@@ -561,8 +615,8 @@ std::string tune_key(const mochii_ctx* c) {
     cudaDeviceProp prop;
     cudaGetDeviceProperties(&prop, c->device);
     char buf[512];
-    std::snprintf(buf, sizeof(buf), "%s|%dx%dx%d|%d|%d|%d|%d", prop.name, c->grid.nx, c->grid.ny, c->grid.nz,
-                  c->fp32 ? 32 : 64, c->nabs, c->nnu, c->metal.ntr);
+    std::snprintf(buf, sizeof(buf), "%s|%dx%dx%d|%lld|%d|%d|%d|%d", prop.name, c->grid.nx, c->grid.ny, c->grid.nz,
+                  c->grid.nleaf, c->fp32 ? 32 : 64, c->nabs, c->nnu, c->metal.ntr);
     return buf;
 }
 }  // namespace
@@ -655,7 +709,8 @@ extern "C" int mochii_get_field(mochii_ctx* c, const char* name, double* out, in
     }
     if (nm == "leaf_half") {
         if (n != c->grid.nleaf) return fail(c, MOCHII_ERR_BAD_PARAM, "leaf_half size mismatch");
-        for (int64_t i = 0; i < n; ++i) out[i] = 0.5 * c->grid.dcell;
+        if (c->oct.ncells > 0) std::memcpy(out, c->lhalf.data(), n * 8);
+        else for (int64_t i = 0; i < n; ++i) out[i] = 0.5 * c->grid.dcell;
         return MOCHII_OK;
     }
     if (nm == "gamma_metal" || nm == "heat_metal" || nm == "x_metal") {

@@ -41,6 +41,7 @@ struct BalArgs {
     unsigned long long* counters;
     long long nleaf;
     double T, yHe, relax, colscale, vol;
+    const double4* lg;                // octree leaf geometry (per-leaf volume), null on the Cartesian grid
     RateSel rs;
     Coef k;   // coefficients at the fixed temperature (equilibrium update)
     int caseA, nabs, fp32;
@@ -49,6 +50,13 @@ struct BalArgs {
     int fast;                         // bracketed Illinois solves (solver_bracketed)
     double nemax;                     // largest n_e per n_H: 1 + 2 y_He + metal electrons
 };
+
+// Volume weight of a leaf in the convergence sums: (2 leaf_half)^3.
+__device__ __forceinline__ double leaf_vol(const BalArgs& a, long long il) {
+    if (!a.lg) return a.vol;
+    const double w = 2.0 * a.lg[il].w;
+    return w * w * w;
+}
 
 // Absorber columns n_i * distance2cm * 1e-18 for one leaf.
 __device__ __forceinline__ void write_columns(void* col, long long il, int nabs, int fp32, double nH, double yHe,
@@ -328,9 +336,10 @@ __global__ void __launch_bounds__(kBThreads) k_balance(const BalArgs a) {
         a.ne[il] = nen;
         write_columns(a.col, il, a.nabs, a.fp32, nH, a.yHe, xn, h1n, h2n, a.colscale);
         const double dx = fabs(xn - x0);
+        const double vol = leaf_vol(a, il);
         mdx = fmax(mdx, dx);
-        sdx = sdx + a.vol * dx;
-        sx = sx + a.vol * (1.0 - xn);
+        sdx = sdx + vol * dx;
+        sx = sx + vol * (1.0 - xn);
     }
     const int t = threadIdx.x;
     sh[0][t] = mdx;
@@ -658,10 +667,11 @@ __global__ void __launch_bounds__(kBThreads) k_thermal(const ThArgs a) {
         const double dx = fabs(xn - x0);
         mdx = fmax(mdx, dx);
         mdt = fmax(mdt, fabs(te - T0) / T0);
-        s1 = s1 + b.vol * dx;
-        s2 = s2 + b.vol * (1.0 - xn);
-        s3 = s3 + b.vol * nen * fabs(te - T0);
-        s4 = s4 + b.vol * nen * te;
+        const double vol = leaf_vol(b, il);
+        s1 = s1 + vol * dx;
+        s2 = s2 + vol * (1.0 - xn);
+        s3 = s3 + vol * nen * fabs(te - T0);
+        s4 = s4 + vol * nen * te;
     }
     const int t = threadIdx.x;
     sh[0][t] = mdx; sh[1][t] = mdt; sh[2][t] = s1; sh[3][t] = s2; sh[4][t] = s3; sh[5][t] = s4;
@@ -768,6 +778,7 @@ static BalArgs bal_args(mochii_ctx* c) {
     a.colscale = c->par.distance2cm * 1.0e-18;
     const double w = c->grid.dcell;   // (2*leaf_half)^3 on the uniform grid
     a.vol = w * w * w;
+    a.lg = c->oct.ncells > 0 ? c->oct.lgeo : nullptr;
     a.rs.hui_gnedin = c->par.recomb_hui_gnedin;
     a.rs.dere_hybrid = c->par.ci_dere_hybrid;
     a.caseA = c->par.caseA;

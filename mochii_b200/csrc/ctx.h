@@ -9,6 +9,7 @@
 #include "band.h"
 #include "diffuse.h"
 #include "mochii_gpu.h"
+#include "octree.h"
 #include "qmc.cuh"
 #include "species.h"
 #include "thermal.h"
@@ -99,6 +100,9 @@ struct mochii_ctx {
     mochii::ThermalDev th;          // thermal tables (solve_te)
     mochii::DiffuseBuffers dif;     // diffuse field (diffuse_field)
     mochii::MetalDev metal;         // trace metals (use_metals); metal.ntr == 0 without
+    mochii::OctDev oct;             // grid_type = 'amr'; oct.ncells == 0 on the Cartesian grid
+    void* oct_blob = nullptr;       // octree: the one allocation behind oct's pointers
+    std::vector<double> lhalf;      // octree: leaf half widths (host copy for leaf_half)
     double* twarm = nullptr;        // bracketed thermal solve: warm-start T_e per leaf ("T_warm")
     bool twarm_set = false;         // consumed by the next thermal update
     mochii::SpeciesHost species;

@@ -105,8 +105,9 @@ struct DiffArgs {
     double* ch;        // 4 x nleaf (channel luminosities, leaf-major)
     double* tot;       // nleaf leaf totals, then their inclusive prefix sum
     MilneDev m;
+    const double4* lg;   // octree leaf geometry (per-leaf volume), null on the Cartesian grid
     long long nleaf;
-    double yHe, vol, eion_max;
+    double yHe, vol, d2cm, eion_max;
     RateSel rs;
     int energy_model;  // 0 milne, 1 exponential, 2 threshold
 };
@@ -173,9 +174,14 @@ __global__ void k_diffuse_lum(const DiffArgs a) {
             } else {
                 e0 = kEthHI; e1 = kEthHeI; e2 = kEthHeII;
             }
-            c0 = ne * nHII * (alphaA_HII(a.rs, T) - alphaB_HII(a.rs, T)) * e0 * kEv2erg * a.vol;
-            c1 = ne * nHeII * (alphaA_HeII(a.rs, T) - alphaB_HeII(a.rs, T)) * e1 * kEv2erg * a.vol;
-            c2 = ne * nHeIII * (alphaA_HeIII(a.rs, T) - alphaB_HeIII(a.rs, T)) * e2 * kEv2erg * a.vol;
+            double vol = a.vol;
+            if (a.lg) {
+                const double w = 2.0 * a.lg[il].w * a.d2cm;
+                vol = w * w * w;
+            }
+            c0 = ne * nHII * (alphaA_HII(a.rs, T) - alphaB_HII(a.rs, T)) * e0 * kEv2erg * vol;
+            c1 = ne * nHeII * (alphaA_HeII(a.rs, T) - alphaB_HeII(a.rs, T)) * e1 * kEv2erg * vol;
+            c2 = ne * nHeIII * (alphaA_HeIII(a.rs, T) - alphaB_HeIII(a.rs, T)) * e2 * kEv2erg * vol;
         }
         a.ch[4 * il + 0] = c0;
         a.ch[4 * il + 1] = c1;
@@ -193,6 +199,7 @@ struct DiffLaunchArgs {
     const double* eedge;
     MilneDev m;
     MetalDev metal;
+    const double4* lg;   // octree leaf geometry, null on the Cartesian grid
     double total, org[3], dcell, eion_max;
     int n[3], nnu, nfuv, energy_model;
     long long nleaf;
@@ -222,11 +229,20 @@ __global__ void __launch_bounds__(kThreads) k_launch_diffuse(const DiffLaunchArg
         if (a.cum[mid - 1] / a.total < u[0]) lo = mid + 1; else hi = mid;
     }
     const long long il = lo - 1;
-    const int ix = (int)(il % a.n[0]), iy = (int)((il / a.n[0]) % a.n[1]), iz = (int)(il / ((long long)a.n[0] * a.n[1]));
-    const double half = 0.5 * a.dcell;
-    const double pos[3] = {(a.org[0] + ((double)ix + 0.5) * a.dcell) + (2.0 * u[1] - 1.0) * half,
-                           (a.org[1] + ((double)iy + 0.5) * a.dcell) + (2.0 * u[2] - 1.0) * half,
-                           (a.org[2] + ((double)iz + 0.5) * a.dcell) + (2.0 * u[3] - 1.0) * half};
+    double pos[3];
+    if (a.lg) {   // leaf centre and half width of the octree leaf
+        const double4 g = a.lg[il];
+        pos[0] = g.x + (2.0 * u[1] - 1.0) * g.w;
+        pos[1] = g.y + (2.0 * u[2] - 1.0) * g.w;
+        pos[2] = g.z + (2.0 * u[3] - 1.0) * g.w;
+    } else {
+        const int ix = (int)(il % a.n[0]), iy = (int)((il / a.n[0]) % a.n[1]);
+        const int iz = (int)(il / ((long long)a.n[0] * a.n[1]));
+        const double half = 0.5 * a.dcell;
+        pos[0] = (a.org[0] + ((double)ix + 0.5) * a.dcell) + (2.0 * u[1] - 1.0) * half;
+        pos[1] = (a.org[1] + ((double)iy + 0.5) * a.dcell) + (2.0 * u[2] - 1.0) * half;
+        pos[2] = (a.org[2] + ((double)iz + 0.5) * a.dcell) + (2.0 * u[3] - 1.0) * half;
+    }
     const double cost = 2.0 * u[4] - 1.0;
     const double sint = sqrt(1.0 - cost * cost);
     double sphi, cphi;
@@ -253,7 +269,8 @@ __global__ void __launch_bounds__(kThreads) k_launch_diffuse(const DiffLaunchArg
         if (a.eedge[mid - 1] <= eph) blo = mid; else bhi = mid - 1;
     }
     const int inu = min(max(blo, a.nfuv + 1), a.nnu) - 1;
-    write_record<R>(rec, i, pos, kk, eph, inu, a.org, a.dcell, a.n);
+    if (a.lg) write_record_amr<R>(rec, i, pos, kk, eph, inu, (int)il);
+    else write_record<R>(rec, i, pos, kk, eph, inu, a.org, a.dcell, a.n);
     if (a.metal.ntr > 0) write_metal_record<R>(rec, a.metal, i, eph);
 }
 
@@ -276,6 +293,8 @@ cudaError_t diffuse_build(mochii_ctx* c, double* total) {
     a.yHe = c->par.He_abund;
     const double w = c->grid.dcell * c->par.distance2cm;
     a.vol = w * w * w;
+    a.lg = c->oct.ncells > 0 ? c->oct.lgeo : nullptr;
+    a.d2cm = c->par.distance2cm;
     a.eion_max = c->par.eion_max;
     a.rs.hui_gnedin = c->par.recomb_hui_gnedin;
     a.rs.dere_hybrid = c->par.ci_dere_hybrid;
@@ -308,6 +327,7 @@ cudaError_t launch_diffuse_chunk(mochii_ctx* c, double total, long long ip0, lon
     a.total = total;
     a.org[0] = c->grid.xmin; a.org[1] = c->grid.ymin; a.org[2] = c->grid.zmin;
     a.metal = c->metal;
+    a.lg = c->oct.ncells > 0 ? c->oct.lgeo : nullptr;
     a.dcell = c->grid.dcell;
     a.eion_max = c->par.eion_max;
     a.n[0] = c->grid.nx; a.n[1] = c->grid.ny; a.n[2] = c->grid.nz;

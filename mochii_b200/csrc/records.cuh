@@ -11,10 +11,10 @@
 namespace mochii {
 
 struct PacketRecords {
-    double* tm;    // 3 x cap
-    double* td;    // 3 x cap
-    int* cell;     // ix | iy << 10 | iz << 20
-    int* bits;     // inu | (stp_x+1) << 16 | (stp_y+1) << 18 | (stp_z+1) << 20
+    double* tm;    // 3 x cap (octree: start point)
+    double* td;    // 3 x cap (octree: direction)
+    int* cell;     // ix | iy << 10 | iz << 20 (octree: start leaf, -1 outside)
+    int* bits;     // inu | (stp_x+1) << 16 | (stp_y+1) << 18 | (stp_z+1) << 20 (octree: inu)
     void* sig;     // 3 x cap of R: sigma_HI, sigma_HeI, sigma_HeII in 1e-18 cm^2
     void* coef;    // 6 x cap of R: Gamma/heat coefficients per unit path
     double* E;     // metals only: packet energy [eV]
@@ -22,14 +22,8 @@ struct PacketRecords {
     long long cap;
 };
 
-// Record of one packet: build_ion_packet_physics (ion_packet_mod.f90:21-53),
-// the per-path coefficients of score_ion_path (ion_score_mod.f90:213-221),
-// scaled by 1e18 so FP32 stays in range (sigma in 1e-18 cm^2, E in eV), and
-// dda_init (raytrace_amr.f90:495-532) in FP64.
 template <typename R>
-__device__ __forceinline__ void write_record(const PacketRecords& rec, long long i, const double pos[3],
-                                             const double kk[3], double E, int inu, const double org[3],
-                                             double d, const int n[3]) {
+__device__ __forceinline__ void write_cross_sections(const PacketRecords& rec, long long i, double E) {
     const double sHI = sigma_HI(E), sHeI = sigma_HeI(E), sHeII = sigma_HeII(E);
     R* sg = static_cast<R*>(rec.sig);
     R* cf = static_cast<R*>(rec.coef);
@@ -43,6 +37,34 @@ __device__ __forceinline__ void write_record(const PacketRecords& rec, long long
     cf[3 * c + i] = (R)(sHeI * 1.0e18 * fmax(1.0 - kEthHeI / E, 0.0));
     cf[4 * c + i] = (R)(sHeII * 1.0e18 / E);
     cf[5 * c + i] = (R)(sHeII * 1.0e18 * fmax(1.0 - kEthHeII / E, 0.0));
+}
+
+// Record of one packet on the octree: the cross sections, start point,
+// direction and start leaf (the walk finds its faces as it goes).
+template <typename R>
+__device__ __forceinline__ void write_record_amr(const PacketRecords& rec, long long i, const double pos[3],
+                                                 const double kk[3], double E, int inu, int leaf) {
+    write_cross_sections<R>(rec, i, E);
+    const long long c = rec.cap;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        rec.tm[k * c + i] = pos[k];
+        rec.td[k * c + i] = kk[k];
+    }
+    rec.cell[i] = leaf;
+    rec.bits[i] = inu;
+}
+
+// Record of one packet: build_ion_packet_physics (ion_packet_mod.f90:21-53),
+// the per-path coefficients of score_ion_path (ion_score_mod.f90:213-221),
+// scaled by 1e18 so FP32 stays in range (sigma in 1e-18 cm^2, E in eV), and
+// dda_init (raytrace_amr.f90:495-532) in FP64.
+template <typename R>
+__device__ __forceinline__ void write_record(const PacketRecords& rec, long long i, const double pos[3],
+                                             const double kk[3], double E, int inu, const double org[3],
+                                             double d, const int n[3]) {
+    write_cross_sections<R>(rec, i, E);
+    const long long c = rec.cap;
     int idx[3], bits = inu;
 #pragma unroll
     for (int k = 0; k < 3; ++k) {

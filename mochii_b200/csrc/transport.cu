@@ -56,7 +56,99 @@ struct PassArgs {
     int ncomp, multi, ndim, nnu;
     MetalDev m;          // trace metals; m.ntr == 0 without
     int metal_abs;       // par%ion_metal_abs
+    OctDev oct;          // octree grid; oct.ncells == 0 on the Cartesian grid
 };
+
+// ---- octree geometry (octree_mod.f90) ------------------------------------------
+// One 32-byte geometry record (centre, half width) through the read-only path.
+__device__ __forceinline__ double4 ld_geo(const double4* p) {
+    const double2 a = __ldg(reinterpret_cast<const double2*>(p));
+    const double2 b = __ldg(reinterpret_cast<const double2*>(p) + 1);
+    return make_double4(a.x, a.y, b.x, b.y);
+}
+
+// amr_find_leaf (:69-93): descent from the root by centre comparisons.  The
+// complete top levels (cells below nshared, all internal cells) come from
+// the copy staged in shared memory when the caller passes one.
+__device__ __forceinline__ int oct_find_leaf(const OctDev& o, double x, double y, double z,
+                                             const double4* sgeo = nullptr, const int* schild = nullptr) {
+    const double h = o.half;
+    if (x < -h || x > h || y < -h || y > h || z < -h || z > h) return -1;
+    int c = 0;
+    for (int guard = 0; guard < 64; ++guard) {
+        const bool st = sgeo && c < o.nshared;
+        if (!st) {
+            const int lf = __ldg(o.ileaf + c);
+            if (lf >= 0) return lf;
+        }
+        const double4 g = st ? sgeo[c] : ld_geo(o.geo + c);
+        int ioct = 0;
+        if (x >= g.x) ioct += 1;
+        if (y >= g.y) ioct += 2;
+        if (z >= g.z) ioct += 4;
+        c = st ? schild[8 * c + ioct] : __ldg(o.children + 8 * c + ioct);
+        if (c < 0) return -1;
+    }
+    return -1;
+}
+
+// Stage the complete top levels (geometry and children) in shared memory.
+__device__ __forceinline__ void oct_stage(const OctDev& o, double4* sgeo, int* schild) {
+    for (int i = threadIdx.x; i < o.nshared; i += blockDim.x) sgeo[i] = o.geo[i];
+    for (int i = threadIdx.x; i < 8 * o.nshared; i += blockDim.x) schild[i] = o.children[i];
+}
+
+// amr_cell_exit (:308-340): distance to the nearest face of the cell and the
+// face (0 +x, 1 -x, 2 +y, 3 -y, 4 +z, 5 -z); minloc over the six candidate
+// times in that order (first minimum on ties), a non-moving axis giving huge.
+__device__ __forceinline__ double oct_cell_exit(const double4 g, double x, double y, double z, double kx, double ky,
+                                                double kz, int* face) {
+    double t0 = kHugest, t1 = kHugest, t2 = kHugest, t3 = kHugest, t4 = kHugest, t5 = kHugest;
+    if (kx > 0.0) t0 = (g.x + g.w - x) / kx; else if (kx < 0.0) t1 = (g.x - g.w - x) / kx;
+    if (ky > 0.0) t2 = (g.y + g.w - y) / ky; else if (ky < 0.0) t3 = (g.y - g.w - y) / ky;
+    if (kz > 0.0) t4 = (g.z + g.w - z) / kz; else if (kz < 0.0) t5 = (g.z - g.w - z) / kz;
+    double t = t0;
+    int f = 0;
+    if (t1 < t) { t = t1; f = 1; }
+    if (t2 < t) { t = t2; f = 2; }
+    if (t3 < t) { t = t3; f = 3; }
+    if (t4 < t) { t = t4; f = 4; }
+    if (t5 < t) { t = t5; f = 5; }
+    *face = f;
+    return t;
+}
+
+// amr_next_leaf (:499-537) from a leaf: the leaf across the face when the
+// face neighbour is one, else descent from the neighbour by the two
+// tangential coordinates with the face-normal octant bit set by the face.
+__device__ __forceinline__ int oct_next_leaf(const OctDev& o, int il, int face, double x, double y, double z) {
+    const int nx = __ldg(o.lnext + 8 * il + face);
+    if (nx >= -1) return nx;
+    int n = -2 - nx;
+    for (int guard = 0; guard < 64; ++guard) {
+        const double4 g = ld_geo(o.geo + n);
+        int ioct = 0;
+        if (face == 0 || face == 1) {
+            ioct = face == 1 ? 1 : 0;
+            if (y >= g.y) ioct += 2;
+            if (z >= g.z) ioct += 4;
+        } else if (face == 2 || face == 3) {
+            if (x >= g.x) ioct += 1;
+            ioct += face == 3 ? 2 : 0;
+            if (z >= g.z) ioct += 4;
+        } else {
+            if (x >= g.x) ioct += 1;
+            if (y >= g.y) ioct += 2;
+            ioct += face == 5 ? 4 : 0;
+        }
+        const int ch = __ldg(o.children + 8 * n + ioct);
+        if (ch < 0) return -1;   // no child there: the walk ends
+        const int lf = __ldg(o.ileaf + ch);
+        if (lf >= 0) return lf;
+        n = ch;
+    }
+    return -1;
+}
 
 // sample_energy_cdf, energy_sampler_mod.f90:187-238.  The bracket search and
 // the exact inverse of the linear density follow the same FP64 operation
@@ -152,9 +244,15 @@ __device__ double block_sum(double v, double* sh) {
 // (:2232-2247), build_ion_packet_physics (ion_packet_mod.f90:21-53), the
 // coefficients of score_ion_path (ion_score_mod.f90:213-221) and dda_init
 // (raytrace_amr.f90:495-532).
-template <typename R>
+//
+// AMR: the octree variant stages the complete top levels of the tree in
+// shared memory for the start-leaf search.
+template <typename R, bool AMR>
 __global__ void __launch_bounds__(kThreads) k_launch(const PassArgs a, PacketRecords rec, long long ip0, long long n) {
     __shared__ QmcTables sq;
+    __shared__ double4 sgeo[AMR ? kOctShared : 1];
+    __shared__ int schild[AMR ? 8 * kOctShared : 1];
+    if constexpr (AMR) oct_stage(a.oct, sgeo, schild);
     {
         const uint32_t* src = reinterpret_cast<const uint32_t*>(a.qmc);
         uint32_t* dst = reinterpret_cast<uint32_t*>(&sq);
@@ -185,7 +283,10 @@ __global__ void __launch_bounds__(kThreads) k_launch(const PassArgs a, PacketRec
     sincos(kTwoPi * uphi, &sphi, &cphi);
     const double kk[3] = {sint * cphi, sint * sphi, cost};
     const int inu = bin_of(a.eedge, a.nnu, E);
-    write_record<R>(rec, i, pos, kk, E, inu, a.org, a.dcell, a.n);
+    if constexpr (AMR)   // emit_point_qmc: photon%icell_amr = amr_find_leaf (ion_band_mod.f90:2245)
+        write_record_amr<R>(rec, i, pos, kk, E, inu, oct_find_leaf(a.oct, pos[0], pos[1], pos[2], sgeo, schild));
+    else
+        write_record<R>(rec, i, pos, kk, E, inu, a.org, a.dcell, a.n);
     if (a.m.ntr > 0) write_metal_record<R>(rec, a.m, i, E);
 }
 
@@ -240,20 +341,124 @@ struct Stepper {
     }
 };
 
+// H/He part of score_ion_path (ion_score_mod.f90:137-231): the rate tallies
+// of the leaf and its diagnostic spectrum bin.
+template <typename T, typename R, int NT>
+__device__ __forceinline__ void score_hhe(T* tal, T* jt, int il, int nnu, int inu, R w, const R* cf) {
+    T* tl = tal + (long long)il * NT;
+#pragma unroll
+    for (int k = 0; k < NT; ++k) tally_add(tl + k, w * cf[k]);
+    tally_add(jt + (long long)il * nnu + inu, w);
+}
+
+// The trace-metal state of one packet in the walk.  The packet's
+// active-prefix cross sections sigma_k sit in dynamic shared memory
+// ([k][thread], ntrp x blockDim of R); per segment the leaf's opacity weights
+// add sum_k w_k sigma_k to the absorption (species_cached_opacity,
+// species_mod.f90:291-303).  The path estimators of species_rate_path_score
+// (:329-343) are either scored directly, two tallies per active transition
+// (MET = 1, with the heating coefficients sigma_k (1 - E_th,k/E) in a second
+// shared array), or as the kMomDeg Chebyshev moments of the packet energy in
+// its moment bin (MET = 2), which the rate kernel contracts with the
+// tabulated integrands.
+template <typename R, int MET>
+struct MetalPacket {
+    int nm = 0, mb = 0;
+    R invE = (R)0;
+    R phi[MET == 2 ? kMomDeg : 1];
+    __device__ __forceinline__ void setup(const MetalDev& m, const PacketRecords& rec, long long i, R* msg, R* mhc) {
+        const int tb = blockDim.x, tx = threadIdx.x;
+        const long long c = rec.cap;
+        const double E = rec.E[i];
+        nm = metal_nactive(m, E);
+        invE = (R)(1.0 / E);
+        const R* ms = static_cast<const R*>(rec.msig);
+        for (int k = 0; k < nm; ++k) {
+            const R sk = ms[k * c + i];
+            msg[k * tb + tx] = sk;
+            if constexpr (MET == 1) mhc[k * tb + tx] = (R)((double)sk * fmax(1.0 - __ldg(m.eth + k) / E, 0.0));
+        }
+        if constexpr (MET == 2) {   // moment bin and the Chebyshev values T_0..T_5 of E in it
+            int lo = 0, hi = m.nmb - 1;
+            while (lo < hi) {
+                const int mid = (lo + hi + 1) >> 1;
+                if (__ldg(m.medge + mid) <= E) lo = mid; else hi = mid - 1;
+            }
+            mb = lo;
+            const double e0 = __ldg(m.medge + mb), e1 = __ldg(m.medge + mb + 1);
+            const double t = fmin(fmax((2.0 * E - (e0 + e1)) / (e1 - e0), -1.0), 1.0);
+            double tm1 = 1.0, tm = t;
+            phi[0] = (R)1;
+            phi[1] = (R)t;
+#pragma unroll
+            for (int q = 2; q < kMomDeg; ++q) {
+                const double tn = 2.0 * t * tm - tm1;
+                phi[q] = (R)tn;
+                tm1 = tm;
+                tm = tn;
+            }
+        }
+    }
+    __device__ __forceinline__ R kappa(const MetalDev& m, int il, const R* msg) const {
+        const int tb = blockDim.x, tx = threadIdx.x;
+        const R* op = static_cast<const R*>(m.opac) + (long long)il * m.ntrp;
+        R km = (R)0;
+        for (int k = 0; k < nm; ++k) km = km + __ldg(op + k) * msg[k * tb + tx];
+        return km;
+    }
+    template <typename T>
+    __device__ __forceinline__ void score(const MetalDev& m, int il, R w, const R* msg, const R* mhc) const {
+        const int tb = blockDim.x, tx = threadIdx.x;
+        if constexpr (MET == 1) {
+            T* rw = static_cast<T*>(m.raw) + (long long)il * m.ntrp * 2;
+            const R wi = w * invE;
+            for (int k = 0; k < nm; ++k) {
+                tally_add(rw + 2 * k, wi * msg[k * tb + tx]);
+                tally_add(rw + 2 * k + 1, w * mhc[k * tb + tx]);
+            }
+        } else if constexpr (MET == 2) {
+            T* mt = static_cast<T*>(m.mom) + ((long long)il * m.nmb + mb) * kMomDeg;
+#pragma unroll
+            for (int q = 0; q < kMomDeg; ++q) tally_add(mt + q, w * phi[q]);
+        }
+    }
+};
+
+// Per-block end of a walk kernel: the energy ledger (ion_score_energy_packet,
+// ion_score_mod.f90:233-252) summed per block, and the counters.
+template <bool METAL>
+__device__ __forceinline__ void walk_epilogue(const PassArgs& a, double emitted, double absorbed, double escaped,
+                                              unsigned long long nseg, unsigned long long kills,
+                                              unsigned long long nact, int accumulate, double* sh) {
+    const double e0 = block_sum(emitted, sh);
+    const double e1 = block_sum(absorbed, sh);
+    const double e2 = block_sum(escaped, sh);
+    if (threadIdx.x == 0) {
+        double* L = a.ledger + 3 * blockIdx.x;
+        if (accumulate) {
+            L[0] += e0; L[1] += e1; L[2] += e2;
+        } else {
+            L[0] = e0; L[1] = e1; L[2] = e2;
+        }
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        nseg += __shfl_down_sync(0xffffffffu, nseg, o);
+        kills += __shfl_down_sync(0xffffffffu, kills, o);
+        if (METAL) nact += __shfl_down_sync(0xffffffffu, nact, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        if (nseg) atomicAdd(a.counters + 0, nseg);
+        if (kills) atomicAdd(a.counters + 1, kills);
+        if (METAL && nact) atomicAdd(a.counters + 2, nact);
+    }
+}
+
 // Walk kernel: raytrace_ion_to_edge_car (raytrace_amr.f90:534-592) for the
 // packets of one chunk, grid-stride.  The stepper runs LA cells ahead of the
 // scoring: slot 0 is scored now, slots 1..LA have their column loads in
 // flight (LA = 0 disables the look-ahead).
 //
-// MET adds the trace-metal terms.  The packet's active-prefix cross
-// sections sigma_k sit in dynamic shared memory ([k][thread], ntrp x 128 of
-// R); per segment the leaf's opacity weights add sum_k w_k sigma_k to the
-// absorption (species_cached_opacity, species_mod.f90:291-303).  The path
-// estimators of species_rate_path_score (:329-343) are either scored
-// directly, two tallies per active transition (MET = 1, with the heating
-// coefficients sigma_k (1 - E_th,k/E) in a second shared array), or as the
-// kMomDeg Chebyshev moments of the packet energy in its moment bin (MET = 2),
-// which the rate kernel contracts with the tabulated integrands.
+// MET adds the trace-metal terms (MetalPacket: 1 exact tallies, 2 moments).
 template <typename R, int NABS, int LA, int MET>
 __global__ void __launch_bounds__(128) k_walk_edge(const PassArgs a, const PacketRecords rec, long long n,
                                                    int accumulate) {
@@ -264,7 +469,6 @@ __global__ void __launch_bounds__(128) k_walk_edge(const PassArgs a, const Packe
     extern __shared__ __align__(16) unsigned char dsm[];
     R* const msg = reinterpret_cast<R*>(dsm);                      // sigma_k      [k][thread]
     R* const mhc = msg + (MET == 1 ? a.m.ntrp * blockDim.x : 0);    // sigma_k h_k  [k][thread]
-    const int tb = blockDim.x, tx = threadIdx.x;
     double emitted = 0.0, absorbed = 0.0, escaped = 0.0;
     unsigned long long nseg = 0, kills = 0, nact = 0;
     T* tal = static_cast<T*>(a.tally);
@@ -289,39 +493,8 @@ __global__ void __launch_bounds__(128) k_walk_edge(const PassArgs a, const Packe
         R cf[NT];
 #pragma unroll
         for (int k = 0; k < NT; ++k) cf[k] = cfp[k * c + i];
-        int nm = 0, mb = 0;
-        R invE = (R)0, phi[kMomDeg];
-        if constexpr (METAL) {
-            const double E = rec.E[i];
-            nm = metal_nactive(a.m, E);
-            invE = (R)(1.0 / E);
-            const R* ms = static_cast<const R*>(rec.msig);
-            for (int k = 0; k < nm; ++k) {
-                const R sk = ms[k * c + i];
-                msg[k * tb + tx] = sk;
-                if constexpr (MET == 1) mhc[k * tb + tx] = (R)((double)sk * fmax(1.0 - __ldg(a.m.eth + k) / E, 0.0));
-            }
-            if constexpr (MET == 2) {   // moment bin and the Chebyshev values T_0..T_5 of E in it
-                int lo = 0, hi = a.m.nmb - 1;
-                while (lo < hi) {
-                    const int mid = (lo + hi + 1) >> 1;
-                    if (__ldg(a.m.medge + mid) <= E) lo = mid; else hi = mid - 1;
-                }
-                mb = lo;
-                const double e0 = __ldg(a.m.medge + mb), e1 = __ldg(a.m.medge + mb + 1);
-                const double t = fmin(fmax((2.0 * E - (e0 + e1)) / (e1 - e0), -1.0), 1.0);
-                double tm1 = 1.0, tm = t;
-                phi[0] = (R)1;
-                phi[1] = (R)t;
-#pragma unroll
-                for (int q = 2; q < kMomDeg; ++q) {
-                    const double tn = 2.0 * t * tm - tm1;
-                    phi[q] = (R)tn;
-                    tm1 = tm;
-                    tm = tn;
-                }
-            }
-        }
+        MetalPacket<R, MET> mp;
+        if constexpr (METAL) mp.setup(a.m, rec, i, msg, mhc);
         // ring of LA+1 cells: il, segment, columns, and whether a next cell exists
         int il[LA + 1] = {};
         double sgm[LA + 1] = {};
@@ -344,12 +517,7 @@ __global__ void __launch_bounds__(128) k_walk_edge(const PassArgs a, const Packe
             if (++nstep > kMaxWalkSteps) { ++kills; break; }
             R kap = cl[0].kappa(s0, s1, s2);
             if constexpr (METAL) {
-                if (a.metal_abs && nm > 0) {
-                    const R* op = static_cast<const R*>(a.m.opac) + (long long)il[0] * a.m.ntrp;
-                    R km = (R)0;
-                    for (int k = 0; k < nm; ++k) km = km + __ldg(op + k) * msg[k * tb + tx];
-                    kap = kap + km;
-                }
+                if (a.metal_abs) kap = kap + mp.kappa(a.m, il[0], msg);
             }
             const R ks = kap * (R)sgm[0];
             R w;
@@ -362,23 +530,9 @@ __global__ void __launch_bounds__(128) k_walk_edge(const PassArgs a, const Packe
             }
             if (w != (R)0) {   // score_ion_path returns on a zero path (ion_score_mod.f90:148)
                 ++nseg;
-                nact += nm;
-                T* tl = tal + (long long)il[0] * NT;
-#pragma unroll
-                for (int k = 0; k < NT; ++k) tally_add(tl + k, w * cf[k]);
-                tally_add(jt + (long long)il[0] * a.nnu + inu, w);
-                if constexpr (MET == 1) {
-                    T* rw = static_cast<T*>(a.m.raw) + (long long)il[0] * a.m.ntrp * 2;
-                    const R wi = w * invE;
-                    for (int k = 0; k < nm; ++k) {
-                        tally_add(rw + 2 * k, wi * msg[k * tb + tx]);
-                        tally_add(rw + 2 * k + 1, w * mhc[k * tb + tx]);
-                    }
-                } else if constexpr (MET == 2) {
-                    T* mt = static_cast<T*>(a.m.mom) + ((long long)il[0] * a.m.nmb + mb) * kMomDeg;
-#pragma unroll
-                    for (int q = 0; q < kMomDeg; ++q) tally_add(mt + q, w * phi[q]);
-                }
+                nact += mp.nm;
+                score_hhe<T, R, NT>(tal, jt, il[0], a.nnu, inu, w, cf);
+                if constexpr (METAL) mp.template score<T>(a.m, il[0], w, msg, mhc);
             }
             tau = tau + (double)ks;
             if (tau >= kTauHuge) break;
@@ -401,27 +555,90 @@ __global__ void __launch_bounds__(128) k_walk_edge(const PassArgs a, const Packe
         absorbed += lum * (1.0 - tr);
         escaped += lum * tr;
     }
-    const double e0 = block_sum(emitted, sh);
-    const double e1 = block_sum(absorbed, sh);
-    const double e2 = block_sum(escaped, sh);
-    if (threadIdx.x == 0) {
-        double* L = a.ledger + 3 * blockIdx.x;
-        if (accumulate) {
-            L[0] += e0; L[1] += e1; L[2] += e2;
-        } else {
-            L[0] = e0; L[1] = e1; L[2] = e2;
+    walk_epilogue<METAL>(a, emitted, absorbed, escaped, nseg, kills, nact, accumulate, sh);
+}
+
+// Walk kernel on the octree: raytrace_ion_to_edge_amr (raytrace_amr.f90:
+// 422-486, without the xy-periodic wrap) for the packets of one chunk,
+// grid-stride.  Per segment: the leaf's geometry record and columns (both
+// leaf-indexed, issued together), the exit face (amr_cell_exit), the
+// attenuated path score, the move to the exit point, and the leaf across the
+// face (amr_next_leaf).  Geometry in FP64 without contraction, as the
+// reference's.
+template <typename R, int NABS, int MET>
+__global__ void __launch_bounds__(128) k_walk_amr(const PassArgs a, const PacketRecords rec, long long n,
+                                                  int accumulate) {
+    typedef typename Acc<R>::T T;
+    constexpr int NT = NABS == 1 ? 2 : 6;
+    constexpr bool METAL = MET > 0;
+    __shared__ double sh[128];
+    extern __shared__ __align__(16) unsigned char dsm[];
+    R* const msg = reinterpret_cast<R*>(dsm);
+    R* const mhc = msg + (MET == 1 ? a.m.ntrp * blockDim.x : 0);
+    double emitted = 0.0, absorbed = 0.0, escaped = 0.0;
+    unsigned long long nseg = 0, kills = 0, nact = 0;
+    T* tal = static_cast<T*>(a.tally);
+    T* jt = static_cast<T*>(a.jt);
+    const R* sg = static_cast<const R*>(rec.sig);
+    const R* cfp = static_cast<const R*>(rec.coef);
+    const long long c = rec.cap;
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+        double x = rec.tm[i], y = rec.tm[c + i], z = rec.tm[2 * c + i];
+        const double kx = rec.td[i], ky = rec.td[c + i], kz = rec.td[2 * c + i];
+        int il = rec.cell[i];
+        const int inu = rec.bits[i] & 0xFFFF;
+        const R s0 = sg[i];
+        const R s1 = NABS == 1 ? (R)0 : sg[c + i];
+        const R s2 = NABS == 1 ? (R)0 : sg[2 * c + i];
+        R cf[NT];
+#pragma unroll
+        for (int k = 0; k < NT; ++k) cf[k] = cfp[k * c + i];
+        MetalPacket<R, MET> mp;
+        if constexpr (METAL) mp.setup(a.m, rec, i, msg, mhc);
+        R expo = (R)1.0;
+        double tau = 0.0;
+        int nstep = 0;
+        while (il >= 0) {
+            if (++nstep > kMaxWalkSteps) { ++kills; break; }
+            const double4 g = ld_geo(a.oct.lgeo + il);
+            Col<R, NABS> cl;
+            cl.load(a.col, il);
+            int face;
+            const double texit = oct_cell_exit(g, x, y, z, kx, ky, kz, &face);
+            R kap = cl.kappa(s0, s1, s2);
+            if constexpr (METAL) {
+                if (a.metal_abs) kap = kap + mp.kappa(a.m, il, msg);
+            }
+            const R ks = kap * (R)texit;
+            R w;
+            if (ks > (R)0) {
+                const R eo = expo * attenuation(ks);
+                w = (expo - eo) / kap;
+                expo = eo;
+            } else {
+                w = expo * (R)texit;
+            }
+            if (w != (R)0) {
+                ++nseg;
+                nact += mp.nm;
+                score_hhe<T, R, NT>(tal, jt, il, a.nnu, inu, w, cf);
+                if constexpr (METAL) mp.template score<T>(a.m, il, w, msg, mhc);
+            }
+            tau = tau + (double)ks;
+            if (tau >= kTauHuge) break;
+            x = x + texit * kx;
+            y = y + texit * ky;
+            z = z + texit * kz;
+            il = oct_next_leaf(a.oct, il, face, x, y, z);
         }
+        const double lum = a.Lpacket;
+        const double tr = exp(-fmax(tau, 0.0));
+        emitted += lum;
+        absorbed += lum * (1.0 - tr);
+        escaped += lum * tr;
     }
-    for (int o = 16; o > 0; o >>= 1) {
-        nseg += __shfl_down_sync(0xffffffffu, nseg, o);
-        kills += __shfl_down_sync(0xffffffffu, kills, o);
-        if (METAL) nact += __shfl_down_sync(0xffffffffu, nact, o);
-    }
-    if ((threadIdx.x & 31) == 0) {
-        if (nseg) atomicAdd(a.counters + 0, nseg);
-        if (kills) atomicAdd(a.counters + 1, kills);
-        if (METAL && nact) atomicAdd(a.counters + 2, nact);
-    }
+    walk_epilogue<METAL>(a, emitted, absorbed, escaped, nseg, kills, nact, accumulate, sh);
 }
 
 // gas_rates_compute + ion_score_apply_hhe (gas_rates_mod.f90:82-153,
@@ -433,10 +650,22 @@ __device__ __forceinline__ double tval(const T& v);
 template <> __device__ __forceinline__ double tval<double>(const double& v) { return v; }
 template <> __device__ __forceinline__ double tval<float2>(const float2& v) { return (double)v.x + (double)v.y; }
 
+//
+// On the octree the leaf volume varies: cg, ch exclude fac and each leaf
+// multiplies by its own 1/((2h)^3 d2), lg = the leaf geometry records.
+__device__ __forceinline__ double leaf_fac(const double4* lg, long long il, double d2) {
+    if (!lg) return 1.0;
+    const double w = 2.0 * ld_geo(lg + il).w;
+    return 1.0 / ((w * w * w) * d2);
+}
+
 template <typename T, int NT>
-__global__ void k_rates(const T* __restrict__ tal, double* __restrict__ rates, long long nleaf, double cg, double ch) {
+__global__ void k_rates(const T* __restrict__ tal, double* __restrict__ rates, long long nleaf, double cg0, double ch0,
+                        const double4* lg, double d2) {
     for (long long il = (long long)blockIdx.x * blockDim.x + threadIdx.x; il < nleaf;
          il += (long long)gridDim.x * blockDim.x) {
+        const double f = leaf_fac(lg, il, d2);
+        const double cg = cg0 * f, ch = ch0 * f;
         const T* t = tal + il * NT;
         rates[0 * nleaf + il] = tval<T>(t[0]) * cg;
         rates[3 * nleaf + il] = tval<T>(t[1]) * ch;
@@ -463,7 +692,7 @@ __global__ void k_jt(const T* __restrict__ jt, double* __restrict__ out, long lo
 // species_gamma_compute (species_mod.f90:493-512): per-leaf metal Gamma and
 // photoheating from the path tallies, into element order.
 template <typename T>
-__global__ void k_metal_rates(const MetalDev m, long long nleaf, double cg, double ch) {
+__global__ void k_metal_rates(const MetalDev m, long long nleaf, double cg, double ch, const double4* lg, double d2) {
     const T* raw = static_cast<const T*>(m.raw);
     for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < nleaf * m.ntr;
          q += (long long)gridDim.x * blockDim.x) {
@@ -471,8 +700,9 @@ __global__ void k_metal_rates(const MetalDev m, long long nleaf, double cg, doub
         const int j = (int)(q - il * m.ntr);
         const int k = m.tr[j].flat;
         const T* r = raw + (il * m.ntrp + k) * 2;
-        m.egam[q] = tval<T>(r[0]) * cg;
-        m.eheat[q] = tval<T>(r[1]) * ch;
+        const double f = leaf_fac(lg, il, d2);
+        m.egam[q] = tval<T>(r[0]) * (cg * f);
+        m.eheat[q] = tval<T>(r[1]) * (ch * f);
     }
 }
 
@@ -481,7 +711,8 @@ __global__ void k_metal_rates(const MetalDev m, long long nleaf, double cg, doub
 // mom(leaf, b, m) * coef(b, m, k, q).  One warp per leaf: the leaf's moments
 // are read once and broadcast, lanes run over the transitions.
 template <typename T>
-__global__ void k_metal_rates_mom(const MetalDev m, long long nleaf, double cg, double ch) {
+__global__ void k_metal_rates_mom(const MetalDev m, long long nleaf, double cg, double ch, const double4* lg,
+                                  double d2) {
     const T* mom = static_cast<const T*>(m.mom);
     const int lane = threadIdx.x & 31;
     const long long warps = (long long)gridDim.x * (blockDim.x >> 5);
@@ -500,8 +731,9 @@ __global__ void k_metal_rates_mom(const MetalDev m, long long nleaf, double cg, 
                     s1 = s1 + v * cf.y;
                 }
             }
-            m.egam[il * m.ntr + j] = s0 * cg;
-            m.eheat[il * m.ntr + j] = s1 * ch;
+            const double f = leaf_fac(lg, il, d2);
+            m.egam[il * m.ntr + j] = s0 * (cg * f);
+            m.eheat[il * m.ntr + j] = s1 * (ch * f);
         }
     }
 }
@@ -542,6 +774,28 @@ __global__ void k_walk(const double* rays, long long nray, int max_steps, int* l
         tmax[ax] = tmax[ax] + tdel[ax];
         idx[ax] += stp[ax];
         if (idx[ax] < 0 || idx[ax] >= n[ax]) break;
+    }
+    nsteps[r] = ns;
+    for (int s = ns; s < max_steps; ++s) leaves[r * max_steps + s] = -1;
+}
+
+// Geometry-only octree walk for the leaf-sequence hook: amr_find_leaf at the
+// start point, then amr_cell_exit / amr_next_leaf to the box edge.
+__global__ void k_walk_amr_leaves(const double* rays, long long nray, int max_steps, int* leaves, int* nsteps,
+                                  const OctDev o) {
+    const long long r = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= nray) return;
+    double x = rays[6 * r], y = rays[6 * r + 1], z = rays[6 * r + 2];
+    const double kx = rays[6 * r + 3], ky = rays[6 * r + 4], kz = rays[6 * r + 5];
+    int il = oct_find_leaf(o, x, y, z), ns = 0;
+    while (il >= 0 && ns < max_steps) {
+        leaves[r * max_steps + ns++] = il;
+        int face;
+        const double t = oct_cell_exit(ld_geo(o.lgeo + il), x, y, z, kx, ky, kz, &face);
+        x = x + t * kx;
+        y = y + t * ky;
+        z = z + t * kz;
+        il = oct_next_leaf(o, il, face, x, y, z);
     }
     nsteps[r] = ns;
     for (int s = ns; s < max_steps; ++s) leaves[r * max_steps + s] = -1;
@@ -602,6 +856,7 @@ PassArgs make_args(mochii_ctx* c) {
     a.nnu = c->nnu;
     a.m = c->metal;
     a.metal_abs = c->par.ion_metal_abs;
+    a.oct = c->oct;
     return a;
 }
 
@@ -669,10 +924,28 @@ cudaError_t walk_abs(mochii_ctx* c, const PassArgs& a, const PacketRecords& r, l
     return c->nabs == 1 ? walk_la<R, 1, MET>(c, a, r, n, acc, blocks) : walk_la<R, 4, MET>(c, a, r, n, acc, blocks);
 }
 
+// The octree walk: no look-ahead variants.
+template <typename R, int NABS, int MET>
+cudaError_t walk_amr(mochii_ctx* c, const PassArgs& a, const PacketRecords& r, long long n, int acc, int blocks) {
+    const size_t smem = MET ? metal_smem(c) : 0;
+    if (MET && smem > 48 * 1024)
+        cudaFuncSetAttribute(k_walk_amr<R, NABS, MET>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k_walk_amr<R, NABS, MET><<<blocks, 128, smem, c->stream>>>(a, r, n, acc);
+    return cudaGetLastError();
+}
+
+template <typename R, int MET>
+cudaError_t walk_abs(mochii_ctx* c, const PassArgs& a, const PacketRecords& r, long long n, int acc, int blocks,
+                     bool amr) {
+    if (amr) return c->nabs == 1 ? walk_amr<R, 1, MET>(c, a, r, n, acc, blocks) : walk_amr<R, 4, MET>(c, a, r, n, acc, blocks);
+    return walk_abs<R, MET>(c, a, r, n, acc, blocks);
+}
+
 template <typename R>
 cudaError_t walk_prec(mochii_ctx* c, const PassArgs& a, const PacketRecords& r, long long n, int acc, int blocks) {
-    if (c->metal.ntr == 0) return walk_abs<R, 0>(c, a, r, n, acc, blocks);
-    return c->metal.nmb > 0 ? walk_abs<R, 2>(c, a, r, n, acc, blocks) : walk_abs<R, 1>(c, a, r, n, acc, blocks);
+    const bool amr = c->oct.ncells > 0;
+    if (c->metal.ntr == 0) return walk_abs<R, 0>(c, a, r, n, acc, blocks, amr);
+    return c->metal.nmb > 0 ? walk_abs<R, 2>(c, a, r, n, acc, blocks, amr) : walk_abs<R, 1>(c, a, r, n, acc, blocks, amr);
 }
 
 cudaError_t launch_walk_variant(mochii_ctx* c, const PassArgs& a, const PacketRecords& r, long long n, int acc,
@@ -704,8 +977,14 @@ cudaError_t launch_transport(mochii_ctx* c) {
         const long long n = a.np - ip0 < r.cap ? a.np - ip0 : r.cap;
         const int lb = grid_blocks(n, kThreads, 1 << 30);
         const int acc = ip0 > 0;
-        if (c->fp32) k_launch<float><<<lb, kThreads, 0, c->stream>>>(a, r, ip0, n);
-        else k_launch<double><<<lb, kThreads, 0, c->stream>>>(a, r, ip0, n);
+        const bool amr = c->oct.ncells > 0;
+        if (c->fp32) {
+            if (amr) k_launch<float, true><<<lb, kThreads, 0, c->stream>>>(a, r, ip0, n);
+            else k_launch<float, false><<<lb, kThreads, 0, c->stream>>>(a, r, ip0, n);
+        } else {
+            if (amr) k_launch<double, true><<<lb, kThreads, 0, c->stream>>>(a, r, ip0, n);
+            else k_launch<double, false><<<lb, kThreads, 0, c->stream>>>(a, r, ip0, n);
+        }
         const cudaError_t e = launch_walk_variant(c, a, r, n, acc, blocks);
         if (e != cudaSuccess) return e;
     }
@@ -729,29 +1008,30 @@ cudaError_t launch_transport_diffuse(mochii_ctx* c, double total, long long nd) 
 }
 
 cudaError_t launch_rates(mochii_ctx* c) {
-    const double h = 0.5 * c->grid.dcell;
-    const double w = 2.0 * h;
-    const double fac = 1.0 / ((w * w * w) * (c->par.distance2cm * c->par.distance2cm));
+    const double d2 = c->par.distance2cm * c->par.distance2cm;
+    const double4* lg = c->oct.ncells > 0 ? c->oct.lgeo : nullptr;   // octree: per-leaf volume
+    const double w = c->grid.dcell;
+    const double fac = lg ? 1.0 : 1.0 / ((w * w * w) * d2);
     const double Lp = c->band.ion_Ltot / (double)c->par.nphotons;
     const double cg = Lp * 1.0e-18 / kEv2erg * fac;
     const double ch = Lp * 1.0e-18 * fac;
     const long long n = c->grid.nleaf;
     const int blocks = grid_blocks(n, 256, 148 * 16);
     if (c->fp32) {
-        if (c->ntally == 2) k_rates<float2, 2><<<blocks, 256, 0, c->stream>>>((const float2*)c->tally, c->rates, n, cg, ch);
-        else k_rates<float2, 6><<<blocks, 256, 0, c->stream>>>((const float2*)c->tally, c->rates, n, cg, ch);
+        if (c->ntally == 2) k_rates<float2, 2><<<blocks, 256, 0, c->stream>>>((const float2*)c->tally, c->rates, n, cg, ch, lg, d2);
+        else k_rates<float2, 6><<<blocks, 256, 0, c->stream>>>((const float2*)c->tally, c->rates, n, cg, ch, lg, d2);
     } else {
-        if (c->ntally == 2) k_rates<double, 2><<<blocks, 256, 0, c->stream>>>((const double*)c->tally, c->rates, n, cg, ch);
-        else k_rates<double, 6><<<blocks, 256, 0, c->stream>>>((const double*)c->tally, c->rates, n, cg, ch);
+        if (c->ntally == 2) k_rates<double, 2><<<blocks, 256, 0, c->stream>>>((const double*)c->tally, c->rates, n, cg, ch, lg, d2);
+        else k_rates<double, 6><<<blocks, 256, 0, c->stream>>>((const double*)c->tally, c->rates, n, cg, ch, lg, d2);
     }
     if (c->metal.ntr > 0 && c->metal.nmb > 0) {
         const int mb = grid_blocks(n * 32, 256, 148 * 32);
-        if (c->fp32) k_metal_rates_mom<float2><<<mb, 256, 0, c->stream>>>(c->metal, n, cg, ch);
-        else k_metal_rates_mom<double><<<mb, 256, 0, c->stream>>>(c->metal, n, cg, ch);
+        if (c->fp32) k_metal_rates_mom<float2><<<mb, 256, 0, c->stream>>>(c->metal, n, cg, ch, lg, d2);
+        else k_metal_rates_mom<double><<<mb, 256, 0, c->stream>>>(c->metal, n, cg, ch, lg, d2);
     } else if (c->metal.ntr > 0) {
         const int mb = grid_blocks(n * c->metal.ntr, 256, 148 * 16);
-        if (c->fp32) k_metal_rates<float2><<<mb, 256, 0, c->stream>>>(c->metal, n, cg, ch);
-        else k_metal_rates<double><<<mb, 256, 0, c->stream>>>(c->metal, n, cg, ch);
+        if (c->fp32) k_metal_rates<float2><<<mb, 256, 0, c->stream>>>(c->metal, n, cg, ch, lg, d2);
+        else k_metal_rates<double><<<mb, 256, 0, c->stream>>>(c->metal, n, cg, ch, lg, d2);
     }
     return cudaGetLastError();
 }
@@ -772,6 +1052,11 @@ cudaError_t launch_sobol(const QmcTables* t, int stream01, long long idx0, long 
 }
 
 cudaError_t launch_walk(mochii_ctx* c, const double* rays, long long nray, int max_steps, int* leaves, int* nsteps) {
+    if (c->oct.ncells > 0) {
+        k_walk_amr_leaves<<<grid_blocks(nray, 128, 1 << 20), 128, 0, c->stream>>>(rays, nray, max_steps, leaves,
+                                                                                 nsteps, c->oct);
+        return cudaGetLastError();
+    }
     k_walk<<<grid_blocks(nray, 128, 1 << 20), 128, 0, c->stream>>>(rays, nray, max_steps, leaves, nsteps,
                                                                      c->grid.xmin, c->grid.ymin, c->grid.zmin,
                                                                      c->grid.dcell, c->grid.nx, c->grid.ny, c->grid.nz);
@@ -844,14 +1129,19 @@ namespace mochii {
 namespace {
 // Dump of packet records for the test hooks: start cell, tMax, the H I
 // cross section and the bin, as (ix, iy, iz, tMax_x, tMax_y, tMax_z,
-// sigma_HI*1e18, inu).
+// sigma_HI*1e18, inu); on the octree (leaf, -1, -1, x, y, z, sigma_HI*1e18,
+// inu).
 template <typename R>
-__global__ void k_records_dump(const PacketRecords r, long long n, double* out) {
+__global__ void k_records_dump(const PacketRecords r, long long n, double* out, int amr) {
     const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const int cell = r.cell[i];
     double* o = out + 8 * i;
-    o[0] = cell & 1023; o[1] = (cell >> 10) & 1023; o[2] = (cell >> 20) & 1023;
+    if (amr) {
+        o[0] = cell; o[1] = -1.0; o[2] = -1.0;
+    } else {
+        o[0] = cell & 1023; o[1] = (cell >> 10) & 1023; o[2] = (cell >> 20) & 1023;
+    }
     o[3] = r.tm[i]; o[4] = r.tm[r.cap + i]; o[5] = r.tm[2 * r.cap + i];
     o[6] = (double)static_cast<const R*>(r.sig)[i];
     o[7] = (double)(r.bits[i] & 0xFFFF);
@@ -863,8 +1153,9 @@ cudaError_t launch_records_from_buffer(mochii_ctx* c, long long n, double* host_
     cudaError_t e = cudaMallocAsync(&d, (size_t)n * 64, c->stream);
     if (e != cudaSuccess) return e;
     const PacketRecords r = packet_records(c);
-    if (c->fp32) k_records_dump<float><<<grid_blocks(n, 128, 1 << 30), 128, 0, c->stream>>>(r, n, d);
-    else k_records_dump<double><<<grid_blocks(n, 128, 1 << 30), 128, 0, c->stream>>>(r, n, d);
+    const int amr = c->oct.ncells > 0;
+    if (c->fp32) k_records_dump<float><<<grid_blocks(n, 128, 1 << 30), 128, 0, c->stream>>>(r, n, d, amr);
+    else k_records_dump<double><<<grid_blocks(n, 128, 1 << 30), 128, 0, c->stream>>>(r, n, d, amr);
     e = cudaGetLastError();
     if (e == cudaSuccess) e = cudaMemcpyAsync(host_out, d, (size_t)n * 64, cudaMemcpyDeviceToHost, c->stream);
     cudaFreeAsync(d, c->stream);

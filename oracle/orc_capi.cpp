@@ -392,7 +392,10 @@ int orc_sim_walk_leaves(void* h, long long nray, const double* rays, int max_ste
     auto* s = static_cast<Sim*>(h);
     for (long long r = 0; r < nray; ++r) {
         const double* q = rays + 6 * r;
-        nsteps[r] = s->walk_leaves_car(q[0], q[1], q[2], q[3], q[4], q[5], max_steps, leaves + r * max_steps);
+        nsteps[r] = s->grid.car
+                        ? s->walk_leaves_car(q[0], q[1], q[2], q[3], q[4], q[5], max_steps, leaves + r * max_steps)
+                        : s->walk_leaves_amr(q[0], q[1], q[2], q[3], q[4], q[5], max_steps, leaves + r * max_steps);
+        for (int k = nsteps[r]; k < max_steps; ++k) leaves[r * max_steps + k] = -1;
     }
     return 0;
 }

@@ -3,6 +3,7 @@
 #include "orc_core.h"
 #include "orc_thermal.h"
 #include "orc_species.h"
+#include "orc_amr.h"
 
 #include <algorithm>
 #include <cctype>
@@ -944,8 +945,12 @@ bool Sim::setup(const std::string& nl, std::string* err) {
     rm.recomb = par.recomb_model == "hui_gnedin" ? RECOMB_HUI_GNEDIN : RECOMB_BADNELL_MILNE;
     rm.ci = par.ci_model == "dere_hybrid" ? CI_DERE_HYBRID : CI_VORONOV;
     qmc.setup(par.qmc_seed);
-    if (par.grid_type != "car") {
-        set_err(err, "oracle: only the namelist car grid is restated");
+    if (par.grid_type != "car" && par.grid_type != "amr") {
+        set_err(err, "oracle: grid_type must be 'car' or 'amr'");
+        return false;
+    }
+    if (par.grid_type == "car" && !par.amr_file.empty()) {
+        set_err(err, "oracle: a 'car' grid from a leaf file is not restated");
         return false;
     }
     if (par.ion_add_dust || par.use_sec_ion || par.add_fuv) {
@@ -956,35 +961,71 @@ bool Sim::setup(const std::string& nl, std::string* err) {
         th = new Thermal();
         if (!th->setup(par, err)) return false;
     }
-    // namelist car grid, grid_mod_amr.f90:64-133,193-198 and octree_mod.f90:648-674
-    grid.car = true;
-    grid.nx = par.nx;
-    grid.ny = par.ny;
-    grid.nz = par.nz;
-    grid.nleaf = par.nx * par.ny * par.nz;
-    grid.xmin = -par.xmax; grid.xmax = par.xmax;
-    grid.ymin = -par.ymax; grid.ymax = par.ymax;
-    grid.zmin = -par.zmax; grid.zmax = par.zmax;
-    grid.dcell = (grid.xmax - grid.xmin) / (double)grid.nx;
-    const int nleaf = grid.nleaf;
-    const double dcx = 2.0 * par.xmax / (double)par.nx;
-    const double dcy = 2.0 * par.ymax / (double)par.ny;
-    const double dcz = 2.0 * par.zmax / (double)par.nz;
-    st.nH.assign(nleaf, 1.0);
-    int il = 0;
-    for (int iz = 0; iz < par.nz; ++iz)
-        for (int iy = 0; iy < par.ny; ++iy)
-            for (int ix = 0; ix < par.nx; ++ix, ++il) {
-                const double xl = -par.xmax + ((double)ix + 0.5) * dcx;
-                const double yl = -par.ymax + ((double)iy + 0.5) * dcy;
-                const double zl = -par.zmax + ((double)iz + 0.5) * dcz;
-                if (par.nH_const >= 0.0) st.nH[il] = par.nH_const;
-                if (par.rmax > 0.0 || par.rmin > 0.0) {
-                    const double rho = std::sqrt(xl * xl + yl * yl + zl * zl);
-                    if (par.rmax > 0.0 && rho > par.rmax) st.nH[il] = 0.0;
-                    if (par.rmin > 0.0 && rho < par.rmin) st.nH[il] = 0.0;
+    std::vector<double> xl, yl, zl;
+    if (par.grid_type == "amr") {
+        // leaf-list octree, grid_mod_amr.f90:50-62 and octree_mod.f90:342-479
+        std::vector<int> lev;
+        double boxlen = 0.0;
+        if (!read_leaf_list(par.amr_file, xl, yl, zl, lev, st.nH, &boxlen, err)) return false;
+        const double half = 0.5 * boxlen;
+        par.xmax = par.ymax = par.zmax = half;
+        grid.car = false;
+        grid.oct = new Octree();
+        grid.oct->build(xl, yl, zl, lev, half);
+        grid.nleaf = (int)xl.size();
+        grid.xmin = grid.ymin = grid.zmin = -half;
+        grid.xmax = grid.ymax = grid.zmax = half;
+        grid.dcell = 0.0;
+        grid.lhalf.resize(grid.nleaf);
+        grid.lcx.resize(grid.nleaf); grid.lcy.resize(grid.nleaf); grid.lcz.resize(grid.nleaf);
+        for (int l = 0; l < grid.nleaf; ++l) {
+            const int c = grid.oct->icell_of_leaf[l];
+            grid.lhalf[l] = grid.oct->ch[c];
+            grid.lcx[l] = grid.oct->cx[c]; grid.lcy[l] = grid.oct->cy[c]; grid.lcz[l] = grid.oct->cz[c];
+        }
+    } else {
+        // namelist car grid, grid_mod_amr.f90:64-133,193-198 and octree_mod.f90:648-674
+        grid.car = true;
+        grid.nx = par.nx;
+        grid.ny = par.ny;
+        grid.nz = par.nz;
+        grid.nleaf = par.nx * par.ny * par.nz;
+        grid.xmin = -par.xmax; grid.xmax = par.xmax;
+        grid.ymin = -par.ymax; grid.ymax = par.ymax;
+        grid.zmin = -par.zmax; grid.zmax = par.zmax;
+        grid.dcell = (grid.xmax - grid.xmin) / (double)grid.nx;
+        const double dcx = 2.0 * par.xmax / (double)par.nx;
+        const double dcy = 2.0 * par.ymax / (double)par.ny;
+        const double dcz = 2.0 * par.zmax / (double)par.nz;
+        st.nH.assign(grid.nleaf, 1.0);
+        xl.resize(grid.nleaf); yl.resize(grid.nleaf); zl.resize(grid.nleaf);
+        int il = 0;
+        for (int iz = 0; iz < par.nz; ++iz)
+            for (int iy = 0; iy < par.ny; ++iy)
+                for (int ix = 0; ix < par.nx; ++ix, ++il) {
+                    xl[il] = -par.xmax + ((double)ix + 0.5) * dcx;
+                    yl[il] = -par.ymax + ((double)iy + 0.5) * dcy;
+                    zl[il] = -par.zmax + ((double)iz + 0.5) * dcz;
                 }
-            }
+        grid.lhalf.assign(grid.nleaf, 0.5 * grid.dcell);
+        grid.lcx.resize(grid.nleaf); grid.lcy.resize(grid.nleaf); grid.lcz.resize(grid.nleaf);
+        for (int l = 0; l < grid.nleaf; ++l) {   // cell_cx, octree_mod.f90:113-121
+            const int ix = l % grid.nx, iy = (l / grid.nx) % grid.ny, iz = l / (grid.nx * grid.ny);
+            grid.lcx[l] = grid.xmin + ((double)ix + 0.5) * grid.dcell;
+            grid.lcy[l] = grid.ymin + ((double)iy + 0.5) * grid.dcell;
+            grid.lcz[l] = grid.zmin + ((double)iz + 0.5) * grid.dcell;
+        }
+    }
+    const int nleaf = grid.nleaf;
+    // gas-density model on the leaf centres, grid_mod_amr.f90:137-147
+    for (int il = 0; il < nleaf; ++il) {
+        if (par.nH_const >= 0.0) st.nH[il] = par.nH_const;
+        if (par.rmax > 0.0 || par.rmin > 0.0) {
+            const double rho = std::sqrt(xl[il] * xl[il] + yl[il] * yl[il] + zl[il] * zl[il]);
+            if (par.rmax > 0.0 && rho > par.rmax) st.nH[il] = 0.0;
+            if (par.rmin > 0.0 && rho < par.rmin) st.nH[il] = 0.0;
+        }
+    }
     // gas_state_setup, gas_state_mod.f90:58-77
     st.xHI.assign(nleaf, par.xHI_init);
     st.xHeI.assign(nleaf, par.xHeI_init);
@@ -1058,6 +1099,7 @@ void Sim::gen_photon_qmc(int64_t ip, Photon& ph) const {
     ph.wgt = 1.0;
     ph.Lpacket = band.ion_Ltot / (double)par.nphotons;
     ph.E = e;
+    ph.il = grid.car ? -1 : grid.oct->find_leaf(ph.x, ph.y, ph.z);   // emit_point_qmc, ion_band_mod.f90:2245
     ph.sHI = sigma_HI(e);
     ph.sHeI = sigma_HeI(e);
     ph.sHeII = sigma_HeII(e);
@@ -1146,6 +1188,68 @@ void Sim::walk_edge_car(const Photon& ph, Tally& t, double* tau_edge) const {
     *tau_edge = tau;
 }
 
+void Sim::walk_edge(const Photon& ph, Tally& t, double* tau_edge) const {
+    if (grid.car) walk_edge_car(ph, t, tau_edge);
+    else walk_edge_amr(ph, t, tau_edge);
+}
+
+// raytrace_ion_to_edge_amr, raytrace_amr.f90:422-486 (no xy-periodic wrap).
+void Sim::walk_edge_amr(const Photon& ph, Tally& t, double* tau_edge) const {
+    const Octree& o = *grid.oct;
+    double x = ph.x, y = ph.y, z = ph.z;
+    const double kx = ph.kx, ky = ph.ky, kz = ph.kz;
+    int il = ph.il;
+    const double wl = ph.wgt * ph.Lpacket;
+    double expo = 1.0, tau = 0.0;
+    *tau_edge = 0.0;
+    if (il < 0) il = o.find_leaf(x, y, z);
+    if (il < 0) return;
+    int nstep = 0;
+    for (;;) {
+        if (++nstep > MAX_WALK_STEPS) break;
+        const int icell = o.icell_of_leaf[il];
+        double texit;
+        int iface;
+        o.cell_exit(icell, x, y, z, kx, ky, kz, &texit, &iface);
+        const double kap = opacity(*this, ph, il);
+        if (kap * texit > 0.0) {
+            const double expo_out = expo * std::exp(-kap * texit);
+            score(*this, ph, il, wl * (expo - expo_out) / kap, t);
+            expo = expo_out;
+        } else {
+            score(*this, ph, il, wl * expo * texit, t);
+        }
+        tau = tau + kap * texit;
+        if (tau >= TAU_HUGE) break;
+        x = x + texit * kx;
+        y = y + texit * ky;
+        z = z + texit * kz;
+        const int nl = o.next_leaf(icell, iface, x, y, z);
+        if (nl < 0) break;
+        il = nl;
+    }
+    *tau_edge = tau;
+}
+
+// Geometry-only octree walk: the leaf sequence of one ray, 0-based.
+int Sim::walk_leaves_amr(double x, double y, double z, double kx, double ky, double kz, int max_steps,
+                         int32_t* out) const {
+    const Octree& o = *grid.oct;
+    int il = o.find_leaf(x, y, z), ns = 0;
+    while (il >= 0 && ns < max_steps) {
+        out[ns++] = il;
+        const int icell = o.icell_of_leaf[il];
+        double texit;
+        int iface;
+        o.cell_exit(icell, x, y, z, kx, ky, kz, &texit, &iface);
+        x = x + texit * kx;
+        y = y + texit * ky;
+        z = z + texit * kz;
+        il = o.next_leaf(icell, iface, x, y, z);
+    }
+    return ns;
+}
+
 // Geometry-only DDA (no tau cut): the leaf sequence of one ray, 0-based.
 int Sim::walk_leaves_car(double x, double y, double z, double kx, double ky,
                          double kz, int max_steps, int32_t* out) const {
@@ -1201,7 +1305,7 @@ void Sim::transport_pass() {
         for (int64_t ip = 1 + tid; ip <= np; ip += nt) {
             gen_photon_qmc(ip - 1, ph);
             double tau_edge = 0.0;
-            walk_edge_car(ph, t, &tau_edge);
+            walk_edge(ph, t, &tau_edge);
             // ion_score_energy_packet, ion_score_mod.f90:233-252 (x87 extended)
             const double lum = ph.Lpacket * ph.wgt;
             const double tr = std::exp(-std::max(tau_edge, 0.0));
@@ -1226,7 +1330,7 @@ void Sim::transport_pass() {
             for (int64_t ip = 1 + tid; ip <= nd; ip += nt) {
                 gen_diffuse_qmc(ip - 1, ph);
                 double tau_edge = 0.0;
-                walk_edge_car(ph, t, &tau_edge);
+                walk_edge(ph, t, &tau_edge);
                 const double lum = ph.Lpacket * ph.wgt;
                 const double tr = std::exp(-std::max(tau_edge, 0.0));
                 t.emitted += (long double)lum;
@@ -1239,8 +1343,12 @@ void Sim::transport_pass() {
     for (auto& t : loc) tally.add(t);
     gas_rates_compute();
     if (metals()) {   // species_gamma_compute, species_mod.f90:493-512
-        const double w = grid.dcell;
-        sp->gamma_compute(tally.metal, 1.0 / ((w * w * w) * (par.distance2cm * par.distance2cm)));
+        std::vector<double> fac(nleaf);
+        for (int il = 0; il < nleaf; ++il) {
+            const double w = 2.0 * grid.lhalf[il];
+            fac[il] = 1.0 / ((w * w * w) * (par.distance2cm * par.distance2cm));
+        }
+        sp->gamma_compute(tally.metal, fac);
     }
 }
 
@@ -1363,11 +1471,11 @@ void Sim::diffuse_build(double lpacket) {
     const int nleaf = grid.nleaf;
     dif_ch.assign((size_t)4 * nleaf, 0.0);
     dif_cdf.assign(nleaf, 0.0);
-    const double w = grid.dcell * par.distance2cm;
-    const double vol = w * w * w;
     for (int il = 0; il < nleaf; ++il) {
         const double nH = st.nH[il];
         if (nH <= 0.0) continue;
+        const double w = 2.0 * grid.lhalf[il] * par.distance2cm;
+        const double vol = w * w * w;
         const double T = st.Te[il], ne = st.ne[il];
         const double kT = KBOLTZ_CGS * T / EV2ERG;
         const double xHeIII = std::max(0.0, 1.0 - st.xHeI[il] - st.xHeII[il]);
@@ -1411,11 +1519,11 @@ void Sim::gen_diffuse_qmc(int64_t ip, Photon& ph) const {
         if (dif_cdf[mid - 1] < u[0]) lo = mid + 1; else hi = mid;
     }
     const int il = lo - 1;
-    const int ix = il % grid.nx, iy = (il / grid.nx) % grid.ny, iz = il / (grid.nx * grid.ny);
-    const double half = 0.5 * grid.dcell;
-    ph.x = (grid.xmin + ((double)ix + 0.5) * grid.dcell) + (2.0 * u[1] - 1.0) * half;
-    ph.y = (grid.ymin + ((double)iy + 0.5) * grid.dcell) + (2.0 * u[2] - 1.0) * half;
-    ph.z = (grid.zmin + ((double)iz + 0.5) * grid.dcell) + (2.0 * u[3] - 1.0) * half;
+    const double half = grid.lhalf[il];
+    ph.x = grid.lcx[il] + (2.0 * u[1] - 1.0) * half;
+    ph.y = grid.lcy[il] + (2.0 * u[2] - 1.0) * half;
+    ph.z = grid.lcz[il] + (2.0 * u[3] - 1.0) * half;
+    ph.il = il;
     const double cost = 2.0 * u[4] - 1.0;
     const double sint = std::sqrt(1.0 - cost * cost);
     const double phi = TWOPI * u[5];
@@ -1451,10 +1559,9 @@ void Sim::gen_diffuse_qmc(int64_t ip, Photon& ph) const {
 // ion_score_mod.f90:298-317.
 void Sim::gas_rates_compute() {
     const int nleaf = grid.nleaf;
-    const double h = 0.5 * grid.dcell;
-    const double w = 2.0 * h;
-    const double fac = 1.0 / ((w * w * w) * (par.distance2cm * par.distance2cm));
     for (int il = 0; il < nleaf; ++il) {
+        const double w = 2.0 * grid.lhalf[il];
+        const double fac = 1.0 / ((w * w * w) * (par.distance2cm * par.distance2cm));
         const double* t = &tally.hhe[(size_t)6 * il];
         gamma_HI[il] = t[0] * fac;
         gamma_HeI[il] = t[1] * fac;
@@ -1517,6 +1624,7 @@ void solve_ion_cell(const RateModel& rm, double yHe, double gH, double gHe1,
 Sim::~Sim() {
     delete th;
     delete sp;
+    delete grid.oct;
 }
 
 // net_rate, thermal_mod.f90:38-115 (H/He; no metals, no grain PE, no
@@ -1587,11 +1695,11 @@ void Sim::gas_thermal_update(double m[4]) {
             ne_new[il] = charge_neutrality_ne(*sp, rm, il, te, nH, ne_new[il], xHI_new[il], ne);
         te_new[il] = te;
     }
-    const double hw = grid.dcell;
-    const double vol = hw * hw * hw;
     double mx = 0.0, mt = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0, s4 = 0.0;
     for (int il = 0; il < nleaf; ++il) {
         if (st.nH[il] <= 0.0) continue;
+        const double hw = 2.0 * grid.lhalf[il];
+        const double vol = hw * hw * hw;
         mx = std::max(mx, std::fabs(xHI_new[il] - st.xHI[il]));
         mt = std::max(mt, std::fabs(te_new[il] - st.Te[il]) / st.Te[il]);
         s1 = s1 + vol * std::fabs(xHI_new[il] - st.xHI[il]);
@@ -1630,11 +1738,11 @@ void Sim::gas_equilibrium_update(double* max_dx, double* dx_vol) {
         if (par.metal_ne && metals())   // ion_balance_mod.f90:401-410
             ne_new[il] = charge_neutrality_ne(*sp, rm, il, T, nH, ne_new[il], xHI_new[il], ne);
     }
-    const double hw = grid.dcell;
-    const double vol = hw * hw * hw;
     double mdx = 0.0, sdx = 0.0, sx = 0.0;
     for (int il = 0; il < nleaf; ++il) {
         if (st.nH[il] <= 0.0) continue;
+        const double hw = 2.0 * grid.lhalf[il];
+        const double vol = hw * hw * hw;
         const double d = std::fabs(xHI_new[il] - st.xHI[il]);
         mdx = std::max(mdx, d);
         sdx = sdx + vol * d;

@@ -176,10 +176,13 @@ int ion_bin_of(const Band& b, double e, bool include_fuv);
 bool band_setup(const Par& p, Band& b, std::string* err, const std::vector<double>& meth = {});
 
 // ---- car grid + state ----------------------------------------------------
+struct Octree;
 struct Grid {
     bool car = true;
     int nx = 0, ny = 0, nz = 0, nleaf = 0;
     double xmin, xmax, ymin, ymax, zmin, zmax, dcell;
+    std::vector<double> lhalf, lcx, lcy, lcz;   // per-leaf half width and centre (leaf_half, leaf_cx..)
+    Octree* oct = nullptr;                      // grid_type = 'amr'
 };
 struct State {
     std::vector<double> nH, xHI, xHeI, xHeII, ne, Te, rhokap;
@@ -203,6 +206,7 @@ struct Photon {
     double sHI, sHeI, sHeII;
     int nm = 0;                      // active metal transitions (E >= E_th)
     double sm[64];                   // their cross sections, threshold order
+    int il = -1;                     // leaf of the start point (photon%icell_amr)
 };
 
 struct Thermal;
@@ -253,6 +257,10 @@ struct Sim {
     ~Sim();
     void gen_photon_qmc(int64_t ip, Photon& ph) const;          // ion_band_mod.f90:1880
     void walk_edge_car(const Photon& ph, Tally& t, double* tau_edge) const;  // raytrace_amr.f90:534
+    void walk_edge_amr(const Photon& ph, Tally& t, double* tau_edge) const;  // raytrace_amr.f90:422-486
+    void walk_edge(const Photon& ph, Tally& t, double* tau_edge) const;
+    int walk_leaves_amr(double x, double y, double z, double kx, double ky, double kz, int max_steps,
+                        int32_t* out) const;
     int walk_leaves_car(double x, double y, double z, double kx, double ky,
                         double kz, int max_steps, int32_t* out) const;
 };

@@ -184,13 +184,13 @@ void Species::score(double E, const double* sig, int n, int il, double path_lum,
     }
 }
 
-void Species::gamma_compute(const std::vector<double>& raw, double fac) {
+void Species::gamma_compute(const std::vector<double>& raw, const std::vector<double>& fac) {
     for (int ie = 0; ie < (int)el.size(); ++ie)
         for (int it = 1; it <= el[ie].nstage - 1; ++it) {
             const int k = flat_of[ie][it - 1];
             for (int il = 0; il < nleaf; ++il) {
-                egam[ie][(size_t)(it - 1) * nleaf + il] = raw[((size_t)il * ntr + k) * 2 + 0] * fac;
-                eheat[ie][(size_t)(it - 1) * nleaf + il] = raw[((size_t)il * ntr + k) * 2 + 1] * fac;
+                egam[ie][(size_t)(it - 1) * nleaf + il] = raw[((size_t)il * ntr + k) * 2 + 0] * fac[il];
+                eheat[ie][(size_t)(it - 1) * nleaf + il] = raw[((size_t)il * ntr + k) * 2 + 1] * fac[il];
             }
         }
 }

@@ -62,7 +62,7 @@ struct Species {
     double cached_opacity(const double* sig, int n, int il) const;              // :291-303
     // species_rate_path_score (:329-343); raw is [(il*ntr + k)*2 + m]
     void score(double E, const double* sig, int n, int il, double path_lum, double* raw) const;
-    void gamma_compute(const std::vector<double>& raw, double fac);             // :493-512
+    void gamma_compute(const std::vector<double>& raw, const std::vector<double>& fac);   // :493-512
     double alpha_rec(const Element& e, int it, double T) const;                 // :428-447
     void prepare(int il, double T, const RateModel& rm, MetalCache& c) const;   // :517-536
     void metal_sums(const MetalCache& c, double nH, double ne, double nHI, double nHII, double& nem,

@@ -38,3 +38,24 @@ def golden_qmc():
 def golden_rates():
     import numpy as np
     return np.load(os.path.join(GOLDEN, "rates_golden.npz"))
+
+
+def octree_leaf_list(path, boxlen, base_level=2, max_level=5, p_split=0.35, seed=7, n0=100.0):
+    """A small irregular octree for the parity tests: every cell of levels
+    base_level..max_level-1 splits with probability p_split (seeded), so face
+    neighbours differ by up to max_level - base_level levels; n_H varies
+    smoothly around n0.  Writes the text leaf list, returns the leaf count."""
+    import numpy as np
+    from mochii_b200 import amr
+    rng = np.random.default_rng(seed)
+
+    def refine(x, y, z, lev):
+        r = np.sqrt(x * x + y * y + z * z) / boxlen
+        return rng.random(np.shape(x)) < p_split * (1.5 - r)
+
+    def dens(x, y, z, lev):
+        return n0 * np.exp(0.4 * np.sin(6.0 * x / boxlen) * np.cos(5.0 * y / boxlen) + 0.2 * z / boxlen)
+
+    x, y, z, lev, nH = amr.build_leaves(boxlen, base_level, max_level, refine, dens)
+    amr.write_leaf_list(path, boxlen, x, y, z, lev, nH)
+    return len(x)

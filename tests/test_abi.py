@@ -135,11 +135,16 @@ def test_init_without_device_reports_status(lib):
 def test_unsupported_configurations_are_refused_before_device_use(lib):
     from mochii_b200 import MochiiError, Nebula, parse_namelist
     from mochii_b200 import configs
-    for extra in ("par%grid_type = 'amr'", "par%launch_sequence = 'random'", "par%ion_add_dust = .true."):
+    for extra in ("par%car_walk = 'amr'", "par%launch_sequence = 'random'", "par%ion_add_dust = .true."):
         p = parse_namelist(configs.stromgren64(nphotons=1000, n=8).replace("/\n", extra + "\n/\n"))
         with pytest.raises(MochiiError) as ei:
             Nebula(p)
         assert ei.value.status == 8, extra   # MOCHII_ERR_UNSUPPORTED
+    # an octree needs its leaf list
+    p = parse_namelist(configs.stromgren64(nphotons=1000, n=8).replace("par%grid_type = 'car'", "par%grid_type = 'amr'"))
+    with pytest.raises(MochiiError) as ei:
+        Nebula(p)
+    assert ei.value.status == 1 and "amr_file" in str(ei.value)
 
 
 def test_bad_grid_is_refused(lib):

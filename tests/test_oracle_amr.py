@@ -1,0 +1,86 @@
+"""The oracle's octree (octree_mod.f90 restatement) against geometry computed
+independently: the leaf sequence of a ray through the tree is the list of
+leaves whose boxes the ray crosses with positive length, ordered by entry
+distance (slab intersection of the ray with every leaf box).  Also the leaf
+lists written by mochii_b200.amr: they tile the box exactly and come in
+Morton order.
+"""
+import numpy as np
+import pytest
+
+from conftest import octree_leaf_list
+from mochii_b200 import amr, configs
+
+
+def slab_intervals(leaves, o, k):
+    """Entry and exit distances of the ray o + t k through every leaf box."""
+    c = leaves[:, :3]
+    h = 0.5 * leaves[:, 5:6]
+    lo, hi = c - h, c + h
+    with np.errstate(divide="ignore", invalid="ignore"):
+        ta = (lo - o) / k
+        tb = (hi - o) / k
+    t0 = np.minimum(ta, tb)
+    t1 = np.maximum(ta, tb)
+    for a in range(3):
+        if k[a] == 0.0:
+            inside = (o[a] >= lo[:, a]) & (o[a] < hi[:, a])
+            t0[:, a] = np.where(inside, -np.inf, np.inf)
+            t1[:, a] = np.where(inside, np.inf, -np.inf)
+    return t0.max(axis=1), t1.min(axis=1)
+
+
+@pytest.fixture(scope="module")
+def tree(tmp_path_factory, orc):
+    path = str(tmp_path_factory.mktemp("amr") / "leaves.txt")
+    boxlen = 8.0
+    nleaf = octree_leaf_list(path, boxlen, base_level=2, max_level=5, seed=11)
+    d = np.loadtxt(path, skiprows=1)
+    side = boxlen / 2.0 ** d[:, 3]
+    leaves = np.column_stack([d[:, :3], d[:, 3], d[:, 4], side])
+    nl = configs.on_octree(configs.stromgren64(nphotons=1000, niter=1, precision="fp64"), path)
+    sim = orc.Sim(nl)
+    return sim, leaves, boxlen, nleaf
+
+
+def test_leaf_list_tiles_the_box_in_morton_order(tree):
+    _, leaves, boxlen, nleaf = tree
+    assert leaves.shape[0] == nleaf
+    assert abs(np.sum(leaves[:, 5] ** 3) / boxlen ** 3 - 1.0) < 1e-12
+    # Morton order: the lower corners on the finest lattice have increasing keys
+    fine = 1 << 5
+    ijk = np.round((leaves[:, :3] - 0.5 * leaves[:, 5:6] + 0.5 * boxlen) / boxlen * fine).astype(np.int64)
+    key = amr._morton(ijk[:, 0], ijk[:, 1], ijk[:, 2], 5)
+    assert np.all(np.diff(key.astype(np.int64)) > 0)
+
+
+def test_generated_levels_and_density_model():
+    x, y, z, lev, nH = amr.build_leaves(4.0, 1, 3, lambda x, y, z, L: x > 0, lambda x, y, z, L: 10.0 + x)
+    # x > 0 half refined twice: 4 coarse leaves on the -x side, 4*8*8 fine ones on the +x side
+    assert np.bincount(lev).tolist() == [0, 4, 0, 256]
+    np.testing.assert_array_equal(nH, 10.0 + x)
+
+
+def test_oracle_octree_walk_matches_slab_geometry(tree):
+    sim, leaves, boxlen, _ = tree
+    rng = np.random.default_rng(3)
+    nray = 300
+    o = rng.uniform(-0.49 * boxlen, 0.49 * boxlen, (nray, 3))
+    o[:40] = 0.0   # from the box centre, a corner of eight base cells
+    mu = rng.uniform(-1, 1, nray)
+    ph = rng.uniform(0, 2 * np.pi, nray)
+    k = np.column_stack([np.sqrt(1 - mu * mu) * np.cos(ph), np.sqrt(1 - mu * mu) * np.sin(ph), mu])
+    k[40:46] = [[1, 0, 0], [-1, 0, 0], [0, 1, 0], [0, -1, 0], [0, 0, 1], [0, 0, -1]]
+    rays = np.column_stack([o, k])
+    seq, ns = sim.walk_leaves(rays, 512)
+    eps = 1e-9 * boxlen
+    for r in range(nray):
+        t0, t1 = slab_intervals(leaves, o[r], k[r])
+        t0 = np.maximum(t0, 0.0)
+        crossed = np.nonzero(t1 - t0 > eps)[0]
+        expect = crossed[np.argsort(t0[crossed], kind="stable")]
+        got = seq[r, :ns[r]]
+        # leaves the walk touches for a vanishing length (an edge or corner) are not in the slab list
+        got_long = got[(t1[got] - t0[got]) > eps]
+        assert np.array_equal(got_long, expect), r
+        assert np.all(t1[got] - t0[got] > -eps), r   # every visited leaf is on the ray
