@@ -132,6 +132,9 @@ typedef struct mochii_params {
      * iterations, n_e from the cell's current state and T_e from a warm start
      * (the cell's current T_e, or a supplied prediction) */
     int solver_bracketed;
+    /* grain optics reference wavelength [um] and the dust normalisations
+     * (define.f90:211-212,361); taumax / tauhomo > 0 are not built */
+    double lambda_ref, taumax, tauhomo;
 } mochii_params;
 
 /* Per-pass statistics (ion_score_report_energy_closure, ion_score_mod.f90:364-387). */
@@ -241,6 +244,12 @@ double mochii_ion_Ltot(const mochii_ctx* ctx);
  * (qmc_uniforms_stream, qmc_mod.f90:157-168): out[i*nd + d] for the 0-based
  * indices idx0 .. idx0+n-1, stream 1 (stellar) or 2 (diffuse), nd <= 12. */
 int mochii_sobol_uniforms(int seed, int stream, int64_t idx0, int64_t n, int nd, double* out);
+/* The scattered flights' random numbers computed on the device: draws
+ * n0 .. n0+n-1 of the Philox4x32-10 stream of one packet (key par%iseed and
+ * stream 0 stellar / 1 diffuse, counter = the packet index).  No reference
+ * counterpart: the reference draws these from a per-rank MT19937
+ * (random.f90 rand_number, used at raytrace_amr.f90:268-320). */
+int mochii_philox_uniforms(int64_t seed, int stream, int64_t packet, int n0, int n, double* out);
 /* Geometry-only cell walk of nray rays (x,y,z,kx,ky,kz each, code units)
  * on ctx's grid (raytrace_ion_to_edge_car, raytrace_amr.f90:534-592, with
  * no optical-depth cut): leaves[r*max_steps + s] (0-based leaf index, -1

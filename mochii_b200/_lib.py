@@ -53,6 +53,7 @@ class Params(C.Structure):
         ("ion_dust_kext", C.c_char * STRLEN), ("data_dir", C.c_char * STRLEN), ("atomic_dir", C.c_char * STRLEN),
         ("precision", C.c_int),
         ("fe_levels_full", C.c_int), ("metal_moments", C.c_int), ("solver_bracketed", C.c_int),
+        ("lambda_ref", C.c_double), ("taumax", C.c_double), ("tauhomo", C.c_double),
     ]
 
 
@@ -109,6 +110,7 @@ SIGNATURES = {
     "mochii_set_nphotons": (C.c_int, [C.c_void_p, C.c_int64]),
     "mochii_ion_Ltot": (C.c_double, [C.c_void_p]),
     "mochii_sobol_uniforms": (C.c_int, [C.c_int, C.c_int, C.c_int64, C.c_int64, C.c_int, C.c_void_p]),
+    "mochii_philox_uniforms": (C.c_int, [C.c_int64, C.c_int, C.c_int64, C.c_int, C.c_int, C.c_void_p]),
     "mochii_walk_leaves": (C.c_int, [C.c_void_p, C.c_int64, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]),
     "mochii_launch_records": (C.c_int, [C.c_void_p, C.c_int64, C.c_int64, C.c_void_p]),
     "mochii_autotune": (C.c_int, [C.c_void_p, C.c_int64, _P(Tuning)]),

@@ -44,7 +44,7 @@ cudaError_t dalloc(T** p, size_t n) {
 
 void free_records(mochii_ctx* c) {
     for (void* q : {(void*)c->rec.tm, (void*)c->rec.td, (void*)c->rec.cell, (void*)c->rec.bits, c->rec.sig, c->rec.coef,
-                    (void*)c->rec.E, c->rec.msig})
+                    (void*)c->rec.E, c->rec.msig, c->rec.dsc, (void*)c->rec.p0})
         if (q) cudaFree(q);
     c->rec = RecordBuffers();
 }
@@ -58,8 +58,13 @@ cudaError_t alloc_records(mochii_ctx* c, long long cap) {
     if ((e = dalloc(&c->rec.td, 3 * (size_t)cap)) != cudaSuccess) return e;
     if ((e = dalloc(&c->rec.cell, (size_t)cap)) != cudaSuccess) return e;
     if ((e = dalloc(&c->rec.bits, (size_t)cap)) != cudaSuccess) return e;
-    if ((e = cudaMalloc(&c->rec.sig, 3 * (size_t)cap * rsz + 64)) != cudaSuccess) return e;
-    if ((e = cudaMalloc(&c->rec.coef, 6 * (size_t)cap * rsz + 64)) != cudaSuccess) return e;
+    const size_t nsig = c->xscore ? 4 : 3, ncoef = c->xscore ? 8 : 6;   // + grain / FUV rows
+    if ((e = cudaMalloc(&c->rec.sig, nsig * (size_t)cap * rsz + 64)) != cudaSuccess) return e;
+    if ((e = cudaMalloc(&c->rec.coef, ncoef * (size_t)cap * rsz + 64)) != cudaSuccess) return e;
+    if (c->scatter) {
+        if ((e = cudaMalloc(&c->rec.dsc, 2 * (size_t)cap * rsz + 64)) != cudaSuccess) return e;
+        if (c->oct.ncells == 0 && (e = dalloc(&c->rec.p0, 6 * (size_t)cap)) != cudaSuccess) return e;
+    }
     if (c->metal.ntr > 0) {
         if ((e = dalloc(&c->rec.E, (size_t)cap)) != cudaSuccess) return e;
         if ((e = cudaMalloc(&c->rec.msig, (size_t)c->metal.ntrp * cap * rsz + 64)) != cudaSuccess) return e;
@@ -77,7 +82,8 @@ void release(mochii_ctx* c) {
                     c->dif.ch, c->dif.tot, c->dif.scan_tmp, c->dif.tables,
                     (void*)c->metal.el, c->metal.egam, c->metal.eheat, c->metal.opac, c->metal.raw,
                     (void*)c->metal.medge, c->metal.mom, c->twarm,
-                    (void*)c->rec.E, c->rec.msig, c->oct_blob};
+                    (void*)c->rec.E, c->rec.msig, c->oct_blob, c->rec.dsc, (void*)c->rec.p0,
+                    (void*)c->dust_blob, (void*)c->rhokap};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     for (cudaEvent_t e : {c->ev0, c->ev1, c->evA, c->evB})
@@ -103,12 +109,15 @@ int validate(const mochii_params& p, std::string* why, int* code) {
     if (p.He_abund < 0.0) return *why = "par%He_abund must be >= 0", 1;
     if (!p.grid_car && !p.amr_file[0]) return *why = "grid_type='amr' needs par%amr_file (a text leaf list)", 1;
     *code = MOCHII_ERR_UNSUPPORTED;
-    if (p.grid_car && !p.car_walk_dda) return *why = "car_walk='amr' is not built; use the DDA walk (car_walk='dda')", 1;
     if (!p.source_point) return *why = "only internal point sources are built", 1;
     if (!p.launch_sobol) return *why = "launch_sequence='random' is not built; use 'sobol'", 1;
-    if (p.ion_add_dust) return *why = "ion_add_dust is not built in this library version", 1;
+    if (p.ion_add_dust && p.dust_law == 2)
+        return *why = "dust_density_law: only 'global_dgr' and 'none' are built", 1;
+    if (p.ion_add_dust && (p.taumax > 0.0 || p.tauhomo > 0.0))
+        return *why = "the taumax / tauhomo dust normalisations are not built", 1;
+    if (p.ion_add_dust && !p.ion_dust_kext[0])
+        return *why = "ion_add_dust needs par%ion_dust_kext (the grain-model optics are not built)", 1;
     if (p.use_sec_ion) return *why = "use_sec_ion is not built in this library version", 1;
-    if (p.add_fuv) return *why = "add_fuv is not built in this library version", 1;
     if (p.grain_pe) return *why = "grain_pe is not built in this library version", 1;
     return 0;
 }
@@ -193,8 +202,17 @@ extern "C" int mochii_init(const mochii_params* pin, mochii_ctx** out) {
         g.dcell = (g.xmax - g.xmin) / (double)g.nx;
     }
     c->fp32 = p.precision == MOCHII_PREC_FP32;
-    c->nabs = p.He_abund > 0.0 ? 4 : 1;
-    c->ntally = p.He_abund > 0.0 ? 6 : 2;
+    c->xscore = p.ion_add_dust || p.add_fuv;
+    c->scatter = p.ion_add_dust && p.ion_dust_scatter;
+    c->nabs = p.He_abund > 0.0 || c->xscore ? 4 : 1;
+    c->ntally = c->xscore ? 8 : p.He_abund > 0.0 ? 6 : 2;
+    if (p.ion_add_dust) {   // ion_dust_read (gas_opacity_mod.f90:69-121)
+        if (!dust_table_read(p.ion_dust_kext, p.lambda_ref, c->dust_host, &why)) {
+            delete c;
+            return fail(nullptr, MOCHII_ERR_TABLE, why);
+        }
+        c->dust.n = (int)c->dust_host.lam.size();
+    }
     c->nnu = c->band.nnu_band;
     const long long n = g.nleaf;
     auto bail = [&](int rc) {
@@ -231,25 +249,6 @@ extern "C" int mochii_init(const mochii_params* pin, mochii_ctx** out) {
         }
         for (long long i = 0; i < n; ++i)
             ne[i] = nH[i] * ((1.0 - xHI[i]) + p.He_abund * (xHeII[i] + 2.0 * std::max(0.0, 1.0 - xHeI[i] - xHeII[i])));
-        // the octree tables in one allocation: cell geo | children | leaf of cell | leaf geo | leaf faces
-        const size_t nc = oh.ncells, nl = oh.nleaf;
-        auto al = [](size_t b) { return (b + 255) & ~(size_t)255; };
-        const size_t b_geo = al(nc * 32), b_ch = al(nc * 32), b_il = al(nc * 4), b_lg = al(nl * 32), b_ln = al(nl * 32);
-        CKI(cudaMalloc(&c->oct_blob, b_geo + b_ch + b_il + b_lg + b_ln));
-        char* base = static_cast<char*>(c->oct_blob);
-        CKI(cudaMemcpy(base, oh.geo.data(), nc * 32, cudaMemcpyHostToDevice));
-        CKI(cudaMemcpy(base + b_geo, oh.children.data(), nc * 32, cudaMemcpyHostToDevice));
-        CKI(cudaMemcpy(base + b_geo + b_ch, oh.ileaf.data(), nc * 4, cudaMemcpyHostToDevice));
-        CKI(cudaMemcpy(base + b_geo + b_ch + b_il, oh.lgeo.data(), nl * 32, cudaMemcpyHostToDevice));
-        CKI(cudaMemcpy(base + b_geo + b_ch + b_il + b_lg, oh.lnext.data(), nl * 32, cudaMemcpyHostToDevice));
-        c->oct.ncells = oh.ncells;
-        c->oct.nshared = oh.nshared;
-        c->oct.half = oh.half;
-        c->oct.geo = reinterpret_cast<const double4*>(base);
-        c->oct.children = reinterpret_cast<const int*>(base + b_geo);
-        c->oct.ileaf = reinterpret_cast<const int*>(base + b_geo + b_ch);
-        c->oct.lgeo = reinterpret_cast<const double4*>(base + b_geo + b_ch + b_il);
-        c->oct.lnext = reinterpret_cast<const int*>(base + b_geo + b_ch + b_il + b_lg);
     } else {
         const double dcx = 2.0 * p.xmax / p.nx, dcy = 2.0 * p.ymax / p.ny, dcz = 2.0 * p.zmax / p.nz;
         long long il = 0;
@@ -269,6 +268,39 @@ extern "C" int mochii_init(const mochii_params* pin, mochii_ctx** out) {
         for (long long i = 0; i < n; ++i)
             ne[i] = nH[i] * ((1.0 - xHI[i]) + p.He_abund * (xHeII[i] + 2.0 * std::max(0.0, 1.0 - xHeI[i] - xHeII[i])));
     }
+    if (!p.grid_car || !p.car_walk_dda) {
+        if (p.grid_car) {   // par%car_walk = 'amr': the car grid's walk tables
+            car_walk_tables(g.nx, g.ny, g.nz, g.xmin, g.ymin, g.zmin, g.dcell, oh);
+            c->lhalf.assign(n, 0.5 * g.dcell);
+        }
+        // the octree tables in one allocation: cell geo | children | leaf of cell | leaf geo | leaf faces
+        const size_t nc = oh.ncells, nl = oh.nleaf;
+        auto al = [](size_t b) { return (b + 255) & ~(size_t)255; };
+        const size_t b_geo = al(nc * 32), b_ch = al(nc * 32), b_il = al(nc * 4), b_lg = al(nl * 32), b_ln = al(nl * 32);
+        CKI(cudaMalloc(&c->oct_blob, b_geo + b_ch + b_il + b_lg + b_ln));
+        char* base = static_cast<char*>(c->oct_blob);
+        CKI(cudaMemcpy(base, oh.geo.data(), nc * 32, cudaMemcpyHostToDevice));
+        CKI(cudaMemcpy(base + b_geo, oh.children.data(), nc * 32, cudaMemcpyHostToDevice));
+        CKI(cudaMemcpy(base + b_geo + b_ch, oh.ileaf.data(), nc * 4, cudaMemcpyHostToDevice));
+        CKI(cudaMemcpy(base + b_geo + b_ch + b_il, oh.lgeo.data(), nl * 32, cudaMemcpyHostToDevice));
+        CKI(cudaMemcpy(base + b_geo + b_ch + b_il + b_lg, oh.lnext.data(), nl * 32, cudaMemcpyHostToDevice));
+        c->oct.ncells = oh.ncells;
+        c->oct.nshared = oh.nshared;
+        c->oct.half = oh.half;
+        c->oct.geo = reinterpret_cast<const double4*>(base);
+        c->oct.children = reinterpret_cast<const int*>(base + b_geo);
+        c->oct.ileaf = reinterpret_cast<const int*>(base + b_geo + b_ch);
+        c->oct.lgeo = reinterpret_cast<const double4*>(base + b_geo + b_ch + b_il);
+        c->oct.lnext = reinterpret_cast<const int*>(base + b_geo + b_ch + b_il + b_lg);
+        if (p.grid_car) {
+            c->oct.ncells = (int)n;   // no cell tables: every walk step stays on leaves
+            c->oct.car = 1;
+            c->oct.n[0] = g.nx; c->oct.n[1] = g.ny; c->oct.n[2] = g.nz;
+            c->oct.org[0] = g.xmin; c->oct.org[1] = g.ymin; c->oct.org[2] = g.zmin;
+            c->oct.hi[0] = g.xmax; c->oct.hi[1] = g.ymax; c->oct.hi[2] = g.zmax;
+            c->oct.dcell = g.dcell;
+        }
+    }
     CKI(dalloc(&c->nH, n));
     CKI(dalloc(&c->xHI, n));
     CKI(dalloc(&c->xHeI, n));
@@ -286,7 +318,26 @@ extern "C" int mochii_init(const mochii_params* pin, mochii_ctx** out) {
     CKI(cudaMalloc(&c->col, (size_t)n * c->nabs * rsz + 64));
     CKI(cudaMalloc(&c->tally, (size_t)n * c->ntally * tsz + 64));
     CKI(cudaMalloc(&c->jt, (size_t)n * c->nnu * tsz + 64));
-    CKI(dalloc(&c->rates, 6 * (size_t)n));
+    CKI(dalloc(&c->rates, 8 * (size_t)n));   // gamma/heat of H I, He I, He II; heat_dust; G0
+    CKI(cudaMemsetAsync(c->rates, 0, 8 * (size_t)n * 8, c->stream));
+    if (c->dust.n > 0) {   // grey dust opacity per leaf, grid_mod_amr.f90:233-278 ('global_dgr' or 'none')
+        std::vector<double> rk(n, 0.0);
+        if (p.dust_law == 0)
+            for (long long il = 0; il < n; ++il) rk[il] = nH[il] * p.cext_dust * p.DGR * p.distance2cm;
+        CKI(dalloc(&c->rhokap, (size_t)n));
+        CKI(cudaMemcpy(c->rhokap, rk.data(), n * 8, cudaMemcpyHostToDevice));
+        const size_t nd = c->dust_host.lam.size();
+        CKI(dalloc(&c->dust_blob, 4 * nd));
+        CKI(cudaMemcpy(c->dust_blob, c->dust_host.lam.data(), nd * 8, cudaMemcpyHostToDevice));
+        CKI(cudaMemcpy(c->dust_blob + nd, c->dust_host.alb.data(), nd * 8, cudaMemcpyHostToDevice));
+        CKI(cudaMemcpy(c->dust_blob + 2 * nd, c->dust_host.gcos.data(), nd * 8, cudaMemcpyHostToDevice));
+        CKI(cudaMemcpy(c->dust_blob + 3 * nd, c->dust_host.cext.data(), nd * 8, cudaMemcpyHostToDevice));
+        c->dust.lam = c->dust_blob;
+        c->dust.alb = c->dust_blob + nd;
+        c->dust.gcos = c->dust_blob + 2 * nd;
+        c->dust.cext = c->dust_blob + 3 * nd;
+        c->dust.cref = c->dust_host.cref;
+    }
     CKI(cudaMemset(c->rates, 0, 6 * (size_t)n * 8));
     if (!c->species.tr.empty()) {
         // registry tables in one blob: el | tr | st | photo | form | eth | lamref | Ssup
@@ -525,6 +576,7 @@ extern "C" int mochii_transport_pass(mochii_ctx* c, int with_peel, mochii_pass_s
     s.closure = std::fabs(s.energy_absorbed + s.energy_escaped - s.energy_emitted) /
                 std::max(s.energy_emitted, kTinest);
     s.direct_segments = (int64_t)cnt[0];
+    s.scattered_segments = (int64_t)cnt[3];
     s.walk_kills = (int64_t)cnt[1];
     s.metal_active = (int64_t)cnt[2];
     s.kernel_ms = ms;
@@ -692,9 +744,11 @@ double* field_ptr(mochii_ctx* c, const std::string& n, long long* count) {
     if (n == "x_HeII") return c->xHeII;
     if (n == "n_e") return c->ne;
     if (n == "T_e") return c->Te;
-    static const char* rn[6] = {"gamma_HI", "gamma_HeI", "gamma_HeII", "heat_HI", "heat_HeI", "heat_HeII"};
-    for (int k = 0; k < 6; ++k)
+    static const char* rn[8] = {"gamma_HI", "gamma_HeI", "gamma_HeII", "heat_HI", "heat_HeI", "heat_HeII",
+                                "heat_dust", "g0_fuv"};
+    for (int k = 0; k < 8; ++k)
         if (n == rn[k]) return c->rates + (size_t)k * nl;
+    if (n == "rhokap") return c->rhokap;   // null (no such field) without grains
     return nullptr;
 }
 }  // namespace
@@ -806,6 +860,19 @@ extern "C" int mochii_sobol_uniforms(int seed, int stream, int64_t idx0, int64_t
     CKS(cudaStreamSynchronize(s));
 #undef CKS
     cleanup();
+    return MOCHII_OK;
+}
+
+extern "C" int mochii_philox_uniforms(int64_t seed, int stream, int64_t packet, int n0, int n, double* out) {
+    if (!out || n < 0 || n0 < 0 || packet < 0 || (stream != 0 && stream != 1))
+        return fail(nullptr, MOCHII_ERR_BAD_PARAM, "mochii_philox_uniforms: bad argument");
+    if (n == 0) return MOCHII_OK;
+    double* d = nullptr;
+    cudaError_t e = cudaMalloc(&d, (size_t)n * 8);
+    if (e == cudaSuccess) e = launch_philox((uint64_t)seed, (uint32_t)stream, (uint64_t)packet, n0, n, d);
+    if (e == cudaSuccess) e = cudaMemcpy(out, d, (size_t)n * 8, cudaMemcpyDeviceToHost);
+    if (d) cudaFree(d);
+    if (e != cudaSuccess) return fail(nullptr, MOCHII_ERR_CUDA, std::string("mochii_philox_uniforms: ") + cudaGetErrorString(e));
     return MOCHII_OK;
 }
 

@@ -42,6 +42,7 @@ struct BalArgs {
     long long nleaf;
     double T, yHe, relax, colscale, vol;
     const double4* lg;                // octree leaf geometry (per-leaf volume), null on the Cartesian grid
+    const double* rhokap;             // grey dust opacity per leaf, null without grains
     RateSel rs;
     Coef k;   // coefficients at the fixed temperature (equilibrium update)
     int caseA, nabs, fp32;
@@ -58,9 +59,11 @@ __device__ __forceinline__ double leaf_vol(const BalArgs& a, long long il) {
     return w * w * w;
 }
 
-// Absorber columns n_i * distance2cm * 1e-18 for one leaf.
+// Absorber columns n_i * distance2cm * 1e-18 for one leaf; the fourth
+// slot of the 4-wide layout holds the grey dust opacity per code length
+// rhokap (0 without grains).
 __device__ __forceinline__ void write_columns(void* col, long long il, int nabs, int fp32, double nH, double yHe,
-                                              double xHI, double xHeI, double xHeII, double scale) {
+                                              double xHI, double xHeI, double xHeII, double scale, double rk) {
     const double c0 = nH * xHI * scale;
     if (nabs == 1) {
         if (fp32) static_cast<float*>(col)[il] = (float)c0;
@@ -69,11 +72,11 @@ __device__ __forceinline__ void write_columns(void* col, long long il, int nabs,
     }
     const double c1 = nH * yHe * xHeI * scale, c2 = nH * yHe * xHeII * scale;
     if (fp32) {
-        static_cast<float4*>(col)[il] = make_float4((float)c0, (float)c1, (float)c2, 0.0f);
+        static_cast<float4*>(col)[il] = make_float4((float)c0, (float)c1, (float)c2, (float)rk);
     } else {
         double2* p = static_cast<double2*>(col) + 2 * il;
         p[0] = make_double2(c0, c1);
-        p[1] = make_double2(c2, 0.0);
+        p[1] = make_double2(c2, rk);
     }
 }
 
@@ -90,10 +93,12 @@ __device__ __noinline__ void metal_fill_at(const MetalDev& m, MetalCache& mc, lo
 __global__ void k_columns(const double* __restrict__ nH, const double* __restrict__ xHI,
                           const double* __restrict__ xHeI, const double* __restrict__ xHeII,
                           const double* __restrict__ ne, const double* __restrict__ Te, void* col,
-                          long long nleaf, int nabs, int fp32, double yHe, double scale, const MetalDev m) {
+                          long long nleaf, int nabs, int fp32, double yHe, double scale, const MetalDev m,
+                          const double* __restrict__ rhokap) {
     for (long long il = (long long)blockIdx.x * blockDim.x + threadIdx.x; il < nleaf;
          il += (long long)gridDim.x * blockDim.x) {
-        write_columns(col, il, nabs, fp32, nH[il], yHe, xHI[il], xHeI[il], xHeII[il], scale);
+        write_columns(col, il, nabs, fp32, nH[il], yHe, xHI[il], xHeI[il], xHeII[il], scale,
+                      rhokap ? rhokap[il] : 0.0);
         if (m.ntr > 0) {
             MetalCache mc;
             metal_fill_at(m, mc, il, Te[il], nH[il], ne[il], xHI[il], scale, fp32);
@@ -292,7 +297,7 @@ __global__ void __launch_bounds__(kBThreads) k_balance(const BalArgs a) {
         const double x0 = a.xHI[il], h10 = a.xHeI[il], h20 = a.xHeII[il];
         if (nH <= 0.0) {   // ion_balance_mod.f90:383-387
             a.ne[il] = 0.0;
-            write_columns(a.col, il, a.nabs, a.fp32, nH, a.yHe, x0, h10, h20, a.colscale);
+            write_columns(a.col, il, a.nabs, a.fp32, nH, a.yHe, x0, h10, h20, a.colscale, a.rhokap ? a.rhokap[il] : 0.0);
             continue;
         }
         double xHI = x0, xHeI = h10, xHeII = h20, ne;
@@ -334,7 +339,7 @@ __global__ void __launch_bounds__(kBThreads) k_balance(const BalArgs a) {
             else metal_opacity_fill<double>(a.m, mc, il, nH, nen, xn, a.colscale);
         }
         a.ne[il] = nen;
-        write_columns(a.col, il, a.nabs, a.fp32, nH, a.yHe, xn, h1n, h2n, a.colscale);
+        write_columns(a.col, il, a.nabs, a.fp32, nH, a.yHe, xn, h1n, h2n, a.colscale, a.rhokap ? a.rhokap[il] : 0.0);
         const double dx = fabs(xn - x0);
         const double vol = leaf_vol(a, il);
         mdx = fmax(mdx, dx);
@@ -608,7 +613,7 @@ __global__ void __launch_bounds__(kBThreads) k_thermal(const ThArgs a) {
         const double x0 = b.xHI[il], h10 = b.xHeI[il], h20 = b.xHeII[il], T0 = b.Te[il];
         if (nH <= 0.0) {
             b.ne[il] = 0.0;
-            write_columns(b.col, il, b.nabs, b.fp32, nH, b.yHe, x0, h10, h20, b.colscale);
+            write_columns(b.col, il, b.nabs, b.fp32, nH, b.yHe, x0, h10, h20, b.colscale, b.rhokap ? b.rhokap[il] : 0.0);
             continue;
         }
         double xHI = x0, xHeI = h10, xHeII = h20, ne = 0.0;
@@ -663,7 +668,7 @@ __global__ void __launch_bounds__(kBThreads) k_thermal(const ThArgs a) {
         b.xHeII[il] = h2n;
         b.ne[il] = nen;
         b.Te[il] = te;
-        write_columns(b.col, il, b.nabs, b.fp32, nH, b.yHe, xn, h1n, h2n, b.colscale);
+        write_columns(b.col, il, b.nabs, b.fp32, nH, b.yHe, xn, h1n, h2n, b.colscale, b.rhokap ? b.rhokap[il] : 0.0);
         const double dx = fabs(xn - x0);
         mdx = fmax(mdx, dx);
         mdt = fmax(mdt, fabs(te - T0) / T0);
@@ -749,7 +754,7 @@ int balance_blocks(const mochii_ctx* c) {
 cudaError_t launch_columns(mochii_ctx* c) {
     k_columns<<<nblocks(c->grid.nleaf, 256, 148 * 16), 256, 0, c->stream>>>(
         c->nH, c->xHI, c->xHeI, c->xHeII, c->ne, c->Te, c->col, c->grid.nleaf, c->nabs, c->fp32 ? 1 : 0,
-        c->par.He_abund, c->par.distance2cm * 1.0e-18, c->metal);
+        c->par.He_abund, c->par.distance2cm * 1.0e-18, c->metal, c->rhokap);
     return cudaGetLastError();
 }
 
@@ -779,6 +784,7 @@ static BalArgs bal_args(mochii_ctx* c) {
     const double w = c->grid.dcell;   // (2*leaf_half)^3 on the uniform grid
     a.vol = w * w * w;
     a.lg = c->oct.ncells > 0 ? c->oct.lgeo : nullptr;
+    a.rhokap = c->rhokap;
     a.rs.hui_gnedin = c->par.recomb_hui_gnedin;
     a.rs.dere_hybrid = c->par.ci_dere_hybrid;
     a.caseA = c->par.caseA;

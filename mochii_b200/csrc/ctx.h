@@ -8,6 +8,7 @@
 
 #include "band.h"
 #include "diffuse.h"
+#include "dust.h"
 #include "mochii_gpu.h"
 #include "octree.h"
 #include "qmc.cuh"
@@ -58,6 +59,8 @@ struct RecordBuffers {
     void* coef = nullptr;
     double* E = nullptr;      // metals: packet energy
     void* msig = nullptr;     // metals: ntrp x cap cross sections
+    void* dsc = nullptr;      // scattering: 2 x cap (dust scattering coefficient, <cos>)
+    double* p0 = nullptr;     // scattering on the Cartesian grid: start point and direction, 6 x cap
     long long cap = 0;
 };
 
@@ -102,6 +105,12 @@ struct mochii_ctx {
     mochii::MetalDev metal;         // trace metals (use_metals); metal.ntr == 0 without
     mochii::OctDev oct;             // grid_type = 'amr'; oct.ncells == 0 on the Cartesian grid
     void* oct_blob = nullptr;       // octree: the one allocation behind oct's pointers
+    mochii::DustDev dust;           // ion_add_dust grain optics; dust.n == 0 without
+    mochii::DustHost dust_host;
+    double* dust_blob = nullptr;    // the allocation behind dust's tables
+    double* rhokap = nullptr;       // ion_add_dust: grey dust opacity per leaf [1/code length]
+    bool xscore = false;            // dust or FUV path estimators (8 tallies per leaf)
+    bool scatter = false;           // ion_dust_scatter: forced first interaction and scattered flights
     std::vector<double> lhalf;      // octree: leaf half widths (host copy for leaf_half)
     double* twarm = nullptr;        // bracketed thermal solve: warm-start T_e per leaf ("T_warm")
     bool twarm_set = false;         // consumed by the next thermal update

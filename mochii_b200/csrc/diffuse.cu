@@ -200,6 +200,9 @@ struct DiffLaunchArgs {
     MilneDev m;
     MetalDev metal;
     const double4* lg;   // octree leaf geometry, null on the Cartesian grid
+    DustDev dust;        // grain optics; dust.n == 0 without
+    int xs, scatter;     // grain / FUV record terms; scattered flights
+    double eion_min;
     double total, org[3], dcell, eion_max;
     int n[3], nnu, nfuv, energy_model;
     long long nleaf;
@@ -271,6 +274,7 @@ __global__ void __launch_bounds__(kThreads) k_launch_diffuse(const DiffLaunchArg
     const int inu = min(max(blo, a.nfuv + 1), a.nnu) - 1;
     if (a.lg) write_record_amr<R>(rec, i, pos, kk, eph, inu, (int)il);
     else write_record<R>(rec, i, pos, kk, eph, inu, a.org, a.dcell, a.n);
+    if (a.xs) write_grain_record<R>(rec, i, a.dust, a.scatter, a.eion_min, eph, pos, kk, a.lg ? 0 : 1);
     if (a.metal.ntr > 0) write_metal_record<R>(rec, a.metal, i, eph);
 }
 
@@ -328,6 +332,10 @@ cudaError_t launch_diffuse_chunk(mochii_ctx* c, double total, long long ip0, lon
     a.org[0] = c->grid.xmin; a.org[1] = c->grid.ymin; a.org[2] = c->grid.zmin;
     a.metal = c->metal;
     a.lg = c->oct.ncells > 0 ? c->oct.lgeo : nullptr;
+    a.dust = c->dust;
+    a.xs = c->xscore ? 1 : 0;
+    a.scatter = c->scatter ? 1 : 0;
+    a.eion_min = c->par.eion_min;
     a.dcell = c->grid.dcell;
     a.eion_max = c->par.eion_max;
     a.n[0] = c->grid.nx; a.n[1] = c->grid.ny; a.n[2] = c->grid.nz;

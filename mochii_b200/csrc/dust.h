@@ -1,0 +1,37 @@
+// Grain optics of the ionizing band (gas_opacity_mod.f90) and the random
+// stream of the scattered flights.
+//
+// Host: the extinction table par%ion_dust_kext (ion_dust_read, :69-121):
+// the rows of four leading reals "lambda [um]  albedo  <cos>  C_ext/H" with
+// lambda > 0, sorted ascending in lambda (stable, as sort4 :258-275), and
+// C_ext at par%lambda_ref.  Device: the exact-energy evaluators
+// ion_dust_sabs_at / ssca_at / g_at (:231-256) over one copy of the table
+// (5 x n doubles), the interpolation bracket found by a binary search that
+// returns the bracket the reference's linear scan returns.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+namespace mochii {
+
+struct DustHost {
+    std::vector<double> lam, alb, gcos, cext;
+    double cref = 0.0;
+};
+
+// Read and sort the table; false with *err on failure.
+bool dust_table_read(const std::string& path, double lambda_ref, DustHost& d, std::string* err);
+
+struct DustDev {
+    int n = 0;                      // 0: no grain optics
+    const double* lam = nullptr;    // ascending [um]
+    const double* alb = nullptr;
+    const double* gcos = nullptr;
+    const double* cext = nullptr;
+    double cref = 0.0;
+};
+
+}  // namespace mochii

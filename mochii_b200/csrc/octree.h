@@ -45,6 +45,13 @@ struct OctDev {
     const int* ileaf = nullptr;         // per cell
     const double4* lgeo = nullptr;      // per leaf
     const int* lnext = nullptr;         // 8 per leaf
+    // the car grid walked as an octree (par%car_walk = 'amr'): leaves in
+    // raster order, no cell tables; the start leaf is car_index
+    int car = 0;
+    int n[3] = {0, 0, 0};
+    double org[3] = {0.0, 0.0, 0.0};   // xmin, ymin, zmin
+    double hi[3] = {0.0, 0.0, 0.0};    // xmax, ymax, zmax
+    double dcell = 0.0;
 };
 
 // read_generic_amr.f90:60-81 text leaf list: "nleaf boxlen", then
@@ -54,5 +61,8 @@ bool leaf_list_read(const std::string& path, std::vector<double>& x, std::vector
 // amr_build_tree + amr_build_neighbors (octree_mod.f90:342-479).
 bool octree_build(const std::vector<double>& x, const std::vector<double>& y, const std::vector<double>& z,
                   const std::vector<int>& lev, double half, OctHost& o, std::string* err);
+// The walk tables of the namelist car grid for par%car_walk = 'amr':
+// cell_cx/cy/cz/ch (octree_mod.f90:113-153) and car_next (:620-641).
+void car_walk_tables(int nx, int ny, int nz, double xmin, double ymin, double zmin, double dcell, OctHost& o);
 
 }  // namespace mochii

@@ -171,4 +171,30 @@ bool octree_build(const std::vector<double>& x, const std::vector<double>& y, co
     return true;
 }
 
+void car_walk_tables(int nx, int ny, int nz, double xmin, double ymin, double zmin, double dcell, OctHost& o) {
+    o = OctHost();
+    const long long n = (long long)nx * ny * nz;
+    o.nleaf = (int)n;
+    o.half = 0.5 * (dcell * nx);
+    o.lgeo.resize(4 * (size_t)n);
+    o.lnext.assign(8 * (size_t)n, -1);
+    long long il = 0;
+    for (int iz = 0; iz < nz; ++iz)
+        for (int iy = 0; iy < ny; ++iy)
+            for (int ix = 0; ix < nx; ++ix, ++il) {
+                double* g = &o.lgeo[4 * (size_t)il];
+                g[0] = xmin + ((double)ix + 0.5) * dcell;
+                g[1] = ymin + ((double)iy + 0.5) * dcell;
+                g[2] = zmin + ((double)iz + 0.5) * dcell;
+                g[3] = 0.5 * dcell;
+                int* f = &o.lnext[8 * (size_t)il];
+                if (ix + 1 < nx) f[0] = (int)(il + 1);
+                if (ix > 0) f[1] = (int)(il - 1);
+                if (iy + 1 < ny) f[2] = (int)(il + nx);
+                if (iy > 0) f[3] = (int)(il - nx);
+                if (iz + 1 < nz) f[4] = (int)(il + (long long)nx * ny);
+                if (iz > 0) f[5] = (int)(il - (long long)nx * ny);
+            }
+}
+
 }  // namespace mochii

@@ -33,7 +33,7 @@ const char* const kOtherKeys[] = {
     "emis_output", "exetime", "ext_geometry", "ext_intensity", "ext_scale", "ext_spectrum", "ext_tstar",
     "f_ion_dust", "f_ion_pah", "f_pah", "file_format", "gamma", "geometry", "h_coll_effects",
     "hei_diffuse", "hei_metastable", "hgg", "inclination_angle", "ion_peel", "ion_spectrum", "kext_file",
-    "lambda0", "lambda_max", "lambda_min", "lambda_ref", "line_case", "mrw_gamma", "nlambda", "no_print",
+    "lambda0", "lambda_max", "lambda_min", "line_case", "mrw_gamma", "nlambda", "no_print",
     "nobs", "nprint", "nr", "nscatt_tot", "num_send_at_once", "nxim", "nyim", "obsx", "obsy", "obsz",
     "out_bitpix", "out_bitpix_force", "out_file", "output_normalization", "pe_scale", "peel_bins",
     "phase_angle", "position_angle", "radiation_angular_pdf_file", "reduce_factor", "refine_dx",
@@ -44,7 +44,7 @@ const char* const kOtherKeys[] = {
     "slab_top_source", "slab_top_theta", "source_rscale", "source_spectrum", "source_zscale",
     "spectrum_type", "spiral_amp", "spiral_m", "spiral_pitch", "src_axial_ratio", "src_boxiness",
     "src_geometry", "src_reff", "src_rscale", "src_sersic_index", "src_spectrum", "src_spectrum_file",
-    "src_zscale", "tauhomo", "taumax", "use_amr_grid", "use_dustemis", "use_master_slave", "use_mrw",
+    "src_zscale", "use_amr_grid", "use_dustemis", "use_master_slave", "use_mrw",
     "use_reduced_wgt", "use_sed", "use_stokes", "xy_periodic", "xyz_symmetry", "z_global", "z_ref",
     "z_symmetry", "dust_density_law_file"};
 
@@ -134,6 +134,9 @@ extern "C" int mochii_params_default(mochii_params* p) {
     p->DGR = 1.0e-2; p->cext_dust = 1.6059e-21;
     p->precision = MOCHII_PREC_FP64;
     p->metal_moments = 1;
+    p->lambda_ref = 0.55;
+    p->taumax = -999.0;
+    p->tauhomo = -999.0;
     return MOCHII_OK;
 }
 
@@ -253,7 +256,8 @@ int set_key(mochii_params* p, std::string key, const std::vector<std::string>& v
     BOOL("fe_levels_full", fe_levels_full)
     BOOL("diffuse_field", diffuse_field) BOOL("use_sec_ion", use_sec_ion)
     BOOL("ion_add_dust", ion_add_dust) BOOL("ion_dust_scatter", ion_dust_scatter) BOOL("grain_pe", grain_pe)
-    REAL("dgr", DGR) REAL("cext_dust", cext_dust)
+    REAL("dgr", DGR) REAL("cext_dust", cext_dust) REAL("lambda_ref", lambda_ref)
+    REAL("taumax", taumax) REAL("tauhomo", tauhomo)
     if (key == "dust_density_law") {
         const std::string s = lower(unquote(v));
         p->dust_law = s == "global_dgr" ? 0 : s == "none" ? 1 : 2;

@@ -6,6 +6,7 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include "dust.cuh"
 #include "physics.cuh"
 
 namespace mochii {
@@ -16,9 +17,13 @@ struct PacketRecords {
     int* cell;     // ix | iy << 10 | iz << 20 (octree: start leaf, -1 outside)
     int* bits;     // inu | (stp_x+1) << 16 | (stp_y+1) << 18 | (stp_z+1) << 20 (octree: inu)
     void* sig;     // 3 x cap of R: sigma_HI, sigma_HeI, sigma_HeII in 1e-18 cm^2
+                   // (+ a 4th row with grains or FUV: the dust extinction coefficient)
     void* coef;    // 6 x cap of R: Gamma/heat coefficients per unit path
+                   // (+ rows 6, 7 with grains or FUV: dust absorption coefficient, E < eion_min)
     double* E;     // metals only: packet energy [eV]
     void* msig;    // metals only: ntrp x cap of R, active-prefix sigma_k in 1e-18 cm^2
+    void* dsc;     // scattering only: 2 x cap of R, dust scattering coefficient and <cos>
+    double* p0;    // scattering on the Cartesian grid: start point and direction, 6 x cap
     long long cap;
 };
 
@@ -37,6 +42,38 @@ __device__ __forceinline__ void write_cross_sections(const PacketRecords& rec, l
     cf[3 * c + i] = (R)(sHeI * 1.0e18 * fmax(1.0 - kEthHeI / E, 0.0));
     cf[4 * c + i] = (R)(sHeII * 1.0e18 / E);
     cf[5 * c + i] = (R)(sHeII * 1.0e18 * fmax(1.0 - kEthHeII / E, 0.0));
+}
+
+// The grain and FUV part of a packet record (build_ion_packet_physics
+// dust cache, ion_packet_mod.f90:42-50; score_ion_path dust_abs_path and
+// fuv_field_path terms, ion_score_mod.f90:163-166,206-209): the extinction
+// coefficient the walk multiplies with rhokap (absorption, plus scattering
+// when scattering is on), the absorption coefficient it scores, whether the
+// packet is an FUV packet, and for the scattered flights the scattering
+// coefficient, <cos> and (Cartesian grid) the start point and direction.
+template <typename R>
+__device__ __forceinline__ void write_grain_record(const PacketRecords& rec, long long i, const DustDev& d,
+                                                   int scatter, double eion_min, double E, const double pos[3],
+                                                   const double kk[3], int car) {
+    const long long c = rec.cap;
+    DustOptics o = {0.0, 0.0, 0.0};
+    if (d.n > 0) o = dust_optics(d, E);
+    static_cast<R*>(rec.sig)[3 * c + i] = (R)(scatter ? o.sabs + o.ssca : o.sabs);
+    R* cf = static_cast<R*>(rec.coef);
+    cf[6 * c + i] = (R)o.sabs;
+    cf[7 * c + i] = E < eion_min ? (R)1 : (R)0;
+    if (scatter) {
+        R* ds = static_cast<R*>(rec.dsc);
+        ds[i] = (R)o.ssca;
+        ds[c + i] = (R)o.g;
+        if (car) {
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                rec.p0[k * c + i] = pos[k];
+                rec.p0[(3 + k) * c + i] = kk[k];
+            }
+        }
+    }
 }
 
 // Record of one packet on the octree: the cross sections, start point,

@@ -57,6 +57,12 @@ struct PassArgs {
     MetalDev m;          // trace metals; m.ntr == 0 without
     int metal_abs;       // par%ion_metal_abs
     OctDev oct;          // octree grid; oct.ncells == 0 on the Cartesian grid
+    DustDev dust;        // grain optics (ion_add_dust); dust.n == 0 without
+    const double* rhokap;   // grey dust opacity per leaf (scattered flights' albedo)
+    int xs;              // dust or FUV path estimators (8 tallies per leaf)
+    int scatter;         // ion_dust_scatter
+    double eion_min;
+    unsigned long long seed;   // par%iseed: key of the scattered flights' streams
 };
 
 // ---- octree geometry (octree_mod.f90) ------------------------------------------
@@ -72,6 +78,13 @@ __device__ __forceinline__ double4 ld_geo(const double4* p) {
 // the copy staged in shared memory when the caller passes one.
 __device__ __forceinline__ int oct_find_leaf(const OctDev& o, double x, double y, double z,
                                              const double4* sgeo = nullptr, const int* schild = nullptr) {
+    if (o.car) {   // car_index (octree_mod.f90:185-195) inside the box
+        if (x < o.org[0] || x > o.hi[0] || y < o.org[1] || y > o.hi[1] || z < o.org[2] || z > o.hi[2]) return -1;
+        const int ix = min(max((int)((x - o.org[0]) / o.dcell), 0), o.n[0] - 1);
+        const int iy = min(max((int)((y - o.org[1]) / o.dcell), 0), o.n[1] - 1);
+        const int iz = min(max((int)((z - o.org[2]) / o.dcell), 0), o.n[2] - 1);
+        return ix + o.n[0] * (iy + o.n[1] * iz);
+    }
     const double h = o.half;
     if (x < -h || x > h || y < -h || y > h || z < -h || z > h) return -1;
     int c = 0;
@@ -287,31 +300,40 @@ __global__ void __launch_bounds__(kThreads) k_launch(const PassArgs a, PacketRec
         write_record_amr<R>(rec, i, pos, kk, E, inu, oct_find_leaf(a.oct, pos[0], pos[1], pos[2], sgeo, schild));
     else
         write_record<R>(rec, i, pos, kk, E, inu, a.org, a.dcell, a.n);
+    if (a.xs) write_grain_record<R>(rec, i, a.dust, a.scatter, a.eion_min, E, pos, kk, AMR ? 0 : 1);
     if (a.m.ntr > 0) write_metal_record<R>(rec, a.m, i, E);
 }
 
 // Absorber columns of one leaf, loaded ahead of use.
 template <typename R, int NABS> struct Col;
+// The 4-wide layout's fourth slot is the leaf's rhokap; with X (grains or
+// FUV) the packet's dust extinction coefficient s3 multiplies it.
 template <typename R> struct Col<R, 1> {
     R c0;
     __device__ __forceinline__ void load(const void* col, int il) { c0 = __ldg(static_cast<const R*>(col) + il); }
-    __device__ __forceinline__ R kappa(R s0, R, R) const { return c0 * s0; }
+    template <int X>
+    __device__ __forceinline__ R kappa(R s0, R, R, R) const { return c0 * s0; }
 };
 template <> struct Col<float, 4> {
     float4 c;
     __device__ __forceinline__ void load(const void* col, int il) { c = __ldg(static_cast<const float4*>(col) + il); }
-    __device__ __forceinline__ float kappa(float s0, float s1, float s2) const { return c.x * s0 + (c.y * s1 + c.z * s2); }
+    template <int X>
+    __device__ __forceinline__ float kappa(float s0, float s1, float s2, float s3) const {
+        const float k = c.x * s0 + (c.y * s1 + c.z * s2);
+        return X ? k + c.w * s3 : k;
+    }
 };
 template <> struct Col<double, 4> {
-    double2 a;
-    double b;
+    double2 a, b;
     __device__ __forceinline__ void load(const void* col, int il) {
         const double2* p = static_cast<const double2*>(col) + 2 * (long long)il;
         a = __ldg(p);
-        b = __ldg(reinterpret_cast<const double*>(p + 1));
+        b = __ldg(p + 1);
     }
-    __device__ __forceinline__ double kappa(double s0, double s1, double s2) const {
-        return a.x * s0 + (a.y * s1 + b * s2);
+    template <int X>
+    __device__ __forceinline__ double kappa(double s0, double s1, double s2, double s3) const {
+        const double k = a.x * s0 + (a.y * s1 + b.x * s2);
+        return X ? k + b.y * s3 : k;
     }
 };
 
@@ -343,11 +365,18 @@ struct Stepper {
 
 // H/He part of score_ion_path (ion_score_mod.f90:137-231): the rate tallies
 // of the leaf and its diagnostic spectrum bin.
+//
+// With grains or FUV (NT = 8) the last two tallies are dust_abs_path (w x the
+// dust absorption coefficient) and fuv_field_path (w for E < eion_min,
+// ion_score_mod.f90:163-166,206-209); a zero coefficient skips its update.
 template <typename T, typename R, int NT>
 __device__ __forceinline__ void score_hhe(T* tal, T* jt, int il, int nnu, int inu, R w, const R* cf) {
     T* tl = tal + (long long)il * NT;
 #pragma unroll
-    for (int k = 0; k < NT; ++k) tally_add(tl + k, w * cf[k]);
+    for (int k = 0; k < (NT < 6 ? NT : 6); ++k) tally_add(tl + k, w * cf[k]);
+#pragma unroll
+    for (int k = 6; k < NT; ++k)
+        if (cf[k] != (R)0) tally_add(tl + k, w * cf[k]);
     tally_add(jt + (long long)il * nnu + inu, w);
 }
 
@@ -429,7 +458,8 @@ struct MetalPacket {
 template <bool METAL>
 __device__ __forceinline__ void walk_epilogue(const PassArgs& a, double emitted, double absorbed, double escaped,
                                               unsigned long long nseg, unsigned long long kills,
-                                              unsigned long long nact, int accumulate, double* sh) {
+                                              unsigned long long nact, unsigned long long nscat, int accumulate,
+                                              double* sh) {
     const double e0 = block_sum(emitted, sh);
     const double e1 = block_sum(absorbed, sh);
     const double e2 = block_sum(escaped, sh);
@@ -444,12 +474,157 @@ __device__ __forceinline__ void walk_epilogue(const PassArgs& a, double emitted,
     for (int o = 16; o > 0; o >>= 1) {
         nseg += __shfl_down_sync(0xffffffffu, nseg, o);
         kills += __shfl_down_sync(0xffffffffu, kills, o);
+        nscat += __shfl_down_sync(0xffffffffu, nscat, o);
         if (METAL) nact += __shfl_down_sync(0xffffffffu, nact, o);
     }
     if ((threadIdx.x & 31) == 0) {
         if (nseg) atomicAdd(a.counters + 0, nseg);
         if (kills) atomicAdd(a.counters + 1, kills);
         if (METAL && nact) atomicAdd(a.counters + 2, nact);
+        if (nscat) atomicAdd(a.counters + 3, nscat);
+    }
+}
+
+// ---- scattered flights (transport_ion_packet, raytrace_amr.f90:249-323) -------
+constexpr int kMaxScatterings = 100000;   // a bound on scatterings per packet; the reference relies on the roulette
+
+// raytrace_ion_to_tau_amr (raytrace_amr.f90:348-420) on the octree and
+// raytrace_ion_to_tau_car (:594-676) on the Cartesian grid: from (x, y, z)
+// along k to optical depth tau_in (extinction kappa_at(leaf)); scattered
+// flights score every segment with wgt x length (score_at).  Returns whether
+// the packet is still inside; then (x, y, z) is the interaction point and il
+// its leaf.
+template <bool AMR, typename KapF, typename ScoreF>
+__device__ __forceinline__ bool walk_to_tau(const PassArgs& a, double tau_in, bool tally, double wgt, double& x,
+                                            double& y, double& z, double kx, double ky, double kz, int& il,
+                                            KapF& kappa_at, ScoreF& score_at, unsigned long long& kills) {
+    if constexpr (AMR) {
+        if (il < 0) il = oct_find_leaf(a.oct, x, y, z);
+        if (il < 0) return false;
+        double tau = 0.0;
+        for (int nstep = 1;; ++nstep) {
+            if (nstep > kMaxWalkSteps) { ++kills; return false; }
+            int face;
+            const double texit = oct_cell_exit(ld_geo(a.oct.lgeo + il), x, y, z, kx, ky, kz, &face);
+            const double kap = (double)kappa_at(il);
+            if (tau + texit * kap >= tau_in) {
+                const double d = kap > 0.0 ? (tau_in - tau) / kap : texit;
+                if (tally) score_at(il, wgt * d);
+                x = x + d * kx;
+                y = y + d * ky;
+                z = z + d * kz;
+                return true;
+            }
+            if (tally) score_at(il, wgt * texit);
+            tau = tau + texit * kap;
+            x = x + texit * kx;
+            y = y + texit * ky;
+            z = z + texit * kz;
+            const int nl = oct_next_leaf(a.oct, il, face, x, y, z);
+            if (nl < 0) return false;
+            il = nl;
+        }
+    } else {
+        // dda_init (raytrace_amr.f90:495-532) from the point
+        const double pos[3] = {x, y, z}, kk[3] = {kx, ky, kz};
+        int idx[3], stp[3];
+        double tmax[3], tdel[3];
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            idx[k] = min(max((int)((pos[k] - a.org[k]) / a.dcell), 0), a.n[k] - 1);
+            if (kk[k] > 0.0) {
+                stp[k] = 1; tmax[k] = (a.org[k] + (double)(idx[k] + 1) * a.dcell - pos[k]) / kk[k]; tdel[k] = a.dcell / kk[k];
+            } else if (kk[k] < 0.0) {
+                stp[k] = -1; tmax[k] = (a.org[k] + (double)idx[k] * a.dcell - pos[k]) / kk[k]; tdel[k] = -a.dcell / kk[k];
+            } else {
+                stp[k] = 0; tmax[k] = kHugest; tdel[k] = kHugest;
+            }
+        }
+        double tau = 0.0, t_cur = 0.0;
+        bool inside = true;
+        for (int nstep = 1;; ++nstep) {
+            if (nstep > kMaxWalkSteps) { ++kills; inside = false; break; }
+            const int c = idx[0] + a.n[0] * (idx[1] + a.n[1] * idx[2]);
+            int ax = 0;
+            if (tmax[1] < tmax[ax]) ax = 1;
+            if (tmax[2] < tmax[ax]) ax = 2;
+            const double seg = tmax[ax] - t_cur;
+            const double kap = (double)kappa_at(c);
+            if (tau + seg * kap >= tau_in) {
+                const double d = kap > 0.0 ? (tau_in - tau) / kap : seg;
+                if (tally) score_at(c, wgt * d);
+                t_cur = t_cur + d;
+                break;
+            }
+            if (tally) score_at(c, wgt * seg);
+            tau = tau + seg * kap;
+            t_cur = tmax[ax];
+            tmax[ax] = tmax[ax] + tdel[ax];
+            idx[ax] += stp[ax];
+            if (idx[ax] < 0 || idx[ax] >= a.n[ax]) { inside = false; break; }
+        }
+        x = x + t_cur * kx;
+        y = y + t_cur * ky;
+        z = z + t_cur * kz;
+        if (inside) il = idx[0] + a.n[0] * (idx[1] + a.n[1] * idx[2]);
+        return inside;
+    }
+}
+
+// The forced first interaction and the scattered flights of one packet
+// (transport_ion_packet after its edge walk): weight 1 - e^-tau_edge, the
+// albedo weight rhokap s_sca / kappa at each interaction, Russian roulette
+// below 1e-4 (survival 0.1), a Henyey-Greenstein direction about the
+// current one, an unforced flight to -ln(u).  Draws come from the packet's
+// Philox stream in the reference's order.
+template <bool AMR, typename KapF, typename ScoreF>
+__device__ __noinline__ void scattered_flights(const PassArgs& a, double x, double y, double z, double kx, double ky,
+                                               double kz, int il, double tau_edge, double ssca, double gg,
+                                               uint32_t stream, uint64_t packet, KapF kappa_at, ScoreF score_at,
+                                               unsigned long long& kills) {
+    PacketStream rs;
+    rs.init(a.seed, stream, packet);
+    const double w1 = 1.0 - exp(-tau_edge);
+    double wgt = w1;
+    double tau = -log(1.0 - rs.next() * w1);
+    bool inside = walk_to_tau<AMR>(a, tau, false, wgt, x, y, z, kx, ky, kz, il, kappa_at, score_at, kills);
+    for (int nev = 1; inside; ++nev) {
+        if (il < 0) break;
+        if (nev > kMaxScatterings) { ++kills; break; }
+        const double a_eff = __ldg(a.rhokap + il) * ssca / fmax((double)kappa_at(il), kTinest);
+        wgt = wgt * a_eff;
+        if (wgt < 1.0e-4) {
+            if (rs.next() > 0.1) break;
+            wgt = wgt / 0.1;
+        }
+        double cost;
+        if (fabs(gg) > 1.0e-3) {
+            const double q = (1.0 - gg * gg) / (1.0 + gg * (2.0 * rs.next() - 1.0));
+            cost = (1.0 + gg * gg - q * q) / (2.0 * gg);
+        } else {
+            cost = 2.0 * rs.next() - 1.0;
+        }
+        cost = fmin(fmax(cost, -1.0), 1.0);
+        const double sint = sqrt(1.0 - cost * cost);
+        const double phi = kTwoPi * rs.next();
+        double norm = sqrt(kx * kx + ky * ky + kz * kz);
+        if (norm <= 0.0) break;
+        kx = kx / norm; ky = ky / norm; kz = kz / norm;
+        double ux, uy, uz;
+        if (fabs(kz) < 0.99) { ux = -ky; uy = kx; uz = 0.0; }
+        else { ux = 0.0; uy = -kz; uz = ky; }
+        norm = sqrt(ux * ux + uy * uy + uz * uz);
+        ux = ux / norm; uy = uy / norm; uz = uz / norm;
+        const double vx = ky * uz - kz * uy, vy = kz * ux - kx * uz, vz = kx * uy - ky * ux;
+        double sp, cp;
+        sincos(phi, &sp, &cp);
+        const double nx = sint * (cp * ux + sp * vx) + cost * kx;
+        const double ny = sint * (cp * uy + sp * vy) + cost * ky;
+        const double nz = sint * (cp * uz + sp * vz) + cost * kz;
+        norm = sqrt(nx * nx + ny * ny + nz * nz);
+        kx = nx / norm; ky = ny / norm; kz = nz / norm;
+        tau = -log(fmax(rs.next(), kTinest));
+        inside = walk_to_tau<AMR>(a, tau, true, wgt, x, y, z, kx, ky, kz, il, kappa_at, score_at, kills);
     }
 }
 
@@ -458,19 +633,22 @@ __device__ __forceinline__ void walk_epilogue(const PassArgs& a, double emitted,
 // scoring: slot 0 is scored now, slots 1..LA have their column loads in
 // flight (LA = 0 disables the look-ahead).
 //
-// MET adds the trace-metal terms (MetalPacket: 1 exact tallies, 2 moments).
-template <typename R, int NABS, int LA, int MET>
+// MET adds the trace-metal terms (MetalPacket: 1 exact tallies, 2 moments);
+// X the grain and FUV terms (NABS = 4) and, with a.scatter, the scattered
+// flights after the edge walk.  Packet i of the chunk is packet ip0 + i of
+// its stream (0 stellar, 1 diffuse).
+template <typename R, int NABS, int LA, int MET, int X>
 __global__ void __launch_bounds__(128) k_walk_edge(const PassArgs a, const PacketRecords rec, long long n,
-                                                   int accumulate) {
+                                                   int accumulate, long long ip0, int stream) {
     typedef typename Acc<R>::T T;
-    constexpr int NT = NABS == 1 ? 2 : 6;
+    constexpr int NT = X ? 8 : (NABS == 1 ? 2 : 6);
     constexpr bool METAL = MET > 0;
     __shared__ double sh[128];
     extern __shared__ __align__(16) unsigned char dsm[];
     R* const msg = reinterpret_cast<R*>(dsm);                      // sigma_k      [k][thread]
     R* const mhc = msg + (MET == 1 ? a.m.ntrp * blockDim.x : 0);    // sigma_k h_k  [k][thread]
     double emitted = 0.0, absorbed = 0.0, escaped = 0.0;
-    unsigned long long nseg = 0, kills = 0, nact = 0;
+    unsigned long long nseg = 0, kills = 0, nact = 0, nscat = 0;
     T* tal = static_cast<T*>(a.tally);
     T* jt = static_cast<T*>(a.jt);
     const R* sg = static_cast<const R*>(rec.sig);
@@ -490,6 +668,7 @@ __global__ void __launch_bounds__(128) k_walk_edge(const PassArgs a, const Packe
         const R s0 = sg[i];
         const R s1 = NABS == 1 ? (R)0 : sg[c + i];
         const R s2 = NABS == 1 ? (R)0 : sg[2 * c + i];
+        const R s3 = X ? sg[3 * c + i] : (R)0;
         R cf[NT];
 #pragma unroll
         for (int k = 0; k < NT; ++k) cf[k] = cfp[k * c + i];
@@ -515,7 +694,7 @@ __global__ void __launch_bounds__(128) k_walk_edge(const PassArgs a, const Packe
         int nstep = 0;
         for (;;) {
             if (++nstep > kMaxWalkSteps) { ++kills; break; }
-            R kap = cl[0].kappa(s0, s1, s2);
+            R kap = cl[0].template kappa<X>(s0, s1, s2, s3);
             if constexpr (METAL) {
                 if (a.metal_abs) kap = kap + mp.kappa(a.m, il[0], msg);
             }
@@ -554,8 +733,34 @@ __global__ void __launch_bounds__(128) k_walk_edge(const PassArgs a, const Packe
         emitted += lum;
         absorbed += lum * (1.0 - tr);
         escaped += lum * tr;
+        if constexpr (X) {
+            if (a.scatter && tau > 1.0e-12) {
+                auto kappa_at = [&](int q) -> R {
+                    Col<R, NABS> cq;
+                    cq.load(a.col, q);
+                    R k = cq.template kappa<X>(s0, s1, s2, s3);
+                    if constexpr (METAL) {
+                        if (a.metal_abs) k = k + mp.kappa(a.m, q, msg);
+                    }
+                    return k;
+                };
+                auto score_at = [&](int q, double pl) {
+                    const R w = (R)pl;
+                    if (w != (R)0) {
+                        ++nscat;
+                        nact += mp.nm;
+                        score_hhe<T, R, NT>(tal, jt, q, a.nnu, inu, w, cf);
+                        if constexpr (METAL) mp.template score<T>(a.m, q, w, msg, mhc);
+                    }
+                };
+                const R* ds = static_cast<const R*>(rec.dsc);
+                scattered_flights<false>(a, rec.p0[i], rec.p0[c + i], rec.p0[2 * c + i], rec.p0[3 * c + i], rec.p0[4 * c + i],
+                                         rec.p0[5 * c + i], -1, tau, (double)ds[i], (double)ds[c + i], (uint32_t)stream,
+                                         (uint64_t)(ip0 + i), kappa_at, score_at, kills);
+            }
+        }
     }
-    walk_epilogue<METAL>(a, emitted, absorbed, escaped, nseg, kills, nact, accumulate, sh);
+    walk_epilogue<METAL>(a, emitted, absorbed, escaped, nseg, kills, nact, nscat, accumulate, sh);
 }
 
 // Walk kernel on the octree: raytrace_ion_to_edge_amr (raytrace_amr.f90:
@@ -564,19 +769,19 @@ __global__ void __launch_bounds__(128) k_walk_edge(const PassArgs a, const Packe
 // leaf-indexed, issued together), the exit face (amr_cell_exit), the
 // attenuated path score, the move to the exit point, and the leaf across the
 // face (amr_next_leaf).  Geometry in FP64 without contraction, as the
-// reference's.
-template <typename R, int NABS, int MET>
+// reference's.  MET, X, ip0 and stream as for k_walk_edge.
+template <typename R, int NABS, int MET, int X>
 __global__ void __launch_bounds__(128) k_walk_amr(const PassArgs a, const PacketRecords rec, long long n,
-                                                  int accumulate) {
+                                                  int accumulate, long long ip0, int stream) {
     typedef typename Acc<R>::T T;
-    constexpr int NT = NABS == 1 ? 2 : 6;
+    constexpr int NT = X ? 8 : (NABS == 1 ? 2 : 6);
     constexpr bool METAL = MET > 0;
     __shared__ double sh[128];
     extern __shared__ __align__(16) unsigned char dsm[];
     R* const msg = reinterpret_cast<R*>(dsm);
     R* const mhc = msg + (MET == 1 ? a.m.ntrp * blockDim.x : 0);
     double emitted = 0.0, absorbed = 0.0, escaped = 0.0;
-    unsigned long long nseg = 0, kills = 0, nact = 0;
+    unsigned long long nseg = 0, kills = 0, nact = 0, nscat = 0;
     T* tal = static_cast<T*>(a.tally);
     T* jt = static_cast<T*>(a.jt);
     const R* sg = static_cast<const R*>(rec.sig);
@@ -591,6 +796,7 @@ __global__ void __launch_bounds__(128) k_walk_amr(const PassArgs a, const Packet
         const R s0 = sg[i];
         const R s1 = NABS == 1 ? (R)0 : sg[c + i];
         const R s2 = NABS == 1 ? (R)0 : sg[2 * c + i];
+        const R s3 = X ? sg[3 * c + i] : (R)0;
         R cf[NT];
 #pragma unroll
         for (int k = 0; k < NT; ++k) cf[k] = cfp[k * c + i];
@@ -606,7 +812,7 @@ __global__ void __launch_bounds__(128) k_walk_amr(const PassArgs a, const Packet
             cl.load(a.col, il);
             int face;
             const double texit = oct_cell_exit(g, x, y, z, kx, ky, kz, &face);
-            R kap = cl.kappa(s0, s1, s2);
+            R kap = cl.template kappa<X>(s0, s1, s2, s3);
             if constexpr (METAL) {
                 if (a.metal_abs) kap = kap + mp.kappa(a.m, il, msg);
             }
@@ -637,8 +843,34 @@ __global__ void __launch_bounds__(128) k_walk_amr(const PassArgs a, const Packet
         emitted += lum;
         absorbed += lum * (1.0 - tr);
         escaped += lum * tr;
+        if constexpr (X) {
+            if (a.scatter && tau > 1.0e-12) {
+                auto kappa_at = [&](int q) -> R {
+                    Col<R, NABS> cq;
+                    cq.load(a.col, q);
+                    R k = cq.template kappa<X>(s0, s1, s2, s3);
+                    if constexpr (METAL) {
+                        if (a.metal_abs) k = k + mp.kappa(a.m, q, msg);
+                    }
+                    return k;
+                };
+                auto score_at = [&](int q, double pl) {
+                    const R w = (R)pl;
+                    if (w != (R)0) {
+                        ++nscat;
+                        nact += mp.nm;
+                        score_hhe<T, R, NT>(tal, jt, q, a.nnu, inu, w, cf);
+                        if constexpr (METAL) mp.template score<T>(a.m, q, w, msg, mhc);
+                    }
+                };
+                const R* ds = static_cast<const R*>(rec.dsc);
+                scattered_flights<true>(a, rec.tm[i], rec.tm[c + i], rec.tm[2 * c + i], kx, ky, kz, rec.cell[i], tau,
+                                        (double)ds[i], (double)ds[c + i], (uint32_t)stream, (uint64_t)(ip0 + i),
+                                        kappa_at, score_at, kills);
+            }
+        }
     }
-    walk_epilogue<METAL>(a, emitted, absorbed, escaped, nseg, kills, nact, accumulate, sh);
+    walk_epilogue<METAL>(a, emitted, absorbed, escaped, nseg, kills, nact, nscat, accumulate, sh);
 }
 
 // gas_rates_compute + ion_score_apply_hhe (gas_rates_mod.f90:82-153,
@@ -659,9 +891,13 @@ __device__ __forceinline__ double leaf_fac(const double4* lg, long long il, doub
     return 1.0 / ((w * w * w) * d2);
 }
 
+//
+// NT = 8 adds ion_score_apply_dust_heat and ion_score_apply_g0
+// (ion_score_mod.f90:319-355): heat_dust = sum(w s_abs) Lpacket fac rhokap /
+// distance2cm and G0 = sum_FUV(w) Lpacket fac / 1.6e-3, rows 6 and 7.
 template <typename T, int NT>
 __global__ void k_rates(const T* __restrict__ tal, double* __restrict__ rates, long long nleaf, double cg0, double ch0,
-                        const double4* lg, double d2) {
+                        const double4* lg, double d2, const double* __restrict__ rhokap, double d2cm) {
     for (long long il = (long long)blockIdx.x * blockDim.x + threadIdx.x; il < nleaf;
          il += (long long)gridDim.x * blockDim.x) {
         const double f = leaf_fac(lg, il, d2);
@@ -674,6 +910,11 @@ __global__ void k_rates(const T* __restrict__ tal, double* __restrict__ rates, l
             rates[4 * nleaf + il] = tval<T>(t[3]) * ch;
             rates[2 * nleaf + il] = tval<T>(t[4]) * cg;
             rates[5 * nleaf + il] = tval<T>(t[5]) * ch;
+            if (NT == 8) {
+                const double lf = ch * 1.0e18;   // Lpacket x fac
+                rates[6 * nleaf + il] = rhokap ? tval<T>(t[6]) * lf * rhokap[il] / d2cm : 0.0;
+                rates[7 * nleaf + il] = tval<T>(t[7]) * lf / 1.6e-3;
+            }
         } else {
             rates[1 * nleaf + il] = 0.0;
             rates[4 * nleaf + il] = 0.0;
@@ -742,6 +983,19 @@ __global__ void k_metal_rates_mom(const MetalDev m, long long nleaf, double cg, 
 __global__ void k_sobol(const QmcTables* t, int stream, long long idx0, long long n, int nd, double* out) {
     for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
         for (int d = 0; d < nd; ++d) out[i * nd + d] = qmc_uniform(*t, (uint64_t)(idx0 + i), d, stream);
+}
+
+// Draws n0 .. n0+n-1 of one packet's Philox stream, for the test hook (one
+// thread walks the stream in order, as a packet does).
+__global__ void k_philox(unsigned long long seed, unsigned stream, unsigned long long packet, int n0, int n,
+                         double* out) {
+    if (blockIdx.x != 0 || threadIdx.x != 0) return;
+    PacketStream rs;
+    rs.init(seed, stream, packet);
+    for (int k = 0; k < n0 + n; ++k) {
+        const double u = rs.next();
+        if (k >= n0) out[k - n0] = u;
+    }
 }
 
 // Geometry-only DDA (no optical-depth cut) for the leaf-sequence hook.
@@ -857,6 +1111,12 @@ PassArgs make_args(mochii_ctx* c) {
     a.m = c->metal;
     a.metal_abs = c->par.ion_metal_abs;
     a.oct = c->oct;
+    a.dust = c->dust;
+    a.rhokap = c->rhokap;
+    a.xs = c->xscore ? 1 : 0;
+    a.scatter = c->scatter ? 1 : 0;
+    a.eion_min = c->par.eion_min;
+    a.seed = (unsigned long long)(long long)c->par.random_seed;
     return a;
 }
 
@@ -876,9 +1136,18 @@ size_t metal_smem(const mochii_ctx* c) {
     return (c->metal.nmb > 0 ? 1 : 2) * (size_t)c->metal.ntrp * 128 * (c->fp32 ? 4 : 8);
 }
 
-template <typename R, int NABS, int LA, int MET>
+// Absorber variants of the walk kernels: V = 1 (H I), 4 (H I, He I, He II),
+// 5 (4 + grains and FUV: X).
+template <int V> struct AbsV {
+    static constexpr int NABS = V == 1 ? 1 : 4;
+    static constexpr int X = V == 5 ? 1 : 0;
+};
+
+int abs_variant(const mochii_ctx* c) { return c->xscore ? 5 : c->nabs == 1 ? 1 : 4; }
+
+template <typename R, int V, int LA, int MET>
 int walk_occupancy(size_t smem) {
-    auto k = k_walk_edge<R, NABS, LA, MET>;
+    auto k = k_walk_edge<R, AbsV<V>::NABS, LA, MET, AbsV<V>::X>;
     if (smem > 48 * 1024) cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     int nb = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k, 128, smem) != cudaSuccess) {
@@ -888,69 +1157,82 @@ int walk_occupancy(size_t smem) {
     return nb > 0 ? nb : 1;
 }
 
+template <typename R>
+int walk_occupancy_any(const mochii_ctx* c, size_t smem) {
+    switch (abs_variant(c)) {
+        case 1: return walk_occupancy<R, 1, 2, 1>(smem);
+        case 4: return walk_occupancy<R, 4, 2, 1>(smem);
+        default: return walk_occupancy<R, 5, 2, 1>(smem);
+    }
+}
+
 int transport_blocks(const mochii_ctx* c) {
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device);
     int per_sm = c->tune.walk_blocks_per_sm > 0 ? c->tune.walk_blocks_per_sm : 8;
     if (c->metal.ntr > 0) {   // resident blocks only: each holds its packets' sigma_k in shared memory
         const size_t smem = metal_smem(c);
-        const int occ = c->fp32 ? (c->nabs == 1 ? walk_occupancy<float, 1, 2, 1>(smem) : walk_occupancy<float, 4, 2, 1>(smem))
-                                : (c->nabs == 1 ? walk_occupancy<double, 1, 2, 1>(smem) : walk_occupancy<double, 4, 2, 1>(smem));
+        const int occ = c->fp32 ? walk_occupancy_any<float>(c, smem) : walk_occupancy_any<double>(c, smem);
         per_sm = per_sm < occ ? per_sm : occ;
     }
     return grid_blocks(c->par.nphotons, 128, sms * per_sm);
 }
 
+// One chunk's walk: packets ip0 .. ip0 + n - 1 of a stream (0 stellar, 1
+// diffuse), accumulate into the per-block ledger unless acc == 0.
+struct WalkLaunch {
+    long long n, ip0;
+    int acc, blocks, stream;
+};
+
 // Walk-kernel variants: look-ahead depth 0..2 (the autotuned choice is
 // c->tune.lookahead); 128-thread blocks.
-template <typename R, int NABS, int MET>
-cudaError_t walk_la(mochii_ctx* c, const PassArgs& a, const PacketRecords& r, long long n, int acc, int blocks) {
+template <typename R, int V, int MET>
+cudaError_t walk_la(mochii_ctx* c, const PassArgs& a, const PacketRecords& r, const WalkLaunch& w) {
+    constexpr int NABS = AbsV<V>::NABS, X = AbsV<V>::X;
     const size_t smem = MET ? metal_smem(c) : 0;
     if (MET && smem > 48 * 1024) {
-        cudaFuncSetAttribute(k_walk_edge<R, NABS, 0, MET>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        cudaFuncSetAttribute(k_walk_edge<R, NABS, 1, MET>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        cudaFuncSetAttribute(k_walk_edge<R, NABS, 2, MET>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        cudaFuncSetAttribute(k_walk_edge<R, NABS, 0, MET, X>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        cudaFuncSetAttribute(k_walk_edge<R, NABS, 1, MET, X>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        cudaFuncSetAttribute(k_walk_edge<R, NABS, 2, MET, X>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     }
     switch (c->tune.lookahead) {
-        case 0: k_walk_edge<R, NABS, 0, MET><<<blocks, 128, smem, c->stream>>>(a, r, n, acc); break;
-        case 1: k_walk_edge<R, NABS, 1, MET><<<blocks, 128, smem, c->stream>>>(a, r, n, acc); break;
-        default: k_walk_edge<R, NABS, 2, MET><<<blocks, 128, smem, c->stream>>>(a, r, n, acc); break;
+        case 0: k_walk_edge<R, NABS, 0, MET, X><<<w.blocks, 128, smem, c->stream>>>(a, r, w.n, w.acc, w.ip0, w.stream); break;
+        case 1: k_walk_edge<R, NABS, 1, MET, X><<<w.blocks, 128, smem, c->stream>>>(a, r, w.n, w.acc, w.ip0, w.stream); break;
+        default: k_walk_edge<R, NABS, 2, MET, X><<<w.blocks, 128, smem, c->stream>>>(a, r, w.n, w.acc, w.ip0, w.stream); break;
     }
     return cudaGetLastError();
-}
-
-template <typename R, int MET>
-cudaError_t walk_abs(mochii_ctx* c, const PassArgs& a, const PacketRecords& r, long long n, int acc, int blocks) {
-    return c->nabs == 1 ? walk_la<R, 1, MET>(c, a, r, n, acc, blocks) : walk_la<R, 4, MET>(c, a, r, n, acc, blocks);
 }
 
 // The octree walk: no look-ahead variants.
-template <typename R, int NABS, int MET>
-cudaError_t walk_amr(mochii_ctx* c, const PassArgs& a, const PacketRecords& r, long long n, int acc, int blocks) {
+template <typename R, int V, int MET>
+cudaError_t walk_amr(mochii_ctx* c, const PassArgs& a, const PacketRecords& r, const WalkLaunch& w) {
+    constexpr int NABS = AbsV<V>::NABS, X = AbsV<V>::X;
     const size_t smem = MET ? metal_smem(c) : 0;
     if (MET && smem > 48 * 1024)
-        cudaFuncSetAttribute(k_walk_amr<R, NABS, MET>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    k_walk_amr<R, NABS, MET><<<blocks, 128, smem, c->stream>>>(a, r, n, acc);
+        cudaFuncSetAttribute(k_walk_amr<R, NABS, MET, X>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k_walk_amr<R, NABS, MET, X><<<w.blocks, 128, smem, c->stream>>>(a, r, w.n, w.acc, w.ip0, w.stream);
     return cudaGetLastError();
 }
 
 template <typename R, int MET>
-cudaError_t walk_abs(mochii_ctx* c, const PassArgs& a, const PacketRecords& r, long long n, int acc, int blocks,
-                     bool amr) {
-    if (amr) return c->nabs == 1 ? walk_amr<R, 1, MET>(c, a, r, n, acc, blocks) : walk_amr<R, 4, MET>(c, a, r, n, acc, blocks);
-    return walk_abs<R, MET>(c, a, r, n, acc, blocks);
+cudaError_t walk_abs(mochii_ctx* c, const PassArgs& a, const PacketRecords& r, const WalkLaunch& w) {
+    const bool amr = c->oct.ncells > 0;
+    switch (abs_variant(c)) {
+        case 1: return amr ? walk_amr<R, 1, MET>(c, a, r, w) : walk_la<R, 1, MET>(c, a, r, w);
+        case 4: return amr ? walk_amr<R, 4, MET>(c, a, r, w) : walk_la<R, 4, MET>(c, a, r, w);
+        default: return amr ? walk_amr<R, 5, MET>(c, a, r, w) : walk_la<R, 5, MET>(c, a, r, w);
+    }
 }
 
 template <typename R>
-cudaError_t walk_prec(mochii_ctx* c, const PassArgs& a, const PacketRecords& r, long long n, int acc, int blocks) {
-    const bool amr = c->oct.ncells > 0;
-    if (c->metal.ntr == 0) return walk_abs<R, 0>(c, a, r, n, acc, blocks, amr);
-    return c->metal.nmb > 0 ? walk_abs<R, 2>(c, a, r, n, acc, blocks, amr) : walk_abs<R, 1>(c, a, r, n, acc, blocks, amr);
+cudaError_t walk_prec(mochii_ctx* c, const PassArgs& a, const PacketRecords& r, const WalkLaunch& w) {
+    if (c->metal.ntr == 0) return walk_abs<R, 0>(c, a, r, w);
+    return c->metal.nmb > 0 ? walk_abs<R, 2>(c, a, r, w) : walk_abs<R, 1>(c, a, r, w);
 }
 
-cudaError_t launch_walk_variant(mochii_ctx* c, const PassArgs& a, const PacketRecords& r, long long n, int acc,
-                                int blocks) {
-    return c->fp32 ? walk_prec<float>(c, a, r, n, acc, blocks) : walk_prec<double>(c, a, r, n, acc, blocks);
+cudaError_t launch_walk_variant(mochii_ctx* c, const PassArgs& a, const PacketRecords& r, const WalkLaunch& w) {
+    return c->fp32 ? walk_prec<float>(c, a, r, w) : walk_prec<double>(c, a, r, w);
 }
 
 PacketRecords packet_records(mochii_ctx* c) {
@@ -964,6 +1246,8 @@ PacketRecords packet_records(mochii_ctx* c) {
     r.coef = c->rec.coef;
     r.E = c->rec.E;
     r.msig = c->rec.msig;
+    r.dsc = c->rec.dsc;
+    r.p0 = c->rec.p0;
     return r;
 }
 
@@ -985,7 +1269,7 @@ cudaError_t launch_transport(mochii_ctx* c) {
             if (amr) k_launch<double, true><<<lb, kThreads, 0, c->stream>>>(a, r, ip0, n);
             else k_launch<double, false><<<lb, kThreads, 0, c->stream>>>(a, r, ip0, n);
         }
-        const cudaError_t e = launch_walk_variant(c, a, r, n, acc, blocks);
+        const cudaError_t e = launch_walk_variant(c, a, r, WalkLaunch{n, ip0, acc, blocks, 0});
         if (e != cudaSuccess) return e;
     }
     return cudaGetLastError();
@@ -1001,7 +1285,7 @@ cudaError_t launch_transport_diffuse(mochii_ctx* c, double total, long long nd) 
         const long long n = nd - ip0 < r.cap ? nd - ip0 : r.cap;
         cudaError_t e = launch_diffuse_chunk(c, total, ip0, n);
         if (e != cudaSuccess) return e;
-        e = launch_walk_variant(c, a, r, n, 1, blocks);
+        e = launch_walk_variant(c, a, r, WalkLaunch{n, ip0, 1, blocks, 1});
         if (e != cudaSuccess) return e;
     }
     return cudaGetLastError();
@@ -1017,13 +1301,19 @@ cudaError_t launch_rates(mochii_ctx* c) {
     const double ch = Lp * 1.0e-18 * fac;
     const long long n = c->grid.nleaf;
     const int blocks = grid_blocks(n, 256, 148 * 16);
+    const double* rk = c->rhokap;
+    const double dc = c->par.distance2cm;
+#define RATES(T, NT) k_rates<T, NT><<<blocks, 256, 0, c->stream>>>((const T*)c->tally, c->rates, n, cg, ch, lg, d2, rk, dc)
     if (c->fp32) {
-        if (c->ntally == 2) k_rates<float2, 2><<<blocks, 256, 0, c->stream>>>((const float2*)c->tally, c->rates, n, cg, ch, lg, d2);
-        else k_rates<float2, 6><<<blocks, 256, 0, c->stream>>>((const float2*)c->tally, c->rates, n, cg, ch, lg, d2);
+        if (c->ntally == 2) RATES(float2, 2);
+        else if (c->ntally == 6) RATES(float2, 6);
+        else RATES(float2, 8);
     } else {
-        if (c->ntally == 2) k_rates<double, 2><<<blocks, 256, 0, c->stream>>>((const double*)c->tally, c->rates, n, cg, ch, lg, d2);
-        else k_rates<double, 6><<<blocks, 256, 0, c->stream>>>((const double*)c->tally, c->rates, n, cg, ch, lg, d2);
+        if (c->ntally == 2) RATES(double, 2);
+        else if (c->ntally == 6) RATES(double, 6);
+        else RATES(double, 8);
     }
+#undef RATES
     if (c->metal.ntr > 0 && c->metal.nmb > 0) {
         const int mb = grid_blocks(n * 32, 256, 148 * 32);
         if (c->fp32) k_metal_rates_mom<float2><<<mb, 256, 0, c->stream>>>(c->metal, n, cg, ch, lg, d2);
@@ -1060,6 +1350,11 @@ cudaError_t launch_walk(mochii_ctx* c, const double* rays, long long nray, int m
     k_walk<<<grid_blocks(nray, 128, 1 << 20), 128, 0, c->stream>>>(rays, nray, max_steps, leaves, nsteps,
                                                                      c->grid.xmin, c->grid.ymin, c->grid.zmin,
                                                                      c->grid.dcell, c->grid.nx, c->grid.ny, c->grid.nz);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_philox(uint64_t seed, uint32_t stream, uint64_t packet, int n0, int n, double* out) {
+    k_philox<<<1, 32>>>(seed, stream, packet, n0, n, out);
     return cudaGetLastError();
 }
 

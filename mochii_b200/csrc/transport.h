@@ -19,6 +19,7 @@ cudaError_t launch_jt_export(mochii_ctx* c, double* dst);
 cudaError_t launch_sobol(const QmcTables* t, int stream01, long long idx0, long long n, int nd, double* out,
                          cudaStream_t s);
 cudaError_t launch_walk(mochii_ctx* c, const double* rays, long long nray, int max_steps, int* leaves, int* nsteps);
+cudaError_t launch_philox(uint64_t seed, uint32_t stream, uint64_t packet, int n0, int n, double* out);
 cudaError_t launch_records(mochii_ctx* c, long long ip0, long long n, double* out);
 long long noalloc_max_records();
 cudaError_t launch_records_from_buffer(mochii_ctx* c, long long n, double* host_out);

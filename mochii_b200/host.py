@@ -75,6 +75,16 @@ def sobol_uniforms(seed, stream, idx0, n, nd):
     return out
 
 
+def philox_uniforms(seed, stream, packet, n0, n):
+    """Draws n0 .. n0+n-1 of one packet's scattering stream, computed on the
+    device (the Philox4x32-10 stream keyed by par%iseed and the packet)."""
+    lib = _lib.load()
+    out = np.zeros(n)
+    rc = lib.mochii_philox_uniforms(int(seed), int(stream), int(packet), int(n0), int(n), out.ctypes.data)
+    _check(lib, rc)
+    return out
+
+
 class Nebula:
     """One nebula on the current CUDA device (a mochii_ctx)."""
 

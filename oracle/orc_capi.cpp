@@ -277,6 +277,25 @@ double orc_nlevel_cooling_at(const char* path, double T, double ne) {
     if (!a.load(path)) return -1.0;
     return nlevel_cooling_at(a, T, ne);
 }
+// Philox packet-stream uniforms: out[i] = draw n0 + i of (seed, stream, packet)
+void orc_philox(unsigned long long seed, unsigned stream, unsigned long long packet, unsigned n0, int n,
+                double* out) {
+    for (int i = 0; i < n; ++i) out[i] = philox_uniform(seed, stream, packet, n0 + (unsigned)i);
+}
+void orc_philox_block(const unsigned* ctr4, const unsigned* key2, unsigned* out4) {
+    philox4x32_10(ctr4, key2, out4);
+}
+// grain optics of the simulation at energies E: (sabs, ssca, g) per energy
+int orc_sim_dust_optics(void* h, long long n, const double* E, double* out3) {
+    auto* s = static_cast<Sim*>(h);
+    if (!s->par.ion_add_dust) return -1;
+    for (long long i = 0; i < n; ++i) {
+        out3[3 * i] = s->dust.sabs_at(E[i]);
+        out3[3 * i + 1] = s->dust.ssca_at(E[i]);
+        out3[3 * i + 2] = s->dust.g_at(E[i]);
+    }
+    return 0;
+}
 // energy ledger (emitted, absorbed, escaped) and segment counts
 void orc_sim_energy(void* h, double* e3, long long* segs2) {
     auto* s = static_cast<Sim*>(h);
@@ -305,6 +324,9 @@ long long orc_sim_get(void* h, const char* name, double* out, long long cap) {
     else if (n == "heat_HeI") v = &s->heat_HeI;
     else if (n == "heat_HeII") v = &s->heat_HeII;
     else if (n == "jt_ion") v = &s->tally.jt;
+    else if (n == "heat_dust") v = &s->heat_dust;
+    else if (n == "g0_fuv") v = &s->g0_fuv;
+    else if (n == "rhokap") v = &s->st.rhokap;
     else if (n == "hhe") v = &s->tally.hhe;
     else if (n == "eedge") v = &s->band.eedge;
     else if (s->metals() && (n == "gamma_metal" || n == "heat_metal" || n == "x_metal" || n == "metal_raw")) {
@@ -392,9 +414,9 @@ int orc_sim_walk_leaves(void* h, long long nray, const double* rays, int max_ste
     auto* s = static_cast<Sim*>(h);
     for (long long r = 0; r < nray; ++r) {
         const double* q = rays + 6 * r;
-        nsteps[r] = s->grid.car
-                        ? s->walk_leaves_car(q[0], q[1], q[2], q[3], q[4], q[5], max_steps, leaves + r * max_steps)
-                        : s->walk_leaves_amr(q[0], q[1], q[2], q[3], q[4], q[5], max_steps, leaves + r * max_steps);
+        nsteps[r] = s->amr_walk()
+                        ? s->walk_leaves_amr(q[0], q[1], q[2], q[3], q[4], q[5], max_steps, leaves + r * max_steps)
+                        : s->walk_leaves_car(q[0], q[1], q[2], q[3], q[4], q[5], max_steps, leaves + r * max_steps);
         for (int k = nsteps[r]; k < max_steps; ++k) leaves[r * max_steps + k] = -1;
     }
     return 0;

@@ -657,7 +657,8 @@ bool parse_namelist(const std::string& text, Par& p, std::string* err) {
         B(solve_te); D(te_min); D(te_max); D(gas_tol_te); B(use_metals);
         B(diffuse_field); B(use_sec_ion); B(ion_add_dust); B(ion_dust_scatter);
         S(dust_density_law); D(cext_dust); S(data_dir); S(atomic_dir); S(ion_dust_kext);
-        S(diffuse_energy_model);
+        S(diffuse_energy_model); D(lambda_ref); D(taumax); D(tauhomo);
+        else if (k == "iseed") p.iseed = (int64_t)std::llround(to_dbl(s));
         B(ion_metal_abs); B(metal_ne); B(metal_heat); B(metal_freefree); B(fe_levels_full);
         else if (k == "abund_c") p.abund_C = to_dbl(s);
         else if (k == "abund_n") p.abund_N = to_dbl(s);
@@ -918,10 +919,12 @@ bool band_setup(const Par& p, Band& b, std::string* err, const std::vector<doubl
 // =========================================================================
 // Tallies
 // =========================================================================
-void Tally::reset(int nleaf, int nnu, int ntr) {
+void Tally::reset(int nleaf, int nnu, int ntr, bool dust, bool fuvt) {
     hhe.assign((size_t)6 * nleaf, 0.0);
     jt.assign((size_t)nnu * nleaf, 0.0);
     metal.assign((size_t)2 * ntr * nleaf, 0.0);
+    dust_abs.assign(dust ? (size_t)nleaf : 0, 0.0);
+    fuv.assign(fuvt ? (size_t)nleaf : 0, 0.0);
     emitted = absorbed = escaped = 0;
     direct_segments = scattered_segments = 0;
 }
@@ -929,6 +932,8 @@ void Tally::add(const Tally& o) {
     for (size_t i = 0; i < hhe.size(); ++i) hhe[i] += o.hhe[i];
     for (size_t i = 0; i < jt.size(); ++i) jt[i] += o.jt[i];
     for (size_t i = 0; i < metal.size(); ++i) metal[i] += o.metal[i];
+    for (size_t i = 0; i < dust_abs.size(); ++i) dust_abs[i] += o.dust_abs[i];
+    for (size_t i = 0; i < fuv.size(); ++i) fuv[i] += o.fuv[i];
     emitted += o.emitted;
     absorbed += o.absorbed;
     escaped += o.escaped;
@@ -953,9 +958,20 @@ bool Sim::setup(const std::string& nl, std::string* err) {
         set_err(err, "oracle: a 'car' grid from a leaf file is not restated");
         return false;
     }
-    if (par.ion_add_dust || par.use_sec_ion || par.add_fuv) {
-        set_err(err, "oracle: dust/sec_ion/fuv not restated yet");
+    if (par.use_sec_ion) {
+        set_err(err, "oracle: use_sec_ion is not restated");
         return false;
+    }
+    if (par.ion_add_dust) {
+        if (par.dust_density_law != "global_dgr" && par.dust_density_law != "none") {
+            set_err(err, "oracle: dust_density_law must be 'global_dgr' or 'none'");
+            return false;
+        }
+        if (par.taumax > 0.0 || par.tauhomo > 0.0) {
+            set_err(err, "oracle: taumax / tauhomo normalisation is not restated");
+            return false;
+        }
+        if (!dust.read(par.ion_dust_kext, par.lambda_ref, err)) return false;   // ion_dust_read
     }
     if (par.solve_te) {
         th = new Thermal();
@@ -1049,9 +1065,14 @@ bool Sim::setup(const std::string& nl, std::string* err) {
         set_err(err, "oracle: only the sobol launch sequence is restated");
         return false;
     }
-    tally.reset(nleaf, band.nnu_band, metals() ? sp->ntr : 0);
+    // grey dust opacity per code length of each leaf, grid_mod_amr.f90:233-278
+    st.rhokap.assign(nleaf, 0.0);
+    if (par.ion_add_dust && par.dust_density_law == "global_dgr")
+        for (int il = 0; il < nleaf; ++il) st.rhokap[il] = st.nH[il] * par.cext_dust * par.DGR * par.distance2cm;
+    tally.reset(nleaf, band.nnu_band, metals() ? sp->ntr : 0, par.ion_add_dust, par.add_fuv);
     gamma_HI.assign(nleaf, 0.0); gamma_HeI.assign(nleaf, 0.0); gamma_HeII.assign(nleaf, 0.0);
     heat_HI.assign(nleaf, 0.0); heat_HeI.assign(nleaf, 0.0); heat_HeII.assign(nleaf, 0.0);
+    heat_dust.assign(nleaf, 0.0); g0_fuv.assign(nleaf, 0.0);
     opacity_fill();   // gas_opacity_setup -> gas_opacity_fill (gas_opacity_mod.f90:240-290)
     return true;
 }
@@ -1065,6 +1086,15 @@ void Sim::opacity_fill() {
 void Sim::metal_sigma(Photon& ph) const {
     ph.nm = 0;
     if (metals()) ph.nm = sp->packet_sigma(ph.E, ph.sm);
+    // the dust part of build_ion_packet_physics (ion_packet_mod.f90:42-50)
+    ph.dust_abs = ph.dust_sca = ph.dust_g = 0.0;
+    if (par.ion_add_dust) {
+        ph.dust_abs = dust.sabs_at(ph.E);
+        ph.dust_sca = dust.ssca_at(ph.E);
+        ph.dust_g = dust.g_at(ph.E);
+    }
+    ph.nscatt = 0;
+    ph.inside = true;
 }
 
 // gen_ion_photon_qmc, ion_band_mod.f90:1880-1935, with emit_point_qmc
@@ -1099,7 +1129,7 @@ void Sim::gen_photon_qmc(int64_t ip, Photon& ph) const {
     ph.wgt = 1.0;
     ph.Lpacket = band.ion_Ltot / (double)par.nphotons;
     ph.E = e;
-    ph.il = grid.car ? -1 : grid.oct->find_leaf(ph.x, ph.y, ph.z);   // emit_point_qmc, ion_band_mod.f90:2245
+    ph.il = amr_walk() ? leaf_find(ph.x, ph.y, ph.z) : -1;   // emit_point_qmc, ion_band_mod.f90:2245
     ph.sHI = sigma_HI(e);
     ph.sHeI = sigma_HeI(e);
     ph.sHeII = sigma_HeII(e);
@@ -1110,7 +1140,10 @@ void Sim::gen_photon_qmc(int64_t ip, Photon& ph) const {
 static inline void score(const Sim& s, const Photon& ph, int il, double path_lum, Tally& t) {
     if (path_lum == 0.0) return;
     t.jt[(size_t)s.band.nnu_band * il + ph.inu] += path_lum;
-    t.direct_segments += 1;
+    if (!t.dust_abs.empty()) t.dust_abs[il] += path_lum * ph.dust_abs;
+    if (!t.fuv.empty() && ph.E < s.par.eion_min) t.fuv[il] += path_lum;
+    if (ph.nscatt > 0) t.scattered_segments += 1;
+    else t.direct_segments += 1;
     const double energy = ph.E;
     double c[6];
     c[0] = ph.sHI / (energy * EV2ERG);
@@ -1124,14 +1157,19 @@ static inline void score(const Sim& s, const Photon& ph, int il, double path_lum
     if (ph.nm > 0) s.sp->score(energy, ph.sm, ph.nm, il, path_lum, t.metal.data());
 }
 
-// ion_packet_opacity, ion_packet_mod.f90:55-87 (gas part).
+// ion_packet_opacity, ion_packet_mod.f90:55-87 (gas, metals and grains).
 static inline double opacity(const Sim& s, const Photon& ph, int il) {
     double metal = 0.0;
     if (ph.nm > 0 && s.par.ion_metal_abs) metal = s.sp->cached_opacity(ph.sm, ph.nm, il);
-    return s.st.nH[il] *
-           (s.st.xHI[il] * ph.sHI + s.par.He_abund * (s.st.xHeI[il] * ph.sHeI + s.st.xHeII[il] * ph.sHeII) +
-            metal) *
-           s.par.distance2cm;
+    double kap = s.st.nH[il] *
+                 (s.st.xHI[il] * ph.sHI + s.par.He_abund * (s.st.xHeI[il] * ph.sHeI + s.st.xHeII[il] * ph.sHeII) +
+                  metal) *
+                 s.par.distance2cm;
+    if (s.par.ion_add_dust) {
+        kap = kap + s.st.rhokap[il] * ph.dust_abs;
+        if (s.par.ion_dust_scatter) kap = kap + s.st.rhokap[il] * ph.dust_sca;
+    }
+    return kap;
 }
 
 // dda_init (raytrace_amr.f90:495-532) + raytrace_ion_to_edge_car (:534-592).
@@ -1189,28 +1227,83 @@ void Sim::walk_edge_car(const Photon& ph, Tally& t, double* tau_edge) const {
 }
 
 void Sim::walk_edge(const Photon& ph, Tally& t, double* tau_edge) const {
-    if (grid.car) walk_edge_car(ph, t, tau_edge);
-    else walk_edge_amr(ph, t, tau_edge);
+    if (amr_walk()) walk_edge_amr(ph, t, tau_edge);
+    else walk_edge_car(ph, t, tau_edge);
 }
 
-// raytrace_ion_to_edge_amr, raytrace_amr.f90:422-486 (no xy-periodic wrap).
+int Sim::leaf_find(double x, double y, double z) const {
+    if (!grid.car) return grid.oct->find_leaf(x, y, z);
+    if (x < grid.xmin || x > grid.xmax || y < grid.ymin || y > grid.ymax || z < grid.zmin || z > grid.zmax) return -1;
+    int ix = (int)((x - grid.xmin) / grid.dcell);
+    int iy = (int)((y - grid.ymin) / grid.dcell);
+    int iz = (int)((z - grid.zmin) / grid.dcell);
+    ix = std::min(std::max(ix, 0), grid.nx - 1);
+    iy = std::min(std::max(iy, 0), grid.ny - 1);
+    iz = std::min(std::max(iz, 0), grid.nz - 1);
+    return ix + grid.nx * (iy + grid.ny * iz);
+}
+
+void Sim::leaf_exit(int il, double x, double y, double z, double kx, double ky, double kz, double* tout,
+                    int* iface) const {
+    if (!grid.car) {
+        grid.oct->cell_exit(grid.oct->icell_of_leaf[il], x, y, z, kx, ky, kz, tout, iface);
+        return;
+    }
+    // cell_cx/cy/cz/ch of the car grid (octree_mod.f90:113-153), then the same exit
+    const int ix = il % grid.nx, iy = (il / grid.nx) % grid.ny, iz = il / (grid.nx * grid.ny);
+    const double cx = grid.xmin + ((double)ix + 0.5) * grid.dcell;
+    const double cy = grid.ymin + ((double)iy + 0.5) * grid.dcell;
+    const double cz = grid.zmin + ((double)iz + 0.5) * grid.dcell;
+    const double h = 0.5 * grid.dcell;
+    double t[6];
+    if (kx > 0.0) { t[0] = (cx + h - x) / kx; t[1] = HUGEST; }
+    else if (kx < 0.0) { t[0] = HUGEST; t[1] = (cx - h - x) / kx; }
+    else { t[0] = HUGEST; t[1] = HUGEST; }
+    if (ky > 0.0) { t[2] = (cy + h - y) / ky; t[3] = HUGEST; }
+    else if (ky < 0.0) { t[2] = HUGEST; t[3] = (cy - h - y) / ky; }
+    else { t[2] = HUGEST; t[3] = HUGEST; }
+    if (kz > 0.0) { t[4] = (cz + h - z) / kz; t[5] = HUGEST; }
+    else if (kz < 0.0) { t[4] = HUGEST; t[5] = (cz - h - z) / kz; }
+    else { t[4] = HUGEST; t[5] = HUGEST; }
+    int f = 0;
+    for (int k = 1; k < 6; ++k)
+        if (t[k] < t[f]) f = k;
+    *iface = f;
+    *tout = t[f];
+}
+
+int Sim::leaf_next(int il, int iface, double x, double y, double z) const {
+    if (!grid.car) return grid.oct->next_leaf(grid.oct->icell_of_leaf[il], iface, x, y, z);
+    int ix = il % grid.nx, iy = (il / grid.nx) % grid.ny, iz = il / (grid.nx * grid.ny);
+    switch (iface) {
+        case 0: ++ix; break;
+        case 1: --ix; break;
+        case 2: ++iy; break;
+        case 3: --iy; break;
+        case 4: ++iz; break;
+        default: --iz; break;
+    }
+    if (ix < 0 || ix >= grid.nx || iy < 0 || iy >= grid.ny || iz < 0 || iz >= grid.nz) return -1;
+    return ix + grid.nx * (iy + grid.ny * iz);
+}
+
+// raytrace_ion_to_edge_amr, raytrace_amr.f90:422-486 (no xy-periodic wrap):
+// the octree walk, also on the car grid with par%car_walk = 'amr'.
 void Sim::walk_edge_amr(const Photon& ph, Tally& t, double* tau_edge) const {
-    const Octree& o = *grid.oct;
     double x = ph.x, y = ph.y, z = ph.z;
     const double kx = ph.kx, ky = ph.ky, kz = ph.kz;
     int il = ph.il;
     const double wl = ph.wgt * ph.Lpacket;
     double expo = 1.0, tau = 0.0;
     *tau_edge = 0.0;
-    if (il < 0) il = o.find_leaf(x, y, z);
+    if (il < 0) il = leaf_find(x, y, z);
     if (il < 0) return;
     int nstep = 0;
     for (;;) {
         if (++nstep > MAX_WALK_STEPS) break;
-        const int icell = o.icell_of_leaf[il];
         double texit;
         int iface;
-        o.cell_exit(icell, x, y, z, kx, ky, kz, &texit, &iface);
+        leaf_exit(il, x, y, z, kx, ky, kz, &texit, &iface);
         const double kap = opacity(*this, ph, il);
         if (kap * texit > 0.0) {
             const double expo_out = expo * std::exp(-kap * texit);
@@ -1224,28 +1317,185 @@ void Sim::walk_edge_amr(const Photon& ph, Tally& t, double* tau_edge) const {
         x = x + texit * kx;
         y = y + texit * ky;
         z = z + texit * kz;
-        const int nl = o.next_leaf(icell, iface, x, y, z);
+        const int nl = leaf_next(il, iface, x, y, z);
         if (nl < 0) break;
         il = nl;
     }
     *tau_edge = tau;
 }
 
+void Sim::walk_to_tau(Photon& ph, double tau_in, Tally& t) const {
+    const bool do_tally = ph.nscatt > 0;
+    const double wl = ph.wgt * ph.Lpacket;
+    if (amr_walk()) {   // raytrace_ion_to_tau_amr, raytrace_amr.f90:348-420
+        double x = ph.x, y = ph.y, z = ph.z;
+        int il = ph.il;
+        if (il < 0) {
+            il = leaf_find(x, y, z);
+            if (il < 0) {
+                ph.inside = false;
+                return;
+            }
+        }
+        double tau = 0.0;
+        int nstep = 0;
+        while (ph.inside) {
+            if (++nstep > MAX_WALK_STEPS) {
+                ph.inside = false;
+                break;
+            }
+            double texit;
+            int iface;
+            leaf_exit(il, x, y, z, ph.kx, ph.ky, ph.kz, &texit, &iface);
+            const double kap = opacity(*this, ph, il);
+            if (tau + texit * kap >= tau_in) {
+                const double d = kap > 0.0 ? (tau_in - tau) / kap : texit;
+                if (do_tally) score(*this, ph, il, wl * d, t);
+                x = x + d * ph.kx; y = y + d * ph.ky; z = z + d * ph.kz;
+                break;
+            }
+            if (do_tally) score(*this, ph, il, wl * texit, t);
+            tau = tau + texit * kap;
+            x = x + texit * ph.kx; y = y + texit * ph.ky; z = z + texit * ph.kz;
+            const int nl = leaf_next(il, iface, x, y, z);
+            if (nl < 0) {
+                ph.inside = false;
+                break;
+            }
+            il = nl;
+        }
+        ph.x = x; ph.y = y; ph.z = z;
+        ph.il = il;
+        return;
+    }
+    // raytrace_ion_to_tau_car, raytrace_amr.f90:594-676: dda_init from the
+    // packet's point, the DDA to tau_in, the end point from the total path
+    const double d = grid.dcell;
+    const double pos[3] = {ph.x, ph.y, ph.z};
+    const double kk[3] = {ph.kx, ph.ky, ph.kz};
+    const double org[3] = {grid.xmin, grid.ymin, grid.zmin};
+    const int n[3] = {grid.nx, grid.ny, grid.nz};
+    int idx[3], stp[3];
+    double tmax[3], tdel[3];
+    for (int a = 0; a < 3; ++a) {
+        idx[a] = std::min(std::max((int)((pos[a] - org[a]) / d), 0), n[a] - 1);
+        if (kk[a] > 0.0) {
+            stp[a] = 1; tmax[a] = (org[a] + (double)(idx[a] + 1) * d - pos[a]) / kk[a]; tdel[a] = d / kk[a];
+        } else if (kk[a] < 0.0) {
+            stp[a] = -1; tmax[a] = (org[a] + (double)idx[a] * d - pos[a]) / kk[a]; tdel[a] = -d / kk[a];
+        } else {
+            stp[a] = 0; tmax[a] = HUGEST; tdel[a] = HUGEST;
+        }
+    }
+    double tau = 0.0, t_cur = 0.0;
+    int nstep = 0;
+    for (;;) {
+        if (++nstep > MAX_WALK_STEPS) {
+            ph.inside = false;
+            break;
+        }
+        const int il = idx[0] + n[0] * (idx[1] + n[1] * idx[2]);
+        int a = 0;
+        if (tmax[1] < tmax[a]) a = 1;
+        if (tmax[2] < tmax[a]) a = 2;
+        const double seg = tmax[a] - t_cur;
+        const double kap = opacity(*this, ph, il);
+        if (tau + seg * kap >= tau_in) {
+            const double ds = kap > 0.0 ? (tau_in - tau) / kap : seg;
+            if (do_tally) score(*this, ph, il, wl * ds, t);
+            t_cur = t_cur + ds;
+            break;
+        }
+        if (do_tally) score(*this, ph, il, wl * seg, t);
+        tau = tau + seg * kap;
+        t_cur = tmax[a];
+        tmax[a] = tmax[a] + tdel[a];
+        idx[a] += stp[a];
+        if (idx[a] < 0 || idx[a] >= n[a]) {
+            ph.inside = false;
+            break;
+        }
+    }
+    ph.x = ph.x + t_cur * ph.kx;
+    ph.y = ph.y + t_cur * ph.ky;
+    ph.z = ph.z + t_cur * ph.kz;
+    if (ph.inside) ph.il = idx[0] + n[0] * (idx[1] + n[1] * idx[2]);
+}
+
+void Sim::transport_packet(Photon& ph, Tally& t) const {
+    double tau_edge = 0.0;
+    walk_edge(ph, t, &tau_edge);
+    // ion_score_energy_packet, ion_score_mod.f90:233-252 (x87 extended)
+    const double lum = ph.Lpacket * ph.wgt;
+    const double tr = std::exp(-std::max(tau_edge, 0.0));
+    t.emitted += (long double)lum;
+    t.absorbed += (long double)(lum * (1.0 - tr));
+    t.escaped += (long double)(lum * tr);
+    if (!(par.ion_add_dust && par.ion_dust_scatter)) return;
+    if (tau_edge <= 1.0e-12) return;
+    const double WMIN = 1.0e-4, PSURV = 0.1;
+    // forced first interaction (the direct field is already tallied)
+    const double w1 = 1.0 - std::exp(-tau_edge);
+    ph.wgt = ph.wgt * w1;
+    double tau = -std::log(1.0 - ph.rng.next() * w1);
+    walk_to_tau(ph, tau, t);
+    int nev = 0;
+    while (ph.inside) {
+        const int il = ph.il;
+        if (il < 0) break;
+        if (++nev > MAX_SCATTERINGS) break;
+        const double a_eff = st.rhokap[il] * ph.dust_sca / std::max(opacity(*this, ph, il), TINEST);
+        ph.wgt = ph.wgt * a_eff;
+        if (ph.wgt < WMIN) {
+            if (ph.rng.next() > PSURV) break;
+            ph.wgt = ph.wgt / PSURV;
+        }
+        const double gg = ph.dust_g;
+        double cost;
+        if (std::fabs(gg) > 1.0e-3) {
+            const double q = (1.0 - gg * gg) / (1.0 + gg * (2.0 * ph.rng.next() - 1.0));
+            cost = (1.0 + gg * gg - q * q) / (2.0 * gg);
+        } else {
+            cost = 2.0 * ph.rng.next() - 1.0;
+        }
+        cost = std::min(std::max(cost, -1.0), 1.0);
+        const double sint = std::sqrt(1.0 - cost * cost);
+        const double phi = TWOPI * ph.rng.next();
+        double kx = ph.kx, ky = ph.ky, kz = ph.kz;
+        double norm = std::sqrt(kx * kx + ky * ky + kz * kz);
+        if (norm <= 0.0) break;
+        kx = kx / norm; ky = ky / norm; kz = kz / norm;
+        double ux, uy, uz;
+        if (std::fabs(kz) < 0.99) { ux = -ky; uy = kx; uz = 0.0; }
+        else { ux = 0.0; uy = -kz; uz = ky; }
+        norm = std::sqrt(ux * ux + uy * uy + uz * uz);
+        ux = ux / norm; uy = uy / norm; uz = uz / norm;
+        const double vx = ky * uz - kz * uy, vy = kz * ux - kx * uz, vz = kx * uy - ky * ux;
+        const double cp = std::cos(phi), sp_ = std::sin(phi);
+        double nkx = sint * (cp * ux + sp_ * vx) + cost * kx;
+        double nky = sint * (cp * uy + sp_ * vy) + cost * ky;
+        double nkz = sint * (cp * uz + sp_ * vz) + cost * kz;
+        norm = std::sqrt(nkx * nkx + nky * nky + nkz * nkz);
+        ph.kx = nkx / norm; ph.ky = nky / norm; ph.kz = nkz / norm;
+        ph.nscatt += 1;
+        tau = -std::log(std::max(ph.rng.next(), TINEST));
+        walk_to_tau(ph, tau, t);
+    }
+}
+
 // Geometry-only octree walk: the leaf sequence of one ray, 0-based.
 int Sim::walk_leaves_amr(double x, double y, double z, double kx, double ky, double kz, int max_steps,
                          int32_t* out) const {
-    const Octree& o = *grid.oct;
-    int il = o.find_leaf(x, y, z), ns = 0;
+    int il = leaf_find(x, y, z), ns = 0;
     while (il >= 0 && ns < max_steps) {
         out[ns++] = il;
-        const int icell = o.icell_of_leaf[il];
         double texit;
         int iface;
-        o.cell_exit(icell, x, y, z, kx, ky, kz, &texit, &iface);
+        leaf_exit(il, x, y, z, kx, ky, kz, &texit, &iface);
         x = x + texit * kx;
         y = y + texit * ky;
         z = z + texit * kz;
-        il = o.next_leaf(icell, iface, x, y, z);
+        il = leaf_next(il, iface, x, y, z);
     }
     return ns;
 }
@@ -1292,7 +1542,7 @@ void Sim::transport_pass() {
     const int nt = std::max(1, nthreads);
     std::vector<Tally> loc(nt);
     const int ntr = metals() ? sp->ntr : 0;
-    for (auto& t : loc) t.reset(nleaf, nnu, ntr);
+    for (auto& t : loc) t.reset(nleaf, nnu, ntr, par.ion_add_dust, par.add_fuv);
     const int64_t np = par.nphotons;
 #pragma omp parallel num_threads(nt)
     {
@@ -1304,14 +1554,8 @@ void Sim::transport_pass() {
         Photon ph;
         for (int64_t ip = 1 + tid; ip <= np; ip += nt) {
             gen_photon_qmc(ip - 1, ph);
-            double tau_edge = 0.0;
-            walk_edge(ph, t, &tau_edge);
-            // ion_score_energy_packet, ion_score_mod.f90:233-252 (x87 extended)
-            const double lum = ph.Lpacket * ph.wgt;
-            const double tr = std::exp(-std::max(tau_edge, 0.0));
-            t.emitted += (long double)lum;
-            t.absorbed += (long double)(lum * (1.0 - tr));
-            t.escaped += (long double)(lum * tr);
+            ph.rng = PacketRng{(uint64_t)par.iseed, (uint64_t)(ip - 1), 0u, 0u};
+            transport_packet(ph, t);
         }
     }
     // diffuse ground-recombination packets from the current state,
@@ -1329,17 +1573,12 @@ void Sim::transport_pass() {
             Photon ph;
             for (int64_t ip = 1 + tid; ip <= nd; ip += nt) {
                 gen_diffuse_qmc(ip - 1, ph);
-                double tau_edge = 0.0;
-                walk_edge(ph, t, &tau_edge);
-                const double lum = ph.Lpacket * ph.wgt;
-                const double tr = std::exp(-std::max(tau_edge, 0.0));
-                t.emitted += (long double)lum;
-                t.absorbed += (long double)(lum * (1.0 - tr));
-                t.escaped += (long double)(lum * tr);
+                ph.rng = PacketRng{(uint64_t)par.iseed, (uint64_t)(ip - 1), 1u, 0u};
+                transport_packet(ph, t);
             }
         }
     }
-    tally.reset(nleaf, nnu, ntr);
+    tally.reset(nleaf, nnu, ntr, par.ion_add_dust, par.add_fuv);
     for (auto& t : loc) tally.add(t);
     gas_rates_compute();
     if (metals()) {   // species_gamma_compute, species_mod.f90:493-512
@@ -1569,6 +1808,9 @@ void Sim::gas_rates_compute() {
         heat_HI[il] = t[3] * fac;
         heat_HeI[il] = t[4] * fac;
         heat_HeII[il] = t[5] * fac;
+        // ion_score_apply_dust_heat and ion_score_apply_g0 (ion_score_mod.f90:319-355)
+        if (!tally.dust_abs.empty()) heat_dust[il] = tally.dust_abs[il] * fac * st.rhokap[il] / par.distance2cm;
+        if (!tally.fuv.empty()) g0_fuv[il] = tally.fuv[il] * fac / 1.6e-3;
     }
 }
 

@@ -15,10 +15,15 @@
 #include <vector>
 #include <map>
 
+#include "orc_dust.h"
+
 namespace orc {
 
 // ---- constants: define.f90:29-67, energy_sampler_mod.f90:16-18 ----------
 constexpr double PI = 3.141592653589793238462643383279502884197;
+// a bound on scattering events per packet (not in the reference, whose loop
+// ends by the roulette alone); a packet that reaches it stops scattering
+constexpr int MAX_SCATTERINGS = 100000;
 constexpr double TWOPI = 6.283185307179586476925286766559005768394;
 constexpr double PC2CM = 3.0856776e18;
 constexpr double KPC2CM = PC2CM * 1e3;
@@ -146,6 +151,8 @@ struct Par {
     bool ion_add_dust = false, ion_dust_scatter = false;
     std::string dust_density_law = "global_dgr";
     double DGR = 1.0e-2, cext_dust = 1.6059e-21;
+    double lambda_ref = 0.55, taumax = -999.0, tauhomo = -999.0;   // define.f90:211-212,361
+    int64_t iseed = 0;                                             // define.f90:194
     std::string data_dir, atomic_dir, ion_dust_kext;
     // metals (define.f90:578-580, 593, 622-623, 652, 843-857)
     double abund_C = 2.2e-4, abund_N = 4.0e-5, abund_O = 3.3e-4, abund_Ne = 5.0e-5, abund_S = 9.0e-6;
@@ -193,9 +200,11 @@ struct Tally {
     std::vector<double> hhe;         // (6, nleaf), leaf-major: hhe[6*il + k]
     std::vector<double> jt;          // (nnu_band, nleaf): jt[nnu*il + inu]
     std::vector<double> metal;       // metal path estimators [(il*ntr + k)*2 + m]
+    std::vector<double> dust_abs;    // dust_abs_path (nleaf), with ion_add_dust
+    std::vector<double> fuv;         // fuv_field_path (nleaf), with add_fuv
     long double emitted = 0, absorbed = 0, escaped = 0;
     int64_t direct_segments = 0, scattered_segments = 0;
-    void reset(int nleaf, int nnu, int ntr = 0);
+    void reset(int nleaf, int nnu, int ntr = 0, bool dust = false, bool fuv = false);
     void add(const Tally& o);
 };
 
@@ -207,6 +216,10 @@ struct Photon {
     int nm = 0;                      // active metal transitions (E >= E_th)
     double sm[64];                   // their cross sections, threshold order
     int il = -1;                     // leaf of the start point (photon%icell_amr)
+    double dust_abs = 0.0, dust_sca = 0.0, dust_g = 0.0;   // ionphys dust cache
+    int nscatt = 0;
+    bool inside = true;
+    PacketRng rng;                   // the packet's scattering stream
 };
 
 struct Thermal;
@@ -235,6 +248,8 @@ struct Sim {
     State st;
     Tally tally;
     std::vector<double> gamma_HI, gamma_HeI, gamma_HeII, heat_HI, heat_HeI, heat_HeII;
+    std::vector<double> heat_dust, g0_fuv;   // ion_score_apply_dust_heat / _g0 (ion_score_mod.f90:319-355)
+    DustTable dust;                          // ion_add_dust optics
     int nthreads = 1;
     // diffuse field (diffuse_mod.f90)
     Milne milne;
@@ -259,6 +274,21 @@ struct Sim {
     void walk_edge_car(const Photon& ph, Tally& t, double* tau_edge) const;  // raytrace_amr.f90:534
     void walk_edge_amr(const Photon& ph, Tally& t, double* tau_edge) const;  // raytrace_amr.f90:422-486
     void walk_edge(const Photon& ph, Tally& t, double* tau_edge) const;
+    // transport_ion_packet (raytrace_amr.f90:249-323): the edge walk, the
+    // ledger, then with ion_dust_scatter the forced first interaction and the
+    // scattered flights
+    void transport_packet(Photon& ph, Tally& t) const;
+    // raytrace_ion_to_tau_amr (:348-420) / raytrace_ion_to_tau_car (:594-676)
+    void walk_to_tau(Photon& ph, double tau_in, Tally& t) const;
+    // the leaf accessors of the edge walk on either grid: amr_find_leaf
+    // (octree_mod.f90:69-93, car_index :185-195 on the car grid),
+    // amr_cell_exit (:309-340) of the leaf's cell, amr_next_leaf (:518-559,
+    // car_next :620-641 on the car grid); leaves 0-based, -1 none
+    int leaf_find(double x, double y, double z) const;
+    void leaf_exit(int il, double x, double y, double z, double kx, double ky, double kz, double* t,
+                   int* iface) const;
+    int leaf_next(int il, int iface, double x, double y, double z) const;
+    bool amr_walk() const { return !grid.car || par.car_walk == "amr"; }
     int walk_leaves_amr(double x, double y, double z, double kx, double ky, double kz, int max_steps,
                         int32_t* out) const;
     int walk_leaves_car(double x, double y, double z, double kx, double ky,

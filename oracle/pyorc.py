@@ -53,6 +53,9 @@ def load():
         "orc_sim_transport_pass": (I, [V]),
         "orc_sim_equilibrium_update": (I, [V, V]),
         "orc_sim_energy": (None, [V, V, V]),
+        "orc_philox": (None, [C.c_ulonglong, C.c_uint, C.c_ulonglong, C.c_uint, I, V]),
+        "orc_sim_dust_optics": (I, [V, LL, V, V]),
+        "orc_philox_block": (None, [V, V, V]),
         "orc_sim_get": (LL, [V, C.c_char_p, V, LL]),
         "orc_sim_set": (LL, [V, C.c_char_p, V, LL]),
         "orc_sim_photon": (None, [V, LL, V]),
@@ -181,6 +184,13 @@ def solve_ion_cell(gH, gHe1, gHe2, nH, T, caseA, x3, yHe=0.1, model=0):
     return x, ne.value
 
 
+
+def philox(seed, stream, packet, n0, n):
+    """Draws n0 .. n0+n-1 of one packet's scattering stream."""
+    out = np.zeros(n)
+    load().orc_philox(seed, stream, packet, n0, n, out.ctypes.data)
+    return out
+
 class Sim:
     """The oracle's nebula: the same namelist text the product reads."""
 
@@ -218,6 +228,12 @@ class Sim:
     @property
     def ion_Ltot(self):
         return load().orc_sim_ion_Ltot(self.h)
+
+    def dust_optics(self, E):
+        E = np.ascontiguousarray(E, dtype=float)
+        out = np.zeros((E.size, 3))
+        assert load().orc_sim_dust_optics(self.h, E.size, E.ctypes.data, out.ctypes.data) == 0
+        return out
 
     def energy(self):
         e = np.zeros(3)

@@ -135,7 +135,7 @@ def test_init_without_device_reports_status(lib):
 def test_unsupported_configurations_are_refused_before_device_use(lib):
     from mochii_b200 import MochiiError, Nebula, parse_namelist
     from mochii_b200 import configs
-    for extra in ("par%car_walk = 'amr'", "par%launch_sequence = 'random'", "par%ion_add_dust = .true."):
+    for extra in ("par%use_sec_ion = .true.", "par%launch_sequence = 'random'", "par%ion_add_dust = .true."):
         p = parse_namelist(configs.stromgren64(nphotons=1000, n=8).replace("/\n", extra + "\n/\n"))
         with pytest.raises(MochiiError) as ei:
             Nebula(p)

@@ -156,3 +156,34 @@ def test_octree_errors(tmp_path):
     bad.write_text("3 1.0\n0.25 0.25 0.25 1 1.0\n")
     with pytest.raises(MochiiError, match="fewer leaf rows"):
         Nebula(parse_namelist(configs.on_octree(configs.stromgren64(nphotons=1000, niter=1), str(bad))))
+
+
+def test_car_grid_amr_walk_matches_oracle(orc):
+    """par%car_walk = 'amr': the namelist car grid walked by cell exits and
+    car_next (raytrace_ion_to_edge_amr on the car grid) -- leaf sequences
+    bit-exact and the FP64 pass within 1e-9 of the oracle's same walk."""
+    nl = configs.hhe128(nphotons=200000, niter=1, n=20, precision="fp64").replace(
+        "par%grid_type = 'car'", "par%grid_type = 'car'\n par%car_walk = 'amr'")
+    sim = orc.Sim(nl)
+    neb = Nebula(parse_namelist(nl))
+    L = parse_namelist(nl).xmax
+    rng = np.random.default_rng(4)
+    o = rng.uniform(-L, L, (3000, 3))
+    o[:100] = 0.0
+    mu = rng.uniform(-1, 1, 3000)
+    ph = rng.uniform(0, 2 * np.pi, 3000)
+    k = np.column_stack([np.sqrt(1 - mu * mu) * np.cos(ph), np.sqrt(1 - mu * mu) * np.sin(ph), mu])
+    k[100:400] = np.array([[1, 0, 0], [0, -1, 0], [0, 0, 1]], float)[np.arange(300) % 3]
+    rays = np.column_stack([o, k])
+    lg, ng = neb.walk_leaves(rays, 100)
+    lo, no = sim.walk_leaves(rays, 100)
+    assert np.array_equal(ng, no) and np.array_equal(lg, lo)
+    st = neb.ionizing_field_and_rates()
+    sim.transport_pass()
+    e, _ = sim.energy()
+    assert abs(st.energy_absorbed / e[1] - 1) < 1e-12
+    for f in ("gamma_HI", "gamma_HeI", "heat_HeII"):
+        g, o_ = neb.get(f), sim.get(f)
+        big = o_ > 1e-12 * o_.max()
+        assert np.max(np.abs(g[big] / o_[big] - 1)) < 1e-9, f
+    neb.close()

@@ -84,3 +84,33 @@ def test_oracle_octree_walk_matches_slab_geometry(tree):
         got_long = got[(t1[got] - t0[got]) > eps]
         assert np.array_equal(got_long, expect), r
         assert np.all(t1[got] - t0[got] > -eps), r   # every visited leaf is on the ray
+
+
+def test_uniform_octree_walk_equals_car_amr_walk(tmp_path, orc):
+    """The octree walk on a uniform tree and the car grid walked as an octree
+    (par%car_walk = 'amr') take the same exit faces from the same centres, so
+    their leaf sequences agree bit for bit once the Morton leaf order is
+    mapped to raster order."""
+    boxlen, lev = 8.0, 4
+    n = 1 << lev
+    x, y, z, lv, nH = amr.build_leaves(boxlen, lev, lev, lambda *a: False, lambda x, y, z, L: np.full(np.shape(x), 50.0))
+    path = str(tmp_path / "uniform.txt")
+    amr.write_leaf_list(path, boxlen, x, y, z, lv, nH)
+    ijk = np.floor((np.column_stack([x, y, z]) + 0.5 * boxlen) / (boxlen / n)).astype(int)
+    raster = ijk[:, 0] + n * (ijk[:, 1] + n * ijk[:, 2])
+    car = configs.stromgren64(nphotons=1000, niter=1, n=n).replace("par%xmax", "par%xmax = 4.0 !").replace(
+        "par%ymax", "par%ymax = 4.0 !").replace("par%zmax", "par%zmax = 4.0 !")
+    s_car = orc.Sim(car.replace("par%car_walk = 'dda'", "par%car_walk = 'amr'"))
+    s_oct = orc.Sim(configs.on_octree(car, path))
+    rng = np.random.default_rng(8)
+    o = rng.uniform(-4, 4, (500, 3))
+    o[:50] = 0.0
+    mu = rng.uniform(-1, 1, 500)
+    ph = rng.uniform(0, 2 * np.pi, 500)
+    k = np.column_stack([np.sqrt(1 - mu * mu) * np.cos(ph), np.sqrt(1 - mu * mu) * np.sin(ph), mu])
+    rays = np.column_stack([o, k])
+    la, na = s_car.walk_leaves(rays, 200)
+    lb, nb = s_oct.walk_leaves(rays, 200)
+    assert np.array_equal(na, nb)
+    mapped = np.where(lb >= 0, raster[np.maximum(lb, 0)], -1)
+    assert np.array_equal(la, mapped)

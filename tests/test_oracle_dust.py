@@ -1,0 +1,157 @@
+"""The oracle's grain optics, FUV band and scattered-flight stream, checked
+independently of the oracle's own code:
+
+* Philox4x32-10 against the published known-answer vectors of Salmon et
+  al. (Random123 kat_vectors: zero, all-ones and pi-digits counters/keys);
+* the extinction-table read and the exact-energy evaluators
+  ion_dust_sabs_at / ssca_at / g_at (gas_opacity_mod.f90:231-315) against a
+  numpy re-read of the same table;
+* energy closure with grains: every packet's absorbed luminosity
+  (ion_score_energy_packet) equals the sum over its segments of path x
+  kappa, i.e. sum_leaves [n_H d2cm (x_HI S_HI + y (x_HeI S_HeI + x_HeII
+  S_HeII)) + rhokap dust_abs_path], with S_i = heat_i + gamma_i E_th,i the
+  sigma-weighted path sums recovered from the two H/He tallies;
+* the Habing-G0 estimator equals the FUV bins of the diagnostic spectrum;
+* scattering: deterministic (the counter-based stream) and it adds
+  scattered segments and dust heating.
+"""
+import os
+
+import numpy as np
+import pytest
+
+from mochii_b200 import configs
+
+KEXT = os.path.join(os.path.dirname(configs.ATOMIC_DIR), "kext_albedo_WD_MW_3.1_60_D03.all_2003")
+EV2ERG = 1.602176634e-12
+ETH = (13.598, 24.587, 54.416)   # define.f90 eth_HI, eth_HeI, eth_HeII [eV]
+
+
+def dusty(nl, scatter=False, fuv=False, seed=77, dgr=0.01):
+    extra = (f" par%ion_add_dust = .true.\n par%ion_dust_scatter = {'.true.' if scatter else '.false.'}\n"
+             f" par%ion_dust_kext = '{KEXT}'\n par%DGR = {dgr}\n par%iseed = {seed}\n")
+    if fuv:
+        extra += " par%add_fuv = .true.\n par%efuv_min = 6.0\n"
+    return nl.replace("/\n", extra + "/\n")
+
+
+def test_philox_known_answers(orc):
+    lib = orc.load()
+    kat = [([0, 0, 0, 0], [0, 0], [0x6627e8d5, 0xe169c58d, 0xbc57ac4c, 0x9b00dbd8]),
+           ([0xffffffff] * 4, [0xffffffff] * 2, [0x408f276d, 0x41c83b0e, 0xa20bc7c6, 0x6d5451fd]),
+           ([0x243f6a88, 0x85a308d3, 0x13198a2e, 0x03707344], [0xa4093822, 0x299f31d0],
+            [0xd16cfe09, 0x94fdcceb, 0x5001e420, 0x24126ea1])]
+    for ctr, key, want in kat:
+        c = np.array(ctr, dtype=np.uint32)
+        k = np.array(key, dtype=np.uint32)
+        o = np.zeros(4, dtype=np.uint32)
+        lib.orc_philox_block(c.ctypes.data, k.ctypes.data, o.ctypes.data)
+        assert o.tolist() == want
+
+
+def test_philox_stream_is_uniform_and_keyed(orc):
+    u = orc.philox(77, 0, 12345, 0, 200000)
+    assert np.all((u > 0) & (u < 1))
+    assert abs(u.mean() - 0.5) < 3e-3 and abs(u.var() - 1 / 12) < 2e-3
+    assert not np.array_equal(u[:100], orc.philox(77, 1, 12345, 0, 100))    # stream
+    assert not np.array_equal(u[:100], orc.philox(77, 0, 12346, 0, 100))    # packet
+    np.testing.assert_array_equal(u[10:20], orc.philox(77, 0, 12345, 10, 10))  # draw index
+
+
+def numpy_table():
+    rows = []
+    for line in open(KEXT):
+        tok = line.split()
+        try:
+            v = [float(t) for t in tok[:4]]
+        except ValueError:
+            continue
+        if len(v) == 4 and v[0] > 0:
+            rows.append(v)
+    a = np.array(rows)
+    return a[np.argsort(a[:, 0], kind="stable")]
+
+
+def test_dust_table_and_optics_match_numpy(orc):
+    sim = orc.Sim(dusty(configs.stromgren64(nphotons=1000, niter=1, n=8, precision="fp64")))
+    t = numpy_table()
+    lam, alb, gcos, cext = t.T
+    assert len(lam) > 1000
+
+    def lin(y, x0):
+        if x0 <= lam[0]:
+            return y[0]
+        if x0 >= lam[-1]:
+            return y[-1]
+        i = np.searchsorted(lam, x0, side="right") - 1
+        w = (x0 - lam[i]) / (lam[i + 1] - lam[i])
+        return y[i] * (1 - w) + y[i + 1] * w
+
+    def lg(y, x0):
+        if x0 <= lam[0]:
+            return y[0]
+        if x0 >= lam[-1]:
+            return y[-1]
+        i = np.searchsorted(lam, x0, side="right") - 1
+        w = np.log(x0 / lam[i]) / np.log(lam[i + 1] / lam[i])
+        return np.exp(np.log(max(y[i], 1e-300)) * (1 - w) + np.log(max(y[i + 1], 1e-300)) * w)
+
+    cref = lg(cext, 0.55)
+    E = np.geomspace(6.0, 100.0, 97)
+    got = sim.dust_optics(E)
+    for e, (sa, ss, g) in zip(E, got):
+        lb = 1.23984 / e
+        np.testing.assert_allclose([sa, ss, g], [(1 - lin(alb, lb)) * lg(cext, lb) / cref,
+                                                 lin(alb, lb) * lg(cext, lb) / cref, lin(gcos, lb)], rtol=1e-12)
+
+
+@pytest.mark.parametrize("he", [False, True])
+def test_energy_closure_with_grains(orc, he):
+    base = configs.hhe128(nphotons=30000, niter=1, n=12, precision="fp64") if he else \
+        configs.stromgren64(nphotons=30000, niter=1, n=12, precision="fp64")
+    sim = orc.Sim(dusty(base, dgr=0.05))
+    sim.set("x_HI", np.full(sim.nleaf, 1e-3))   # mostly ionized: the grains take a visible share
+    sim.transport_pass()
+    e, _ = sim.energy()
+    L = float([ln for ln in base.splitlines() if "par%xmax" in ln][0].split("=")[1])
+    d2cm = 3.0856776e18
+    vol = (2 * L / 12) ** 3
+    hhe = sim.get("hhe").reshape(-1, 6)
+    nH, xHI, xHeI, xHeII = (sim.get(f) for f in ("nH", "x_HI", "x_HeI", "x_HeII"))
+    y = 0.1 if he else 0.0
+    S = [hhe[:, 3 + k] + hhe[:, k] * ETH[k] * EV2ERG for k in range(3)]
+    gas = nH * d2cm * (xHI * S[0] + y * (xHeI * S[1] + xHeII * S[2]))
+    dust = sim.get("heat_dust") * vol * d2cm ** 3
+    assert dust.sum() > 1e-3 * e[1]
+    assert abs((gas.sum() + dust.sum()) / e[1] - 1) < 1e-10
+
+
+def test_g0_equals_fuv_bins(orc):
+    sim = orc.Sim(dusty(configs.hhe128(nphotons=20000, niter=1, n=10, precision="fp64"), fuv=True))
+    sim.transport_pass()
+    jt = sim.get("jt_ion")
+    nfuv = 8
+    L = float([ln for ln in configs.hhe128(n=10).splitlines() if "par%xmax" in ln][0].split("=")[1])
+    d2cm = 3.0856776e18
+    fac = 1.0 / ((2 * L / 10) ** 3 * d2cm ** 2)
+    g0 = sim.get("g0_fuv")
+    assert g0.max() > 0
+    np.testing.assert_allclose(g0, jt[:, :nfuv].sum(axis=1) * fac / 1.6e-3, rtol=1e-12, atol=0)
+
+
+def test_scattering_is_deterministic_and_scores(orc):
+    base = configs.hhe128(nphotons=20000, niter=1, n=12, precision="fp64")
+    runs = []
+    for _ in range(2):
+        sim = orc.Sim(dusty(base, scatter=True, dgr=0.05))
+        sim.set("x_HI", np.full(sim.nleaf, 1e-3))
+        sim.transport_pass()
+        runs.append((sim.energy(), sim.get("gamma_HI"), sim.get("heat_dust")))
+    (e0, s0), g0, h0 = runs[0]
+    (e1, s1), g1, h1 = runs[1]
+    np.testing.assert_array_equal(g0, g1)
+    assert s0[1] == s1[1] and s0[1] > 0.1 * s0[0]
+    plain = orc.Sim(dusty(base, scatter=False, dgr=0.05))
+    plain.set("x_HI", np.full(plain.nleaf, 1e-3))
+    plain.transport_pass()
+    assert h0.sum() > plain.get("heat_dust").sum()   # scattered light heats the grains too
