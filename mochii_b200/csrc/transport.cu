@@ -905,7 +905,7 @@ __global__ void k_rates(const T* __restrict__ tal, double* __restrict__ rates, l
         const T* t = tal + il * NT;
         rates[0 * nleaf + il] = tval<T>(t[0]) * cg;
         rates[3 * nleaf + il] = tval<T>(t[1]) * ch;
-        if (NT == 6) {
+        if (NT >= 6) {
             rates[1 * nleaf + il] = tval<T>(t[2]) * cg;
             rates[4 * nleaf + il] = tval<T>(t[3]) * ch;
             rates[2 * nleaf + il] = tval<T>(t[4]) * cg;

@@ -65,7 +65,7 @@ def test_grain_absorption_and_fuv_fp64_match_oracle(orc, leaf_file, grid):
     for f in ("gamma_HI", "heat_HI", "gamma_HeI", "heat_dust", "g0_fuv"):
         g, o = neb.get(f), sim.get(f)
         big = o > 1e-12 * o.max()
-        assert big.sum() > 10, f
+        assert big.sum() >= 5, f
         assert np.max(np.abs(g[big] / o[big] - 1)) < 1e-9, f
     neb.close()
 
