@@ -17,6 +17,13 @@ Workloads (--workload):
   stromgren64    the pure-H Stromgren sphere: 64^3, 40 kK, Q(H) = 1e49,
                  1e6 packets, case B, T_e = 1e4 K, FP64; prepared to the
                  converged sphere.
+  clumpy_dusty   the dusty clumpy nebula on an octree of about 3e6 leaves
+                 (log-normal n_H, mean 30, from a seeded 256^3 random field;
+                 base level 6, refined towards level 10), three point
+                 sources (35/40/50 kK, Q(H) = 2e49 each), MW R_V = 3.1 grains
+                 with <cos> = 0.6 and scattering, FUV band from 6 eV, T_e
+                 solved (H + He), 3e7 packets per pass, FP32 segments.  The
+                 leaf list is generated once into the temp directory.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--workload W] [--impl reference]
 
@@ -76,6 +83,13 @@ class Workload:
             self.grid, self.nphot, self.thermal, self.prep = 64, 1_000_000, False, 60
             self.default_precision = "fp64"
             self.make = lambda nphot, prec, seed: configs.stromgren64(nphotons=nphot, n=64, precision=prec, seed=seed)
+        elif name == "clumpy_dusty":
+            import tempfile
+            cases = os.path.join(tempfile.gettempdir(), "mochii_b200_cases")
+            self.grid, self.nphot, self.thermal, self.prep = None, 30_000_000, True, 3
+            self.default_precision = "fp32"
+            self.make = lambda nphot, prec, seed: configs.clumpy_dusty(cases, nphotons=nphot, precision=prec,
+                                                                        qmc_seed=seed)
         else:
             raise SystemExit(f"unknown workload {name}")
 
@@ -89,6 +103,8 @@ def bytes_per_segment(wl, precision):
     w = 8 if precision == "fp64" else 4
     if wl.name == "stromgren64":
         return w * 2 + 16 * 3          # n_H, x_HI; Gamma_HI, H_HI, jt_ion
+    if wl.name == "clumpy_dusty":
+        return w * 5 + 16 * 9          # n_H, x_HI, x_HeI, x_HeII, rhokap; 6 H/He + jt_ion + dust_abs + FUV
     return w * 4 + 16 * (7 + 6)        # n_H, x_HI, x_HeI, x_HeII; 6 H/He + jt_ion + 6 metal moments
 
 
@@ -178,7 +194,8 @@ def cpu_threads(wl):
         mem = os.sysconf("SC_PAGE_SIZE") * os.sysconf("SC_PHYS_PAGES")
     except (ValueError, OSError):
         mem = 64 << 30
-    per = wl.grid ** 3 * 8 * (6 + 16 + (2 * 32 if wl.name == "hii_metals128" else 0))
+    nleaf = wl.grid ** 3 if wl.grid else 3_100_000
+    per = nleaf * 8 * (6 + 16 + (2 * 32 if wl.name == "hii_metals128" else 0) + (2 if wl.name == "clumpy_dusty" else 0))
     return max(1, min(n, int(0.5 * mem // max(per, 1))))
 
 
@@ -188,7 +205,7 @@ def cpu_reference(wl, state, nthreads, budget_s=20.0):
     thermal (or ionisation) solve on every stride-th leaf, each scaled to the
     step's packet / leaf count.  Returns (packets/s, description)."""
     from oracle import pyorc
-    sample = int(os.environ.get("MOCHII_CPU_SAMPLE", "200000" if wl.grid <= 64 else "100000"))
+    sample = int(os.environ.get("MOCHII_CPU_SAMPLE", "200000" if (wl.grid or 1024) <= 64 else "100000"))
     sim = pyorc.Sim(wl.make(sample, "fp64", 12345), nthreads=nthreads)
     for k, v in state.items():
         sim.set(k, v)
@@ -208,7 +225,7 @@ def cpu_reference(wl, state, nthreads, budget_s=20.0):
     t_pp = max(t_of[2 * sample] - t_of[sample], 1e-3 * t_of[sample]) / sample
     t_fixed = max(t_of[sample] - sample * t_pp, 0.0)
     t_pass = t_fixed + t_pp * wl.nphot
-    nleaf = wl.grid ** 3
+    nleaf = sim.nleaf
     if wl.thermal:
         stride = int(os.environ.get("MOCHII_CPU_CELL_STRIDE", "256"))
         t1 = time.perf_counter()
@@ -249,7 +266,7 @@ def run_reference(args, wl):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt / args.steps * 1e3,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic",
-            "config": {"workload": wl.name, "grid": f"{wl.grid}^3", "packets_per_step": wl.nphot,
+            "config": {"workload": wl.name, "grid": grid_name(wl, None), "packets_per_step": wl.nphot,
                        "state": "the workload's initial state",
                        "note": "each step a bounded sample of the workload's step, scaled"},
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": nthreads, "kind": "port", "sample": desc},
@@ -264,7 +281,7 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="mochii_b200")
-    ap.add_argument("--workload", default="hii_metals128", choices=["hii_metals128", "stromgren64"])
+    ap.add_argument("--workload", default="hii_metals128", choices=["hii_metals128", "stromgren64", "clumpy_dusty"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-converge", action="store_true", help="skip the time-to-converged comparison")
     ap.add_argument("--precision", default=None, choices=["fp64", "fp32"],
@@ -405,7 +422,7 @@ def main():
             "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64" if prec == "fp64" else "f32+f64",
             "data": "synthetic",
-            "config": {"workload": wl.name, "grid": f"{wl.grid}^3", "stellar_packets_per_step": wl.nphot,
+            "config": {"workload": wl.name, "grid": grid_name(wl, nleaf), "stellar_packets_per_step": wl.nphot,
                        "packets_per_step": packets / args.steps / world,
                        "precision": prec, "balance": "thermal" if wl.thermal else "ionisation, fixed T_e",
                        "solver": args.solver,
@@ -501,6 +518,10 @@ def time_to_converged(n=64, nphot=1_000_000, iters=20, train_iters=10, seed_trai
                     "iteration then carries Monte Carlo differences at the ionization front",
             "training": {"pairs": int(len(X)), "data_s": t_data, "train_s": t_train, "epochs": 20,
                          "loss_first": float(losses[0]), "loss_last": float(losses[-1])}}
+
+
+def grid_name(wl, nleaf):
+    return f"{wl.grid}^3" if wl.grid else f"octree, {nleaf or 'about 3e6'} leaves"
 
 
 def launches_per_step(wl, diffuse_packets):

@@ -99,7 +99,7 @@ def lognormal_field(n=256, mean=30.0, sigma_ln=1.0, slope=-11.0 / 3.0, seed=2024
     nz = k2 > 0
     amp[nz] = k2[nz] ** (slope / 4.0)   # |g_k| ~ sqrt(P(k)) = k^(slope/2)
     w = rng.standard_normal((n, n, n))
-    g = np.fft.irfftn(np.fft.rfftn(w) * amp, s=(n, n, n))
+    g = np.fft.irfftn(np.fft.rfftn(w) * amp, s=(n, n, n), axes=(0, 1, 2))
     g = (g - g.mean()) / g.std()
     return mean * np.exp(sigma_ln * g - 0.5 * sigma_ln * sigma_ln)
 

@@ -213,3 +213,96 @@ def on_octree(namelist, amr_file, density_from_file=True):
             out.append(f" par%amr_file = '{amr_file}'")
         out.append(line)
     return "\n".join(out) + "\n"
+
+
+def kext_with_g(src, dst, g=0.6):
+    """A copy of an extinction table whose <cos> column is g in every data
+    row (the row test of the table reader: four leading reals, lambda > 0),
+    so the Henyey-Greenstein asymmetry of the run is g at every energy while
+    the code path stays the table read."""
+    out = []
+    for line in open(src):
+        tok = line.split()
+        try:
+            v = [float(t) for t in tok[:4]]
+            ok = len(v) == 4 and v[0] > 0
+        except ValueError:
+            ok = False
+        if ok:
+            tok[2] = f"{g:.4f}"
+            line = " ".join(tok) + "\n"
+        out.append(line)
+    with open(dst, "w") as f:
+        f.writelines(out)
+    return dst
+
+
+KEXT_MW31 = os.path.join(os.path.dirname(ATOMIC_DIR), "kext_albedo_WD_MW_3.1_60_D03.all_2003")
+
+
+def clumpy_dusty(workdir, nphotons=30_000_000, niter=20, precision="fp32", seed=2024, box_pc=40.0,
+                 base_level=6, max_level=10, field_n=256, growth=1.47, scatter=True, qmc_seed=12345):
+    """The dusty clumpy nebula on an octree: a log-normal n_H (mean 30,
+    sigma_ln n = 1) from a seeded Gaussian random field with P(k) ~ k^-11/3
+    on field_n^3, an octree with base level base_level refined towards
+    max_level where n_H exceeds 4 <n_H> growth^(L - base_level) (about 3e6
+    leaves at the defaults), written as a text leaf list; three point
+    sources at seeded positions (35, 40, 50 kK, Q(H) = 2e49 s^-1 each); MW
+    R_V = 3.1 grains with the Henyey-Greenstein <cos> set to 0.6, dust-to-gas
+    0.01, scattering on; the band extended down to 6 eV (FUV); T_e solved
+    (H + He, case B), 3e7 packets per iteration.  Writes the leaf list and
+    the extinction table into workdir (reused when present) and returns the
+    namelist."""
+    import numpy as np
+    from . import amr
+    os.makedirs(workdir, exist_ok=True)
+    tag = f"s{seed}_b{base_level}_m{max_level}_n{field_n}_g{growth}_L{box_pc}"
+    leaves = os.path.join(workdir, f"clumpy_{tag}.txt")
+    if not os.path.exists(leaves):
+        field = amr.lognormal_field(n=field_n, mean=30.0, sigma_ln=1.0, seed=seed)
+        x, y, z, lev, nH = amr.clumpy_nebula(box_pc, field, base_level=base_level, max_level=max_level,
+                                             threshold=120.0, growth=growth)
+        tmp = leaves + ".part"
+        amr.write_leaf_list(tmp, box_pc, x, y, z, lev, nH)
+        os.replace(tmp, leaves)
+    kext = os.path.join(workdir, "kext_MW31_g0.6.txt")
+    if not os.path.exists(kext):
+        kext_with_g(KEXT_MW31, kext + ".part", 0.6)
+        os.replace(kext + ".part", kext)
+    rng = np.random.default_rng(seed + 1)
+    pos = rng.uniform(-0.3 * box_pc, 0.3 * box_pc, (3, 3))
+    temps = (3.5e4, 4.0e4, 5.0e4)
+    lums = [2.0e49 * mean_photon_energy_ev(t) * EV2ERG for t in temps]
+    arr = lambda v: ", ".join(f"{a:.10e}" for a in v)   # noqa: E731
+    return f"""&parameters
+ par%no_photons = {float(nphotons):.6e}
+ par%launch_sequence = 'sobol'
+ par%qmc_seed = {qmc_seed}
+ par%iseed = {seed}
+ par%grid_type = 'amr'
+ par%amr_file = '{leaves}'
+ par%distance_unit = 'pc'
+ par%He_abund = 0.1
+ par%nsource = 3
+ par%src_tstar(1) = {arr(temps)}
+ par%src_lum(1) = {arr(lums)}
+ par%src_x(1) = {arr(pos[:, 0])}
+ par%src_y(1) = {arr(pos[:, 1])}
+ par%src_z(1) = {arr(pos[:, 2])}
+ par%case_ab = 'B'
+ par%add_fuv = .true.
+ par%efuv_min = 6.0
+ par%ion_add_dust = .true.
+ par%ion_dust_scatter = {'.true.' if scatter else '.false.'}
+ par%ion_dust_kext = '{kext}'
+ par%dust_density_law = 'global_dgr'
+ par%DGR = 0.01
+ par%solve_te = .true.
+ par%te_min = 3.0e3
+ par%te_max = 3.0e4
+ par%te_fixed = 1.0e4
+ par%gas_niter = {niter}
+ par%atomic_dir = '{ATOMIC_DIR}'
+ par%precision = '{precision}'
+/
+"""

@@ -118,3 +118,30 @@ def test_grain_settings_errors(tmp_path):
     with pytest.raises(MochiiError) as ei:
         Nebula(parse_namelist(dusty(base).replace("/\n", " par%taumax = 2.0\n/\n")))
     assert ei.value.status == 8
+
+
+def test_clumpy_dusty_case_matches_oracle(orc, tmp_path):
+    """The dusty clumpy nebula at a reduced size (64^3 field, octree levels
+    4-6): three sources on the octree, FUV band, grain absorption and
+    scattering, then the thermal update, FP64 on both sides."""
+    nl = configs.clumpy_dusty(str(tmp_path), nphotons=200000, base_level=4, max_level=6, field_n=64,
+                              precision="fp64")
+    neb, sim = pair(orc, nl)
+    assert neb.nleaf == sim.nleaf > 3000
+    st = neb.ionizing_field_and_rates()
+    sim.transport_pass()
+    e, seg = sim.energy()
+    assert abs(st.energy_emitted / e[0] - 1) < 1e-12 and abs(st.energy_absorbed / e[1] - 1) < 1e-12
+    assert abs(st.scattered_segments / seg[1] - 1) < 5e-3
+    for f in ("gamma_HI", "gamma_HeI", "heat_dust", "g0_fuv"):
+        g, o = neb.get(f), sim.get(f)
+        big = o > 1e-3 * o.max()
+        assert np.median(np.abs(g[big] / o[big] - 1)) < 1e-6, f
+        assert abs(g.sum() / o.sum() - 1) < 1e-4, f
+    neb.gas_thermal_update()
+    sim.thermal_update()
+    dT = np.abs(neb.get("T_e") - sim.get("T_e"))
+    assert np.median(dT) < 1.0 and np.mean(dT > 20.0) < 0.01
+    dx = np.abs(neb.get("x_HI") - sim.get("x_HI"))
+    assert np.mean(dx > 1e-3) < 0.01
+    neb.close()
