@@ -288,6 +288,8 @@ def main():
                     help="transport arithmetic (default: the workload's)")
     ap.add_argument("--solver", default="bracketed", choices=["bisection", "bracketed"],
                     help="cell solver: the reference's bisection or the bracketed roots")
+    ap.add_argument("--cell-layout", default="warp", choices=["warp", "thread"],
+                    help="thermal solve with metals: one warp or one thread per leaf")
     args = ap.parse_args()
     wl = Workload(args.workload)
     prec = args.precision or wl.default_precision
@@ -311,7 +313,7 @@ def main():
         dist.barrier()
 
     par = parse_namelist(wl.make(wl.nphot, prec, 12345 + rank).replace(
-        "/\n", f" par%thermal_solver = '{args.solver}'\n/\n"))
+        "/\n", f" par%thermal_solver = '{args.solver}'\n par%cell_layout = '{args.cell_layout}'\n/\n"))
     neb = Nebula(par)
     prep_iters = prepare(neb, wl)
     tuning = neb.autotune(1 << 20)   # launch shape for this grid / precision / device
@@ -425,7 +427,7 @@ def main():
             "config": {"workload": wl.name, "grid": grid_name(wl, nleaf), "stellar_packets_per_step": wl.nphot,
                        "packets_per_step": packets / args.steps / world,
                        "precision": prec, "balance": "thermal" if wl.thermal else "ionisation, fixed T_e",
-                       "solver": args.solver,
+                       "solver": args.solver, "cell_layout": args.cell_layout,
                        "state": f"{prep_iters} untimed preparation iterations from the configured start",
                        "l2": "flushed between steps (256 MiB write)", "tuning": tuning,
                        "parallelism": "replicas" if world > 1 else "single"},

@@ -135,6 +135,10 @@ typedef struct mochii_params {
     /* grain optics reference wavelength [um] and the dust normalisations
      * (define.f90:211-212,361); taumax / tauhomo > 0 are not built */
     double lambda_ref, taumax, tauhomo;
+    /* thermal solve with metals (not a reference key, 'warp' or 'thread'):
+     * 1 = one warp per leaf, the metal cascade spread over the lanes;
+     * 0 = one thread per leaf */
+    int solver_warp;
 } mochii_params;
 
 /* Per-pass statistics (ion_score_report_energy_closure, ion_score_mod.f90:364-387). */

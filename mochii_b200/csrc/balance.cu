@@ -150,9 +150,10 @@ __device__ int solve_cell(const Coef& k, double yHe, double gH, double gHe1, dou
 // electrons join the n_e closure (metal_ne), and with the two-way charge
 // exchange x_HI is the root of hydrogen's balance at each n_e
 // (hydrogen_neutral_fraction); the cache mc is prepared at T.
+template <class Cas>
 __device__ __noinline__ int solve_cell_metal(const Coef& k, double yHe, double gH, double gHe1, double gHe2, double nH,
-                                             double& xHI, double& xHeI, double& xHeII, double& ne, const MetalDev& m,
-                                             const MetalCache& mc, int with_ne, int with_cx, int* nsum) {
+                                             double& xHI, double& xHeI, double& xHeII, double& ne, const Cas& mc,
+                                             int with_ne, int with_cx, int* nsum) {
     double xHeIII = fmax(0.0, 1.0 - xHeI - xHeII);
     ne = nH * ((1.0 - xHI) + yHe * (xHeII + 2.0 * xHeIII));
     ne = fmax(ne, 1.0e-12 * nH);
@@ -161,7 +162,7 @@ __device__ __noinline__ int solve_cell_metal(const Coef& k, double yHe, double g
     for (; it <= 200; ++it) {
         const double ne_old = ne;
         if (with_ne || with_cx) {
-            metal_sums(m, mc, nH, ne_old, nH * xHI, nH * (1.0 - xHI), nem, rin, rout);
+            mc.sums(nH, ne_old, nH * xHI, nH * (1.0 - xHI), nem, rin, rout);
             ++*nsum;
             if (!with_cx) {
                 rin = 0.0;
@@ -169,7 +170,7 @@ __device__ __noinline__ int solve_cell_metal(const Coef& k, double yHe, double g
             }
         }
         if (with_cx) {
-            xHI = hydrogen_neutral_fraction(m, mc, nH, ne, k.aH * ne, gH + (k.cH + k.aH) * ne, nsum);
+            xHI = hydrogen_neutral_fraction(mc, nH, ne, k.aH * ne, gH + (k.cH + k.aH) * ne, nsum);
         } else {
             const double denH = gH + (k.cH + k.aH) * ne + rin + rout;
             xHI = denH > 0.0 ? (k.aH * ne + rin) / denH : 1.0;
@@ -199,12 +200,12 @@ struct CellState {
     double x, h1, h2;
 };
 
+template <class Cas>
 __device__ __noinline__ double cell_electrons(const Coef& k, double yHe, double gH, double gHe1, double gHe2, double nH,
-                                              double ne, const MetalDev& m, const MetalCache& mc, int with_ne,
-                                              int with_cx, int* nsum, CellState& o) {
-    const bool metals = m.ntr > 0;
+                                              double ne, bool metals, const Cas& mc, int with_ne, int with_cx,
+                                              int* nsum, CellState& o) {
     if (metals && with_cx) {
-        o.x = hydrogen_neutral_fraction(m, mc, nH, ne, k.aH * ne, gH + (k.cH + k.aH) * ne, nsum);
+        o.x = hydrogen_neutral_fraction(mc, nH, ne, k.aH * ne, gH + (k.cH + k.aH) * ne, nsum);
     } else {
         const double denH = gH + (k.cH + k.aH) * ne;
         o.x = denH > 0.0 ? (k.aH * ne) / denH : 1.0;
@@ -217,7 +218,7 @@ __device__ __noinline__ double cell_electrons(const Coef& k, double yHe, double 
     double nen = nH * ((1.0 - o.x) + yHe * (o.h2 + 2.0 * h3));
     if (metals && with_ne) {
         double nem, rin, rout;
-        metal_sums(m, mc, nH, ne, nH * o.x, nH * (1.0 - o.x), nem, rin, rout);
+        mc.sums(nH, ne, nH * o.x, nH * (1.0 - o.x), nem, rin, rout);
         ++*nsum;
         nen = nen + nem;
     }
@@ -225,16 +226,17 @@ __device__ __noinline__ double cell_electrons(const Coef& k, double yHe, double 
 }
 
 // Returns the number of F evaluations.
+template <class Cas>
 __device__ __noinline__ int solve_cell_fast(const Coef& k, double yHe, double gH, double gHe1, double gHe2, double nH,
-                                            double& xHI, double& xHeI, double& xHeII, double& ne, const MetalDev& m,
-                                            const MetalCache& mc, int with_ne, int with_cx, int* nsum, double nemax) {
+                                            double& xHI, double& xHeI, double& xHeII, double& ne, bool metals,
+                                            const Cas& mc, int with_ne, int with_cx, int* nsum, double nemax) {
     const double floor = 1.0e-12 * nH, top = nemax * nH;
     const double xHeIII = fmax(0.0, 1.0 - xHeI - xHeII);
     double a = ne > floor ? ne : fmax(nH * ((1.0 - xHI) + yHe * (xHeII + 2.0 * xHeIII)), floor);
     a = fmin(a, top);
     int nev = 0;
     CellState ea, eb, ec;
-    double fa = cell_electrons(k, yHe, gH, gHe1, gHe2, nH, a, m, mc, with_ne, with_cx, nsum, ea) - a;
+    double fa = cell_electrons(k, yHe, gH, gHe1, gHe2, nH, a, metals, mc, with_ne, with_cx, nsum, ea) - a;
     ++nev;
     double b = a, fb = fa;
     eb = ea;
@@ -243,7 +245,7 @@ __device__ __noinline__ int solve_cell_fast(const Coef& k, double yHe, double gH
         double fac = 1.25;
         while (nev < 60) {
             const double c = fa > 0.0 ? fmin(a * fac, top) : fmax(a / fac, floor);
-            const double fc = cell_electrons(k, yHe, gH, gHe1, gHe2, nH, c, m, mc, with_ne, with_cx, nsum, ec) - c;
+            const double fc = cell_electrons(k, yHe, gH, gHe1, gHe2, nH, c, metals, mc, with_ne, with_cx, nsum, ec) - c;
             ++nev;
             b = c; fb = fc; eb = ec;
             if (fc == 0.0 || (fc > 0.0) != (fa > 0.0)) break;
@@ -265,7 +267,7 @@ __device__ __noinline__ int solve_cell_fast(const Coef& k, double yHe, double gH
             double lc = (la * fb - lb * fa) / (fb - fa);
             if (bisect || !(fabs(lc - la) > 0.05 * width && fabs(lc - lb) > 0.05 * width)) lc = 0.5 * (la + lb);
             const double c = exp(lc);
-            const double fc = cell_electrons(k, yHe, gH, gHe1, gHe2, nH, c, m, mc, with_ne, with_cx, nsum, ec) - c;
+            const double fc = cell_electrons(k, yHe, gH, gHe1, gHe2, nH, c, metals, mc, with_ne, with_cx, nsum, ec) - c;
             ++nev;
             b = c;          // the returned point is the last one evaluated
             eb = ec;
@@ -301,17 +303,18 @@ __global__ void __launch_bounds__(kBThreads) k_balance(const BalArgs a) {
             continue;
         }
         double xHI = x0, xHeI = h10, xHeII = h20, ne;
-        MetalCache mc;
+        SerialCascade mc;
+        mc.m = &a.m;
         int it, nsum = 0;
         if (a.fast) {
-            if (a.m.ntr > 0) metal_prepare(a.m, il, a.T, mc);
+            if (a.m.ntr > 0) mc.prepare(il, a.T);
             ne = a.ne[il];
             it = solve_cell_fast(a.k, a.yHe, a.rates[il], a.rates[a.nleaf + il], a.rates[2 * a.nleaf + il], nH, xHI,
-                                 xHeI, xHeII, ne, a.m, mc, a.metal_ne, a.two_way, &nsum, a.nemax);
+                                 xHeI, xHeII, ne, a.m.ntr > 0, mc, a.metal_ne, a.two_way, &nsum, a.nemax);
         } else if (a.m.ntr > 0) {
-            metal_prepare(a.m, il, a.T, mc);
+            mc.prepare(il, a.T);
             it = solve_cell_metal(a.k, a.yHe, a.rates[il], a.rates[a.nleaf + il], a.rates[2 * a.nleaf + il], nH, xHI,
-                                  xHeI, xHeII, ne, a.m, mc, a.metal_ne, a.two_way, &nsum);
+                                  xHeI, xHeII, ne, mc, a.metal_ne, a.two_way, &nsum);
         } else {
             it = solve_cell(a.k, a.yHe, a.rates[il], a.rates[a.nleaf + il], a.rates[2 * a.nleaf + il], nH, xHI, xHeI,
                             xHeII, ne);
@@ -332,11 +335,11 @@ __global__ void __launch_bounds__(kBThreads) k_balance(const BalArgs a) {
         if (a.m.ntr > 0) {
             // metal electrons of the written state (ion_balance_mod.f90:401-410),
             // then the stage cache at the written T_e (gas_opacity_fill)
-            if (a.metal_ne) nen = charge_neutrality_ne(a.m, mc, nH, nen, xn, ne);
+            if (a.metal_ne) nen = charge_neutrality_ne(mc, nH, nen, xn, ne);
             const double Tw = a.Te[il];
-            if (Tw != a.T) metal_prepare(a.m, il, Tw, mc);
-            if (a.fp32) metal_opacity_fill<float>(a.m, mc, il, nH, nen, xn, a.colscale);
-            else metal_opacity_fill<double>(a.m, mc, il, nH, nen, xn, a.colscale);
+            if (Tw != a.T) mc.prepare(il, Tw);
+            if (a.fp32) mc.opacity_fill<float>(il, nH, nen, xn, a.colscale);
+            else mc.opacity_fill<double>(il, nH, nen, xn, a.colscale);
         }
         a.ne[il] = nen;
         write_columns(a.col, il, a.nabs, a.fp32, nH, a.yHe, xn, h1n, h2n, a.colscale, a.rhokap ? a.rhokap[il] : 0.0);
@@ -515,28 +518,251 @@ __device__ __noinline__ MetalThermalTerms metal_thermal(const ThermalDev& td, co
     return o;
 }
 
+__device__ __forceinline__ MetalThermalTerms thermal_terms(const ThermalDev& td, const SerialCascade& cas, long long il,
+                                                         double T, double nH, double ne, double nHI, double nHII) {
+    return metal_thermal(td, *cas.m, cas.c, il, T, nH, ne, nHI, nHII);
+}
+
+// ---- the metal cascade of one leaf spread over one warp ---------------------
+// The thermal solve of a leaf with metals evaluates, per trial temperature,
+// every transition's collisional-ionisation, recombination and charge-
+// exchange coefficients and every stage's line cooling, then walks each
+// element's stage chain many times (the n_e closure and the H root).  One
+// thread per leaf keeps that cache in local memory and runs the leaves of a
+// warp through different trial sequences.  Here one warp owns one leaf:
+// lane j % 32 evaluates the coefficients of transition j and the line
+// cooling of stage s (lane s % 32), element e's chain is walked by lane e
+// from its own registers (its <= 5 transitions, fetched once per trial
+// temperature), and the per-element sums are added in element order with
+// the result in every lane.  Every lane runs the same solver control flow
+// on the same values; the leaf's H/He arithmetic is repeated in all lanes.
+constexpr unsigned kFull = 0xffffffffu;
+constexpr int kTrSlots = (kMaxTr + 31) / 32;
+constexpr int kStSlots = (kMaxEl * kMaxSt + 31) / 32;
+constexpr int kEt = kMaxSt - 1;   // transitions per element
+
+template <int S>
+__device__ __forceinline__ double lane_fetch(const double (&v)[S], int j) {
+    double out = 0.0;
+#pragma unroll
+    for (int q = 0; q < S; ++q) {
+        const double x = __shfl_sync(kFull, v[q], j & 31);
+        if ((j >> 5) == q) out = x;
+    }
+    return out;
+}
+
+struct WarpCascade {
+    const MetalDev* m;
+    int lane, ns, tr0, st0, kind, coolmask;
+    long long il = -1;
+    double abund;
+    double gam[kEt], eheat[kEt], ci[kEt], rec[kEt], cxi[kEt], cxr[kEt];
+
+    __device__ void init(const MetalDev& md) {
+        m = &md;
+        lane = threadIdx.x & 31;
+        ns = 1; tr0 = 0; st0 = 0; kind = 0; coolmask = 0; abund = 0.0;
+        if (lane < md.nel) {
+            const MetalEl e = md.el[lane];
+            ns = e.nstage; tr0 = e.tr0; st0 = e.st0; kind = e.kind; abund = e.abund;
+            for (int i = 0; i < ns; ++i)
+                if (md.st[st0 + i].has_cool) coolmask |= 1 << i;
+        }
+    }
+    // the element's photoionisation and photoheating rates in leaf l
+    __device__ void leaf(long long l) {
+        il = l;
+#pragma unroll
+        for (int i = 0; i < kEt; ++i) {
+            gam[i] = 0.0;
+            eheat[i] = 0.0;
+            if (i < ns - 1) {
+                gam[i] = m->egam[l * m->ntr + tr0 + i];
+                eheat[i] = m->eheat[l * m->ntr + tr0 + i];
+            }
+        }
+    }
+    // species_ne_prepare (species_mod.f90:517-536) at T
+    __device__ void prepare(long long l, double T) {
+        if (l != il) leaf(l);
+        double tci[kTrSlots], trec[kTrSlots], tcxi[kTrSlots], tcxr[kTrSlots];
+#pragma unroll
+        for (int q = 0; q < kTrSlots; ++q) {
+            const int j = lane + 32 * q;
+            tci[q] = trec[q] = tcxi[q] = tcxr[q] = 0.0;
+            if (j < m->ntr) {
+                const MetalTr& r = m->tr[j];
+                tci[q] = voronov(T, r.ci[0], r.ci[1], r.ci[2], r.ci[3], r.ci[4]) * r.cidr;
+                trec[q] = metal_alpha_rec(r, T);
+                tcxi[q] = r.cxi_form > 0 ? metal_cx_rate(r.cxi_form, r.cxi, T) : 0.0;
+                tcxr[q] = r.cxr_form > 0 ? metal_cx_rate(r.cxr_form, r.cxr, T) : 0.0;
+            }
+        }
+#pragma unroll
+        for (int i = 0; i < kEt; ++i) {
+            const int j = i < ns - 1 ? tr0 + i : 0;
+            ci[i] = lane_fetch(tci, j);
+            rec[i] = lane_fetch(trec, j);
+            cxi[i] = lane_fetch(tcxi, j);
+            cxr[i] = lane_fetch(tcxr, j);
+        }
+    }
+    // metal_chain: ratios n_{i+1}/n_i and the stage-1 fraction
+    __device__ __forceinline__ double chain(double ne, double nHI, double nHII, double (&r)[kEt]) const {
+#pragma unroll
+        for (int i = 0; i < kEt; ++i) {
+            double rion = gam[i] + ne * ci[i];
+            if (cxi[i] > 0.0) rion = rion + nHII * cxi[i];
+            double rrec = ne * rec[i];
+            if (cxr[i] > 0.0) rrec = rrec + nHI * cxr[i];
+            r[i] = rion / fmax(rrec, kTinest);
+        }
+        double s = 1.0, prod = 1.0;
+#pragma unroll
+        for (int i = 0; i < kEt; ++i)
+            if (i < ns - 1) {
+                prod = prod * r[i];
+                s = s + prod;
+            }
+        return 1.0 / s;
+    }
+    __device__ __forceinline__ double element_sum(double v) const {
+        double t = 0.0;
+        for (int e = 0; e < m->nel; ++e) t = t + __shfl_sync(kFull, v, e);
+        return t;
+    }
+    // species_metal_sums (species_mod.f90:566-614)
+    __device__ void sums(double nH, double ne, double nHI, double nHII, double& nem, double& rin, double& rout) const {
+        double pn = 0.0, pi = 0.0, po = 0.0;
+        if (lane < m->nel) {
+            double r[kEt];
+            double fr = chain(ne, nHI, nHII, r);
+            const double nX = abund * nH;
+            if (ns > 1) pi = cxi[0] * nX * fr;
+#pragma unroll
+            for (int i = 2; i <= kMaxSt; ++i)
+                if (i <= ns) {
+                    fr = fr * r[i - 2];
+                    pn = pn + abund * nH * fr * (double)(i - 1);
+                    po = po + cxr[i - 2] * nX * fr;
+                    if (i < ns) pi = pi + cxi[i - 1] * nX * fr;
+                }
+        }
+        nem = element_sum(pn);
+        rin = element_sum(pi);
+        rout = element_sum(po);
+    }
+    // species_stage_cache_refresh (species_mod.f90:247-261): the element
+    // lanes write their transitions' opacity weights
+    template <typename R>
+    __device__ void opacity_fill(long long l, double nH, double ne, double xHI, double colscale) const {
+        if (lane >= m->nel) return;
+        R* o = static_cast<R*>(m->opac) + l * m->ntrp;
+        double r[kEt];
+        double fr = chain(ne, nH * xHI, nH * (1.0 - xHI), r);
+#pragma unroll
+        for (int it = 1; it <= kEt; ++it)
+            if (it <= ns - 1) {
+                if (it > 1) fr = fr * r[it - 2];
+                o[m->tr[tr0 + it - 1].flat] = (R)(nH * (abund * fr) * colscale);
+            }
+    }
+    // the metal terms of net_rate (thermal_mod.f90:53-71), as metal_thermal
+    __device__ MetalThermalTerms thermal(const ThermalDev& td, double T, double nH, double ne, double nHI,
+                                         double nHII) const {
+        const double A_CII = 2.321e-6, A_OI = 8.865e-5;
+        const double rsT = 1.0 / sqrt(T);
+        double lam[kStSlots];
+#pragma unroll
+        for (int q = 0; q < kStSlots; ++q) {
+            const int sidx = lane + 32 * q;
+            lam[q] = 0.0;
+            if (sidx < m->nst) {
+                const MetalStage& st = m->st[sidx];
+                if (st.has_cool) {
+                    double fit = 0.0;
+                    for (int k = 0; k < st.nterm; ++k) fit = fit + st.A[k] * exp(-st.Ti[k] / T);
+                    fit = fit * rsT;
+                    lam[q] = st.table >= 0 ? nl_apply(m->lamref + (size_t)st.table * kNlNT,
+                                                      m->Ssup + (size_t)st.table * kNlNT * kNlNNE, td.tinv, fit, T, ne)
+                                           : fit;
+                }
+            }
+        }
+        double lm[kMaxSt];
+#pragma unroll
+        for (int i = 0; i < kMaxSt; ++i) lm[i] = lane_fetch(lam, i < ns ? st0 + i : 0);
+        double pc = 0.0, ph = 0.0, pf = 0.0, pq = 0.0;
+        if (lane < m->nel) {
+            double g[4];
+            for (int z = 1; z <= 4; ++z) g[z - 1] = gbar_ff(td.gff, T, z);
+            double r[kEt], frac[kMaxSt];
+            frac[0] = chain(ne, nHI, nHII, r);
+#pragma unroll
+            for (int i = 1; i < kMaxSt; ++i) frac[i] = i < ns ? frac[i - 1] * r[i - 1] : 0.0;
+            const double nel = abund * nH;
+#pragma unroll
+            for (int i = 0; i < kMaxSt; ++i)
+                if (i < ns && ((coolmask >> i) & 1)) pc = pc + ne * nel * frac[i] * lm[i];
+            if (kind == 1 && ns >= 2) {   // [C II] 158 um, H impact
+                const double nion = abund * nH * frac[1];
+                const double qul = 7.6e-10 * pow(T / 100.0, 0.14);
+                const double qlu = 2.0 * qul * exp(-91.25 / T);
+                ph = nion * nHI * qlu * (91.25 * kKboltz) / (1.0 + nHI * (qul + qlu) / A_CII);
+            } else if (kind == 2) {       // [O I] 63 um
+                const double nion = abund * nH * frac[0];
+                const double qul = 9.2e-11 * pow(T / 100.0, 0.67);
+                const double qlu = 0.6 * qul * exp(-227.7 / T);
+                ph = nion * nHI * qlu * (227.7 * kKboltz) / (1.0 + nHI * (qul + qlu) / A_OI);
+            }
+#pragma unroll
+            for (int j = 2; j <= kMaxSt; ++j)
+                if (j <= ns) {
+                    const int zion = j - 1;
+                    pf = pf + abund * frac[j - 1] * (double)(zion * zion) * g[min(zion, 4) - 1];
+                }
+#pragma unroll
+            for (int i = 1; i <= kEt; ++i)
+                if (i <= ns - 1) pq = pq + abund * nH * frac[i - 1] * eheat[i - 1];
+        }
+        MetalThermalTerms o;
+        o.cool = element_sum(pc);
+        o.cool_H = element_sum(ph);
+        o.freefree = 1.42554e-27 * sqrt(T) * ne * nH * element_sum(pf);
+        o.heat = element_sum(pq);
+        return o;
+    }
+};
+
+__device__ __forceinline__ MetalThermalTerms thermal_terms(const ThermalDev& td, const WarpCascade& cas, long long,
+                                                         double T, double nH, double ne, double nHI, double nHII) {
+    return cas.thermal(td, T, nH, ne, nHI, nHII);
+}
+
 // net_rate (thermal_mod.f90:38-115).  With metals the (leaf, T) cache mc is
 // prepared here at T and left for the caller.
+template <class Cas>
 __device__ double net_rate(const ThArgs& a, long long il, double T, double nH, double& xHI, double& xHeI,
-                           double& xHeII, double& ne, int* passes, MetalCache& mc, int* nsum) {
+                           double& xHeII, double& ne, int* passes, Cas& mc, int* nsum) {
     const BalArgs& b = a.b;
     const long long n = b.nleaf;
     const Coef k = coef_at_call(b.rs, b.caseA, T);
     if (b.fast) {
-        if (b.m.ntr > 0) metal_prepare(b.m, il, T, mc);
+        if (b.m.ntr > 0) mc.prepare(il, T);
         *passes += solve_cell_fast(k, b.yHe, b.rates[il], b.rates[n + il], b.rates[2 * n + il], nH, xHI, xHeI, xHeII,
-                                   ne, b.m, mc, b.metal_ne, b.two_way, nsum, b.nemax);
+                                   ne, b.m.ntr > 0, mc, b.metal_ne, b.two_way, nsum, b.nemax);
     } else if (b.m.ntr > 0) {
-        metal_prepare(b.m, il, T, mc);
+        mc.prepare(il, T);
         *passes += solve_cell_metal(k, b.yHe, b.rates[il], b.rates[n + il], b.rates[2 * n + il], nH, xHI, xHeI, xHeII,
-                                    ne, b.m, mc, b.metal_ne, b.two_way, nsum);
+                                    ne, mc, b.metal_ne, b.two_way, nsum);
     } else {
         *passes += solve_cell(k, b.yHe, b.rates[il], b.rates[n + il], b.rates[2 * n + il], nH, xHI, xHeI, xHeII, ne);
     }
     const double heat = nH * (xHI * b.rates[3 * n + il] + b.yHe * (xHeI * b.rates[4 * n + il] + xHeII * b.rates[5 * n + il]));
     double net = heat - cooling_total(a.td, b.rs, b.caseA, b.yHe, T, nH, ne, xHI, xHeI, xHeII);
     if (b.m.ntr > 0) {
-        const MetalThermalTerms mt = metal_thermal(a.td, b.m, mc, il, T, nH, ne, nH * xHI, nH * (1.0 - xHI));
+        const MetalThermalTerms mt = thermal_terms(a.td, mc, il, T, nH, ne, nH * xHI, nH * (1.0 - xHI));
         net = net - mt.cool;
         net = net - mt.cool_H;
         if (b.metal_ff) net = net - mt.freefree;
@@ -553,8 +779,9 @@ __device__ double net_rate(const ThArgs& a, long long il, double T, double nH, d
 // safeguarded false position in ln T until the bracket is below 1e-5 in ln T
 // (the reference's bisection stops at thi/tlo - 1 < 1e-5).  The cell state
 // left behind is the one solved at the returned T_e.
+template <class Cas>
 __device__ double thermal_bracketed(const ThArgs& a, long long il, double nH, double& xHI, double& xHeI, double& xHeII,
-                                    double& ne, int* passes, MetalCache& mc, int* nsum, int* nev, double Tw) {
+                                    double& ne, int* passes, Cas& mc, int* nsum, int* nev, double Tw) {
     const double lo_lim = a.te_min, hi_lim = a.te_max;
     double ta = fmin(fmax(Tw, lo_lim), hi_lim);
     double fa = net_rate(a, il, ta, nH, xHI, xHeI, xHeII, ne, passes, mc, nsum);
@@ -619,7 +846,8 @@ __global__ void __launch_bounds__(kBThreads) k_thermal(const ThArgs a) {
         double xHI = x0, xHeI = h10, xHeII = h20, ne = 0.0;
         int passes = 0, nsum = 0, nev = 0, last = 0;
         double te;
-        MetalCache mc;
+        SerialCascade mc;
+        mc.m = &b.m;
         if (b.fast) {
             ne = b.ne[il];
             te = thermal_bracketed(a, il, nH, xHI, xHeI, xHeII, ne, &passes, mc, &nsum, &nev,
@@ -659,9 +887,9 @@ __global__ void __launch_bounds__(kBThreads) k_thermal(const ThArgs a) {
         if (b.m.ntr > 0) {
             // written state at te (thermal_mod.f90:191-203); mc is at te from
             // the final net_rate, which is also the stage cache's temperature
-            if (b.metal_ne) nen = charge_neutrality_ne(b.m, mc, nH, nen, xn, ne);
-            if (b.fp32) metal_opacity_fill<float>(b.m, mc, il, nH, nen, xn, b.colscale);
-            else metal_opacity_fill<double>(b.m, mc, il, nH, nen, xn, b.colscale);
+            if (b.metal_ne) nen = charge_neutrality_ne(mc, nH, nen, xn, ne);
+            if (b.fp32) mc.opacity_fill<float>(il, nH, nen, xn, b.colscale);
+            else mc.opacity_fill<double>(il, nH, nen, xn, b.colscale);
         }
         b.xHI[il] = xn;
         b.xHeI[il] = h1n;
@@ -704,6 +932,114 @@ __global__ void __launch_bounds__(kBThreads) k_thermal(const ThArgs a) {
         if (tpass) atomicAdd(b.counters + 2, tpass);
         if (tsums) atomicAdd(b.counters + 3, tsums);
         if (nevals) atomicAdd(b.counters + 4, nevals);
+    }
+}
+
+// gas_thermal_update with metals, one warp per leaf (WarpCascade): the
+// same solve as k_thermal; lane 0 writes the leaf's state, the element lanes
+// its opacity weights.  128-thread blocks, grid-stride over leaves by warps.
+constexpr int kWThreads = 128;
+
+__global__ void __launch_bounds__(kWThreads) k_thermal_warp(const ThArgs a) {
+    __shared__ double sh[6][kWThreads / 32];
+    const BalArgs& b = a.b;
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    double mdx = 0.0, mdt = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0, s4 = 0.0;
+    unsigned long long solved = 0, caps = 0, tpass = 0, tsums = 0, nevals = 0;
+    WarpCascade mc;
+    mc.init(b.m);
+    const long long nw = (long long)gridDim.x * (blockDim.x >> 5);
+    for (long long il = (long long)blockIdx.x * (blockDim.x >> 5) + wib; il < b.nleaf; il += nw) {
+        const double nH = b.nH[il];
+        const double x0 = b.xHI[il], h10 = b.xHeI[il], h20 = b.xHeII[il], T0 = b.Te[il];
+        if (nH <= 0.0) {
+            if (lane == 0) {
+                b.ne[il] = 0.0;
+                write_columns(b.col, il, b.nabs, b.fp32, nH, b.yHe, x0, h10, h20, b.colscale,
+                              b.rhokap ? b.rhokap[il] : 0.0);
+            }
+            continue;
+        }
+        double xHI = x0, xHeI = h10, xHeII = h20, ne = 0.0;
+        int passes = 0, nsum = 0, nev = 0, last = 0;
+        double te;
+        if (b.fast) {
+            ne = b.ne[il];
+            te = thermal_bracketed(a, il, nH, xHI, xHeI, xHeII, ne, &passes, mc, &nsum, &nev,
+                                   a.Twarm ? a.Twarm[il] : T0);
+        } else {
+            double tlo = a.te_min, thi = a.te_max;
+            nev = 3;
+            const double net_lo = net_rate(a, il, tlo, nH, xHI, xHeI, xHeII, ne, &passes, mc, &nsum);
+            const double net_hi = net_rate(a, il, thi, nH, xHI, xHeI, xHeII, ne, &passes, mc, &nsum);
+            if (net_lo <= 0.0) {
+                te = tlo;
+            } else if (net_hi >= 0.0) {
+                te = thi;
+            } else {
+                for (int it = 1; it <= 60; ++it) {
+                    const double tmid = sqrt(tlo * thi);
+                    const double nm = net_rate(a, il, tmid, nH, xHI, xHeI, xHeII, ne, &passes, mc, &nsum);
+                    ++nev;
+                    if (nm > 0.0) tlo = tmid; else thi = tmid;
+                    if (thi / tlo - 1.0 < 1.0e-5) break;
+                }
+                te = sqrt(tlo * thi);
+            }
+            net_rate(a, il, te, nH, xHI, xHeI, xHeII, ne, &last, mc, &nsum);
+            if (last > 200) ++caps;
+        }
+        ++solved;
+        tpass += (unsigned long long)(passes + last);
+        tsums += (unsigned long long)nsum;
+        nevals += (unsigned long long)nev;
+        const double w = b.relax;
+        const double xn = (1.0 - w) * x0 + w * xHI;
+        const double h1n = (1.0 - w) * h10 + w * xHeI;
+        const double h2n = (1.0 - w) * h20 + w * xHeII;
+        const double h3n = fmax(0.0, 1.0 - h1n - h2n);
+        double nen = nH * ((1.0 - xn) + b.yHe * (h2n + 2.0 * h3n));
+        // written state at te (thermal_mod.f90:191-203); the cascade is at te
+        // from the final net_rate
+        if (b.metal_ne) nen = charge_neutrality_ne(mc, nH, nen, xn, ne);
+        if (b.fp32) mc.opacity_fill<float>(il, nH, nen, xn, b.colscale);
+        else mc.opacity_fill<double>(il, nH, nen, xn, b.colscale);
+        if (lane == 0) {
+            b.xHI[il] = xn;
+            b.xHeI[il] = h1n;
+            b.xHeII[il] = h2n;
+            b.ne[il] = nen;
+            b.Te[il] = te;
+            write_columns(b.col, il, b.nabs, b.fp32, nH, b.yHe, xn, h1n, h2n, b.colscale,
+                          b.rhokap ? b.rhokap[il] : 0.0);
+        }
+        const double dx = fabs(xn - x0);
+        mdx = fmax(mdx, dx);
+        mdt = fmax(mdt, fabs(te - T0) / T0);
+        const double vol = leaf_vol(b, il);
+        s1 = s1 + vol * dx;
+        s2 = s2 + vol * (1.0 - xn);
+        s3 = s3 + vol * nen * fabs(te - T0);
+        s4 = s4 + vol * nen * te;
+    }
+    // every lane of a warp holds the same sums; lane 0 reports them
+    if (lane == 0) {
+        sh[0][wib] = mdx; sh[1][wib] = mdt; sh[2][wib] = s1; sh[3][wib] = s2; sh[4][wib] = s3; sh[5][wib] = s4;
+        if (solved) atomicAdd(b.counters + 0, solved);
+        if (caps) atomicAdd(b.counters + 1, caps);
+        if (tpass) atomicAdd(b.counters + 2, tpass);
+        if (tsums) atomicAdd(b.counters + 3, tsums);
+        if (nevals) atomicAdd(b.counters + 4, nevals);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double r[6] = {sh[0][0], sh[1][0], sh[2][0], sh[3][0], sh[4][0], sh[5][0]};
+        for (int w = 1; w < (int)(blockDim.x >> 5); ++w) {
+            r[0] = fmax(r[0], sh[0][w]);
+            r[1] = fmax(r[1], sh[1][w]);
+            for (int k = 2; k < 6; ++k) r[k] = r[k] + sh[k][w];
+        }
+        for (int k = 0; k < 6; ++k) b.partial[6 * blockIdx.x + k] = r[k];
     }
 }
 
@@ -815,7 +1151,8 @@ cudaError_t launch_thermal(mochii_ctx* c) {
     a.te_min = c->par.te_min;
     a.te_max = c->par.te_max;
     a.Twarm = c->twarm_set ? c->twarm : nullptr;
-    k_thermal<<<c->bw.blocks, kBThreads, 0, c->stream>>>(a);
+    if (c->metal.ntr > 0 && c->par.solver_warp) k_thermal_warp<<<c->bw.blocks, kWThreads, 0, c->stream>>>(a);
+    else k_thermal<<<c->bw.blocks, kBThreads, 0, c->stream>>>(a);
     return cudaGetLastError();
 }
 

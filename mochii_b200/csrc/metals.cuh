@@ -153,16 +153,20 @@ static __device__ __noinline__ void metal_sums(const MetalDev& m, const MetalCac
 
 // hydrogen_neutral_fraction (ion_balance_mod.f90:177-208): Illinois false
 // position for x_HI on [0, 1] with the charge-exchange terms re-evaluated at
-// every trial x.
-static __device__ __noinline__ double hydrogen_neutral_fraction(const MetalDev& m, const MetalCache& c, double nH, double ne,
-                                                         double A, double B, int* nsum) {
+// every trial x.  Cas is the metal cascade at the cell's temperature: a
+// type with sums(nH, ne, nHI, nHII, nem, rin, rout) (species_metal_sums) --
+// SerialCascade below (one thread per leaf) or WarpCascade (one warp per
+// leaf, cascade_warp.cuh).
+template <class Cas>
+static __device__ __noinline__ double hydrogen_neutral_fraction(const Cas& cas, double nH, double ne, double A,
+                                                                double B, int* nsum) {
     double nem, rin, rout;
     *nsum += 2;
     double xa = 0.0;
-    metal_sums(m, c, nH, ne, 0.0, nH, nem, rin, rout);
+    cas.sums(nH, ne, 0.0, nH, nem, rin, rout);
     double Ra = -(A + rin);
     double xb = 1.0;
-    metal_sums(m, c, nH, ne, nH, 0.0, nem, rin, rout);
+    cas.sums(nH, ne, nH, 0.0, nem, rin, rout);
     double Rb = B + rout;
     const double scale = A + B + fabs(Ra) + fabs(Rb);
     double x = xb;
@@ -170,7 +174,7 @@ static __device__ __noinline__ double hydrogen_neutral_fraction(const MetalDev& 
         if (Rb == Ra) break;
         x = xb - Rb * (xb - xa) / (Rb - Ra);
         x = fmin(fmax(x, fmin(xa, xb)), fmax(xa, xb));
-        metal_sums(m, c, nH, ne, nH * x, nH * (1.0 - x), nem, rin, rout);
+        cas.sums(nH, ne, nH * x, nH * (1.0 - x), nem, rin, rout);
         ++*nsum;
         const double Rx = x * (B + rin + rout) - (A + rin);
         if (fabs(Rx) <= 1.0e-15 * scale) break;
@@ -187,16 +191,17 @@ static __device__ __noinline__ double hydrogen_neutral_fraction(const MetalDev& 
     return x;
 }
 
-// charge_neutrality_ne (ion_balance_mod.f90:235-253) with a cache already
-// prepared at the written temperature.
-static __device__ __noinline__ double charge_neutrality_ne(const MetalDev& m, const MetalCache& c, double nH, double ne_HHe,
-                                                    double xHI, double ne_seed) {
+// charge_neutrality_ne (ion_balance_mod.f90:235-253) with the cascade
+// already prepared at the written temperature.
+template <class Cas>
+static __device__ __noinline__ double charge_neutrality_ne(const Cas& cas, double nH, double ne_HHe, double xHI,
+                                                           double ne_seed) {
     const double nHI = nH * xHI, nHII = nH * (1.0 - xHI);
     double ne = fmax(ne_seed, 1.0e-12 * nH);
     for (int it = 1; it <= 200; ++it) {
         const double ne_old = ne;
         double nem, rin, rout;
-        metal_sums(m, c, nH, ne_old, nHI, nHII, nem, rin, rout);
+        cas.sums(nH, ne_old, nHI, nHII, nem, rin, rout);
         ne = ne_HHe + nem;
         ne = fmax(0.5 * (ne + ne_old), 1.0e-12 * nH);
         if (fabs(ne - ne_old) <= 1.0e-10 * ne) break;
@@ -223,6 +228,20 @@ static __device__ __noinline__ void metal_opacity_fill(const MetalDev& m, const 
         }
     }
 }
+
+// The cascade of one leaf held by one thread: the (leaf, T) rate cache.
+struct SerialCascade {
+    const MetalDev* m;
+    MetalCache c;
+    __device__ void prepare(long long il, double T) { metal_prepare(*m, il, T, c); }
+    __device__ void sums(double nH, double ne, double nHI, double nHII, double& nem, double& rin, double& rout) const {
+        metal_sums(*m, c, nH, ne, nHI, nHII, nem, rin, rout);
+    }
+    template <typename R>
+    __device__ void opacity_fill(long long il, double nH, double ne, double xHI, double colscale) const {
+        metal_opacity_fill<R>(*m, c, il, nH, ne, xHI, colscale);
+    }
+};
 
 // The four metal terms of net_rate (thermal_mod.f90:53-71): line cooling
 // (fits with the n-level suppression), H-impact [C II] 158 um / [O I] 63 um,

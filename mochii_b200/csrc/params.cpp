@@ -137,6 +137,7 @@ extern "C" int mochii_params_default(mochii_params* p) {
     p->lambda_ref = 0.55;
     p->taumax = -999.0;
     p->tauhomo = -999.0;
+    p->solver_warp = 1;
     return MOCHII_OK;
 }
 
@@ -274,6 +275,12 @@ int set_key(mochii_params* p, std::string key, const std::vector<std::string>& v
     if (key == "ion_dust_kext") { copy_str(p->ion_dust_kext, sizeof(p->ion_dust_kext), unquote(v)); return 0; }
     if (key == "data_dir") { copy_str(p->data_dir, sizeof(p->data_dir), unquote(v)); return 0; }
     if (key == "atomic_dir") { copy_str(p->atomic_dir, sizeof(p->atomic_dir), unquote(v)); return 0; }
+    if (key == "cell_layout") {
+        const std::string s = lower(unquote(v));
+        if (s != "warp" && s != "thread") return bad("must be 'warp' or 'thread'");
+        p->solver_warp = s == "warp";
+        return 0;
+    }
     if (key == "thermal_solver") {
         const std::string s = lower(unquote(v));
         if (s != "bisection" && s != "bracketed") return bad("must be 'bisection' or 'bracketed'");
