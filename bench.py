@@ -71,22 +71,26 @@ DRAM_BYTES_PER_SEGMENT = {}
 class Workload:
     """A benchmark configuration: its namelist and how a step is run."""
 
-    def __init__(self, name):
+    def __init__(self, name, grid=None, packets=None):
+        """grid / packets override the workload's grid side and stellar
+        packets per pass (smaller cases for profiling)."""
         from mochii_b200 import configs
         self.name = name
         if name == "hii_metals128":
-            self.grid, self.nphot, self.thermal, self.prep = 128, 10_000_000, True, 8
+            self.grid, self.nphot, self.thermal, self.prep = grid or 128, packets or 10_000_000, True, 8
             self.default_precision = "fp32"
-            self.make = lambda nphot, prec, seed: configs.hii_metals(nphotons=nphot, niter=20, n=128,
+            n = self.grid
+            self.make = lambda nphot, prec, seed: configs.hii_metals(nphotons=nphot, niter=20, n=n,
                                                                       precision=prec, seed=seed)
         elif name == "stromgren64":
-            self.grid, self.nphot, self.thermal, self.prep = 64, 1_000_000, False, 60
+            self.grid, self.nphot, self.thermal, self.prep = grid or 64, packets or 1_000_000, False, 60
             self.default_precision = "fp64"
-            self.make = lambda nphot, prec, seed: configs.stromgren64(nphotons=nphot, n=64, precision=prec, seed=seed)
+            n = self.grid
+            self.make = lambda nphot, prec, seed: configs.stromgren64(nphotons=nphot, n=n, precision=prec, seed=seed)
         elif name == "clumpy_dusty":
             import tempfile
             cases = os.path.join(tempfile.gettempdir(), "mochii_b200_cases")
-            self.grid, self.nphot, self.thermal, self.prep = None, 30_000_000, True, 3
+            self.grid, self.nphot, self.thermal, self.prep = None, packets or 30_000_000, True, 3
             self.default_precision = "fp32"
             self.make = lambda nphot, prec, seed: configs.clumpy_dusty(cases, nphotons=nphot, precision=prec,
                                                                         qmc_seed=seed)
@@ -288,10 +292,12 @@ def main():
                     help="transport arithmetic (default: the workload's)")
     ap.add_argument("--solver", default="bracketed", choices=["bisection", "bracketed"],
                     help="cell solver: the reference's bisection or the bracketed roots")
-    ap.add_argument("--cell-layout", default="warp", choices=["warp", "thread"],
+    ap.add_argument("--cell-layout", default="thread", choices=["warp", "thread"],
                     help="thermal solve with metals: one warp or one thread per leaf")
+    ap.add_argument("--grid", type=int, default=None, help="grid side of a Cartesian workload (default: its own)")
+    ap.add_argument("--packets", type=int, default=None, help="stellar packets per pass (default: the workload's)")
     args = ap.parse_args()
-    wl = Workload(args.workload)
+    wl = Workload(args.workload, args.grid, args.packets)
     prec = args.precision or wl.default_precision
     if args.impl == "reference":
         return run_reference(args, wl)

@@ -135,9 +135,9 @@ typedef struct mochii_params {
     /* grain optics reference wavelength [um] and the dust normalisations
      * (define.f90:211-212,361); taumax / tauhomo > 0 are not built */
     double lambda_ref, taumax, tauhomo;
-    /* thermal solve with metals (not a reference key, 'warp' or 'thread'):
-     * 1 = one warp per leaf, the metal cascade spread over the lanes;
-     * 0 = one thread per leaf */
+    /* thermal solve with metals (not a reference key, 'thread' or 'warp'):
+     * 0 = one thread per leaf (default); 1 = one warp per leaf, the metal
+     * cascade spread over the lanes */
     int solver_warp;
 } mochii_params;
 

@@ -137,7 +137,7 @@ extern "C" int mochii_params_default(mochii_params* p) {
     p->lambda_ref = 0.55;
     p->taumax = -999.0;
     p->tauhomo = -999.0;
-    p->solver_warp = 1;
+    p->solver_warp = 0;
     return MOCHII_OK;
 }
 
