@@ -330,7 +330,7 @@ def main():
         neb.gas_opacity_fill()
 
     # ---- device-timed steps ---------------------------------------------
-    pass_ms, kern_ms, bal_ms, segs, nact, npk = [], [], [], [], [], []
+    pass_ms, kern_ms, bal_ms, segs, nact, npk, bcnt = [], [], [], [], [], [], []
     if dist is not None:
         dist.barrier()
     torch.cuda.synchronize()
@@ -345,6 +345,8 @@ def main():
             pass_ms.append(st.pass_ms)
             kern_ms.append(st.kernel_ms)
             bal_ms.append(neb.last_metrics.kernel_ms)
+            lm = neb.last_metrics
+            bcnt.append((lm.cells_solved, lm.rate_evaluations, lm.metal_sum_calls, lm.fixed_point_passes))
             segs.append(st.direct_segments)
             nact.append(st.metal_active)
             npk.append(st.packets)
@@ -449,6 +451,8 @@ def main():
             "clocks": clk.summary(),
             "gpu_launches": int(sum(launches_per_step(wl, n_ - wl.nphot) for n_ in npk)),
             "breakdown_ms": {"transport": float(np.mean(pass_ms)), "balance": float(np.mean(bal_ms))},
+            "balance_counts_per_step": dict(zip(("cells", "rate_evaluations", "metal_sums", "ne_evaluations"),
+                                                (float(v) for v in np.mean(np.array(bcnt, dtype=float), axis=0)))),
             "wall_s": t_wall,
         }
         print(json.dumps(line), flush=True)

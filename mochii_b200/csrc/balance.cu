@@ -200,12 +200,18 @@ struct CellState {
     double x, h1, h2;
 };
 
+//
+// xg: a guess of x_HI (the previous evaluation's), from which the H root
+// with charge exchange is found (hydrogen_neutral_fraction_warm).
 template <class Cas>
 __device__ __noinline__ double cell_electrons(const Coef& k, double yHe, double gH, double gHe1, double gHe2, double nH,
                                               double ne, bool metals, const Cas& mc, int with_ne, int with_cx,
-                                              int* nsum, CellState& o) {
+                                              int* nsum, CellState& o, double xg) {
+    double nem_x = 0.0;
+    bool have_nem = false;
     if (metals && with_cx) {
-        o.x = hydrogen_neutral_fraction(mc, nH, ne, k.aH * ne, gH + (k.cH + k.aH) * ne, nsum);
+        o.x = hydrogen_neutral_fraction_warm(mc, nH, ne, k.aH * ne, gH + (k.cH + k.aH) * ne, xg, nsum, &nem_x);
+        have_nem = true;
     } else {
         const double denH = gH + (k.cH + k.aH) * ne;
         o.x = denH > 0.0 ? (k.aH * ne) / denH : 1.0;
@@ -217,10 +223,12 @@ __device__ __noinline__ double cell_electrons(const Coef& k, double yHe, double 
     const double h3 = o.h2 * r2;
     double nen = nH * ((1.0 - o.x) + yHe * (o.h2 + 2.0 * h3));
     if (metals && with_ne) {
-        double nem, rin, rout;
-        mc.sums(nH, ne, nH * o.x, nH * (1.0 - o.x), nem, rin, rout);
-        ++*nsum;
-        nen = nen + nem;
+        if (!have_nem) {
+            double rin, rout;
+            mc.sums(nH, ne, nH * o.x, nH * (1.0 - o.x), nem_x, rin, rout);
+            ++*nsum;
+        }
+        nen = nen + nem_x;
     }
     return nen;
 }
@@ -236,16 +244,17 @@ __device__ __noinline__ int solve_cell_fast(const Coef& k, double yHe, double gH
     a = fmin(a, top);
     int nev = 0;
     CellState ea, eb, ec;
-    double fa = cell_electrons(k, yHe, gH, gHe1, gHe2, nH, a, metals, mc, with_ne, with_cx, nsum, ea) - a;
+    double fa = cell_electrons(k, yHe, gH, gHe1, gHe2, nH, a, metals, mc, with_ne, with_cx, nsum, ea, xHI) - a;
     ++nev;
     double b = a, fb = fa;
     eb = ea;
+    ec = ea;   // ec.x: the guess of the next evaluation's H root
     bool done = fabs(fa) <= 2.0e-10 * a;
     if (!done) {   // geometric bracketing toward the root
         double fac = 1.25;
         while (nev < 60) {
             const double c = fa > 0.0 ? fmin(a * fac, top) : fmax(a / fac, floor);
-            const double fc = cell_electrons(k, yHe, gH, gHe1, gHe2, nH, c, metals, mc, with_ne, with_cx, nsum, ec) - c;
+            const double fc = cell_electrons(k, yHe, gH, gHe1, gHe2, nH, c, metals, mc, with_ne, with_cx, nsum, ec, ec.x) - c;
             ++nev;
             b = c; fb = fc; eb = ec;
             if (fc == 0.0 || (fc > 0.0) != (fa > 0.0)) break;
@@ -267,7 +276,7 @@ __device__ __noinline__ int solve_cell_fast(const Coef& k, double yHe, double gH
             double lc = (la * fb - lb * fa) / (fb - fa);
             if (bisect || !(fabs(lc - la) > 0.05 * width && fabs(lc - lb) > 0.05 * width)) lc = 0.5 * (la + lb);
             const double c = exp(lc);
-            const double fc = cell_electrons(k, yHe, gH, gHe1, gHe2, nH, c, metals, mc, with_ne, with_cx, nsum, ec) - c;
+            const double fc = cell_electrons(k, yHe, gH, gHe1, gHe2, nH, c, metals, mc, with_ne, with_cx, nsum, ec, ec.x) - c;
             ++nev;
             b = c;          // the returned point is the last one evaluated
             eb = ec;

@@ -191,6 +191,39 @@ static __device__ __noinline__ double hydrogen_neutral_fraction(const Cas& cas, 
     return x;
 }
 
+// The same root from a warm start xg (the bracketed cell solve): the
+// substitution x <- (A + rin(x)) / (B + rin(x) + rout(x)), whose fixed point
+// is the root of R(x) = x (B + rin + rout) - (A + rin), while |R| falls,
+// stopping when |R| <= 1e-15 scale or the step is below 1e-15; Illinois on
+// [0, 1] when it does not settle in 8 steps.  *nem_x: the metal electrons
+// of the sums at the returned x.
+template <class Cas>
+static __device__ __noinline__ double hydrogen_neutral_fraction_warm(const Cas& cas, double nH, double ne, double A,
+                                                                     double B, double xg, int* nsum, double* nem_x) {
+    double x = fmin(fmax(xg, 0.0), 1.0);
+    double prev = 1.0e300;
+    for (int k = 0; k < 8; ++k) {
+        double nem, rin, rout;
+        cas.sums(nH, ne, nH * x, nH * (1.0 - x), nem, rin, rout);
+        ++*nsum;
+        const double Rx = x * (B + rin + rout) - (A + rin);
+        const double scale = A + B + fabs(A + rin) + fabs(B + rout);
+        const double xn = fmin(fmax((A + rin) / (B + rin + rout), 0.0), 1.0);
+        if (fabs(Rx) <= 1.0e-15 * scale || fabs(xn - x) <= 1.0e-15) {
+            *nem_x = nem;
+            return x;
+        }
+        if (!(fabs(Rx) < prev)) break;   // not contracting: bracket instead
+        prev = fabs(Rx);
+        x = xn;
+    }
+    x = hydrogen_neutral_fraction(cas, nH, ne, A, B, nsum);
+    double rin, rout;
+    cas.sums(nH, ne, nH * x, nH * (1.0 - x), *nem_x, rin, rout);
+    ++*nsum;
+    return x;
+}
+
 // charge_neutrality_ne (ion_balance_mod.f90:235-253) with the cascade
 // already prepared at the written temperature.
 template <class Cas>
