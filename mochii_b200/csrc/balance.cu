@@ -250,45 +250,68 @@ __device__ __noinline__ int solve_cell_fast(const Coef& k, double yHe, double gH
     eb = ea;
     ec = ea;   // ec.x: the guess of the next evaluation's H root
     bool done = fabs(fa) <= 2.0e-10 * a;
-    if (!done) {   // geometric bracketing toward the root
-        double fac = 1.25;
+    auto F = [&](double c, CellState& st) {
+        ++nev;
+        return cell_electrons(k, yHe, gH, gHe1, gHe2, nH, c, metals, mc, with_ne, with_cx, nsum, st, ec.x) - c;
+    };
+    // search from the warm start: the undamped fixed-point step n_e <- F(n_e),
+    // then secant steps in ln n_e while |h| falls and the root stays ahead,
+    // else geometric steps (x4, then squared) toward the root, until h
+    // changes sign; on a clamp with h still of the same sign the damped
+    // iteration would sit there
+    if (!done) {
+        double c = fa > 0.0 ? fmin(a + fa, top) : fmax(a + fa, floor);
+        if (!(c > 0.0)) c = floor;
+        double fac = 4.0;
         while (nev < 60) {
-            const double c = fa > 0.0 ? fmin(a * fac, top) : fmax(a / fac, floor);
-            const double fc = cell_electrons(k, yHe, gH, gHe1, gHe2, nH, c, metals, mc, with_ne, with_cx, nsum, ec, ec.x) - c;
-            ++nev;
+            const double fc = F(c, ec);
             b = c; fb = fc; eb = ec;
-            if (fc == 0.0 || (fc > 0.0) != (fa > 0.0)) break;
-            if (c >= top || c <= floor) {   // the damped iteration would sit on its clamp
+            if (fabs(fc) <= 2.0e-10 * c || fc == 0.0) {
                 done = true;
                 break;
             }
+            if ((fc > 0.0) != (fa > 0.0)) break;            // bracketed by [a, c]
+            if (c >= top || c <= floor) {
+                done = true;
+                break;
+            }
+            const double la = log(a), lc = log(c);
+            double ld = lc - fc * (lc - la) / (fc - fa);     // secant in ln n_e
+            const bool ahead = fc > 0.0 ? ld > lc : ld < lc;
+            const double lim = log(fac);
+            if (!(fabs(fc) < fabs(fa)) || !ahead || !(fabs(ld - lc) <= lim)) ld = fc > 0.0 ? lc + lim : lc - lim;
             a = c; fa = fc; ea = ec;
+            c = fc > 0.0 ? fmin(exp(ld), top) : fmax(exp(ld), floor);
             fac = fac * fac;
         }
-        if (fb == 0.0) done = true;
     }
-    if (!done) {   // safeguarded false position in ln n_e on the bracket [a, b]
+    // Anderson-Bjorck false position in ln n_e on the bracket [a, b]
+    if (!done) {
         double la = log(a), lb = log(b);
-        bool bisect = false;
+        int side = 0;
         for (int it = 0; it < 100 && nev < 160; ++it) {
             const double width = fabs(lb - la);
             if (width <= 1.0e-13) break;
             double lc = (la * fb - lb * fa) / (fb - fa);
-            if (bisect || !(fabs(lc - la) > 0.05 * width && fabs(lc - lb) > 0.05 * width)) lc = 0.5 * (la + lb);
+            if (!(fabs(lc - la) > 1.0e-3 * width && fabs(lc - lb) > 1.0e-3 * width)) lc = 0.5 * (la + lb);
             const double c = exp(lc);
-            const double fc = cell_electrons(k, yHe, gH, gHe1, gHe2, nH, c, metals, mc, with_ne, with_cx, nsum, ec, ec.x) - c;
-            ++nev;
+            const double fc = F(c, ec);
             b = c;          // the returned point is the last one evaluated
             eb = ec;
-            if (fabs(fc) <= 2.0e-10 * c) break;
-            if ((fc > 0.0) == (fa > 0.0)) {
-                la = lc;
-                fa = fc;
-            } else {
-                lb = lc;
-                fb = fc;
+            if (fabs(fc) <= 2.0e-10 * c || fc == 0.0) break;
+            if ((fc > 0.0) == (fb > 0.0)) {   // c replaces the b end
+                if (side == -1) {
+                    const double m = 1.0 - fc / fb;
+                    fa = fa * (m > 0.0 ? m : 0.5);
+                }
+                lb = lc; fb = fc; side = -1;
+            } else {                          // c replaces the a end
+                if (side == +1) {
+                    const double m = 1.0 - fc / fa;
+                    fb = fb * (m > 0.0 ? m : 0.5);
+                }
+                la = lc; fa = fc; side = +1;
             }
-            bisect = fabs(lb - la) > 0.5 * width;
         }
     }
     ne = b;
