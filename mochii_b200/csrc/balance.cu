@@ -858,6 +858,321 @@ __device__ double thermal_bracketed(const ThArgs& a, long long il, double nH, do
     return t;
 }
 
+// ---- the bracketed solves in warp lockstep -----------------------------------
+// With one leaf per thread, the leaves of a warp need different numbers of
+// root-finding steps, and a warp whose lanes sit in different loops runs the
+// expensive evaluations (rate cache, cascade sums, cooling) one lane group
+// at a time, reading the per-thread caches uncoalesced.  Here every root
+// search is a loop whose trip count is uniform over the warp (__any_sync on
+// the lanes still searching): each trip, every searching lane makes one
+// evaluation at its own point, the evaluations of all lanes at the same
+// program point, and then updates its own search state.  Each lane's
+// sequence of points and results is that of the bracketed solves above
+// (hydrogen_neutral_fraction_warm, solve_cell_fast, thermal_bracketed).
+// Every function here is entered by all 32 lanes; `act` marks the lanes
+// whose leaf takes part.
+
+// The H root with charge exchange (hydrogen_neutral_fraction_warm, falling
+// back to hydrogen_neutral_fraction's Illinois iteration).
+__device__ __noinline__ double h_root_ls(const SerialCascade& mc, bool act, double nH, double ne, double A, double B,
+                                         double xg, int* nsum, double* nem_x) {
+    // ph: 0 substitution, 1-2 Illinois end points x = 0, 1, 3 Illinois steps,
+    // 4 the sums at the Illinois root, 5 done
+    int ph = act ? 0 : 5, k = 0, kk = 0;
+    double x = fmin(fmax(xg, 0.0), 1.0), prev = 1.0e300;
+    double xa = 0.0, xb = 1.0, Ra = 0.0, Rb = 0.0, scale = 0.0, nem = 0.0;
+    while (__any_sync(kFull, ph != 5)) {
+        if (ph == 5) continue;
+        const double xe = ph == 1 ? 0.0 : ph == 2 ? 1.0 : x;
+        double em, rin, rout;
+        mc.sums(nH, ne, nH * xe, nH * (1.0 - xe), em, rin, rout);
+        ++*nsum;
+        if (ph == 0) {
+            const double Rx = x * (B + rin + rout) - (A + rin);
+            const double sc = A + B + fabs(A + rin) + fabs(B + rout);
+            const double xn = fmin(fmax((A + rin) / (B + rin + rout), 0.0), 1.0);
+            if (fabs(Rx) <= 1.0e-15 * sc || fabs(xn - x) <= 1.0e-15) {
+                nem = em;
+                ph = 5;
+            } else if (!(fabs(Rx) < prev) || ++k >= 8) {
+                ph = 1;
+            } else {
+                prev = fabs(Rx);
+                x = xn;
+            }
+        } else if (ph == 1) {
+            Ra = -(A + rin);
+            ph = 2;
+        } else if (ph == 2) {
+            Rb = B + rout;
+            scale = A + B + fabs(Ra) + fabs(Rb);
+            x = xb;
+            kk = 0;
+            ph = 3;
+        } else if (ph == 3) {
+            const double Rx = x * (B + rin + rout) - (A + rin);
+            if (fabs(Rx) <= 1.0e-15 * scale || fabs(xb - xa) <= 1.0e-15) {
+                ph = 4;
+            } else {
+                if (Rx * Rb < 0.0) {
+                    xa = xb;
+                    Ra = Rb;
+                } else {
+                    Ra = 0.5 * Ra;
+                }
+                xb = x;
+                Rb = Rx;
+            }
+        } else {   // ph == 4
+            nem = em;
+            ph = 5;
+        }
+        if (ph == 3) {   // the next Illinois point (hydrogen_neutral_fraction's loop head)
+            if (++kk > 80 || Rb == Ra) {
+                ph = 4;
+            } else {
+                x = xb - Rb * (xb - xa) / (Rb - Ra);
+                x = fmin(fmax(x, fmin(xa, xb)), fmax(xa, xb));
+            }
+        }
+    }
+    *nem_x = nem;
+    return x;
+}
+
+__device__ __forceinline__ double cell_electrons_ls(const Coef& k, double yHe, double gH, double gHe1, double gHe2,
+                                                    double nH, double ne, bool act, const SerialCascade& mc,
+                                                    int with_ne, int with_cx, int* nsum, CellState& o, double xg) {
+    double nem_x = 0.0;
+    if (with_cx) {
+        o.x = h_root_ls(mc, act, nH, ne, k.aH * ne, gH + (k.cH + k.aH) * ne, xg, nsum, &nem_x);
+    } else if (act) {
+        const double denH = gH + (k.cH + k.aH) * ne;
+        o.x = denH > 0.0 ? (k.aH * ne) / denH : 1.0;
+    }
+    if (!act) return 0.0;
+    const double r1 = fmin((gHe1 + k.cHe1 * ne) / (k.aHe2 * ne), 1.0e150);
+    const double r2 = fmin((gHe2 + k.cHe2 * ne) / (k.aHe3 * ne), 1.0e150);
+    o.h1 = 1.0 / (1.0 + r1 + r1 * r2);
+    o.h2 = o.h1 * r1;
+    const double h3 = o.h2 * r2;
+    double nen = nH * ((1.0 - o.x) + yHe * (o.h2 + 2.0 * h3));
+    if (with_ne) {
+        if (!with_cx) {
+            double rin, rout;
+            mc.sums(nH, ne, nH * o.x, nH * (1.0 - o.x), nem_x, rin, rout);
+            ++*nsum;
+        }
+        nen = nen + nem_x;
+    }
+    return nen;
+}
+
+// solve_cell_fast with metals as a per-lane state machine.
+__device__ __noinline__ int solve_cell_ls(const Coef& k, double yHe, double gH, double gHe1, double gHe2, double nH,
+                                          double& xHI, double& xHeI, double& xHeII, double& ne, bool act,
+                                          const SerialCascade& mc, int with_ne, int with_cx, int* nsum, double nemax) {
+    const double floor = 1.0e-12 * nH, top = nemax * nH;
+    double a = 0.0, fa = 0.0, b = 0.0, fb = 0.0, c = 0.0, fac = 4.0, la = 0.0, lb = 0.0;
+    int ph = act ? 0 : 9, nev = 0, side = 0, it = 0;   // 0 first point, 1 search, 2 false position, 9 done
+    CellState ea = {xHI, xHeI, xHeII}, eb = ea, ec = ea;
+    if (act) {
+        const double xHeIII = fmax(0.0, 1.0 - xHeI - xHeII);
+        a = ne > floor ? ne : fmax(nH * ((1.0 - xHI) + yHe * (xHeII + 2.0 * xHeIII)), floor);
+        a = fmin(a, top);
+        c = a;
+    }
+    while (__any_sync(kFull, ph != 9)) {
+        const bool ev = ph != 9;
+        const double fc = cell_electrons_ls(k, yHe, gH, gHe1, gHe2, nH, c, ev, mc, with_ne, with_cx, nsum, ec, ec.x) - c;
+        if (!ev) continue;
+        ++nev;
+        bool to_fp = false;
+        if (ph == 0) {
+            fa = fc; ea = ec; b = a; fb = fa; eb = ea;
+            if (fabs(fa) <= 2.0e-10 * a) {
+                ph = 9;
+            } else {
+                c = fa > 0.0 ? fmin(a + fa, top) : fmax(a + fa, floor);
+                if (!(c > 0.0)) c = floor;
+                ph = 1;
+            }
+        } else if (ph == 1) {
+            b = c; fb = fc; eb = ec;
+            if (fabs(fc) <= 2.0e-10 * c || fc == 0.0) {
+                ph = 9;
+            } else if ((fc > 0.0) != (fa > 0.0)) {
+                to_fp = true;
+            } else if (c >= top || c <= floor) {
+                ph = 9;
+            } else {
+                const double lA = log(a), lC = log(c);
+                double ld = lC - fc * (lC - lA) / (fc - fa);
+                const bool ahead = fc > 0.0 ? ld > lC : ld < lC;
+                const double lim = log(fac);
+                if (!(fabs(fc) < fabs(fa)) || !ahead || !(fabs(ld - lC) <= lim)) ld = fc > 0.0 ? lC + lim : lC - lim;
+                a = c; fa = fc; ea = ec;
+                c = fc > 0.0 ? fmin(exp(ld), top) : fmax(exp(ld), floor);
+                fac = fac * fac;
+                if (nev >= 60) to_fp = true;
+            }
+        } else {   // ph == 2: Anderson-Bjorck step at c
+            b = c;
+            eb = ec;
+            ++it;
+            const double lc = log(c);
+            if (fabs(fc) <= 2.0e-10 * c || fc == 0.0) {
+                ph = 9;
+            } else if ((fc > 0.0) == (fb > 0.0)) {
+                if (side == -1) {
+                    const double m = 1.0 - fc / fb;
+                    fa = fa * (m > 0.0 ? m : 0.5);
+                }
+                lb = lc; fb = fc; side = -1;
+            } else {
+                if (side == +1) {
+                    const double m = 1.0 - fc / fa;
+                    fb = fb * (m > 0.0 ? m : 0.5);
+                }
+                la = lc; fa = fc; side = +1;
+            }
+        }
+        if (to_fp) {
+            la = log(a);
+            lb = log(b);
+            side = 0;
+            it = 0;
+            ph = 2;
+        }
+        if (ph == 2) {   // the next false-position point, or the end of the search
+            const double width = fabs(lb - la);
+            if (width <= 1.0e-13 || it >= 100 || nev >= 160) {
+                ph = 9;
+            } else {
+                double lc = (la * fb - lb * fa) / (fb - fa);
+                if (!(fabs(lc - la) > 1.0e-3 * width && fabs(lc - lb) > 1.0e-3 * width)) lc = 0.5 * (la + lb);
+                c = exp(lc);
+            }
+        }
+    }
+    if (act) {
+        ne = b;
+        xHI = eb.x;
+        xHeI = eb.h1;
+        xHeII = eb.h2;
+    }
+    return nev;
+}
+
+__device__ __noinline__ double net_rate_ls(const ThArgs& a, long long il, bool act, double T, double nH, double& xHI,
+                                           double& xHeI, double& xHeII, double& ne, int* passes, SerialCascade& mc,
+                                           int* nsum) {
+    const BalArgs& b = a.b;
+    const long long n = b.nleaf;
+    Coef k = {};
+    double g0 = 0.0, g1 = 0.0, g2 = 0.0;
+    if (act) {
+        k = coef_at_call(b.rs, b.caseA, T);
+        mc.prepare(il, T);
+        g0 = b.rates[il]; g1 = b.rates[n + il]; g2 = b.rates[2 * n + il];
+    }
+    *passes += solve_cell_ls(k, b.yHe, g0, g1, g2, nH, xHI, xHeI, xHeII, ne, act, mc, b.metal_ne, b.two_way, nsum,
+                             b.nemax);
+    if (!act) return 0.0;
+    const double heat = nH * (xHI * b.rates[3 * n + il] + b.yHe * (xHeI * b.rates[4 * n + il] + xHeII * b.rates[5 * n + il]));
+    double net = heat - cooling_total(a.td, b.rs, b.caseA, b.yHe, T, nH, ne, xHI, xHeI, xHeII);
+    const MetalThermalTerms mt = thermal_terms(a.td, mc, il, T, nH, ne, nH * xHI, nH * (1.0 - xHI));
+    net = net - mt.cool;
+    net = net - mt.cool_H;
+    if (b.metal_ff) net = net - mt.freefree;
+    if (b.metal_heat) net = net + mt.heat;
+    return net;
+}
+
+// thermal_bracketed as a per-lane state machine.
+__device__ __noinline__ double thermal_ls(const ThArgs& a, long long il, bool act, double nH, double& xHI,
+                                          double& xHeI, double& xHeII, double& ne, int* passes, SerialCascade& mc,
+                                          int* nsum, int* nev, double Tw) {
+    const double lo_lim = a.te_min, hi_lim = a.te_max;
+    // ph: 0 warm start, 1 bracketing, 2 false position, 9 done
+    int ph = act ? 0 : 9, s = 0, it = 0;
+    double ta = fmin(fmax(Tw, lo_lim), hi_lim), fa = 0.0, tb = ta, fb = 0.0, fac = 1.05, la = 0.0, lb = 0.0;
+    double t = ta, tr = ta;
+    bool bisect = false;
+    while (__any_sync(kFull, ph != 9)) {
+        const bool ev = ph != 9;
+        const double f = net_rate_ls(a, il, ev, t, nH, xHI, xHeI, xHeII, ne, passes, mc, nsum);
+        if (!ev) continue;
+        ++*nev;
+        bool to_fp = false;
+        if (ph == 0) {
+            fa = f;
+            if (fa == 0.0 || (ta <= lo_lim && fa < 0.0) || (ta >= hi_lim && fa > 0.0)) {
+                tr = ta;
+                ph = 9;
+            } else {
+                ph = 1;
+                s = 0;
+            }
+        } else if (ph == 1) {
+            fb = f;
+            ++s;
+            if (fb == 0.0) {
+                tr = tb;
+                ph = 9;
+            } else if ((fb > 0.0) != (fa > 0.0)) {
+                to_fp = true;
+            } else if (tb >= hi_lim || tb <= lo_lim) {
+                tr = tb;
+                ph = 9;
+            } else {
+                ta = tb;
+                fa = fb;
+                fac = fac * fac;
+                if (s >= 40) to_fp = true;
+            }
+        } else {   // ph == 2
+            const double fc = f, lc = log(t), width = fabs(lb - la);
+            ++it;
+            tr = t;
+            if (fc == 0.0) {
+                ph = 9;
+            } else {
+                if ((fc > 0.0) == (fa > 0.0)) {
+                    la = lc;
+                    fa = fc;
+                } else {
+                    lb = lc;
+                    fb = fc;
+                }
+                bisect = fabs(lb - la) > 0.5 * width;
+            }
+        }
+        if (to_fp) {
+            la = log(ta);
+            lb = log(tb);
+            tr = tb;
+            bisect = false;
+            it = 0;
+            ph = 2;
+        }
+        if (ph == 1) {
+            tb = fa > 0.0 ? fmin(ta * fac, hi_lim) : fmax(ta / fac, lo_lim);
+            t = tb;
+        } else if (ph == 2) {
+            const double width = fabs(lb - la);
+            if (width < 1.0e-5 || it >= 80) {
+                ph = 9;
+            } else {
+                double lc = (la * fb - lb * fa) / (fb - fa);
+                if (bisect || !(fabs(lc - la) > 0.05 * width && fabs(lc - lb) > 0.05 * width)) lc = 0.5 * (la + lb);
+                t = exp(lc);
+            }
+        }
+    }
+    return tr;
+}
+
 // gas_thermal_update (thermal_mod.f90:124-249): bisection on log T in
 // [te_min, te_max] (at most 60 halvings, stop at thi/tlo - 1 < 1e-5), the
 // ionisation re-solved at every trial temperature.
@@ -961,6 +1276,111 @@ __global__ void __launch_bounds__(kBThreads) k_thermal(const ThArgs a) {
     if ((t & 31) == 0) {
         if (solved) atomicAdd(b.counters + 0, solved);
         if (caps) atomicAdd(b.counters + 1, caps);
+        if (tpass) atomicAdd(b.counters + 2, tpass);
+        if (tsums) atomicAdd(b.counters + 3, tsums);
+        if (nevals) atomicAdd(b.counters + 4, nevals);
+    }
+}
+
+// charge_neutrality_ne in warp lockstep.
+__device__ __noinline__ double neutrality_ls(const SerialCascade& mc, bool act, double nH, double ne_HHe, double xHI,
+                                             double ne_seed) {
+    const double nHI = nH * xHI, nHII = nH * (1.0 - xHI);
+    double ne = fmax(ne_seed, 1.0e-12 * nH);
+    int it = 0;
+    bool run = act;
+    while (__any_sync(kFull, run)) {
+        if (!run) continue;
+        const double ne_old = ne;
+        double nem, rin, rout;
+        mc.sums(nH, ne_old, nHI, nHII, nem, rin, rout);
+        ne = ne_HHe + nem;
+        ne = fmax(0.5 * (ne + ne_old), 1.0e-12 * nH);
+        if (fabs(ne - ne_old) <= 1.0e-10 * ne || ++it >= 200) run = false;
+    }
+    return ne;
+}
+
+// gas_thermal_update with metals and the bracketed solve, one leaf per
+// thread in warp lockstep (thermal_ls).  The leaf loop steps by whole warps
+// so that every lane of a warp makes the same number of trips.
+__global__ void __launch_bounds__(kBThreads) k_thermal_ls(const ThArgs a) {
+    __shared__ double sh[6][kBThreads];
+    const BalArgs& b = a.b;
+    double mdx = 0.0, mdt = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0, s4 = 0.0;
+    unsigned long long solved = 0, tpass = 0, tsums = 0, nevals = 0;
+    const int lane = threadIdx.x & 31;
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long base = (long long)blockIdx.x * blockDim.x + (threadIdx.x - lane); base < b.nleaf; base += stride) {
+        const long long il0 = base + lane;
+        const bool valid = il0 < b.nleaf;
+        const long long il = valid ? il0 : b.nleaf - 1;
+        const double nH = b.nH[il];
+        const double x0 = b.xHI[il], h10 = b.xHeI[il], h20 = b.xHeII[il], T0 = b.Te[il];
+        const bool act = valid && nH > 0.0;
+        if (valid && !act) {
+            b.ne[il] = 0.0;
+            write_columns(b.col, il, b.nabs, b.fp32, nH, b.yHe, x0, h10, h20, b.colscale,
+                          b.rhokap ? b.rhokap[il] : 0.0);
+        }
+        double xHI = x0, xHeI = h10, xHeII = h20, ne = b.ne[il];
+        int passes = 0, nsum = 0, nev = 0;
+        SerialCascade mc;
+        mc.m = &b.m;
+        const double te = thermal_ls(a, il, act, nH, xHI, xHeI, xHeII, ne, &passes, mc, &nsum, &nev,
+                                     a.Twarm ? a.Twarm[il] : T0);
+        const double w = b.relax;
+        const double xn = (1.0 - w) * x0 + w * xHI;
+        const double h1n = (1.0 - w) * h10 + w * xHeI;
+        const double h2n = (1.0 - w) * h20 + w * xHeII;
+        const double h3n = fmax(0.0, 1.0 - h1n - h2n);
+        double nen = nH * ((1.0 - xn) + b.yHe * (h2n + 2.0 * h3n));
+        // written state at te (thermal_mod.f90:191-203); the cache is at te
+        // from the final net_rate
+        if (b.metal_ne) nen = neutrality_ls(mc, act, nH, nen, xn, ne);
+        if (!act) continue;
+        if (b.fp32) mc.opacity_fill<float>(il, nH, nen, xn, b.colscale);
+        else mc.opacity_fill<double>(il, nH, nen, xn, b.colscale);
+        ++solved;
+        tpass += (unsigned long long)passes;
+        tsums += (unsigned long long)nsum;
+        nevals += (unsigned long long)nev;
+        b.xHI[il] = xn;
+        b.xHeI[il] = h1n;
+        b.xHeII[il] = h2n;
+        b.ne[il] = nen;
+        b.Te[il] = te;
+        write_columns(b.col, il, b.nabs, b.fp32, nH, b.yHe, xn, h1n, h2n, b.colscale, b.rhokap ? b.rhokap[il] : 0.0);
+        const double dx = fabs(xn - x0);
+        mdx = fmax(mdx, dx);
+        mdt = fmax(mdt, fabs(te - T0) / T0);
+        const double vol = leaf_vol(b, il);
+        s1 = s1 + vol * dx;
+        s2 = s2 + vol * (1.0 - xn);
+        s3 = s3 + vol * nen * fabs(te - T0);
+        s4 = s4 + vol * nen * te;
+    }
+    const int t = threadIdx.x;
+    sh[0][t] = mdx; sh[1][t] = mdt; sh[2][t] = s1; sh[3][t] = s2; sh[4][t] = s3; sh[5][t] = s4;
+    __syncthreads();
+    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+        if (t < s) {
+            sh[0][t] = fmax(sh[0][t], sh[0][t + s]);
+            sh[1][t] = fmax(sh[1][t], sh[1][t + s]);
+            for (int k = 2; k < 6; ++k) sh[k][t] = sh[k][t] + sh[k][t + s];
+        }
+        __syncthreads();
+    }
+    if (t == 0)
+        for (int k = 0; k < 6; ++k) b.partial[6 * blockIdx.x + k] = sh[k][0];
+    for (int o = 16; o > 0; o >>= 1) {
+        solved += __shfl_down_sync(kFull, solved, o);
+        tpass += __shfl_down_sync(kFull, tpass, o);
+        tsums += __shfl_down_sync(kFull, tsums, o);
+        nevals += __shfl_down_sync(kFull, nevals, o);
+    }
+    if ((t & 31) == 0) {
+        if (solved) atomicAdd(b.counters + 0, solved);
         if (tpass) atomicAdd(b.counters + 2, tpass);
         if (tsums) atomicAdd(b.counters + 3, tsums);
         if (nevals) atomicAdd(b.counters + 4, nevals);
@@ -1184,6 +1604,7 @@ cudaError_t launch_thermal(mochii_ctx* c) {
     a.te_max = c->par.te_max;
     a.Twarm = c->twarm_set ? c->twarm : nullptr;
     if (c->metal.ntr > 0 && c->par.solver_warp) k_thermal_warp<<<c->bw.blocks, kWThreads, 0, c->stream>>>(a);
+    else if (c->metal.ntr > 0 && c->par.solver_bracketed) k_thermal_ls<<<c->bw.blocks, kBThreads, 0, c->stream>>>(a);
     else k_thermal<<<c->bw.blocks, kBThreads, 0, c->stream>>>(a);
     return cudaGetLastError();
 }
