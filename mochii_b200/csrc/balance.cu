@@ -8,6 +8,7 @@
 // (gas_opacity_fill, gas_opacity_mod.f90:299, fused here).  Convergence
 // measures are reduced per block in a fixed order and summed on the host,
 // so the metrics are deterministic.
+#include <cub/cub.cuh>
 #include <cuda_runtime.h>
 
 #include "ctx.h"
@@ -420,6 +421,8 @@ struct ThArgs {
     ThermalDev td;
     double te_min, te_max;
     const double* Twarm;   // bracketed solve: warm-start T_e per leaf (nullptr: the current T_e)
+    const int* order;      // lockstep solve: the order to visit leaves in (nullptr: leaf order)
+    unsigned* work;        // lockstep solve: cascade sums per leaf, written for the next update's order
 };
 
 // gbar_ff (cooling_mod.f90:223-234): linear in log10 T on the 41-node table.
@@ -1282,6 +1285,10 @@ __global__ void __launch_bounds__(kBThreads) k_thermal(const ThArgs a) {
     }
 }
 
+__global__ void k_iota(int* v, int n) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) v[i] = i;
+}
+
 // charge_neutrality_ne in warp lockstep.
 __device__ __noinline__ double neutrality_ls(const SerialCascade& mc, bool act, double nH, double ne_HHe, double xHI,
                                              double ne_seed) {
@@ -1312,9 +1319,10 @@ __global__ void __launch_bounds__(kBThreads) k_thermal_ls(const ThArgs a) {
     const int lane = threadIdx.x & 31;
     const long long stride = (long long)gridDim.x * blockDim.x;
     for (long long base = (long long)blockIdx.x * blockDim.x + (threadIdx.x - lane); base < b.nleaf; base += stride) {
-        const long long il0 = base + lane;
-        const bool valid = il0 < b.nleaf;
-        const long long il = valid ? il0 : b.nleaf - 1;
+        const long long i0 = base + lane;
+        const bool valid = i0 < b.nleaf;
+        const long long ip = valid ? i0 : b.nleaf - 1;
+        const long long il = a.order ? (long long)a.order[ip] : ip;
         const double nH = b.nH[il];
         const double x0 = b.xHI[il], h10 = b.xHeI[il], h20 = b.xHeII[il], T0 = b.Te[il];
         const bool act = valid && nH > 0.0;
@@ -1322,6 +1330,7 @@ __global__ void __launch_bounds__(kBThreads) k_thermal_ls(const ThArgs a) {
             b.ne[il] = 0.0;
             write_columns(b.col, il, b.nabs, b.fp32, nH, b.yHe, x0, h10, h20, b.colscale,
                           b.rhokap ? b.rhokap[il] : 0.0);
+            if (a.work) a.work[il] = 0u;
         }
         double xHI = x0, xHeI = h10, xHeII = h20, ne = b.ne[il];
         int passes = 0, nsum = 0, nev = 0;
@@ -1345,6 +1354,7 @@ __global__ void __launch_bounds__(kBThreads) k_thermal_ls(const ThArgs a) {
         tpass += (unsigned long long)passes;
         tsums += (unsigned long long)nsum;
         nevals += (unsigned long long)nev;
+        if (a.work) a.work[il] = (unsigned)min(nsum, 65535);
         b.xHI[il] = xn;
         b.xHeI[il] = h1n;
         b.xHeII[il] = h2n;
@@ -1603,9 +1613,36 @@ cudaError_t launch_thermal(mochii_ctx* c) {
     a.te_min = c->par.te_min;
     a.te_max = c->par.te_max;
     a.Twarm = c->twarm_set ? c->twarm : nullptr;
-    if (c->metal.ntr > 0 && c->par.solver_warp) k_thermal_warp<<<c->bw.blocks, kWThreads, 0, c->stream>>>(a);
-    else if (c->metal.ntr > 0 && c->par.solver_bracketed) k_thermal_ls<<<c->bw.blocks, kBThreads, 0, c->stream>>>(a);
-    else k_thermal<<<c->bw.blocks, kBThreads, 0, c->stream>>>(a);
+    a.order = nullptr;
+    a.work = nullptr;
+    if (c->metal.ntr > 0 && c->par.solver_warp) {
+        k_thermal_warp<<<c->bw.blocks, kWThreads, 0, c->stream>>>(a);
+    } else if (c->metal.ntr > 0 && c->par.solver_bracketed) {
+        BalanceWork& w = c->bw;
+        const int n = (int)c->grid.nleaf;
+        cudaError_t e;
+        if (!w.work) {
+            if ((e = cudaMalloc(&w.work, (size_t)n * 4)) != cudaSuccess) return e;
+            if ((e = cudaMalloc(&w.work_sorted, (size_t)n * 4)) != cudaSuccess) return e;
+            if ((e = cudaMalloc(&w.iota, (size_t)n * 4)) != cudaSuccess) return e;
+            if ((e = cudaMalloc(&w.order, (size_t)n * 4)) != cudaSuccess) return e;
+            cub::DeviceRadixSort::SortPairs(nullptr, w.sort_bytes, w.work, w.work_sorted, w.iota, w.order, n, 0, 16);
+            if ((e = cudaMalloc(&w.sort_tmp, w.sort_bytes)) != cudaSuccess) return e;
+            k_iota<<<nblocks(n, 256, 148 * 16), 256, 0, c->stream>>>(w.iota, n);
+            w.have_work = false;
+        }
+        if (w.have_work) {
+            e = cub::DeviceRadixSort::SortPairs(w.sort_tmp, w.sort_bytes, w.work, w.work_sorted, w.iota, w.order, n, 0,
+                                                16, c->stream);
+            if (e != cudaSuccess) return e;
+            a.order = w.order;
+        }
+        a.work = w.work;
+        k_thermal_ls<<<c->bw.blocks, kBThreads, 0, c->stream>>>(a);
+        w.have_work = true;
+    } else {
+        k_thermal<<<c->bw.blocks, kBThreads, 0, c->stream>>>(a);
+    }
     return cudaGetLastError();
 }
 

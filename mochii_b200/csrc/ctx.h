@@ -76,6 +76,15 @@ struct BalanceWork {
     double* partial = nullptr;   // per block: max_dx, max_dte, sum_dxv, sum_xv, sum_dtv, sum_tv
     unsigned long long* counters = nullptr;
     int blocks = 0;
+    // the lockstep thermal solve visits leaves sorted by the cascade sums
+    // each needed in the previous update, so a warp's leaves need similar work
+    unsigned* work = nullptr;         // per leaf: cascade sums of its last solve (clamped to 16 bits)
+    unsigned* work_sorted = nullptr;
+    int* iota = nullptr;              // 0 .. nleaf-1
+    int* order = nullptr;             // leaves by ascending work
+    void* sort_tmp = nullptr;
+    size_t sort_bytes = 0;
+    bool have_work = false;
 };
 
 }  // namespace mochii
