@@ -135,9 +135,11 @@ typedef struct mochii_params {
     /* grain optics reference wavelength [um] and the dust normalisations
      * (define.f90:211-212,361); taumax / tauhomo > 0 are not built */
     double lambda_ref, taumax, tauhomo;
-    /* thermal solve with metals (not a reference key, 'thread' or 'warp'):
-     * 0 = one thread per leaf (default); 1 = one warp per leaf, the metal
-     * cascade spread over the lanes */
+    /* thermal solve with metals (not a reference key, par%cell_layout):
+     * 0 'thread' = one thread per leaf, each lane's whole bracketed solve a
+     * state machine served by warp-wide evaluations (default); 1 'warp' = one
+     * warp per leaf, the metal cascade spread over the lanes; 2 'lockstep' =
+     * one thread per leaf, nested warp-uniform loops */
     int solver_warp;
 } mochii_params;
 

@@ -77,7 +77,7 @@ void release(mochii_ctx* c) {
     void* ptrs[] = {c->nH, c->xHI, c->xHeI, c->xHeII, c->ne, c->Te, c->col, c->tally, c->jt, c->rates,
                     c->tab.tab_e, c->tab.tab_f, c->tab.tab_c, c->tab.tab_off, c->tab.comp, c->tab.eedge,
                     c->tab.qmc, c->tw.ledger, c->tw.counters, c->bw.partial, c->bw.counters,
-                    c->bw.work, c->bw.work_sorted, c->bw.iota, c->bw.order, c->bw.sort_tmp,
+                    c->bw.work, c->bw.work_sorted, c->bw.iota, c->bw.order, c->bw.sort_tmp, c->bw.next,
                     c->rec.tm, c->rec.td, c->rec.cell, c->rec.bits, c->rec.sig, c->rec.coef,
                     c->th.gff, c->th.lamref, c->th.Ssup, c->th.tinv,
                     c->dif.ch, c->dif.tot, c->dif.scan_tmp, c->dif.tables,

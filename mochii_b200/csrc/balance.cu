@@ -1397,6 +1397,509 @@ __global__ void __launch_bounds__(kBThreads) k_thermal_ls(const ThArgs a) {
     }
 }
 
+// ---- the bracketed thermal solve as one flat per-lane state machine ---------
+// The nested lockstep loops above still make a warp wait, at every level,
+// for its slowest lane (the T steps, the n_e steps within a T step, the H
+// root within an n_e step).  Here each lane runs its leaf's whole solve as
+// one state machine (LeafFlow) that stops only to ask for an expensive
+// evaluation -- the rate cache at a new T (kReqPrepare), one cascade sum
+// (kReqSums), or the net heating at the solved state (kReqFinish) -- and the
+// warp serves each kind of request for all lanes that ask for it, once per
+// trip.  A lane whose leaf is done takes the next leaf of the (work-sorted)
+// order from a global counter.  Each lane's sequence of points and results
+// is that of thermal_bracketed / solve_cell_fast /
+// hydrogen_neutral_fraction_warm / charge_neutrality_ne.
+enum : int { kReqNone = 0, kReqPrepare = 1, kReqSums = 2, kReqFinish = 3 };
+
+struct LeafFlow {
+    const ThArgs* A;
+    int req = kReqNone;
+    bool live = false;
+    // the leaf
+    long long pos = 0, il = 0;
+    double nH = 0, x0 = 0, h10 = 0, h20 = 0, T0 = 0;
+    double xHI = 0, xHeI = 0, xHeII = 0, ne = 0;
+    int passes = 0, nsum = 0, nev = 0;
+    // request arguments
+    double q_T = 0, q_ne = 0, q_x = 0;
+    // T level (thermal_bracketed)
+    int tph = 0, ts = 0, tit = 0;
+    double ta = 0, tfa = 0, tb = 0, tfb = 0, tfac = 1.05, tla = 0, tlb = 0, t = 0, tr = 0;
+    bool bisect = false;
+    // net_rate level
+    Coef k = {};
+    double g0 = 0, g1 = 0, g2 = 0;
+    // n_e level (solve_cell_fast)
+    int eph = 0, enev = 0, eside = 0, eit = 0;
+    double ea = 0, efa = 0, eb = 0, efb = 0, ec = 0, efac = 4.0, ela = 0, elb = 0;
+    CellState Sa = {}, Sb = {}, Sc = {};
+    // F level (cell_electrons at ec)
+    int fph = 0;
+    double fnem = 0;
+    // H root level
+    int hph = 0, hk = 0, hkk = 0;
+    double hx = 0, hprev = 0, hxa = 0, hxb = 0, hRa = 0, hRb = 0, hscale = 0, hA = 0, hB = 0;
+    // leaf end: n_e closure of the written state
+    int nit = 0;
+    double te = 0, xn = 0, h1n = 0, h2n = 0, nen_hhe = 0, nen = 0;
+    bool in_neu = false;
+
+    __device__ void start_leaf(long long p, long long leaf) {
+        const BalArgs& b = A->b;
+        pos = p;
+        il = leaf;
+        nH = b.nH[il];
+        x0 = b.xHI[il]; h10 = b.xHeI[il]; h20 = b.xHeII[il]; T0 = b.Te[il];
+        xHI = x0; xHeI = h10; xHeII = h20; ne = b.ne[il];
+        passes = nsum = nev = 0;
+        in_neu = false;
+        live = true;
+        // thermal_bracketed: the warm start
+        const double Tw = A->Twarm ? A->Twarm[il] : T0;
+        ta = fmin(fmax(Tw, A->te_min), A->te_max);
+        tph = 0;
+        t = ta;
+        tr = ta;
+        start_net(t);
+    }
+    __device__ void start_net(double T) {
+        q_T = T;
+        req = kReqPrepare;
+    }
+    // after the rate cache is at q_T (the warp ran prepare)
+    __device__ void on_prepare() {
+        const BalArgs& b = A->b;
+        const long long n = b.nleaf;
+        k = coef_at_call(b.rs, b.caseA, q_T);
+        g0 = b.rates[il]; g1 = b.rates[n + il]; g2 = b.rates[2 * n + il];
+        // solve_cell_fast: the first point
+        const double floor = 1.0e-12 * nH, top = b.nemax * nH;
+        const double xHeIII = fmax(0.0, 1.0 - xHeI - xHeII);
+        ea = ne > floor ? ne : fmax(nH * ((1.0 - xHI) + b.yHe * (xHeII + 2.0 * xHeIII)), floor);
+        ea = fmin(ea, top);
+        enev = 0;
+        efac = 4.0;
+        Sc = {xHI, xHeI, xHeII};
+        eph = 0;
+        start_F(ea);
+    }
+    __device__ void start_F(double c) {
+        ec = c;
+        if (A->b.two_way) {
+            hA = k.aH * c;
+            hB = g0 + (k.cH + k.aH) * c;
+            hx = fmin(fmax(Sc.x, 0.0), 1.0);
+            hprev = 1.0e300;
+            hk = 0;
+            hph = 0;
+            fph = 0;
+            ask_sums(c, hx);
+        } else {
+            const double denH = g0 + (k.cH + k.aH) * c;
+            Sc.x = denH > 0.0 ? (k.aH * c) / denH : 1.0;
+            after_x(0.0, false);
+        }
+    }
+    __device__ void ask_sums(double c, double x) {
+        q_ne = c;
+        q_x = x;
+        req = kReqSums;
+    }
+    __device__ void on_sums(double em, double rin, double rout) {
+        if (in_neu) { on_neu(em); return; }   // the closure's sums are not counted (as charge_neutrality_ne)
+        ++nsum;
+        if (fph == 1) { after_nem(em); return; }
+        // H root (hydrogen_neutral_fraction_warm)
+        if (hph == 0) {
+            const double Rx = hx * (hB + rin + rout) - (hA + rin);
+            const double sc = hA + hB + fabs(hA + rin) + fabs(hB + rout);
+            const double xn_ = fmin(fmax((hA + rin) / (hB + rin + rout), 0.0), 1.0);
+            if (fabs(Rx) <= 1.0e-15 * sc || fabs(xn_ - hx) <= 1.0e-15) {
+                Sc.x = hx;
+                after_x(em, true);
+                return;
+            }
+            if (!(fabs(Rx) < hprev) || ++hk >= 8) {
+                hph = 1;
+                ask_sums(ec, 0.0);
+                return;
+            }
+            hprev = fabs(Rx);
+            hx = xn_;
+            ask_sums(ec, hx);
+            return;
+        }
+        if (hph == 1) {
+            hRa = -(hA + rin);
+            hph = 2;
+            ask_sums(ec, 1.0);
+            return;
+        }
+        if (hph == 2) {
+            hRb = hB + rout;
+            hscale = hA + hB + fabs(hRa) + fabs(hRb);
+            hxa = 0.0;
+            hxb = 1.0;
+            hx = hxb;
+            hkk = 0;
+            hph = 3;
+        } else if (hph == 3) {
+            const double Rx = hx * (hB + rin + rout) - (hA + rin);
+            if (fabs(Rx) <= 1.0e-15 * hscale || fabs(hxb - hxa) <= 1.0e-15) {
+                hph = 4;
+            } else {
+                if (Rx * hRb < 0.0) {
+                    hxa = hxb;
+                    hRa = hRb;
+                } else {
+                    hRa = 0.5 * hRa;
+                }
+                hxb = hx;
+                hRb = Rx;
+            }
+        } else {   // hph == 4: the sums at the Illinois root
+            Sc.x = hx;
+            after_x(em, true);
+            return;
+        }
+        if (hph == 3) {
+            if (++hkk > 80 || hRb == hRa) {
+                hph = 4;
+            } else {
+                hx = hxb - hRb * (hxb - hxa) / (hRb - hRa);
+                hx = fmin(fmax(hx, fmin(hxa, hxb)), fmax(hxa, hxb));
+            }
+        }
+        ask_sums(ec, hx);
+    }
+    // cell_electrons after x_HI: He, then the metal electrons
+    __device__ void after_x(double nem_x, bool have_nem) {
+        const BalArgs& b = A->b;
+        const double c = ec;
+        const double r1 = fmin((g1 + k.cHe1 * c) / (k.aHe2 * c), 1.0e150);
+        const double r2 = fmin((g2 + k.cHe2 * c) / (k.aHe3 * c), 1.0e150);
+        Sc.h1 = 1.0 / (1.0 + r1 + r1 * r2);
+        Sc.h2 = Sc.h1 * r1;
+        if (b.metal_ne && !have_nem) {
+            fph = 1;
+            ask_sums(c, Sc.x);
+            return;
+        }
+        after_nem(b.metal_ne ? nem_x : 0.0);
+    }
+    __device__ void after_nem(double nem) {
+        const BalArgs& b = A->b;
+        fph = 0;
+        const double h3 = Sc.h2 * fmin((g2 + k.cHe2 * ec) / (k.aHe3 * ec), 1.0e150);
+        double nenF = nH * ((1.0 - Sc.x) + b.yHe * (Sc.h2 + 2.0 * h3));
+        if (b.metal_ne) nenF = nenF + nem;
+        on_F(nenF - ec);
+    }
+    // solve_cell_fast after F(ec) = fc
+    __device__ void on_F(double fc) {
+        const BalArgs& b = A->b;
+        const double floor = 1.0e-12 * nH, top = b.nemax * nH;
+        ++enev;
+        bool to_fp = false;
+        if (eph == 0) {
+            efa = fc; Sa = Sc; eb = ea; efb = efa; Sb = Sa;
+            if (fabs(efa) <= 2.0e-10 * ea) {
+                eph = 9;
+            } else {
+                double c = efa > 0.0 ? fmin(ea + efa, top) : fmax(ea + efa, floor);
+                if (!(c > 0.0)) c = floor;
+                ec = c;
+                eph = 1;
+            }
+        } else if (eph == 1) {
+            eb = ec; efb = fc; Sb = Sc;
+            if (fabs(fc) <= 2.0e-10 * ec || fc == 0.0) {
+                eph = 9;
+            } else if ((fc > 0.0) != (efa > 0.0)) {
+                to_fp = true;
+            } else if (ec >= top || ec <= floor) {
+                eph = 9;
+            } else {
+                const double lA = log(ea), lC = log(ec);
+                double ld = lC - fc * (lC - lA) / (fc - efa);
+                const bool ahead = fc > 0.0 ? ld > lC : ld < lC;
+                const double lim = log(efac);
+                if (!(fabs(fc) < fabs(efa)) || !ahead || !(fabs(ld - lC) <= lim)) ld = fc > 0.0 ? lC + lim : lC - lim;
+                ea = ec; efa = fc; Sa = Sc;
+                ec = fc > 0.0 ? fmin(exp(ld), top) : fmax(exp(ld), floor);
+                efac = efac * efac;
+                if (enev >= 60) to_fp = true;
+            }
+        } else {   // eph == 2
+            eb = ec;
+            Sb = Sc;
+            ++eit;
+            const double lc = log(ec);
+            if (fabs(fc) <= 2.0e-10 * ec || fc == 0.0) {
+                eph = 9;
+            } else if ((fc > 0.0) == (efb > 0.0)) {
+                if (eside == -1) {
+                    const double m = 1.0 - fc / efb;
+                    efa = efa * (m > 0.0 ? m : 0.5);
+                }
+                elb = lc; efb = fc; eside = -1;
+            } else {
+                if (eside == +1) {
+                    const double m = 1.0 - fc / efa;
+                    efb = efb * (m > 0.0 ? m : 0.5);
+                }
+                ela = lc; efa = fc; eside = +1;
+            }
+        }
+        if (to_fp) {
+            ela = log(ea);
+            elb = log(eb);
+            eside = 0;
+            eit = 0;
+            eph = 2;
+        }
+        if (eph == 2) {
+            const double width = fabs(elb - ela);
+            if (width <= 1.0e-13 || eit >= 100 || enev >= 160) {
+                eph = 9;
+            } else {
+                double lc = (ela * efb - elb * efa) / (efb - efa);
+                if (!(fabs(lc - ela) > 1.0e-3 * width && fabs(lc - elb) > 1.0e-3 * width)) lc = 0.5 * (ela + elb);
+                ec = exp(lc);
+            }
+        }
+        if (eph != 9) {
+            start_F(ec);
+            return;
+        }
+        // the n_e root: the state of the last point evaluated
+        passes += enev;
+        ne = eb;
+        xHI = Sb.x;
+        xHeI = Sb.h1;
+        xHeII = Sb.h2;
+        req = kReqFinish;
+    }
+    // thermal_bracketed after net(t)
+    __device__ void on_net(double f) {
+        const double lo_lim = A->te_min, hi_lim = A->te_max;
+        ++nev;
+        bool to_fp = false;
+        if (tph == 0) {
+            tfa = f;
+            if (tfa == 0.0 || (ta <= lo_lim && tfa < 0.0) || (ta >= hi_lim && tfa > 0.0)) {
+                tr = ta;
+                tph = 9;
+            } else {
+                tph = 1;
+                ts = 0;
+                tfac = 1.05;
+            }
+        } else if (tph == 1) {
+            tfb = f;
+            ++ts;
+            if (tfb == 0.0) {
+                tr = tb;
+                tph = 9;
+            } else if ((tfb > 0.0) != (tfa > 0.0)) {
+                to_fp = true;
+            } else if (tb >= hi_lim || tb <= lo_lim) {
+                tr = tb;
+                tph = 9;
+            } else {
+                ta = tb;
+                tfa = tfb;
+                tfac = tfac * tfac;
+                if (ts >= 40) to_fp = true;
+            }
+        } else {   // tph == 2
+            const double lc = log(t), width = fabs(tlb - tla);
+            ++tit;
+            tr = t;
+            if (f == 0.0) {
+                tph = 9;
+            } else {
+                if ((f > 0.0) == (tfa > 0.0)) {
+                    tla = lc;
+                    tfa = f;
+                } else {
+                    tlb = lc;
+                    tfb = f;
+                }
+                bisect = fabs(tlb - tla) > 0.5 * width;
+            }
+        }
+        if (to_fp) {
+            tla = log(ta);
+            tlb = log(tb);
+            tr = tb;
+            bisect = false;
+            tit = 0;
+            tph = 2;
+        }
+        if (tph == 1) {
+            tb = tfa > 0.0 ? fmin(ta * tfac, hi_lim) : fmax(ta / tfac, lo_lim);
+            t = tb;
+        } else if (tph == 2) {
+            const double width = fabs(tlb - tla);
+            if (width < 1.0e-5 || tit >= 80) {
+                tph = 9;
+            } else {
+                double lc = (tla * tfb - tlb * tfa) / (tfb - tfa);
+                if (bisect || !(fabs(lc - tla) > 0.05 * width && fabs(lc - tlb) > 0.05 * width))
+                    lc = 0.5 * (tla + tlb);
+                t = exp(lc);
+            }
+        }
+        if (tph != 9) {
+            start_net(t);
+            return;
+        }
+        // the leaf's T_e; the written state (thermal_mod.f90:191-203)
+        const BalArgs& b = A->b;
+        te = tr;
+        const double w = b.relax;
+        xn = (1.0 - w) * x0 + w * xHI;
+        h1n = (1.0 - w) * h10 + w * xHeI;
+        h2n = (1.0 - w) * h20 + w * xHeII;
+        const double h3n = fmax(0.0, 1.0 - h1n - h2n);
+        nen_hhe = nH * ((1.0 - xn) + b.yHe * (h2n + 2.0 * h3n));
+        nen = nen_hhe;
+        req = kReqNone;
+        if (b.metal_ne) {   // charge_neutrality_ne from the solved n_e
+            in_neu = true;
+            nit = 0;
+            nen = fmax(ne, 1.0e-12 * nH);
+            ask_sums(nen, xn);
+        }
+    }
+    __device__ void on_neu(double em) {
+        const double ne_old = nen;
+        double v = nen_hhe + em;
+        v = fmax(0.5 * (v + ne_old), 1.0e-12 * nH);
+        nen = v;
+        if (fabs(v - ne_old) <= 1.0e-10 * v || ++nit >= 200) {
+            in_neu = false;
+            req = kReqNone;
+        } else {
+            ask_sums(nen, xn);
+        }
+    }
+};
+
+__global__ void __launch_bounds__(kBThreads) k_thermal_flow(const ThArgs a, unsigned long long* next) {
+    __shared__ double sh[6][kBThreads];
+    const BalArgs& b = a.b;
+    double mdx = 0.0, mdt = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0, s4 = 0.0;
+    unsigned long long solved = 0, tpass = 0, tsums = 0, nevals = 0;
+    SerialCascade mc;
+    mc.m = &b.m;
+    LeafFlow L;
+    L.A = &a;
+    // the first leaf of each lane: its own position; then from the counter
+    long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long long n = b.nleaf;
+    const long long first_claimed = (long long)gridDim.x * blockDim.x;
+    for (;;) {
+        // start leaves until one needs solving (empty leaves finish at once)
+        while (!L.live && p < n) {
+            const long long il = a.order ? (long long)a.order[n - 1 - p] : p;   // the most work first
+            if (b.nH[il] <= 0.0) {
+                b.ne[il] = 0.0;
+                write_columns(b.col, il, b.nabs, b.fp32, b.nH[il], b.yHe, b.xHI[il], b.xHeI[il], b.xHeII[il],
+                              b.colscale, b.rhokap ? b.rhokap[il] : 0.0);
+                if (a.work) a.work[il] = 0u;
+                p = first_claimed + (long long)atomicAdd(next, 1ull);
+                continue;
+            }
+            L.start_leaf(p, il);
+        }
+        if (!__any_sync(kFull, L.live)) break;
+        if (__any_sync(kFull, L.live && L.req == kReqPrepare)) {
+            if (L.live && L.req == kReqPrepare) {
+                mc.prepare(L.il, L.q_T);
+                L.on_prepare();
+            }
+        }
+        if (__any_sync(kFull, L.live && L.req == kReqSums)) {
+            if (L.live && L.req == kReqSums) {
+                double nem, rin, rout;
+                mc.sums(L.nH, L.q_ne, L.nH * L.q_x, L.nH * (1.0 - L.q_x), nem, rin, rout);
+                L.on_sums(nem, rin, rout);
+            }
+        }
+        if (__any_sync(kFull, L.live && L.req == kReqFinish)) {
+            if (L.live && L.req == kReqFinish) {
+                const long long il = L.il;
+                const long long nl = b.nleaf;
+                const double heat = L.nH * (L.xHI * b.rates[3 * nl + il] +
+                                            b.yHe * (L.xHeI * b.rates[4 * nl + il] + L.xHeII * b.rates[5 * nl + il]));
+                double net = heat - cooling_total(a.td, b.rs, b.caseA, b.yHe, L.q_T, L.nH, L.ne, L.xHI, L.xHeI, L.xHeII);
+                const MetalThermalTerms mt =
+                    thermal_terms(a.td, mc, il, L.q_T, L.nH, L.ne, L.nH * L.xHI, L.nH * (1.0 - L.xHI));
+                net = net - mt.cool;
+                net = net - mt.cool_H;
+                if (b.metal_ff) net = net - mt.freefree;
+                if (b.metal_heat) net = net + mt.heat;
+                L.on_net(net);
+            }
+        }
+        // a lane whose leaf is solved writes it and takes the next one
+        if (L.live && L.req == kReqNone) {
+            const long long il = L.il;
+            if (b.fp32) mc.opacity_fill<float>(il, L.nH, L.nen, L.xn, b.colscale);
+            else mc.opacity_fill<double>(il, L.nH, L.nen, L.xn, b.colscale);
+            ++solved;
+            tpass += (unsigned long long)L.passes;
+            tsums += (unsigned long long)L.nsum;
+            nevals += (unsigned long long)L.nev;
+            if (a.work) a.work[il] = (unsigned)min(L.nsum, 65535);
+            b.xHI[il] = L.xn;
+            b.xHeI[il] = L.h1n;
+            b.xHeII[il] = L.h2n;
+            b.ne[il] = L.nen;
+            b.Te[il] = L.te;
+            write_columns(b.col, il, b.nabs, b.fp32, L.nH, b.yHe, L.xn, L.h1n, L.h2n, b.colscale,
+                          b.rhokap ? b.rhokap[il] : 0.0);
+            const double dx = fabs(L.xn - L.x0);
+            mdx = fmax(mdx, dx);
+            mdt = fmax(mdt, fabs(L.te - L.T0) / L.T0);
+            const double vol = leaf_vol(b, il);
+            s1 = s1 + vol * dx;
+            s2 = s2 + vol * (1.0 - L.xn);
+            s3 = s3 + vol * L.nen * fabs(L.te - L.T0);
+            s4 = s4 + vol * L.nen * L.te;
+            L.live = false;
+            p = first_claimed + (long long)atomicAdd(next, 1ull);
+        }
+    }
+    const int t = threadIdx.x;
+    sh[0][t] = mdx; sh[1][t] = mdt; sh[2][t] = s1; sh[3][t] = s2; sh[4][t] = s3; sh[5][t] = s4;
+    __syncthreads();
+    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+        if (t < s) {
+            sh[0][t] = fmax(sh[0][t], sh[0][t + s]);
+            sh[1][t] = fmax(sh[1][t], sh[1][t + s]);
+            for (int k = 2; k < 6; ++k) sh[k][t] = sh[k][t] + sh[k][t + s];
+        }
+        __syncthreads();
+    }
+    if (t == 0)
+        for (int k = 0; k < 6; ++k) b.partial[6 * blockIdx.x + k] = sh[k][0];
+    for (int o = 16; o > 0; o >>= 1) {
+        solved += __shfl_down_sync(kFull, solved, o);
+        tpass += __shfl_down_sync(kFull, tpass, o);
+        tsums += __shfl_down_sync(kFull, tsums, o);
+        nevals += __shfl_down_sync(kFull, nevals, o);
+    }
+    if ((t & 31) == 0) {
+        if (solved) atomicAdd(b.counters + 0, solved);
+        if (tpass) atomicAdd(b.counters + 2, tpass);
+        if (tsums) atomicAdd(b.counters + 3, tsums);
+        if (nevals) atomicAdd(b.counters + 4, nevals);
+    }
+}
+
 // gas_thermal_update with metals, one warp per leaf (WarpCascade): the
 // same solve as k_thermal; lane 0 writes the leaf's state, the element lanes
 // its opacity weights.  128-thread blocks, grid-stride over leaves by warps.
@@ -1615,7 +2118,7 @@ cudaError_t launch_thermal(mochii_ctx* c) {
     a.Twarm = c->twarm_set ? c->twarm : nullptr;
     a.order = nullptr;
     a.work = nullptr;
-    if (c->metal.ntr > 0 && c->par.solver_warp) {
+    if (c->metal.ntr > 0 && c->par.solver_warp == 1) {
         k_thermal_warp<<<c->bw.blocks, kWThreads, 0, c->stream>>>(a);
     } else if (c->metal.ntr > 0 && c->par.solver_bracketed) {
         BalanceWork& w = c->bw;
@@ -1626,6 +2129,7 @@ cudaError_t launch_thermal(mochii_ctx* c) {
             if ((e = cudaMalloc(&w.work_sorted, (size_t)n * 4)) != cudaSuccess) return e;
             if ((e = cudaMalloc(&w.iota, (size_t)n * 4)) != cudaSuccess) return e;
             if ((e = cudaMalloc(&w.order, (size_t)n * 4)) != cudaSuccess) return e;
+            if ((e = cudaMalloc(&w.next, sizeof(unsigned long long))) != cudaSuccess) return e;
             cub::DeviceRadixSort::SortPairs(nullptr, w.sort_bytes, w.work, w.work_sorted, w.iota, w.order, n, 0, 16);
             if ((e = cudaMalloc(&w.sort_tmp, w.sort_bytes)) != cudaSuccess) return e;
             k_iota<<<nblocks(n, 256, 148 * 16), 256, 0, c->stream>>>(w.iota, n);
@@ -1638,7 +2142,12 @@ cudaError_t launch_thermal(mochii_ctx* c) {
             a.order = w.order;
         }
         a.work = w.work;
-        k_thermal_ls<<<c->bw.blocks, kBThreads, 0, c->stream>>>(a);
+        if (c->par.solver_warp == 2) {
+            k_thermal_ls<<<c->bw.blocks, kBThreads, 0, c->stream>>>(a);
+        } else {
+            if ((e = cudaMemsetAsync(w.next, 0, sizeof(unsigned long long), c->stream)) != cudaSuccess) return e;
+            k_thermal_flow<<<c->bw.blocks, kBThreads, 0, c->stream>>>(a, w.next);
+        }
         w.have_work = true;
     } else {
         k_thermal<<<c->bw.blocks, kBThreads, 0, c->stream>>>(a);

@@ -84,6 +84,7 @@ struct BalanceWork {
     int* order = nullptr;             // leaves by ascending work
     void* sort_tmp = nullptr;
     size_t sort_bytes = 0;
+    unsigned long long* next = nullptr;   // the flat solve's leaf counter
     bool have_work = false;
 };
 
