@@ -1814,8 +1814,18 @@ __global__ void __launch_bounds__(kBThreads) k_thermal_flow(const ThArgs a, unsi
             }
             L.start_leaf(p, il);
         }
-        if (!__any_sync(kFull, L.live)) break;
-        if (__any_sync(kFull, L.live && L.req == kReqPrepare)) {
+        const unsigned live = __ballot_sync(kFull, L.live);
+        if (!live) break;
+        // the rate cache and the net heating are costly and asked for once per
+        // trial T, so they are served when at least half the live lanes ask,
+        // or when no live lane asks for a cascade sum
+        const unsigned wp = __ballot_sync(kFull, L.live && L.req == kReqPrepare);
+        const unsigned wf = __ballot_sync(kFull, L.live && L.req == kReqFinish);
+        const unsigned ws = __ballot_sync(kFull, L.live && L.req == kReqSums);
+        const int nl = __popc(live);
+        const bool serve_p = wp && (2 * __popc(wp) >= nl || !ws);
+        const bool serve_f = wf && (2 * __popc(wf) >= nl || !ws);
+        if (serve_p) {
             if (L.live && L.req == kReqPrepare) {
                 mc.prepare(L.il, L.q_T);
                 L.on_prepare();
@@ -1828,7 +1838,7 @@ __global__ void __launch_bounds__(kBThreads) k_thermal_flow(const ThArgs a, unsi
                 L.on_sums(nem, rin, rout);
             }
         }
-        if (__any_sync(kFull, L.live && L.req == kReqFinish)) {
+        if (serve_f) {
             if (L.live && L.req == kReqFinish) {
                 const long long il = L.il;
                 const long long nl = b.nleaf;
