@@ -292,7 +292,7 @@ def main():
                     help="transport arithmetic (default: the workload's)")
     ap.add_argument("--solver", default="bracketed", choices=["bisection", "bracketed"],
                     help="cell solver: the reference's bisection or the bracketed roots")
-    ap.add_argument("--cell-layout", default="thread", choices=["thread", "warp", "lockstep"],
+    ap.add_argument("--cell-layout", default="lockstep", choices=["lockstep", "flow", "warp"],
                     help="thermal solve with metals: one warp or one thread per leaf")
     ap.add_argument("--grid", type=int, default=None, help="grid side of a Cartesian workload (default: its own)")
     ap.add_argument("--packets", type=int, default=None, help="stellar packets per pass (default: the workload's)")

@@ -136,10 +136,11 @@ typedef struct mochii_params {
      * (define.f90:211-212,361); taumax / tauhomo > 0 are not built */
     double lambda_ref, taumax, tauhomo;
     /* thermal solve with metals (not a reference key, par%cell_layout):
-     * 0 'thread' = one thread per leaf, each lane's whole bracketed solve a
-     * state machine served by warp-wide evaluations (default); 1 'warp' = one
-     * warp per leaf, the metal cascade spread over the lanes; 2 'lockstep' =
-     * one thread per leaf, nested warp-uniform loops */
+     * 0 'lockstep' (or 'thread') = one thread per leaf, warp-uniform root
+     * loops over leaves sorted by work (default); 1 'warp' = one warp per
+     * leaf, the metal cascade spread over the lanes; 2 'flow' = one thread
+     * per leaf, each lane's whole solve a state machine served by warp-wide
+     * evaluations */
     int solver_warp;
 } mochii_params;
 

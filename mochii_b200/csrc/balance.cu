@@ -2153,10 +2153,10 @@ cudaError_t launch_thermal(mochii_ctx* c) {
         }
         a.work = w.work;
         if (c->par.solver_warp == 2) {
-            k_thermal_ls<<<c->bw.blocks, kBThreads, 0, c->stream>>>(a);
-        } else {
             if ((e = cudaMemsetAsync(w.next, 0, sizeof(unsigned long long), c->stream)) != cudaSuccess) return e;
             k_thermal_flow<<<c->bw.blocks, kBThreads, 0, c->stream>>>(a, w.next);
+        } else {
+            k_thermal_ls<<<c->bw.blocks, kBThreads, 0, c->stream>>>(a);
         }
         w.have_work = true;
     } else {

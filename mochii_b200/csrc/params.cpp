@@ -277,8 +277,9 @@ int set_key(mochii_params* p, std::string key, const std::vector<std::string>& v
     if (key == "atomic_dir") { copy_str(p->atomic_dir, sizeof(p->atomic_dir), unquote(v)); return 0; }
     if (key == "cell_layout") {
         const std::string s = lower(unquote(v));
-        if (s != "warp" && s != "thread" && s != "lockstep") return bad("must be 'thread', 'warp' or 'lockstep'");
-        p->solver_warp = s == "warp" ? 1 : s == "lockstep" ? 2 : 0;
+        if (s != "warp" && s != "thread" && s != "lockstep" && s != "flow")
+            return bad("must be 'lockstep', 'flow' or 'warp'");
+        p->solver_warp = s == "warp" ? 1 : s == "flow" ? 2 : 0;
         return 0;
     }
     if (key == "thermal_solver") {

@@ -101,17 +101,17 @@ def test_bracketed_solve_needs_fewer_evaluations():
 
 
 def test_cell_layouts_agree():
-    """The thermal solve with metals in its three layouts -- each leaf's solve
-    a state machine served by warp-wide evaluations ('thread', the default),
-    nested warp-uniform loops ('lockstep'), one warp per leaf ('warp') -- make
-    the same solves per leaf.  Separate runs accumulate the transport tallies
+    """The thermal solve with metals in its three layouts -- warp-uniform root
+    loops ('lockstep', the default), each leaf's solve a state machine served
+    by warp-wide evaluations ('flow'), one warp per leaf ('warp') -- make the
+    same solves per leaf.  Separate runs accumulate the transport tallies
     in different atomic orders, so the rates differ in their last bits and a
     leaf's T_e can move by a fraction of a kelvin where net(T) is flat."""
     n = 16
     nl = with_solver(configs.hii_metals(nphotons=60000, niter=2, n=n, precision="fp64", rs_factor=1.3,
                                         diffuse=False), "bracketed")
     out = {}
-    for layout in ("thread", "lockstep", "warp"):
+    for layout in ("lockstep", "flow", "warp"):
         neb = Nebula(parse_namelist(nl.replace("/\n", f" par%cell_layout = '{layout}'\n/\n")))
         st = partial_state(n, parse_namelist(nl).xmax)
         for k, v in st.items():
@@ -122,8 +122,8 @@ def test_cell_layouts_agree():
             neb.gas_thermal_update()
         out[layout] = (neb.get("T_e"), neb.get("x_HI"), neb.last_metrics.rate_evaluations)
         neb.close()
-    for other in ("lockstep", "warp"):
-        dT = np.abs(out[other][0] - out["thread"][0])
+    for other in ("flow", "warp"):
+        dT = np.abs(out[other][0] - out["lockstep"][0])
         assert np.median(dT) < 1e-6 and dT.max() < 1.0, (other, dT.max())
-        assert np.max(np.abs(out[other][1] - out["thread"][1])) < 1e-6
-        assert abs(out[other][2] / out["thread"][2] - 1) < 0.01
+        assert np.max(np.abs(out[other][1] - out["lockstep"][1])) < 1e-5
+        assert abs(out[other][2] / out["lockstep"][2] - 1) < 0.01
