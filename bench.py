@@ -294,6 +294,8 @@ def main():
                     help="cell solver: the reference's bisection or the bracketed roots")
     ap.add_argument("--cell-layout", default="lockstep", choices=["lockstep", "flow", "warp"],
                     help="thermal solve with metals: one warp or one thread per leaf")
+    ap.add_argument("--tally", default="compensated", choices=["compensated", "fp64"],
+                    help="path tallies with FP32 segments: compensated FP32 pairs or FP64 atomics")
     ap.add_argument("--grid", type=int, default=None, help="grid side of a Cartesian workload (default: its own)")
     ap.add_argument("--packets", type=int, default=None, help="stellar packets per pass (default: the workload's)")
     args = ap.parse_args()
@@ -319,7 +321,8 @@ def main():
         dist.barrier()
 
     par = parse_namelist(wl.make(wl.nphot, prec, 12345 + rank).replace(
-        "/\n", f" par%thermal_solver = '{args.solver}'\n par%cell_layout = '{args.cell_layout}'\n/\n"))
+        "/\n", f" par%thermal_solver = '{args.solver}'\n par%cell_layout = '{args.cell_layout}'\n"
+              f" par%tally_precision = '{args.tally}'\n/\n"))
     neb = Nebula(par)
     prep_iters = prepare(neb, wl)
     tuning = neb.autotune(1 << 20)   # launch shape for this grid / precision / device
@@ -435,7 +438,7 @@ def main():
             "config": {"workload": wl.name, "grid": grid_name(wl, nleaf), "stellar_packets_per_step": wl.nphot,
                        "packets_per_step": packets / args.steps / world,
                        "precision": prec, "balance": "thermal" if wl.thermal else "ionisation, fixed T_e",
-                       "solver": args.solver, "cell_layout": args.cell_layout,
+                       "solver": args.solver, "cell_layout": args.cell_layout, "tallies": args.tally,
                        "state": f"{prep_iters} untimed preparation iterations from the configured start",
                        "l2": "flushed between steps (256 MiB write)", "tuning": tuning,
                        "parallelism": "replicas" if world > 1 else "single"},

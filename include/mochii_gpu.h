@@ -142,6 +142,10 @@ typedef struct mochii_params {
      * per leaf, each lane's whole solve a state machine served by warp-wide
      * evaluations */
     int solver_warp;
+    /* path tallies with FP32 segments (not a reference key,
+     * par%tally_precision): 0 'compensated' = (hi, lo) FP32 pairs summed in
+     * FP64 after the pass; 1 'fp64' = FP64 atomic tallies */
+    int tally64;
 } mochii_params;
 
 /* Per-pass statistics (ion_score_report_energy_closure, ion_score_mod.f90:364-387). */

@@ -203,6 +203,7 @@ extern "C" int mochii_init(const mochii_params* pin, mochii_ctx** out) {
         g.dcell = (g.xmax - g.xmin) / (double)g.nx;
     }
     c->fp32 = p.precision == MOCHII_PREC_FP32;
+    c->tally64 = !c->fp32 || p.tally64;
     c->xscore = p.ion_add_dust || p.add_fuv;
     c->scatter = p.ion_add_dust && p.ion_dust_scatter;
     c->nabs = p.He_abund > 0.0 || c->xscore ? 4 : 1;

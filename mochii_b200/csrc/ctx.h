@@ -99,6 +99,7 @@ struct mochii_ctx {
     cudaEvent_t ev0 = nullptr, ev1 = nullptr, evA = nullptr, evB = nullptr;
     bool columns_fresh = false;   // absorber columns match the state
     bool fp32 = false;
+    bool tally64 = true;          // FP64 tallies (always with FP64 segments)
     int nabs = 1, ntally = 2, nnu = 0;
     // device memory
     double *nH = nullptr, *xHI = nullptr, *xHeI = nullptr, *xHeII = nullptr, *ne = nullptr, *Te = nullptr;

@@ -275,6 +275,12 @@ int set_key(mochii_params* p, std::string key, const std::vector<std::string>& v
     if (key == "ion_dust_kext") { copy_str(p->ion_dust_kext, sizeof(p->ion_dust_kext), unquote(v)); return 0; }
     if (key == "data_dir") { copy_str(p->data_dir, sizeof(p->data_dir), unquote(v)); return 0; }
     if (key == "atomic_dir") { copy_str(p->atomic_dir, sizeof(p->atomic_dir), unquote(v)); return 0; }
+    if (key == "tally_precision") {
+        const std::string s = lower(unquote(v));
+        if (s != "compensated" && s != "fp64") return bad("must be 'compensated' or 'fp64'");
+        p->tally64 = s == "fp64";
+        return 0;
+    }
     if (key == "cell_layout") {
         const std::string s = lower(unquote(v));
         if (s != "warp" && s != "thread" && s != "lockstep" && s != "flow")

@@ -218,9 +218,6 @@ __device__ __forceinline__ void tally_add(double* p, double v) { atomicAdd(p, v)
 __device__ __forceinline__ float attenuation(float x) { return expf(-x); }
 __device__ __forceinline__ double attenuation(double x) { return exp(-x); }
 
-template <typename R> struct Acc;
-template <> struct Acc<double> { typedef double T; };
-template <> struct Acc<float> { typedef float2 T; };
 
 template <typename R, int NABS>
 __device__ __forceinline__ R opacity(const void* col, long long il, R s0, R s1, R s2) {
@@ -637,10 +634,9 @@ __device__ __noinline__ void scattered_flights(const PassArgs& a, double x, doub
 // X the grain and FUV terms (NABS = 4) and, with a.scatter, the scattered
 // flights after the edge walk.  Packet i of the chunk is packet ip0 + i of
 // its stream (0 stellar, 1 diffuse).
-template <typename R, int NABS, int LA, int MET, int X>
+template <typename R, int NABS, int LA, int MET, int X, typename T>
 __global__ void __launch_bounds__(128) k_walk_edge(const PassArgs a, const PacketRecords rec, long long n,
                                                    int accumulate, long long ip0, int stream) {
-    typedef typename Acc<R>::T T;
     constexpr int NT = X ? 8 : (NABS == 1 ? 2 : 6);
     constexpr bool METAL = MET > 0;
     __shared__ double sh[128];
@@ -770,10 +766,9 @@ __global__ void __launch_bounds__(128) k_walk_edge(const PassArgs a, const Packe
 // attenuated path score, the move to the exit point, and the leaf across the
 // face (amr_next_leaf).  Geometry in FP64 without contraction, as the
 // reference's.  MET, X, ip0 and stream as for k_walk_edge.
-template <typename R, int NABS, int MET, int X>
+template <typename R, int NABS, int MET, int X, typename T>
 __global__ void __launch_bounds__(128) k_walk_amr(const PassArgs a, const PacketRecords rec, long long n,
                                                   int accumulate, long long ip0, int stream) {
-    typedef typename Acc<R>::T T;
     constexpr int NT = X ? 8 : (NABS == 1 ? 2 : 6);
     constexpr bool METAL = MET > 0;
     __shared__ double sh[128];
@@ -1145,9 +1140,9 @@ template <int V> struct AbsV {
 
 int abs_variant(const mochii_ctx* c) { return c->xscore ? 5 : c->nabs == 1 ? 1 : 4; }
 
-template <typename R, int V, int LA, int MET>
+template <typename R, typename T, int V, int LA, int MET>
 int walk_occupancy(size_t smem) {
-    auto k = k_walk_edge<R, AbsV<V>::NABS, LA, MET, AbsV<V>::X>;
+    auto k = k_walk_edge<R, AbsV<V>::NABS, LA, MET, AbsV<V>::X, T>;
     if (smem > 48 * 1024) cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     int nb = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k, 128, smem) != cudaSuccess) {
@@ -1157,12 +1152,12 @@ int walk_occupancy(size_t smem) {
     return nb > 0 ? nb : 1;
 }
 
-template <typename R>
+template <typename R, typename T>
 int walk_occupancy_any(const mochii_ctx* c, size_t smem) {
     switch (abs_variant(c)) {
-        case 1: return walk_occupancy<R, 1, 2, 1>(smem);
-        case 4: return walk_occupancy<R, 4, 2, 1>(smem);
-        default: return walk_occupancy<R, 5, 2, 1>(smem);
+        case 1: return walk_occupancy<R, T, 1, 2, 1>(smem);
+        case 4: return walk_occupancy<R, T, 4, 2, 1>(smem);
+        default: return walk_occupancy<R, T, 5, 2, 1>(smem);
     }
 }
 
@@ -1172,7 +1167,9 @@ int transport_blocks(const mochii_ctx* c) {
     int per_sm = c->tune.walk_blocks_per_sm > 0 ? c->tune.walk_blocks_per_sm : 8;
     if (c->metal.ntr > 0) {   // resident blocks only: each holds its packets' sigma_k in shared memory
         const size_t smem = metal_smem(c);
-        const int occ = c->fp32 ? walk_occupancy_any<float>(c, smem) : walk_occupancy_any<double>(c, smem);
+        const int occ = !c->fp32 ? walk_occupancy_any<double, double>(c, smem)
+                        : c->tally64 ? walk_occupancy_any<float, double>(c, smem)
+                                     : walk_occupancy_any<float, float2>(c, smem);
         per_sm = per_sm < occ ? per_sm : occ;
     }
     return grid_blocks(c->par.nphotons, 128, sms * per_sm);
@@ -1187,52 +1184,55 @@ struct WalkLaunch {
 
 // Walk-kernel variants: look-ahead depth 0..2 (the autotuned choice is
 // c->tune.lookahead); 128-thread blocks.
-template <typename R, int V, int MET>
+template <typename R, typename T, int V, int MET>
 cudaError_t walk_la(mochii_ctx* c, const PassArgs& a, const PacketRecords& r, const WalkLaunch& w) {
     constexpr int NABS = AbsV<V>::NABS, X = AbsV<V>::X;
     const size_t smem = MET ? metal_smem(c) : 0;
     if (MET && smem > 48 * 1024) {
-        cudaFuncSetAttribute(k_walk_edge<R, NABS, 0, MET, X>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        cudaFuncSetAttribute(k_walk_edge<R, NABS, 1, MET, X>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        cudaFuncSetAttribute(k_walk_edge<R, NABS, 2, MET, X>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        cudaFuncSetAttribute(k_walk_edge<R, NABS, 0, MET, X, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        cudaFuncSetAttribute(k_walk_edge<R, NABS, 1, MET, X, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        cudaFuncSetAttribute(k_walk_edge<R, NABS, 2, MET, X, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     }
     switch (c->tune.lookahead) {
-        case 0: k_walk_edge<R, NABS, 0, MET, X><<<w.blocks, 128, smem, c->stream>>>(a, r, w.n, w.acc, w.ip0, w.stream); break;
-        case 1: k_walk_edge<R, NABS, 1, MET, X><<<w.blocks, 128, smem, c->stream>>>(a, r, w.n, w.acc, w.ip0, w.stream); break;
-        default: k_walk_edge<R, NABS, 2, MET, X><<<w.blocks, 128, smem, c->stream>>>(a, r, w.n, w.acc, w.ip0, w.stream); break;
+        case 0: k_walk_edge<R, NABS, 0, MET, X, T><<<w.blocks, 128, smem, c->stream>>>(a, r, w.n, w.acc, w.ip0, w.stream); break;
+        case 1: k_walk_edge<R, NABS, 1, MET, X, T><<<w.blocks, 128, smem, c->stream>>>(a, r, w.n, w.acc, w.ip0, w.stream); break;
+        default: k_walk_edge<R, NABS, 2, MET, X, T><<<w.blocks, 128, smem, c->stream>>>(a, r, w.n, w.acc, w.ip0, w.stream); break;
     }
     return cudaGetLastError();
 }
 
 // The octree walk: no look-ahead variants.
-template <typename R, int V, int MET>
+template <typename R, typename T, int V, int MET>
 cudaError_t walk_amr(mochii_ctx* c, const PassArgs& a, const PacketRecords& r, const WalkLaunch& w) {
     constexpr int NABS = AbsV<V>::NABS, X = AbsV<V>::X;
     const size_t smem = MET ? metal_smem(c) : 0;
     if (MET && smem > 48 * 1024)
-        cudaFuncSetAttribute(k_walk_amr<R, NABS, MET, X>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    k_walk_amr<R, NABS, MET, X><<<w.blocks, 128, smem, c->stream>>>(a, r, w.n, w.acc, w.ip0, w.stream);
+        cudaFuncSetAttribute(k_walk_amr<R, NABS, MET, X, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k_walk_amr<R, NABS, MET, X, T><<<w.blocks, 128, smem, c->stream>>>(a, r, w.n, w.acc, w.ip0, w.stream);
     return cudaGetLastError();
 }
 
-template <typename R, int MET>
+template <typename R, typename T, int MET>
 cudaError_t walk_abs(mochii_ctx* c, const PassArgs& a, const PacketRecords& r, const WalkLaunch& w) {
     const bool amr = c->oct.ncells > 0;
     switch (abs_variant(c)) {
-        case 1: return amr ? walk_amr<R, 1, MET>(c, a, r, w) : walk_la<R, 1, MET>(c, a, r, w);
-        case 4: return amr ? walk_amr<R, 4, MET>(c, a, r, w) : walk_la<R, 4, MET>(c, a, r, w);
-        default: return amr ? walk_amr<R, 5, MET>(c, a, r, w) : walk_la<R, 5, MET>(c, a, r, w);
+        case 1: return amr ? walk_amr<R, T, 1, MET>(c, a, r, w) : walk_la<R, T, 1, MET>(c, a, r, w);
+        case 4: return amr ? walk_amr<R, T, 4, MET>(c, a, r, w) : walk_la<R, T, 4, MET>(c, a, r, w);
+        default: return amr ? walk_amr<R, T, 5, MET>(c, a, r, w) : walk_la<R, T, 5, MET>(c, a, r, w);
     }
 }
 
-template <typename R>
+template <typename R, typename T>
 cudaError_t walk_prec(mochii_ctx* c, const PassArgs& a, const PacketRecords& r, const WalkLaunch& w) {
-    if (c->metal.ntr == 0) return walk_abs<R, 0>(c, a, r, w);
-    return c->metal.nmb > 0 ? walk_abs<R, 2>(c, a, r, w) : walk_abs<R, 1>(c, a, r, w);
+    if (c->metal.ntr == 0) return walk_abs<R, T, 0>(c, a, r, w);
+    return c->metal.nmb > 0 ? walk_abs<R, T, 2>(c, a, r, w) : walk_abs<R, T, 1>(c, a, r, w);
 }
 
+// Segment arithmetic R and tally type T: FP64 / FP64; FP32 with FP64 tallies
+// (tally64); FP32 with compensated FP32 pairs.
 cudaError_t launch_walk_variant(mochii_ctx* c, const PassArgs& a, const PacketRecords& r, const WalkLaunch& w) {
-    return c->fp32 ? walk_prec<float>(c, a, r, w) : walk_prec<double>(c, a, r, w);
+    if (!c->fp32) return walk_prec<double, double>(c, a, r, w);
+    return c->tally64 ? walk_prec<float, double>(c, a, r, w) : walk_prec<float, float2>(c, a, r, w);
 }
 
 PacketRecords packet_records(mochii_ctx* c) {
@@ -1304,7 +1304,7 @@ cudaError_t launch_rates(mochii_ctx* c) {
     const double* rk = c->rhokap;
     const double dc = c->par.distance2cm;
 #define RATES(T, NT) k_rates<T, NT><<<blocks, 256, 0, c->stream>>>((const T*)c->tally, c->rates, n, cg, ch, lg, d2, rk, dc)
-    if (c->fp32) {
+    if (c->fp32 && !c->tally64) {
         if (c->ntally == 2) RATES(float2, 2);
         else if (c->ntally == 6) RATES(float2, 6);
         else RATES(float2, 8);
@@ -1316,11 +1316,11 @@ cudaError_t launch_rates(mochii_ctx* c) {
 #undef RATES
     if (c->metal.ntr > 0 && c->metal.nmb > 0) {
         const int mb = grid_blocks(n * 32, 256, 148 * 32);
-        if (c->fp32) k_metal_rates_mom<float2><<<mb, 256, 0, c->stream>>>(c->metal, n, cg, ch, lg, d2);
+        if (c->fp32 && !c->tally64) k_metal_rates_mom<float2><<<mb, 256, 0, c->stream>>>(c->metal, n, cg, ch, lg, d2);
         else k_metal_rates_mom<double><<<mb, 256, 0, c->stream>>>(c->metal, n, cg, ch, lg, d2);
     } else if (c->metal.ntr > 0) {
         const int mb = grid_blocks(n * c->metal.ntr, 256, 148 * 16);
-        if (c->fp32) k_metal_rates<float2><<<mb, 256, 0, c->stream>>>(c->metal, n, cg, ch, lg, d2);
+        if (c->fp32 && !c->tally64) k_metal_rates<float2><<<mb, 256, 0, c->stream>>>(c->metal, n, cg, ch, lg, d2);
         else k_metal_rates<double><<<mb, 256, 0, c->stream>>>(c->metal, n, cg, ch, lg, d2);
     }
     return cudaGetLastError();
@@ -1330,7 +1330,7 @@ cudaError_t launch_jt_export(mochii_ctx* c, double* dst) {
     const long long n = c->grid.nleaf * (long long)c->nnu;
     const double Lp = c->band.ion_Ltot / (double)c->par.nphotons;
     const int blocks = grid_blocks(n, 256, 148 * 16);
-    if (c->fp32) k_jt<float2><<<blocks, 256, 0, c->stream>>>((const float2*)c->jt, dst, n, Lp);
+    if (c->fp32 && !c->tally64) k_jt<float2><<<blocks, 256, 0, c->stream>>>((const float2*)c->jt, dst, n, Lp);
     else k_jt<double><<<blocks, 256, 0, c->stream>>>((const double*)c->jt, dst, n, Lp);
     return cudaGetLastError();
 }

@@ -144,9 +144,12 @@ def test_fp64_pass_with_helium_matches_oracle(orc):
     neb.close()
 
 
-def test_fp32_compensated_tallies_within_tolerance(orc):
+@pytest.mark.parametrize("tally", ["compensated", "fp64"])
+def test_fp32_compensated_tallies_within_tolerance(orc, tally):
+    """FP32 segments with compensated FP32 tally pairs or FP64 atomic
+    tallies: the FP32 opacity and attenuation error only."""
     n = 32
-    nl = small_nl(n=n, nphot=20000, precision="fp32")
+    nl = small_nl(n=n, nphot=20000, precision="fp32").replace("/\n", f" par%tally_precision = '{tally}'\n/\n")
     L = parse_namelist(nl).xmax
     neb, sim, st = pass_pair(orc, nl, partially_ionised_state(n, L))
     for f in ("gamma_HI", "heat_HI"):
