@@ -11,7 +11,8 @@ Workloads (--workload):
                  balance: 128^3 grid, n_H = 100, He/H 0.1, eleven metals,
                  45 kK blackbody with Q(H) = 5e49 s^-1, case A with explicit
                  diffuse Milne packets, 1e7 stellar packets per pass, FP32
-                 segments with compensated FP32 tallies (metal rates from
+                 segments with FP64 atomic tallies (--tally compensated for
+                 the (hi, lo) FP32 pairs; metal rates from
                  the energy-moment tallies).  Untimed preparation iterations
                  bring the ionized start to a developed H II region first.
   stromgren64    the pure-H Stromgren sphere: 64^3, 40 kK, Q(H) = 1e49,
@@ -34,8 +35,9 @@ e2e       the same metric through the C ABI with host buffers: each step
           uploads the leaf state (x_HI, T_e) from pinned host memory and
           reads back x_HI, T_e and Gamma_HI, copies inside the timing.
 roofline  the transport kernels: algorithmic bytes per scored segment
-          B_seg = 4 F_state + 16 F_tally (state words read, compensated
-          tally pairs read and written; FP64 words count 8 B) over their
+          B_seg = 4 F_state + 16 F_tally (state words read, 8-byte tallies
+          (FP64, or a compensated FP32 pair) read and written; FP64 state
+          words count 8 B) over their
           event-timed duration; the metal state words are counted per
           segment in the kernel (one per active transition).
 N > 1     one process per GPU, each an independent nebula (replicas: the
@@ -294,7 +296,7 @@ def main():
                     help="cell solver: the reference's bisection or the bracketed roots")
     ap.add_argument("--cell-layout", default="lockstep", choices=["lockstep", "flow", "warp"],
                     help="thermal solve with metals: one warp or one thread per leaf")
-    ap.add_argument("--tally", default="compensated", choices=["compensated", "fp64"],
+    ap.add_argument("--tally", default="fp64", choices=["fp64", "compensated"],
                     help="path tallies with FP32 segments: compensated FP32 pairs or FP64 atomics")
     ap.add_argument("--grid", type=int, default=None, help="grid side of a Cartesian workload (default: its own)")
     ap.add_argument("--packets", type=int, default=None, help="stellar packets per pass (default: the workload's)")

@@ -143,8 +143,10 @@ typedef struct mochii_params {
      * evaluations */
     int solver_warp;
     /* path tallies with FP32 segments (not a reference key,
-     * par%tally_precision): 0 'compensated' = (hi, lo) FP32 pairs summed in
-     * FP64 after the pass; 1 'fp64' = FP64 atomic tallies */
+     * par%tally_precision): 1 'fp64' = FP64 atomic tallies (default: on B200
+     * the FP64 reduction is a native L2 atomic, faster than the two-word
+     * compensated update); 0 'compensated' = (hi, lo) FP32 pairs summed in
+     * FP64 after the pass */
     int tally64;
 } mochii_params;
 

@@ -138,6 +138,7 @@ extern "C" int mochii_params_default(mochii_params* p) {
     p->taumax = -999.0;
     p->tauhomo = -999.0;
     p->solver_warp = 0;
+    p->tally64 = 1;
     return MOCHII_OK;
 }
 
