@@ -11,6 +11,8 @@
 #include <cub/cub.cuh>
 #include <cuda_runtime.h>
 
+#include <algorithm>
+
 #include "ctx.h"
 #include "metals.cuh"
 #include "physics.cuh"
@@ -423,6 +425,7 @@ struct ThArgs {
     const double* Twarm;   // bracketed solve: warm-start T_e per leaf (nullptr: the current T_e)
     const int* order;      // lockstep solve: the order to visit leaves in (nullptr: leaf order)
     unsigned* work;        // lockstep solve: cascade sums per leaf, written for the next update's order
+    unsigned long long* next;   // lockstep solve: the chunk counter (warps claim 32 leaves at a time)
 };
 
 // gbar_ff (cooling_mod.f90:223-234): linear in log10 T on the 41-node table.
@@ -894,10 +897,11 @@ __device__ __noinline__ double h_root_ls(const SerialCascade& mc, bool act, doub
             const double Rx = x * (B + rin + rout) - (A + rin);
             const double sc = A + B + fabs(A + rin) + fabs(B + rout);
             const double xn = fmin(fmax((A + rin) / (B + rin + rout), 0.0), 1.0);
-            if (fabs(Rx) <= 1.0e-15 * sc || fabs(xn - x) <= 1.0e-15) {
+            const int v = h_subst_verdict(x, xn, Rx, sc, prev);
+            if (v == 1) {
                 nem = em;
                 ph = 5;
-            } else if (!(fabs(Rx) < prev) || ++k >= 8) {
+            } else if (v == 2 || ++k >= 8) {
                 ph = 1;
             } else {
                 prev = fabs(Rx);
@@ -1309,20 +1313,30 @@ __device__ __noinline__ double neutrality_ls(const SerialCascade& mc, bool act, 
 }
 
 // gas_thermal_update with metals and the bracketed solve, one leaf per
-// thread in warp lockstep (thermal_ls).  The leaf loop steps by whole warps
-// so that every lane of a warp makes the same number of trips.
+// thread in warp lockstep (thermal_ls).  Persistent warps claim chunks of 32
+// consecutive leaves of the work order (the most work first) from a global
+// counter, so every lane of a warp makes the same number of trips and a warp
+// that finishes early takes more leaves instead of idling.
 __global__ void __launch_bounds__(kBThreads) k_thermal_ls(const ThArgs a) {
     __shared__ double sh[6][kBThreads];
     const BalArgs& b = a.b;
     double mdx = 0.0, mdt = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0, s4 = 0.0;
     unsigned long long solved = 0, tpass = 0, tsums = 0, nevals = 0;
     const int lane = threadIdx.x & 31;
-    const long long stride = (long long)gridDim.x * blockDim.x;
-    for (long long base = (long long)blockIdx.x * blockDim.x + (threadIdx.x - lane); base < b.nleaf; base += stride) {
+    const long long nwarp = (long long)gridDim.x * (blockDim.x >> 5);
+    long long chunk = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    for (;; ) {
+        const long long base = chunk * 32;
+        if (base >= b.nleaf) break;
+        {   // the next chunk
+            unsigned long long c = 0;
+            if (lane == 0) c = atomicAdd(a.next, 1ull);
+            chunk = nwarp + (long long)__shfl_sync(kFull, c, 0);
+        }
         const long long i0 = base + lane;
         const bool valid = i0 < b.nleaf;
         const long long ip = valid ? i0 : b.nleaf - 1;
-        const long long il = a.order ? (long long)a.order[ip] : ip;
+        const long long il = a.order ? (long long)a.order[b.nleaf - 1 - ip] : ip;
         const double nH = b.nH[il];
         const double x0 = b.xHI[il], h10 = b.xHeI[il], h20 = b.xHeII[il], T0 = b.Te[il];
         const bool act = valid && nH > 0.0;
@@ -1514,12 +1528,13 @@ struct LeafFlow {
             const double Rx = hx * (hB + rin + rout) - (hA + rin);
             const double sc = hA + hB + fabs(hA + rin) + fabs(hB + rout);
             const double xn_ = fmin(fmax((hA + rin) / (hB + rin + rout), 0.0), 1.0);
-            if (fabs(Rx) <= 1.0e-15 * sc || fabs(xn_ - hx) <= 1.0e-15) {
+            const int v = h_subst_verdict(hx, xn_, Rx, sc, hprev);
+            if (v == 1) {
                 Sc.x = hx;
                 after_x(em, true);
                 return;
             }
-            if (!(fabs(Rx) < hprev) || ++hk >= 8) {
+            if (v == 2 || ++hk >= 8) {
                 hph = 1;
                 ask_sums(ec, 0.0);
                 return;
@@ -2128,6 +2143,7 @@ cudaError_t launch_thermal(mochii_ctx* c) {
     a.Twarm = c->twarm_set ? c->twarm : nullptr;
     a.order = nullptr;
     a.work = nullptr;
+    a.next = nullptr;
     if (c->metal.ntr > 0 && c->par.solver_warp == 1) {
         k_thermal_warp<<<c->bw.blocks, kWThreads, 0, c->stream>>>(a);
     } else if (c->metal.ntr > 0 && c->par.solver_bracketed) {
@@ -2156,7 +2172,16 @@ cudaError_t launch_thermal(mochii_ctx* c) {
             if ((e = cudaMemsetAsync(w.next, 0, sizeof(unsigned long long), c->stream)) != cudaSuccess) return e;
             k_thermal_flow<<<c->bw.blocks, kBThreads, 0, c->stream>>>(a, w.next);
         } else {
-            k_thermal_ls<<<c->bw.blocks, kBThreads, 0, c->stream>>>(a);
+            if (w.ls_blocks == 0) {   // persistent: the resident blocks of the device
+                int per = 1, sms = 148;
+                cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_thermal_ls, kBThreads, 0);
+                cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device);
+                w.ls_blocks = std::max(1, std::min(c->bw.blocks, std::max(per, 1) * sms));
+            }
+            if ((e = cudaMemsetAsync(w.next, 0, sizeof(unsigned long long), c->stream)) != cudaSuccess) return e;
+            if ((e = cudaMemsetAsync(c->bw.partial, 0, 6 * (size_t)c->bw.blocks * 8, c->stream)) != cudaSuccess) return e;
+            a.next = w.next;
+            k_thermal_ls<<<w.ls_blocks, kBThreads, 0, c->stream>>>(a);
         }
         w.have_work = true;
     } else {

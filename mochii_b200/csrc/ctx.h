@@ -84,7 +84,8 @@ struct BalanceWork {
     int* order = nullptr;             // leaves by ascending work
     void* sort_tmp = nullptr;
     size_t sort_bytes = 0;
-    unsigned long long* next = nullptr;   // the flat solve's leaf counter
+    unsigned long long* next = nullptr;   // the flat / lockstep solves' work counter
+    int ls_blocks = 0;                    // the lockstep solve's persistent grid
     bool have_work = false;
 };
 

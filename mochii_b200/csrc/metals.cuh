@@ -191,11 +191,21 @@ static __device__ __noinline__ double hydrogen_neutral_fraction(const Cas& cas, 
     return x;
 }
 
+// Verdict on one substitution step x -> xn of the warm H root with residual
+// R(x) and scale sc: 1 converged (|R| <= 1e-15 sc as the Illinois iteration
+// stops, or the step within rounding of x), 2 not contracting (|R| did not
+// fall below prev) while the step is still above 1e-12 x, 0 step on.
+__device__ __forceinline__ int h_subst_verdict(double x, double xn, double Rx, double sc, double prev) {
+    if (fabs(Rx) <= 1.0e-15 * sc || fabs(xn - x) <= 1.0e-15 || fabs(xn - x) <= 4.0e-16 * x) return 1;
+    if (!(fabs(Rx) < prev)) return fabs(xn - x) <= 1.0e-12 * x ? 1 : 2;
+    return 0;
+}
+
 // The same root from a warm start xg (the bracketed cell solve): the
 // substitution x <- (A + rin(x)) / (B + rin(x) + rout(x)), whose fixed point
 // is the root of R(x) = x (B + rin + rout) - (A + rin), while |R| falls,
-// stopping when |R| <= 1e-15 scale or the step is below 1e-15; Illinois on
-// [0, 1] when it does not settle in 8 steps.  *nem_x: the metal electrons
+// stopping on h_subst_verdict; Illinois on [0, 1] when the steps stop
+// contracting or do not settle in 8 steps.  *nem_x: the metal electrons
 // of the sums at the returned x.
 template <class Cas>
 static __device__ __noinline__ double hydrogen_neutral_fraction_warm(const Cas& cas, double nH, double ne, double A,
@@ -209,11 +219,12 @@ static __device__ __noinline__ double hydrogen_neutral_fraction_warm(const Cas& 
         const double Rx = x * (B + rin + rout) - (A + rin);
         const double scale = A + B + fabs(A + rin) + fabs(B + rout);
         const double xn = fmin(fmax((A + rin) / (B + rin + rout), 0.0), 1.0);
-        if (fabs(Rx) <= 1.0e-15 * scale || fabs(xn - x) <= 1.0e-15) {
+        const int v = h_subst_verdict(x, xn, Rx, scale, prev);
+        if (v == 1) {
             *nem_x = nem;
             return x;
         }
-        if (!(fabs(Rx) < prev)) break;   // not contracting: bracket instead
+        if (v == 2) break;   // not contracting: bracket instead
         prev = fabs(Rx);
         x = xn;
     }
