@@ -148,6 +148,10 @@ typedef struct mochii_params {
      * compensated update); 0 'compensated' = (hi, lo) FP32 pairs summed in
      * FP64 after the pass */
     int tally64;
+    /* metal rate coefficients in the thermal solve (not a reference key,
+     * par%metal_rates): 1 'table' = interpolated from a 4096-node ln T table
+     * over [te_min, te_max] (default); 0 'exact' = every evaluation direct */
+    int metal_rate_table;
 } mochii_params;
 
 /* Per-pass statistics (ion_score_report_energy_closure, ion_score_mod.f90:364-387). */

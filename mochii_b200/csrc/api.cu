@@ -84,7 +84,7 @@ void release(mochii_ctx* c) {
                     (void*)c->metal.el, c->metal.egam, c->metal.eheat, c->metal.opac, c->metal.raw,
                     (void*)c->metal.medge, c->metal.mom, c->twarm,
                     (void*)c->rec.E, c->rec.msig, c->oct_blob, c->rec.dsc, (void*)c->rec.p0,
-                    (void*)c->dust_blob, (void*)c->rhokap};
+                    (void*)c->dust_blob, (void*)c->rhokap, (void*)c->ttab};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     for (cudaEvent_t e : {c->ev0, c->ev1, c->evA, c->evB})
@@ -480,6 +480,7 @@ extern "C" int mochii_init(const mochii_params* pin, mochii_ctx** out) {
             CKI(cudaMemcpy(c->th.Ssup, th.hi_Ssup.data(), (size_t)kNlNT * kNlNNE * 8, cudaMemcpyHostToDevice));
         }
         c->thermal_ready = true;
+        if (c->metal.ntr > 0 && p.metal_rate_table) CKI(metal_ttable_build(c));
     }
     CKI(dalloc(&c->bw.partial, 6 * (size_t)c->bw.blocks));
     CKI(dalloc(&c->bw.counters, 8));

@@ -2128,6 +2128,27 @@ static BalArgs bal_args(mochii_ctx* c) {
     return a;
 }
 
+cudaError_t metal_ttable_build(mochii_ctx* c) {
+    MetalDev& m = c->metal;
+    const int nt = 4096;
+    const double u0 = log(c->par.te_min), u1 = log(c->par.te_max);
+    m.tnt = 0;
+    m.tdu = (u1 - u0) / (double)(nt - 6);
+    m.tu0 = u0 - 3.0 * m.tdu;
+    double* t = nullptr;
+    cudaError_t e = cudaMalloc(&t, (size_t)m.ntr * 4 * nt * 8);
+    if (e != cudaSuccess) return e;
+    c->ttab = t;
+    MetalDev mb = m;
+    mb.tnt = nt;
+    k_metal_ttable<<<nblocks((long long)m.ntr * 4 * nt, 256, 148 * 16), 256, 0, c->stream>>>(mb, t);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    if ((e = cudaStreamSynchronize(c->stream)) != cudaSuccess) return e;
+    m.ttab = t;
+    m.tnt = nt;
+    return cudaSuccess;
+}
+
 cudaError_t launch_balance(mochii_ctx* c) {
     const BalArgs a = bal_args(c);
     k_balance<<<c->bw.blocks, kBThreads, 0, c->stream>>>(a);

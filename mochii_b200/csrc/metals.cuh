@@ -97,14 +97,69 @@ struct MetalCache {
     double gam[kMaxTr], ci[kMaxTr], rec[kMaxTr], cxi[kMaxTr], cxr[kMaxTr];
 };
 
+// The four T-dependent coefficients of transition j at T: collisional
+// ionisation, recombination, CX ionisation, CX recombination.
+__device__ __forceinline__ double metal_coef(const MetalTr& r, int c, double T) {
+    switch (c) {
+        case 0: return voronov(T, r.ci[0], r.ci[1], r.ci[2], r.ci[3], r.ci[4]) * r.cidr;
+        case 1: return metal_alpha_rec(r, T);
+        case 2: return r.cxi_form > 0 ? metal_cx_rate(r.cxi_form, r.cxi, T) : 0.0;
+        default: return r.cxr_form > 0 ? metal_cx_rate(r.cxr_form, r.cxr, T) : 0.0;
+    }
+}
+
+// species_ne_prepare (species_mod.f90:517-536).  Inside the range of the T
+// table the coefficients come from 4-point Lagrange interpolation of their
+// logarithms in ln T (relative error ~1e-12 on the 4096-node table of the
+// thermal solve); the charge-exchange fits clamped in T (forms 6, 7) and
+// every T outside the table are evaluated directly.
 static __device__ __noinline__ void metal_prepare(const MetalDev& m, long long il, double T, MetalCache& c) {
+    int i0 = -1;
+    double w0 = 0.0, w1 = 0.0, w2 = 0.0, w3 = 0.0;
+    if (m.tnt > 0) {
+        const double s = (log(T) - m.tu0) / m.tdu;
+        const int i = (int)floor(s);
+        if (i >= 1 && i <= m.tnt - 3) {
+            const double t = s - (double)i;
+            w0 = -t * (t - 1.0) * (t - 2.0) / 6.0;
+            w1 = (t + 1.0) * (t - 1.0) * (t - 2.0) / 2.0;
+            w2 = -(t + 1.0) * t * (t - 2.0) / 2.0;
+            w3 = (t + 1.0) * t * (t - 1.0) / 6.0;
+            i0 = i - 1;
+        }
+    }
     for (int j = 0; j < m.ntr; ++j) {
         const MetalTr& r = m.tr[j];
         c.gam[j] = m.egam[il * m.ntr + j];
-        c.ci[j] = voronov(T, r.ci[0], r.ci[1], r.ci[2], r.ci[3], r.ci[4]) * r.cidr;
-        c.rec[j] = metal_alpha_rec(r, T);
-        c.cxi[j] = r.cxi_form > 0 ? metal_cx_rate(r.cxi_form, r.cxi, T) : 0.0;
-        c.cxr[j] = r.cxr_form > 0 ? metal_cx_rate(r.cxr_form, r.cxr, T) : 0.0;
+        if (i0 >= 0) {
+            const double* L = m.ttab + (size_t)j * 4 * m.tnt + i0;
+            c.ci[j] = exp(w0 * L[0] + w1 * L[1] + w2 * L[2] + w3 * L[3]);
+            L += m.tnt;
+            c.rec[j] = exp(w0 * L[0] + w1 * L[1] + w2 * L[2] + w3 * L[3]);
+            L += m.tnt;
+            c.cxi[j] = r.cxi_form <= 0 ? 0.0 : r.cxi_form >= 6 ? metal_cx_rate(r.cxi_form, r.cxi, T)
+                                                             : exp(w0 * L[0] + w1 * L[1] + w2 * L[2] + w3 * L[3]);
+            L += m.tnt;
+            c.cxr[j] = r.cxr_form <= 0 ? 0.0 : r.cxr_form >= 6 ? metal_cx_rate(r.cxr_form, r.cxr, T)
+                                                             : exp(w0 * L[0] + w1 * L[1] + w2 * L[2] + w3 * L[3]);
+        } else {
+            c.ci[j] = metal_coef(r, 0, T);
+            c.rec[j] = metal_coef(r, 1, T);
+            c.cxi[j] = metal_coef(r, 2, T);
+            c.cxr[j] = metal_coef(r, 3, T);
+        }
+    }
+}
+
+// The T table: ln max(coefficient, 1e-300) at every node.
+static __global__ void k_metal_ttable(const MetalDev m, double* out) {
+    const long long total = (long long)m.ntr * 4 * m.tnt;
+    for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < total; q += (long long)gridDim.x * blockDim.x) {
+        const int i = (int)(q % m.tnt);
+        const int c = (int)((q / m.tnt) % 4);
+        const int j = (int)(q / (4LL * m.tnt));
+        const double T = exp(m.tu0 + (double)i * m.tdu);
+        out[q] = log(fmax(metal_coef(m.tr[j], c, T), 1.0e-300));
     }
 }
 

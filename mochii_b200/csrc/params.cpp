@@ -139,6 +139,7 @@ extern "C" int mochii_params_default(mochii_params* p) {
     p->tauhomo = -999.0;
     p->solver_warp = 0;
     p->tally64 = 1;
+    p->metal_rate_table = 1;
     return MOCHII_OK;
 }
 
@@ -276,6 +277,12 @@ int set_key(mochii_params* p, std::string key, const std::vector<std::string>& v
     if (key == "ion_dust_kext") { copy_str(p->ion_dust_kext, sizeof(p->ion_dust_kext), unquote(v)); return 0; }
     if (key == "data_dir") { copy_str(p->data_dir, sizeof(p->data_dir), unquote(v)); return 0; }
     if (key == "atomic_dir") { copy_str(p->atomic_dir, sizeof(p->atomic_dir), unquote(v)); return 0; }
+    if (key == "metal_rates") {
+        const std::string s = lower(unquote(v));
+        if (s != "table" && s != "exact") return bad("must be 'table' or 'exact'");
+        p->metal_rate_table = s == "table";
+        return 0;
+    }
     if (key == "tally_precision") {
         const std::string s = lower(unquote(v));
         if (s != "compensated" && s != "fp64") return bad("must be 'compensated' or 'fp64'");

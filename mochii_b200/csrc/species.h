@@ -83,6 +83,13 @@ struct MetalDev {
     const double* mcoef = nullptr;     // (nmb*kMomDeg) x ntrp x 2
     const int* mb0 = nullptr;          // ntr, threshold order
     void* mom = nullptr;               // nleaf x nmb x kMomDeg tallies
+    // T table of the rate coefficients (thermal solve): ln of collisional
+    // ionisation, recombination, CX ionisation, CX recombination per
+    // transition on tnt nodes uniform in ln T from tu0 by tdu,
+    // ttab[(j * 4 + c) * tnt + i]; tnt == 0: exact evaluation only
+    const double* ttab = nullptr;
+    int tnt = 0;
+    double tu0 = 0.0, tdu = 0.0;
 };
 
 bool species_build(const mochii_params& p, SpeciesHost& s, std::string* err);

@@ -30,5 +30,6 @@ cudaError_t launch_columns(mochii_ctx* c);
 cudaError_t launch_metal_fractions(mochii_ctx* c, double* out);   // nleaf x nstages, registry order
 cudaError_t launch_balance(mochii_ctx* c);
 cudaError_t launch_thermal(mochii_ctx* c);
+cudaError_t metal_ttable_build(mochii_ctx* c);   // the T table of the metal rate coefficients
 
 }  // namespace mochii

@@ -127,3 +127,28 @@ def test_cell_layouts_agree():
         assert np.median(dT) < 1e-6 and dT.max() < 1.0, (other, dT.max())
         assert np.max(np.abs(out[other][1] - out["lockstep"][1])) < 1e-5
         assert abs(out[other][2] / out["lockstep"][2] - 1) < 0.01
+
+
+def test_metal_rate_table_matches_exact():
+    """The thermal solve with the interpolated T table of the metal rate
+    coefficients against every coefficient evaluated directly, on the same
+    nebula: T_e and x_HI agree to the table's interpolation error (up to
+    rate-bit differences between separate runs)."""
+    n = 16
+    nl = with_solver(configs.hii_metals(nphotons=60000, niter=2, n=n, precision="fp64", rs_factor=1.3,
+                                        diffuse=False), "bracketed")
+    out = {}
+    for mode in ("table", "exact"):
+        neb = Nebula(parse_namelist(nl.replace("/\n", f" par%metal_rates = '{mode}'\n/\n")))
+        st = partial_state(n, parse_namelist(nl).xmax)
+        for k, v in st.items():
+            neb.set(k, v)
+        neb.gas_opacity_fill()
+        for _ in range(2):
+            neb.ionizing_field_and_rates()
+            neb.gas_thermal_update()
+        out[mode] = (neb.get("T_e"), neb.get("x_HI"))
+        neb.close()
+    dT = np.abs(out["table"][0] - out["exact"][0])
+    assert np.median(dT) < 1e-6 and dT.max() < 1.0, dT.max()
+    assert np.max(np.abs(out["table"][1] - out["exact"][1])) < 1e-5
