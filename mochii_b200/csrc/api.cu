@@ -84,7 +84,8 @@ void release(mochii_ctx* c) {
                     (void*)c->metal.el, c->metal.egam, c->metal.eheat, c->metal.opac, c->metal.raw,
                     (void*)c->metal.medge, c->metal.mom, c->twarm,
                     (void*)c->rec.E, c->rec.msig, c->oct_blob, c->rec.dsc, (void*)c->rec.p0,
-                    (void*)c->dust_blob, (void*)c->rhokap, (void*)c->ttab};
+                    (void*)c->dust_blob, (void*)c->rhokap, (void*)c->ttab, (void*)c->metal_lnl,
+                    (void*)c->th.lnL};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     for (cudaEvent_t e : {c->ev0, c->ev1, c->evA, c->evB})
@@ -372,6 +373,10 @@ extern "C" int mochii_init(const mochii_params* pin, mochii_ctx** out) {
         m.lamref = reinterpret_cast<const double*>(put(sp.lamref.data(), sp.lamref.size() * 8, b_lr));
         m.Ssup = reinterpret_cast<const double*>(put(sp.Ssup.data(), sp.Ssup.size() * 8, b_ss));
         CKI(cudaGetLastError());
+        if (sp.ntab > 0) {
+            CKI(nl_log_tables(m.lamref, m.Ssup, sp.ntab, &c->metal_lnl, c->stream));
+            m.lnL = c->metal_lnl;
+        }
         CKI(dalloc(&m.egam, (size_t)n * m.ntr));
         CKI(dalloc(&m.eheat, (size_t)n * m.ntr));
         CKI(cudaMemset(m.egam, 0, (size_t)n * m.ntr * 8));
@@ -478,6 +483,7 @@ extern "C" int mochii_init(const mochii_params* pin, mochii_ctx** out) {
             CKI(dalloc(&c->th.Ssup, (size_t)kNlNT * kNlNNE));
             CKI(cudaMemcpy(c->th.lamref, th.hi_lamref.data(), kNlNT * 8, cudaMemcpyHostToDevice));
             CKI(cudaMemcpy(c->th.Ssup, th.hi_Ssup.data(), (size_t)kNlNT * kNlNNE * 8, cudaMemcpyHostToDevice));
+            CKI(nl_log_tables(c->th.lamref, c->th.Ssup, 1, &c->th.lnL, c->stream));
         }
         c->thermal_ready = true;
         if (c->metal.ntr > 0 && p.metal_rate_table) CKI(metal_ttable_build(c));

@@ -451,30 +451,80 @@ __device__ double nl_col(const double* lamref, const double* Ssup, int it, int j
     return Li * (1.0 - wt) + Lip * wt;
 }
 
-__device__ __noinline__ double nl_apply(const double* lamref, const double* Ssup, const double* tinv, double lam_fit,
-                                        double T, double ne) {
+// The (T, n_e) cell of the suppression tables, shared by every table at
+// one (T, n_e): the log-T row it and its weights, the log-n_e column.
+struct NlAt {
+    int it, je, band;   // band: 0 n_e at or below the grid, 1 above it, 2 inside
+    double w1, wt, wn;
+};
+
+__device__ __forceinline__ NlAt nl_at(const double* tinv, double T, double ne) {
+    NlAt a;
     const double lt = fmin(fmax(log10(T), 2.0), 2.0 + 0.01 * (double)(kNlNT - 1));
-    const int it = min((int)((lt - 2.0) / 0.01) + 1, kNlNT - 1);
-    const double gi = 2.0 + 0.01 * (double)(it - 1), gi1 = 2.0 + 0.01 * (double)it;
-    const double w1 = (1.0 / pow(10.0, lt) - tinv[it - 1]) / (tinv[it] - tinv[it - 1]);
-    const double wt = fmin(fmax((lt - gi) / (gi1 - gi), 0.0), 1.0);
-    const double lref = nl_col(lamref, Ssup, it, 1, w1, wt);
+    a.it = min((int)((lt - 2.0) / 0.01) + 1, kNlNT - 1);
+    const double gi = 2.0 + 0.01 * (double)(a.it - 1), gi1 = 2.0 + 0.01 * (double)a.it;
+    a.w1 = (1.0 / pow(10.0, lt) - tinv[a.it - 1]) / (tinv[a.it] - tinv[a.it - 1]);
+    a.wt = fmin(fmax((lt - gi) / (gi1 - gi), 0.0), 1.0);
     const double lne = log10(ne);
-    double lam;
+    a.je = 1;
+    a.wn = 0.0;
     if (lne <= -6.0) {
-        lam = lref;
+        a.band = 0;
     } else if (lne >= -6.0 + 0.1 * (double)(kNlNNE - 1)) {
-        lam = nl_col(lamref, Ssup, it, kNlNNE, w1, wt);
+        a.band = 1;
     } else {
-        const int je = min((int)((lne + 6.0) / 0.1) + 1, kNlNNE - 1);
-        const double gj = -6.0 + 0.1 * (double)(je - 1), gj1 = -6.0 + 0.1 * (double)je;
-        const double wn = (lne - gj) / (gj1 - gj);
-        const double L0 = nl_col(lamref, Ssup, it, je, w1, wt), L1 = nl_col(lamref, Ssup, it, je + 1, w1, wt);
-        lam = (L0 > 0.0 && L1 > 0.0) ? exp(log(L0) + wn * (log(L1) - log(L0))) : L0 * (1.0 - wn) + L1 * wn;
+        a.band = 2;
+        a.je = min((int)((lne + 6.0) / 0.1) + 1, kNlNNE - 1);
+        const double gj = -6.0 + 0.1 * (double)(a.je - 1), gj1 = -6.0 + 0.1 * (double)a.je;
+        a.wn = (lne - gj) / (gj1 - gj);
+    }
+    return a;
+}
+
+// One column of one table at the row pair of a: ln(Lambda) linear in 1/T
+// (lnL holds log(lamref * Ssup), computed once at set-up), else linear in T.
+__device__ __forceinline__ double nl_col(const double* lamref, const double* Ssup, const double* lnL, const NlAt& a,
+                                         int j) {
+    const int it = a.it;
+    const double Li = lamref[it - 1] * Ssup[(it - 1) * kNlNNE + (j - 1)];
+    const double Lip = lamref[it] * Ssup[it * kNlNNE + (j - 1)];
+    if (Li > 0.0 && Lip > 0.0) {
+        const double li = lnL[(it - 1) * kNlNNE + (j - 1)], lip = lnL[it * kNlNNE + (j - 1)];
+        return exp(li + a.w1 * (lip - li));
+    }
+    return Li * (1.0 - a.wt) + Lip * a.wt;
+}
+
+// The n-level suppression of a line-cooling fit at (T, n_e):
+// Lambda = lam_fit [f_cov S + 1 - f_cov], S = Lambda_SE(T, ne)/Lambda_SE(T, floor),
+// f_cov = min(1, Lambda_SE(T, floor)/lam_fit); ln(Lambda) linear in 1/T
+// inside a log-T cell and log-linear in log n_e (nlevel_cooling_mod.f90:163-271).
+__device__ __noinline__ double nl_apply(const double* lamref, const double* Ssup, const double* lnL, const NlAt& a,
+                                        double lam_fit) {
+    const double lref = nl_col(lamref, Ssup, lnL, a, 1);
+    double lam;
+    if (a.band == 0) {
+        lam = lref;
+    } else if (a.band == 1) {
+        lam = nl_col(lamref, Ssup, lnL, a, kNlNNE);
+    } else {
+        const double L0 = nl_col(lamref, Ssup, lnL, a, a.je), L1 = nl_col(lamref, Ssup, lnL, a, a.je + 1);
+        lam = (L0 > 0.0 && L1 > 0.0) ? exp(log(L0) + a.wn * (log(L1) - log(L0))) : L0 * (1.0 - a.wn) + L1 * a.wn;
     }
     const double S = lam / fmax(lref, kTinest);
     const double fcov = fmin(1.0, lref / fmax(lam_fit, kTinest));
     return lam_fit * (fcov * S + (1.0 - fcov));
+}
+
+// log(lamref * Ssup) of ntab tables (0 where the product is not positive).
+__global__ void k_nl_log(const double* __restrict__ lamref, const double* __restrict__ Ssup, int ntab,
+                         double* __restrict__ out) {
+    const long long total = (long long)ntab * kNlNT * kNlNNE;
+    for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < total; q += (long long)gridDim.x * blockDim.x) {
+        const long long row = q / kNlNNE;   // table * kNlNT + it
+        const double L = lamref[row] * Ssup[q];
+        out[q] = L > 0.0 ? log(L) : 0.0;
+    }
 }
 
 // cooling_total (cooling_mod.f90:240-276): recombination (Hui & Gnedin
@@ -500,7 +550,11 @@ __device__ __noinline__ double cooling_total(const ThermalDev& t, const RateSel&
     double fit = 0.0;
     for (int i = 0; i < t.hi_nterm; ++i) fit = fit + t.hi_A[i] * exp(-t.hi_T[i] / T);
     fit = fit / sqrt(T);
-    const double lam = t.use_hi_table ? nl_apply(t.lamref, t.Ssup, t.tinv, fit, T, ne) : fit;
+    double lam = fit;
+    if (t.use_hi_table) {
+        const NlAt at = nl_at(t.tinv, T, ne);
+        lam = nl_apply(t.lamref, t.Ssup, t.lnL, at, fit);
+    }
     return cool + ne * nHI * lam;
 }
 
@@ -518,6 +572,7 @@ __device__ __noinline__ MetalThermalTerms metal_thermal(const ThermalDev& td, co
     const double rsT = 1.0 / sqrt(T);
     double ff = 0.0;
     double r[kMaxSt], frac[kMaxSt];
+    const NlAt at = nl_at(td.tinv, T, ne);
     for (int ie = 0; ie < m.nel; ++ie) {
         const MetalEl e = m.el[ie];
         frac[0] = metal_chain(c, e.tr0, e.nstage, ne, nHI, nHII, r);
@@ -530,7 +585,8 @@ __device__ __noinline__ MetalThermalTerms metal_thermal(const ThermalDev& td, co
             for (int q = 0; q < st.nterm; ++q) fit = fit + st.A[q] * exp(-st.Ti[q] / T);
             fit = fit * rsT;
             const double lam = st.table >= 0 ? nl_apply(m.lamref + (size_t)st.table * kNlNT,
-                                                        m.Ssup + (size_t)st.table * kNlNT * kNlNNE, td.tinv, fit, T, ne)
+                                                        m.Ssup + (size_t)st.table * kNlNT * kNlNNE,
+                                                        m.lnL + (size_t)st.table * kNlNT * kNlNNE, at, fit)
                                              : fit;
             o.cool = o.cool + ne * nel * frac[i - 1] * lam;
         }
@@ -723,7 +779,9 @@ struct WarpCascade {
                     for (int k = 0; k < st.nterm; ++k) fit = fit + st.A[k] * exp(-st.Ti[k] / T);
                     fit = fit * rsT;
                     lam[q] = st.table >= 0 ? nl_apply(m->lamref + (size_t)st.table * kNlNT,
-                                                      m->Ssup + (size_t)st.table * kNlNT * kNlNNE, td.tinv, fit, T, ne)
+                                                      m->Ssup + (size_t)st.table * kNlNT * kNlNNE,
+                                                      m->lnL + (size_t)st.table * kNlNT * kNlNNE,
+                                                      nl_at(td.tinv, T, ne), fit)
                                            : fit;
                 }
             }
@@ -2126,6 +2184,14 @@ static BalArgs bal_args(mochii_ctx* c) {
     a.nemax = 1.0 + 2.0 * c->par.He_abund;
     for (const MetalEl& e : c->species.el) a.nemax += e.abund * (double)(e.nstage - 1);
     return a;
+}
+
+cudaError_t nl_log_tables(const double* lamref, const double* Ssup, int ntab, double** out, cudaStream_t s) {
+    cudaError_t e = cudaMalloc(out, (size_t)ntab * kNlNT * kNlNNE * 8);
+    if (e != cudaSuccess) return e;
+    k_nl_log<<<nblocks((long long)ntab * kNlNT * kNlNNE, 256, 148 * 16), 256, 0, s>>>(lamref, Ssup, ntab, *out);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    return cudaStreamSynchronize(s);
 }
 
 cudaError_t metal_ttable_build(mochii_ctx* c) {

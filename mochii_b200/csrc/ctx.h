@@ -122,6 +122,7 @@ struct mochii_ctx {
     double* dust_blob = nullptr;    // the allocation behind dust's tables
     double* rhokap = nullptr;       // ion_add_dust: grey dust opacity per leaf [1/code length]
     double* ttab = nullptr;         // metals with solve_te: the T table of the rate coefficients
+    double* metal_lnl = nullptr;    // metals: log of the n-level suppression tables
     bool xscore = false;            // dust or FUV path estimators (8 tallies per leaf)
     bool scatter = false;           // ion_dust_scatter: forced first interaction and scattered flights
     std::vector<double> lhalf;      // octree: leaf half widths (host copy for leaf_half)

@@ -74,6 +74,7 @@ struct MetalDev {
     const double* eth = nullptr;       // threshold order
     const double* lamref = nullptr;
     const double* Ssup = nullptr;
+    const double* lnL = nullptr;       // log(lamref * Ssup) per table (0 where not positive)
     double* egam = nullptr;            // nleaf x ntr, element order [s^-1]
     double* eheat = nullptr;           // nleaf x ntr, element order [erg/s]
     void* opac = nullptr;              // nleaf x ntrp (R), threshold order: n_H A_el f_it d2cm 1e-18

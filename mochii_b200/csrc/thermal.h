@@ -39,6 +39,7 @@ struct ThermalDev {
     double* lamref = nullptr;   // kNlNT
     double* Ssup = nullptr;     // kNlNT x kNlNNE
     double* tinv = nullptr;     // kNlNT: 1 / 10^logT_i
+    double* lnL = nullptr;      // kNlNT x kNlNNE: log(lamref * Ssup), 0 where not positive
     double hi_A[kMaxFitTerms], hi_T[kMaxFitTerms];
     int hi_nterm = 0, use_hi_table = 0;
 };

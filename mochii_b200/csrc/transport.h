@@ -31,5 +31,6 @@ cudaError_t launch_metal_fractions(mochii_ctx* c, double* out);   // nleaf x nst
 cudaError_t launch_balance(mochii_ctx* c);
 cudaError_t launch_thermal(mochii_ctx* c);
 cudaError_t metal_ttable_build(mochii_ctx* c);   // the T table of the metal rate coefficients
+cudaError_t nl_log_tables(const double* lamref, const double* Ssup, int ntab, double** out, cudaStream_t s);
 
 }  // namespace mochii
