@@ -223,6 +223,24 @@ int mochii_balance_update(mochii_ctx* ctx, int solve_te, mochii_metrics* m);
 /* gas_opacity_fill: refresh the per-leaf absorber columns the transport reads. */
 int mochii_opacity_fill(mochii_ctx* ctx);
 
+/* ---- batched nebulae (no reference counterpart: one job is one nebula) ------ */
+/* Several contexts on the current device advanced together.  One iteration of
+ * every nebula -- its transport pass (as mochii_transport_pass), then its
+ * balance (as mochii_balance_update with solve_te; with metals and the
+ * bracketed solver all nebulae's thermal solves run in ONE persistent launch
+ * that claims 32-leaf chunks of every nebula from one counter) -- is recorded
+ * as one CUDA graph at the first mochii_batch_iterate and replayed after.
+ * The contexts must not use the diffuse field (its packet count is read back
+ * mid-pass) or the MLP warm start; their own calls stay usable between
+ * iterations, but changing a context's parameters or tuning needs a new batch. */
+typedef struct mochii_batch mochii_batch;
+int mochii_batch_create(mochii_ctx* const* ctxs, int n, mochii_batch** out);
+/* stats[n], m[n] receive each nebula's pass statistics and balance metrics;
+ * *device_ms the device time of the whole iteration (may be NULL). */
+int mochii_batch_iterate(mochii_batch* b, int solve_te, mochii_pass_stats* stats, mochii_metrics* m,
+                         double* device_ms);
+void mochii_batch_destroy(mochii_batch* b);
+
 /* ---- autotuner: packet-block and look-ahead shapes ---------------------- */
 /* Time trial transport passes of sample_packets packets on the current
  * state for every walk variant and keep the fastest; the choice is cached

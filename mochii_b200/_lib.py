@@ -112,6 +112,9 @@ SIGNATURES = {
     "mochii_ion_Ltot": (C.c_double, [C.c_void_p]),
     "mochii_sobol_uniforms": (C.c_int, [C.c_int, C.c_int, C.c_int64, C.c_int64, C.c_int, C.c_void_p]),
     "mochii_philox_uniforms": (C.c_int, [C.c_int64, C.c_int, C.c_int64, C.c_int, C.c_int, C.c_void_p]),
+    "mochii_batch_create": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p]),
+    "mochii_batch_iterate": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "mochii_batch_destroy": (None, [C.c_void_p]),
     "mochii_walk_leaves": (C.c_int, [C.c_void_p, C.c_int64, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]),
     "mochii_launch_records": (C.c_int, [C.c_void_p, C.c_int64, C.c_int64, C.c_void_p]),
     "mochii_autotune": (C.c_int, [C.c_void_p, C.c_int64, _P(Tuning)]),

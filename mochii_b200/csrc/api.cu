@@ -505,6 +505,242 @@ extern "C" void mochii_destroy(mochii_ctx* c) {
     delete c;
 }
 
+// ---- batched nebulae -------------------------------------------------------
+struct mochii_batch {
+    std::vector<mochii_ctx*> ctx;
+    cudaStream_t s = nullptr;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    cudaGraphExec_t exec[2] = {nullptr, nullptr};   // per solve_te
+    void* tb = nullptr;                             // the batched thermal solve
+    bool batched_thermal = false;
+    // pinned host copies the graph writes each iteration
+    std::vector<double*> ledger;                    // 3 x ledger_blocks per nebula
+    std::vector<unsigned long long*> tcount;        // 4 per nebula
+    std::vector<double*> part;                      // 6 x balance blocks per nebula
+    std::vector<unsigned long long*> bcount;        // 8 per nebula
+    std::string err;
+};
+
+namespace {
+
+// One nebula's pass into stream s, without synchronisation: the tally reset,
+// the stellar transport, the rate normalisation, and copies of the ledger and
+// counters to the batch's host buffers.
+cudaError_t batch_pass(mochii_ctx* c, mochii_batch* b, int k, cudaStream_t s) {
+    const long long n = c->grid.nleaf;
+    const size_t tsz = 8;
+    cudaError_t e;
+    const cudaStream_t own = c->stream;
+    c->stream = s;
+    do {
+        if ((e = cudaMemsetAsync(c->tally, 0, (size_t)n * c->ntally * tsz, s)) != cudaSuccess) break;
+        if ((e = cudaMemsetAsync(c->jt, 0, (size_t)n * c->nnu * tsz, s)) != cudaSuccess) break;
+        if (c->metal.ntr > 0 && c->metal.nmb > 0)
+            e = cudaMemsetAsync(c->metal.mom, 0, (size_t)n * c->metal.nmb * kMomDeg * tsz, s);
+        else if (c->metal.ntr > 0)
+            e = cudaMemsetAsync(c->metal.raw, 0, (size_t)n * c->metal.ntrp * 2 * tsz, s);
+        if (e != cudaSuccess) break;
+        if ((e = cudaMemsetAsync(c->tw.counters, 0, 4 * sizeof(unsigned long long), s)) != cudaSuccess) break;
+        if ((e = launch_transport(c)) != cudaSuccess) break;
+        if ((e = launch_rates(c)) != cudaSuccess) break;
+        if ((e = cudaMemcpyAsync(b->ledger[k], c->tw.ledger, 3 * (size_t)c->tw.ledger_blocks * 8, cudaMemcpyDeviceToHost,
+                                 s)) != cudaSuccess)
+            break;
+        e = cudaMemcpyAsync(b->tcount[k], c->tw.counters, 4 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s);
+    } while (false);
+    c->stream = own;
+    return e;
+}
+
+cudaError_t batch_record(mochii_batch* b, int solve_te, cudaGraphExec_t* out) {
+    cudaError_t e = cudaStreamBeginCapture(b->s, cudaStreamCaptureModeThreadLocal);
+    if (e != cudaSuccess) return e;
+    const int n = (int)b->ctx.size();
+    for (int k = 0; k < n && e == cudaSuccess; ++k) e = batch_pass(b->ctx[k], b, k, b->s);
+    if (e == cudaSuccess) {
+        if (solve_te && b->batched_thermal) {
+            e = thermal_batch_enqueue(b->tb, b->ctx.data(), b->s);
+        } else {
+            for (int k = 0; k < n && e == cudaSuccess; ++k) {
+                mochii_ctx* c = b->ctx[k];
+                const cudaStream_t own = c->stream;
+                c->stream = b->s;
+                e = cudaMemsetAsync(c->bw.counters, 0, 8 * sizeof(unsigned long long), b->s);
+                if (e == cudaSuccess) e = solve_te ? launch_thermal(c) : launch_balance(c);
+                c->stream = own;
+            }
+        }
+    }
+    for (int k = 0; k < n && e == cudaSuccess; ++k) {
+        mochii_ctx* c = b->ctx[k];
+        e = cudaMemcpyAsync(b->part[k], c->bw.partial, 6 * (size_t)c->bw.blocks * 8, cudaMemcpyDeviceToHost, b->s);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(b->bcount[k], c->bw.counters, 8 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, b->s);
+    }
+    cudaGraph_t g = nullptr;
+    const cudaError_t ee = cudaStreamEndCapture(b->s, &g);
+    if (e == cudaSuccess) e = ee;
+    if (e == cudaSuccess) e = cudaGraphInstantiate(out, g, 0);
+    if (g) cudaGraphDestroy(g);
+    return e;
+}
+
+void batch_free(mochii_batch* b) {
+    if (!b) return;
+    if (b->s) cudaStreamSynchronize(b->s);
+    for (cudaGraphExec_t& x : b->exec)
+        if (x) cudaGraphExecDestroy(x);
+    if (b->tb) thermal_batch_destroy(b->tb);
+    for (auto* p : b->ledger) if (p) cudaFreeHost(p);
+    for (auto* p : b->tcount) if (p) cudaFreeHost(p);
+    for (auto* p : b->part) if (p) cudaFreeHost(p);
+    for (auto* p : b->bcount) if (p) cudaFreeHost(p);
+    if (b->e0) cudaEventDestroy(b->e0);
+    if (b->e1) cudaEventDestroy(b->e1);
+    if (b->s) cudaStreamDestroy(b->s);
+    delete b;
+}
+
+}  // namespace
+
+extern "C" int mochii_batch_create(mochii_ctx* const* ctxs, int n, mochii_batch** out) {
+    if (!ctxs || n < 1 || !out) return fail(nullptr, MOCHII_ERR_BAD_PARAM, "mochii_batch_create: bad argument");
+    *out = nullptr;
+    for (int k = 0; k < n; ++k) {
+        mochii_ctx* c = ctxs[k];
+        if (!c) return fail(nullptr, MOCHII_ERR_BAD_PARAM, "mochii_batch_create: null context");
+        if (c->par.diffuse_field)
+            return fail(nullptr, MOCHII_ERR_UNSUPPORTED, "batched nebulae: par%diffuse_field must be off");
+        if (c->device != ctxs[0]->device)
+            return fail(nullptr, MOCHII_ERR_BAD_PARAM, "batched nebulae: the contexts must share one device");
+    }
+    auto* b = new mochii_batch();
+    b->ctx.assign(ctxs, ctxs + n);
+    cudaError_t e = cudaStreamCreateWithFlags(&b->s, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreate(&b->e0);
+    if (e == cudaSuccess) e = cudaEventCreate(&b->e1);
+    b->ledger.assign(n, nullptr);
+    b->tcount.assign(n, nullptr);
+    b->part.assign(n, nullptr);
+    b->bcount.assign(n, nullptr);
+    for (int k = 0; k < n && e == cudaSuccess; ++k) {
+        mochii_ctx* c = ctxs[k];
+        e = cudaMallocHost(&b->ledger[k], 3 * (size_t)c->tw.ledger_blocks * 8);
+        if (e == cudaSuccess) e = cudaMallocHost(&b->tcount[k], 4 * sizeof(unsigned long long));
+        if (e == cudaSuccess) e = cudaMallocHost(&b->part[k], 6 * (size_t)c->bw.blocks * 8);
+        if (e == cudaSuccess) e = cudaMallocHost(&b->bcount[k], 8 * sizeof(unsigned long long));
+        // the state the first recorded pass reads must be on the device
+        if (e == cudaSuccess && !c->columns_fresh) {
+            e = launch_columns(c);
+            c->columns_fresh = true;
+        }
+        if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    }
+    bool all = true;
+    for (int k = 0; k < n; ++k) {
+        const mochii_ctx* c = ctxs[k];
+        all = all && c->metal.ntr > 0 && c->par.solver_bracketed && c->par.solver_warp == 0 && c->thermal_ready;
+    }
+    if (e == cudaSuccess && all) {
+        b->tb = thermal_batch_create(ctxs, n, &e);
+        b->batched_thermal = b->tb != nullptr;
+    }
+    if (e != cudaSuccess) {
+        const std::string m = std::string("mochii_batch_create: ") + cudaGetErrorString(e);
+        batch_free(b);
+        return fail(nullptr, MOCHII_ERR_CUDA, m);
+    }
+    *out = b;
+    return MOCHII_OK;
+}
+
+extern "C" int mochii_batch_iterate(mochii_batch* b, int solve_te, mochii_pass_stats* st, mochii_metrics* mm,
+                                    double* device_ms) {
+    if (!b) return MOCHII_ERR_BAD_PARAM;
+    const int n = (int)b->ctx.size();
+    const int slot = solve_te ? 1 : 0;
+    for (mochii_ctx* c : b->ctx)
+        if (solve_te && !c->thermal_ready)
+            return fail(c, MOCHII_ERR_BAD_PARAM, "the thermal solve needs par%solve_te = .true. at mochii_init");
+    cudaError_t e = cudaSuccess;
+    for (mochii_ctx* c : b->ctx) {   // the contexts' own work first
+        if (!c->columns_fresh) {
+            e = launch_columns(c);
+            c->columns_fresh = true;
+        }
+        if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+        if (e != cudaSuccess) return fail(c, MOCHII_ERR_CUDA, cudaGetErrorString(e));
+    }
+    if (!b->exec[slot] && (e = batch_record(b, solve_te, &b->exec[slot])) != cudaSuccess) {
+        cudaGetLastError();
+        return fail(nullptr, MOCHII_ERR_CUDA, std::string("recording the batch graph: ") + cudaGetErrorString(e));
+    }
+    e = cudaEventRecord(b->e0, b->s);
+    if (e == cudaSuccess) e = cudaGraphLaunch(b->exec[slot], b->s);
+    if (e == cudaSuccess) e = cudaEventRecord(b->e1, b->s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(b->s);
+    if (e != cudaSuccess) return fail(nullptr, MOCHII_ERR_CUDA, cudaGetErrorString(e));
+    float ms = 0.0f;
+    cudaEventElapsedTime(&ms, b->e0, b->e1);
+    if (device_ms) *device_ms = ms;
+    int status = MOCHII_OK;
+    for (int k = 0; k < n; ++k) {
+        mochii_ctx* c = b->ctx[k];
+        c->columns_fresh = true;
+        mochii_pass_stats s;
+        std::memset(&s, 0, sizeof(s));
+        long double en[3] = {0, 0, 0};
+        for (int q = 0; q < c->tw.ledger_blocks; ++q)
+            for (int j = 0; j < 3; ++j) en[j] += (long double)b->ledger[k][3 * (size_t)q + j];
+        s.energy_emitted = (double)en[0];
+        s.energy_absorbed = (double)en[1];
+        s.energy_escaped = (double)en[2];
+        s.closure = std::fabs(s.energy_absorbed + s.energy_escaped - s.energy_emitted) / std::max(s.energy_emitted, kTinest);
+        s.direct_segments = (int64_t)b->tcount[k][0];
+        s.walk_kills = (int64_t)b->tcount[k][1];
+        s.metal_active = (int64_t)b->tcount[k][2];
+        s.scattered_segments = (int64_t)b->tcount[k][3];
+        s.packets = c->par.nphotons;
+        if (st) st[k] = s;
+        mochii_metrics r;
+        std::memset(&r, 0, sizeof(r));
+        const double* q = b->part[k];
+        if (solve_te) {
+            double sm[4] = {0, 0, 0, 0};
+            for (int bl = 0; bl < c->bw.blocks; ++bl) {
+                r.max_dx = std::max(r.max_dx, q[6 * (size_t)bl]);
+                r.max_dte = std::max(r.max_dte, q[6 * (size_t)bl + 1]);
+                for (int j = 0; j < 4; ++j) sm[j] += q[6 * (size_t)bl + 2 + j];
+            }
+            r.dx_vol = sm[0] / std::max(sm[1], kTinest);
+            r.dte_vol = sm[2] / std::max(sm[3], kTinest);
+        } else {
+            double sdx = 0.0, sx = 0.0;
+            for (int bl = 0; bl < c->bw.blocks; ++bl) {
+                r.max_dx = std::max(r.max_dx, q[3 * (size_t)bl]);
+                sdx += q[3 * (size_t)bl + 1];
+                sx += q[3 * (size_t)bl + 2];
+            }
+            r.dx_vol = sdx / std::max(sx, kTinest);
+        }
+        const unsigned long long* cnt = b->bcount[k];
+        r.cells_solved = (int64_t)cnt[0];
+        r.fixed_point_cap_hits = (int64_t)cnt[1];
+        r.fixed_point_passes = (int64_t)cnt[2];
+        r.metal_sum_calls = (int64_t)cnt[3];
+        r.rate_evaluations = (int64_t)cnt[4];
+        if (mm) mm[k] = r;
+        if (!std::isfinite(s.energy_emitted) || !std::isfinite(s.energy_absorbed)) {
+            status = fail(c, MOCHII_ERR_NONFINITE, "non-finite energy ledger");
+        } else if (s.closure > 5.0e-13) {
+            status = fail(c, MOCHII_ERR_CLOSURE, "energy closure exceeds 5e-13");
+        }
+    }
+    return status;
+}
+
+extern "C" void mochii_batch_destroy(mochii_batch* b) { batch_free(b); }
+
 extern "C" int64_t mochii_nleaf(const mochii_ctx* c) { return c ? c->grid.nleaf : 0; }
 extern "C" int mochii_metal_shape(const mochii_ctx* c, int* ntransitions, int* nstages) {
     if (!c) return MOCHII_ERR_BAD_PARAM;

@@ -1375,15 +1375,76 @@ __device__ __noinline__ double neutrality_ls(const SerialCascade& mc, bool act, 
 // consecutive leaves of the work order (the most work first) from a global
 // counter, so every lane of a warp makes the same number of trips and a warp
 // that finishes early takes more leaves instead of idling.
+// The per-lane sums a thermal kernel reports (thermal_mod.f90:223-224 and the
+// solver counters).
+struct ThermalAcc {
+    double mdx = 0.0, mdt = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0, s4 = 0.0;
+    unsigned long long solved = 0, tpass = 0, tsums = 0, nevals = 0;
+};
+
+// One warp's 32 leaves at positions base .. base+31 of a's order, in lockstep.
+__device__ __forceinline__ void thermal_chunk_ls(const ThArgs& a, long long base, int lane, ThermalAcc& acc) {
+    const BalArgs& b = a.b;
+    const long long i0 = base + lane;
+    const bool valid = i0 < b.nleaf;
+    const long long ip = valid ? i0 : b.nleaf - 1;
+    const long long il = a.order ? (long long)a.order[b.nleaf - 1 - ip] : ip;
+    const double nH = b.nH[il];
+    const double x0 = b.xHI[il], h10 = b.xHeI[il], h20 = b.xHeII[il], T0 = b.Te[il];
+    const bool act = valid && nH > 0.0;
+    if (valid && !act) {
+        b.ne[il] = 0.0;
+        write_columns(b.col, il, b.nabs, b.fp32, nH, b.yHe, x0, h10, h20, b.colscale,
+                      b.rhokap ? b.rhokap[il] : 0.0);
+        if (a.work) a.work[il] = 0u;
+    }
+    double xHI = x0, xHeI = h10, xHeII = h20, ne = b.ne[il];
+    int passes = 0, nsum = 0, nev = 0;
+    SerialCascade mc;
+    mc.m = &b.m;
+    const double te = thermal_ls(a, il, act, nH, xHI, xHeI, xHeII, ne, &passes, mc, &nsum, &nev,
+                                 a.Twarm ? a.Twarm[il] : T0);
+    const double w = b.relax;
+    const double xn = (1.0 - w) * x0 + w * xHI;
+    const double h1n = (1.0 - w) * h10 + w * xHeI;
+    const double h2n = (1.0 - w) * h20 + w * xHeII;
+    const double h3n = fmax(0.0, 1.0 - h1n - h2n);
+    double nen = nH * ((1.0 - xn) + b.yHe * (h2n + 2.0 * h3n));
+    // written state at te (thermal_mod.f90:191-203); the cache is at te from
+    // the final net_rate
+    if (b.metal_ne) nen = neutrality_ls(mc, act, nH, nen, xn, ne);
+    if (!act) return;
+    if (b.fp32) mc.opacity_fill<float>(il, nH, nen, xn, b.colscale);
+    else mc.opacity_fill<double>(il, nH, nen, xn, b.colscale);
+    ++acc.solved;
+    acc.tpass += (unsigned long long)passes;
+    acc.tsums += (unsigned long long)nsum;
+    acc.nevals += (unsigned long long)nev;
+    if (a.work) a.work[il] = (unsigned)min(nsum, 65535);
+    b.xHI[il] = xn;
+    b.xHeI[il] = h1n;
+    b.xHeII[il] = h2n;
+    b.ne[il] = nen;
+    b.Te[il] = te;
+    write_columns(b.col, il, b.nabs, b.fp32, nH, b.yHe, xn, h1n, h2n, b.colscale, b.rhokap ? b.rhokap[il] : 0.0);
+    const double dx = fabs(xn - x0);
+    acc.mdx = fmax(acc.mdx, dx);
+    acc.mdt = fmax(acc.mdt, fabs(te - T0) / T0);
+    const double vol = leaf_vol(b, il);
+    acc.s1 = acc.s1 + vol * dx;
+    acc.s2 = acc.s2 + vol * (1.0 - xn);
+    acc.s3 = acc.s3 + vol * nen * fabs(te - T0);
+    acc.s4 = acc.s4 + vol * nen * te;
+}
+
 __global__ void __launch_bounds__(kBThreads) k_thermal_ls(const ThArgs a) {
     __shared__ double sh[6][kBThreads];
     const BalArgs& b = a.b;
-    double mdx = 0.0, mdt = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0, s4 = 0.0;
-    unsigned long long solved = 0, tpass = 0, tsums = 0, nevals = 0;
+    ThermalAcc acc;
     const int lane = threadIdx.x & 31;
     const long long nwarp = (long long)gridDim.x * (blockDim.x >> 5);
     long long chunk = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-    for (;; ) {
+    for (;;) {
         const long long base = chunk * 32;
         if (base >= b.nleaf) break;
         {   // the next chunk
@@ -1391,59 +1452,10 @@ __global__ void __launch_bounds__(kBThreads) k_thermal_ls(const ThArgs a) {
             if (lane == 0) c = atomicAdd(a.next, 1ull);
             chunk = nwarp + (long long)__shfl_sync(kFull, c, 0);
         }
-        const long long i0 = base + lane;
-        const bool valid = i0 < b.nleaf;
-        const long long ip = valid ? i0 : b.nleaf - 1;
-        const long long il = a.order ? (long long)a.order[b.nleaf - 1 - ip] : ip;
-        const double nH = b.nH[il];
-        const double x0 = b.xHI[il], h10 = b.xHeI[il], h20 = b.xHeII[il], T0 = b.Te[il];
-        const bool act = valid && nH > 0.0;
-        if (valid && !act) {
-            b.ne[il] = 0.0;
-            write_columns(b.col, il, b.nabs, b.fp32, nH, b.yHe, x0, h10, h20, b.colscale,
-                          b.rhokap ? b.rhokap[il] : 0.0);
-            if (a.work) a.work[il] = 0u;
-        }
-        double xHI = x0, xHeI = h10, xHeII = h20, ne = b.ne[il];
-        int passes = 0, nsum = 0, nev = 0;
-        SerialCascade mc;
-        mc.m = &b.m;
-        const double te = thermal_ls(a, il, act, nH, xHI, xHeI, xHeII, ne, &passes, mc, &nsum, &nev,
-                                     a.Twarm ? a.Twarm[il] : T0);
-        const double w = b.relax;
-        const double xn = (1.0 - w) * x0 + w * xHI;
-        const double h1n = (1.0 - w) * h10 + w * xHeI;
-        const double h2n = (1.0 - w) * h20 + w * xHeII;
-        const double h3n = fmax(0.0, 1.0 - h1n - h2n);
-        double nen = nH * ((1.0 - xn) + b.yHe * (h2n + 2.0 * h3n));
-        // written state at te (thermal_mod.f90:191-203); the cache is at te
-        // from the final net_rate
-        if (b.metal_ne) nen = neutrality_ls(mc, act, nH, nen, xn, ne);
-        if (!act) continue;
-        if (b.fp32) mc.opacity_fill<float>(il, nH, nen, xn, b.colscale);
-        else mc.opacity_fill<double>(il, nH, nen, xn, b.colscale);
-        ++solved;
-        tpass += (unsigned long long)passes;
-        tsums += (unsigned long long)nsum;
-        nevals += (unsigned long long)nev;
-        if (a.work) a.work[il] = (unsigned)min(nsum, 65535);
-        b.xHI[il] = xn;
-        b.xHeI[il] = h1n;
-        b.xHeII[il] = h2n;
-        b.ne[il] = nen;
-        b.Te[il] = te;
-        write_columns(b.col, il, b.nabs, b.fp32, nH, b.yHe, xn, h1n, h2n, b.colscale, b.rhokap ? b.rhokap[il] : 0.0);
-        const double dx = fabs(xn - x0);
-        mdx = fmax(mdx, dx);
-        mdt = fmax(mdt, fabs(te - T0) / T0);
-        const double vol = leaf_vol(b, il);
-        s1 = s1 + vol * dx;
-        s2 = s2 + vol * (1.0 - xn);
-        s3 = s3 + vol * nen * fabs(te - T0);
-        s4 = s4 + vol * nen * te;
+        thermal_chunk_ls(a, base, lane, acc);
     }
     const int t = threadIdx.x;
-    sh[0][t] = mdx; sh[1][t] = mdt; sh[2][t] = s1; sh[3][t] = s2; sh[4][t] = s3; sh[5][t] = s4;
+    sh[0][t] = acc.mdx; sh[1][t] = acc.mdt; sh[2][t] = acc.s1; sh[3][t] = acc.s2; sh[4][t] = acc.s3; sh[5][t] = acc.s4;
     __syncthreads();
     for (int s = blockDim.x / 2; s > 0; s >>= 1) {
         if (t < s) {
@@ -1455,6 +1467,7 @@ __global__ void __launch_bounds__(kBThreads) k_thermal_ls(const ThArgs a) {
     }
     if (t == 0)
         for (int k = 0; k < 6; ++k) b.partial[6 * blockIdx.x + k] = sh[k][0];
+    unsigned long long solved = acc.solved, tpass = acc.tpass, tsums = acc.tsums, nevals = acc.nevals;
     for (int o = 16; o > 0; o >>= 1) {
         solved += __shfl_down_sync(kFull, solved, o);
         tpass += __shfl_down_sync(kFull, tpass, o);
@@ -1467,6 +1480,77 @@ __global__ void __launch_bounds__(kBThreads) k_thermal_ls(const ThArgs a) {
         if (tsums) atomicAdd(b.counters + 3, tsums);
         if (nevals) atomicAdd(b.counters + 4, nevals);
     }
+}
+
+// A warp's sums into its nebula's first partial slot and counters (the
+// values are non-negative, so their bit patterns order as the numbers).
+__device__ __forceinline__ void thermal_acc_flush(const BalArgs& b, ThermalAcc& acc) {
+    double v[6] = {acc.mdx, acc.mdt, acc.s1, acc.s2, acc.s3, acc.s4};
+    unsigned long long c[4] = {acc.solved, acc.tpass, acc.tsums, acc.nevals};
+    for (int o = 16; o > 0; o >>= 1) {
+        v[0] = fmax(v[0], __shfl_down_sync(kFull, v[0], o));
+        v[1] = fmax(v[1], __shfl_down_sync(kFull, v[1], o));
+        for (int k = 2; k < 6; ++k) v[k] += __shfl_down_sync(kFull, v[k], o);
+        for (int k = 0; k < 4; ++k) c[k] += __shfl_down_sync(kFull, c[k], o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        unsigned long long* pm = reinterpret_cast<unsigned long long*>(b.partial);
+        atomicMax(pm + 0, (unsigned long long)__double_as_longlong(v[0]));
+        atomicMax(pm + 1, (unsigned long long)__double_as_longlong(v[1]));
+        for (int k = 2; k < 6; ++k) atomicAdd(b.partial + k, v[k]);
+        if (c[0]) atomicAdd(b.counters + 0, c[0]);
+        if (c[1]) atomicAdd(b.counters + 2, c[1]);
+        if (c[2]) atomicAdd(b.counters + 3, c[2]);
+        if (c[3]) atomicAdd(b.counters + 4, c[3]);
+    }
+    acc = ThermalAcc();
+}
+
+// The lockstep thermal solve of many nebulae in one persistent launch: the
+// 32-leaf chunks of all nebulae are numbered consecutively (chunk_off: the
+// first chunk of each nebula, nneb + 1 entries) and claimed from one counter;
+// a warp copies its nebula's arguments into shared memory and reports its
+// sums to that nebula when it moves to another one or ends.
+__global__ void __launch_bounds__(kBThreads) k_thermal_batch(const ThArgs* __restrict__ args, int nneb,
+                                                             const long long* __restrict__ chunk_off,
+                                                             unsigned long long* next) {
+    __shared__ ThArgs sa[kBThreads / 32];
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    const long long total = chunk_off[nneb];
+    const long long nwarp = (long long)gridDim.x * (blockDim.x >> 5);
+    long long chunk = (long long)blockIdx.x * (blockDim.x >> 5) + wib;
+    int cur = -1;
+    ThermalAcc acc;
+    for (;;) {
+        if (chunk >= total) break;
+        int k = 0;   // the nebula of this chunk
+        {
+            int lo = 0, hi = nneb - 1;
+            while (lo < hi) {
+                const int mid = (lo + hi + 1) >> 1;
+                if (chunk_off[mid] <= chunk) lo = mid; else hi = mid - 1;
+            }
+            k = lo;
+        }
+        if (k != cur) {
+            if (cur >= 0) thermal_acc_flush(sa[wib].b, acc);
+            __syncwarp();
+            const int nw = (int)(sizeof(ThArgs) / 4);
+            const unsigned* src = reinterpret_cast<const unsigned*>(args + k);
+            unsigned* dst = reinterpret_cast<unsigned*>(sa + wib);
+            for (int q = lane; q < nw; q += 32) dst[q] = src[q];
+            __syncwarp();
+            cur = k;
+        }
+        const long long base = (chunk - chunk_off[k]) * 32;
+        {
+            unsigned long long c = 0;
+            if (lane == 0) c = atomicAdd(next, 1ull);
+            chunk = nwarp + (long long)__shfl_sync(kFull, c, 0);
+        }
+        thermal_chunk_ls(sa[wib], base, lane, acc);
+    }
+    if (cur >= 0) thermal_acc_flush(sa[wib].b, acc);
 }
 
 // ---- the bracketed thermal solve as one flat per-lane state machine ---------
@@ -2221,6 +2305,100 @@ cudaError_t launch_balance(mochii_ctx* c) {
     return cudaGetLastError();
 }
 
+// The work-order buffers of the lockstep solve (sorted leaves, chunk counter).
+cudaError_t thermal_work_alloc(mochii_ctx* c) {
+    BalanceWork& w = c->bw;
+    const int n = (int)c->grid.nleaf;
+    cudaError_t e;
+    if ((e = cudaMalloc(&w.work, (size_t)n * 4)) != cudaSuccess) return e;
+    if ((e = cudaMalloc(&w.work_sorted, (size_t)n * 4)) != cudaSuccess) return e;
+    if ((e = cudaMalloc(&w.iota, (size_t)n * 4)) != cudaSuccess) return e;
+    if ((e = cudaMalloc(&w.order, (size_t)n * 4)) != cudaSuccess) return e;
+    if ((e = cudaMalloc(&w.next, sizeof(unsigned long long))) != cudaSuccess) return e;
+    cub::DeviceRadixSort::SortPairs(nullptr, w.sort_bytes, w.work, w.work_sorted, w.iota, w.order, n, 0, 16);
+    if ((e = cudaMalloc(&w.sort_tmp, w.sort_bytes)) != cudaSuccess) return e;
+    k_iota<<<nblocks(n, 256, 148 * 16), 256, 0, c->stream>>>(w.iota, n);
+    w.have_work = false;
+    return cudaGetLastError();
+}
+
+// ---- batched nebulae --------------------------------------------------------
+struct ThermalBatch {
+    ThArgs* d_args = nullptr;
+    long long* d_off = nullptr;
+    unsigned long long* d_next = nullptr;
+    int n = 0, blocks = 0;
+};
+
+void* thermal_batch_create(mochii_ctx* const* cs, int n, cudaError_t* err) {
+    *err = cudaSuccess;
+    auto* tb = new ThermalBatch();
+    tb->n = n;
+    std::vector<ThArgs> args(n);
+    std::vector<long long> off(n + 1, 0);
+    for (int k = 0; k < n; ++k) {
+        mochii_ctx* c = cs[k];
+        if (!c->bw.work && (*err = thermal_work_alloc(c)) != cudaSuccess) break;
+        // a zero work array sorts to a valid order: the graph always sorts
+        if ((*err = cudaMemsetAsync(c->bw.work, 0, (size_t)c->grid.nleaf * 4, c->stream)) != cudaSuccess) break;
+        c->bw.have_work = true;
+        ThArgs& a = args[k];
+        a.b = bal_args(c);
+        a.td = c->th;
+        a.te_min = c->par.te_min;
+        a.te_max = c->par.te_max;
+        a.Twarm = nullptr;
+        a.order = c->bw.order;
+        a.work = c->bw.work;
+        a.next = nullptr;
+        off[k + 1] = off[k] + (c->grid.nleaf + 31) / 32;
+        if ((*err = cudaStreamSynchronize(c->stream)) != cudaSuccess) break;
+    }
+    if (*err == cudaSuccess) *err = cudaMalloc(&tb->d_args, sizeof(ThArgs) * n);
+    if (*err == cudaSuccess) *err = cudaMalloc(&tb->d_off, sizeof(long long) * (n + 1));
+    if (*err == cudaSuccess) *err = cudaMalloc(&tb->d_next, sizeof(unsigned long long));
+    if (*err == cudaSuccess) *err = cudaMemcpy(tb->d_args, args.data(), sizeof(ThArgs) * n, cudaMemcpyHostToDevice);
+    if (*err == cudaSuccess) *err = cudaMemcpy(tb->d_off, off.data(), sizeof(long long) * (n + 1), cudaMemcpyHostToDevice);
+    if (*err == cudaSuccess) {
+        int per = 1, sms = 148;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_thermal_batch, kBThreads, 0);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, cs[0]->device);
+        tb->blocks = std::max(1, per) * sms;
+    }
+    if (*err != cudaSuccess) {
+        thermal_batch_destroy(tb);
+        return nullptr;
+    }
+    return tb;
+}
+
+void thermal_batch_destroy(void* p) {
+    auto* tb = static_cast<ThermalBatch*>(p);
+    if (!tb) return;
+    for (void* q : {(void*)tb->d_args, (void*)tb->d_off, (void*)tb->d_next})
+        if (q) cudaFree(q);
+    delete tb;
+}
+
+// One batched thermal update on stream s: each nebula's leaves sorted by
+// their last work and its sums cleared, then one persistent launch.
+cudaError_t thermal_batch_enqueue(void* p, mochii_ctx* const* cs, cudaStream_t s) {
+    auto* tb = static_cast<ThermalBatch*>(p);
+    cudaError_t e;
+    for (int k = 0; k < tb->n; ++k) {
+        mochii_ctx* c = cs[k];
+        BalanceWork& w = c->bw;
+        const int n = (int)c->grid.nleaf;
+        if ((e = cudaMemsetAsync(w.counters, 0, 8 * sizeof(unsigned long long), s)) != cudaSuccess) return e;
+        if ((e = cudaMemsetAsync(w.partial, 0, 6 * (size_t)w.blocks * 8, s)) != cudaSuccess) return e;
+        e = cub::DeviceRadixSort::SortPairs(w.sort_tmp, w.sort_bytes, w.work, w.work_sorted, w.iota, w.order, n, 0, 16, s);
+        if (e != cudaSuccess) return e;
+    }
+    if ((e = cudaMemsetAsync(tb->d_next, 0, sizeof(unsigned long long), s)) != cudaSuccess) return e;
+    k_thermal_batch<<<tb->blocks, kBThreads, 0, s>>>(tb->d_args, tb->n, tb->d_off, tb->d_next);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_thermal(mochii_ctx* c) {
     ThArgs a;
     a.b = bal_args(c);
@@ -2237,17 +2415,7 @@ cudaError_t launch_thermal(mochii_ctx* c) {
         BalanceWork& w = c->bw;
         const int n = (int)c->grid.nleaf;
         cudaError_t e;
-        if (!w.work) {
-            if ((e = cudaMalloc(&w.work, (size_t)n * 4)) != cudaSuccess) return e;
-            if ((e = cudaMalloc(&w.work_sorted, (size_t)n * 4)) != cudaSuccess) return e;
-            if ((e = cudaMalloc(&w.iota, (size_t)n * 4)) != cudaSuccess) return e;
-            if ((e = cudaMalloc(&w.order, (size_t)n * 4)) != cudaSuccess) return e;
-            if ((e = cudaMalloc(&w.next, sizeof(unsigned long long))) != cudaSuccess) return e;
-            cub::DeviceRadixSort::SortPairs(nullptr, w.sort_bytes, w.work, w.work_sorted, w.iota, w.order, n, 0, 16);
-            if ((e = cudaMalloc(&w.sort_tmp, w.sort_bytes)) != cudaSuccess) return e;
-            k_iota<<<nblocks(n, 256, 148 * 16), 256, 0, c->stream>>>(w.iota, n);
-            w.have_work = false;
-        }
+        if (!w.work && (e = thermal_work_alloc(c)) != cudaSuccess) return e;
         if (w.have_work) {
             e = cub::DeviceRadixSort::SortPairs(w.sort_tmp, w.sort_bytes, w.work, w.work_sorted, w.iota, w.order, n, 0,
                                                 16, c->stream);

@@ -32,5 +32,10 @@ cudaError_t launch_balance(mochii_ctx* c);
 cudaError_t launch_thermal(mochii_ctx* c);
 cudaError_t metal_ttable_build(mochii_ctx* c);   // the T table of the metal rate coefficients
 cudaError_t nl_log_tables(const double* lamref, const double* Ssup, int ntab, double** out, cudaStream_t s);
+cudaError_t thermal_work_alloc(mochii_ctx* c);
+// batched nebulae: the one-launch lockstep thermal solve of several contexts
+void* thermal_batch_create(mochii_ctx* const* cs, int n, cudaError_t* err);
+void thermal_batch_destroy(void* tb);
+cudaError_t thermal_batch_enqueue(void* tb, mochii_ctx* const* cs, cudaStream_t s);
 
 }  // namespace mochii

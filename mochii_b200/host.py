@@ -250,3 +250,45 @@ def run(par, log=None, final_pass=True):
     if final_pass and par.gas_niter >= 1:
         neb.ionizing_field_and_rates()   # final consistency pass, main.f90:225
     return neb, history
+
+
+class Batch:
+    """Several nebulae on one device advanced together (mochii_batch_*): one
+    iteration of every nebula -- transport pass, then balance -- recorded as
+    one CUDA graph at the first call and replayed; with metals and the
+    bracketed solver the thermal solves of all nebulae run in one persistent
+    launch.  The nebulae stay usable on their own between iterations."""
+
+    def __init__(self, nebulae):
+        self.lib = _lib.load()
+        self.nebulae = list(nebulae)
+        n = len(self.nebulae)
+        arr = (C.c_void_p * n)(*[neb.ctx for neb in self.nebulae])
+        h = C.c_void_p()
+        rc = self.lib.mochii_batch_create(arr, n, C.byref(h))
+        _check(self.lib, rc)
+        self.h = h
+
+    def iterate(self, solve_te=True):
+        """One iteration of every nebula: (pass statistics, balance metrics,
+        device milliseconds of the whole batch)."""
+        n = len(self.nebulae)
+        st = (PassStats * n)()
+        m = (Metrics * n)()
+        ms = C.c_double()
+        rc = self.lib.mochii_batch_iterate(self.h, int(bool(solve_te)), st, m, C.byref(ms))
+        _check(self.lib, rc)
+        for neb, mm in zip(self.nebulae, m):
+            neb.last_metrics = mm
+        return list(st), list(m), ms.value
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.mochii_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -1,0 +1,62 @@
+"""Batched nebulae (mochii_batch_*): several H II regions of different grid
+sizes advanced together, one iteration recorded as one CUDA graph and
+replayed, the thermal solves of all nebulae in one persistent launch.  Each
+nebula's iteration equals its own standalone iteration (the transport tallies
+are atomic sums in another order, so rates agree to 1e-12 and the solved
+states to the balance's rounding), energy closure holds per nebula, and the
+graph replays."""
+import numpy as np
+import pytest
+
+from mochii_b200 import Batch, Nebula, MochiiError, configs, parse_namelist
+
+pytestmark = pytest.mark.gpu
+
+
+def nebulae(sizes, solve_te=True):
+    out = []
+    for k, n in enumerate(sizes):
+        nl = configs.hii_metals(nphotons=30000 + 10000 * k, niter=3, n=n, precision="fp64", rs_factor=1.2 + 0.1 * k,
+                                diffuse=False, solve_te=solve_te)
+        out.append(Nebula(parse_namelist(nl)))
+    return out
+
+
+@pytest.mark.parametrize("solve_te", [True, False])
+def test_batch_iteration_equals_standalone(solve_te):
+    sizes = (12, 16, 20)
+    alone = nebulae(sizes, solve_te)
+    together = nebulae(sizes, solve_te)
+    batch = Batch(together)
+    for it in range(3):
+        st, m, ms = batch.iterate(solve_te=solve_te)
+        assert ms > 0
+        for k, neb in enumerate(alone):
+            s1 = neb.ionizing_field_and_rates()
+            if solve_te:
+                neb.gas_thermal_update()
+            else:
+                neb.gas_equilibrium_update()
+            m1 = neb.last_metrics
+            assert st[k].closure <= 5e-13
+            assert abs(st[k].energy_absorbed / s1.energy_absorbed - 1) < 1e-12
+            assert st[k].direct_segments == s1.direct_segments
+            g_b, g_a = together[k].get("gamma_HI"), neb.get("gamma_HI")
+            big = g_a > 1e-12 * g_a.max()
+            assert np.max(np.abs(g_b[big] / g_a[big] - 1)) < 1e-9
+            dT = np.abs(together[k].get("T_e") - neb.get("T_e"))
+            assert np.median(dT) < 1e-6 and dT.max() < 1.0, (it, k, dT.max())
+            assert np.max(np.abs(together[k].get("x_HI") - neb.get("x_HI"))) < 1e-5
+            assert m[k].cells_solved == m1.cells_solved
+    batch.close()
+    for neb in alone + together:
+        neb.close()
+
+
+def test_batch_refuses_the_diffuse_field():
+    nl = configs.hii_metals(nphotons=10000, niter=1, n=8, precision="fp64", diffuse=True)
+    neb = Nebula(parse_namelist(nl))
+    with pytest.raises(MochiiError) as ei:
+        Batch([neb])
+    assert ei.value.status == 8
+    neb.close()
