@@ -25,6 +25,13 @@ Workloads (--workload):
                  with <cos> = 0.6 and scattering, FUV band from 6 eV, T_e
                  solved (H + He), 3e7 packets per pass, FP32 segments.  The
                  leaf list is generated once into the temp directory.
+  batch64        64 independent H II regions advanced together (the batch
+                 API: one CUDA graph per iteration, one persistent thermal
+                 launch for all): seeded cubic grids of 32^3..128^3, n_H
+                 log-uniform in 10-1000, T_eff 30-50 kK, Q(H) 1e48-1e50,
+                 He/H 0.1 and the eleven metals, case A, 2e6 packets per
+                 instance per iteration, T_e solved, FP32 segments.  A step
+                 is one iteration of all 64.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--workload W] [--impl reference]
 
@@ -96,8 +103,20 @@ class Workload:
             self.default_precision = "fp32"
             self.make = lambda nphot, prec, seed: configs.clumpy_dusty(cases, nphotons=nphot, precision=prec,
                                                                         qmc_seed=seed)
+        elif name == "batch64":
+            self.grid, self.nphot, self.thermal, self.prep = None, packets or 2_000_000, True, 0
+            self.default_precision = "fp32"
+            self.count = 64
+            self.make = None   # one namelist per instance: instances()
         else:
             raise SystemExit(f"unknown workload {name}")
+
+    def instances(self, prec, extra=""):
+        """batch64: the instances' namelists (with extra keys) and their
+        (n, n_H, T_eff, Q) parameters."""
+        from mochii_b200 import configs
+        nls, par = configs.batch_instances(count=self.count, nphotons=self.nphot, precision=prec)
+        return [nl.replace("/\n", extra + "/\n") for nl in nls], par
 
     def balance(self, neb):
         return neb.gas_thermal_update() if self.thermal else neb.gas_equilibrium_update()
@@ -111,6 +130,8 @@ def bytes_per_segment(wl, precision):
         return w * 2 + 16 * 3          # n_H, x_HI; Gamma_HI, H_HI, jt_ion
     if wl.name == "clumpy_dusty":
         return w * 5 + 16 * 9          # n_H, x_HI, x_HeI, x_HeII, rhokap; 6 H/He + jt_ion + dust_abs + FUV
+    if wl.name == "batch64":
+        return w * 4 + 16 * 7          # n_H, x_HI, x_HeI, x_HeII; 6 H/He + jt_ion (metal words per segment)
     return w * 4 + 16 * (7 + 6)        # n_H, x_HI, x_HeI, x_HeII; 6 H/He + jt_ion + 6 metal moments
 
 
@@ -200,8 +221,9 @@ def cpu_threads(wl):
         mem = os.sysconf("SC_PAGE_SIZE") * os.sysconf("SC_PHYS_PAGES")
     except (ValueError, OSError):
         mem = 64 << 30
-    nleaf = wl.grid ** 3 if wl.grid else 3_100_000
-    per = nleaf * 8 * (6 + 16 + (2 * 32 if wl.name == "hii_metals128" else 0) + (2 if wl.name == "clumpy_dusty" else 0))
+    nleaf = wl.grid ** 3 if wl.grid else (128 ** 3 if wl.name == "batch64" else 3_100_000)
+    metals = wl.name in ("hii_metals128", "batch64")
+    per = nleaf * 8 * (6 + 16 + (2 * 32 if metals else 0) + (2 if wl.name == "clumpy_dusty" else 0))
     return max(1, min(n, int(0.5 * mem // max(per, 1))))
 
 
@@ -250,6 +272,48 @@ def cpu_reference(wl, state, nthreads, budget_s=20.0):
     desc = (f"transport passes of {sample} and {2 * sample} stellar packets (per-packet time scaled to "
             f"{wl.nphot}, plus the per-pass fixed cost) + {what}, scaled to all leaves; stellar packets "
             f"only; {nthreads} threads")
+    return value, desc, t_step, {"t_pp": t_pp, "t_fixed": t_fixed, "t_bal": t_bal, "nleaf": nleaf}
+
+
+class InstanceWorkload:
+    """One batch64 instance as a single-nebula workload (for the CPU port)."""
+
+    def __init__(self, p, nphot):
+        from mochii_b200 import configs
+        self.name, self.grid, self.nphot, self.thermal = "batch_instance", p["n"], nphot, True
+        self.make = lambda nphot_, prec, seed: configs.hii_instance(p["n"], p["nH"], p["tstar"], p["Q"],
+                                                                     nphotons=nphot_, precision=prec, seed=seed)
+
+
+def cpu_reference_batch(wl, states, nthreads, budget_s=24.0):
+    """The oracle port on the batch64 workload: three instances (the
+    smallest, the median and the largest grid) each timed as a single
+    nebula (cpu_reference: packet-sample passes and a leaf sample of the
+    thermal solve); the per-packet time taken as linear in the grid side
+    (the walk crosses O(n) leaves) and the per-leaf solve time averaged,
+    then summed over all instances.  states: per-instance state dicts for
+    the three sampled instances (or {}).  Returns (packets/s, description,
+    step seconds)."""
+    _, par = wl.instances("fp64")
+    order = sorted(range(len(par)), key=lambda k: par[k]["n"])
+    pick = [order[0], order[len(order) // 2], order[-1]]
+    ns, tpp, tfix, tcell = [], [], [], []
+    for k in pick:
+        iw = InstanceWorkload(par[k], wl.nphot)
+        _, _, _, comp = cpu_reference(iw, states.get(k, {}), nthreads, budget_s=budget_s / 3)
+        ns.append(par[k]["n"])
+        tpp.append(comp["t_pp"])
+        tfix.append(comp["t_fixed"])
+        tcell.append(comp["t_bal"] / comp["nleaf"])
+    slope, icpt = np.polyfit(np.array(ns, float), np.array(tpp), 1)
+    t_cell = float(np.mean(tcell))
+    t_step = sum(max(icpt + slope * p["n"], min(tpp)) * wl.nphot + float(np.mean(tfix)) + t_cell * p["n"] ** 3
+                 for p in par)
+    value = wl.nphot * len(par) / t_step
+    desc = (f"instances of {ns[0]}^3, {ns[1]}^3, {ns[2]}^3 each timed as one nebula (transport passes of packet "
+            f"samples, the thermal solve on every 256th leaf); per-packet time fitted linear in the grid side, "
+            f"per-leaf solve time averaged, summed over the {len(par)} instances at {wl.nphot} packets each; "
+            f"{nthreads} threads")
     return value, desc, t_step
 
 
@@ -263,16 +327,20 @@ def run_reference(args, wl):
     state = {}
     times = []
     for k in range(args.warmup + args.steps):
-        _, desc, t_step = cpu_reference(wl, state, nthreads, budget_s=10.0)
+        if wl.name == "batch64":
+            _, desc, t_step = cpu_reference_batch(wl, {}, nthreads, budget_s=12.0)
+        else:
+            _, desc, t_step, _ = cpu_reference(wl, state, nthreads, budget_s=10.0)
         if k >= args.warmup:
             times.append(t_step)
     dt = sum(times)
-    value = wl.nphot * args.steps / dt
+    value = wl.nphot * getattr(wl, "count", 1) * args.steps / dt
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt / args.steps * 1e3,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic",
-            "config": {"workload": wl.name, "grid": grid_name(wl, None), "packets_per_step": wl.nphot,
+            "config": {"workload": wl.name, "grid": grid_name(wl, None),
+                       "packets_per_step": wl.nphot * getattr(wl, "count", 1),
                        "state": "the workload's initial state",
                        "note": "each step a bounded sample of the workload's step, scaled"},
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": nthreads, "kind": "port", "sample": desc},
@@ -287,7 +355,8 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="mochii_b200")
-    ap.add_argument("--workload", default="hii_metals128", choices=["hii_metals128", "stromgren64", "clumpy_dusty"])
+    ap.add_argument("--workload", default="hii_metals128",
+                    choices=["hii_metals128", "stromgren64", "clumpy_dusty", "batch64"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-converge", action="store_true", help="skip the time-to-converged comparison")
     ap.add_argument("--precision", default=None, choices=["fp64", "fp32"],
@@ -305,6 +374,8 @@ def main():
     prec = args.precision or wl.default_precision
     if args.impl == "reference":
         return run_reference(args, wl)
+    if wl.name == "batch64":
+        return run_batch(args, wl, prec)
 
     rank, world, local = dist_env()
     import torch
@@ -424,7 +495,7 @@ def main():
     if rank == 0 and not args.no_cpu_baseline:
         nthreads = cpu_threads(wl)
         state = {f: neb.get(f) for f in ("x_HI", "x_HeI", "x_HeII", "n_e", "T_e")}
-        v, desc, _ = cpu_reference(wl, state, nthreads)
+        v, desc, _, _ = cpu_reference(wl, state, nthreads)
         cpu = {"value": v, "unit": UNIT, "cores": nthreads, "kind": "port", "sample": desc}
 
     conv = None
@@ -462,6 +533,169 @@ def main():
         }
         print(json.dumps(line), flush=True)
     neb.close()
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def run_batch(args, wl, prec):
+    """batch64: the instances as one Batch (mochii_batch_*); a step is one
+    iteration of every instance, timed by the library's CUDA events around
+    the graph launch.  After the timed steps, one iteration per instance
+    through the single-nebula calls gives the transport kernels' own time
+    (roofline) and the unbatched step time for comparison."""
+    rank, world, local = dist_env()
+    import torch
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=torch.device("cuda", local))
+    from mochii_b200 import Batch, Nebula, parse_namelist
+    from mochii_b200.build import build
+    if rank == 0 or not os.path.exists(os.path.join(ROOT, "mochii_b200", "libmochii_gpu.so")):
+        build()
+    if dist is not None:
+        dist.barrier()
+    extra = (f" par%thermal_solver = '{args.solver}'\n par%cell_layout = '{args.cell_layout}'\n"
+             f" par%tally_precision = '{args.tally}'\n par%packet_chunk = 1048576\n")
+    nls, par = wl.instances(prec, extra)
+    t0 = time.perf_counter()
+    nebs = [Nebula(parse_namelist(nl)) for nl in nls]
+    batch = Batch(nebs)
+    t_setup = time.perf_counter() - t0
+    nleaf = [neb.nleaf for neb in nebs]
+    free, total = torch.cuda.mem_get_info()
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    for _ in range(args.warmup):
+        batch.iterate()
+
+    ms_steps, packets, segs, nact, bcnt = [], 0, [], [], []
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        t_wall = time.perf_counter()
+        for _ in range(args.steps):
+            flush.zero_()
+            torch.cuda.synchronize()
+            st, m, ms = batch.iterate()
+            ms_steps.append(ms)
+            packets += sum(s_.packets for s_ in st)
+            segs.append([s_.direct_segments for s_ in st])
+            nact.append([s_.metal_active for s_ in st])
+            bcnt.append([sum(getattr(x, f) for x in m)
+                         for f in ("cells_solved", "rate_evaluations", "metal_sum_calls", "fixed_point_passes")])
+        torch.cuda.synchronize()
+        t_wall = time.perf_counter() - t_wall
+    total_ms = sum(ms_steps)
+    if dist is not None:
+        t = torch.tensor([total_ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+        p = torch.tensor([float(packets)], device="cuda", dtype=torch.float64)
+        dist.all_reduce(p, op=dist.ReduceOp.SUM)
+        packets = int(p.item())
+    value = packets / (total_ms * 1e-3)
+
+    # ---- end-to-end: every instance's state up from pinned host buffers,
+    # the batch iteration, x_HI, T_e and Gamma_HI of every instance back
+    lib = nebs[0].lib
+    x_host = [torch.from_numpy(neb.get("x_HI")).pin_memory() for neb in nebs]
+    t_host = [torch.from_numpy(neb.get("T_e")).pin_memory() for neb in nebs]
+    outs = [[torch.empty(n, dtype=torch.float64).pin_memory() for _ in range(3)] for n in nleaf]
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e_packets = 0
+    e0 = time.perf_counter()
+    for _ in range(args.steps):
+        rc = 0
+        for neb, xh, th, n in zip(nebs, x_host, t_host, nleaf):
+            rc |= lib.mochii_set_field(neb.ctx, b"x_HI", xh.data_ptr(), n)
+            rc |= lib.mochii_set_field(neb.ctx, b"T_e", th.data_ptr(), n)
+            rc |= lib.mochii_opacity_fill(neb.ctx)
+        st, _, _ = batch.iterate()
+        e_packets += sum(s_.packets for s_ in st)
+        for neb, o, n in zip(nebs, outs, nleaf):
+            rc |= lib.mochii_get_field(neb.ctx, b"x_HI", o[0].data_ptr(), n)
+            rc |= lib.mochii_get_field(neb.ctx, b"T_e", o[1].data_ptr(), n)
+            rc |= lib.mochii_get_field(neb.ctx, b"gamma_HI", o[2].data_ptr(), n)
+        assert rc == 0
+    torch.cuda.synchronize()
+    e2e_s = time.perf_counter() - e0
+    if dist is not None:
+        t = torch.tensor([e2e_s], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+        p = torch.tensor([float(e_packets)], device="cuda", dtype=torch.float64)
+        dist.all_reduce(p, op=dist.ReduceOp.SUM)
+        e_packets = int(p.item())
+    e2e_value = e_packets / e2e_s
+
+    # ---- one unbatched iteration: the transport kernels' own time and the
+    # single-nebula step time
+    kern_ms, pass_ms, bal_ms, useg, uact = 0.0, 0.0, 0.0, 0, 0
+    for neb in nebs:
+        s_ = neb.ionizing_field_and_rates()
+        neb.gas_thermal_update()
+        kern_ms += s_.kernel_ms
+        pass_ms += s_.pass_ms
+        bal_ms += neb.last_metrics.kernel_ms
+        useg += s_.direct_segments
+        uact += s_.metal_active
+    batch.close()
+    peak, peak_kind = peaks()
+    w = 8 if prec == "fp64" else 4
+    alg_bytes = bytes_per_segment(wl, prec) * useg + (w + 32) * uact
+    achieved = alg_bytes / (kern_ms * 1e-3) / 1e9
+
+    cpu = None
+    if rank == 0 and not args.no_cpu_baseline:
+        nthreads = cpu_threads(wl)
+        order = sorted(range(len(par)), key=lambda k: par[k]["n"])
+        pick = [order[0], order[len(order) // 2], order[-1]]
+        states = {k: {f: nebs[k].get(f) for f in ("x_HI", "x_HeI", "x_HeII", "n_e", "T_e")} for k in pick}
+        v, desc, _ = cpu_reference_batch(wl, states, nthreads)
+        cpu = {"value": v, "unit": UNIT, "cores": nthreads, "kind": "port", "sample": desc}
+    for neb in nebs:
+        neb.close()
+
+    if rank == 0:
+        n_all = int(sum(nleaf))
+        chunks = sum(2 * -(-wl.nphot // 1048576) + 2 for _ in nebs)
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64" if prec == "fp64" else "f32+f64",
+            "data": "synthetic",
+            "config": {"workload": wl.name, "grid": grid_name(wl, n_all), "instances": len(nebs),
+                       "stellar_packets_per_instance": wl.nphot, "packets_per_step": packets / args.steps / world,
+                       "precision": prec, "balance": "thermal", "solver": args.solver,
+                       "cell_layout": args.cell_layout, "tallies": args.tally, "metal_tallies": "exact",
+                       "state": "each instance's ionized start, then the warm-up iterations",
+                       "l2": "flushed between steps (256 MiB write)", "packet_chunk": 1048576,
+                       "execution": "one CUDA graph per iteration (all passes, then one persistent thermal launch)",
+                       "parallelism": "replicas" if world > 1 else "single"},
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 16 * n_all,
+                    "d2h_bytes_per_step": 24 * n_all},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "peak_kind": peak_kind, "traffic": None,
+                         "kernel": "k_launch + k_walk_edge (transport passes, one unbatched iteration)",
+                         "segments_per_step": useg, "kernel_ms": kern_ms},
+            "cpu_baseline": cpu,
+            "clocks": clk.summary(),
+            "gpu_launches": int(args.steps * (chunks + 1)),
+            "unbatched_ms_per_step": {"transport": pass_ms, "balance": bal_ms, "total": pass_ms + bal_ms},
+            "balance_counts_per_step": dict(zip(("cells", "rate_evaluations", "metal_sums", "ne_evaluations"),
+                                                (float(v) for v in np.mean(np.array(bcnt, dtype=float), axis=0)))),
+            "device_memory_gb": {"used": (total - free) / 1e9, "total": total / 1e9},
+            "setup_s": t_setup, "wall_s": t_wall,
+        }
+        print(json.dumps(line), flush=True)
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()
@@ -538,6 +772,8 @@ def time_to_converged(n=64, nphot=1_000_000, iters=20, train_iters=10, seed_trai
 
 
 def grid_name(wl, nleaf):
+    if wl.name == "batch64":
+        return f"{wl.count} instances, cubic grids 32^3..128^3, {nleaf or 'about 4.5e7'} leaves in all"
     return f"{wl.grid}^3" if wl.grid else f"octree, {nleaf or 'about 3e6'} leaves"
 
 

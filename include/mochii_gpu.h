@@ -152,6 +152,9 @@ typedef struct mochii_params {
      * par%metal_rates): 1 'table' = interpolated from a 4096-node ln T table
      * over [te_min, te_max] (default); 0 'exact' = every evaluation direct */
     int metal_rate_table;
+    /* packets per launch-walk chunk (not a reference key, par%packet_chunk):
+     * the size of the packet-record buffer, default 4194304 */
+    int64_t packet_chunk;
 } mochii_params;
 
 /* Per-pass statistics (ion_score_report_energy_closure, ion_score_mod.f90:364-387). */

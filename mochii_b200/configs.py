@@ -306,3 +306,66 @@ def clumpy_dusty(workdir, nphotons=30_000_000, niter=20, precision="fp32", seed=
  par%precision = '{precision}'
 /
 """
+
+
+def hii_instance(n, nH, tstar, Q, nphotons=2_000_000, niter=20, precision="fp32", seed=12345, rs_factor=1.2,
+                 metal_tally="exact"):
+    """One H II region of the batched workload: an n^3 uniform grid whose box
+    half-width is rs_factor times the Stromgren radius of (Q, n_H), He/H 0.1
+    and the eleven trace metals of hii_metals, a tstar blackbody with photon
+    rate Q(H) over 13.598-100 eV, case A, T_e solved in [3e3, 3e4] K from an
+    ionized start, no diffuse packets."""
+    rs = stromgren_radius_pc(Q=Q, nH=nH) * rs_factor
+    ab = "\n".join(f" par%abund_{k} = {v:.6e}" for k, v in METALS.items())
+    return f"""&parameters
+ par%no_photons = {float(nphotons):.6e}
+ par%launch_sequence = 'sobol'
+ par%qmc_seed = {seed}
+ par%grid_type = 'car'
+ par%nx = {n}
+ par%ny = {n}
+ par%nz = {n}
+ par%xmax = {rs:.10f}
+ par%ymax = {rs:.10f}
+ par%zmax = {rs:.10f}
+ par%distance_unit = 'pc'
+ par%nH_const = {nH:.8e}
+ par%He_abund = 0.1
+ par%tstar = {tstar:.6e}
+ par%luminosity = {Q * mean_photon_energy_ev(tstar, n=20001) * EV2ERG:.6e}
+ par%case_ab = 'A'
+ par%xHI_init = 1.0e-3
+ par%xHeI_init = 0.5
+ par%xHeII_init = 0.5
+ par%solve_te = .true.
+ par%te_min = 3.0e3
+ par%te_max = 3.0e4
+ par%te_fixed = 1.0e4
+ par%gas_niter = {niter}
+ par%use_metals = .true.
+{ab}
+ par%metal_tally = '{metal_tally}'
+ par%atomic_dir = '{ATOMIC_DIR}'
+ par%precision = '{precision}'
+/
+"""
+
+
+def batch_instances(count=64, seed=5, nmin=32, nmax=128, nphotons=2_000_000, precision="fp32",
+                    metal_tally="exact"):
+    """The batched-nebulae workload: count H II regions with seeded uneven
+    cubic grid sizes uniform in {nmin..nmax}, n_H log-uniform in 10-1000
+    cm^-3, T_eff uniform in 30-50 kK and Q(H) log-uniform in 1e48-1e50 s^-1.
+    Returns (namelists, parameters)."""
+    import random
+    rng = random.Random(seed)
+    out, par = [], []
+    for k in range(count):
+        n = rng.randint(nmin, nmax)
+        nH = 10.0 ** rng.uniform(1.0, 3.0)
+        tstar = rng.uniform(3.0e4, 5.0e4)
+        Q = 10.0 ** rng.uniform(48.0, 50.0)
+        out.append(hii_instance(n, nH, tstar, Q, nphotons=nphotons, precision=precision, seed=12345 + k,
+                                metal_tally=metal_tally))
+        par.append(dict(n=n, nH=nH, tstar=tstar, Q=Q))
+    return out, par

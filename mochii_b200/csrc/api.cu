@@ -437,7 +437,7 @@ extern "C" int mochii_init(const mochii_params* pin, mochii_ctx** out) {
     CKI(dalloc(&c->tw.ledger, 3 * (size_t)c->tw.ledger_blocks));
     CKI(dalloc(&c->tw.counters, 4));
     // packet records: launch chunks of up to 4 Mi packets
-    CKI(alloc_records(c, std::min<long long>(p.nphotons, 1LL << 22)));
+    CKI(alloc_records(c, std::min<long long>(p.nphotons, std::max<long long>(p.packet_chunk, 1024))));
     c->bw.blocks = balance_blocks(c);
     if (p.diffuse_field) {
         MilneHost mh;
@@ -761,7 +761,7 @@ extern "C" int mochii_set_nphotons(mochii_ctx* c, int64_t np) {
         CK(c, dalloc(&c->tw.ledger, 3 * (size_t)nb));
     }
     c->tw.ledger_blocks = nb;
-    const long long cap = std::min<long long>(np, 1LL << 22);
+    const long long cap = std::min<long long>(np, std::max<long long>(c->par.packet_chunk, 1024));
     if (cap > c->rec.cap) {
         CK(c, cudaStreamSynchronize(c->stream));
         free_records(c);

@@ -60,3 +60,20 @@ def test_batch_refuses_the_diffuse_field():
         Batch([neb])
     assert ei.value.status == 8
     neb.close()
+
+
+def test_packet_chunk_splits_the_pass():
+    """par%packet_chunk bounds the per-launch record buffers: a pass in
+    chunks of 4096 packets scores what a pass in one chunk scores."""
+    nl = configs.hii_metals(nphotons=30000, niter=1, n=16, precision="fp64", diffuse=False)
+    one = Nebula(parse_namelist(nl))
+    many = Nebula(parse_namelist(nl.replace("/\n", " par%packet_chunk = 4096\n/\n")))
+    s1, s2 = one.ionizing_field_and_rates(), many.ionizing_field_and_rates()
+    assert s1.direct_segments == s2.direct_segments
+    assert abs(s1.energy_absorbed / s2.energy_absorbed - 1) < 1e-12
+    for f in ("gamma_HI", "heat_HeI"):
+        a, b = one.get(f), many.get(f)
+        big = a > 1e-12 * a.max()
+        assert np.max(np.abs(b[big] / a[big] - 1)) < 1e-9, f
+    one.close()
+    many.close()
