@@ -363,8 +363,9 @@ def main():
                     help="transport arithmetic (default: the workload's)")
     ap.add_argument("--solver", default="bracketed", choices=["bisection", "bracketed"],
                     help="cell solver: the reference's bisection or the bracketed roots")
-    ap.add_argument("--cell-layout", default="lockstep", choices=["lockstep", "flow", "warp"],
-                    help="thermal solve with metals: one warp or one thread per leaf")
+    ap.add_argument("--cell-layout", default="lane", choices=["lane", "lockstep", "flow", "warp"],
+                    help="thermal solve with metals: per-lane machines with the cache in shared memory, "
+                         "lockstep nested loops, one flat machine per leaf, or one warp per leaf")
     ap.add_argument("--tally", default="fp64", choices=["fp64", "compensated"],
                     help="path tallies with FP32 segments: compensated FP32 pairs or FP64 atomics")
     ap.add_argument("--grid", type=int, default=None, help="grid side of a Cartesian workload (default: its own)")
@@ -565,6 +566,9 @@ def run_batch(args, wl, prec):
     nls, par = wl.instances(prec, extra)
     t0 = time.perf_counter()
     nebs = [Nebula(parse_namelist(nl)) for nl in nls]
+    tuned = {}
+    for neb, p_ in zip(nebs, par):   # walk shape per grid size, before the graph is recorded
+        tuned[p_["n"]] = neb.autotune(1 << 18)
     batch = Batch(nebs)
     t_setup = time.perf_counter() - t0
     nleaf = [neb.nleaf for neb in nebs]
@@ -679,6 +683,7 @@ def run_batch(args, wl, prec):
                        "state": "each instance's ionized start, then the warm-up iterations",
                        "l2": "flushed between steps (256 MiB write)", "packet_chunk": 1048576,
                        "execution": "one CUDA graph per iteration (all passes, then one persistent thermal launch)",
+                       "tuning": f"walk shape autotuned per grid size ({len(tuned)} sizes)",
                        "parallelism": "replicas" if world > 1 else "single"},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 16 * n_all,
                     "d2h_bytes_per_step": 24 * n_all},

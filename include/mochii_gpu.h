@@ -136,11 +136,14 @@ typedef struct mochii_params {
      * (define.f90:211-212,361); taumax / tauhomo > 0 are not built */
     double lambda_ref, taumax, tauhomo;
     /* thermal solve with metals (not a reference key, par%cell_layout):
-     * 0 'lockstep' (or 'thread') = one thread per leaf, warp-uniform root
-     * loops over leaves sorted by work (default); 1 'warp' = one warp per
-     * leaf, the metal cascade spread over the lanes; 2 'flow' = one thread
-     * per leaf, each lane's whole solve a state machine served by warp-wide
-     * evaluations */
+     * 3 'lane' = one thread per leaf, the metal rate cache in shared memory,
+     * the n_e and H roots one per-lane machine, each lane claiming the next
+     * leaf of the work order as it finishes (default); 0 'lockstep' (or
+     * 'thread') = one thread per leaf, warp-uniform nested root loops over
+     * 32-leaf chunks sorted by work, the cache in local memory; 1 'warp' = one
+     * warp per leaf, the metal cascade spread over the lanes; 2 'flow' = one
+     * thread per leaf, each lane's whole solve a state machine served by
+     * warp-wide evaluations */
     int solver_warp;
     /* path tallies with FP32 segments (not a reference key,
      * par%tally_precision): 1 'fp64' = FP64 atomic tallies (default: on B200

@@ -387,16 +387,21 @@ extern "C" int mochii_init(const mochii_params* pin, mochii_ctx** out) {
             species_moment_tables(c->species, p.add_fuv ? p.efuv_min : p.eion_min, p.eion_max);
             const SpeciesHost& s2 = c->species;
             m.nmb = (int)s2.medge.size() - 1;
-            // one allocation: medge | mcoef | mb0
-            const size_t b1 = al(s2.medge.size() * 8), b2 = al(s2.mcoef.size() * 8), b3 = al(s2.mb0.size() * 4);
+            // one allocation: medge | mcoef | mb0 | jof (element order of each threshold-order index)
+            std::vector<int> jof(m.ntrp, -1);
+            for (int j = 0; j < m.ntr; ++j) jof[s2.tr[j].flat] = j;
+            const size_t b1 = al(s2.medge.size() * 8), b2 = al(s2.mcoef.size() * 8), b3 = al(s2.mb0.size() * 4),
+                         b4 = al(jof.size() * 4);
             char* mq = nullptr;
-            CKI(cudaMalloc(&mq, b1 + b2 + b3));
+            CKI(cudaMalloc(&mq, b1 + b2 + b3 + b4));
             CKI(cudaMemcpy(mq, s2.medge.data(), s2.medge.size() * 8, cudaMemcpyHostToDevice));
             CKI(cudaMemcpy(mq + b1, s2.mcoef.data(), s2.mcoef.size() * 8, cudaMemcpyHostToDevice));
             CKI(cudaMemcpy(mq + b1 + b2, s2.mb0.data(), s2.mb0.size() * 4, cudaMemcpyHostToDevice));
+            CKI(cudaMemcpy(mq + b1 + b2 + b3, jof.data(), jof.size() * 4, cudaMemcpyHostToDevice));
             m.medge = reinterpret_cast<const double*>(mq);
             m.mcoef = reinterpret_cast<const double*>(mq + b1);
             m.mb0 = reinterpret_cast<const int*>(mq + b1 + b2);
+            m.jof = reinterpret_cast<const int*>(mq + b1 + b2 + b3);
             CKI(cudaMalloc(&m.mom, (size_t)n * m.nmb * kMomDeg * tsz + 64));
         } else {
             CKI(cudaMalloc(&m.raw, (size_t)n * m.ntrp * 2 * tsz + 64));
@@ -639,7 +644,8 @@ extern "C" int mochii_batch_create(mochii_ctx* const* ctxs, int n, mochii_batch*
     bool all = true;
     for (int k = 0; k < n; ++k) {
         const mochii_ctx* c = ctxs[k];
-        all = all && c->metal.ntr > 0 && c->par.solver_bracketed && c->par.solver_warp == 0 && c->thermal_ready;
+        all = all && c->metal.ntr > 0 && c->par.solver_bracketed && c->thermal_ready &&
+              (c->par.solver_warp == 0 || c->par.solver_warp == 3) && c->par.solver_warp == ctxs[0]->par.solver_warp;
     }
     if (e == cudaSuccess && all) {
         b->tb = thermal_batch_create(ctxs, n, &e);

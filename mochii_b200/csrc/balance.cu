@@ -1506,6 +1506,8 @@ __device__ __forceinline__ void thermal_acc_flush(const BalArgs& b, ThermalAcc& 
     acc = ThermalAcc();
 }
 
+#include "thermal_lane.cuh"
+
 // The lockstep thermal solve of many nebulae in one persistent launch: the
 // 32-leaf chunks of all nebulae are numbered consecutively (chunk_off: the
 // first chunk of each nebula, nneb + 1 entries) and claimed from one counter;
@@ -1551,6 +1553,33 @@ __global__ void __launch_bounds__(kBThreads) k_thermal_batch(const ThArgs* __res
         thermal_chunk_ls(sa[wib], base, lane, acc);
     }
     if (cur >= 0) thermal_acc_flush(sa[wib].b, acc);
+}
+
+// The per-lane solve (k_thermal_lane) of many nebulae in one persistent
+// launch: every warp takes the nebulae in turn, its lanes claiming leaves of
+// nebula q's work order from next[q] until it is exhausted; the warp's sums
+// go to nebula q before it moves on.
+__global__ void __launch_bounds__(kBThreads, 1) k_thermal_lane_batch(const ThArgs* __restrict__ args, int nneb,
+                                                                     unsigned long long* next) {
+    extern __shared__ __align__(16) unsigned char lane_smem[];
+    __shared__ ThArgs sa[kBThreads / 32];
+    __shared__ LaneLayout sl[kBThreads / 32];
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    double* S = reinterpret_cast<double*>(lane_smem);
+    for (int q = 0; q < nneb; ++q) {
+        __syncwarp();
+        const int nw = (int)(sizeof(ThArgs) / 4);
+        const unsigned* src = reinterpret_cast<const unsigned*>(args + q);
+        unsigned* dst = reinterpret_cast<unsigned*>(sa + wib);
+        for (int k = lane; k < nw; k += 32) dst[k] = src[k];
+        __syncwarp();
+        if (lane == 0) lane_layout_build(sa[wib].b.m, sl[wib]);
+        __syncwarp();
+        LaneCache cache{S + threadIdx.x, (int)blockDim.x, &sl[wib], &sa[wib].b.m, sa[wib].b.m.el, sa[wib].b.m.nel};
+        ThermalAcc acc;
+        lane_solve(sa[wib], next + q, cache, acc, lane);
+        thermal_acc_flush(sa[wib].b, acc);
+    }
 }
 
 // ---- the bracketed thermal solve as one flat per-lane state machine ---------
@@ -2322,12 +2351,41 @@ cudaError_t thermal_work_alloc(mochii_ctx* c) {
     return cudaGetLastError();
 }
 
+// Launch shape of k_thermal_lane: the cache slots per lane decide how many
+// lanes fit in shared memory; one block per SM (at most kBThreads threads,
+// at least one warp), never more blocks than the balance's partial slots.
+cudaError_t thermal_lane_setup(mochii_ctx* c) {
+    BalanceWork& w = c->bw;
+    int nslot = 0;
+    for (const MetalTr& t : c->species.tr) nslot += lane_slots(lane_kind(t));
+    int smem_max = 0, sms = 148;
+    cudaError_t e = cudaDeviceGetAttribute(&smem_max, cudaDevAttrMaxSharedMemoryPerBlockOptin, c->device);
+    if (e != cudaSuccess) return e;
+    if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device)) != cudaSuccess) return e;
+    const size_t fixed = lane_cache_offset() + 6 * (kBThreads / 32) * 8 + 1024;   // layout, reduction, reserve
+    const size_t per_lane = (size_t)std::max(nslot, 1) * 8;
+    int threads = (int)(((size_t)smem_max - fixed) / per_lane) / 32 * 32;
+    threads = std::max(32, std::min(kBThreads, threads));
+    w.lane_threads = threads;
+    w.lane_smem = lane_cache_offset() + per_lane * threads;
+    w.lane_blocks = std::max(1, std::min(sms, c->bw.blocks));
+    e = cudaFuncSetAttribute(k_thermal_lane, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)w.lane_smem);
+    if (e != cudaSuccess) {
+        w.lane_threads = 0;
+        return e;
+    }
+    return cudaSuccess;
+}
+
 // ---- batched nebulae --------------------------------------------------------
 struct ThermalBatch {
     ThArgs* d_args = nullptr;
     long long* d_off = nullptr;
-    unsigned long long* d_next = nullptr;
+    unsigned long long* d_next = nullptr;   // lockstep: one chunk counter; lane: one leaf counter per nebula
     int n = 0, blocks = 0;
+    bool lane = false;                      // the per-lane solve (cell_layout 'lane')
+    int threads = kBThreads;
+    size_t smem = 0;
 };
 
 void* thermal_batch_create(mochii_ctx* const* cs, int n, cudaError_t* err) {
@@ -2356,10 +2414,32 @@ void* thermal_batch_create(mochii_ctx* const* cs, int n, cudaError_t* err) {
     }
     if (*err == cudaSuccess) *err = cudaMalloc(&tb->d_args, sizeof(ThArgs) * n);
     if (*err == cudaSuccess) *err = cudaMalloc(&tb->d_off, sizeof(long long) * (n + 1));
-    if (*err == cudaSuccess) *err = cudaMalloc(&tb->d_next, sizeof(unsigned long long));
+    tb->lane = cs[0]->par.solver_warp == 3;
+    if (*err == cudaSuccess) *err = cudaMalloc(&tb->d_next, sizeof(unsigned long long) * (tb->lane ? n : 1));
     if (*err == cudaSuccess) *err = cudaMemcpy(tb->d_args, args.data(), sizeof(ThArgs) * n, cudaMemcpyHostToDevice);
     if (*err == cudaSuccess) *err = cudaMemcpy(tb->d_off, off.data(), sizeof(long long) * (n + 1), cudaMemcpyHostToDevice);
-    if (*err == cudaSuccess) {
+    if (*err == cudaSuccess && tb->lane) {   // shared cache sized to the largest nebula's slots
+        int nslot = 1, smem_max = 0, sms = 148;
+        for (int k = 0; k < n; ++k) {
+            int q = 0;
+            for (const MetalTr& t : cs[k]->species.tr) q += lane_slots(lane_kind(t));
+            nslot = std::max(nslot, q);
+        }
+        cudaFuncAttributes fa;
+        *err = cudaFuncGetAttributes(&fa, k_thermal_lane_batch);
+        if (*err == cudaSuccess) *err = cudaDeviceGetAttribute(&smem_max, cudaDevAttrMaxSharedMemoryPerBlockOptin,
+                                                               cs[0]->device);
+        if (*err == cudaSuccess) *err = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, cs[0]->device);
+        if (*err == cudaSuccess) {
+            const size_t avail = (size_t)smem_max - fa.sharedSizeBytes - 1024;
+            int threads = (int)(avail / ((size_t)nslot * 8)) / 32 * 32;
+            tb->threads = std::max(32, std::min(kBThreads, threads));
+            tb->smem = (size_t)nslot * 8 * tb->threads;
+            tb->blocks = sms;
+            *err = cudaFuncSetAttribute(k_thermal_lane_batch, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        (int)tb->smem);
+        }
+    } else if (*err == cudaSuccess) {
         int per = 1, sms = 148;
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_thermal_batch, kBThreads, 0);
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, cs[0]->device);
@@ -2394,6 +2474,11 @@ cudaError_t thermal_batch_enqueue(void* p, mochii_ctx* const* cs, cudaStream_t s
         e = cub::DeviceRadixSort::SortPairs(w.sort_tmp, w.sort_bytes, w.work, w.work_sorted, w.iota, w.order, n, 0, 16, s);
         if (e != cudaSuccess) return e;
     }
+    if (tb->lane) {
+        if ((e = cudaMemsetAsync(tb->d_next, 0, sizeof(unsigned long long) * tb->n, s)) != cudaSuccess) return e;
+        k_thermal_lane_batch<<<tb->blocks, tb->threads, tb->smem, s>>>(tb->d_args, tb->n, tb->d_next);
+        return cudaGetLastError();
+    }
     if ((e = cudaMemsetAsync(tb->d_next, 0, sizeof(unsigned long long), s)) != cudaSuccess) return e;
     k_thermal_batch<<<tb->blocks, kBThreads, 0, s>>>(tb->d_args, tb->n, tb->d_off, tb->d_next);
     return cudaGetLastError();
@@ -2426,6 +2511,12 @@ cudaError_t launch_thermal(mochii_ctx* c) {
         if (c->par.solver_warp == 2) {
             if ((e = cudaMemsetAsync(w.next, 0, sizeof(unsigned long long), c->stream)) != cudaSuccess) return e;
             k_thermal_flow<<<c->bw.blocks, kBThreads, 0, c->stream>>>(a, w.next);
+        } else if (c->par.solver_warp == 3) {
+            if (w.lane_threads == 0 && (e = thermal_lane_setup(c)) != cudaSuccess) return e;
+            if ((e = cudaMemsetAsync(w.next, 0, sizeof(unsigned long long), c->stream)) != cudaSuccess) return e;
+            if ((e = cudaMemsetAsync(c->bw.partial, 0, 6 * (size_t)c->bw.blocks * 8, c->stream)) != cudaSuccess) return e;
+            a.next = w.next;
+            k_thermal_lane<<<w.lane_blocks, w.lane_threads, w.lane_smem, c->stream>>>(a);
         } else {
             if (w.ls_blocks == 0) {   // persistent: the resident blocks of the device
                 int per = 1, sms = 148;

@@ -86,6 +86,9 @@ struct BalanceWork {
     size_t sort_bytes = 0;
     unsigned long long* next = nullptr;   // the flat / lockstep solves' work counter
     int ls_blocks = 0;                    // the lockstep solve's persistent grid
+    // the per-lane solve (metal cache in shared memory): block size, grid, bytes
+    int lane_threads = 0, lane_blocks = 0;
+    size_t lane_smem = 0;
     bool have_work = false;
 };
 

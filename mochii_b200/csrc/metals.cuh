@@ -186,10 +186,9 @@ __device__ __forceinline__ double metal_chain(const MetalCache& c, int tr0, int 
 // species_metal_sums (species_mod.f90:566-614): metal electrons and the two
 // charge-exchange rates hydrogen sees, from one walk of each chain.
 static __device__ __noinline__ void metal_sums(const MetalDev& m, const MetalCache& c, double nH, double ne, double nHI,
-                                        double nHII, double& nem, double& rin, double& rout) {
-    nem = 0.0;
-    rin = 0.0;
-    rout = 0.0;
+                                        double nHII, double& nem_out, double& rin_out, double& rout_out) {
+    // accumulated in registers, stored once (the outputs live in the caller's frame)
+    double nem = 0.0, rin = 0.0, rout = 0.0;
     double r[kMaxSt];
     for (int ie = 0; ie < m.nel; ++ie) {
         const MetalEl e = m.el[ie];
@@ -204,6 +203,9 @@ static __device__ __noinline__ void metal_sums(const MetalDev& m, const MetalCac
             if (i < ns) rin = rin + c.cxi[e.tr0 + i - 1] * nX * fr;
         }
     }
+    nem_out = nem;
+    rin_out = rin;
+    rout_out = rout;
 }
 
 // hydrogen_neutral_fraction (ion_balance_mod.f90:177-208): Illinois false

@@ -137,7 +137,7 @@ extern "C" int mochii_params_default(mochii_params* p) {
     p->lambda_ref = 0.55;
     p->taumax = -999.0;
     p->tauhomo = -999.0;
-    p->solver_warp = 0;
+    p->solver_warp = 3;
     p->tally64 = 1;
     p->metal_rate_table = 1;
     p->packet_chunk = 1 << 22;
@@ -297,9 +297,9 @@ int set_key(mochii_params* p, std::string key, const std::vector<std::string>& v
     }
     if (key == "cell_layout") {
         const std::string s = lower(unquote(v));
-        if (s != "warp" && s != "thread" && s != "lockstep" && s != "flow")
-            return bad("must be 'lockstep', 'flow' or 'warp'");
-        p->solver_warp = s == "warp" ? 1 : s == "flow" ? 2 : 0;
+        if (s != "warp" && s != "thread" && s != "lockstep" && s != "flow" && s != "lane")
+            return bad("must be 'lockstep', 'lane', 'flow' or 'warp'");
+        p->solver_warp = s == "warp" ? 1 : s == "flow" ? 2 : s == "lane" ? 3 : 0;
         return 0;
     }
     if (key == "thermal_solver") {

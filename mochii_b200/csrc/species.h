@@ -83,6 +83,7 @@ struct MetalDev {
     const double* medge = nullptr;     // nmb + 1
     const double* mcoef = nullptr;     // (nmb*kMomDeg) x ntrp x 2
     const int* mb0 = nullptr;          // ntr, threshold order
+    const int* jof = nullptr;          // ntrp: element-order index of each threshold-order index (-1: padding)
     void* mom = nullptr;               // nleaf x nmb x kMomDeg tallies
     // T table of the rate coefficients (thermal solve): ln of collisional
     // ionisation, recombination, CX ionisation, CX recombination per

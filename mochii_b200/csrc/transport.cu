@@ -942,34 +942,74 @@ __global__ void k_metal_rates(const MetalDev m, long long nleaf, double cg, doub
     }
 }
 
-// The same from the energy moments: raw_{k,q}(leaf) = sum over the moment
-// bins b where transition k is active and the Chebyshev orders m of
-// mom(leaf, b, m) * coef(b, m, k, q).  One warp per leaf: the leaf's moments
-// are read once and broadcast, lanes run over the transitions.
-template <typename T>
-__global__ void k_metal_rates_mom(const MetalDev m, long long nleaf, double cg, double ch, const double4* lg,
-                                  double d2) {
+// The same from the energy moments: raw_{k,c}(leaf) = sum over the moment
+// bins b and Chebyshev orders q of mom(leaf, b, q) * coef(b, q, k, c), as a
+// tiled product of the (leaves x nmb*kMomDeg) moments with the
+// (nmb*kMomDeg x 2 ntrp) coefficients.  A transition's coefficients are zero
+// below its first active bin, so the dense sum adds the bin-restricted sum's
+// terms in the same order (b, then q, ascending) and zeros before them.
+// Block: 64 leaves x all outputs, 256 threads, each 4 leaves x NU outputs;
+// the moments and coefficients staged through shared memory KC orders at a
+// time.
+constexpr int kRtM = 64, kRtThreads = 256;
+
+template <typename T, int NU, int KC>
+__global__ void __launch_bounds__(kRtThreads) k_metal_rates_mom(const MetalDev m, long long nleaf, double cg,
+                                                                double ch, const double4* lg, double d2) {
+    __shared__ double sA[kRtM][KC + 1];
+    __shared__ double sB[KC][16 * NU];
+    const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
+    const int K = m.nmb * kMomDeg, N = 2 * m.ntrp;
     const T* mom = static_cast<const T*>(m.mom);
-    const int lane = threadIdx.x & 31;
-    const long long warps = (long long)gridDim.x * (blockDim.x >> 5);
-    for (long long il = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); il < nleaf; il += warps) {
-        const T* ml = mom + il * m.nmb * kMomDeg;
-        for (int j = lane; j < m.ntr; j += 32) {
-            const int k = m.tr[j].flat;
-            double s0 = 0.0, s1 = 0.0;
-            for (int b = m.mb0[k]; b < m.nmb; ++b) {
+    const double* C = m.mcoef;   // [K][ntrp][2] = K x N, row-major
+    for (long long tile = blockIdx.x; tile * kRtM < nleaf; tile += gridDim.x) {
+        const long long l0 = tile * kRtM;
+        double acc[4][NU];
 #pragma unroll
-                for (int q = 0; q < kMomDeg; ++q) {
-                    const double v = tval<T>(ml[b * kMomDeg + q]);
-                    const double2 cf = __ldg(reinterpret_cast<const double2*>(m.mcoef) +
-                                             ((long long)(b * kMomDeg + q) * m.ntrp + k));
-                    s0 = s0 + v * cf.x;
-                    s1 = s1 + v * cf.y;
-                }
+        for (int i = 0; i < 4; ++i)
+#pragma unroll
+            for (int u = 0; u < NU; ++u) acc[i][u] = 0.0;
+        for (int k0 = 0; k0 < K; k0 += KC) {
+            __syncthreads();
+            for (int e = tid; e < kRtM * KC; e += kRtThreads) {
+                const int r = e / KC, q = e - r * KC;
+                const long long il = l0 + r;
+                const int kk = k0 + q;
+                sA[r][q] = (il < nleaf && kk < K) ? tval<T>(mom[il * K + kk]) : 0.0;
             }
+            for (int e = tid; e < KC * 16 * NU; e += kRtThreads) {
+                const int r = e / (16 * NU), q = e - r * (16 * NU);
+                const int kk = k0 + r;
+                sB[r][q] = (kk < K && q < N) ? __ldg(C + (size_t)kk * N + q) : 0.0;
+            }
+            __syncthreads();
+            const int kn = min(KC, K - k0);
+            for (int kk = 0; kk < kn; ++kk) {
+                double a[4], b[NU];
+#pragma unroll
+                for (int i = 0; i < 4; ++i) a[i] = sA[ty * 4 + i][kk];
+#pragma unroll
+                for (int u = 0; u < NU; ++u) b[u] = sB[kk][tx + 16 * u];
+#pragma unroll
+                for (int i = 0; i < 4; ++i)
+#pragma unroll
+                    for (int u = 0; u < NU; ++u) acc[i][u] = acc[i][u] + a[i] * b[u];
+            }
+        }
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            const long long il = l0 + ty * 4 + i;
+            if (il >= nleaf) continue;
             const double f = leaf_fac(lg, il, d2);
-            m.egam[il * m.ntr + j] = s0 * (cg * f);
-            m.eheat[il * m.ntr + j] = s1 * (ch * f);
+#pragma unroll
+            for (int u = 0; u < NU; ++u) {
+                const int col = tx + 16 * u;
+                if (col >= N) continue;
+                const int j = m.jof[col >> 1];
+                if (j < 0) continue;
+                if (col & 1) m.eheat[il * m.ntr + j] = acc[i][u] * (ch * f);
+                else m.egam[il * m.ntr + j] = acc[i][u] * (cg * f);
+            }
         }
     }
 }
@@ -1315,9 +1355,18 @@ cudaError_t launch_rates(mochii_ctx* c) {
     }
 #undef RATES
     if (c->metal.ntr > 0 && c->metal.nmb > 0) {
-        const int mb = grid_blocks(n * 32, 256, 148 * 32);
-        if (c->fp32 && !c->tally64) k_metal_rates_mom<float2><<<mb, 256, 0, c->stream>>>(c->metal, n, cg, ch, lg, d2);
-        else k_metal_rates_mom<double><<<mb, 256, 0, c->stream>>>(c->metal, n, cg, ch, lg, d2);
+        const int mb = (int)std::min<long long>((n + kRtM - 1) / kRtM, 148LL * 8);
+        const int N = 2 * c->metal.ntrp;
+        const bool pairs = c->fp32 && !c->tally64;
+#define MOM(NU, KC)                                                                                       \
+    do {                                                                                                  \
+        if (pairs) k_metal_rates_mom<float2, NU, KC><<<mb, kRtThreads, 0, c->stream>>>(c->metal, n, cg, ch, lg, d2); \
+        else k_metal_rates_mom<double, NU, KC><<<mb, kRtThreads, 0, c->stream>>>(c->metal, n, cg, ch, lg, d2);       \
+    } while (0)
+        if (N <= 32) MOM(2, 32);
+        else if (N <= 64) MOM(4, 32);
+        else MOM(8, 16);
+#undef MOM
     } else if (c->metal.ntr > 0) {
         const int mb = grid_blocks(n * c->metal.ntr, 256, 148 * 16);
         if (c->fp32 && !c->tally64) k_metal_rates<float2><<<mb, 256, 0, c->stream>>>(c->metal, n, cg, ch, lg, d2);

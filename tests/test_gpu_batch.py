@@ -13,20 +13,20 @@ from mochii_b200 import Batch, Nebula, MochiiError, configs, parse_namelist
 pytestmark = pytest.mark.gpu
 
 
-def nebulae(sizes, solve_te=True):
+def nebulae(sizes, solve_te=True, layout="lockstep"):
     out = []
     for k, n in enumerate(sizes):
         nl = configs.hii_metals(nphotons=30000 + 10000 * k, niter=3, n=n, precision="fp64", rs_factor=1.2 + 0.1 * k,
                                 diffuse=False, solve_te=solve_te)
-        out.append(Nebula(parse_namelist(nl)))
+        out.append(Nebula(parse_namelist(nl.replace("/\n", f" par%cell_layout = '{layout}'\n/\n"))))
     return out
 
 
-@pytest.mark.parametrize("solve_te", [True, False])
-def test_batch_iteration_equals_standalone(solve_te):
+@pytest.mark.parametrize("solve_te,layout", [(True, "lockstep"), (True, "lane"), (False, "lockstep")])
+def test_batch_iteration_equals_standalone(solve_te, layout):
     sizes = (12, 16, 20)
-    alone = nebulae(sizes, solve_te)
-    together = nebulae(sizes, solve_te)
+    alone = nebulae(sizes, solve_te, layout)
+    together = nebulae(sizes, solve_te, layout)
     batch = Batch(together)
     for it in range(3):
         st, m, ms = batch.iterate(solve_te=solve_te)

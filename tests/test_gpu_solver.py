@@ -101,8 +101,9 @@ def test_bracketed_solve_needs_fewer_evaluations():
 
 
 def test_cell_layouts_agree():
-    """The thermal solve with metals in its three layouts -- warp-uniform root
-    loops ('lockstep', the default), each leaf's solve a state machine served
+    """The thermal solve with metals in its four layouts -- warp-uniform root
+    loops ('lockstep'), per-lane root machines with the metal cache in shared
+    memory ('lane', the default), each leaf's solve a state machine served
     by warp-wide evaluations ('flow'), one warp per leaf ('warp') -- make the
     same solves per leaf.  Separate runs accumulate the transport tallies
     in different atomic orders, so the rates differ in their last bits and a
@@ -111,7 +112,7 @@ def test_cell_layouts_agree():
     nl = with_solver(configs.hii_metals(nphotons=60000, niter=2, n=n, precision="fp64", rs_factor=1.3,
                                         diffuse=False), "bracketed")
     out = {}
-    for layout in ("lockstep", "flow", "warp"):
+    for layout in ("lockstep", "lane", "flow", "warp"):
         neb = Nebula(parse_namelist(nl.replace("/\n", f" par%cell_layout = '{layout}'\n/\n")))
         st = partial_state(n, parse_namelist(nl).xmax)
         for k, v in st.items():
@@ -122,11 +123,44 @@ def test_cell_layouts_agree():
             neb.gas_thermal_update()
         out[layout] = (neb.get("T_e"), neb.get("x_HI"), neb.last_metrics.rate_evaluations)
         neb.close()
-    for other in ("flow", "warp"):
+    for other in ("lane", "flow", "warp"):
         dT = np.abs(out[other][0] - out["lockstep"][0])
         assert np.median(dT) < 1e-6 and dT.max() < 1.0, (other, dT.max())
         assert np.max(np.abs(out[other][1] - out["lockstep"][1])) < 1e-5
         assert abs(out[other][2] / out["lockstep"][2] - 1) < 0.01
+
+
+def test_lane_layout_refills_lanes():
+    """The per-lane layout on more leaves than the device has lanes (each
+    lane solves several leaves, claimed as it frees) and with the reference's
+    one-way charge exchange (no H root iteration): the same solves as the
+    lockstep layout, every leaf written once."""
+    n = 44
+    for cx in ("two_way", "one_way"):
+        nl = with_solver(configs.hii_metals(nphotons=200000, niter=2, n=n, precision="fp64", rs_factor=1.3,
+                                            diffuse=False), "bracketed")
+        nl = nl.replace("/\n", f" par%charge_exchange = '{cx}'\n/\n")
+        out = {}
+        for layout in ("lockstep", "lane"):
+            neb = Nebula(parse_namelist(nl.replace("/\n", f" par%cell_layout = '{layout}'\n/\n")))
+            st = partial_state(n, parse_namelist(nl).xmax)
+            for k, v in st.items():
+                neb.set(k, v)
+            neb.gas_opacity_fill()
+            for _ in range(2):
+                neb.ionizing_field_and_rates()
+                neb.gas_thermal_update()
+            m = neb.last_metrics
+            out[layout] = (neb.get("T_e"), neb.get("x_HI"), m.rate_evaluations, m.cells_solved, m.metal_sum_calls,
+                           neb.get("n_e"))
+            neb.close()
+        a_, b_ = out["lockstep"], out["lane"]
+        assert b_[3] == a_[3] == n ** 3
+        dT = np.abs(b_[0] - a_[0])
+        assert np.median(dT) < 1e-6 and dT.max() < 1.0, (cx, dT.max())
+        assert np.max(np.abs(b_[1] - a_[1])) < 1e-5
+        assert np.median(np.abs(b_[5] / a_[5] - 1)) < 1e-8
+        assert abs(b_[2] / a_[2] - 1) < 0.01 and abs(b_[4] / a_[4] - 1) < 0.01
 
 
 def test_metal_rate_table_matches_exact():
