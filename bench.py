@@ -122,9 +122,11 @@ class Workload:
         return neb.gas_thermal_update() if self.thermal else neb.gas_equilibrium_update()
 
 
-def bytes_per_segment(wl, precision):
+def bytes_per_segment(wl, precision, tally="fp64"):
     """B_seg = 4 F_state + 16 F_tally without the per-segment metal words
-    (added from the kernel's count), state words 8 B in FP64."""
+    (added from the kernel's count), state words 8 B in FP64; the six metal
+    moment words are FP32 (8 B each, read and written) with FP32 segments and
+    FP64 tallies."""
     w = 8 if precision == "fp64" else 4
     if wl.name == "stromgren64":
         return w * 2 + 16 * 3          # n_H, x_HI; Gamma_HI, H_HI, jt_ion
@@ -132,7 +134,8 @@ def bytes_per_segment(wl, precision):
         return w * 5 + 16 * 9          # n_H, x_HI, x_HeI, x_HeII, rhokap; 6 H/He + jt_ion + dust_abs + FUV
     if wl.name == "batch64":
         return w * 4 + 16 * 7          # n_H, x_HI, x_HeI, x_HeII; 6 H/He + jt_ion (metal words per segment)
-    return w * 4 + 16 * (7 + 6)        # n_H, x_HI, x_HeI, x_HeII; 6 H/He + jt_ion + 6 metal moments
+    mom = 8 if precision == "fp32" and tally == "fp64" else 16
+    return w * 4 + 16 * 7 + mom * 6   # n_H, x_HI, x_HeI, x_HeII; 6 H/He + jt_ion; 6 metal moments
 
 
 def prepare(neb, wl):
@@ -483,7 +486,7 @@ def main():
     # ---- roofline of the transport kernels -----------------------------------
     peak, peak_kind = peaks()
     wbytes = 8 if prec == "fp64" else 4
-    bseg = bytes_per_segment(wl, prec)
+    bseg = bytes_per_segment(wl, prec, args.tally)
     alg_bytes = float(np.mean([bseg * s_ + wbytes * a_ for s_, a_ in zip(segs, nact)]))
     mean_seg = float(np.mean(segs))
     mean_ms = float(np.mean(kern_ms))

@@ -42,6 +42,14 @@ cudaError_t dalloc(T** p, size_t n) {
     return cudaMalloc(reinterpret_cast<void**>(p), n * sizeof(T) + 16);
 }
 
+// Bytes of the metal moment tallies: nmb bins per leaf of kMomDeg FP64 words
+// (or compensated FP32 pairs), or with FP32 moments 8 floats (6 used) so a
+// bin's update is one aligned 32-byte sector.
+size_t mom_bytes(const mochii_ctx* c) {
+    const MetalDev& m = c->metal;
+    return (size_t)c->grid.nleaf * m.nmb * (m.mom32 ? 8 * sizeof(float) : kMomDeg * 8);
+}
+
 void free_records(mochii_ctx* c) {
     for (void* q : {(void*)c->rec.tm, (void*)c->rec.td, (void*)c->rec.cell, (void*)c->rec.bits, c->rec.sig, c->rec.coef,
                     (void*)c->rec.E, c->rec.msig, c->rec.dsc, (void*)c->rec.p0})
@@ -402,7 +410,8 @@ extern "C" int mochii_init(const mochii_params* pin, mochii_ctx** out) {
             m.mcoef = reinterpret_cast<const double*>(mq + b1);
             m.mb0 = reinterpret_cast<const int*>(mq + b1 + b2);
             m.jof = reinterpret_cast<const int*>(mq + b1 + b2 + b3);
-            CKI(cudaMalloc(&m.mom, (size_t)n * m.nmb * kMomDeg * tsz + 64));
+            m.mom32 = c->fp32 && c->tally64;
+            CKI(cudaMalloc(&m.mom, mom_bytes(c) + 64));
         } else {
             CKI(cudaMalloc(&m.raw, (size_t)n * m.ntrp * 2 * tsz + 64));
         }
@@ -541,7 +550,7 @@ cudaError_t batch_pass(mochii_ctx* c, mochii_batch* b, int k, cudaStream_t s) {
         if ((e = cudaMemsetAsync(c->tally, 0, (size_t)n * c->ntally * tsz, s)) != cudaSuccess) break;
         if ((e = cudaMemsetAsync(c->jt, 0, (size_t)n * c->nnu * tsz, s)) != cudaSuccess) break;
         if (c->metal.ntr > 0 && c->metal.nmb > 0)
-            e = cudaMemsetAsync(c->metal.mom, 0, (size_t)n * c->metal.nmb * kMomDeg * tsz, s);
+            e = cudaMemsetAsync(c->metal.mom, 0, mom_bytes(c), s);
         else if (c->metal.ntr > 0)
             e = cudaMemsetAsync(c->metal.raw, 0, (size_t)n * c->metal.ntrp * 2 * tsz, s);
         if (e != cudaSuccess) break;
@@ -791,7 +800,7 @@ extern "C" int mochii_transport_pass(mochii_ctx* c, int with_peel, mochii_pass_s
     CK(c, cudaMemsetAsync(c->tally, 0, (size_t)n * c->ntally * tsz, c->stream));
     CK(c, cudaMemsetAsync(c->jt, 0, (size_t)n * c->nnu * tsz, c->stream));
     if (c->metal.ntr > 0 && c->metal.nmb > 0)   // species_rate_path_reset (species_mod.f90:321-326)
-        CK(c, cudaMemsetAsync(c->metal.mom, 0, (size_t)n * c->metal.nmb * kMomDeg * tsz, c->stream));
+        CK(c, cudaMemsetAsync(c->metal.mom, 0, mom_bytes(c), c->stream));
     else if (c->metal.ntr > 0)
         CK(c, cudaMemsetAsync(c->metal.raw, 0, (size_t)n * c->metal.ntrp * 2 * tsz, c->stream));
     CK(c, cudaMemsetAsync(c->tw.counters, 0, 4 * sizeof(unsigned long long), c->stream));

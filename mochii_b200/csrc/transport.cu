@@ -21,6 +21,7 @@
 #include <stdint.h>
 
 #include <mutex>
+#include <type_traits>
 
 #include "ctx.h"
 #include "metals.cuh"
@@ -443,6 +444,17 @@ struct MetalPacket {
                 tally_add(rw + 2 * k + 1, w * mhc[k * tb + tx]);
             }
         } else if constexpr (MET == 2) {
+            if constexpr (std::is_same<R, float>::value && std::is_same<T, double>::value) {
+                if (m.mom32) {   // FP32 moments: one sector, two vector reductions
+                    float* mt = static_cast<float*>(m.mom) + ((long long)il * m.nmb + mb) * 8;
+                    asm volatile("red.global.add.v4.f32 [%0], {%1, %2, %3, %4};" ::"l"(mt), "f"(w * phi[0]),
+                                 "f"(w * phi[1]), "f"(w * phi[2]), "f"(w * phi[3])
+                                 : "memory");
+                    asm volatile("red.global.add.v2.f32 [%0], {%1, %2};" ::"l"(mt + 4), "f"(w * phi[4]), "f"(w * phi[5])
+                                 : "memory");
+                    return;
+                }
+            }
             T* mt = static_cast<T*>(m.mom) + ((long long)il * m.nmb + mb) * kMomDeg;
 #pragma unroll
             for (int q = 0; q < kMomDeg; ++q) tally_add(mt + q, w * phi[q]);
@@ -875,6 +887,7 @@ __global__ void __launch_bounds__(128) k_walk_amr(const PassArgs a, const Packet
 template <typename T>
 __device__ __forceinline__ double tval(const T& v);
 template <> __device__ __forceinline__ double tval<double>(const double& v) { return v; }
+template <> __device__ __forceinline__ double tval<float>(const float& v) { return (double)v; }
 template <> __device__ __forceinline__ double tval<float2>(const float2& v) { return (double)v.x + (double)v.y; }
 
 //
@@ -950,10 +963,11 @@ __global__ void k_metal_rates(const MetalDev m, long long nleaf, double cg, doub
 // terms in the same order (b, then q, ascending) and zeros before them.
 // Block: 64 leaves x all outputs, 256 threads, each 4 leaves x NU outputs;
 // the moments and coefficients staged through shared memory KC orders at a
-// time.
+// time.  RS: the words per (leaf, bin) in the tally (kMomDeg, or 8 for the
+// padded FP32 moments).
 constexpr int kRtM = 64, kRtThreads = 256;
 
-template <typename T, int NU, int KC>
+template <typename T, int NU, int KC, int RS>
 __global__ void __launch_bounds__(kRtThreads) k_metal_rates_mom(const MetalDev m, long long nleaf, double cg,
                                                                 double ch, const double4* lg, double d2) {
     __shared__ double sA[kRtM][KC + 1];
@@ -975,7 +989,10 @@ __global__ void __launch_bounds__(kRtThreads) k_metal_rates_mom(const MetalDev m
                 const int r = e / KC, q = e - r * KC;
                 const long long il = l0 + r;
                 const int kk = k0 + q;
-                sA[r][q] = (il < nleaf && kk < K) ? tval<T>(mom[il * K + kk]) : 0.0;
+                const int bin = kk / kMomDeg;
+                sA[r][q] = (il < nleaf && kk < K)
+                               ? tval<T>(mom[il * ((long long)m.nmb * RS) + bin * RS + (kk - bin * kMomDeg)])
+                               : 0.0;
             }
             for (int e = tid; e < KC * 16 * NU; e += kRtThreads) {
                 const int r = e / (16 * NU), q = e - r * (16 * NU);
@@ -1358,10 +1375,14 @@ cudaError_t launch_rates(mochii_ctx* c) {
         const int mb = (int)std::min<long long>((n + kRtM - 1) / kRtM, 148LL * 8);
         const int N = 2 * c->metal.ntrp;
         const bool pairs = c->fp32 && !c->tally64;
-#define MOM(NU, KC)                                                                                       \
-    do {                                                                                                  \
-        if (pairs) k_metal_rates_mom<float2, NU, KC><<<mb, kRtThreads, 0, c->stream>>>(c->metal, n, cg, ch, lg, d2); \
-        else k_metal_rates_mom<double, NU, KC><<<mb, kRtThreads, 0, c->stream>>>(c->metal, n, cg, ch, lg, d2);       \
+#define MOM(NU, KC)                                                                                              \
+    do {                                                                                                         \
+        if (c->metal.mom32)                                                                                      \
+            k_metal_rates_mom<float, NU, KC, 8><<<mb, kRtThreads, 0, c->stream>>>(c->metal, n, cg, ch, lg, d2);  \
+        else if (pairs)                                                                                          \
+            k_metal_rates_mom<float2, NU, KC, kMomDeg><<<mb, kRtThreads, 0, c->stream>>>(c->metal, n, cg, ch, lg, d2); \
+        else                                                                                                     \
+            k_metal_rates_mom<double, NU, KC, kMomDeg><<<mb, kRtThreads, 0, c->stream>>>(c->metal, n, cg, ch, lg, d2); \
     } while (0)
         if (N <= 32) MOM(2, 32);
         else if (N <= 64) MOM(4, 32);
