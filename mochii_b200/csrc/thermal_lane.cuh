@@ -201,15 +201,15 @@ __device__ __forceinline__ void lane_fracs(int ns, const double (&n)[kMaxSt - 1]
     for (int i = 1; i < kMaxSt; ++i) f[i] = i <= nt ? f[i - 1] * r[i - 1] : 0.0;
 }
 
-// species_metal_sums: metal electrons and the two CX rates hydrogen sees.
-// The sums accumulate in registers and are stored once at the end (the
-// outputs live in the caller's frame).
+// species_metal_sums: metal electrons and the two CX rates hydrogen sees,
+// over the elements e0, e0 + estep, ...  The sums accumulate in registers
+// and are stored once at the end (the outputs live in the caller's frame).
 __device__ __noinline__ void lane_sums(const LaneCache c, double nH, double ne, double nHI, double nHII, double& nem_out,
-                                       double& rin_out, double& rout_out) {
+                                       double& rin_out, double& rout_out, int e0 = 0, int estep = 1) {
     const int nel = c.nel;
     const MetalEl* __restrict__ els = c.el;
     double nem = 0.0, rin = 0.0, rout = 0.0;
-    for (int ie = 0; ie < nel; ++ie) {
+    for (int ie = e0; ie < nel; ie += estep) {
         const MetalEl e = els[ie];
         double n[kMaxSt - 1], d[kMaxSt - 1], xi[kMaxSt - 1], xr[kMaxSt - 1], f[kMaxSt];
         lane_rates(c, e, ne, nHI, nHII, n, d, xi, xr);
@@ -227,6 +227,51 @@ __device__ __noinline__ void lane_sums(const LaneCache c, double nH, double ne, 
     nem_out = nem;
     rin_out = rin;
     rout_out = rout;
+}
+
+// The cascade sums of every lane with `need`, computed by the whole warp
+// (every lane enters): with k such lanes, each is served by G = 8, 4, 2 or 1
+// lanes (k <= 4, 8, 16, more), which split its elements (group lane s takes
+// elements s, s + G, ...; the caches are in shared memory, so any lane can
+// read them) and add their parts by shuffles within the group.  A search's
+// tail, where a few lanes are still iterating, then runs on all 32 lanes.
+__device__ __forceinline__ void warp_sums(const LaneCache& c, bool need, double nH, double ne, double nHI, double nHII,
+                                          double& em, double& rin, double& rout) {
+    const unsigned mask = __ballot_sync(kFull, need);
+    const int k = __popc(mask);
+    const int lane = threadIdx.x & 31;
+    const int G = k <= 4 ? 8 : k <= 8 ? 4 : k <= 16 ? 2 : 1;
+    if (G == 1) {
+        if (need) lane_sums(c, nH, ne, nHI, nHII, em, rin, rout);
+        return;
+    }
+    const int g = lane / G, sub = lane - g * G;
+    int owner = lane;
+    if (g < k) {   // the g-th lane of the mask
+        unsigned m = mask;
+        for (int t = 0; t < g; ++t) m &= m - 1u;
+        owner = __ffs(m) - 1;
+    }
+    const double oH = __shfl_sync(kFull, nH, owner), oNe = __shfl_sync(kFull, ne, owner);
+    const double oHI = __shfl_sync(kFull, nHI, owner), oHII = __shfl_sync(kFull, nHII, owner);
+    double a = 0.0, b = 0.0, d = 0.0;
+    if (g < k) {
+        LaneCache co = c;
+        co.S = c.S + (owner - lane);
+        lane_sums(co, oH, oNe, oHI, oHII, a, b, d, sub, G);
+    }
+    for (int o = 1; o < G; o <<= 1) {
+        a = a + __shfl_xor_sync(kFull, a, o);
+        b = b + __shfl_xor_sync(kFull, b, o);
+        d = d + __shfl_xor_sync(kFull, d, o);
+    }
+    const int src = need ? __popc(mask & ((1u << lane) - 1u)) * G : lane;
+    const double ta = __shfl_sync(kFull, a, src), tb = __shfl_sync(kFull, b, src), td = __shfl_sync(kFull, d, src);
+    if (need) {
+        em = ta;
+        rin = tb;
+        rout = td;
+    }
 }
 
 // The metal terms of net_rate (as metal_thermal) from the shared cache.
@@ -658,10 +703,10 @@ __device__ __noinline__ void lane_finish(const ThArgs& a, const LaneCache& cache
         int itn = 0;
         bool run = fin;
         while (__any_sync(kFull, run)) {
-            if (!run) continue;
             const double ne_old = ne;
-            double nem, rin, rout;
-            lane_sums(cache, nH, ne_old, nHI, nHII, nem, rin, rout);
+            double nem = 0.0, rin, rout;
+            warp_sums(cache, run, nH, ne_old, nHI, nHII, nem, rin, rout);
+            if (!run) continue;
             ne = ne_HHe + nem;
             ne = fmax(0.5 * (ne + ne_old), 1.0e-12 * nH);
             if (fabs(ne - ne_old) <= 1.0e-10 * ne || ++itn >= 200) run = false;
@@ -723,10 +768,11 @@ __device__ __noinline__ void lane_solve(const ThArgs& a, unsigned long long* nex
         }
         int nsum = 0;
         while (__any_sync(kFull, need)) {   // one cascade sum per searching lane per trip
+            double em = 0.0, rin = 0.0, rout = 0.0;
+            const double x = need ? cs.xe() : 0.0;
+            const double cnH = need ? cs.nH : 0.0, cc = need ? cs.c : 0.0;
+            warp_sums(cache, need, cnH, cc, cnH * x, cnH * (1.0 - x), em, rin, rout);
             if (!need) continue;
-            double em, rin, rout;
-            const double x = cs.xe();
-            lane_sums(cache, cs.nH, cs.c, cs.nH * x, cs.nH * (1.0 - x), em, rin, rout);
             ++nsum;
             cs.h_feed(em, rin, rout);
             need = cs.settle();
