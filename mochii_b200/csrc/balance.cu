@@ -2315,15 +2315,20 @@ cudaError_t metal_ttable_build(mochii_ctx* c) {
     m.tdu = (u1 - u0) / (double)(nt - 6);
     m.tu0 = u0 - 3.0 * m.tdu;
     double* t = nullptr;
-    cudaError_t e = cudaMalloc(&t, (size_t)m.ntr * 4 * nt * 8);
+    // one allocation: the rate coefficients (ntr x 4 x nt), then the cooling fits (nst x nt)
+    cudaError_t e = cudaMalloc(&t, ((size_t)m.ntr * 4 + m.nst) * nt * 8);
     if (e != cudaSuccess) return e;
     c->ttab = t;
     MetalDev mb = m;
     mb.tnt = nt;
+    double* ct = t + (size_t)m.ntr * 4 * nt;
     k_metal_ttable<<<nblocks((long long)m.ntr * 4 * nt, 256, 148 * 16), 256, 0, c->stream>>>(mb, t);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    if (m.nst > 0) k_metal_ctable<<<nblocks((long long)m.nst * nt, 256, 148 * 16), 256, 0, c->stream>>>(mb, ct);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     if ((e = cudaStreamSynchronize(c->stream)) != cudaSuccess) return e;
     m.ttab = t;
+    m.ctab = ct;
     m.tnt = nt;
     return cudaSuccess;
 }

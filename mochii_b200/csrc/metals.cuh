@@ -163,6 +163,22 @@ static __global__ void k_metal_ttable(const MetalDev m, double* out) {
     }
 }
 
+// The line-cooling fit table: ln max(sum_k A_k exp(-T_k/T) / sqrt(T), 1e-300)
+// of every stage at every node (cooling_mod.f90:98-122 fits).
+static __global__ void k_metal_ctable(const MetalDev m, double* out) {
+    const long long total = (long long)m.nst * m.tnt;
+    for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < total; q += (long long)gridDim.x * blockDim.x) {
+        const int i = (int)(q % m.tnt);
+        const int s = (int)(q / m.tnt);
+        const double T = exp(m.tu0 + (double)i * m.tdu);
+        const MetalStage& st = m.st[s];
+        double fit = 0.0;
+        for (int k = 0; k < st.nterm; ++k) fit = fit + st.A[k] * exp(-st.Ti[k] / T);
+        fit = fit * (1.0 / sqrt(T));
+        out[q] = log(fmax(fit, 1.0e-300));
+    }
+}
+
 // Ratio chain n_{i+1}/n_i of one element from the cache; returns the stage-1
 // fraction 1/s and leaves the ratios in r (species_mod.f90:591-603, 794-812).
 __device__ __forceinline__ double metal_chain(const MetalCache& c, int tr0, int ns, double ne, double nHI, double nHII,

@@ -91,6 +91,7 @@ struct MetalDev {
     // transition on tnt nodes uniform in ln T from tu0 by tdu,
     // ttab[(j * 4 + c) * tnt + i]; tnt == 0: exact evaluation only
     const double* ttab = nullptr;
+    const double* ctab = nullptr;      // nst x tnt: ln of each stage's line-cooling fit at the same nodes
     int tnt = 0;
     double tu0 = 0.0, tdu = 0.0;
 };

@@ -65,24 +65,36 @@ struct LaneCache {
     __device__ __forceinline__ double& at(int s) const { return S[s * stride]; }
 };
 
-// species_ne_prepare at T for leaf il (as metal_prepare: the T table inside
-// its range, the clamped CX fits and any T outside it evaluated directly).
-__device__ __noinline__ void lane_prepare(const LaneCache c, long long il, double T) {
-    const MetalDev& m = *c.m;
-    int i0 = -1;
-    double w0 = 0.0, w1 = 0.0, w2 = 0.0, w3 = 0.0;
+// The 4-point Lagrange stencil of T on the ln T nodes of the T tables
+// (i0 < 0: T outside them, or no tables).
+struct TNode {
+    int i0;
+    double w0, w1, w2, w3;
+};
+__device__ __forceinline__ TNode t_node(const MetalDev& m, double T) {
+    TNode n = {-1, 0.0, 0.0, 0.0, 0.0};
     if (m.tnt > 0) {
         const double s = (log(T) - m.tu0) / m.tdu;
         const int i = (int)floor(s);
         if (i >= 1 && i <= m.tnt - 3) {
             const double t = s - (double)i;
-            w0 = -t * (t - 1.0) * (t - 2.0) / 6.0;
-            w1 = (t + 1.0) * (t - 1.0) * (t - 2.0) / 2.0;
-            w2 = -(t + 1.0) * t * (t - 2.0) / 2.0;
-            w3 = (t + 1.0) * t * (t - 1.0) / 6.0;
-            i0 = i - 1;
+            n.w0 = -t * (t - 1.0) * (t - 2.0) / 6.0;
+            n.w1 = (t + 1.0) * (t - 1.0) * (t - 2.0) / 2.0;
+            n.w2 = -(t + 1.0) * t * (t - 2.0) / 2.0;
+            n.w3 = (t + 1.0) * t * (t - 1.0) / 6.0;
+            n.i0 = i - 1;
         }
     }
+    return n;
+}
+
+// species_ne_prepare at T for leaf il (as metal_prepare: the T table inside
+// its range, the clamped CX fits and any T outside it evaluated directly).
+__device__ __noinline__ void lane_prepare(const LaneCache c, long long il, double T) {
+    const MetalDev& m = *c.m;
+    const TNode tn = t_node(m, T);
+    const int i0 = tn.i0;
+    const double w0 = tn.w0, w1 = tn.w1, w2 = tn.w2, w3 = tn.w3;
     for (int j = 0; j < m.ntr; ++j) {
         const MetalTr& r = m.tr[j];
         const double gam = m.egam[il * m.ntr + j];
@@ -285,6 +297,7 @@ __device__ __noinline__ MetalThermalTerms lane_thermal(const LaneCache c, const 
     const double rsT = 1.0 / sqrt(T);
     double ff = 0.0;
     const NlAt at = nl_at(td.tinv, T, ne);
+    const TNode tn = m.ctab ? t_node(m, T) : TNode{-1, 0.0, 0.0, 0.0, 0.0};
     for (int ie = 0; ie < m.nel; ++ie) {
         const MetalEl e = m.el[ie];
         double n[kMaxSt - 1], d[kMaxSt - 1], xi[kMaxSt - 1], xr[kMaxSt - 1], frac[kMaxSt];
@@ -297,8 +310,13 @@ __device__ __noinline__ MetalThermalTerms lane_thermal(const LaneCache c, const 
             const MetalStage& st = m.st[e.st0 + i - 1];
             if (!st.has_cool) continue;
             double fit = 0.0;
-            for (int q = 0; q < st.nterm; ++q) fit = fit + st.A[q] * exp(-st.Ti[q] / T);
-            fit = fit * rsT;
+            if (tn.i0 >= 0) {   // the fit from its ln T table
+                const double* Lt = m.ctab + (size_t)(e.st0 + i - 1) * m.tnt + tn.i0;
+                fit = exp(tn.w0 * Lt[0] + tn.w1 * Lt[1] + tn.w2 * Lt[2] + tn.w3 * Lt[3]);
+            } else {
+                for (int q = 0; q < st.nterm; ++q) fit = fit + st.A[q] * exp(-st.Ti[q] / T);
+                fit = fit * rsT;
+            }
             const double lam = st.table >= 0 ? nl_apply(m.lamref + (size_t)st.table * kNlNT,
                                                         m.Ssup + (size_t)st.table * kNlNT * kNlNNE,
                                                         m.lnL + (size_t)st.table * kNlNT * kNlNNE, at, fit)
