@@ -50,6 +50,13 @@ size_t mom_bytes(const mochii_ctx* c) {
     return (size_t)c->grid.nleaf * m.nmb * (m.mom32 ? 8 * sizeof(float) : kMomDeg * 8);
 }
 
+// Bytes of the exact metal tallies: two words (Gamma, heating path sums) per
+// transition slot, FP64 (or a compensated FP32 pair), or FP32 with raw32.
+size_t raw_bytes(const mochii_ctx* c) {
+    const MetalDev& m = c->metal;
+    return (size_t)c->grid.nleaf * m.ntrp * 2 * (m.raw32 ? sizeof(float) : 8);
+}
+
 void free_records(mochii_ctx* c) {
     for (void* q : {(void*)c->rec.tm, (void*)c->rec.td, (void*)c->rec.cell, (void*)c->rec.bits, c->rec.sig, c->rec.coef,
                     (void*)c->rec.E, c->rec.msig, c->rec.dsc, (void*)c->rec.p0})
@@ -413,7 +420,8 @@ extern "C" int mochii_init(const mochii_params* pin, mochii_ctx** out) {
             m.mom32 = c->fp32 && c->tally64;
             CKI(cudaMalloc(&m.mom, mom_bytes(c) + 64));
         } else {
-            CKI(cudaMalloc(&m.raw, (size_t)n * m.ntrp * 2 * tsz + 64));
+            m.raw32 = c->fp32 && c->tally64;
+            CKI(cudaMalloc(&m.raw, raw_bytes(c) + 64));
         }
     }
     // sampler tables, component table, bin edges, QMC tables
@@ -552,7 +560,7 @@ cudaError_t batch_pass(mochii_ctx* c, mochii_batch* b, int k, cudaStream_t s) {
         if (c->metal.ntr > 0 && c->metal.nmb > 0)
             e = cudaMemsetAsync(c->metal.mom, 0, mom_bytes(c), s);
         else if (c->metal.ntr > 0)
-            e = cudaMemsetAsync(c->metal.raw, 0, (size_t)n * c->metal.ntrp * 2 * tsz, s);
+            e = cudaMemsetAsync(c->metal.raw, 0, raw_bytes(c), s);
         if (e != cudaSuccess) break;
         if ((e = cudaMemsetAsync(c->tw.counters, 0, 4 * sizeof(unsigned long long), s)) != cudaSuccess) break;
         if ((e = launch_transport(c)) != cudaSuccess) break;
@@ -802,7 +810,7 @@ extern "C" int mochii_transport_pass(mochii_ctx* c, int with_peel, mochii_pass_s
     if (c->metal.ntr > 0 && c->metal.nmb > 0)   // species_rate_path_reset (species_mod.f90:321-326)
         CK(c, cudaMemsetAsync(c->metal.mom, 0, mom_bytes(c), c->stream));
     else if (c->metal.ntr > 0)
-        CK(c, cudaMemsetAsync(c->metal.raw, 0, (size_t)n * c->metal.ntrp * 2 * tsz, c->stream));
+        CK(c, cudaMemsetAsync(c->metal.raw, 0, raw_bytes(c), c->stream));
     CK(c, cudaMemsetAsync(c->tw.counters, 0, 4 * sizeof(unsigned long long), c->stream));
     CK(c, cudaEventRecord(c->ev0, c->stream));
     CK(c, launch_transport(c));

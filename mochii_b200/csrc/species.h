@@ -86,6 +86,7 @@ struct MetalDev {
     const int* jof = nullptr;          // ntrp: element-order index of each threshold-order index (-1: padding)
     void* mom = nullptr;               // nleaf x nmb x kMomDeg tallies, or with mom32 nleaf x nmb x 8 floats
     int mom32 = 0;                     // FP32 moments, one 32-byte sector per (leaf, bin): FP32 segments with FP64 tallies
+    int raw32 = 0;                     // FP32 exact tallies (same condition): 8 bytes per transition, vector reductions
     // T table of the rate coefficients (thermal solve): ln of collisional
     // ionisation, recombination, CX ionisation, CX recombination per
     // transition on tnt nodes uniform in ln T from tu0 by tdu,

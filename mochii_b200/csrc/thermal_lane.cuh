@@ -383,6 +383,10 @@ struct CellSolve {
     // points, 3 Illinois steps, 4 the sums at the root, 5 done
     int hph, hk, hkk;
     double hx, hprev, xa, xb, Ra, Rb, hscale, A, B, hnem;
+    // the last two evaluations (n_e, x) of this solve: the H root's start is
+    // their linear extrapolation to the next n_e
+    double pc1, px1, pc2, px2;
+    int npv;
 
     // the x at which the pending sum is taken
     __device__ __forceinline__ double xe() const { return hph == 1 ? 0.0 : hph == 2 ? 1.0 : hx; }
@@ -393,7 +397,9 @@ struct CellSolve {
         hnem = 0.0;
         if (with_cx) {
             hph = 0; hk = 0; hkk = 0;
-            hx = fmin(fmax(ec.x, 0.0), 1.0);
+            double xg = ec.x;
+            if (npv >= 2 && pc1 != pc2) xg = px1 + (px1 - px2) * ((c - pc1) / (pc1 - pc2));
+            hx = fmin(fmax(xg, 0.0), 1.0);
             hprev = 1.0e300;
             xa = 0.0; xb = 1.0; Ra = 0.0; Rb = 0.0; hscale = 0.0;
         } else {
@@ -460,6 +466,9 @@ struct CellSolve {
         const double r1 = fmin((g1 + k.cHe1 * c) / (k.aHe2 * c), 1.0e150);
         const double r2 = fmin((g2 + k.cHe2 * c) / (k.aHe3 * c), 1.0e150);
         ec.x = hx;
+        pc2 = pc1; px2 = px1;
+        pc1 = c; px1 = hx;
+        ++npv;
         ec.h1 = 1.0 / (1.0 + r1 + r1 * r2);
         ec.h2 = ec.h1 * r1;
         const double h3 = ec.h2 * r2;
@@ -552,6 +561,7 @@ struct CellSolve {
         top = nemax * nH;
         ph = 0; nev = 0; side = 0; it = 0;
         fa = 0.0; b = 0.0; fb = 0.0; fac = 4.0; la = 0.0; lb = 0.0;
+        npv = 0; pc1 = pc2 = px1 = px2 = 0.0;
         ea = {xHI, xHeI, xHeII};
         eb = ea;
         ec = ea;

@@ -437,6 +437,23 @@ struct MetalPacket {
     __device__ __forceinline__ void score(const MetalDev& m, int il, R w, const R* msg, const R* mhc) const {
         const int tb = blockDim.x, tx = threadIdx.x;
         if constexpr (MET == 1) {
+            if constexpr (std::is_same<R, float>::value && std::is_same<T, double>::value) {
+                if (m.raw32) {   // FP32 exact tallies: two transitions per vector reduction
+                    float* rw = static_cast<float*>(m.raw) + (long long)il * m.ntrp * 2;
+                    const R wi = w * invE;
+                    int k = 0;
+                    for (; k + 1 < nm; k += 2)
+                        asm volatile("red.global.add.v4.f32 [%0], {%1, %2, %3, %4};" ::"l"(rw + 2 * k),
+                                     "f"(wi * msg[k * tb + tx]), "f"(w * mhc[k * tb + tx]),
+                                     "f"(wi * msg[(k + 1) * tb + tx]), "f"(w * mhc[(k + 1) * tb + tx])
+                                     : "memory");
+                    if (k < nm)
+                        asm volatile("red.global.add.v2.f32 [%0], {%1, %2};" ::"l"(rw + 2 * k), "f"(wi * msg[k * tb + tx]),
+                                     "f"(w * mhc[k * tb + tx])
+                                     : "memory");
+                    return;
+                }
+            }
             T* rw = static_cast<T*>(m.raw) + (long long)il * m.ntrp * 2;
             const R wi = w * invE;
             for (int k = 0; k < nm; ++k) {
@@ -1390,7 +1407,8 @@ cudaError_t launch_rates(mochii_ctx* c) {
 #undef MOM
     } else if (c->metal.ntr > 0) {
         const int mb = grid_blocks(n * c->metal.ntr, 256, 148 * 16);
-        if (c->fp32 && !c->tally64) k_metal_rates<float2><<<mb, 256, 0, c->stream>>>(c->metal, n, cg, ch, lg, d2);
+        if (c->metal.raw32) k_metal_rates<float><<<mb, 256, 0, c->stream>>>(c->metal, n, cg, ch, lg, d2);
+        else if (c->fp32 && !c->tally64) k_metal_rates<float2><<<mb, 256, 0, c->stream>>>(c->metal, n, cg, ch, lg, d2);
         else k_metal_rates<double><<<mb, 256, 0, c->stream>>>(c->metal, n, cg, ch, lg, d2);
     }
     return cudaGetLastError();

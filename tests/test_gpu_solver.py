@@ -159,8 +159,15 @@ def test_lane_layout_refills_lanes():
         dT = np.abs(b_[0] - a_[0])
         assert np.median(dT) < 1e-6 and dT.max() < 1.0, (cx, dT.max())
         assert np.max(np.abs(b_[1] - a_[1])) < 1e-5
-        assert np.median(np.abs(b_[5] / a_[5] - 1)) < 1e-8
-        assert abs(b_[2] / a_[2] - 1) < 0.01 and abs(b_[4] / a_[4] - 1) < 0.01
+        # n_e where hydrogen is ionized, to the T root's tolerance (1e-5 in
+        # ln T); in neutral leaves n_e ~ n_H (1 - x_HI) ~ 1e-9 n_H sits below
+        # the H root's resolution and differs between root paths by percents
+        ion = a_[1] < 0.99
+        assert ion.sum() > 1000
+        assert np.max(np.abs(b_[5][ion] / a_[5][ion] - 1)) < 1e-4
+        # the same temperature trials; the per-lane H root starts from the
+        # extrapolation of its last two n_e evaluations, so it needs fewer sums
+        assert abs(b_[2] / a_[2] - 1) < 0.01 and b_[4] <= 1.01 * a_[4]
 
 
 def test_metal_rate_table_matches_exact():
