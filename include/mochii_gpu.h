@@ -158,6 +158,12 @@ typedef struct mochii_params {
     /* packets per launch-walk chunk (not a reference key, par%packet_chunk):
      * the size of the packet-record buffer, default 4194304 */
     int64_t packet_chunk;
+    /* walk order of a chunk's stellar packets (not a reference key,
+     * par%packet_order): 0 'launch' = the launch (Sobol) order (default);
+     * 1 'direction' = sorted by source and direction cell, so a warp's
+     * packets cross the same leaves (their tally reductions then meet on the
+     * same addresses, which measured slower on B200) */
+    int packet_order;
 } mochii_params;
 
 /* Per-pass statistics (ion_score_report_energy_closure, ion_score_mod.f90:364-387). */

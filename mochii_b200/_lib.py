@@ -55,7 +55,7 @@ class Params(C.Structure):
         ("fe_levels_full", C.c_int), ("metal_moments", C.c_int), ("solver_bracketed", C.c_int),
         ("lambda_ref", C.c_double), ("taumax", C.c_double), ("tauhomo", C.c_double),
         ("solver_warp", C.c_int), ("tally64", C.c_int), ("metal_rate_table", C.c_int),
-        ("packet_chunk", C.c_int64),
+        ("packet_chunk", C.c_int64), ("packet_order", C.c_int),
     ]
 
 

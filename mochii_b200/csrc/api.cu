@@ -59,7 +59,8 @@ size_t raw_bytes(const mochii_ctx* c) {
 
 void free_records(mochii_ctx* c) {
     for (void* q : {(void*)c->rec.tm, (void*)c->rec.td, (void*)c->rec.cell, (void*)c->rec.bits, c->rec.sig, c->rec.coef,
-                    (void*)c->rec.E, c->rec.msig, c->rec.dsc, (void*)c->rec.p0})
+                    (void*)c->rec.E, c->rec.msig, c->rec.dsc, (void*)c->rec.p0, (void*)c->rec.key,
+                    (void*)c->rec.key_sorted, (void*)c->rec.seq, (void*)c->rec.perm, c->rec.sort_tmp})
         if (q) cudaFree(q);
     c->rec = RecordBuffers();
 }
@@ -84,6 +85,7 @@ cudaError_t alloc_records(mochii_ctx* c, long long cap) {
         if ((e = dalloc(&c->rec.E, (size_t)cap)) != cudaSuccess) return e;
         if ((e = cudaMalloc(&c->rec.msig, (size_t)c->metal.ntrp * cap * rsz + 64)) != cudaSuccess) return e;
     }
+    if (c->par.packet_order && (e = packet_order_alloc(c, cap)) != cudaSuccess) return e;
     return cudaSuccess;
 }
 
@@ -100,7 +102,8 @@ void release(mochii_ctx* c) {
                     (void*)c->metal.medge, c->metal.mom, c->twarm,
                     (void*)c->rec.E, c->rec.msig, c->oct_blob, c->rec.dsc, (void*)c->rec.p0,
                     (void*)c->dust_blob, (void*)c->rhokap, (void*)c->ttab, (void*)c->metal_lnl,
-                    (void*)c->th.lnL};
+                    (void*)c->th.lnL, (void*)c->rec.key, (void*)c->rec.key_sorted, (void*)c->rec.seq,
+                    (void*)c->rec.perm, c->rec.sort_tmp};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     for (cudaEvent_t e : {c->ev0, c->ev1, c->evA, c->evB})

@@ -62,6 +62,13 @@ struct RecordBuffers {
     void* dsc = nullptr;      // scattering: 2 x cap (dust scattering coefficient, <cos>)
     double* p0 = nullptr;     // scattering on the Cartesian grid: start point and direction, 6 x cap
     long long cap = 0;
+    // packet_order 'direction': keys, the walk order, and the sort's buffers
+    unsigned* key = nullptr;
+    unsigned* key_sorted = nullptr;
+    int* seq = nullptr;       // 0 .. cap-1
+    int* perm = nullptr;
+    void* sort_tmp = nullptr;
+    size_t sort_bytes = 0;
 };
 
 // Launch shapes chosen by the autotuner (tune.cu) or set by hand.

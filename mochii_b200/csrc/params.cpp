@@ -141,6 +141,7 @@ extern "C" int mochii_params_default(mochii_params* p) {
     p->tally64 = 1;
     p->metal_rate_table = 1;
     p->packet_chunk = 1 << 22;
+    p->packet_order = 0;
     return MOCHII_OK;
 }
 
@@ -278,6 +279,12 @@ int set_key(mochii_params* p, std::string key, const std::vector<std::string>& v
     if (key == "ion_dust_kext") { copy_str(p->ion_dust_kext, sizeof(p->ion_dust_kext), unquote(v)); return 0; }
     if (key == "data_dir") { copy_str(p->data_dir, sizeof(p->data_dir), unquote(v)); return 0; }
     if (key == "atomic_dir") { copy_str(p->atomic_dir, sizeof(p->atomic_dir), unquote(v)); return 0; }
+    if (key == "packet_order") {
+        const std::string s = lower(unquote(v));
+        if (s != "direction" && s != "launch") return bad("must be 'direction' or 'launch'");
+        p->packet_order = s == "direction";
+        return 0;
+    }
     if (key == "packet_chunk") {
         if (!parse_int(v, &i) || i < 1024) return bad("must be an integer >= 1024");
         p->packet_chunk = i;

@@ -25,7 +25,23 @@ struct PacketRecords {
     void* dsc;     // scattering only: 2 x cap of R, dust scattering coefficient and <cos>
     double* p0;    // scattering on the Cartesian grid: start point and direction, 6 x cap
     long long cap;
+    unsigned* key = nullptr;     // packet_order 'direction': source and direction cell of each packet
+    const int* perm = nullptr;   // walk order (the chunk's packets by key), null: launch order
 };
+
+constexpr int kPacketKeyBits = 18;
+
+// Walk-order key of a stellar packet: source component (3 bits), direction
+// octant (3 bits) and a 64 x 64 cell of (|k_x|, |k_y|) in the octant,
+// Morton-interleaved so nearby directions get nearby keys.
+__device__ __forceinline__ unsigned packet_dir_key(int ic, const double* kk) {
+    const unsigned oct = (kk[0] < 0.0 ? 1u : 0u) | (kk[1] < 0.0 ? 2u : 0u) | (kk[2] < 0.0 ? 4u : 0u);
+    const unsigned qx = (unsigned)min((int)(fabs(kk[0]) * 64.0), 63), qy = (unsigned)min((int)(fabs(kk[1]) * 64.0), 63);
+    unsigned m = 0;
+#pragma unroll
+    for (int b = 0; b < 6; ++b) m |= (((qx >> b) & 1u) << (2 * b)) | (((qy >> b) & 1u) << (2 * b + 1));
+    return ((unsigned)(ic & 7) << 15) | (oct << 12) | m;
+}
 
 template <typename R>
 __device__ __forceinline__ void write_cross_sections(const PacketRecords& rec, long long i, double E) {

@@ -23,6 +23,8 @@
 #include <mutex>
 #include <type_traits>
 
+#include <cub/cub.cuh>
+
 #include "ctx.h"
 #include "metals.cuh"
 #include "physics.cuh"
@@ -300,6 +302,7 @@ __global__ void __launch_bounds__(kThreads) k_launch(const PassArgs a, PacketRec
         write_record<R>(rec, i, pos, kk, E, inu, a.org, a.dcell, a.n);
     if (a.xs) write_grain_record<R>(rec, i, a.dust, a.scatter, a.eion_min, E, pos, kk, AMR ? 0 : 1);
     if (a.m.ntr > 0) write_metal_record<R>(rec, a.m, i, E);
+    if (rec.key) rec.key[i] = packet_dir_key(ic, kk);
 }
 
 // Absorber columns of one leaf, loaded ahead of use.
@@ -681,7 +684,8 @@ __global__ void __launch_bounds__(128) k_walk_edge(const PassArgs a, const Packe
     const long long c = rec.cap;
     const long long stride = (long long)gridDim.x * blockDim.x;
     const int nx = a.n[0], ny = a.n[1], nz = a.n[2];
-    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+    for (long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x; j < n; j += stride) {
+        const long long i = rec.perm ? (long long)rec.perm[j] : j;
         Stepper g;
         g.t0 = rec.tm[i]; g.t1 = rec.tm[c + i]; g.t2 = rec.tm[2 * c + i];
         g.d0 = rec.td[i]; g.d1 = rec.td[c + i]; g.d2 = rec.td[2 * c + i];
@@ -812,7 +816,8 @@ __global__ void __launch_bounds__(128) k_walk_amr(const PassArgs a, const Packet
     const R* cfp = static_cast<const R*>(rec.coef);
     const long long c = rec.cap;
     const long long stride = (long long)gridDim.x * blockDim.x;
-    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+    for (long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x; j < n; j += stride) {
+        const long long i = rec.perm ? (long long)rec.perm[j] : j;
         double x = rec.tm[i], y = rec.tm[c + i], z = rec.tm[2 * c + i];
         const double kx = rec.td[i], ky = rec.td[c + i], kz = rec.td[2 * c + i];
         int il = rec.cell[i];
@@ -1322,7 +1327,32 @@ PacketRecords packet_records(mochii_ctx* c) {
     r.msig = c->rec.msig;
     r.dsc = c->rec.dsc;
     r.p0 = c->rec.p0;
+    r.key = c->rec.key;
     return r;
+}
+
+namespace {
+__global__ void k_seq(int* v, long long n) {
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        v[i] = (int)i;
+}
+}  // namespace
+
+// The walk-order buffers of packet_order 'direction' for chunks of cap packets.
+cudaError_t packet_order_alloc(mochii_ctx* c, long long cap) {
+    RecordBuffers& r = c->rec;
+    cudaError_t e;
+    if ((e = cudaMalloc(&r.key, (size_t)cap * 4)) != cudaSuccess) return e;
+    if ((e = cudaMalloc(&r.key_sorted, (size_t)cap * 4)) != cudaSuccess) return e;
+    if ((e = cudaMalloc(&r.seq, (size_t)cap * 4)) != cudaSuccess) return e;
+    if ((e = cudaMalloc(&r.perm, (size_t)cap * 4)) != cudaSuccess) return e;
+    r.sort_bytes = 0;
+    if ((e = cub::DeviceRadixSort::SortPairs(nullptr, r.sort_bytes, r.key, r.key_sorted, r.seq, r.perm, (int)cap, 0,
+                                             kPacketKeyBits)) != cudaSuccess)
+        return e;
+    if ((e = cudaMalloc(&r.sort_tmp, r.sort_bytes + 16)) != cudaSuccess) return e;
+    k_seq<<<grid_blocks(cap, 256, 148 * 16), 256, 0, c->stream>>>(r.seq, cap);
+    return cudaGetLastError();
 }
 
 // The stellar packets of ionizing_field_and_rates (ionizing_field_mod.f90:
@@ -1343,7 +1373,15 @@ cudaError_t launch_transport(mochii_ctx* c) {
             if (amr) k_launch<double, true><<<lb, kThreads, 0, c->stream>>>(a, r, ip0, n);
             else k_launch<double, false><<<lb, kThreads, 0, c->stream>>>(a, r, ip0, n);
         }
-        const cudaError_t e = launch_walk_variant(c, a, r, WalkLaunch{n, ip0, acc, blocks, 0});
+        PacketRecords rw = r;
+        if (r.key) {   // walk the chunk's packets in (source, direction) order
+            cudaError_t e = cub::DeviceRadixSort::SortPairs(c->rec.sort_tmp, c->rec.sort_bytes, c->rec.key,
+                                                            c->rec.key_sorted, c->rec.seq, c->rec.perm, (int)n, 0,
+                                                            kPacketKeyBits, c->stream);
+            if (e != cudaSuccess) return e;
+            rw.perm = c->rec.perm;
+        }
+        const cudaError_t e = launch_walk_variant(c, a, rw, WalkLaunch{n, ip0, acc, blocks, 0});
         if (e != cudaSuccess) return e;
     }
     return cudaGetLastError();

@@ -9,6 +9,7 @@ namespace mochii {
 
 int transport_blocks(const mochii_ctx* c);
 cudaError_t launch_transport(mochii_ctx* c);
+cudaError_t packet_order_alloc(mochii_ctx* c, long long cap);   // packet_order: keys, walk order, sort buffers
 PacketRecords packet_records(mochii_ctx* c);
 cudaError_t launch_transport_diffuse(mochii_ctx* c, double total, long long nd);
 cudaError_t diffuse_build(mochii_ctx* c, double* total);

@@ -88,12 +88,15 @@ def test_namelist_errors(lib):
 
 
 def test_execution_keys(lib):
-    from mochii_b200 import default_params, parse_namelist
+    from mochii_b200 import MochiiError, default_params, parse_namelist
     d = default_params()
     assert d.packet_chunk == 1 << 22 and d.tally64 == 1 and d.metal_rate_table == 1 and d.solver_warp == 3
     p = parse_namelist("&parameters par%packet_chunk = 1048576, par%tally_precision = 'compensated'\n"
                        " par%metal_rates = 'exact', par%cell_layout = 'flow' /")
     assert p.packet_chunk == 1048576 and p.tally64 == 0 and p.metal_rate_table == 0 and p.solver_warp == 2
+    assert d.packet_order == 0 and parse_namelist("&parameters par%packet_order = 'direction' /").packet_order == 1
+    with pytest.raises(MochiiError, match="'direction' or 'launch'"):
+        parse_namelist("&parameters par%packet_order = 'random' /")
 
 
 def test_reference_style_input_reads_unchanged(lib, tmp_path):

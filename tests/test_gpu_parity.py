@@ -108,9 +108,12 @@ def partially_ionised_state(n, L):
     return {"x_HI": xHI}
 
 
-def test_fp64_pass_matches_oracle(orc):
+@pytest.mark.parametrize("order", ["launch", "direction"])
+def test_fp64_pass_matches_oracle(orc, order):
+    """Also with the walk in (source, direction) order: the same packets,
+    visited in another order, score the same tallies."""
     n = 32
-    nl = small_nl(n=n, nphot=20000)
+    nl = small_nl(n=n, nphot=20000).replace("/\n", f" par%packet_order = '{order}'\n/\n")
     L = parse_namelist(nl).xmax
     neb, sim, st = pass_pair(orc, nl, partially_ionised_state(n, L))
     for f in ("gamma_HI", "heat_HI"):
