@@ -72,9 +72,12 @@ METRIC = "packets/s on 1 B200 (transport + balance iteration)"
 UNIT = "packets/s"
 
 
-# DRAM bytes per scored segment of the transport kernels, from the ncu
-# captures summarised in profiles/ (absent until captured).
-DRAM_BYTES_PER_SEGMENT = {}
+# DRAM bytes (read + written) per scored segment of the transport kernels,
+# from the ncu captures summarised in profiles/: hii_metals at 96^3 (FP32
+# segments, FP64 tallies, FP32 moments), the stellar and diffuse walks of one
+# pass, 29.97 GB over 1.742e8 segments; scaled to the 128^3 pass by its
+# segment count (the traffic grows with the segments).
+DRAM_BYTES_PER_SEGMENT = {"hii_metals128": 172.1}
 
 
 class Workload:
