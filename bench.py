@@ -495,7 +495,7 @@ def main():
     mean_ms = float(np.mean(kern_ms))
     achieved = alg_bytes / (mean_ms * 1e-3) / 1e9
     traffic = None
-    if DRAM_BYTES_PER_SEGMENT.get(wl.name):
+    if DRAM_BYTES_PER_SEGMENT.get(wl.name) and prec == "fp32" and args.tally == "fp64":   # the captured configuration
         traffic = DRAM_BYTES_PER_SEGMENT[wl.name] * mean_seg
 
     cpu = None
