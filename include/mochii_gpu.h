@@ -244,7 +244,10 @@ int mochii_opacity_fill(mochii_ctx* ctx);
  * as one CUDA graph at the first mochii_batch_iterate and replayed after.
  * The contexts must not use the diffuse field (its packet count is read back
  * mid-pass) or the MLP warm start; their own calls stay usable between
- * iterations, but changing a context's parameters or tuning needs a new batch. */
+ * iterations, but changing a context's parameters or tuning (mochii_set_nphotons,
+ * mochii_set_tuning, mochii_autotune, a first T_warm or MLP warm start) needs
+ * a new batch: mochii_batch_iterate refuses with MOCHII_ERR_BAD_PARAM before
+ * any launch when a context changed after mochii_batch_create. */
 typedef struct mochii_batch mochii_batch;
 int mochii_batch_create(mochii_ctx* const* ctxs, int n, mochii_batch** out);
 /* stats[n], m[n] receive each nebula's pass statistics and balance metrics;
@@ -323,7 +326,9 @@ int mochii_diffuse_records(mochii_ctx* ctx, int64_t ip0, int64_t n, double* out8
  * by every GPU that loads the library until exit).  n <= 65536 records per
  * call, larger n is refused with MOCHII_ERR_BAD_PARAM.  The first call on a
  * device looks up that array's device address (make it before any stream
- * capture).  Calls share the array: calls that overlap on the GPU race. */
+ * capture).  The context's device must be the current device (else
+ * MOCHII_ERR_BAD_PARAM).  Calls share the array: calls that overlap on the
+ * GPU race. */
 int mochii_launch_records_noalloc(mochii_ctx* ctx, int64_t ip0, int64_t n, double* out8);
 
 /* ---- learned warm start of the thermal balance (no reference counterpart:

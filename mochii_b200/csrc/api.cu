@@ -543,6 +543,7 @@ struct mochii_batch {
     std::vector<unsigned long long*> tcount;        // 4 per nebula
     std::vector<double*> part;                      // 6 x balance blocks per nebula
     std::vector<unsigned long long*> bcount;        // 8 per nebula
+    std::vector<uint64_t> gen;                      // each context's generation at mochii_batch_create
     std::string err;
 };
 
@@ -641,6 +642,7 @@ extern "C" int mochii_batch_create(mochii_ctx* const* ctxs, int n, mochii_batch*
     }
     auto* b = new mochii_batch();
     b->ctx.assign(ctxs, ctxs + n);
+    for (int k = 0; k < n; ++k) b->gen.push_back(ctxs[k]->generation);
     cudaError_t e = cudaStreamCreateWithFlags(&b->s, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaEventCreate(&b->e0);
     if (e == cudaSuccess) e = cudaEventCreate(&b->e1);
@@ -685,9 +687,15 @@ extern "C" int mochii_batch_iterate(mochii_batch* b, int solve_te, mochii_pass_s
     if (!b) return MOCHII_ERR_BAD_PARAM;
     const int n = (int)b->ctx.size();
     const int slot = solve_te ? 1 : 0;
-    for (mochii_ctx* c : b->ctx)
+    for (int k = 0; k < n; ++k) {
+        mochii_ctx* c = b->ctx[k];
         if (solve_te && !c->thermal_ready)
             return fail(c, MOCHII_ERR_BAD_PARAM, "the thermal solve needs par%solve_te = .true. at mochii_init");
+        // the recorded graph holds this context's launch shapes and buffers
+        if (c->generation != b->gen[k])
+            return fail(c, MOCHII_ERR_BAD_PARAM,
+                        "a batched context's parameters or tuning changed after mochii_batch_create; create a new batch");
+    }
     cudaError_t e = cudaSuccess;
     for (mochii_ctx* c : b->ctx) {   // the contexts' own work first
         if (!c->columns_fresh) {
@@ -779,6 +787,7 @@ extern "C" double mochii_ion_Ltot(const mochii_ctx* c) { return c ? c->band.ion_
 
 extern "C" int mochii_set_nphotons(mochii_ctx* c, int64_t np) {
     if (!c || np < 1) return MOCHII_ERR_BAD_PARAM;
+    ++c->generation;
     c->par.nphotons = np;
     const int nb = transport_blocks(c);
     if (nb > c->tw.ledger_blocks) {
@@ -947,6 +956,7 @@ std::string tune_key(const mochii_ctx* c) {
 extern "C" int mochii_set_tuning(mochii_ctx* c, const mochii_tuning* t) {
     if (!c || !t || t->lookahead < 0 || t->lookahead > 2 || t->walk_blocks_per_sm < 1 || t->walk_blocks_per_sm > 64)
         return fail(c, MOCHII_ERR_BAD_PARAM, "tuning out of range (lookahead 0..2, blocks per SM 1..64)");
+    ++c->generation;
     c->tune.lookahead = t->lookahead;
     c->tune.walk_blocks_per_sm = t->walk_blocks_per_sm;
     const int nb = transport_blocks(c);
@@ -1083,7 +1093,10 @@ extern "C" int mochii_set_field(mochii_ctx* c, const char* name, const double* i
     const std::string nm(name);
     if (nm == "T_warm") {   // warm start of the next bracketed thermal solve
         if (n != c->grid.nleaf) return fail(c, MOCHII_ERR_BAD_PARAM, "size mismatch for T_warm");
-        if (!c->twarm) CK(c, dalloc(&c->twarm, (size_t)n));
+        if (!c->twarm) {
+            ++c->generation;
+            CK(c, dalloc(&c->twarm, (size_t)n));
+        }
         CK(c, cudaMemcpyAsync(c->twarm, in, n * 8, cudaMemcpyHostToDevice, c->stream));
         CK(c, cudaStreamSynchronize(c->stream));
         c->twarm_set = true;
@@ -1187,6 +1200,14 @@ extern "C" int mochii_launch_records_noalloc(mochii_ctx* c, int64_t ip0, int64_t
         return fail(c, MOCHII_ERR_BAD_PARAM,
                     "mochii_launch_records_noalloc: n exceeds the 65536 records of the static staging array");
     if (n == 0) return MOCHII_OK;
+    // the static array's address is per device: take it on the context's own
+    // device, never on whichever device the caller left current
+    int dev = -1;
+    CK(c, cudaGetDevice(&dev));
+    if (dev != c->device)
+        return fail(c, MOCHII_ERR_BAD_PARAM,
+                    "mochii_launch_records_noalloc: the current device is not the context's device; "
+                    "call cudaSetDevice on the context's device first");
     CK(c, launch_records_noalloc(c, ip0, n, out8));
     return MOCHII_OK;
 }

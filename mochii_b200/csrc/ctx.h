@@ -141,5 +141,9 @@ struct mochii_ctx {
     mochii::SpeciesHost species;
     bool thermal_ready = false;
     mochii::BalanceWork bw;
+    // bumped by every call that changes a launch parameter or reallocates a
+    // buffer a recorded batch graph holds (set_nphotons, set_tuning,
+    // autotune, the T_warm buffer); a batch refuses to replay after a change
+    uint64_t generation = 0;
     std::string last_error;
 };

@@ -574,7 +574,10 @@ extern "C" int mochii_mlp_warm_start(mochii_ctx* c, mochii_mlp* m) {
     const long long n = c->grid.nleaf, chunk = 1 << 20;
     int rc = ensure_batch(m, std::min<long long>(n, chunk));
     if (rc) return rc;
-    if (!c->twarm && cudaMalloc(&c->twarm, (size_t)n * 8 + 16) != cudaSuccess) return MOCHII_ERR_CUDA;
+    if (!c->twarm) {
+        ++c->generation;   // a new buffer: batches recorded before it are stale
+        if (cudaMalloc(&c->twarm, (size_t)n * 8 + 16) != cudaSuccess) return MOCHII_ERR_CUDA;
+    }
     if (cudaStreamSynchronize(c->stream) != cudaSuccess) return MOCHII_ERR_CUDA;
     for (long long i0 = 0; i0 < n; i0 += chunk) {
         const long long k = std::min<long long>(chunk, n - i0);

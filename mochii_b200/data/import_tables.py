@@ -1,6 +1,8 @@
 #!/usr/bin/env python3
 """Copy the physical data tables this path reads from a MoCHII checkout
-(default /root/reference, or argv[1]) into mochii_b200/data/.
+(its path is the one required argument) into mochii_b200/data/.
+
+  python import_tables.py <MoCHII checkout>
 
   atomic/cooling_<el>_<stage>.txt   collisional line-cooling fits (cooling_mod)
   atomic/nlevel_<el>_<stage>.txt    n-level atom data (nlevel_mod)
@@ -15,7 +17,9 @@ import os
 import shutil
 import sys
 
-SRC = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+if len(sys.argv) != 2:
+    sys.exit("usage: import_tables.py <path of a MoCHII checkout>")
+SRC = sys.argv[1]
 DST = os.path.dirname(os.path.abspath(__file__))
 
 os.makedirs(os.path.join(DST, "atomic"), exist_ok=True)

@@ -1,8 +1,8 @@
 #!/usr/bin/env python3
 """Regenerate the golden fixtures under tests/golden/ from the MoCHII source tree.
 
-Run once in a container that has the reference checkout (default path
-/root/reference, or pass it as argv[1]).  The fixtures it writes are small and
+Run once where a MoCHII checkout exists, with its path as the one required
+argument: python make_golden.py <MoCHII checkout>.  The fixtures it writes are small and
 committed, so the tests never read the reference tree at run time.
 
   qmc_golden.npz   Sobol integer codes pinned by the reference's own dumps
@@ -21,7 +21,9 @@ import sys
 
 import numpy as np
 
-REF = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+if len(sys.argv) != 2:
+    sys.exit("usage: make_golden.py <path of a MoCHII checkout>")
+REF = sys.argv[1]
 HERE = os.path.dirname(os.path.abspath(__file__))
 
 

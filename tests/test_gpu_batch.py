@@ -77,3 +77,26 @@ def test_packet_chunk_splits_the_pass():
         assert np.max(np.abs(b[big] / a[big] - 1)) < 1e-9, f
     one.close()
     many.close()
+
+
+def test_batch_refuses_a_changed_context():
+    """A recorded batch graph holds each context's launch shapes and
+    buffers: after mochii_set_nphotons on a batched context the next
+    iterate is refused (MOCHII_ERR_BAD_PARAM) before any launch, the
+    context's tallies are untouched, and a new batch runs."""
+    nebs = nebulae((8, 10))
+    batch = Batch(nebs)
+    batch.iterate()
+    g0 = nebs[0].get("gamma_HI")
+    nebs[0].set_nphotons(50000)
+    with pytest.raises(MochiiError) as ei:
+        batch.iterate()
+    assert ei.value.status == 1
+    assert np.array_equal(nebs[0].get("gamma_HI"), g0)
+    batch.close()
+    batch = Batch(nebs)
+    st, _, _ = batch.iterate()
+    assert st[0].packets == 50000
+    batch.close()
+    for neb in nebs:
+        neb.close()
