@@ -374,6 +374,8 @@ def main():
                          "lockstep nested loops, one flat machine per leaf, or one warp per leaf")
     ap.add_argument("--tally", default="fp64", choices=["fp64", "compensated"],
                     help="path tallies with FP32 segments: compensated FP32 pairs or FP64 atomics")
+    ap.add_argument("--order", default=None, choices=["launch", "direction", "coherent"],
+                    help="walk order of the stellar packets (default: the library's)")
     ap.add_argument("--grid", type=int, default=None, help="grid side of a Cartesian workload (default: its own)")
     ap.add_argument("--packets", type=int, default=None, help="stellar packets per pass (default: the workload's)")
     args = ap.parse_args()
@@ -400,9 +402,10 @@ def main():
     if dist is not None:
         dist.barrier()
 
+    order = f" par%packet_order = '{args.order}'\n" if args.order else ""
     par = parse_namelist(wl.make(wl.nphot, prec, 12345 + rank).replace(
         "/\n", f" par%thermal_solver = '{args.solver}'\n par%cell_layout = '{args.cell_layout}'\n"
-              f" par%tally_precision = '{args.tally}'\n/\n"))
+              f" par%tally_precision = '{args.tally}'\n{order}/\n"))
     neb = Nebula(par)
     prep_iters = prepare(neb, wl)
     tuning = neb.autotune(1 << 20)   # launch shape for this grid / precision / device

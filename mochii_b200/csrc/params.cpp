@@ -281,8 +281,9 @@ int set_key(mochii_params* p, std::string key, const std::vector<std::string>& v
     if (key == "atomic_dir") { copy_str(p->atomic_dir, sizeof(p->atomic_dir), unquote(v)); return 0; }
     if (key == "packet_order") {
         const std::string s = lower(unquote(v));
-        if (s != "direction" && s != "launch") return bad("must be 'direction' or 'launch'");
-        p->packet_order = s == "direction";
+        if (s != "direction" && s != "launch" && s != "coherent")
+            return bad("must be 'coherent', 'direction' or 'launch'");
+        p->packet_order = s == "coherent" ? 2 : s == "direction" ? 1 : 0;
         return 0;
     }
     if (key == "packet_chunk") {

@@ -27,7 +27,25 @@ struct PacketRecords {
     long long cap;
     unsigned* key = nullptr;     // packet_order 'direction': source and direction cell of each packet
     const int* perm = nullptr;   // walk order (the chunk's packets by key), null: launch order
+    const int* order = nullptr;  // packet_order 'coherent': record t holds chunk packet order[t]
 };
+
+// Walk-order key of packet_order 'coherent', from the packet's launch
+// uniforms alone (so the chunk can be sorted before its records exist):
+// source component (4 bits), a direction cell of 64 equal-area bands in
+// cos(theta) x 128 sectors in phi, the sectors of odd bands reversed so that
+// consecutive cells are neighbours on the sphere (13 bits), and the energy
+// quantile of the source spectrum in 256 steps (8 bits).  Packets of one
+// warp then leave in nearly the same direction with nearly the same energy,
+// so they cross the same leaves and score the same spectrum and moment bins.
+constexpr int kCohKeyBits = 25;
+__device__ __forceinline__ unsigned coherent_key(int ic, double umu, double uphi, double ue) {
+    const unsigned band = (unsigned)min((int)(umu * 64.0), 63);
+    unsigned sec = (unsigned)min((int)(uphi * 128.0), 127);
+    if (band & 1u) sec = 127u - sec;
+    const unsigned eq = (unsigned)min((int)(ue * 256.0), 255);
+    return ((unsigned)(ic & 15) << 21) | (((band << 7) | sec) << 8) | eq;
+}
 
 constexpr int kPacketKeyBits = 18;
 

@@ -274,7 +274,8 @@ __global__ void __launch_bounds__(kThreads) k_launch(const PassArgs a, PacketRec
     __syncthreads();
     const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    const long long ip = ip0 + i;
+    // packet_order 'coherent': record i is the chunk's packet rec.order[i]
+    const long long ip = ip0 + (rec.order ? (long long)rec.order[i] : i);
     double u[7];
     for (int d = 0; d < a.ndim; ++d) u[d] = qmc_uniform(sq, (uint64_t)ip, d, 0);
     int ic = 0;
@@ -303,6 +304,39 @@ __global__ void __launch_bounds__(kThreads) k_launch(const PassArgs a, PacketRec
     if (a.xs) write_grain_record<R>(rec, i, a.dust, a.scatter, a.eion_min, E, pos, kk, AMR ? 0 : 1);
     if (a.m.ntr > 0) write_metal_record<R>(rec, a.m, i, E);
     if (rec.key) rec.key[i] = packet_dir_key(ic, kk);
+}
+
+// Walk-order keys of packet_order 'coherent' for packets ip0 .. ip0+n-1 of
+// the stellar stream: the launch uniforms of gen_ion_photon_qmc
+// (ion_band_mod.f90:1880-1935) reduced to coherent_key.
+__global__ void __launch_bounds__(kThreads) k_coherent_keys(const PassArgs a, long long ip0, long long n,
+                                                            unsigned* __restrict__ key) {
+    __shared__ QmcTables sq;
+    {
+        const uint32_t* src = reinterpret_cast<const uint32_t*>(a.qmc);
+        uint32_t* dst = reinterpret_cast<uint32_t*>(&sq);
+        for (int i = threadIdx.x; i < (int)(sizeof(QmcTables) / 4); i += blockDim.x) dst[i] = src[i];
+    }
+    __syncthreads();
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const uint64_t ip = (uint64_t)(ip0 + i);
+    int ic = 0;
+    double ue, umu, uphi;
+    if (!a.multi) {
+        ue = qmc_uniform(sq, ip, 0, 0);
+        umu = qmc_uniform(sq, ip, 1, 0);
+        uphi = qmc_uniform(sq, ip, 2, 0);
+    } else {
+        const double u0 = qmc_uniform(sq, ip, 0, 0);
+        ic = a.ncomp - 1;
+        for (int k = 0; k < a.ncomp; ++k)
+            if (u0 <= a.comp[4 * k]) { ic = k; break; }
+        ue = qmc_uniform(sq, ip, 1, 0);
+        umu = qmc_uniform(sq, ip, 2, 0);
+        uphi = qmc_uniform(sq, ip, 3, 0);
+    }
+    key[i] = coherent_key(ic, umu, uphi, ue);
 }
 
 // Absorber columns of one leaf, loaded ahead of use.
@@ -792,6 +826,202 @@ __global__ void __launch_bounds__(128) k_walk_edge(const PassArgs a, const Packe
     walk_epilogue<METAL>(a, emitted, absorbed, escaped, nseg, kills, nact, nscat, accumulate, sh);
 }
 
+// ---- coherent walk with warp-aggregated tallies ----------------------------------
+// Sum of v over the lanes of `peers` (the lanes holding this lane's key),
+// left in the group's lowest lane, which the return value marks.  A pairwise
+// tree over each group's lanes in lane order: every round each remaining lane
+// adds the value of its next remaining peer, and the lanes whose rank in the
+// group is odd drop out; ceil(log2(group size)) rounds, none when every lane
+// is alone.  All 32 lanes must call it together.
+template <typename A, int N>
+__device__ __forceinline__ bool peer_sum(unsigned peers, int lane, A (&v)[N]) {
+    const unsigned below = (1u << lane) - 1u;
+    unsigned rest = peers & ~(below | (1u << lane));   // peers above this lane
+    int rank = __popc(peers & below);
+    while (__any_sync(0xffffffffu, rest != 0u)) {
+        const int next = __ffs(rest);                  // 1 + lane of the next remaining peer, 0: none
+        const int src = next ? next - 1 : lane;
+#pragma unroll
+        for (int k = 0; k < N; ++k) {
+            const A t = __shfl_sync(0xffffffffu, v[k], src);
+            if (next) v[k] += t;
+        }
+        const bool done = rank & 1;
+        const unsigned keep = __ballot_sync(0xffffffffu, !done);
+        rest = done ? 0u : (rest & keep);
+        rank >>= 1;
+    }
+    return (peers & below) == 0u;
+}
+
+// Walk kernel of packet_order 'coherent' (raytrace_ion_to_edge_car,
+// raytrace_amr.f90:534-592, and score_ion_path, ion_score_mod.f90:137-231):
+// each warp walks 32 consecutive packets of the sorted chunk -- nearly
+// parallel rays of nearly equal energy -- in step with one another.  Every
+// step the lanes that score the same (leaf, spectrum bin, moment bin) are
+// found with one match and their path luminosities summed over the warp, so
+// each distinct tally sector takes one reduction instead of one per lane:
+// the H/He rate tallies, the spectrum bin and (MET 2) the six energy
+// moments.  Exact metal tallies (MET 1) stay per lane.  The leaf sequences,
+// segments and energy ledger are those of k_walk_edge; only the summation
+// order of the tallies differs.  No grain or FUV terms (X = 0).
+template <typename R, int NABS, int LA, int MET, typename T>
+__global__ void __launch_bounds__(128) k_walk_coh(const PassArgs a, const PacketRecords rec, long long n,
+                                                  int accumulate) {
+    constexpr int NT = NABS == 1 ? 2 : 6;
+    constexpr bool METAL = MET > 0;
+    constexpr int NM = MET == 2 ? kMomDeg : 0;      // moment values aggregated per step
+    constexpr int NV = NT + 1 + NM;                  // + the spectrum bin
+    __shared__ double sh[128];
+    extern __shared__ __align__(16) unsigned char dsm[];
+    R* const msg = reinterpret_cast<R*>(dsm);
+    R* const mhc = msg + (MET == 1 ? a.m.ntrp * blockDim.x : 0);
+    double emitted = 0.0, absorbed = 0.0, escaped = 0.0;
+    unsigned long long nseg = 0, kills = 0, nact = 0, nscat = 0;
+    T* tal = static_cast<T*>(a.tally);
+    T* jt = static_cast<T*>(a.jt);
+    const R* sg = static_cast<const R*>(rec.sig);
+    const R* cfp = static_cast<const R*>(rec.coef);
+    const long long c = rec.cap;
+    const int nx = a.n[0], ny = a.n[1], nz = a.n[2];
+    const int lane = threadIdx.x & 31;
+    const long long warp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
+    const unsigned long long nnu = (unsigned long long)a.nnu;
+    const unsigned long long nmb = MET == 2 ? (unsigned long long)a.m.nmb : 1ull;
+    for (long long base = warp * 32; base < n; base += nwarps * 32) {
+        const long long i = base + lane;
+        bool alive = i < n;
+        const long long ir = alive ? i : base;   // a lane past the chunk end reads a valid record and idles
+        Stepper g;
+        g.t0 = rec.tm[ir]; g.t1 = rec.tm[c + ir]; g.t2 = rec.tm[2 * c + ir];
+        g.d0 = rec.td[ir]; g.d1 = rec.td[c + ir]; g.d2 = rec.td[2 * c + ir];
+        g.t_cur = 0.0;
+        const int cell = rec.cell[ir], bits = rec.bits[ir];
+        g.ix = cell & 1023; g.iy = (cell >> 10) & 1023; g.iz = (cell >> 20) & 1023;
+        g.sx = ((bits >> 16) & 3) - 1; g.sy = ((bits >> 18) & 3) - 1; g.sz = ((bits >> 20) & 3) - 1;
+        const int inu = bits & 0xFFFF;
+        const R s0 = sg[ir];
+        const R s1 = NABS == 1 ? (R)0 : sg[c + ir];
+        const R s2 = NABS == 1 ? (R)0 : sg[2 * c + ir];
+        R cf[NT];
+#pragma unroll
+        for (int k = 0; k < NT; ++k) cf[k] = cfp[k * c + ir];
+        MetalPacket<R, MET> mp;
+        if constexpr (METAL) mp.setup(a.m, rec, ir, msg, mhc);
+        int il[LA + 1] = {};
+        double sgm[LA + 1] = {};
+        Col<R, NABS> cl[LA + 1];
+        bool more[LA + 1];
+        more[0] = g.emit(nx, ny, nz, &il[0], &sgm[0]);
+        cl[0].load(a.col, il[0]);
+#pragma unroll
+        for (int k = 1; k <= LA; ++k) {
+            more[k] = false;
+            if (more[k - 1]) {
+                more[k] = g.emit(nx, ny, nz, &il[k], &sgm[k]);
+                cl[k].load(a.col, il[k]);
+            }
+        }
+        R expo = (R)1.0;
+        double tau = 0.0;
+        int nstep = 0;
+        while (__any_sync(0xffffffffu, alive)) {
+            R w = (R)0;
+            bool finish = false;
+            if (alive) {
+                if (++nstep > kMaxWalkSteps) {
+                    ++kills;
+                    finish = true;
+                } else {
+                    R kap = cl[0].template kappa<0>(s0, s1, s2, (R)0);
+                    if constexpr (METAL) {
+                        if (a.metal_abs) kap = kap + mp.kappa(a.m, il[0], msg);
+                    }
+                    const R ks = kap * (R)sgm[0];
+                    if (ks > (R)0) {
+                        const R eo = expo * attenuation(ks);
+                        w = (expo - eo) / kap;
+                        expo = eo;
+                    } else {
+                        w = expo * (R)sgm[0];
+                    }
+                    tau = tau + (double)ks;
+                    finish = tau >= kTauHuge || !more[0];
+                }
+            }
+            // score_ion_path over the warp: one reduction per distinct key
+            const bool scored = w != (R)0;   // score_ion_path returns on a zero path (ion_score_mod.f90:148)
+            const unsigned long long key =
+                scored ? (((unsigned long long)il[0] * nmb + (unsigned long long)mp.mb) * nnu + (unsigned long long)inu)
+                       : ~(unsigned long long)lane;
+            const unsigned peers = __match_any_sync(0xffffffffu, key);
+            R v[NV];
+#pragma unroll
+            for (int k = 0; k < NT; ++k) v[k] = w * cf[k];
+            v[NT] = w;
+            if constexpr (MET == 2) {
+#pragma unroll
+                for (int q = 0; q < NM; ++q) v[NT + 1 + q] = w * mp.phi[q];
+            }
+            const bool lead = peer_sum<R, NV>(peers, lane, v);
+            if (scored) {
+                ++nseg;
+                nact += mp.nm;
+                if (lead) {
+                    T* tl = tal + (long long)il[0] * NT;
+#pragma unroll
+                    for (int k = 0; k < NT; ++k) tally_add(tl + k, v[k]);
+                    tally_add(jt + (long long)il[0] * a.nnu + inu, v[NT]);
+                    if constexpr (MET == 2) {
+                        bool vec = false;
+                        if constexpr (std::is_same<R, float>::value && std::is_same<T, double>::value) {
+                            if (a.m.mom32) {   // FP32 moments: one sector, two vector reductions
+                                float* mt = static_cast<float*>(a.m.mom) + ((long long)il[0] * a.m.nmb + mp.mb) * 8;
+                                asm volatile("red.global.add.v4.f32 [%0], {%1, %2, %3, %4};" ::"l"(mt),
+                                             "f"(v[NT + 1]), "f"(v[NT + 2]), "f"(v[NT + 3]), "f"(v[NT + 4])
+                                             : "memory");
+                                asm volatile("red.global.add.v2.f32 [%0], {%1, %2};" ::"l"(mt + 4), "f"(v[NT + 5]),
+                                             "f"(v[NT + 6])
+                                             : "memory");
+                                vec = true;
+                            }
+                        }
+                        if (!vec) {
+                            T* mt = static_cast<T*>(a.m.mom) + ((long long)il[0] * a.m.nmb + mp.mb) * kMomDeg;
+#pragma unroll
+                            for (int q = 0; q < kMomDeg; ++q) tally_add(mt + q, v[NT + 1 + q]);
+                        }
+                    }
+                }
+                if constexpr (MET == 1) mp.template score<T>(a.m, il[0], w, msg, mhc);
+            }
+            if (alive) {
+                if (finish) {   // ion_score_energy_packet (ion_score_mod.f90:233-252)
+                    const double lum = a.Lpacket;
+                    const double tr = exp(-fmax(tau, 0.0));
+                    emitted += lum;
+                    absorbed += lum * (1.0 - tr);
+                    escaped += lum * tr;
+                    alive = false;
+                } else {
+#pragma unroll
+                    for (int k = 0; k < LA; ++k) {
+                        il[k] = il[k + 1]; sgm[k] = sgm[k + 1]; cl[k] = cl[k + 1]; more[k] = more[k + 1];
+                    }
+                    if (LA == 0 || more[LA - (LA > 0)]) {
+                        more[LA] = g.emit(nx, ny, nz, &il[LA], &sgm[LA]);
+                        cl[LA].load(a.col, il[LA]);
+                    } else {
+                        more[LA] = false;
+                    }
+                }
+            }
+        }
+    }
+    walk_epilogue<METAL>(a, emitted, absorbed, escaped, nseg, kills, nact, nscat, accumulate, sh);
+}
+
 // Walk kernel on the octree: raytrace_ion_to_edge_amr (raytrace_amr.f90:
 // 422-486, without the xy-periodic wrap) for the packets of one chunk,
 // grid-stride.  Per segment: the leaf's geometry record and columns (both
@@ -1259,7 +1489,14 @@ int transport_blocks(const mochii_ctx* c) {
 struct WalkLaunch {
     long long n, ip0;
     int acc, blocks, stream;
+    bool coherent = false;   // records in coherent_key order, walked by k_walk_coh
 };
+
+// packet_order 'coherent' applies to the stellar packets on the Cartesian
+// grid without grain or FUV terms; elsewhere the launch order is walked.
+bool coherent_walk_applies(const mochii_ctx* c) {
+    return c->par.packet_order == 2 && c->oct.ncells == 0 && !c->xscore && c->rec.key != nullptr;
+}
 
 // Walk-kernel variants: look-ahead depth 0..2 (the autotuned choice is
 // c->tune.lookahead); 128-thread blocks.
@@ -1280,6 +1517,24 @@ cudaError_t walk_la(mochii_ctx* c, const PassArgs& a, const PacketRecords& r, co
     return cudaGetLastError();
 }
 
+// The coherent walk (packet_order 'coherent', no grains): look-ahead 0..2.
+template <typename R, typename T, int V, int MET>
+cudaError_t walk_coh(mochii_ctx* c, const PassArgs& a, const PacketRecords& r, const WalkLaunch& w) {
+    constexpr int NABS = AbsV<V>::NABS;
+    const size_t smem = MET ? metal_smem(c) : 0;
+    if (MET && smem > 48 * 1024) {
+        cudaFuncSetAttribute(k_walk_coh<R, NABS, 0, MET, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        cudaFuncSetAttribute(k_walk_coh<R, NABS, 1, MET, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        cudaFuncSetAttribute(k_walk_coh<R, NABS, 2, MET, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    }
+    switch (c->tune.lookahead) {
+        case 0: k_walk_coh<R, NABS, 0, MET, T><<<w.blocks, 128, smem, c->stream>>>(a, r, w.n, w.acc); break;
+        case 1: k_walk_coh<R, NABS, 1, MET, T><<<w.blocks, 128, smem, c->stream>>>(a, r, w.n, w.acc); break;
+        default: k_walk_coh<R, NABS, 2, MET, T><<<w.blocks, 128, smem, c->stream>>>(a, r, w.n, w.acc); break;
+    }
+    return cudaGetLastError();
+}
+
 // The octree walk: no look-ahead variants.
 template <typename R, typename T, int V, int MET>
 cudaError_t walk_amr(mochii_ctx* c, const PassArgs& a, const PacketRecords& r, const WalkLaunch& w) {
@@ -1294,6 +1549,10 @@ cudaError_t walk_amr(mochii_ctx* c, const PassArgs& a, const PacketRecords& r, c
 template <typename R, typename T, int MET>
 cudaError_t walk_abs(mochii_ctx* c, const PassArgs& a, const PacketRecords& r, const WalkLaunch& w) {
     const bool amr = c->oct.ncells > 0;
+    if (w.coherent) {   // Cartesian grid, no grain or FUV terms (coherent_walk_applies)
+        if (abs_variant(c) == 1) return walk_coh<R, T, 1, MET>(c, a, r, w);
+        return walk_coh<R, T, 4, MET>(c, a, r, w);
+    }
     switch (abs_variant(c)) {
         case 1: return amr ? walk_amr<R, T, 1, MET>(c, a, r, w) : walk_la<R, T, 1, MET>(c, a, r, w);
         case 4: return amr ? walk_amr<R, T, 4, MET>(c, a, r, w) : walk_la<R, T, 4, MET>(c, a, r, w);
@@ -1327,7 +1586,7 @@ PacketRecords packet_records(mochii_ctx* c) {
     r.msig = c->rec.msig;
     r.dsc = c->rec.dsc;
     r.p0 = c->rec.p0;
-    r.key = c->rec.key;
+    r.key = c->par.packet_order == 1 ? c->rec.key : nullptr;   // 'direction': the launch writes the keys
     return r;
 }
 
@@ -1348,7 +1607,7 @@ cudaError_t packet_order_alloc(mochii_ctx* c, long long cap) {
     if ((e = cudaMalloc(&r.perm, (size_t)cap * 4)) != cudaSuccess) return e;
     r.sort_bytes = 0;
     if ((e = cub::DeviceRadixSort::SortPairs(nullptr, r.sort_bytes, r.key, r.key_sorted, r.seq, r.perm, (int)cap, 0,
-                                             kPacketKeyBits)) != cudaSuccess)
+                                             kCohKeyBits > kPacketKeyBits ? kCohKeyBits : kPacketKeyBits)) != cudaSuccess)
         return e;
     if ((e = cudaMalloc(&r.sort_tmp, r.sort_bytes + 16)) != cudaSuccess) return e;
     k_seq<<<grid_blocks(cap, 256, 148 * 16), 256, 0, c->stream>>>(r.seq, cap);
@@ -1366,6 +1625,23 @@ cudaError_t launch_transport(mochii_ctx* c) {
         const int lb = grid_blocks(n, kThreads, 1 << 30);
         const int acc = ip0 > 0;
         const bool amr = c->oct.ncells > 0;
+        if (coherent_walk_applies(c)) {   // sort the chunk by coherent_key, launch and walk in that order
+            k_coherent_keys<<<lb, kThreads, 0, c->stream>>>(a, ip0, n, c->rec.key);
+            cudaError_t e = cub::DeviceRadixSort::SortPairs(c->rec.sort_tmp, c->rec.sort_bytes, c->rec.key,
+                                                            c->rec.key_sorted, c->rec.seq, c->rec.perm, (int)n, 0,
+                                                            kCohKeyBits, c->stream);
+            if (e != cudaSuccess) return e;
+            PacketRecords rl = r;
+            rl.key = nullptr;
+            rl.order = c->rec.perm;
+            if (c->fp32) k_launch<float, false><<<lb, kThreads, 0, c->stream>>>(a, rl, ip0, n);
+            else k_launch<double, false><<<lb, kThreads, 0, c->stream>>>(a, rl, ip0, n);
+            WalkLaunch wl{n, ip0, acc, blocks, 0};
+            wl.coherent = true;
+            e = launch_walk_variant(c, a, r, wl);
+            if (e != cudaSuccess) return e;
+            continue;
+        }
         if (c->fp32) {
             if (amr) k_launch<float, true><<<lb, kThreads, 0, c->stream>>>(a, r, ip0, n);
             else k_launch<float, false><<<lb, kThreads, 0, c->stream>>>(a, r, ip0, n);
@@ -1381,7 +1657,7 @@ cudaError_t launch_transport(mochii_ctx* c) {
             if (e != cudaSuccess) return e;
             rw.perm = c->rec.perm;
         }
-        const cudaError_t e = launch_walk_variant(c, a, rw, WalkLaunch{n, ip0, acc, blocks, 0});
+        const cudaError_t e = launch_walk_variant(c, a, rw, WalkLaunch{n, ip0, acc, blocks, 0, false});
         if (e != cudaSuccess) return e;
     }
     return cudaGetLastError();
@@ -1397,7 +1673,7 @@ cudaError_t launch_transport_diffuse(mochii_ctx* c, double total, long long nd) 
         const long long n = nd - ip0 < r.cap ? nd - ip0 : r.cap;
         cudaError_t e = launch_diffuse_chunk(c, total, ip0, n);
         if (e != cudaSuccess) return e;
-        e = launch_walk_variant(c, a, r, WalkLaunch{n, ip0, 1, blocks, 1});
+        e = launch_walk_variant(c, a, r, WalkLaunch{n, ip0, 1, blocks, 1, false});
         if (e != cudaSuccess) return e;
     }
     return cudaGetLastError();

@@ -154,10 +154,11 @@ def test_moment_tallies_match_exact_tallies():
         assert ok, (i, worst)
 
 
-@pytest.mark.parametrize("tally", ["exact", "moments"])
-def test_fp32_metal_pass_within_tolerance(orc, tally):
+@pytest.mark.parametrize("tally,order", [("exact", "launch"), ("moments", "launch"), ("exact", "coherent"),
+                                         ("moments", "coherent")])
+def test_fp32_metal_pass_within_tolerance(orc, tally, order):
     n = 16
-    nl = metal_nl(n=n, precision="fp32", tally=tally)
+    nl = metal_nl(n=n, precision="fp32", tally=tally).replace("/\n", f" par%packet_order = '{order}'\n/\n")
     L = parse_namelist(nl).xmax
     neb, sim = pair(orc, nl, partial_state(n, L))
     st = neb.ionizing_field_and_rates()

@@ -108,10 +108,12 @@ def partially_ionised_state(n, L):
     return {"x_HI": xHI}
 
 
-@pytest.mark.parametrize("order", ["launch", "direction"])
+@pytest.mark.parametrize("order", ["launch", "direction", "coherent"])
 def test_fp64_pass_matches_oracle(orc, order):
-    """Also with the walk in (source, direction) order: the same packets,
-    visited in another order, score the same tallies."""
+    """Also with the walk in (source, direction) order, and in the coherent
+    order (launched sorted by source, direction cell and energy quantile,
+    tallies summed over each warp's lanes before the atomic): the same
+    packets, visited in another order, score the same tallies."""
     n = 32
     nl = small_nl(n=n, nphot=20000).replace("/\n", f" par%packet_order = '{order}'\n/\n")
     L = parse_namelist(nl).xmax
@@ -133,9 +135,10 @@ def test_fp64_pass_matches_oracle(orc, order):
     neb.close()
 
 
-def test_fp64_pass_with_helium_matches_oracle(orc):
+@pytest.mark.parametrize("order", ["launch", "coherent"])
+def test_fp64_pass_with_helium_matches_oracle(orc, order):
     n = 24
-    nl = small_nl(n=n, nphot=20000, he=0.1)
+    nl = small_nl(n=n, nphot=20000, he=0.1).replace("/\n", f" par%packet_order = '{order}'\n/\n")
     L = parse_namelist(nl).xmax
     state = partially_ionised_state(n, L)
     state["x_HeI"] = np.clip(state["x_HI"] * 1.5, 0, 1)
@@ -147,12 +150,15 @@ def test_fp64_pass_with_helium_matches_oracle(orc):
     neb.close()
 
 
-@pytest.mark.parametrize("tally", ["compensated", "fp64"])
-def test_fp32_compensated_tallies_within_tolerance(orc, tally):
+@pytest.mark.parametrize("tally,order", [("compensated", "launch"), ("fp64", "launch"), ("compensated", "coherent"),
+                                         ("fp64", "coherent")])
+def test_fp32_compensated_tallies_within_tolerance(orc, tally, order):
     """FP32 segments with compensated FP32 tally pairs or FP64 atomic
-    tallies: the FP32 opacity and attenuation error only."""
+    tallies: the FP32 opacity and attenuation error only (in the coherent
+    order also the FP32 warp sums of up to 32 path luminosities)."""
     n = 32
-    nl = small_nl(n=n, nphot=20000, precision="fp32").replace("/\n", f" par%tally_precision = '{tally}'\n/\n")
+    nl = small_nl(n=n, nphot=20000, precision="fp32").replace(
+        "/\n", f" par%tally_precision = '{tally}'\n par%packet_order = '{order}'\n/\n")
     L = parse_namelist(nl).xmax
     neb, sim, st = pass_pair(orc, nl, partially_ionised_state(n, L))
     for f in ("gamma_HI", "heat_HI"):
@@ -320,3 +326,35 @@ def test_pass_with_diffuse_matches_oracle(orc):
         assert np.median(np.abs(g[big] / o[big] - 1)) < 1e-9
         assert abs(g.sum() / o.sum() - 1) < 2e-3, f
     neb.close()
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_coherent_order_scores_what_launch_order_scores(precision):
+    """The coherent walk (sorted launch, warp-aggregated tallies) against the
+    launch-order walk on one nebula, chunked so that several sorted chunks
+    accumulate: the same scored segments and energy ledger, rates equal to
+    FP64 reassociation (FP64) or to the FP32 warp sums (FP32)."""
+    n = 40
+    nl = small_nl(n=n, nphot=60000, he=0.1, precision=precision).replace("/\n", " par%packet_chunk = 16384\n/\n")
+    L = parse_namelist(nl).xmax
+    state = partially_ionised_state(n, L)
+    state["x_HeI"] = np.clip(state["x_HI"] * 1.5, 0, 1)
+    state["x_HeII"] = 1.0 - state["x_HeI"]
+    out = {}
+    for order in ("launch", "coherent"):
+        neb = Nebula(parse_namelist(nl.replace("/\n", f" par%packet_order = '{order}'\n/\n")))
+        for k, v in state.items():
+            neb.set(k, v)
+        neb.gas_opacity_fill()
+        st = neb.ionizing_field_and_rates()
+        out[order] = (st, {f: neb.get(f) for f in ("gamma_HI", "gamma_HeI", "heat_HeII", "jt_ion")})
+        neb.close()
+    a, b = out["launch"], out["coherent"]
+    assert a[0].direct_segments == b[0].direct_segments
+    assert abs(a[0].energy_absorbed / b[0].energy_absorbed - 1) < 1e-12
+    assert b[0].closure <= 5e-13
+    tol = 1e-12 if precision == "fp64" else 2e-6
+    for f in a[1]:
+        x, y = a[1][f], b[1][f]
+        big = x > 1e-9 * x.max()
+        assert np.max(np.abs(y[big] / x[big] - 1)) < tol, (f, np.max(np.abs(y[big] / x[big] - 1)))
