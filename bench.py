@@ -124,6 +124,32 @@ class Workload:
     def balance(self, neb):
         return neb.gas_thermal_update() if self.thermal else neb.gas_equilibrium_update()
 
+    def state(self):
+        """The analytic developed state every step starts from (Cartesian
+        workloads; configs.prepared_state), or None: the octree and batch
+        workloads run from their configured start after preparation
+        iterations."""
+        from mochii_b200 import configs
+        if self.name == "hii_metals128":
+            return configs.prepared_state(self.grid, front=0.7, he=True)
+        if self.name == "stromgren64":
+            return configs.prepared_state(self.grid, front=1.0, he=False, T_in=1.0e4, T_out=1.0e4)
+        return None
+
+    def cpu_fraction(self):
+        """The CPU reference times 1/f of a step: 1/f of the stellar packets
+        (and so of the diffuse ones) and the balance of every f-th leaf."""
+        return 100 if self.thermal else 1
+
+
+def set_state(target, state):
+    """Upload a state dict (x_HI, x_HeI, x_HeII, n_e, T_e) to a Nebula or an
+    oracle Sim and refresh the opacities it implies."""
+    for k, v in state.items():
+        target.set(k, v)
+    if hasattr(target, "gas_opacity_fill"):
+        target.gas_opacity_fill()
+
 
 def bytes_per_segment(wl, precision, tally="fp64"):
     """B_seg = 4 F_state + 16 F_tally without the per-segment metal words
@@ -233,56 +259,51 @@ def cpu_threads(wl):
     return max(1, min(n, int(0.5 * mem // max(per, 1))))
 
 
-def cpu_reference(wl, state, nthreads, budget_s=20.0):
-    """The oracle port (FP64 CPU restatement, OpenMP) on a bounded sample of
-    one step: transport passes of `sample` packets on the given state and the
-    thermal (or ionisation) solve on every stride-th leaf, each scaled to the
-    step's packet / leaf count.  Returns (packets/s, description)."""
+def cpu_reference(wl, nthreads, steps=1, warmup=1, state=None):
+    """The reference's algorithm (the oracle port: FP64, OpenMP over packets
+    and leaves, the reference's damped n_e fixed point and bisection on T_e)
+    on 1/f of the workload's step, measured: a transport pass of nphot/f
+    stellar packets (and the diffuse packets their luminosity implies) and
+    the thermal bisection of every f-th leaf (f = wl.cpu_fraction(); the
+    ionisation-only workload runs whole steps).  Every step starts from the
+    workload's analytic state (or `state`), as the device steps do; warm-up
+    steps first give the metal stage fractions the rates of a pass on that
+    state.  Returns (packets/s, description, seconds per sample step, packets
+    per sample step)."""
     from oracle import pyorc
-    sample = int(os.environ.get("MOCHII_CPU_SAMPLE", "200000" if (wl.grid or 1024) <= 64 else "100000"))
-    sim = pyorc.Sim(wl.make(sample, "fp64", 12345), nthreads=nthreads)
-    for k, v in state.items():
-        sim.set(k, v)
-    # per-packet cost from passes of sample and 2 x sample packets (the
-    # per-pass tally reset and reduction is a fixed cost of a pass)
-    t_of = {}
-    for n in (sample, 2 * sample):
-        sim.set_nphotons(n)
+    f = wl.cpu_fraction()
+    nph = max(wl.nphot // f, 1)
+    sim = pyorc.Sim(wl.make(nph, "fp64", 12345), nthreads=nthreads)
+    st0 = state if state is not None else wl.state()
+    idx = np.arange(0, sim.nleaf, f, dtype=np.int64)
+    times, pk = [], []
+    for k in range(warmup + steps):
+        if st0 is not None:
+            for name, v in st0.items():
+                sim.set(name, v)
         t0 = time.perf_counter()
-        reps = 0
-        while True:
-            sim.transport_pass()
-            reps += 1
-            if time.perf_counter() - t0 > 0.25 * budget_s or reps >= 5:
-                break
-        t_of[n] = (time.perf_counter() - t0) / reps
-    t_pp = max(t_of[2 * sample] - t_of[sample], 1e-3 * t_of[sample]) / sample
-    t_fixed = max(t_of[sample] - sample * t_pp, 0.0)
-    t_pass = t_fixed + t_pp * wl.nphot
-    nleaf = sim.nleaf
-    if wl.thermal:
-        stride = int(os.environ.get("MOCHII_CPU_CELL_STRIDE", "256"))
-        t1 = time.perf_counter()
-        solved = sim.thermal_sample(stride)
-        t_cells = time.perf_counter() - t1
-        ngas = int(np.count_nonzero(state.get("nH", np.ones(nleaf)) > 0)) if "nH" in state else nleaf
-        t_bal = t_cells / max(solved, 1) * ngas
-        what = f"thermal solve of {solved} leaves (every {stride}th)"
-    else:
-        t1 = time.perf_counter()
-        sim.equilibrium_update()
-        t_bal = time.perf_counter() - t1
-        what = "ionisation solve of every leaf"
-    t_step = t_pass + t_bal
-    value = wl.nphot / t_step
-    desc = (f"transport passes of {sample} and {2 * sample} stellar packets (per-packet time scaled to "
-            f"{wl.nphot}, plus the per-pass fixed cost) + {what}, scaled to all leaves; stellar packets "
-            f"only; {nthreads} threads")
-    return value, desc, t_step, {"t_pp": t_pp, "t_fixed": t_fixed, "t_bal": t_bal, "nleaf": nleaf}
+        sim.transport_pass()
+        if wl.thermal:
+            sim.thermal_cells(idx)
+        else:
+            sim.equilibrium_update()
+        dt = time.perf_counter() - t0
+        if k >= warmup:
+            times.append(dt)
+            pk.append(nph + sim.diffuse_count)
+    t_step = float(np.mean(times))
+    value = float(np.sum(pk)) / float(np.sum(times))
+    what = (f"the thermal bisection of every {f}th leaf ({idx.size} leaves)" if wl.thermal
+            else "the ionisation solve of every leaf")
+    desc = (f"{'1/' + str(f) + ' of ' if f > 1 else ''}a step, measured: {nph} stellar packets plus their "
+            f"{int(np.mean(pk)) - nph} diffuse packets, then {what}, from the workload's analytic state; "
+            f"{steps} timed step(s) after {warmup} warm-up; {nthreads} threads")
+    return value, desc, t_step, float(np.mean(pk))
 
 
 class InstanceWorkload:
-    """One batch64 instance as a single-nebula workload (for the CPU port)."""
+    """One batch64 instance as a single-nebula workload (for the CPU port),
+    from its configured ionized start."""
 
     def __init__(self, p, nphot):
         from mochii_b200 import configs
@@ -290,69 +311,69 @@ class InstanceWorkload:
         self.make = lambda nphot_, prec, seed: configs.hii_instance(p["n"], p["nH"], p["tstar"], p["Q"],
                                                                      nphotons=nphot_, precision=prec, seed=seed)
 
+    def state(self):
+        return None
 
-def cpu_reference_batch(wl, states, nthreads, budget_s=24.0):
-    """The oracle port on the batch64 workload: three instances (the
-    smallest, the median and the largest grid) each timed as a single
-    nebula (cpu_reference: packet-sample passes and a leaf sample of the
-    thermal solve); the per-packet time taken as linear in the grid side
-    (the walk crosses O(n) leaves) and the per-leaf solve time averaged,
-    then summed over all instances.  states: per-instance state dicts for
-    the three sampled instances (or {}).  Returns (packets/s, description,
-    step seconds)."""
+    def cpu_fraction(self):
+        return 100
+
+
+def cpu_reference_batch(wl, nthreads, steps=1):
+    """The oracle port on three batch64 instances (the smallest, the median
+    and the largest grid), each measured on 1/100 of its step from its
+    configured start: packets over time summed over the three."""
     _, par = wl.instances("fp64")
     order = sorted(range(len(par)), key=lambda k: par[k]["n"])
     pick = [order[0], order[len(order) // 2], order[-1]]
-    ns, tpp, tfix, tcell = [], [], [], []
+    pk, tt, ns = 0.0, 0.0, []
     for k in pick:
         iw = InstanceWorkload(par[k], wl.nphot)
-        _, _, _, comp = cpu_reference(iw, states.get(k, {}), nthreads, budget_s=budget_s / 3)
+        _, _, t_step, p_step = cpu_reference(iw, nthreads, steps=steps, warmup=1)
+        pk += p_step
+        tt += t_step
         ns.append(par[k]["n"])
-        tpp.append(comp["t_pp"])
-        tfix.append(comp["t_fixed"])
-        tcell.append(comp["t_bal"] / comp["nleaf"])
-    slope, icpt = np.polyfit(np.array(ns, float), np.array(tpp), 1)
-    t_cell = float(np.mean(tcell))
-    t_step = sum(max(icpt + slope * p["n"], min(tpp)) * wl.nphot + float(np.mean(tfix)) + t_cell * p["n"] ** 3
-                 for p in par)
-    value = wl.nphot * len(par) / t_step
-    desc = (f"instances of {ns[0]}^3, {ns[1]}^3, {ns[2]}^3 each timed as one nebula (transport passes of packet "
-            f"samples, the thermal solve on every 256th leaf); per-packet time fitted linear in the grid side, "
-            f"per-leaf solve time averaged, summed over the {len(par)} instances at {wl.nphot} packets each; "
-            f"{nthreads} threads")
-    return value, desc, t_step
+    desc = (f"instances of {ns[0]}^3, {ns[1]}^3, {ns[2]}^3 from their configured start, each on 1/100 of a step "
+            f"(stellar packets and every 100th leaf's thermal bisection), measured; {nthreads} threads")
+    return pk / tt, desc, tt
 
 
 def run_reference(args, wl):
+    """--impl reference: the reference's algorithm (the oracle port) on the
+    host cores, every step 1/f of the workload's step from the same analytic
+    state the device steps start from, each step measured."""
     rank, world, _ = dist_env()
     if rank != 0:
         return 0
     nthreads = cpu_threads(wl)
-    # the workload's initial state (the GPU arm's preparation iterations would
-    # take the CPU port hours at this grid size)
-    state = {}
-    times = []
-    for k in range(args.warmup + args.steps):
-        if wl.name == "batch64":
-            _, desc, t_step = cpu_reference_batch(wl, {}, nthreads, budget_s=12.0)
-        else:
-            _, desc, t_step, _ = cpu_reference(wl, state, nthreads, budget_s=10.0)
-        if k >= args.warmup:
-            times.append(t_step)
-    dt = sum(times)
-    value = wl.nphot * getattr(wl, "count", 1) * args.steps / dt
+    if wl.name == "batch64":
+        value, desc, t_step = cpu_reference_batch(wl, nthreads, steps=args.steps)
+        p_step = value * t_step
+    else:
+        value, desc, t_step, p_step = cpu_reference(wl, nthreads, steps=args.steps, warmup=args.warmup)
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt / args.steps * 1e3,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_step * 1e3,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic",
-            "config": {"workload": wl.name, "grid": grid_name(wl, None),
-                       "packets_per_step": wl.nphot * getattr(wl, "count", 1),
-                       "state": "the workload's initial state",
-                       "note": "each step a bounded sample of the workload's step, scaled"},
+            "data": "synthetic", "config": config_of(wl),
+            "sample": {"packets_per_step": p_step, "fraction_of_step": 1.0 / wl.cpu_fraction(),
+                       "note": "each timed step is the stated fraction of the workload's step, measured (not scaled)"},
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": nthreads, "kind": "port", "sample": desc},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
     return 0
+
+
+def config_of(wl, nleaf=None):
+    """The workload's identity, the same for the device arm and the
+    reference arm."""
+    cfg = {"workload": wl.name, "grid": grid_name(wl, nleaf), "stellar_packets_per_step": wl.nphot,
+           "balance": "thermal" if wl.thermal else "ionisation, fixed T_e"}
+    if wl.name == "batch64":
+        cfg.update({"instances": wl.count, "state": "each instance's configured ionized start"})
+    elif wl.state() is not None:
+        cfg["state"] = "every step from the analytic developed H II region of configs.prepared_state"
+    else:
+        cfg["state"] = f"{wl.prep} preparation iterations from the configured start"
+    return cfg
 
 
 def main():
@@ -407,10 +428,21 @@ def main():
         "/\n", f" par%thermal_solver = '{args.solver}'\n par%cell_layout = '{args.cell_layout}'\n"
               f" par%tally_precision = '{args.tally}'\n{order}/\n"))
     neb = Nebula(par)
-    prep_iters = prepare(neb, wl)
+    state0 = wl.state()
+    if state0 is not None:
+        set_state(neb, state0)
+    else:
+        prepare(neb, wl)
     tuning = neb.autotune(1 << 20)   # launch shape for this grid / precision / device
+
+    def start():
+        """Every step from the same analytic state (Cartesian workloads)."""
+        if state0 is not None:
+            set_state(neb, state0)
+
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
     for _ in range(args.warmup):
+        start()
         neb.ionizing_field_and_rates()
         wl.balance(neb)
         neb.gas_opacity_fill()
@@ -424,6 +456,7 @@ def main():
         t_wall = time.perf_counter()
         for k in range(args.steps):
             flush.zero_()
+            start()
             torch.cuda.synchronize()
             st = neb.ionizing_field_and_rates()
             wl.balance(neb)
@@ -456,8 +489,10 @@ def main():
 
     # ---- end-to-end through the C ABI with host buffers --------------------
     nleaf = neb.nleaf
-    x_host = torch.from_numpy(neb.get("x_HI")).pin_memory()
-    t_host = torch.from_numpy(neb.get("T_e")).pin_memory()
+    # each step's inputs: the start state (every field of it) from pinned host memory
+    src = state0 if state0 is not None else {f: neb.get(f) for f in ("x_HI", "T_e")}
+    host_in = {f.encode(): torch.from_numpy(np.ascontiguousarray(v, dtype=np.float64)).pin_memory()
+               for f, v in src.items()}
     x_out = torch.empty(nleaf, dtype=torch.float64).pin_memory()
     t_out = torch.empty(nleaf, dtype=torch.float64).pin_memory()
     g_out = torch.empty(nleaf, dtype=torch.float64).pin_memory()
@@ -468,8 +503,9 @@ def main():
     e_packets = 0
     e0 = time.perf_counter()
     for k in range(args.steps):
-        rc = lib.mochii_set_field(ctx, b"x_HI", x_host.data_ptr(), nleaf)
-        rc |= lib.mochii_set_field(ctx, b"T_e", t_host.data_ptr(), nleaf)
+        rc = 0
+        for f, hb in host_in.items():
+            rc |= lib.mochii_set_field(ctx, f, hb.data_ptr(), nleaf)
         rc |= lib.mochii_opacity_fill(ctx)
         st = neb.ionizing_field_and_rates()
         e_packets += st.packets
@@ -502,10 +538,10 @@ def main():
         traffic = DRAM_BYTES_PER_SEGMENT[wl.name] * mean_seg
 
     cpu = None
-    if rank == 0 and not args.no_cpu_baseline:
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
         nthreads = cpu_threads(wl)
-        state = {f: neb.get(f) for f in ("x_HI", "x_HeI", "x_HeII", "n_e", "T_e")}
-        v, desc, _, _ = cpu_reference(wl, state, nthreads)
+        # the same start state as the device steps (octree: the configured start)
+        v, desc, _, _ = cpu_reference(wl, nthreads, steps=2, warmup=1)
         cpu = {"value": v, "unit": UNIT, "cores": nthreads, "kind": "port", "sample": desc}
 
     conv = None
@@ -518,14 +554,12 @@ def main():
             "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64" if prec == "fp64" else "f32+f64",
             "data": "synthetic",
-            "config": {"workload": wl.name, "grid": grid_name(wl, nleaf), "stellar_packets_per_step": wl.nphot,
-                       "packets_per_step": packets / args.steps / world,
-                       "precision": prec, "balance": "thermal" if wl.thermal else "ionisation, fixed T_e",
-                       "solver": args.solver, "cell_layout": args.cell_layout, "tallies": args.tally,
-                       "state": f"{prep_iters} untimed preparation iterations from the configured start",
-                       "l2": "flushed between steps (256 MiB write)", "tuning": tuning,
-                       "parallelism": "replicas" if world > 1 else "single"},
-            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 16 * nleaf,
+            "config": config_of(wl, nleaf),
+            "implementation": {"packets_per_step": packets / args.steps / world, "precision": prec,
+                               "solver": args.solver, "cell_layout": args.cell_layout, "tallies": args.tally,
+                               "packet_order": neb_order(neb), "l2": "flushed between steps (256 MiB write)",
+                               "tuning": tuning, "parallelism": "replicas" if world > 1 else "single"},
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 8 * len(host_in) * nleaf,
                     "d2h_bytes_per_step": 24 * nleaf},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "peak_kind": peak_kind,
@@ -783,6 +817,10 @@ def time_to_converged(n=64, nphot=1_000_000, iters=20, train_iters=10, seed_trai
                     "iteration then carries Monte Carlo differences at the ionization front",
             "training": {"pairs": int(len(X)), "data_s": t_data, "train_s": t_train, "epochs": 20,
                          "loss_first": float(losses[0]), "loss_last": float(losses[-1])}}
+
+
+def neb_order(neb):
+    return {0: "launch", 1: "direction", 2: "coherent"}.get(int(neb.par.packet_order), "?")
 
 
 def grid_name(wl, nleaf):

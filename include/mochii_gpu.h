@@ -188,6 +188,8 @@ typedef struct mochii_metrics {
     int64_t fixed_point_passes;      /* n_e fixed-point passes over all cells and trial T */
     int64_t metal_sum_calls;         /* metal cascade sums (species_metal_sums) evaluated */
     int64_t rate_evaluations;        /* net_rate evaluations (thermal) or cell solves      */
+    int64_t warm_accepted;           /* leaves whose learned warm start passed the residual
+                                        gate at its one evaluation (mochii_mlp_warm_start)  */
 } mochii_metrics;
 
 /* Launch shapes of the transport walk (the autotuner's choice). */

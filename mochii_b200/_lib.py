@@ -70,7 +70,8 @@ class PassStats(C.Structure):
 class Metrics(C.Structure):
     _fields_ = [("max_dx", C.c_double), ("max_dte", C.c_double), ("dx_vol", C.c_double), ("dte_vol", C.c_double),
                 ("cells_solved", C.c_int64), ("fixed_point_cap_hits", C.c_int64), ("kernel_ms", C.c_double),
-                ("fixed_point_passes", C.c_int64), ("metal_sum_calls", C.c_int64), ("rate_evaluations", C.c_int64)]
+                ("fixed_point_passes", C.c_int64), ("metal_sum_calls", C.c_int64), ("rate_evaluations", C.c_int64),
+                ("warm_accepted", C.c_int64)]
 
 
 class Tuning(C.Structure):

@@ -369,3 +369,28 @@ def batch_instances(count=64, seed=5, nmin=32, nmax=128, nphotons=2_000_000, pre
                                 metal_tally=metal_tally))
         par.append(dict(n=n, nH=nH, tstar=tstar, Q=Q))
     return out, par
+
+
+def prepared_state(n, front=0.7, width=1.0, he=True, T_in=8.0e3, T_out=3.0e3, nH=100.0, yHe=0.1):
+    """A deterministic developed-H II-region state on an n^3 Cartesian grid
+    (raster leaf order, il = ix + n (iy + n iz)): an ionized sphere of radius
+    front x the box half-width around the centre, x_HI = 1e-3 inside rising
+    to 1 over a logistic edge `width` cells wide; with He, He singly ionized
+    where H is (x_HeI = x_HI, x_HeII = 1 - x_HI, no He III); T_e = T_in inside
+    and T_out outside, blended by the same edge; n_e from charge balance.
+    The benchmark's device steps and its CPU reference steps both start from
+    this state, so both measure the same iteration."""
+    import numpy as np
+    c = (np.arange(n) + 0.5) - 0.5 * n
+    z, y, x = np.meshgrid(c, c, c, indexing="ij")
+    r = np.sqrt(x * x + y * y + z * z).ravel()
+    s = 1.0 / (1.0 + np.exp(-(r - front * 0.5 * n) / width))   # 0 inside, 1 outside
+    xHI = 1.0e-3 + (1.0 - 1.0e-3) * s
+    out = {"x_HI": xHI, "T_e": T_in + (T_out - T_in) * s}
+    ne = nH * (1.0 - xHI)
+    if he:
+        out["x_HeI"] = xHI.copy()
+        out["x_HeII"] = 1.0 - xHI
+        ne = ne + nH * yHe * out["x_HeII"]
+    out["n_e"] = ne
+    return out

@@ -763,6 +763,7 @@ extern "C" int mochii_batch_iterate(mochii_batch* b, int solve_te, mochii_pass_s
         r.fixed_point_passes = (int64_t)cnt[2];
         r.metal_sum_calls = (int64_t)cnt[3];
         r.rate_evaluations = (int64_t)cnt[4];
+        r.warm_accepted = (int64_t)cnt[5];
         if (mm) mm[k] = r;
         if (!std::isfinite(s.energy_emitted) || !std::isfinite(s.energy_absorbed)) {
             status = fail(c, MOCHII_ERR_NONFINITE, "non-finite energy ledger");
@@ -919,6 +920,7 @@ extern "C" int mochii_balance_update(mochii_ctx* c, int solve_te, mochii_metrics
     r.fixed_point_passes = (int64_t)cnt[2];
     r.metal_sum_calls = (int64_t)cnt[3];
     r.rate_evaluations = (int64_t)cnt[4];
+    r.warm_accepted = (int64_t)cnt[5];
     r.kernel_ms = ms;
     if (m) *m = r;
     if (!std::isfinite(r.max_dx) || !std::isfinite(r.dx_vol) || !std::isfinite(r.max_dte))
@@ -1098,6 +1100,8 @@ extern "C" int mochii_set_field(mochii_ctx* c, const char* name, const double* i
             CK(c, dalloc(&c->twarm, (size_t)n));
         }
         CK(c, cudaMemcpyAsync(c->twarm, in, n * 8, cudaMemcpyHostToDevice, c->stream));
+        c->twarm_fac = 1.05;   // a caller's warm start: the default first step, no gate
+        c->twarm_gate = 0.0;
         CK(c, cudaStreamSynchronize(c->stream));
         c->twarm_set = true;
         return MOCHII_OK;

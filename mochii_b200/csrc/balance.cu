@@ -423,6 +423,8 @@ struct ThArgs {
     ThermalDev td;
     double te_min, te_max;
     const double* Twarm;   // bracketed solve: warm-start T_e per leaf (nullptr: the current T_e)
+    double tfac0;          // bracketed solve: the first bracketing step in T (1.05; smaller after a learned warm start)
+    double gate;           // bracketed solve: residual gate of a learned warm start (0: none), lane layout
     const int* order;      // lockstep solve: the order to visit leaves in (nullptr: leaf order)
     unsigned* work;        // lockstep solve: cascade sums per leaf, written for the next update's order
     unsigned long long* next;   // lockstep solve: the chunk counter (warps claim 32 leaves at a time)
@@ -867,59 +869,144 @@ __device__ double net_rate(const ThArgs& a, long long il, double T, double nH, d
     return net;
 }
 
+// The temperature search of the bracketed thermal solve, one leaf, driven
+// by its caller one evaluation at a time: begin() at the warm start, then
+// feed() the net heating at each requested temperature t until ph == 9; tr
+// is the solved T_e, always the last temperature evaluated (so the cell
+// state the caller holds is the one solved at it).
+//
+// net(T) is bracketed from the warm start by geometric steps in ln T (the
+// first by fac0, each later one squaring the factor), stopping at te_min
+// with net <= 0 (cooling wins) or at te_max with net >= 0 (heating wins) as
+// the reference's bisection pins those leaves.  The sign change is then
+// closed by Anderson-Bjorck false position in ln T: the new point replaces
+// the newest end; when it keeps that end's sign the far end is retained and
+// its value scaled by 1 - f_new / f_newest (by 1/2 when that is not
+// positive), which moves the next point past the root.  A secant point
+// within half the tolerance of the newest end is moved half the tolerance
+// past the root estimate towards the far end, so one more sign change closes
+// the bracket; a bracket that has not halved in three points is bisected.
+// Done when the bracket is below 1e-5 in ln T (the reference's bisection
+// stops at thi/tlo - 1 < 1e-5), at most 80 points.
+//
+// gate > 0 (the learned warm start): the warm start is accepted as the root
+// after its one evaluation when |net| <= gate x (heating + cooling) there.
+struct TRoot {
+    int ph, s, it, stall;   // ph: 0 warm start, 1 bracketing, 2 false position, 9 done
+    double ta, fa, tb, fb, fac, x1, f1, x2, f2, wref, t, tr, gate;
+    bool accepted;
+    __device__ __forceinline__ void begin(double Tw, double lo, double hi, double fac0 = 1.05, double g = 0.0) {
+        ph = 0; s = 0; it = 0; stall = 0;
+        ta = fmin(fmax(Tw, lo), hi);
+        fa = 0.0; tb = ta; fb = 0.0; fac = fac0;
+        x1 = x2 = f1 = f2 = wref = 0.0;
+        t = ta; tr = ta;
+        gate = g;
+        accepted = false;
+    }
+    __device__ __forceinline__ void feed(double f, double lo_lim, double hi_lim, double scale = 0.0) {
+        constexpr double kTol = 1.0e-5;
+        bool to_fp = false;
+        if (ph == 0) {
+            fa = f;
+            if (fa == 0.0 || (ta <= lo_lim && fa < 0.0) || (ta >= hi_lim && fa > 0.0)) {
+                tr = ta;
+                ph = 9;
+            } else if (gate > 0.0 && fabs(fa) <= gate * scale) {
+                tr = ta;
+                ph = 9;
+                accepted = true;
+            } else {
+                ph = 1;
+                s = 0;
+            }
+        } else if (ph == 1) {
+            fb = f;
+            ++s;
+            if (fb == 0.0) {
+                tr = tb;
+                ph = 9;
+            } else if ((fb > 0.0) != (fa > 0.0)) {
+                to_fp = true;
+            } else if (tb >= hi_lim || tb <= lo_lim) {
+                tr = tb;
+                ph = 9;
+            } else {
+                ta = tb;
+                fa = fb;
+                fac = fac * fac;
+                if (s >= 40) to_fp = true;
+            }
+        } else {   // ph == 2: f at t
+            ++it;
+            tr = t;
+            if (f == 0.0) {
+                ph = 9;
+            } else {
+                if ((f > 0.0) != (f2 > 0.0)) {
+                    x1 = x2;
+                    f1 = f2;
+                } else {
+                    const double m = 1.0 - f / f2;
+                    f1 = f1 * (m > 0.0 ? m : 0.5);
+                }
+                x2 = log(t);
+                f2 = f;
+            }
+        }
+        if (to_fp) {
+            x1 = log(ta);
+            f1 = fa;
+            x2 = log(tb);
+            f2 = fb;
+            wref = fabs(x2 - x1);
+            tr = tb;
+            it = 0;
+            stall = 0;
+            ph = 2;
+        }
+        if (ph == 1) {
+            tb = fa > 0.0 ? fmin(ta * fac, hi_lim) : fmax(ta / fac, lo_lim);
+            t = tb;
+        } else if (ph == 2) {
+            const double w = fabs(x2 - x1);
+            if (w < kTol || it >= 80) {
+                ph = 9;
+            } else {
+                if (w <= 0.5 * wref) {
+                    wref = w;
+                    stall = 0;
+                } else {
+                    ++stall;
+                }
+                double x3 = (x1 * f2 - x2 * f1) / (f2 - f1);
+                if (fabs(x3 - x2) < 0.5 * kTol) x3 = x3 + copysign(0.5 * kTol, x1 - x2);
+                if (stall >= 3 || !(x3 > fmin(x1, x2) && x3 < fmax(x1, x2))) {
+                    x3 = 0.5 * (x1 + x2);
+                    stall = 0;
+                    wref = 0.5 * w;
+                }
+                t = exp(x3);
+            }
+        }
+    }
+};
+
 // The bracketed T_e solve (solver_bracketed): the root of net(T) that the
-// reference's bisection on [te_min, te_max] converges to, found from a warm
-// start T_w.  net(T_w) gives the direction; geometric steps in ln T (x1.05,
-// squared each step) bracket the sign change, or reach te_min with net <= 0
-// (the reference's "cooling wins at te_min") or te_max with net >= 0; then
-// safeguarded false position in ln T until the bracket is below 1e-5 in ln T
-// (the reference's bisection stops at thi/tlo - 1 < 1e-5).  The cell state
-// left behind is the one solved at the returned T_e.
+// reference's bisection on [te_min, te_max] converges to (thermal_mod.f90:
+// 159-180), found from a warm start T_w by the search of TRoot.  The cell
+// state left behind is the one solved at the returned T_e.
 template <class Cas>
 __device__ double thermal_bracketed(const ThArgs& a, long long il, double nH, double& xHI, double& xHeI, double& xHeII,
                                     double& ne, int* passes, Cas& mc, int* nsum, int* nev, double Tw) {
-    const double lo_lim = a.te_min, hi_lim = a.te_max;
-    double ta = fmin(fmax(Tw, lo_lim), hi_lim);
-    double fa = net_rate(a, il, ta, nH, xHI, xHeI, xHeII, ne, passes, mc, nsum);
-    ++*nev;
-    if (fa == 0.0) return ta;
-    if ((ta <= lo_lim && fa < 0.0) || (ta >= hi_lim && fa > 0.0)) return ta;   // pinned at a limit
-    double tb = ta, fb = fa, fac = 1.05;
-    for (int s = 0; s < 40; ++s) {
-        tb = fa > 0.0 ? fmin(ta * fac, hi_lim) : fmax(ta / fac, lo_lim);
-        fb = net_rate(a, il, tb, nH, xHI, xHeI, xHeII, ne, passes, mc, nsum);
+    TRoot r;
+    r.begin(Tw, a.te_min, a.te_max, a.tfac0);
+    while (r.ph != 9) {
+        const double f = net_rate(a, il, r.t, nH, xHI, xHeI, xHeII, ne, passes, mc, nsum);
         ++*nev;
-        if (fb == 0.0) return tb;
-        if ((fb > 0.0) != (fa > 0.0)) break;
-        if (tb >= hi_lim || tb <= lo_lim) return tb;   // heating wins at te_max / cooling at te_min
-        ta = tb;
-        fa = fb;
-        fac = fac * fac;
+        r.feed(f, a.te_min, a.te_max);
     }
-    // safeguarded false position: net(T) spans many decades across the
-    // bracket, so a point within 5% of an end, or a bracket that did not
-    // halve, is replaced by the midpoint
-    double la = log(ta), lb = log(tb), t = tb;
-    bool bisect = false;
-    for (int it = 0; it < 80; ++it) {
-        const double width = fabs(lb - la);
-        if (width < 1.0e-5) break;
-        double lc = (la * fb - lb * fa) / (fb - fa);
-        if (bisect || !(fabs(lc - la) > 0.05 * width && fabs(lc - lb) > 0.05 * width)) lc = 0.5 * (la + lb);
-        t = exp(lc);
-        const double fc = net_rate(a, il, t, nH, xHI, xHeI, xHeII, ne, passes, mc, nsum);
-        ++*nev;
-        if (fc == 0.0) break;
-        if ((fc > 0.0) == (fa > 0.0)) {
-            la = lc;
-            fa = fc;
-        } else {
-            lb = lc;
-            fb = fc;
-        }
-        bisect = fabs(lb - la) > 0.5 * width;
-    }
-    return t;
+    return r.tr;
 }
 
 // ---- the bracketed solves in warp lockstep -----------------------------------
@@ -1158,84 +1245,17 @@ __device__ __noinline__ double net_rate_ls(const ThArgs& a, long long il, bool a
 __device__ __noinline__ double thermal_ls(const ThArgs& a, long long il, bool act, double nH, double& xHI,
                                           double& xHeI, double& xHeII, double& ne, int* passes, SerialCascade& mc,
                                           int* nsum, int* nev, double Tw) {
-    const double lo_lim = a.te_min, hi_lim = a.te_max;
-    // ph: 0 warm start, 1 bracketing, 2 false position, 9 done
-    int ph = act ? 0 : 9, s = 0, it = 0;
-    double ta = fmin(fmax(Tw, lo_lim), hi_lim), fa = 0.0, tb = ta, fb = 0.0, fac = 1.05, la = 0.0, lb = 0.0;
-    double t = ta, tr = ta;
-    bool bisect = false;
-    while (__any_sync(kFull, ph != 9)) {
-        const bool ev = ph != 9;
-        const double f = net_rate_ls(a, il, ev, t, nH, xHI, xHeI, xHeII, ne, passes, mc, nsum);
+    TRoot r;
+    r.begin(Tw, a.te_min, a.te_max, a.tfac0);
+    if (!act) r.ph = 9;
+    while (__any_sync(kFull, r.ph != 9)) {
+        const bool ev = r.ph != 9;
+        const double f = net_rate_ls(a, il, ev, r.t, nH, xHI, xHeI, xHeII, ne, passes, mc, nsum);
         if (!ev) continue;
         ++*nev;
-        bool to_fp = false;
-        if (ph == 0) {
-            fa = f;
-            if (fa == 0.0 || (ta <= lo_lim && fa < 0.0) || (ta >= hi_lim && fa > 0.0)) {
-                tr = ta;
-                ph = 9;
-            } else {
-                ph = 1;
-                s = 0;
-            }
-        } else if (ph == 1) {
-            fb = f;
-            ++s;
-            if (fb == 0.0) {
-                tr = tb;
-                ph = 9;
-            } else if ((fb > 0.0) != (fa > 0.0)) {
-                to_fp = true;
-            } else if (tb >= hi_lim || tb <= lo_lim) {
-                tr = tb;
-                ph = 9;
-            } else {
-                ta = tb;
-                fa = fb;
-                fac = fac * fac;
-                if (s >= 40) to_fp = true;
-            }
-        } else {   // ph == 2
-            const double fc = f, lc = log(t), width = fabs(lb - la);
-            ++it;
-            tr = t;
-            if (fc == 0.0) {
-                ph = 9;
-            } else {
-                if ((fc > 0.0) == (fa > 0.0)) {
-                    la = lc;
-                    fa = fc;
-                } else {
-                    lb = lc;
-                    fb = fc;
-                }
-                bisect = fabs(lb - la) > 0.5 * width;
-            }
-        }
-        if (to_fp) {
-            la = log(ta);
-            lb = log(tb);
-            tr = tb;
-            bisect = false;
-            it = 0;
-            ph = 2;
-        }
-        if (ph == 1) {
-            tb = fa > 0.0 ? fmin(ta * fac, hi_lim) : fmax(ta / fac, lo_lim);
-            t = tb;
-        } else if (ph == 2) {
-            const double width = fabs(lb - la);
-            if (width < 1.0e-5 || it >= 80) {
-                ph = 9;
-            } else {
-                double lc = (la * fb - lb * fa) / (fb - fa);
-                if (bisect || !(fabs(lc - la) > 0.05 * width && fabs(lc - lb) > 0.05 * width)) lc = 0.5 * (la + lb);
-                t = exp(lc);
-            }
-        }
+        r.feed(f, a.te_min, a.te_max);
     }
-    return tr;
+    return r.tr;
 }
 
 // gas_thermal_update (thermal_mod.f90:124-249): bisection on log T in
@@ -1380,6 +1400,7 @@ __device__ __noinline__ double neutrality_ls(const SerialCascade& mc, bool act, 
 struct ThermalAcc {
     double mdx = 0.0, mdt = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0, s4 = 0.0;
     unsigned long long solved = 0, tpass = 0, tsums = 0, nevals = 0;
+    unsigned long long accepted = 0;   // learned warm starts accepted by the residual gate
 };
 
 // One warp's 32 leaves at positions base .. base+31 of a's order, in lockstep.
@@ -1486,12 +1507,12 @@ __global__ void __launch_bounds__(kBThreads) k_thermal_ls(const ThArgs a) {
 // values are non-negative, so their bit patterns order as the numbers).
 __device__ __forceinline__ void thermal_acc_flush(const BalArgs& b, ThermalAcc& acc) {
     double v[6] = {acc.mdx, acc.mdt, acc.s1, acc.s2, acc.s3, acc.s4};
-    unsigned long long c[4] = {acc.solved, acc.tpass, acc.tsums, acc.nevals};
+    unsigned long long c[5] = {acc.solved, acc.tpass, acc.tsums, acc.nevals, acc.accepted};
     for (int o = 16; o > 0; o >>= 1) {
         v[0] = fmax(v[0], __shfl_down_sync(kFull, v[0], o));
         v[1] = fmax(v[1], __shfl_down_sync(kFull, v[1], o));
         for (int k = 2; k < 6; ++k) v[k] += __shfl_down_sync(kFull, v[k], o);
-        for (int k = 0; k < 4; ++k) c[k] += __shfl_down_sync(kFull, c[k], o);
+        for (int k = 0; k < 5; ++k) c[k] += __shfl_down_sync(kFull, c[k], o);
     }
     if ((threadIdx.x & 31) == 0) {
         unsigned long long* pm = reinterpret_cast<unsigned long long*>(b.partial);
@@ -1502,6 +1523,7 @@ __device__ __forceinline__ void thermal_acc_flush(const BalArgs& b, ThermalAcc& 
         if (c[1]) atomicAdd(b.counters + 2, c[1]);
         if (c[2]) atomicAdd(b.counters + 3, c[2]);
         if (c[3]) atomicAdd(b.counters + 4, c[3]);
+        if (c[4]) atomicAdd(b.counters + 5, c[4]);
     }
     acc = ThermalAcc();
 }
@@ -1608,9 +1630,7 @@ struct LeafFlow {
     // request arguments
     double q_T = 0, q_ne = 0, q_x = 0;
     // T level (thermal_bracketed)
-    int tph = 0, ts = 0, tit = 0;
-    double ta = 0, tfa = 0, tb = 0, tfb = 0, tfac = 1.05, tla = 0, tlb = 0, t = 0, tr = 0;
-    bool bisect = false;
+    TRoot tsr;
     // net_rate level
     Coef k = {};
     double g0 = 0, g1 = 0, g2 = 0;
@@ -1640,12 +1660,8 @@ struct LeafFlow {
         in_neu = false;
         live = true;
         // thermal_bracketed: the warm start
-        const double Tw = A->Twarm ? A->Twarm[il] : T0;
-        ta = fmin(fmax(Tw, A->te_min), A->te_max);
-        tph = 0;
-        t = ta;
-        tr = ta;
-        start_net(t);
+        tsr.begin(A->Twarm ? A->Twarm[il] : T0, A->te_min, A->te_max, A->tfac0);
+        start_net(tsr.t);
     }
     __device__ void start_net(double T) {
         q_T = T;
@@ -1868,82 +1884,15 @@ struct LeafFlow {
     }
     // thermal_bracketed after net(t)
     __device__ void on_net(double f) {
-        const double lo_lim = A->te_min, hi_lim = A->te_max;
         ++nev;
-        bool to_fp = false;
-        if (tph == 0) {
-            tfa = f;
-            if (tfa == 0.0 || (ta <= lo_lim && tfa < 0.0) || (ta >= hi_lim && tfa > 0.0)) {
-                tr = ta;
-                tph = 9;
-            } else {
-                tph = 1;
-                ts = 0;
-                tfac = 1.05;
-            }
-        } else if (tph == 1) {
-            tfb = f;
-            ++ts;
-            if (tfb == 0.0) {
-                tr = tb;
-                tph = 9;
-            } else if ((tfb > 0.0) != (tfa > 0.0)) {
-                to_fp = true;
-            } else if (tb >= hi_lim || tb <= lo_lim) {
-                tr = tb;
-                tph = 9;
-            } else {
-                ta = tb;
-                tfa = tfb;
-                tfac = tfac * tfac;
-                if (ts >= 40) to_fp = true;
-            }
-        } else {   // tph == 2
-            const double lc = log(t), width = fabs(tlb - tla);
-            ++tit;
-            tr = t;
-            if (f == 0.0) {
-                tph = 9;
-            } else {
-                if ((f > 0.0) == (tfa > 0.0)) {
-                    tla = lc;
-                    tfa = f;
-                } else {
-                    tlb = lc;
-                    tfb = f;
-                }
-                bisect = fabs(tlb - tla) > 0.5 * width;
-            }
-        }
-        if (to_fp) {
-            tla = log(ta);
-            tlb = log(tb);
-            tr = tb;
-            bisect = false;
-            tit = 0;
-            tph = 2;
-        }
-        if (tph == 1) {
-            tb = tfa > 0.0 ? fmin(ta * tfac, hi_lim) : fmax(ta / tfac, lo_lim);
-            t = tb;
-        } else if (tph == 2) {
-            const double width = fabs(tlb - tla);
-            if (width < 1.0e-5 || tit >= 80) {
-                tph = 9;
-            } else {
-                double lc = (tla * tfb - tlb * tfa) / (tfb - tfa);
-                if (bisect || !(fabs(lc - tla) > 0.05 * width && fabs(lc - tlb) > 0.05 * width))
-                    lc = 0.5 * (tla + tlb);
-                t = exp(lc);
-            }
-        }
-        if (tph != 9) {
-            start_net(t);
+        tsr.feed(f, A->te_min, A->te_max);
+        if (tsr.ph != 9) {
+            start_net(tsr.t);
             return;
         }
         // the leaf's T_e; the written state (thermal_mod.f90:191-203)
         const BalArgs& b = A->b;
-        te = tr;
+        te = tsr.tr;
         const double w = b.relax;
         xn = (1.0 - w) * x0 + w * xHI;
         h1n = (1.0 - w) * h10 + w * xHeI;
@@ -2411,6 +2360,8 @@ void* thermal_batch_create(mochii_ctx* const* cs, int n, cudaError_t* err) {
         a.te_min = c->par.te_min;
         a.te_max = c->par.te_max;
         a.Twarm = nullptr;
+        a.tfac0 = 1.05;
+        a.gate = 0.0;
         a.order = c->bw.order;
         a.work = c->bw.work;
         a.next = nullptr;
@@ -2496,6 +2447,8 @@ cudaError_t launch_thermal(mochii_ctx* c) {
     a.te_min = c->par.te_min;
     a.te_max = c->par.te_max;
     a.Twarm = c->twarm_set ? c->twarm : nullptr;
+    a.tfac0 = c->twarm_set ? c->twarm_fac : 1.05;
+    a.gate = c->twarm_set ? c->twarm_gate : 0.0;
     a.order = nullptr;
     a.work = nullptr;
     a.next = nullptr;

@@ -138,6 +138,8 @@ struct mochii_ctx {
     std::vector<double> lhalf;      // octree: leaf half widths (host copy for leaf_half)
     double* twarm = nullptr;        // bracketed thermal solve: warm-start T_e per leaf ("T_warm")
     bool twarm_set = false;         // consumed by the next thermal update
+    double twarm_fac = 1.05;        // first bracketing step from the warm start (learned: narrower)
+    double twarm_gate = 0.0;        // residual gate of a learned warm start (0: none)
     mochii::SpeciesHost species;
     bool thermal_ready = false;
     mochii::BalanceWork bw;

@@ -148,6 +148,21 @@ __device__ __forceinline__ void head(const float* o, float* p, float* he) {
     p[3] = o[3];
 }
 
+// Sum over B rows of the squared error of the T_e output (4 (log10 T_e -
+// log10 T_e,prev)), for the calibration of the warm start's first step.
+__global__ void k_t_sqerr(int B, const float* __restrict__ out, const float* __restrict__ y, float* __restrict__ acc) {
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    float e2 = 0.0f;
+    if (b < B) {
+        float p[4], he0;
+        head(out + (long long)b * kOut, p, &he0);
+        const float e = p[3] - y[(long long)b * kOut + 3];
+        e2 = e * e;
+    }
+    for (int o = 16; o > 0; o >>= 1) e2 += __shfl_down_sync(0xffffffffu, e2, o);
+    if ((threadIdx.x & 31) == 0 && e2 != 0.0f) atomicAdd(acc, e2);
+}
+
 // Loss (mean over the batch of the mean squared error of p against y) and
 // its gradient with respect to the raw outputs, scaled by 1/B.
 __global__ void k_loss(int B, const float* __restrict__ out, const float* __restrict__ y, float* __restrict__ dout,
@@ -279,6 +294,10 @@ struct mochii_mlp {
     float *X = nullptr, *Y = nullptr;   // resident training set
     long long cap = 0, nset = 0, setcap = 0;
     long long step = 0;
+    // RMS error of the T_e prediction in ln T over the training set after
+    // the last mochii_mlp_train (0: not trained): sets the warm start's first
+    // bracketing step
+    double t_rms_ln = 0.0;
     std::string err;
 };
 
@@ -525,6 +544,25 @@ extern "C" int mochii_mlp_train(mochii_mlp* m, const float* X, const float* Y, i
         MK(cudaGetLastError());
         if (losses) losses[e] = nbatch ? lh / (float)(nbatch * batch) : 0.0f;
     }
+    // calibration: RMS error of the T_e output over (up to 2^20 rows of) the set
+    {
+        const int64_t ncal = std::min<int64_t>(n, (int64_t)batch * std::max<int64_t>(1, (1 << 20) / batch));
+        MK(cudaMemsetAsync(m->loss, 0, 4, m->stream));
+        int64_t done = 0;
+        for (int64_t b0 = 0; b0 < ncal; b0 += batch) {
+            const int nb_ = (int)std::min<int64_t>(batch, ncal - b0);
+            const int* ib = dperm + b0;
+            k_gather<<<(nb_ * kIn + 255) / 256, 256, 0, m->stream>>>(nb_, kIn, ib, m->X, m->H[0]);
+            k_gather<<<(nb_ * kOut + 255) / 256, 256, 0, m->stream>>>(nb_, kOut, ib, m->Y, ybatch);
+            forward(m, nb_);
+            k_t_sqerr<<<(nb_ + 255) / 256, 256, 0, m->stream>>>(nb_, m->out, ybatch, m->loss);
+            done += nb_;
+        }
+        float se = 0.0f;
+        MK(cudaMemcpyAsync(&se, m->loss, 4, cudaMemcpyDeviceToHost, m->stream));
+        MK(cudaStreamSynchronize(m->stream));
+        m->t_rms_ln = done ? std::log(10.0) / 4.0 * std::sqrt((double)se / (double)done) : 0.0;
+    }
     MK(cudaFreeAsync(ybatch, m->stream));
     MK(cudaFreeAsync(dperm, m->stream));
     MK(cudaStreamSynchronize(m->stream));
@@ -591,5 +629,11 @@ extern "C" int mochii_mlp_warm_start(mochii_ctx* c, mochii_mlp* m) {
     MK(cudaStreamSynchronize(m->stream));
     MK(cudaGetLastError());
     c->twarm_set = true;
+    // the first bracketing step spans 2.5 RMS errors of the prediction
+    // (within x1.002 .. x1.05); the residual gate accepts a prediction whose
+    // net heating is below 1e-6 of heating plus cooling
+    const double band = m->t_rms_ln > 0.0 ? 2.5 * m->t_rms_ln : std::log(1.05);
+    c->twarm_fac = std::exp(std::min(std::max(band, std::log(1.002)), std::log(1.05)));
+    c->twarm_gate = 1.0e-6;
     return MOCHII_OK;
 }

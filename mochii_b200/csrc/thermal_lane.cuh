@@ -573,86 +573,8 @@ struct CellSolve {
     }
 };
 
-// thermal_bracketed's temperature search for one lane.
-struct TempSearch {
-    int ph, s, it;   // 0 warm start, 1 bracketing, 2 false position, 9 done
-    double ta, fa, tb, fb, fac, la, lb, t, tr;
-    bool bisect;
-    __device__ __forceinline__ void begin(double Tw, double lo, double hi) {
-        ph = 0; s = 0; it = 0;
-        ta = fmin(fmax(Tw, lo), hi);
-        fa = 0.0; tb = ta; fb = 0.0; fac = 1.05; la = 0.0; lb = 0.0;
-        t = ta; tr = ta;
-        bisect = false;
-    }
-    __device__ __forceinline__ void feed(double f, double lo_lim, double hi_lim) {
-        bool to_fp = false;
-        if (ph == 0) {
-            fa = f;
-            if (fa == 0.0 || (ta <= lo_lim && fa < 0.0) || (ta >= hi_lim && fa > 0.0)) {
-                tr = ta;
-                ph = 9;
-            } else {
-                ph = 1;
-                s = 0;
-            }
-        } else if (ph == 1) {
-            fb = f;
-            ++s;
-            if (fb == 0.0) {
-                tr = tb;
-                ph = 9;
-            } else if ((fb > 0.0) != (fa > 0.0)) {
-                to_fp = true;
-            } else if (tb >= hi_lim || tb <= lo_lim) {
-                tr = tb;
-                ph = 9;
-            } else {
-                ta = tb;
-                fa = fb;
-                fac = fac * fac;
-                if (s >= 40) to_fp = true;
-            }
-        } else {   // ph == 2
-            const double fc = f, lc = log(t), width = fabs(lb - la);
-            ++it;
-            tr = t;
-            if (fc == 0.0) {
-                ph = 9;
-            } else {
-                if ((fc > 0.0) == (fa > 0.0)) {
-                    la = lc;
-                    fa = fc;
-                } else {
-                    lb = lc;
-                    fb = fc;
-                }
-                bisect = fabs(lb - la) > 0.5 * width;
-            }
-        }
-        if (to_fp) {
-            la = log(ta);
-            lb = log(tb);
-            tr = tb;
-            bisect = false;
-            it = 0;
-            ph = 2;
-        }
-        if (ph == 1) {
-            tb = fa > 0.0 ? fmin(ta * fac, hi_lim) : fmax(ta / fac, lo_lim);
-            t = tb;
-        } else if (ph == 2) {
-            const double width = fabs(lb - la);
-            if (width < 1.0e-5 || it >= 80) {
-                ph = 9;
-            } else {
-                double lc = (la * fb - lb * fa) / (fb - fa);
-                if (bisect || !(fabs(lc - la) > 0.05 * width && fabs(lc - lb) > 0.05 * width)) lc = 0.5 * (la + lb);
-                t = exp(lc);
-            }
-        }
-    }
-};
+// thermal_bracketed's temperature search for one lane: TRoot.
+using TempSearch = TRoot;
 
 // One lane's leaf.
 struct LaneLeaf {
@@ -699,7 +621,7 @@ __device__ __forceinline__ void lane_claim(const ThArgs& a, unsigned long long* 
                     L.xHI = L.x0; L.xHeI = L.h10; L.xHeII = L.h20;
                     L.ne = b.ne[il];
                     L.passes = 0; L.nsum = 0; L.nev = 0;
-                    L.ts.begin(a.Twarm ? a.Twarm[il] : L.T0, a.te_min, a.te_max);
+                    L.ts.begin(a.Twarm ? a.Twarm[il] : L.T0, a.te_min, a.te_max, a.tfac0, a.Twarm ? a.gate : 0.0);
                 } else {
                     b.ne[il] = 0.0;
                     write_columns(b.col, il, b.nabs, b.fp32, nH, b.yHe, L.x0, L.h10, L.h20, b.colscale,
@@ -749,6 +671,7 @@ __device__ __noinline__ void lane_finish(const ThArgs& a, const LaneCache& cache
     acc.tpass += (unsigned long long)L.passes;
     acc.tsums += (unsigned long long)L.nsum;
     acc.nevals += (unsigned long long)L.nev;
+    if (L.ts.accepted) ++acc.accepted;
     if (a.work) a.work[il] = (unsigned)min(L.nsum, 65535);
     b.xHI[il] = xn;
     b.xHeI[il] = h1n;
@@ -817,14 +740,18 @@ __device__ __noinline__ void lane_solve(const ThArgs& a, unsigned long long* nex
             const long long il = L.il;
             const double heat = nH * (L.xHI * b.rates[3 * n + il] +
                                       b.yHe * (L.xHeI * b.rates[4 * n + il] + L.xHeII * b.rates[5 * n + il]));
-            double net = heat - cooling_total(a.td, b.rs, b.caseA, b.yHe, T, nH, L.ne, L.xHI, L.xHeI, L.xHeII);
+            const double cool = cooling_total(a.td, b.rs, b.caseA, b.yHe, T, nH, L.ne, L.xHI, L.xHeI, L.xHeII);
+            double net = heat - cool;
             const MetalThermalTerms mt = lane_thermal(cache, a.td, il, T, nH, L.ne, nH * L.xHI, nH * (1.0 - L.xHI));
             net = net - mt.cool;
             net = net - mt.cool_H;
             if (b.metal_ff) net = net - mt.freefree;
             if (b.metal_heat) net = net + mt.heat;
+            // heating plus cooling: the scale of the learned warm start's residual gate
+            const double scale = fabs(heat) + fabs(cool) + fabs(mt.cool) + fabs(mt.cool_H) +
+                                 (b.metal_ff ? fabs(mt.freefree) : 0.0) + (b.metal_heat ? fabs(mt.heat) : 0.0);
             ++L.nev;
-            L.ts.feed(net, a.te_min, a.te_max);
+            L.ts.feed(net, a.te_min, a.te_max, scale);
             fin = L.ts.ph == 9;
         }
         lane_finish(a, cache, L, fin, acc);
@@ -847,12 +774,12 @@ __global__ void __launch_bounds__(kBThreads, 1) k_thermal_lane(const ThArgs a) {
     lane_solve(a, a.next, cache, acc, lane);
     // block sums into partial[6 x block], counters
     double v[6] = {acc.mdx, acc.mdt, acc.s1, acc.s2, acc.s3, acc.s4};
-    unsigned long long cnt[4] = {acc.solved, acc.tpass, acc.tsums, acc.nevals};
+    unsigned long long cnt[5] = {acc.solved, acc.tpass, acc.tsums, acc.nevals, acc.accepted};
     for (int o = 16; o > 0; o >>= 1) {
         v[0] = fmax(v[0], __shfl_down_sync(kFull, v[0], o));
         v[1] = fmax(v[1], __shfl_down_sync(kFull, v[1], o));
         for (int k = 2; k < 6; ++k) v[k] += __shfl_down_sync(kFull, v[k], o);
-        for (int k = 0; k < 4; ++k) cnt[k] += __shfl_down_sync(kFull, cnt[k], o);
+        for (int k = 0; k < 5; ++k) cnt[k] += __shfl_down_sync(kFull, cnt[k], o);
     }
     const int w = threadIdx.x >> 5, nw = blockDim.x >> 5;
     if (lane == 0) {
@@ -861,6 +788,7 @@ __global__ void __launch_bounds__(kBThreads, 1) k_thermal_lane(const ThArgs a) {
         if (cnt[1]) atomicAdd(a.b.counters + 2, cnt[1]);
         if (cnt[2]) atomicAdd(a.b.counters + 3, cnt[2]);
         if (cnt[3]) atomicAdd(a.b.counters + 4, cnt[3]);
+        if (cnt[4]) atomicAdd(a.b.counters + 5, cnt[4]);
     }
     __syncthreads();
     if (threadIdx.x == 0) {

@@ -376,11 +376,56 @@ long long orc_sim_set(void* h, const char* name, const double* in, long long n) 
     else if (nm == "n_e") v = &s->st.ne;
     else if (nm == "T_e") v = &s->st.Te;
     else if (nm == "nH") v = &s->st.nH;
+    else if (nm == "gamma_HI") v = &s->gamma_HI;
+    else if (nm == "gamma_HeI") v = &s->gamma_HeI;
+    else if (nm == "gamma_HeII") v = &s->gamma_HeII;
+    else if (nm == "heat_HI") v = &s->heat_HI;
+    else if (nm == "heat_HeI") v = &s->heat_HeI;
+    else if (nm == "heat_HeII") v = &s->heat_HeII;
+    else if (s->metals() && (nm == "gamma_metal" || nm == "heat_metal")) {
+        // leaf-major in element order, in[il*ntr + j], as orc_sim_get returns them
+        Species& sp = *s->sp;
+        const int nl = sp.nleaf;
+        if (n != (long long)sp.ntr * nl) return -1;
+        auto& dst = nm == "gamma_metal" ? sp.egam : sp.eheat;
+        int j0 = 0;
+        for (size_t ie = 0; ie < sp.el.size(); ++ie) {
+            const int nt = sp.el[ie].nstage - 1;
+            for (int i = 0; i < nt; ++i)
+                for (int il = 0; il < nl; ++il) dst[ie][(size_t)i * nl + il] = in[(size_t)il * sp.ntr + j0 + i];
+            j0 += nt;
+        }
+        return n;
+    }
     if (!v || (long long)v->size() != n) return -1;
     std::memcpy(v->data(), in, (size_t)n * sizeof(double));
-    s->opacity_fill();   // the stage cache follows the state it is read from
+    if (nm.rfind("gamma_", 0) != 0 && nm.rfind("heat_", 0) != 0)
+        s->opacity_fill();   // the stage cache follows the state it is read from
     return n;
 }
+// The thermal bisection (thermal_cell, thermal_mod.f90:159-188) of the given
+// leaves from the current state and rates, state unchanged: out5[k*5 + .] =
+// T_e, x_HI, x_HeI, x_HeII, n_e of leaf idx[k] (as the solve leaves them,
+// before under-relaxation).  Returns the leaves solved, -1 without T_e.
+long long orc_sim_thermal_cells(void* h, const long long* idx, long long n, double* out5) {
+    auto* s = static_cast<Sim*>(h);
+    if (!s->th) return -1;
+#pragma omp parallel for num_threads(std::max(1, s->nthreads)) schedule(dynamic, 8)
+    for (long long k = 0; k < n; ++k) {
+        const long long il = idx[k];
+        double* o = out5 + 5 * k;
+        if (il < 0 || il >= s->grid.nleaf || s->st.nH[il] <= 0.0) {
+            o[0] = o[1] = o[2] = o[3] = o[4] = -1.0;
+            continue;
+        }
+        double x, h1, h2, ne;
+        o[0] = s->thermal_cell((int)il, x, h1, h2, ne);
+        o[1] = x; o[2] = h1; o[3] = h2; o[4] = ne;
+    }
+    return n;
+}
+// Diffuse packets launched by the last transport pass (diffuse_nphot).
+long long orc_sim_diffuse_count(void* h) { return static_cast<Sim*>(h)->diffuse_nphot; }
 // Diffuse field: build from the current state, then launch records.
 double orc_sim_diffuse_build(void* h, long long* nphot) {
     auto* s = static_cast<Sim*>(h);

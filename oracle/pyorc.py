@@ -81,6 +81,8 @@ def load():
         "orc_sim_diffuse_build": (D, [V, V]),
         "orc_sim_diffuse_photon": (None, [V, LL, V]),
         "orc_milne_sample": (D, [V, I, D, D]),
+        "orc_sim_thermal_cells": (LL, [V, V, LL, V]),
+        "orc_sim_diffuse_count": (LL, [V]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)
@@ -281,6 +283,19 @@ class Sim:
         """The thermal bisection on every stride-th gas leaf, state unchanged."""
         return load().orc_sim_thermal_sample(self.h, int(stride))
 
+    def thermal_cells(self, idx):
+        """The reference's thermal bisection of the leaves idx from the current
+        state and rates, state unchanged: (n, 5) = T_e, x_HI, x_HeI, x_HeII, n_e."""
+        idx = np.ascontiguousarray(idx, dtype=np.int64)
+        out = np.zeros((idx.size, 5))
+        assert load().orc_sim_thermal_cells(self.h, idx.ctypes.data, idx.size, out.ctypes.data) == idx.size
+        return out
+
+    @property
+    def diffuse_count(self):
+        """Diffuse packets of the last transport pass."""
+        return int(load().orc_sim_diffuse_count(self.h))
+
     def net_rate(self, il, T):
         """thermal_mod.f90 net_rate on leaf il at T: (net, x_HI, x_HeI, x_HeII, n_e)."""
         o = np.zeros(5)
@@ -323,8 +338,10 @@ class Sim:
         return out
 
     def set(self, name, values):
+        """State fields (x_HI, x_HeI, x_HeII, n_e, T_e, nH) or rates (gamma_*,
+        heat_*, and with metals gamma_metal / heat_metal, leaf-major)."""
         a = np.ascontiguousarray(values, dtype=float)
-        assert load().orc_sim_set(self.h, name.encode(), a.ctypes.data, a.size) == a.size
+        assert load().orc_sim_set(self.h, name.encode(), a.ctypes.data, a.size) == a.size, name
 
     def diffuse_build(self):
         n = C.c_longlong()

@@ -68,3 +68,32 @@ def test_launch_count(bench):
     # 3 chunks of <= 4 Mi packets: launch + walk each, rates, metal rates,
     # balance, diffuse luminosities, one diffuse chunk
     assert bench.launches_per_step(m, 1_000_000) == 2 * 3 + 2 + 2 + 2
+
+
+def test_prepared_state_is_a_developed_hii_region():
+    """The analytic start state both bench arms use: deterministic, an
+    ionized sphere of about 18 % of the box, charge balance in n_e."""
+    import numpy as np
+    a, b = configs.prepared_state(32), configs.prepared_state(32)
+    for k in a:
+        assert np.array_equal(a[k], b[k])
+    x = a["x_HI"]
+    assert x.size == 32 ** 3 and 0.15 < np.mean(x < 0.5) < 0.21
+    assert x.min() >= 1e-3 and x.max() <= 1.0
+    assert np.allclose(a["n_e"], 100.0 * ((1 - x) + 0.1 * a["x_HeII"]))
+    assert a["T_e"].min() >= 3e3 - 1e-6 and a["T_e"].max() <= 8e3 + 1e-6
+    s = configs.prepared_state(16, front=1.0, he=False, T_in=1e4, T_out=1e4)
+    assert set(s) == {"x_HI", "T_e", "n_e"} and np.all(s["T_e"] == 1e4)
+
+
+def test_reference_arm_measures_the_same_workload(bench, lib):
+    """The reference arm (the oracle port on the host) times a measured
+    fraction of the same step from the same analytic state: its config is
+    the device arm's, and the sample's packet count includes the diffuse
+    packets, as the device arm counts them."""
+    wl = bench.Workload("hii_metals128", grid=12, packets=20000)
+    assert bench.config_of(wl) == bench.config_of(wl) and "analytic" in bench.config_of(wl)["state"]
+    v, desc, t_step, pk = bench.cpu_reference(wl, 2, steps=1, warmup=1)
+    assert v > 0 and t_step > 0
+    assert pk > 20000 // wl.cpu_fraction()   # stellar plus diffuse packets
+    assert abs(v * t_step - pk) < 1e-6 * pk
