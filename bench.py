@@ -386,6 +386,8 @@ def main():
                     choices=["hii_metals128", "stromgren64", "clumpy_dusty", "batch64"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-converge", action="store_true", help="skip the time-to-converged comparison")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the dusty-octree and batched-nebulae figures the default run adds")
     ap.add_argument("--precision", default=None, choices=["fp64", "fp32"],
                     help="transport arithmetic (default: the workload's)")
     ap.add_argument("--solver", default="bracketed", choices=["bisection", "bracketed"],
@@ -547,6 +549,15 @@ def main():
     conv = None
     if rank == 0 and not args.no_converge and wl.name == "hii_metals128":
         conv = time_to_converged()
+    extras = None
+    if rank == 0 and world == 1 and not args.no_extras and wl.name == "hii_metals128" and wl.grid == 128:
+        extras = run_extras()
+    # the thermal solve (the step's other kernel): leaves and net-rate
+    # evaluations per second of its device time
+    bm = np.mean(np.array(bcnt, dtype=float), axis=0)
+    bal_s = float(np.mean(bal_ms)) * 1e-3
+    balance = {"cells_per_s": bm[0] / bal_s, "net_rate_evaluations_per_s": bm[1] / bal_s,
+               "evaluations_per_cell": bm[1] / max(bm[0], 1.0), "kernel_ms": bal_s * 1e3}
 
     if rank == 0:
         line = {
@@ -569,12 +580,16 @@ def main():
             "cpu_baseline": cpu,
             "time_to_converged": conv,
             "clocks": clk.summary(),
-            "gpu_launches": int(sum(launches_per_step(wl, n_ - wl.nphot) for n_ in npk)),
+            "gpu_launches": int(sum(launches_per_step(wl, n_ - wl.nphot, neb_order(neb) == "coherent" and wl.grid)
+                                    for n_ in npk)),
             "breakdown_ms": {"transport": float(np.mean(pass_ms)), "balance": float(np.mean(bal_ms))},
             "balance_counts_per_step": dict(zip(("cells", "rate_evaluations", "metal_sums", "ne_evaluations"),
-                                                (float(v) for v in np.mean(np.array(bcnt, dtype=float), axis=0)))),
+                                                (float(v) for v in bm))),
+            "balance": balance,
             "wall_s": t_wall,
         }
+        if extras:
+            line["extras"] = extras
         print(json.dumps(line), flush=True)
     neb.close()
     if dist is not None:
@@ -713,26 +728,26 @@ def run_batch(args, wl, prec):
 
     if rank == 0:
         n_all = int(sum(nleaf))
-        chunks = sum(2 * -(-wl.nphot // 1048576) + 2 for _ in nebs)
+        chunks = sum(3 * -(-wl.nphot // 1048576) + 2 for _ in nebs)   # keys, launch, walk per chunk; rates
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64" if prec == "fp64" else "f32+f64",
             "data": "synthetic",
-            "config": {"workload": wl.name, "grid": grid_name(wl, n_all), "instances": len(nebs),
-                       "stellar_packets_per_instance": wl.nphot, "packets_per_step": packets / args.steps / world,
-                       "precision": prec, "balance": "thermal", "solver": args.solver,
-                       "cell_layout": args.cell_layout, "tallies": args.tally, "metal_tallies": "exact",
-                       "state": "each instance's ionized start, then the warm-up iterations",
-                       "l2": "flushed between steps (256 MiB write)", "packet_chunk": 1048576,
-                       "execution": "one CUDA graph per iteration (all passes, then one persistent thermal launch)",
-                       "tuning": f"walk shape autotuned per grid size ({len(tuned)} sizes)",
-                       "parallelism": "replicas" if world > 1 else "single"},
+            "config": config_of(wl, n_all),
+            "implementation": {"packets_per_step": packets / args.steps / world, "precision": prec,
+                               "solver": args.solver, "cell_layout": args.cell_layout, "tallies": args.tally,
+                               "metal_tallies": "exact", "packet_order": neb_order(nebs[0]),
+                               "l2": "flushed between steps (256 MiB write)", "packet_chunk": 1048576,
+                               "execution": "one CUDA graph per iteration (all passes, then one persistent thermal "
+                                            "launch)",
+                               "tuning": f"walk shape autotuned per grid size ({len(tuned)} sizes)",
+                               "parallelism": "replicas" if world > 1 else "single"},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 16 * n_all,
                     "d2h_bytes_per_step": 24 * n_all},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "peak_kind": peak_kind, "traffic": None,
-                         "kernel": "k_launch + k_walk_edge (transport passes, one unbatched iteration)",
+                         "kernel": "transport passes (keys, launch, walk; one unbatched iteration)",
                          "segments_per_step": useg, "kernel_ms": kern_ms},
             "cpu_baseline": cpu,
             "clocks": clk.summary(),
@@ -750,21 +765,52 @@ def run_batch(args, wl, prec):
     return 0
 
 
-def time_to_converged(n=64, nphot=1_000_000, iters=20, train_iters=10, seed_train=777, seed=12345):
+def solve_check(neb, sim, idx):
+    """The device's next thermal update against the reference's bisection
+    (the FP64 oracle) on the same inputs: the device state and rates before
+    the update go to the oracle, which solves the leaves idx; returns a
+    function that, called after the device update, gives the largest
+    |dT_e| [K] and |dx_HII| over idx."""
+    for f in ("x_HI", "x_HeI", "x_HeII", "n_e", "T_e"):
+        sim.set(f, neb.get(f))
+    for f in ("gamma_HI", "gamma_HeI", "gamma_HeII", "heat_HI", "heat_HeI", "heat_HeII", "gamma_metal", "heat_metal"):
+        sim.set(f, np.ascontiguousarray(neb.get(f)).ravel())
+    ref = sim.thermal_cells(idx)
+
+    def after():
+        T, x = neb.get("T_e")[idx], neb.get("x_HI")[idx]
+        return float(np.max(np.abs(T - ref[:, 0]))), float(np.max(np.abs(x - ref[:, 1])))
+    return after
+
+
+def time_to_converged(n=64, nphot=1_000_000, iters=20, train_iters=10, seed_train=777, seed=12345, checks=(1, 10, 20),
+                      nsample=3000):
     """Time to a converged nebula of the metals H II-region class (n^3, the
-    128^3 workload's physics): `iters` transport + thermal iterations from the
-    ionized start with the reference's solver (damped n_e fixed point,
-    bisection on T_e) against the bracketed solver warm-started by the MLP.
+    128^3 workload's physics, FP32 transport) from its configured ionized
+    start, `iters` transport + thermal iterations, three ways:
+      plain      the reference's solver on the device (damped n_e fixed
+                 point, bisection on log T over [te_min, te_max]);
+      bracketed  the same roots by the bracketed search from the previous T_e;
+      mlp        the bracketed search from the learned warm start: the MLP's
+                 T_e is accepted where its net heating is below 1e-6 of
+                 heating plus cooling, else it seeds a narrow first bracket.
     The MLP is trained first on the plain solver's (features, solved state)
     pairs of another nebula of the class (launch seed seed_train).  Device
-    time from the library's CUDA events; the accuracy is the largest |dx_HII|
-    and |dT_e| between the two final states."""
+    time from the library's CUDA events (the warm start's inference by host
+    clock around its synchronous call).  Accuracy: at the iterations in
+    `checks`, each arm's update of nsample leaves against the FP64 oracle's
+    bisection on the same inputs (state and rates copied from the device).
+    The final states of the arms are also compared with each other against
+    the Monte Carlo noise of the iteration (the plain arm's last change)."""
+    from oracle import pyorc
     from mochii_b200 import Nebula, configs, parse_namelist
     from mochii_b200.mlp import WarmStartMLP
 
+    def nl_of(sd, prec="fp32"):
+        return configs.hii_metals(nphotons=nphot, niter=iters, n=n, precision=prec, seed=sd)
+
     def neb_of(solver, sd):
-        nl = configs.hii_metals(nphotons=nphot, niter=iters, n=n, precision="fp32", seed=sd)
-        return Nebula(parse_namelist(nl.replace("/\n", f" par%thermal_solver = '{solver}'\n/\n")))
+        return Nebula(parse_namelist(nl_of(sd).replace("/\n", f" par%thermal_solver = '{solver}'\n/\n")))
 
     t0 = time.perf_counter()
     X, Y = [], []
@@ -781,42 +827,89 @@ def time_to_converged(n=64, nphot=1_000_000, iters=20, train_iters=10, seed_trai
     t0 = time.perf_counter()
     losses = mlp.train(X, Y, epochs=20, batch=4096, lr=2e-3, seed=2)
     t_train = time.perf_counter() - t0
+    sim = pyorc.Sim(nl_of(seed, "fp64"), nthreads=cpu_threads(Workload("hii_metals128", grid=n)))
+    rng = np.random.default_rng(3)
     res = {}
     for mode in ("plain", "bracketed", "mlp"):
         neb = neb_of("bisection" if mode == "plain" else "bracketed", seed)
-        ms, evals = 0.0, 0
-        for _ in range(iters):
+        ms, evals, accepted, acc = 0.0, 0, 0, []
+        prev_T = None
+        for it in range(1, iters + 1):
             st = neb.ionizing_field_and_rates()
             ms += st.pass_ms
+            check = None
+            if it in checks:   # half the sample from the ionized leaves, where the solve iterates
+                x = neb.get("x_HI")
+                ion = np.flatnonzero(x < 0.9)
+                k = min(nsample // 2, ion.size)
+                idx = np.unique(np.concatenate([rng.choice(ion, k, replace=False) if k else ion[:0],
+                                                rng.choice(x.size, nsample - k, replace=False)]))
+                check = solve_check(neb, sim, idx)
             if mode == "mlp":
                 e0 = time.perf_counter()
-                mlp.warm_start(neb)          # synchronous: device inference + features
+                mlp.warm_start(neb)          # synchronous: device features + inference
                 ms += (time.perf_counter() - e0) * 1e3
+            if it == iters:
+                prev_T = neb.get("T_e")
             neb.gas_thermal_update()
             ms += neb.last_metrics.kernel_ms
             evals += neb.last_metrics.rate_evaluations
-        res[mode] = (ms / 1e3, evals, neb.get("x_HI"), neb.get("T_e"))
+            accepted += neb.last_metrics.warm_accepted
+            if check is not None:
+                dT, dx = check()
+                acc.append({"iteration": it, "leaves": int(idx.size), "max_dT_e_K": dT, "max_dx_HII": dx})
+        res[mode] = dict(s=ms / 1e3, evals=evals, accepted=accepted, acc=acc, x=neb.get("x_HI"), T=neb.get("T_e"),
+                         last_change=np.abs(neb.get("T_e") - prev_T))
         neb.close()
     mlp.close()
-    def stats(a, b, k):
-        d = np.abs(res[a][k] - res[b][k])
+
+    def stats(d):
         return {"p50": float(np.percentile(d, 50)), "p99": float(np.percentile(d, 99)), "max": float(d.max())}
 
-    def glob(a):
-        x, T = res[a][2], res[a][3]
+    def glob(r):
+        x, T = r["x"], r["T"]
         return {"ionized_fraction": float(np.mean(1 - x)), "mean_T_e_ionized": float(np.mean(T[x < 0.5]))}
-    return {"config": f"hii_metals {n}^3, {nphot:.0e} packets, {iters} iterations, FP32 transport",
-            "plain_s": res["plain"][0], "bracketed_s": res["bracketed"][0], "mlp_s": res["mlp"][0],
-            "speedup_mlp_vs_plain": res["plain"][0] / res["mlp"][0],
-            "speedup_bracketed_vs_plain": res["plain"][0] / res["bracketed"][0],
-            "net_rate_evaluations": {k: v[1] for k, v in res.items()},
-            "dx_HII_vs_plain": {"bracketed": stats("bracketed", "plain", 2), "mlp": stats("mlp", "plain", 2)},
-            "dT_e_vs_plain_K": {"bracketed": stats("bracketed", "plain", 3), "mlp": stats("mlp", "plain", 3)},
-            "global": {k: glob(k) for k in res},
-            "note": "final states after the same iterations; the solvers agree per iteration (tests), the coupled "
-                    "iteration then carries Monte Carlo differences at the ionization front",
+    ion = res["plain"]["x"] < 0.5
+    worst = {m: {"max_dT_e_K": max(a["max_dT_e_K"] for a in r["acc"]), "max_dx_HII": max(a["max_dx_HII"] for a in r["acc"])}
+             for m, r in res.items()}
+    return {"config": f"hii_metals {n}^3, {nphot:.0e} packets, {iters} iterations from the configured ionized start, "
+                      f"FP32 transport",
+            "plain_s": res["plain"]["s"], "bracketed_s": res["bracketed"]["s"], "mlp_s": res["mlp"]["s"],
+            "speedup_mlp_vs_plain": res["plain"]["s"] / res["mlp"]["s"],
+            "speedup_bracketed_vs_plain": res["plain"]["s"] / res["bracketed"]["s"],
+            "speedup_mlp_vs_bracketed": res["bracketed"]["s"] / res["mlp"]["s"],
+            "net_rate_evaluations": {k: int(v["evals"]) for k, v in res.items()},
+            "mlp_gate_accepted_leaves": int(res["mlp"]["accepted"]),
+            "solve_vs_fp64_oracle": {"bars": {"T_e_K": 20.0, "x_HII": 1e-3}, "worst": worst,
+                                     "per_check": {k: v["acc"] for k, v in res.items()}},
+            "final_state_between_arms": {
+                "note": "the coupled iteration carries Monte Carlo noise: the diffuse packets relaunch from "
+                        "different leaves as the state moves; compare with the plain arm's own last change",
+                "plain_last_change_T_e_K_ionized": stats(res["plain"]["last_change"][ion]),
+                "dT_e_K_ionized": {m: stats(np.abs(res[m]["T"] - res["plain"]["T"])[ion]) for m in ("bracketed", "mlp")},
+                "global": {k: glob(v) for k, v in res.items()}},
             "training": {"pairs": int(len(X)), "data_s": t_data, "train_s": t_train, "epochs": 20,
                          "loss_first": float(losses[0]), "loss_last": float(losses[-1])}}
+
+
+def run_extras(steps=2, warmup=3):
+    """The other single-GPU configurations as extra keys of the headline
+    line: the dusty clumpy nebula on the octree and the 64 batched H II
+    regions, each this script in a child process (its own device memory),
+    reduced to value, e2e, step time and roofline."""
+    out = {}
+    for name in ("clumpy_dusty", "batch64"):
+        cmd = [sys.executable, os.path.abspath(__file__), "--workload", name, "--steps", str(steps), "--warmup",
+               str(warmup), "--no-converge", "--no-cpu-baseline", "--no-extras"]
+        try:
+            r = subprocess.run(cmd, capture_output=True, text=True, timeout=1500)
+            d = json.loads([l for l in r.stdout.splitlines() if l.startswith("{")][-1])
+            out[name] = {k: d.get(k) for k in ("value", "unit", "ms_per_step", "steps", "warmup", "config",
+                                               "implementation", "e2e", "clocks", "gpu_launches")}
+            out[name]["roofline"] = {k: d["roofline"].get(k) for k in ("achieved", "peak", "frac", "kernel_ms")}
+        except Exception as e:   # reported, not fatal: the headline stands on its own
+            out[name] = {"error": f"{type(e).__name__}: {e}"[:300]}
+    return out
 
 
 def neb_order(neb):
@@ -829,15 +922,20 @@ def grid_name(wl, nleaf):
     return f"{wl.grid}^3" if wl.grid else f"octree, {nleaf or 'about 3e6'} leaves"
 
 
-def launches_per_step(wl, diffuse_packets):
-    """Kernels of this library per step: a launch and a walk per chunk of up
-    to 4 Mi stellar packets, the H/He rates (+ the metal rates), the balance;
-    with the diffuse field the leaf luminosities and a launch and a walk per
-    diffuse chunk (the prefix sum is a library scan, not counted)."""
+def launches_per_step(wl, diffuse_packets, coherent=True):
+    """Kernels of this library per step: per chunk of up to 4 Mi stellar
+    packets a launch and a walk (coherent order: also the key kernel; the
+    sort is a library radix sort, not counted), the H/He rates (+ the metal
+    rates), the balance; with the diffuse field the leaf luminosities and a
+    launch and a walk per diffuse chunk (the prefix sum is a library scan, not
+    counted); on the Cartesian workloads the opacity refresh of the step's
+    start state (one kernel)."""
     cap = 1 << 22
-    n = 2 * -(-wl.nphot // cap) + 1 + 1
+    n = (3 if coherent else 2) * -(-wl.nphot // cap) + 1 + 1
     if wl.name == "hii_metals128":
         n += 1 + 1 + 2 * -(-diffuse_packets // cap)
+    if wl.state() is not None:
+        n += 1
     return n
 
 

@@ -159,10 +159,13 @@ typedef struct mochii_params {
      * the size of the packet-record buffer, default 4194304 */
     int64_t packet_chunk;
     /* walk order of a chunk's stellar packets (not a reference key,
-     * par%packet_order): 0 'launch' = the launch (Sobol) order (default);
-     * 1 'direction' = sorted by source and direction cell, so a warp's
-     * packets cross the same leaves (their tally reductions then meet on the
-     * same addresses, which measured slower on B200) */
+     * par%packet_order): 2 'coherent' (default) = the chunk sorted by source,
+     * direction cell and energy quantile before its launch, each warp walking
+     * 32 nearly parallel packets of nearly equal energy and summing the
+     * tallies of lanes in the same leaf and bins before one reduction (the
+     * Cartesian grid without grains or FUV; elsewhere the launch order);
+     * 0 'launch' = the launch (Sobol) order; 1 'direction' = sorted by source
+     * and direction cell after the launch, per-lane reductions */
     int packet_order;
 } mochii_params;
 
@@ -236,6 +239,29 @@ int mochii_transport_pass(mochii_ctx* ctx, int with_peel, mochii_pass_stats* sta
 int mochii_balance_update(mochii_ctx* ctx, int solve_te, mochii_metrics* m);
 /* gas_opacity_fill: refresh the per-leaf absorber columns the transport reads. */
 int mochii_opacity_fill(mochii_ctx* ctx);
+
+/* ---- the rates file: gas_rates_write (gas_rates_mod.f90:216-366) -------------- */
+/* The run's convergence record, written as the file's header keywords
+ * (CONVERGD, NITERDON, FINALDX, FINALDTE, FLDCONS; main.f90:188-225). */
+typedef struct mochii_run_info {
+    int converged;          /* the gas iteration met its convergence test        */
+    int iterations;         /* gas iterations run                                 */
+    double final_dx;        /* final max|delta x_HII|                             */
+    double final_dte;       /* final max|delta T_e|/T_e                           */
+    int field_consistent;   /* the rates come from a pass through the written state */
+} mochii_run_info;
+/* Write the rates and state of the current iterate as the reference's rates
+ * file does (gas_rates_write, with species_write for the metals): the same
+ * dataset names (Gamma_HI ... Heat_HeII, Heat_dust with grains, J_nu, x_HI,
+ * x_HeI, x_HeII, n_e, T_e, E_bin, dE_bin, LeafXYZ, LeafSize,
+ * x_<el>_stages, Gamma_<el>_stages, Heat_<el>_stages) and header keywords,
+ * in a format that needs no I/O library: directory <base>_rates/ with one
+ * .npy file per dataset (FP64, C order; the reference's Fortran array
+ * a(n1, n2) is shape (n2, n1), the same bytes) and header.json (keywords,
+ * and per dataset its file, shape and comment).  The energy ledger keywords
+ * are those of the last transport pass; run may be NULL (not converged,
+ * zero iterations). */
+int mochii_write_rates(mochii_ctx* ctx, const char* base, const mochii_run_info* run);
 
 /* ---- batched nebulae (no reference counterpart: one job is one nebula) ------ */
 /* Several contexts on the current device advanced together.  One iteration of

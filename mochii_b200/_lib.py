@@ -74,6 +74,11 @@ class Metrics(C.Structure):
                 ("warm_accepted", C.c_int64)]
 
 
+class RunInfo(C.Structure):
+    _fields_ = [("converged", C.c_int), ("iterations", C.c_int), ("final_dx", C.c_double), ("final_dte", C.c_double),
+                ("field_consistent", C.c_int)]
+
+
 class Tuning(C.Structure):
     _fields_ = [("lookahead", C.c_int), ("walk_blocks_per_sm", C.c_int), ("best_ms", C.c_double)]
 
@@ -109,6 +114,7 @@ SIGNATURES = {
     "mochii_metal_shape": (C.c_int, [C.c_void_p, _P(C.c_int), _P(C.c_int)]),
     "mochii_nnu_band": (C.c_int, [C.c_void_p]),
     "mochii_get_field": (C.c_int, [C.c_void_p, C.c_char_p, C.c_void_p, C.c_int64]),
+    "mochii_write_rates": (C.c_int, [C.c_void_p, C.c_char_p, _P(RunInfo)]),
     "mochii_set_field": (C.c_int, [C.c_void_p, C.c_char_p, C.c_void_p, C.c_int64]),
     "mochii_set_nphotons": (C.c_int, [C.c_void_p, C.c_int64]),
     "mochii_ion_Ltot": (C.c_double, [C.c_void_p]),

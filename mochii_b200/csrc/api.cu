@@ -735,6 +735,7 @@ extern "C" int mochii_batch_iterate(mochii_batch* b, int solve_te, mochii_pass_s
         s.metal_active = (int64_t)b->tcount[k][2];
         s.scattered_segments = (int64_t)b->tcount[k][3];
         s.packets = c->par.nphotons;
+        c->last_pass = s;
         if (st) st[k] = s;
         mochii_metrics r;
         std::memset(&r, 0, sizeof(r));
@@ -865,6 +866,7 @@ extern "C" int mochii_transport_pass(mochii_ctx* c, int with_peel, mochii_pass_s
     s.diffuse_packets = nd;
     s.diffuse_lum = dlum;
     s.packets = c->par.nphotons + nd;
+    c->last_pass = s;
     if (st) *st = s;
     if (!std::isfinite(s.energy_emitted) || !std::isfinite(s.energy_absorbed))
         return fail(c, MOCHII_ERR_NONFINITE, "non-finite energy ledger");

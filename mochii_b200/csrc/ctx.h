@@ -147,5 +147,6 @@ struct mochii_ctx {
     // buffer a recorded batch graph holds (set_nphotons, set_tuning,
     // autotune, the T_warm buffer); a batch refuses to replay after a change
     uint64_t generation = 0;
+    mochii_pass_stats last_pass = {};   // statistics of the last transport pass (the rates file's ledger)
     std::string last_error;
 };

@@ -141,7 +141,7 @@ extern "C" int mochii_params_default(mochii_params* p) {
     p->tally64 = 1;
     p->metal_rate_table = 1;
     p->packet_chunk = 1 << 22;
-    p->packet_order = 0;
+    p->packet_order = 2;   // 'coherent' (the launch order where it does not apply)
     return MOCHII_OK;
 }
 

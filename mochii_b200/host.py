@@ -163,6 +163,16 @@ class Nebula:
             out = out.reshape(self.nleaf, nst)
         return out
 
+    def write_rates(self, base, converged=False, iterations=0, final_dx=0.0, final_dte=0.0, field_consistent=False):
+        """gas_rates_write: the rates and state of the current iterate as
+        <base>_rates/ (one .npy per dataset of the reference's rates file,
+        header.json with its keywords); returns the directory."""
+        from ._lib import RunInfo
+        ri = RunInfo(int(bool(converged)), int(iterations), float(final_dx), float(final_dte),
+                     int(bool(field_consistent)))
+        self._ok(self.lib.mochii_write_rates(self.ctx, str(base).encode(), C.byref(ri)))
+        return str(base) + "_rates"
+
     def set(self, name, values):
         a = np.ascontiguousarray(values, dtype=np.float64)
         self._ok(self.lib.mochii_set_field(self.ctx, name.encode(), a.ctypes.data, a.size))

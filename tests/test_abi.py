@@ -94,8 +94,9 @@ def test_execution_keys(lib):
     p = parse_namelist("&parameters par%packet_chunk = 1048576, par%tally_precision = 'compensated'\n"
                        " par%metal_rates = 'exact', par%cell_layout = 'flow' /")
     assert p.packet_chunk == 1048576 and p.tally64 == 0 and p.metal_rate_table == 0 and p.solver_warp == 2
-    assert d.packet_order == 0 and parse_namelist("&parameters par%packet_order = 'direction' /").packet_order == 1
-    with pytest.raises(MochiiError, match="'direction' or 'launch'"):
+    assert d.packet_order == 2 and parse_namelist("&parameters par%packet_order = 'direction' /").packet_order == 1
+    assert parse_namelist("&parameters par%packet_order = 'launch' /").packet_order == 0
+    with pytest.raises(MochiiError, match="'coherent', 'direction' or 'launch'"):
         parse_namelist("&parameters par%packet_order = 'random' /")
 
 

@@ -114,3 +114,44 @@ def test_warm_start_gain():
     assert runs["mlp"][0].sum() < runs["previous"][0].sum() < runs["bisection"][0].sum(), \
         {k: v[0].tolist() for k, v in runs.items()}
     mlp.close()
+
+
+def test_warm_started_update_matches_oracle_on_every_leaf(orc):
+    """One thermal update warm-started by the trained MLP (residual gate, then
+    the bracketed search from the prediction) against the reference's
+    bisection in the FP64 oracle on the same inputs -- the device state and
+    rates before the update copied into the oracle -- on every leaf of a
+    nebula with diffuse packets: T_e within 20 K and x_HII within 1e-3 (the
+    north-star bars); gate acceptances are counted and bounded by the leaves."""
+    X, Y = [], []
+    neb = nebula("bisection", 12345, n=20, nphot=80000)
+    for _ in range(5):
+        neb.ionizing_field_and_rates()
+        X.append(WarmStartMLP.features(neb))
+        neb.gas_thermal_update()
+        Y.append(WarmStartMLP.targets(neb, X[-1]))
+    neb.close()
+    mlp = WarmStartMLP(seed=1)
+    mlp.train(np.concatenate(X), np.concatenate(Y), epochs=30, batch=2048, lr=2e-3, seed=2)
+    n = 20
+    nl = configs.hii_metals(nphotons=80000, niter=8, n=n, precision="fp32", seed=4242, rs_factor=1.2, diffuse=True)
+    neb = Nebula(parse_namelist(nl.replace("/\n", " par%thermal_solver = 'bracketed'\n/\n")))
+    sim = orc.Sim(nl.replace("'fp32'", "'fp64'"))
+    for it in range(3):
+        neb.ionizing_field_and_rates()
+        for f in ("x_HI", "x_HeI", "x_HeII", "n_e", "T_e"):
+            sim.set(f, neb.get(f))
+        for f in ("gamma_HI", "gamma_HeI", "gamma_HeII", "heat_HI", "heat_HeI", "heat_HeII", "gamma_metal",
+                  "heat_metal"):
+            sim.set(f, np.ascontiguousarray(neb.get(f)).ravel())
+        ref = sim.thermal_cells(np.arange(n ** 3))
+        mlp.warm_start(neb)
+        neb.gas_thermal_update()
+        m = neb.last_metrics
+        assert 0 <= m.warm_accepted <= m.cells_solved
+        dT = np.abs(neb.get("T_e") - ref[:, 0])
+        dx = np.abs(neb.get("x_HI") - ref[:, 1])
+        assert dT.max() < 20.0, (it, dT.max())
+        assert dx.max() < 1e-3, (it, dx.max())
+    neb.close()
+    mlp.close()
