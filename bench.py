@@ -279,8 +279,7 @@ def cpu_reference(wl, nthreads, steps=1, warmup=1, state=None):
     times, pk = [], []
     for k in range(warmup + steps):
         if st0 is not None:
-            for name, v in st0.items():
-                sim.set(name, v)
+            sim.set_state(st0)
         t0 = time.perf_counter()
         sim.transport_pass()
         if wl.thermal:
@@ -771,8 +770,7 @@ def solve_check(neb, sim, idx):
     the update go to the oracle, which solves the leaves idx; returns a
     function that, called after the device update, gives the largest
     |dT_e| [K] and |dx_HII| over idx."""
-    for f in ("x_HI", "x_HeI", "x_HeII", "n_e", "T_e"):
-        sim.set(f, neb.get(f))
+    sim.set_state({f: neb.get(f) for f in ("x_HI", "x_HeI", "x_HeII", "n_e", "T_e")})
     for f in ("gamma_HI", "gamma_HeI", "gamma_HeII", "heat_HI", "heat_HeI", "heat_HeII", "gamma_metal", "heat_metal"):
         sim.set(f, np.ascontiguousarray(neb.get(f)).ravel())
     ref = sim.thermal_cells(idx)

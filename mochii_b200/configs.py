@@ -394,3 +394,63 @@ def prepared_state(n, front=0.7, width=1.0, he=True, T_in=8.0e3, T_out=3.0e3, nH
         ne = ne + nH * yHe * out["x_HeII"]
     out["n_e"] = ne
     return out
+
+
+def hii40(workdir, nphotons=40_000_000, niter=100, precision="fp32", level=6, rin_pc=0.97223, rout_pc=4.73154):
+    """The Lexington HII40 H II region (the reference's G2 gate input,
+    tests/g2_hii/hii40.in): a hollow uniform sphere of n_H = 100 between
+    rin_pc and rout_pc on a uniform octree of the given level spanning
+    +-rout_pc, a 40 kK blackbody with Q(H) = 4.26e49 s^-1 (luminosity
+    1.353758e39 erg/s over 13.598-100 eV, 32 bins), case B, thermal balance
+    in [3e3, 3e4] K with the Lexington metals (C, N, O, Ne, S: the reference
+    defaults), metal n_e and heating off, from an ionized start; iterated to
+    gas_tol = gas_tol_te = 5e-3 (at most niter).  The reference publishes
+    <T[NpNe]> = 8169 K for this case.  Writes the leaf list into workdir and
+    returns the namelist."""
+    import numpy as np
+    from . import amr
+    os.makedirs(workdir, exist_ok=True)
+    leaves = os.path.join(workdir, f"hii40_L{level}.txt")
+    if not os.path.exists(leaves):
+        box = 2.0 * rout_pc
+
+        def dens(x, y, z, lev):
+            r = np.sqrt(x * x + y * y + z * z)
+            return np.where((r >= rin_pc) & (r < rout_pc), 100.0, 0.0)
+
+        x, y, z, lev, nH = amr.build_leaves(box, level, level, lambda *a: None, dens)
+        amr.write_leaf_list(leaves + ".part", box, x, y, z, lev, nH)
+        os.replace(leaves + ".part", leaves)
+    return f"""&parameters
+ par%no_photons = {float(nphotons):.6e}
+ par%iseed = 1234
+ par%launch_sequence = 'sobol'
+ par%grid_type = 'amr'
+ par%amr_file = '{leaves}'
+ par%dust_density_law = 'none'
+ par%distance_unit = 'pc'
+ par%nnu_ion = 32
+ par%eion_min = 13.598
+ par%eion_max = 100.0
+ par%tstar = 4.0e4
+ par%luminosity = 1.353758e39
+ par%xHI_init = 1.0e-3
+ par%xHeI_init = 0.5
+ par%xHeII_init = 0.5
+ par%He_abund = 0.1
+ par%ion_add_dust = .false.
+ par%gas_niter = {niter}
+ par%gas_tol = 5.0e-3
+ par%ion_relax = 1.0
+ par%case_ab = 'B'
+ par%solve_te = .true.
+ par%te_min = 3.0e3
+ par%te_max = 3.0e4
+ par%gas_tol_te = 5.0e-3
+ par%use_metals = .true.
+ par%metal_ne = .false.
+ par%metal_heat = .false.
+ par%atomic_dir = '{ATOMIC_DIR}'
+ par%precision = '{precision}'
+/
+"""

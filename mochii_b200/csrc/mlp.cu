@@ -5,9 +5,10 @@
 // produces; its T_e prediction seeds the bracketed thermal solve, which still
 // solves every leaf to the same tolerance.
 //
-// The GEMMs run on the tensor cores with BF16 operands (FP32 master weights
+// The GEMMs run on the 5th-generation tensor cores (tcgen05.mma with the
+// accumulator in tensor memory) with BF16 operands (FP32 master weights
 // rounded to BF16 as tiles are staged; activations and gradients likewise)
-// and FP32 accumulation: mma.sync m16n8k16 BF16 tiles, 64x64x32 block tiles.
+// and FP32 accumulation, 128 x 128 tiles.
 // Forward, backward (weight and activation gradients), the GELU derivative,
 // bias gradients and the Adam step are kernels of this file.
 #include <cuda_bf16.h>
@@ -31,21 +32,87 @@ namespace {
 constexpr int kIn = 16, kHid = 128, kOut = 4, kLayers = 4;
 constexpr int kDim[kLayers + 1] = {kIn, kHid, kHid, kHid, kOut};
 
-// ---- BF16 tensor-core GEMM ---------------------------------------------------
+// ---- BF16 tensor-core GEMM on the 5th-generation tensor cores ----------------
 // C[m, n] = sum_k A(m, k) B(k, n) with A(m, k) = A[m*am + k*ak] and
-// B(k, n) = B[k*bk + n*bn], both FP32 in memory, rounded to BF16 in shared
-// memory; FP32 accumulation.  Epilogue: EPI_STORE C = acc; EPI_BIAS C = acc +
-// bias[n]; EPI_BIAS_GELU Z = acc + bias[n] (kept), C = GELU(Z).
+// B(k, n) = B[k*bk + n*bn], both FP32 in memory, rounded to BF16 as they are
+// staged in shared memory; FP32 accumulation in tensor memory.  Epilogue:
+// EPI_STORE C = acc; EPI_BIAS C = acc + bias[n]; EPI_BIAS_GELU Z = acc +
+// bias[n] (kept), C = GELU(Z).
+//
+// One CTA (4 warps) per 128 x 128 tile of C.  The CTA allocates 128 columns
+// of tensor memory (the FP32 accumulator: lane = row of the tile, column =
+// column), then per 64-wide K chunk: every thread stages its share of the A
+// and B chunks as BF16 in the canonical K-major layout without swizzle (8x8
+// core matrices of 128 contiguous bytes, the next K core matrix 128 bytes on,
+// the next 8 rows 1024 bytes on), makes the writes visible to the tensor
+// core (fence.proxy.async), and one thread issues the chunk's four
+// tcgen05.mma (M = 128, N = 128, K = 16 each, kind::f16 with BF16 operands)
+// and commits them to an mbarrier the CTA waits on before the chunk's
+// buffers are reused.  The epilogue reads the accumulator with tcgen05.ld
+// (warp w owns rows 32w .. 32w+31).  At most four CTAs fit on an SM (their
+// shared memory), so the four 128-column allocations never exceed the SM's
+// 512 columns.  The completion wait is bounded: a wait that runs out sets
+// g_tc_timeout, skips the epilogue and still frees the tensor memory.
 enum { EPI_STORE = 0, EPI_BIAS = 1, EPI_BIAS_GELU = 2 };
-constexpr int BM = 64, BN = 64, BK = 32, PAD = 8;
+constexpr int TC_M = 128, TC_N = 128, TC_K = 64;
+constexpr uint32_t kTmemCols = 128;
+constexpr size_t kTcSmem = 56 * 1024;   // A and B chunks (32 KiB) and padding: <= 4 CTAs per SM
+// instruction descriptor of kind::f16: FP32 accumulator (bits 4-5 = 1), A and
+// B BF16 (bits 7-9 = 1, 10-12 = 1), both K-major (bits 15, 16 = 0), N >> 3 at
+// bit 17, M >> 4 at bit 24
+constexpr uint32_t kIdesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(TC_N >> 3) << 17) |
+                            ((uint32_t)(TC_M >> 4) << 24);
 
-__device__ __forceinline__ uint32_t pack2(__nv_bfloat16 lo, __nv_bfloat16 hi) {
-    return (uint32_t)__bfloat16_as_ushort(lo) | ((uint32_t)__bfloat16_as_ushort(hi) << 16);
-}
+__device__ int g_tc_timeout;   // an MMA completion wait ran out (read by the host after each call)
 
 __device__ __forceinline__ float gelu(float z) { return 0.5f * z * (1.0f + erff(z * 0.70710678118654752f)); }
 __device__ __forceinline__ float gelu_grad(float z) {
     return 0.5f * (1.0f + erff(z * 0.70710678118654752f)) + z * 0.39894228040143268f * expf(-0.5f * z * z);
+}
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+// Shared-memory matrix descriptor, K-major without swizzle: start address,
+// leading byte offset 128 (the next core matrix along K), stride byte offset
+// 1024 (the next 8 rows), all in 16-byte units; descriptor version 1 (bit 46).
+__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr) {
+    return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)(128 >> 4) << 16) | ((uint64_t)(1024 >> 4) << 32) |
+           (1ull << 46);
+}
+
+// Byte offset of element (row r, k) of a 128 x 64 BF16 chunk in that layout.
+__device__ __forceinline__ int core_off(int r, int k) {
+    return ((((r >> 3) * (TC_K / 8)) + (k >> 3)) << 7) + ((r & 7) << 4) + ((k & 7) << 1);
+}
+
+// Bounded wait for phase `parity` of the mbarrier at shared address `bar`.
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
+    for (int i = 0; i < (1 << 22); ++i) {
+        uint32_t done;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}\n"
+            : "=r"(done)
+            : "r"(bar), "r"(parity)
+            : "memory");
+        if (done) return true;
+    }
+    atomicExch(&g_tc_timeout, 1);
+    return false;
+}
+
+// Stage rows r of a 128-row operand chunk (row index q0 + r of the matrix,
+// K columns k0 .. k0+63) as BF16: element (q, k) = X[q*sq + k*sk].
+__device__ __forceinline__ void stage_chunk(unsigned char* dst, const float* __restrict__ X, long long sq, long long sk,
+                                            int q0, int nq, int k0, int K) {
+    const int tid = threadIdx.x;
+    for (int e = tid; e < TC_M * TC_K; e += 128) {
+        int r, k;
+        if (sk == 1) { r = e / TC_K; k = e % TC_K; }   // consecutive threads along the contiguous index
+        else { k = e / TC_M; r = e % TC_M; }
+        const int q = q0 + r, kk = k0 + k;
+        const float v = (q < nq && kk < K) ? X[(long long)q * sq + (long long)kk * sk] : 0.0f;
+        *reinterpret_cast<__nv_bfloat16*>(dst + core_off(r, k)) = __float2bfloat16_rn(v);
+    }
 }
 
 template <int EPI>
@@ -53,84 +120,103 @@ __global__ void __launch_bounds__(128) k_gemm(int M, int N, int K, const float* 
                                               long long ak, const float* __restrict__ B, long long bk, long long bn,
                                               float* __restrict__ C, long long ldc, const float* __restrict__ bias,
                                               float* __restrict__ Z) {
-    __shared__ __nv_bfloat16 As[BM][BK + PAD];
-    __shared__ __nv_bfloat16 Bs[BN][BK + PAD];   // [n][k]
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const int wm = (warp >> 1) * 32, wn = (warp & 1) * 32;
-    const int g = lane >> 2, t = lane & 3;
-    const int m0 = blockIdx.y * BM, n0 = blockIdx.x * BN;
-    float acc[2][4][4];
-#pragma unroll
-    for (int i = 0; i < 2; ++i)
-#pragma unroll
-        for (int j = 0; j < 4; ++j)
-#pragma unroll
-            for (int q = 0; q < 4; ++q) acc[i][j][q] = 0.0f;
-    for (int k0 = 0; k0 < K; k0 += BK) {
-        for (int e = tid; e < BM * BK; e += 128) {
-            const int r = e / BK, c = e % BK;
-            const int m = m0 + r, k = k0 + c;
-            As[r][c] = __float2bfloat16_rn(m < M && k < K ? A[(long long)m * am + (long long)k * ak] : 0.0f);
-        }
-        for (int e = tid; e < BN * BK; e += 128) {
-            const int r = e / BK, c = e % BK;
-            const int n = n0 + r, k = k0 + c;
-            Bs[r][c] = __float2bfloat16_rn(n < N && k < K ? B[(long long)k * bk + (long long)n * bn] : 0.0f);
-        }
-        __syncthreads();
-#pragma unroll
-        for (int kk = 0; kk < BK; kk += 16) {
-            uint32_t a[2][4], b[4][2];
-#pragma unroll
-            for (int i = 0; i < 2; ++i) {
-                const int r = wm + i * 16 + g, c = kk + t * 2;
-                a[i][0] = pack2(As[r][c], As[r][c + 1]);
-                a[i][1] = pack2(As[r + 8][c], As[r + 8][c + 1]);
-                a[i][2] = pack2(As[r][c + 8], As[r][c + 9]);
-                a[i][3] = pack2(As[r + 8][c + 8], As[r + 8][c + 9]);
-            }
-#pragma unroll
-            for (int j = 0; j < 4; ++j) {
-                const int n = wn + j * 8 + g, c = kk + t * 2;
-                b[j][0] = pack2(Bs[n][c], Bs[n][c + 1]);
-                b[j][1] = pack2(Bs[n][c + 8], Bs[n][c + 9]);
-            }
-#pragma unroll
-            for (int i = 0; i < 2; ++i)
-#pragma unroll
-                for (int j = 0; j < 4; ++j)
-                    asm volatile(
-                        "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, "
-                        "{%8,%9}, {%0,%1,%2,%3};\n"
-                        : "+f"(acc[i][j][0]), "+f"(acc[i][j][1]), "+f"(acc[i][j][2]), "+f"(acc[i][j][3])
-                        : "r"(a[i][0]), "r"(a[i][1]), "r"(a[i][2]), "r"(a[i][3]), "r"(b[j][0]), "r"(b[j][1]));
-        }
-        __syncthreads();
+    extern __shared__ __align__(1024) unsigned char tsm[];
+    __shared__ __align__(8) uint64_t bar;
+    __shared__ uint32_t tmem_slot;
+    unsigned char* As = tsm;
+    unsigned char* Bs = tsm + TC_M * TC_K * 2;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int m0 = blockIdx.y * TC_M, n0 = blockIdx.x * TC_N;
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_slot)),
+                     "r"(kTmemCols)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
     }
+    if (tid == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&bar)) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = tmem_slot;
+    uint32_t phase = 0;
+    bool ok = true;
+    const int nchunk = (K + TC_K - 1) / TC_K;
+    for (int kc = 0; kc < nchunk && ok; ++kc) {
+        const int k0 = kc * TC_K;
+        stage_chunk(As, A, am, ak, m0, M, k0, K);
+        stage_chunk(Bs, B, bn, bk, n0, N, k0, K);   // B(k, n) as rows n, K-major
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        __syncthreads();
+        if (tid == 0) {
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
 #pragma unroll
-    for (int i = 0; i < 2; ++i)
-#pragma unroll
-        for (int j = 0; j < 4; ++j)
-#pragma unroll
-            for (int q = 0; q < 4; ++q) {
-                const int m = m0 + wm + i * 16 + g + (q >= 2 ? 8 : 0);
-                const int n = n0 + wn + j * 8 + t * 2 + (q & 1);
-                if (m >= M || n >= N) continue;
-                float v = acc[i][j][q];
-                if (EPI != EPI_STORE) v = v + bias[n];
-                if (EPI == EPI_BIAS_GELU) {
-                    Z[(long long)m * ldc + n] = v;
-                    v = gelu(v);
-                }
-                C[(long long)m * ldc + n] = v;
+            for (int j = 0; j < TC_K / 16; ++j) {
+                const uint64_t da = umma_desc(smem_u32(As) + j * 256), db = umma_desc(smem_u32(Bs) + j * 256);
+                const uint32_t accumulate = (kc > 0 || j > 0) ? 1u : 0u;
+                const uint32_t zero = 0u;
+                asm volatile(
+                    "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+                    "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(tmem),
+                    "l"(da), "l"(db), "r"(kIdesc), "r"(accumulate), "r"(zero), "r"(zero), "r"(zero), "r"(zero)
+                    : "memory");
             }
+            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                             smem_u32(&bar))
+                         : "memory");
+        }
+        ok = mbar_wait(smem_u32(&bar), phase);   // the chunk's MMAs are done with As and Bs
+        phase ^= 1u;
+        ok = __syncthreads_and(ok) != 0;
+    }
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    if (ok) {
+        const int row = m0 + warp * 32 + lane;
+#pragma unroll 1
+        for (int c0 = 0; c0 < TC_N; c0 += 32) {
+            if (n0 + c0 >= N) break;   // uniform over the CTA
+            uint32_t r[32];
+            const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0;
+            asm volatile("tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+                         : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+                         : "r"(taddr));
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+            if (row < M) {
+#pragma unroll
+                for (int j = 0; j < 32; ++j) {
+                    const int n = n0 + c0 + j;
+                    if (n >= N) break;
+                    float v = __uint_as_float(r[j]);
+                    if (EPI != EPI_STORE) v = v + bias[n];
+                    if (EPI == EPI_BIAS_GELU) {
+                        Z[(long long)row * ldc + n] = v;
+                        v = gelu(v);
+                    }
+                    C[(long long)row * ldc + n] = v;
+                }
+            }
+        }
+    } else if (tid == 0) {   // a wait ran out: give the tensor core one more bounded wait before the free
+        mbar_wait(smem_u32(&bar), phase ^ 1u);
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols) : "memory");
 }
 
 template <int EPI>
 void gemm(cudaStream_t s, int M, int N, int K, const float* A, long long am, long long ak, const float* B, long long bk,
           long long bn, float* C, long long ldc, const float* bias = nullptr, float* Z = nullptr) {
-    dim3 grid((N + BN - 1) / BN, (M + BM - 1) / BM);
-    k_gemm<EPI><<<grid, 128, 0, s>>>(M, N, K, A, am, ak, B, bk, bn, C, ldc, bias, Z);
+    static bool attr = false;
+    if (!attr) {
+        cudaFuncSetAttribute(k_gemm<EPI>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTcSmem);
+        attr = true;
+    }
+    dim3 grid((N + TC_N - 1) / TC_N, (M + TC_M - 1) / TC_M);
+    k_gemm<EPI><<<grid, 128, kTcSmem, s>>>(M, N, K, A, am, ak, B, bk, bn, C, ldc, bias, Z);
 }
 
 // ---- elementwise kernels ------------------------------------------------------
@@ -306,6 +392,18 @@ namespace {
 int mlp_fail(mochii_mlp* m, int code, const std::string& msg) {
     if (m) m->err = msg;
     return code;
+}
+
+// After a synchronised call: did a tensor-core completion wait run out?
+int tc_check(mochii_mlp* m) {
+    int v = 0;
+    if (cudaMemcpyFromSymbol(&v, g_tc_timeout, sizeof(int)) != cudaSuccess) return mlp_fail(m, MOCHII_ERR_CUDA, "g_tc_timeout");
+    if (v) {
+        const int zero = 0;
+        cudaMemcpyToSymbol(g_tc_timeout, &zero, sizeof(int));
+        return mlp_fail(m, MOCHII_ERR_TIMEOUT, "a tensor-core MMA completion wait ran out");
+    }
+    return MOCHII_OK;
 }
 
 #define MK(call)                                                                                   \
@@ -496,6 +594,7 @@ extern "C" int mochii_mlp_gradients(mochii_mlp* m, const float* X, const float* 
     MK(cudaFreeAsync(dy, m->stream));
     MK(cudaStreamSynchronize(m->stream));
     if (loss) *loss = lh / (float)n;
+    if (int rc_tc = tc_check(m)) return rc_tc;
     return MOCHII_OK;
 }
 
@@ -566,6 +665,7 @@ extern "C" int mochii_mlp_train(mochii_mlp* m, const float* X, const float* Y, i
     MK(cudaFreeAsync(ybatch, m->stream));
     MK(cudaFreeAsync(dperm, m->stream));
     MK(cudaStreamSynchronize(m->stream));
+    if (int rc_tc = tc_check(m)) return rc_tc;
     return MOCHII_OK;
 }
 
@@ -587,6 +687,7 @@ extern "C" int mochii_mlp_predict(mochii_mlp* m, const float* X, int64_t n, doub
     MK(cudaFreeAsync(d, m->stream));
     MK(cudaStreamSynchronize(m->stream));
     MK(cudaGetLastError());
+    if (int rc_tc = tc_check(m)) return rc_tc;
     return MOCHII_OK;
 }
 
@@ -635,5 +736,6 @@ extern "C" int mochii_mlp_warm_start(mochii_ctx* c, mochii_mlp* m) {
     const double band = m->t_rms_ln > 0.0 ? 2.5 * m->t_rms_ln : std::log(1.05);
     c->twarm_fac = std::exp(std::min(std::max(band, std::log(1.002)), std::log(1.05)));
     c->twarm_gate = 1.0e-6;
+    if (int rc_tc = tc_check(m)) return rc_tc;
     return MOCHII_OK;
 }

@@ -399,9 +399,16 @@ long long orc_sim_set(void* h, const char* name, const double* in, long long n) 
     }
     if (!v || (long long)v->size() != n) return -1;
     std::memcpy(v->data(), in, (size_t)n * sizeof(double));
-    if (nm.rfind("gamma_", 0) != 0 && nm.rfind("heat_", 0) != 0)
+    if (nm.rfind("gamma_", 0) != 0 && nm.rfind("heat_", 0) != 0 && !s->defer_fill)
         s->opacity_fill();   // the stage cache follows the state it is read from
     return n;
+}
+// Several state fields at once: orc_sim_defer_fill(h, 1), the sets, then
+// orc_sim_defer_fill(h, 0) refreshes the opacities once.
+void orc_sim_defer_fill(void* h, int on) {
+    auto* s = static_cast<Sim*>(h);
+    s->defer_fill = on != 0;
+    if (!on) s->opacity_fill();
 }
 // The thermal bisection (thermal_cell, thermal_mod.f90:159-188) of the given
 // leaves from the current state and rates, state unchanged: out5[k*5 + .] =

@@ -256,6 +256,7 @@ struct Sim {
     std::vector<double> dif_ch, dif_cdf;   // (4, nleaf), (nleaf)
     double diffuse_lum = 0.0;
     int64_t diffuse_nphot = 0;
+    bool defer_fill = false;   // orc_sim_set leaves the opacity refresh to the caller
     void diffuse_build(double lpacket);                          // diffuse_mod.f90:60-121
     void gen_diffuse_qmc(int64_t ip, Photon& ph) const;          // diffuse_mod.f90:221-296
     bool setup(const std::string& namelist, std::string* err);

@@ -83,6 +83,7 @@ def load():
         "orc_milne_sample": (D, [V, I, D, D]),
         "orc_sim_thermal_cells": (LL, [V, V, LL, V]),
         "orc_sim_diffuse_count": (LL, [V]),
+        "orc_sim_defer_fill": (None, [V, I]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)
@@ -342,6 +343,15 @@ class Sim:
         heat_*, and with metals gamma_metal / heat_metal, leaf-major)."""
         a = np.ascontiguousarray(values, dtype=float)
         assert load().orc_sim_set(self.h, name.encode(), a.ctypes.data, a.size) == a.size, name
+
+    def set_state(self, fields):
+        """Several fields (dict name -> values) with one opacity refresh."""
+        load().orc_sim_defer_fill(self.h, 1)
+        try:
+            for k, v in fields.items():
+                self.set(k, v)
+        finally:
+            load().orc_sim_defer_fill(self.h, 0)
 
     def diffuse_build(self):
         n = C.c_longlong()

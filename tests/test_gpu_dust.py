@@ -138,10 +138,16 @@ def test_clumpy_dusty_case_matches_oracle(orc, tmp_path):
         big = o > 1e-3 * o.max()
         assert np.median(np.abs(g[big] / o[big] - 1)) < 1e-6, f
         assert abs(g.sum() / o.sum() - 1) < 1e-4, f
+    # the thermal update on every leaf: the device state and rates before it
+    # go to the oracle, whose bisection must agree with the device solve
+    sim.set_state({f: neb.get(f) for f in ("x_HI", "x_HeI", "x_HeII", "n_e", "T_e")})
+    for f in ("gamma_HI", "gamma_HeI", "gamma_HeII", "heat_HI", "heat_HeI", "heat_HeII"):
+        sim.set(f, neb.get(f))
+    ref = sim.thermal_cells(np.arange(neb.nleaf))
     neb.gas_thermal_update()
-    sim.thermal_update()
-    dT = np.abs(neb.get("T_e") - sim.get("T_e"))
-    assert np.median(dT) < 1.0 and np.mean(dT > 20.0) < 0.01
-    dx = np.abs(neb.get("x_HI") - sim.get("x_HI"))
-    assert np.mean(dx > 1e-3) < 0.01
+    gas = neb.get("nH") > 0
+    dT = np.abs(neb.get("T_e") - ref[:, 0])[gas]
+    dx = np.abs(neb.get("x_HI") - ref[:, 1])[gas]
+    assert dT.max() < 20.0, dT.max()
+    assert dx.max() < 1e-3, dx.max()
     neb.close()
