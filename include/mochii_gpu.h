@@ -46,6 +46,7 @@ enum {
 };
 
 #define MOCHII_MAX_SRC 16   /* define.f90:74 MAX_SRC */
+#define MOCHII_MAX_OBS 16   /* observers of the peel-off images (define.f90:76 allows 181) */
 #define MOCHII_STRLEN 256
 
 /* Device arithmetic for the transport pass. */
@@ -167,6 +168,17 @@ typedef struct mochii_params {
      * 0 'launch' = the launch (Sobol) order; 1 'direction' = sorted by source
      * and direction cell after the launch, per-lane reductions */
     int packet_order;
+    /* peel-off imaging (par%ion_peel; ion_peel_mod.f90, define.f90:518-544,
+     * 658-664): observers by angle lists (alpha, beta, gamma [deg]; or the
+     * phase, inclination and position angles) or by position (obsx/y/z,
+     * code units), all NaN when unset as in the reference; at most
+     * MOCHII_MAX_OBS observers here.  distance, dxim, dyim NaN: derived. */
+    int ion_peel, peel_bins, save_direc0;
+    int nxim, nyim;
+    double distance, dxim, dyim;
+    double alpha[MOCHII_MAX_OBS], beta[MOCHII_MAX_OBS], gamma[MOCHII_MAX_OBS];
+    double obsx[MOCHII_MAX_OBS], obsy[MOCHII_MAX_OBS], obsz[MOCHII_MAX_OBS];
+    double phase_angle[MOCHII_MAX_OBS], inclination_angle[MOCHII_MAX_OBS], position_angle[MOCHII_MAX_OBS];
 } mochii_params;
 
 /* Per-pass statistics (ion_score_report_energy_closure, ion_score_mod.f90:364-387). */
@@ -232,11 +244,34 @@ const char* mochii_last_error(const mochii_ctx* ctx);
 /* ---- the replaced entry points ------------------------------------------------- */
 /* ionizing_field_and_rates (ionizing_field_mod.f90:72-170): one transport
  * pass of every stellar packet through the current opacity, the energy
- * ledger, and the rate normalisation (gas_rates_compute).  with_peel must
- * be 0 (observer imaging is outside this library). */
+ * ledger, and the rate normalisation (gas_rates_compute).  with_peel = 1 is
+ * the imaging pass (below; needs par%ion_peel). */
 int mochii_transport_pass(mochii_ctx* ctx, int with_peel, mochii_pass_stats* stats);
 /* gas_equilibrium_update (solve_te = 0) or gas_thermal_update (solve_te = 1). */
 int mochii_balance_update(mochii_ctx* ctx, int solve_te, mochii_metrics* m);
+/* The imaging pass (main.f90:234-235, ionizing_field_and_rates with
+ * with_peel): mochii_transport_pass(ctx, 1, st) needs par%ion_peel at
+ * mochii_init; it is a full pass that also peels every stellar and diffuse
+ * packet toward each observer at emission (ion_peel_direct,
+ * ion_peel_mod.f90:225-277) and, with dust scattering, at every interaction
+ * (ion_peel_scatter, :284-344), the optical depth to the box edge by the
+ * tau-only walks (raytrace_amr.f90:678-775).  The images (nobs, nchan,
+ * nyim, nxim; channels ionizing/FUV, or one per band bin with peel_bins)
+ * hold erg/s per code length^2 per pixel: which = 0 direct, 1 scattered,
+ * 2 unattenuated direct (save_direc0). */
+int mochii_image_shape(const mochii_ctx* ctx, int* shape4);
+int mochii_get_image(mochii_ctx* ctx, int which, double* out, int64_t n);
+/* Observer k as ion_peel_setup derived it: x, y, z (code units), alpha,
+ * beta, gamma [deg], distance, dxim, dyim [deg], then the grid -> observer
+ * rotation matrix row by row (18 doubles). */
+int mochii_image_observer(const mochii_ctx* ctx, int k, double* out18);
+/* ion_peel_write (ion_peel_mod.f90:359-523): surface brightness images
+ * [erg/s/cm^2/sr] as <base>_image/ with one .npy per block (direct_ion,
+ * scatt_ion, direct_fuv ..., direc0_*, suffix _obs<k> with several
+ * observers; with peel_bins the cubes and E_bin, dE_bin, wl_bin) and
+ * header.json (DXIM, DIST, ALPHA, BETA, GAMMA per block). */
+int mochii_write_image(mochii_ctx* ctx, const char* base);
+
 /* gas_opacity_fill: refresh the per-leaf absorber columns the transport reads. */
 int mochii_opacity_fill(mochii_ctx* ctx);
 

@@ -11,6 +11,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libmochii_gpu.so")
 
 MAX_SRC = 16
+MAX_OBS = 16
 STRLEN = 256
 
 OK = 0
@@ -56,6 +57,12 @@ class Params(C.Structure):
         ("lambda_ref", C.c_double), ("taumax", C.c_double), ("tauhomo", C.c_double),
         ("solver_warp", C.c_int), ("tally64", C.c_int), ("metal_rate_table", C.c_int),
         ("packet_chunk", C.c_int64), ("packet_order", C.c_int),
+        ("ion_peel", C.c_int), ("peel_bins", C.c_int), ("save_direc0", C.c_int), ("nxim", C.c_int),
+        ("nyim", C.c_int), ("distance", C.c_double), ("dxim", C.c_double), ("dyim", C.c_double),
+        ("alpha", C.c_double * MAX_OBS), ("beta", C.c_double * MAX_OBS), ("gamma", C.c_double * MAX_OBS),
+        ("obsx", C.c_double * MAX_OBS), ("obsy", C.c_double * MAX_OBS), ("obsz", C.c_double * MAX_OBS),
+        ("phase_angle", C.c_double * MAX_OBS), ("inclination_angle", C.c_double * MAX_OBS),
+        ("position_angle", C.c_double * MAX_OBS),
     ]
 
 
@@ -115,6 +122,10 @@ SIGNATURES = {
     "mochii_nnu_band": (C.c_int, [C.c_void_p]),
     "mochii_get_field": (C.c_int, [C.c_void_p, C.c_char_p, C.c_void_p, C.c_int64]),
     "mochii_write_rates": (C.c_int, [C.c_void_p, C.c_char_p, _P(RunInfo)]),
+    "mochii_image_shape": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "mochii_get_image": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_int64]),
+    "mochii_image_observer": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p]),
+    "mochii_write_image": (C.c_int, [C.c_void_p, C.c_char_p]),
     "mochii_set_field": (C.c_int, [C.c_void_p, C.c_char_p, C.c_void_p, C.c_int64]),
     "mochii_set_nphotons": (C.c_int, [C.c_void_p, C.c_int64]),
     "mochii_ion_Ltot": (C.c_double, [C.c_void_p]),

@@ -77,10 +77,9 @@ cudaError_t alloc_records(mochii_ctx* c, long long cap) {
     const size_t nsig = c->xscore ? 4 : 3, ncoef = c->xscore ? 8 : 6;   // + grain / FUV rows
     if ((e = cudaMalloc(&c->rec.sig, nsig * (size_t)cap * rsz + 64)) != cudaSuccess) return e;
     if ((e = cudaMalloc(&c->rec.coef, ncoef * (size_t)cap * rsz + 64)) != cudaSuccess) return e;
-    if (c->scatter) {
-        if ((e = cudaMalloc(&c->rec.dsc, 2 * (size_t)cap * rsz + 64)) != cudaSuccess) return e;
-        if (c->oct.ncells == 0 && (e = dalloc(&c->rec.p0, 6 * (size_t)cap)) != cudaSuccess) return e;
-    }
+    if (c->scatter && (e = cudaMalloc(&c->rec.dsc, 2 * (size_t)cap * rsz + 64)) != cudaSuccess) return e;
+    if ((c->scatter || c->par.ion_peel) && c->oct.ncells == 0 && (e = dalloc(&c->rec.p0, 6 * (size_t)cap)) != cudaSuccess)
+        return e;
     if (c->metal.ntr > 0) {
         if ((e = dalloc(&c->rec.E, (size_t)cap)) != cudaSuccess) return e;
         if ((e = cudaMalloc(&c->rec.msig, (size_t)c->metal.ntrp * cap * rsz + 64)) != cudaSuccess) return e;
@@ -103,7 +102,7 @@ void release(mochii_ctx* c) {
                     (void*)c->rec.E, c->rec.msig, c->oct_blob, c->rec.dsc, (void*)c->rec.p0,
                     (void*)c->dust_blob, (void*)c->rhokap, (void*)c->ttab, (void*)c->metal_lnl,
                     (void*)c->th.lnL, (void*)c->rec.key, (void*)c->rec.key_sorted, (void*)c->rec.seq,
-                    (void*)c->rec.perm, c->rec.sort_tmp};
+                    (void*)c->rec.perm, c->rec.sort_tmp, c->peel_blob};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     for (cudaEvent_t e : {c->ev0, c->ev1, c->evA, c->evB})
@@ -463,6 +462,7 @@ extern "C" int mochii_init(const mochii_params* pin, mochii_ctx** out) {
     CKI(dalloc(&c->tw.counters, 4));
     // packet records: launch chunks of up to 4 Mi packets
     CKI(alloc_records(c, std::min<long long>(p.nphotons, std::max<long long>(p.packet_chunk, 1024))));
+    CKI(peel_setup(c));   // ion_peel_setup: observers and image plane (par%ion_peel)
     c->bw.blocks = balance_blocks(c);
     if (p.diffuse_field) {
         MilneHost mh;
@@ -810,7 +810,14 @@ extern "C" int mochii_set_nphotons(mochii_ctx* c, int64_t np) {
 // ionizing_field_and_rates, ionizing_field_mod.f90:72-170.
 extern "C" int mochii_transport_pass(mochii_ctx* c, int with_peel, mochii_pass_stats* st) {
     if (!c) return MOCHII_ERR_BAD_PARAM;
-    if (with_peel) return fail(c, MOCHII_ERR_UNSUPPORTED, "observer peel-off is not built (with_peel must be 0)");
+    if (with_peel && !c->par.ion_peel)
+        return fail(c, MOCHII_ERR_BAD_PARAM, "with_peel needs par%ion_peel = .true. at mochii_init (the observers)");
+    if (with_peel) CK(c, peel_clear(c));
+    c->peeling = with_peel != 0;   // the walk kernels peel every packet toward the observers
+    struct PeelEnd {
+        mochii_ctx* c;
+        ~PeelEnd() { c->peeling = false; }
+    } peel_end{c};
     const long long n = c->grid.nleaf;
     const size_t tsz = 8;
     if (!c->columns_fresh) {

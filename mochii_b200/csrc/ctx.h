@@ -49,6 +49,18 @@ struct TransportWork {
     int ledger_blocks = 0;
 };
 
+// Peel-off imaging (par%ion_peel; ion_peel_mod.f90): the observers on the
+// device and the images the imaging pass accumulates.
+struct PeelDev {
+    int nobs = 0, nchan = 1, nxim = 0, nyim = 0, direc0 = 0;
+    const double* obs = nullptr;     // kPeelObs doubles per observer (see peel.cpp)
+    const int* chan = nullptr;       // image channel of each band bin
+    double* img_dir = nullptr;       // (nobs, nchan, nyim, nxim): erg/s per code length^2
+    double* img_sca = nullptr;
+    double* img_dir0 = nullptr;      // save_direc0 only
+};
+constexpr int kPeelObs = 18;         // x, y, z, alpha, beta, gamma, distance, dxim, dyim, R (row-major)
+
 // Per-packet launch records of one chunk (see transport.cu).
 struct RecordBuffers {
     double* tm = nullptr;
@@ -148,5 +160,10 @@ struct mochii_ctx {
     // autotune, the T_warm buffer); a batch refuses to replay after a change
     uint64_t generation = 0;
     mochii_pass_stats last_pass = {};   // statistics of the last transport pass (the rates file's ledger)
+    mochii::PeelDev peel;                 // par%ion_peel: observers and images
+    std::vector<double> peel_obs;         // host copy of the observers (kPeelObs each)
+    void* peel_blob = nullptr;            // the allocation behind peel's pointers
+    bool peel_done = false;               // an imaging pass has filled the images
+    bool peeling = false;                 // the pass in progress peels (mochii_transport_pass with_peel)
     std::string last_error;
 };

@@ -12,6 +12,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <fstream>
+#include <limits>
 #include <sstream>
 #include <string>
 #include <vector>
@@ -25,19 +26,19 @@ namespace {
 
 // params_type components outside this path (define.f90:189-861).
 const char* const kOtherKeys[] = {
-    "albedo", "allsky", "allsky_nside", "allsky_x", "allsky_y", "allsky_z", "alpha", "amr_type",
-    "base_name", "beta", "centering", "cone_opening", "density_file", "density_powerlaw_index",
-    "density_rscale", "density_zprofile", "density_zscale", "distance",
+    "albedo", "allsky", "allsky_nside", "allsky_x", "allsky_y", "allsky_z", "amr_type",
+    "base_name", "centering", "cone_opening", "density_file", "density_powerlaw_index",
+    "density_rscale", "density_zprofile", "density_zscale",
     "dust_emis_bands", "dust_emis_transport", "dust_emission_method", "dust_fast_table", "dust_model",
-    "dust_niter", "dust_no_photons", "dust_nu", "dust_sed", "dust_single_teq", "dust_tol", "dxim", "dyim",
+    "dust_niter", "dust_no_photons", "dust_nu", "dust_sed", "dust_single_teq", "dust_tol",
     "emis_output", "exetime", "ext_geometry", "ext_intensity", "ext_scale", "ext_spectrum", "ext_tstar",
-    "f_ion_dust", "f_ion_pah", "f_pah", "file_format", "gamma", "geometry", "h_coll_effects",
-    "hei_diffuse", "hei_metastable", "hgg", "inclination_angle", "ion_peel", "ion_spectrum", "kext_file",
+    "f_ion_dust", "f_ion_pah", "f_pah", "file_format", "geometry", "h_coll_effects",
+    "hei_diffuse", "hei_metastable", "hgg", "ion_spectrum", "kext_file",
     "lambda0", "lambda_max", "lambda_min", "line_case", "mrw_gamma", "nlambda", "no_print",
-    "nobs", "nprint", "nr", "nscatt_tot", "num_send_at_once", "nxim", "nyim", "obsx", "obsy", "obsz",
-    "out_bitpix", "out_bitpix_force", "out_file", "output_normalization", "pe_scale", "peel_bins",
-    "phase_angle", "position_angle", "radiation_angular_pdf_file", "reduce_factor", "refine_dx",
-    "refine_eps", "refine_front", "refine_iter", "refine_lbase", "refine_lmax", "save_direc0", "save_jlam",
+    "nobs", "nprint", "nr", "nscatt_tot", "num_send_at_once",
+    "out_bitpix", "out_bitpix_force", "out_file", "output_normalization", "pe_scale",
+    "radiation_angular_pdf_file", "reduce_factor", "refine_dx",
+    "refine_eps", "refine_front", "refine_iter", "refine_lbase", "refine_lmax", "save_jlam",
     "scatt_mat_file", "sed_data_dir", "sed_dl07_sdindex", "sed_dl07_uisrf", "sed_kext", "sed_nt",
     "sed_pah_live", "sed_thi", "sed_tlo", "sightline_tau", "slab_bot_mode", "slab_bot_phi",
     "slab_bot_source", "slab_bot_theta", "slab_faces", "slab_nmu", "slab_top_mode", "slab_top_phi",
@@ -142,6 +143,15 @@ extern "C" int mochii_params_default(mochii_params* p) {
     p->metal_rate_table = 1;
     p->packet_chunk = 1 << 22;
     p->packet_order = 2;   // 'coherent' (the launch order where it does not apply)
+    p->ion_peel = 0; p->peel_bins = 0; p->save_direc0 = 0;
+    p->nxim = 129; p->nyim = 129;   // define.f90:531-532
+    const double nan = std::numeric_limits<double>::quiet_NaN();
+    p->distance = nan; p->dxim = nan; p->dyim = nan;
+    for (int i = 0; i < MOCHII_MAX_OBS; ++i) {
+        p->alpha[i] = p->beta[i] = p->gamma[i] = nan;
+        p->obsx[i] = p->obsy[i] = p->obsz[i] = nan;
+        p->phase_angle[i] = p->inclination_angle[i] = p->position_angle[i] = nan;
+    }
     return MOCHII_OK;
 }
 
@@ -210,6 +220,24 @@ int set_key(mochii_params* p, std::string key, const std::vector<std::string>& v
     }
     REAL("xs_point", xs_point) REAL("ys_point", ys_point) REAL("zs_point", zs_point)
     INT("nsource", nsource)
+    if (key == "alpha" || key == "beta" || key == "gamma" || key == "obsx" || key == "obsy" || key == "obsz" ||
+        key == "phase_angle" || key == "inclination_angle" || key == "position_angle") {
+        double* arr = key == "alpha" ? p->alpha : key == "beta" ? p->beta : key == "gamma" ? p->gamma
+                    : key == "obsx" ? p->obsx : key == "obsy" ? p->obsy : key == "obsz" ? p->obsz
+                    : key == "phase_angle" ? p->phase_angle : key == "inclination_angle" ? p->inclination_angle
+                                                                                       : p->position_angle;
+        for (size_t k = 0; k < vals.size(); ++k) {
+            const int slot = index - 1 + (int)k;
+            if (slot < 0 || slot >= MOCHII_MAX_OBS) return bad("observer index outside 1..16");
+            if (vals[k].empty()) continue;
+            if (!parse_real(vals[k], &d)) return bad("not a real");
+            arr[slot] = d;
+        }
+        return 0;
+    }
+    BOOL("ion_peel", ion_peel) BOOL("peel_bins", peel_bins) BOOL("save_direc0", save_direc0)
+    INT("nxim", nxim) INT("nyim", nyim) REAL("distance", distance) REAL("dxim", dxim) REAL("dyim", dyim)
+    if (key == "nobs") return 0;   // derived from the observer lists (ion_peel_setup)
     if (key == "src_tstar" || key == "src_lum" || key == "src_x" || key == "src_y" || key == "src_z") {
         double* arr = key == "src_tstar" ? p->src_tstar : key == "src_lum" ? p->src_lum
                     : key == "src_x" ? p->src_x : key == "src_y" ? p->src_y : p->src_z;

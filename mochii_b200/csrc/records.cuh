@@ -100,13 +100,6 @@ __device__ __forceinline__ void write_grain_record(const PacketRecords& rec, lon
         R* ds = static_cast<R*>(rec.dsc);
         ds[i] = (R)o.ssca;
         ds[c + i] = (R)o.g;
-        if (car) {
-#pragma unroll
-            for (int k = 0; k < 3; ++k) {
-                rec.p0[k * c + i] = pos[k];
-                rec.p0[(3 + k) * c + i] = kk[k];
-            }
-        }
     }
 }
 
@@ -155,6 +148,13 @@ __device__ __forceinline__ void write_record(const PacketRecords& rec, long long
     }
     rec.cell[i] = idx[0] | (idx[1] << 10) | (idx[2] << 20);
     rec.bits[i] = bits;
+    if (rec.p0) {   // start point and direction: scattered flights and peel-off
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            rec.p0[k * c + i] = pos[k];
+            rec.p0[(3 + k) * c + i] = kk[k];
+        }
+    }
 }
 
 }  // namespace mochii

@@ -62,6 +62,8 @@ struct PassArgs {
     OctDev oct;          // octree grid; oct.ncells == 0 on the Cartesian grid
     DustDev dust;        // grain optics (ion_add_dust); dust.n == 0 without
     const double* rhokap;   // grey dust opacity per leaf (scattered flights' albedo)
+    PeelDev peel;        // peel-off observers and images
+    int peeling;         // this pass is the imaging pass (with_peel)
     int xs;              // dust or FUV path estimators (8 tallies per leaf)
     int scatter;         // ion_dust_scatter
     double eion_min;
@@ -634,17 +636,140 @@ __device__ __forceinline__ bool walk_to_tau(const PassArgs& a, double tau_in, bo
     }
 }
 
+// ---- peel-off imaging (ion_peel_mod.f90) ---------------------------------------
+// Optical depth from (x, y, z) along (kx, ky, kz) to the box edge at the
+// packet's energy, no tally (raytrace_ion_tau_only_car / _amr,
+// raytrace_amr.f90:678-775): the DDA from the point on the Cartesian grid,
+// leaf exits on the octree (starting in leaf il when known); stops at
+// tau_huge.  FP64 geometry as the edge walk.
+template <bool AMR, typename KapF>
+__device__ double tau_to_edge(const PassArgs& a, double x, double y, double z, double kx, double ky, double kz, int il,
+                              KapF& kappa_at) {
+    double tau = 0.0;
+    if constexpr (AMR) {
+        if (il < 0) il = oct_find_leaf(a.oct, x, y, z);
+        if (il < 0) return 0.0;
+        for (int nstep = 1; nstep <= kMaxWalkSteps; ++nstep) {
+            int face;
+            const double texit = oct_cell_exit(ld_geo(a.oct.lgeo + il), x, y, z, kx, ky, kz, &face);
+            tau = tau + (double)kappa_at(il) * texit;
+            if (tau >= kTauHuge) break;
+            x = x + texit * kx;
+            y = y + texit * ky;
+            z = z + texit * kz;
+            const int nl = oct_next_leaf(a.oct, il, face, x, y, z);
+            if (nl < 0) break;
+            il = nl;
+        }
+    } else {
+        const double pos[3] = {x, y, z}, kk[3] = {kx, ky, kz};
+        int idx[3], stp[3];
+        double tmax[3], tdel[3];
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            idx[k] = min(max((int)((pos[k] - a.org[k]) / a.dcell), 0), a.n[k] - 1);
+            if (kk[k] > 0.0) {
+                stp[k] = 1; tmax[k] = (a.org[k] + (double)(idx[k] + 1) * a.dcell - pos[k]) / kk[k]; tdel[k] = a.dcell / kk[k];
+            } else if (kk[k] < 0.0) {
+                stp[k] = -1; tmax[k] = (a.org[k] + (double)idx[k] * a.dcell - pos[k]) / kk[k]; tdel[k] = -a.dcell / kk[k];
+            } else {
+                stp[k] = 0; tmax[k] = kHugest; tdel[k] = kHugest;
+            }
+        }
+        double t_cur = 0.0;
+        for (int nstep = 1; nstep <= kMaxWalkSteps; ++nstep) {
+            const int c = idx[0] + a.n[0] * (idx[1] + a.n[1] * idx[2]);
+            int ax = 0;
+            if (tmax[1] < tmax[ax]) ax = 1;
+            if (tmax[2] < tmax[ax]) ax = 2;
+            tau = tau + (double)kappa_at(c) * (tmax[ax] - t_cur);
+            if (tau >= kTauHuge) break;
+            t_cur = tmax[ax];
+            tmax[ax] = tmax[ax] + tdel[ax];
+            idx[ax] += stp[ax];
+            if (idx[ax] < 0 || idx[ax] >= a.n[ax]) break;
+        }
+    }
+    return tau;
+}
+
+// The observer-frame pixel of direction (kx, ky, kz) for observer o (the
+// TAN image plane of ion_peel_direct, 0-based); false outside the image.
+__device__ __forceinline__ bool peel_pixel(const PeelDev& p, const double* o, double kx, double ky, double kz, int* ix,
+                                           int* iy) {
+    const double v0 = o[9] * kx + o[10] * ky + o[11] * kz;
+    const double v1 = o[12] * kx + o[13] * ky + o[14] * kz;
+    const double v2 = o[15] * kx + o[16] * ky + o[17] * kz;
+    constexpr double r2d = 180.0 / kPi;
+    *ix = (int)floor(atan2(-v0, v2) * r2d / o[7] + p.nxim / 2.0);
+    *iy = (int)floor(atan2(-v1, v2) * r2d / o[8] + p.nyim / 2.0);
+    return *ix >= 0 && *ix < p.nxim && *iy >= 0 && *iy < p.nyim;
+}
+
+// ion_peel_direct (ion_peel_mod.f90:225-277): the isotropic source's
+// wl / (4 pi r^2) e^-tau (wl = packet luminosity x weight) toward every
+// observer's pixel, the unattenuated part to the direc0 image.
+template <bool AMR, typename KapF>
+__device__ void peel_direct(const PassArgs& a, double x, double y, double z, int il, int inu, double wl,
+                            KapF& kappa_at) {
+    const PeelDev& p = a.peel;
+    const int ch = __ldg(p.chan + inu);
+    for (int k = 0; k < p.nobs; ++k) {
+        const double* o = p.obs + k * kPeelObs;
+        double kx = __ldg(o) - x, ky = __ldg(o + 1) - y, kz = __ldg(o + 2) - z;
+        const double r2 = kx * kx + ky * ky + kz * kz, r = sqrt(r2);
+        kx = kx / r; ky = ky / r; kz = kz / r;
+        int ix, iy;
+        if (!peel_pixel(p, o, kx, ky, kz, &ix, &iy)) continue;
+        const long long pix = ((long long)(k * p.nchan + ch) * p.nyim + iy) * p.nxim + ix;
+        const double contrib = wl / (4.0 * kPi * r2);
+        if (p.direc0) atomicAdd(p.img_dir0 + pix, contrib);
+        const double tau = tau_to_edge<AMR>(a, x, y, z, kx, ky, kz, il, kappa_at);
+        if (tau > 500.0) continue;
+        atomicAdd(p.img_dir + pix, contrib * exp(-tau));
+    }
+}
+
+// ion_peel_scatter (ion_peel_mod.f90:284-344): at a dust interaction (after
+// the albedo weight, before the new direction; (kx, ky, kz) the incident
+// direction) the Henyey-Greenstein phase function toward each observer.
+template <bool AMR, typename KapF>
+__device__ void peel_scatter(const PassArgs& a, double x, double y, double z, int il, double kx, double ky, double kz,
+                             double wl, double g, int inu, KapF& kappa_at) {
+    const PeelDev& p = a.peel;
+    const int ch = __ldg(p.chan + inu);
+    const double gg = fmin(fmax(g, -0.9999), 0.9999);
+    const double kn2 = kx * kx + ky * ky + kz * kz;
+    for (int k = 0; k < p.nobs; ++k) {
+        const double* o = p.obs + k * kPeelObs;
+        double ox = __ldg(o) - x, oy = __ldg(o + 1) - y, oz = __ldg(o + 2) - z;
+        const double r2 = ox * ox + oy * oy + oz * oz, r = sqrt(r2);
+        ox = ox / r; oy = oy / r; oz = oz / r;
+        int ix, iy;
+        if (!peel_pixel(p, o, ox, oy, oz, &ix, &iy)) continue;
+        const double tau = tau_to_edge<AMR>(a, x, y, z, ox, oy, oz, il, kappa_at);
+        if (tau > 500.0 || kn2 <= 0.0) continue;
+        const double cosa = fmin(fmax((kx * ox + ky * oy + kz * oz) / sqrt(kn2), -1.0), 1.0);
+        const double dmin = (1.0 - fabs(gg)) * (1.0 - fabs(gg));
+        const double den = fmax((1.0 + gg * gg) - 2.0 * gg * cosa, dmin);
+        const double phase = (1.0 - gg * gg) / (den * sqrt(den) * 4.0 * kPi);
+        const double contrib = wl * phase / r2 * exp(-tau);
+        if (!isfinite(contrib)) continue;
+        atomicAdd(p.img_sca + ((long long)(k * p.nchan + ch) * p.nyim + iy) * p.nxim + ix, contrib);
+    }
+}
+
 // The forced first interaction and the scattered flights of one packet
 // (transport_ion_packet after its edge walk): weight 1 - e^-tau_edge, the
 // albedo weight rhokap s_sca / kappa at each interaction, Russian roulette
 // below 1e-4 (survival 0.1), a Henyey-Greenstein direction about the
 // current one, an unforced flight to -ln(u).  Draws come from the packet's
 // Philox stream in the reference's order.
-template <bool AMR, typename KapF, typename ScoreF>
+template <bool AMR, typename KapF, typename ScoreF, typename PeelF>
 __device__ __noinline__ void scattered_flights(const PassArgs& a, double x, double y, double z, double kx, double ky,
                                                double kz, int il, double tau_edge, double ssca, double gg,
                                                uint32_t stream, uint64_t packet, KapF kappa_at, ScoreF score_at,
-                                               unsigned long long& kills) {
+                                               PeelF peel_at, unsigned long long& kills) {
     PacketStream rs;
     rs.init(a.seed, stream, packet);
     const double w1 = 1.0 - exp(-tau_edge);
@@ -656,6 +781,7 @@ __device__ __noinline__ void scattered_flights(const PassArgs& a, double x, doub
         if (nev > kMaxScatterings) { ++kills; break; }
         const double a_eff = __ldg(a.rhokap + il) * ssca / fmax((double)kappa_at(il), kTinest);
         wgt = wgt * a_eff;
+        peel_at(x, y, z, il, kx, ky, kz, wgt);   // the imaging pass (raytrace_amr.f90:280-281)
         if (wgt < 1.0e-4) {
             if (rs.next() > 0.1) break;
             wgt = wgt / 0.1;
@@ -737,6 +863,18 @@ __global__ void __launch_bounds__(128) k_walk_edge(const PassArgs a, const Packe
         for (int k = 0; k < NT; ++k) cf[k] = cfp[k * c + i];
         MetalPacket<R, MET> mp;
         if constexpr (METAL) mp.setup(a.m, rec, i, msg, mhc);
+        if (a.peeling) {   // the imaging pass: ion_peel_direct at emission (ionizing_field_mod.f90:126, 157)
+            auto kap_p = [&](int q) -> R {
+                Col<R, NABS> cq;
+                cq.load(a.col, q);
+                R k = cq.template kappa<X>(s0, s1, s2, s3);
+                if constexpr (METAL) {
+                    if (a.metal_abs) k = k + mp.kappa(a.m, q, msg);
+                }
+                return k;
+            };
+            peel_direct<false>(a, rec.p0[i], rec.p0[c + i], rec.p0[2 * c + i], -1, inu, a.Lpacket, kap_p);
+        }
         // ring of LA+1 cells: il, segment, columns, and whether a next cell exists
         int il[LA + 1] = {};
         double sgm[LA + 1] = {};
@@ -817,9 +955,13 @@ __global__ void __launch_bounds__(128) k_walk_edge(const PassArgs a, const Packe
                     }
                 };
                 const R* ds = static_cast<const R*>(rec.dsc);
+                auto peel_at = [&](double px, double py, double pz, int q, double qx, double qy, double qz, double w) {
+                    if (a.peeling)
+                        peel_scatter<false>(a, px, py, pz, q, qx, qy, qz, a.Lpacket * w, (double)ds[c + i], inu, kappa_at);
+                };
                 scattered_flights<false>(a, rec.p0[i], rec.p0[c + i], rec.p0[2 * c + i], rec.p0[3 * c + i], rec.p0[4 * c + i],
                                          rec.p0[5 * c + i], -1, tau, (double)ds[i], (double)ds[c + i], (uint32_t)stream,
-                                         (uint64_t)(ip0 + i), kappa_at, score_at, kills);
+                                         (uint64_t)(ip0 + i), kappa_at, score_at, peel_at, kills);
             }
         }
     }
@@ -1061,6 +1203,18 @@ __global__ void __launch_bounds__(128) k_walk_amr(const PassArgs a, const Packet
         for (int k = 0; k < NT; ++k) cf[k] = cfp[k * c + i];
         MetalPacket<R, MET> mp;
         if constexpr (METAL) mp.setup(a.m, rec, i, msg, mhc);
+        if (a.peeling) {   // the imaging pass: ion_peel_direct at emission (ionizing_field_mod.f90:126, 157)
+            auto kap_p = [&](int q) -> R {
+                Col<R, NABS> cq;
+                cq.load(a.col, q);
+                R k = cq.template kappa<X>(s0, s1, s2, s3);
+                if constexpr (METAL) {
+                    if (a.metal_abs) k = k + mp.kappa(a.m, q, msg);
+                }
+                return k;
+            };
+            peel_direct<true>(a, x, y, z, il, inu, a.Lpacket, kap_p);
+        }
         R expo = (R)1.0;
         double tau = 0.0;
         int nstep = 0;
@@ -1123,9 +1277,13 @@ __global__ void __launch_bounds__(128) k_walk_amr(const PassArgs a, const Packet
                     }
                 };
                 const R* ds = static_cast<const R*>(rec.dsc);
+                auto peel_at = [&](double px, double py, double pz, int q, double qx, double qy, double qz, double w) {
+                    if (a.peeling)
+                        peel_scatter<true>(a, px, py, pz, q, qx, qy, qz, a.Lpacket * w, (double)ds[c + i], inu, kappa_at);
+                };
                 scattered_flights<true>(a, rec.tm[i], rec.tm[c + i], rec.tm[2 * c + i], kx, ky, kz, rec.cell[i], tau,
                                         (double)ds[i], (double)ds[c + i], (uint32_t)stream, (uint64_t)(ip0 + i),
-                                        kappa_at, score_at, kills);
+                                        kappa_at, score_at, peel_at, kills);
             }
         }
     }
@@ -1421,6 +1579,8 @@ PassArgs make_args(mochii_ctx* c) {
     a.scatter = c->scatter ? 1 : 0;
     a.eion_min = c->par.eion_min;
     a.seed = (unsigned long long)(long long)c->par.random_seed;
+    a.peel = c->peel;
+    a.peeling = c->peeling ? 1 : 0;
     return a;
 }
 
@@ -1495,7 +1655,7 @@ struct WalkLaunch {
 // packet_order 'coherent' applies to the stellar packets on the Cartesian
 // grid without grain or FUV terms; elsewhere the launch order is walked.
 bool coherent_walk_applies(const mochii_ctx* c) {
-    return c->par.packet_order == 2 && c->oct.ncells == 0 && !c->xscore && c->rec.key != nullptr;
+    return c->par.packet_order == 2 && c->oct.ncells == 0 && !c->xscore && c->rec.key != nullptr && !c->peeling;
 }
 
 // Walk-kernel variants: look-ahead depth 0..2 (the autotuned choice is

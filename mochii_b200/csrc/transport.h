@@ -16,6 +16,8 @@ cudaError_t diffuse_build(mochii_ctx* c, double* total);
 size_t diffuse_scan_bytes(long long nleaf);
 cudaError_t launch_diffuse_chunk(mochii_ctx* c, double total, long long ip0, long long n);
 cudaError_t launch_rates(mochii_ctx* c);
+cudaError_t peel_setup(mochii_ctx* c);   // par%ion_peel: observers, image plane, device images (peel.cpp)
+cudaError_t peel_clear(mochii_ctx* c);   // zero the images before an imaging pass
 cudaError_t launch_jt_export(mochii_ctx* c, double* dst);
 cudaError_t launch_sobol(const QmcTables* t, int stream01, long long idx0, long long n, int nd, double* out,
                          cudaStream_t s);

@@ -173,6 +173,33 @@ class Nebula:
         self._ok(self.lib.mochii_write_rates(self.ctx, str(base).encode(), C.byref(ri)))
         return str(base) + "_rates"
 
+    def imaging_pass(self):
+        """The peel-off imaging pass (main.f90:234-235): a transport pass with
+        with_peel; needs par%ion_peel."""
+        return self.ionizing_field_and_rates(with_peel=True)
+
+    def image(self, which="direct"):
+        """Peel-off image of the last imaging pass: 'direct', 'scattered' or
+        'direct0', shape (nobs, nchan, nyim, nxim), erg/s per code length^2
+        per pixel."""
+        shape = np.zeros(4, dtype=np.int32)
+        self._ok(self.lib.mochii_image_shape(self.ctx, shape.ctypes.data))
+        out = np.zeros(int(np.prod(shape)), dtype=np.float64)
+        k = {"direct": 0, "scattered": 1, "direct0": 2}[which]
+        self._ok(self.lib.mochii_get_image(self.ctx, k, out.ctypes.data, out.size))
+        return out.reshape(tuple(int(v) for v in shape))
+
+    def image_observer(self, k):
+        """Observer k: x, y, z, alpha, beta, gamma, distance, dxim, dyim, R (9)."""
+        out = np.zeros(18)
+        self._ok(self.lib.mochii_image_observer(self.ctx, int(k), out.ctypes.data))
+        return out
+
+    def write_image(self, base):
+        """ion_peel_write: <base>_image/ with the surface-brightness images."""
+        self._ok(self.lib.mochii_write_image(self.ctx, str(base).encode()))
+        return str(base) + "_image"
+
     def set(self, name, values):
         a = np.ascontiguousarray(values, dtype=np.float64)
         self._ok(self.lib.mochii_set_field(self.ctx, name.encode(), a.ctypes.data, a.size))

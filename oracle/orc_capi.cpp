@@ -431,6 +431,40 @@ long long orc_sim_thermal_cells(void* h, const long long* idx, long long n, doub
     }
     return n;
 }
+// The imaging pass (ionizing_field_and_rates with with_peel, main.f90:234-235):
+// one transport pass that also peels every packet toward the observers.
+int orc_sim_transport_pass_peel(void* h) {
+    auto* s = static_cast<Sim*>(h);
+    if (!s->peel_on) return 1;
+    s->peel_pass = true;
+    s->transport_pass();
+    s->peel_pass = false;
+    return 0;
+}
+// Peel-off images of the last imaging pass, which = 0 direct, 1 scattered,
+// 2 unattenuated direct; (nobs, nchan, nyim, nxim) in erg/s per code length^2
+// per pixel (before ion_peel_write's conversion).  shape4 receives the shape.
+long long orc_sim_peel_image(void* h, int which, double* out, long long cap, int* shape4) {
+    auto* s = static_cast<Sim*>(h);
+    const std::vector<double>& v = which == 0 ? s->tally.img_dir : which == 1 ? s->tally.img_sca : s->tally.img_dir0;
+    shape4[0] = (int)s->obs.size(); shape4[1] = s->nchan; shape4[2] = s->par.nyim; shape4[3] = s->par.nxim;
+    if ((long long)v.size() > cap) return -(long long)v.size();
+    std::memcpy(out, v.data(), v.size() * sizeof(double));
+    return (long long)v.size();
+}
+// Observer k: x, y, z, alpha, beta, gamma, distance, dxim, dyim, then the
+// rotation matrix row by row (18 doubles).
+int orc_sim_peel_observer(void* h, int k, double* out18) {
+    auto* s = static_cast<Sim*>(h);
+    if (k < 0 || k >= (int)s->obs.size()) return 1;
+    const PeelObserver& o = s->obs[k];
+    const double v[7] = {o.x, o.y, o.z, o.alpha, o.beta, o.gamma, o.distance};
+    for (int i = 0; i < 7; ++i) out18[i] = v[i];
+    out18[7] = s->dxim; out18[8] = s->dyim;
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) out18[9 + 3 * i + j] = o.R[i][j];
+    return 0;
+}
 // Diffuse packets launched by the last transport pass (diffuse_nphot).
 long long orc_sim_diffuse_count(void* h) { return static_cast<Sim*>(h)->diffuse_nphot; }
 // Diffuse field: build from the current state, then launch records.

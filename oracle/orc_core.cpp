@@ -511,6 +511,10 @@ Par::Par() {
         src_lum[i] = -999.0;
         src_x[i] = src_y[i] = src_z[i] = 0.0;
     }
+    for (int i = 0; i < MAX_OBS; ++i) {
+        alpha[i] = beta[i] = gamma_[i] = obsx[i] = obsy[i] = obsz[i] = NAN;
+        phase_angle[i] = inclination_angle[i] = position_angle[i] = NAN;
+    }
 }
 
 static std::string lower(std::string s) {
@@ -677,6 +681,16 @@ bool parse_namelist(const std::string& text, Par& p, std::string* err) {
         else if (k == "xhi_init") p.xHI_init = to_dbl(s);
         else if (k == "xhei_init") p.xHeI_init = to_dbl(s);
         else if (k == "xheii_init") p.xHeII_init = to_dbl(s);
+        B(ion_peel); B(peel_bins); B(save_direc0); I(nxim); I(nyim); D(distance); D(dxim); D(dyim);
+        else if (k == "alpha" || k == "beta" || k == "gamma" || k == "obsx" || k == "obsy" || k == "obsz" ||
+                 k == "phase_angle" || k == "inclination_angle" || k == "position_angle") {
+            double* arr = k == "alpha" ? p.alpha : k == "beta" ? p.beta : k == "gamma" ? p.gamma_
+                        : k == "obsx" ? p.obsx : k == "obsy" ? p.obsy : k == "obsz" ? p.obsz
+                        : k == "phase_angle" ? p.phase_angle : k == "inclination_angle" ? p.inclination_angle
+                                                                                       : p.position_angle;
+            for (size_t j = 0; j < v.size() && j < (size_t)MAX_OBS; ++j)
+                if (!v[j].empty()) arr[j] = to_dbl(v[j]);
+        }
         else if (k == "src_tstar" || k == "src_lum" || k == "src_x" || k == "src_y" || k == "src_z") {
             double* arr = k == "src_tstar" ? p.src_tstar : k == "src_lum" ? p.src_lum
                         : k == "src_x" ? p.src_x : k == "src_y" ? p.src_y : p.src_z;
@@ -927,8 +941,12 @@ void Tally::reset(int nleaf, int nnu, int ntr, bool dust, bool fuvt) {
     fuv.assign(fuvt ? (size_t)nleaf : 0, 0.0);
     emitted = absorbed = escaped = 0;
     direct_segments = scattered_segments = 0;
+    img_dir.clear(); img_sca.clear(); img_dir0.clear();
 }
 void Tally::add(const Tally& o) {
+    for (size_t i = 0; i < img_dir.size() && i < o.img_dir.size(); ++i) img_dir[i] += o.img_dir[i];
+    for (size_t i = 0; i < img_sca.size() && i < o.img_sca.size(); ++i) img_sca[i] += o.img_sca[i];
+    for (size_t i = 0; i < img_dir0.size() && i < o.img_dir0.size(); ++i) img_dir0[i] += o.img_dir0[i];
     for (size_t i = 0; i < hhe.size(); ++i) hhe[i] += o.hhe[i];
     for (size_t i = 0; i < jt.size(); ++i) jt[i] += o.jt[i];
     for (size_t i = 0; i < metal.size(); ++i) metal[i] += o.metal[i];
@@ -1074,6 +1092,7 @@ bool Sim::setup(const std::string& nl, std::string* err) {
     heat_HI.assign(nleaf, 0.0); heat_HeI.assign(nleaf, 0.0); heat_HeII.assign(nleaf, 0.0);
     heat_dust.assign(nleaf, 0.0); g0_fuv.assign(nleaf, 0.0);
     opacity_fill();   // gas_opacity_setup -> gas_opacity_fill (gas_opacity_mod.f90:240-290)
+    peel_setup();     // ion_peel_setup: observers and image plane
     return true;
 }
 
@@ -1446,6 +1465,7 @@ void Sim::transport_packet(Photon& ph, Tally& t) const {
         if (++nev > MAX_SCATTERINGS) break;
         const double a_eff = st.rhokap[il] * ph.dust_sca / std::max(opacity(*this, ph, il), TINEST);
         ph.wgt = ph.wgt * a_eff;
+        if (peel_on && peel_pass) peel_scatter(ph, t);   // raytrace_amr.f90:280-281
         if (ph.wgt < WMIN) {
             if (ph.rng.next() > PSURV) break;
             ph.wgt = ph.wgt / PSURV;
@@ -1542,7 +1562,14 @@ void Sim::transport_pass() {
     const int nt = std::max(1, nthreads);
     std::vector<Tally> loc(nt);
     const int ntr = metals() ? sp->ntr : 0;
-    for (auto& t : loc) t.reset(nleaf, nnu, ntr, par.ion_add_dust, par.add_fuv);
+    const bool peel = peel_on && peel_pass;
+    const size_t npix = peel ? obs.size() * (size_t)nchan * par.nxim * par.nyim : 0;
+    for (auto& t : loc) {
+        t.reset(nleaf, nnu, ntr, par.ion_add_dust, par.add_fuv);
+        t.img_dir.assign(npix, 0.0);
+        t.img_sca.assign(npix, 0.0);
+        t.img_dir0.assign(peel && par.save_direc0 ? npix : 0, 0.0);
+    }
     const int64_t np = par.nphotons;
 #pragma omp parallel num_threads(nt)
     {
@@ -1555,6 +1582,7 @@ void Sim::transport_pass() {
         for (int64_t ip = 1 + tid; ip <= np; ip += nt) {
             gen_photon_qmc(ip - 1, ph);
             ph.rng = PacketRng{(uint64_t)par.iseed, (uint64_t)(ip - 1), 0u, 0u};
+            if (peel) peel_direct(ph, t);   // ionizing_field_mod.f90:126
             transport_packet(ph, t);
         }
     }
@@ -1574,11 +1602,15 @@ void Sim::transport_pass() {
             for (int64_t ip = 1 + tid; ip <= nd; ip += nt) {
                 gen_diffuse_qmc(ip - 1, ph);
                 ph.rng = PacketRng{(uint64_t)par.iseed, (uint64_t)(ip - 1), 1u, 0u};
+                if (peel) peel_direct(ph, t);   // ionizing_field_mod.f90:157
                 transport_packet(ph, t);
             }
         }
     }
     tally.reset(nleaf, nnu, ntr, par.ion_add_dust, par.add_fuv);
+    tally.img_dir.assign(npix, 0.0);
+    tally.img_sca.assign(npix, 0.0);
+    tally.img_dir0.assign(peel && par.save_direc0 ? npix : 0, 0.0);
     for (auto& t : loc) tally.add(t);
     gas_rates_compute();
     if (metals()) {   // species_gamma_compute, species_mod.f90:493-512
@@ -1994,5 +2026,223 @@ void Sim::gas_equilibrium_update(double* max_dx, double* dx_vol) {
     *dx_vol = sdx / std::max(sx, TINEST);
     st.xHI = xHI_new; st.xHeI = xHeI_new; st.xHeII = xHeII_new; st.ne = ne_new;
 }
+
+// ---- peel-off imaging: ion_peel_mod.f90 and the optical-depth-only walks
+// raytrace_ion_tau_only_car / _amr (raytrace_amr.f90:678-775) -------------
+namespace {
+constexpr double DEG2RAD = PI / 180.0, RAD2DEG = 180.0 / PI;
+constexpr double FOURPI = 4.0 * PI;
+bool finite(double x) { return std::isfinite(x); }
+}  // namespace
+
+// ion_peel_setup (ion_peel_mod.f90:49-206): observers from the angle lists or
+// the positions, the grid -> observer rotation, the auto pixel scale.
+void Sim::peel_setup() {
+    Par& p = par;
+    peel_on = p.ion_peel;
+    obs.clear();
+    if (!peel_on) return;
+    for (int i = 0; i < MAX_OBS; ++i) {
+        if (finite(p.phase_angle[i])) p.alpha[i] = -p.phase_angle[i];
+        if (finite(p.inclination_angle[i])) p.beta[i] = -p.inclination_angle[i];
+        if (finite(p.position_angle[i])) p.gamma_[i] = -p.position_angle[i];
+        if (finite(p.beta[i]) && !finite(p.alpha[i])) p.alpha[i] = 0.0;
+        if (finite(p.alpha[i]) && !finite(p.beta[i])) p.beta[i] = 0.0;
+    }
+    const double xm = std::max({grid.xmax, grid.ymax, grid.zmax});
+    if (!(finite(p.alpha[0]) && finite(p.beta[0])) && !(finite(p.obsx[0]) && finite(p.obsy[0]) && finite(p.obsz[0]))) {
+        if (!finite(p.distance)) p.distance = xm * 1.0e3;
+        p.obsx[0] = 0.0; p.obsy[0] = 0.0; p.obsz[0] = p.distance;
+        p.alpha[0] = 0.0; p.beta[0] = 0.0;
+    }
+    std::vector<double> ca, sa, cb, sb, cg, sg;
+    if (finite(p.alpha[0]) && finite(p.beta[0])) {
+        if (!finite(p.distance)) p.distance = xm * 1.0e3;
+        for (int i = 0; i < MAX_OBS; ++i) {
+            if (!(finite(p.alpha[i]) && finite(p.beta[i]))) continue;
+            if (!finite(p.gamma_[i])) {
+                if (p.beta[i] > 0.0 && p.beta[i] <= 90.0) p.gamma_[i] = 90.0;
+                else if (p.beta[i] > 90.0) p.gamma_[i] = -90.0;
+                else p.gamma_[i] = 0.0;
+            }
+            PeelObserver o;
+            ca.push_back(std::cos(p.alpha[i] * DEG2RAD)); sa.push_back(std::sin(p.alpha[i] * DEG2RAD));
+            cb.push_back(std::cos(p.beta[i] * DEG2RAD)); sb.push_back(std::sin(p.beta[i] * DEG2RAD));
+            cg.push_back(std::cos(p.gamma_[i] * DEG2RAD)); sg.push_back(std::sin(p.gamma_[i] * DEG2RAD));
+            o.x = p.distance * ca.back() * sb.back();
+            o.y = p.distance * sa.back() * sb.back();
+            o.z = p.distance * cb.back();
+            o.alpha = p.alpha[i]; o.beta = p.beta[i]; o.gamma = p.gamma_[i]; o.distance = p.distance;
+            obs.push_back(o);
+        }
+    } else {
+        if (!finite(p.distance)) {
+            p.distance = std::sqrt(p.obsx[0] * p.obsx[0] + p.obsy[0] * p.obsy[0] + p.obsz[0] * p.obsz[0]);
+            if (p.distance < 10.0 * xm) p.distance = xm * 1.0e3;
+        }
+        for (int i = 0; i < MAX_OBS; ++i) {
+            if (!(finite(p.obsx[i]) && finite(p.obsy[i]) && finite(p.obsz[i]))) continue;
+            if (!finite(p.gamma_[i])) p.gamma_[i] = 0.0;
+            const double robs = std::sqrt(p.obsx[i] * p.obsx[i] + p.obsy[i] * p.obsy[i] + p.obsz[i] * p.obsz[i]);
+            const double ds = p.distance / robs;
+            PeelObserver o;
+            if (ds > 1.001) { o.x = p.obsx[i] * ds; o.y = p.obsy[i] * ds; o.z = p.obsz[i] * ds; }
+            else { o.x = p.obsx[i]; o.y = p.obsy[i]; o.z = p.obsz[i]; }
+            double c_b = robs > 0.0 ? p.obsz[i] / robs : 1.0;
+            c_b = std::min(std::max(c_b, -1.0), 1.0);
+            const double s_b = std::sqrt(1.0 - c_b * c_b);
+            p.beta[i] = std::atan2(s_b, c_b) * RAD2DEG;
+            double c_a, s_a;
+            if (s_b == 0.0) {
+                c_a = 1.0; s_a = 0.0; p.alpha[i] = 0.0;
+            } else {
+                const double al = std::atan2(o.y, o.x);
+                c_a = std::cos(al); s_a = std::sin(al);
+                p.alpha[i] = al * RAD2DEG;
+            }
+            ca.push_back(c_a); sa.push_back(s_a); cb.push_back(c_b); sb.push_back(s_b);
+            cg.push_back(std::cos(p.gamma_[i] * DEG2RAD)); sg.push_back(std::sin(p.gamma_[i] * DEG2RAD));
+            o.alpha = p.alpha[i]; o.beta = p.beta[i]; o.gamma = p.gamma_[i]; o.distance = p.distance;
+            obs.push_back(o);
+        }
+    }
+    for (size_t i = 0; i < obs.size(); ++i) {
+        PeelObserver& o = obs[i];
+        o.R[0][0] = ca[i] * cb[i] * cg[i] - sa[i] * sg[i];
+        o.R[0][1] = sa[i] * cb[i] * cg[i] + ca[i] * sg[i];
+        o.R[0][2] = -sb[i] * cg[i];
+        o.R[1][0] = -ca[i] * cb[i] * sg[i] - sa[i] * cg[i];
+        o.R[1][1] = -sa[i] * cb[i] * sg[i] + ca[i] * cg[i];
+        o.R[1][2] = sb[i] * sg[i];
+        o.R[2][0] = ca[i] * sb[i];
+        o.R[2][1] = sa[i] * sb[i];
+        o.R[2][2] = cb[i];
+    }
+    if (!(finite(p.dxim) && finite(p.dyim))) {
+        p.dxim = std::atan2(xm * std::sqrt(3.0), p.distance) / (p.nxim / 2.0) * RAD2DEG;
+        p.dyim = std::atan2(xm * std::sqrt(3.0), p.distance) / (p.nyim / 2.0) * RAD2DEG;
+    }
+    dxim = p.dxim;
+    dyim = p.dyim;
+    nchan = p.peel_bins ? band.nnu_band : (p.add_fuv ? 2 : 1);
+}
+
+int Sim::peel_channel(int inu) const {   // ion_peel_mod.f90:212-220 (0-based)
+    if (par.peel_bins) return inu;
+    if (nchan == 2 && std::sqrt(band.eedge[inu] * band.eedge[inu + 1]) < par.eion_min) return 1;
+    return 0;
+}
+
+bool Sim::peel_pixel(const PeelObserver& o, double kx, double ky, double kz, int* ix, int* iy) const {
+    double v[3];
+    for (int i = 0; i < 3; ++i) v[i] = o.R[i][0] * kx + o.R[i][1] * ky + o.R[i][2] * kz;
+    *ix = (int)std::floor(std::atan2(-v[0], v[2]) * RAD2DEG / dxim + par.nxim / 2.0);
+    *iy = (int)std::floor(std::atan2(-v[1], v[2]) * RAD2DEG / dyim + par.nyim / 2.0);
+    return *ix >= 0 && *ix < par.nxim && *iy >= 0 && *iy < par.nyim;
+}
+
+// Optical depth from the packet's point along (kx, ky, kz) to the box edge at
+// the packet's energy, no tally; stops at tau_huge.
+double Sim::tau_only(const Photon& ph, double kx, double ky, double kz) const {
+    double tau = 0.0;
+    if (amr_walk()) {
+        double x = ph.x, y = ph.y, z = ph.z;
+        int il = ph.il >= 0 ? ph.il : leaf_find(x, y, z);
+        if (il < 0) return 0.0;
+        for (int nstep = 1; nstep <= MAX_WALK_STEPS; ++nstep) {
+            double texit;
+            int iface;
+            leaf_exit(il, x, y, z, kx, ky, kz, &texit, &iface);
+            tau = tau + opacity(*this, ph, il) * texit;
+            if (tau >= TAU_HUGE) break;
+            x = x + texit * kx; y = y + texit * ky; z = z + texit * kz;
+            const int nl = leaf_next(il, iface, x, y, z);
+            if (nl < 0) break;
+            il = nl;
+        }
+        return tau;
+    }
+    const double d = grid.dcell;
+    const double pos[3] = {ph.x, ph.y, ph.z}, kk[3] = {kx, ky, kz};
+    const double org[3] = {grid.xmin, grid.ymin, grid.zmin};
+    const int n[3] = {grid.nx, grid.ny, grid.nz};
+    int idx[3], stp[3];
+    double tmax[3], tdel[3];
+    for (int a = 0; a < 3; ++a) {
+        idx[a] = std::min(std::max((int)((pos[a] - org[a]) / d), 0), n[a] - 1);
+        if (kk[a] > 0.0) {
+            stp[a] = 1; tmax[a] = (org[a] + (double)(idx[a] + 1) * d - pos[a]) / kk[a]; tdel[a] = d / kk[a];
+        } else if (kk[a] < 0.0) {
+            stp[a] = -1; tmax[a] = (org[a] + (double)idx[a] * d - pos[a]) / kk[a]; tdel[a] = -d / kk[a];
+        } else {
+            stp[a] = 0; tmax[a] = HUGEST; tdel[a] = HUGEST;
+        }
+    }
+    double t_cur = 0.0;
+    for (int nstep = 1; nstep <= MAX_WALK_STEPS; ++nstep) {
+        const int il = idx[0] + n[0] * (idx[1] + n[1] * idx[2]);
+        int a = 0;
+        if (tmax[1] < tmax[a]) a = 1;
+        if (tmax[2] < tmax[a]) a = 2;
+        tau = tau + opacity(*this, ph, il) * (tmax[a] - t_cur);
+        if (tau >= TAU_HUGE) break;
+        t_cur = tmax[a];
+        tmax[a] = tmax[a] + tdel[a];
+        idx[a] += stp[a];
+        if (idx[a] < 0 || idx[a] >= n[a]) break;
+    }
+    return tau;
+}
+
+// ion_peel_direct (ion_peel_mod.f90:225-277): the isotropic source's
+// Lpacket wgt / (4 pi r^2) e^-tau to its pixel of every observer.
+void Sim::peel_direct(const Photon& ph, Tally& t) const {
+    const int ch = peel_channel(ph.inu);
+    const int nx = par.nxim, ny = par.nyim;
+    for (size_t k = 0; k < obs.size(); ++k) {
+        const PeelObserver& o = obs[k];
+        double kx = o.x - ph.x, ky = o.y - ph.y, kz = o.z - ph.z;
+        const double r2 = kx * kx + ky * ky + kz * kz, r = std::sqrt(r2);
+        kx = kx / r; ky = ky / r; kz = kz / r;
+        int ix, iy;
+        if (!peel_pixel(o, kx, ky, kz, &ix, &iy)) continue;
+        const size_t pix = ((k * nchan + ch) * (size_t)ny + iy) * nx + ix;
+        double contrib = ph.Lpacket * ph.wgt / (FOURPI * r2);
+        if (par.save_direc0) t.img_dir0[pix] += contrib;
+        const double tau = tau_only(ph, kx, ky, kz);
+        if (tau > 500.0) continue;
+        t.img_dir[pix] += contrib * std::exp(-tau);
+    }
+}
+
+// ion_peel_scatter (ion_peel_mod.f90:284-344): at a dust interaction, after
+// the albedo weight and before the new direction, the Henyey-Greenstein
+// phase function toward each observer.
+void Sim::peel_scatter(const Photon& ph, Tally& t) const {
+    const int ch = peel_channel(ph.inu);
+    const int nx = par.nxim, ny = par.nyim;
+    const double gg = std::min(std::max(ph.dust_g, -0.9999), 0.9999);
+    for (size_t k = 0; k < obs.size(); ++k) {
+        const PeelObserver& o = obs[k];
+        double kx = o.x - ph.x, ky = o.y - ph.y, kz = o.z - ph.z;
+        const double r2 = kx * kx + ky * ky + kz * kz, r = std::sqrt(r2);
+        kx = kx / r; ky = ky / r; kz = kz / r;
+        int ix, iy;
+        if (!peel_pixel(o, kx, ky, kz, &ix, &iy)) continue;
+        const double tau = tau_only(ph, kx, ky, kz);
+        if (tau > 500.0) continue;
+        const double kn2 = ph.kx * ph.kx + ph.ky * ph.ky + ph.kz * ph.kz;
+        if (kn2 <= 0.0) continue;
+        double cosa = (ph.kx * kx + ph.ky * ky + ph.kz * kz) / std::sqrt(kn2);
+        cosa = std::min(std::max(cosa, -1.0), 1.0);
+        const double dmin = (1.0 - std::fabs(gg)) * (1.0 - std::fabs(gg));
+        const double den = std::max((1.0 + gg * gg) - 2.0 * gg * cosa, dmin);
+        const double peel = (1.0 - gg * gg) / (den * std::sqrt(den) * FOURPI);
+        const double contrib = ph.Lpacket * ph.wgt * peel / r2 * std::exp(-tau);
+        if (!std::isfinite(contrib)) continue;
+        t.img_sca[((k * nchan + ch) * (size_t)ny + iy) * nx + ix] += contrib;
+    }
+}
+
 
 }  // namespace orc

@@ -40,6 +40,7 @@ constexpr double TAU_HUGE = 745.2;             // raytrace_amr.f90:33
 constexpr int MAX_WALK_STEPS = 20000000;       // raytrace_amr.f90:43
 constexpr int MAX_PLANCK_KNOTS = 200000;       // energy_sampler_mod.f90:16
 constexpr int MAX_SRC = 16;                    // define.f90:74
+constexpr int MAX_OBS = 16;                    // peel-off observers (define.f90:76 allows 181)
 constexpr double HUGEST = 1.7976931348623157e308;
 constexpr double TINEST = 2.2250738585072014e-308;
 
@@ -158,6 +159,12 @@ struct Par {
     double abund_C = 2.2e-4, abund_N = 4.0e-5, abund_O = 3.3e-4, abund_Ne = 5.0e-5, abund_S = 9.0e-6;
     double abund_Ar = 0.0, abund_Mg = 0.0, abund_Fe = 0.0, abund_Si = 0.0, abund_Cl = 0.0, abund_Ca = 0.0;
     bool ion_metal_abs = true, metal_ne = true, metal_heat = true, metal_freefree = true;
+    // peel-off imaging (define.f90:518-544, 658-664); NaN = unset
+    bool ion_peel = false, peel_bins = false, save_direc0 = false;
+    int nxim = 129, nyim = 129;
+    double distance = NAN, dxim = NAN, dyim = NAN;
+    double alpha[MAX_OBS], beta[MAX_OBS], gamma_[MAX_OBS], obsx[MAX_OBS], obsy[MAX_OBS], obsz[MAX_OBS];
+    double phase_angle[MAX_OBS], inclination_angle[MAX_OBS], position_angle[MAX_OBS];
     bool fe_levels_full = false;
     Par();
 };
@@ -202,6 +209,7 @@ struct Tally {
     std::vector<double> metal;       // metal path estimators [(il*ntr + k)*2 + m]
     std::vector<double> dust_abs;    // dust_abs_path (nleaf), with ion_add_dust
     std::vector<double> fuv;         // fuv_field_path (nleaf), with add_fuv
+    std::vector<double> img_dir, img_sca, img_dir0;   // peel-off images (nobs, nchan, nyim, nxim)
     long double emitted = 0, absorbed = 0, escaped = 0;
     int64_t direct_segments = 0, scattered_segments = 0;
     void reset(int nleaf, int nnu, int ntr = 0, bool dust = false, bool fuv = false);
@@ -224,6 +232,12 @@ struct Photon {
 
 struct Thermal;
 struct Species;
+
+// One peel-off observer (ion_peel_mod.f90 ion_peel_setup).
+struct PeelObserver {
+    double x, y, z, alpha, beta, gamma, distance;
+    double R[3][3];            // grid -> observer frame
+};
 
 // milne_recomb_spectrum_mod.f90: ground-continuum recombination spectra.
 struct Milne {
@@ -257,6 +271,18 @@ struct Sim {
     double diffuse_lum = 0.0;
     int64_t diffuse_nphot = 0;
     bool defer_fill = false;   // orc_sim_set leaves the opacity refresh to the caller
+    // peel-off imaging (ion_peel_mod.f90), set up by peel_setup()
+    bool peel_on = false;            // par%ion_peel
+    bool peel_pass = false;          // this pass peels (the imaging pass, main.f90:234-235)
+    std::vector<PeelObserver> obs;
+    int nchan = 1;
+    double dxim = 0.0, dyim = 0.0;
+    void peel_setup();                                            // ion_peel_setup, :49-206
+    double tau_only(const Photon& ph, double kx, double ky, double kz) const;   // raytrace_amr.f90:678-775
+    bool peel_pixel(const PeelObserver& o, double kx, double ky, double kz, int* ix, int* iy) const;
+    void peel_direct(const Photon& ph, Tally& t) const;           // ion_peel_direct, :225-277
+    void peel_scatter(const Photon& ph, Tally& t) const;          // ion_peel_scatter, :284-344
+    int peel_channel(int inu) const;                              // :212-220
     void diffuse_build(double lpacket);                          // diffuse_mod.f90:60-121
     void gen_diffuse_qmc(int64_t ip, Photon& ph) const;          // diffuse_mod.f90:221-296
     bool setup(const std::string& namelist, std::string* err);

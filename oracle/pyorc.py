@@ -84,6 +84,9 @@ def load():
         "orc_sim_thermal_cells": (LL, [V, V, LL, V]),
         "orc_sim_diffuse_count": (LL, [V]),
         "orc_sim_defer_fill": (None, [V, I]),
+        "orc_sim_transport_pass_peel": (I, [V]),
+        "orc_sim_peel_image": (LL, [V, I, V, LL, V]),
+        "orc_sim_peel_observer": (I, [V, I, V]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)
@@ -343,6 +346,25 @@ class Sim:
         heat_*, and with metals gamma_metal / heat_metal, leaf-major)."""
         a = np.ascontiguousarray(values, dtype=float)
         assert load().orc_sim_set(self.h, name.encode(), a.ctypes.data, a.size) == a.size, name
+
+    def imaging_pass(self):
+        """The transport pass with peel-off (par%ion_peel)."""
+        assert load().orc_sim_transport_pass_peel(self.h) == 0
+
+    def peel_image(self, which):
+        """'direct', 'scattered' or 'direct0' images of the last imaging pass,
+        (nobs, nchan, nyim, nxim), erg/s per code length^2 per pixel."""
+        k = {"direct": 0, "scattered": 1, "direct0": 2}[which]
+        shape = np.zeros(4, dtype=np.int32)
+        n = load().orc_sim_peel_image(self.h, k, None, 0, shape.ctypes.data)
+        out = np.zeros(max(-n, n, 0))
+        load().orc_sim_peel_image(self.h, k, out.ctypes.data, out.size, shape.ctypes.data)
+        return out.reshape(tuple(shape)) if out.size else out
+
+    def peel_observer(self, k):
+        out = np.zeros(18)
+        assert load().orc_sim_peel_observer(self.h, int(k), out.ctypes.data) == 0
+        return out
 
     def set_state(self, fields):
         """Several fields (dict name -> values) with one opacity refresh."""
