@@ -212,6 +212,9 @@ typedef struct mochii_tuning {
     int lookahead;           /* cells the DDA stepper runs ahead of the scoring, 0..2 */
     int walk_blocks_per_sm;  /* persistent walk grid: SMs x this, 128-thread blocks  */
     double best_ms;          /* device time of the winning trial pass (autotune)     */
+    int lane_threads;        /* per-lane thermal solve: leaves (lanes) per block, a
+                                multiple of 32; 0 = as many as the rate cache fits   */
+    double thermal_ms;       /* device time of the winning trial thermal update      */
 } mochii_tuning;
 
 typedef struct mochii_ctx mochii_ctx;
@@ -319,11 +322,14 @@ int mochii_batch_iterate(mochii_batch* b, int solve_te, mochii_pass_stats* stats
                          double* device_ms);
 void mochii_batch_destroy(mochii_batch* b);
 
-/* ---- autotuner: packet-block and look-ahead shapes ---------------------- */
+/* ---- autotuner: packet-block, look-ahead and cell-tile shapes ----------- */
 /* Time trial transport passes of sample_packets packets on the current
- * state for every walk variant and keep the fastest; the choice is cached
- * per (grid shape, precision, absorber set, device) for the process.  The
- * trial passes overwrite the tallies, so call it before a pass. */
+ * state for every walk variant and keep the fastest; with the per-lane
+ * thermal solve also trial thermal updates from a saved copy of the state
+ * for several lanes per block (the cell tile), the state restored after.
+ * The choice is cached per (grid shape, precision, absorber set, device)
+ * for the process.  The trial passes overwrite the tallies and rates, so
+ * call it before a pass. */
 int mochii_autotune(mochii_ctx* ctx, int64_t sample_packets, mochii_tuning* out);
 int mochii_set_tuning(mochii_ctx* ctx, const mochii_tuning* t);
 int mochii_get_tuning(const mochii_ctx* ctx, mochii_tuning* out);

@@ -87,7 +87,8 @@ class RunInfo(C.Structure):
 
 
 class Tuning(C.Structure):
-    _fields_ = [("lookahead", C.c_int), ("walk_blocks_per_sm", C.c_int), ("best_ms", C.c_double)]
+    _fields_ = [("lookahead", C.c_int), ("walk_blocks_per_sm", C.c_int), ("best_ms", C.c_double),
+                ("lane_threads", C.c_int), ("thermal_ms", C.c_double)]
 
 
 # Every symbol the header declares, with its ctypes signature.

@@ -965,11 +965,17 @@ std::string tune_key(const mochii_ctx* c) {
 }  // namespace
 
 extern "C" int mochii_set_tuning(mochii_ctx* c, const mochii_tuning* t) {
-    if (!c || !t || t->lookahead < 0 || t->lookahead > 2 || t->walk_blocks_per_sm < 1 || t->walk_blocks_per_sm > 64)
-        return fail(c, MOCHII_ERR_BAD_PARAM, "tuning out of range (lookahead 0..2, blocks per SM 1..64)");
+    if (!c || !t || t->lookahead < 0 || t->lookahead > 2 || t->walk_blocks_per_sm < 1 || t->walk_blocks_per_sm > 64 ||
+        t->lane_threads < 0 || t->lane_threads % 32 != 0 || t->lane_threads > 1024)
+        return fail(c, MOCHII_ERR_BAD_PARAM,
+                    "tuning out of range (lookahead 0..2, blocks per SM 1..64, lane threads a multiple of 32)");
     ++c->generation;
     c->tune.lookahead = t->lookahead;
     c->tune.walk_blocks_per_sm = t->walk_blocks_per_sm;
+    if (t->lane_threads != c->tune.lane_threads) {
+        c->tune.lane_threads = t->lane_threads;
+        c->bw.lane_threads = 0;   // the lane kernel's launch shape is rebuilt at the next thermal update
+    }
     const int nb = transport_blocks(c);
     if (nb > c->tw.ledger_blocks) {
         cudaFree(c->tw.ledger);
@@ -985,6 +991,8 @@ extern "C" int mochii_get_tuning(const mochii_ctx* c, mochii_tuning* t) {
     t->lookahead = c->tune.lookahead;
     t->walk_blocks_per_sm = c->tune.walk_blocks_per_sm;
     t->best_ms = c->tune.best_ms;
+    t->lane_threads = c->tune.lane_threads;
+    t->thermal_ms = c->tune.thermal_ms;
     return MOCHII_OK;
 }
 
@@ -993,9 +1001,11 @@ extern "C" int mochii_autotune(mochii_ctx* c, int64_t sample, mochii_tuning* out
     const std::string key = tune_key(c);
     auto it = tune_cache().find(key);
     if (it != tune_cache().end()) {
-        c->tune = it->second;
-        mochii_tuning t{c->tune.lookahead, c->tune.walk_blocks_per_sm, c->tune.best_ms};
+        const Tuning cached = it->second;
+        mochii_tuning t{cached.lookahead, cached.walk_blocks_per_sm, cached.best_ms, cached.lane_threads,
+                        cached.thermal_ms};
         int rc = mochii_set_tuning(c, &t);
+        c->tune = cached;
         if (out) *out = t;
         return rc;
     }
@@ -1003,10 +1013,10 @@ extern "C" int mochii_autotune(mochii_ctx* c, int64_t sample, mochii_tuning* out
     int rc = mochii_set_nphotons(c, std::min<int64_t>(sample, keep));
     if (rc) return rc;
     double best = 1e300;
-    mochii_tuning bt{2, 8, 0.0};
+    mochii_tuning bt{2, 8, 0.0, 0, 0.0};
     for (int la = 0; la <= 2; ++la)
         for (int bps : {4, 8, 16, 32}) {
-            mochii_tuning t{la, bps, 0.0};
+            mochii_tuning t{la, bps, 0.0, c->tune.lane_threads, 0.0};
             if ((rc = mochii_set_tuning(c, &t))) return rc;
             double ms = 0.0;
             for (int rep = 0; rep < 3; ++rep) {
@@ -1019,6 +1029,50 @@ extern "C" int mochii_autotune(mochii_ctx* c, int64_t sample, mochii_tuning* out
     bt.best_ms = best / 2.0;
     if ((rc = mochii_set_tuning(c, &bt))) return rc;
     c->tune.best_ms = bt.best_ms;
+    // the cell tile of the per-lane thermal solve: trial updates on the rates
+    // of the last trial pass, each from the saved state, the state restored
+    if (c->thermal_ready && c->metal.ntr > 0 && c->par.solver_bracketed && c->par.solver_warp == 3) {
+        const long long n = c->grid.nleaf;
+        double* save = nullptr;
+        CK(c, cudaMalloc(&save, (size_t)5 * n * 8));
+        double* fields[5] = {c->xHI, c->xHeI, c->xHeII, c->ne, c->Te};
+        auto copy = [&](bool to_save) -> cudaError_t {
+            for (int f = 0; f < 5; ++f) {
+                cudaError_t e = to_save ? cudaMemcpyAsync(save + f * n, fields[f], n * 8, cudaMemcpyDeviceToDevice, c->stream)
+                                        : cudaMemcpyAsync(fields[f], save + f * n, n * 8, cudaMemcpyDeviceToDevice, c->stream);
+                if (e != cudaSuccess) return e;
+            }
+            return cudaSuccess;
+        };
+        cudaError_t e = copy(true);
+        int best_threads = 0;
+        double best_t = 1e300;
+        for (int threads : {0, 192, 160, 128, 96}) {   // 0: the most lanes the rate cache fits
+            if (e != cudaSuccess) break;
+            c->tune.lane_threads = threads;
+            c->bw.lane_threads = 0;
+            double ms = 0.0;
+            for (int rep = 0; rep < 2 && e == cudaSuccess; ++rep) {
+                if ((e = copy(false)) != cudaSuccess) break;
+                mochii_metrics m;
+                c->twarm_set = false;
+                const int r2 = mochii_balance_update(c, 1, &m);
+                if (r2) { cudaFree(save); return r2; }
+                if (rep > 0) ms = m.kernel_ms;   // the first update warms the shape
+            }
+            if (e == cudaSuccess && ms < best_t) { best_t = ms; best_threads = threads; }
+        }
+        if (e == cudaSuccess) e = copy(false);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+        cudaFree(save);
+        CK(c, e);
+        c->tune.lane_threads = best_threads;
+        c->bw.lane_threads = 0;
+        c->tune.thermal_ms = best_t;
+        bt.lane_threads = best_threads;
+        bt.thermal_ms = best_t;
+        c->columns_fresh = false;   // the trial updates rewrote the columns
+    }
     c->tune.tuned = true;
     tune_cache()[key] = c->tune;
     if ((rc = mochii_set_nphotons(c, keep))) return rc;

@@ -2320,6 +2320,7 @@ cudaError_t thermal_lane_setup(mochii_ctx* c) {
     const size_t per_lane = (size_t)std::max(nslot, 1) * 8;
     int threads = (int)(((size_t)smem_max - fixed) / per_lane) / 32 * 32;
     threads = std::max(32, std::min(kBThreads, threads));
+    if (c->tune.lane_threads > 0) threads = std::max(32, std::min(threads, c->tune.lane_threads / 32 * 32));   // the cell tile
     w.lane_threads = threads;
     w.lane_smem = lane_cache_offset() + per_lane * threads;
     w.lane_blocks = std::max(1, std::min(sms, c->bw.blocks));

@@ -89,6 +89,8 @@ struct Tuning {
     int walk_blocks_per_sm = 8;   // persistent walk grid = SMs x this, 128-thread blocks
     bool tuned = false;
     double best_ms = 0.0;
+    int lane_threads = 0;         // per-lane thermal solve: lanes per block (0: the most the cache fits)
+    double thermal_ms = 0.0;
 };
 
 struct BalanceWork {

@@ -212,16 +212,23 @@ class Nebula:
         overwritten by the trial passes)."""
         t = Tuning()
         self._ok(self.lib.mochii_autotune(self.ctx, int(sample_packets), C.byref(t)))
-        return {"lookahead": t.lookahead, "walk_blocks_per_sm": t.walk_blocks_per_sm, "best_ms": t.best_ms}
+        return self._tuning_dict(t)
 
-    def set_tuning(self, lookahead, walk_blocks_per_sm):
-        t = Tuning(int(lookahead), int(walk_blocks_per_sm), 0.0)
+    @staticmethod
+    def _tuning_dict(t):
+        return {"lookahead": t.lookahead, "walk_blocks_per_sm": t.walk_blocks_per_sm, "best_ms": t.best_ms,
+                "lane_threads": t.lane_threads, "thermal_ms": t.thermal_ms}
+
+    def set_tuning(self, lookahead, walk_blocks_per_sm, lane_threads=None):
+        cur = self.tuning()
+        t = Tuning(int(lookahead), int(walk_blocks_per_sm), 0.0,
+                   int(cur["lane_threads"] if lane_threads is None else lane_threads), 0.0)
         self._ok(self.lib.mochii_set_tuning(self.ctx, C.byref(t)))
 
     def tuning(self):
         t = Tuning()
         self._ok(self.lib.mochii_get_tuning(self.ctx, C.byref(t)))
-        return {"lookahead": t.lookahead, "walk_blocks_per_sm": t.walk_blocks_per_sm, "best_ms": t.best_ms}
+        return self._tuning_dict(t)
 
     @property
     def ion_Ltot(self):

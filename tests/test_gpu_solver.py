@@ -193,3 +193,35 @@ def test_metal_rate_table_matches_exact():
     dT = np.abs(out["table"][0] - out["exact"][0])
     assert np.median(dT) < 1e-6 and dT.max() < 1.0, dT.max()
     assert np.max(np.abs(out["table"][1] - out["exact"][1])) < 1e-5
+
+
+def test_autotune_picks_a_cell_tile_and_keeps_the_state():
+    """The autotuner's thermal trials (lanes per block of the per-lane solve)
+    restore the state they start from, and the solve with any tile gives the
+    same leaves."""
+    n = 20
+    nl = with_solver(configs.hii_metals(nphotons=60000, niter=2, n=n, precision="fp32", rs_factor=1.3,
+                                        diffuse=False), "bracketed")
+    neb = Nebula(parse_namelist(nl))
+    st = partial_state(n, parse_namelist(nl).xmax)
+    for k, v in st.items():
+        neb.set(k, v)
+    neb.gas_opacity_fill()
+    before = {f: neb.get(f) for f in ("x_HI", "T_e", "n_e")}
+    t = neb.autotune(20000)
+    assert t["lane_threads"] in (0, 192, 160, 128, 96) and t["thermal_ms"] > 0
+    for f, v in before.items():
+        assert np.array_equal(neb.get(f), v), f
+    out = {}
+    for lanes in (0, 96):
+        neb.set_tuning(t["lookahead"], t["walk_blocks_per_sm"], lanes)
+        for k, v in before.items():
+            neb.set(k, v)
+        neb.gas_opacity_fill()
+        neb.ionizing_field_and_rates()
+        neb.gas_thermal_update()
+        out[lanes] = (neb.get("T_e"), neb.get("x_HI"))
+    dT = np.abs(out[0][0] - out[96][0])
+    assert np.median(dT) < 1e-6 and dT.max() < 1.0, dT.max()
+    assert np.max(np.abs(out[0][1] - out[96][1])) < 1e-5
+    neb.close()
