@@ -428,8 +428,19 @@ int mochii_mlp_predict(mochii_mlp* m, const float* X, int64_t n, double* out4);
 /* features of every leaf from the nebula's current rates and state (nleaf x 16) */
 int mochii_mlp_features(mochii_ctx* ctx, float* out);
 /* predicted T_e of every leaf as the warm start of the next bracketed
- * thermal solve (par thermal_solver = 'bracketed'), computed on the device */
+ * thermal solve (par thermal_solver = 'bracketed'), computed on the device;
+ * the solve accepts a prediction whose net heating is below 1e-6 of heating
+ * plus cooling after that one evaluation (counted in
+ * mochii_metrics.warm_accepted), else brackets the root from it with a first
+ * step of 2.5 RMS errors of the network's training fit */
 int mochii_mlp_warm_start(mochii_ctx* ctx, mochii_mlp* m);
+/* The same warm start inside a batch's recorded iteration: each nebula's
+ * inference runs after its pass and the batched thermal launch starts from
+ * the predictions.  Needs the batched thermal solve (metals, the bracketed
+ * solver, cell_layout 'lane' or 'lockstep'); m must outlive the batch, and
+ * retraining m takes effect at the next iteration (the graph reads its
+ * weights where they lie). */
+int mochii_batch_set_warm_start(mochii_batch* b, mochii_mlp* m);
 
 #ifdef __cplusplus
 }

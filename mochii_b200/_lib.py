@@ -133,6 +133,7 @@ SIGNATURES = {
     "mochii_sobol_uniforms": (C.c_int, [C.c_int, C.c_int, C.c_int64, C.c_int64, C.c_int, C.c_void_p]),
     "mochii_philox_uniforms": (C.c_int, [C.c_int64, C.c_int, C.c_int64, C.c_int, C.c_int, C.c_void_p]),
     "mochii_batch_create": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p]),
+    "mochii_batch_set_warm_start": (C.c_int, [C.c_void_p, C.c_void_p]),
     "mochii_batch_iterate": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]),
     "mochii_batch_destroy": (None, [C.c_void_p]),
     "mochii_walk_leaves": (C.c_int, [C.c_void_p, C.c_int64, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]),

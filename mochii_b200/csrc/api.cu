@@ -544,6 +544,7 @@ struct mochii_batch {
     std::vector<double*> part;                      // 6 x balance blocks per nebula
     std::vector<unsigned long long*> bcount;        // 8 per nebula
     std::vector<uint64_t> gen;                      // each context's generation at mochii_batch_create
+    mochii_mlp* mlp = nullptr;                      // the learned warm start recorded in the graph
     std::string err;
 };
 
@@ -582,7 +583,11 @@ cudaError_t batch_record(mochii_batch* b, int solve_te, cudaGraphExec_t* out) {
     cudaError_t e = cudaStreamBeginCapture(b->s, cudaStreamCaptureModeThreadLocal);
     if (e != cudaSuccess) return e;
     const int n = (int)b->ctx.size();
-    for (int k = 0; k < n && e == cudaSuccess; ++k) e = batch_pass(b->ctx[k], b, k, b->s);
+    for (int k = 0; k < n && e == cudaSuccess; ++k) {
+        e = batch_pass(b->ctx[k], b, k, b->s);
+        // the learned warm start from this pass's rates (mochii_batch_set_warm_start)
+        if (e == cudaSuccess && b->mlp && solve_te) e = mlp_warm_start_enqueue(b->ctx[k], b->mlp, b->s);
+    }
     if (e == cudaSuccess) {
         if (solve_te && b->batched_thermal) {
             e = thermal_batch_enqueue(b->tb, b->ctx.data(), b->s);
@@ -773,6 +778,29 @@ extern "C" int mochii_batch_iterate(mochii_batch* b, int solve_te, mochii_pass_s
         }
     }
     return status;
+}
+
+extern "C" int mochii_batch_set_warm_start(mochii_batch* b, mochii_mlp* m) {
+    if (!b || !m) return MOCHII_ERR_BAD_PARAM;
+    if (!b->batched_thermal)
+        return fail(nullptr, MOCHII_ERR_UNSUPPORTED,
+                    "the batch warm start needs the batched thermal solve (metals, thermal_solver 'bracketed', "
+                    "cell_layout 'lane' or 'lockstep')");
+    const int n = (int)b->ctx.size();
+    double fac = 1.05;
+    int rc = mlp_batch_prepare(m, b->ctx.data(), n, &fac);
+    if (rc) return fail(nullptr, rc, "preparing the warm start for the batch");
+    std::vector<double> facs(n, fac);
+    cudaError_t e = thermal_batch_set_warm(b->tb, b->ctx.data(), facs.data(), 1.0e-6);
+    if (e != cudaSuccess) return fail(nullptr, MOCHII_ERR_CUDA, cudaGetErrorString(e));
+    for (int k = 0; k < n; ++k) b->gen[k] = b->ctx[k]->generation;   // the new warm-start arrays are the batch's own
+    for (cudaGraphExec_t& x : b->exec)   // recorded again, now with the inference
+        if (x) {
+            cudaGraphExecDestroy(x);
+            x = nullptr;
+        }
+    b->mlp = m;
+    return MOCHII_OK;
 }
 
 extern "C" void mochii_batch_destroy(mochii_batch* b) { batch_free(b); }

@@ -2334,6 +2334,7 @@ cudaError_t thermal_lane_setup(mochii_ctx* c) {
 
 // ---- batched nebulae --------------------------------------------------------
 struct ThermalBatch {
+    std::vector<ThArgs> h_args;             // host copy of d_args
     ThArgs* d_args = nullptr;
     long long* d_off = nullptr;
     unsigned long long* d_next = nullptr;   // lockstep: one chunk counter; lane: one leaf counter per nebula
@@ -2374,6 +2375,7 @@ void* thermal_batch_create(mochii_ctx* const* cs, int n, cudaError_t* err) {
     tb->lane = cs[0]->par.solver_warp == 3;
     if (*err == cudaSuccess) *err = cudaMalloc(&tb->d_next, sizeof(unsigned long long) * (tb->lane ? n : 1));
     if (*err == cudaSuccess) *err = cudaMemcpy(tb->d_args, args.data(), sizeof(ThArgs) * n, cudaMemcpyHostToDevice);
+    tb->h_args = args;
     if (*err == cudaSuccess) *err = cudaMemcpy(tb->d_off, off.data(), sizeof(long long) * (n + 1), cudaMemcpyHostToDevice);
     if (*err == cudaSuccess && tb->lane) {   // shared cache sized to the largest nebula's slots
         int nslot = 1, smem_max = 0, sms = 148;
@@ -2415,6 +2417,18 @@ void thermal_batch_destroy(void* p) {
     for (void* q : {(void*)tb->d_args, (void*)tb->d_off, (void*)tb->d_next})
         if (q) cudaFree(q);
     delete tb;
+}
+
+// The learned warm start in the batched thermal update: nebula k's solve
+// starts from cs[k]->twarm with the first step fac[k] and the residual gate.
+cudaError_t thermal_batch_set_warm(void* p, mochii_ctx* const* cs, const double* fac, double gate) {
+    auto* tb = static_cast<ThermalBatch*>(p);
+    for (int k = 0; k < tb->n; ++k) {
+        tb->h_args[k].Twarm = cs[k]->twarm;
+        tb->h_args[k].tfac0 = fac[k];
+        tb->h_args[k].gate = gate;
+    }
+    return cudaMemcpy(tb->d_args, tb->h_args.data(), sizeof(ThArgs) * tb->n, cudaMemcpyHostToDevice);
 }
 
 // One batched thermal update on stream s: each nebula's leaves sorted by

@@ -30,6 +30,7 @@ namespace mochii {
 namespace {
 
 constexpr int kIn = 16, kHid = 128, kOut = 4, kLayers = 4;
+constexpr double kMlpGate = 1.0e-6;   // residual gate of a warm start: |net| <= this x (heating + cooling)
 constexpr int kDim[kLayers + 1] = {kIn, kHid, kHid, kHid, kOut};
 
 // ---- BF16 tensor-core GEMM on the 5th-generation tensor cores ----------------
@@ -436,8 +437,8 @@ int ensure_batch(mochii_mlp* m, long long B) {
 }
 
 // Forward of B rows already in H[0]: Z/H of the hidden layers and the raw outputs.
-void forward(mochii_mlp* m, long long B) {
-    cudaStream_t s = m->stream;
+void forward(mochii_mlp* m, long long B, cudaStream_t s = nullptr) {
+    if (!s) s = m->stream;
     for (int l = 0; l < kLayers - 1; ++l)
         gemm<EPI_BIAS_GELU>(s, (int)B, kDim[l + 1], kDim[l], m->H[l], kDim[l], 1, m->W[l], 1, kDim[l], m->H[l + 1],
                             kDim[l + 1], m->b[l], m->Z[l + 1]);
@@ -704,6 +705,55 @@ extern "C" int mochii_mlp_features(mochii_ctx* c, float* out) {
                                                                                                 : MOCHII_ERR_CUDA;
 }
 
+namespace mochii {
+
+// The first bracketing step of a solve warm-started by m: 2.5 RMS errors of
+// its T_e prediction over the training set (within x1.002 .. x1.05).
+double mlp_step_factor(const mochii_mlp* m) {
+    const double band = m->t_rms_ln > 0.0 ? 2.5 * m->t_rms_ln : std::log(1.05);
+    return std::exp(std::min(std::max(band, std::log(1.002)), std::log(1.05)));
+}
+
+// The warm start of nebula c enqueued on stream s without a host
+// synchronisation (for a recorded batch graph): features, inference and the
+// predicted T_e into c->twarm, in chunks through m's activation buffers
+// (sized by mlp_batch_prepare).
+cudaError_t mlp_warm_start_enqueue(mochii_ctx* c, mochii_mlp* m, cudaStream_t s) {
+    const long long n = c->grid.nleaf;
+    const long long chunk = std::min<long long>(m->cap, 1 << 20);
+    for (long long i0 = 0; i0 < n; i0 += chunk) {
+        const long long k = std::min<long long>(chunk, n - i0);
+        k_features<<<nb(k, 256), 256, 0, s>>>(k, n, c->rates + i0, c->nH + i0, c->xHI + i0, c->xHeI + i0,
+                                              c->xHeII + i0, c->Te + i0, m->H[0]);
+        forward(m, k, s);
+        k_predict<<<nb(k, 256), 256, 0, s>>>(k, m->out, m->H[0], nullptr, c->twarm + i0, c->par.te_min, c->par.te_max);
+    }
+    return cudaGetLastError();
+}
+
+// Before recording: m's buffers hold a chunk of the largest nebula, the GEMM
+// kernels' shared-memory attribute is set, and every nebula has its
+// warm-start array; returns the first bracketing step in *fac.
+int mlp_batch_prepare(mochii_mlp* m, mochii_ctx* const* cs, int n, double* fac) {
+    long long nmax = 1;
+    for (int k = 0; k < n; ++k) nmax = std::max<long long>(nmax, cs[k]->grid.nleaf);
+    int rc = ensure_batch(m, std::min<long long>(nmax, 1 << 20));
+    if (rc) return rc;
+    forward(m, 1);   // the first launch of each GEMM variant sets its attribute (outside any capture)
+    MK(cudaStreamSynchronize(m->stream));
+    for (int k = 0; k < n; ++k) {
+        mochii_ctx* c = cs[k];
+        if (!c->twarm) {
+            ++c->generation;
+            if (cudaMalloc(&c->twarm, (size_t)c->grid.nleaf * 8 + 16) != cudaSuccess) return MOCHII_ERR_CUDA;
+        }
+    }
+    *fac = mlp_step_factor(m);
+    return MOCHII_OK;
+}
+
+}  // namespace mochii
+
 // The warm start of the next thermal update: features of every leaf from the
 // nebula's current rates and state, inference, and the predicted T_e (clamped
 // to [te_min, te_max]) as the bracketed solve's starting point.  All on the
@@ -730,12 +780,11 @@ extern "C" int mochii_mlp_warm_start(mochii_ctx* c, mochii_mlp* m) {
     MK(cudaStreamSynchronize(m->stream));
     MK(cudaGetLastError());
     c->twarm_set = true;
-    // the first bracketing step spans 2.5 RMS errors of the prediction
-    // (within x1.002 .. x1.05); the residual gate accepts a prediction whose
-    // net heating is below 1e-6 of heating plus cooling
-    const double band = m->t_rms_ln > 0.0 ? 2.5 * m->t_rms_ln : std::log(1.05);
-    c->twarm_fac = std::exp(std::min(std::max(band, std::log(1.002)), std::log(1.05)));
-    c->twarm_gate = 1.0e-6;
+    // the first bracketing step spans 2.5 RMS errors of the prediction; the
+    // residual gate accepts a prediction whose net heating is below 1e-6 of
+    // heating plus cooling
+    c->twarm_fac = mlp_step_factor(m);
+    c->twarm_gate = kMlpGate;
     if (int rc_tc = tc_check(m)) return rc_tc;
     return MOCHII_OK;
 }

@@ -313,6 +313,12 @@ class Batch:
         _check(self.lib, rc)
         self.h = h
 
+    def set_warm_start(self, mlp):
+        """Record the learned warm start (a trained WarmStartMLP) into the
+        batch's iteration: each nebula's inference after its pass."""
+        _check(self.lib, self.lib.mochii_batch_set_warm_start(self.h, mlp.h))
+        self.mlp = mlp
+
     def iterate(self, solve_te=True):
         """One iteration of every nebula: (pass statistics, balance metrics,
         device milliseconds of the whole batch)."""

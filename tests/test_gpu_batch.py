@@ -100,3 +100,39 @@ def test_batch_refuses_a_changed_context():
     batch.close()
     for neb in nebs:
         neb.close()
+
+
+def test_batch_with_learned_warm_start_equals_standalone():
+    """The learned warm start recorded into the batch iteration (each
+    nebula's inference after its pass, the batched thermal launch from the
+    predictions) solves each nebula as its own warm-started update does."""
+    from mochii_b200.mlp import WarmStartMLP
+    train = nebulae((12,), layout="lane")[0]
+    X, Y = [], []
+    for _ in range(3):
+        train.ionizing_field_and_rates()
+        X.append(WarmStartMLP.features(train))
+        train.gas_thermal_update()
+        Y.append(WarmStartMLP.targets(train, X[-1]))
+    train.close()
+    mlp = WarmStartMLP(seed=1)
+    mlp.train(np.concatenate(X), np.concatenate(Y), epochs=10, batch=512, lr=2e-3, seed=2)
+    sizes = (12, 16)
+    alone = nebulae(sizes, layout="lane")
+    together = nebulae(sizes, layout="lane")
+    batch = Batch(together)
+    batch.set_warm_start(mlp)
+    for it in range(2):
+        st, m, _ = batch.iterate()
+        for k, neb in enumerate(alone):
+            neb.ionizing_field_and_rates()
+            mlp.warm_start(neb)
+            neb.gas_thermal_update()
+            dT = np.abs(together[k].get("T_e") - neb.get("T_e"))
+            assert np.median(dT) < 1e-6 and dT.max() < 1.0, (it, k, dT.max())
+            assert m[k].warm_accepted == neb.last_metrics.warm_accepted
+            assert abs(m[k].rate_evaluations / neb.last_metrics.rate_evaluations - 1) < 0.01
+    batch.close()
+    for neb in alone + together:
+        neb.close()
+    mlp.close()
