@@ -67,9 +67,9 @@ def test_launch_count(bench):
     m = bench.Workload("hii_metals128", grid=16, packets=10_000_000)
     # 3 chunks of <= 4 Mi packets: keys + launch + walk each (coherent
     # order), rates, metal rates, balance, diffuse luminosities, one diffuse
-    # chunk, the opacity refresh of the start state
-    assert bench.launches_per_step(m, 1_000_000) == 3 * 3 + 2 + 2 + 2 + 1
-    assert bench.launches_per_step(m, 1_000_000, coherent=False) == 2 * 3 + 2 + 2 + 2 + 1
+    # chunk
+    assert bench.launches_per_step(m, 1_000_000) == 3 * 3 + 2 + 2 + 2
+    assert bench.launches_per_step(m, 1_000_000, coherent=False) == 2 * 3 + 2 + 2 + 2
 
 
 def test_prepared_state_is_a_developed_hii_region():
