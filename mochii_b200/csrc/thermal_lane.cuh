@@ -584,6 +584,10 @@ struct LaneLeaf {
     double xHI, xHeI, xHeII, ne;
     int passes, nsum, nev;
     TempSearch ts;
+    // the last two solved (ln T, ln n_e) of this leaf: the next trial's n_e
+    // root starts from their linear extrapolation
+    double lt1, ln1, lt2, ln2;
+    int ntr;
 };
 
 // Leaf number q of the work order (the most work first).
@@ -620,7 +624,7 @@ __device__ __forceinline__ void lane_claim(const ThArgs& a, unsigned long long* 
                     L.has = true;
                     L.xHI = L.x0; L.xHeI = L.h10; L.xHeII = L.h20;
                     L.ne = b.ne[il];
-                    L.passes = 0; L.nsum = 0; L.nev = 0;
+                    L.passes = 0; L.nsum = 0; L.nev = 0; L.ntr = 0;
                     L.ts.begin(a.Twarm ? a.Twarm[il] : L.T0, a.te_min, a.te_max, a.tfac0, a.Twarm ? a.gate : 0.0);
                 } else {
                     b.ne[il] = 0.0;
@@ -714,7 +718,14 @@ __device__ __noinline__ void lane_solve(const ThArgs& a, unsigned long long* nex
             cs.g1 = b.rates[n + L.il];
             cs.g2 = b.rates[2 * n + L.il];
             cs.nH = L.nH;
-            cs.begin(L.xHI, L.xHeI, L.xHeII, L.ne, b.nemax);
+            double ne0 = L.ne;   // the n_e root's first point
+            if (L.ntr >= 2 && L.lt1 != L.lt2 && L.ne > 0.0) {
+                const double lnT = log(T);
+                double d = (L.ln1 - L.ln2) / (L.lt1 - L.lt2) * (lnT - L.lt1);
+                d = fmin(fmax(d, -0.7), 0.7);   // within a factor of two of the last root
+                ne0 = exp(L.ln1 + d);
+            }
+            cs.begin(L.xHI, L.xHeI, L.xHeII, ne0, b.nemax);
             need = cs.settle();
         }
         int nsum = 0;
@@ -733,6 +744,11 @@ __device__ __noinline__ void lane_solve(const ThArgs& a, unsigned long long* nex
         if (ev) {
             L.passes += cs.nev;
             L.ne = cs.b;
+            if (L.ne > 0.0) {
+                L.lt2 = L.lt1; L.ln2 = L.ln1;
+                L.lt1 = log(T); L.ln1 = log(L.ne);
+                ++L.ntr;
+            }
             L.xHI = cs.eb.x;
             L.xHeI = cs.eb.h1;
             L.xHeII = cs.eb.h2;
