@@ -396,17 +396,26 @@ def prepared_state(n, front=0.7, width=1.0, he=True, T_in=8.0e3, T_out=3.0e3, nH
     return out
 
 
-def hii40(workdir, nphotons=40_000_000, niter=100, precision="fp32", level=6, rin_pc=0.97223, rout_pc=4.73154):
-    """The Lexington HII40 H II region (the reference's G2 gate input,
-    tests/g2_hii/hii40.in): a hollow uniform sphere of n_H = 100 between
-    rin_pc and rout_pc on a uniform octree of the given level spanning
-    +-rout_pc, a 40 kK blackbody with Q(H) = 4.26e49 s^-1 (luminosity
-    1.353758e39 erg/s over 13.598-100 eV, 32 bins), case B, thermal balance
-    in [3e3, 3e4] K with the Lexington metals (C, N, O, Ne, S: the reference
-    defaults), metal n_e and heating off, from an ionized start; iterated to
-    gas_tol = gas_tol_te = 5e-3 (at most niter).  The reference publishes
-    <T[NpNe]> = 8169 K for this case.  Writes the leaf list into workdir and
-    returns the namelist."""
+def hii40(workdir, nphotons=40_000_000, niter=100, precision="fp32", level=6, rin_pc=0.97223, rout_pc=4.73154,
+          production=False):
+    """The Lexington HII40 H II region: a hollow uniform sphere of n_H = 100
+    between rin_pc and rout_pc on a uniform octree of the given level
+    spanning +-rout_pc around a 40 kK blackbody (13.598-100 eV, 32 bins),
+    thermal balance in [3e3, 3e4] K with the Lexington metals (C, N, O, Ne,
+    S: the reference defaults), from an ionized start, at most niter
+    iterations.  Writes the leaf list into workdir and returns the namelist.
+
+    production=False: the reference's G2 gate input (tests/g2_hii/hii40.in):
+    Q(H) = 4.26e49 s^-1 (luminosity 1.353758e39 erg/s), case B on the spot,
+    metal n_e and heating off, gas_tol = gas_tol_te = 5e-3.
+
+    production=True: the reference's production input
+    (tests/continuous_energy/hii40_continuous.in), for which it publishes
+    <T[NpNe]> = 8169 K: luminosity 1.2734e39 erg/s, case A with the Milne
+    diffuse field, metal absorption, metal n_e and heating on, the volume
+    convergence criterion with gas_tol 5e-3 and gas_tol_te 1e-2, 2^25
+    packets by default.  The He I diffuse channel (hei_diffuse) is not part
+    of this path and is left out."""
     import numpy as np
     from . import amr
     os.makedirs(workdir, exist_ok=True)
@@ -421,8 +430,30 @@ def hii40(workdir, nphotons=40_000_000, niter=100, precision="fp32", level=6, ri
         x, y, z, lev, nH = amr.build_leaves(box, level, level, lambda *a: None, dens)
         amr.write_leaf_list(leaves + ".part", box, x, y, z, lev, nH)
         os.replace(leaves + ".part", leaves)
+    if production:
+        if nphotons == 40_000_000:
+            nphotons = 33_554_432
+        run = """ par%luminosity = 1.273400e39
+ par%conv_crit = 'vol'
+ par%gas_tol = 5.0e-3
+ par%gas_tol_te = 1.0e-2
+ par%case_ab = 'A'
+ par%diffuse_field = .true.
+ par%diffuse_energy_model = 'milne'
+ par%ion_metal_abs = .true.
+ par%metal_ne = .true.
+ par%metal_heat = .true.
+"""
+    else:
+        run = """ par%luminosity = 1.353758e39
+ par%gas_tol = 5.0e-3
+ par%gas_tol_te = 5.0e-3
+ par%case_ab = 'B'
+ par%metal_ne = .false.
+ par%metal_heat = .false.
+"""
     return f"""&parameters
- par%no_photons = {float(nphotons):.6e}
+ par%no_photons = {float(nphotons)!r}
  par%iseed = 1234
  par%launch_sequence = 'sobol'
  par%grid_type = 'amr'
@@ -433,23 +464,70 @@ def hii40(workdir, nphotons=40_000_000, niter=100, precision="fp32", level=6, ri
  par%eion_min = 13.598
  par%eion_max = 100.0
  par%tstar = 4.0e4
- par%luminosity = 1.353758e39
  par%xHI_init = 1.0e-3
  par%xHeI_init = 0.5
  par%xHeII_init = 0.5
  par%He_abund = 0.1
  par%ion_add_dust = .false.
  par%gas_niter = {niter}
- par%gas_tol = 5.0e-3
+ par%ion_relax = 1.0
+ par%solve_te = .true.
+ par%te_min = 3.0e3
+ par%te_max = 3.0e4
+ par%use_metals = .true.
+{run} par%atomic_dir = '{ATOMIC_DIR}'
+ par%precision = '{precision}'
+/
+"""
+
+
+def g2a(workdir, nphotons=40_000_000, niter=100, precision="fp32", level=6):
+    """The reference's G2a thermal gate input (tests/g2a_thermal/
+    g2a_thermal.in): a uniform n_H = 100 sphere of radius 4 pc (He/H 0.1) on
+    a uniform octree of the given level over an 8 pc box, a central 40 kK
+    blackbody with Q(H) = 1e49 s^-1 (luminosity 3.177837e38 erg/s over
+    13.598-100 eV, 32 bins), case B, H/He thermal balance in [3e3, 5e4] K
+    with no metals, from x_HI = 1e-3, He all He II and T_e = 1e4 K; iterated
+    to gas_tol = gas_tol_te = 2e-3 (at most niter).  Writes the leaf list
+    into workdir and returns the namelist."""
+    import numpy as np
+    from . import amr
+    os.makedirs(workdir, exist_ok=True)
+    leaves = os.path.join(workdir, f"sphere_L{level}_nH100.txt")
+    if not os.path.exists(leaves):
+        def dens(x, y, z, lev):
+            return np.where(np.sqrt(x * x + y * y + z * z) < 4.0, 100.0, 0.0)
+
+        x, y, z, lev, nH = amr.build_leaves(8.0, level, level, lambda *a: None, dens)
+        amr.write_leaf_list(leaves + ".part", 8.0, x, y, z, lev, nH)
+        os.replace(leaves + ".part", leaves)
+    return f"""&parameters
+ par%no_photons = {float(nphotons)!r}
+ par%iseed = 1234
+ par%launch_sequence = 'sobol'
+ par%grid_type = 'amr'
+ par%amr_file = '{leaves}'
+ par%dust_density_law = 'none'
+ par%distance_unit = 'pc'
+ par%nnu_ion = 32
+ par%eion_min = 13.598
+ par%eion_max = 100.0
+ par%tstar = 4.0e4
+ par%luminosity = 3.177837e38
+ par%xHI_init = 1.0e-3
+ par%xHeI_init = 0.0
+ par%xHeII_init = 1.0
+ par%He_abund = 0.1
+ par%ion_add_dust = .false.
+ par%gas_niter = {niter}
+ par%gas_tol = 2.0e-3
+ par%te_fixed = 1.0e4
  par%ion_relax = 1.0
  par%case_ab = 'B'
  par%solve_te = .true.
  par%te_min = 3.0e3
- par%te_max = 3.0e4
- par%gas_tol_te = 5.0e-3
- par%use_metals = .true.
- par%metal_ne = .false.
- par%metal_heat = .false.
+ par%te_max = 5.0e4
+ par%gas_tol_te = 2.0e-3
  par%atomic_dir = '{ATOMIC_DIR}'
  par%precision = '{precision}'
 /

@@ -220,8 +220,23 @@ __device__ __forceinline__ void tally_add(float2* p, float v) {
 }
 __device__ __forceinline__ void tally_add(double* p, double v) { atomicAdd(p, v); }
 
-__device__ __forceinline__ float attenuation(float x) { return expf(-x); }
-__device__ __forceinline__ double attenuation(double x) { return exp(-x); }
+// Path weight of one segment of optical depth ks > 0 and the attenuation
+// after it: (expo - expo e^-ks) / kap (raytrace_amr.f90:462).  In FP32 the
+// difference of two attenuations keeps only about ulp/ks of relative
+// precision on a thin segment, so below ks = 1/4 the absorbed fraction comes
+// from expm1f; FP64 keeps the reference's own difference.
+__device__ __forceinline__ float segment_weight(float& expo, float ks, float kap) {
+    const float eo = expo * expf(-ks);
+    const float w = (ks < 0.25f ? -expo * expm1f(-ks) : expo - eo) / kap;
+    expo = eo;
+    return w;
+}
+__device__ __forceinline__ double segment_weight(double& expo, double ks, double kap) {
+    const double eo = expo * exp(-ks);
+    const double w = (expo - eo) / kap;
+    expo = eo;
+    return w;
+}
 
 
 template <typename R, int NABS>
@@ -902,9 +917,7 @@ __global__ void __launch_bounds__(128) k_walk_edge(const PassArgs a, const Packe
             const R ks = kap * (R)sgm[0];
             R w;
             if (ks > (R)0) {
-                const R eo = expo * attenuation(ks);
-                w = (expo - eo) / kap;
-                expo = eo;
+                w = segment_weight(expo, ks, kap);
             } else {
                 w = expo * (R)sgm[0];
             }
@@ -1082,9 +1095,7 @@ __global__ void __launch_bounds__(128) k_walk_coh(const PassArgs a, const Packet
                     }
                     const R ks = kap * (R)sgm[0];
                     if (ks > (R)0) {
-                        const R eo = expo * attenuation(ks);
-                        w = (expo - eo) / kap;
-                        expo = eo;
+                        w = segment_weight(expo, ks, kap);
                     } else {
                         w = expo * (R)sgm[0];
                     }
@@ -1232,9 +1243,7 @@ __global__ void __launch_bounds__(128) k_walk_amr(const PassArgs a, const Packet
             const R ks = kap * (R)texit;
             R w;
             if (ks > (R)0) {
-                const R eo = expo * attenuation(ks);
-                w = (expo - eo) / kap;
-                expo = eo;
+                w = segment_weight(expo, ks, kap);
             } else {
                 w = expo * (R)texit;
             }

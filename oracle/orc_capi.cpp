@@ -515,4 +515,25 @@ void orc_solve_ion_cell(int recomb_model, double yHe, double gH, double gHe1, do
     solve_ion_cell(m, yHe, gH, gHe1, gHe2, nH, T, caseA != 0, x3[0], x3[1], x3[2], *ne);
 }
 
+
+// The 1D thermal reference of the G2a gate (check_g2a.py:150-207) with the
+// H I line-cooling fit of atomic_dir/cooling_h_1.txt and no n-level
+// suppression.  cfg10 = nnu, emin, emax, tstar, lband, nH, yHe, rsph_pc,
+// te_min, te_max; out5 = r_pc, x_HI, x_HeI, x_HeII, T_e, each nr long.
+int orc_thermal_1d(const char* atomic_dir, const double* cfg10, int nr, int nsweep, double* out5) {
+    Thermal th;
+    th.gff.build();
+    if (!th.hi_fit.load(std::string(atomic_dir) + "/cooling_h_1.txt")) {
+        g_err = std::string("cannot open ") + atomic_dir + "/cooling_h_1.txt";
+        return 1;
+    }
+    th.use_hi_table = false;
+    Sphere1D s;
+    s.nnu = (int)cfg10[0]; s.emin = cfg10[1]; s.emax = cfg10[2]; s.tstar = cfg10[3]; s.lband = cfg10[4];
+    s.nH = cfg10[5]; s.yHe = cfg10[6]; s.rsph_pc = cfg10[7]; s.te_min = cfg10[8]; s.te_max = cfg10[9];
+    const RateModel rm;
+    return thermal_1d(th, rm, s, nr, nsweep, out5, out5 + nr, out5 + 2 * (size_t)nr, out5 + 3 * (size_t)nr,
+                      out5 + 4 * (size_t)nr);
+}
+
 }  // extern "C"

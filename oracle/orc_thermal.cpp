@@ -400,3 +400,123 @@ double cooling_total(const Thermal& th, const RateModel& rm, bool caseA, double 
 }
 
 }  // namespace orc
+
+namespace orc {
+
+namespace {
+
+struct Bins1D {
+    std::vector<double> ec, lum, sH, sHe1, sHe2;
+};
+
+// band_bins (check_g2a.py:94-103): geometric bin centres of nnu log-spaced
+// bins, the Planck photon-energy shape integrated with 32 midpoint samples
+// per bin, normalised to the band luminosity.
+Bins1D band_bins_1d(const Sphere1D& s) {
+    Bins1D b;
+    const int n = s.nnu;
+    std::vector<double> edge(n + 1);
+    for (int i = 0; i <= n; ++i)
+        edge[i] = std::exp(std::log(s.emin) + (std::log(s.emax) - std::log(s.emin)) * (double)i / (double)n);
+    double tot = 0.0;
+    for (int i = 0; i < n; ++i) {
+        b.ec.push_back(std::sqrt(edge[i] * edge[i + 1]));
+        const double w = edge[i + 1] - edge[i];
+        double acc = 0.0;
+        for (int k = 0; k < 32; ++k) {
+            const double e = edge[i] + w * ((double)k + 0.5) / 32.0;
+            acc += e * e * e / std::expm1(e * EV2ERG / (KBOLTZ_CGS * s.tstar));
+        }
+        b.lum.push_back(acc * w / 32.0);
+        tot += b.lum.back();
+    }
+    for (int i = 0; i < n; ++i) {
+        b.lum[i] *= s.lband / tot;
+        b.sH.push_back(sigma_HI(b.ec[i]));
+        b.sHe1.push_back(sigma_HeI(b.ec[i]));
+        b.sHe2.push_back(sigma_HeII(b.ec[i]));
+    }
+    return b;
+}
+
+struct Rates1D {
+    double gH, gHe1, gHe2, hH, hHe1, hHe2;
+};
+
+// net_rate (check_g2a.py:144-147): the ionization solved at T from the
+// shell's state xs, heating from the attenuated fluxes minus cooling_total.
+double net_1d(const Thermal& th, const RateModel& rm, const Sphere1D& s, const Rates1D& q, double T,
+              const double xs[3], double out[3]) {
+    double xHI = xs[0], xHeI = xs[1], xHeII = xs[2], ne = 0.0;
+    solve_ion_cell(rm, s.yHe, q.gH, q.gHe1, q.gHe2, s.nH, T, false, xHI, xHeI, xHeII, ne);
+    out[0] = xHI; out[1] = xHeI; out[2] = xHeII;
+    const double heat = s.nH * (xHI * q.hH + s.yHe * (xHeI * q.hHe1 + xHeII * q.hHe2));
+    return heat - cooling_total(th, rm, false, s.yHe, T, s.nH, ne, xHI, xHeI, xHeII);
+}
+
+}  // namespace
+
+// reference_1d, check_g2a.py:150-207.
+int thermal_1d(const Thermal& th, const RateModel& rm, const Sphere1D& s, int nr, int nsweep, double* r_pc,
+               double* xHI, double* xHeI, double* xHeII, double* Te) {
+    if (nr < 1 || nsweep < 1 || s.nnu < 1) return 1;
+    const Bins1D b = band_bins_1d(s);
+    const int nb = s.nnu;
+    const double dr_pc = s.rsph_pc / (double)nr, dr_cm = dr_pc * PC2CM;
+    for (int i = 0; i < nr; ++i) {
+        r_pc[i] = ((double)i + 0.5) * dr_pc;
+        xHI[i] = 1.0e-3; xHeI[i] = 0.0; xHeII[i] = 1.0; Te[i] = 1.0e4;
+    }
+    std::vector<double> prev(nr), tau(nb), flux(nb);
+    for (int sweep = 0; sweep < nsweep; ++sweep) {
+        std::copy(Te, Te + nr, prev.begin());
+        std::fill(tau.begin(), tau.end(), 0.0);
+        for (int i = 0; i < nr; ++i) {
+            double xs[3] = {xHI[i], xHeI[i], xHeII[i]}, te = Te[i];
+            const double rc = r_pc[i] * PC2CM;
+            for (int pass = 0; pass < 2; ++pass) {
+                Rates1D q = {0, 0, 0, 0, 0, 0};
+                for (int k = 0; k < nb; ++k) {
+                    const double kap = s.nH * (xs[0] * b.sH[k] + s.yHe * (xs[1] * b.sHe1[k] + xs[2] * b.sHe2[k]));
+                    const double f = b.lum[k] * std::exp(-(tau[k] + 0.5 * kap * dr_cm)) / (4.0 * PI * rc * rc);
+                    const double hnu = b.ec[k] * EV2ERG;
+                    q.gH += f * b.sH[k] / hnu;
+                    q.gHe1 += f * b.sHe1[k] / hnu;
+                    q.gHe2 += f * b.sHe2[k] / hnu;
+                    q.hH += f * b.sH[k] * (1.0 - ETH_HI / b.ec[k]);
+                    q.hHe1 += f * b.sHe1[k] * (1.0 - ETH_HEI / b.ec[k]);
+                    q.hHe2 += f * b.sHe2[k] * (1.0 - ETH_HEII / b.ec[k]);
+                }
+                double tlo = s.te_min, thi = s.te_max, xlo[3], xhi[3], xm[3];
+                const double nlo = net_1d(th, rm, s, q, tlo, xs, xlo);
+                const double nhi = net_1d(th, rm, s, q, thi, xs, xhi);
+                if (nlo <= 0.0) {
+                    te = tlo;
+                    std::copy(xlo, xlo + 3, xs);
+                } else if (nhi >= 0.0) {
+                    te = thi;
+                    std::copy(xhi, xhi + 3, xs);
+                } else {
+                    for (int it = 0; it < 60; ++it) {
+                        const double tm = std::sqrt(tlo * thi);
+                        if (net_1d(th, rm, s, q, tm, xs, xm) > 0.0) tlo = tm;
+                        else thi = tm;
+                        if (thi / tlo - 1.0 < 1.0e-5) break;
+                    }
+                    te = std::sqrt(tlo * thi);
+                    net_1d(th, rm, s, q, te, xs, xm);
+                    std::copy(xm, xm + 3, xs);
+                }
+            }
+            xHI[i] = xs[0]; xHeI[i] = xs[1]; xHeII[i] = xs[2]; Te[i] = te;
+            for (int k = 0; k < nb; ++k)
+                tau[k] += s.nH * (xs[0] * b.sH[k] + s.yHe * (xs[1] * b.sHe1[k] + xs[2] * b.sHe2[k])) * dr_cm;
+        }
+        double dmax = 0.0;
+        for (int i = 0; i < nr; ++i) dmax = std::max(dmax, std::fabs(Te[i] / prev[i] - 1.0));
+        if (dmax < 1.0e-6) break;
+    }
+    return 0;
+}
+
+}  // namespace orc

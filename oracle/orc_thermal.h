@@ -64,4 +64,19 @@ struct Thermal {
 double cooling_total(const Thermal& th, const RateModel& rm, bool caseA, double yHe, double T, double nH,
                      double ne, double xHI, double xHeI, double xHeII);
 
+// The 1D radial-marching thermal reference of the reference's G2a gate
+// (tests/g2a_thermal/check_g2a.py:94-207): a uniform H/He sphere around a
+// central blackbody, nr shells marched outward with the attenuated bin
+// fluxes, each shell's T_e bisected in ln T on heating = cooling (every
+// evaluation re-solving the ionization from the shell's state), two
+// self-shielding passes per shell, Gauss-Seidel sweeps until T_e moves by
+// less than 1e-6.
+struct Sphere1D {
+    int nnu = 32;
+    double emin = 13.598, emax = 100.0, tstar = 4.0e4, lband = 3.177837e38;
+    double nH = 100.0, yHe = 0.1, rsph_pc = 4.0, te_min = 3.0e3, te_max = 5.0e4;
+};
+int thermal_1d(const Thermal& th, const RateModel& rm, const Sphere1D& s, int nr, int nsweep, double* r_pc,
+               double* xHI, double* xHeI, double* xHeII, double* Te);
+
 }  // namespace orc

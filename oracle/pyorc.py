@@ -87,6 +87,7 @@ def load():
         "orc_sim_transport_pass_peel": (I, [V]),
         "orc_sim_peel_image": (LL, [V, I, V, LL, V]),
         "orc_sim_peel_observer": (I, [V, I, V]),
+        "orc_thermal_1d": (I, [C.c_char_p, V, I, I, V]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)
@@ -189,6 +190,18 @@ def solve_ion_cell(gH, gHe1, gHe2, nH, T, caseA, x3, yHe=0.1, model=0):
     load().orc_solve_ion_cell(model, yHe, gH, gHe1, gHe2, nH, T, int(caseA), x.ctypes.data, C.byref(ne))
     return x, ne.value
 
+
+
+def thermal_1d(atomic_dir, nr=8000, nsweep=4, nnu=32, emin=13.598, emax=100.0, tstar=4.0e4,
+               lband=3.177837e38, nH=100.0, yHe=0.1, rsph_pc=4.0, te_min=3.0e3, te_max=5.0e4):
+    """The G2a gate's 1D thermal reference (check_g2a.py:150-207): radii [pc]
+    and x_HI, x_HeI, x_HeII, T_e of nr shells of a uniform H/He sphere
+    around a central blackbody."""
+    cfg = np.array([nnu, emin, emax, tstar, lband, nH, yHe, rsph_pc, te_min, te_max], dtype=np.float64)
+    out = np.zeros((5, nr))
+    if load().orc_thermal_1d(str(atomic_dir).encode(), cfg.ctypes.data, int(nr), int(nsweep), out.ctypes.data):
+        raise RuntimeError(load().orc_last_error().decode())
+    return out
 
 
 def philox(seed, stream, packet, n0, n):

@@ -15,6 +15,11 @@ committed, so the tests never read the reference tree at run time.
                    free-free Gaunt values from tools/python/mochii_rates.py,
                    which tests/rates/check_python_rates.py pins to the Fortran
                    recomb_mod / photo_xsec / cooling_mod at 1e-10 relative.
+  g2a_1d_golden.npz The 1D thermal reference of the G2a gate
+                   (tests/g2a_thermal/check_g2a.py reference_1d) on 400
+                   shells: its definitions are executed from the checkout's
+                   own file (h5py stubbed, since only the run's output needs
+                   it) and reference_1d(nr=400) is recorded.
 """
 import os
 import sys
@@ -84,6 +89,26 @@ def make_rates():
     print("rates_golden.npz:", sorted(out))
 
 
+def make_g2a(nr=400):
+    import types
+    d = os.path.join(REF, "tests", "g2a_thermal")
+    path = os.path.join(d, "check_g2a.py")
+    src = open(path).read()
+    src = src[:src.rindex("\n", 0, src.index(" main --"))]   # the definitions, not the run's check
+    sys.modules.setdefault("h5py", types.ModuleType("h5py"))
+    cwd = os.getcwd()
+    os.chdir(d)
+    try:
+        ns = {"__file__": path, "__name__": "check_g2a_defs"}
+        exec(compile(src, path, "exec"), ns)
+        r, xHI, xHeI, xHeII, Te = ns["reference_1d"](nr=nr)
+    finally:
+        os.chdir(cwd)
+    np.savez_compressed(os.path.join(HERE, "g2a_1d_golden.npz"), r=r, xHI=xHI, xHeI=xHeI, xHeII=xHeII, Te=Te)
+    print("g2a_1d_golden.npz: nr =", nr, "Te range", Te.min(), Te.max())
+
+
 if __name__ == "__main__":
     make_qmc()
     make_rates()
+    make_g2a()

@@ -13,12 +13,13 @@ from mochii_b200 import Batch, Nebula, MochiiError, configs, parse_namelist
 pytestmark = pytest.mark.gpu
 
 
-def nebulae(sizes, solve_te=True, layout="lockstep"):
+def nebulae(sizes, solve_te=True, layout="lockstep", solver=None):
     out = []
     for k, n in enumerate(sizes):
         nl = configs.hii_metals(nphotons=30000 + 10000 * k, niter=3, n=n, precision="fp64", rs_factor=1.2 + 0.1 * k,
                                 diffuse=False, solve_te=solve_te)
-        out.append(Nebula(parse_namelist(nl.replace("/\n", f" par%cell_layout = '{layout}'\n/\n"))))
+        extra = f" par%cell_layout = '{layout}'\n" + (f" par%thermal_solver = '{solver}'\n" if solver else "")
+        out.append(Nebula(parse_namelist(nl.replace("/\n", extra + "/\n"))))
     return out
 
 
@@ -107,7 +108,7 @@ def test_batch_with_learned_warm_start_equals_standalone():
     nebula's inference after its pass, the batched thermal launch from the
     predictions) solves each nebula as its own warm-started update does."""
     from mochii_b200.mlp import WarmStartMLP
-    train = nebulae((12,), layout="lane")[0]
+    train = nebulae((12,), layout="lane", solver="bracketed")[0]
     X, Y = [], []
     for _ in range(3):
         train.ionizing_field_and_rates()
@@ -118,8 +119,8 @@ def test_batch_with_learned_warm_start_equals_standalone():
     mlp = WarmStartMLP(seed=1)
     mlp.train(np.concatenate(X), np.concatenate(Y), epochs=10, batch=512, lr=2e-3, seed=2)
     sizes = (12, 16)
-    alone = nebulae(sizes, layout="lane")
-    together = nebulae(sizes, layout="lane")
+    alone = nebulae(sizes, layout="lane", solver="bracketed")
+    together = nebulae(sizes, layout="lane", solver="bracketed")
     batch = Batch(together)
     batch.set_warm_start(mlp)
     for it in range(2):

@@ -32,9 +32,9 @@ def copy_inputs(neb, sim):
 
 
 def check_update(neb, sim, rng):
-    x = neb.get("x_HI")
-    front = np.flatnonzero(x < 0.99)
-    idx = np.unique(np.concatenate([front[::4], rng.choice(x.size, 20000, replace=False)]))
+    x, g = neb.get("x_HI"), neb.get("gamma_HI")
+    front = np.flatnonzero((x < 0.99) | (g > 0.0))   # the ionized region, its front and every lit leaf
+    idx = np.unique(np.concatenate([front[::max(4, front.size // 20000)], rng.choice(x.size, 20000, replace=False)]))
     copy_inputs(neb, sim)
     ref = sim.thermal_cells(idx)
     neb.gas_thermal_update()

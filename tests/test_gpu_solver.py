@@ -207,7 +207,7 @@ def test_autotune_picks_a_cell_tile_and_keeps_the_state():
     for k, v in st.items():
         neb.set(k, v)
     neb.gas_opacity_fill()
-    before = {f: neb.get(f) for f in ("x_HI", "T_e", "n_e")}
+    before = {f: neb.get(f) for f in ("x_HI", "x_HeI", "x_HeII", "T_e", "n_e")}
     t = neb.autotune(20000)
     assert t["lane_threads"] in (0, 192, 160, 128, 96) and t["thermal_ms"] > 0
     for f, v in before.items():

@@ -7,6 +7,8 @@ codes in tests/golden/qmc_golden.npz).  Samplers: the known answers of
 tests/energy_sampler/energy_sampler_dump.f90:22-37 and the tolerances of
 check_energy_sampler.py:59-168.  Rates: tools/python/mochii_rates.py, pinned
 to the Fortran at 1e-10 by tests/rates/check_python_rates.py:38-40.
+G2a 1D thermal reference: tests/g2a_thermal/check_g2a.py reference_1d,
+run from the reference's own file on 400 shells (g2a_1d_golden.npz).
 """
 import numpy as np
 import pytest
@@ -168,3 +170,19 @@ def test_hi_nlevel_cooling_low_density_limit_equals_fit(orc):
         lam = lib.orc_nlevel_cooling_at(os.path.join(d, "nlevel_h_1.txt").encode(), T, 1e-6)
         fit = np.sum(A[:, 0] * np.exp(-A[:, 1] / T)) / np.sqrt(T)
         assert abs(lam / fit - 1) < 6e-3, T
+
+
+def test_g2a_1d_thermal_reference_matches_reference_script(orc):
+    """The oracle's restatement of the G2a gate's 1D radial-marching thermal
+    reference against reference_1d(nr=400) of check_g2a.py: T_e equal, the
+    ion fractions within 1e-13."""
+    import os
+    from mochii_b200 import configs
+    g = np.load(os.path.join(os.path.dirname(__file__), "golden", "g2a_1d_golden.npz"))
+    o = orc.thermal_1d(configs.ATOMIC_DIR, nr=400)
+    np.testing.assert_array_equal(o[0], g["r"])
+    np.testing.assert_allclose(o[4], g["Te"], rtol=1e-12, atol=0)
+    for i, k in ((1, "xHI"), (2, "xHeI"), (3, "xHeII")):
+        np.testing.assert_allclose(o[i], g[k], rtol=0, atol=1e-13)
+    inside = o[0] < 2.5
+    assert 17e3 < o[4][inside].min() and o[4][inside].max() < 28e3   # the pure H/He overshoot
