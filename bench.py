@@ -460,6 +460,7 @@ def main():
     torch.cuda.synchronize()
     with ClockSampler(local) as clk:
         t_wall = time.perf_counter()
+        torch.cuda.nvtx.range_push("timed")   # ncu --nvtx --nvtx-include "timed/" selects these launches
         for k in range(args.steps):
             flush.zero_()
             torch.cuda.synchronize()
@@ -475,6 +476,7 @@ def main():
             nact.append(st.metal_active)
             npk.append(st.packets)
         torch.cuda.synchronize()
+        torch.cuda.nvtx.range_pop()
         t_wall = time.perf_counter() - t_wall
     # Each API call synchronises its own stream and reports the device time
     # (CUDA events on the library's stream) of its work: the pass (tally
@@ -835,7 +837,7 @@ def time_to_converged(n=64, nphot=1_000_000, iters=20, train_iters=10, seed_trai
     res = {}
     for mode in ("plain", "bracketed", "mlp"):
         neb = neb_of("bisection" if mode == "plain" else "bracketed", seed)
-        ms, evals, accepted, acc = 0.0, 0, 0, []
+        ms, evals, accepted, acc, werr = 0.0, 0, 0, [], []
         prev_T = None
         for it in range(1, iters + 1):
             st = neb.ionizing_field_and_rates()
@@ -852,17 +854,24 @@ def time_to_converged(n=64, nphot=1_000_000, iters=20, train_iters=10, seed_trai
                 e0 = time.perf_counter()
                 mlp.warm_start(neb)          # synchronous: device features + inference
                 ms += (time.perf_counter() - e0) * 1e3
+                t_warm, t_prev = neb.get("T_warm"), neb.get("T_e")   # untimed: the start-point diagnostics
             if it == iters:
                 prev_T = neb.get("T_e")
             neb.gas_thermal_update()
             ms += neb.last_metrics.kernel_ms
             evals += neb.last_metrics.rate_evaluations
             accepted += neb.last_metrics.warm_accepted
+            if mode == "mlp":   # RMS distance in ln T of the solved T_e from the two possible starts
+                t_new = neb.get("T_e")
+                inner = (t_new > neb.par.te_min * (1 + 1e-9)) & (t_new < neb.par.te_max * (1 - 1e-9)) & (neb.get("nH") > 0)
+                werr.append((float(np.sqrt(np.mean(np.log(t_new[inner] / t_warm[inner]) ** 2))),
+                             float(np.sqrt(np.mean(np.log(t_new[inner] / t_prev[inner]) ** 2))),
+                             neb.last_metrics.rate_evaluations))
             if check is not None:
                 dT, dx = check()
                 acc.append({"iteration": it, "leaves": int(idx.size), "max_dT_e_K": dT, "max_dx_HII": dx})
         res[mode] = dict(s=ms / 1e3, evals=evals, accepted=accepted, acc=acc, x=neb.get("x_HI"), T=neb.get("T_e"),
-                         last_change=np.abs(neb.get("T_e") - prev_T))
+                         last_change=np.abs(neb.get("T_e") - prev_T), werr=werr)
         neb.close()
     mlp.close()
 
@@ -883,6 +892,12 @@ def time_to_converged(n=64, nphot=1_000_000, iters=20, train_iters=10, seed_trai
             "speedup_mlp_vs_bracketed": res["bracketed"]["s"] / res["mlp"]["s"],
             "net_rate_evaluations": {k: int(v["evals"]) for k, v in res.items()},
             "mlp_gate_accepted_leaves": int(res["mlp"]["accepted"]),
+            "mlp_start_rms_ln": {"note": "per iteration: RMS over the solved leaves inside (te_min, te_max) of "
+                                         "ln(T_e / start) for the MLP's start and for the previous T_e, and the "
+                                         "update's net-rate evaluations",
+                                 "mlp_start": [round(w[0], 5) for w in res["mlp"]["werr"]],
+                                 "previous_T_e": [round(w[1], 5) for w in res["mlp"]["werr"]],
+                                 "evaluations": [int(w[2]) for w in res["mlp"]["werr"]]},
             "solve_vs_fp64_oracle": {"bars": {"T_e_K": 20.0, "x_HII": 1e-3}, "worst": worst,
                                      "per_check": {k: v["acc"] for k, v in res.items()}},
             "final_state_between_arms": {

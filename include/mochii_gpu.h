@@ -432,7 +432,10 @@ int mochii_mlp_features(mochii_ctx* ctx, float* out);
  * the solve accepts a prediction whose net heating is below 1e-6 of heating
  * plus cooling after that one evaluation (counted in
  * mochii_metrics.warm_accepted), else brackets the root from it with a first
- * step of 2.5 RMS errors of the network's training fit */
+ * step of 2.5 RMS errors of the prediction: the RMS of ln(T_e / T_warm) that
+ * the nebula's last learned warm start left (measured after that update), or
+ * the network's training fit before the first.  "T_warm" reads the
+ * predictions through mochii_get_field until the update consumes them. */
 int mochii_mlp_warm_start(mochii_ctx* ctx, mochii_mlp* m);
 /* The same warm start inside a batch's recorded iteration: each nebula's
  * inference runs after its pass and the batched thermal launch starts from

@@ -98,7 +98,7 @@ void release(mochii_ctx* c) {
                     c->th.gff, c->th.lamref, c->th.Ssup, c->th.tinv,
                     c->dif.ch, c->dif.tot, c->dif.scan_tmp, c->dif.tables,
                     (void*)c->metal.el, c->metal.egam, c->metal.eheat, c->metal.opac, c->metal.raw,
-                    (void*)c->metal.medge, c->metal.mom, c->twarm,
+                    (void*)c->metal.medge, c->metal.mom, c->twarm, c->twarm_err,
                     (void*)c->rec.E, c->rec.msig, c->oct_blob, c->rec.dsc, (void*)c->rec.p0,
                     (void*)c->dust_blob, (void*)c->rhokap, (void*)c->ttab, (void*)c->metal_lnl,
                     (void*)c->th.lnL, (void*)c->rec.key, (void*)c->rec.key_sorted, (void*)c->rec.seq,
@@ -920,15 +920,23 @@ extern "C" int mochii_balance_update(mochii_ctx* c, int solve_te, mochii_metrics
     CK(c, cudaEventRecord(c->ev0, c->stream));
     if (solve_te) CK(c, launch_thermal(c));
     else CK(c, launch_balance(c));
-    c->twarm_set = false;
     CK(c, cudaEventRecord(c->ev1, c->stream));
+    // how far the solved T_e landed from a learned warm start: the first
+    // bracketing step of the next one
+    const bool learned = solve_te && c->twarm_set && c->twarm_learned;
+    double werr[2] = {0.0, 0.0};
+    if (learned) CK(c, warm_error_launch(c));
+    c->twarm_set = false;
+    c->twarm_learned = false;
     c->columns_fresh = true;   // both kernels refresh the columns they change
     const int np = solve_te ? 6 : 3;
     std::vector<double> part((size_t)np * c->bw.blocks);
     unsigned long long cnt[8];
     CK(c, cudaMemcpyAsync(part.data(), c->bw.partial, part.size() * 8, cudaMemcpyDeviceToHost, c->stream));
     CK(c, cudaMemcpyAsync(cnt, c->bw.counters, sizeof(cnt), cudaMemcpyDeviceToHost, c->stream));
+    if (learned) CK(c, cudaMemcpyAsync(werr, c->twarm_err, sizeof(werr), cudaMemcpyDeviceToHost, c->stream));
     CK(c, cudaStreamSynchronize(c->stream));
+    if (learned && werr[1] >= 64.0) c->warm_err_ln = std::sqrt(werr[0] / werr[1]);
     float ms = 0.0f;
     cudaEventElapsedTime(&ms, c->ev0, c->ev1);
     mochii_metrics r;
@@ -1135,6 +1143,13 @@ extern "C" int mochii_get_field(mochii_ctx* c, const char* name, double* out, in
         std::memcpy(out, c->band.eedge.data(), n * 8);
         return MOCHII_OK;
     }
+    if (nm == "T_warm") {   // the warm start of the next bracketed thermal solve, as set or predicted
+        if (n != c->grid.nleaf) return fail(c, MOCHII_ERR_BAD_PARAM, "T_warm size mismatch");
+        if (!c->twarm_set) return fail(c, MOCHII_ERR_BAD_PARAM, "T_warm: no warm start is set");
+        CK(c, cudaMemcpyAsync(out, c->twarm, (size_t)n * 8, cudaMemcpyDeviceToHost, c->stream));
+        CK(c, cudaStreamSynchronize(c->stream));
+        return MOCHII_OK;
+    }
     if (nm == "leaf_half") {
         if (n != c->grid.nleaf) return fail(c, MOCHII_ERR_BAD_PARAM, "leaf_half size mismatch");
         if (c->oct.ncells > 0) std::memcpy(out, c->lhalf.data(), n * 8);
@@ -1193,6 +1208,7 @@ extern "C" int mochii_set_field(mochii_ctx* c, const char* name, const double* i
         CK(c, cudaMemcpyAsync(c->twarm, in, n * 8, cudaMemcpyHostToDevice, c->stream));
         c->twarm_fac = 1.05;   // a caller's warm start: the default first step, no gate
         c->twarm_gate = 0.0;
+        c->twarm_learned = false;
         CK(c, cudaStreamSynchronize(c->stream));
         c->twarm_set = true;
         return MOCHII_OK;

@@ -154,6 +154,9 @@ struct mochii_ctx {
     bool twarm_set = false;         // consumed by the next thermal update
     double twarm_fac = 1.05;        // first bracketing step from the warm start (learned: narrower)
     double twarm_gate = 0.0;        // residual gate of a learned warm start (0: none)
+    bool twarm_learned = false;     // the warm start came from mochii_mlp_warm_start
+    double* twarm_err = nullptr;    // device: sum of ln^2(T_e / T_warm) and its count after a learned start
+    double warm_err_ln = 0.0;       // RMS of ln(T_e / T_warm) of the last learned warm start (0: none yet)
     mochii::SpeciesHost species;
     bool thermal_ready = false;
     mochii::BalanceWork bw;

@@ -362,6 +362,30 @@ __global__ void k_predict(long long n, const float* __restrict__ out, const floa
 
 int nb(long long n, int t) { return (int)std::min<long long>((n + t - 1) / t, 148LL * 32); }
 
+// Sum of ln^2(T_e / T_warm) and its count over the gas leaves whose solved
+// T_e lies inside (te_min, te_max): how far the solve moved from a learned
+// warm start.
+__global__ void k_warm_error(long long n, const double* __restrict__ nH, const double* __restrict__ Te,
+                             const double* __restrict__ Tw, double te_min, double te_max, double* __restrict__ acc) {
+    double s = 0.0, c = 0.0;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const double t = Te[i];
+        if (nH[i] > 0.0 && t > te_min * (1.0 + 1e-9) && t < te_max * (1.0 - 1e-9)) {
+            const double d = log(t / Tw[i]);
+            s += d * d;
+            c += 1.0;
+        }
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        s += __shfl_down_sync(0xffffffffu, s, o);
+        c += __shfl_down_sync(0xffffffffu, c, o);
+    }
+    if ((threadIdx.x & 31) == 0 && c > 0.0) {
+        atomicAdd(acc, s);
+        atomicAdd(acc + 1, c);
+    }
+}
+
 }  // namespace
 }  // namespace mochii
 
@@ -708,10 +732,23 @@ extern "C" int mochii_mlp_features(mochii_ctx* c, float* out) {
 namespace mochii {
 
 // The first bracketing step of a solve warm-started by m: 2.5 RMS errors of
-// its T_e prediction over the training set (within x1.002 .. x1.05).
-double mlp_step_factor(const mochii_mlp* m) {
-    const double band = m->t_rms_ln > 0.0 ? 2.5 * m->t_rms_ln : std::log(1.05);
-    return std::exp(std::min(std::max(band, std::log(1.002)), std::log(1.05)));
+// its T_e prediction -- observed_ln, the RMS of ln(T_e / T_warm) that the
+// nebula's last learned warm start left, when there is one, else the RMS
+// over the training set -- within x1.002 .. x1.10.
+double mlp_step_factor(const mochii_mlp* m, double observed_ln) {
+    const double rms = observed_ln > 0.0 ? observed_ln : m->t_rms_ln;
+    const double band = rms > 0.0 ? 2.5 * rms : std::log(1.05);
+    return std::exp(std::min(std::max(band, std::log(1.002)), std::log(1.10)));
+}
+
+cudaError_t warm_error_launch(mochii_ctx* c) {
+    if (!c->twarm_err && cudaMalloc(&c->twarm_err, 2 * sizeof(double)) != cudaSuccess) return cudaGetLastError();
+    cudaError_t e = cudaMemsetAsync(c->twarm_err, 0, 2 * sizeof(double), c->stream);
+    if (e != cudaSuccess) return e;
+    const long long n = c->grid.nleaf;
+    k_warm_error<<<nb(n, 256), 256, 0, c->stream>>>(n, c->nH, c->Te, c->twarm, c->par.te_min, c->par.te_max,
+                                                    c->twarm_err);
+    return cudaGetLastError();
 }
 
 // The warm start of nebula c enqueued on stream s without a host
@@ -780,10 +817,12 @@ extern "C" int mochii_mlp_warm_start(mochii_ctx* c, mochii_mlp* m) {
     MK(cudaStreamSynchronize(m->stream));
     MK(cudaGetLastError());
     c->twarm_set = true;
-    // the first bracketing step spans 2.5 RMS errors of the prediction; the
-    // residual gate accepts a prediction whose net heating is below 1e-6 of
-    // heating plus cooling
-    c->twarm_fac = mlp_step_factor(m);
+    c->twarm_learned = true;
+    // the first bracketing step spans 2.5 RMS errors of the prediction (as
+    // the nebula's last learned warm start measured it, else the training
+    // fit's); the residual gate accepts a prediction whose net heating is
+    // below 1e-6 of heating plus cooling
+    c->twarm_fac = mlp_step_factor(m, c->warm_err_ln);
     c->twarm_gate = kMlpGate;
     if (int rc_tc = tc_check(m)) return rc_tc;
     return MOCHII_OK;

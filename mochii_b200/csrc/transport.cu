@@ -929,6 +929,9 @@ __global__ void __launch_bounds__(128) k_walk_edge(const PassArgs a, const Packe
             }
             tau = tau + (double)ks;
             if (tau >= kTauHuge) break;
+            if constexpr (!X && sizeof(R) == 4) {
+                if (expo == (R)0) break;   // FP32 attenuation underflowed: every later segment scores zero
+            }
             if (!more[0]) break;   // the scored cell was the last one inside the grid
 #pragma unroll
             for (int k = 0; k < LA; ++k) {
@@ -1100,7 +1103,8 @@ __global__ void __launch_bounds__(128) k_walk_coh(const PassArgs a, const Packet
                         w = expo * (R)sgm[0];
                     }
                     tau = tau + (double)ks;
-                    finish = tau >= kTauHuge || !more[0];
+                    // an FP32 attenuation that underflowed scores zero on every later segment
+                    finish = tau >= kTauHuge || !more[0] || (sizeof(R) == 4 && expo == (R)0);
                 }
             }
             // score_ion_path over the warp: one reduction per distinct key
@@ -1255,6 +1259,9 @@ __global__ void __launch_bounds__(128) k_walk_amr(const PassArgs a, const Packet
             }
             tau = tau + (double)ks;
             if (tau >= kTauHuge) break;
+            if constexpr (!X && sizeof(R) == 4) {
+                if (expo == (R)0) break;   // FP32 attenuation underflowed: every later segment scores zero
+            }
             x = x + texit * kx;
             y = y + texit * ky;
             z = z + texit * kz;

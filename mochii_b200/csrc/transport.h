@@ -41,7 +41,8 @@ void* thermal_batch_create(mochii_ctx* const* cs, int n, cudaError_t* err);
 void thermal_batch_destroy(void* tb);
 cudaError_t thermal_batch_enqueue(void* tb, mochii_ctx* const* cs, cudaStream_t s);
 cudaError_t thermal_batch_set_warm(void* tb, mochii_ctx* const* cs, const double* fac, double gate);
-double mlp_step_factor(const mochii_mlp* m);
+double mlp_step_factor(const mochii_mlp* m, double observed_ln = 0.0);
+cudaError_t warm_error_launch(mochii_ctx* c);
 int mlp_batch_prepare(mochii_mlp* m, mochii_ctx* const* cs, int n, double* fac);
 cudaError_t mlp_warm_start_enqueue(mochii_ctx* c, mochii_mlp* m, cudaStream_t s);
 

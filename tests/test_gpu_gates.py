@@ -44,6 +44,8 @@ def test_g2a_thermal_gate_against_1d_reference(tmp_path):
     ref = pyorc.thermal_1d(configs.ATOMIC_DIR)
     sel = (r > 0.3) & (r < 2.8) & (ne > 0)
     dev = te[sel] / np.interp(r[sel], ref[0], ref[4]) - 1.0
+    print(f"G2a: median |dev| {np.median(np.abs(dev)):.4%}, mean {dev.mean():+.4%}, "
+          f"{sel.sum()} leaves, {len(hist)} iterations")
     assert sel.sum() > 10000
     assert np.median(np.abs(dev)) < 0.01, (np.median(np.abs(dev)), dev.mean(), len(hist))
 
@@ -56,5 +58,6 @@ def test_hii40_production_mean_electron_temperature(tmp_path):
     w = (nH * (1.0 - x) * ne)[gas]
     t_mean = float(np.sum(T[gas] * w) / np.sum(w))
     neb.close()
+    print(f"HII40: <T[NpNe]> = {t_mean:.1f} K after {len(hist)} iterations")
     assert len(hist) >= 5
     assert abs(t_mean / 8169.0 - 1.0) < 0.015, (t_mean, len(hist), hist[-1])
