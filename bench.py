@@ -77,7 +77,8 @@ UNIT = "packets/s"
 # segments, FP64 tallies, FP32 moments), the stellar and diffuse walks of one
 # pass, 29.97 GB over 1.742e8 segments; scaled to the 128^3 pass by its
 # segment count (the traffic grows with the segments).
-DRAM_BYTES_PER_SEGMENT = {"hii_metals128": 172.1}
+DRAM_BYTES_PER_SEGMENT = {"hii_metals128": (172.1, "derived: DRAM bytes per scored segment of an ncu capture "
+                                                   "of the 96^3 case's walks, times this pass's segments")}
 
 
 class Workload:
@@ -455,6 +456,10 @@ def main():
 
     # ---- device-timed steps ---------------------------------------------
     pass_ms, kern_ms, bal_ms, segs, nact, npk, bcnt = [], [], [], [], [], [], []
+    # each timed step's start state, kept on the host (untimed) so that the
+    # end-to-end steps below redo exactly these steps from host buffers
+    fields = ("x_HI", "x_HeI", "x_HeII", "n_e", "T_e")
+    step_in = []
     if dist is not None:
         dist.barrier()
     torch.cuda.synchronize()
@@ -462,6 +467,7 @@ def main():
         t_wall = time.perf_counter()
         torch.cuda.nvtx.range_push("timed")   # ncu --nvtx --nvtx-include "timed/" selects these launches
         for k in range(args.steps):
+            step_in.append({f: neb.get(f) for f in fields})
             flush.zero_()
             torch.cuda.synchronize()
             st = neb.ionizing_field_and_rates()
@@ -496,11 +502,11 @@ def main():
 
     # ---- end-to-end through the C ABI with host buffers --------------------
     nleaf = neb.nleaf
-    # each step's inputs: the state after the timed steps (every field of it)
+    # step k's inputs: the start state of timed step k (every field of it)
     # from pinned host memory
-    src = {f: neb.get(f) for f in (("x_HI", "x_HeI", "x_HeII", "n_e", "T_e") if state0 is not None else ("x_HI", "T_e"))}
-    host_in = {f.encode(): torch.from_numpy(np.ascontiguousarray(v, dtype=np.float64)).pin_memory()
-               for f, v in src.items()}
+    host_in = [{f.encode(): torch.from_numpy(np.ascontiguousarray(v, dtype=np.float64)).pin_memory()
+                for f, v in src.items()} for src in step_in]
+    del step_in
     x_out = torch.empty(nleaf, dtype=torch.float64).pin_memory()
     t_out = torch.empty(nleaf, dtype=torch.float64).pin_memory()
     g_out = torch.empty(nleaf, dtype=torch.float64).pin_memory()
@@ -512,7 +518,7 @@ def main():
     e0 = time.perf_counter()
     for k in range(args.steps):
         rc = 0
-        for f, hb in host_in.items():
+        for f, hb in host_in[k].items():
             rc |= lib.mochii_set_field(ctx, f, hb.data_ptr(), nleaf)
         rc |= lib.mochii_opacity_fill(ctx)
         st = neb.ionizing_field_and_rates()
@@ -541,9 +547,10 @@ def main():
     mean_seg = float(np.mean(segs))
     mean_ms = float(np.mean(kern_ms))
     achieved = alg_bytes / (mean_ms * 1e-3) / 1e9
-    traffic = None
+    traffic, traffic_kind = None, None
     if DRAM_BYTES_PER_SEGMENT.get(wl.name) and prec == "fp32" and args.tally == "fp64":   # the captured configuration
-        traffic = DRAM_BYTES_PER_SEGMENT[wl.name] * mean_seg
+        b_, kind_ = DRAM_BYTES_PER_SEGMENT[wl.name]
+        traffic, traffic_kind = b_ * mean_seg, kind_
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -576,11 +583,14 @@ def main():
                                "solver": args.solver, "cell_layout": args.cell_layout, "tallies": args.tally,
                                "packet_order": neb_order(neb), "l2": "flushed between steps (256 MiB write)",
                                "tuning": tuning, "parallelism": "replicas" if world > 1 else "single"},
-            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 8 * len(host_in) * nleaf,
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 8 * len(fields) * nleaf,
                     "d2h_bytes_per_step": 24 * nleaf},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "peak_kind": peak_kind,
-                         "traffic": traffic, "kernel": "k_launch + k_walk_edge (transport pass)",
+                         "traffic": traffic, "traffic_kind": traffic_kind,
+                         "kernel": ("transport pass: k_coherent_keys, key sort, k_launch, k_walk_coh (stellar "
+                                    "chunks); k_launch_diffuse, k_walk_edge (diffuse chunks)"
+                                    if neb_order(neb) == "coherent" else "transport pass: k_launch + k_walk_edge"),
                          "bytes_per_segment": alg_bytes / mean_seg, "segments_per_launch": mean_seg,
                          "kernel_ms": mean_ms},
             "cpu_baseline": cpu,
@@ -642,12 +652,17 @@ def run_batch(args, wl, prec):
         batch.iterate()
 
     ms_steps, packets, segs, nact, bcnt = [], 0, [], [], []
+    # each timed step's start state of every instance, kept on the host
+    # (untimed) so that the end-to-end steps below redo exactly these steps
+    fields = ("x_HI", "x_HeI", "x_HeII", "n_e", "T_e")
+    step_in = []
     if dist is not None:
         dist.barrier()
     torch.cuda.synchronize()
     with ClockSampler(local) as clk:
         t_wall = time.perf_counter()
         for _ in range(args.steps):
+            step_in.append([{f: torch.from_numpy(neb.get(f)).pin_memory() for f in fields} for neb in nebs])
             flush.zero_()
             torch.cuda.synchronize()
             st, m, ms = batch.iterate()
@@ -669,22 +684,21 @@ def run_batch(args, wl, prec):
         packets = int(p.item())
     value = packets / (total_ms * 1e-3)
 
-    # ---- end-to-end: every instance's state up from pinned host buffers,
-    # the batch iteration, x_HI, T_e and Gamma_HI of every instance back
+    # ---- end-to-end: every instance's state of timed step k up from pinned
+    # host buffers, the batch iteration, x_HI, T_e and Gamma_HI of every
+    # instance back
     lib = nebs[0].lib
-    x_host = [torch.from_numpy(neb.get("x_HI")).pin_memory() for neb in nebs]
-    t_host = [torch.from_numpy(neb.get("T_e")).pin_memory() for neb in nebs]
     outs = [[torch.empty(n, dtype=torch.float64).pin_memory() for _ in range(3)] for n in nleaf]
     if dist is not None:
         dist.barrier()
     torch.cuda.synchronize()
     e_packets = 0
     e0 = time.perf_counter()
-    for _ in range(args.steps):
+    for k in range(args.steps):
         rc = 0
-        for neb, xh, th, n in zip(nebs, x_host, t_host, nleaf):
-            rc |= lib.mochii_set_field(neb.ctx, b"x_HI", xh.data_ptr(), n)
-            rc |= lib.mochii_set_field(neb.ctx, b"T_e", th.data_ptr(), n)
+        for neb, hin, n in zip(nebs, step_in[k], nleaf):
+            for f, hb in hin.items():
+                rc |= lib.mochii_set_field(neb.ctx, f.encode(), hb.data_ptr(), n)
             rc |= lib.mochii_opacity_fill(neb.ctx)
         st, _, _ = batch.iterate()
         e_packets += sum(s_.packets for s_ in st)
@@ -749,7 +763,7 @@ def run_batch(args, wl, prec):
                                             "launch)",
                                "tuning": f"walk shape autotuned per grid size ({len(tuned)} sizes)",
                                "parallelism": "replicas" if world > 1 else "single"},
-            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 16 * n_all,
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 8 * len(fields) * n_all,
                     "d2h_bytes_per_step": 24 * n_all},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "peak_kind": peak_kind, "traffic": None,

@@ -411,7 +411,8 @@ def hii40(workdir, nphotons=40_000_000, niter=100, precision="fp32", level=6, ri
 
     production=True: the reference's production input
     (tests/continuous_energy/hii40_continuous.in), for which it publishes
-    <T[NpNe]> = 8169 K: luminosity 1.2734e39 erg/s, case A with the Milne
+    <T[NpNe]> = 8169 K: luminosity 1.2734e39 erg/s, its Sobol scramble seed
+    (qmc_seed 20260728), case A with the Milne
     diffuse field, metal absorption, metal n_e and heating on, the volume
     convergence criterion with gas_tol 5e-3 and gas_tol_te 1e-2, 2^25
     packets by default.  The He I diffuse channel (hei_diffuse) is not part
@@ -434,6 +435,7 @@ def hii40(workdir, nphotons=40_000_000, niter=100, precision="fp32", level=6, ri
         if nphotons == 40_000_000:
             nphotons = 33_554_432
         run = """ par%luminosity = 1.273400e39
+ par%qmc_seed = 20260728
  par%conv_crit = 'vol'
  par%gas_tol = 5.0e-3
  par%gas_tol_te = 1.0e-2
