@@ -72,13 +72,20 @@ METRIC = "packets/s on 1 B200 (transport + balance iteration)"
 UNIT = "packets/s"
 
 
-# DRAM bytes (read + written) per scored segment of the transport kernels,
-# from the ncu captures summarised in profiles/: hii_metals at 96^3 (FP32
-# segments, FP64 tallies, FP32 moments), the stellar and diffuse walks of one
-# pass, 29.97 GB over 1.742e8 segments; scaled to the 128^3 pass by its
-# segment count (the traffic grows with the segments).
-DRAM_BYTES_PER_SEGMENT = {"hii_metals128": (172.1, "derived: DRAM bytes per scored segment of an ncu capture "
-                                                   "of the 96^3 case's walks, times this pass's segments")}
+# DRAM bytes (read + written) per scored segment of the transport pass (keys, sort, launch,
+# coherent walk, diffuse launch and walk) from the ncu launch list summarised
+# in profiles/walk_coh_hii96.md: hii_metals at 96^3 (FP32 segments, FP64
+# tallies, FP32 moments), 15.33 GB over 5.554e8 segments; scaled to the
+# 128^3 pass by its segment count.
+DRAM_BYTES_PER_SEGMENT = {"hii_metals128": (27.6, "derived: ncu DRAM bytes of the 96^3 case's transport-pass "
+                                                  "launches per scored segment, times this pass's segments")}
+
+
+# FP64 work of the thermal solve per net-rate evaluation: DADD + DMUL +
+# 2 DFMA thread instructions of the per-lane solve's 96^3 update (ncu,
+# profiles/thermal_lane_hii96.md), 69.9e9 FLOP over 1 659 987 evaluations.
+FP64_FLOP_PER_EVALUATION = 42100.0
+FP64_PEAK_TFLOPS = 148 * 64 * 2 * 1.965e9 / 1e12
 
 
 class Workload:
@@ -571,6 +578,14 @@ def main():
     bal_s = float(np.mean(bal_ms)) * 1e-3
     balance = {"cells_per_s": bm[0] / bal_s, "net_rate_evaluations_per_s": bm[1] / bal_s,
                "evaluations_per_cell": bm[1] / max(bm[0], 1.0), "kernel_ms": bal_s * 1e3}
+    if wl.name == "hii_metals128" and wl.thermal:
+        fl = FP64_FLOP_PER_EVALUATION * bm[1] / bal_s
+        balance["fp64"] = {"flop_per_evaluation": FP64_FLOP_PER_EVALUATION,
+                           "flop_source": "ncu DADD + DMUL + 2 DFMA thread instructions of one 96^3 update over its "
+                                          "counted evaluations",
+                           "achieved_tflops": fl / 1e12, "peak_tflops": FP64_PEAK_TFLOPS,
+                           "peak_kind": "nominal: 148 SMs x 64 FP64 FMA per clock x 2 x 1.965 GHz",
+                           "frac": fl / 1e12 / FP64_PEAK_TFLOPS}
 
     if rank == 0:
         line = {

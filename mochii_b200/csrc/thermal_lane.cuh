@@ -694,7 +694,8 @@ __device__ __noinline__ void lane_finish(const ThArgs& a, const LaneCache& cache
     L.has = false;
 }
 
-// The leaves of one nebula by one warp until its work order is exhausted.
+// The leaves of one nebula by the warps of one block until its work order is
+// exhausted (every thread of the block calls it).
 __device__ __noinline__ void lane_solve(const ThArgs& a, unsigned long long* next, const LaneCache& cache,
                                         ThermalAcc& acc, int lane) {
     const BalArgs& b = a.b;
@@ -707,7 +708,10 @@ __device__ __noinline__ void lane_solve(const ThArgs& a, unsigned long long* nex
     cs.with_cx = b.two_way;
     for (;;) {
         lane_claim(a, next, L, exhausted, lane);
-        if (!__any_sync(kFull, L.has)) return;
+        // every warp of the block takes the same trips, one barrier each: the
+        // block's warps stay at the same point of the solver's code, which
+        // then stays in the instruction cache
+        if (!__syncthreads_or(L.has ? 1 : 0)) return;
         const bool ev = L.has;   // every lane with a leaf evaluates its net rate at ts.t
         const double T = L.ts.t;
         bool need = false;
