@@ -179,6 +179,12 @@ typedef struct mochii_params {
     double alpha[MOCHII_MAX_OBS], beta[MOCHII_MAX_OBS], gamma[MOCHII_MAX_OBS];
     double obsx[MOCHII_MAX_OBS], obsy[MOCHII_MAX_OBS], obsz[MOCHII_MAX_OBS];
     double phase_angle[MOCHII_MAX_OBS], inclination_angle[MOCHII_MAX_OBS], position_angle[MOCHII_MAX_OBS];
+    /* par%hei_diffuse (define.f90:634): with the diffuse field, a fourth
+     * channel of He I excited-level recombination radiation -- the 2^3S and
+     * 584 A lines and the 2^1S two-photon continuum above the H I edge
+     * (diffuse_mod.f90:96-106, 274-284; hei_cascade_mod, hei_twophoton_mod),
+     * the two-photon shape read from <data_dir>/HeI2phot.dat */
+    int hei_diffuse;
 } mochii_params;
 
 /* Per-pass statistics (ion_score_report_energy_closure, ion_score_mod.f90:364-387). */

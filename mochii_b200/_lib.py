@@ -63,6 +63,7 @@ class Params(C.Structure):
         ("obsx", C.c_double * MAX_OBS), ("obsy", C.c_double * MAX_OBS), ("obsz", C.c_double * MAX_OBS),
         ("phase_angle", C.c_double * MAX_OBS), ("inclination_angle", C.c_double * MAX_OBS),
         ("position_angle", C.c_double * MAX_OBS),
+        ("hei_diffuse", C.c_int),
     ]
 
 

@@ -413,10 +413,9 @@ def hii40(workdir, nphotons=40_000_000, niter=100, precision="fp32", level=6, ri
     (tests/continuous_energy/hii40_continuous.in), for which it publishes
     <T[NpNe]> = 8169 K: luminosity 1.2734e39 erg/s, its Sobol scramble seed
     (qmc_seed 20260728), case A with the Milne
-    diffuse field, metal absorption, metal n_e and heating on, the volume
-    convergence criterion with gas_tol 5e-3 and gas_tol_te 1e-2, 2^25
-    packets by default.  The He I diffuse channel (hei_diffuse) is not part
-    of this path and is left out."""
+    diffuse field and its He I excited channel (hei_diffuse), metal
+    absorption, metal n_e and heating on, the volume convergence criterion
+    with gas_tol 5e-3 and gas_tol_te 1e-2, 2^25 packets by default."""
     import numpy as np
     from . import amr
     os.makedirs(workdir, exist_ok=True)
@@ -442,6 +441,7 @@ def hii40(workdir, nphotons=40_000_000, niter=100, precision="fp32", level=6, ri
  par%case_ab = 'A'
  par%diffuse_field = .true.
  par%diffuse_energy_model = 'milne'
+ par%hei_diffuse = .true.
  par%ion_metal_abs = .true.
  par%metal_ne = .true.
  par%metal_heat = .true.

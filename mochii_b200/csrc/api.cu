@@ -96,7 +96,7 @@ void release(mochii_ctx* c) {
                     c->bw.work, c->bw.work_sorted, c->bw.iota, c->bw.order, c->bw.sort_tmp, c->bw.next,
                     c->rec.tm, c->rec.td, c->rec.cell, c->rec.bits, c->rec.sig, c->rec.coef,
                     c->th.gff, c->th.lamref, c->th.Ssup, c->th.tinv,
-                    c->dif.ch, c->dif.tot, c->dif.scan_tmp, c->dif.tables,
+                    c->dif.ch, c->dif.tot, c->dif.scan_tmp, c->dif.tables, c->dif.he_tab,
                     (void*)c->metal.el, c->metal.egam, c->metal.eheat, c->metal.opac, c->metal.raw,
                     (void*)c->metal.medge, c->metal.mom, c->twarm, c->twarm_err,
                     (void*)c->rec.E, c->rec.msig, c->oct_blob, c->rec.dsc, (void*)c->rec.p0,
@@ -483,6 +483,25 @@ extern "C" int mochii_init(const mochii_params* pin, mochii_ctx** out) {
         c->dif.m.frac = q;
         c->dif.m.lgT0 = mh.lgT[0];
         c->dif.m.dlgT = mh.lgT[1] - mh.lgT[0];
+        if (p.hei_diffuse) {   // main.f90:107-112: the He I excited channel's two-photon table
+            std::string dir = p.data_dir;
+            if (dir.empty()) {   // the directory above the atomic tables (<data_dir>/atomic)
+                const std::string ad = atomic_dir(p);
+                const size_t k = ad.find_last_of('/');
+                dir = k == std::string::npos ? std::string(".") : ad.substr(0, k);
+            }
+            HeI2phHost hh;
+            if (!hei_2ph_build(dir + "/HeI2phot.dat", p.eion_max, hh)) {
+                c->last_error = "cannot read " + dir + "/HeI2phot.dat (par%data_dir)";
+                return bail(MOCHII_ERR_TABLE);
+            }
+            CKI(dalloc(&c->dif.he_tab, 2 * (size_t)kHe2phN));
+            CKI(cudaMemcpy(c->dif.he_tab, hh.cdf_e.data(), kHe2phN * 8, cudaMemcpyHostToDevice));
+            CKI(cudaMemcpy(c->dif.he_tab + kHe2phN, hh.grid_y.data(), kHe2phN * 8, cudaMemcpyHostToDevice));
+            c->dif.he.cdf_e = c->dif.he_tab;
+            c->dif.he.grid_y = c->dif.he_tab + kHe2phN;
+            c->dif.he.e_per_decay = hh.e_per_decay;
+        }
         CKI(dalloc(&c->dif.ch, 4 * (size_t)n));
         CKI(dalloc(&c->dif.tot, (size_t)n));
         c->dif.scan_bytes = diffuse_scan_bytes(n);

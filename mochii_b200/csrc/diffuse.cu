@@ -9,12 +9,16 @@
 // then draws leaf (binary search of the CDF), position in the leaf, isotropic
 // direction, channel and Milne energy from the 9-dimensional diffuse Sobol
 // stream (diffuse_mod.f90:221-296) and writes the same packet records as the
-// stellar launch, so the walk kernel is shared.
+// stellar launch, so the walk kernel is shared.  With par%hei_diffuse a
+// fourth channel carries the He I excited-level recombination radiation
+// (diffuse_mod.f90:96-106, 274-284): the 2^3S and 584 A lines and the 2^1S
+// two-photon continuum above the H I edge.
 #include <cub/cub.cuh>
 #include <cuda_runtime.h>
 
 #include <algorithm>
 #include <cmath>
+#include <cstdio>
 
 #include "ctx.h"
 #include "diffuse.h"
@@ -91,9 +95,104 @@ void milne_tables_build(double eion_max, MilneHost& m) {
     }
 }
 
+// ---- host: He I two-photon table (hei_twophoton_mod.f90:97-192) ------------
+// A(y) linearly interpolated between the tabulated points; its integral over
+// [0, 1] by Simpson panels per table interval (midpoints interpolated) is the
+// normalisation; on the in-band window [13.598, min(20.62, eion_max)] / 20.62
+// 1023 equal Simpson panels give the photons and energy per decay (two
+// photons per decay) and the CDF of the energy density y A(y).
+bool hei_2ph_build(const std::string& path, double eion_max, HeI2phHost& h) {
+    std::vector<double> ty, ta;
+    if (FILE* f = std::fopen(path.c_str(), "r")) {
+        double y, a;
+        while (std::fscanf(f, "%lf %lf", &y, &a) == 2) {
+            ty.push_back(y);
+            ta.push_back(a);
+        }
+        std::fclose(f);
+    }
+    const int n = (int)ty.size();
+    if (n < 4) return false;
+    auto shape = [&](double y) {
+        if (y <= ty[0] || y >= ty[n - 1]) return 0.0;
+        int i = 0;
+        while (i < n - 2 && ty[i + 1] < y) ++i;
+        return ta[i] + (ta[i + 1] - ta[i]) * (y - ty[i]) / (ty[i + 1] - ty[i]);
+    };
+    double tot = 0.0;
+    for (int i = 0; i < n - 1; ++i) {
+        const double ya = ty[i], yb = ty[i + 1];
+        tot = tot + (yb - ya) / 6.0 * (ta[i] + 4.0 * shape(0.5 * (ya + yb)) + ta[i + 1]);
+    }
+    if (tot <= 0.0) return false;
+    h.cdf_e.assign(kHe2phN, 1.0);
+    h.grid_y.assign(kHe2phN, 0.0);
+    const double y_lo = kEthHI / kHe2phEtot, y_hi = std::min(kHe2phEtot, eion_max) / kHe2phEtot;
+    if (y_hi <= y_lo) {
+        h.n_per_decay = h.e_per_decay = 0.0;
+        for (double& g : h.grid_y) g = y_lo;
+        return true;
+    }
+    double an = 0.0, ae = 0.0, seg = 0.0;
+    h.grid_y[0] = y_lo;
+    h.cdf_e[0] = 0.0;
+    for (int i = 1; i < kHe2phN; ++i) {
+        const double ya = y_lo + (y_hi - y_lo) * (double)(i - 1) / (double)(kHe2phN - 1);
+        const double yb = y_lo + (y_hi - y_lo) * (double)i / (double)(kHe2phN - 1);
+        const double ym = 0.5 * (ya + yb);
+        const double fa = shape(ya), fm = shape(ym), fb = shape(yb);
+        const double w = (fa * ya + 4.0 * fm * ym + fb * yb);
+        an = an + (yb - ya) / 6.0 * (fa + 4.0 * fm + fb);
+        ae = ae + (yb - ya) / 6.0 * w * kHe2phEtot;
+        seg = seg + (yb - ya) / 6.0 * w;
+        h.grid_y[i] = yb;
+        h.cdf_e[i] = seg;
+    }
+    h.n_per_decay = 2.0 * an / tot;
+    h.e_per_decay = 2.0 * ae / tot;
+    for (double& c : h.cdf_e) c = seg > 0.0 ? c / seg : 1.0;
+    h.cdf_e[kHe2phN - 1] = 1.0;
+    return true;
+}
+
 namespace {
 
 constexpr int kThreads = 256;
+
+// hei_branch_energies (diffuse_mod.f90:308-325 with hei_cascade_mod.f90): the
+// in-band energy per case-B He II recombination through the 2^3S line
+// (19.82 eV), the 584 A line when its trapped photon ionizes hydrogen
+// (21.22 eV; escape closure p = 1 / (1 + 77 x(He0) / (sqrt(T) x(H0)))), and
+// the two-photon continuum of 2^1S and of the 2^1P decays converted to it.
+// Branch fractions from the Benjamin, Skillman & Smits (1999) effective
+// coefficients normalised by their sum, T clamped to [3e3, 2e4] K.
+__device__ __forceinline__ void hei_branches(const HeI2phDev& h, double T, double xHI, double xHeI, double& e3s,
+                                             double& e1p, double& e1s) {
+    const double Tc = fmin(fmax(T, 3.0e3), 2.0e4) / 1.0e4;
+    const double a3 = 2.10e-13 * pow(Tc, -0.381);
+    const double a1s = 2.06e-14 * pow(Tc, -0.451);
+    const double a1p = 4.17e-14 * pow(Tc, -0.695);
+    const double sum = a3 + a1s + a1p;
+    const double f3s = a3 / sum, f1s = a1s / sum, f1p = a1p / sum;
+    const double p584 = 1.0 / (1.0 + 77.0 / sqrt(fmax(T, kTinest)) * fmax(xHeI, 0.0) / fmax(xHI, kTinest));
+    e3s = f3s * 19.82;
+    e1p = f1p * p584 * 21.22;
+    e1s = (f1s + f1p * (1.0 - p584)) * h.e_per_decay;
+}
+
+// hei_2ph_sample_energy (hei_twophoton_mod.f90:199-219): bisection of the
+// energy CDF and linear interpolation within the bracket.
+__device__ double hei_2ph_sample(const HeI2phDev& h, double u) {
+    const double uu = fmin(fmax(u, 0.0), 1.0);
+    int lo = 0, hi = kHe2phN - 1;
+    while (hi - lo > 1) {
+        const int mid = (lo + hi + 2) / 2 - 1;
+        if (uu > h.cdf_e[mid]) lo = mid; else hi = mid;
+    }
+    const double cl = h.cdf_e[lo], ch = h.cdf_e[hi];
+    const double y = ch > cl ? h.grid_y[lo] + (h.grid_y[hi] - h.grid_y[lo]) * (uu - cl) / (ch - cl) : h.grid_y[lo];
+    return y * kHe2phEtot;
+}
 
 struct DiffArgs {
     const double* nH;
@@ -105,11 +204,13 @@ struct DiffArgs {
     double* ch;        // 4 x nleaf (channel luminosities, leaf-major)
     double* tot;       // nleaf leaf totals, then their inclusive prefix sum
     MilneDev m;
+    HeI2phDev he;
     const double4* lg;   // octree leaf geometry (per-leaf volume), null on the Cartesian grid
     long long nleaf;
     double yHe, vol, d2cm, eion_max;
     RateSel rs;
     int energy_model;  // 0 milne, 1 exponential, 2 threshold
+    int hei;           // the He I excited channel (par%hei_diffuse)
 };
 
 // milne_tbracket (:286-297): it is 1-based as in the reference.
@@ -155,7 +256,7 @@ __device__ double milne_sample(const MilneDev& m, int ich, double T, double u, d
 __global__ void k_diffuse_lum(const DiffArgs a) {
     for (long long il = (long long)blockIdx.x * blockDim.x + threadIdx.x; il < a.nleaf;
          il += (long long)gridDim.x * blockDim.x) {
-        double c0 = 0.0, c1 = 0.0, c2 = 0.0;
+        double c0 = 0.0, c1 = 0.0, c2 = 0.0, c3 = 0.0;
         const double nH = a.nH[il];
         if (nH > 0.0) {
             const double T = a.Te[il], ne = a.ne[il];
@@ -182,12 +283,17 @@ __global__ void k_diffuse_lum(const DiffArgs a) {
             c0 = ne * nHII * (alphaA_HII(a.rs, T) - alphaB_HII(a.rs, T)) * e0 * kEv2erg * vol;
             c1 = ne * nHeII * (alphaA_HeII(a.rs, T) - alphaB_HeII(a.rs, T)) * e1 * kEv2erg * vol;
             c2 = ne * nHeIII * (alphaA_HeIII(a.rs, T) - alphaB_HeIII(a.rs, T)) * e2 * kEv2erg * vol;
+            if (a.hei) {   // channel 4: every case-B He II recombination through the n = 2 cascade
+                double e3s, e1p, e1s;
+                hei_branches(a.he, T, a.xHI[il], a.xHeI[il], e3s, e1p, e1s);
+                c3 = ne * nHeII * alphaB_HeII(a.rs, T) * vol * kEv2erg * ((e3s + e1p) + e1s);
+            }
         }
         a.ch[4 * il + 0] = c0;
         a.ch[4 * il + 1] = c1;
         a.ch[4 * il + 2] = c2;
-        a.ch[4 * il + 3] = 0.0;
-        a.tot[il] = ((c0 + c1) + c2) + 0.0;
+        a.ch[4 * il + 3] = c3;
+        a.tot[il] = ((c0 + c1) + c2) + c3;
     }
 }
 
@@ -196,8 +302,11 @@ struct DiffLaunchArgs {
     const double* cum;     // inclusive prefix sum of the leaf totals
     const double* ch;
     const double* Te;
+    const double* xHI;
+    const double* xHeI;
     const double* eedge;
     MilneDev m;
+    HeI2phDev he;
     MetalDev metal;
     const double4* lg;   // octree leaf geometry, null on the Cartesian grid
     DustDev dust;        // grain optics; dust.n == 0 without
@@ -222,9 +331,9 @@ __global__ void __launch_bounds__(kThreads) k_launch_diffuse(const DiffLaunchArg
     const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const uint64_t ip = (uint64_t)(ip0 + i);
-    double u[8];
+    double u[9];
 #pragma unroll
-    for (int d = 0; d < 8; ++d) u[d] = qmc_uniform(sq, ip, d, 1);
+    for (int d = 0; d < 9; ++d) u[d] = qmc_uniform(sq, ip, d, 1);
     // first leaf whose normalised CDF reaches u1
     long long lo = 1, hi = a.nleaf;
     while (lo < hi) {
@@ -264,6 +373,13 @@ __global__ void __launch_bounds__(kThreads) k_launch_diffuse(const DiffLaunchArg
         if (a.energy_model == 0) eph = milne_sample(a.m, ch, T, u[7], eph, a.eion_max);
         else if (a.energy_model == 1) eph = eph + (kKboltz * T / kEv2erg) * (-log(fmax(u[7], kTinest)));
         eph = fmin(eph, a.eion_max * 0.999);
+    } else {   // the He I excited channel: 2^3S line, 584 A line or two-photon continuum
+        double e3s, e1p, e1s;
+        hei_branches(a.he, a.Te[il], a.xHI[il], a.xHeI[il], e3s, e1p, e1s);
+        const double ub = u[7] * ((e3s + e1p) + e1s);
+        if (ub <= e3s) eph = 19.82;
+        else if (ub <= e3s + e1p) eph = 21.22;
+        else eph = hei_2ph_sample(a.he, u[8]);
     }
     // ion_bin_of without the FUV bins (ion_band_mod.f90:624-646)
     int blo = 1, bhi = a.nnu;
@@ -303,6 +419,8 @@ cudaError_t diffuse_build(mochii_ctx* c, double* total) {
     a.rs.hui_gnedin = c->par.recomb_hui_gnedin;
     a.rs.dere_hybrid = c->par.ci_dere_hybrid;
     a.energy_model = c->par.diffuse_model;
+    a.he = c->dif.he;
+    a.hei = c->par.hei_diffuse ? 1 : 0;
     k_diffuse_lum<<<nblk(a.nleaf, kThreads, 148 * 16), kThreads, 0, c->stream>>>(a);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
@@ -326,8 +444,11 @@ cudaError_t launch_diffuse_chunk(mochii_ctx* c, double total, long long ip0, lon
     a.cum = c->dif.tot;
     a.ch = c->dif.ch;
     a.Te = c->Te;
+    a.xHI = c->xHI;
+    a.xHeI = c->xHeI;
     a.eedge = c->tab.eedge;
     a.m = c->dif.m;
+    a.he = c->dif.he;
     a.total = total;
     a.org[0] = c->grid.xmin; a.org[1] = c->grid.ymin; a.org[2] = c->grid.zmin;
     a.metal = c->metal;

@@ -33,7 +33,7 @@ const char* const kOtherKeys[] = {
     "dust_niter", "dust_no_photons", "dust_nu", "dust_sed", "dust_single_teq", "dust_tol",
     "emis_output", "exetime", "ext_geometry", "ext_intensity", "ext_scale", "ext_spectrum", "ext_tstar",
     "f_ion_dust", "f_ion_pah", "f_pah", "file_format", "geometry", "h_coll_effects",
-    "hei_diffuse", "hei_metastable", "hgg", "ion_spectrum", "kext_file",
+    "hei_metastable", "hgg", "ion_spectrum", "kext_file",
     "lambda0", "lambda_max", "lambda_min", "line_case", "mrw_gamma", "nlambda", "no_print",
     "nobs", "nprint", "nr", "nscatt_tot", "num_send_at_once",
     "out_bitpix", "out_bitpix_force", "out_file", "output_normalization", "pe_scale",
@@ -287,7 +287,7 @@ int set_key(mochii_params* p, std::string key, const std::vector<std::string>& v
     BOOL("ion_metal_abs", ion_metal_abs) BOOL("metal_ne", metal_ne) BOOL("metal_heat", metal_heat)
     BOOL("metal_freefree", metal_freefree) BOOL("gaunt_vh14", gaunt_vh14)
     BOOL("fe_levels_full", fe_levels_full)
-    BOOL("diffuse_field", diffuse_field) BOOL("use_sec_ion", use_sec_ion)
+    BOOL("diffuse_field", diffuse_field) BOOL("use_sec_ion", use_sec_ion) BOOL("hei_diffuse", hei_diffuse)
     BOOL("ion_add_dust", ion_add_dust) BOOL("ion_dust_scatter", ion_dust_scatter) BOOL("grain_pe", grain_pe)
     REAL("dgr", DGR) REAL("cext_dust", cext_dust) REAL("lambda_ref", lambda_ref)
     REAL("taumax", taumax) REAL("tauhomo", tauhomo)

@@ -8,6 +8,8 @@
   atomic/nlevel_<el>_<stage>.txt    n-level atom data (nlevel_mod)
   atomic/element_<el>.txt           trace-element registry (species_mod)
   kext_albedo_WD_MW_3.1_60_D03.all_2003   MW R_V = 3.1 grain extinction (gas_opacity_mod)
+  HeI2phot.dat                      He I 2^1S two-photon shape A(y), Drake, Victor &
+                                    Dalgarno 1969 (hei_twophoton_mod)
 
 These are data (CHIANTI / Verner / Weingartner & Draine fits with provenance
 headers), not code; the library loads them at set-up.
@@ -28,6 +30,6 @@ for pat in ("cooling_*.txt", "nlevel_*.txt", "element_*.txt"):
         if f.endswith("cooling_fit_parameters.txt"):
             continue
         shutil.copyfile(f, os.path.join(DST, "atomic", os.path.basename(f)))
-shutil.copyfile(os.path.join(SRC, "data", "kext_albedo_WD_MW_3.1_60_D03.all_2003"),
-                os.path.join(DST, "kext_albedo_WD_MW_3.1_60_D03.all_2003"))
+for name in ("kext_albedo_WD_MW_3.1_60_D03.all_2003", "HeI2phot.dat"):
+    shutil.copyfile(os.path.join(SRC, "data", name), os.path.join(DST, name))
 print("copied", len(os.listdir(os.path.join(DST, "atomic"))), "atomic tables")

@@ -536,4 +536,31 @@ int orc_thermal_1d(const char* atomic_dir, const double* cfg10, int nr, int nswe
                       out5 + 4 * (size_t)nr);
 }
 
+
+// The He I two-photon table of the file at path (hei_twophoton_mod.f90):
+// out2 = in-band photons and energy [eV] per 2^1S decay; E[k] = the sampled
+// energy of u[k].
+int orc_hei_2ph(const char* path, double eion_max, const double* u, long long n, double* E, double* out2) {
+    HeI2ph h;
+    if (!h.setup(path, eion_max)) {
+        g_err = std::string("cannot read ") + path;
+        return 1;
+    }
+    out2[0] = h.n_per_decay;
+    out2[1] = h.e_per_decay;
+    for (long long k = 0; k < n; ++k) E[k] = h.sample(u[k]);
+    return 0;
+}
+// hei_branch_energies (diffuse_mod.f90:308-325) with the table at path:
+// out3 = e3s, e1p, e1s [eV per case-B He II recombination].
+int orc_hei_branch_energies(const char* path, double T, double xHI, double xHeI, double* out3) {
+    HeI2ph h;
+    if (!h.setup(path, 100.0)) {
+        g_err = std::string("cannot read ") + path;
+        return 1;
+    }
+    hei_branch_energies(h, T, xHI, xHeI, out3[0], out3[1], out3[2]);
+    return 0;
+}
+
 }  // extern "C"

@@ -9,6 +9,7 @@
 #include <cctype>
 #include <cstdio>
 #include <cstring>
+#include <fstream>
 #include <sstream>
 #ifdef _OPENMP
 #include <omp.h>
@@ -659,7 +660,7 @@ bool parse_namelist(const std::string& text, Par& p, std::string* err) {
         I(gas_niter); D(gas_tol); D(te_fixed); D(ion_relax); S(case_ab); S(ci_model);
         S(recomb_model); S(cooling_model); S(charge_exchange); S(conv_crit);
         B(solve_te); D(te_min); D(te_max); D(gas_tol_te); B(use_metals);
-        B(diffuse_field); B(use_sec_ion); B(ion_add_dust); B(ion_dust_scatter);
+        B(diffuse_field); B(use_sec_ion); B(ion_add_dust); B(ion_dust_scatter); B(hei_diffuse);
         S(dust_density_law); D(cext_dust); S(data_dir); S(atomic_dir); S(ion_dust_kext);
         S(diffuse_energy_model); D(lambda_ref); D(taumax); D(tauhomo);
         else if (k == "iseed") p.iseed = (int64_t)std::llround(to_dbl(s));
@@ -1079,6 +1080,18 @@ bool Sim::setup(const std::string& nl, std::string* err) {
     }
     if (!band_setup(par, band, err, meth)) return false;
     if (par.diffuse_field) milne.setup(par.eion_max);   // main.f90:102
+    if (par.diffuse_field && par.hei_diffuse) {          // main.f90:107-112
+        std::string dir = par.data_dir;
+        if (dir.empty()) {   // the directory above atomic_dir (<data_dir>/atomic)
+            const size_t k = par.atomic_dir.find_last_of('/');
+            dir = par.atomic_dir.empty() ? std::string("data")
+                                         : (k == std::string::npos ? std::string(".") : par.atomic_dir.substr(0, k));
+        }
+        if (!hei2ph.setup(dir + "/HeI2phot.dat", par.eion_max)) {
+            set_err(err, ("cannot read " + dir + "/HeI2phot.dat").c_str());
+            return false;
+        }
+    }
     if (par.launch_sequence != "sobol") {
         set_err(err, "oracle: only the sobol launch sequence is restated");
         return false;
@@ -1735,9 +1748,85 @@ double Milne::sample(int ich, double T, double u, double eion_max) const {
     return std::min(E, eion_max * (1.0 - 1.0e-12));
 }
 
+// ---- hei_twophoton_mod.f90, hei_cascade_mod.f90 ------------------------------
+double HeI2ph::shape(double y) const {
+    const int n = (int)ty.size();
+    if (y <= ty[0] || y >= ty[n - 1]) return 0.0;
+    int i = 0;
+    while (i < n - 2 && ty[i + 1] < y) ++i;
+    return tA[i] + (tA[i + 1] - tA[i]) * (y - ty[i]) / (ty[i + 1] - ty[i]);
+}
+
+bool HeI2ph::setup(const std::string& path, double eion_max) {
+    std::ifstream f(path);
+    if (!f) return false;
+    ty.clear(); tA.clear();
+    double a, b;
+    while (f >> a >> b) { ty.push_back(a); tA.push_back(b); }
+    const int n = (int)ty.size();
+    if (n < 4) return false;
+    double tot = 0.0;   // Simpson over each table interval
+    for (int i = 0; i < n - 1; ++i) {
+        const double ya = ty[i], yb = ty[i + 1], ym = 0.5 * (ya + yb);
+        tot = tot + (yb - ya) / 6.0 * (tA[i] + 4.0 * shape(ym) + tA[i + 1]);
+    }
+    if (tot <= 0.0) return false;
+    const double y_lo = ETH_HI / E_TOT, y_hi = std::min(E_TOT, eion_max) / E_TOT;
+    if (y_hi <= y_lo) {
+        n_per_decay = 0.0; e_per_decay = 0.0;
+        for (int i = 0; i < NCDF; ++i) { cdf_e[i] = 1.0; grid_y[i] = y_lo; }
+        return true;
+    }
+    double an = 0.0, ae = 0.0, seg = 0.0;
+    grid_y[0] = y_lo;
+    cdf_e[0] = 0.0;
+    for (int i = 1; i <= NCDF - 1; ++i) {
+        const double ya = y_lo + (y_hi - y_lo) * (double)(i - 1) / (double)(NCDF - 1);
+        const double yb = y_lo + (y_hi - y_lo) * (double)i / (double)(NCDF - 1);
+        const double ym = 0.5 * (ya + yb);
+        const double fa = shape(ya), fm = shape(ym), fb = shape(yb);
+        an = an + (yb - ya) / 6.0 * (fa + 4.0 * fm + fb);
+        ae = ae + (yb - ya) / 6.0 * (fa * ya + 4.0 * fm * ym + fb * yb) * E_TOT;
+        seg = seg + (yb - ya) / 6.0 * (fa * ya + 4.0 * fm * ym + fb * yb);
+        grid_y[i] = yb;
+        cdf_e[i] = seg;
+    }
+    n_per_decay = 2.0 * an / tot;
+    e_per_decay = 2.0 * ae / tot;
+    for (int i = 0; i < NCDF; ++i) cdf_e[i] = seg > 0.0 ? cdf_e[i] / seg : 1.0;
+    cdf_e[NCDF - 1] = 1.0;
+    return true;
+}
+
+double HeI2ph::sample(double u) const {
+    const double uu = std::min(std::max(u, 0.0), 1.0);
+    int lo = 0, hi = NCDF - 1;
+    while (hi - lo > 1) {
+        const int mid = (lo + hi + 2) / 2 - 1;   // the 1-based (lo + hi) / 2 of the reference
+        if (uu > cdf_e[mid]) lo = mid; else hi = mid;
+    }
+    const double y = cdf_e[hi] > cdf_e[lo]
+                         ? grid_y[lo] + (grid_y[hi] - grid_y[lo]) * (uu - cdf_e[lo]) / (cdf_e[hi] - cdf_e[lo])
+                         : grid_y[lo];
+    return y * E_TOT;
+}
+
+void hei_branch_energies(const HeI2ph& h, double T, double xHI, double xHeI, double& e3s, double& e1p, double& e1s) {
+    const double Tc = std::min(std::max(T, 3.0e3), 2.0e4) / 1.0e4;   // the fits are clamped, not extrapolated
+    const double a3 = 2.10e-13 * std::pow(Tc, -0.381);
+    const double a1s = 2.06e-14 * std::pow(Tc, -0.451);
+    const double a1p = 4.17e-14 * std::pow(Tc, -0.695);
+    const double sum = a3 + a1s + a1p;
+    const double f3s = a3 / sum, f1s = a1s / sum, f1p = a1p / sum;
+    const double p584 = 1.0 / (1.0 + 77.0 / std::sqrt(std::max(T, TINEST)) * std::max(xHeI, 0.0) / std::max(xHI, TINEST));
+    e3s = f3s * 19.82;
+    e1p = f1p * p584 * 21.22;
+    e1s = (f1s + f1p * (1.0 - p584)) * h.e_per_decay;
+}
+
 // ---- diffuse_mod.f90 ---------------------------------------------------------
-// diffuse_build, diffuse_mod.f90:60-121 (milne energy model; no He I
-// excited channel).
+// diffuse_build, diffuse_mod.f90:60-121, with the He I excited channel
+// (par%hei_diffuse, :96-106).
 void Sim::diffuse_build(double lpacket) {
     const int nleaf = grid.nleaf;
     dif_ch.assign((size_t)4 * nleaf, 0.0);
@@ -1764,6 +1853,11 @@ void Sim::diffuse_build(double lpacket) {
         dif_ch[4 * (size_t)il + 1] = ne * nHeII * a1 * mean_e(1, ETH_HEI) * EV2ERG * vol;
         a1 = alphaA_HeIII(rm, T) - alphaB_HeIII(rm, T);
         dif_ch[4 * (size_t)il + 2] = ne * nHeIII * a1 * mean_e(2, ETH_HEII) * EV2ERG * vol;
+        if (par.hei_diffuse) {
+            double e3s, e1p, e1s;
+            hei_branch_energies(hei2ph, T, st.xHI[il], st.xHeI[il], e3s, e1p, e1s);
+            dif_ch[4 * (size_t)il + 3] = ne * nHeII * alphaB_HeII(rm, T) * vol * EV2ERG * (e3s + e1p + e1s);
+        }
     }
     diffuse_lum = 0.0;
     for (int il = 0; il < nleaf; ++il) {
@@ -1779,7 +1873,7 @@ void Sim::diffuse_build(double lpacket) {
     }
 }
 
-// gen_diffuse_photon_qmc, diffuse_mod.f90:221-296 (ground channels).
+// gen_diffuse_photon_qmc, diffuse_mod.f90:221-296.
 void Sim::gen_diffuse_qmc(int64_t ip, Photon& ph) const {
     double u[9];
     for (int d = 1; d <= 9; ++d) u[d - 1] = qmc.uniform(ip, d, 2);
@@ -1815,6 +1909,13 @@ void Sim::gen_diffuse_qmc(int64_t ip, Photon& ph) const {
         if (par.diffuse_energy_model == "milne") eph = milne.sample(ch, T, u[7], par.eion_max);
         else if (par.diffuse_energy_model == "exponential") eph = eph + kT * (-std::log(std::max(u[7], TINEST)));
         eph = std::min(eph, par.eion_max * 0.999);
+    } else {   // the He I excited channel: 2^3S line, 584 A line or two-photon continuum
+        double e3s, e1p, e1s;
+        hei_branch_energies(hei2ph, st.Te[il], st.xHI[il], st.xHeI[il], e3s, e1p, e1s);
+        const double ub = u[7] * ((e3s + e1p) + e1s);
+        if (ub <= e3s) eph = 19.82;
+        else if (ub <= e3s + e1p) eph = 21.22;
+        else eph = hei2ph.sample(u[8]);
     }
     ph.inu = ion_bin_of(band, eph, false);
     ph.wgt = 1.0;

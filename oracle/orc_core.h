@@ -147,7 +147,7 @@ struct Par {
     std::string conv_crit = "cell";
     bool solve_te = false;
     double te_min = 1.0e3, te_max = 5.0e4, gas_tol_te = 1.0e-3;
-    bool use_metals = false, diffuse_field = false, use_sec_ion = false;
+    bool use_metals = false, diffuse_field = false, use_sec_ion = false, hei_diffuse = false;
     std::string diffuse_energy_model = "milne";
     bool ion_add_dust = false, ion_dust_scatter = false;
     std::string dust_density_law = "global_dgr";
@@ -251,6 +251,24 @@ struct Milne {
     double sample(int ich, double T, double u, double eion_max) const;  // :320-350
 };
 
+// hei_twophoton_mod.f90: He I 2^1S -> 1^1S two-photon continuum above the
+// H I edge (moments and energy-weighted sampling CDF of the tabulated A(y)).
+struct HeI2ph {
+    static constexpr int NCDF = 1024;
+    static constexpr double E_TOT = 20.62;
+    std::vector<double> ty, tA;
+    double cdf_e[NCDF], grid_y[NCDF];
+    double n_per_decay = 0.0, e_per_decay = 0.0;
+    bool setup(const std::string& path, double eion_max);   // :97-192
+    double shape(double y) const;                           // :82-93
+    double sample(double u) const;                          // :199-219
+};
+
+// hei_cascade_mod.f90 and diffuse_mod.f90:308-325: the in-band energy per
+// case-B He II recombination of the 2^3S line, the 584 A line that ionizes
+// hydrogen and the two-photon continuum.
+void hei_branch_energies(const HeI2ph& h, double T, double xHI, double xHeI, double& e3s, double& e1p, double& e1s);
+
 struct Sim {
     Par par;
     Thermal* th = nullptr;           // thermal tables (solve_te)
@@ -267,6 +285,7 @@ struct Sim {
     int nthreads = 1;
     // diffuse field (diffuse_mod.f90)
     Milne milne;
+    HeI2ph hei2ph;                         // par%hei_diffuse
     std::vector<double> dif_ch, dif_cdf;   // (4, nleaf), (nleaf)
     double diffuse_lum = 0.0;
     int64_t diffuse_nphot = 0;

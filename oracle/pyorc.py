@@ -88,6 +88,8 @@ def load():
         "orc_sim_peel_image": (LL, [V, I, V, LL, V]),
         "orc_sim_peel_observer": (I, [V, I, V]),
         "orc_thermal_1d": (I, [C.c_char_p, V, I, I, V]),
+        "orc_hei_2ph": (I, [C.c_char_p, D, V, LL, V, V]),
+        "orc_hei_branch_energies": (I, [C.c_char_p, D, D, D, V]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)
@@ -190,6 +192,26 @@ def solve_ion_cell(gH, gHe1, gHe2, nH, T, caseA, x3, yHe=0.1, model=0):
     load().orc_solve_ion_cell(model, yHe, gH, gHe1, gHe2, nH, T, int(caseA), x.ctypes.data, C.byref(ne))
     return x, ne.value
 
+
+
+def hei_2ph(path, u, eion_max=100.0):
+    """The He I two-photon table (hei_twophoton_mod.f90): (photons per decay,
+    in-band energy per decay [eV], sampled energies of the uniforms u)."""
+    u = np.ascontiguousarray(u, dtype=np.float64)
+    E = np.zeros_like(u)
+    out = np.zeros(2)
+    if load().orc_hei_2ph(str(path).encode(), float(eion_max), u.ctypes.data, u.size, E.ctypes.data, out.ctypes.data):
+        raise RuntimeError(load().orc_last_error().decode())
+    return out[0], out[1], E
+
+
+def hei_branch_energies(path, T, xHI, xHeI):
+    """diffuse_mod.f90 hei_branch_energies: (e3s, e1p, e1s) in eV per case-B
+    He II recombination."""
+    out = np.zeros(3)
+    if load().orc_hei_branch_energies(str(path).encode(), float(T), float(xHI), float(xHeI), out.ctypes.data):
+        raise RuntimeError(load().orc_last_error().decode())
+    return tuple(out)
 
 
 def thermal_1d(atomic_dir, nr=8000, nsweep=4, nnu=32, emin=13.598, emax=100.0, tstar=4.0e4,

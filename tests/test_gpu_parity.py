@@ -276,9 +276,9 @@ def test_thermal_balance_matches_oracle(orc):
     neb.close()
 
 
-def diffuse_pair(orc, n=24, nphot=60000, iters=3):
+def diffuse_pair(orc, n=24, nphot=60000, iters=3, hei=False):
     nl = configs.hii_thermal(nphotons=nphot, niter=iters, n=n, precision="fp64", rs_factor=1.2)
-    nl = nl.replace("/\n", " par%diffuse_field = .true.\n/\n")
+    nl = nl.replace("/\n", " par%diffuse_field = .true.\n" + (" par%hei_diffuse = .true.\n" if hei else "") + "/\n")
     sim = orc.Sim(nl)
     for _ in range(iters):
         sim.transport_pass()
@@ -290,13 +290,15 @@ def diffuse_pair(orc, n=24, nphot=60000, iters=3):
     return nl, sim, neb
 
 
-def test_diffuse_field_matches_oracle(orc):
+@pytest.mark.parametrize("hei", [False, True])
+def test_diffuse_field_matches_oracle(orc, hei):
     """diffuse_build (per-leaf ground-recombination luminosities, Milne mean
-    energies) and the diffuse launch on the same state as the oracle.  The leaf
-    CDF is a device prefix sum whose rounding differs from the sequential sum,
-    so a packet may land in the neighbouring leaf when u1 sits within rounding
-    of a CDF step; everything else is bit-exact."""
-    nl, sim, neb = diffuse_pair(orc)
+    energies; with hei_diffuse the He I excited channel's lines and two-photon
+    continuum) and the diffuse launch on the same state as the oracle.  The
+    leaf CDF is a device prefix sum whose rounding differs from the sequential
+    sum, so a packet may land in the neighbouring leaf when u1 sits within
+    rounding of a CDF step; everything else is bit-exact."""
+    nl, sim, neb = diffuse_pair(orc, hei=hei)
     lum_o, n_o = sim.diffuse_build()
     nrec = min(n_o, 4000)
     rec, lum_g, n_g = neb.diffuse_records(0, nrec)
@@ -309,11 +311,15 @@ def test_diffuse_field_matches_oracle(orc):
     sig_o = np.array([orc.evaluate("sigma_HI", [e])[0] for e in ref[:, 6]]) * 1e18
     np.testing.assert_allclose(rec[same, 6], sig_o[same], rtol=1e-14)   # Milne energies bit-exact
     assert np.array_equal(rec[same, 7], ref[same, 7])
+    if hei:   # the He I lines (19.82, 21.22 eV) and the two-photon continuum below 20.62 eV are drawn
+        e = ref[same, 6]
+        assert np.sum(e == 19.82) > 10 and np.sum(e == 21.22) > 0 and np.sum((e > 13.598) & (e < 20.62)) > 10
     neb.close()
 
 
-def test_pass_with_diffuse_matches_oracle(orc):
-    nl, sim, neb = diffuse_pair(orc)
+@pytest.mark.parametrize("hei", [False, True])
+def test_pass_with_diffuse_matches_oracle(orc, hei):
+    nl, sim, neb = diffuse_pair(orc, hei=hei)
     st = neb.ionizing_field_and_rates()
     sim.transport_pass()
     assert st.diffuse_packets > 100 and st.closure <= 5e-13
