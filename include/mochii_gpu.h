@@ -281,6 +281,18 @@ int mochii_image_observer(const mochii_ctx* ctx, int k, double* out18);
  * header.json (DXIM, DIST, ALPHA, BETA, GAMMA per block). */
 int mochii_write_image(mochii_ctx* ctx, const char* base);
 
+/* The equilibrium dust temperature (dust_temp_mod.f90, par%ion_add_dust):
+ * mochii_get_field(ctx, "T_dust", ...) solves Heat_dust = (rhokap / d_cm)
+ * femit(T) per leaf from the last pass's grain heating (femit = 4 pi Int
+ * s_abs B_nu dnu over the extinction table the transport uses), and the
+ * rates file carries it as T_dust.  mochii_dust_ir: the grains' infrared
+ * spectrum of it, lam[240] [um] from 1 to 1000 um, lnu[240] [erg/s/Hz] and
+ * labs_lir[2] = the absorbed power sum Heat_dust V and the integral of L_nu
+ * over frequency [erg/s] (dust_ir_write); mochii_write_dust_ir writes them
+ * as <base>_dustir.txt. */
+int mochii_dust_ir(mochii_ctx* ctx, double* lam, double* lnu, double* labs_lir);
+int mochii_write_dust_ir(mochii_ctx* ctx, const char* base);
+
 /* gas_opacity_fill: refresh the per-leaf absorber columns the transport reads. */
 int mochii_opacity_fill(mochii_ctx* ctx);
 

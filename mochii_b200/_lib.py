@@ -128,6 +128,8 @@ SIGNATURES = {
     "mochii_get_image": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_int64]),
     "mochii_image_observer": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p]),
     "mochii_write_image": (C.c_int, [C.c_void_p, C.c_char_p]),
+    "mochii_dust_ir": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "mochii_write_dust_ir": (C.c_int, [C.c_void_p, C.c_char_p]),
     "mochii_set_field": (C.c_int, [C.c_void_p, C.c_char_p, C.c_void_p, C.c_int64]),
     "mochii_set_nphotons": (C.c_int, [C.c_void_p, C.c_int64]),
     "mochii_ion_Ltot": (C.c_double, [C.c_void_p]),

@@ -98,7 +98,7 @@ void release(mochii_ctx* c) {
                     c->th.gff, c->th.lamref, c->th.Ssup, c->th.tinv,
                     c->dif.ch, c->dif.tot, c->dif.scan_tmp, c->dif.tables, c->dif.he_tab,
                     (void*)c->metal.el, c->metal.egam, c->metal.eheat, c->metal.opac, c->metal.raw,
-                    (void*)c->metal.medge, c->metal.mom, c->twarm, c->twarm_err,
+                    (void*)c->metal.medge, c->metal.mom, c->twarm, c->twarm_err, c->tdust, c->tdust_tab,
                     (void*)c->rec.E, c->rec.msig, c->oct_blob, c->rec.dsc, (void*)c->rec.p0,
                     (void*)c->dust_blob, (void*)c->rhokap, (void*)c->ttab, (void*)c->metal_lnl,
                     (void*)c->th.lnL, (void*)c->rec.key, (void*)c->rec.key_sorted, (void*)c->rec.seq,
@@ -1160,6 +1160,14 @@ extern "C" int mochii_get_field(mochii_ctx* c, const char* name, double* out, in
     if (nm == "eedge") {
         if (n != (int64_t)c->band.eedge.size()) return fail(c, MOCHII_ERR_BAD_PARAM, "eedge size mismatch");
         std::memcpy(out, c->band.eedge.data(), n * 8);
+        return MOCHII_OK;
+    }
+    if (nm == "T_dust") {   // dust_temp_compute (dust_temp_mod.f90:137-170) from the last pass's Heat_dust
+        if (n != c->grid.nleaf) return fail(c, MOCHII_ERR_BAD_PARAM, "T_dust size mismatch");
+        if (!c->par.ion_add_dust || !c->rhokap) return fail(c, MOCHII_ERR_BAD_PARAM, "T_dust: needs par%ion_add_dust");
+        CK(c, dust_temp_launch(c));
+        CK(c, cudaMemcpyAsync(out, c->tdust, (size_t)n * 8, cudaMemcpyDeviceToHost, c->stream));
+        CK(c, cudaStreamSynchronize(c->stream));
         return MOCHII_OK;
     }
     if (nm == "T_warm") {   // the warm start of the next bracketed thermal solve, as set or predicted

@@ -157,6 +157,10 @@ struct mochii_ctx {
     bool twarm_learned = false;     // the warm start came from mochii_mlp_warm_start
     double* twarm_err = nullptr;    // device: sum of ln^2(T_e / T_warm) and its count after a learned start
     double warm_err_ln = 0.0;       // RMS of ln(T_e / T_warm) of the last learned warm start (0: none yet)
+    // equilibrium dust temperature (dust_temp_mod.f90), built on first use
+    double* tdust = nullptr;        // nleaf T_dust [K]
+    double* tdust_tab = nullptr;    // lam_ir | sabs_ir | tgrid | femit
+    mochii::DustTempHost tdust_host;
     mochii::SpeciesHost species;
     bool thermal_ready = false;
     mochii::BalanceWork bw;

@@ -34,4 +34,14 @@ struct DustDev {
     double cref = 0.0;
 };
 
+// The equilibrium dust temperature's tables (dust_temp_mod.f90:38-115):
+// femit(T) on 61 log nodes of T (10^0.5 .. 10^3.5 K) and s_abs at 240 log
+// wavelengths from 1 to 1000 um.
+constexpr int kDustTN = 61, kDustIrN = 240;
+struct DustTempHost {
+    double tgrid[kDustTN] = {}, femit[kDustTN] = {};
+    double lam_ir[kDustIrN] = {}, sabs_ir[kDustIrN] = {};
+};
+void dust_temp_tables(const DustHost& d, DustTempHost& t);
+
 }  // namespace mochii

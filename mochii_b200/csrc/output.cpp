@@ -23,6 +23,7 @@
 
 #include "ctx.h"
 #include "mochii_gpu.h"
+#include "transport.h"
 #include "physics.cuh"
 
 namespace mochii {
@@ -118,6 +119,8 @@ extern "C" int mochii_write_rates(mochii_ctx* c, const char* base, const mochii_
     for (auto& f : rate_fields)
         if ((rc = field(f[0], f[1], f[2]))) return rc;
     if (c->par.ion_add_dust && (rc = field("heat_dust", "Heat_dust", "grain heating [erg/s/cm^3]"))) return rc;
+    // dust_temp_compute at output (main.f90:241-248), then its dataset (gas_rates_mod.f90:287-293)
+    if (c->par.ion_add_dust && (rc = field("T_dust", "T_dust", "equilibrium mixture dust temperature [K]"))) return rc;
 
     // geometry: leaf centres and half widths
     std::vector<double> half((size_t)nl), cx((size_t)nl), cy((size_t)nl), cz((size_t)nl);
@@ -271,4 +274,63 @@ extern "C" int mochii_write_rates(mochii_ctx* c, const char* base, const mochii_
         return MOCHII_ERR_BAD_PARAM;
     }
     return MOCHII_OK;
+}
+
+// The grains' infrared spectrum of the current T_dust (dust_ir_write,
+// dust_temp_mod.f90:173-214): lam[240] [um], lnu[240] [erg/s/Hz] and
+// labs_lir[2] = the absorbed power sum Heat_dust V and the trapezoid integral
+// of L_nu over frequency [erg/s].
+extern "C" int mochii_dust_ir(mochii_ctx* c, double* lam, double* lnu, double* labs_lir) {
+    if (!c || !lam || !lnu || !labs_lir) return MOCHII_ERR_BAD_PARAM;
+    if (!c->par.ion_add_dust || !c->rhokap) {
+        c->last_error = "mochii_dust_ir: needs par%ion_add_dust";
+        return MOCHII_ERR_BAD_PARAM;
+    }
+    double* d = nullptr;
+    std::vector<double> out(kDustIrN + 1);
+    cudaError_t e = dust_temp_launch(c);
+    if (e == cudaSuccess) e = cudaMallocAsync(&d, (kDustIrN + 1) * 8, c->stream);
+    if (e == cudaSuccess) e = dust_ir_launch(c, d);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(out.data(), d, (kDustIrN + 1) * 8, cudaMemcpyDeviceToHost, c->stream);
+    if (d) cudaFreeAsync(d, c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    if (e != cudaSuccess) {
+        c->last_error = std::string("mochii_dust_ir: ") + cudaGetErrorString(e);
+        return MOCHII_ERR_CUDA;
+    }
+    double lir = 0.0;
+    for (int k = 0; k < kDustIrN; ++k) {
+        lam[k] = c->tdust_host.lam_ir[k];
+        lnu[k] = out[k];
+    }
+    for (int k = 0; k + 1 < kDustIrN; ++k) {
+        const double dnu = 2.99792458e10 / (lam[k] * 1.0e-4) - 2.99792458e10 / (lam[k + 1] * 1.0e-4);
+        lir = lir + 0.5 * (lnu[k] + lnu[k + 1]) * dnu;
+    }
+    labs_lir[0] = out[kDustIrN];
+    labs_lir[1] = lir;
+    return MOCHII_OK;
+}
+
+// dust_ir_write's text file <base>_dustir.txt: two header lines with the
+// absorbed power, the integral of L_nu and their ratio, then lambda [um] and
+// L_nu [erg/s/Hz] per line.
+extern "C" int mochii_write_dust_ir(mochii_ctx* c, const char* base) {
+    if (!c || !base || !base[0]) return MOCHII_ERR_BAD_PARAM;
+    double lam[kDustIrN], lnu[kDustIrN], ab[2];
+    const int rc = mochii_dust_ir(c, lam, lnu, ab);
+    if (rc) return rc;
+    const std::string path = std::string(base) + "_dustir.txt";
+    FILE* f = std::fopen(path.c_str(), "w");
+    if (!f) {
+        c->last_error = "cannot write " + path;
+        return MOCHII_ERR_BAD_PARAM;
+    }
+    std::fprintf(f, "# MoCHII equilibrium-mixture dust IR spectrum (single T_d per leaf; SEDust stochastic/PAH "
+                    "bands are the next stage)\n");
+    std::fprintf(f, "# L_abs(dust) = %14.6E erg/s;  integral L_nu dnu = %14.6E;  ratio = %7.3f\n", ab[0], ab[1],
+                 ab[1] / std::max(ab[0], 2.2250738585072014e-308));
+    std::fprintf(f, "# lambda[um]   L_nu[erg/s/Hz]\n");
+    for (int k = 0; k < kDustIrN; ++k) std::fprintf(f, "%12.4f%15.6E\n", lam[k], lnu[k]);
+    return std::fclose(f) == 0 ? MOCHII_OK : MOCHII_ERR_BAD_PARAM;
 }

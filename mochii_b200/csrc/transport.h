@@ -43,6 +43,10 @@ cudaError_t thermal_batch_enqueue(void* tb, mochii_ctx* const* cs, cudaStream_t 
 cudaError_t thermal_batch_set_warm(void* tb, mochii_ctx* const* cs, const double* fac, double gate);
 double mlp_step_factor(const mochii_mlp* m, double observed_ln = 0.0);
 cudaError_t warm_error_launch(mochii_ctx* c);
+// dust_temp_mod.f90: T_dust of every leaf into c->tdust; the IR spectrum of
+// it (out_dev[0..239] = L_nu at the IR wavelengths, out_dev[240] = absorbed power)
+cudaError_t dust_temp_launch(mochii_ctx* c);
+cudaError_t dust_ir_launch(mochii_ctx* c, double* out_dev);
 int mlp_batch_prepare(mochii_mlp* m, mochii_ctx* const* cs, int n, double* fac);
 cudaError_t mlp_warm_start_enqueue(mochii_ctx* c, mochii_mlp* m, cudaStream_t s);
 

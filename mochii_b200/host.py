@@ -173,6 +173,19 @@ class Nebula:
         self._ok(self.lib.mochii_write_rates(self.ctx, str(base).encode(), C.byref(ri)))
         return str(base) + "_rates"
 
+    def dust_ir(self):
+        """The grains' infrared spectrum of the equilibrium dust temperature
+        (dust_ir_write): (lambda [um], L_nu [erg/s/Hz], absorbed power
+        [erg/s], integral of L_nu over frequency [erg/s])."""
+        lam, lnu, ab = np.zeros(240), np.zeros(240), np.zeros(2)
+        self._ok(self.lib.mochii_dust_ir(self.ctx, lam.ctypes.data, lnu.ctypes.data, ab.ctypes.data))
+        return lam, lnu, float(ab[0]), float(ab[1])
+
+    def write_dust_ir(self, base):
+        """dust_ir_write: <base>_dustir.txt; returns its path."""
+        self._ok(self.lib.mochii_write_dust_ir(self.ctx, str(base).encode()))
+        return str(base) + "_dustir.txt"
+
     def imaging_pass(self):
         """The peel-off imaging pass (main.f90:234-235): a transport pass with
         with_peel; needs par%ion_peel."""

@@ -382,6 +382,7 @@ long long orc_sim_set(void* h, const char* name, const double* in, long long n) 
     else if (nm == "heat_HI") v = &s->heat_HI;
     else if (nm == "heat_HeI") v = &s->heat_HeI;
     else if (nm == "heat_HeII") v = &s->heat_HeII;
+    else if (nm == "heat_dust") v = &s->heat_dust;
     else if (s->metals() && (nm == "gamma_metal" || nm == "heat_metal")) {
         // leaf-major in element order, in[il*ntr + j], as orc_sim_get returns them
         Species& sp = *s->sp;
@@ -560,6 +561,35 @@ int orc_hei_branch_energies(const char* path, double T, double xHI, double xHeI,
         return 1;
     }
     hei_branch_energies(h, T, xHI, xHeI, out3[0], out3[1], out3[2]);
+    return 0;
+}
+
+
+// dust_temp_compute on the sim's current Heat_dust and rhokap: out[nleaf] =
+// T_dust; ir[240] = L_nu at the IR wavelengths, ir[240] = absorbed power
+// (dust_ir_write); lam[240] the wavelengths [um].
+int orc_sim_dust_temp(void* h, double* out, double* lam, double* ir) {
+    auto* s = static_cast<Sim*>(h);
+    if (!s->par.ion_add_dust || s->dust.lam.empty()) return 1;
+    DustTemp t;
+    t.setup(s->dust);
+    const int nleaf = s->grid.nleaf;
+    std::vector<double> td(nleaf);
+    for (int il = 0; il < nleaf; ++il) td[il] = t.solve(s->st.rhokap[il] / s->par.distance2cm, s->heat_dust[il]);
+    std::copy(td.begin(), td.end(), out);
+    std::fill(ir, ir + DustTemp::NIR + 1, 0.0);
+    const double fourpi = 12.566370614359172953850573533118;
+    for (int k = 0; k < DustTemp::NIR; ++k) lam[k] = t.lam_ir[k];
+    for (int il = 0; il < nleaf; ++il) {
+        if (td[il] <= 0.0) continue;
+        const double w = 2.0 * s->grid.lhalf[il] * s->par.distance2cm;
+        const double vol = w * w * w, kd = s->st.rhokap[il] / s->par.distance2cm;
+        ir[DustTemp::NIR] += s->heat_dust[il] * vol;
+        for (int k = 0; k < DustTemp::NIR; ++k) {
+            const double nu = 2.99792458e10 / (t.lam_ir[k] * 1.0e-4);
+            ir[k] += fourpi * kd * t.sabs_ir[k] * planck_nu(nu, td[il]) * vol;
+        }
+    }
     return 0;
 }
 

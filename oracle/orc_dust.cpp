@@ -98,6 +98,55 @@ double interp_lin(const std::vector<double>& x, const std::vector<double>& y, do
     return y[i] * (1.0 - w) + y[i + 1] * w;
 }
 
+// ---- dust_temp_mod.f90 --------------------------------------------------
+double planck_nu(double nu, double T) {   // :118-127
+    const double x = 6.62607015e-27 * nu / (1.380649e-16 * T);
+    return x < 700.0 ? 2.0 * 6.62607015e-27 * nu * nu * nu / (2.99792458e10 * 2.99792458e10) / (std::exp(x) - 1.0)
+                     : 0.0;
+}
+
+void DustTemp::setup(const DustTable& d) {   // dust_temp_setup, :38-115
+    const double c = 2.99792458e10, fourpi = 12.566370614359172953850573533118;
+    for (int k = 0; k < NIR; ++k) {
+        lam_ir[k] = std::exp(std::log(1.0) + (std::log(1000.0) - std::log(1.0)) * (double)k / (double)(NIR - 1));
+        sabs_ir[k] = (1.0 - interp_lin(d.lam, d.alb, lam_ir[k])) * interp_log(d.lam, d.cext, lam_ir[k]) / d.cref;
+    }
+    const size_t n = d.lam.size();
+    for (int i = 0; i < NT; ++i) {
+        tgrid[i] = std::pow(10.0, 0.5 + 3.0 * (double)i / (double)(NT - 1));
+        const double T = tgrid[i];
+        double f = 0.0;
+        for (size_t k = 0; k + 1 < n; ++k) {
+            const double nu1 = c / (d.lam[k + 1] * 1.0e-4), nu2 = c / (d.lam[k] * 1.0e-4);
+            const double snu = 0.5 * ((1.0 - d.alb[k]) * d.cext[k] + (1.0 - d.alb[k + 1]) * d.cext[k + 1]) / d.cref;
+            const double bnu = 0.5 * (planck_nu(nu1, T) + planck_nu(nu2, T));
+            f = f + fourpi * snu * bnu * (nu2 - nu1);
+        }
+        femit[i] = f;
+    }
+}
+
+double DustTemp::femit_of(double T) const {   // :129-135
+    const double lt = std::min(std::max(std::log10(T), std::log10(tgrid[0])), std::log10(tgrid[NT - 1]));
+    const int i = std::min((int)((lt - std::log10(tgrid[0])) / (3.0 / (double)(NT - 1))) + 1, NT - 1) - 1;
+    const double w = (lt - std::log10(tgrid[i])) / (std::log10(tgrid[i + 1]) - std::log10(tgrid[i]));
+    return std::exp(std::log(femit[i]) * (1.0 - w) + std::log(femit[i + 1]) * w);
+}
+
+double DustTemp::solve(double kd, double heat) const {   // dust_temp_compute, :137-170
+    if (kd <= 0.0 || heat <= 0.0) return 0.0;
+    const double target = heat / kd;
+    double tlo = tgrid[0], thi = tgrid[NT - 1];
+    if (femit_of(thi) <= target) return thi;
+    for (int it = 0; it < 60; ++it) {
+        const double tm = std::sqrt(tlo * thi);
+        if (femit_of(tm) < target) tlo = tm;
+        else thi = tm;
+        if (thi / tlo - 1.0 < 1.0e-5) break;
+    }
+    return std::sqrt(tlo * thi);
+}
+
 double DustTable::sabs_at(double E) const {
     const double lb = 1.23984 / E;
     return (1.0 - interp_lin(lam, alb, lb)) * interp_log(lam, cext, lb) / cref;

@@ -31,6 +31,19 @@ struct DustTable {
     double g_at(double E) const;                // <cos>
 };
 
+// dust_temp_mod.f90:38-170: the equilibrium mixture dust temperature's
+// emission function femit(T) = 4 pi Int s_abs B_nu dnu (trapezoid on the
+// table's frequency grid) on 61 log T nodes, s_abs at 240 log IR wavelengths
+// (1 - 1000 um), and the per-leaf root of Heat_dust = kd femit(T).
+struct DustTemp {
+    static constexpr int NT = 61, NIR = 240;
+    double tgrid[NT], femit[NT], lam_ir[NIR], sabs_ir[NIR];
+    void setup(const DustTable& d);
+    double femit_of(double T) const;
+    double solve(double kd, double heat) const;   // 0 where kd or heat is not positive
+};
+double planck_nu(double nu, double T);
+
 double interp_log(const std::vector<double>& x, const std::vector<double>& y, double x0);
 double interp_lin(const std::vector<double>& x, const std::vector<double>& y, double x0);
 // One Fortran list-directed real (1.5, 1.5E+3, 1.5D3, 1.5-3 = 1.5E-3).

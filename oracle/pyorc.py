@@ -89,6 +89,7 @@ def load():
         "orc_sim_peel_observer": (I, [V, I, V]),
         "orc_thermal_1d": (I, [C.c_char_p, V, I, I, V]),
         "orc_hei_2ph": (I, [C.c_char_p, D, V, LL, V, V]),
+        "orc_sim_dust_temp": (I, [V, V, V, V]),
         "orc_hei_branch_energies": (I, [C.c_char_p, D, D, D, V]),
     }
     for name, (res, args) in sig.items():
@@ -414,6 +415,14 @@ class Sim:
         n = C.c_longlong()
         lum = load().orc_sim_diffuse_build(self.h, C.byref(n))
         return lum, n.value
+
+    def dust_temp(self):
+        """dust_temp_compute and dust_ir_write's sums on the current Heat_dust:
+        (T_dust per leaf, IR wavelengths [um], L_nu [erg/s/Hz], absorbed
+        power [erg/s])."""
+        td, lam, ir = np.zeros(self.nleaf), np.zeros(240), np.zeros(241)
+        assert load().orc_sim_dust_temp(self.h, td.ctypes.data, lam.ctypes.data, ir.ctypes.data) == 0
+        return td, lam, ir[:240], ir[240]
 
     def diffuse_photon(self, ip):
         out = np.zeros(8)

@@ -151,3 +151,44 @@ def test_clumpy_dusty_case_matches_oracle(orc, tmp_path):
     assert dT.max() < 20.0, dT.max()
     assert dx.max() < 1e-3, dx.max()
     neb.close()
+
+
+@pytest.mark.parametrize("grid", ["car", "amr"])
+def test_dust_temperature_and_ir_spectrum_match_oracle(orc, leaf_file, grid, tmp_path):
+    """The equilibrium dust temperature (dust_temp_mod.f90) from the same
+    pass's grain heating: every leaf within one bisection interval (1e-5 in
+    T) of the oracle's, the IR spectrum and absorbed power within 1e-6, the
+    integrated IR within a few percent of the absorbed power (the 1-1000 um
+    window cuts the tails), T_dust in the rates file and the _dustir.txt
+    file as the reference writes them."""
+    base = configs.hhe128(nphotons=150000, niter=1, n=12, precision="fp64")
+    if grid == "amr":
+        base = configs.on_octree(base, leaf_file)
+    nl = dusty(base, fuv=True, dgr=0.05)
+    neb, sim = pair(orc, nl)
+    ionized(neb, sim)
+    neb.ionizing_field_and_rates()
+    sim.transport_pass()
+    np.testing.assert_allclose(neb.get("heat_dust"), sim.get("heat_dust"), rtol=1e-9, atol=0)
+    sim.set("heat_dust", np.ascontiguousarray(neb.get("heat_dust")))   # the same input on both sides
+    td_o, lam_o, lnu_o, labs_o = sim.dust_temp()
+    td = neb.get("T_dust")
+    lit = td_o > 0
+    assert lit.sum() > 100 and np.array_equal(td > 0, lit)
+    assert np.max(np.abs(td[lit] / td_o[lit] - 1)) < 1.1e-5
+    assert np.median(np.abs(td[lit] / td_o[lit] - 1)) < 1e-12
+    assert 3.0 < td[lit].min() and td[lit].max() < 3200.0
+    lam, lnu, labs, lir = neb.dust_ir()
+    np.testing.assert_allclose(lam, lam_o, rtol=1e-15)
+    np.testing.assert_allclose(lnu, lnu_o, rtol=1e-6, atol=1e-12 * lnu_o.max())
+    assert abs(labs / labs_o - 1) < 1e-10
+    assert 0.9 < lir / labs < 1.01
+    d = neb.write_rates(str(tmp_path / "dusty"))
+    np.testing.assert_array_equal(np.load(d + "/T_dust.npy"), td)
+    path = neb.write_dust_ir(str(tmp_path / "dusty"))
+    rows = np.loadtxt(path)
+    assert rows.shape == (240, 2)
+    np.testing.assert_allclose(rows[:, 1], lnu, rtol=1e-6)
+    head = open(path).read().splitlines()[1]
+    assert head.startswith("# L_abs(dust) =") and "ratio =" in head
+    neb.close()

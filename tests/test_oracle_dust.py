@@ -155,3 +155,45 @@ def test_scattering_is_deterministic_and_scores(orc):
     plain.set("x_HI", np.full(plain.nleaf, 1e-3))
     plain.transport_pass()
     assert h0.sum() > plain.get("heat_dust").sum()   # scattered light heats the grains too
+
+
+def test_dust_temperature_balances_heating(orc):
+    """dust_temp_mod.f90 in the oracle: per leaf the temperature at which
+    the grains emit what they absorb (Heat_dust = kd femit(T), femit from
+    the same extinction table by an independent numpy trapezoid; the table
+    interpolation in log T and the bisection leave well under 0.5 %), T
+    rising with the heating, and the IR spectrum returning the absorbed
+    power to within the 1-1000 um window's cut."""
+    nl = dusty(configs.hhe128(nphotons=1000, niter=1, n=6, precision="fp64"), dgr=0.05)   # distance unit pc
+    sim = orc.Sim(nl)
+    kd = sim.get("rhokap") / configs.PC2CM
+    heat = np.geomspace(1e-26, 1e-18, sim.nleaf)
+    sim.set("heat_dust", heat)
+    td, lam, lnu, labs = sim.dust_temp()
+    assert np.all(td > 3.0) and np.all(np.diff(td) > 0)
+    rows = []
+    for line in open(KEXT):
+        try:
+            v = [float(x) for x in line.split()[:4]]
+        except ValueError:
+            continue
+        if len(v) == 4 and v[0] > 0:
+            rows.append(v)
+    t = np.array(rows)
+    t = t[np.argsort(t[:, 0], kind="stable")]
+    lm, alb, cext = t[:, 0], t[:, 1], t[:, 3]
+    cref = np.exp(np.interp(np.log(0.55), np.log(lm), np.log(cext)))
+    h, k, c = 6.62607015e-27, 1.380649e-16, 2.99792458e10
+    nu = c / (lm * 1e-4)
+    s = (1 - alb) * cext / cref
+
+    def femit(T):
+        x = h * nu / (k * T)
+        b = np.where(x < 700, 2 * h * nu ** 3 / c ** 2 / np.expm1(np.minimum(x, 700)), 0.0)
+        return np.sum(4 * np.pi * 0.5 * (s[1:] + s[:-1]) * 0.5 * (b[1:] + b[:-1]) * (nu[:-1] - nu[1:]))
+    for il in range(0, sim.nleaf, max(1, sim.nleaf // 20)):
+        if td[il] < 3000.0:
+            assert abs(femit(td[il]) * kd[il] / heat[il] - 1) < 5e-3, (il, td[il])
+    dnu = c / (lam[:-1] * 1e-4) - c / (lam[1:] * 1e-4)
+    lir = np.sum(0.5 * (lnu[1:] + lnu[:-1]) * dnu)
+    assert 0.9 < lir / labs < 1.01
