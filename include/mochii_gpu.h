@@ -185,6 +185,13 @@ typedef struct mochii_params {
      * (diffuse_mod.f90:96-106, 274-284; hei_cascade_mod, hei_twophoton_mod),
      * the two-photon shape read from <data_dir>/HeI2phot.dat */
     int hei_diffuse;
+    /* solution-driven I-front re-refinement of the octree (define.f90:821-831,
+     * amr_refine_mod.f90): at iteration refine_iter the tree is rebuilt to
+     * level refine_lmax where refine_eps < x_HI < 1 - refine_eps or a face
+     * neighbour's x_HI differs by more than refine_dx, refine_lbase
+     * elsewhere (mochii_refine_front) */
+    int refine_front, refine_iter, refine_lbase, refine_lmax;
+    double refine_eps, refine_dx;
 } mochii_params;
 
 /* Per-pass statistics (ion_score_report_energy_closure, ion_score_mod.f90:364-387). */
@@ -292,6 +299,33 @@ int mochii_write_image(mochii_ctx* ctx, const char* base);
  * as <base>_dustir.txt. */
 int mochii_dust_ir(mochii_ctx* ctx, double* lam, double* lnu, double* labs_lir);
 int mochii_write_dust_ir(mochii_ctx* ctx, const char* base);
+
+/* amr_refine_front (amr_refine_mod.f90:46-186): the octree rebuilt on the
+ * current solution.  Front leaves: gas leaves with refine_eps < x_HI <
+ * 1 - refine_eps, or whose face-neighbour gas leaf differs in x_HI by more
+ * than refine_dx; the new tree is level refine_lmax where a cell overlaps a
+ * front leaf and refine_lbase elsewhere; nH, n_e and rhokap are remapped by
+ * overlap volume, the ion fractions by nH V, T_e by (nH (1 + He/H) + n_e) V,
+ * and the seven conserved box integrals (H nuclei, H I, He I, He II,
+ * electrons, extinction, thermal content) must agree to 1e-8.  Every
+ * leaf-indexed buffer changes size, so the result is a NEW context:
+ * mochii_refine_front writes the new leaf list to out_list (the generic
+ * text format, with the remapped x_HI, x_HeI, x_HeII, n_e, T_e and rhokap
+ * as extra columns), initialises *out from it with ctx's parameters and
+ * sets the remapped state; ctx is left as it was (destroy it when done).
+ * The grains' rhokap of the new context follows from the remapped nH as
+ * at any set-up (the same volume remap for the supported dust laws).
+ * mochii_refine_plan is the host part alone (no device): the old leaf
+ * list, its state (rhokap may be NULL), and the new leaf list out;
+ * counts2 = new leaf count and front leaves, *worst = the largest relative
+ * change of a conserved integral; mochii_refine_last_error explains a
+ * failure of either. */
+int mochii_refine_plan(const char* in_list, const double* nH, const double* xHI, const double* xHeI,
+                       const double* xHeII, const double* ne, const double* Te, const double* rhokap,
+                       double He_abund, double te_min, int lbase, int lmax, double eps, double dx,
+                       const char* out_list, int64_t* counts2, double* worst);
+int mochii_refine_front(mochii_ctx* ctx, const char* out_list, mochii_ctx** out);
+const char* mochii_refine_last_error(void);
 
 /* gas_opacity_fill: refresh the per-leaf absorber columns the transport reads. */
 int mochii_opacity_fill(mochii_ctx* ctx);

@@ -64,6 +64,8 @@ class Params(C.Structure):
         ("phase_angle", C.c_double * MAX_OBS), ("inclination_angle", C.c_double * MAX_OBS),
         ("position_angle", C.c_double * MAX_OBS),
         ("hei_diffuse", C.c_int),
+        ("refine_front", C.c_int), ("refine_iter", C.c_int), ("refine_lbase", C.c_int), ("refine_lmax", C.c_int),
+        ("refine_eps", C.c_double), ("refine_dx", C.c_double),
     ]
 
 
@@ -130,6 +132,11 @@ SIGNATURES = {
     "mochii_write_image": (C.c_int, [C.c_void_p, C.c_char_p]),
     "mochii_dust_ir": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "mochii_write_dust_ir": (C.c_int, [C.c_void_p, C.c_char_p]),
+    "mochii_refine_plan": (C.c_int, [C.c_char_p] + [C.c_void_p] * 7 + [C.c_double, C.c_double, C.c_int, C.c_int,
+                                                                       C.c_double, C.c_double, C.c_char_p,
+                                                                       C.c_void_p, C.c_void_p]),
+    "mochii_refine_front": (C.c_int, [C.c_void_p, C.c_char_p, C.c_void_p]),
+    "mochii_refine_last_error": (C.c_char_p, []),
     "mochii_set_field": (C.c_int, [C.c_void_p, C.c_char_p, C.c_void_p, C.c_int64]),
     "mochii_set_nphotons": (C.c_int, [C.c_void_p, C.c_int64]),
     "mochii_ion_Ltot": (C.c_double, [C.c_void_p]),

@@ -37,8 +37,8 @@ const char* const kOtherKeys[] = {
     "lambda0", "lambda_max", "lambda_min", "line_case", "mrw_gamma", "nlambda", "no_print",
     "nobs", "nprint", "nr", "nscatt_tot", "num_send_at_once",
     "out_bitpix", "out_bitpix_force", "out_file", "output_normalization", "pe_scale",
-    "radiation_angular_pdf_file", "reduce_factor", "refine_dx",
-    "refine_eps", "refine_front", "refine_iter", "refine_lbase", "refine_lmax", "save_jlam",
+    "radiation_angular_pdf_file", "reduce_factor",
+    "save_jlam",
     "scatt_mat_file", "sed_data_dir", "sed_dl07_sdindex", "sed_dl07_uisrf", "sed_kext", "sed_nt",
     "sed_pah_live", "sed_thi", "sed_tlo", "sightline_tau", "slab_bot_mode", "slab_bot_phi",
     "slab_bot_source", "slab_bot_theta", "slab_faces", "slab_nmu", "slab_top_mode", "slab_top_phi",
@@ -145,6 +145,8 @@ extern "C" int mochii_params_default(mochii_params* p) {
     p->packet_order = 2;   // 'coherent' (the launch order where it does not apply)
     p->ion_peel = 0; p->peel_bins = 0; p->save_direc0 = 0;
     p->nxim = 129; p->nyim = 129;   // define.f90:531-532
+    p->refine_front = 0; p->refine_iter = 20; p->refine_lbase = 5; p->refine_lmax = 7;   // define.f90:826-831
+    p->refine_eps = 1.0e-2; p->refine_dx = 0.2;
     const double nan = std::numeric_limits<double>::quiet_NaN();
     p->distance = nan; p->dxim = nan; p->dyim = nan;
     for (int i = 0; i < MOCHII_MAX_OBS; ++i) {
@@ -288,6 +290,8 @@ int set_key(mochii_params* p, std::string key, const std::vector<std::string>& v
     BOOL("metal_freefree", metal_freefree) BOOL("gaunt_vh14", gaunt_vh14)
     BOOL("fe_levels_full", fe_levels_full)
     BOOL("diffuse_field", diffuse_field) BOOL("use_sec_ion", use_sec_ion) BOOL("hei_diffuse", hei_diffuse)
+    BOOL("refine_front", refine_front) INT("refine_iter", refine_iter) INT("refine_lbase", refine_lbase)
+    INT("refine_lmax", refine_lmax) REAL("refine_eps", refine_eps) REAL("refine_dx", refine_dx)
     BOOL("ion_add_dust", ion_add_dust) BOOL("ion_dust_scatter", ion_dust_scatter) BOOL("grain_pe", grain_pe)
     REAL("dgr", DGR) REAL("cext_dust", cext_dust) REAL("lambda_ref", lambda_ref)
     REAL("taumax", taumax) REAL("tauhomo", tauhomo)

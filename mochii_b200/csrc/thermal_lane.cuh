@@ -576,6 +576,12 @@ struct CellSolve {
 // thermal_bracketed's temperature search for one lane: TRoot.
 using TempSearch = TRoot;
 
+// Solver trips between the block barriers of lane_solve.
+#ifndef MOCHII_LANE_SYNC_TRIPS
+#define MOCHII_LANE_SYNC_TRIPS 1
+#endif
+constexpr int kLaneSyncTrips = MOCHII_LANE_SYNC_TRIPS;
+
 // One lane's leaf.
 struct LaneLeaf {
     long long il;
@@ -706,12 +712,13 @@ __device__ __noinline__ void lane_solve(const ThArgs& a, unsigned long long* nex
     cs.yHe = b.yHe;
     cs.with_ne = b.metal_ne;
     cs.with_cx = b.two_way;
-    for (;;) {
+    for (int trip = 0;; ++trip) {
         lane_claim(a, next, L, exhausted, lane);
-        // every warp of the block takes the same trips, one barrier each: the
-        // block's warps stay at the same point of the solver's code, which
-        // then stays in the instruction cache
-        if (!__syncthreads_or(L.has ? 1 : 0)) return;
+        // every warp of the block takes the same trips, with a barrier every
+        // kLaneSyncTrips of them: the block's warps stay near the same point
+        // of the solver's code, which then stays in the instruction cache.
+        // Only a barrier trip ends the loop, for every warp at once.
+        if (trip % kLaneSyncTrips == 0 && !__syncthreads_or(L.has ? 1 : 0)) return;
         const bool ev = L.has;   // every lane with a leaf evaluates its net rate at ts.t
         const double T = L.ts.t;
         bool need = false;

@@ -11,6 +11,8 @@ Every call goes through libmochii_gpu.so; errors come back as MochiiError
 carrying the library's status code (the reference aborts instead).
 """
 import ctypes as C
+import os
+import tempfile
 
 import numpy as np
 
@@ -88,11 +90,13 @@ def philox_uniforms(seed, stream, packet, n0, n):
 class Nebula:
     """One nebula on the current CUDA device (a mochii_ctx)."""
 
-    def __init__(self, par):
+    def __init__(self, par, _ctx=None):
         self.lib = _lib.load()
         self.par = par
-        h = C.c_void_p()
-        _check(self.lib, self.lib.mochii_init(C.byref(par), C.byref(h)))
+        h = _ctx
+        if h is None:
+            h = C.c_void_p()
+            _check(self.lib, self.lib.mochii_init(C.byref(par), C.byref(h)))
         self.ctx = h
         self.nleaf = int(self.lib.mochii_nleaf(h))
         self.nnu_band = int(self.lib.mochii_nnu_band(h))
@@ -172,6 +176,18 @@ class Nebula:
                      int(bool(field_consistent)))
         self._ok(self.lib.mochii_write_rates(self.ctx, str(base).encode(), C.byref(ri)))
         return str(base) + "_rates"
+
+    def refine_front(self, out_list):
+        """amr_refine_front: the octree rebuilt on the current solution
+        (par%refine_lbase, refine_lmax, refine_eps, refine_dx) as a NEW
+        nebula whose leaf list is written to out_list, its state remapped by
+        overlap volume; this nebula stays as it was."""
+        h = C.c_void_p()
+        self._ok(self.lib.mochii_refine_front(self.ctx, str(out_list).encode(), C.byref(h)))
+        par = _lib.Params()
+        C.memmove(C.byref(par), C.byref(self.par), C.sizeof(par))
+        par.amr_file = str(out_list).encode()
+        return Nebula(par, _ctx=h)
 
     def dust_ir(self):
         """The grains' infrared spectrum of the equilibrium dust temperature
@@ -297,6 +313,13 @@ def run(par, log=None, final_pass=True):
             rec.update(max_dx=max_dx, dx_vol=dx_vol)
         rec["balance_ms"] = neb.last_metrics.kernel_ms
         neb.gas_opacity_fill()
+        if par.refine_front and it == par.refine_iter:   # one re-refinement event (main.f90:172-178)
+            work = tempfile.mkdtemp(prefix="mochii_refine_")
+            new = neb.refine_front(os.path.join(work, f"leaves_refined_{it}.txt"))
+            rec["refined"] = {"leaves_before": neb.nleaf, "leaves_after": new.nleaf}
+            neb.close()
+            neb, par = new, new.par
+            converged = False   # keep iterating on the new grid
         history.append(rec)
         if log:
             log(rec)
@@ -307,6 +330,27 @@ def run(par, log=None, final_pass=True):
     if final_pass and par.gas_niter >= 1:
         neb.ionizing_field_and_rates()   # final consistency pass, main.f90:225
     return neb, history
+
+
+def refine_plan(in_list, state, rhokap=None, He_abund=0.1, te_min=1.0e3, lbase=5, lmax=7, eps=1.0e-2, dx=0.2,
+                out_list="refined.txt"):
+    """The host part of amr_refine_front without a device: the leaf list
+    in_list with its state (dict of nH, x_HI, x_HeI, x_HeII, n_e, T_e) to a
+    new leaf list out_list (remapped state as extra columns).  Returns
+    (new leaf count, front leaves, largest relative change of a conserved
+    box integral)."""
+    lib = _lib.load()
+    f = [np.ascontiguousarray(state[k], dtype=np.float64) for k in ("nH", "x_HI", "x_HeI", "x_HeII", "n_e", "T_e")]
+    rk = None if rhokap is None else np.ascontiguousarray(rhokap, dtype=np.float64)
+    counts = np.zeros(2, dtype=np.int64)
+    worst = C.c_double()
+    rc = lib.mochii_refine_plan(str(in_list).encode(), *[a.ctypes.data for a in f],
+                                None if rk is None else rk.ctypes.data, float(He_abund), float(te_min), int(lbase),
+                                int(lmax), float(eps), float(dx), str(out_list).encode(), counts.ctypes.data,
+                                C.byref(worst))
+    if rc != _lib.OK:
+        raise MochiiError(rc, lib.mochii_refine_last_error().decode())
+    return int(counts[0]), int(counts[1]), worst.value
 
 
 class Batch:

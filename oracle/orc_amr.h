@@ -31,4 +31,17 @@ bool read_leaf_list(const std::string& path, std::vector<double>& x, std::vector
                     std::vector<double>& z, std::vector<int>& lev, std::vector<double>& nH, double* boxlen,
                     std::string* err);
 
+// amr_refine_front (amr_refine_mod.f90:46-436): front flags on the old
+// leaves, the new leaf list (rec_build / cell_has_front), the overlap-volume
+// remap (remap_leaf) and the conserved box integrals (conservation_report).
+// st6 = nH, x_HI, x_HeI, x_HeII, n_e, T_e per old leaf; rk may be empty.
+struct RefineResult {
+    std::vector<double> x, y, z, nH, x1, x2, x3, ne, te, rk;
+    std::vector<int> lev;
+    long long nfront = 0;
+    double worst = 0.0;
+};
+bool refine_front(const Octree& o, const std::vector<double>* st6, const std::vector<double>& rk, double yHe,
+                  double te_min, int lbase, int lmax, double eps, double dx, RefineResult& r, std::string* err);
+
 }  // namespace orc

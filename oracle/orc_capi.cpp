@@ -1,11 +1,13 @@
 // Oracle C entry points for ctypes (test infrastructure only).
 #include <algorithm>
+#include <cstdio>
 #include <cstring>
 #include <string>
 
 #include "orc_core.h"
 #include "orc_thermal.h"
 #include "orc_species.h"
+#include "orc_amr.h"
 
 using namespace orc;
 
@@ -590,6 +592,40 @@ int orc_sim_dust_temp(void* h, double* out, double* lam, double* ir) {
             ir[k] += fourpi * kd * t.sabs_ir[k] * planck_nu(nu, td[il]) * vol;
         }
     }
+    return 0;
+}
+
+
+// amr_refine_front on the leaf list in_list with state st6 (6 x nleaf:
+// nH, x_HI, x_HeI, x_HeII, n_e, T_e) and rhokap rk (NULL: none): the new
+// leaf list in the library's refined-list format (%.17g; x y z level nH
+// x_HI x_HeI x_HeII n_e T_e rhokap) to out_list; counts2 = new leaves,
+// front leaves; *worst = largest relative change of a conserved integral.
+int orc_refine_plan(const char* in_list, const double* st6, const double* rk, double yHe, double te_min, int lbase,
+                    int lmax, double eps, double dx, const char* out_list, long long* counts2, double* worst) {
+    std::vector<double> x, y, z, nH;
+    std::vector<int> lev;
+    double boxlen = 0.0;
+    if (!read_leaf_list(in_list, x, y, z, lev, nH, &boxlen, &g_err)) return 1;
+    Octree o;
+    o.build(x, y, z, lev, 0.5 * boxlen);
+    const size_t n = x.size();
+    std::vector<double> st[6];
+    for (int k = 0; k < 6; ++k) st[k].assign(st6 + k * n, st6 + (k + 1) * n);
+    std::vector<double> r_k;
+    if (rk) r_k.assign(rk, rk + n);
+    RefineResult r;
+    if (!refine_front(o, st, r_k, yHe, te_min, lbase, lmax, eps, dx, r, &g_err)) return 2;
+    FILE* f = std::fopen(out_list, "w");
+    if (!f) return 3;
+    std::fprintf(f, "%zu %.17g\n", r.x.size(), boxlen);
+    for (size_t i = 0; i < r.x.size(); ++i)
+        std::fprintf(f, "%.17g %.17g %.17g %d %.17g %.17g %.17g %.17g %.17g %.17g %.17g\n", r.x[i], r.y[i], r.z[i],
+                     r.lev[i], r.nH[i], r.x1[i], r.x2[i], r.x3[i], r.ne[i], r.te[i], r.rk[i]);
+    std::fclose(f);
+    counts2[0] = (long long)r.x.size();
+    counts2[1] = r.nfront;
+    *worst = r.worst;
     return 0;
 }
 

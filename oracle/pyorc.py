@@ -90,6 +90,7 @@ def load():
         "orc_thermal_1d": (I, [C.c_char_p, V, I, I, V]),
         "orc_hei_2ph": (I, [C.c_char_p, D, V, LL, V, V]),
         "orc_sim_dust_temp": (I, [V, V, V, V]),
+        "orc_refine_plan": (I, [C.c_char_p, V, V, D, D, I, I, D, D, C.c_char_p, V, V]),
         "orc_hei_branch_energies": (I, [C.c_char_p, D, D, D, V]),
     }
     for name, (res, args) in sig.items():
@@ -213,6 +214,23 @@ def hei_branch_energies(path, T, xHI, xHeI):
     if load().orc_hei_branch_energies(str(path).encode(), float(T), float(xHI), float(xHeI), out.ctypes.data):
         raise RuntimeError(load().orc_last_error().decode())
     return tuple(out)
+
+
+def refine_plan(in_list, state, rhokap=None, yHe=0.1, te_min=1.0e3, lbase=5, lmax=7, eps=1.0e-2, dx=0.2,
+                out_list="refined_oracle.txt"):
+    """amr_refine_front restated: (new leaves, front leaves, worst relative
+    change of a conserved integral); the new list goes to out_list."""
+    st = np.ascontiguousarray(np.stack([state[k] for k in ("nH", "x_HI", "x_HeI", "x_HeII", "n_e", "T_e")]),
+                              dtype=np.float64)
+    rk = None if rhokap is None else np.ascontiguousarray(rhokap, dtype=np.float64)
+    counts = np.zeros(2, dtype=np.int64)
+    worst = np.zeros(1)
+    rc = load().orc_refine_plan(str(in_list).encode(), st.ctypes.data, None if rk is None else rk.ctypes.data,
+                                float(yHe), float(te_min), int(lbase), int(lmax), float(eps), float(dx),
+                                str(out_list).encode(), counts.ctypes.data, worst.ctypes.data)
+    if rc:
+        raise RuntimeError(f"orc_refine_plan: {rc} {load().orc_last_error().decode()}")
+    return int(counts[0]), int(counts[1]), float(worst[0])
 
 
 def thermal_1d(atomic_dir, nr=8000, nsweep=4, nnu=32, emin=13.598, emax=100.0, tstar=4.0e4,
