@@ -192,6 +192,17 @@ typedef struct mochii_params {
      * elsewhere (mochii_refine_front) */
     int refine_front, refine_iter, refine_lbase, refine_lmax;
     double refine_eps, refine_dx;
+    /* isotropic external radiation field (define.f90:266-278): on when
+     * ext_intensity (band J [erg/s/cm^2/sr]) > 0, a source component after
+     * the nsource point sources entering through the box faces
+     * (ext_geometry 0 'rec') or a bounding sphere of radius rmax (1 'sph');
+     * Planck spectrum at ext_tstar (> 0) else tstar.  source_geometry
+     * 'external' / 'external_rec' / 'external_sph' is the external-only
+     * shorthand (source_external 1 / 1 / 2: nsource taken as 0).
+     * ext_spectrum_set: a par%ext_spectrum file or preset was named (not
+     * built; refused) */
+    double ext_intensity, ext_tstar;
+    int ext_geometry, source_external, ext_spectrum_set;
 } mochii_params;
 
 /* Per-pass statistics (ion_score_report_energy_closure, ion_score_mod.f90:364-387). */

@@ -66,6 +66,8 @@ class Params(C.Structure):
         ("hei_diffuse", C.c_int),
         ("refine_front", C.c_int), ("refine_iter", C.c_int), ("refine_lbase", C.c_int), ("refine_lmax", C.c_int),
         ("refine_eps", C.c_double), ("refine_dx", C.c_double),
+        ("ext_intensity", C.c_double), ("ext_tstar", C.c_double), ("ext_geometry", C.c_int),
+        ("source_external", C.c_int), ("ext_spectrum_set", C.c_int),
     ]
 
 

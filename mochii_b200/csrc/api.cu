@@ -136,6 +136,8 @@ int validate(const mochii_params& p, std::string* why, int* code) {
         return *why = "the taumax / tauhomo dust normalisations are not built", 1;
     if (p.ion_add_dust && !p.ion_dust_kext[0])
         return *why = "ion_add_dust needs par%ion_dust_kext (the grain-model optics are not built)", 1;
+    if (p.ion_peel && (p.ext_intensity > 0.0 || p.source_external))
+        return *why = "the peel-off of external-field packets is not built", 1;
     if (p.use_sec_ion) return *why = "use_sec_ion is not built in this library version", 1;
     if (p.grain_pe) return *why = "grain_pe is not built in this library version", 1;
     return 0;
@@ -184,10 +186,6 @@ extern "C" int mochii_init(const mochii_params* pin, mochii_ctx** out) {
         delete c;
         return fail(nullptr, MOCHII_ERR_TABLE, why);
     }
-    if (!band_build(p, c->band, &why, c->species.thresholds())) {
-        delete c;
-        return fail(nullptr, MOCHII_ERR_BAD_PARAM, why);
-    }
     cudaGetDevice(&c->device);
     Grid& g = c->grid;
     // octree from a text leaf list (grid_mod_amr.f90:50-62, read_generic_amr.f90:60-81,
@@ -219,6 +217,13 @@ extern "C" int mochii_init(const mochii_params* pin, mochii_ctx** out) {
         g.ymin = -p.ymax; g.ymax = p.ymax;
         g.zmin = -p.zmax; g.zmax = p.zmax;
         g.dcell = (g.xmax - g.xmin) / (double)g.nx;
+    }
+    {   // the band after the grid: an external field enters through the box
+        const double box[3] = {g.xmax - g.xmin, g.ymax - g.ymin, g.zmax - g.zmin};
+        if (!band_build(p, c->band, &why, c->species.thresholds(), box)) {
+            delete c;
+            return fail(nullptr, MOCHII_ERR_BAD_PARAM, why);
+        }
     }
     c->fp32 = p.precision == MOCHII_PREC_FP32;
     c->tally64 = !c->fp32 || p.tally64;

@@ -229,7 +229,8 @@ bool aligned_edges(std::vector<double>& edge, int nfuv, int nnu, double lo, doub
 // ion_setup + setup_continuous_source_sampler + build_point_source_sampler
 // (ion_band_mod.f90:122-258, :275-353, :437-495) for internal point sources
 // with Planck spectra, and ion_qmc_ndim (:654-663).
-bool band_build(const mochii_params& p, BandSetup& b, std::string* err, const std::vector<double>& metal_eth) {
+bool band_build(const mochii_params& p, BandSetup& b, std::string* err, const std::vector<double>& metal_eth,
+                const double* box) {
     const int nfuv = p.add_fuv ? p.nnu_fuv : 0;
     if (p.add_fuv && p.efuv_min >= p.eion_min) return fail(err, "add_fuv requires par%efuv_min < par%eion_min");
     if (p.nnu_ion < 1) return fail(err, "par%nnu_ion must be >= 1");
@@ -246,11 +247,21 @@ bool band_build(const mochii_params& p, BandSetup& b, std::string* err, const st
         for (int i = nfuv; i <= nnu; ++i)
             b.eedge[i] = std::exp(lo + (hi - lo) * (double)(i - nfuv) / (double)(nnu - nfuv));
     }
-    if (!p.source_point) return fail(err, "only point sources are built (par%source_geometry = 'point')");
-    if (p.nsource < 1 || p.nsource > MOCHII_MAX_SRC) return fail(err, "par%nsource out of range");
-    b.ncomp = p.nsource;
+    if (!p.source_point) return fail(err, "only point sources and external fields are built (par%source_geometry)");
+    // components (ion_band_mod.f90:188-199, 683-711): the point sources, then
+    // the external field when par%ext_intensity > 0
+    const bool ext_on = p.ext_intensity > 0.0;
+    if (p.ext_spectrum_set) return fail(err, "par%ext_spectrum (files and ISRF presets) is not built");
+    if (p.source_external && !ext_on)
+        return fail(err, "external source_geometry requires par%ext_intensity > 0 (setup.f90:249-254)");
+    const int npt = p.source_external ? 0 : p.nsource;
+    if (npt < 0 || npt > MOCHII_MAX_SRC) return fail(err, "par%nsource out of range");
+    b.ncomp = npt + (ext_on ? 1 : 0);
+    if (b.ncomp < 1) return fail(err, "no source: par%nsource = 0 without an external field");
     b.multi = b.ncomp >= 2;
-    b.qmc_ndim = b.multi ? 7 : 3;
+    b.ext_ic = ext_on ? b.ncomp - 1 : -1;
+    b.ext_sph = p.source_external ? (p.source_external == 2) : (p.ext_geometry == 1);
+    b.qmc_ndim = (b.ncomp == 1 && !ext_on) ? 3 : 7;   // ion_qmc_ndim (:654-663)
     const double elo = p.add_fuv ? p.efuv_min : p.eion_min;
     // photoionization_threshold_knots (ion_band_mod.f90:408-419): H, He, the
     // metal thresholds in registry order, then eion_min with the FUV band
@@ -263,7 +274,27 @@ bool band_build(const mochii_params& p, BandSetup& b, std::string* err, const st
     b.comp_z.assign(b.ncomp, 0.0);
     std::vector<double> L(b.ncomp);
     for (int c = 0; c < b.ncomp; ++c) {
-        const double T = b.multi ? p.src_tstar[c] : p.tstar;
+        if (c == b.ext_ic) {   // build_external_field_sampler (:516-615), Planck spectra
+            const double T = p.ext_tstar > 0.0 ? p.ext_tstar : p.tstar;
+            if (T <= 0.0) return fail(err, "external field needs a Planck temperature (par%ext_tstar / par%tstar)");
+            if (!planck_table(b.tables[c], T, elo, p.eion_max, p.source_cdf_tol, knots, err)) return false;
+            if (!box) return fail(err, "external field: the box extent is unknown");
+            double asurf;
+            if (b.ext_sph) {
+                if (!(p.rmax > 0.0)) return fail(err, "ext_geometry 'sph' needs par%rmax > 0");
+                if (2.0 * p.rmax > std::min(box[0], std::min(box[1], box[2])))
+                    return fail(err, "ext_geometry 'sph': the bounding sphere (par%rmax) must lie inside the grid");
+                asurf = 4.0 * kPi * ((p.rmax * p.distance2cm) * (p.rmax * p.distance2cm));
+            } else {
+                const double xr = box[0] * p.distance2cm, yr = box[1] * p.distance2cm, zr = box[2] * p.distance2cm;
+                asurf = 2.0 * (xr * yr + yr * zr + zr * xr);
+            }
+            const double f_ion = 1.0 - table_cdf(b.tables[c], p.eion_min);
+            if (f_ion <= 0.0) return fail(err, "the external spectrum has no luminosity inside the ionizing band");
+            L[c] = kPi * p.ext_intensity * asurf / f_ion;
+            continue;
+        }
+        const double T = (b.multi && p.src_tstar[c] > 0.0) ? p.src_tstar[c] : p.tstar;
         const double scale = b.multi ? p.src_lum[c] : p.luminosity;
         if (T <= 0.0) return fail(err, "point source needs a Planck temperature (par%tstar / par%src_tstar)");
         if (scale <= 0.0) return fail(err, "point source needs a luminosity (par%luminosity / par%src_lum)");

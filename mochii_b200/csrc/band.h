@@ -32,10 +32,15 @@ struct BandSetup {
     std::vector<double> comp_x, comp_y, comp_z;
     std::vector<EnergyTable> tables;    // one per component
     double ion_Ltot = 0.0;
+    int ext_ic = -1;                    // component of the external field, -1 none
+    int ext_sph = 0;                    // its entry surface: 0 the box faces, 1 the sphere of radius rmax
 };
 
 // metal_eth: the active metal thresholds in registry order (main.f90:65-82),
 // which pin band edges and sampler knots as the H/He thresholds do.
-bool band_build(const mochii_params& p, BandSetup& b, std::string* err, const std::vector<double>& metal_eth = {});
+// box: the grid's x, y, z extents in code units (the external field's entry
+// surface), null when unknown.
+bool band_build(const mochii_params& p, BandSetup& b, std::string* err, const std::vector<double>& metal_eth = {},
+                const double* box = nullptr);
 
 }  // namespace mochii

@@ -31,7 +31,7 @@ const char* const kOtherKeys[] = {
     "density_rscale", "density_zprofile", "density_zscale",
     "dust_emis_bands", "dust_emis_transport", "dust_emission_method", "dust_fast_table", "dust_model",
     "dust_niter", "dust_no_photons", "dust_nu", "dust_sed", "dust_single_teq", "dust_tol",
-    "emis_output", "exetime", "ext_geometry", "ext_intensity", "ext_scale", "ext_spectrum", "ext_tstar",
+    "emis_output", "exetime", "ext_scale",
     "f_ion_dust", "f_ion_pah", "f_pah", "file_format", "geometry", "h_coll_effects",
     "hei_metastable", "hgg", "ion_spectrum", "kext_file",
     "lambda0", "lambda_max", "lambda_min", "line_case", "mrw_gamma", "nlambda", "no_print",
@@ -147,6 +147,7 @@ extern "C" int mochii_params_default(mochii_params* p) {
     p->nxim = 129; p->nyim = 129;   // define.f90:531-532
     p->refine_front = 0; p->refine_iter = 20; p->refine_lbase = 5; p->refine_lmax = 7;   // define.f90:826-831
     p->refine_eps = 1.0e-2; p->refine_dx = 0.2;
+    p->ext_intensity = -1.0; p->ext_tstar = -999.0; p->ext_geometry = 0;   // define.f90:270-277
     const double nan = std::numeric_limits<double>::quiet_NaN();
     p->distance = nan; p->dxim = nan; p->dyim = nan;
     for (int i = 0; i < MOCHII_MAX_OBS; ++i) {
@@ -218,8 +219,18 @@ int set_key(mochii_params* p, std::string key, const std::vector<std::string>& v
     if (key == "source_geometry") {
         const std::string s = lower(unquote(v));
         p->source_point = s == "point";
+        p->source_external = (s == "external" || s == "external_rec") ? 1 : s == "external_sph" ? 2 : 0;
+        if (p->source_external) p->source_point = 1;   // the external-only shorthand of setup.f90:240-258
         return 0;
     }
+    if (key == "ext_geometry") {
+        const std::string s = lower(unquote(v));
+        if (s != "rec" && s != "sph") return bad("must be 'rec' or 'sph'");
+        p->ext_geometry = s == "sph" ? 1 : 0;
+        return 0;
+    }
+    if (key == "ext_spectrum") { p->ext_spectrum_set = unquote(v).find_first_not_of(' ') != std::string::npos; return 0; }
+    REAL("ext_intensity", ext_intensity) REAL("ext_tstar", ext_tstar)
     REAL("xs_point", xs_point) REAL("ys_point", ys_point) REAL("zs_point", zs_point)
     INT("nsource", nsource)
     if (key == "alpha" || key == "beta" || key == "gamma" || key == "obsx" || key == "obsy" || key == "obsz" ||

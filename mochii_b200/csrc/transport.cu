@@ -57,6 +57,9 @@ struct PassArgs {
     double dcell;
     int n[3];
     int ncomp, multi, ndim, nnu;
+    int ext_ic, ext_sph;   // the external field's component (-1 none) and entry surface (0 box faces, 1 sphere)
+    double ext_rmax;       // the entry sphere's radius (code units)
+    double bmin[3], bmax[3];   // the grid box (code units)
     MetalDev m;          // trace metals; m.ntr == 0 without
     int metal_abs;       // par%ion_metal_abs
     OctDev oct;          // octree grid; oct.ncells == 0 on the Cartesian grid
@@ -277,6 +280,109 @@ __device__ double block_sum(double v, double* sh) {
 //
 // AMR: the octree variant stages the complete top levels of the tree in
 // shared memory for the start-leaf search.
+// emit_external_rec_qmc (ion_band_mod.f90:2253-2323): the isotropic
+// external field entering the box: an area-weighted face (u_face), a
+// Lambert incidence about its inward normal (mu = sqrt(u_mu), azimuth
+// 2 pi u_phi), the entry point uniform on the face (u_c1, u_c2), nudged
+// 1e-6 of the smallest extent inside.
+__device__ void emit_external_rec(const PassArgs& a, double u_mu, double u_phi, double u_face, double u_c1,
+                                  double u_c2, double pos[3], double kk[3]) {
+    const double xr = a.bmax[0] - a.bmin[0], yr = a.bmax[1] - a.bmin[1], zr = a.bmax[2] - a.bmin[2];
+    const double nudge = 1.0e-6 * fmin(xr, fmin(yr, zr));
+    double fcum[6];
+    fcum[0] = yr * zr;
+    fcum[1] = fcum[0] + yr * zr;
+    fcum[2] = fcum[1] + zr * xr;
+    fcum[3] = fcum[2] + zr * xr;
+    fcum[4] = fcum[3] + xr * yr;
+    fcum[5] = fcum[4] + xr * yr;
+    const double fpick = u_face * fcum[5];
+    int f = 5;
+    for (int k = 0; k < 6; ++k)
+        if (fpick <= fcum[k]) { f = k; break; }
+    const double mu = sqrt(u_mu), sinm = sqrt(1.0 - mu * mu);
+    double sphi, cphi;
+    sincos(kTwoPi * u_phi, &sphi, &cphi);
+    const int ax = f >> 1;                        // the face's axis: x, y, z
+    const double sgn = (f & 1) ? 1.0 : -1.0;      // inward normal along it: -1 on the + face
+    const int a1 = ax == 0 ? 1 : 0, a2 = ax == 2 ? 1 : 2;   // the in-face coordinates, in order
+    pos[ax] = (f & 1) ? a.bmin[ax] + nudge : a.bmax[ax] - nudge;
+    pos[a1] = a.bmin[a1] + (a.bmax[a1] - a.bmin[a1]) * u_c1;
+    pos[a2] = a.bmin[a2] + (a.bmax[a2] - a.bmin[a2]) * u_c2;
+    kk[ax] = sgn * mu;
+    kk[a1] = sinm * cphi;
+    kk[a2] = sinm * sphi;
+}
+
+// emit_external_sph_qmc (:2328-2361) with ortho_frame (:2368-2385): the
+// entry point uniform on the sphere of radius rmax about the box centre
+// (u_cost, u_saz), a Lambert incidence about the inward radial (u_mu,
+// u_phi) in a frame completed from the coordinate axis most orthogonal to
+// it, the point nudged inside.
+__device__ void emit_external_sph(const PassArgs& a, double u_mu, double u_phi, double u_cost, double u_saz,
+                                  double pos[3], double kk[3]) {
+    const double xc = 0.5 * (a.bmin[0] + a.bmax[0]), yc = 0.5 * (a.bmin[1] + a.bmax[1]);
+    const double zc = 0.5 * (a.bmin[2] + a.bmax[2]);
+    const double cost = 2.0 * u_cost - 1.0, sint = sqrt(1.0 - cost * cost);
+    double sp, cp;
+    sincos(kTwoPi * u_saz, &sp, &cp);
+    const double rx = sint * cp, ry = sint * sp, rz = cost;
+    pos[0] = xc + a.ext_rmax * rx;
+    pos[1] = yc + a.ext_rmax * ry;
+    pos[2] = zc + a.ext_rmax * rz;
+    const double nx = -rx, ny = -ry, nz = -rz;
+    double tx, ty, tz;
+    if (fabs(nx) <= fabs(ny) && fabs(nx) <= fabs(nz)) { tx = 0.0; ty = nz; tz = -ny; }
+    else if (fabs(ny) <= fabs(nz)) { tx = -nz; ty = 0.0; tz = nx; }
+    else { tx = ny; ty = -nx; tz = 0.0; }
+    const double inv = 1.0 / sqrt(tx * tx + ty * ty + tz * tz);
+    tx = tx * inv; ty = ty * inv; tz = tz * inv;
+    const double bx = ny * tz - nz * ty, by = nz * tx - nx * tz, bz = nx * ty - ny * tx;
+    const double mu = sqrt(u_mu), sinm = sqrt(1.0 - mu * mu);
+    double sphi, cphi;
+    sincos(kTwoPi * u_phi, &sphi, &cphi);
+    kk[0] = -mu * rx + sinm * (cphi * tx + sphi * bx);
+    kk[1] = -mu * ry + sinm * (cphi * ty + sphi * by);
+    kk[2] = -mu * rz + sinm * (cphi * tz + sphi * bz);
+    const double nudge = 1.0e-6 * fmin(a.bmax[0] - a.bmin[0], fmin(a.bmax[1] - a.bmin[1], a.bmax[2] - a.bmin[2]));
+    pos[0] = pos[0] - nudge * rx;
+    pos[1] = pos[1] - nudge * ry;
+    pos[2] = pos[2] - nudge * rz;
+}
+
+// The launch of one stellar packet from its uniforms u (gen_ion_photon_qmc,
+// ion_band_mod.f90:1880-1935): a single point source reads u1 energy, u2 mu,
+// u3 phi; every other configuration the superset layout -- u1 component,
+// u2 energy, u3/u4 angles, u5-u7 the entry surface of an external field.
+__device__ __forceinline__ void launch_packet(const PassArgs& a, const double* u, int& ic, double& E, double pos[3],
+                                              double kk[3]) {
+    ic = 0;
+    double umu, uphi, ue;
+    if (a.ndim == 3) {
+        ue = u[0]; umu = u[1]; uphi = u[2];
+    } else {
+        if (a.multi) {
+            ic = a.ncomp - 1;
+            for (int k = 0; k < a.ncomp; ++k)
+                if (u[0] <= a.comp[4 * k]) { ic = k; break; }
+        }
+        ue = u[1]; umu = u[2]; uphi = u[3];
+    }
+    const int t0 = a.tab_off[ic], t1 = a.tab_off[ic + 1];
+    E = sample_energy(a.tab_e + t0, a.tab_f + t0, a.tab_c + t0, t1 - t0, ue);
+    if (ic == a.ext_ic) {
+        if (a.ext_sph) emit_external_sph(a, u[2], u[3], u[4], u[5], pos, kk);
+        else emit_external_rec(a, u[2], u[3], u[4], u[5], u[6], pos, kk);
+    } else {   // emit_point_qmc (:2232-2247)
+        pos[0] = a.comp[4 * ic + 1]; pos[1] = a.comp[4 * ic + 2]; pos[2] = a.comp[4 * ic + 3];
+        const double cost = 2.0 * umu - 1.0;
+        const double sint = sqrt(1.0 - cost * cost);
+        double sphi, cphi;
+        sincos(kTwoPi * uphi, &sphi, &cphi);
+        kk[0] = sint * cphi; kk[1] = sint * sphi; kk[2] = cost;
+    }
+}
+
 template <typename R, bool AMR>
 __global__ void __launch_bounds__(kThreads) k_launch(const PassArgs a, PacketRecords rec, long long ip0, long long n) {
     __shared__ QmcTables sq;
@@ -295,24 +401,9 @@ __global__ void __launch_bounds__(kThreads) k_launch(const PassArgs a, PacketRec
     const long long ip = ip0 + (rec.order ? (long long)rec.order[i] : i);
     double u[7];
     for (int d = 0; d < a.ndim; ++d) u[d] = qmc_uniform(sq, (uint64_t)ip, d, 0);
-    int ic = 0;
-    double umu, uphi, ue;
-    if (!a.multi) {
-        ue = u[0]; umu = u[1]; uphi = u[2];
-    } else {
-        ic = a.ncomp - 1;
-        for (int k = 0; k < a.ncomp; ++k)
-            if (u[0] <= a.comp[4 * k]) { ic = k; break; }
-        ue = u[1]; umu = u[2]; uphi = u[3];
-    }
-    const int t0 = a.tab_off[ic], t1 = a.tab_off[ic + 1];
-    const double E = sample_energy(a.tab_e + t0, a.tab_f + t0, a.tab_c + t0, t1 - t0, ue);
-    const double pos[3] = {a.comp[4 * ic + 1], a.comp[4 * ic + 2], a.comp[4 * ic + 3]};
-    const double cost = 2.0 * umu - 1.0;
-    const double sint = sqrt(1.0 - cost * cost);
-    double sphi, cphi;
-    sincos(kTwoPi * uphi, &sphi, &cphi);
-    const double kk[3] = {sint * cphi, sint * sphi, cost};
+    int ic;
+    double E, pos[3], kk[3];
+    launch_packet(a, u, ic, E, pos, kk);
     const int inu = bin_of(a.eedge, a.nnu, E);
     if constexpr (AMR)   // emit_point_qmc: photon%icell_amr = amr_find_leaf (ion_band_mod.f90:2245)
         write_record_amr<R>(rec, i, pos, kk, E, inu, oct_find_leaf(a.oct, pos[0], pos[1], pos[2], sgeo, schild));
@@ -340,15 +431,17 @@ __global__ void __launch_bounds__(kThreads) k_coherent_keys(const PassArgs a, lo
     const uint64_t ip = (uint64_t)(ip0 + i);
     int ic = 0;
     double ue, umu, uphi;
-    if (!a.multi) {
+    if (a.ndim == 3) {
         ue = qmc_uniform(sq, ip, 0, 0);
         umu = qmc_uniform(sq, ip, 1, 0);
         uphi = qmc_uniform(sq, ip, 2, 0);
     } else {
-        const double u0 = qmc_uniform(sq, ip, 0, 0);
-        ic = a.ncomp - 1;
-        for (int k = 0; k < a.ncomp; ++k)
-            if (u0 <= a.comp[4 * k]) { ic = k; break; }
+        if (a.multi) {
+            const double u0 = qmc_uniform(sq, ip, 0, 0);
+            ic = a.ncomp - 1;
+            for (int k = 0; k < a.ncomp; ++k)
+                if (u0 <= a.comp[4 * k]) { ic = k; break; }
+        }
         ue = qmc_uniform(sq, ip, 1, 0);
         umu = qmc_uniform(sq, ip, 2, 0);
         uphi = qmc_uniform(sq, ip, 3, 0);
@@ -1540,25 +1633,12 @@ __global__ void k_launch_records(const PassArgs a, long long ip0, long long n, d
     const long long ip = ip0 + i;
     double u[7];
     for (int d = 0; d < a.ndim; ++d) u[d] = qmc_uniform(*a.qmc, (uint64_t)ip, d, 0);
-    int ic = 0;
-    double umu, uphi, ue;
-    if (!a.multi) {
-        ue = u[0]; umu = u[1]; uphi = u[2];
-    } else {
-        ic = a.ncomp - 1;
-        for (int k = 0; k < a.ncomp; ++k)
-            if (u[0] <= a.comp[4 * k]) { ic = k; break; }
-        ue = u[1]; umu = u[2]; uphi = u[3];
-    }
-    const int t0 = a.tab_off[ic], t1 = a.tab_off[ic + 1];
-    const double E = sample_energy(a.tab_e + t0, a.tab_f + t0, a.tab_c + t0, t1 - t0, ue);
-    const double cost = 2.0 * umu - 1.0;
-    const double sint = sqrt(1.0 - cost * cost);
-    double sphi, cphi;
-    sincos(kTwoPi * uphi, &sphi, &cphi);
+    int ic;
+    double E, pos[3], kk[3];
+    launch_packet(a, u, ic, E, pos, kk);
     double* o = out + 8 * i;
-    o[0] = a.comp[4 * ic + 1]; o[1] = a.comp[4 * ic + 2]; o[2] = a.comp[4 * ic + 3];
-    o[3] = sint * cphi; o[4] = sint * sphi; o[5] = cost;
+    o[0] = pos[0]; o[1] = pos[1]; o[2] = pos[2];
+    o[3] = kk[0]; o[4] = kk[1]; o[5] = kk[2];
     o[6] = E;
     o[7] = (double)bin_of(a.eedge, a.nnu, E);
 }
@@ -1585,6 +1665,11 @@ PassArgs make_args(mochii_ctx* c) {
     a.ncomp = c->band.ncomp;
     a.multi = c->band.multi;
     a.ndim = c->band.qmc_ndim;
+    a.ext_ic = c->band.ext_ic;
+    a.ext_sph = c->band.ext_sph;
+    a.ext_rmax = c->par.rmax;
+    a.bmin[0] = c->grid.xmin; a.bmin[1] = c->grid.ymin; a.bmin[2] = c->grid.zmin;
+    a.bmax[0] = c->grid.xmax; a.bmax[1] = c->grid.ymax; a.bmax[2] = c->grid.zmax;
     a.nnu = c->nnu;
     a.m = c->metal;
     a.metal_abs = c->par.ion_metal_abs;

@@ -661,6 +661,7 @@ bool parse_namelist(const std::string& text, Par& p, std::string* err) {
         S(recomb_model); S(cooling_model); S(charge_exchange); S(conv_crit);
         B(solve_te); D(te_min); D(te_max); D(gas_tol_te); B(use_metals);
         B(diffuse_field); B(use_sec_ion); B(ion_add_dust); B(ion_dust_scatter); B(hei_diffuse);
+        D(ext_intensity); D(ext_tstar); S(ext_geometry);
         S(dust_density_law); D(cext_dust); S(data_dir); S(atomic_dir); S(ion_dust_kext);
         S(diffuse_energy_model); D(lambda_ref); D(taumax); D(tauhomo);
         else if (k == "iseed") p.iseed = (int64_t)std::llround(to_dbl(s));
@@ -712,6 +713,12 @@ bool parse_namelist(const std::string& text, Par& p, std::string* err) {
     else if (du == "au") p.distance2cm = AU2CM;
     else if (du == "cm") p.distance2cm = 1.0;
     if (p.diffuse_field && p.case_ab != "A") p.case_ab = "A";  // setup.f90:580-583
+    if (p.source_geometry == "external" || p.source_geometry == "external_rec" ||
+        p.source_geometry == "external_sph") {   // the external-only shorthand, setup.f90:240-258
+        p.ext_geometry = p.source_geometry == "external_sph" ? "sph" : "rec";
+        p.nsource = 0;
+        p.source_geometry = "external";
+    }
     if (p.grid_type == "uniform") p.grid_type = "car";
     (void)err;
     return true;
@@ -864,7 +871,7 @@ int ion_bin_of(const Band& b, double eph, bool include_fuv) {
 // sources with Planck spectra (the hot-path configurations), plus
 // setup_continuous_source_sampler / build_point_source_sampler
 // (:275-353, :437-495) and ion_qmc_ndim (:654-663).
-bool band_setup(const Par& p, Band& b, std::string* err, const std::vector<double>& metal_eth) {
+bool band_setup(const Par& p, Band& b, std::string* err, const std::vector<double>& metal_eth, const double* box) {
     int nfuv = 0;
     if (p.add_fuv) {
         if (p.efuv_min >= p.eion_min) {
@@ -887,13 +894,21 @@ bool band_setup(const Par& p, Band& b, std::string* err, const std::vector<doubl
         for (int i = nfuv + 1; i <= nnu + 1; ++i)
             b.eedge[i - 1] = std::exp(lo + (hi - lo) * (double)(i - 1 - nfuv) / (double)(nnu - nfuv));
     }
-    if (p.source_geometry != "point") {
-        set_err(err, "oracle: only point sources are restated");
+    if (p.source_geometry != "point" && p.source_geometry != "external") {
+        set_err(err, "oracle: only point sources and external fields are restated");
         return false;
     }
-    b.ncomp = p.nsource;
+    // components, ion_band_mod.f90:188-199 and 683-711: the point sources,
+    // then the external field
+    const bool ext_on = p.ext_intensity > 0.0;
+    if (ext_on && !box && p.ext_geometry != "sph") {
+        set_err(err, "oracle: the external field needs the box extent");
+        return false;
+    }
+    b.ncomp = p.nsource + (ext_on ? 1 : 0);
     b.multi_src = b.ncomp >= 2;
-    b.qmc_ndim = b.multi_src ? 7 : 3;
+    b.ext_ic = ext_on ? b.ncomp - 1 : -1;
+    b.qmc_ndim = (!b.multi_src && p.source_geometry == "point") ? 3 : 7;   // ion_qmc_ndim, :654-663
     const double elo = p.add_fuv ? p.efuv_min : p.eion_min;
     // photoionization_threshold_knots, ion_band_mod.f90:408-419
     std::vector<double> knots = {ETH_HI, ETH_HEI, ETH_HEII};
@@ -902,7 +917,25 @@ bool band_setup(const Par& p, Band& b, std::string* err, const std::vector<doubl
     b.samplers.resize(b.ncomp);
     std::vector<double> band_L(b.ncomp);
     for (int ic = 0; ic < b.ncomp; ++ic) {
-        const double tst = b.multi_src ? p.src_tstar[ic] : p.tstar;
+        if (ic == b.ext_ic) {   // build_external_field_sampler, :516-615 (Planck spectra)
+            const double tst = p.ext_tstar > 0.0 ? p.ext_tstar : p.tstar;
+            if (!build_planck_sampler(b.samplers[ic], tst, elo, p.eion_max, p.source_cdf_tol, knots, err)) return false;
+            double asurf;
+            if (p.ext_geometry == "sph") {
+                asurf = 4.0 * PI * ((p.rmax * p.distance2cm) * (p.rmax * p.distance2cm));
+            } else {
+                const double xr = box[0] * p.distance2cm, yr = box[1] * p.distance2cm, zr = box[2] * p.distance2cm;
+                asurf = 2.0 * (xr * yr + yr * zr + zr * xr);
+            }
+            const double f_ion = 1.0 - energy_cdf_value(b.samplers[ic], p.eion_min);
+            if (f_ion <= 0.0) {
+                set_err(err, "the external spectrum has no luminosity inside the ionizing band");
+                return false;
+            }
+            band_L[ic] = PI * p.ext_intensity * asurf / f_ion;
+            continue;
+        }
+        const double tst = (b.multi_src && p.src_tstar[ic] > 0.0) ? p.src_tstar[ic] : p.tstar;
         const double scale = b.multi_src ? p.src_lum[ic] : p.luminosity;
         if (tst <= 0.0) {
             set_err(err, "oracle: point source needs a Planck temperature");
@@ -922,7 +955,7 @@ bool band_setup(const Par& p, Band& b, std::string* err, const std::vector<doubl
     if (b.multi_src) {
         b.comp_kind.resize(b.ncomp);
         b.src_cdf.resize(b.ncomp);
-        for (int ic = 0; ic < b.ncomp; ++ic) b.comp_kind[ic] = ic + 1;
+        for (int ic = 0; ic < b.ncomp; ++ic) b.comp_kind[ic] = ic == b.ext_ic ? 0 : ic + 1;
         b.src_cdf[0] = band_L[0];
         for (int ic = 1; ic < b.ncomp; ++ic) b.src_cdf[ic] = b.src_cdf[ic - 1] + band_L[ic];
         const double last = b.src_cdf[b.ncomp - 1];
@@ -1078,7 +1111,10 @@ bool Sim::setup(const std::string& nl, std::string* err) {
         if (!sp->setup(par, nleaf, err)) return false;
         meth = sp->thresholds();
     }
-    if (!band_setup(par, band, err, meth)) return false;
+    {
+        const double box[3] = {grid.xmax - grid.xmin, grid.ymax - grid.ymin, grid.zmax - grid.zmin};
+        if (!band_setup(par, band, err, meth, box)) return false;
+    }
     if (par.diffuse_field) milne.setup(par.eion_max);   // main.f90:102
     if (par.diffuse_field && par.hei_diffuse) {          // main.f90:107-112
         std::string dir = par.data_dir;
@@ -1129,34 +1165,100 @@ void Sim::metal_sigma(Photon& ph) const {
     ph.inside = true;
 }
 
+// emit_external_rec_qmc, ion_band_mod.f90:2253-2323.
+void Sim::emit_external_rec(double u_mu, double u_phi, double u_face, double u_c1, double u_c2, Photon& ph) const {
+    const double xr = grid.xmax - grid.xmin, yr = grid.ymax - grid.ymin, zr = grid.zmax - grid.zmin;
+    const double nudge = 1.0e-6 * std::min(xr, std::min(yr, zr));
+    double farea[6], fcum[6];
+    farea[0] = yr * zr; farea[1] = farea[0];
+    farea[2] = zr * xr; farea[3] = farea[2];
+    farea[4] = xr * yr; farea[5] = farea[4];
+    fcum[0] = farea[0];
+    for (int i = 1; i < 6; ++i) fcum[i] = fcum[i - 1] + farea[i];
+    const double fpick = u_face * fcum[5];
+    int iface = 6;
+    for (int i = 0; i < 6; ++i)
+        if (fpick <= fcum[i]) { iface = i + 1; break; }
+    const double mu = std::sqrt(u_mu), sinm = std::sqrt(1.0 - mu * mu), phi = TWOPI * u_phi;
+    const double cphi = std::cos(phi), sphi = std::sin(phi);
+    switch (iface) {
+        case 1: ph.x = grid.xmax - nudge; ph.y = grid.ymin + yr * u_c1; ph.z = grid.zmin + zr * u_c2;
+                ph.kx = -mu; ph.ky = sinm * cphi; ph.kz = sinm * sphi; break;
+        case 2: ph.x = grid.xmin + nudge; ph.y = grid.ymin + yr * u_c1; ph.z = grid.zmin + zr * u_c2;
+                ph.kx = mu; ph.ky = sinm * cphi; ph.kz = sinm * sphi; break;
+        case 3: ph.x = grid.xmin + xr * u_c1; ph.y = grid.ymax - nudge; ph.z = grid.zmin + zr * u_c2;
+                ph.kx = sinm * cphi; ph.ky = -mu; ph.kz = sinm * sphi; break;
+        case 4: ph.x = grid.xmin + xr * u_c1; ph.y = grid.ymin + nudge; ph.z = grid.zmin + zr * u_c2;
+                ph.kx = sinm * cphi; ph.ky = mu; ph.kz = sinm * sphi; break;
+        case 5: ph.x = grid.xmin + xr * u_c1; ph.y = grid.ymin + yr * u_c2; ph.z = grid.zmax - nudge;
+                ph.kx = sinm * cphi; ph.ky = sinm * sphi; ph.kz = -mu; break;
+        default: ph.x = grid.xmin + xr * u_c1; ph.y = grid.ymin + yr * u_c2; ph.z = grid.zmin + nudge;
+                 ph.kx = sinm * cphi; ph.ky = sinm * sphi; ph.kz = mu; break;
+    }
+}
+
+// emit_external_sph_qmc and ortho_frame, ion_band_mod.f90:2328-2385.
+void Sim::emit_external_sph(double u_mu, double u_phi, double u_cost, double u_saz, Photon& ph) const {
+    const double xc = 0.5 * (grid.xmin + grid.xmax), yc = 0.5 * (grid.ymin + grid.ymax), zc = 0.5 * (grid.zmin + grid.zmax);
+    const double cost = 2.0 * u_cost - 1.0, sint = std::sqrt(1.0 - cost * cost), phi = TWOPI * u_saz;
+    const double rhx = sint * std::cos(phi), rhy = sint * std::sin(phi), rhz = cost;
+    ph.x = xc + par.rmax * rhx;
+    ph.y = yc + par.rmax * rhy;
+    ph.z = zc + par.rmax * rhz;
+    const double nx = -rhx, ny = -rhy, nz = -rhz;
+    double tx, ty, tz;
+    if (std::fabs(nx) <= std::fabs(ny) && std::fabs(nx) <= std::fabs(nz)) { tx = 0.0; ty = nz; tz = -ny; }
+    else if (std::fabs(ny) <= std::fabs(nz)) { tx = -nz; ty = 0.0; tz = nx; }
+    else { tx = ny; ty = -nx; tz = 0.0; }
+    const double inv = 1.0 / std::sqrt(tx * tx + ty * ty + tz * tz);
+    tx = tx * inv; ty = ty * inv; tz = tz * inv;
+    const double bx = ny * tz - nz * ty, by = nz * tx - nx * tz, bz = nx * ty - ny * tx;
+    const double mu = std::sqrt(u_mu), sinm = std::sqrt(1.0 - mu * mu), ph2 = TWOPI * u_phi;
+    const double cphi = std::cos(ph2), sphi = std::sin(ph2);
+    ph.kx = -mu * rhx + sinm * (cphi * tx + sphi * bx);
+    ph.ky = -mu * rhy + sinm * (cphi * ty + sphi * by);
+    ph.kz = -mu * rhz + sinm * (cphi * tz + sphi * bz);
+    const double nudge = 1.0e-6 * std::min(grid.xmax - grid.xmin, std::min(grid.ymax - grid.ymin, grid.zmax - grid.zmin));
+    ph.x = ph.x - nudge * rhx;
+    ph.y = ph.y - nudge * rhy;
+    ph.z = ph.z - nudge * rhz;
+}
+
 // gen_ion_photon_qmc, ion_band_mod.f90:1880-1935, with emit_point_qmc
 // (:2232-2247) and build_ion_packet_physics (ion_packet_mod.f90:21-53).
 void Sim::gen_photon_qmc(int64_t ip, Photon& ph) const {
     double u[12];
     for (int d = 1; d <= band.qmc_ndim; ++d) u[d - 1] = qmc.uniform(ip, d, 1);
     double e;
-    double umu, uphi, xs, ys, zs;
+    double umu, uphi, xs = 0.0, ys = 0.0, zs = 0.0;
     int ic = 0;
-    if (!band.multi_src) {
+    if (!band.multi_src && band.qmc_ndim == 3) {
         xs = par.xs_point; ys = par.ys_point; zs = par.zs_point;
         umu = u[1]; uphi = u[2];
         e = sample_energy_cdf(band.samplers[0], u[0]);
     } else {
-        ic = band.ncomp - 1;
-        for (int i = 0; i < band.ncomp; ++i)
-            if (u[0] <= band.src_cdf[i]) { ic = i; break; }
-        const int ik = band.comp_kind[ic];
-        xs = par.src_x[ik - 1]; ys = par.src_y[ik - 1]; zs = par.src_z[ik - 1];
+        if (band.multi_src) {
+            ic = band.ncomp - 1;
+            for (int i = 0; i < band.ncomp; ++i)
+                if (u[0] <= band.src_cdf[i]) { ic = i; break; }
+            const int ik = band.comp_kind[ic];
+            if (ik >= 1) { xs = par.src_x[ik - 1]; ys = par.src_y[ik - 1]; zs = par.src_z[ik - 1]; }
+        }
         umu = u[2]; uphi = u[3];
         e = sample_energy_cdf(band.samplers[ic], u[1]);
     }
-    ph.x = xs; ph.y = ys; ph.z = zs;
-    const double cost = 2.0 * umu - 1.0;
-    const double sint = std::sqrt(1.0 - cost * cost);
-    const double phi = TWOPI * uphi;
-    ph.kx = sint * std::cos(phi);
-    ph.ky = sint * std::sin(phi);
-    ph.kz = cost;
+    if (ic == band.ext_ic) {
+        if (par.ext_geometry == "sph") emit_external_sph(u[2], u[3], u[4], u[5], ph);
+        else emit_external_rec(u[2], u[3], u[4], u[5], u[6], ph);
+    } else {
+        ph.x = xs; ph.y = ys; ph.z = zs;
+        const double cost = 2.0 * umu - 1.0;
+        const double sint = std::sqrt(1.0 - cost * cost);
+        const double phi = TWOPI * uphi;
+        ph.kx = sint * std::cos(phi);
+        ph.ky = sint * std::sin(phi);
+        ph.kz = cost;
+    }
     ph.inu = ion_bin_of(band, e, true);
     ph.wgt = 1.0;
     ph.Lpacket = band.ion_Ltot / (double)par.nphotons;

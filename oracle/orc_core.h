@@ -130,6 +130,8 @@ struct Par {
     std::string distance_unit = "kpc";
     double distance2cm = KPC2CM;
     std::string source_geometry = "point";
+    double ext_intensity = -1.0, ext_tstar = -999.0;   // define.f90:270-277
+    std::string ext_geometry = "rec";
     double xs_point = 0.0, ys_point = 0.0, zs_point = 0.0;
     int nsource = 1;
     double src_tstar[MAX_SRC], src_lum[MAX_SRC];
@@ -179,6 +181,7 @@ struct Band {
     bool multi_src = false;
     std::vector<int> comp_kind;      // multi only
     std::vector<double> src_cdf;     // multi only
+    int ext_ic = -1;                 // the external field's component, -1 none
     std::vector<Sampler> samplers;   // source_energy_sampler
     double ion_Ltot = 0.0;
     int qmc_ndim = 3;
@@ -187,7 +190,8 @@ bool build_aligned_edges(std::vector<double>& eedge, int nfuv, int nnu,
                          double lo, double hi, const std::vector<double>& meth,
                          std::string* err);
 int ion_bin_of(const Band& b, double e, bool include_fuv);
-bool band_setup(const Par& p, Band& b, std::string* err, const std::vector<double>& meth = {});
+bool band_setup(const Par& p, Band& b, std::string* err, const std::vector<double>& meth = {},
+                const double* box = nullptr);
 
 // ---- car grid + state ----------------------------------------------------
 struct Octree;
@@ -304,6 +308,8 @@ struct Sim {
     int peel_channel(int inu) const;                              // :212-220
     void diffuse_build(double lpacket);                          // diffuse_mod.f90:60-121
     void gen_diffuse_qmc(int64_t ip, Photon& ph) const;          // diffuse_mod.f90:221-296
+    void emit_external_rec(double u_mu, double u_phi, double u_face, double u_c1, double u_c2, Photon& ph) const;
+    void emit_external_sph(double u_mu, double u_phi, double u_cost, double u_saz, Photon& ph) const;
     bool setup(const std::string& namelist, std::string* err);
     void transport_pass();           // ionizing_field_mod.f90:72-170
     void gas_rates_compute();        // gas_rates_mod.f90:82-153

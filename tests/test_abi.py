@@ -174,3 +174,19 @@ def test_bad_grid_is_refused(lib):
 def test_strerror_covers_every_status(lib):
     for s in range(10):
         assert lib.mochii_strerror(s)
+
+
+def test_external_field_keys():
+    from mochii_b200 import parse_namelist
+    """The external field's keys (define.f90:266-278) and the external-only
+    source_geometry shorthand (setup.f90:240-258)."""
+    base = "&parameters\n par%no_photons = 1000\n"
+    p = parse_namelist(base + " par%source_geometry = 'external_sph'\n par%ext_intensity = 2.5e-3\n"
+                              " par%ext_tstar = 3.0e4\n par%rmax = 1.5\n/\n")
+    assert p.source_external == 2 and p.ext_intensity == 2.5e-3 and p.ext_tstar == 3.0e4 and p.rmax == 1.5
+    p = parse_namelist(base + " par%ext_intensity = 1e-3\n par%ext_geometry = 'sph'\n/\n")
+    assert p.source_external == 0 and p.ext_geometry == 1 and p.ext_spectrum_set == 0
+    p = parse_namelist(base + " par%ext_spectrum = 'draine'\n/\n")
+    assert p.ext_spectrum_set == 1
+    d = parse_namelist(base + "/\n")
+    assert d.ext_intensity < 0 and d.source_external == 0 and d.ext_geometry == 0
