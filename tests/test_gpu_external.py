@@ -4,7 +4,8 @@ emit_external_sph_qmc) against the oracle: the launched packets of an
 external-only field through the box faces and through a bounding sphere, and
 of a point source composed with the field -- energies and bins bit-exact,
 entry points exact on the faces (the sphere's within the last bits of its
-cos/sin), directions within the last ulp of cos/sin, every packet inside the
+cos/sin), directions within the last ulp of cos/sin (a few ulp for the
+sphere's frame), every packet inside the
 box and heading inward -- the entering power pi J A, and the FP64 pass over
 the same packets."""
 import numpy as np
@@ -54,7 +55,8 @@ def test_external_launch_matches_oracle(orc, leaves, kind, grid):
     assert np.array_equal(rec[:, 6], ref[:, 6]) and np.array_equal(rec[:, 7], ref[:, 7])
     tol = 0.0 if kind != "sph" else 1e-14 * L
     np.testing.assert_allclose(rec[:, :3], ref[:, :3], rtol=0, atol=tol)
-    np.testing.assert_allclose(rec[:, 3:6], ref[:, 3:6], rtol=0, atol=4e-16)
+    # cos/sin last ulp; the sphere's directions combine two cos/sin pairs in a frame
+    np.testing.assert_allclose(rec[:, 3:6], ref[:, 3:6], rtol=0, atol=4e-16 if kind != "sph" else 1.2e-15)
     assert np.all(np.abs(rec[:, :3]) < L)
     if kind == "sph":   # entry on the sphere, the direction within the inward hemisphere
         assert np.all(-np.sum(rec[:, :3] * rec[:, 3:6], axis=1) > -1e-12 * L)
