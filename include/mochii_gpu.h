@@ -203,6 +203,17 @@ typedef struct mochii_params {
      * built; refused) */
     double ext_intensity, ext_tstar;
     int ext_geometry, source_external, ext_spectrum_set;
+    /* plane-parallel slab illumination (define.f90:217, 304-321):
+     * source_geometry 'slab' (source_slab 1) on an xy-periodic grid
+     * (xy_periodic: the walks wrap the x and y faces, z faces are open).
+     * slab_faces bit 1 top (+z), bit 2 bottom (-z); per face [0] top, [1]
+     * bottom: mode 0 beam / 1 isotropic, incidence theta and beam azimuth phi
+     * [deg], source = F_n [erg/s/cm^2] (beam) or I [erg/s/cm^2/sr]
+     * (isotropic).  slab_nmu: mu bins of the emergent-intensity tally at the
+     * z faces (mochii_slab_imu) */
+    int xy_periodic, source_slab, slab_faces, slab_nmu;
+    int slab_mode[2];
+    double slab_theta[2], slab_phi[2], slab_source[2];
 } mochii_params;
 
 /* Per-pass statistics (ion_score_report_energy_closure, ion_score_mod.f90:364-387). */
@@ -310,6 +321,20 @@ int mochii_write_image(mochii_ctx* ctx, const char* base);
  * as <base>_dustir.txt. */
 int mochii_dust_ir(mochii_ctx* ctx, double* lam, double* lnu, double* labs_lir);
 int mochii_write_dust_ir(mochii_ctx* ctx, const char* base);
+
+/* The plane-parallel slab's boundary tally of the last transport pass
+ * (slab_Iesc, jtally_mod.f90:39-86; filled by the edge walks and the
+ * scattered flights, raytrace_amr.f90:407-481, 586-660): iesc[0, nmu) the
+ * luminosity [erg/s] leaving the top face (+z) per bin of mu = |k_z|,
+ * iesc[nmu, 2 nmu) the bottom face, n = 2 par%slab_nmu; meta[0] L_in (the
+ * entering ionizing luminosity of one tile), meta[1] A_zface [cm^2].
+ * MOCHII_ERR_BAD_PARAM without source_geometry 'slab'.
+ * mochii_write_slab_imu: slab_write_Imu (jtally_mod.f90:103-150), the
+ * budget (escaping, absorbed, reflected / transmitted with one lit face)
+ * and I(mu) = Iesc / (A_zface 2 pi mu dmu) of both faces as the text file
+ * <base>_slab_Imu.txt. */
+int mochii_slab_tally(mochii_ctx* ctx, double* iesc, int n, double* meta);
+int mochii_write_slab_imu(mochii_ctx* ctx, const char* base);
 
 /* amr_refine_front (amr_refine_mod.f90:46-186): the octree rebuilt on the
  * current solution.  Front leaves: gas leaves with refine_eps < x_HI <

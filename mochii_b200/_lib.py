@@ -68,6 +68,9 @@ class Params(C.Structure):
         ("refine_eps", C.c_double), ("refine_dx", C.c_double),
         ("ext_intensity", C.c_double), ("ext_tstar", C.c_double), ("ext_geometry", C.c_int),
         ("source_external", C.c_int), ("ext_spectrum_set", C.c_int),
+        ("xy_periodic", C.c_int), ("source_slab", C.c_int), ("slab_faces", C.c_int), ("slab_nmu", C.c_int),
+        ("slab_mode", C.c_int * 2), ("slab_theta", C.c_double * 2), ("slab_phi", C.c_double * 2),
+        ("slab_source", C.c_double * 2),
     ]
 
 
@@ -134,6 +137,8 @@ SIGNATURES = {
     "mochii_write_image": (C.c_int, [C.c_void_p, C.c_char_p]),
     "mochii_dust_ir": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "mochii_write_dust_ir": (C.c_int, [C.c_void_p, C.c_char_p]),
+    "mochii_slab_tally": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p]),
+    "mochii_write_slab_imu": (C.c_int, [C.c_void_p, C.c_char_p]),
     "mochii_refine_plan": (C.c_int, [C.c_char_p] + [C.c_void_p] * 7 + [C.c_double, C.c_double, C.c_int, C.c_int,
                                                                        C.c_double, C.c_double, C.c_char_p,
                                                                        C.c_void_p, C.c_void_p]),

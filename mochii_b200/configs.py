@@ -534,3 +534,52 @@ def g2a(workdir, nphotons=40_000_000, niter=100, precision="fp32", level=6):
  par%precision = '{precision}'
 /
 """
+
+
+def slab(nphotons=400_000, faces="top", mode="beam", theta=0.0, phi=0.0, source=1.0e-5, nx=1, nz=64,
+         car_walk="dda", precision="fp64", nH=0.1, zmax=0.5, nnu=1, niter=0, bot=None, rmax=100.0):
+    """The plane-parallel slab inputs of the reference's slab gates
+    (tests/slab/ga_*.in): a frozen neutral pure-hydrogen column of n_H = 0.1
+    and thickness 2 zmax = 1 pc on nz = 64 cubic cells, periodic in x and y
+    (nx = ny columns of side 2 zmax / nz), lit from the top face by a 40 kK
+    blackbody of band flux F_n = 1e-5 erg/s/cm^2 (beam at incidence theta)
+    or intensity I (isotropic), one band bin, fixed T_e = 1e4 K, no
+    iteration (rates only).  bot = (mode, theta, source) lights the bottom
+    face as well (faces 'both')."""
+    half = zmax / nz * nx
+    lines = [
+        f" par%no_photons = {float(nphotons)!r}",
+        " par%iseed = 1234",
+        " par%launch_sequence = 'sobol'",
+        " par%grid_type = 'car'",
+        f" par%car_walk = '{car_walk}'",
+        f" par%nx = {nx}", f" par%ny = {nx}", f" par%nz = {nz}",
+        f" par%xmax = {half!r}", f" par%ymax = {half!r}", f" par%zmax = {zmax!r}",
+        f" par%nH_const = {nH!r}",
+        f" par%rmax = {rmax!r}",
+        " par%dust_density_law = 'none'",
+        " par%distance_unit = 'pc'",
+        " par%xy_periodic = .true.",
+        " par%ion_align_edges = .false.",
+        f" par%nnu_ion = {nnu}",
+        " par%eion_min = 13.598",
+        " par%eion_max = 100.0",
+        " par%tstar = 4.0e4",
+        " par%He_abund = 0.0",
+        " par%xHI_init = 1.0",
+        " par%ion_add_dust = .false.",
+        f" par%gas_niter = {niter}",
+        " par%te_fixed = 1.0e4",
+        " par%source_geometry = 'slab'",
+        f" par%slab_faces = '{faces}'",
+        f" par%slab_top_mode = '{mode}'",
+        f" par%slab_top_theta = {theta!r}",
+        f" par%slab_top_phi = {phi!r}",
+        f" par%slab_top_source = {source!r}",
+        f" par%atomic_dir = '{ATOMIC_DIR}'",
+        f" par%precision = '{precision}'",
+    ]
+    if bot is not None:
+        lines += [f" par%slab_bot_mode = '{bot[0]}'", f" par%slab_bot_theta = {bot[1]!r}",
+                  f" par%slab_bot_source = {bot[2]!r}"]
+    return "&parameters\n" + "\n".join(lines) + "\n/\n"

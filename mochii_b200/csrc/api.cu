@@ -78,7 +78,8 @@ cudaError_t alloc_records(mochii_ctx* c, long long cap) {
     if ((e = cudaMalloc(&c->rec.sig, nsig * (size_t)cap * rsz + 64)) != cudaSuccess) return e;
     if ((e = cudaMalloc(&c->rec.coef, ncoef * (size_t)cap * rsz + 64)) != cudaSuccess) return e;
     if (c->scatter && (e = cudaMalloc(&c->rec.dsc, 2 * (size_t)cap * rsz + 64)) != cudaSuccess) return e;
-    if ((c->scatter || c->par.ion_peel) && c->oct.ncells == 0 && (e = dalloc(&c->rec.p0, 6 * (size_t)cap)) != cudaSuccess)
+    if ((c->scatter || c->par.ion_peel || c->band.slab) && c->oct.ncells == 0 &&
+        (e = dalloc(&c->rec.p0, 6 * (size_t)cap)) != cudaSuccess)
         return e;
     if (c->metal.ntr > 0) {
         if ((e = dalloc(&c->rec.E, (size_t)cap)) != cudaSuccess) return e;
@@ -102,7 +103,7 @@ void release(mochii_ctx* c) {
                     (void*)c->rec.E, c->rec.msig, c->oct_blob, c->rec.dsc, (void*)c->rec.p0,
                     (void*)c->dust_blob, (void*)c->rhokap, (void*)c->ttab, (void*)c->metal_lnl,
                     (void*)c->th.lnL, (void*)c->rec.key, (void*)c->rec.key_sorted, (void*)c->rec.seq,
-                    (void*)c->rec.perm, c->rec.sort_tmp, c->peel_blob};
+                    (void*)c->rec.perm, c->rec.sort_tmp, c->peel_blob, (void*)c->slab_iesc};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     for (cudaEvent_t e : {c->ev0, c->ev1, c->evA, c->evB})
@@ -127,8 +128,20 @@ int validate(const mochii_params& p, std::string* why, int* code) {
     if (p.solve_te && !(p.te_min > 0.0 && p.te_max > p.te_min)) return *why = "need 0 < par%te_min < par%te_max", 1;
     if (p.He_abund < 0.0) return *why = "par%He_abund must be >= 0", 1;
     if (!p.grid_car && !p.amr_file[0]) return *why = "grid_type='amr' needs par%amr_file (a text leaf list)", 1;
+    if (p.source_slab) {   // setup.f90:259-327
+        if (!p.xy_periodic) return *why = "source_geometry='slab' needs par%xy_periodic (a slab is periodic in x and y)", 1;
+        if (p.nsource > 1 || p.ext_intensity > 0.0)
+            return *why = "source_geometry='slab' cannot be combined with point sources (nsource > 1) or an external field", 1;
+        if (p.slab_nmu < 1) return *why = "par%slab_nmu must be >= 1", 1;
+        for (int f = 0; f < 2; ++f) {
+            if (!((p.slab_faces >> f) & 1)) continue;
+            if (!p.slab_mode[f] && (p.slab_theta[f] < 0.0 || p.slab_theta[f] >= 90.0))
+                return *why = "par%slab_top_theta / slab_bot_theta must lie in [0, 90) degrees for a beam", 1;
+            if (p.slab_source[f] <= 0.0) return *why = "par%slab_top_source / slab_bot_source must be > 0 on a lit face", 1;
+        }
+    }
     *code = MOCHII_ERR_UNSUPPORTED;
-    if (!p.source_point) return *why = "only internal point sources are built", 1;
+    if (!p.source_point && !p.source_slab) return *why = "only point sources, external fields and the slab are built", 1;
     if (!p.launch_sobol) return *why = "launch_sequence='random' is not built; use 'sobol'", 1;
     if (p.ion_add_dust && p.dust_law == 2)
         return *why = "dust_density_law: only 'global_dgr' and 'none' are built", 1;
@@ -138,6 +151,10 @@ int validate(const mochii_params& p, std::string* why, int* code) {
         return *why = "ion_add_dust needs par%ion_dust_kext (the grain-model optics are not built)", 1;
     if (p.ion_peel && (p.ext_intensity > 0.0 || p.source_external))
         return *why = "the peel-off of external-field packets is not built", 1;
+    *code = MOCHII_ERR_BAD_PARAM;
+    if (p.ion_peel && p.xy_periodic)   // setup.f90:531-539
+        return *why = "par%ion_peel is not supported with par%xy_periodic (use the slab's boundary I(mu) tally)", 1;
+    *code = MOCHII_ERR_UNSUPPORTED;
     if (p.use_sec_ion) return *why = "use_sec_ion is not built in this library version", 1;
     if (p.grain_pe) return *why = "grain_pe is not built in this library version", 1;
     return 0;
@@ -465,6 +482,11 @@ extern "C" int mochii_init(const mochii_params* pin, mochii_ctx** out) {
     c->tw.ledger_blocks = transport_blocks(c);
     CKI(dalloc(&c->tw.ledger, 3 * (size_t)c->tw.ledger_blocks));
     CKI(dalloc(&c->tw.counters, 4));
+    if (c->band.slab) {   // slab_tally_setup (jtally_mod.f90:60-71)
+        CKI(dalloc(&c->slab_iesc, 2 * (size_t)p.slab_nmu));
+        CKI(cudaMemset(c->slab_iesc, 0, 2 * (size_t)p.slab_nmu * 8));
+        c->slab_host.assign(2 * (size_t)p.slab_nmu, 0.0);
+    }
     // packet records: launch chunks of up to 4 Mi packets
     CKI(alloc_records(c, std::min<long long>(p.nphotons, std::max<long long>(p.packet_chunk, 1024))));
     CKI(peel_setup(c));   // ion_peel_setup: observers and image plane (par%ion_peel)
@@ -885,6 +907,7 @@ extern "C" int mochii_transport_pass(mochii_ctx* c, int with_peel, mochii_pass_s
     else if (c->metal.ntr > 0)
         CK(c, cudaMemsetAsync(c->metal.raw, 0, raw_bytes(c), c->stream));
     CK(c, cudaMemsetAsync(c->tw.counters, 0, 4 * sizeof(unsigned long long), c->stream));
+    if (c->slab_iesc) CK(c, cudaMemsetAsync(c->slab_iesc, 0, c->slab_host.size() * 8, c->stream));
     CK(c, cudaEventRecord(c->ev0, c->stream));
     CK(c, launch_transport(c));
     double dlum = 0.0;
@@ -902,6 +925,9 @@ extern "C" int mochii_transport_pass(mochii_ctx* c, int with_peel, mochii_pass_s
     unsigned long long cnt[4];
     CK(c, cudaMemcpyAsync(led.data(), c->tw.ledger, led.size() * 8, cudaMemcpyDeviceToHost, c->stream));
     CK(c, cudaMemcpyAsync(cnt, c->tw.counters, sizeof(cnt), cudaMemcpyDeviceToHost, c->stream));
+    if (c->slab_iesc)
+        CK(c, cudaMemcpyAsync(c->slab_host.data(), c->slab_iesc, c->slab_host.size() * 8, cudaMemcpyDeviceToHost,
+                              c->stream));
     CK(c, cudaStreamSynchronize(c->stream));
     float ms = 0.0f, pms = 0.0f;
     cudaEventElapsedTime(&ms, c->ev0, c->ev1);

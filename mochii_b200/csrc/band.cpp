@@ -224,6 +224,69 @@ bool aligned_edges(std::vector<double>& edge, int nfuv, int nnu, double lo, doub
             edge[++ip] = std::exp(std::log(pts[j]) + (std::log(pts[j + 1]) - std::log(pts[j])) * (double)b / (double)nb[j]);
     return true;
 }
+
+// photoionization_threshold_knots (ion_band_mod.f90:408-419): H, He, the
+// metal thresholds in registry order, then eion_min with the FUV band.
+std::vector<double> knots_of(const mochii_params& p, const std::vector<double>& metal_eth) {
+    std::vector<double> knots{kEthHI, kEthHeI, kEthHeII};
+    knots.insert(knots.end(), metal_eth.begin(), metal_eth.end());
+    if (p.add_fuv) knots.push_back(p.eion_min);
+    return knots;
+}
+
+// The plane-parallel slab (setup.f90:259-330, slab_setup
+// ion_band_mod.f90:2083-2130, ion_setup :312-328): one component with the
+// single point source's Planck spectrum at tstar, its luminosity the
+// ionizing power entering one periodic tile, L = sum_face F_z A_z / f_ion,
+// F_z = pi I (isotropic) or cos(theta) F_n (beam).
+bool slab_build(const mochii_params& p, BandSetup& b, std::string* err, const std::vector<double>& knots,
+                const double* box) {
+    if (!p.xy_periodic) return fail(err, "source_geometry='slab' needs par%xy_periodic (a slab is periodic in x and y)");
+    if (p.nsource > 1 || p.ext_intensity > 0.0)
+        return fail(err, "source_geometry='slab' cannot be combined with point sources (nsource > 1) or an external field");
+    if (p.slab_faces < 1 || p.slab_faces > 3) return fail(err, "par%slab_faces must be 'top', 'bottom' or 'both'");
+    if (p.slab_nmu < 1) return fail(err, "par%slab_nmu must be >= 1");
+    if (!box) return fail(err, "slab: the box extent is unknown");
+    b.slab = 1;
+    b.ncomp = 1;
+    b.multi = 0;
+    b.ext_ic = -1;
+    b.qmc_ndim = 6;   // ion_qmc_ndim (:654-663): u1 energy, u2 face, u3/u4 xy, u5 mu, u6 phi
+    double fz = 0.0;
+    for (int f = 0; f < 2; ++f) {
+        b.slab_lit[f] = (p.slab_faces >> f) & 1;
+        b.slab_mode[f] = p.slab_mode[f] ? 1 : 0;
+        b.slab_phi[f] = p.slab_phi[f] * (kPi / 180.0);
+        b.slab_mu[f] = 1.0;
+        b.slab_Fz[f] = 0.0;
+        if (!b.slab_lit[f]) continue;
+        if (b.slab_mode[f] == 0 && (p.slab_theta[f] < 0.0 || p.slab_theta[f] >= 90.0))
+            return fail(err, "par%slab_top_theta / slab_bot_theta must lie in [0, 90) degrees for a beam");
+        if (p.slab_source[f] <= 0.0) return fail(err, "par%slab_top_source / slab_bot_source must be > 0 on a lit face");
+        if (b.slab_mode[f] == 1) {
+            b.slab_Fz[f] = kPi * p.slab_source[f];
+        } else {
+            b.slab_mu[f] = std::cos(p.slab_theta[f] * (kPi / 180.0));
+            b.slab_Fz[f] = b.slab_mu[f] * p.slab_source[f];
+        }
+        fz += b.slab_Fz[f];
+    }
+    b.slab_azface = (box[0] * p.distance2cm) * (box[1] * p.distance2cm);
+    if (!(fz * b.slab_azface > 0.0)) return fail(err, "source_geometry='slab' has zero entering flux");
+    b.slab_ptop = b.slab_Fz[0] / fz;
+    const double elo = p.add_fuv ? p.efuv_min : p.eion_min;
+    if (p.tstar <= 0.0) return fail(err, "slab needs a Planck temperature (par%tstar)");
+    b.tables.assign(1, EnergyTable());
+    if (!planck_table(b.tables[0], p.tstar, elo, p.eion_max, p.source_cdf_tol, knots, err)) return false;
+    const double f_ion = 1.0 - table_cdf(b.tables[0], p.eion_min);
+    if (f_ion <= 0.0) return fail(err, "the slab spectrum has no luminosity inside the ionizing band");
+    b.comp_x.assign(1, 0.0);
+    b.comp_y.assign(1, 0.0);
+    b.comp_z.assign(1, 0.0);
+    b.comp_cdf.assign(1, 1.0);
+    b.ion_Ltot = fz * b.slab_azface / f_ion;
+    return true;
+}
 }  // namespace
 
 // ion_setup + setup_continuous_source_sampler + build_point_source_sampler
@@ -247,7 +310,9 @@ bool band_build(const mochii_params& p, BandSetup& b, std::string* err, const st
         for (int i = nfuv; i <= nnu; ++i)
             b.eedge[i] = std::exp(lo + (hi - lo) * (double)(i - nfuv) / (double)(nnu - nfuv));
     }
-    if (!p.source_point) return fail(err, "only point sources and external fields are built (par%source_geometry)");
+    if (!p.source_point && !p.source_slab)
+        return fail(err, "par%source_geometry must be 'point', 'slab', 'external_rec' or 'external_sph'");
+    if (p.source_slab) return slab_build(p, b, err, knots_of(p, metal_eth), box);
     // components (ion_band_mod.f90:188-199, 683-711): the point sources, then
     // the external field when par%ext_intensity > 0
     const bool ext_on = p.ext_intensity > 0.0;
@@ -263,11 +328,7 @@ bool band_build(const mochii_params& p, BandSetup& b, std::string* err, const st
     b.ext_sph = p.source_external ? (p.source_external == 2) : (p.ext_geometry == 1);
     b.qmc_ndim = (b.ncomp == 1 && !ext_on) ? 3 : 7;   // ion_qmc_ndim (:654-663)
     const double elo = p.add_fuv ? p.efuv_min : p.eion_min;
-    // photoionization_threshold_knots (ion_band_mod.f90:408-419): H, He, the
-    // metal thresholds in registry order, then eion_min with the FUV band
-    std::vector<double> knots{kEthHI, kEthHeI, kEthHeII};
-    knots.insert(knots.end(), metal_eth.begin(), metal_eth.end());
-    if (p.add_fuv) knots.push_back(p.eion_min);
+    const std::vector<double> knots = knots_of(p, metal_eth);
     b.tables.assign(b.ncomp, EnergyTable());
     b.comp_x.assign(b.ncomp, 0.0);
     b.comp_y.assign(b.ncomp, 0.0);

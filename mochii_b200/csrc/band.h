@@ -34,6 +34,14 @@ struct BandSetup {
     double ion_Ltot = 0.0;
     int ext_ic = -1;                    // component of the external field, -1 none
     int ext_sph = 0;                    // its entry surface: 0 the box faces, 1 the sphere of radius rmax
+    // plane-parallel slab (slab_setup, ion_band_mod.f90:2083-2130): the one
+    // component; per face [0] top (+z), [1] bottom (-z): lit, mode (0 beam,
+    // 1 Lambert), beam mu = cos(theta) and azimuth [rad], horizontal flux F_z
+    int slab = 0;
+    int slab_lit[2] = {0, 0}, slab_mode[2] = {0, 0};
+    double slab_mu[2] = {1.0, 1.0}, slab_phi[2] = {0.0, 0.0}, slab_Fz[2] = {0.0, 0.0};
+    double slab_ptop = 1.0;             // probability of the top face
+    double slab_azface = 0.0;           // z-face area of one periodic tile [cm^2]
 };
 
 // metal_eth: the active metal thresholds in registry order (main.f90:65-82),

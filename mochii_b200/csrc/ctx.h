@@ -161,6 +161,9 @@ struct mochii_ctx {
     double* tdust = nullptr;        // nleaf T_dust [K]
     double* tdust_tab = nullptr;    // lam_ir | sabs_ir | tgrid | femit
     mochii::DustTempHost tdust_host;
+    // plane-parallel slab: the boundary tally of the last pass (jtally_mod.f90:39-86)
+    double* slab_iesc = nullptr;    // device: 2 x slab_nmu escaping luminosity, top | bottom [erg/s]
+    std::vector<double> slab_host;  // its copy after the pass
     mochii::SpeciesHost species;
     bool thermal_ready = false;
     mochii::BalanceWork bw;

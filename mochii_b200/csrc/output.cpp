@@ -334,3 +334,68 @@ extern "C" int mochii_write_dust_ir(mochii_ctx* c, const char* base) {
     for (int k = 0; k < kDustIrN; ++k) std::fprintf(f, "%12.4f%15.6E\n", lam[k], lnu[k]);
     return std::fclose(f) == 0 ? MOCHII_OK : MOCHII_ERR_BAD_PARAM;
 }
+
+extern "C" int mochii_slab_tally(mochii_ctx* c, double* iesc, int n, double* meta) {
+    if (!c) return MOCHII_ERR_BAD_PARAM;
+    if (!c->band.slab || !c->slab_iesc) {
+        c->last_error = "the boundary tally needs par%source_geometry = 'slab'";
+        return MOCHII_ERR_BAD_PARAM;
+    }
+    if (n != (int)c->slab_host.size() || (!iesc && n > 0)) {
+        c->last_error = "mochii_slab_tally: n must be 2 * par%slab_nmu";
+        return MOCHII_ERR_BAD_PARAM;
+    }
+    for (int k = 0; k < n; ++k) iesc[k] = c->slab_host[k];
+    if (meta) {
+        meta[0] = c->band.ion_Ltot;
+        meta[1] = c->band.slab_azface;
+    }
+    return MOCHII_OK;
+}
+
+extern "C" int mochii_write_slab_imu(mochii_ctx* c, const char* base) {
+    if (!c || !base || !base[0]) return MOCHII_ERR_BAD_PARAM;
+    const int n = (int)c->slab_host.size();
+    std::vector<double> v(std::max(n, 1));
+    double meta[2];
+    const int rc = mochii_slab_tally(c, v.data(), n, meta);
+    if (rc) return rc;
+    const int nmu = n / 2;
+    const double lin = meta[0], az = meta[1], dmu = 1.0 / (double)nmu;
+    double top = 0.0, bot = 0.0;
+    for (int k = 0; k < nmu; ++k) {
+        top += v[k];
+        bot += v[nmu + k];
+    }
+    const double labs = lin - top - bot;
+    const bool lit_top = c->band.slab_lit[0], lit_bot = c->band.slab_lit[1];
+    const std::string path = std::string(base) + "_slab_Imu.txt";
+    FILE* f = std::fopen(path.c_str(), "w");
+    if (!f) {
+        c->last_error = "cannot write " + path;
+        return MOCHII_ERR_BAD_PARAM;
+    }
+    std::fprintf(f, "# MoCHII plane-parallel slab: emergent intensity I(mu) at the z-boundaries.\n");
+    std::fprintf(f, "# L_in           [erg/s] = %14.6E\n", lin);
+    std::fprintf(f, "# L_escape_top   [erg/s] = %14.6E   fraction = %8.5f\n", top, top / lin);
+    std::fprintf(f, "# L_escape_bottom[erg/s] = %14.6E   fraction = %8.5f\n", bot, bot / lin);
+    std::fprintf(f, "# L_absorbed     [erg/s] = %14.6E   fraction = %8.5f\n", labs, labs / lin);
+    if (lit_top != lit_bot) {   // one lit face: escape there is reflected, at the other transmitted
+        const double refl = lit_top ? top : bot, tran = lit_top ? bot : top;
+        std::fprintf(f, lit_top ? "# illuminated face = top: escape at top = reflected, at bottom = transmitted.\n"
+                                : "# illuminated face = bottom: escape at bottom = reflected, at top = transmitted.\n");
+        std::fprintf(f, "# L_reflected    [erg/s] = %14.6E   fraction = %8.5f\n", refl, refl / lin);
+        std::fprintf(f, "# L_transmitted  [erg/s] = %14.6E   fraction = %8.5f\n", tran, tran / lin);
+    } else {
+        std::fprintf(f, "# both (or neither) faces illuminated: the top and bottom escape each mix\n");
+        std::fprintf(f, "# reflection and transmission and are not separable without an incident-face tag.\n");
+    }
+    std::fprintf(f, "# A_zface        [cm^2]  = %14.6E\n", az);
+    std::fprintf(f, "#   mu        I_top[erg/s/cm^2/sr]   I_bot[erg/s/cm^2/sr]\n");
+    for (int k = 0; k < nmu; ++k) {
+        const double mu = ((double)(k + 1) - 0.5) * dmu;
+        const double norm = az * kTwoPi * mu * dmu;
+        std::fprintf(f, "%8.5f%22.8E%22.8E\n", mu, v[k] / norm, v[nmu + k] / norm);
+    }
+    return std::fclose(f) == 0 ? MOCHII_OK : MOCHII_ERR_BAD_PARAM;
+}

@@ -40,13 +40,11 @@ const char* const kOtherKeys[] = {
     "radiation_angular_pdf_file", "reduce_factor",
     "save_jlam",
     "scatt_mat_file", "sed_data_dir", "sed_dl07_sdindex", "sed_dl07_uisrf", "sed_kext", "sed_nt",
-    "sed_pah_live", "sed_thi", "sed_tlo", "sightline_tau", "slab_bot_mode", "slab_bot_phi",
-    "slab_bot_source", "slab_bot_theta", "slab_faces", "slab_nmu", "slab_top_mode", "slab_top_phi",
-    "slab_top_source", "slab_top_theta", "source_rscale", "source_spectrum", "source_zscale",
+    "sed_pah_live", "sed_thi", "sed_tlo", "sightline_tau", "source_rscale", "source_spectrum", "source_zscale",
     "spectrum_type", "spiral_amp", "spiral_m", "spiral_pitch", "src_axial_ratio", "src_boxiness",
     "src_geometry", "src_reff", "src_rscale", "src_sersic_index", "src_spectrum", "src_spectrum_file",
     "src_zscale", "use_amr_grid", "use_dustemis", "use_master_slave", "use_mrw",
-    "use_reduced_wgt", "use_sed", "use_stokes", "xy_periodic", "xyz_symmetry", "z_global", "z_ref",
+    "use_reduced_wgt", "use_sed", "use_stokes", "xyz_symmetry", "z_global", "z_ref",
     "z_symmetry", "dust_density_law_file"};
 
 std::string lower(std::string s) {
@@ -148,6 +146,7 @@ extern "C" int mochii_params_default(mochii_params* p) {
     p->refine_front = 0; p->refine_iter = 20; p->refine_lbase = 5; p->refine_lmax = 7;   // define.f90:826-831
     p->refine_eps = 1.0e-2; p->refine_dx = 0.2;
     p->ext_intensity = -1.0; p->ext_tstar = -999.0; p->ext_geometry = 0;   // define.f90:270-277
+    p->slab_faces = 1; p->slab_nmu = 20;                                    // define.f90:312-321
     const double nan = std::numeric_limits<double>::quiet_NaN();
     p->distance = nan; p->dxim = nan; p->dyim = nan;
     for (int i = 0; i < MOCHII_MAX_OBS; ++i) {
@@ -221,8 +220,26 @@ int set_key(mochii_params* p, std::string key, const std::vector<std::string>& v
         p->source_point = s == "point";
         p->source_external = (s == "external" || s == "external_rec") ? 1 : s == "external_sph" ? 2 : 0;
         if (p->source_external) p->source_point = 1;   // the external-only shorthand of setup.f90:240-258
+        p->source_slab = s == "slab";
+        if (!p->source_point && !p->source_slab) return bad("must be 'point', 'slab', 'external_rec' or 'external_sph'");
         return 0;
     }
+    BOOL("xy_periodic", xy_periodic) INT("slab_nmu", slab_nmu)
+    if (key == "slab_faces") {   // setup.f90:267-271
+        const std::string s = lower(unquote(v));
+        if (s != "top" && s != "bottom" && s != "both") return bad("must be 'top', 'bottom' or 'both'");
+        p->slab_faces = s == "top" ? 1 : s == "bottom" ? 2 : 3;
+        return 0;
+    }
+    if (key == "slab_top_mode" || key == "slab_bot_mode") {   // setup.f90:273-277
+        const std::string s = lower(unquote(v));
+        if (s != "beam" && s != "isotropic") return bad("must be 'beam' or 'isotropic'");
+        p->slab_mode[key == "slab_bot_mode"] = s == "isotropic";
+        return 0;
+    }
+    REAL("slab_top_theta", slab_theta[0]) REAL("slab_bot_theta", slab_theta[1])
+    REAL("slab_top_phi", slab_phi[0]) REAL("slab_bot_phi", slab_phi[1])
+    REAL("slab_top_source", slab_source[0]) REAL("slab_bot_source", slab_source[1])
     if (key == "ext_geometry") {
         const std::string s = lower(unquote(v));
         if (s != "rec" && s != "sph") return bad("must be 'rec' or 'sph'");

@@ -60,6 +60,12 @@ struct PassArgs {
     int ext_ic, ext_sph;   // the external field's component (-1 none) and entry surface (0 box faces, 1 sphere)
     double ext_rmax;       // the entry sphere's radius (code units)
     double bmin[3], bmax[3];   // the grid box (code units)
+    int xyper;             // par%xy_periodic: the walks wrap the x and y faces, z faces are open
+    int slab;              // plane-parallel slab illumination (the one component)
+    int slab_mode[2];      // per face [top, bottom]: 0 beam, 1 Lambert
+    double slab_mu[2], slab_phi[2], slab_ptop;
+    int slab_nmu;          // mu bins of the boundary tally
+    double* slab_iesc;     // 2 x slab_nmu luminosity escaping the top | bottom face, null: no tally
     MetalDev m;          // trace metals; m.ntr == 0 without
     int metal_abs;       // par%ion_metal_abs
     OctDev oct;          // octree grid; oct.ncells == 0 on the Cartesian grid
@@ -350,14 +356,50 @@ __device__ void emit_external_sph(const PassArgs& a, double u_mu, double u_phi, 
     pos[2] = pos[2] - nudge * rz;
 }
 
+// emit_slab_qmc (ion_band_mod.f90:2183-2208): the lit z face drawn by its
+// share of the entering flux (u_face against the top's), the entry point
+// uniform over it (u_c1, u_c2) nudged 1e-6 of the smallest extent inside,
+// the direction a beam at the face's incidence and azimuth or a Lambert ray
+// (mu = sqrt(u_mu) floored at 1e-6, azimuth 2 pi u_phi) into the slab.
+__device__ void emit_slab(const PassArgs& a, double u_face, double u_c1, double u_c2, double u_mu, double u_phi,
+                          double pos[3], double kk[3]) {
+    const double xr = a.bmax[0] - a.bmin[0], yr = a.bmax[1] - a.bmin[1], zr = a.bmax[2] - a.bmin[2];
+    const double nudge = 1.0e-6 * fmin(xr, fmin(yr, zr));
+    const int f = u_face > a.slab_ptop ? 1 : 0;   // 0 top (+z), 1 bottom (-z)
+    pos[0] = a.bmin[0] + xr * u_c1;
+    pos[1] = a.bmin[1] + yr * u_c2;
+    pos[2] = f == 0 ? a.bmax[2] - nudge : a.bmin[2] + nudge;
+    double mu, ph;
+    if (a.slab_mode[f]) {
+        mu = fmax(sqrt(u_mu), 1.0e-6);
+        ph = kTwoPi * u_phi;
+    } else {
+        mu = a.slab_mu[f];
+        ph = a.slab_phi[f];
+    }
+    const double sinm = sqrt(fmax(1.0 - mu * mu, 0.0));
+    double sp, cp;
+    sincos(ph, &sp, &cp);
+    kk[0] = sinm * cp;
+    kk[1] = sinm * sp;
+    kk[2] = f == 0 ? -mu : mu;
+}
+
 // The launch of one stellar packet from its uniforms u (gen_ion_photon_qmc,
 // ion_band_mod.f90:1880-1935): a single point source reads u1 energy, u2 mu,
-// u3 phi; every other configuration the superset layout -- u1 component,
-// u2 energy, u3/u4 angles, u5-u7 the entry surface of an external field.
+// u3 phi; the slab u1 energy, u2 face, u3/u4 the entry point, u5 mu, u6
+// phi; every other configuration the superset layout -- u1 component, u2
+// energy, u3/u4 angles, u5-u7 the entry surface of an external field.
 __device__ __forceinline__ void launch_packet(const PassArgs& a, const double* u, int& ic, double& E, double pos[3],
                                               double kk[3]) {
     ic = 0;
     double umu, uphi, ue;
+    if (a.slab) {
+        const int t0 = a.tab_off[0], t1 = a.tab_off[1];
+        E = sample_energy(a.tab_e + t0, a.tab_f + t0, a.tab_c + t0, t1 - t0, u[0]);
+        emit_slab(a, u[1], u[2], u[3], u[4], u[5], pos, kk);
+        return;
+    }
     if (a.ndim == 3) {
         ue = u[0]; umu = u[1]; uphi = u[2];
     } else {
@@ -487,9 +529,13 @@ template <> struct Col<double, 4> {
 // nearest face (minloc first-minimum tie rule).  Pure FP64 geometry, so it
 // runs ahead of the opacity work and the column loads of upcoming cells are
 // in flight while the current cell is scored.
+// per: xy-periodic (raytrace_amr.f90:575-582): a step out of an x or y face
+// re-enters at the opposite one (the uniform grid keeps tMax and tDelta), so
+// only the z faces end the walk.
 struct Stepper {
     double t0, t1, t2, d0, d1, d2, t_cur;
     int ix, iy, iz, sx, sy, sz;
+    int per = 0;
     __device__ __forceinline__ bool emit(int nx, int ny, int nz, int* il, double* seg) {
         *il = ix + nx * (iy + ny * iz);
         int ax = 0;
@@ -504,9 +550,29 @@ struct Stepper {
         ix += ax == 0 ? sx : 0;
         iy += ax == 1 ? sy : 0;
         iz += ax == 2 ? sz : 0;
+        if (per) {
+            ix = ix < 0 ? nx - 1 : (ix >= nx ? 0 : ix);
+            iy = iy < 0 ? ny - 1 : (iy >= ny ? 0 : iy);
+        }
         return ix >= 0 && ix < nx && iy >= 0 && iy < ny && iz >= 0 && iz < nz;   // next cell inside?
     }
 };
+
+// slab_bnd_add (jtally_mod.f90:76-86): luminosity leaving a z face into its
+// bin of mu = |k_z| (nmu equal bins in (0, 1]), the top face for k_z > 0.
+__device__ __forceinline__ void slab_add(const PassArgs& a, double kz, double lum) {
+    const int ib = min(max((int)(fabs(kz) * (double)a.slab_nmu), 0), a.slab_nmu - 1);
+    atomicAdd(a.slab_iesc + (kz > 0.0 ? 0 : a.slab_nmu) + ib, lum);
+}
+
+// slab_wrap_xy (raytrace_amr.f90:330-345): a packet that left an x or y
+// face of the box re-enters at the opposite face's exact boundary value.
+__device__ __forceinline__ void slab_wrap_xy(const PassArgs& a, int face, double& x, double& y) {
+    if (face == 0) x = a.bmin[0];
+    else if (face == 1) x = a.bmax[0];
+    else if (face == 2) y = a.bmin[1];
+    else if (face == 3) y = a.bmax[1];
+}
 
 // H/He part of score_ion_path (ion_score_mod.f90:137-231): the rate tallies
 // of the leaf and its diagnostic spectrum bin.
@@ -693,8 +759,15 @@ __device__ __forceinline__ bool walk_to_tau(const PassArgs& a, double tau_in, bo
             x = x + texit * kx;
             y = y + texit * ky;
             z = z + texit * kz;
-            const int nl = oct_next_leaf(a.oct, il, face, x, y, z);
-            if (nl < 0) return false;
+            int nl = oct_next_leaf(a.oct, il, face, x, y, z);
+            if (nl < 0 && a.xyper) {   // raytrace_amr.f90:403-406
+                slab_wrap_xy(a, face, x, y);
+                if (face <= 3) nl = oct_find_leaf(a.oct, x, y, z);
+            }
+            if (nl < 0) {   // a scattered flight leaving a z face: the slab's reflected / diffuse part (:407-413)
+                if (face >= 4 && a.slab_iesc) slab_add(a, kz, wgt * a.Lpacket);
+                return false;
+            }
             il = nl;
         }
     } else {
@@ -734,11 +807,24 @@ __device__ __forceinline__ bool walk_to_tau(const PassArgs& a, double tau_in, bo
             t_cur = tmax[ax];
             tmax[ax] = tmax[ax] + tdel[ax];
             idx[ax] += stp[ax];
-            if (idx[ax] < 0 || idx[ax] >= a.n[ax]) { inside = false; break; }
+            if (idx[ax] < 0 || idx[ax] >= a.n[ax]) {
+                if (a.xyper && ax < 2) {   // raytrace_amr.f90:639-654
+                    idx[ax] = idx[ax] < 0 ? a.n[ax] - 1 : 0;
+                } else {
+                    if (ax == 2 && a.slab_iesc) slab_add(a, kz, wgt * a.Lpacket);   // :655-660
+                    inside = false;
+                    break;
+                }
+            }
         }
         x = x + t_cur * kx;
         y = y + t_cur * ky;
         z = z + t_cur * kz;
+        if (a.xyper) {   // the unwrapped end point folded back into the box (:666-672)
+            const double xr = a.bmax[0] - a.bmin[0], yr = a.bmax[1] - a.bmin[1];
+            x = x - floor((x - a.bmin[0]) / xr) * xr;
+            y = y - floor((y - a.bmin[1]) / yr) * yr;
+        }
         if (inside) il = idx[0] + a.n[0] * (idx[1] + a.n[1] * idx[2]);
         return inside;
     }
@@ -958,6 +1044,7 @@ __global__ void __launch_bounds__(128) k_walk_edge(const PassArgs a, const Packe
         g.t0 = rec.tm[i]; g.t1 = rec.tm[c + i]; g.t2 = rec.tm[2 * c + i];
         g.d0 = rec.td[i]; g.d1 = rec.td[c + i]; g.d2 = rec.td[2 * c + i];
         g.t_cur = 0.0;
+        g.per = a.xyper;
         const int cell = rec.cell[i], bits = rec.bits[i];
         g.ix = cell & 1023; g.iy = (cell >> 10) & 1023; g.iz = (cell >> 20) & 1023;
         g.sx = ((bits >> 16) & 3) - 1; g.sy = ((bits >> 18) & 3) - 1; g.sz = ((bits >> 20) & 3) - 1;
@@ -1001,6 +1088,7 @@ __global__ void __launch_bounds__(128) k_walk_edge(const PassArgs a, const Packe
         R expo = (R)1.0;
         double tau = 0.0;
         int nstep = 0;
+        bool out = false;   // left the grid through a face (not the tau or step limits)
         for (;;) {
             if (++nstep > kMaxWalkSteps) { ++kills; break; }
             R kap = cl[0].template kappa<X>(s0, s1, s2, s3);
@@ -1025,7 +1113,7 @@ __global__ void __launch_bounds__(128) k_walk_edge(const PassArgs a, const Packe
             if constexpr (!X && sizeof(R) == 4) {
                 if (expo == (R)0) break;   // FP32 attenuation underflowed: every later segment scores zero
             }
-            if (!more[0]) break;   // the scored cell was the last one inside the grid
+            if (!more[0]) { out = true; break; }   // the scored cell was the last one inside the grid
 #pragma unroll
             for (int k = 0; k < LA; ++k) {
                 il[k] = il[k + 1]; sgm[k] = sgm[k + 1]; cl[k] = cl[k + 1]; more[k] = more[k + 1];
@@ -1037,6 +1125,9 @@ __global__ void __launch_bounds__(128) k_walk_edge(const PassArgs a, const Packe
                 more[LA] = false;
             }
         }
+        // a z-face escape carries the surviving luminosity to the slab's
+        // boundary tally (raytrace_amr.f90:586-588)
+        if (out && a.slab_iesc) slab_add(a, rec.p0[5 * c + i], (double)expo * a.Lpacket);
         // ion_score_energy_packet (ion_score_mod.f90:233-252)
         const double lum = a.Lpacket;
         const double tr = exp(-fmax(tau, 0.0));
@@ -1148,6 +1239,7 @@ __global__ void __launch_bounds__(128) k_walk_coh(const PassArgs a, const Packet
         g.t0 = rec.tm[ir]; g.t1 = rec.tm[c + ir]; g.t2 = rec.tm[2 * c + ir];
         g.d0 = rec.td[ir]; g.d1 = rec.td[c + ir]; g.d2 = rec.td[2 * c + ir];
         g.t_cur = 0.0;
+        g.per = a.xyper;
         const int cell = rec.cell[ir], bits = rec.bits[ir];
         g.ix = cell & 1023; g.iy = (cell >> 10) & 1023; g.iz = (cell >> 20) & 1023;
         g.sx = ((bits >> 16) & 3) - 1; g.sy = ((bits >> 18) & 3) - 1; g.sz = ((bits >> 20) & 3) - 1;
@@ -1326,12 +1418,12 @@ __global__ void __launch_bounds__(128) k_walk_amr(const PassArgs a, const Packet
         R expo = (R)1.0;
         double tau = 0.0;
         int nstep = 0;
+        int face = -1;   // the face the last leaf was left by; il < 0 after it: out of the grid
         while (il >= 0) {
             if (++nstep > kMaxWalkSteps) { ++kills; break; }
             const double4 g = ld_geo(a.oct.lgeo + il);
             Col<R, NABS> cl;
             cl.load(a.col, il);
-            int face;
             const double texit = oct_cell_exit(g, x, y, z, kx, ky, kz, &face);
             R kap = cl.template kappa<X>(s0, s1, s2, s3);
             if constexpr (METAL) {
@@ -1359,7 +1451,14 @@ __global__ void __launch_bounds__(128) k_walk_amr(const PassArgs a, const Packet
             y = y + texit * ky;
             z = z + texit * kz;
             il = oct_next_leaf(a.oct, il, face, x, y, z);
+            if (il < 0 && a.xyper) {   // raytrace_amr.f90:473-476
+                slab_wrap_xy(a, face, x, y);
+                if (face <= 3) il = oct_find_leaf(a.oct, x, y, z);
+            }
         }
+        // a z-face escape carries the surviving luminosity to the slab's
+        // boundary tally (raytrace_amr.f90:477-481)
+        if (il < 0 && face >= 4 && a.slab_iesc) slab_add(a, kz, (double)expo * a.Lpacket);
         const double lum = a.Lpacket;
         const double tr = exp(-fmax(tau, 0.0));
         emitted += lum;
@@ -1670,6 +1769,16 @@ PassArgs make_args(mochii_ctx* c) {
     a.ext_rmax = c->par.rmax;
     a.bmin[0] = c->grid.xmin; a.bmin[1] = c->grid.ymin; a.bmin[2] = c->grid.zmin;
     a.bmax[0] = c->grid.xmax; a.bmax[1] = c->grid.ymax; a.bmax[2] = c->grid.zmax;
+    a.xyper = c->par.xy_periodic ? 1 : 0;
+    a.slab = c->band.slab;
+    for (int f = 0; f < 2; ++f) {
+        a.slab_mode[f] = c->band.slab_mode[f];
+        a.slab_mu[f] = c->band.slab_mu[f];
+        a.slab_phi[f] = c->band.slab_phi[f];
+    }
+    a.slab_ptop = c->band.slab_ptop;
+    a.slab_nmu = c->band.slab ? c->par.slab_nmu : 0;
+    a.slab_iesc = c->band.slab ? c->slab_iesc : nullptr;
     a.nnu = c->nnu;
     a.m = c->metal;
     a.metal_abs = c->par.ion_metal_abs;
@@ -1756,7 +1865,8 @@ struct WalkLaunch {
 // packet_order 'coherent' applies to the stellar packets on the Cartesian
 // grid without grain or FUV terms; elsewhere the launch order is walked.
 bool coherent_walk_applies(const mochii_ctx* c) {
-    return c->par.packet_order == 2 && c->oct.ncells == 0 && !c->xscore && c->rec.key != nullptr && !c->peeling;
+    return c->par.packet_order == 2 && c->oct.ncells == 0 && !c->xscore && c->rec.key != nullptr && !c->peeling &&
+           !c->band.slab;
 }
 
 // Walk-kernel variants: look-ahead depth 0..2 (the autotuned choice is

@@ -202,6 +202,20 @@ class Nebula:
         self._ok(self.lib.mochii_write_dust_ir(self.ctx, str(base).encode()))
         return str(base) + "_dustir.txt"
 
+    def slab_tally(self):
+        """The plane-parallel slab's boundary tally of the last pass
+        (slab_Iesc): (escaping luminosity [erg/s] per mu bin at the top face,
+        the same at the bottom face, L_in [erg/s], A_zface [cm^2])."""
+        n = 2 * int(self.par.slab_nmu)
+        v, meta = np.zeros(n), np.zeros(2)
+        self._ok(self.lib.mochii_slab_tally(self.ctx, v.ctypes.data, n, meta.ctypes.data))
+        return v[: n // 2], v[n // 2:], float(meta[0]), float(meta[1])
+
+    def write_slab_imu(self, base):
+        """slab_write_Imu: <base>_slab_Imu.txt; returns its path."""
+        self._ok(self.lib.mochii_write_slab_imu(self.ctx, str(base).encode()))
+        return str(base) + "_slab_Imu.txt"
+
     def imaging_pass(self):
         """The peel-off imaging pass (main.f90:234-235): a transport pass with
         with_peel; needs par%ion_peel."""

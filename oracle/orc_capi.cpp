@@ -307,6 +307,14 @@ void orc_sim_energy(void* h, double* e3, long long* segs2) {
     segs2[0] = s->tally.direct_segments;
     segs2[1] = s->tally.scattered_segments;
 }
+// slab_Iesc of the last pass (jtally_mod.f90:39-86): n = 2 nmu values,
+// [face * nmu + bin], face 0 top; returns the count, 0 without the slab.
+int orc_sim_slab(void* h, double* out, int n) {
+    auto* s = static_cast<Sim*>(h);
+    const int m = (int)s->tally.slab.size();
+    for (int k = 0; k < m && k < n; ++k) out[k] = s->tally.slab[k];
+    return m;
+}
 // field names: nH x_HI x_HeI x_HeII n_e T_e gamma_HI gamma_HeI gamma_HeII
 // heat_HI heat_HeI heat_HeII jt_ion (nleaf*nnu, leaf-major) hhe (nleaf*6)
 long long orc_sim_get(void* h, const char* name, double* out, long long cap) {

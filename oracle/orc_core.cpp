@@ -662,6 +662,8 @@ bool parse_namelist(const std::string& text, Par& p, std::string* err) {
         B(solve_te); D(te_min); D(te_max); D(gas_tol_te); B(use_metals);
         B(diffuse_field); B(use_sec_ion); B(ion_add_dust); B(ion_dust_scatter); B(hei_diffuse);
         D(ext_intensity); D(ext_tstar); S(ext_geometry);
+        B(xy_periodic); S(slab_faces); S(slab_top_mode); S(slab_bot_mode); D(slab_top_theta); D(slab_bot_theta);
+        D(slab_top_phi); D(slab_bot_phi); D(slab_top_source); D(slab_bot_source); I(slab_nmu);
         S(dust_density_law); D(cext_dust); S(data_dir); S(atomic_dir); S(ion_dust_kext);
         S(diffuse_energy_model); D(lambda_ref); D(taumax); D(tauhomo);
         else if (k == "iseed") p.iseed = (int64_t)std::llround(to_dbl(s));
@@ -720,6 +722,7 @@ bool parse_namelist(const std::string& text, Par& p, std::string* err) {
         p.source_geometry = "external";
     }
     if (p.grid_type == "uniform") p.grid_type = "car";
+    if (p.source_geometry == "slab") p.nsource = 0;   // setup.f90:327
     (void)err;
     return true;
 }
@@ -894,8 +897,60 @@ bool band_setup(const Par& p, Band& b, std::string* err, const std::vector<doubl
         for (int i = nfuv + 1; i <= nnu + 1; ++i)
             b.eedge[i - 1] = std::exp(lo + (hi - lo) * (double)(i - 1 - nfuv) / (double)(nnu - nfuv));
     }
+    if (p.source_geometry == "slab") {   // slab_setup, :2083-2130, and ion_setup :312-328
+        if (!p.xy_periodic || !box) {
+            set_err(err, "source_geometry='slab' needs par%xy_periodic and the box extent");
+            return false;
+        }
+        b.slab = true;
+        b.ncomp = 1;
+        b.multi_src = false;
+        b.ext_ic = -1;
+        b.qmc_ndim = 6;
+        const std::string faces = lower(p.slab_faces);
+        b.slab_lit[0] = faces == "top" || faces == "both";
+        b.slab_lit[1] = faces == "bottom" || faces == "both";
+        const double src[2] = {p.slab_top_source, p.slab_bot_source};
+        const double theta[2] = {p.slab_top_theta, p.slab_bot_theta};
+        const double deg2rad = PI / 180.0;
+        b.slab_phi[0] = p.slab_top_phi * deg2rad;
+        b.slab_phi[1] = p.slab_bot_phi * deg2rad;
+        b.slab_mode[0] = lower(p.slab_top_mode) == "isotropic" ? 1 : 0;
+        b.slab_mode[1] = lower(p.slab_bot_mode) == "isotropic" ? 1 : 0;
+        b.slab_azface = (box[0] * p.distance2cm) * (box[1] * p.distance2cm);
+        for (int f = 0; f < 2; ++f) {
+            b.slab_Fz[f] = 0.0;
+            b.slab_mu[f] = 1.0;
+            if (!b.slab_lit[f]) continue;
+            if (b.slab_mode[f] == 1) {
+                b.slab_Fz[f] = PI * src[f];
+            } else {
+                b.slab_mu[f] = std::cos(theta[f] * deg2rad);
+                b.slab_Fz[f] = b.slab_mu[f] * src[f];
+            }
+        }
+        const double fz = b.slab_Fz[0] + b.slab_Fz[1];
+        if (!(fz * b.slab_azface > 0.0)) {
+            set_err(err, "source_geometry='slab' has zero entering flux");
+            return false;
+        }
+        b.slab_ptop = b.slab_Fz[0] / fz;
+        std::vector<double> knots = {ETH_HI, ETH_HEI, ETH_HEII};
+        for (double e : meth) knots.push_back(e);
+        if (p.add_fuv) knots.push_back(p.eion_min);
+        b.samplers.resize(1);
+        const double elo = p.add_fuv ? p.efuv_min : p.eion_min;
+        if (!build_planck_sampler(b.samplers[0], p.tstar, elo, p.eion_max, p.source_cdf_tol, knots, err)) return false;
+        const double f_ion = 1.0 - energy_cdf_value(b.samplers[0], p.eion_min);
+        if (f_ion <= 0.0) {
+            set_err(err, "the slab spectrum has no luminosity inside the ionizing band");
+            return false;
+        }
+        b.ion_Ltot = fz * b.slab_azface / f_ion;
+        return true;
+    }
     if (p.source_geometry != "point" && p.source_geometry != "external") {
-        set_err(err, "oracle: only point sources and external fields are restated");
+        set_err(err, "oracle: only point sources, external fields and the slab are restated");
         return false;
     }
     // components, ion_band_mod.f90:188-199 and 683-711: the point sources,
@@ -986,6 +1041,7 @@ void Tally::add(const Tally& o) {
     for (size_t i = 0; i < metal.size(); ++i) metal[i] += o.metal[i];
     for (size_t i = 0; i < dust_abs.size(); ++i) dust_abs[i] += o.dust_abs[i];
     for (size_t i = 0; i < fuv.size(); ++i) fuv[i] += o.fuv[i];
+    for (size_t i = 0; i < slab.size() && i < o.slab.size(); ++i) slab[i] += o.slab[i];
     emitted += o.emitted;
     absorbed += o.absorbed;
     escaped += o.escaped;
@@ -1165,6 +1221,52 @@ void Sim::metal_sigma(Photon& ph) const {
     ph.inside = true;
 }
 
+// emit_slab_qmc, ion_band_mod.f90:2183-2208.
+void Sim::emit_slab(double u_face, double u_c1, double u_c2, double u_mu, double u_phi, Photon& ph) const {
+    const double xr = grid.xmax - grid.xmin, yr = grid.ymax - grid.ymin, zr = grid.zmax - grid.zmin;
+    const double span = std::min(xr, std::min(yr, zr));
+    const double nudge = 1.0e-6 * span;
+    int f = 1;
+    if (u_face > band.slab_ptop) f = 2;
+    const double sgn = f == 1 ? -1.0 : 1.0;
+    ph.x = grid.xmin + xr * u_c1;
+    ph.y = grid.ymin + yr * u_c2;
+    ph.z = f == 1 ? grid.zmax - nudge : grid.zmin + nudge;
+    double mu, phv;
+    if (band.slab_mode[f - 1] == 1) {
+        mu = std::max(std::sqrt(u_mu), 1.0e-6);
+        phv = TWOPI * u_phi;
+    } else {
+        mu = band.slab_mu[f - 1];
+        phv = band.slab_phi[f - 1];
+    }
+    const double sinm = std::sqrt(std::max(1.0 - mu * mu, 0.0));
+    ph.kx = sinm * std::cos(phv);
+    ph.ky = sinm * std::sin(phv);
+    ph.kz = sgn * mu;
+}
+
+// slab_bnd_add, jtally_mod.f90:76-86.
+void Sim::slab_add(Tally& t, double kz, double lum) const {
+    if (t.slab.empty()) return;
+    const int nmu = par.slab_nmu;
+    const double mu = std::fabs(kz);
+    const int ib = std::min(std::max((int)(mu * nmu) + 1, 1), nmu);
+    const int face = kz > 0.0 ? 1 : 2;
+    t.slab[(size_t)(face - 1) * nmu + (ib - 1)] += lum;
+}
+
+// slab_wrap_xy, raytrace_amr.f90:330-345 (faces 0-based: 0 +x, 1 -x, 2 +y, 3 -y).
+void Sim::slab_wrap_xy(int iface, double& x, double& y) const {
+    switch (iface) {
+        case 0: x = grid.xmin; break;
+        case 1: x = grid.xmax; break;
+        case 2: y = grid.ymin; break;
+        case 3: y = grid.ymax; break;
+        default: break;
+    }
+}
+
 // emit_external_rec_qmc, ion_band_mod.f90:2253-2323.
 void Sim::emit_external_rec(double u_mu, double u_phi, double u_face, double u_c1, double u_c2, Photon& ph) const {
     const double xr = grid.xmax - grid.xmin, yr = grid.ymax - grid.ymin, zr = grid.zmax - grid.zmin;
@@ -1230,9 +1332,12 @@ void Sim::gen_photon_qmc(int64_t ip, Photon& ph) const {
     double u[12];
     for (int d = 1; d <= band.qmc_ndim; ++d) u[d - 1] = qmc.uniform(ip, d, 1);
     double e;
-    double umu, uphi, xs = 0.0, ys = 0.0, zs = 0.0;
+    double umu = 0.0, uphi = 0.0, xs = 0.0, ys = 0.0, zs = 0.0;
     int ic = 0;
-    if (!band.multi_src && band.qmc_ndim == 3) {
+    if (band.slab) {   // slab layout (:1895-1898): u1 energy, u2 face, u3/u4 xy, u5 mu, u6 phi
+        emit_slab(u[1], u[2], u[3], u[4], u[5], ph);
+        e = sample_energy_cdf(band.samplers[0], u[0]);
+    } else if (!band.multi_src && band.qmc_ndim == 3) {
         xs = par.xs_point; ys = par.ys_point; zs = par.zs_point;
         umu = u[1]; uphi = u[2];
         e = sample_energy_cdf(band.samplers[0], u[0]);
@@ -1247,7 +1352,8 @@ void Sim::gen_photon_qmc(int64_t ip, Photon& ph) const {
         umu = u[2]; uphi = u[3];
         e = sample_energy_cdf(band.samplers[ic], u[1]);
     }
-    if (ic == band.ext_ic) {
+    if (band.slab) {
+    } else if (ic == band.ext_ic) {
         if (par.ext_geometry == "sph") emit_external_sph(u[2], u[3], u[4], u[5], ph);
         else emit_external_rec(u[2], u[3], u[4], u[5], u[6], ph);
     } else {
@@ -1355,7 +1461,14 @@ void Sim::walk_edge_car(const Photon& ph, Tally& t, double* tau_edge) const {
         t_cur = tmax[a];
         tmax[a] = tmax[a] + tdel[a];
         idx[a] += stp[a];
-        if (idx[a] < 0 || idx[a] >= n[a]) break;
+        if (idx[a] < 0 || idx[a] >= n[a]) {
+            if (par.xy_periodic && a < 2) {   // :575-582, modulo
+                idx[a] = ((idx[a] % n[a]) + n[a]) % n[a];
+            } else {
+                if (a == 2) slab_add(t, ph.kz, expo * wl);   // :583-588
+                break;
+            }
+        }
     }
     *tau_edge = tau;
 }
@@ -1451,8 +1564,15 @@ void Sim::walk_edge_amr(const Photon& ph, Tally& t, double* tau_edge) const {
         x = x + texit * kx;
         y = y + texit * ky;
         z = z + texit * kz;
-        const int nl = leaf_next(il, iface, x, y, z);
-        if (nl < 0) break;
+        int nl = leaf_next(il, iface, x, y, z);
+        if (nl < 0 && par.xy_periodic) {   // :473-476
+            slab_wrap_xy(iface, x, y);
+            if (iface <= 3) nl = leaf_find(x, y, z);
+        }
+        if (nl < 0) {
+            if (iface >= 4) slab_add(t, kz, expo * wl);   // :477-481
+            break;
+        }
         il = nl;
     }
     *tau_edge = tau;
@@ -1491,9 +1611,14 @@ void Sim::walk_to_tau(Photon& ph, double tau_in, Tally& t) const {
             if (do_tally) score(*this, ph, il, wl * texit, t);
             tau = tau + texit * kap;
             x = x + texit * ph.kx; y = y + texit * ph.ky; z = z + texit * ph.kz;
-            const int nl = leaf_next(il, iface, x, y, z);
+            int nl = leaf_next(il, iface, x, y, z);
+            if (nl < 0 && par.xy_periodic) {   // :403-406
+                slab_wrap_xy(iface, x, y);
+                if (iface <= 3) nl = leaf_find(x, y, z);
+            }
             if (nl < 0) {
                 ph.inside = false;
+                if (iface >= 4) slab_add(t, ph.kz, wl);   // :407-413
                 break;
             }
             il = nl;
@@ -1546,13 +1671,23 @@ void Sim::walk_to_tau(Photon& ph, double tau_in, Tally& t) const {
         tmax[a] = tmax[a] + tdel[a];
         idx[a] += stp[a];
         if (idx[a] < 0 || idx[a] >= n[a]) {
-            ph.inside = false;
-            break;
+            if (par.xy_periodic && a < 2) {   // :639-654
+                idx[a] = ((idx[a] % n[a]) + n[a]) % n[a];
+            } else {
+                ph.inside = false;
+                if (a == 2) slab_add(t, ph.kz, wl);   // :655-660
+                break;
+            }
         }
     }
     ph.x = ph.x + t_cur * ph.kx;
     ph.y = ph.y + t_cur * ph.ky;
     ph.z = ph.z + t_cur * ph.kz;
+    if (par.xy_periodic) {   // :666-672
+        const double xr = grid.xmax - grid.xmin, yr = grid.ymax - grid.ymin;
+        ph.x = ph.x - std::floor((ph.x - grid.xmin) / xr) * xr;
+        ph.y = ph.y - std::floor((ph.y - grid.ymin) / yr) * yr;
+    }
     if (ph.inside) ph.il = idx[0] + n[0] * (idx[1] + n[1] * idx[2]);
 }
 
@@ -1684,6 +1819,7 @@ void Sim::transport_pass() {
         t.img_dir.assign(npix, 0.0);
         t.img_sca.assign(npix, 0.0);
         t.img_dir0.assign(peel && par.save_direc0 ? npix : 0, 0.0);
+        t.slab.assign(band.slab ? 2 * (size_t)par.slab_nmu : 0, 0.0);
     }
     const int64_t np = par.nphotons;
 #pragma omp parallel num_threads(nt)
@@ -1726,6 +1862,7 @@ void Sim::transport_pass() {
     tally.img_dir.assign(npix, 0.0);
     tally.img_sca.assign(npix, 0.0);
     tally.img_dir0.assign(peel && par.save_direc0 ? npix : 0, 0.0);
+    tally.slab.assign(band.slab ? 2 * (size_t)par.slab_nmu : 0, 0.0);
     for (auto& t : loc) tally.add(t);
     gas_rates_compute();
     if (metals()) {   // species_gamma_compute, species_mod.f90:493-512

@@ -132,6 +132,12 @@ struct Par {
     std::string source_geometry = "point";
     double ext_intensity = -1.0, ext_tstar = -999.0;   // define.f90:270-277
     std::string ext_geometry = "rec";
+    // plane-parallel slab illumination on an xy-periodic grid (define.f90:217, 304-321)
+    bool xy_periodic = false;
+    std::string slab_faces = "top", slab_top_mode = "beam", slab_bot_mode = "beam";
+    double slab_top_theta = 0.0, slab_bot_theta = 0.0, slab_top_phi = 0.0, slab_bot_phi = 0.0;
+    double slab_top_source = 0.0, slab_bot_source = 0.0;
+    int slab_nmu = 20;
     double xs_point = 0.0, ys_point = 0.0, zs_point = 0.0;
     int nsource = 1;
     double src_tstar[MAX_SRC], src_lum[MAX_SRC];
@@ -185,6 +191,12 @@ struct Band {
     std::vector<Sampler> samplers;   // source_energy_sampler
     double ion_Ltot = 0.0;
     int qmc_ndim = 3;
+    // slab_setup (ion_band_mod.f90:2083-2130), per face [top, bottom]
+    bool slab = false;
+    bool slab_lit[2] = {false, false};
+    int slab_mode[2] = {0, 0};
+    double slab_mu[2] = {1.0, 1.0}, slab_phi[2] = {0.0, 0.0}, slab_Fz[2] = {0.0, 0.0};
+    double slab_ptop = 1.0, slab_azface = 0.0;
 };
 bool build_aligned_edges(std::vector<double>& eedge, int nfuv, int nnu,
                          double lo, double hi, const std::vector<double>& meth,
@@ -214,6 +226,7 @@ struct Tally {
     std::vector<double> dust_abs;    // dust_abs_path (nleaf), with ion_add_dust
     std::vector<double> fuv;         // fuv_field_path (nleaf), with add_fuv
     std::vector<double> img_dir, img_sca, img_dir0;   // peel-off images (nobs, nchan, nyim, nxim)
+    std::vector<double> slab;        // slab_Iesc (nmu, 2) as [face * nmu + bin], face 0 top
     long double emitted = 0, absorbed = 0, escaped = 0;
     int64_t direct_segments = 0, scattered_segments = 0;
     void reset(int nleaf, int nnu, int ntr = 0, bool dust = false, bool fuv = false);
@@ -310,6 +323,9 @@ struct Sim {
     void gen_diffuse_qmc(int64_t ip, Photon& ph) const;          // diffuse_mod.f90:221-296
     void emit_external_rec(double u_mu, double u_phi, double u_face, double u_c1, double u_c2, Photon& ph) const;
     void emit_external_sph(double u_mu, double u_phi, double u_cost, double u_saz, Photon& ph) const;
+    void emit_slab(double u_face, double u_c1, double u_c2, double u_mu, double u_phi, Photon& ph) const;
+    void slab_add(Tally& t, double kz, double lum) const;            // slab_bnd_add, jtally_mod.f90:76-86
+    void slab_wrap_xy(int iface, double& x, double& y) const;      // raytrace_amr.f90:330-345
     bool setup(const std::string& namelist, std::string* err);
     void transport_pass();           // ionizing_field_mod.f90:72-170
     void gas_rates_compute();        // gas_rates_mod.f90:82-153

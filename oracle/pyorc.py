@@ -53,6 +53,7 @@ def load():
         "orc_sim_transport_pass": (I, [V]),
         "orc_sim_equilibrium_update": (I, [V, V]),
         "orc_sim_energy": (None, [V, V, V]),
+        "orc_sim_slab": (I, [V, V, I]),
         "orc_philox": (None, [C.c_ulonglong, C.c_uint, C.c_ulonglong, C.c_uint, I, V]),
         "orc_sim_dust_optics": (I, [V, LL, V, V]),
         "orc_philox_block": (None, [V, V, V]),
@@ -294,6 +295,12 @@ class Sim:
         out = np.zeros((E.size, 3))
         assert load().orc_sim_dust_optics(self.h, E.size, E.ctypes.data, out.ctypes.data) == 0
         return out
+
+    def slab_tally(self, nmu):
+        """slab_Iesc of the last pass: (top face per mu bin, bottom face)."""
+        out = np.zeros(2 * nmu)
+        assert load().orc_sim_slab(self.h, out.ctypes.data, 2 * nmu) == 2 * nmu
+        return out[:nmu], out[nmu:]
 
     def energy(self):
         e = np.zeros(3)
