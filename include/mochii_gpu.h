@@ -199,8 +199,7 @@ typedef struct mochii_params {
      * Planck spectrum at ext_tstar (> 0) else tstar.  source_geometry
      * 'external' / 'external_rec' / 'external_sph' is the external-only
      * shorthand (source_external 1 / 1 / 2: nsource taken as 0).
-     * ext_spectrum_set: a par%ext_spectrum file or preset was named (not
-     * built; refused) */
+     * ext_spectrum_set: a par%ext_spectrum file or preset was named */
     double ext_intensity, ext_tstar;
     int ext_geometry, source_external, ext_spectrum_set;
     /* plane-parallel slab illumination (define.f90:217, 304-321):
@@ -214,6 +213,16 @@ typedef struct mochii_params {
     int xy_periodic, source_slab, slab_faces, slab_nmu;
     int slab_mode[2];
     double slab_theta[2], slab_phi[2], slab_source[2];
+    /* tabulated spectra (define.f90:276-303): ion_spectrum (the primary
+     * source), src_spectrum_file (column i for point source i),
+     * ext_spectrum (the external field's J: a file, or the ISRF preset
+     * 'draine', 'habing' or 'mathis' scaled by ext_scale); spectrum_type
+     * the column units of every file: 0 'shape_ev' (E [eV], any scale),
+     * 1 'per_ev', 2 'per_hz', 3 'per_ang', 4 'per_um' (absolute densities
+     * per eV, Hz, Angstrom, micron) */
+    char ion_spectrum[MOCHII_STRLEN], src_spectrum_file[MOCHII_STRLEN], ext_spectrum[MOCHII_STRLEN];
+    int spectrum_type;
+    double ext_scale;
 } mochii_params;
 
 /* Per-pass statistics (ion_score_report_energy_closure, ion_score_mod.f90:364-387). */

@@ -71,6 +71,8 @@ class Params(C.Structure):
         ("xy_periodic", C.c_int), ("source_slab", C.c_int), ("slab_faces", C.c_int), ("slab_nmu", C.c_int),
         ("slab_mode", C.c_int * 2), ("slab_theta", C.c_double * 2), ("slab_phi", C.c_double * 2),
         ("slab_source", C.c_double * 2),
+        ("ion_spectrum", C.c_char * STRLEN), ("src_spectrum_file", C.c_char * STRLEN),
+        ("ext_spectrum", C.c_char * STRLEN), ("spectrum_type", C.c_int), ("ext_scale", C.c_double),
     ]
 
 

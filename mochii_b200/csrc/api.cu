@@ -128,6 +128,13 @@ int validate(const mochii_params& p, std::string* why, int* code) {
     if (p.solve_te && !(p.te_min > 0.0 && p.te_max > p.te_min)) return *why = "need 0 < par%te_min < par%te_max", 1;
     if (p.He_abund < 0.0) return *why = "par%He_abund must be >= 0", 1;
     if (!p.grid_car && !p.amr_file[0]) return *why = "grid_type='amr' needs par%amr_file (a text leaf list)", 1;
+    if (spectrum_preset_id(p.ion_spectrum) > 0 || spectrum_preset_id(p.src_spectrum_file) > 0)   // setup.f90:224-232
+        return *why = "ISRF preset names (draine/habing/mathis) are valid only for par%ext_spectrum", 1;
+    if (spectrum_preset_id(p.ext_spectrum) > 0) {   // setup.f90:339-352
+        if (p.ext_scale <= 0.0) return *why = "par%ext_scale must be > 0 for an ISRF preset", 1;
+        if (!p.add_fuv)
+            return *why = "the ISRF presets are FUV-only; set par%add_fuv (with par%efuv_min < 13.6)", 1;
+    }
     if (p.source_slab) {   // setup.f90:259-327
         if (!p.xy_periodic) return *why = "source_geometry='slab' needs par%xy_periodic (a slab is periodic in x and y)", 1;
         if (p.nsource > 1 || p.ext_intensity > 0.0)
@@ -149,7 +156,8 @@ int validate(const mochii_params& p, std::string* why, int* code) {
         return *why = "the taumax / tauhomo dust normalisations are not built", 1;
     if (p.ion_add_dust && !p.ion_dust_kext[0])
         return *why = "ion_add_dust needs par%ion_dust_kext (the grain-model optics are not built)", 1;
-    if (p.ion_peel && (p.ext_intensity > 0.0 || p.source_external))
+    if (p.ion_peel && (p.ext_intensity > 0.0 || p.source_external || spectrum_preset_id(p.ext_spectrum) > 0 ||
+                       (p.spectrum_type != 0 && p.ext_spectrum[0])))
         return *why = "the peel-off of external-field packets is not built", 1;
     *code = MOCHII_ERR_BAD_PARAM;
     if (p.ion_peel && p.xy_periodic)   // setup.f90:531-539

@@ -234,6 +234,125 @@ std::vector<double> knots_of(const mochii_params& p, const std::vector<double>& 
     return knots;
 }
 
+// The luminosity sentinel and the point sources' scales (setup.f90:374-442):
+// an unset par%luminosity is 1 unless an absolute (physical-type) file feeds
+// the primary source; a lone point source takes the legacy scalars into slot
+// 1 when src_lum(1) is unset; several sources with no src_lum split
+// luminosity equally (shape spectra) or derive it from the file (absolute).
+bool resolve_sources(mochii_params& q, int npt, std::string* err) {
+    const bool phys = q.spectrum_type != 0;
+    const bool src_abs = phys && (q.src_spectrum_file[0] || q.ion_spectrum[0]);
+    if (q.luminosity < -900.0 && !(npt >= 1 && src_abs)) q.luminosity = 1.0;
+    if (npt == 1) {
+        if (q.src_lum[0] <= 0.0) {
+            q.src_x[0] = q.xs_point;
+            q.src_y[0] = q.ys_point;
+            q.src_z[0] = q.zs_point;
+            q.src_lum[0] = q.luminosity;
+        }
+    } else if (npt > 1) {
+        int nset = 0;
+        for (int i = 0; i < npt; ++i) nset += q.src_lum[i] > 0.0;
+        if (nset == 0) {
+            if (!src_abs)
+                for (int i = 0; i < npt; ++i) q.src_lum[i] = q.luminosity / (double)npt;
+        } else if (nset != npt) {
+            return fail(err, "set par%src_lum for ALL sources or for NONE (setup.f90:428-433)");
+        }
+    }
+    return true;
+}
+
+// source_band_luminosity (ion_band_mod.f90:379-399): an absolute spectrum
+// with no scale keeps its own integral; otherwise the scale is the ionizing
+// luminosity and the band carries scale / f_ion.
+bool band_luminosity(const EnergyTable& t, bool is_abs, double scale, double eion_min, double* L, std::string* err) {
+    if (is_abs && scale <= 0.0) {
+        *L = t.total;
+        return true;
+    }
+    const double f_ion = 1.0 - table_cdf(t, eion_min);
+    if (f_ion <= 0.0) return fail(err, "cannot rescale a source with no ionizing-band luminosity (FUV-only spectrum)");
+    *L = scale / f_ion;
+    return true;
+}
+
+// A tabulated file slot clipped to the band (build_tabulated_band_sampler).
+bool file_table(EnergyTable& t, const char* path, int icol, int ncol, const mochii_params& q, double elo,
+                std::string* err) {
+    std::vector<double> e, f;
+    if (!spectrum_read(path, icol, ncol, q.spectrum_type, e, f, err)) return false;
+    return table_band(t, e, f, elo, q.eion_max, err);
+}
+
+// build_point_source_sampler (ion_band_mod.f90:437-495): the spectrum of
+// point source is (0-based) from src_spectrum_file column is + 1 >
+// src_tstar(is) Planck (several components only) > ion_spectrum > tstar
+// Planck, its band luminosity normalised in the branch that chose it.
+bool point_sampler(const mochii_params& q, int is, bool multi, double elo, const std::vector<double>& knots,
+                   EnergyTable& t, double* L, std::string* err) {
+    const double scale = multi ? q.src_lum[is] : q.luminosity;
+    const bool phys = q.spectrum_type != 0;
+    if (q.src_spectrum_file[0]) {
+        if (!file_table(t, q.src_spectrum_file, is + 1, std::max(q.nsource, 1), q, elo, err)) return false;
+        return band_luminosity(t, phys, scale, q.eion_min, L, err);
+    }
+    if (multi && q.src_tstar[is] > 0.0) {
+        if (!planck_table(t, q.src_tstar[is], elo, q.eion_max, q.source_cdf_tol, knots, err)) return false;
+        return band_luminosity(t, false, scale, q.eion_min, L, err);
+    }
+    if (q.ion_spectrum[0]) {
+        if (!file_table(t, q.ion_spectrum, 1, 1, q, elo, err)) return false;
+        return band_luminosity(t, phys, scale, q.eion_min, L, err);
+    }
+    if (q.tstar <= 0.0) return fail(err, "point source needs a spectrum (par%tstar, par%ion_spectrum or a file)");
+    if (!planck_table(t, q.tstar, elo, q.eion_max, q.source_cdf_tol, knots, err)) return false;
+    return band_luminosity(t, false, scale, q.eion_min, L, err);
+}
+
+// build_external_field_sampler (ion_band_mod.f90:516-615): an ISRF preset >
+// an ext_spectrum file > ext_tstar Planck > ion_spectrum > tstar Planck; the
+// power entering the surface A is pi A J with an absolute J (a preset or a
+// physical-type file; rescaled to ext_intensity when that is set), else
+// pi J A / f_ion with J the ionizing-band intensity.
+bool external_sampler(const mochii_params& q, bool sph, double elo, const std::vector<double>& knots, const double* box,
+                      EnergyTable& t, double* L, std::string* err) {
+    const int presid = spectrum_preset_id(q.ext_spectrum);
+    const bool phys = q.spectrum_type != 0;
+    const bool is_abs = presid > 0 || (phys && q.ext_spectrum[0]);
+    if (presid > 0) {
+        if (!preset_table(t, presid, elo, q.eion_max, q.ext_scale, err)) return false;
+    } else if (q.ext_spectrum[0]) {
+        if (!file_table(t, q.ext_spectrum, 1, 1, q, elo, err)) return false;
+    } else if (q.ext_tstar > 0.0) {
+        if (!planck_table(t, q.ext_tstar, elo, q.eion_max, q.source_cdf_tol, knots, err)) return false;
+    } else if (q.ion_spectrum[0]) {
+        if (!file_table(t, q.ion_spectrum, 1, 1, q, elo, err)) return false;
+    } else {
+        if (q.tstar <= 0.0) return fail(err, "external field needs a spectrum (par%ext_tstar / par%tstar or a file)");
+        if (!planck_table(t, q.tstar, elo, q.eion_max, q.source_cdf_tol, knots, err)) return false;
+    }
+    if (!box) return fail(err, "external field: the box extent is unknown");
+    double asurf;
+    if (sph) {
+        if (!(q.rmax > 0.0)) return fail(err, "ext_geometry 'sph' needs par%rmax > 0");
+        if (2.0 * q.rmax > std::min(box[0], std::min(box[1], box[2])))
+            return fail(err, "ext_geometry 'sph': the bounding sphere (par%rmax) must lie inside the grid");
+        asurf = 4.0 * kPi * ((q.rmax * q.distance2cm) * (q.rmax * q.distance2cm));
+    } else {
+        const double xr = box[0] * q.distance2cm, yr = box[1] * q.distance2cm, zr = box[2] * q.distance2cm;
+        asurf = 2.0 * (xr * yr + yr * zr + zr * xr);
+    }
+    if (is_abs) {
+        *L = q.ext_intensity > 0.0 ? kPi * asurf * q.ext_intensity : kPi * asurf * t.total;
+        return true;
+    }
+    const double f_ion = 1.0 - table_cdf(t, q.eion_min);
+    if (f_ion <= 0.0) return fail(err, "the external spectrum has no luminosity inside the ionizing band");
+    *L = kPi * q.ext_intensity * asurf / f_ion;
+    return true;
+}
+
 // The plane-parallel slab (setup.f90:259-330, slab_setup
 // ion_band_mod.f90:2083-2130, ion_setup :312-328): one component with the
 // single point source's Planck spectrum at tstar, its luminosity the
@@ -275,9 +394,12 @@ bool slab_build(const mochii_params& p, BandSetup& b, std::string* err, const st
     if (!(fz * b.slab_azface > 0.0)) return fail(err, "source_geometry='slab' has zero entering flux");
     b.slab_ptop = b.slab_Fz[0] / fz;
     const double elo = p.add_fuv ? p.efuv_min : p.eion_min;
-    if (p.tstar <= 0.0) return fail(err, "slab needs a Planck temperature (par%tstar)");
     b.tables.assign(1, EnergyTable());
-    if (!planck_table(b.tables[0], p.tstar, elo, p.eion_max, p.source_cdf_tol, knots, err)) return false;
+    double unused;
+    mochii_params q = p;   // the spectrum resolves as point source 1's (ion_band_mod.f90:296-297)
+    q.nsource = 0;
+    if (!resolve_sources(q, 0, err) || !point_sampler(q, 0, false, elo, knots, b.tables[0], &unused, err))
+        return false;
     const double f_ion = 1.0 - table_cdf(b.tables[0], p.eion_min);
     if (f_ion <= 0.0) return fail(err, "the slab spectrum has no luminosity inside the ionizing band");
     b.comp_x.assign(1, 0.0);
@@ -314,13 +436,16 @@ bool band_build(const mochii_params& p, BandSetup& b, std::string* err, const st
         return fail(err, "par%source_geometry must be 'point', 'slab', 'external_rec' or 'external_sph'");
     if (p.source_slab) return slab_build(p, b, err, knots_of(p, metal_eth), box);
     // components (ion_band_mod.f90:188-199, 683-711): the point sources, then
-    // the external field when par%ext_intensity > 0
-    const bool ext_on = p.ext_intensity > 0.0;
-    if (p.ext_spectrum_set) return fail(err, "par%ext_spectrum (files and ISRF presets) is not built");
+    // the external field when it is on (external_on, :884-889)
+    const bool ext_on = p.ext_intensity > 0.0 || spectrum_preset_id(p.ext_spectrum) > 0 ||
+                        (p.spectrum_type != 0 && p.ext_spectrum[0]);
     if (p.source_external && !ext_on)
-        return fail(err, "external source_geometry requires par%ext_intensity > 0 (setup.f90:249-254)");
+        return fail(err, "external source_geometry requires par%ext_intensity > 0, an ISRF preset or a physical-type "
+                         "ext_spectrum (setup.f90:246-253)");
     const int npt = p.source_external ? 0 : p.nsource;
     if (npt < 0 || npt > MOCHII_MAX_SRC) return fail(err, "par%nsource out of range");
+    mochii_params q = p;
+    if (!resolve_sources(q, npt, err)) return false;
     b.ncomp = npt + (ext_on ? 1 : 0);
     if (b.ncomp < 1) return fail(err, "no source: par%nsource = 0 without an external field");
     b.multi = b.ncomp >= 2;
@@ -335,37 +460,14 @@ bool band_build(const mochii_params& p, BandSetup& b, std::string* err, const st
     b.comp_z.assign(b.ncomp, 0.0);
     std::vector<double> L(b.ncomp);
     for (int c = 0; c < b.ncomp; ++c) {
-        if (c == b.ext_ic) {   // build_external_field_sampler (:516-615), Planck spectra
-            const double T = p.ext_tstar > 0.0 ? p.ext_tstar : p.tstar;
-            if (T <= 0.0) return fail(err, "external field needs a Planck temperature (par%ext_tstar / par%tstar)");
-            if (!planck_table(b.tables[c], T, elo, p.eion_max, p.source_cdf_tol, knots, err)) return false;
-            if (!box) return fail(err, "external field: the box extent is unknown");
-            double asurf;
-            if (b.ext_sph) {
-                if (!(p.rmax > 0.0)) return fail(err, "ext_geometry 'sph' needs par%rmax > 0");
-                if (2.0 * p.rmax > std::min(box[0], std::min(box[1], box[2])))
-                    return fail(err, "ext_geometry 'sph': the bounding sphere (par%rmax) must lie inside the grid");
-                asurf = 4.0 * kPi * ((p.rmax * p.distance2cm) * (p.rmax * p.distance2cm));
-            } else {
-                const double xr = box[0] * p.distance2cm, yr = box[1] * p.distance2cm, zr = box[2] * p.distance2cm;
-                asurf = 2.0 * (xr * yr + yr * zr + zr * xr);
-            }
-            const double f_ion = 1.0 - table_cdf(b.tables[c], p.eion_min);
-            if (f_ion <= 0.0) return fail(err, "the external spectrum has no luminosity inside the ionizing band");
-            L[c] = kPi * p.ext_intensity * asurf / f_ion;
+        if (c == b.ext_ic) {
+            if (!external_sampler(q, b.ext_sph, elo, knots, box, b.tables[c], &L[c], err)) return false;
             continue;
         }
-        const double T = (b.multi && p.src_tstar[c] > 0.0) ? p.src_tstar[c] : p.tstar;
-        const double scale = b.multi ? p.src_lum[c] : p.luminosity;
-        if (T <= 0.0) return fail(err, "point source needs a Planck temperature (par%tstar / par%src_tstar)");
-        if (scale <= 0.0) return fail(err, "point source needs a luminosity (par%luminosity / par%src_lum)");
-        if (!planck_table(b.tables[c], T, elo, p.eion_max, p.source_cdf_tol, knots, err)) return false;
-        const double f_ion = 1.0 - table_cdf(b.tables[c], p.eion_min);   // ionizing_fraction
-        if (f_ion <= 0.0) return fail(err, "source has no ionizing-band luminosity");
-        L[c] = scale / f_ion;
-        b.comp_x[c] = b.multi ? p.src_x[c] : p.xs_point;
-        b.comp_y[c] = b.multi ? p.src_y[c] : p.ys_point;
-        b.comp_z[c] = b.multi ? p.src_z[c] : p.zs_point;
+        if (!point_sampler(q, c, b.multi, elo, knots, b.tables[c], &L[c], err)) return false;
+        b.comp_x[c] = b.multi ? q.src_x[c] : q.xs_point;
+        b.comp_y[c] = b.multi ? q.src_y[c] : q.ys_point;
+        b.comp_z[c] = b.multi ? q.src_z[c] : q.zs_point;
     }
     b.ion_Ltot = 0.0;
     for (double x : L) b.ion_Ltot += x;

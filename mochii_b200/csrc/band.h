@@ -44,6 +44,21 @@ struct BandSetup {
     double slab_azface = 0.0;           // z-face area of one periodic tile [cm^2]
 };
 
+// Tabulated spectra (spectrum.cpp).  spectrum_preset_id: 'draine' 1,
+// 'habing' 2, 'mathis' 3, else 0 (ion_ext_preset_id).  spectrum_read: the
+// icol-th of ncol value columns of a spectrum file as ascending (E [eV],
+// density per eV), converted from spectrum_type (0 shape_ev, 1 per_ev,
+// 2 per_hz, 3 per_ang, 4 per_um).  table_band: the tabulated sampler
+// clipped to [emin, emax].  preset_table: a preset's J_E x scale on 4096
+// uniform nodes from elo to min(emax, 13.6 eV).
+int spectrum_preset_id(const char* name);
+double preset_je(double E, int id);
+bool spectrum_read(const std::string& path, int icol, int ncol, int type, std::vector<double>& e,
+                   std::vector<double>& f, std::string* err);
+bool table_band(EnergyTable& t, const std::vector<double>& e, const std::vector<double>& f, double emin, double emax,
+                std::string* err);
+bool preset_table(EnergyTable& t, int id, double elo, double emax, double scale, std::string* err);
+
 // metal_eth: the active metal thresholds in registry order (main.f90:65-82),
 // which pin band edges and sampler knots as the H/He thresholds do.
 // box: the grid's x, y, z extents in code units (the external field's entry

@@ -31,9 +31,9 @@ const char* const kOtherKeys[] = {
     "density_rscale", "density_zprofile", "density_zscale",
     "dust_emis_bands", "dust_emis_transport", "dust_emission_method", "dust_fast_table", "dust_model",
     "dust_niter", "dust_no_photons", "dust_nu", "dust_sed", "dust_single_teq", "dust_tol",
-    "emis_output", "exetime", "ext_scale",
+    "emis_output", "exetime", 
     "f_ion_dust", "f_ion_pah", "f_pah", "file_format", "geometry", "h_coll_effects",
-    "hei_metastable", "hgg", "ion_spectrum", "kext_file",
+    "hei_metastable", "hgg", "kext_file",
     "lambda0", "lambda_max", "lambda_min", "line_case", "mrw_gamma", "nlambda", "no_print",
     "nobs", "nprint", "nr", "nscatt_tot", "num_send_at_once",
     "out_bitpix", "out_bitpix_force", "out_file", "output_normalization", "pe_scale",
@@ -41,8 +41,8 @@ const char* const kOtherKeys[] = {
     "save_jlam",
     "scatt_mat_file", "sed_data_dir", "sed_dl07_sdindex", "sed_dl07_uisrf", "sed_kext", "sed_nt",
     "sed_pah_live", "sed_thi", "sed_tlo", "sightline_tau", "source_rscale", "source_spectrum", "source_zscale",
-    "spectrum_type", "spiral_amp", "spiral_m", "spiral_pitch", "src_axial_ratio", "src_boxiness",
-    "src_geometry", "src_reff", "src_rscale", "src_sersic_index", "src_spectrum", "src_spectrum_file",
+    "spiral_amp", "spiral_m", "spiral_pitch", "src_axial_ratio", "src_boxiness",
+    "src_geometry", "src_reff", "src_rscale", "src_sersic_index", "src_spectrum",
     "src_zscale", "use_amr_grid", "use_dustemis", "use_master_slave", "use_mrw",
     "use_reduced_wgt", "use_sed", "use_stokes", "xyz_symmetry", "z_global", "z_ref",
     "z_symmetry", "dust_density_law_file"};
@@ -147,6 +147,7 @@ extern "C" int mochii_params_default(mochii_params* p) {
     p->refine_eps = 1.0e-2; p->refine_dx = 0.2;
     p->ext_intensity = -1.0; p->ext_tstar = -999.0; p->ext_geometry = 0;   // define.f90:270-277
     p->slab_faces = 1; p->slab_nmu = 20;                                    // define.f90:312-321
+    p->ext_scale = 1.0;                                                     // define.f90:303
     const double nan = std::numeric_limits<double>::quiet_NaN();
     p->distance = nan; p->dxim = nan; p->dyim = nan;
     for (int i = 0; i < MOCHII_MAX_OBS; ++i) {
@@ -246,7 +247,23 @@ int set_key(mochii_params* p, std::string key, const std::vector<std::string>& v
         p->ext_geometry = s == "sph" ? 1 : 0;
         return 0;
     }
-    if (key == "ext_spectrum") { p->ext_spectrum_set = unquote(v).find_first_not_of(' ') != std::string::npos; return 0; }
+    if (key == "ext_spectrum" || key == "ion_spectrum" || key == "src_spectrum_file") {
+        const std::string s = strip(unquote(v));
+        char* dst = key == "ext_spectrum" ? p->ext_spectrum : key == "ion_spectrum" ? p->ion_spectrum
+                                                                                : p->src_spectrum_file;
+        if (s.size() >= MOCHII_STRLEN) return bad("path too long");
+        copy_str(dst, MOCHII_STRLEN, s);
+        if (key == "ext_spectrum") p->ext_spectrum_set = !s.empty();
+        return 0;
+    }
+    if (key == "spectrum_type") {   // setup.f90:213-221
+        const std::string s = lower(strip(unquote(v)));
+        static const char* const names[] = {"shape_ev", "per_ev", "per_hz", "per_ang", "per_um"};
+        for (int k = 0; k < 5; ++k)
+            if (s == names[k]) { p->spectrum_type = k; return 0; }
+        return bad("must be 'shape_ev', 'per_ev', 'per_hz', 'per_ang' or 'per_um'");
+    }
+    REAL("ext_scale", ext_scale)
     REAL("ext_intensity", ext_intensity) REAL("ext_tstar", ext_tstar)
     REAL("xs_point", xs_point) REAL("ys_point", ys_point) REAL("zs_point", zs_point)
     INT("nsource", nsource)

@@ -662,6 +662,7 @@ bool parse_namelist(const std::string& text, Par& p, std::string* err) {
         B(solve_te); D(te_min); D(te_max); D(gas_tol_te); B(use_metals);
         B(diffuse_field); B(use_sec_ion); B(ion_add_dust); B(ion_dust_scatter); B(hei_diffuse);
         D(ext_intensity); D(ext_tstar); S(ext_geometry);
+        S(ion_spectrum); S(src_spectrum_file); S(ext_spectrum); S(spectrum_type); D(ext_scale);
         B(xy_periodic); S(slab_faces); S(slab_top_mode); S(slab_bot_mode); D(slab_top_theta); D(slab_bot_theta);
         D(slab_top_phi); D(slab_bot_phi); D(slab_top_source); D(slab_bot_source); I(slab_nmu);
         S(dust_density_law); D(cext_dust); S(data_dir); S(atomic_dir); S(ion_dust_kext);
@@ -870,11 +871,241 @@ int ion_bin_of(const Band& b, double eph, bool include_fuv) {
     return r - 1;
 }
 
-// ion_setup (ion_band_mod.f90:122-258) restricted to internal point
-// sources with Planck spectra (the hot-path configurations), plus
+// ---- tabulated spectra and ISRF presets (ion_band_mod.f90:870-911, 1438-1720)
+static const double HC_EVANG = 12398.42;   // define.f90:62
+static const double H_CGS = 6.62607015e-27;   // define.f90:59
+
+// spec_is_physical, ion_band_mod.f90:870-877.
+static bool spec_is_physical(const Par& p) {
+    const std::string t = lower(p.spectrum_type);
+    return t == "per_ev" || t == "per_hz" || t == "per_ang" || t == "per_um";
+}
+
+// ion_ext_preset_id, ion_band_mod.f90:895-911.
+static int ext_preset_id(const std::string& name) {
+    const std::string t = lower(trim(name));
+    if (t == "draine") return 1;
+    if (t == "habing") return 2;
+    if (t == "mathis") return 3;
+    return 0;
+}
+
+// draine_je, ion_band_mod.f90:1648-1658.
+static double draine_je(double E) {
+    if (E < 5.0 || E > 13.6) return 0.0;
+    const double E2 = E * E, E3 = E2 * E, E4 = E2 * E2;
+    return EV2ERG * (1.658e6 * E2 - 2.152e5 * E3 + 6.919e3 * E4);
+}
+
+// bbody_si, ion_band_mod.f90:1700-1720.
+static double bbody_si(double T, double lam_um) {
+    const double c_si = 2.99792458e8, h_si = 6.62606957e-34, kB_si = 1.3806488e-23;
+    const double hc2 = (2.0 * h_si) * (c_si * c_si), hckB = h_si * c_si / kB_si;
+    if (T <= 0.0 || lam_um <= 0.0) return 0.0;
+    const double lam_m = lam_um * 1.0e-6;
+    const double x = hckB / (T * lam_m);
+    if (x >= 700.0) return 0.0;
+    const double l2 = lam_m * lam_m, l4 = l2 * l2;
+    return hc2 / (l4 * lam_m) / (std::exp(x) - 1.0);
+}
+
+// mathis_jl_si and mathis_je, ion_band_mod.f90:1660-1698.
+static double mathis_je(double E) {
+    const double lam = HC_EVANG * 1.0e-4 / E;
+    double Jl;
+    if (lam < 0.0912) Jl = 0.0;
+    else if (lam < 0.110) Jl = 3069.0 * std::pow(lam, 3.4172);
+    else if (lam < 0.134) Jl = 1.627;
+    else if (lam < 0.250) Jl = 0.0566 * std::pow(lam, -1.6678);
+    else Jl = 1.0e-14 * bbody_si(7500.0, lam) + 1.65e-13 * bbody_si(4000.0, lam) + 4.0e-13 * bbody_si(3000.0, lam);
+    return Jl * (HC_EVANG * 1.0e-7) / (E * E);
+}
+
+// preset_je, ion_band_mod.f90:1627-1637.
+static double preset_je(double E, int id) {
+    switch (id) {
+        case 1: return draine_je(E);
+        case 2: return draine_je(E) / 1.71;
+        case 3: return mathis_je(E);
+        default: return 0.0;
+    }
+}
+
+// read_shape_table / read_phys_table, ion_band_mod.f90:1438-1597: column
+// icol of ncol value columns, converted to (E [eV], per eV), sorted
+// ascending by insertion.
+static bool read_spec_table(const Par& p, const std::string& fname, int icol, int ncol, std::vector<double>& et,
+                            std::vector<double>& ft, std::string* err) {
+    std::ifstream in(fname);
+    if (!in) {
+        set_err(err, ("cannot open " + fname).c_str());
+        return false;
+    }
+    const std::string type = lower(p.spectrum_type);
+    et.clear();
+    ft.clear();
+    std::string line;
+    while (std::getline(in, line)) {
+        std::string t = trim(line);
+        if (t.empty() || t[0] == '#') continue;
+        for (auto& ch : t) {
+            if (ch == ',') ch = ' ';
+            if (ch == 'd' || ch == 'D') ch = 'e';
+        }
+        std::istringstream ss(t);
+        std::vector<double> row;
+        double v;
+        while ((int)row.size() < ncol + 1 && ss >> v) row.push_back(v);
+        if ((int)row.size() < ncol + 1) {
+            set_err(err, (fname + ": too few columns").c_str());
+            return false;
+        }
+        const double c1 = row[0], cv = row[icol];
+        double ee = c1, xe = cv;
+        if (type == "per_hz") {
+            ee = H_CGS * c1 / EV2ERG;
+            xe = cv * EV2ERG / H_CGS;
+        } else if (type == "per_ang") {
+            ee = HC_EVANG / c1;
+            xe = cv * HC_EVANG / (ee * ee);
+        } else if (type == "per_um") {
+            const double hc = HC_EVANG * 1.0e-4;
+            ee = hc / c1;
+            xe = cv * hc / (ee * ee);
+        }
+        et.push_back(ee);
+        ft.push_back(xe);
+    }
+    const int n = (int)et.size();
+    for (int i = 2; i <= n; ++i)
+        for (int j = i; j >= 2; --j) {
+            if (et[j - 2] <= et[j - 1]) break;
+            std::swap(et[j - 2], et[j - 1]);
+            std::swap(ft[j - 2], ft[j - 1]);
+        }
+    return true;
+}
+
+// source_band_luminosity, ion_band_mod.f90:379-399.
+static bool source_band_L(const Sampler& s, bool is_abs, double scale, double eion_min, double* L, std::string* err) {
+    if (is_abs && scale <= 0.0) {
+        *L = s.total_integral;
+        return true;
+    }
+    const double f_ion = 1.0 - energy_cdf_value(s, eion_min);
+    if (f_ion <= 0.0) {
+        set_err(err, "cannot rescale a source with no ionizing-band luminosity");
+        return false;
+    }
+    *L = scale / f_ion;
+    return true;
+}
+
+// build_point_source_sampler, ion_band_mod.f90:437-495 (is 1-based).
+static bool point_source_sampler(const Par& p, int is, bool multi, double elo, const std::vector<double>& knots,
+                                 Sampler& s, double* L, std::string* err) {
+    const double scale = multi ? p.src_lum[is - 1] : p.luminosity;
+    const bool phys = spec_is_physical(p);
+    std::vector<double> et, ft;
+    if (!p.src_spectrum_file.empty()) {
+        if (!read_spec_table(p, p.src_spectrum_file, is, std::max(p.nsource, 1), et, ft, err)) return false;
+        if (!build_tabulated_band_sampler(s, et, ft, elo, p.eion_max, err)) return false;
+        return source_band_L(s, phys, scale, p.eion_min, L, err);
+    }
+    const double tst = multi ? p.src_tstar[is - 1] : -1.0;
+    if (tst > 0.0) {
+        if (!build_planck_sampler(s, tst, elo, p.eion_max, p.source_cdf_tol, knots, err)) return false;
+        return source_band_L(s, false, scale, p.eion_min, L, err);
+    }
+    if (!p.ion_spectrum.empty()) {
+        if (!read_spec_table(p, p.ion_spectrum, 1, 1, et, ft, err)) return false;
+        if (!build_tabulated_band_sampler(s, et, ft, elo, p.eion_max, err)) return false;
+        return source_band_L(s, phys, scale, p.eion_min, L, err);
+    }
+    if (p.tstar <= 0.0) {
+        set_err(err, "oracle: point source needs a spectrum");
+        return false;
+    }
+    if (!build_planck_sampler(s, p.tstar, elo, p.eion_max, p.source_cdf_tol, knots, err)) return false;
+    return source_band_L(s, false, scale, p.eion_min, L, err);
+}
+
+// build_external_field_sampler, ion_band_mod.f90:516-615.
+static bool external_field_sampler(const Par& p, double elo, const std::vector<double>& knots, const double* box,
+                                   Sampler& s, double* L, std::string* err) {
+    const int presid = ext_preset_id(p.ext_spectrum);
+    const bool is_abs = presid > 0 || (spec_is_physical(p) && !p.ext_spectrum.empty());
+    std::vector<double> et, ft;
+    if (presid > 0) {
+        const double ehi = std::min(p.eion_max, 13.6);
+        if (ehi <= elo) {
+            set_err(err, "the ISRF preset does not overlap the band");
+            return false;
+        }
+        const int N = 4096;
+        et.resize(N);
+        ft.resize(N);
+        for (int k = 1; k <= N; ++k) {
+            et[k - 1] = elo + (ehi - elo) * (double)(k - 1) / (double)(N - 1);
+            ft[k - 1] = preset_je(et[k - 1], presid) * p.ext_scale;
+        }
+        if (!build_tabulated_sampler(s, et, ft, err)) return false;
+    } else if (!p.ext_spectrum.empty()) {
+        if (!read_spec_table(p, p.ext_spectrum, 1, 1, et, ft, err)) return false;
+        if (!build_tabulated_band_sampler(s, et, ft, elo, p.eion_max, err)) return false;
+    } else if (p.ext_tstar > 0.0) {
+        if (!build_planck_sampler(s, p.ext_tstar, elo, p.eion_max, p.source_cdf_tol, knots, err)) return false;
+    } else if (!p.ion_spectrum.empty()) {
+        if (!read_spec_table(p, p.ion_spectrum, 1, 1, et, ft, err)) return false;
+        if (!build_tabulated_band_sampler(s, et, ft, elo, p.eion_max, err)) return false;
+    } else {
+        if (!build_planck_sampler(s, p.tstar, elo, p.eion_max, p.source_cdf_tol, knots, err)) return false;
+    }
+    double asurf;
+    if (p.ext_geometry == "sph") {
+        asurf = 4.0 * PI * ((p.rmax * p.distance2cm) * (p.rmax * p.distance2cm));
+    } else {
+        const double xr = box[0] * p.distance2cm, yr = box[1] * p.distance2cm, zr = box[2] * p.distance2cm;
+        asurf = 2.0 * (xr * yr + yr * zr + zr * xr);
+    }
+    if (is_abs) {
+        *L = p.ext_intensity > 0.0 ? PI * asurf * p.ext_intensity : PI * asurf * s.total_integral;
+        return true;
+    }
+    const double f_ion = 1.0 - energy_cdf_value(s, p.eion_min);
+    if (f_ion <= 0.0) {
+        set_err(err, "the external spectrum has no luminosity inside the ionizing band");
+        return false;
+    }
+    *L = PI * p.ext_intensity * asurf / f_ion;
+    return true;
+}
+
+// ion_setup (ion_band_mod.f90:122-258) for point sources, the external
+// field and the slab, with each component's spectrum chain, plus
 // setup_continuous_source_sampler / build_point_source_sampler
 // (:275-353, :437-495) and ion_qmc_ndim (:654-663).
-bool band_setup(const Par& p, Band& b, std::string* err, const std::vector<double>& metal_eth, const double* box) {
+bool band_setup(const Par& p0, Band& b, std::string* err, const std::vector<double>& metal_eth, const double* box) {
+    // setup.f90:374-442: the luminosity sentinel and the point sources' scales
+    Par p = p0;
+    {
+        const int npt = p.source_geometry == "external" ? 0 : p.nsource;
+        const bool src_abs = spec_is_physical(p) && (!p.src_spectrum_file.empty() || !p.ion_spectrum.empty());
+        if (p.luminosity < -900.0 && !(npt >= 1 && src_abs)) p.luminosity = 1.0;
+        if (npt == 1 && p.src_lum[0] <= 0.0) {
+            p.src_x[0] = p.xs_point; p.src_y[0] = p.ys_point; p.src_z[0] = p.zs_point;
+            p.src_lum[0] = p.luminosity;
+        } else if (npt > 1) {
+            int nset = 0;
+            for (int i = 0; i < npt; ++i) if (p.src_lum[i] > 0.0) ++nset;
+            if (nset == 0 && !src_abs) {
+                for (int i = 0; i < npt; ++i) p.src_lum[i] = p.luminosity / (double)npt;
+            } else if (nset != 0 && nset != npt) {
+                set_err(err, "set par%src_lum for ALL sources or for NONE");
+                return false;
+            }
+        }
+    }
     int nfuv = 0;
     if (p.add_fuv) {
         if (p.efuv_min >= p.eion_min) {
@@ -940,7 +1171,8 @@ bool band_setup(const Par& p, Band& b, std::string* err, const std::vector<doubl
         if (p.add_fuv) knots.push_back(p.eion_min);
         b.samplers.resize(1);
         const double elo = p.add_fuv ? p.efuv_min : p.eion_min;
-        if (!build_planck_sampler(b.samplers[0], p.tstar, elo, p.eion_max, p.source_cdf_tol, knots, err)) return false;
+        double unused;
+        if (!point_source_sampler(p, 1, false, elo, knots, b.samplers[0], &unused, err)) return false;
         const double f_ion = 1.0 - energy_cdf_value(b.samplers[0], p.eion_min);
         if (f_ion <= 0.0) {
             set_err(err, "the slab spectrum has no luminosity inside the ionizing band");
@@ -955,7 +1187,8 @@ bool band_setup(const Par& p, Band& b, std::string* err, const std::vector<doubl
     }
     // components, ion_band_mod.f90:188-199 and 683-711: the point sources,
     // then the external field
-    const bool ext_on = p.ext_intensity > 0.0;
+    const bool ext_on = p.ext_intensity > 0.0 || ext_preset_id(p.ext_spectrum) > 0 ||
+                        (spec_is_physical(p) && !p.ext_spectrum.empty());   // external_on, :884-889
     if (ext_on && !box && p.ext_geometry != "sph") {
         set_err(err, "oracle: the external field needs the box extent");
         return false;
@@ -972,38 +1205,11 @@ bool band_setup(const Par& p, Band& b, std::string* err, const std::vector<doubl
     b.samplers.resize(b.ncomp);
     std::vector<double> band_L(b.ncomp);
     for (int ic = 0; ic < b.ncomp; ++ic) {
-        if (ic == b.ext_ic) {   // build_external_field_sampler, :516-615 (Planck spectra)
-            const double tst = p.ext_tstar > 0.0 ? p.ext_tstar : p.tstar;
-            if (!build_planck_sampler(b.samplers[ic], tst, elo, p.eion_max, p.source_cdf_tol, knots, err)) return false;
-            double asurf;
-            if (p.ext_geometry == "sph") {
-                asurf = 4.0 * PI * ((p.rmax * p.distance2cm) * (p.rmax * p.distance2cm));
-            } else {
-                const double xr = box[0] * p.distance2cm, yr = box[1] * p.distance2cm, zr = box[2] * p.distance2cm;
-                asurf = 2.0 * (xr * yr + yr * zr + zr * xr);
-            }
-            const double f_ion = 1.0 - energy_cdf_value(b.samplers[ic], p.eion_min);
-            if (f_ion <= 0.0) {
-                set_err(err, "the external spectrum has no luminosity inside the ionizing band");
-                return false;
-            }
-            band_L[ic] = PI * p.ext_intensity * asurf / f_ion;
+        if (ic == b.ext_ic) {
+            if (!external_field_sampler(p, elo, knots, box, b.samplers[ic], &band_L[ic], err)) return false;
             continue;
         }
-        const double tst = (b.multi_src && p.src_tstar[ic] > 0.0) ? p.src_tstar[ic] : p.tstar;
-        const double scale = b.multi_src ? p.src_lum[ic] : p.luminosity;
-        if (tst <= 0.0) {
-            set_err(err, "oracle: point source needs a Planck temperature");
-            return false;
-        }
-        if (!build_planck_sampler(b.samplers[ic], tst, elo, p.eion_max, p.source_cdf_tol, knots, err)) return false;
-        // source_band_luminosity, ion_band_mod.f90:379-399
-        const double f_ion = 1.0 - energy_cdf_value(b.samplers[ic], p.eion_min);
-        if (f_ion <= 0.0) {
-            set_err(err, "source has no ionizing-band luminosity");
-            return false;
-        }
-        band_L[ic] = scale / f_ion;
+        if (!point_source_sampler(p, ic + 1, b.multi_src, elo, knots, b.samplers[ic], &band_L[ic], err)) return false;
     }
     b.ion_Ltot = 0.0;
     for (double L : band_L) b.ion_Ltot += L;
@@ -1011,6 +1217,9 @@ bool band_setup(const Par& p, Band& b, std::string* err, const std::vector<doubl
         b.comp_kind.resize(b.ncomp);
         b.src_cdf.resize(b.ncomp);
         for (int ic = 0; ic < b.ncomp; ++ic) b.comp_kind[ic] = ic == b.ext_ic ? 0 : ic + 1;
+        b.src_x.assign(p.src_x, p.src_x + MAX_SRC);
+        b.src_y.assign(p.src_y, p.src_y + MAX_SRC);
+        b.src_z.assign(p.src_z, p.src_z + MAX_SRC);
         b.src_cdf[0] = band_L[0];
         for (int ic = 1; ic < b.ncomp; ++ic) b.src_cdf[ic] = b.src_cdf[ic - 1] + band_L[ic];
         const double last = b.src_cdf[b.ncomp - 1];
@@ -1347,7 +1556,7 @@ void Sim::gen_photon_qmc(int64_t ip, Photon& ph) const {
             for (int i = 0; i < band.ncomp; ++i)
                 if (u[0] <= band.src_cdf[i]) { ic = i; break; }
             const int ik = band.comp_kind[ic];
-            if (ik >= 1) { xs = par.src_x[ik - 1]; ys = par.src_y[ik - 1]; zs = par.src_z[ik - 1]; }
+            if (ik >= 1) { xs = band.src_x[ik - 1]; ys = band.src_y[ik - 1]; zs = band.src_z[ik - 1]; }
         }
         umu = u[2]; uphi = u[3];
         e = sample_energy_cdf(band.samplers[ic], u[1]);

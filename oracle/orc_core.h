@@ -138,6 +138,9 @@ struct Par {
     double slab_top_theta = 0.0, slab_bot_theta = 0.0, slab_top_phi = 0.0, slab_bot_phi = 0.0;
     double slab_top_source = 0.0, slab_bot_source = 0.0;
     int slab_nmu = 20;
+    // tabulated spectra and ISRF presets (define.f90:276-303)
+    std::string ion_spectrum, src_spectrum_file, ext_spectrum, spectrum_type = "shape_ev";
+    double ext_scale = 1.0;
     double xs_point = 0.0, ys_point = 0.0, zs_point = 0.0;
     int nsource = 1;
     double src_tstar[MAX_SRC], src_lum[MAX_SRC];
@@ -187,6 +190,7 @@ struct Band {
     bool multi_src = false;
     std::vector<int> comp_kind;      // multi only
     std::vector<double> src_cdf;     // multi only
+    std::vector<double> src_x, src_y, src_z;   // point positions after setup.f90:398-407
     int ext_ic = -1;                 // the external field's component, -1 none
     std::vector<Sampler> samplers;   // source_energy_sampler
     double ion_Ltot = 0.0;
