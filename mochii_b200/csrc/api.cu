@@ -156,9 +156,6 @@ int validate(const mochii_params& p, std::string* why, int* code) {
         return *why = "the taumax / tauhomo dust normalisations are not built", 1;
     if (p.ion_add_dust && !p.ion_dust_kext[0])
         return *why = "ion_add_dust needs par%ion_dust_kext (the grain-model optics are not built)", 1;
-    if (p.ion_peel && (p.ext_intensity > 0.0 || p.source_external || spectrum_preset_id(p.ext_spectrum) > 0 ||
-                       (p.spectrum_type != 0 && p.ext_spectrum[0])))
-        return *why = "the peel-off of external-field packets is not built", 1;
     *code = MOCHII_ERR_BAD_PARAM;
     if (p.ion_peel && p.xy_periodic)   // setup.f90:531-539
         return *why = "par%ion_peel is not supported with par%xy_periodic (use the slab's boundary I(mu) tally)", 1;

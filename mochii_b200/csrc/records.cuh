@@ -11,11 +11,18 @@
 
 namespace mochii {
 
+// Record bits above the bin and DDA steps: an external-field packet
+// (photon%from_external) and its entry surface, 0-5 the box face
+// (+x, -x, +y, -y, +z, -z), 6 the sphere.
+constexpr int kExternalBit = 1 << 22;
+constexpr int kExternalFaceShift = 23;
+
 struct PacketRecords {
     double* tm;    // 3 x cap (octree: start point)
     double* td;    // 3 x cap (octree: direction)
     int* cell;     // ix | iy << 10 | iz << 20 (octree: start leaf, -1 outside)
-    int* bits;     // inu | (stp_x+1) << 16 | (stp_y+1) << 18 | (stp_z+1) << 20 (octree: inu)
+    int* bits;     // inu | (stp_x+1) << 16 | (stp_y+1) << 18 | (stp_z+1) << 20 (octree: inu),
+                   // + kExternalBit | face << kExternalFaceShift for external packets
     void* sig;     // 3 x cap of R: sigma_HI, sigma_HeI, sigma_HeII in 1e-18 cm^2
                    // (+ a 4th row with grains or FUV: the dust extinction coefficient)
     void* coef;    // 6 x cap of R: Gamma/heat coefficients per unit path

@@ -292,7 +292,7 @@ __device__ double block_sum(double v, double* sh) {
 // 2 pi u_phi), the entry point uniform on the face (u_c1, u_c2), nudged
 // 1e-6 of the smallest extent inside.
 __device__ void emit_external_rec(const PassArgs& a, double u_mu, double u_phi, double u_face, double u_c1,
-                                  double u_c2, double pos[3], double kk[3]) {
+                                  double u_c2, double pos[3], double kk[3], int* face_out = nullptr) {
     const double xr = a.bmax[0] - a.bmin[0], yr = a.bmax[1] - a.bmin[1], zr = a.bmax[2] - a.bmin[2];
     const double nudge = 1.0e-6 * fmin(xr, fmin(yr, zr));
     double fcum[6];
@@ -318,6 +318,7 @@ __device__ void emit_external_rec(const PassArgs& a, double u_mu, double u_phi, 
     kk[ax] = sgn * mu;
     kk[a1] = sinm * cphi;
     kk[a2] = sinm * sphi;
+    if (face_out) *face_out = f;
 }
 
 // emit_external_sph_qmc (:2328-2361) with ortho_frame (:2368-2385): the
@@ -391,8 +392,9 @@ __device__ void emit_slab(const PassArgs& a, double u_face, double u_c1, double 
 // phi; every other configuration the superset layout -- u1 component, u2
 // energy, u3/u4 angles, u5-u7 the entry surface of an external field.
 __device__ __forceinline__ void launch_packet(const PassArgs& a, const double* u, int& ic, double& E, double pos[3],
-                                              double kk[3]) {
+                                              double kk[3], int* xface = nullptr) {
     ic = 0;
+    if (xface) *xface = -1;
     double umu, uphi, ue;
     if (a.slab) {
         const int t0 = a.tab_off[0], t1 = a.tab_off[1];
@@ -414,7 +416,8 @@ __device__ __forceinline__ void launch_packet(const PassArgs& a, const double* u
     E = sample_energy(a.tab_e + t0, a.tab_f + t0, a.tab_c + t0, t1 - t0, ue);
     if (ic == a.ext_ic) {
         if (a.ext_sph) emit_external_sph(a, u[2], u[3], u[4], u[5], pos, kk);
-        else emit_external_rec(a, u[2], u[3], u[4], u[5], u[6], pos, kk);
+        else emit_external_rec(a, u[2], u[3], u[4], u[5], u[6], pos, kk, xface);
+        if (xface && a.ext_sph) *xface = 6;
     } else {   // emit_point_qmc (:2232-2247)
         pos[0] = a.comp[4 * ic + 1]; pos[1] = a.comp[4 * ic + 2]; pos[2] = a.comp[4 * ic + 3];
         const double cost = 2.0 * umu - 1.0;
@@ -443,14 +446,15 @@ __global__ void __launch_bounds__(kThreads) k_launch(const PassArgs a, PacketRec
     const long long ip = ip0 + (rec.order ? (long long)rec.order[i] : i);
     double u[7];
     for (int d = 0; d < a.ndim; ++d) u[d] = qmc_uniform(sq, (uint64_t)ip, d, 0);
-    int ic;
+    int ic, xface;
     double E, pos[3], kk[3];
-    launch_packet(a, u, ic, E, pos, kk);
+    launch_packet(a, u, ic, E, pos, kk, &xface);
     const int inu = bin_of(a.eedge, a.nnu, E);
     if constexpr (AMR)   // emit_point_qmc: photon%icell_amr = amr_find_leaf (ion_band_mod.f90:2245)
         write_record_amr<R>(rec, i, pos, kk, E, inu, oct_find_leaf(a.oct, pos[0], pos[1], pos[2], sgeo, schild));
     else
         write_record<R>(rec, i, pos, kk, E, inu, a.org, a.dcell, a.n);
+    if (xface >= 0) rec.bits[i] |= kExternalBit | (xface << kExternalFaceShift);   // photon%from_external
     if (a.xs) write_grain_record<R>(rec, i, a.dust, a.scatter, a.eion_min, E, pos, kk, AMR ? 0 : 1);
     if (a.m.ntr > 0) write_metal_record<R>(rec, a.m, i, E);
     if (rec.key) rec.key[i] = packet_dir_key(ic, kk);
@@ -905,9 +909,25 @@ __device__ __forceinline__ bool peel_pixel(const PeelDev& p, const double* o, do
 // observer's pixel, the unattenuated part to the direc0 image.
 template <bool AMR, typename KapF>
 __device__ void peel_direct(const PassArgs& a, double x, double y, double z, int il, int inu, double wl,
-                            KapF& kappa_at) {
+                            KapF& kappa_at, int bits = 0) {
     const PeelDev& p = a.peel;
     const int ch = __ldg(p.chan + inu);
+    // an external packet peels max(k_obs . n_in, 0) / pi about the inward
+    // normal of its entry surface (ion_peel_mod.f90:254-263): a box face's
+    // axis, or toward the sphere's centre
+    const bool ext = bits & kExternalBit;
+    double nin[3] = {0.0, 0.0, 0.0};
+    if (ext) {
+        const int f = (bits >> kExternalFaceShift) & 7;
+        if (f < 6) {
+            nin[f >> 1] = (f & 1) ? 1.0 : -1.0;
+        } else {
+            const double dx = x - 0.5 * (a.bmin[0] + a.bmax[0]), dy = y - 0.5 * (a.bmin[1] + a.bmax[1]);
+            const double dz = z - 0.5 * (a.bmin[2] + a.bmax[2]);
+            const double rr = sqrt(dx * dx + dy * dy + dz * dz);
+            nin[0] = -dx / rr; nin[1] = -dy / rr; nin[2] = -dz / rr;
+        }
+    }
     for (int k = 0; k < p.nobs; ++k) {
         const double* o = p.obs + k * kPeelObs;
         double kx = __ldg(o) - x, ky = __ldg(o + 1) - y, kz = __ldg(o + 2) - z;
@@ -916,7 +936,14 @@ __device__ void peel_direct(const PassArgs& a, double x, double y, double z, int
         int ix, iy;
         if (!peel_pixel(p, o, kx, ky, kz, &ix, &iy)) continue;
         const long long pix = ((long long)(k * p.nchan + ch) * p.nyim + iy) * p.nxim + ix;
-        const double contrib = wl / (4.0 * kPi * r2);
+        double contrib;
+        if (ext) {
+            const double cos_obs = kx * nin[0] + ky * nin[1] + kz * nin[2];
+            if (cos_obs <= 0.0) continue;   // the observer-side surface shows nothing
+            contrib = wl * cos_obs / (kPi * r2);
+        } else {
+            contrib = wl / (4.0 * kPi * r2);
+        }
         if (p.direc0) atomicAdd(p.img_dir0 + pix, contrib);
         const double tau = tau_to_edge<AMR>(a, x, y, z, kx, ky, kz, il, kappa_at);
         if (tau > 500.0) continue;
@@ -1068,7 +1095,7 @@ __global__ void __launch_bounds__(128) k_walk_edge(const PassArgs a, const Packe
                 }
                 return k;
             };
-            peel_direct<false>(a, rec.p0[i], rec.p0[c + i], rec.p0[2 * c + i], -1, inu, a.Lpacket, kap_p);
+            peel_direct<false>(a, rec.p0[i], rec.p0[c + i], rec.p0[2 * c + i], -1, inu, a.Lpacket, kap_p, bits);
         }
         // ring of LA+1 cells: il, segment, columns, and whether a next cell exists
         int il[LA + 1] = {};
@@ -1413,7 +1440,7 @@ __global__ void __launch_bounds__(128) k_walk_amr(const PassArgs a, const Packet
                 }
                 return k;
             };
-            peel_direct<true>(a, x, y, z, il, inu, a.Lpacket, kap_p);
+            peel_direct<true>(a, x, y, z, il, inu, a.Lpacket, kap_p, rec.bits[i]);
         }
         R expo = (R)1.0;
         double tau = 0.0;

@@ -1492,6 +1492,10 @@ void Sim::emit_external_rec(double u_mu, double u_phi, double u_face, double u_c
         if (fpick <= fcum[i]) { iface = i + 1; break; }
     const double mu = std::sqrt(u_mu), sinm = std::sqrt(1.0 - mu * mu), phi = TWOPI * u_phi;
     const double cphi = std::cos(phi), sphi = std::sin(phi);
+    ph.from_external = true;
+    ph.snx = iface == 1 ? -1.0 : iface == 2 ? 1.0 : 0.0;
+    ph.sny = iface == 3 ? -1.0 : iface == 4 ? 1.0 : 0.0;
+    ph.snz = iface == 5 ? -1.0 : iface == 6 ? 1.0 : 0.0;
     switch (iface) {
         case 1: ph.x = grid.xmax - nudge; ph.y = grid.ymin + yr * u_c1; ph.z = grid.zmin + zr * u_c2;
                 ph.kx = -mu; ph.ky = sinm * cphi; ph.kz = sinm * sphi; break;
@@ -1516,6 +1520,8 @@ void Sim::emit_external_sph(double u_mu, double u_phi, double u_cost, double u_s
     ph.x = xc + par.rmax * rhx;
     ph.y = yc + par.rmax * rhy;
     ph.z = zc + par.rmax * rhz;
+    ph.from_external = true;
+    ph.snx = -rhx; ph.sny = -rhy; ph.snz = -rhz;
     const double nx = -rhx, ny = -rhy, nz = -rhz;
     double tx, ty, tz;
     if (std::fabs(nx) <= std::fabs(ny) && std::fabs(nx) <= std::fabs(nz)) { tx = 0.0; ty = nz; tz = -ny; }
@@ -1538,6 +1544,8 @@ void Sim::emit_external_sph(double u_mu, double u_phi, double u_cost, double u_s
 // gen_ion_photon_qmc, ion_band_mod.f90:1880-1935, with emit_point_qmc
 // (:2232-2247) and build_ion_packet_physics (ion_packet_mod.f90:21-53).
 void Sim::gen_photon_qmc(int64_t ip, Photon& ph) const {
+    ph.from_external = false;
+    ph.snx = ph.sny = ph.snz = 0.0;
     double u[12];
     for (int d = 1; d <= band.qmc_ndim; ++d) u[d - 1] = qmc.uniform(ip, d, 1);
     double e;
@@ -2323,6 +2331,8 @@ void Sim::diffuse_build(double lpacket) {
 
 // gen_diffuse_photon_qmc, diffuse_mod.f90:221-296.
 void Sim::gen_diffuse_qmc(int64_t ip, Photon& ph) const {
+    ph.from_external = false;
+    ph.snx = ph.sny = ph.snz = 0.0;
     double u[9];
     for (int d = 1; d <= 9; ++d) u[d - 1] = qmc.uniform(ip, d, 2);
     const int nleaf = grid.nleaf;
@@ -2756,7 +2766,14 @@ void Sim::peel_direct(const Photon& ph, Tally& t) const {
         int ix, iy;
         if (!peel_pixel(o, kx, ky, kz, &ix, &iy)) continue;
         const size_t pix = ((k * nchan + ch) * (size_t)ny + iy) * nx + ix;
-        double contrib = ph.Lpacket * ph.wgt / (FOURPI * r2);
+        double contrib;
+        if (ph.from_external) {   // ion_peel_mod.f90:254-263
+            const double cos_obs = kx * ph.snx + ky * ph.sny + kz * ph.snz;
+            if (cos_obs <= 0.0) continue;
+            contrib = ph.Lpacket * ph.wgt * cos_obs / (PI * r2);
+        } else {
+            contrib = ph.Lpacket * ph.wgt / (FOURPI * r2);
+        }
         if (par.save_direc0) t.img_dir0[pix] += contrib;
         const double tau = tau_only(ph, kx, ky, kz);
         if (tau > 500.0) continue;

@@ -248,6 +248,8 @@ struct Photon {
     double dust_abs = 0.0, dust_sca = 0.0, dust_g = 0.0;   // ionphys dust cache
     int nscatt = 0;
     bool inside = true;
+    bool from_external = false;      // photon%from_external and the entry surface's inward normal
+    double snx = 0.0, sny = 0.0, snz = 0.0;
     PacketRng rng;                   // the packet's scattering stream
 };
 

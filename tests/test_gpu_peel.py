@@ -89,3 +89,35 @@ def test_imaging_pass_needs_observers():
         neb.imaging_pass()
     assert ei.value.status == 1
     neb.close()
+
+
+@pytest.mark.parametrize("kind", ["rec_car", "mixed_car", "sph_amr"])
+def test_peel_external_field_matches_oracle(orc, tmp_path, kind):
+    """External-field packets peel max(k_obs . n_in, 0) / pi about the inward
+    normal of their entry surface (ion_peel_mod.f90:254-263): the box faces
+    on the Cartesian grid, alone and composed with a point source, and the
+    bounding sphere on the octree; direct and unattenuated images."""
+    from conftest import octree_leaf_list
+    nl = configs.hhe128(nphotons=20000, niter=1, n=16, precision="fp64")
+    L = parse_namelist(nl).xmax
+    if kind == "sph_amr":
+        leaves = str(tmp_path / "leaves.txt")
+        octree_leaf_list(leaves, 2.0 * L, base_level=3, max_level=5, seed=9)
+        nl = configs.on_octree(nl, leaves)
+        ext = f" par%source_geometry = 'external_sph'\n par%ext_intensity = 3.0e-3\n par%rmax = {0.8 * L}\n"
+    elif kind == "rec_car":
+        ext = " par%source_geometry = 'external_rec'\n par%ext_intensity = 3.0e-3\n"
+    else:
+        ext = " par%ext_intensity = 3.0e-3\n par%ext_geometry = 'rec'\n par%xs_point = 0.3\n"
+    nl = nl.replace("/\n", ext + " par%ion_peel = .true.\n par%nxim = 33\n par%nyim = 29\n par%save_direc0 = .true.\n"
+                                 " par%alpha(1) = 0.0, 40.0\n par%beta(1) = 0.0, 70.0\n/\n")
+    neb = Nebula(parse_namelist(nl))
+    sim = orc.Sim(nl)
+    st = neb.imaging_pass()
+    sim.imaging_pass()
+    assert st.closure <= 5e-13
+    for which in ("direct", "direct0"):
+        g, o = neb.image(which), sim.peel_image(which)
+        assert o.sum() > 0 and np.count_nonzero(o) > 50, which   # the field lights the whole box outline
+        np.testing.assert_allclose(g, o, rtol=1e-9, atol=1e-12 * o.max(), err_msg=which)
+    neb.close()
