@@ -24,7 +24,7 @@ LIB = os.path.join(HERE, "libmochii_gpu.so")
 
 SOURCES = ["api.cu", "transport.cu", "balance.cu", "diffuse.cu", "band.cpp", "params.cpp", "thermal_setup.cpp", "species_setup.cpp",
            "octree_setup.cpp", "dust_setup.cpp", "dust_temp.cu", "mlp.cu", "output.cpp", "peel.cpp",
-           "refine.cpp", "spectrum.cpp"]
+           "refine.cpp", "refine_dev.cu", "spectrum.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FMA_SOURCES = {"balance.cu"}   # tolerance-checked FP64 solves: fused multiply-add allowed
 

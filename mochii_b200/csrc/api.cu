@@ -217,8 +217,16 @@ extern "C" int mochii_init(const mochii_params* pin, mochii_ctx** out) {
     if (!p.grid_car) {
         std::vector<int> lev;
         double boxlen = 0.0;
-        if (!leaf_list_read(p.amr_file, lx, ly, lz, lev, lnH, &boxlen, &why) ||
-            !octree_build(lx, ly, lz, lev, 0.5 * boxlen, oh, &why)) {
+        bool read_ok;
+        if (g_leaf_preload) {   // the refined leaves of mochii_refine_front
+            lx = *g_leaf_preload->x; ly = *g_leaf_preload->y; lz = *g_leaf_preload->z;
+            lev = *g_leaf_preload->lev; lnH = *g_leaf_preload->nH;
+            boxlen = g_leaf_preload->boxlen;
+            read_ok = true;
+        } else {
+            read_ok = leaf_list_read(p.amr_file, lx, ly, lz, lev, lnH, &boxlen, &why);
+        }
+        if (!read_ok || !octree_build(lx, ly, lz, lev, 0.5 * boxlen, oh, &why)) {
             delete c;
             return fail(nullptr, MOCHII_ERR_BAD_PARAM, why);
         }

@@ -65,4 +65,14 @@ bool octree_build(const std::vector<double>& x, const std::vector<double>& y, co
 // cell_cx/cy/cz/ch (octree_mod.f90:113-153) and car_next (:620-641).
 void car_walk_tables(int nx, int ny, int nz, double xmin, double ymin, double zmin, double dcell, OctHost& o);
 
+// A leaf list held in memory: set by the re-refinement around the
+// mochii_init of the refined context, which then takes its leaves from here
+// instead of reading par%amr_file (same thread only).
+struct LeafList {
+    const std::vector<double>*x, *y, *z, *nH;
+    const std::vector<int>* lev;
+    double boxlen;
+};
+extern thread_local const LeafList* g_leaf_preload;
+
 }  // namespace mochii

@@ -197,4 +197,6 @@ void car_walk_tables(int nx, int ny, int nz, double xmin, double ymin, double zm
             }
 }
 
+thread_local const LeafList* g_leaf_preload = nullptr;
+
 }  // namespace mochii

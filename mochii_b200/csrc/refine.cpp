@@ -27,25 +27,14 @@
 #include <string>
 #include <vector>
 
+#include <charconv>
+
 #include "ctx.h"
 #include "mochii_gpu.h"
 #include "octree.h"
+#include "refine.h"
 
 namespace mochii {
-
-struct RefineIn {
-    const double *nH, *xHI, *xHeI, *xHeII, *ne, *Te, *rk;   // rk may be null (no grains)
-    double yHe, te_min;
-    int lbase, lmax;
-    double eps, dx;
-};
-
-struct RefineOut {
-    std::vector<double> x, y, z, nH, x1, x2, x3, ne, te, rk;
-    std::vector<int> lev;
-    long long nfront = 0;
-    double before[7] = {}, after[7] = {}, worst = 0.0;
-};
 
 namespace {
 
@@ -213,13 +202,23 @@ bool refine_plan(const OctHost& o, const RefineIn& in, RefineOut& out, std::stri
         if (err) *err = "re-refinement: octree descent stack overflow";
         return false;
     }
+    std::vector<double> lh(nold);
+    for (int il = 0; il < nold; ++il) lh[il] = o.lgeo[4 * (size_t)il + 3];
+    return refine_check(in, lh, o.half, out, err);
+}
+
+// conservation_report (:299-352): the seven box integrals before (old leaf
+// half widths lh) and after, the largest relative change at most 1e-8.
+bool refine_check(const RefineIn& in, const std::vector<double>& lh, double half, RefineOut& out, std::string* err) {
+    const long long nold = (long long)lh.size();
+    const size_t nn = out.x.size();
     std::vector<double> vold(nold), vnew(nn);
-    for (int il = 0; il < nold; ++il) {
-        const double w = 2.0 * o.lgeo[4 * (size_t)il + 3];
+    for (long long il = 0; il < nold; ++il) {
+        const double w = 2.0 * lh[il];
         vold[il] = w * w * w;
     }
     for (size_t i = 0; i < nn; ++i) {
-        const double w = 2.0 * o.half / std::ldexp(1.0, out.lev[i]);
+        const double w = 2.0 * half / std::ldexp(1.0, out.lev[i]);
         vnew[i] = w * w * w;
     }
     integrals(nold, in.nH, in.xHI, in.xHeI, in.xHeII, in.ne, in.Te, in.rk, in.yHe, vold, out.before);
@@ -246,9 +245,36 @@ bool refine_write(const std::string& path, double boxlen, const RefineOut& r, st
         return false;
     }
     std::fprintf(f, "%zu %.17g\n", r.x.size(), boxlen);
-    for (size_t i = 0; i < r.x.size(); ++i)
-        std::fprintf(f, "%.17g %.17g %.17g %d %.17g %.17g %.17g %.17g %.17g %.17g %.17g\n", r.x[i], r.y[i], r.z[i],
-                     r.lev[i], r.nH[i], r.x1[i], r.x2[i], r.x3[i], r.ne[i], r.te[i], r.rk[i]);
+    // std::to_chars in general format with precision 17 writes what printf's
+    // %.17g does, without the format parsing
+    std::vector<char> buf;
+    buf.reserve(1 << 22);
+    char tmp[64];
+    auto put = [&](double v, char sep) {
+        const auto res = std::to_chars(tmp, tmp + sizeof(tmp), v, std::chars_format::general, 17);
+        buf.insert(buf.end(), tmp, res.ptr);
+        buf.push_back(sep);
+    };
+    for (size_t i = 0; i < r.x.size(); ++i) {
+        put(r.x[i], ' ');
+        put(r.y[i], ' ');
+        put(r.z[i], ' ');
+        const auto res = std::to_chars(tmp, tmp + sizeof(tmp), r.lev[i]);
+        buf.insert(buf.end(), tmp, res.ptr);
+        buf.push_back(' ');
+        put(r.nH[i], ' ');
+        put(r.x1[i], ' ');
+        put(r.x2[i], ' ');
+        put(r.x3[i], ' ');
+        put(r.ne[i], ' ');
+        put(r.te[i], ' ');
+        put(r.rk[i], '\n');
+        if (buf.size() > (1u << 22) - 512) {
+            std::fwrite(buf.data(), 1, buf.size(), f);
+            buf.clear();
+        }
+    }
+    if (!buf.empty()) std::fwrite(buf.data(), 1, buf.size(), f);
     if (std::fclose(f) != 0) {
         if (err) *err = "cannot write " + path;
         return false;
@@ -293,11 +319,17 @@ extern "C" int mochii_refine_plan(const char* in_list, const double* nH, const d
 extern "C" const char* mochii_refine_last_error(void) { return g_refine_err.c_str(); }
 
 extern "C" int mochii_refine_front(mochii_ctx* c, const char* out_list, mochii_ctx** out) {
-    if (!c || !out_list || !out) return MOCHII_ERR_BAD_PARAM;
+    if (!c || !out) return MOCHII_ERR_BAD_PARAM;
     if (c->oct.ncells == 0 || c->par.grid_car) {
         c->last_error = "mochii_refine_front: needs an octree grid (grid_type = 'amr')";
         return MOCHII_ERR_UNSUPPORTED;
     }
+    const mochii_params& p = c->par;
+    if (p.refine_lbase < 0 || p.refine_lmax < p.refine_lbase || p.refine_lmax > 20) {
+        c->last_error = "mochii_refine_front: need 0 <= par%refine_lbase <= par%refine_lmax <= 20";
+        return MOCHII_ERR_BAD_PARAM;
+    }
+    // the old state on the host for the conserved integrals
     const long long n = c->grid.nleaf;
     std::vector<double> f[6];
     const char* names[6] = {"nH", "x_HI", "x_HeI", "x_HeII", "n_e", "T_e"};
@@ -311,43 +343,37 @@ extern "C" int mochii_refine_front(mochii_ctx* c, const char* out_list, mochii_c
         if (cudaMemcpy(rk.data(), c->rhokap, (size_t)n * 8, cudaMemcpyDeviceToHost) != cudaSuccess)
             return MOCHII_ERR_CUDA;
     }
-    const mochii_params& p = c->par;
-    int64_t counts[2];
-    double worst = 0.0;
-    int rc = mochii_refine_plan(p.amr_file, f[0].data(), f[1].data(), f[2].data(), f[3].data(), f[4].data(),
-                                f[5].data(), c->rhokap ? rk.data() : nullptr, p.He_abund, p.te_min, p.refine_lbase,
-                                p.refine_lmax, p.refine_eps, p.refine_dx, out_list, counts, &worst);
-    if (rc) {
-        c->last_error = "mochii_refine_front: " + g_refine_err;
-        return rc;
+    RefineIn in{f[0].data(), f[1].data(), f[2].data(), f[3].data(), f[4].data(), f[5].data(),
+                c->rhokap ? rk.data() : nullptr, p.He_abund, p.te_min, p.refine_lbase, p.refine_lmax,
+                p.refine_eps, p.refine_dx};
+    RefineOut r;
+    std::string why;
+    if (!refine_plan_device(c, in, r, &why) || !refine_check(in, c->lhalf, c->oct.half, r, &why)) {
+        c->last_error = "mochii_refine_front: " + why;
+        return MOCHII_ERR_BAD_PARAM;
     }
-    // the new context from the refined leaf list, its state set from the remap
+    const double boxlen = 2.0 * c->oct.half;
+    if (out_list && out_list[0] && !refine_write(out_list, boxlen, r, &why)) {
+        c->last_error = "mochii_refine_front: " + why;
+        return MOCHII_ERR_BAD_PARAM;
+    }
+    // the new context from the refined leaves in memory, its state from the remap
     mochii_params q = p;
-    std::snprintf(q.amr_file, sizeof(q.amr_file), "%s", out_list);
+    std::snprintf(q.amr_file, sizeof(q.amr_file), "%s", out_list && out_list[0] ? out_list : "(refined in memory)");
+    const LeafList ll{&r.x, &r.y, &r.z, &r.nH, &r.lev, boxlen};
     mochii_ctx* nc = nullptr;
-    if ((rc = mochii_init(&q, &nc))) {
+    g_leaf_preload = &ll;
+    int rc = mochii_init(&q, &nc);
+    g_leaf_preload = nullptr;
+    if (rc) {
         c->last_error = std::string("mochii_refine_front: ") + mochii_last_error(nullptr);
         return rc;
     }
-    std::vector<double> cols[5];
-    for (auto& v : cols) v.reserve((size_t)counts[0]);
-    FILE* fl = std::fopen(out_list, "r");
-    bool ok = fl != nullptr;
-    if (ok) {
-        long long nl = 0;
-        double bl = 0.0;
-        ok = std::fscanf(fl, "%lld %lf", &nl, &bl) == 2 && nl == counts[0];
-        for (long long i = 0; ok && i < nl; ++i) {
-            double x, y, z, nh, v[6];
-            int lv;
-            ok = std::fscanf(fl, "%lf %lf %lf %d %lf %lf %lf %lf %lf %lf %lf", &x, &y, &z, &lv, &nh, &v[0], &v[1], &v[2],
-                             &v[3], &v[4], &v[5]) == 11;
-            for (int k = 0; ok && k < 5; ++k) cols[k].push_back(v[k]);
-        }
-        std::fclose(fl);
-    }
+    const long long nn = (long long)r.x.size();
+    const std::vector<double>* cols[5] = {&r.x1, &r.x2, &r.x3, &r.ne, &r.te};
     const char* set[5] = {"x_HI", "x_HeI", "x_HeII", "n_e", "T_e"};
-    for (int k = 0; ok && k < 5; ++k) ok = mochii_set_field(nc, set[k], cols[k].data(), counts[0]) == MOCHII_OK;
+    bool ok = true;
+    for (int k = 0; ok && k < 5; ++k) ok = mochii_set_field(nc, set[k], cols[k]->data(), nn) == MOCHII_OK;
     if (!ok || (rc = mochii_opacity_fill(nc))) {
         mochii_destroy(nc);
         c->last_error = "mochii_refine_front: cannot set the remapped state";

@@ -71,3 +71,46 @@ def test_driver_refines_once_and_keeps_iterating(tmp_path):
     assert ev[0]["refined"]["leaves_after"] == neb.nleaf != ev[0]["refined"]["leaves_before"]
     assert len(hist) >= 3 and all(h["closure"] <= 5e-13 for h in hist)
     neb.close()
+
+
+@pytest.mark.parametrize("grid", ["g2a", "irregular"])
+def test_device_plan_equals_host_plan(tmp_path, grid):
+    """The device plan (front flags, level-by-level build sorted into
+    depth-first order, remap) writes the same leaf list as the host plan on
+    the same tree and state, to the last bit of every remapped value."""
+    from conftest import octree_leaf_list
+    if grid == "g2a":
+        nl = sphere(tmp_path)
+        par = parse_namelist(nl.replace("/\n", " par%refine_lbase = 3\n par%refine_lmax = 6\n/\n"))
+        neb = Nebula(par)
+        for _ in range(2):
+            neb.ionizing_field_and_rates()
+            neb.gas_equilibrium_update()
+            neb.gas_opacity_fill()
+        lbase, lmax = 3, 6
+    else:
+        src = str(tmp_path / "leaves.txt")
+        octree_leaf_list(src, 8.0, base_level=2, max_level=5, p_split=0.35, seed=11)
+        nl = configs.on_octree(configs.hhe128(nphotons=1000, niter=1, n=8, precision="fp64"), src)
+        par = parse_namelist(nl.replace("/\n", " par%refine_lbase = 2\n par%refine_lmax = 6\n/\n"))
+        neb = Nebula(par)
+        rows = np.loadtxt(src, skiprows=1, ndmin=2)
+        r = np.sqrt((rows[:, :3] ** 2).sum(axis=1)) / 4.0
+        xHI = np.clip(1.0 / (1.0 + np.exp(-(r - 0.5) / 0.08)), 1e-6, 1.0)
+        xHeI = np.clip(1.5 * xHI, 0.0, 1.0)
+        neb.set("x_HI", xHI)
+        neb.set("x_HeI", xHeI)
+        neb.set("x_HeII", 1.0 - xHeI)
+        neb.set("n_e", rows[:, 4] * ((1.0 - xHI) + 0.1 * (1.0 - xHeI)))
+        neb.set("T_e", 3e3 + 7e3 * (1.0 - xHI))
+        lbase, lmax = 2, 6
+    st = {k: neb.get(k) for k in ("nH", "x_HI", "x_HeI", "x_HeII", "n_e", "T_e")}
+    dev = str(tmp_path / "device.txt")
+    new = neb.refine_front(dev)
+    hst = str(tmp_path / "host.txt")
+    nn, nf, worst = host.refine_plan(par.amr_file.decode(), st, He_abund=par.He_abund, te_min=par.te_min,
+                                     lbase=lbase, lmax=lmax, eps=par.refine_eps, dx=par.refine_dx, out_list=hst)
+    assert nf > 10 and nn == new.nleaf and worst < 1e-8
+    assert open(dev).read() == open(hst).read()
+    new.close()
+    neb.close()
