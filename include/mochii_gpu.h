@@ -406,7 +406,8 @@ int mochii_write_rates(mochii_ctx* ctx, const char* base, const mochii_run_info*
  * that claims 32-leaf chunks of every nebula from one counter) -- is recorded
  * as one CUDA graph at the first mochii_batch_iterate and replayed after.
  * The contexts must not use the diffuse field (its packet count is read back
- * mid-pass) or the MLP warm start; their own calls stay usable between
+ * mid-pass), the slab (its boundary tally is read back after each standalone
+ * pass) or the MLP warm start; their own calls stay usable between
  * iterations, but changing a context's parameters or tuning (mochii_set_nphotons,
  * mochii_set_tuning, mochii_autotune, a first T_warm or MLP warm start) needs
  * a new batch: mochii_batch_iterate refuses with MOCHII_ERR_BAD_PARAM before

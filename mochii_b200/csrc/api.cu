@@ -701,6 +701,8 @@ extern "C" int mochii_batch_create(mochii_ctx* const* ctxs, int n, mochii_batch*
         if (!c) return fail(nullptr, MOCHII_ERR_BAD_PARAM, "mochii_batch_create: null context");
         if (c->par.diffuse_field)
             return fail(nullptr, MOCHII_ERR_UNSUPPORTED, "batched nebulae: par%diffuse_field must be off");
+        if (c->band.slab)   // the slab's boundary tally is read back per standalone pass only
+            return fail(nullptr, MOCHII_ERR_UNSUPPORTED, "batched nebulae: source_geometry='slab' is not batched");
         if (c->device != ctxs[0]->device)
             return fail(nullptr, MOCHII_ERR_BAD_PARAM, "batched nebulae: the contexts must share one device");
     }
