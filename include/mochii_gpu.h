@@ -354,9 +354,11 @@ int mochii_write_slab_imu(mochii_ctx* ctx, const char* base);
  * and the seven conserved box integrals (H nuclei, H I, He I, He II,
  * electrons, extinction, thermal content) must agree to 1e-8.  Every
  * leaf-indexed buffer changes size, so the result is a NEW context:
- * mochii_refine_front writes the new leaf list to out_list (the generic
- * text format, with the remapped x_HI, x_HeI, x_HeII, n_e, T_e and rhokap
- * as extra columns), initialises *out from it with ctx's parameters and
+ * mochii_refine_front plans on the device (front flags, the new tree level
+ * by level in depth-first order, the remap), writes the new leaf list to
+ * out_list when it is a non-empty path (the generic text format, with the
+ * remapped x_HI, x_HeI, x_HeII, n_e, T_e and rhokap as extra columns),
+ * initialises *out from the new leaves in memory with ctx's parameters and
  * sets the remapped state; ctx is left as it was (destroy it when done).
  * The grains' rhokap of the new context follows from the remapped nH as
  * at any set-up (the same volume remap for the supported dust laws).
