@@ -604,7 +604,8 @@ def main():
                          "frac": achieved / peak, "peak_kind": peak_kind,
                          "traffic": traffic, "traffic_kind": traffic_kind,
                          "kernel": ("transport pass: k_coherent_keys, key sort, k_launch, k_walk_coh (stellar "
-                                    "chunks); k_launch_diffuse, k_walk_edge (diffuse chunks)"
+                                    "chunks); k_diffuse_keys, key sort, k_launch_diffuse, k_walk_coh (diffuse "
+                                    "chunks)"
                                     if neb_order(neb) == "coherent" else "transport pass: k_launch + k_walk_edge"),
                          "bytes_per_segment": alg_bytes / mean_seg, "segments_per_launch": mean_seg,
                          "kernel_ms": mean_ms},

@@ -317,7 +317,19 @@ struct DiffLaunchArgs {
     long long nleaf;
 };
 
-// gen_diffuse_photon_qmc (diffuse_mod.f90:221-296) and dda_init.
+// The emitting leaf of gen_diffuse_photon_qmc: the first leaf whose
+// normalised CDF reaches u1.
+__device__ __forceinline__ long long diffuse_leaf(const DiffLaunchArgs& a, double u0) {
+    long long lo = 1, hi = a.nleaf;
+    while (lo < hi) {
+        const long long mid = (lo + hi) / 2;
+        if (a.cum[mid - 1] / a.total < u0) lo = mid + 1; else hi = mid;
+    }
+    return lo - 1;
+}
+
+// gen_diffuse_photon_qmc (diffuse_mod.f90:221-296) and dda_init.  With
+// rec.order (packet_order 'coherent') record i holds chunk packet order[i].
 template <typename R>
 __global__ void __launch_bounds__(kThreads) k_launch_diffuse(const DiffLaunchArgs a, PacketRecords rec, long long ip0,
                                                              long long n) {
@@ -330,17 +342,11 @@ __global__ void __launch_bounds__(kThreads) k_launch_diffuse(const DiffLaunchArg
     __syncthreads();
     const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    const uint64_t ip = (uint64_t)(ip0 + i);
+    const uint64_t ip = (uint64_t)(ip0 + (rec.order ? (long long)rec.order[i] : i));
     double u[9];
 #pragma unroll
     for (int d = 0; d < 9; ++d) u[d] = qmc_uniform(sq, ip, d, 1);
-    // first leaf whose normalised CDF reaches u1
-    long long lo = 1, hi = a.nleaf;
-    while (lo < hi) {
-        const long long mid = (lo + hi) / 2;
-        if (a.cum[mid - 1] / a.total < u[0]) lo = mid + 1; else hi = mid;
-    }
-    const long long il = lo - 1;
+    const long long il = diffuse_leaf(a, u[0]);
     double pos[3];
     if (a.lg) {   // leaf centre and half width of the octree leaf
         const double4 g = a.lg[il];
@@ -394,6 +400,27 @@ __global__ void __launch_bounds__(kThreads) k_launch_diffuse(const DiffLaunchArg
     if (a.metal.ntr > 0) write_metal_record<R>(rec, a.metal, i, eph);
 }
 
+// Walk-order keys of packet_order 'coherent' for the diffuse packets
+// ip0 .. ip0+n-1 on the Cartesian grid: the emitting leaf and the direction
+// uniforms of gen_diffuse_photon_qmc reduced to diffuse_coherent_key.
+__global__ void __launch_bounds__(kThreads) k_diffuse_keys(const DiffLaunchArgs a, long long ip0, long long n,
+                                                           unsigned* __restrict__ key) {
+    __shared__ QmcTables sq;
+    {
+        const uint32_t* src = reinterpret_cast<const uint32_t*>(a.qmc);
+        uint32_t* dst = reinterpret_cast<uint32_t*>(&sq);
+        for (int i = threadIdx.x; i < (int)(sizeof(QmcTables) / 4); i += blockDim.x) dst[i] = src[i];
+    }
+    __syncthreads();
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const uint64_t ip = (uint64_t)(ip0 + i);
+    const long long il = diffuse_leaf(a, qmc_uniform(sq, ip, 0, 1));
+    const int ix = (int)(il % a.n[0]), iy = (int)((il / a.n[0]) % a.n[1]);
+    const int iz = (int)(il / ((long long)a.n[0] * a.n[1]));
+    key[i] = diffuse_coherent_key(qmc_uniform(sq, ip, 4, 1), qmc_uniform(sq, ip, 5, 1), ix, iy, iz, a.n);
+}
+
 int nblk(long long work, int threads, int cap) {
     long long b = (work + threads - 1) / threads;
     return (int)(b < 1 ? 1 : b > cap ? cap : b);
@@ -438,7 +465,8 @@ size_t diffuse_scan_bytes(long long nleaf) {
     return bytes;
 }
 
-cudaError_t launch_diffuse_chunk(mochii_ctx* c, double total, long long ip0, long long n) {
+namespace {
+DiffLaunchArgs diffuse_launch_args(mochii_ctx* c, double total) {
     DiffLaunchArgs a;
     a.qmc = c->tab.qmc;
     a.cum = c->dif.tot;
@@ -464,7 +492,20 @@ cudaError_t launch_diffuse_chunk(mochii_ctx* c, double total, long long ip0, lon
     a.nfuv = c->band.nfuv_band;
     a.energy_model = c->par.diffuse_model;
     a.nleaf = c->grid.nleaf;
-    const PacketRecords r = packet_records(c);
+    return a;
+}
+}  // namespace
+
+cudaError_t launch_diffuse_keys(mochii_ctx* c, double total, long long ip0, long long n, unsigned* key) {
+    const DiffLaunchArgs a = diffuse_launch_args(c, total);
+    k_diffuse_keys<<<nblk(n, kThreads, 1 << 30), kThreads, 0, c->stream>>>(a, ip0, n, key);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_diffuse_chunk(mochii_ctx* c, double total, long long ip0, long long n, const int* order) {
+    const DiffLaunchArgs a = diffuse_launch_args(c, total);
+    PacketRecords r = packet_records(c);
+    r.order = order;
     if (c->fp32) k_launch_diffuse<float><<<nblk(n, kThreads, 1 << 30), kThreads, 0, c->stream>>>(a, r, ip0, n);
     else k_launch_diffuse<double><<<nblk(n, kThreads, 1 << 30), kThreads, 0, c->stream>>>(a, r, ip0, n);
     return cudaGetLastError();

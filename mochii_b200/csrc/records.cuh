@@ -54,6 +54,27 @@ __device__ __forceinline__ unsigned coherent_key(int ic, double umu, double uphi
     return ((unsigned)(ic & 15) << 21) | (((band << 7) | sec) << 8) | eq;
 }
 
+// Walk-order key of a diffuse packet under packet_order 'coherent', from
+// its launch uniforms and start cell: a direction cell of 32 equal-area
+// bands in cos(theta) x 32 sectors in phi, the sectors of odd bands
+// reversed (10 bits), above the Morton code of the start cell on a 32^3
+// coarsening of the grid (15 bits).  Packets of one warp then leave nearly
+// parallel from one neighbourhood, so their walks stay together and end
+// together.  Fits the kCohKeyBits of the stellar key.
+__device__ __forceinline__ unsigned diffuse_coherent_key(double umu, double uphi, int ix, int iy, int iz,
+                                                         const int* n) {
+    const unsigned band = (unsigned)min((int)(umu * 32.0), 31);
+    unsigned sec = (unsigned)min((int)(uphi * 32.0), 31);
+    if (band & 1u) sec = 31u - sec;
+    const unsigned cx = (unsigned)min((ix * 32) / n[0], 31), cy = (unsigned)min((iy * 32) / n[1], 31),
+                   cz = (unsigned)min((iz * 32) / n[2], 31);
+    unsigned m = 0;
+#pragma unroll
+    for (int b = 0; b < 5; ++b)
+        m |= (((cx >> b) & 1u) << (3 * b)) | (((cy >> b) & 1u) << (3 * b + 1)) | (((cz >> b) & 1u) << (3 * b + 2));
+    return (((band << 5) | sec) << 15) | m;
+}
+
 constexpr int kPacketKeyBits = 18;
 
 // Walk-order key of a stellar packet: source component (3 bits), direction

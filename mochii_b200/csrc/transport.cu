@@ -1889,8 +1889,9 @@ struct WalkLaunch {
     bool coherent = false;   // records in coherent_key order, walked by k_walk_coh
 };
 
-// packet_order 'coherent' applies to the stellar packets on the Cartesian
-// grid without grain or FUV terms; elsewhere the launch order is walked.
+// packet_order 'coherent' applies to the stellar and the diffuse packets on
+// the Cartesian grid without grain or FUV terms; elsewhere the launch order
+// is walked.
 bool coherent_walk_applies(const mochii_ctx* c) {
     return c->par.packet_order == 2 && c->oct.ncells == 0 && !c->xscore && c->rec.key != nullptr && !c->peeling &&
            !c->band.slab;
@@ -2062,13 +2063,27 @@ cudaError_t launch_transport(mochii_ctx* c) {
 }
 
 // The diffuse packets (ionizing_field_mod.f90:139-161): their launch records
-// come from launch_diffuse_chunk, the walk is the stellar one.
+// come from launch_diffuse_chunk, the walk is the stellar one.  Under
+// packet_order 'coherent' each chunk is sorted by diffuse_coherent_key and
+// launched and walked (k_walk_coh) in that order, as the stellar chunks are.
 cudaError_t launch_transport_diffuse(mochii_ctx* c, double total, long long nd) {
     const PassArgs a = make_args(c);
     const PacketRecords r = packet_records(c);
     const int blocks = c->tw.ledger_blocks;
     for (long long ip0 = 0; ip0 < nd; ip0 += r.cap) {
         const long long n = nd - ip0 < r.cap ? nd - ip0 : r.cap;
+        if (coherent_walk_applies(c)) {
+            cudaError_t e = launch_diffuse_keys(c, total, ip0, n, c->rec.key);
+            if (e != cudaSuccess) return e;
+            e = cub::DeviceRadixSort::SortPairs(c->rec.sort_tmp, c->rec.sort_bytes, c->rec.key, c->rec.key_sorted,
+                                                c->rec.seq, c->rec.perm, (int)n, 0, kCohKeyBits, c->stream);
+            if (e != cudaSuccess) return e;
+            if ((e = launch_diffuse_chunk(c, total, ip0, n, c->rec.perm)) != cudaSuccess) return e;
+            WalkLaunch wl{n, ip0, 1, blocks, 1};
+            wl.coherent = true;
+            if ((e = launch_walk_variant(c, a, r, wl)) != cudaSuccess) return e;
+            continue;
+        }
         cudaError_t e = launch_diffuse_chunk(c, total, ip0, n);
         if (e != cudaSuccess) return e;
         e = launch_walk_variant(c, a, r, WalkLaunch{n, ip0, 1, blocks, 1, false});

@@ -14,7 +14,12 @@ PacketRecords packet_records(mochii_ctx* c);
 cudaError_t launch_transport_diffuse(mochii_ctx* c, double total, long long nd);
 cudaError_t diffuse_build(mochii_ctx* c, double* total);
 size_t diffuse_scan_bytes(long long nleaf);
-cudaError_t launch_diffuse_chunk(mochii_ctx* c, double total, long long ip0, long long n);
+// Records of diffuse packets ip0 .. ip0+n-1; with order, record i holds
+// chunk packet order[i].
+cudaError_t launch_diffuse_chunk(mochii_ctx* c, double total, long long ip0, long long n,
+                                 const int* order = nullptr);
+// diffuse_coherent_key of diffuse packets ip0 .. ip0+n-1 (Cartesian grid).
+cudaError_t launch_diffuse_keys(mochii_ctx* c, double total, long long ip0, long long n, unsigned* key);
 cudaError_t launch_rates(mochii_ctx* c);
 cudaError_t peel_setup(mochii_ctx* c);   // par%ion_peel: observers, image plane, device images (peel.cpp)
 cudaError_t peel_clear(mochii_ctx* c);   // zero the images before an imaging pass

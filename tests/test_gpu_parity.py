@@ -364,3 +364,41 @@ def test_coherent_order_scores_what_launch_order_scores(precision):
         x, y = a[1][f], b[1][f]
         big = x > 1e-9 * x.max()
         assert np.max(np.abs(y[big] / x[big] - 1)) < tol, (f, np.max(np.abs(y[big] / x[big] - 1)))
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_coherent_diffuse_order_scores_what_launch_order_scores(precision):
+    """Diffuse packets sorted by direction cell and start neighbourhood and
+    walked by the coherent walk, against the same packets walked in launch
+    order, in chunks so that several sorted diffuse chunks accumulate: the
+    same packet count, scored segments and energy ledger, rates equal to
+    FP64 reassociation (FP64) or to the FP32 warp sums (FP32)."""
+    n = 32
+    nl = small_nl(n=n, nphot=40000, he=0.1, precision=precision)
+    nl = nl.replace("/\n", " par%packet_chunk = 1024\n par%diffuse_field = .true.\n/\n")
+    L = parse_namelist(nl).xmax
+    state = partially_ionised_state(n, L)
+    state["x_HeI"] = np.clip(state["x_HI"] * 1.5, 0, 1)
+    state["x_HeII"] = 1.0 - state["x_HeI"]
+    state["n_e"] = 100.0 * ((1.0 - state["x_HI"]) + 0.1 * state["x_HeII"])   # nH_const 100
+    state["T_e"] = np.full(n ** 3, 9000.0)
+    out = {}
+    for order in ("launch", "coherent"):
+        neb = Nebula(parse_namelist(nl.replace("/\n", f" par%packet_order = '{order}'\n/\n")))
+        for k, v in state.items():
+            neb.set(k, v)
+        neb.gas_opacity_fill()
+        st = neb.ionizing_field_and_rates()
+        out[order] = (st, {f: neb.get(f) for f in ("gamma_HI", "gamma_HeI", "heat_HI", "jt_ion")})
+        neb.close()
+    a, b = out["launch"], out["coherent"]
+    assert a[0].diffuse_packets > 2 * 1024 and a[0].diffuse_packets == b[0].diffuse_packets
+    assert a[0].direct_segments == b[0].direct_segments
+    assert abs(a[0].energy_emitted / b[0].energy_emitted - 1) < 1e-12
+    assert abs(a[0].energy_absorbed / b[0].energy_absorbed - 1) < 1e-12
+    assert b[0].closure <= 5e-13
+    tol = 1e-12 if precision == "fp64" else 2e-6
+    for f in a[1]:
+        x, y = a[1][f], b[1][f]
+        big = x > 1e-9 * x.max()
+        assert np.max(np.abs(y[big] / x[big] - 1)) < tol, (f, np.max(np.abs(y[big] / x[big] - 1)))
