@@ -159,12 +159,13 @@ typedef struct mochii_params {
     /* packets per launch-walk chunk (not a reference key, par%packet_chunk):
      * the size of the packet-record buffer, default 4194304 */
     int64_t packet_chunk;
-    /* walk order of a chunk's stellar packets (not a reference key,
+    /* walk order of a chunk's packets (not a reference key,
      * par%packet_order): 2 'coherent' (default) = the chunk sorted by source,
-     * direction cell and energy quantile before its launch, each warp walking
-     * 32 nearly parallel packets of nearly equal energy and summing the
-     * tallies of lanes in the same leaf and bins before one reduction (the
-     * Cartesian grid without grains or FUV; elsewhere the launch order);
+     * direction cell and energy quantile (diffuse packets: direction cell and
+     * start neighbourhood) before its launch, each warp walking 32 nearly
+     * parallel packets and summing the tallies of lanes in the same leaf and
+     * bins before one reduction (the Cartesian grid without grains or FUV;
+     * elsewhere the launch order);
      * 0 'launch' = the launch (Sobol) order; 1 'direction' = sorted by source
      * and direction cell after the launch, per-lane reductions */
     int packet_order;
